@@ -1,0 +1,211 @@
+"""ctypes mirrors of the plain-data structs in include/lotus_cuda.h.
+
+The C ABI is the boundary that replaces the reference's
+``Lotus::OffscreenRenderer`` (include/lotus/vulkan_backend.hpp:753-842 in
+hydra-lotus); these mirrors let Python hosts, tests and the benchmark fill
+and read its structs. ``check_struct_sizes`` compares them with the sizes
+the compiled library reports.
+"""
+
+import ctypes as C
+
+PASS = 0
+FAIL = 1
+SKIP = 77
+
+INTEGRATOR_REFERENCE = 0
+INTEGRATOR_WAVEFRONT = 1
+
+LIGHT_SAMPLING_BSDF = 0
+LIGHT_SAMPLING_MIS = 1
+LIGHT_SAMPLING_RESTIR_INITIAL = 2
+
+MAX_BOUNCES = 1024
+MAX_REPORTED_BOUNCES = 64
+
+MATERIAL_SPECULAR_WORKFLOW = 1
+MATERIAL_THIN_WALLED = 2
+
+ABI_VERSION = 1
+
+
+class Geometry(C.Structure):
+    _fields_ = [
+        ("positions", C.POINTER(C.c_float)),
+        ("triangles", C.POINTER(C.c_uint32)),
+        ("normals", C.POINTER(C.c_float)),
+        ("vertex_count", C.c_uint32),
+        ("triangle_count", C.c_uint32),
+    ]
+
+
+class Instance(C.Structure):
+    _fields_ = [
+        ("world_from_object", C.c_float * 16),
+        ("geometry", C.c_uint32),
+        ("material", C.c_uint32),
+    ]
+
+
+class Material(C.Structure):
+    _fields_ = [
+        ("base_color", C.c_float * 3),
+        ("roughness", C.c_float),
+        ("emission", C.c_float * 3),
+        ("metallic", C.c_float),
+        ("specular_color", C.c_float * 3),
+        ("ior", C.c_float),
+        ("transmission_color", C.c_float * 3),
+        ("transmission", C.c_float),
+        ("opacity", C.c_float),
+        ("opacity_threshold", C.c_float),
+        ("flags", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class Environment(C.Structure):
+    _fields_ = [
+        ("texels", C.POINTER(C.c_float)),
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("scale", C.c_float * 3),
+        ("environment_from_world", C.c_float * 9),
+    ]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("geometries", C.POINTER(Geometry)),
+        ("instances", C.POINTER(Instance)),
+        ("materials", C.POINTER(Material)),
+        ("environment", C.POINTER(Environment)),
+        ("geometry_count", C.c_uint32),
+        ("instance_count", C.c_uint32),
+        ("material_count", C.c_uint32),
+        ("environment_constant", C.c_float * 3),
+    ]
+
+
+class SceneResult(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("triangle_count", C.c_uint32),
+        ("instance_count", C.c_uint32),
+        ("light_count", C.c_uint32),
+        ("bvh_node_count", C.c_uint32),
+        ("tlas_node_count", C.c_uint32),
+        ("build_gpu_ms", C.c_double),
+        ("device_bytes", C.c_uint64),
+        ("detail", C.c_char * 256),
+    ]
+
+
+class Target(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("display_window", C.c_float * 4),
+        ("data_window", C.c_int32 * 4),
+        ("clear_color", C.c_float * 4),
+        ("read_back", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class Settings(C.Structure):
+    _fields_ = [
+        ("integrator", C.c_uint32),
+        ("light_sampling", C.c_uint32),
+        ("sample_index", C.c_uint32),
+        ("max_bounces", C.c_uint32),
+        ("max_samples", C.c_uint32),
+        ("restir_candidates", C.c_uint32),
+        ("restir_temporal", C.c_uint32),
+        ("restir_max_history_candidates", C.c_uint32),
+        ("restir_spatial", C.c_uint32),
+        ("restir_spatial_radius", C.c_uint32),
+        ("restir_proposal", C.c_uint32),
+        ("environment_background", C.c_uint32),
+    ]
+
+
+class FrameDesc(C.Structure):
+    _fields_ = [
+        ("world_to_clip", C.c_float * 16),
+        ("target", Target),
+        ("settings", Settings),
+        ("frame_count", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class FrameResult(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("frames_rendered", C.c_uint32),
+        ("samples_per_pixel", C.c_uint32),
+        ("wavefront_rounds", C.c_uint32),
+        ("completion", C.c_uint64),
+        ("camera_rays", C.c_uint64),
+        ("extension_rays", C.c_uint64),
+        ("shadow_rays", C.c_uint64),
+        ("gpu_ms", C.c_double),
+        ("wavefront_path_counts", C.c_uint32 * MAX_REPORTED_BOUNCES),
+        ("wavefront_path_count_size", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("detail", C.c_char * 256),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int32), ("flags", C.c_uint32)]
+
+
+# The order lotus_cuda_struct_sizes reports them in.
+STRUCTS = [Geometry, Instance, Material, Environment, SceneDesc, SceneResult,
+           Target, Settings, FrameDesc, FrameResult, Options]
+
+
+def default_settings(**overrides):
+    """PathTracingSettings' defaults (vulkan_backend.hpp:697-738)."""
+    s = Settings(integrator=INTEGRATOR_REFERENCE,
+                 light_sampling=LIGHT_SAMPLING_MIS,
+                 sample_index=0, max_bounces=64, max_samples=0,
+                 restir_candidates=8, restir_temporal=0,
+                 restir_max_history_candidates=32, restir_spatial=0,
+                 restir_spatial_radius=1, restir_proposal=0,
+                 environment_background=0)
+    for k, v in overrides.items():
+        setattr(s, k, v)
+    return s
+
+
+def make_frame(world_to_clip, width, height, settings=None, frame_count=1,
+               clear_color=(0.0, 0.0, 0.0, 0.0), data_window=(0, 0, 0, 0),
+               display_window=(0.0, 0.0, 0.0, 0.0), read_back=True):
+    f = FrameDesc()
+    for i, v in enumerate(world_to_clip):
+        f.world_to_clip[i] = float(v)
+    f.target.width = width
+    f.target.height = height
+    for i in range(4):
+        f.target.display_window[i] = display_window[i]
+        f.target.data_window[i] = data_window[i]
+        f.target.clear_color[i] = clear_color[i]
+    f.target.read_back = 1 if read_back else 0
+    f.settings = settings if settings is not None else default_settings()
+    f.frame_count = frame_count
+    return f
+
+
+def check_struct_sizes(lib):
+    """Raises when a ctypes mirror's size differs from the C struct's."""
+    sizes = (C.c_uint64 * 32)()
+    n = lib.lotus_cuda_struct_sizes(sizes, 32)
+    if n != len(STRUCTS):
+        raise RuntimeError(f"library reports {n} structs, bindings know {len(STRUCTS)}")
+    for i, s in enumerate(STRUCTS):
+        if C.sizeof(s) != sizes[i]:
+            raise RuntimeError(f"{s.__name__}: ctypes {C.sizeof(s)} bytes, C {sizes[i]} bytes")
+    return [int(sizes[i]) for i in range(n)]

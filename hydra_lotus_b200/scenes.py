@@ -1,0 +1,483 @@
+"""Scene descriptions and the seeded synthetic workloads.
+
+A ``Scene`` holds numpy arrays in the layout of include/lotus_cuda.h and
+turns them into a ``lotus_scene_desc`` that both the CUDA library and the
+oracle read. The workloads are procedural and seeded; no dataset is used:
+
+- ``cornell_reference``: the reference's own Cornell box fixture
+  (adapters/common/reference.cpp:221-279 in hydra-lotus), which its golden
+  images validation/reference/cornell-box-{mean,variance}.pfm were rendered
+  from. Used to pin the oracle and the kernels against those images.
+- ``box_room``: the small box room workload (36 triangles, 256x256).
+- ``sphere_field``: the 1080p workload of 4096 instanced, Perlin-displaced
+  icospheres over a 100x100 ground grid with 64 emissive triangles and an
+  importance-sampled 2048x1024 sky.
+"""
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import abi
+
+F32 = np.float32
+
+
+# ---------------------------------------------------------------------------
+# Matrices (column-major 4x4 floats, Lotus::Matrix4)
+
+def identity():
+    return np.eye(4, dtype=F32).reshape(-1, order="F")
+
+
+def multiply(left, right):
+    """Multiply (render_world.cpp:288-300): float sums in the same order."""
+    left = np.asarray(left, dtype=F32)
+    right = np.asarray(right, dtype=F32)
+    out = np.zeros(16, dtype=F32)
+    for column in range(4):
+        for row in range(4):
+            s = F32(0.0)
+            for index in range(4):
+                s = F32(s + F32(left[index * 4 + row] * right[column * 4 + index]))
+            out[column * 4 + row] = s
+    return out
+
+
+def perspective(fovy_degrees, aspect, near, far):
+    """OpenGL projection, column-major."""
+    f = 1.0 / math.tan(math.radians(fovy_degrees) / 2.0)
+    m = np.zeros(16, dtype=F32)
+    m[0] = f / aspect
+    m[5] = f
+    m[10] = (far + near) / (near - far)
+    m[11] = -1.0
+    m[14] = 2.0 * far * near / (near - far)
+    return m
+
+
+def look_at(eye, target, up=(0.0, 1.0, 0.0)):
+    """World to a right-handed view space looking down -Z, column-major."""
+    eye = np.asarray(eye, dtype=np.float64)
+    forward = np.asarray(target, dtype=np.float64) - eye
+    forward /= np.linalg.norm(forward)
+    right = np.cross(forward, np.asarray(up, dtype=np.float64))
+    right /= np.linalg.norm(right)
+    true_up = np.cross(right, forward)
+    rot = np.stack([right, true_up, -forward])  # rows
+    m = np.eye(4)
+    m[:3, :3] = rot
+    m[:3, 3] = -rot @ eye
+    return m.astype(F32).reshape(-1, order="F")
+
+
+def affine(linear=None, translation=(0.0, 0.0, 0.0)):
+    m = np.eye(4, dtype=np.float64)
+    if linear is not None:
+        m[:3, :3] = linear
+    m[:3, 3] = translation
+    return m.astype(F32).reshape(-1, order="F")
+
+
+def rotation_y(radians):
+    c, s = math.cos(radians), math.sin(radians)
+    return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]], dtype=np.float64)
+
+
+def rotation_xyz(rx, ry, rz):
+    cx, sx = math.cos(rx), math.sin(rx)
+    cy, sy = math.cos(ry), math.sin(ry)
+    cz, sz = math.cos(rz), math.sin(rz)
+    x = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    y = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    z = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    return z @ y @ x
+
+
+# ---------------------------------------------------------------------------
+# Scene
+
+def preview_material(base_color=(0.18, 0.18, 0.18), roughness=0.5, metallic=0.0,
+                     ior=1.5, emission=(0.0, 0.0, 0.0), specular_color=(0.0, 0.0, 0.0),
+                     transmission=0.0, transmission_color=(1.0, 1.0, 1.0),
+                     opacity=1.0, opacity_threshold=0.0, flags=0):
+    """UsdPreviewSurface with its defaults (material.hpp:137-173)."""
+    m = abi.Material()
+    m.base_color[:] = [float(v) for v in base_color]
+    m.roughness = roughness
+    m.metallic = metallic
+    m.ior = ior
+    m.emission[:] = [float(v) for v in emission]
+    m.specular_color[:] = [float(v) for v in specular_color]
+    m.transmission = transmission
+    m.transmission_color[:] = [float(v) for v in transmission_color]
+    m.opacity = opacity
+    m.opacity_threshold = opacity_threshold
+    m.flags = flags
+    return m
+
+
+class Scene:
+    """A scene in the C ABI's layout, plus its camera and target size."""
+
+    def __init__(self, name="scene"):
+        self.name = name
+        self.geometries = []
+        self.instances = []
+        self.materials = [preview_material()]  # slot 0: the default material
+        self.environment = None
+        self.environment_constant = (0.0, 0.0, 0.0)
+        self.world_to_clip = identity()
+        self.width = 0
+        self.height = 0
+        self._desc = None
+
+    def add_geometry(self, positions, triangles, normals=None):
+        positions = np.ascontiguousarray(positions, dtype=F32).reshape(-1, 3)
+        triangles = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        if normals is not None:
+            normals = np.ascontiguousarray(normals, dtype=F32).reshape(-1, 3, 3)
+        self.geometries.append((positions, triangles, normals))
+        self._desc = None
+        return len(self.geometries) - 1
+
+    def add_material(self, material):
+        self.materials.append(material)
+        self._desc = None
+        return len(self.materials) - 1
+
+    def add_instance(self, geometry, material, world_from_object=None):
+        m = identity() if world_from_object is None else np.asarray(world_from_object, dtype=F32)
+        self.instances.append((m.copy(), geometry, material))
+        self._desc = None
+        return len(self.instances) - 1
+
+    def set_environment(self, texels, scale=(1.0, 1.0, 1.0), rows=None):
+        texels = np.ascontiguousarray(texels, dtype=F32)
+        assert texels.ndim == 3 and texels.shape[2] == 4
+        rows = np.eye(3, dtype=F32) if rows is None else np.asarray(rows, dtype=F32)
+        self.environment = (texels, tuple(scale), rows)
+        self._desc = None
+
+    @property
+    def triangle_count(self):
+        return sum(int(t.shape[0]) for _, t, _ in self.geometries)
+
+    @property
+    def traced_triangle_count(self):
+        return sum(int(self.geometries[g][1].shape[0]) for _, g, _ in self.instances)
+
+    def desc(self):
+        """The lotus_scene_desc; the Scene keeps its arrays alive."""
+        if self._desc is not None:
+            return self._desc
+        geos = (abi.Geometry * max(1, len(self.geometries)))()
+        for i, (p, t, n) in enumerate(self.geometries):
+            geos[i].positions = p.ctypes.data_as(C.POINTER(C.c_float))
+            geos[i].triangles = t.ctypes.data_as(C.POINTER(C.c_uint32))
+            geos[i].normals = (n.ctypes.data_as(C.POINTER(C.c_float)) if n is not None
+                               else C.POINTER(C.c_float)())
+            geos[i].vertex_count = p.shape[0]
+            geos[i].triangle_count = t.shape[0]
+        insts = (abi.Instance * max(1, len(self.instances)))()
+        for i, (m, g, mat) in enumerate(self.instances):
+            insts[i].world_from_object[:] = [float(v) for v in m]
+            insts[i].geometry = g
+            insts[i].material = mat
+        mats = (abi.Material * len(self.materials))(*self.materials)
+        d = abi.SceneDesc()
+        d.geometries = geos
+        d.instances = insts
+        d.materials = mats
+        d.geometry_count = len(self.geometries)
+        d.instance_count = len(self.instances)
+        d.material_count = len(self.materials)
+        d.environment_constant[:] = [float(v) for v in self.environment_constant]
+        env = None
+        if self.environment is not None:
+            texels, scale, rows = self.environment
+            env = abi.Environment()
+            env.texels = texels.ctypes.data_as(C.POINTER(C.c_float))
+            env.height, env.width = texels.shape[0], texels.shape[1]
+            env.scale[:] = [float(v) for v in scale]
+            env.environment_from_world[:] = [float(v) for v in rows.reshape(-1)]
+            d.environment = C.pointer(env)
+        self._keep = (geos, insts, mats, env)
+        self._desc = d
+        return d
+
+    def frame(self, settings=None, frame_count=1, **kw):
+        return abi.make_frame(self.world_to_clip, self.width, self.height, settings,
+                              frame_count, **kw)
+
+
+# ---------------------------------------------------------------------------
+# Meshes
+
+def quad(corners):
+    """Quad (reference.cpp:24-31): four corners around it, two triangles."""
+    return np.asarray(corners, dtype=F32), np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32)
+
+
+def unit_cube():
+    """UnitCube (reference.cpp:33-43)."""
+    p = np.array([[-.5, -.5, -.5], [.5, -.5, -.5], [.5, .5, -.5], [-.5, .5, -.5],
+                  [-.5, -.5, .5], [.5, -.5, .5], [.5, .5, .5], [-.5, .5, .5]], dtype=F32)
+    t = np.array([[0, 2, 1], [0, 3, 2], [4, 5, 6], [4, 6, 7], [0, 1, 5], [0, 5, 4],
+                  [3, 7, 6], [3, 6, 2], [0, 4, 7], [0, 7, 3], [1, 2, 6], [1, 6, 5]],
+                 dtype=np.uint32)
+    return p, t
+
+
+def block(size, degrees, centre):
+    """Block (reference.cpp:45-56): scale the unit cube, turn it about +Y,
+    move it."""
+    radians = degrees * 3.14159265358979323846 / 180.0
+    c = F32(math.cos(radians))
+    s = F32(math.sin(radians))
+    sx, sy, sz = (F32(v) for v in size)
+    return np.array([c * sx, 0, -s * sx, 0, 0, sy, 0, 0, s * sz, 0, c * sz, 0,
+                     centre[0], centre[1], centre[2], 1], dtype=F32)
+
+
+def icosphere(subdivisions):
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t),
+             (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9),
+             (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2),
+             (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+             (8, 6, 7), (9, 8, 1)]
+    v = np.array(verts, dtype=np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array(faces, dtype=np.int64)
+    for _ in range(subdivisions):
+        edges = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        edges.sort(axis=1)
+        unique, inverse = np.unique(edges, axis=0, return_inverse=True)
+        mids = v[unique[:, 0]] + v[unique[:, 1]]
+        mids /= np.linalg.norm(mids, axis=1, keepdims=True)
+        base = v.shape[0]
+        v = np.concatenate([v, mids])
+        n = f.shape[0]
+        inverse = inverse.reshape(-1)
+        a = base + inverse[:n]
+        b = base + inverse[n:2 * n]
+        c = base + inverse[2 * n:]
+        f = np.concatenate([np.stack([f[:, 0], a, c], 1), np.stack([f[:, 1], b, a], 1),
+                            np.stack([f[:, 2], c, b], 1), np.stack([a, b, c], 1)])
+    return v, f.astype(np.uint32)
+
+
+def perlin3(points, seed):
+    """Perlin's improved gradient noise (SIGGRAPH 2002) at (N, 3) points."""
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(256)
+    perm = np.concatenate([perm, perm])
+    grads = np.array([[1, 1, 0], [-1, 1, 0], [1, -1, 0], [-1, -1, 0], [1, 0, 1], [-1, 0, 1],
+                      [1, 0, -1], [-1, 0, -1], [0, 1, 1], [0, -1, 1], [0, 1, -1], [0, -1, -1]],
+                     dtype=np.float64)
+    p = np.asarray(points, dtype=np.float64)
+    cell = np.floor(p).astype(np.int64)
+    frac = p - cell
+    cell &= 255
+    fade = frac * frac * frac * (frac * (frac * 6 - 15) + 10)
+    result = np.zeros(p.shape[0])
+    for corner in range(8):
+        o = np.array([(corner >> 0) & 1, (corner >> 1) & 1, (corner >> 2) & 1])
+        c = (cell + o) & 255
+        h = perm[perm[perm[c[:, 0]] + c[:, 1]] + c[:, 2]] % 12
+        d = frac - o
+        dotp = np.sum(grads[h] * d, axis=1)
+        w = np.prod(np.where(o == 1, fade, 1 - fade), axis=1)
+        result += w * dotp
+    return result
+
+
+def corner_normals(positions, triangles):
+    """Smooth (area-weighted) vertex normals, one per triangle corner."""
+    p = positions.astype(np.float64)
+    t = triangles.astype(np.int64)
+    face = np.cross(p[t[:, 1]] - p[t[:, 0]], p[t[:, 2]] - p[t[:, 0]])
+    vn = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(vn, t[:, k], face)
+    vn /= np.maximum(np.linalg.norm(vn, axis=1, keepdims=True), 1e-30)
+    return vn[t].astype(F32)
+
+
+# ---------------------------------------------------------------------------
+# Workloads
+
+CORNELL_WHITE = (0.73, 0.73, 0.73)
+CORNELL_RED = (0.63, 0.065, 0.05)
+CORNELL_GREEN = (0.14, 0.45, 0.091)
+
+
+def cornell_camera():
+    """The bootstrap camera of SetCornellBox (reference.cpp:222-237)."""
+    focal, near, far = F32(2.41421356), F32(1.0), F32(10.0)
+    view = identity()
+    view[14] = -3.0
+    projection = np.array([focal, 0, 0, 0, 0, focal, 0, 0,
+                           0, 0, (far + near) / (near - far), -1,
+                           0, 0, F32(2.0) * far * near / (near - far), 0], dtype=F32)
+    return multiply(projection, view)
+
+
+def cornell_reference(red_scale=1.0, size=128):
+    """The reference's Cornell box fixture (reference.cpp:221-279): coated
+    diffuse walls (ior 1.5, roughness 0.5), a GGX metal block, a coated
+    white block and an emitter under the ceiling; black environment.
+    ``red_scale`` scales the red wall's albedo (SetCornellRedWall, the
+    comparison's negative control)."""
+    s = Scene("cornell-reference")
+    white = s.add_material(preview_material(CORNELL_WHITE))
+    red = s.add_material(preview_material(tuple(F32(c * red_scale) for c in CORNELL_RED)))
+    green = s.add_material(preview_material(CORNELL_GREEN))
+    for corners, mat in [
+        ([[-1, -1, 1], [1, -1, 1], [1, -1, -1], [-1, -1, -1]], white),   # floor
+        ([[-1, 1, 1], [-1, 1, -1], [1, 1, -1], [1, 1, 1]], white),       # ceiling
+        ([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1]], white),   # back
+        ([[-1, -1, 1], [-1, -1, -1], [-1, 1, -1], [-1, 1, 1]], red),     # left
+        ([[1, -1, -1], [1, -1, 1], [1, 1, 1], [1, 1, -1]], green),       # right
+    ]:
+        s.add_instance(s.add_geometry(*quad(corners)), mat)
+    light = s.add_material(preview_material((0.0, 0.0, 0.0), emission=(15.0, 13.0, 10.0)))
+    s.add_instance(s.add_geometry(*quad([[-0.35, 0.98, 0.35], [-0.35, 0.98, -0.35],
+                                         [0.35, 0.98, -0.35], [0.35, 0.98, 0.35]])), light)
+    metal = s.add_material(preview_material((0.95, 0.85, 0.6), roughness=0.35, metallic=1.0))
+    cube = s.add_geometry(*unit_cube())
+    s.add_instance(cube, metal, block((0.6, 1.2, 0.6), 17.0, (-0.35, -0.399, -0.3)))
+    cube2 = s.add_geometry(*unit_cube())
+    s.add_instance(cube2, white, block((0.6, 0.6, 0.6), -18.0, (0.38, -0.699, 0.3)))
+    s.world_to_clip = cornell_camera()
+    s.width = s.height = size
+    return s
+
+
+def box_room(seed=0, size=256):
+    """The seeded box room: 10 wall triangles (floor, ceiling, back, left,
+    right; open front), two boxes of 12 triangles with a y-rotation in
+    [0, pi) and sides in [0.2, 0.6], resting on the floor, and a 2-triangle
+    ceiling light of radiance (17, 12, 4): 36 triangles. Lambert walls and
+    boxes (ior 1: uncoated) with albedo in [0.1, 0.8] per channel; the
+    Cornell camera."""
+    rng = np.random.default_rng(seed)
+    s = Scene(f"box-room-{seed}")
+
+    def lambert():
+        return s.add_material(preview_material(tuple(rng.uniform(0.1, 0.8, 3)), ior=1.0))
+
+    for corners in ([[-1, -1, 1], [1, -1, 1], [1, -1, -1], [-1, -1, -1]],
+                    [[-1, 1, 1], [-1, 1, -1], [1, 1, -1], [1, 1, 1]],
+                    [[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1]],
+                    [[-1, -1, 1], [-1, -1, -1], [-1, 1, -1], [-1, 1, 1]],
+                    [[1, -1, -1], [1, -1, 1], [1, 1, 1], [1, 1, -1]]):
+        s.add_instance(s.add_geometry(*quad(corners)), lambert())
+    light = s.add_material(preview_material((0.0, 0.0, 0.0), ior=1.0,
+                                            emission=(17.0, 12.0, 4.0)))
+    s.add_instance(s.add_geometry(*quad([[-0.35, 0.98, 0.35], [-0.35, 0.98, -0.35],
+                                         [0.35, 0.98, -0.35], [0.35, 0.98, 0.35]])), light)
+    cube = s.add_geometry(*unit_cube())
+    for k in range(2):
+        size_xyz = rng.uniform(0.2, 0.6, 3)
+        angle = rng.uniform(0.0, math.pi)
+        cx = (-0.4 if k == 0 else 0.4) + rng.uniform(-0.15, 0.15)
+        cz = rng.uniform(-0.5, 0.3)
+        centre = (cx, -1.0 + size_xyz[1] / 2 + 1e-3, cz)
+        s.add_instance(cube, lambert(), block(size_xyz, math.degrees(angle), centre))
+    s.world_to_clip = cornell_camera()
+    s.width = s.height = size
+    return s
+
+
+def procedural_sky(width=2048, height=1024, seed=0, sun_elevation=0.6, sun_azimuth=0.8):
+    """A lat-long sky: a log-normal field over a vertical gradient, plus one
+    sun lobe. Rows run from +Y (top) to -Y, as the environment lookup
+    expects."""
+    rng = np.random.default_rng(seed)
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    theta = np.pi * v[:, None]
+    phi = np.pi * (1.0 - 2.0 * u[None, :])
+    d = np.stack([np.sin(theta) * np.sin(phi), np.cos(theta) * np.ones_like(phi),
+                  np.sin(theta) * np.cos(phi)], axis=-1)
+    coarse = rng.normal(0.0, 1.0, (16, 32))
+    yi = np.clip((v * 16).astype(int), 0, 15)
+    xi = np.clip((u * 32).astype(int), 0, 31)
+    field = np.exp(0.35 * coarse[yi][:, xi])
+    up = np.clip(d[..., 1], 0.0, 1.0)
+    base = np.where(d[..., 1] >= 0.0, 0.6 + 0.8 * up, 0.15)
+    sky = np.stack([0.55 * base, 0.7 * base, 1.0 * base], -1) * field[..., None]
+    sun = np.array([math.cos(sun_elevation) * math.sin(sun_azimuth), math.sin(sun_elevation),
+                    math.cos(sun_elevation) * math.cos(sun_azimuth)])
+    cosine = np.clip(d @ sun, -1.0, 1.0)
+    lobe = 4000.0 * np.exp((cosine - 1.0) * 4000.0)
+    sky += np.stack([lobe, 0.9 * lobe, 0.75 * lobe], -1)
+    texels = np.ones((height, width, 4), dtype=F32)
+    texels[..., :3] = sky.astype(F32)
+    return texels
+
+
+def sphere_field(seed=0, width=1920, height=1080, prototypes=320, grid=100,
+                 spacing=2.0, spheres=4096, emitters=64, sky_size=(2048, 1024)):
+    """4096 instanced, Perlin-displaced icospheres (subdivision 3 or 4 by
+    seed; ``prototypes`` unique meshes, about 1M unique triangles) with radii
+    log-uniform in [0.05, 2] on a ``grid`` x ``grid`` ground; equal thirds
+    Lambert, GGX conductor (roughness in [0.02, 0.8]) and smooth dielectric
+    (ior 1.5); 64 emissive triangles with log-normal radiance (sigma 1); an
+    importance-sampled procedural sky."""
+    rng = np.random.default_rng(seed)
+    s = Scene(f"sphere-field-{seed}")
+    protos = []
+    for k in range(prototypes):
+        sub = 3 if rng.random() < 0.5 else 4
+        v, f = icosphere(sub)
+        freq = rng.uniform(1.5, 3.0)
+        offset = rng.uniform(-100, 100, 3)
+        r = 1.0 + 0.25 * perlin3(v * freq + offset, seed * 7919 + k)
+        p = (v * r[:, None]).astype(F32)
+        protos.append(s.add_geometry(p, f, corner_normals(p, f)))
+    half = grid * spacing / 2.0
+    ground = s.add_material(preview_material((0.45, 0.45, 0.42), roughness=0.8, ior=1.0))
+    s.add_instance(s.add_geometry(*quad([[-half, 0, half], [half, 0, half],
+                                         [half, 0, -half], [-half, 0, -half]])), ground)
+    cells = rng.choice(grid * grid, spheres, replace=False)
+    kinds = rng.permutation(np.arange(spheres) % 3)
+    for n, cell in enumerate(cells):
+        i, j = divmod(int(cell), grid)
+        radius = math.exp(rng.uniform(math.log(0.05), math.log(2.0)))
+        x = (i - (grid - 1) / 2.0) * spacing
+        z = (j - (grid - 1) / 2.0) * spacing
+        kind = kinds[n]
+        if kind == 0:
+            mat = preview_material(tuple(rng.uniform(0.1, 0.8, 3)), roughness=0.6, ior=1.0)
+        elif kind == 1:
+            mat = preview_material(tuple(rng.uniform(0.5, 1.0, 3)),
+                                   roughness=rng.uniform(0.02, 0.8), metallic=1.0)
+        else:
+            mat = preview_material((1.0, 1.0, 1.0), roughness=0.0, ior=1.5, transmission=1.0)
+        m = s.add_material(mat)
+        lin = rotation_y(rng.uniform(0, 2 * math.pi)) * radius
+        s.add_instance(protos[int(rng.integers(prototypes))], m,
+                       affine(lin, (x, radius * 0.9, z)))
+    tri = s.add_geometry(np.array([[-0.5, 0, -0.2887], [0.5, 0, -0.2887], [0, 0, 0.5774]],
+                                  dtype=F32), np.array([[0, 1, 2]], dtype=np.uint32))
+    for k in range(emitters):
+        radiance = math.exp(rng.normal(0.0, 1.0)) * 20.0
+        tint = rng.uniform(0.6, 1.0, 3)
+        mat = s.add_material(preview_material((0.0, 0.0, 0.0), ior=1.0,
+                                              emission=tuple(radiance * tint)))
+        lin = rotation_xyz(rng.uniform(-0.5, 0.5) + math.pi, rng.uniform(0, 2 * math.pi),
+                           rng.uniform(-0.5, 0.5)) * rng.uniform(2.0, 5.0)
+        pos = (rng.uniform(-half * 0.6, half * 0.6), rng.uniform(6.0, 14.0),
+               rng.uniform(-half * 0.6, half * 0.6))
+        s.add_instance(tri, mat, affine(lin, pos))
+    s.set_environment(procedural_sky(sky_size[0], sky_size[1], seed))
+    eye = (48.0, 22.0, 48.0)
+    view = look_at(eye, (0.0, 0.0, 0.0))
+    s.world_to_clip = multiply(perspective(50.0, width / height, 0.1, 1000.0), view)
+    s.width, s.height = width, height
+    return s

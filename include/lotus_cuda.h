@@ -1,0 +1,249 @@
+/* SPDX-License-Identifier: Apache-2.0
+ *
+ * lotus_cuda.h: the C ABI of the B200 (sm_100a) integrator backend.
+ *
+ * This is the drop-in boundary that stands in for the reference's
+ * Vulkan backend (`lotus-render-vulkan`). A host that drives
+ * `Lotus::OffscreenRenderer` (include/lotus/vulkan_backend.hpp:753-842 in the
+ * reference) maps its calls onto these entry points one for one:
+ *
+ *   CreateOffscreenRenderer  (vulkan_backend.hpp:879-883)  -> lotus_cuda_create
+ *   UpdateScene(SceneUpdate) (vulkan_backend.hpp:816-817)  -> lotus_cuda_update_scene
+ *   RenderScene(...)         (vulkan_backend.hpp:789-791)  -> lotus_cuda_render
+ *   RayQueryCapability()     (vulkan_backend.hpp:767)      -> lotus_cuda_capability
+ *   ~OffscreenRenderer       (vulkan_backend.hpp:757)      -> lotus_cuda_destroy
+ *
+ * Conventions (the reference's, vulkan_backend.hpp:744-759, 812-815):
+ *   - Every call returns LOTUS_PASS, LOTUS_FAIL or LOTUS_SKIP (the reference's
+ *     FrameStatus) and never throws across the boundary. A detail string
+ *     says why on Fail/Skip.
+ *   - Invalid settings Fail without poisoning the renderer. A failed device
+ *     operation poisons it: later calls Fail until it is destroyed.
+ *   - Calls are synchronous, one frame in flight, one CUDA stream per
+ *     renderer; a handle is not thread-safe.
+ *   - The renderer owns all device memory. Input arrays are host memory,
+ *     read during the call only.
+ *   - Structs are plain data; matrices are column-major 4x4 floats
+ *     (Lotus::Matrix4, include/lotus/render_world.hpp:16-18).
+ */
+#ifndef LOTUS_CUDA_H
+#define LOTUS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LOTUS_CUDA_ABI_VERSION 1u
+
+/* FrameStatus (vulkan_backend.hpp:23-27). */
+#define LOTUS_PASS 0
+#define LOTUS_FAIL 1
+#define LOTUS_SKIP 77
+
+/* Integrator (vulkan_backend.hpp:639-648). */
+#define LOTUS_INTEGRATOR_REFERENCE 0u
+#define LOTUS_INTEGRATOR_WAVEFRONT 1u
+
+/* LightSampling (vulkan_backend.hpp:650-670). */
+#define LOTUS_LIGHT_SAMPLING_BSDF 0u
+#define LOTUS_LIGHT_SAMPLING_MIS 1u
+#define LOTUS_LIGHT_SAMPLING_RESTIR_INITIAL 2u
+
+/* kMaxWavefrontBounces (vulkan_backend.hpp:694): a larger max_bounces Fails. */
+#define LOTUS_MAX_BOUNCES 1024u
+/* How many per-bounce queue counts a frame result reports. */
+#define LOTUS_MAX_REPORTED_BOUNCES 64u
+
+/* UsdPreviewSurface flags (gpu_scene.hpp:82-87). */
+#define LOTUS_MATERIAL_SPECULAR_WORKFLOW 1u
+#define LOTUS_MATERIAL_THIN_WALLED 2u
+
+/* One mesh: Lotus::MeshGeometry (render_world.hpp:39-58), object space. */
+typedef struct lotus_geometry {
+  const float* positions;     /* 3 floats per vertex */
+  const uint32_t* triangles;  /* 3 vertex indices per triangle */
+  const float* normals;       /* NULL, or 9 floats per triangle: corner normals */
+  uint32_t vertex_count;
+  uint32_t triangle_count;
+} lotus_geometry;
+
+/* One placed mesh: SceneUpdate's instance (extraction.hpp:313-354). */
+typedef struct lotus_instance {
+  float world_from_object[16]; /* column-major; the last row must be 0 0 0 1 */
+  uint32_t geometry;           /* index into lotus_scene_desc::geometries */
+  uint32_t material;           /* index into lotus_scene_desc::materials */
+} lotus_instance;
+
+/* UsdPreviewSurface's constants (material.hpp:137-173) plus the material's
+ * coverage (material.hpp:103-116). */
+typedef struct lotus_material {
+  float base_color[3];
+  float roughness;
+  float emission[3];
+  float metallic;
+  float specular_color[3];
+  float ior;
+  float transmission_color[3];
+  float transmission;
+  float opacity;            /* surface coverage in [0, 1] */
+  float opacity_threshold;  /* > 0: binary coverage */
+  uint32_t flags;           /* LOTUS_MATERIAL_* */
+  uint32_t reserved;
+} lotus_material;
+
+/* A latitude-longitude environment image (render_world.hpp:122-133): RGBA
+ * float texels, rows from the top. The renderer builds its sampling
+ * distribution (gpu_scene.cpp:620-711). */
+typedef struct lotus_environment {
+  const float* texels;              /* 4 floats per texel, width*height texels */
+  uint32_t width;
+  uint32_t height;
+  float scale[3];                   /* multiplies the texels' RGB */
+  float environment_from_world[9];  /* rows: the image frame's unit axes in world space */
+} lotus_environment;
+
+/* The whole scene. Slot 0 of materials is the default material. */
+typedef struct lotus_scene_desc {
+  const lotus_geometry* geometries;
+  const lotus_instance* instances;
+  const lotus_material* materials;
+  const lotus_environment* environment; /* NULL: no environment image */
+  uint32_t geometry_count;
+  uint32_t instance_count;
+  uint32_t material_count;
+  float environment_constant[3];  /* the constant environment radiance */
+} lotus_scene_desc;
+
+/* GpuSceneEvidence, in part. */
+typedef struct lotus_scene_result {
+  int32_t status;
+  uint32_t triangle_count;      /* unique triangles over all geometries */
+  uint32_t instance_count;
+  uint32_t light_count;         /* light table entries */
+  uint32_t bvh_node_count;      /* BLAS nodes over all geometries */
+  uint32_t tlas_node_count;
+  double build_gpu_ms;          /* device LBVH builds and table uploads */
+  uint64_t device_bytes;        /* scene bytes resident on the device */
+  char detail[256];
+} lotus_scene_result;
+
+/* OffscreenTarget (vulkan_backend.hpp:253-282). */
+typedef struct lotus_target {
+  uint32_t width;
+  uint32_t height;
+  float display_window[4];   /* {x, y, w, h}; w or h <= 0 means the whole image */
+  int32_t data_window[4];    /* {x, y, w, h}; w or h <= 0 means the whole image */
+  float clear_color[4];
+  uint32_t read_back;        /* 0 keeps the frame on the device */
+  uint32_t reserved;
+} lotus_target;
+
+/* PathTracingSettings (vulkan_backend.hpp:697-738). */
+typedef struct lotus_settings {
+  uint32_t integrator;        /* LOTUS_INTEGRATOR_* */
+  uint32_t light_sampling;    /* LOTUS_LIGHT_SAMPLING_* */
+  uint32_t sample_index;
+  uint32_t max_bounces;
+  uint32_t max_samples;       /* 0: no limit */
+  uint32_t restir_candidates;
+  uint32_t restir_temporal;
+  uint32_t restir_max_history_candidates;
+  uint32_t restir_spatial;
+  uint32_t restir_spatial_radius;
+  uint32_t restir_proposal;
+  uint32_t environment_background;
+} lotus_settings;
+
+/* One RenderScene call: DrawSummary::world_to_clip in the OpenGL clip
+ * convention (extraction.hpp:23), the target and the settings. */
+typedef struct lotus_frame_desc {
+  float world_to_clip[16];
+  lotus_target target;
+  lotus_settings settings;
+  uint32_t frame_count;
+  uint32_t reserved;
+} lotus_frame_desc;
+
+/* GpuFrameEvidence (vulkan_backend.hpp:202-249), in part. */
+typedef struct lotus_frame_result {
+  int32_t status;
+  uint32_t frames_rendered;
+  uint32_t samples_per_pixel;
+  uint32_t wavefront_rounds;
+  uint64_t completion;
+  /* Rays traced by this call, over all its samples. */
+  uint64_t camera_rays;
+  uint64_t extension_rays;
+  uint64_t shadow_rays;
+  /* Device time of the call's samples (CUDA events), readback excluded. */
+  double gpu_ms;
+  /* Queue occupancy of the last sample: per bounce, paths that entered the
+   * ray queue; element 0 is the camera rays. */
+  uint32_t wavefront_path_counts[LOTUS_MAX_REPORTED_BOUNCES];
+  uint32_t wavefront_path_count_size;
+  uint32_t reserved;
+  char detail[256];
+} lotus_frame_result;
+
+typedef struct lotus_cuda_options {
+  int32_t device;     /* CUDA device ordinal */
+  uint32_t flags;     /* reserved, 0 */
+} lotus_cuda_options;
+
+typedef struct lotus_cuda_renderer lotus_cuda_renderer;
+
+/* The library's ABI version (LOTUS_CUDA_ABI_VERSION). Needs no GPU. */
+uint32_t lotus_cuda_abi_version(void);
+
+/* sizeof of each struct above, in declaration order, so a binding can check
+ * its mirrors. Writes at most `capacity` sizes; returns how many there are.
+ * Needs no GPU. */
+uint32_t lotus_cuda_struct_sizes(uint64_t* sizes, uint32_t capacity);
+
+/* RayQueryCapability (vulkan_backend.hpp:767): LOTUS_PASS when an sm_100
+ * device is present, LOTUS_SKIP with the reason otherwise. */
+int32_t lotus_cuda_capability(int32_t device, char* detail, size_t detail_size);
+
+/* CreateOffscreenRenderer (vulkan_backend.hpp:879-883). */
+int32_t lotus_cuda_create(const lotus_cuda_options* options,
+    lotus_cuda_renderer** renderer, char* error, size_t error_size);
+
+void lotus_cuda_destroy(lotus_cuda_renderer* renderer);
+
+/* UpdateScene (vulkan_backend.hpp:816-817): replaces the resident scene.
+ * Builds one LBVH per geometry and one over the instances on the device,
+ * the light table and the environment distribution. Restarts the
+ * accumulation. */
+int32_t lotus_cuda_update_scene(lotus_cuda_renderer* renderer,
+    const lotus_scene_desc* scene, lotus_scene_result* result);
+
+/* RenderScene (vulkan_backend.hpp:789-791), Radiance output: adds
+ * frame_count samples per pixel (up to max_samples) to the accumulation and
+ * writes its mean. With target.read_back and a non-NULL `color`, copies the
+ * RGBA32F colour (width*height*4 floats, top-left rows) into `color`. */
+int32_t lotus_cuda_render(lotus_cuda_renderer* renderer,
+    const lotus_frame_desc* frame, lotus_frame_result* result, float* color);
+
+/* The colour of the latest frame into host memory (width*height*4 floats). */
+int32_t lotus_cuda_read_color(lotus_cuda_renderer* renderer, float* color,
+    uint64_t capacity_floats);
+
+/* The renderer's CUDA stream (a cudaStream_t), for callers that time its
+ * work with their own events. */
+void* lotus_cuda_stream(lotus_cuda_renderer* renderer);
+
+/* The light table as the device holds it (GpuLightRecord, gpu_scene.hpp:
+ * 120-126): 4 words per entry {pdf, threshold, alias, instance}, then the
+ * per-instance first entries. Returns the entry count, or -1. */
+int64_t lotus_cuda_read_light_table(lotus_cuda_renderer* renderer,
+    uint32_t* records, uint64_t record_capacity, uint32_t* offsets,
+    uint64_t offset_capacity);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LOTUS_CUDA_H */

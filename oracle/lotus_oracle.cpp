@@ -1,0 +1,1833 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// TEST INFRASTRUCTURE ONLY: the oracle. A scalar, FP32 CPU restatement of the
+// reference's integrator (hydra-lotus v0.9.0), written from its Slang shaders
+// and host-side table builders, expression by expression, so that the same
+// (pixel, sample index) gives the same path. Each function names the reference
+// function it restates. Only tests, the smoke check and the benchmark's CPU
+// baseline leg load it, as the checker.
+//
+// What differs from the reference, and why:
+// - Traversal. The reference asks RT hardware for the closest accepted hit
+//   (backend/vulkan/shaders/common/scene.slang:424-439). The oracle traverses
+//   its own binned-SAH BVH and intersects triangles with the watertight test
+//   of Woop, Benthin and Wald (JCGT 2013) in each instance's object space,
+//   which is what the CUDA kernels do too. Equal distances resolve to the
+//   smaller (instance, primitive), so the closest hit does not depend on the
+//   traversal order.
+// - Textures. Only the environment image is a texture here; it is filtered
+//   bilinearly in FP32 (repeat across longitude, clamp at the poles, as the
+//   reference's sampler, gpu_scene.cpp:2212-2214), where the reference's
+//   sampler hardware uses fixed-point weights.
+// - Accumulation. Samples are summed in FP64 (the precision policy), where
+//   the reference's image is RGBA32F.
+// Analytic lights, textured inputs and the glTF closure are not in the
+// restated path (no workload uses them).
+
+#include "lotus_oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kFloatMax = 3.402823466e+38f;
+constexpr uint32_t kNoLights = 0xFFFFFFFFu;
+constexpr uint32_t kEnvironmentLight = 0xFFFFFFFFu;
+constexpr uint32_t kRouletteBounces = 3;  // transport.slang:21
+constexpr float kMaxSurvival = 0.95f;     // transport.slang:22
+constexpr float kMinAlpha = 1.0e-3f;      // preview.slang:17
+
+// ---------------------------------------------------------------------------
+// Vectors, with the evaluation order written out.
+
+struct F3 {
+  float x, y, z;
+};
+inline F3 V(float x, float y, float z) { return F3{x, y, z}; }
+inline F3 V(float s) { return F3{s, s, s}; }
+inline F3 operator+(F3 a, F3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline F3 operator-(F3 a, F3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline F3 operator-(F3 a) { return V(-a.x, -a.y, -a.z); }
+inline F3 operator*(F3 a, F3 b) { return V(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline F3 operator*(F3 a, float s) { return V(a.x * s, a.y * s, a.z * s); }
+inline F3 operator*(float s, F3 a) { return V(s * a.x, s * a.y, s * a.z); }
+inline F3 operator/(F3 a, float s) { return V(a.x / s, a.y / s, a.z / s); }
+inline float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline F3 cross(F3 a, F3 b) {
+  return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+inline float rsqrt(float x) { return 1.0f / std::sqrt(x); }
+inline F3 normalize(F3 a) { return a * rsqrt(dot(a, a)); }
+inline float length(F3 a) { return std::sqrt(dot(a, a)); }
+inline float saturate(float x) { return std::fmin(std::fmax(x, 0.0f), 1.0f); }
+inline float MaxComponent(F3 a) { return std::fmax(a.x, std::fmax(a.y, a.z)); }
+inline bool IsFinite(F3 a) {
+  return std::isfinite(a.x) && std::isfinite(a.y) && std::isfinite(a.z);
+}
+inline float Component(F3 a, int axis) { return axis == 0 ? a.x : axis == 1 ? a.y : a.z; }
+inline uint32_t AsUint(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+inline float AsFloat(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+
+// ---------------------------------------------------------------------------
+// sampling.slang
+
+// PcgHash (sampling.slang:9-13).
+inline uint32_t PcgHash(uint32_t value) {
+  const uint32_t state = value * 747796405u + 2891336453u;
+  const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+  return (word >> 22u) ^ word;
+}
+
+// SeedRandom (sampling.slang:16-18).
+inline uint32_t SeedRandom(uint32_t pixel_index, uint32_t sample_index) {
+  return PcgHash(pixel_index ^ PcgHash(sample_index));
+}
+
+// NextRandom (sampling.slang:21-25).
+inline float NextRandom(uint32_t& state) {
+  state = state * 747796405u + 2891336453u;
+  const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+  return float(((word >> 22u) ^ word) >> 8u) * (1.0f / 16777216.0f);
+}
+
+struct ShadingFrame {
+  F3 tangent, bitangent, normal;
+  F3 ToLocal(F3 d) const { return V(dot(d, tangent), dot(d, bitangent), dot(d, normal)); }
+  F3 ToWorld(F3 d) const { return d.x * tangent + d.y * bitangent + d.z * normal; }
+};
+
+// MakeShadingFrame (sampling.slang:45-55).
+inline ShadingFrame MakeShadingFrame(F3 n) {
+  const float sign = n.z >= 0.0f ? 1.0f : -1.0f;
+  const float a = -1.0f / (sign + n.z);
+  const float b = n.x * n.y * a;
+  ShadingFrame f;
+  f.tangent = V(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x);
+  f.bitangent = V(b, sign + n.y * n.y * a, -n.y);
+  f.normal = n;
+  return f;
+}
+
+// PowerHeuristic (sampling.slang:67-76).
+inline float PowerHeuristic(float chosen, float other) {
+  if (!(chosen > 0.0f)) return 0.0f;
+  if (std::isinf(chosen)) return std::isinf(other) ? 0.5f : 1.0f;
+  const float ratio = other / chosen;
+  return 1.0f / (1.0f + ratio * ratio);
+}
+
+// SampleCosineHemisphere (sampling.slang:79-84).
+inline F3 SampleCosineHemisphere(float ux, float uy) {
+  const float radius = std::sqrt(ux);
+  const float phi = 2.0f * kPi * uy;
+  return V(radius * std::cos(phi), radius * std::sin(phi),
+      std::sqrt(std::fmax(0.0f, 1.0f - ux)));
+}
+
+// ---------------------------------------------------------------------------
+// bsdf/preview.slang
+
+struct PreviewClosure {
+  F3 base_color;
+  float alpha;
+  float metallic;
+  F3 dielectric_f0;
+  float dielectric_f90;
+  F3 f0;
+  float f90;
+  float transmission;
+  F3 transmission_color;
+  float eta;
+  bool thin_walled;
+  bool smooth;
+};
+
+// MakePreviewClosure (preview.slang:60-89).
+PreviewClosure MakePreviewClosure(F3 base_color, float roughness, float metallic,
+    float ior, bool specular_workflow, F3 specular, float transmission,
+    F3 transmission_color, bool thin_walled, bool entering) {
+  PreviewClosure b;
+  b.base_color = base_color;
+  b.alpha = std::fmax(roughness * roughness, kMinAlpha);
+  b.metallic = specular_workflow ? 0.0f : metallic;
+  b.transmission = (1.0f - b.metallic) * transmission;
+  b.transmission_color = transmission_color;
+  b.eta = thin_walled || entering ? ior : 1.0f / ior;
+  b.thin_walled = thin_walled;
+  b.smooth = roughness * roughness < kMinAlpha || ior == 1.0f;
+  if (b.transmission > 0.0f) {
+    b.metallic = b.transmission < 1.0f
+        ? std::fmin(b.metallic / (1.0f - b.transmission), 1.0f)
+        : 0.0f;
+  }
+  const float ratio = 1.0f - 2.0f / (ior + 1.0f);
+  b.dielectric_f0 = specular_workflow ? specular : V(ratio * ratio);
+  b.dielectric_f90 = specular_workflow || ior > 1.0f ? 1.0f : 0.0f;
+  b.f0 = b.base_color * b.metallic + b.dielectric_f0 * (1.0f - b.metallic);
+  b.f90 = b.metallic + (1.0f - b.metallic) * b.dielectric_f90;
+  return b;
+}
+
+// FresnelSchlick (preview.slang:92-95).
+inline F3 FresnelSchlick(F3 f0, float f90, float cos_theta) {
+  const float weight = std::pow(saturate(1.0f - cos_theta), 5.0f);
+  return f0 * (1.0f - weight) + V(f90 * weight);
+}
+
+// DielectricTransmission (preview.slang:100-104).
+inline F3 DielectricTransmission(const PreviewClosure& b, float cos_theta) {
+  const F3 fresnel = FresnelSchlick(b.dielectric_f0, b.dielectric_f90, cos_theta);
+  return V(1.0f) + fresnel * -1.0f;
+}
+
+// SpecularProbability (preview.slang:106-112).
+inline float SpecularProbability(const PreviewClosure& b, F3 wo) {
+  if (b.metallic == 1.0f) return 1.0f;
+  if (b.dielectric_f90 == 0.0f) return b.metallic;
+  const float dielectric = std::fmin(std::fmax(MaxComponent(FresnelSchlick(
+      b.dielectric_f0, b.dielectric_f90, wo.z)), 0.05f), 0.95f);
+  return b.metallic + (1.0f - b.metallic) * dielectric;
+}
+
+// FresnelDielectric (preview.slang:118-127).
+inline float FresnelDielectric(float cos_theta, float eta) {
+  cos_theta = saturate(cos_theta);
+  const float sin2_t = (1.0f - cos_theta * cos_theta) / (eta * eta);
+  if (sin2_t >= 1.0f) return 1.0f;
+  const float cos_t = std::sqrt(1.0f - sin2_t);
+  const float parallel = (eta * cos_theta - cos_t) / (eta * cos_theta + cos_t);
+  const float perpendicular = (cos_theta - eta * cos_t) / (cos_theta + eta * cos_t);
+  return 0.5f * (parallel * parallel + perpendicular * perpendicular);
+}
+
+// InterfaceReflectance (preview.slang:132-135).
+inline float InterfaceReflectance(const PreviewClosure& b, float cos_theta) {
+  const float r = FresnelDielectric(cos_theta, b.eta);
+  return b.thin_walled ? 2.0f * r / (1.0f + r) : r;
+}
+
+// GgxD (preview.slang:138-142).
+inline float GgxD(F3 h, float alpha) {
+  const float alpha2 = alpha * alpha;
+  const float denominator = h.z * h.z * (alpha2 - 1.0f) + 1.0f;
+  return alpha2 / (kPi * denominator * denominator);
+}
+
+// GgxLambda (preview.slang:145-148).
+inline float GgxLambda(F3 w, float alpha) {
+  const float tan2 = std::fmax(0.0f, 1.0f - w.z * w.z) / (w.z * w.z);
+  return 0.5f * (std::sqrt(1.0f + alpha * alpha * tan2) - 1.0f);
+}
+
+// SampleGgxVisibleNormal (preview.slang:152-160).
+inline F3 SampleGgxVisibleNormal(F3 wo, float alpha, float ux, float uy) {
+  const F3 wo_std = normalize(V(wo.x * alpha, wo.y * alpha, wo.z));
+  const float phi = 2.0f * kPi * ux;
+  const float z = (1.0f - uy) * (1.0f + wo_std.z) - wo_std.z;
+  const float sin_theta = std::sqrt(saturate(1.0f - z * z));
+  const F3 h_std = V(sin_theta * std::cos(phi), sin_theta * std::sin(phi), z) + wo_std;
+  return normalize(V(h_std.x * alpha, h_std.y * alpha, h_std.z));
+}
+
+// GgxEvalCos (preview.slang:164-170).
+inline F3 GgxEvalCos(const PreviewClosure& b, F3 wo, F3 wi) {
+  const F3 h = normalize(wo + wi);
+  const float g2 = 1.0f / (1.0f + GgxLambda(wo, b.alpha) + GgxLambda(wi, b.alpha));
+  return FresnelSchlick(b.f0, b.f90, dot(wo, h)) *
+         (GgxD(h, b.alpha) * g2 / (4.0f * wo.z));
+}
+
+// GgxPdf (preview.slang:173-177).
+inline float GgxPdf(const PreviewClosure& b, F3 wo, F3 wi) {
+  const F3 h = normalize(wo + wi);
+  const float g1 = 1.0f / (1.0f + GgxLambda(wo, b.alpha));
+  return GgxD(h, b.alpha) * g1 / (4.0f * wo.z);
+}
+
+// SmithRatio (preview.slang:180-183).
+inline float SmithRatio(const PreviewClosure& b, F3 wo, F3 wi) {
+  const float lambda_o = GgxLambda(wo, b.alpha);
+  return (1.0f + lambda_o) / (1.0f + lambda_o + GgxLambda(wi, b.alpha));
+}
+
+// LayeredEvalCos (preview.slang:187-198).
+F3 LayeredEvalCos(const PreviewClosure& b, F3 wo, F3 wi) {
+  if (wo.z <= 0.0f || wi.z <= 0.0f) return V(0.0f);
+  F3 value = b.base_color * ((1.0f - b.metallic) * wi.z / kPi);
+  value = value * DielectricTransmission(b, wo.z) * DielectricTransmission(b, wi.z);
+  if (b.f90 > 0.0f) value = value + GgxEvalCos(b, wo, wi);
+  return value;
+}
+
+// LayeredPdf (preview.slang:202-212).
+float LayeredPdf(const PreviewClosure& b, F3 wo, F3 wi) {
+  if (wo.z <= 0.0f || wi.z <= 0.0f) return 0.0f;
+  const float specular = SpecularProbability(b, wo);
+  float pdf = (1.0f - specular) * wi.z / kPi;
+  if (specular > 0.0f) pdf += specular * GgxPdf(b, wo, wi);
+  return pdf;
+}
+
+// InterfaceReflectionEvalCos (preview.slang:216-222).
+float InterfaceReflectionEvalCos(const PreviewClosure& b, F3 wo, F3 wi) {
+  const F3 h = normalize(wo + wi);
+  const float g2 = 1.0f / (1.0f + GgxLambda(wo, b.alpha) + GgxLambda(wi, b.alpha));
+  return InterfaceReflectance(b, dot(wo, h)) * GgxD(h, b.alpha) * g2 / (4.0f * wo.z);
+}
+
+// PreviewReflectionEvaluate (preview.slang:227-238).
+F3 PreviewReflectionEvaluate(const PreviewClosure& b, F3 wo, F3 wi) {
+  const F3 layered = LayeredEvalCos(b, wo, wi);
+  if (b.transmission == 0.0f) return layered;
+  F3 value = layered * (1.0f - b.transmission);
+  if (!b.smooth && wo.z > 0.0f && wi.z > 0.0f)
+    value = value + V(b.transmission * InterfaceReflectionEvalCos(b, wo, wi));
+  return value;
+}
+
+// PreviewReflectionPdf (preview.slang:240-252).
+float PreviewReflectionPdf(const PreviewClosure& b, F3 wo, F3 wi) {
+  const float layered = LayeredPdf(b, wo, wi);
+  if (b.transmission == 0.0f) return layered;
+  float pdf = (1.0f - b.transmission) * layered;
+  if (!b.smooth && wo.z > 0.0f && wi.z > 0.0f) {
+    const F3 h = normalize(wo + wi);
+    pdf += b.transmission * InterfaceReflectance(b, dot(wo, h)) * GgxPdf(b, wo, wi);
+  }
+  return pdf;
+}
+
+struct InterfaceTransmission {
+  float value;
+  float pdf;
+};
+
+// PreviewTransmission (preview.slang:267-310).
+InterfaceTransmission PreviewTransmission(const PreviewClosure& b, F3 wo, F3 wi) {
+  InterfaceTransmission r{0.0f, 0.0f};
+  if (b.transmission == 0.0f || b.smooth || !(wo.z > 0.0f) || !(wi.z < 0.0f)) return r;
+  if (b.thin_walled) {
+    const F3 reflected = V(wi.x, wi.y, -wi.z);
+    const F3 h = normalize(wo + reflected);
+    const float share = b.transmission * (1.0f - InterfaceReflectance(b, dot(wo, h)));
+    const float g2 = 1.0f / (1.0f + GgxLambda(wo, b.alpha) + GgxLambda(reflected, b.alpha));
+    r.value = share * GgxD(h, b.alpha) * g2 / (4.0f * wo.z);
+    r.pdf = share * GgxPdf(b, wo, reflected);
+    return r;
+  }
+  F3 h = normalize(wo + b.eta * wi);
+  if (h.z < 0.0f) h = -h;
+  const float cos_oh = dot(wo, h);
+  const float cos_ih = dot(wi, h);
+  if (!(cos_oh > 0.0f) || !(cos_ih < 0.0f)) return r;
+  const float denominator = cos_ih + cos_oh / b.eta;
+  const float jacobian = -cos_ih / (denominator * denominator);
+  const float share = b.transmission * (1.0f - InterfaceReflectance(b, cos_oh));
+  const float d = GgxD(h, b.alpha);
+  const float lambda_o = GgxLambda(wo, b.alpha);
+  const float g1 = 1.0f / (1.0f + lambda_o);
+  const float g2 = 1.0f / (1.0f + lambda_o + GgxLambda(wi, b.alpha));
+  r.pdf = share * (g1 * cos_oh * d / wo.z) * jacobian;
+  r.value = share * (g2 * cos_oh * d / wo.z) * jacobian / (b.eta * b.eta);
+  return r;
+}
+
+// PreviewEvaluate (preview.slang:314-319).
+F3 PreviewEvaluate(const PreviewClosure& b, F3 wo, F3 wi) {
+  if (wi.z < 0.0f) return b.transmission_color * PreviewTransmission(b, wo, wi).value;
+  return PreviewReflectionEvaluate(b, wo, wi);
+}
+
+// PreviewPdf (preview.slang:322-327).
+float PreviewPdf(const PreviewClosure& b, F3 wo, F3 wi) {
+  if (wi.z < 0.0f) return PreviewTransmission(b, wo, wi).pdf;
+  return PreviewReflectionPdf(b, wo, wi);
+}
+
+struct BsdfSampleResult {
+  F3 wi;
+  F3 weight;
+  float pdf;
+  bool delta;
+  bool transmitted;
+};
+
+// SampleInterface (preview.slang:348-405).
+bool SampleInterface(const PreviewClosure& b, F3 wo, F3 u, BsdfSampleResult& s) {
+  const F3 h = b.smooth ? V(0.0f, 0.0f, 1.0f) : SampleGgxVisibleNormal(wo, b.alpha, u.x, u.y);
+  const float cos_oh = dot(wo, h);
+  if (!(cos_oh > 0.0f)) return false;
+  const F3 reflected = 2.0f * cos_oh * h - wo;
+  s.delta = b.smooth;
+  if (u.z < InterfaceReflectance(b, cos_oh)) {
+    s.wi = reflected;
+    if (b.smooth) {
+      s.weight = V(1.0f);
+      return true;
+    }
+    if (reflected.z <= 0.0f) return false;
+    s.weight = V(SmithRatio(b, wo, reflected));
+    s.pdf = PreviewReflectionPdf(b, wo, reflected);
+    return s.pdf > 0.0f && IsFinite(s.weight);
+  }
+  s.transmitted = true;
+  if (b.thin_walled) {
+    if (!b.smooth && reflected.z <= 0.0f) return false;
+    s.wi = V(reflected.x, reflected.y, -reflected.z);
+    s.weight = b.transmission_color * (b.smooth ? 1.0f : SmithRatio(b, wo, reflected));
+    if (!b.smooth) s.pdf = PreviewTransmission(b, wo, s.wi).pdf;
+    return IsFinite(s.weight);
+  }
+  const float sin2_t = (1.0f - cos_oh * cos_oh) / (b.eta * b.eta);
+  if (sin2_t >= 1.0f) return false;
+  const float cos_t = std::sqrt(1.0f - sin2_t);
+  s.wi = -wo / b.eta + (cos_oh / b.eta - cos_t) * h;
+  if (s.wi.z >= 0.0f) return false;
+  s.weight = b.transmission_color *
+      ((b.smooth ? 1.0f : SmithRatio(b, wo, s.wi)) / (b.eta * b.eta));
+  if (!b.smooth) s.pdf = PreviewTransmission(b, wo, s.wi).pdf;
+  return IsFinite(s.weight);
+}
+
+// PreviewSample (preview.slang:411-454).
+bool PreviewSample(const PreviewClosure& b, F3 wo, F3 u, BsdfSampleResult& s) {
+  s.wi = V(0.0f);
+  s.weight = V(0.0f);
+  s.pdf = 0.0f;
+  s.delta = false;
+  s.transmitted = false;
+  if (wo.z <= 0.0f) return false;
+  if (b.transmission > 0.0f) {
+    if (u.z < b.transmission)
+      return SampleInterface(b, wo, V(u.x, u.y, u.z / b.transmission), s);
+    u.z = (u.z - b.transmission) / (1.0f - b.transmission);
+  }
+  if (u.z < SpecularProbability(b, wo)) {
+    const F3 h = SampleGgxVisibleNormal(wo, b.alpha, u.x, u.y);
+    s.wi = 2.0f * dot(wo, h) * h - wo;
+  } else {
+    s.wi = SampleCosineHemisphere(u.x, u.y);
+  }
+  const float layered_pdf = LayeredPdf(b, wo, s.wi);
+  if (!(layered_pdf > 0.0f)) return false;
+  s.pdf = b.transmission > 0.0f ? PreviewReflectionPdf(b, wo, s.wi) : layered_pdf;
+  s.weight = LayeredEvalCos(b, wo, s.wi) / layered_pdf;
+  if (b.metallic == 1.0f) {
+    const F3 h = normalize(wo + s.wi);
+    const float lambda_o = GgxLambda(wo, b.alpha);
+    s.weight = FresnelSchlick(b.f0, b.f90, dot(wo, h)) *
+        ((1.0f + lambda_o) / (1.0f + lambda_o + GgxLambda(s.wi, b.alpha)));
+  }
+  return IsFinite(s.weight);
+}
+
+// ---------------------------------------------------------------------------
+// Scene
+
+struct Box {
+  float lo[3] = {kFloatMax, kFloatMax, kFloatMax};
+  float hi[3] = {-kFloatMax, -kFloatMax, -kFloatMax};
+  void Grow(const float* p) {
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], p[a]);
+      hi[a] = std::max(hi[a], p[a]);
+    }
+  }
+  void Grow(const Box& b) {
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], b.lo[a]);
+      hi[a] = std::max(hi[a], b.hi[a]);
+    }
+  }
+  float Area() const {
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    if (!(dx >= 0.0f)) return 0.0f;
+    return 2.0f * (dx * dy + dy * dz + dz * dx);
+  }
+};
+
+// A binary BVH over boxes, built top-down with binned SAH. Leaves hold up
+// to four primitives from `order`.
+struct Bvh {
+  struct Node {
+    Box box;
+    uint32_t left = 0;   // interior: left child; right child is left + 1
+    uint32_t first = 0;  // leaf: first index into order
+    uint32_t count = 0;  // leaf: primitive count; 0 for an interior node
+  };
+  std::vector<Node> nodes;
+  std::vector<uint32_t> order;
+
+  void Build(const std::vector<Box>& boxes) {
+    const uint32_t n = static_cast<uint32_t>(boxes.size());
+    order.resize(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    nodes.clear();
+    nodes.reserve(n > 0 ? 2 * n : 1);
+    nodes.emplace_back();
+    if (n == 0) return;
+    std::vector<float> centroids(3 * size_t{n});
+    for (uint32_t i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a)
+        centroids[3 * i + a] = 0.5f * (boxes[i].lo[a] + boxes[i].hi[a]);
+    struct Task { uint32_t node, first, count; };
+    std::vector<Task> stack{{0, 0, n}};
+    while (!stack.empty()) {
+      const Task t = stack.back();
+      stack.pop_back();
+      Node& node = nodes[t.node];
+      Box bounds, cbounds;
+      for (uint32_t i = t.first; i < t.first + t.count; ++i) {
+        bounds.Grow(boxes[order[i]]);
+        cbounds.Grow(&centroids[3 * order[i]]);
+      }
+      node.box = bounds;
+      if (t.count <= 4) {
+        node.first = t.first;
+        node.count = t.count;
+        continue;
+      }
+      constexpr int kBins = 16;
+      float best_cost = std::numeric_limits<float>::infinity();
+      int best_axis = -1, best_split = 0;
+      for (int a = 0; a < 3; ++a) {
+        const float extent = cbounds.hi[a] - cbounds.lo[a];
+        if (!(extent > 0.0f)) continue;
+        Box bin_box[kBins];
+        uint32_t bin_count[kBins] = {};
+        for (uint32_t i = t.first; i < t.first + t.count; ++i) {
+          int b = static_cast<int>((centroids[3 * order[i] + a] - cbounds.lo[a]) / extent * kBins);
+          b = std::min(std::max(b, 0), kBins - 1);
+          bin_box[b].Grow(boxes[order[i]]);
+          ++bin_count[b];
+        }
+        float right_area[kBins];
+        uint32_t right_count[kBins];
+        Box acc;
+        uint32_t cnt = 0;
+        for (int b = kBins - 1; b > 0; --b) {
+          acc.Grow(bin_box[b]);
+          cnt += bin_count[b];
+          right_area[b] = acc.Area();
+          right_count[b] = cnt;
+        }
+        acc = Box();
+        cnt = 0;
+        for (int b = 0; b < kBins - 1; ++b) {
+          acc.Grow(bin_box[b]);
+          cnt += bin_count[b];
+          if (cnt == 0 || right_count[b + 1] == 0) continue;
+          const float cost = acc.Area() * cnt + right_area[b + 1] * right_count[b + 1];
+          if (cost < best_cost) {
+            best_cost = cost;
+            best_axis = a;
+            best_split = b;
+          }
+        }
+      }
+      uint32_t mid;
+      if (best_axis < 0) {
+        mid = t.first + t.count / 2;  // coincident centroids: split the list
+      } else {
+        const int a = best_axis;
+        const float extent = cbounds.hi[a] - cbounds.lo[a];
+        auto it = std::partition(order.begin() + t.first, order.begin() + t.first + t.count,
+            [&](uint32_t p) {
+              int b = static_cast<int>((centroids[3 * p + a] - cbounds.lo[a]) / extent * kBins);
+              b = std::min(std::max(b, 0), kBins - 1);
+              return b <= best_split;
+            });
+        mid = static_cast<uint32_t>(it - order.begin());
+        if (mid == t.first || mid == t.first + t.count) mid = t.first + t.count / 2;
+      }
+      const uint32_t left = static_cast<uint32_t>(nodes.size());
+      nodes.emplace_back();
+      nodes.emplace_back();
+      nodes[t.node].left = left;
+      nodes[t.node].count = 0;
+      stack.push_back({left, t.first, mid - t.first});
+      stack.push_back({left + 1, mid, t.first + t.count - mid});
+    }
+  }
+};
+
+struct Geometry {
+  std::vector<F3> positions;
+  std::vector<uint32_t> triangles;
+  std::vector<F3> normals;  // 3 per triangle, or empty
+  Bvh bvh;
+};
+
+struct Instance {
+  float m[16];   // world_from_object, column-major
+  float inv[12]; // object_from_world, rows of a 3x4 matrix
+  uint32_t geometry;
+  uint32_t material;
+  Box world;
+};
+
+struct LightRecord {
+  float pdf;
+  float threshold;
+  uint32_t alias;
+  uint32_t instance;
+};
+
+struct Environment {
+  bool bound = false;
+  uint32_t width = 0, height = 0;
+  std::vector<float> texels;  // RGBA
+  F3 scale{1, 1, 1};
+  F3 rows[3];                 // environment_from_world
+  uint32_t columns = 0, rows_count = 0;
+  std::vector<float> floats;  // density, marginal, conditional
+  double mean = 0.0;
+};
+
+}  // namespace
+
+struct oracle_scene {
+  std::vector<Geometry> geometries;
+  std::vector<Instance> instances;
+  std::vector<lotus_material> materials;
+  Bvh tlas;
+  std::vector<LightRecord> lights;
+  std::vector<uint32_t> light_offsets;
+  float environment_selection = 0.0f;
+  F3 environment_constant{0, 0, 0};
+  Environment env;
+};
+
+namespace {
+
+// Object-from-world as a 3x4 float matrix, by Gauss-Jordan elimination in
+// double of the affine part.
+bool InvertAffine(const float* m, float* inv) {
+  double a[3][4];
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) a[r][c] = m[c * 4 + r];
+    a[r][3] = m[12 + r];
+  }
+  // [A | t] -> inverse [A^-1 | -A^-1 t]
+  double aug[3][6];
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) aug[r][c] = a[r][c];
+    for (int c = 0; c < 3; ++c) aug[r][3 + c] = r == c ? 1.0 : 0.0;
+  }
+  for (int c = 0; c < 3; ++c) {
+    int p = c;
+    for (int r = c + 1; r < 3; ++r)
+      if (std::fabs(aug[r][c]) > std::fabs(aug[p][c])) p = r;
+    if (aug[p][c] == 0.0) return false;
+    for (int k = 0; k < 6; ++k) std::swap(aug[c][k], aug[p][k]);
+    const double s = aug[c][c];
+    for (int k = 0; k < 6; ++k) aug[c][k] /= s;
+    for (int r = 0; r < 3; ++r) {
+      if (r == c) continue;
+      const double f = aug[r][c];
+      for (int k = 0; k < 6; ++k) aug[r][k] -= f * aug[c][k];
+    }
+  }
+  for (int r = 0; r < 3; ++r) {
+    double t = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      inv[r * 4 + c] = static_cast<float>(aug[r][3 + c]);
+      t -= aug[r][3 + c] * a[c][3];
+    }
+    inv[r * 4 + 3] = static_cast<float>(t);
+  }
+  return true;
+}
+
+// mul(world_from_object, float4(p, 1)).xyz
+inline F3 TransformPoint(const float* m, F3 p) {
+  return V(m[0] * p.x + m[4] * p.y + m[8] * p.z + m[12],
+           m[1] * p.x + m[5] * p.y + m[9] * p.z + m[13],
+           m[2] * p.x + m[6] * p.y + m[10] * p.z + m[14]);
+}
+
+// EmissionEstimate for a constant UsdPreviewSurface (gpu_scene.cpp:144-180).
+double EmissionEstimate(const lotus_material& m) {
+  double e[3];
+  for (int c = 0; c < 3; ++c) e[c] = m.emission[c];
+  const double factor = 1.0;
+  const double mean = factor * (e[0] + e[1] + e[2]) / 3.0;
+  return std::isfinite(mean) && mean > 0.0 ? mean : 0.0;
+}
+
+// WorldTriangleArea (gpu_scene.cpp:182-203).
+double WorldTriangleArea(const Geometry& g, uint32_t t, const float* m) {
+  double corners[3][3];
+  for (int k = 0; k < 3; ++k) {
+    const F3 p = g.positions[g.triangles[3 * t + k]];
+    for (int r = 0; r < 3; ++r)
+      corners[k][r] = double{m[r]} * p.x + double{m[4 + r]} * p.y +
+                      double{m[8 + r]} * p.z + m[12 + r];
+  }
+  double a[3], b[3];
+  for (int r = 0; r < 3; ++r) {
+    a[r] = corners[1][r] - corners[0][r];
+    b[r] = corners[2][r] - corners[0][r];
+  }
+  const double x = a[1] * b[2] - a[2] * b[1];
+  const double y = a[2] * b[0] - a[0] * b[2];
+  const double z = a[0] * b[1] - a[1] * b[0];
+  const double area = 0.5 * std::sqrt(x * x + y * y + z * z);
+  return std::isfinite(area) ? area : 0.0;
+}
+
+// SceneRadius (gpu_scene.cpp:233-270).
+double SceneRadius(const oracle_scene& s) {
+  constexpr double kInf = std::numeric_limits<double>::infinity();
+  std::vector<std::array<double, 6>> object(s.geometries.size());
+  std::vector<bool> done(s.geometries.size(), false);
+  std::array<double, 6> world{kInf, kInf, kInf, -kInf, -kInf, -kInf};
+  for (const Instance& inst : s.instances) {
+    auto& b = object[inst.geometry];
+    if (!done[inst.geometry]) {
+      done[inst.geometry] = true;
+      b = {kInf, kInf, kInf, -kInf, -kInf, -kInf};
+      for (const F3& p : s.geometries[inst.geometry].positions) {
+        const double v[3] = {p.x, p.y, p.z};
+        for (int a = 0; a < 3; ++a) {
+          b[a] = std::min(b[a], v[a]);
+          b[3 + a] = std::max(b[3 + a], v[a]);
+        }
+      }
+    }
+    if (!(b[0] <= b[3])) continue;
+    const float* m = inst.m;
+    for (int corner = 0; corner < 8; ++corner) {
+      const double p[3] = {b[(corner & 1) ? 3 : 0], b[(corner & 2) ? 4 : 1], b[(corner & 4) ? 5 : 2]};
+      for (int r = 0; r < 3; ++r) {
+        const double v = m[r] * p[0] + m[4 + r] * p[1] + m[8 + r] * p[2] + m[12 + r];
+        world[r] = std::min(world[r], v);
+        world[3 + r] = std::max(world[3 + r], v);
+      }
+    }
+  }
+  if (!(world[0] <= world[3])) return 0.0;
+  const double d[3] = {world[3] - world[0], world[4] - world[1], world[5] - world[2]};
+  const double radius = 0.5 * std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  return std::isfinite(radius) ? radius : 0.0;
+}
+
+// BuildEnvironmentDistribution (gpu_scene.cpp:638-711), RGBA32F texels.
+void BuildEnvironmentDistribution(Environment& env) {
+  constexpr double kPiD = 3.14159265358979323846;
+  const uint32_t columns = std::min(env.width, 2048u);
+  const uint32_t rows = std::min(env.height, 1024u);
+  env.columns = columns;
+  env.rows_count = rows;
+  const size_t cells = size_t{columns} * rows;
+  std::vector<double> sums(cells, 0.0);
+  std::vector<uint32_t> counts(cells, 0);
+  const double scale[3] = {env.scale.x, env.scale.y, env.scale.z};
+  for (uint32_t y = 0; y < env.height; ++y) {
+    const size_t row = uint64_t{y} * rows / env.height;
+    for (uint32_t x = 0; x < env.width; ++x) {
+      const size_t column = uint64_t{x} * columns / env.width;
+      const float* t = &env.texels[4 * (size_t{y} * env.width + x)];
+      double radiance = 0.0;
+      for (int c = 0; c < 3; ++c) radiance += std::max(double{t[c]}, 0.0) * scale[c];
+      sums[row * columns + column] += radiance / 3.0;
+      ++counts[row * columns + column];
+    }
+  }
+  std::vector<double> values(cells), row_sums(rows, 0.0);
+  double total = 0.0;
+  for (uint32_t row = 0; row < rows; ++row) {
+    const double sin_theta = std::sin(kPiD * (row + 0.5) / rows);
+    for (uint32_t column = 0; column < columns; ++column) {
+      const size_t cell = size_t{row} * columns + column;
+      values[cell] = sums[cell] / counts[cell] * sin_theta;
+      row_sums[row] += values[cell];
+    }
+    total += row_sums[row];
+  }
+  const double mean = total / static_cast<double>(cells);
+  std::vector<float> density(cells, 0.0f), marginal(rows + 1, 0.0f),
+      conditional(size_t{rows} * (columns + 1), 0.0f);
+  env.mean = 0.0;
+  if (mean > 0.0 && std::isfinite(mean)) {
+    env.mean = mean;
+    for (size_t cell = 0; cell < cells; ++cell)
+      density[cell] = static_cast<float>(values[cell] / mean);
+    double cumulative = 0.0;
+    for (uint32_t row = 0; row < rows; ++row) {
+      cumulative += row_sums[row];
+      marginal[row + 1] = static_cast<float>(cumulative / total);
+      float* cdf = conditional.data() + size_t{row} * (columns + 1);
+      double along = 0.0;
+      for (uint32_t column = 0; column < columns; ++column) {
+        along += values[size_t{row} * columns + column];
+        cdf[column + 1] = row_sums[row] > 0.0
+            ? static_cast<float>(along / row_sums[row])
+            : static_cast<float>(column + 1) / columns;
+      }
+      cdf[columns] = 1.0f;
+    }
+    marginal[rows] = 1.0f;
+  }
+  env.floats.clear();
+  env.floats.insert(env.floats.end(), density.begin(), density.end());
+  env.floats.insert(env.floats.end(), marginal.begin(), marginal.end());
+  env.floats.insert(env.floats.end(), conditional.begin(), conditional.end());
+  env.bound = env.mean > 0.0;
+}
+
+// BuildLightTable (gpu_scene.cpp:515-610), emissive triangles and the
+// environment image; no analytic lights.
+void BuildLightTable(oracle_scene& s) {
+  s.light_offsets.assign(s.instances.size(), kNoLights);
+  s.lights.clear();
+  std::vector<double> weights;
+  for (size_t index = 0; index < s.instances.size(); ++index) {
+    const Instance& inst = s.instances[index];
+    const Geometry& g = s.geometries[inst.geometry];
+    const double emission = EmissionEstimate(s.materials[inst.material]);
+    const uint32_t tris = static_cast<uint32_t>(g.triangles.size() / 3);
+    if (emission <= 0.0 || tris == 0) continue;
+    s.light_offsets[index] = static_cast<uint32_t>(s.lights.size());
+    for (uint32_t t = 0; t < tris; ++t) {
+      weights.push_back(emission * WorldTriangleArea(g, t, inst.m));
+      s.lights.push_back({0.0f, 1.0f, 0, static_cast<uint32_t>(index)});
+    }
+  }
+  const double environment_mean = s.env.mean;
+  const bool distant = environment_mean > 0.0;
+  const double scene_radius = distant ? SceneRadius(s) : 0.0;
+  double environment_weight = 0.0;
+  if (environment_mean > 0.0) {
+    constexpr double kPiD = 3.14159265358979323846;
+    environment_weight = kPiD * kPiD * scene_radius * scene_radius * environment_mean;
+    if (!std::isfinite(environment_weight))
+      environment_weight = std::numeric_limits<double>::max();
+  }
+  if (environment_weight > 0.0) {
+    weights.push_back(environment_weight);
+    s.lights.push_back({0.0f, 1.0f, 0, kEnvironmentLight});
+  }
+  double total = 0.0;
+  for (double w : weights) total += w;
+  s.environment_selection = 0.0f;
+  if (!(total > 0.0) || !std::isfinite(total)) {
+    s.light_offsets.assign(s.instances.size(), kNoLights);
+    s.lights.clear();
+    return;
+  }
+  const size_t count = s.lights.size();
+  std::vector<double> scaled(count);
+  std::vector<uint32_t> small, large;
+  for (size_t i = 0; i < count; ++i) {
+    s.lights[i].pdf = static_cast<float>(weights[i] / total);
+    scaled[i] = weights[i] / total * static_cast<double>(count);
+    (scaled[i] < 1.0 ? small : large).push_back(static_cast<uint32_t>(i));
+  }
+  while (!small.empty() && !large.empty()) {
+    const uint32_t less = small.back();
+    small.pop_back();
+    const uint32_t more = large.back();
+    s.lights[less].threshold = static_cast<float>(scaled[less]);
+    s.lights[less].alias = more;
+    scaled[more] -= 1.0 - scaled[less];
+    if (scaled[more] < 1.0) {
+      large.pop_back();
+      small.push_back(more);
+    }
+  }
+  for (uint32_t i : small) { s.lights[i].threshold = 1.0f; s.lights[i].alias = i; }
+  for (uint32_t i : large) { s.lights[i].threshold = 1.0f; s.lights[i].alias = i; }
+  if (environment_weight > 0.0) s.environment_selection = s.lights.back().pdf;
+}
+
+// ---------------------------------------------------------------------------
+// Traversal
+
+struct Ray {
+  F3 origin;
+  float tmin;
+  F3 direction;
+  float tmax;
+};
+
+struct Hit {
+  uint32_t instance = 0;
+  uint32_t primitive = 0;
+  float b1 = 0.0f, b2 = 0.0f;
+  float t = 0.0f;
+};
+
+struct Counters {
+  uint64_t nodes = 0;
+  uint64_t triangles = 0;
+};
+
+// The watertight ray/triangle test (Woop, Benthin and Wald, "Watertight
+// Ray/Triangle Intersection", JCGT 2(1), 2013), with its double-precision
+// fallback on an edge.
+struct WatertightRay {
+  F3 org;
+  int kx, ky, kz;
+  float sx, sy, sz;
+};
+
+inline WatertightRay PrepareRay(F3 org, F3 dir) {
+  WatertightRay w;
+  w.org = org;
+  const float ax = std::fabs(dir.x), ay = std::fabs(dir.y), az = std::fabs(dir.z);
+  w.kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  w.kx = w.kz == 2 ? 0 : w.kz + 1;
+  w.ky = w.kx == 2 ? 0 : w.kx + 1;
+  if (Component(dir, w.kz) < 0.0f) std::swap(w.kx, w.ky);
+  const float dz = Component(dir, w.kz);
+  w.sx = Component(dir, w.kx) / dz;
+  w.sy = Component(dir, w.ky) / dz;
+  w.sz = 1.0f / dz;
+  return w;
+}
+
+inline bool IntersectTriangle(const WatertightRay& r, F3 v0, F3 v1, F3 v2,
+    float& t, float& b1, float& b2) {
+  const F3 A = v0 - r.org, B = v1 - r.org, C = v2 - r.org;
+  const float Akz = Component(A, r.kz), Bkz = Component(B, r.kz), Ckz = Component(C, r.kz);
+  const float Ax = Component(A, r.kx) - r.sx * Akz;
+  const float Ay = Component(A, r.ky) - r.sy * Akz;
+  const float Bx = Component(B, r.kx) - r.sx * Bkz;
+  const float By = Component(B, r.ky) - r.sy * Bkz;
+  const float Cx = Component(C, r.kx) - r.sx * Ckz;
+  const float Cy = Component(C, r.ky) - r.sy * Ckz;
+  float U = Cx * By - Cy * Bx;
+  float Vv = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.0f || Vv == 0.0f || W == 0.0f) {
+    U = static_cast<float>(double(Cx) * double(By) - double(Cy) * double(Bx));
+    Vv = static_cast<float>(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+    W = static_cast<float>(double(Bx) * double(Ay) - double(By) * double(Ax));
+  }
+  if ((U < 0.0f || Vv < 0.0f || W < 0.0f) && (U > 0.0f || Vv > 0.0f || W > 0.0f)) return false;
+  const float det = U + Vv + W;
+  if (det == 0.0f) return false;
+  const float Az = r.sz * Akz, Bz = r.sz * Bkz, Cz = r.sz * Ckz;
+  const float T = U * Az + Vv * Bz + W * Cz;
+  const float rcp = 1.0f / det;
+  t = T * rcp;
+  b1 = Vv * rcp;
+  b2 = W * rcp;
+  return true;
+}
+
+// Whether the segment [tmin, tmax] meets the box; conservative by the
+// relative margin of Pharr et al. (PBR 3rd ed., section 3.9.2).
+inline bool OverlapsBox(const Box& b, F3 org, F3 inv, float tmin, float tmax) {
+  float t0 = tmin, t1 = tmax;
+  const float o[3] = {org.x, org.y, org.z};
+  const float d[3] = {inv.x, inv.y, inv.z};
+  for (int a = 0; a < 3; ++a) {
+    float tn = (b.lo[a] - o[a]) * d[a];
+    float tf = (b.hi[a] - o[a]) * d[a];
+    if (tn > tf) std::swap(tn, tf);
+    tf *= 1.0000004f;
+    t0 = tn > t0 ? tn : t0;
+    t1 = tf < t1 ? tf : t1;
+    if (t0 > t1) return false;
+  }
+  return true;
+}
+
+inline F3 Inverse(F3 d) {
+  auto inv = [](float x) {
+    return 1.0f / (std::fabs(x) > 1e-30f ? x : (x < 0.0f ? -1e-30f : 1e-30f));
+  };
+  return V(inv(d.x), inv(d.y), inv(d.z));
+}
+
+// Coverage (scene.slang:393-406): a material's constant opacity.
+inline float Coverage(const oracle_scene& s, uint32_t instance) {
+  const lotus_material& m = s.materials[s.instances[instance].material];
+  const float opacity = m.opacity;
+  const float threshold = m.opacity_threshold;
+  if (threshold > 0.0f) return opacity >= threshold ? 1.0f : 0.0f;
+  return opacity;
+}
+
+// AcceptSurface (scene.slang:408-413).
+inline bool AcceptSurface(const oracle_scene& s, uint32_t instance, uint32_t& rng) {
+  const float coverage = Coverage(s, instance);
+  if (coverage <= 0.0f) return false;
+  if (coverage >= 1.0f) return true;
+  return NextRandom(rng) < coverage;
+}
+
+inline F3 ObjectPoint(const float* inv, F3 p) {
+  return V(inv[0] * p.x + inv[1] * p.y + inv[2] * p.z + inv[3],
+           inv[4] * p.x + inv[5] * p.y + inv[6] * p.z + inv[7],
+           inv[8] * p.x + inv[9] * p.y + inv[10] * p.z + inv[11]);
+}
+inline F3 ObjectVector(const float* inv, F3 d) {
+  return V(inv[0] * d.x + inv[1] * d.y + inv[2] * d.z,
+           inv[4] * d.x + inv[5] * d.y + inv[6] * d.z,
+           inv[8] * d.x + inv[9] * d.y + inv[10] * d.z);
+}
+
+// Visits every triangle the ray's segment may meet, in BVH order, calling
+// `candidate(instance, primitive, t, b1, b2)` for each intersection with t
+// in [tmin, limit()]. `candidate` returns false to end the traversal.
+template <typename Candidate, typename Limit>
+void Traverse(const oracle_scene& s, const Ray& ray, Candidate&& candidate,
+    Limit&& limit, Counters* counters) {
+  if (s.tlas.nodes.empty() || s.instances.empty()) return;
+  const F3 inv_world = Inverse(ray.direction);
+  uint32_t stack[128];
+  int top = 0;
+  stack[top++] = 0;
+  while (top > 0) {
+    const Bvh::Node& node = s.tlas.nodes[stack[--top]];
+    if (counters) ++counters->nodes;
+    if (!OverlapsBox(node.box, ray.origin, inv_world, ray.tmin, limit())) continue;
+    if (node.count == 0) {
+      stack[top++] = node.left + 1;
+      stack[top++] = node.left;
+      continue;
+    }
+    for (uint32_t k = 0; k < node.count; ++k) {
+      const uint32_t ii = s.tlas.order[node.first + k];
+      const Instance& inst = s.instances[ii];
+      const Geometry& g = s.geometries[inst.geometry];
+      if (g.bvh.nodes.empty() || g.triangles.empty()) continue;
+      const F3 o = ObjectPoint(inst.inv, ray.origin);
+      const F3 d = ObjectVector(inst.inv, ray.direction);
+      const WatertightRay w = PrepareRay(o, d);
+      const F3 inv = Inverse(d);
+      uint32_t bstack[128];
+      int btop = 0;
+      bstack[btop++] = 0;
+      while (btop > 0) {
+        const Bvh::Node& bn = g.bvh.nodes[bstack[--btop]];
+        if (counters) ++counters->nodes;
+        if (!OverlapsBox(bn.box, o, inv, ray.tmin, limit())) continue;
+        if (bn.count == 0) {
+          bstack[btop++] = bn.left + 1;
+          bstack[btop++] = bn.left;
+          continue;
+        }
+        for (uint32_t j = 0; j < bn.count; ++j) {
+          const uint32_t p = g.bvh.order[bn.first + j];
+          if (counters) ++counters->triangles;
+          float t, b1, b2;
+          if (!IntersectTriangle(w, g.positions[g.triangles[3 * p]],
+                  g.positions[g.triangles[3 * p + 1]],
+                  g.positions[g.triangles[3 * p + 2]], t, b1, b2))
+            continue;
+          if (!(t >= ray.tmin) || !(t <= limit())) continue;
+          if (!candidate(ii, p, t, b1, b2)) return;
+        }
+      }
+    }
+  }
+}
+
+// Trace (scene.slang:424-439): the closest accepted hit.
+bool Trace(const oracle_scene& s, const Ray& ray, uint32_t& rng, Hit& hit,
+    Counters* counters = nullptr) {
+  bool found = false;
+  float best = ray.tmax;
+  Hit h;
+  Traverse(s, ray,
+      [&](uint32_t ii, uint32_t p, float t, float b1, float b2) {
+        if (found && (t > best || (t == best &&
+                (ii > h.instance || (ii == h.instance && p >= h.primitive)))))
+          return true;
+        if (!AcceptSurface(s, ii, rng)) return true;
+        found = true;
+        best = t;
+        h.instance = ii;
+        h.primitive = p;
+        h.b1 = b1;
+        h.b2 = b2;
+        h.t = t;
+        return true;
+      },
+      [&]() { return best; }, counters);
+  hit = found ? h : Hit{};
+  return found;
+}
+
+// ShadowTransmittance (scene.slang:445-460).
+float ShadowTransmittance(const oracle_scene& s, const Ray& ray) {
+  float transmittance = 1.0f;
+  bool blocked = false;
+  Traverse(s, ray,
+      [&](uint32_t ii, uint32_t, float, float, float) {
+        const float coverage = Coverage(s, ii);
+        if (coverage >= 1.0f) {
+          blocked = true;
+          return false;
+        }
+        if (coverage > 0.0f) transmittance *= 1.0f - coverage;
+        return true;
+      },
+      [&]() { return ray.tmax; }, nullptr);
+  return blocked ? 0.0f : transmittance;
+}
+
+// ---------------------------------------------------------------------------
+// Hits, lights and the environment
+
+struct SurfaceHit {
+  F3 position;
+  F3 normal;
+  F3 shading_normal;
+  float area;
+  F3 base_color;
+  float roughness;
+  float metallic;
+  PreviewClosure bsdf;
+  F3 emission;
+};
+
+// OffsetRayOrigin (scene.slang:1454-1469).
+F3 OffsetRayOrigin(F3 position, F3 normal) {
+  constexpr float kOrigin = 1.0f / 32.0f;
+  constexpr float kFloatScale = 1.0f / 65536.0f;
+  constexpr float kIntScale = 256.0f;
+  float p[3] = {position.x, position.y, position.z};
+  const float n[3] = {normal.x, normal.y, normal.z};
+  float r[3];
+  for (int a = 0; a < 3; ++a) {
+    const int offset = static_cast<int>(kIntScale * n[a]);
+    const float moved = AsFloat(static_cast<uint32_t>(
+        static_cast<int32_t>(AsUint(p[a])) + (p[a] < 0.0f ? -offset : offset)));
+    r[a] = std::fabs(p[a]) < kOrigin ? p[a] + kFloatScale * n[a] : moved;
+  }
+  return V(r[0], r[1], r[2]);
+}
+
+// ShadingNormal (scene.slang:467-488).
+F3 ShadingNormal(const F3* n, float b1, float b2, const float* m, F3 geometric, F3 direction) {
+  const F3 object = n[0] + b1 * (n[1] - n[0]) + b2 * (n[2] - n[0]);
+  const F3 c0 = V(m[0], m[1], m[2]);
+  const F3 c1 = V(m[4], m[5], m[6]);
+  const F3 c2 = V(m[8], m[9], m[10]);
+  const F3 world = cross(c1, c2) * object.x + cross(c2, c0) * object.y + cross(c0, c1) * object.z;
+  const float length2 = dot(world, world);
+  if (!(length2 > 0.0f) || std::isinf(length2)) return geometric;
+  F3 shading = world * rsqrt(length2);
+  if (dot(shading, geometric) < 0.0f) shading = -shading;
+  return dot(shading, direction) < 0.0f ? shading : geometric;
+}
+
+inline float TriangleArea(F3 p0, F3 p1, F3 p2) { return 0.5f * length(cross(p1 - p0, p2 - p0)); }
+
+// ReconstructHit + EvaluatePreview for constant inputs
+// (scene.slang:1408-1449, 1184-1260).
+SurfaceHit ReconstructHit(const oracle_scene& s, const Hit& hit, F3 direction) {
+  const Instance& inst = s.instances[hit.instance];
+  const Geometry& g = s.geometries[inst.geometry];
+  const uint32_t* tri = &g.triangles[3 * hit.primitive];
+  const F3 p0 = TransformPoint(inst.m, g.positions[tri[0]]);
+  const F3 p1 = TransformPoint(inst.m, g.positions[tri[1]]);
+  const F3 p2 = TransformPoint(inst.m, g.positions[tri[2]]);
+  SurfaceHit sh;
+  sh.position = p0 + hit.b1 * (p1 - p0) + hit.b2 * (p2 - p0);
+  const F3 normal = normalize(cross(p1 - p0, p2 - p0));
+  sh.area = TriangleArea(p0, p1, p2);
+  sh.normal = dot(normal, direction) > 0.0f ? -normal : normal;
+  sh.shading_normal = sh.normal;
+  if (!g.normals.empty())
+    sh.shading_normal = ShadingNormal(&g.normals[3 * hit.primitive], hit.b1, hit.b2,
+        inst.m, sh.normal, direction);
+  const lotus_material& mat = s.materials[inst.material];
+  sh.base_color = V(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
+  sh.roughness = mat.roughness;
+  sh.metallic = mat.metallic;
+  const F3 emission = V(mat.emission[0], mat.emission[1], mat.emission[2]);
+  const F3 specular = V(mat.specular_color[0], mat.specular_color[1], mat.specular_color[2]);
+  bool entering = true;
+  const float transmission = mat.transmission;
+  if (transmission > 0.0f) {
+    const F3 c0 = V(inst.m[0], inst.m[1], inst.m[2]);
+    const F3 c1 = V(inst.m[4], inst.m[5], inst.m[6]);
+    const F3 c2 = V(inst.m[8], inst.m[9], inst.m[10]);
+    const F3 outward = dot(c0, cross(c1, c2)) < 0.0f ? -normal : normal;
+    entering = dot(outward, direction) < 0.0f;
+  }
+  sh.bsdf = MakePreviewClosure(sh.base_color, sh.roughness, sh.metallic, mat.ior,
+      (mat.flags & LOTUS_MATERIAL_SPECULAR_WORKFLOW) != 0, specular, transmission,
+      V(mat.transmission_color[0], mat.transmission_color[1], mat.transmission_color[2]),
+      (mat.flags & LOTUS_MATERIAL_THIN_WALLED) != 0, entering);
+  sh.emission = emission;
+  return sh;
+}
+
+struct LightSample {
+  F3 direction;
+  float distance;
+  F3 radiance;
+  float pdf;
+  bool delta;
+};
+
+inline LightSample NoLight() { return LightSample{V(0.0f, 0.0f, 1.0f), 0.0f, V(0.0f), 0.0f, false}; }
+
+// SampleTriangle (scene.slang:632-677).
+LightSample SampleTriangle(const oracle_scene& s, uint32_t light, const LightRecord& chosen,
+    float ux, float uy, F3 origin) {
+  const uint32_t primitive = light - s.light_offsets[chosen.instance];
+  const float root = std::sqrt(ux);
+  const float b1 = root * (1.0f - uy), b2 = root * uy;
+  const Instance& inst = s.instances[chosen.instance];
+  const Geometry& g = s.geometries[inst.geometry];
+  const uint32_t* tri = &g.triangles[3 * primitive];
+  const F3 p0 = TransformPoint(inst.m, g.positions[tri[0]]);
+  const F3 p1 = TransformPoint(inst.m, g.positions[tri[1]]);
+  const F3 p2 = TransformPoint(inst.m, g.positions[tri[2]]);
+  const lotus_material& mat = s.materials[inst.material];
+  const F3 position = p0 + b1 * (p1 - p0) + b2 * (p2 - p0);
+  const F3 normal = normalize(cross(p1 - p0, p2 - p0));
+  const float area = TriangleArea(p0, p1, p2);
+  const F3 radiance = V(mat.emission[0], mat.emission[1], mat.emission[2]) * Coverage(s, chosen.instance);
+  const F3 toward = position - origin;
+  const float distance2 = dot(toward, toward);
+  if (!(area > 0.0f) || !(distance2 > 0.0f) || MaxComponent(radiance) <= 0.0f) return NoLight();
+  LightSample ls;
+  ls.direction = toward * rsqrt(distance2);
+  const float cosine = std::fabs(dot(normal, ls.direction));
+  if (!(cosine > 0.0f)) return NoLight();
+  const F3 end = OffsetRayOrigin(position, dot(normal, ls.direction) > 0.0f ? -normal : normal);
+  ls.distance = std::fmax(0.0f, dot(end - origin, ls.direction));
+  ls.radiance = radiance;
+  ls.pdf = chosen.pdf / area * distance2 / cosine;
+  ls.delta = false;
+  return ls;
+}
+
+inline float EnvFloat(const oracle_scene& s, uint64_t index) { return s.env.floats[index]; }
+
+// FindInterval (scene.slang:775-789).
+uint32_t FindInterval(const oracle_scene& s, uint64_t first, uint32_t count, float u) {
+  uint32_t low = 0;
+  uint32_t len = count + 1;
+  while (len > 0) {
+    const uint32_t half = len >> 1;
+    const uint32_t middle = low + half;
+    if (EnvFloat(s, first + middle) <= u) {
+      low = middle + 1;
+      len -= half + 1;
+    } else {
+      len = half;
+    }
+  }
+  return std::min(std::max(low, 1u), count) - 1;
+}
+
+// SampleCumulative (scene.slang:794-800).
+float SampleCumulative(const oracle_scene& s, uint64_t first, uint32_t count, float u, uint32_t& cell) {
+  cell = FindInterval(s, first, count, u);
+  const float low = EnvFloat(s, first + cell);
+  const float width = EnvFloat(s, first + cell + 1) - low;
+  const float offset = width > 0.0f ? (u - low) / width : 0.5f;
+  return std::fmin((float(cell) + offset) / float(count), 0.99999994f);
+}
+
+// EnvironmentUv (scene.slang:805-809).
+inline void EnvironmentUv(F3 local, float& u, float& v) {
+  const float uu = 0.5f - std::atan2(local.x, local.z) * (0.5f / kPi);
+  v = std::acos(std::fmin(std::fmax(local.y, -1.0f), 1.0f)) * (1.0f / kPi);
+  u = uu - std::floor(uu);
+}
+
+// EnvironmentDirection (scene.slang:811-816).
+inline F3 EnvironmentDirection(float u, float v) {
+  const float theta = kPi * v;
+  const float phi = kPi * (1.0f - 2.0f * u);
+  const float sin_theta = std::sin(theta);
+  return V(sin_theta * std::sin(phi), std::cos(theta), sin_theta * std::cos(phi));
+}
+
+// EnvironmentLookup (scene.slang:819-824): the bilinear texel, repeating
+// across longitude and clamped at the poles, times the scale.
+F3 EnvironmentLookup(const oracle_scene& s, float u, float v) {
+  const Environment& e = s.env;
+  const float x = u * float(e.width) - 0.5f;
+  const float y = v * float(e.height) - 0.5f;
+  const float fx0 = std::floor(x), fy0 = std::floor(y);
+  const float ax = x - fx0, ay = y - fy0;
+  const int w = static_cast<int>(e.width), h = static_cast<int>(e.height);
+  int x0 = static_cast<int>(fx0) % w;
+  if (x0 < 0) x0 += w;
+  const int x1 = x0 + 1 == w ? 0 : x0 + 1;
+  const int iy = static_cast<int>(fy0);
+  const int y0 = std::min(std::max(iy, 0), h - 1);
+  const int y1 = std::min(std::max(iy + 1, 0), h - 1);
+  const float* t00 = &e.texels[4 * (size_t(y0) * w + x0)];
+  const float* t10 = &e.texels[4 * (size_t(y0) * w + x1)];
+  const float* t01 = &e.texels[4 * (size_t(y1) * w + x0)];
+  const float* t11 = &e.texels[4 * (size_t(y1) * w + x1)];
+  float c[3];
+  for (int k = 0; k < 3; ++k) {
+    const float top = t00[k] * (1.0f - ax) + t10[k] * ax;
+    const float bottom = t01[k] * (1.0f - ax) + t11[k] * ax;
+    c[k] = top * (1.0f - ay) + bottom * ay;
+  }
+  return V(std::fmax(c[0], 0.0f) * e.scale.x, std::fmax(c[1], 0.0f) * e.scale.y,
+      std::fmax(c[2], 0.0f) * e.scale.z);
+}
+
+// EnvironmentDirectionPdf (scene.slang:829-840).
+float EnvironmentDirectionPdf(const oracle_scene& s, float u, float v) {
+  const uint32_t column = std::min(static_cast<uint32_t>(u * float(s.env.columns)), s.env.columns - 1);
+  const uint32_t row = std::min(static_cast<uint32_t>(v * float(s.env.rows_count)), s.env.rows_count - 1);
+  const float sin_theta = std::sin(kPi * v);
+  if (!(sin_theta > 0.0f)) return 0.0f;
+  return EnvFloat(s, uint64_t(row) * s.env.columns + column) / (2.0f * kPi * kPi * sin_theta);
+}
+
+// SampleEnvironment (scene.slang:845-872).
+LightSample SampleEnvironment(const oracle_scene& s, float selection, float ux, float uy) {
+  const Environment& e = s.env;
+  const uint64_t cells = uint64_t(e.columns) * e.rows_count;
+  uint32_t row, column;
+  const float v = SampleCumulative(s, cells, e.rows_count, ux, row);
+  const float u = SampleCumulative(s, cells + e.rows_count + 1 + uint64_t(row) * (e.columns + 1),
+      e.columns, uy, column);
+  const float sin_theta = std::sin(kPi * v);
+  const float density = EnvFloat(s, uint64_t(row) * e.columns + column);
+  if (!(sin_theta > 0.0f) || !(density > 0.0f)) return NoLight();
+  const F3 local = EnvironmentDirection(u, v);
+  LightSample ls;
+  ls.direction = normalize(local.x * e.rows[0] + local.y * e.rows[1] + local.z * e.rows[2]);
+  ls.distance = kFloatMax;
+  ls.radiance = EnvironmentLookup(s, u, v);
+  ls.pdf = selection * density / (2.0f * kPi * kPi * sin_theta);
+  ls.delta = false;
+  return ls;
+}
+
+// EnvironmentRadiance (scene.slang:877-890).
+F3 EnvironmentRadiance(const oracle_scene& s, F3 direction, bool weigh, float pdf) {
+  const Environment& e = s.env;
+  const F3 local = V(dot(e.rows[0], direction), dot(e.rows[1], direction), dot(e.rows[2], direction));
+  float u, v;
+  EnvironmentUv(local, u, v);
+  const F3 radiance = EnvironmentLookup(s, u, v);
+  if (!weigh || !(s.environment_selection > 0.0f)) return radiance;
+  return radiance * PowerHeuristic(pdf, s.environment_selection * EnvironmentDirectionPdf(s, u, v));
+}
+
+// SampleLight (scene.slang:894-909).
+LightSample SampleLight(const oracle_scene& s, const float* u, F3 origin) {
+  const uint32_t count = static_cast<uint32_t>(s.lights.size());
+  const uint32_t column = std::min(static_cast<uint32_t>(u[0] * float(count)), count - 1);
+  const LightRecord& record = s.lights[column];
+  const uint32_t light = u[1] < record.threshold ? column : record.alias;
+  const LightRecord& chosen = s.lights[light];
+  if (chosen.instance == kEnvironmentLight) return SampleEnvironment(s, chosen.pdf, u[2], u[3]);
+  return SampleTriangle(s, light, chosen, u[2], u[3], origin);
+}
+
+// EmitterPdf (scene.slang:1004-1010).
+float EmitterPdf(const oracle_scene& s, const Hit& hit, float area) {
+  const uint32_t first = s.light_offsets[hit.instance];
+  if (first == kNoLights || !(area > 0.0f)) return 0.0f;
+  return s.lights[first + hit.primitive].pdf / area;
+}
+
+// ---------------------------------------------------------------------------
+// transport.slang
+
+struct PathState {
+  Ray ray;
+  F3 throughput;
+  F3 radiance;
+  uint32_t pixel_index;
+  uint32_t depth;
+  uint32_t rng;
+  float last_pdf;
+  uint32_t flags;
+};
+constexpr uint32_t kUnweightedLight = 1;
+
+struct FrameConstants {
+  float clip_to_world[16];
+  float ndc_from_pixel[4];
+  uint32_t width;
+  uint32_t max_bounces;
+  bool sample_lights;
+};
+
+struct RayCounts {
+  uint64_t camera = 0, extension = 0, shadow = 0;
+};
+
+// CameraRay (scene.slang:273-283).
+Ray CameraRay(const FrameConstants& f, float nx, float ny, float nz_far) {
+  (void)nz_far;
+  const float* c = f.clip_to_world;
+  auto mul = [&](float x, float y, float z, float w, float* out) {
+    for (int r = 0; r < 4; ++r)
+      out[r] = c[r] * x + c[4 + r] * y + c[8 + r] * z + c[12 + r] * w;
+  };
+  float n[4], fa[4];
+  mul(nx, ny, 0.0f, 1.0f, n);
+  mul(nx, ny, 1.0f, 1.0f, fa);
+  Ray ray;
+  ray.origin = V(n[0] / n[3], n[1] / n[3], n[2] / n[3]);
+  ray.direction = normalize(V(fa[0], fa[1], fa[2]) * n[3] - V(n[0], n[1], n[2]) * fa[3]);
+  ray.tmin = 0.0f;
+  ray.tmax = fa[3] == 0.0f ? kFloatMax
+                           : length(V(fa[0] / fa[3], fa[1] / fa[3], fa[2] / fa[3]) - ray.origin);
+  return ray;
+}
+
+// StartPath (transport.slang:53-69).
+PathState StartPath(const FrameConstants& f, uint32_t px, uint32_t py, uint32_t sample_index) {
+  PathState p;
+  p.throughput = V(1.0f);
+  p.radiance = V(0.0f);
+  p.pixel_index = py * f.width + px;
+  p.depth = 0;
+  p.rng = SeedRandom(p.pixel_index, sample_index);
+  p.last_pdf = 0.0f;
+  p.flags = 0;
+  const float ux = NextRandom(p.rng);
+  const float uy = NextRandom(p.rng);
+  const float film_x = float(px) + 0.5f + (ux - 0.5f);
+  const float film_y = float(py) + 0.5f + (uy - 0.5f);
+  p.ray = CameraRay(f, film_x * f.ndc_from_pixel[0] + f.ndc_from_pixel[2],
+      film_y * f.ndc_from_pixel[1] + f.ndc_from_pixel[3], 1.0f);
+  return p;
+}
+
+inline bool WeighFoundLight(const FrameConstants& f, const PathState& p) {
+  return f.sample_lights && (p.flags & kUnweightedLight) == 0;
+}
+
+// ShadowedLight (transport.slang:82-115).
+F3 ShadowedLight(const oracle_scene& s, const SurfaceHit& sh, const ShadingFrame& basis, F3 wo,
+    F3 origin, const LightSample& ls, RayCounts& rays) {
+  if (!(ls.pdf > 0.0f) || MaxComponent(ls.radiance) <= 0.0f || dot(ls.direction, sh.normal) <= 0.0f)
+    return V(0.0f);
+  const F3 wi = basis.ToLocal(ls.direction);
+  if (wi.z <= 0.0f) return V(0.0f);
+  const F3 f = PreviewEvaluate(sh.bsdf, wo, wi);
+  if (MaxComponent(f) <= 0.0f) return V(0.0f);
+  Ray shadow{origin, 0.0f, ls.direction, ls.distance};
+  ++rays.shadow;
+  const float transmittance = ShadowTransmittance(s, shadow);
+  if (transmittance <= 0.0f) return V(0.0f);
+  const float weight = ls.delta ? 1.0f : PowerHeuristic(ls.pdf, PreviewPdf(sh.bsdf, wo, wi));
+  const F3 contribution = f * ls.radiance * (transmittance * weight / ls.pdf);
+  return IsFinite(contribution) ? contribution : V(0.0f);
+}
+
+// DirectLight (transport.slang:123-135).
+F3 DirectLight(const oracle_scene& s, const SurfaceHit& sh, const ShadingFrame& basis, F3 wo,
+    uint32_t& rng, RayCounts& rays) {
+  if (s.lights.empty()) return V(0.0f);
+  float u[4];
+  u[0] = NextRandom(rng);
+  u[1] = NextRandom(rng);
+  u[2] = NextRandom(rng);
+  u[3] = NextRandom(rng);
+  const F3 origin = OffsetRayOrigin(sh.position, sh.normal);
+  return ShadowedLight(s, sh, basis, wo, origin, SampleLight(s, u, origin), rays);
+}
+
+// EmissionWeight (transport.slang:150-158).
+float EmissionWeight(const oracle_scene& s, const PathState& p, const Hit& hit, const SurfaceHit& sh) {
+  const float area_pdf = EmitterPdf(s, hit, sh.area);
+  if (!(area_pdf > 0.0f)) return 1.0f;
+  const F3 toward = sh.position - p.ray.origin;
+  const float cosine = std::fabs(dot(sh.normal, p.ray.direction));
+  return PowerHeuristic(p.last_pdf, area_pdf * dot(toward, toward) / cosine);
+}
+
+// ScatterPath (transport.slang:164-230), without ReSTIR or analytic lights.
+bool ScatterPath(const oracle_scene& s, const FrameConstants& f, PathState& p, const Hit& hit,
+    RayCounts& rays) {
+  const SurfaceHit sh = ReconstructHit(s, hit, p.ray.direction);
+  F3 emission = sh.emission;
+  if (WeighFoundLight(f, p) && p.depth != 0 && MaxComponent(emission) > 0.0f)
+    emission = emission * EmissionWeight(s, p, hit, sh);
+  p.radiance = p.radiance + p.throughput * emission;
+  if (p.depth >= f.max_bounces) return false;
+  if (p.depth >= kRouletteBounces) {
+    const float survival = std::fmin(MaxComponent(p.throughput), kMaxSurvival);
+    if (NextRandom(p.rng) >= survival) return false;
+    p.throughput = p.throughput / survival;
+  }
+  const ShadingFrame basis = MakeShadingFrame(sh.shading_normal);
+  const F3 wo = basis.ToLocal(-p.ray.direction);
+  if (f.sample_lights)
+    p.radiance = p.radiance + p.throughput * DirectLight(s, sh, basis, wo, p.rng, rays);
+  F3 u;
+  u.x = NextRandom(p.rng);
+  u.y = NextRandom(p.rng);
+  u.z = NextRandom(p.rng);
+  BsdfSampleResult sample;
+  if (!PreviewSample(sh.bsdf, wo, u, sample)) return false;
+  const F3 wi = normalize(basis.ToWorld(sample.wi));
+  const float side = dot(wi, sh.normal);
+  if (sample.transmitted ? side >= 0.0f : side <= 0.0f) return false;
+  p.throughput = p.throughput * sample.weight;
+  p.last_pdf = sample.pdf;
+  if (sample.delta || sample.transmitted)
+    p.flags |= kUnweightedLight;
+  else
+    p.flags &= ~kUnweightedLight;
+  p.ray.origin = OffsetRayOrigin(sh.position, sample.transmitted ? -sh.normal : sh.normal);
+  p.ray.direction = wi;
+  p.ray.tmin = 0.0f;
+  p.ray.tmax = kFloatMax;
+  ++p.depth;
+  return true;
+}
+
+// MissPath (transport.slang:235-247), without analytic lights.
+void MissPath(const oracle_scene& s, const FrameConstants& f, PathState& p) {
+  F3 environment = s.environment_constant;
+  if (s.env.bound)
+    environment = environment + EnvironmentRadiance(s, p.ray.direction, WeighFoundLight(f, p), p.last_pdf);
+  p.radiance = p.radiance + p.throughput * environment;
+}
+
+// TracePath and the radiance pass's sample (path_trace.slang:279-287,
+// 357-366): the radiance of one camera path, or false when it misses.
+bool PathSample(const oracle_scene& s, const FrameConstants& f, uint32_t px, uint32_t py,
+    uint32_t sample_index, F3& radiance, RayCounts& rays) {
+  PathState p = StartPath(f, px, py, sample_index);
+  Hit hit;
+  ++rays.camera;
+  if (!Trace(s, p.ray, p.rng, hit)) return false;
+  while (ScatterPath(s, f, p, hit, rays)) {
+    ++rays.extension;
+    if (!Trace(s, p.ray, p.rng, hit)) {
+      MissPath(s, f, p);
+      break;
+    }
+  }
+  radiance = p.radiance;
+  return true;
+}
+
+// Invert (vulkan_backend.cpp:436-470): Gauss-Jordan in double with partial
+// pivoting.
+bool Invert4(const float* matrix, float* inverse) {
+  double rows[4][8] = {};
+  for (int row = 0; row < 4; ++row) {
+    for (int column = 0; column < 4; ++column) {
+      const float value = matrix[column * 4 + row];
+      if (!std::isfinite(value)) return false;
+      rows[row][column] = value;
+    }
+    rows[row][row + 4] = 1.0;
+  }
+  for (int column = 0; column < 4; ++column) {
+    int pivot = column;
+    for (int row = column + 1; row < 4; ++row)
+      if (std::abs(rows[row][column]) > std::abs(rows[pivot][column])) pivot = row;
+    if (rows[pivot][column] == 0.0) return false;
+    for (int index = 0; index < 8; ++index) std::swap(rows[column][index], rows[pivot][index]);
+    const double scale = rows[column][column];
+    for (double& value : rows[column]) value /= scale;
+    for (int row = 0; row < 4; ++row) {
+      if (row == column) continue;
+      const double factor = rows[row][column];
+      for (int index = 0; index < 8; ++index) rows[row][index] -= factor * rows[column][index];
+    }
+  }
+  for (int row = 0; row < 4; ++row) {
+    for (int column = 0; column < 4; ++column) {
+      const float value = static_cast<float>(rows[row][column + 4]);
+      if (!std::isfinite(value)) return false;
+      inverse[column * 4 + row] = value;
+    }
+  }
+  return true;
+}
+
+// The frame's constants: VulkanWorldToClip (vulkan_internal.hpp:326-336),
+// Invert, and the display viewport's ndc_from_pixel
+// (vulkan_backend.cpp:2406-2412, 651-658).
+bool MakeFrame(const lotus_frame_desc& d, FrameConstants& f, uint32_t rect[4]) {
+  float vulkan[16];
+  std::memcpy(vulkan, d.world_to_clip, sizeof(vulkan));
+  for (int column = 0; column < 4; ++column) {
+    const float y = d.world_to_clip[column * 4 + 1];
+    const float z = d.world_to_clip[column * 4 + 2];
+    const float w = d.world_to_clip[column * 4 + 3];
+    vulkan[column * 4 + 1] = -y;
+    vulkan[column * 4 + 2] = 0.5f * (z + w);
+  }
+  if (!Invert4(vulkan, f.clip_to_world)) return false;
+  const lotus_target& t = d.target;
+  float vx = 0.0f, vy = 0.0f, vw = float(t.width), vh = float(t.height);
+  if (t.display_window[2] > 0.0f && t.display_window[3] > 0.0f) {
+    vx = t.display_window[0];
+    vy = t.display_window[1];
+    vw = t.display_window[2];
+    vh = t.display_window[3];
+  }
+  f.ndc_from_pixel[0] = 2.0f / vw;
+  f.ndc_from_pixel[1] = 2.0f / vh;
+  f.ndc_from_pixel[2] = -2.0f * vx / vw - 1.0f;
+  f.ndc_from_pixel[3] = -2.0f * vy / vh - 1.0f;
+  f.width = t.width;
+  f.max_bounces = d.settings.max_bounces;
+  f.sample_lights = d.settings.light_sampling != LOTUS_LIGHT_SAMPLING_BSDF;
+  const int32_t* w = t.data_window;
+  if (w[2] <= 0 || w[3] <= 0) {
+    rect[0] = 0; rect[1] = 0; rect[2] = t.width; rect[3] = t.height;
+  } else {
+    const int64_t x0 = std::max<int64_t>(w[0], 0), y0 = std::max<int64_t>(w[1], 0);
+    const int64_t x1 = std::min<int64_t>(int64_t{w[0]} + w[2], t.width);
+    const int64_t y1 = std::min<int64_t>(int64_t{w[1]} + w[3], t.height);
+    if (x1 <= x0 || y1 <= y0) {
+      rect[0] = rect[1] = rect[2] = rect[3] = 0;
+    } else {
+      rect[0] = uint32_t(x0); rect[1] = uint32_t(y0);
+      rect[2] = uint32_t(x1 - x0); rect[3] = uint32_t(y1 - y0);
+    }
+  }
+  return true;
+}
+
+int ThreadCount(int32_t threads) {
+#ifdef _OPENMP
+  return threads > 0 ? threads : omp_get_max_threads();
+#else
+  (void)threads;
+  return 1;
+#endif
+}
+
+void SetError(char* error, size_t size, const std::string& message) {
+  if (error && size) std::snprintf(error, size, "%s", message.c_str());
+}
+
+}  // namespace
+
+extern "C" {
+
+oracle_scene* oracle_scene_create(const lotus_scene_desc* d, char* error, size_t error_size) {
+  if (!d) {
+    SetError(error, error_size, "no scene");
+    return nullptr;
+  }
+  auto s = std::make_unique<oracle_scene>();
+  s->materials.assign(d->materials, d->materials + d->material_count);
+  if (s->materials.empty()) {
+    SetError(error, error_size, "the scene has no material");
+    return nullptr;
+  }
+  s->geometries.resize(d->geometry_count);
+  for (uint32_t gi = 0; gi < d->geometry_count; ++gi) {
+    const lotus_geometry& src = d->geometries[gi];
+    Geometry& g = s->geometries[gi];
+    g.positions.resize(src.vertex_count);
+    for (uint32_t v = 0; v < src.vertex_count; ++v)
+      g.positions[v] = V(src.positions[3 * v], src.positions[3 * v + 1], src.positions[3 * v + 2]);
+    g.triangles.assign(src.triangles, src.triangles + 3 * size_t{src.triangle_count});
+    for (uint32_t idx : g.triangles) {
+      if (idx >= src.vertex_count) {
+        SetError(error, error_size, "a triangle indexes past its geometry's vertices");
+        return nullptr;
+      }
+    }
+    if (src.normals) {
+      g.normals.resize(3 * size_t{src.triangle_count});
+      for (size_t k = 0; k < g.normals.size(); ++k)
+        g.normals[k] = V(src.normals[3 * k], src.normals[3 * k + 1], src.normals[3 * k + 2]);
+    }
+    std::vector<Box> boxes(src.triangle_count);
+    for (uint32_t t = 0; t < src.triangle_count; ++t)
+      for (int k = 0; k < 3; ++k) {
+        const F3 p = g.positions[g.triangles[3 * t + k]];
+        const float a[3] = {p.x, p.y, p.z};
+        boxes[t].Grow(a);
+      }
+    g.bvh.Build(boxes);
+  }
+  s->instances.resize(d->instance_count);
+  std::vector<Box> instance_boxes(d->instance_count);
+  for (uint32_t ii = 0; ii < d->instance_count; ++ii) {
+    const lotus_instance& src = d->instances[ii];
+    Instance& inst = s->instances[ii];
+    std::memcpy(inst.m, src.world_from_object, sizeof(inst.m));
+    inst.geometry = src.geometry;
+    inst.material = src.material;
+    if (src.geometry >= d->geometry_count || src.material >= d->material_count) {
+      SetError(error, error_size, "an instance names a missing geometry or material");
+      return nullptr;
+    }
+    if (!InvertAffine(inst.m, inst.inv)) {
+      SetError(error, error_size, "an instance transform is singular");
+      return nullptr;
+    }
+    const Geometry& g = s->geometries[inst.geometry];
+    Box world;
+    if (!g.bvh.nodes.empty() && !g.triangles.empty()) {
+      const Box& b = g.bvh.nodes[0].box;
+      for (int corner = 0; corner < 8; ++corner) {
+        const F3 c = V((corner & 1) ? b.hi[0] : b.lo[0], (corner & 2) ? b.hi[1] : b.lo[1],
+            (corner & 4) ? b.hi[2] : b.lo[2]);
+        const F3 w = TransformPoint(inst.m, c);
+        const float a[3] = {w.x, w.y, w.z};
+        world.Grow(a);
+      }
+      // Widen by a relative margin so that float rounding of the corner
+      // transform cannot cull a hit.
+      for (int a = 0; a < 3; ++a) {
+        const float pad = 1e-6f * std::max(std::fabs(world.lo[a]), std::fabs(world.hi[a])) + 1e-7f;
+        world.lo[a] -= pad;
+        world.hi[a] += pad;
+      }
+    }
+    inst.world = world;
+    instance_boxes[ii] = world;
+  }
+  s->tlas.Build(instance_boxes);
+  s->environment_constant = V(d->environment_constant[0], d->environment_constant[1], d->environment_constant[2]);
+  if (d->environment && d->environment->texels && d->environment->width && d->environment->height) {
+    const lotus_environment& e = *d->environment;
+    s->env.width = e.width;
+    s->env.height = e.height;
+    s->env.texels.assign(e.texels, e.texels + 4 * size_t{e.width} * e.height);
+    s->env.scale = V(e.scale[0], e.scale[1], e.scale[2]);
+    for (int r = 0; r < 3; ++r)
+      s->env.rows[r] = V(e.environment_from_world[3 * r], e.environment_from_world[3 * r + 1],
+          e.environment_from_world[3 * r + 2]);
+    BuildEnvironmentDistribution(s->env);
+  }
+  BuildLightTable(*s);
+  return s.release();
+}
+
+void oracle_scene_destroy(oracle_scene* scene) { delete scene; }
+
+int32_t oracle_sample(const oracle_scene* s, const lotus_frame_desc* d, uint32_t sample_index,
+    float* rgba, uint64_t* rays, int32_t threads) {
+  FrameConstants f;
+  uint32_t rect[4];
+  if (!s || !d || !rgba || !MakeFrame(*d, f, rect)) return LOTUS_FAIL;
+  const int64_t pixels = int64_t{rect[2]} * rect[3];
+  std::atomic<uint64_t> camera{0}, extension{0}, shadow{0};
+#pragma omp parallel num_threads(ThreadCount(threads))
+  {
+    RayCounts local;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < pixels; ++i) {
+      const uint32_t px = rect[0] + uint32_t(i % rect[2]);
+      const uint32_t py = rect[1] + uint32_t(i / rect[2]);
+      F3 radiance;
+      float* out = rgba + 4 * (size_t{py} * d->target.width + px);
+      if (PathSample(*s, f, px, py, sample_index, radiance, local)) {
+        out[0] = radiance.x; out[1] = radiance.y; out[2] = radiance.z; out[3] = 1.0f;
+      } else {
+        out[0] = out[1] = out[2] = out[3] = 0.0f;
+      }
+    }
+    camera += local.camera;
+    extension += local.extension;
+    shadow += local.shadow;
+  }
+  if (rays) {
+    rays[0] = camera;
+    rays[1] = extension;
+    rays[2] = shadow;
+  }
+  return LOTUS_PASS;
+}
+
+int32_t oracle_accumulate(const oracle_scene* s, const lotus_frame_desc* d, uint32_t first_sample,
+    uint32_t count, double* sums, uint64_t* rays, int32_t threads) {
+  FrameConstants f;
+  uint32_t rect[4];
+  if (!s || !d || !sums || !MakeFrame(*d, f, rect)) return LOTUS_FAIL;
+  const int64_t pixels = int64_t{rect[2]} * rect[3];
+  std::atomic<uint64_t> camera{0}, extension{0}, shadow{0};
+#pragma omp parallel num_threads(ThreadCount(threads))
+  {
+    RayCounts local;
+#pragma omp for schedule(dynamic, 16)
+    for (int64_t i = 0; i < pixels; ++i) {
+      const uint32_t px = rect[0] + uint32_t(i % rect[2]);
+      const uint32_t py = rect[1] + uint32_t(i / rect[2]);
+      double* out = sums + 4 * (size_t{py} * d->target.width + px);
+      for (uint32_t k = 0; k < count; ++k) {
+        F3 radiance;
+        if (PathSample(*s, f, px, py, first_sample + k, radiance, local)) {
+          out[0] += radiance.x;
+          out[1] += radiance.y;
+          out[2] += radiance.z;
+          out[3] += 1.0;
+        }
+      }
+    }
+    camera += local.camera;
+    extension += local.extension;
+    shadow += local.shadow;
+  }
+  if (rays) {
+    rays[0] = camera;
+    rays[1] = extension;
+    rays[2] = shadow;
+  }
+  return LOTUS_PASS;
+}
+
+int64_t oracle_light_table(const oracle_scene* s, uint32_t* records, uint64_t record_capacity,
+    uint32_t* offsets, uint64_t offset_capacity) {
+  if (!s) return -1;
+  const uint64_t n = s->lights.size();
+  if (records)
+    for (uint64_t i = 0; i < n && i < record_capacity; ++i) {
+      records[4 * i] = AsUint(s->lights[i].pdf);
+      records[4 * i + 1] = AsUint(s->lights[i].threshold);
+      records[4 * i + 2] = s->lights[i].alias;
+      records[4 * i + 3] = s->lights[i].instance;
+    }
+  if (offsets)
+    for (uint64_t i = 0; i < s->light_offsets.size() && i < offset_capacity; ++i)
+      offsets[i] = s->light_offsets[i];
+  return static_cast<int64_t>(n);
+}
+
+int32_t oracle_traversal_stats(const oracle_scene* s, const lotus_frame_desc* d, uint32_t max_rays,
+    double* nodes_per_ray, double* triangles_per_ray) {
+  FrameConstants f;
+  uint32_t rect[4];
+  if (!s || !d || !MakeFrame(*d, f, rect)) return LOTUS_FAIL;
+  const uint64_t pixels = uint64_t{rect[2]} * rect[3];
+  const uint64_t n = std::min<uint64_t>(pixels, max_rays ? max_rays : pixels);
+  Counters c;
+  for (uint64_t k = 0; k < n; ++k) {
+    const uint64_t i = n == pixels ? k : (k * pixels) / n;
+    const uint32_t px = rect[0] + uint32_t(i % rect[2]);
+    const uint32_t py = rect[1] + uint32_t(i / rect[2]);
+    PathState p = StartPath(f, px, py, 0);
+    Hit hit;
+    Trace(*s, p.ray, p.rng, hit, &c);
+  }
+  if (nodes_per_ray) *nodes_per_ray = n ? double(c.nodes) / n : 0.0;
+  if (triangles_per_ray) *triangles_per_ray = n ? double(c.triangles) / n : 0.0;
+  return LOTUS_PASS;
+}
+
+}  // extern "C"
