@@ -1,0 +1,50 @@
+// SPDX-License-Identifier: Apache-2.0
+// On-device LBVH builder (see bvh_build.cu).
+#pragma once
+
+#include "scene.cuh"
+
+namespace lotus {
+
+// Scratch for building one BVH at a time, grown to the largest primitive
+// count seen. A BVH over n > 1 primitives has n - 1 nodes; over one, one.
+class BvhBuilder {
+ public:
+  ~BvhBuilder() { release(); }
+  // One BLAS: nodes at nodes[node_base ...], leaf-ordered triangles at
+  // tri_pool[3 * tri_base ...]. Positions and triangles are device arrays.
+  cudaError_t build_triangles(const float* positions, const uint32_t* triangles, uint32_t n,
+      BvhNode* nodes, uint32_t node_base, float4* tri_pool, uint32_t tri_base,
+      cudaStream_t stream);
+  // The TLAS over the instances' world boxes; leaves hold instance indices.
+  cudaError_t build_instances(const InstanceShading* shade, const InstanceTraversal* trav,
+      const BvhNode* blas, uint32_t n, BvhNode* nodes, cudaStream_t stream);
+  void release();
+
+  static uint32_t node_count(uint32_t n) { return n > 1 ? n - 1 : n; }
+
+ private:
+  cudaError_t reserve(uint32_t n, cudaStream_t stream);
+  cudaError_t build_common(uint32_t n, BvhNode* nodes, uint32_t node_base, uint32_t leaf_base,
+      bool leaves_are_values, cudaStream_t stream, const uint32_t** sorted);
+
+  uint32_t capacity_ = 0;
+  size_t temp_bytes_ = 0;
+  uint64_t* keys_ = nullptr;
+  uint64_t* keys_alt_ = nullptr;
+  uint32_t* values_ = nullptr;
+  uint32_t* values_alt_ = nullptr;
+  float4* plo_ = nullptr;
+  float4* phi_ = nullptr;
+  float4* nlo_ = nullptr;
+  float4* nhi_ = nullptr;
+  uint32_t* left_ = nullptr;
+  uint32_t* right_ = nullptr;
+  uint32_t* parent_internal_ = nullptr;
+  uint32_t* parent_leaf_ = nullptr;
+  uint32_t* flags_ = nullptr;
+  uint32_t* bounds_ = nullptr;
+  void* temp_ = nullptr;
+};
+
+}  // namespace lotus

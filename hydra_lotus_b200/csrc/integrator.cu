@@ -1,0 +1,485 @@
+// SPDX-License-Identifier: Apache-2.0
+// The reference path tracer as one megakernel, and the wavefront path
+// tracer as camera, shade, shadow and extend kernels over compacted queues
+// (backend/vulkan/shaders/path_trace.slang, wavefront/wavefront.slang and
+// common/transport.slang in hydra-lotus).
+//
+// Both integrators run the same scattering code and draw each path's random
+// numbers in the same order, so a pixel and sample index select the same
+// path in either. The wavefront shade kernel defers next event estimation's
+// shadow ray to the shadow kernel, which adds the light to the path's
+// radiance before the next extension reads it, so the radiance sums run in
+// the reference's order.
+#include "integrator.cuh"
+
+namespace lotus {
+
+namespace {
+
+constexpr int kBlock = 128;
+
+// Pixels in warp tiles of 8 x 4 for coherent camera rays.
+__device__ __forceinline__ bool tile_pixel(uint32_t index, const uint32_t* rect, uint32_t& px,
+    uint32_t& py) {
+  const uint32_t tiles_x = (rect[2] + 7) / 8;
+  const uint32_t tile = index >> 5, lane = index & 31u;
+  const uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
+  const uint32_t x = tx * 8 + (lane & 7u), y = ty * 4 + (lane >> 3);
+  px = rect[0] + x;
+  py = rect[1] + y;
+  return x < rect[2] && y < rect[3];
+}
+
+__host__ __forceinline__ uint32_t tile_threads(const uint32_t* rect) {
+  return ((rect[2] + 7) / 8) * ((rect[3] + 3) / 4) * 32;
+}
+
+// Appends `pred` lanes of the (converged) warp to a queue: one atomic per
+// warp, slots in lane order.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
+  const unsigned mask = __ballot_sync(0xFFFFFFFFu, pred);
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t base = 0;
+  if (mask) {
+    const int leader = __ffs(mask) - 1;
+    if ((int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  }
+  return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void warp_add64(unsigned long long* counter, uint32_t value) {
+  unsigned long long v = value;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+  if ((threadIdx.x & 31u) == 0 && v) atomicAdd(counter, v);
+}
+
+// Next event estimation's pending shadow ray.
+struct ShadowRequest {
+  bool pending;
+  F3 origin;
+  F3 direction;
+  float tmax;
+  F3 fl;        // f * light radiance
+  float weight; // MIS weight (1 for a delta light)
+  float pdf;
+  F3 throughput;
+};
+
+// ScatterPath (transport.slang:164-230) without analytic lights or ReSTIR:
+// adds the hit's emission (weighed against light sampling), applies
+// Russian roulette, prepares next event estimation's shadow ray and samples
+// the BSDF. Returns whether the path continues along (new_o, new_d).
+__device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
+    uint32_t instance, uint32_t tri, float b1, float b2, F3 ray_o, F3 ray_d, uint32_t depth,
+    F3& T, F3& R, float& last_pdf, uint32_t& flags, uint32_t& rng, F3& new_o, F3& new_d,
+    ShadowRequest& req) {
+  req.pending = false;
+  uint32_t primitive;
+  const SurfaceHit sh = reconstruct_hit(S, instance, tri, b1, b2, ray_d, &primitive);
+  const bool weigh = f.sample_lights && (flags & kUnweightedLight) == 0;
+  F3 emission = sh.emission;
+  if (weigh && depth != 0 && max_component(emission) > 0.0f) {
+    // EmissionWeight (transport.slang:150-158).
+    const float area_pdf = emitter_pdf(S, instance, primitive, sh.area);
+    float w = 1.0f;
+    if (area_pdf > 0.0f) {
+      const F3 toward = sh.position - ray_o;
+      const float cosine = fabsf(dot(sh.normal, ray_d));
+      w = power_heuristic(last_pdf, area_pdf * dot(toward, toward) / cosine);
+    }
+    emission = emission * w;
+  }
+  R = R + T * emission;
+  if (depth >= f.max_bounces) return false;
+  if (depth >= kRouletteBounces) {
+    const float survival = fminf(max_component(T), kMaxSurvival);
+    if (next_random(rng) >= survival) return false;
+    T = T / survival;
+  }
+  const Frame basis = make_frame(sh.shading_normal);
+  const F3 wo = basis.to_local(-ray_d);
+  if (f.sample_lights && S.light_count != 0) {
+    // DirectLight and ShadowedLight up to the shadow ray
+    // (transport.slang:82-135).
+    const float u0 = next_random(rng);
+    const float u1 = next_random(rng);
+    const float u2 = next_random(rng);
+    const float u3 = next_random(rng);
+    const F3 origin = offset_ray_origin(sh.position, sh.normal);
+    const LightSample ls = sample_light(S, u0, u1, u2, u3, origin);
+    if (ls.pdf > 0.0f && max_component(ls.radiance) > 0.0f && dot(ls.direction, sh.normal) > 0.0f) {
+      const F3 wi = basis.to_local(ls.direction);
+      if (wi.z > 0.0f) {
+        const F3 fv = bsdf_evaluate(sh.bsdf, wo, wi);
+        if (max_component(fv) > 0.0f) {
+          req.pending = true;
+          req.origin = origin;
+          req.direction = ls.direction;
+          req.tmax = ls.distance;
+          req.fl = fv * ls.radiance;
+          req.weight = ls.delta ? 1.0f : power_heuristic(ls.pdf, bsdf_pdf(sh.bsdf, wo, wi));
+          req.pdf = ls.pdf;
+          req.throughput = T;
+        }
+      }
+    }
+  }
+  F3 u;
+  u.x = next_random(rng);
+  u.y = next_random(rng);
+  u.z = next_random(rng);
+  BsdfSample s;
+  if (!bsdf_sample(sh.bsdf, wo, u, s)) return false;
+  const F3 wi = normalize(basis.to_world(s.wi));
+  const float side = dot(wi, sh.normal);
+  if (s.transmitted ? side >= 0.0f : side <= 0.0f) return false;
+  T = T * s.weight;
+  last_pdf = s.pdf;
+  if (s.delta || s.transmitted)
+    flags |= kUnweightedLight;
+  else
+    flags &= ~kUnweightedLight;
+  new_o = offset_ray_origin(sh.position, s.transmitted ? -sh.normal : sh.normal);
+  new_d = wi;
+  return true;
+}
+
+// The light a pending shadow ray carries once its transmittance is known.
+__device__ __forceinline__ F3 shadow_contribution(F3 fl, float weight, float pdf,
+    float transmittance) {
+  const F3 c = fl * (transmittance * weight / pdf);
+  return is_finite(c) ? c : V(0.0f);
+}
+
+// MissPath (transport.slang:235-247) without analytic lights.
+__device__ __forceinline__ F3 miss_radiance(const SceneView& S, const FrameConst& f, F3 d,
+    uint32_t flags, float last_pdf) {
+  F3 env = V(S.env_constant[0], S.env_constant[1], S.env_constant[2]);
+  if (S.env_bound) {
+    const bool weigh = f.sample_lights && (flags & kUnweightedLight) == 0;
+    env = env + environment_radiance(S, d, weigh, last_pdf);
+  }
+  return env;
+}
+
+// The radiance pass's output (path_trace.slang:369-385) from the FP64
+// accumulation: a pixel no sample has hit keeps the clear colour unless the
+// environment image shows behind it.
+__device__ __forceinline__ float4 resolve_pixel(const SceneView& S, const FrameConst& f,
+    uint32_t px, uint32_t py, double4 sum) {
+  const double count = (double)(f.accumulated + f.add_sample);
+  const bool env_shows = f.environment_background != 0 && S.env_bound != 0;
+  if (sum.w == 0.0 && (!env_shows || count == 0.0))
+    return make_float4(f.background[0], f.background[1], f.background[2], f.background[3]);
+  double bg[4] = {f.background[0], f.background[1], f.background[2], f.background[3]};
+  if (env_shows && sum.w < count) {
+    F3 o, d;
+    float tmax;
+    camera_ray(f, (float(px) + 0.5f) * f.ndc[0] + f.ndc[2], (float(py) + 0.5f) * f.ndc[1] + f.ndc[3],
+        o, d, tmax);
+    const F3 e = environment_radiance(S, d, false, 0.0f);
+    bg[0] = e.x;
+    bg[1] = e.y;
+    bg[2] = e.z;
+    bg[3] = 1.0;
+  }
+  const double miss = count - sum.w;
+  return make_float4((float)((sum.x + miss * bg[0]) / count), (float)((sum.y + miss * bg[1]) / count),
+      (float)((sum.z + miss * bg[2]) / count), (float)((sum.w + miss * bg[3]) / count));
+}
+
+__device__ __forceinline__ double4 add4(double4 a, float4 s) {
+  return make_double4(a.x + (double)s.x, a.y + (double)s.y, a.z + (double)s.z, a.w + (double)s.w);
+}
+
+// ---------------------------------------------------------------------------
+// The reference integrator: one thread follows one camera path to its end
+// (path_trace.slang:279-287, 353-385), then adds it to the pixel's FP64
+// accumulation and writes the mean.
+__global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
+    const FrameConst* __restrict__ fcp, double4* __restrict__ accum, float4* __restrict__ color,
+    RayTotals* totals) {
+  const FrameConst& f = *fcp;
+  const uint32_t rect[4] = {f.rect[0], f.rect[1], f.rect[2], f.rect[3]};
+  uint32_t px, py;
+  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = tile_pixel(index, rect, px, py);
+  uint32_t n_camera = 0, n_extension = 0, n_shadow = 0;
+  if (valid) {
+    const uint32_t slot = py * f.width + px;
+    double4 sum = f.accumulated != 0 ? accum[slot] : make_double4(0.0, 0.0, 0.0, 0.0);
+    if (f.add_sample) {
+      F3 o, d;
+      float tmax;
+      uint32_t rng;
+      start_path(f, px, py, f.sample_index, o, d, tmax, rng);
+      ++n_camera;
+      Hit hit;
+      if (trace_closest(S, o, d, 0.0f, tmax, rng, hit)) {
+        F3 T = V(1.0f), R = V(0.0f);
+        float last_pdf = 0.0f;
+        uint32_t flags = 0;
+        for (uint32_t depth = 0;; ++depth) {
+          F3 no, nd;
+          ShadowRequest req;
+          const bool cont = scatter(S, f, hit.instance, hit.tri, hit.b1, hit.b2, o, d, depth, T, R,
+              last_pdf, flags, rng, no, nd, req);
+          if (req.pending) {
+            ++n_shadow;
+            const float tr = trace_shadow(S, req.origin, req.direction, 0.0f, req.tmax);
+            if (tr > 0.0f) R = R + req.throughput * shadow_contribution(req.fl, req.weight, req.pdf, tr);
+          }
+          if (!cont) break;
+          o = no;
+          d = nd;
+          ++n_extension;
+          if (!trace_closest(S, o, d, 0.0f, kFloatMax, rng, hit)) {
+            R = R + T * miss_radiance(S, f, d, flags, last_pdf);
+            break;
+          }
+        }
+        sum = add4(sum, make_float4(R.x, R.y, R.z, 1.0f));
+      }
+      accum[slot] = sum;
+    }
+    color[slot] = resolve_pixel(S, f, px, py, sum);
+  }
+  warp_add64(&totals->camera, n_camera);
+  warp_add64(&totals->extension, n_extension);
+  warp_add64(&totals->shadow, n_shadow);
+}
+
+// ---------------------------------------------------------------------------
+// The wavefront integrator.
+
+// Camera (wavefront.slang:206-225): starts each pixel's path and traces its
+// camera ray; a hit is queued for shading at bounce 0.
+__global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
+    const FrameConst* __restrict__ fcp, PathState P, Queues Q) {
+  const FrameConst& f = *fcp;
+  if (!f.add_sample) return;
+  const uint32_t rect[4] = {f.rect[0], f.rect[1], f.rect[2], f.rect[3]};
+  uint32_t px, py;
+  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = tile_pixel(index, rect, px, py);
+  bool found = false;
+  uint32_t slot = 0;
+  if (valid) {
+    slot = py * f.width + px;
+    F3 o, d;
+    float tmax;
+    uint32_t rng;
+    start_path(f, px, py, f.sample_index, o, d, tmax, rng);
+    Hit hit;
+    found = trace_closest(S, o, d, 0.0f, tmax, rng, hit);
+    if (found) {
+      P.direction[slot] = F4(d, tmax);
+      P.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng));
+      P.hit[slot] = make_uint4(hit.instance, hit.tri, __float_as_uint(hit.b1), __float_as_uint(hit.b2));
+    } else {
+      P.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+  }
+  const uint32_t at = warp_append(&Q.counts[1], found);
+  if (found) Q.hit[at] = slot;
+}
+
+// Shade (wavefront.slang:264-285) with next event estimation's shadow ray
+// deferred to the shadow queue.
+__global__ void __launch_bounds__(kBlock) k_wf_shade(SceneView S,
+    const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce) {
+  const uint32_t n = Q.counts[3 * bounce + 1];
+  if (blockIdx.x * blockDim.x >= n) return;
+  const FrameConst& f = *fcp;
+  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = index < n;
+  bool cont = false;
+  ShadowRequest req;
+  req.pending = false;
+  uint32_t slot = 0;
+  if (valid) {
+    slot = Q.hit[index];
+    const float4 dir = P.direction[slot];
+    const float4 rad = P.radiance[slot];
+    const uint4 h = P.hit[slot];
+    F3 T = V(1.0f);
+    float last_pdf = 0.0f;
+    uint32_t flags = 0;
+    F3 ro = V(0.0f);
+    if (bounce != 0) {
+      const float4 thr = P.throughput[slot];
+      T = V(thr);
+      last_pdf = thr.w;
+      flags = last_pdf < 0.0f ? kUnweightedLight : 0u;
+      if (f.sample_lights) ro = V(P.origin[slot]);
+    }
+    F3 R = V(rad);
+    uint32_t rng = __float_as_uint(rad.w);
+    F3 no, nd;
+    cont = scatter(S, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
+        T, R, last_pdf, flags, rng, no, nd, req);
+    if (cont) {
+      P.origin[slot] = F4(no, 0.0f);
+      P.direction[slot] = F4(nd, kFloatMax);
+      P.throughput[slot] = F4(T, (flags & kUnweightedLight) ? -1.0f : last_pdf);
+      P.radiance[slot] = F4(R, __uint_as_float(rng));
+    } else {
+      P.radiance[slot] = F4(R, 1.0f);
+    }
+  }
+  const uint32_t ray_at = warp_append(&Q.counts[3 * (bounce + 1)], cont);
+  if (cont) Q.ray[(bounce + 1) & 1][ray_at] = slot;
+  const uint32_t sh_at = warp_append(&Q.counts[3 * bounce + 2], req.pending);
+  if (req.pending) {
+    Q.shadow.ray_o[sh_at] = F4(req.origin, req.tmax);
+    Q.shadow.ray_d[sh_at] = F4(req.direction, req.weight);
+    Q.shadow.fl[sh_at] = F4(req.fl, req.pdf);
+    Q.shadow.thr[sh_at] = F4(req.throughput, __uint_as_float(slot));
+  }
+}
+
+// The shadow rays of bounce `bounce`: ShadowTransmittance and the rest of
+// ShadowedLight, added to the path's radiance.
+__global__ void __launch_bounds__(kBlock) k_wf_shadow(SceneView S, PathState P, Queues Q,
+    uint32_t bounce) {
+  const uint32_t n = Q.counts[3 * bounce + 2];
+  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (index >= n) return;
+  const float4 ro = Q.shadow.ray_o[index];
+  const float4 rd = Q.shadow.ray_d[index];
+  const float tr = trace_shadow(S, V(ro), V(rd), 0.0f, ro.w);
+  if (tr > 0.0f) {
+    const float4 fl = Q.shadow.fl[index];
+    const float4 thr = Q.shadow.thr[index];
+    const uint32_t slot = __float_as_uint(thr.w);
+    const F3 c = shadow_contribution(V(fl), rd.w, fl.w, tr);
+    float4 rad = P.radiance[slot];
+    const F3 R = V(rad) + V(thr) * c;
+    rad.x = R.x;
+    rad.y = R.y;
+    rad.z = R.z;
+    P.radiance[slot] = rad;
+  }
+}
+
+// Intersect (wavefront.slang:230-262): a hit is queued for shading; a miss
+// ends the path with the environment.
+__global__ void __launch_bounds__(kBlock) k_wf_extend(SceneView S,
+    const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce) {
+  const uint32_t n = Q.counts[3 * bounce];
+  if (blockIdx.x * blockDim.x >= n) return;
+  const FrameConst& f = *fcp;
+  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = index < n;
+  bool found = false;
+  uint32_t slot = 0;
+  if (valid) {
+    slot = Q.ray[bounce & 1][index];
+    const float4 o = P.origin[slot];
+    const float4 d = P.direction[slot];
+    float4 rad = P.radiance[slot];
+    uint32_t rng = __float_as_uint(rad.w);
+    Hit hit;
+    found = trace_closest(S, V(o), V(d), o.w, d.w, rng, hit);
+    if (found) {
+      P.hit[slot] = make_uint4(hit.instance, hit.tri, __float_as_uint(hit.b1), __float_as_uint(hit.b2));
+      if (rng != __float_as_uint(rad.w)) {
+        rad.w = __uint_as_float(rng);
+        P.radiance[slot] = rad;
+      }
+    } else {
+      const float4 thr = P.throughput[slot];
+      const uint32_t flags = thr.w < 0.0f ? kUnweightedLight : 0u;
+      const F3 R = V(rad) + V(thr) * miss_radiance(S, f, V(d), flags, thr.w);
+      P.radiance[slot] = F4(R, 1.0f);
+    }
+  }
+  const uint32_t at = warp_append(&Q.counts[3 * bounce + 1], found);
+  if (found) Q.hit[at] = slot;
+}
+
+// Resolve (path_trace.slang:353-385): adds each ended path's sample to its
+// pixel and writes the mean; pixels outside the data window keep the clear
+// colour.
+__global__ void __launch_bounds__(kBlock) k_wf_resolve(SceneView S,
+    const FrameConst* __restrict__ fcp, PathState P, double4* __restrict__ accum,
+    float4* __restrict__ color) {
+  const FrameConst& f = *fcp;
+  const uint32_t rect[4] = {f.rect[0], f.rect[1], f.rect[2], f.rect[3]};
+  uint32_t px, py;
+  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!tile_pixel(index, rect, px, py)) return;
+  const uint32_t slot = py * f.width + px;
+  double4 sum = f.accumulated != 0 ? accum[slot] : make_double4(0.0, 0.0, 0.0, 0.0);
+  if (f.add_sample) {
+    sum = add4(sum, P.radiance[slot]);
+    accum[slot] = sum;
+  }
+  color[slot] = resolve_pixel(S, f, px, py, sum);
+}
+
+// Ends a sample: totals the queues' rays and advances the sample index.
+__global__ void k_wf_finish(FrameConst* fc, const uint32_t* __restrict__ counts,
+    uint32_t max_bounces, RayTotals* totals) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (!fc->add_sample) return;
+  unsigned long long ext = 0, sh = 0;
+  for (uint32_t b = 0; b <= max_bounces; ++b) {
+    if (b != 0) ext += counts[3 * b];
+    sh += counts[3 * b + 2];
+  }
+  totals->camera += (unsigned long long)fc->rect[2] * fc->rect[3];
+  totals->extension += ext;
+  totals->shadow += sh;
+}
+
+__global__ void k_advance(FrameConst* fc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && fc->add_sample) {
+    fc->sample_index += 1;
+    fc->accumulated += 1;
+  }
+}
+
+__global__ void k_fill(float4* color, uint32_t n, float4 v) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) color[i] = v;
+}
+
+}  // namespace
+
+void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream) {
+  const uint32_t threads = tile_threads(rect);
+  if (threads == 0) return;
+  k_reference_pt<<<(threads + kBlock - 1) / kBlock, kBlock, 0, stream>>>(S, fc, accum, color, totals);
+}
+
+void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
+    uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream) {
+  (void)width;
+  (void)height;
+  const uint32_t threads = tile_threads(rect);
+  if (threads == 0) return;
+  cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * 3 * (size_t)(max_bounces + 2), stream);
+  const uint32_t grid_pixels = (threads + kBlock - 1) / kBlock;
+  const uint32_t grid_queue = (Q.capacity + kBlock - 1) / kBlock;
+  k_wf_camera<<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q);
+  for (uint32_t b = 0; b <= max_bounces; ++b) {
+    if (b != 0) k_wf_extend<<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b);
+    k_wf_shade<<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b);
+    k_wf_shadow<<<grid_queue, kBlock, 0, stream>>>(S, P, Q, b);
+  }
+  k_wf_resolve<<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, accum, color);
+  k_wf_finish<<<1, 32, 0, stream>>>(const_cast<FrameConst*>(fc), Q.counts, max_bounces, totals);
+}
+
+void launch_advance(FrameConst* fc, cudaStream_t stream) { k_advance<<<1, 32, 0, stream>>>(fc); }
+
+void launch_clear_color(float4* color, uint32_t pixels, float4 value, cudaStream_t stream) {
+  if (pixels) k_fill<<<(pixels + 255) / 256, 256, 0, stream>>>(color, pixels, value);
+}
+
+}  // namespace lotus

@@ -1,0 +1,60 @@
+// SPDX-License-Identifier: Apache-2.0
+// Path state, queues and kernel entry points of the two integrators.
+#pragma once
+
+#include "transport.cuh"
+
+namespace lotus {
+
+// The wavefront integrator's path state, one slot per target pixel, in
+// 16-byte sections (backend/vulkan/shaders/common/path_state.slang in
+// hydra-lotus): a kernel loads only the sections it uses, as coalesced
+// 16-byte loads.
+struct PathState {
+  float4* origin;      // ray origin, tmin
+  float4* direction;   // ray direction, tmax
+  float4* throughput;  // throughput, last pdf (-1: the light found is unweighted)
+  float4* radiance;    // radiance, random state; once ended: the sample (rgb, hit)
+  uint4* hit;          // instance, leaf-ordered triangle, barycentrics
+};
+
+// Shadow queue entries: the part of ShadowedLight (transport.slang:82-115)
+// left after the shadow ray, split into four 16-byte sections.
+struct ShadowQueue {
+  float4* ray_o;     // origin, tmax
+  float4* ray_d;     // direction, MIS weight
+  float4* fl;        // f * light radiance, light pdf
+  float4* thr;       // path throughput, slot (bits)
+};
+
+// Per-bounce queue counters: [3 * b] rays entering bounce b's extension
+// (b = 0: camera rays), [3 * b + 1] hits shaded at bounce b, [3 * b + 2]
+// shadow rays from bounce b.
+struct Queues {
+  uint32_t* ray[2];
+  uint32_t* hit;
+  ShadowQueue shadow;
+  uint32_t* counts;
+  uint32_t capacity;
+};
+
+// Ray totals over a RenderScene call.
+struct RayTotals {
+  unsigned long long camera;
+  unsigned long long extension;
+  unsigned long long shadow;
+  unsigned long long error;  // traversal or bookkeeping errors
+};
+
+void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream);
+
+void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
+    uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream);
+
+void launch_advance(FrameConst* fc, cudaStream_t stream);
+
+void launch_clear_color(float4* color, uint32_t pixels, float4 value, cudaStream_t stream);
+
+}  // namespace lotus

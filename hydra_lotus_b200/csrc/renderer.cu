@@ -1,0 +1,1053 @@
+// SPDX-License-Identifier: Apache-2.0
+// The C ABI of include/lotus_cuda.h: the renderer that stands in for the
+// reference's VulkanOffscreenRenderer (backend/vulkan/vulkan_backend.cpp:721
+// in hydra-lotus) and its GpuScene (backend/vulkan/gpu_scene.cpp:1606).
+//
+// One renderer owns one CUDA stream and every device allocation. Calls are
+// synchronous: they return after the GPU work and any readback completed.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/lotus_cuda.h"
+#include "bvh_build.cuh"
+#include "integrator.cuh"
+
+namespace lotus {
+namespace {
+
+template <typename T>
+struct DeviceArray {
+  T* ptr = nullptr;
+  size_t count = 0;
+  cudaError_t resize(size_t n) {
+    if (n == count && ptr) return cudaSuccess;
+    release();
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&ptr, n * sizeof(T));
+    if (e == cudaSuccess) count = n;
+    return e;
+  }
+  cudaError_t upload(const T* host, size_t n, cudaStream_t s) {
+    cudaError_t e = resize(n);
+    if (e != cudaSuccess || n == 0) return e;
+    return cudaMemcpyAsync(ptr, host, n * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+  size_t bytes() const { return count * sizeof(T); }
+};
+
+void copy_detail(char* dst, size_t size, const std::string& s) {
+  if (dst && size) std::snprintf(dst, size, "%s", s.c_str());
+}
+
+// Object-from-world rows by Gauss-Jordan elimination in double of the
+// affine part, rounded to float.
+bool invert_affine(const float* m, float4 rows[3]) {
+  double a[3][4];
+  for (int r = 0; r < 3; ++r) {
+    for (int c = 0; c < 3; ++c) a[r][c] = m[c * 4 + r];
+    a[r][3] = m[12 + r];
+  }
+  double aug[3][6];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 6; ++c) aug[r][c] = c < 3 ? a[r][c] : (r == c - 3 ? 1.0 : 0.0);
+  for (int c = 0; c < 3; ++c) {
+    int p = c;
+    for (int r = c + 1; r < 3; ++r)
+      if (std::fabs(aug[r][c]) > std::fabs(aug[p][c])) p = r;
+    if (aug[p][c] == 0.0) return false;
+    for (int k = 0; k < 6; ++k) std::swap(aug[c][k], aug[p][k]);
+    const double s = aug[c][c];
+    for (int k = 0; k < 6; ++k) aug[c][k] /= s;
+    for (int r = 0; r < 3; ++r) {
+      if (r == c) continue;
+      const double f = aug[r][c];
+      for (int k = 0; k < 6; ++k) aug[r][k] -= f * aug[c][k];
+    }
+  }
+  float out[3][4];
+  for (int r = 0; r < 3; ++r) {
+    double t = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      out[r][c] = (float)aug[r][3 + c];
+      t -= aug[r][3 + c] * a[c][3];
+    }
+    out[r][3] = (float)t;
+    if (!std::isfinite(out[r][0]) || !std::isfinite(out[r][1]) || !std::isfinite(out[r][2]) ||
+        !std::isfinite(out[r][3]))
+      return false;
+    rows[r] = make_float4(out[r][0], out[r][1], out[r][2], out[r][3]);
+  }
+  return true;
+}
+
+// Invert (vulkan_backend.cpp:436-470): 4x4 Gauss-Jordan in double.
+bool invert4(const float* matrix, float* inverse) {
+  double rows[4][8] = {};
+  for (int row = 0; row < 4; ++row) {
+    for (int column = 0; column < 4; ++column) {
+      const float value = matrix[column * 4 + row];
+      if (!std::isfinite(value)) return false;
+      rows[row][column] = value;
+    }
+    rows[row][row + 4] = 1.0;
+  }
+  for (int column = 0; column < 4; ++column) {
+    int pivot = column;
+    for (int row = column + 1; row < 4; ++row)
+      if (std::abs(rows[row][column]) > std::abs(rows[pivot][column])) pivot = row;
+    if (rows[pivot][column] == 0.0) return false;
+    for (int index = 0; index < 8; ++index) std::swap(rows[column][index], rows[pivot][index]);
+    const double scale = rows[column][column];
+    for (double& value : rows[column]) value /= scale;
+    for (int row = 0; row < 4; ++row) {
+      if (row == column) continue;
+      const double factor = rows[row][column];
+      for (int index = 0; index < 8; ++index) rows[row][index] -= factor * rows[column][index];
+    }
+  }
+  for (int row = 0; row < 4; ++row)
+    for (int column = 0; column < 4; ++column) {
+      const float value = (float)rows[row][column + 4];
+      if (!std::isfinite(value)) return false;
+      inverse[column * 4 + row] = value;
+    }
+  return true;
+}
+
+struct HostF3 {
+  float x, y, z;
+};
+
+// mul(world_from_object, float4(p, 1)).xyz in the kernels' order.
+HostF3 host_transform(const float* m, const float* p) {
+  return {m[0] * p[0] + m[4] * p[1] + m[8] * p[2] + m[12],
+          m[1] * p[0] + m[5] * p[1] + m[9] * p[2] + m[13],
+          m[2] * p[0] + m[6] * p[1] + m[10] * p[2] + m[14]};
+}
+
+float host_coverage(const lotus_material& m) {
+  if (m.opacity_threshold > 0.0f) return m.opacity >= m.opacity_threshold ? 1.0f : 0.0f;
+  return m.opacity;
+}
+
+// The environment image's sampling distribution (BuildEnvironmentDistribution,
+// gpu_scene.cpp:638-711): cells of at most 2048 x 1024, each the mean
+// scaled radiance of its texels times sin(theta) at the row's centre.
+struct EnvDistribution {
+  uint32_t columns = 0, rows = 0;
+  std::vector<float> floats;  // density, marginal (rows + 1), conditional (rows x (columns + 1))
+  double mean = 0.0;
+};
+
+EnvDistribution build_env_distribution(const lotus_environment& e) {
+  constexpr double kPiD = 3.14159265358979323846;
+  EnvDistribution d;
+  d.columns = std::min(e.width, 2048u);
+  d.rows = std::min(e.height, 1024u);
+  const size_t cells = (size_t)d.columns * d.rows;
+  std::vector<double> sums(cells, 0.0);
+  std::vector<uint32_t> counts(cells, 0);
+  for (uint32_t y = 0; y < e.height; ++y) {
+    const size_t row = (uint64_t)y * d.rows / e.height;
+    for (uint32_t x = 0; x < e.width; ++x) {
+      const size_t column = (uint64_t)x * d.columns / e.width;
+      const float* t = e.texels + 4 * ((size_t)y * e.width + x);
+      double radiance = 0.0;
+      for (int c = 0; c < 3; ++c) radiance += std::max((double)t[c], 0.0) * (double)e.scale[c];
+      sums[row * d.columns + column] += radiance / 3.0;
+      ++counts[row * d.columns + column];
+    }
+  }
+  std::vector<double> values(cells), row_sums(d.rows, 0.0);
+  double total = 0.0;
+  for (uint32_t row = 0; row < d.rows; ++row) {
+    const double sin_theta = std::sin(kPiD * (row + 0.5) / d.rows);
+    for (uint32_t column = 0; column < d.columns; ++column) {
+      const size_t cell = (size_t)row * d.columns + column;
+      values[cell] = sums[cell] / counts[cell] * sin_theta;
+      row_sums[row] += values[cell];
+    }
+    total += row_sums[row];
+  }
+  const double mean = total / (double)cells;
+  d.floats.assign(cells + d.rows + 1 + (size_t)d.rows * (d.columns + 1), 0.0f);
+  if (!(mean > 0.0) || !std::isfinite(mean)) return d;
+  d.mean = mean;
+  float* density = d.floats.data();
+  float* marginal = density + cells;
+  float* conditional = marginal + d.rows + 1;
+  for (size_t cell = 0; cell < cells; ++cell) density[cell] = (float)(values[cell] / mean);
+  double cumulative = 0.0;
+  for (uint32_t row = 0; row < d.rows; ++row) {
+    cumulative += row_sums[row];
+    marginal[row + 1] = (float)(cumulative / total);
+    float* cdf = conditional + (size_t)row * (d.columns + 1);
+    double along = 0.0;
+    for (uint32_t column = 0; column < d.columns; ++column) {
+      along += values[(size_t)row * d.columns + column];
+      cdf[column + 1] = row_sums[row] > 0.0 ? (float)(along / row_sums[row])
+                                            : (float)(column + 1) / d.columns;
+    }
+    cdf[d.columns] = 1.0f;
+  }
+  marginal[d.rows] = 1.0f;
+  return d;
+}
+
+// The light table (BuildLightTable, gpu_scene.cpp:515-610): every emissive
+// triangle weighted by its mean emission times its world area, then the
+// environment image weighted as a distant light over the scene's bounding
+// sphere, chosen by Vose's alias method.
+struct LightTable {
+  std::vector<LightRecord> records;
+  std::vector<uint32_t> offsets;  // per instance
+  std::vector<float4> verts;      // 3 per entry
+  std::vector<float4> radiance;   // 1 per entry
+  float env_selection = 0.0f;
+};
+
+double world_triangle_area(const lotus_geometry& g, uint32_t t, const float* m) {
+  double corners[3][3];
+  for (int k = 0; k < 3; ++k) {
+    const float* p = g.positions + 3 * (size_t)g.triangles[3 * (size_t)t + k];
+    for (int r = 0; r < 3; ++r)
+      corners[k][r] = (double)m[r] * p[0] + (double)m[4 + r] * p[1] + (double)m[8 + r] * p[2] + m[12 + r];
+  }
+  double a[3], b[3];
+  for (int r = 0; r < 3; ++r) {
+    a[r] = corners[1][r] - corners[0][r];
+    b[r] = corners[2][r] - corners[0][r];
+  }
+  const double x = a[1] * b[2] - a[2] * b[1], y = a[2] * b[0] - a[0] * b[2], z = a[0] * b[1] - a[1] * b[0];
+  const double area = 0.5 * std::sqrt(x * x + y * y + z * z);
+  return std::isfinite(area) ? area : 0.0;
+}
+
+double scene_radius(const lotus_scene_desc& s) {
+  constexpr double kInf = std::numeric_limits<double>::infinity();
+  std::vector<std::array<double, 6>> object(s.geometry_count);
+  std::vector<char> done(s.geometry_count, 0);
+  std::array<double, 6> world{kInf, kInf, kInf, -kInf, -kInf, -kInf};
+  for (uint32_t i = 0; i < s.instance_count; ++i) {
+    const lotus_instance& inst = s.instances[i];
+    auto& b = object[inst.geometry];
+    if (!done[inst.geometry]) {
+      done[inst.geometry] = 1;
+      b = {kInf, kInf, kInf, -kInf, -kInf, -kInf};
+      const lotus_geometry& g = s.geometries[inst.geometry];
+      for (uint32_t v = 0; v < g.vertex_count; ++v)
+        for (int a = 0; a < 3; ++a) {
+          b[a] = std::min(b[a], (double)g.positions[3 * (size_t)v + a]);
+          b[3 + a] = std::max(b[3 + a], (double)g.positions[3 * (size_t)v + a]);
+        }
+    }
+    if (!(b[0] <= b[3])) continue;
+    const float* m = inst.world_from_object;
+    for (int corner = 0; corner < 8; ++corner) {
+      const double p[3] = {b[(corner & 1) ? 3 : 0], b[(corner & 2) ? 4 : 1], b[(corner & 4) ? 5 : 2]};
+      for (int r = 0; r < 3; ++r) {
+        const double v = m[r] * p[0] + m[4 + r] * p[1] + m[8 + r] * p[2] + m[12 + r];
+        world[r] = std::min(world[r], v);
+        world[3 + r] = std::max(world[3 + r], v);
+      }
+    }
+  }
+  if (!(world[0] <= world[3])) return 0.0;
+  const double d[3] = {world[3] - world[0], world[4] - world[1], world[5] - world[2]};
+  const double radius = 0.5 * std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  return std::isfinite(radius) ? radius : 0.0;
+}
+
+LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
+  LightTable table;
+  table.offsets.assign(s.instance_count, kNoLights);
+  std::vector<double> weights;
+  for (uint32_t index = 0; index < s.instance_count; ++index) {
+    const lotus_instance& inst = s.instances[index];
+    const lotus_geometry& g = s.geometries[inst.geometry];
+    const lotus_material& mat = s.materials[inst.material];
+    // EmissionEstimate (gpu_scene.cpp:144-180) of a constant input.
+    double e = ((double)mat.emission[0] + (double)mat.emission[1] + (double)mat.emission[2]) / 3.0;
+    if (!(std::isfinite(e) && e > 0.0)) e = 0.0;
+    if (e <= 0.0 || g.triangle_count == 0) continue;
+    table.offsets[index] = (uint32_t)table.records.size();
+    const float coverage = host_coverage(mat);
+    for (uint32_t t = 0; t < g.triangle_count; ++t) {
+      weights.push_back(e * world_triangle_area(g, t, inst.world_from_object));
+      table.records.push_back({0.0f, 1.0f, 0u, index});
+      for (int k = 0; k < 3; ++k) {
+        const HostF3 w = host_transform(inst.world_from_object,
+            g.positions + 3 * (size_t)g.triangles[3 * (size_t)t + k]);
+        table.verts.push_back(make_float4(w.x, w.y, w.z, 0.0f));
+      }
+      table.radiance.push_back(make_float4(mat.emission[0] * coverage, mat.emission[1] * coverage,
+          mat.emission[2] * coverage, 0.0f));
+    }
+  }
+  double env_weight = 0.0;
+  if (env_mean > 0.0) {
+    constexpr double kPiD = 3.14159265358979323846;
+    const double r = scene_radius(s);
+    env_weight = kPiD * kPiD * r * r * env_mean;
+    if (!std::isfinite(env_weight)) env_weight = std::numeric_limits<double>::max();
+  }
+  if (env_weight > 0.0) {
+    weights.push_back(env_weight);
+    table.records.push_back({0.0f, 1.0f, 0u, kEnvironmentLight});
+    for (int k = 0; k < 3; ++k) table.verts.push_back(make_float4(0, 0, 0, 0));
+    table.radiance.push_back(make_float4(0, 0, 0, 0));
+  }
+  double total = 0.0;
+  for (double w : weights) total += w;
+  if (!(total > 0.0) || !std::isfinite(total)) {
+    table.offsets.assign(s.instance_count, kNoLights);
+    table.records.clear();
+    table.verts.clear();
+    table.radiance.clear();
+    return table;
+  }
+  const size_t count = table.records.size();
+  std::vector<double> scaled(count);
+  std::vector<uint32_t> small, large;
+  for (size_t i = 0; i < count; ++i) {
+    table.records[i].pdf = (float)(weights[i] / total);
+    scaled[i] = weights[i] / total * (double)count;
+    (scaled[i] < 1.0 ? small : large).push_back((uint32_t)i);
+  }
+  while (!small.empty() && !large.empty()) {
+    const uint32_t less = small.back();
+    small.pop_back();
+    const uint32_t more = large.back();
+    table.records[less].threshold = (float)scaled[less];
+    table.records[less].alias = more;
+    scaled[more] -= 1.0 - scaled[less];
+    if (scaled[more] < 1.0) {
+      large.pop_back();
+      small.push_back(more);
+    }
+  }
+  for (uint32_t i : small) { table.records[i].threshold = 1.0f; table.records[i].alias = i; }
+  for (uint32_t i : large) { table.records[i].threshold = 1.0f; table.records[i].alias = i; }
+  if (env_weight > 0.0) table.env_selection = table.records.back().pdf;
+  return table;
+}
+
+}  // namespace
+
+struct Renderer {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  std::string failure;
+  uint64_t completion = 0;
+
+  // Scene.
+  DeviceArray<BvhNode> blas, tlas;
+  DeviceArray<float4> tris;
+  DeviceArray<InstanceTraversal> inst_trav;
+  DeviceArray<InstanceShading> inst_shade;
+  DeviceArray<MaterialRecord> materials;
+  DeviceArray<float> normals;
+  DeviceArray<LightRecord> lights;
+  DeviceArray<float4> light_verts, light_radiance;
+  DeviceArray<float4> env_texels;
+  DeviceArray<float> env_floats;
+  std::vector<LightRecord> host_lights;
+  std::vector<uint32_t> host_light_offsets;
+  SceneView view{};
+  bool scene_ready = false;
+  uint64_t scene_generation = 0;
+  BvhBuilder builder;
+
+  // Targets.
+  uint32_t width = 0, height = 0;
+  DeviceArray<double4> accum;
+  DeviceArray<float4> color;
+  DeviceArray<float4> path_origin, path_direction, path_throughput, path_radiance;
+  DeviceArray<uint4> path_hit;
+  DeviceArray<uint32_t> queue_ray0, queue_ray1, queue_hit, counts;
+  DeviceArray<float4> sq_o, sq_d, sq_fl, sq_thr;
+  DeviceArray<FrameConst> frame_const;
+  DeviceArray<RayTotals> totals;
+
+  // Accumulation key (vulkan_backend.cpp:414-431).
+  struct Key {
+    float world_to_clip[16];
+    uint32_t width, height;
+    float display_window[4];
+    int32_t data_window[4];
+    uint32_t integrator, light_sampling, restir_proposal, restir_candidates, sample_index,
+        max_bounces;
+    uint64_t scene_generation;
+    bool operator==(const Key& o) const { return std::memcmp(this, &o, sizeof(Key)) == 0; }
+  };
+  Key key{};
+  bool key_valid = false;
+  uint32_t accumulated = 0;
+
+  // The wavefront sample as a CUDA graph.
+  cudaGraphExec_t graph = nullptr;
+  struct GraphKey {
+    uint64_t scene_generation;
+    uint32_t width, height, max_bounces;
+    uint32_t rect[4];
+    bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
+  } graph_key{};
+
+  ~Renderer() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_stop) cudaEventDestroy(ev_stop);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  bool ok(cudaError_t e, const char* what, std::string& detail) {
+    if (e == cudaSuccess) return true;
+    detail = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+  }
+
+  void release_scene() {
+    blas.release(); tlas.release(); tris.release(); inst_trav.release(); inst_shade.release();
+    materials.release(); normals.release(); lights.release(); light_verts.release();
+    light_radiance.release(); env_texels.release(); env_floats.release();
+    scene_ready = false;
+  }
+
+  uint64_t scene_bytes() const {
+    return blas.bytes() + tlas.bytes() + tris.bytes() + inst_trav.bytes() + inst_shade.bytes() +
+           materials.bytes() + normals.bytes() + lights.bytes() + light_verts.bytes() +
+           light_radiance.bytes() + env_texels.bytes() + env_floats.bytes();
+  }
+};
+
+}  // namespace lotus
+
+using lotus::Renderer;
+
+struct lotus_cuda_renderer {
+  Renderer r;
+};
+
+namespace {
+
+using namespace lotus;
+
+bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
+  if (s.material_count == 0 || !s.materials) {
+    detail = "the scene has no material table";
+    return false;
+  }
+  if ((s.geometry_count && !s.geometries) || (s.instance_count && !s.instances)) {
+    detail = "the scene's geometry or instance array is missing";
+    return false;
+  }
+  for (uint32_t g = 0; g < s.geometry_count; ++g) {
+    const lotus_geometry& geo = s.geometries[g];
+    if (geo.triangle_count && (!geo.triangles || !geo.positions)) {
+      detail = "geometry " + std::to_string(g) + " has triangles without data";
+      return false;
+    }
+    for (uint64_t i = 0; i < 3ull * geo.triangle_count; ++i)
+      if (geo.triangles[i] >= geo.vertex_count) {
+        detail = "geometry " + std::to_string(g) + " indexes past its vertices";
+        return false;
+      }
+    for (uint64_t i = 0; i < 3ull * geo.vertex_count; ++i)
+      if (!std::isfinite(geo.positions[i])) {
+        detail = "geometry " + std::to_string(g) + " has a non-finite position";
+        return false;
+      }
+  }
+  for (uint32_t i = 0; i < s.instance_count; ++i) {
+    const lotus_instance& inst = s.instances[i];
+    if (inst.geometry >= s.geometry_count || inst.material >= s.material_count) {
+      detail = "instance " + std::to_string(i) + " names a missing geometry or material";
+      return false;
+    }
+    const float* m = inst.world_from_object;
+    if (m[3] != 0.0f || m[7] != 0.0f || m[11] != 0.0f || m[15] != 1.0f) {
+      detail = "instance " + std::to_string(i) + " has a projective transform";
+      return false;
+    }
+  }
+  for (uint32_t i = 0; i < s.material_count; ++i) {
+    const lotus_material& m = s.materials[i];
+    const float* f = &m.base_color[0];
+    for (int k = 0; k < 18; ++k)
+      if (!std::isfinite(f[k])) {
+        detail = "material " + std::to_string(i) + " has a non-finite value";
+        return false;
+      }
+    if (!(m.ior >= 1.0f)) {
+      detail = "material " + std::to_string(i) + " has an ior below 1";
+      return false;
+    }
+  }
+  if (s.environment && s.environment->texels == nullptr &&
+      (s.environment->width || s.environment->height)) {
+    detail = "the environment image has no texels";
+    return false;
+  }
+  return true;
+}
+
+int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result& res) {
+  std::string detail;
+  if (!validate_scene(s, detail)) {
+    copy_detail(res.detail, sizeof(res.detail), detail);
+    return res.status = LOTUS_FAIL;
+  }
+  cudaStream_t st = R.stream;
+  auto fail = [&](const std::string& d) {
+    R.failure = d;
+    R.release_scene();
+    copy_detail(res.detail, sizeof(res.detail), d);
+    return res.status = LOTUS_FAIL;
+  };
+  cudaEventRecord(R.ev_start, st);
+  // Geometry pools.
+  std::vector<uint32_t> node_base(s.geometry_count), tri_base(s.geometry_count),
+      normal_base(s.geometry_count, kNoLights);
+  uint64_t nodes = 0, tri_total = 0, normal_total = 0, vert_total = 0;
+  uint32_t max_tris = 0;
+  for (uint32_t g = 0; g < s.geometry_count; ++g) {
+    const lotus_geometry& geo = s.geometries[g];
+    node_base[g] = (uint32_t)nodes;
+    tri_base[g] = (uint32_t)tri_total;
+    nodes += BvhBuilder::node_count(geo.triangle_count);
+    tri_total += geo.triangle_count;
+    vert_total += geo.vertex_count;
+    max_tris = std::max(max_tris, geo.triangle_count);
+    if (geo.normals && geo.triangle_count) {
+      normal_base[g] = (uint32_t)normal_total;
+      normal_total += geo.triangle_count;
+    }
+  }
+  if (nodes >= 0x7FFFFFF0ull || tri_total >= 0x7FFFFFF0ull)
+    return fail("the scene exceeds 2^31 triangles");
+  if (!R.ok(R.blas.resize(std::max<uint64_t>(nodes, 1)), "BLAS pool", detail) ||
+      !R.ok(R.tris.resize(3 * std::max<uint64_t>(tri_total, 1)), "triangle pool", detail))
+    return fail(detail);
+  // Staging: every geometry's positions and triangles in one upload.
+  std::vector<float> h_pos(3 * vert_total);
+  std::vector<uint32_t> h_tri(3 * tri_total);
+  std::vector<uint64_t> vbase(s.geometry_count);
+  {
+    uint64_t v = 0, t = 0;
+    for (uint32_t g = 0; g < s.geometry_count; ++g) {
+      const lotus_geometry& geo = s.geometries[g];
+      vbase[g] = v;
+      if (geo.vertex_count) std::memcpy(&h_pos[3 * v], geo.positions, 12ull * geo.vertex_count);
+      if (geo.triangle_count) std::memcpy(&h_tri[3 * t], geo.triangles, 12ull * geo.triangle_count);
+      v += geo.vertex_count;
+      t += geo.triangle_count;
+    }
+  }
+  DeviceArray<float> d_pos;
+  DeviceArray<uint32_t> d_tri;
+  if (!R.ok(d_pos.upload(h_pos.data(), h_pos.size(), st), "positions", detail) ||
+      !R.ok(d_tri.upload(h_tri.data(), h_tri.size(), st), "triangles", detail))
+    return fail(detail);
+  for (uint32_t g = 0; g < s.geometry_count; ++g) {
+    const lotus_geometry& geo = s.geometries[g];
+    if (!geo.triangle_count) continue;
+    cudaError_t e = R.builder.build_triangles(d_pos.ptr + 3 * vbase[g], d_tri.ptr + 3 * (size_t)tri_base[g],
+        geo.triangle_count, R.blas.ptr, node_base[g], R.tris.ptr, tri_base[g], st);
+    if (!R.ok(e, "BLAS build", detail)) return fail(detail);
+  }
+  // Corner normals.
+  if (normal_total) {
+    std::vector<float> h_n(9 * normal_total);
+    for (uint32_t g = 0; g < s.geometry_count; ++g)
+      if (normal_base[g] != kNoLights)
+        std::memcpy(&h_n[9 * (size_t)normal_base[g]], s.geometries[g].normals,
+            36ull * s.geometries[g].triangle_count);
+    if (!R.ok(R.normals.upload(h_n.data(), h_n.size(), st), "normals", detail)) return fail(detail);
+  } else {
+    R.normals.release();
+  }
+  // Materials.
+  std::vector<MaterialRecord> h_mat(s.material_count);
+  for (uint32_t i = 0; i < s.material_count; ++i) {
+    const lotus_material& m = s.materials[i];
+    MaterialRecord& r = h_mat[i];
+    r.base_roughness = make_float4(m.base_color[0], m.base_color[1], m.base_color[2], m.roughness);
+    r.emission_metallic = make_float4(m.emission[0], m.emission[1], m.emission[2], m.metallic);
+    r.specular_ior = make_float4(m.specular_color[0], m.specular_color[1], m.specular_color[2], m.ior);
+    r.transmission = make_float4(m.transmission_color[0], m.transmission_color[1],
+        m.transmission_color[2], m.transmission);
+    uint32_t flags = m.flags;
+    float fbits;
+    std::memcpy(&fbits, &flags, 4);
+    r.coverage = make_float4(m.opacity, m.opacity_threshold, fbits, 0.0f);
+  }
+  if (!R.ok(R.materials.upload(h_mat.data(), h_mat.size(), st), "materials", detail)) return fail(detail);
+  // Environment.
+  EnvDistribution env;
+  bool env_bound = false;
+  if (s.environment && s.environment->texels && s.environment->width && s.environment->height) {
+    env = build_env_distribution(*s.environment);
+    env_bound = env.mean > 0.0;
+  }
+  if (env_bound) {
+    const size_t texels = (size_t)s.environment->width * s.environment->height;
+    if (!R.ok(R.env_texels.upload(reinterpret_cast<const float4*>(s.environment->texels), texels, st),
+            "environment texels", detail) ||
+        !R.ok(R.env_floats.upload(env.floats.data(), env.floats.size(), st), "environment distribution",
+            detail))
+      return fail(detail);
+  } else {
+    R.env_texels.release();
+    R.env_floats.release();
+  }
+  // Light table.
+  LightTable table = build_light_table(s, env_bound ? env.mean : 0.0);
+  if (!R.ok(R.lights.upload(table.records.data(), table.records.size(), st), "light table", detail) ||
+      !R.ok(R.light_verts.upload(table.verts.data(), table.verts.size(), st), "light corners", detail) ||
+      !R.ok(R.light_radiance.upload(table.radiance.data(), table.radiance.size(), st), "light radiance",
+          detail))
+    return fail(detail);
+  R.host_lights = table.records;
+  R.host_light_offsets = table.offsets;
+  // Instances.
+  std::vector<InstanceTraversal> h_trav(s.instance_count);
+  std::vector<InstanceShading> h_shade(s.instance_count);
+  for (uint32_t i = 0; i < s.instance_count; ++i) {
+    const lotus_instance& inst = s.instances[i];
+    const float* m = inst.world_from_object;
+    InstanceTraversal& t = h_trav[i];
+    InstanceShading& sh = h_shade[i];
+    if (!invert_affine(m, t.inv)) return fail("instance " + std::to_string(i) + " has a singular transform");
+    const lotus_geometry& geo = s.geometries[inst.geometry];
+    t.blas_root = geo.triangle_count ? node_base[inst.geometry] : (uint32_t)kEmptyChild;
+    t.flags = host_coverage(s.materials[inst.material]) >= 1.0f ? kInstanceOpaque : 0u;
+    t.material = inst.material;
+    t.light_offset = table.offsets[i];
+    for (int r = 0; r < 3; ++r) sh.m[r] = make_float4(m[r], m[4 + r], m[8 + r], m[12 + r]);
+    sh.material = inst.material;
+    sh.light_offset = table.offsets[i];
+    sh.normals = normal_base[inst.geometry];
+    // dot(c0, cross(c1, c2)) < 0 (scene.slang:1237-1240).
+    const float c0[3] = {m[0], m[1], m[2]}, c1[3] = {m[4], m[5], m[6]}, c2[3] = {m[8], m[9], m[10]};
+    const float x = c1[1] * c2[2] - c1[2] * c2[1], y = c1[2] * c2[0] - c1[0] * c2[2],
+                z = c1[0] * c2[1] - c1[1] * c2[0];
+    sh.mirror = (c0[0] * x + c0[1] * y + c0[2] * z) < 0.0f ? 1u : 0u;
+  }
+  if (!R.ok(R.inst_trav.upload(h_trav.data(), h_trav.size(), st), "instances", detail) ||
+      !R.ok(R.inst_shade.upload(h_shade.data(), h_shade.size(), st), "instances", detail) ||
+      !R.ok(R.tlas.resize(std::max<uint32_t>(BvhBuilder::node_count(s.instance_count), 1)), "TLAS", detail))
+    return fail(detail);
+  if (!R.ok(R.builder.build_instances(R.inst_shade.ptr, R.inst_trav.ptr, R.blas.ptr, s.instance_count,
+                R.tlas.ptr, st), "TLAS build", detail))
+    return fail(detail);
+  cudaEventRecord(R.ev_stop, st);
+  if (!R.ok(cudaStreamSynchronize(st), "scene update", detail)) return fail(detail);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
+  d_pos.release();
+  d_tri.release();
+
+  SceneView& v = R.view;
+  v = SceneView{};
+  v.tlas = R.tlas.ptr;
+  v.blas = R.blas.ptr;
+  v.tris = R.tris.ptr;
+  v.inst_trav = R.inst_trav.ptr;
+  v.inst_shade = R.inst_shade.ptr;
+  v.materials = R.materials.ptr;
+  v.normals = R.normals.ptr;
+  v.lights = R.lights.ptr;
+  v.light_verts = R.light_verts.ptr;
+  v.light_radiance = R.light_radiance.ptr;
+  v.env_texels = R.env_texels.ptr;
+  v.env_floats = R.env_floats.ptr;
+  v.instance_count = s.instance_count;
+  v.light_count = (uint32_t)table.records.size();
+  v.env_bound = env_bound ? 1u : 0u;
+  if (env_bound) {
+    v.env_width = s.environment->width;
+    v.env_height = s.environment->height;
+    v.env_columns = env.columns;
+    v.env_rows = env.rows;
+    for (int k = 0; k < 3; ++k) v.env_scale[k] = s.environment->scale[k];
+    for (int k = 0; k < 9; ++k) v.env_frame[k] = s.environment->environment_from_world[k];
+  }
+  v.env_selection = table.env_selection;
+  for (int k = 0; k < 3; ++k) v.env_constant[k] = s.environment_constant[k];
+  R.scene_ready = true;
+  ++R.scene_generation;
+  res.status = LOTUS_PASS;
+  res.triangle_count = (uint32_t)tri_total;
+  res.instance_count = s.instance_count;
+  res.light_count = (uint32_t)table.records.size();
+  res.bvh_node_count = (uint32_t)nodes;
+  res.tlas_node_count = BvhBuilder::node_count(s.instance_count);
+  res.build_gpu_ms = ms;
+  res.device_bytes = R.scene_bytes();
+  return LOTUS_PASS;
+}
+
+bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::string& detail) {
+  const size_t n = (size_t)w * h;
+  if (R.width != w || R.height != h) {
+    R.accum.release();
+    R.color.release();
+    R.path_origin.release(); R.path_direction.release(); R.path_throughput.release();
+    R.path_radiance.release(); R.path_hit.release();
+    R.queue_ray0.release(); R.queue_ray1.release(); R.queue_hit.release();
+    R.sq_o.release(); R.sq_d.release(); R.sq_fl.release(); R.sq_thr.release();
+    R.width = w;
+    R.height = h;
+    R.key_valid = false;
+  }
+  if (!R.ok(R.accum.resize(n), "accumulation", detail) || !R.ok(R.color.resize(n), "colour", detail) ||
+      !R.ok(R.counts.resize(3 * (LOTUS_MAX_BOUNCES + 2)), "queue counts", detail) ||
+      !R.ok(R.frame_const.resize(1), "frame constants", detail) ||
+      !R.ok(R.totals.resize(1), "ray totals", detail))
+    return false;
+  if (wavefront) {
+    if (!R.ok(R.path_origin.resize(n), "path state", detail) ||
+        !R.ok(R.path_direction.resize(n), "path state", detail) ||
+        !R.ok(R.path_throughput.resize(n), "path state", detail) ||
+        !R.ok(R.path_radiance.resize(n), "path state", detail) ||
+        !R.ok(R.path_hit.resize(n), "path state", detail) ||
+        !R.ok(R.queue_ray0.resize(n), "queues", detail) || !R.ok(R.queue_ray1.resize(n), "queues", detail) ||
+        !R.ok(R.queue_hit.resize(n), "queues", detail) || !R.ok(R.sq_o.resize(n), "shadow queue", detail) ||
+        !R.ok(R.sq_d.resize(n), "shadow queue", detail) || !R.ok(R.sq_fl.resize(n), "shadow queue", detail) ||
+        !R.ok(R.sq_thr.resize(n), "shadow queue", detail))
+      return false;
+  }
+  return true;
+}
+
+int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, float* color_out) {
+  std::string detail;
+  auto fail = [&](const std::string& msg) {
+    copy_detail(res.detail, sizeof(res.detail), msg);
+    return res.status = LOTUS_FAIL;
+  };
+  auto poison = [&](const std::string& msg) {
+    R.failure = msg;
+    return fail(msg);
+  };
+  const lotus_settings& st = d.settings;
+  const lotus_target& t = d.target;
+  if (!R.scene_ready) return fail("no scene has been uploaded");
+  if (d.frame_count == 0) return fail("frame_count must be at least 1");
+  if (t.width == 0 || t.height == 0) return fail("the offscreen target is empty");
+  if (t.width > 32768 || t.height > 32768) return fail("the offscreen target exceeds 32768 pixels a side");
+  for (int k = 0; k < 4; ++k)
+    if (!std::isfinite(t.clear_color[k])) return fail("invalid offscreen clear values");
+  if (st.integrator > LOTUS_INTEGRATOR_WAVEFRONT) return fail("unknown integrator");
+  if (st.light_sampling > LOTUS_LIGHT_SAMPLING_RESTIR_INITIAL) return fail("unknown light sampling");
+  if (st.light_sampling == LOTUS_LIGHT_SAMPLING_RESTIR_INITIAL)
+    return fail("RestirInitial light sampling runs through the temporal entry point");
+  if (st.max_bounces > LOTUS_MAX_BOUNCES)
+    return fail("max_bounces " + std::to_string(st.max_bounces) + " exceeds " +
+                std::to_string(LOTUS_MAX_BOUNCES));
+  // VulkanWorldToClip (vulkan_internal.hpp:326-336) and Invert.
+  float vulkan[16];
+  std::memcpy(vulkan, d.world_to_clip, sizeof(vulkan));
+  for (int c = 0; c < 4; ++c) {
+    const float y = d.world_to_clip[c * 4 + 1], z = d.world_to_clip[c * 4 + 2], w = d.world_to_clip[c * 4 + 3];
+    vulkan[c * 4 + 1] = -y;
+    vulkan[c * 4 + 2] = 0.5f * (z + w);
+  }
+  FrameConst fc{};
+  if (!invert4(vulkan, fc.clip_to_world)) return fail("ray-query camera is singular or non-finite");
+  const bool wavefront = st.integrator == LOTUS_INTEGRATOR_WAVEFRONT;
+  if (!ensure_targets(R, t.width, t.height, wavefront, detail)) return poison(detail);
+  // DisplayViewport and DataScissor (vulkan_backend.cpp:651-677).
+  float vx = 0.0f, vy = 0.0f, vw = (float)t.width, vh = (float)t.height;
+  if (t.display_window[2] > 0.0f && t.display_window[3] > 0.0f) {
+    vx = t.display_window[0]; vy = t.display_window[1]; vw = t.display_window[2]; vh = t.display_window[3];
+  }
+  fc.ndc[0] = 2.0f / vw;
+  fc.ndc[1] = 2.0f / vh;
+  fc.ndc[2] = -2.0f * vx / vw - 1.0f;
+  fc.ndc[3] = -2.0f * vy / vh - 1.0f;
+  uint32_t rect[4] = {0, 0, t.width, t.height};
+  if (t.data_window[2] > 0 && t.data_window[3] > 0) {
+    const int64_t x0 = std::max<int64_t>(t.data_window[0], 0), y0 = std::max<int64_t>(t.data_window[1], 0);
+    const int64_t x1 = std::min<int64_t>((int64_t)t.data_window[0] + t.data_window[2], t.width);
+    const int64_t y1 = std::min<int64_t>((int64_t)t.data_window[1] + t.data_window[3], t.height);
+    if (x1 <= x0 || y1 <= y0) {
+      rect[0] = rect[1] = rect[2] = rect[3] = 0;
+    } else {
+      rect[0] = (uint32_t)x0; rect[1] = (uint32_t)y0;
+      rect[2] = (uint32_t)(x1 - x0); rect[3] = (uint32_t)(y1 - y0);
+    }
+  }
+  for (int k = 0; k < 4; ++k) {
+    fc.rect[k] = rect[k];
+    fc.background[k] = t.clear_color[k];
+  }
+  fc.width = t.width;
+  fc.height = t.height;
+  fc.max_bounces = st.max_bounces;
+  fc.sample_lights = st.light_sampling != LOTUS_LIGHT_SAMPLING_BSDF ? 1u : 0u;
+  fc.environment_background = st.environment_background ? 1u : 0u;
+  // The accumulation key (vulkan_backend.cpp:1188-1205).
+  Renderer::Key key{};
+  std::memcpy(key.world_to_clip, vulkan, sizeof(vulkan));
+  key.width = t.width;
+  key.height = t.height;
+  std::memcpy(key.display_window, t.display_window, sizeof(key.display_window));
+  std::memcpy(key.data_window, t.data_window, sizeof(key.data_window));
+  key.integrator = st.integrator;
+  key.light_sampling = st.light_sampling;
+  key.restir_proposal = st.restir_proposal;
+  key.restir_candidates = st.restir_candidates;
+  key.sample_index = st.sample_index;
+  key.max_bounces = st.max_bounces;
+  key.scene_generation = R.scene_generation;
+  if (!R.key_valid || !(R.key == key)) {
+    R.key = key;
+    R.key_valid = true;
+    R.accumulated = 0;
+  }
+  const uint32_t room = st.max_samples == 0 ? d.frame_count
+                                            : st.max_samples - std::min(st.max_samples, R.accumulated);
+  const uint32_t to_add = std::min(d.frame_count, room);
+  const uint32_t submissions = std::max(to_add, 1u);
+  fc.sample_index = st.sample_index + R.accumulated;
+  fc.accumulated = R.accumulated;
+  fc.add_sample = to_add > 0 ? 1u : 0u;
+  cudaStream_t s = R.stream;
+  if (!R.ok(cudaMemcpyAsync(R.frame_const.ptr, &fc, sizeof(fc), cudaMemcpyHostToDevice, s), "frame constants", detail) ||
+      !R.ok(cudaMemsetAsync(R.totals.ptr, 0, sizeof(RayTotals), s), "ray totals", detail))
+    return poison(detail);
+  if (rect[2] < t.width || rect[3] < t.height || rect[2] == 0)
+    launch_clear_color(R.color.ptr, t.width * t.height,
+        make_float4(t.clear_color[0], t.clear_color[1], t.clear_color[2], t.clear_color[3]), s);
+  PathState P{R.path_origin.ptr, R.path_direction.ptr, R.path_throughput.ptr, R.path_radiance.ptr, R.path_hit.ptr};
+  Queues Q;
+  Q.ray[0] = R.queue_ray0.ptr;
+  Q.ray[1] = R.queue_ray1.ptr;
+  Q.hit = R.queue_hit.ptr;
+  Q.shadow = ShadowQueue{R.sq_o.ptr, R.sq_d.ptr, R.sq_fl.ptr, R.sq_thr.ptr};
+  Q.counts = R.counts.ptr;
+  Q.capacity = t.width * t.height;
+  cudaEventRecord(R.ev_start, s);
+  for (uint32_t k = 0; k < submissions; ++k) {
+    if (wavefront) {
+      Renderer::GraphKey gk{};
+      gk.scene_generation = R.scene_generation;
+      gk.width = t.width;
+      gk.height = t.height;
+      gk.max_bounces = st.max_bounces;
+      std::memcpy(gk.rect, rect, sizeof(rect));
+      if (!R.graph || !(R.graph_key == gk)) {
+        if (R.graph) {
+          cudaGraphExecDestroy(R.graph);
+          R.graph = nullptr;
+        }
+        cudaGraph_t g;
+        if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
+          return poison(detail);
+        launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
+            R.accum.ptr, R.color.ptr, R.totals.ptr, s);
+        launch_advance(R.frame_const.ptr, s);
+        if (!R.ok(cudaStreamEndCapture(s, &g), "graph capture", detail)) return poison(detail);
+        cudaError_t e = cudaGraphInstantiate(&R.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (!R.ok(e, "graph instantiate", detail)) return poison(detail);
+        R.graph_key = gk;
+      }
+      if (!R.ok(cudaGraphLaunch(R.graph, s), "graph launch", detail)) return poison(detail);
+    } else {
+      launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s);
+      launch_advance(R.frame_const.ptr, s);
+    }
+  }
+  cudaEventRecord(R.ev_stop, s);
+  RayTotals totals{};
+  std::vector<uint32_t> counts(3 * (size_t)(st.max_bounces + 2), 0);
+  cudaMemcpyAsync(&totals, R.totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s);
+  if (wavefront) cudaMemcpyAsync(counts.data(), R.counts.ptr, counts.size() * 4, cudaMemcpyDeviceToHost, s);
+  if (!R.ok(cudaStreamSynchronize(s), "render", detail)) return poison(detail);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
+  R.accumulated += to_add;
+  R.completion += submissions;
+  if (t.read_back && color_out) {
+    if (!R.ok(cudaMemcpyAsync(color_out, R.color.ptr, sizeof(float4) * (size_t)t.width * t.height,
+                  cudaMemcpyDeviceToHost, s), "colour readback", detail) ||
+        !R.ok(cudaStreamSynchronize(s), "colour readback", detail))
+      return poison(detail);
+  }
+  res.status = LOTUS_PASS;
+  res.frames_rendered = submissions;
+  res.samples_per_pixel = R.accumulated;
+  res.completion = R.completion;
+  res.camera_rays = totals.camera;
+  res.extension_rays = totals.extension;
+  res.shadow_rays = totals.shadow;
+  res.gpu_ms = ms;
+  res.wavefront_rounds = 0;
+  res.wavefront_path_count_size = 0;
+  if (wavefront && to_add > 0) {
+    uint32_t last = 0;
+    for (uint32_t b = 0; b <= st.max_bounces && b < LOTUS_MAX_REPORTED_BOUNCES; ++b) {
+      const uint32_t c = b == 0 ? rect[2] * rect[3] : counts[3 * b];
+      res.wavefront_path_counts[b] = c;
+      if (c) last = b + 1;
+    }
+    res.wavefront_path_count_size = last;
+    res.wavefront_rounds = st.max_bounces + 1;
+  }
+  return LOTUS_PASS;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t lotus_cuda_abi_version(void) { return LOTUS_CUDA_ABI_VERSION; }
+
+uint32_t lotus_cuda_struct_sizes(uint64_t* sizes, uint32_t capacity) {
+  const uint64_t s[] = {sizeof(lotus_geometry), sizeof(lotus_instance), sizeof(lotus_material),
+      sizeof(lotus_environment), sizeof(lotus_scene_desc), sizeof(lotus_scene_result),
+      sizeof(lotus_target), sizeof(lotus_settings), sizeof(lotus_frame_desc),
+      sizeof(lotus_frame_result), sizeof(lotus_cuda_options)};
+  const uint32_t n = sizeof(s) / sizeof(s[0]);
+  for (uint32_t i = 0; i < n && i < capacity; ++i) sizes[i] = s[i];
+  return n;
+}
+
+int32_t lotus_cuda_capability(int32_t device, char* detail, size_t detail_size) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    copy_detail(detail, detail_size, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    return LOTUS_SKIP;
+  }
+  if (device < 0 || device >= count) {
+    copy_detail(detail, detail_size, "no CUDA device " + std::to_string(device));
+    return LOTUS_SKIP;
+  }
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess || p.major != 10) {
+    copy_detail(detail, detail_size, "the device is not sm_100 (built for sm_100a only)");
+    return LOTUS_SKIP;
+  }
+  copy_detail(detail, detail_size, p.name);
+  return LOTUS_PASS;
+}
+
+int32_t lotus_cuda_create(const lotus_cuda_options* options, lotus_cuda_renderer** out, char* error,
+    size_t error_size) {
+  if (!out) return LOTUS_FAIL;
+  *out = nullptr;
+  const int device = options ? options->device : 0;
+  const int32_t cap = lotus_cuda_capability(device, error, error_size);
+  if (cap != LOTUS_PASS) return cap;
+  auto* h = new (std::nothrow) lotus_cuda_renderer();
+  if (!h) {
+    copy_detail(error, error_size, "out of host memory");
+    return LOTUS_FAIL;
+  }
+  Renderer& R = h->r;
+  R.device = device;
+  std::string detail;
+  if (!R.ok(cudaSetDevice(device), "cudaSetDevice", detail) ||
+      !R.ok(cudaStreamCreateWithFlags(&R.stream, cudaStreamNonBlocking), "stream", detail) ||
+      !R.ok(cudaEventCreate(&R.ev_start), "event", detail) || !R.ok(cudaEventCreate(&R.ev_stop), "event", detail)) {
+    copy_detail(error, error_size, detail);
+    delete h;
+    return LOTUS_FAIL;
+  }
+  *out = h;
+  return LOTUS_PASS;
+}
+
+void lotus_cuda_destroy(lotus_cuda_renderer* r) {
+  if (!r) return;
+  cudaSetDevice(r->r.device);
+  cudaStreamSynchronize(r->r.stream);
+  delete r;
+}
+
+int32_t lotus_cuda_update_scene(lotus_cuda_renderer* r, const lotus_scene_desc* scene,
+    lotus_scene_result* result) {
+  lotus_scene_result local{};
+  lotus_scene_result& res = result ? *result : local;
+  std::memset(&res, 0, sizeof(res));
+  if (!r || !scene) {
+    copy_detail(res.detail, sizeof(res.detail), "no renderer or scene");
+    return res.status = LOTUS_FAIL;
+  }
+  Renderer& R = r->r;
+  if (!R.failure.empty()) {
+    copy_detail(res.detail, sizeof(res.detail), "the renderer failed earlier: " + R.failure);
+    return res.status = LOTUS_FAIL;
+  }
+  cudaSetDevice(R.device);
+  return update_scene(R, *scene, res);
+}
+
+int32_t lotus_cuda_render(lotus_cuda_renderer* r, const lotus_frame_desc* frame, lotus_frame_result* result,
+    float* color) {
+  lotus_frame_result local{};
+  lotus_frame_result& res = result ? *result : local;
+  std::memset(&res, 0, sizeof(res));
+  if (!r || !frame) {
+    copy_detail(res.detail, sizeof(res.detail), "no renderer or frame");
+    return res.status = LOTUS_FAIL;
+  }
+  Renderer& R = r->r;
+  if (!R.failure.empty()) {
+    copy_detail(res.detail, sizeof(res.detail), "the renderer failed earlier: " + R.failure);
+    return res.status = LOTUS_FAIL;
+  }
+  cudaSetDevice(R.device);
+  return render(R, *frame, res, color);
+}
+
+int32_t lotus_cuda_read_color(lotus_cuda_renderer* r, float* color, uint64_t capacity_floats) {
+  if (!r || !color) return LOTUS_FAIL;
+  Renderer& R = r->r;
+  const uint64_t n = 4ull * R.width * R.height;
+  if (n == 0 || capacity_floats < n || !R.color.ptr) return LOTUS_FAIL;
+  cudaSetDevice(R.device);
+  if (cudaMemcpyAsync(color, R.color.ptr, n * 4, cudaMemcpyDeviceToHost, R.stream) != cudaSuccess ||
+      cudaStreamSynchronize(R.stream) != cudaSuccess)
+    return LOTUS_FAIL;
+  return LOTUS_PASS;
+}
+
+void* lotus_cuda_stream(lotus_cuda_renderer* r) { return r ? (void*)r->r.stream : nullptr; }
+
+int64_t lotus_cuda_read_light_table(lotus_cuda_renderer* r, uint32_t* records, uint64_t record_capacity,
+    uint32_t* offsets, uint64_t offset_capacity) {
+  if (!r) return -1;
+  Renderer& R = r->r;
+  const uint64_t n = R.host_lights.size();
+  if (records) {
+    std::vector<LightRecord> dev(n);
+    if (n) {
+      cudaSetDevice(R.device);
+      if (cudaMemcpy(dev.data(), R.lights.ptr, n * sizeof(LightRecord), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    }
+    for (uint64_t i = 0; i < n && i < record_capacity; ++i) std::memcpy(records + 4 * i, &dev[i], 16);
+  }
+  if (offsets)
+    for (uint64_t i = 0; i < R.host_light_offsets.size() && i < offset_capacity; ++i)
+      offsets[i] = R.host_light_offsets[i];
+  return (int64_t)n;
+}
+
+}  // extern "C"

@@ -1,0 +1,310 @@
+// SPDX-License-Identifier: Apache-2.0
+// Hit reconstruction, light sampling, the environment image and the camera
+// on the device (backend/vulkan/shaders/common/scene.slang and
+// common/transport.slang in hydra-lotus), over the SoA tables of scene.cuh.
+#pragma once
+
+#include "bsdf.cuh"
+#include "scene.cuh"
+
+namespace lotus {
+
+struct SurfaceHit {
+  F3 position;
+  F3 normal;          // geometric, facing the incoming ray
+  F3 shading_normal;
+  float area;
+  F3 base_color;
+  float roughness;
+  float metallic;
+  Closure bsdf;
+  F3 emission;
+};
+
+__device__ __forceinline__ F3 transform_point(const float4* m, F3 p) { return row_point(m, p); }
+
+__device__ __forceinline__ float triangle_area(F3 p0, F3 p1, F3 p2) {
+  return 0.5f * length(cross(p1 - p0, p2 - p0));
+}
+
+// ShadingNormal (scene.slang:467-488).
+__device__ __forceinline__ F3 shading_normal(const float* n, float b1, float b2, const float4* m,
+    F3 geometric, F3 direction) {
+  const F3 n0 = V(n[0], n[1], n[2]), n1 = V(n[3], n[4], n[5]), n2 = V(n[6], n[7], n[8]);
+  const F3 object = n0 + b1 * (n1 - n0) + b2 * (n2 - n0);
+  const F3 c0 = V(m[0].x, m[1].x, m[2].x);
+  const F3 c1 = V(m[0].y, m[1].y, m[2].y);
+  const F3 c2 = V(m[0].z, m[1].z, m[2].z);
+  const F3 world = cross(c1, c2) * object.x + cross(c2, c0) * object.y + cross(c0, c1) * object.z;
+  const float length2 = dot(world, world);
+  if (!(length2 > 0.0f) || isinf(length2)) return geometric;
+  F3 s = world * rsqrt_rn(length2);
+  if (dot(s, geometric) < 0.0f) s = -s;
+  return dot(s, direction) < 0.0f ? s : geometric;
+}
+
+// ReconstructHit and EvaluatePreview for constant material inputs
+// (scene.slang:1408-1449, 1184-1260). The corners come from the
+// leaf-ordered triangle pool, which holds the geometry's own positions.
+__device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32_t instance,
+    uint32_t tri, float b1, float b2, F3 direction, uint32_t* primitive_out = nullptr) {
+  const InstanceShading rec = S.inst_shade[instance];
+  const float4* tv = S.tris + 3 * (size_t)tri;
+  const float4 a = tv[0], b = tv[1], c = tv[2];
+  const uint32_t primitive = __float_as_uint(a.w);
+  if (primitive_out) *primitive_out = primitive;
+  const F3 p0 = transform_point(rec.m, V(a));
+  const F3 p1 = transform_point(rec.m, V(b));
+  const F3 p2 = transform_point(rec.m, V(c));
+  SurfaceHit sh;
+  sh.position = p0 + b1 * (p1 - p0) + b2 * (p2 - p0);
+  const F3 normal = normalize(cross(p1 - p0, p2 - p0));
+  sh.area = triangle_area(p0, p1, p2);
+  sh.normal = dot(normal, direction) > 0.0f ? -normal : normal;
+  sh.shading_normal = sh.normal;
+  if (rec.normals != kNoLights)
+    sh.shading_normal = shading_normal(S.normals + 9 * ((size_t)rec.normals + primitive), b1, b2,
+        rec.m, sh.normal, direction);
+  const MaterialRecord mat = S.materials[rec.material];
+  sh.base_color = V(mat.base_roughness);
+  sh.roughness = mat.base_roughness.w;
+  sh.metallic = mat.emission_metallic.w;
+  const uint32_t flags = __float_as_uint(mat.coverage.z);
+  const float transmission = mat.transmission.w;
+  bool entering = true;
+  if (transmission > 0.0f) {
+    const F3 outward = rec.mirror ? -normal : normal;
+    entering = dot(outward, direction) < 0.0f;
+  }
+  sh.bsdf = make_closure(sh.base_color, sh.roughness, sh.metallic, mat.specular_ior.w,
+      (flags & 1u) != 0, V(mat.specular_ior), transmission, V(mat.transmission),
+      (flags & 2u) != 0, entering);
+  sh.emission = V(mat.emission_metallic);
+  return sh;
+}
+
+struct LightSample {
+  F3 direction;
+  float distance;
+  F3 radiance;
+  float pdf;
+  bool delta;
+};
+
+__device__ __forceinline__ LightSample no_light() {
+  LightSample s;
+  s.direction = V(0.0f, 0.0f, 1.0f);
+  s.distance = 0.0f;
+  s.radiance = V(0.0f);
+  s.pdf = 0.0f;
+  s.delta = false;
+  return s;
+}
+
+// SampleTriangle (scene.slang:632-677), over the light table's
+// world-space corners.
+__device__ __forceinline__ LightSample sample_triangle(const SceneView& S, uint32_t light,
+    float pdf, float ux, float uy, F3 origin) {
+  const float root = sqrtf(ux);
+  const float b1 = root * (1.0f - uy), b2 = root * uy;
+  const float4* lv = S.light_verts + 3 * (size_t)light;
+  const F3 p0 = V(lv[0]), p1 = V(lv[1]), p2 = V(lv[2]);
+  const F3 position = p0 + b1 * (p1 - p0) + b2 * (p2 - p0);
+  const F3 normal = normalize(cross(p1 - p0, p2 - p0));
+  const float area = triangle_area(p0, p1, p2);
+  const F3 radiance = V(S.light_radiance[light]);
+  const F3 toward = position - origin;
+  const float distance2 = dot(toward, toward);
+  if (!(area > 0.0f) || !(distance2 > 0.0f) || max_component(radiance) <= 0.0f) return no_light();
+  LightSample s;
+  s.direction = toward * rsqrt_rn(distance2);
+  const float cosine = fabsf(dot(normal, s.direction));
+  if (!(cosine > 0.0f)) return no_light();
+  const F3 end = offset_ray_origin(position, dot(normal, s.direction) > 0.0f ? -normal : normal);
+  s.distance = fmaxf(0.0f, dot(end - origin, s.direction));
+  s.radiance = radiance;
+  s.pdf = pdf / area * distance2 / cosine;
+  s.delta = false;
+  return s;
+}
+
+// FindInterval (scene.slang:775-789).
+__device__ __forceinline__ uint32_t find_interval(const float* __restrict__ F, uint64_t first,
+    uint32_t count, float u) {
+  uint32_t low = 0, len = count + 1;
+  while (len > 0) {
+    const uint32_t half = len >> 1;
+    const uint32_t middle = low + half;
+    if (F[first + middle] <= u) {
+      low = middle + 1;
+      len -= half + 1;
+    } else {
+      len = half;
+    }
+  }
+  return min(max(low, 1u), count) - 1;
+}
+
+// SampleCumulative (scene.slang:794-800).
+__device__ __forceinline__ float sample_cumulative(const float* __restrict__ F, uint64_t first,
+    uint32_t count, float u, uint32_t& cell) {
+  cell = find_interval(F, first, count, u);
+  const float low = F[first + cell];
+  const float width = F[first + cell + 1] - low;
+  const float offset = width > 0.0f ? (u - low) / width : 0.5f;
+  return fminf((float(cell) + offset) / float(count), 0.99999994f);
+}
+
+__device__ __forceinline__ void environment_uv(F3 local, float& u, float& v) {
+  const float uu = 0.5f - atan2f(local.x, local.z) * (0.5f / kPi);
+  v = acosf(fminf(fmaxf(local.y, -1.0f), 1.0f)) * (1.0f / kPi);
+  u = uu - floorf(uu);
+}
+
+__device__ __forceinline__ F3 environment_direction(float u, float v) {
+  const float theta = kPi * v;
+  const float phi = kPi * (1.0f - 2.0f * u);
+  const float sin_theta = sinf(theta);
+  return V(sin_theta * sinf(phi), cosf(theta), sin_theta * cosf(phi));
+}
+
+// EnvironmentLookup (scene.slang:819-824): FP32 bilinear filtering,
+// repeating across longitude and clamped at the poles.
+__device__ __forceinline__ F3 environment_lookup(const SceneView& S, float u, float v) {
+  const float x = u * float(S.env_width) - 0.5f;
+  const float y = v * float(S.env_height) - 0.5f;
+  const float fx0 = floorf(x), fy0 = floorf(y);
+  const float ax = x - fx0, ay = y - fy0;
+  const int w = (int)S.env_width, h = (int)S.env_height;
+  int x0 = (int)fx0 % w;
+  if (x0 < 0) x0 += w;
+  const int x1 = x0 + 1 == w ? 0 : x0 + 1;
+  const int iy = (int)fy0;
+  const int y0 = min(max(iy, 0), h - 1);
+  const int y1 = min(max(iy + 1, 0), h - 1);
+  const float4 t00 = S.env_texels[(size_t)y0 * w + x0];
+  const float4 t10 = S.env_texels[(size_t)y0 * w + x1];
+  const float4 t01 = S.env_texels[(size_t)y1 * w + x0];
+  const float4 t11 = S.env_texels[(size_t)y1 * w + x1];
+  const float rx = (t00.x * (1.0f - ax) + t10.x * ax) * (1.0f - ay) + (t01.x * (1.0f - ax) + t11.x * ax) * ay;
+  const float ry = (t00.y * (1.0f - ax) + t10.y * ax) * (1.0f - ay) + (t01.y * (1.0f - ax) + t11.y * ax) * ay;
+  const float rz = (t00.z * (1.0f - ax) + t10.z * ax) * (1.0f - ay) + (t01.z * (1.0f - ax) + t11.z * ax) * ay;
+  return V(fmaxf(rx, 0.0f) * S.env_scale[0], fmaxf(ry, 0.0f) * S.env_scale[1],
+      fmaxf(rz, 0.0f) * S.env_scale[2]);
+}
+
+__device__ __forceinline__ float environment_direction_pdf(const SceneView& S, float u, float v) {
+  const uint32_t column = min((uint32_t)(u * float(S.env_columns)), S.env_columns - 1);
+  const uint32_t row = min((uint32_t)(v * float(S.env_rows)), S.env_rows - 1);
+  const float sin_theta = sinf(kPi * v);
+  if (!(sin_theta > 0.0f)) return 0.0f;
+  return S.env_floats[(uint64_t)row * S.env_columns + column] / (2.0f * kPi * kPi * sin_theta);
+}
+
+// SampleEnvironment (scene.slang:845-872).
+__device__ __forceinline__ LightSample sample_environment(const SceneView& S, float selection,
+    float ux, float uy) {
+  const uint64_t cells = (uint64_t)S.env_columns * S.env_rows;
+  uint32_t row, column;
+  const float v = sample_cumulative(S.env_floats, cells, S.env_rows, ux, row);
+  const float u = sample_cumulative(S.env_floats,
+      cells + S.env_rows + 1 + (uint64_t)row * (S.env_columns + 1), S.env_columns, uy, column);
+  const float sin_theta = sinf(kPi * v);
+  const float density = S.env_floats[(uint64_t)row * S.env_columns + column];
+  if (!(sin_theta > 0.0f) || !(density > 0.0f)) return no_light();
+  const F3 local = environment_direction(u, v);
+  const F3 r0 = V(S.env_frame[0], S.env_frame[1], S.env_frame[2]);
+  const F3 r1 = V(S.env_frame[3], S.env_frame[4], S.env_frame[5]);
+  const F3 r2 = V(S.env_frame[6], S.env_frame[7], S.env_frame[8]);
+  LightSample s;
+  s.direction = normalize(local.x * r0 + local.y * r1 + local.z * r2);
+  s.distance = kFloatMax;
+  s.radiance = environment_lookup(S, u, v);
+  s.pdf = selection * density / (2.0f * kPi * kPi * sin_theta);
+  s.delta = false;
+  return s;
+}
+
+// EnvironmentRadiance (scene.slang:877-890).
+__device__ __forceinline__ F3 environment_radiance(const SceneView& S, F3 direction, bool weigh,
+    float pdf) {
+  const F3 r0 = V(S.env_frame[0], S.env_frame[1], S.env_frame[2]);
+  const F3 r1 = V(S.env_frame[3], S.env_frame[4], S.env_frame[5]);
+  const F3 r2 = V(S.env_frame[6], S.env_frame[7], S.env_frame[8]);
+  const F3 local = V(dot(r0, direction), dot(r1, direction), dot(r2, direction));
+  float u, v;
+  environment_uv(local, u, v);
+  const F3 radiance = environment_lookup(S, u, v);
+  if (!weigh || !(S.env_selection > 0.0f)) return radiance;
+  return radiance * power_heuristic(pdf, S.env_selection * environment_direction_pdf(S, u, v));
+}
+
+// SampleLight (scene.slang:894-909): Vose's alias table, then a point.
+__device__ __forceinline__ LightSample sample_light(const SceneView& S, float u0, float u1,
+    float u2, float u3, F3 origin) {
+  const uint32_t count = S.light_count;
+  const uint32_t column = min((uint32_t)(u0 * float(count)), count - 1);
+  const LightRecord record = S.lights[column];
+  const uint32_t light = u1 < record.threshold ? column : record.alias;
+  const LightRecord chosen = S.lights[light];
+  if (chosen.instance == kEnvironmentLight) return sample_environment(S, chosen.pdf, u2, u3);
+  return sample_triangle(S, light, chosen.pdf, u2, u3, origin);
+}
+
+// EmitterPdf (scene.slang:1004-1010).
+__device__ __forceinline__ float emitter_pdf(const SceneView& S, uint32_t instance,
+    uint32_t primitive, float area) {
+  const uint32_t first = S.inst_shade[instance].light_offset;
+  if (first == kNoLights || !(area > 0.0f)) return 0.0f;
+  return S.lights[first + primitive].pdf / area;
+}
+
+// The frame's camera and target, set per RenderScene call; sample_index
+// and accumulated advance on the device between samples.
+struct FrameConst {
+  float clip_to_world[16];
+  float ndc[4];
+  float background[4];
+  uint32_t width, height;
+  uint32_t rect[4];
+  uint32_t max_bounces;
+  uint32_t sample_lights;
+  uint32_t sample_index;
+  uint32_t accumulated;
+  uint32_t add_sample;
+  uint32_t environment_background;
+};
+
+// CameraRay (scene.slang:273-283).
+__device__ __forceinline__ void camera_ray(const FrameConst& f, float nx, float ny, F3& origin,
+    F3& direction, float& tmax) {
+  const float* c = f.clip_to_world;
+  float n[4], a[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    n[r] = c[r] * nx + c[4 + r] * ny + c[8 + r] * 0.0f + c[12 + r] * 1.0f;
+    a[r] = c[r] * nx + c[4 + r] * ny + c[8 + r] * 1.0f + c[12 + r] * 1.0f;
+  }
+  origin = V(n[0] / n[3], n[1] / n[3], n[2] / n[3]);
+  direction = normalize(V(a[0], a[1], a[2]) * n[3] - V(n[0], n[1], n[2]) * a[3]);
+  tmax = a[3] == 0.0f ? kFloatMax : length(V(a[0] / a[3], a[1] / a[3], a[2] / a[3]) - origin);
+}
+
+constexpr uint32_t kUnweightedLight = 1;
+constexpr uint32_t kRouletteBounces = 3;
+constexpr float kMaxSurvival = 0.95f;
+
+// StartPath (transport.slang:53-69): the camera ray through a uniformly
+// distributed point of the pixel, and the path's random state after it.
+__device__ __forceinline__ void start_path(const FrameConst& f, uint32_t px, uint32_t py,
+    uint32_t sample_index, F3& origin, F3& direction, float& tmax, uint32_t& rng) {
+  const uint32_t pixel_index = py * f.width + px;
+  rng = seed_random(pixel_index, sample_index);
+  const float ux = next_random(rng);
+  const float uy = next_random(rng);
+  const float film_x = float(px) + 0.5f + (ux - 0.5f);
+  const float film_y = float(py) + 0.5f + (uy - 0.5f);
+  camera_ray(f, film_x * f.ndc[0] + f.ndc[2], film_y * f.ndc[1] + f.ndc[3], origin, direction, tmax);
+}
+
+}  // namespace lotus

@@ -1,0 +1,157 @@
+"""The Python host of the CUDA backend, mirroring the reference's
+``Lotus::OffscreenRenderer`` (include/lotus/vulkan_backend.hpp:753-842 in
+hydra-lotus) over the C ABI of include/lotus_cuda.h.
+
+``CudaOffscreenRenderer.update_scene`` stands for ``UpdateScene``,
+``render_scene`` for ``RenderScene``; both return the status and detail the
+reference's evidence carries (Pass, Fail, Skip) instead of raising.
+There is no CPU fallback: constructing a renderer without the compiled
+library raises, and without an sm_100 device reports Skip.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from . import build as _build
+
+_lib = None
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+def lib():
+    """The loaded CUDA library. Raises LibraryMissing when it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_build.LIB):
+            raise LibraryMissing(
+                f"{_build.LIB} is not built: run `python -m hydra_lotus_b200.build`")
+        L = C.CDLL(_build.LIB)
+        L.lotus_cuda_abi_version.restype = C.c_uint32
+        L.lotus_cuda_struct_sizes.restype = C.c_uint32
+        L.lotus_cuda_struct_sizes.argtypes = [C.POINTER(C.c_uint64), C.c_uint32]
+        L.lotus_cuda_capability.restype = C.c_int32
+        L.lotus_cuda_capability.argtypes = [C.c_int32, C.c_char_p, C.c_size_t]
+        L.lotus_cuda_create.restype = C.c_int32
+        L.lotus_cuda_create.argtypes = [C.POINTER(abi.Options), C.POINTER(C.c_void_p),
+                                        C.c_char_p, C.c_size_t]
+        L.lotus_cuda_destroy.argtypes = [C.c_void_p]
+        L.lotus_cuda_update_scene.restype = C.c_int32
+        L.lotus_cuda_update_scene.argtypes = [C.c_void_p, C.POINTER(abi.SceneDesc),
+                                              C.POINTER(abi.SceneResult)]
+        L.lotus_cuda_render.restype = C.c_int32
+        L.lotus_cuda_render.argtypes = [C.c_void_p, C.POINTER(abi.FrameDesc),
+                                        C.POINTER(abi.FrameResult), C.c_void_p]
+        L.lotus_cuda_read_color.restype = C.c_int32
+        L.lotus_cuda_read_color.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
+        L.lotus_cuda_stream.restype = C.c_void_p
+        L.lotus_cuda_stream.argtypes = [C.c_void_p]
+        L.lotus_cuda_read_light_table.restype = C.c_int64
+        L.lotus_cuda_read_light_table.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64,
+                                                  C.c_void_p, C.c_uint64]
+        if L.lotus_cuda_abi_version() != abi.ABI_VERSION:
+            raise RuntimeError("liblotus_cuda ABI version mismatch")
+        abi.check_struct_sizes(L)
+        _lib = L
+    return _lib
+
+
+def capability(device=0):
+    """RayQueryCapability: (status, detail)."""
+    buf = C.create_string_buffer(256)
+    status = lib().lotus_cuda_capability(device, buf, 256)
+    return status, buf.value.decode()
+
+
+class RendererError(RuntimeError):
+    def __init__(self, status, detail):
+        super().__init__(f"status {status}: {detail}")
+        self.status = status
+        self.detail = detail
+
+
+class CudaOffscreenRenderer:
+    """One renderer: one device, one stream, the resident scene and the
+    accumulation targets."""
+
+    def __init__(self, device=0):
+        self.handle = None
+        opts = abi.Options(device=device, flags=0)
+        h = C.c_void_p()
+        err = C.create_string_buffer(256)
+        status = lib().lotus_cuda_create(C.byref(opts), C.byref(h), err, 256)
+        if status != abi.PASS:
+            raise RendererError(status, err.value.decode())
+        self.handle = h
+        self.scene = None
+
+    def close(self):
+        if self.handle:
+            lib().lotus_cuda_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def stream(self):
+        """The renderer's cudaStream_t as an integer handle."""
+        return lib().lotus_cuda_stream(self.handle)
+
+    def update_scene(self, scene):
+        """UpdateScene: uploads `scene` (a scenes.Scene). Returns the
+        lotus_scene_result."""
+        res = abi.SceneResult()
+        lib().lotus_cuda_update_scene(self.handle, C.byref(scene.desc()), C.byref(res))
+        self.scene = scene
+        return res
+
+    def render_scene(self, frame, color=None):
+        """RenderScene: returns (lotus_frame_result, colour). With
+        frame.target.read_back, colour is an (H, W, 4) float32 array (or the
+        given one, filled)."""
+        res = abi.FrameResult()
+        ptr = None
+        if frame.target.read_back:
+            if color is None:
+                color = np.empty((frame.target.height, frame.target.width, 4), dtype=np.float32)
+            ptr = color.ctypes.data
+        lib().lotus_cuda_render(self.handle, C.byref(frame), C.byref(res), ptr)
+        return res, (color if frame.target.read_back else None)
+
+    def read_color(self, out):
+        rc = lib().lotus_cuda_read_color(self.handle, out.ctypes.data, out.size)
+        if rc != abi.PASS:
+            raise RendererError(rc, "read_color failed")
+        return out
+
+    def light_table(self):
+        n = lib().lotus_cuda_read_light_table(self.handle, None, 0, None, 0)
+        if n < 0:
+            raise RendererError(abi.FAIL, "no light table")
+        ninst = len(self.scene.instances) if self.scene else 0
+        rec = np.zeros((max(n, 1), 4), dtype=np.uint32)
+        off = np.zeros(max(ninst, 1), dtype=np.uint32)
+        lib().lotus_cuda_read_light_table(self.handle, rec.ctypes.data, n, off.ctypes.data, ninst)
+        return rec[:n], off[:ninst]
+
+
+def check(result, what="call"):
+    """Raises RendererError unless `result.status` is Pass."""
+    if result.status != abi.PASS:
+        raise RendererError(result.status, f"{what}: {result.detail.decode(errors='replace')}")
+    return result

@@ -476,7 +476,8 @@ def sphere_field(seed=0, width=1920, height=1080, prototypes=320, grid=100,
                rng.uniform(-half * 0.6, half * 0.6))
         s.add_instance(tri, mat, affine(lin, pos))
     s.set_environment(procedural_sky(sky_size[0], sky_size[1], seed))
-    eye = (48.0, 22.0, 48.0)
+    extent = grid * spacing
+    eye = (0.24 * extent, 0.11 * extent, 0.24 * extent)
     view = look_at(eye, (0.0, 0.0, 0.0))
     s.world_to_clip = multiply(perspective(50.0, width / height, 0.1, 1000.0), view)
     s.width, s.height = width, height

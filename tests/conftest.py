@@ -1,0 +1,36 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs an sm_100 GPU and the CUDA library")
+
+
+@pytest.fixture(scope="session")
+def oracle_lib():
+    from oracle import build, oracle
+    build.build()
+    return oracle
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    """The CUDA library on an sm_100 device. GPU tests fail loudly (never
+    fall back) when the library is missing or the device is not usable."""
+    from hydra_lotus_b200 import abi, renderer
+    status, detail = renderer.capability(0)
+    assert status == abi.PASS, f"no usable sm_100 device: {detail}"
+    return renderer
+
+
+@pytest.fixture(scope="session")
+def golden():
+    import numpy as np
+    g = np.load(os.path.join(ROOT, "tests", "golden", "cornell_box.npz"))
+    return {"mean": g["mean"], "variance": g["variance"], "samples": int(g["samples"])}

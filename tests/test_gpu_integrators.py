@@ -1,0 +1,105 @@
+"""GPU parity of the integrators against the oracle, through the C ABI."""
+
+import numpy as np
+import pytest
+
+from hydra_lotus_b200 import abi, metrics, scenes
+
+from parity import PathParity
+
+pytestmark = pytest.mark.gpu
+
+INTEGRATORS = [abi.INTEGRATOR_REFERENCE, abi.INTEGRATOR_WAVEFRONT]
+
+
+def small_sphere_field():
+    return scenes.sphere_field(seed=3, width=160, height=96, prototypes=8, grid=12,
+                               spacing=2.0, spheres=60, emitters=8, sky_size=(256, 128))
+
+
+@pytest.fixture(scope="module")
+def renderer(cuda):
+    r = cuda.CudaOffscreenRenderer(0)
+    yield r
+    r.close()
+
+
+def render(cuda, renderer, scene, settings, frame_count=1, **kw):
+    cuda.check(renderer.update_scene(scene), "update_scene")
+    res, color = renderer.render_scene(scene.frame(settings, frame_count, **kw))
+    cuda.check(res, "render_scene")
+    return res, color
+
+
+@pytest.mark.parametrize("integrator", INTEGRATORS)
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+def test_box_room_paths_match_oracle(cuda, renderer, oracle_lib, integrator, light_sampling):
+    scene = scenes.box_room(seed=0, size=128)
+    st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,
+                              max_bounces=6, sample_index=7)
+    res, color = render(cuda, renderer, scene, st)
+    want, rays = oracle_lib.OracleScene(scene).sample(scene.frame(st), 7)
+    p = PathParity(color, want)
+    print(p)
+    p.assert_ok()
+    assert p.exact > 0.9, p
+    assert res.camera_rays == rays[0]
+
+
+@pytest.mark.parametrize("integrator", INTEGRATORS)
+def test_sphere_field_paths_match_oracle(cuda, renderer, oracle_lib, integrator):
+    scene = small_sphere_field()
+    st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=8, sample_index=3)
+    res, color = render(cuda, renderer, scene, st)
+    want, rays = oracle_lib.OracleScene(scene).sample(scene.frame(st), 3)
+    p = PathParity(color, want)
+    print(p, res.camera_rays, res.extension_rays, res.shadow_rays, rays)
+    p.assert_ok()
+
+
+def test_light_table_matches_oracle(cuda, renderer, oracle_lib):
+    for scene in (scenes.box_room(), scenes.cornell_reference(), small_sphere_field()):
+        cuda.check(renderer.update_scene(scene), "update_scene")
+        got_rec, got_off = renderer.light_table()
+        want_rec, want_off = oracle_lib.OracleScene(scene).light_table()
+        np.testing.assert_array_equal(got_rec, want_rec)
+        np.testing.assert_array_equal(got_off, want_off)
+
+
+def test_wavefront_equals_reference_integrator(cuda, renderer):
+    scene = scenes.box_room(seed=0, size=128)
+    out = []
+    for integrator in INTEGRATORS:
+        st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                                  max_bounces=6, sample_index=11)
+        _, color = render(cuda, renderer, scene, st, frame_count=4)
+        out.append(color)
+    p = PathParity(out[1], out[0])
+    print(p)
+    assert p.within >= 0.999, p
+
+
+@pytest.mark.parametrize("integrator", INTEGRATORS)
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+def test_cornell_matches_reference_golden(cuda, renderer, golden, integrator, light_sampling):
+    """DES-Q5 against the reference's committed 1024-spp Cornell images,
+    from sample index 2^20 as renderer.path.reference renders it."""
+    scene = scenes.cornell_reference()
+    st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,
+                              max_bounces=64, sample_index=1 << 20)
+    res, color = render(cuda, renderer, scene, st, frame_count=1024)
+    assert res.samples_per_pixel == 1024
+    c = metrics.compare(color, 1024, golden["mean"], golden["variance"], golden["samples"])
+    print(c)
+    assert c.ok, c
+
+
+def test_cornell_negative_control_rejected(cuda, renderer, golden):
+    scene = scenes.cornell_reference(red_scale=1.1)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT,
+                              light_sampling=abi.LIGHT_SAMPLING_BSDF, max_bounces=64,
+                              sample_index=1 << 20)
+    _, color = render(cuda, renderer, scene, st, frame_count=1024)
+    c = metrics.compare(color, 1024, golden["mean"], golden["variance"], golden["samples"])
+    assert not c.ok, c
