@@ -1,0 +1,339 @@
+"""Benchmark: Mrays/s of the plain wavefront path tracer at 1080p.
+
+One step renders one frame of the 1080p workload (the seeded sphere field:
+4096 instanced, Perlin-displaced icospheres, 1.07M unique and 13.7M
+instanced triangles, 64 emissive triangles and a 2048x1024 importance-
+sampled sky) at 16 samples per pixel, max depth 8, NEE + MIS, through the
+CUDA backend's C ABI. A frame's rays are its camera, extension and shadow
+rays; value = rays over device time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 every rank renders its own frames (independent sample indices)
+on its own GPU and rank 0 prints the job's total: replicas, no collective
+on the data path (weak scaling). `--impl reference` times the CPU oracle
+(the scalar restatement of the reference's path tracer) on the host cores
+on a bounded band of the same frame.
+"""
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+from hydra_lotus_b200 import abi, scenes  # noqa: E402
+
+WIDTH, HEIGHT, SPP, DEPTH = 1920, 1080, 16, 8
+METRIC = "Mrays/s at 1080p (plain wavefront PT)"
+WORKLOAD = ("sphere-field seed 0: 4096 instanced Perlin-displaced icospheres (subdiv 3/4, "
+            "1.07M unique / 13.7M instanced triangles) on a 100x100 grid, 64 emissive "
+            "triangles + 2048x1024 importance-sampled sky; 1920x1080, 16 spp, max depth 8, "
+            "wavefront PT, NEE+MIS, FP32 transport, FP64 accumulation")
+# Algorithmic bytes per extension ray outside the BVH walk: the queue
+# entry (4), origin, direction and radiance sections (48), the hit section
+# (16) and the hit-queue entry (4).
+EXTEND_STATE_BYTES = 72
+NODE_BYTES, TRIANGLE_BYTES, INSTANCE_BYTES = 64, 48, 64
+
+
+def settings(sample_index):
+    return abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT,
+                                light_sampling=abi.LIGHT_SAMPLING_MIS,
+                                max_bounces=DEPTH, sample_index=sample_index)
+
+
+def launches_per_sample(max_bounces):
+    # camera, shade and shadow per bounce, extend per bounce after the
+    # first, resolve, finish, advance
+    return 1 + 2 * (max_bounces + 1) + max_bounces + 3
+
+
+def measured_peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for name, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(scene, seconds, rows=64):
+    """The oracle (the scalar CPU restatement of the reference's path
+    tracer) on a band of the frame, one sample per pass, until `seconds`."""
+    from oracle import oracle
+    o = oracle.OracleScene(scene)
+    threads = os.cpu_count() or 1
+    y0 = (HEIGHT - rows) // 2
+    frame = scene.frame(settings(0), data_window=(0, y0, WIDTH, rows))
+    rays = 0
+    passes = 0
+    t0 = time.perf_counter()
+    while True:
+        _, r = o.sample(frame, passes, threads=threads)
+        rays += int(r.sum())
+        passes += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"rows {y0}-{y0 + rows - 1} of the 1920x1080 frame, {passes} passes of 1 spp "
+                      f"({rays} rays in {dt:.1f} s), OpenMP over {threads} threads"}
+
+
+def run_reference(args, rank):
+    """--impl reference: the CPU oracle on the host cores."""
+    if rank != 0:
+        return
+    scene = scenes.sphere_field(seed=0)
+    for _ in range(args.warmup):
+        cpu_baseline(scene, 0.0, rows=32)
+    results = []
+    total_rays, total_s = 0, 0.0
+    for k in range(args.steps):
+        b = cpu_baseline(scene, 2.0, rows=64)
+        results.append(b)
+    # Aggregate: mean throughput over steps.
+    value = statistics.mean(b["value"] for b in results)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": WORKLOAD, "sample": "a 64-row band of the frame per pass"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s",
+                         "cores": results[0]["cores"], "kind": "port",
+                         "sample": results[0]["sample"]},
+        "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    from hydra_lotus_b200 import renderer
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    scene = scenes.sphere_field(seed=0)
+    r = renderer.CudaOffscreenRenderer(local_rank)
+    sres = renderer.check(r.update_scene(scene), "update_scene")
+    stream = torch.cuda.ExternalStream(r.stream)
+
+    base = 1000003 * rank  # independent samples per rank
+    step_index = [0]
+
+    def frame(read_back=False, flags=0):
+        f = scene.frame(settings(base + SPP * step_index[0]), frame_count=SPP,
+                        read_back=read_back, flags=flags)
+        step_index[0] += 1
+        return f
+
+    for _ in range(args.warmup):
+        renderer.check(r.render_scene(frame())[0], "warmup")
+
+    # Timed region: K frames, device time by CUDA events on the renderer's
+    # stream, bracketed by a barrier and synchronize.
+    barrier()
+    torch.cuda.synchronize()
+    rays = 0
+    with ClockSampler(local_rank) as clocks:
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(args.steps):
+            res, _ = r.render_scene(frame())
+            renderer.check(res, "render")
+            rays += res.camera_rays + res.extension_rays + res.shadow_rays
+        stop.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = start.elapsed_time(stop)
+    clock = clocks.summary()
+
+    # End to end through the C ABI: per step the frame description goes to
+    # the device and the RGBA32F image comes back into pinned host memory.
+    pinned = torch.empty((HEIGHT, WIDTH, 4), dtype=torch.float32, pin_memory=True)
+    color = np.frombuffer((C.c_float * (HEIGHT * WIDTH * 4)).from_address(pinned.data_ptr()),
+                          dtype=np.float32).reshape(HEIGHT, WIDTH, 4)
+    barrier()
+    torch.cuda.synchronize()
+    e2e_rays = 0
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_stop = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(args.steps):
+        res, _ = r.render_scene(frame(read_back=True), color=color)
+        renderer.check(res, "render e2e")
+        e2e_rays += res.camera_rays + res.extension_rays + res.shadow_rays
+    e_stop.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e_start.elapsed_time(e_stop)
+
+    # Kernel timings (one instrumented frame) and BVH visits (another).
+    timed, _ = r.render_scene(frame(flags=abi.FRAME_TIMINGS))
+    renderer.check(timed, "timed frame")
+    counted, _ = r.render_scene(frame(flags=abi.FRAME_COUNT_VISITS))
+    renderer.check(counted, "counted frame")
+
+    stats = torch.tensor([rays, e2e_rays, ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        sums = stats[:2].clone()
+        dist.all_reduce(sums)
+        maxes = stats[2:].clone()
+        dist.all_reduce(maxes, op=dist.ReduceOp.MAX)
+        stats = torch.cat([sums, maxes])
+    total_rays, total_e2e_rays, max_ms, max_e2e_ms = stats.tolist()
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        # Extension kernel roofline: algorithmic bytes of the last sample's
+        # extension rays over the extension kernels' device time.
+        n_ext = max(counted.visit_rays[1], 1)
+        per_ray = (EXTEND_STATE_BYTES + NODE_BYTES * counted.node_visits[1] / n_ext +
+                   TRIANGLE_BYTES * counted.triangle_visits[1] / n_ext +
+                   INSTANCE_BYTES * counted.instance_visits[1] / n_ext)
+        ext_rays_timed = sum(timed.wavefront_path_counts[b]
+                             for b in range(1, timed.wavefront_path_count_size))
+        ext_bytes = ext_rays_timed * per_ray
+        achieved = ext_bytes / (timed.extend_gpu_ms * 1e-3) / 1e9 if timed.extend_gpu_ms else 0.0
+        launches = timed.extend_launches or DEPTH
+        cpu = cpu_baseline(scene, args.cpu_seconds)
+        line = {
+            "metric": METRIC,
+            "value": round(total_rays / (max_ms * 1e-3) / 1e6, 2),
+            "unit": "Mrays/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(max_ms / args.steps, 3),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded procedural scene; no dataset)",
+            "config": {"workload": WORKLOAD, "rays_per_step": int(total_rays / args.steps / world),
+                       "l2": "inputs larger than L2: path state 166 MB + BVH/triangles/normals "
+                             f"{sres.device_bytes / 1e6:.0f} MB per frame pass",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": round(total_e2e_rays / (max_e2e_ms * 1e-3) / 1e6, 2),
+                    "unit": "Mrays/s", "h2d_bytes_per_step": 160,
+                    "d2h_bytes_per_step": WIDTH * HEIGHT * 16 + 64},
+            "gpu_launches": launches_per_sample(DEPTH) * SPP * args.steps,
+            "roofline": {
+                "kernel": "k_wf_extend",
+                "bound": "hbm",
+                "achieved": round(achieved, 1),
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": round(achieved / peak, 4),
+                "peak_kind": peak_kind,
+                "traffic": None,
+                "bytes_per_ray": round(per_ray, 1),
+                "nodes_per_ray": round(counted.node_visits[1] / n_ext, 2),
+                "triangles_per_ray": round(counted.triangle_visits[1] / n_ext, 2),
+                "instances_per_ray": round(counted.instance_visits[1] / n_ext, 2),
+                "extend_ms_per_sample": round(timed.extend_gpu_ms, 4),
+                "extend_launches_per_sample": launches,
+                "kernel_ms_per_sample": {
+                    "camera": round(timed.camera_gpu_ms, 4), "extend": round(timed.extend_gpu_ms, 4),
+                    "shade": round(timed.shade_gpu_ms, 4), "shadow": round(timed.shadow_gpu_ms, 4),
+                    "resolve": round(timed.resolve_gpu_ms, 4)},
+            },
+            "cpu_baseline": cpu,
+            "clocks": clock,
+        }
+        print(json.dumps(line), flush=True)
+    r.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

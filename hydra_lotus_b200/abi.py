@@ -23,6 +23,9 @@ LIGHT_SAMPLING_RESTIR_INITIAL = 2
 MAX_BOUNCES = 1024
 MAX_REPORTED_BOUNCES = 64
 
+FRAME_TIMINGS = 1
+FRAME_COUNT_VISITS = 2
+
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
@@ -136,7 +139,7 @@ class FrameDesc(C.Structure):
         ("target", Target),
         ("settings", Settings),
         ("frame_count", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("flags", C.c_uint32),
     ]
 
 
@@ -153,7 +156,18 @@ class FrameResult(C.Structure):
         ("gpu_ms", C.c_double),
         ("wavefront_path_counts", C.c_uint32 * MAX_REPORTED_BOUNCES),
         ("wavefront_path_count_size", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("timings_available", C.c_uint32),
+        ("camera_gpu_ms", C.c_double),
+        ("extend_gpu_ms", C.c_double),
+        ("shade_gpu_ms", C.c_double),
+        ("shadow_gpu_ms", C.c_double),
+        ("resolve_gpu_ms", C.c_double),
+        ("extend_launches", C.c_uint32),
+        ("shadow_launches", C.c_uint32),
+        ("visit_rays", C.c_uint64 * 3),
+        ("node_visits", C.c_uint64 * 3),
+        ("triangle_visits", C.c_uint64 * 3),
+        ("instance_visits", C.c_uint64 * 3),
         ("detail", C.c_char * 256),
     ]
 
@@ -183,7 +197,7 @@ def default_settings(**overrides):
 
 def make_frame(world_to_clip, width, height, settings=None, frame_count=1,
                clear_color=(0.0, 0.0, 0.0, 0.0), data_window=(0, 0, 0, 0),
-               display_window=(0.0, 0.0, 0.0, 0.0), read_back=True):
+               display_window=(0.0, 0.0, 0.0, 0.0), read_back=True, flags=0):
     f = FrameDesc()
     for i, v in enumerate(world_to_clip):
         f.world_to_clip[i] = float(v)
@@ -196,6 +210,7 @@ def make_frame(world_to_clip, width, height, settings=None, frame_count=1,
     f.target.read_back = 1 if read_back else 0
     f.settings = settings if settings is not None else default_settings()
     f.frame_count = frame_count
+    f.flags = flags
     return f
 
 

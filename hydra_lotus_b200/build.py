@@ -2,8 +2,7 @@
 nvcc for sm_100a.
 
 The library is compiled with --fmad=false so that the transport's multiply
-and add steps round separately in source order; the BVH slab tests use
-explicit fused multiply-adds where rounding cannot change a result.
+and add steps round separately in source order.
 """
 
 import os

@@ -51,7 +51,7 @@ __device__ __forceinline__ Closure make_closure(F3 base_color, float roughness, 
 }
 
 __device__ __forceinline__ F3 fresnel_schlick(F3 f0, float f90, float cos_theta) {
-  const float weight = powf(saturate(1.0f - cos_theta), 5.0f);
+  const float weight = lpow5(saturate(1.0f - cos_theta));
   return f0 * (1.0f - weight) + V(f90 * weight);
 }
 
@@ -101,7 +101,9 @@ __device__ __forceinline__ F3 sample_ggx_visible_normal(F3 wo, float alpha, floa
   const float phi = 2.0f * kPi * ux;
   const float z = (1.0f - uy) * (1.0f + wo_std.z) - wo_std.z;
   const float sin_theta = sqrtf(saturate(1.0f - z * z));
-  const F3 h_std = V(sin_theta * cosf(phi), sin_theta * sinf(phi), z) + wo_std;
+  float sp, cp;
+  lsincos(phi, sp, cp);
+  const F3 h_std = V(sin_theta * cp, sin_theta * sp, z) + wo_std;
   return normalize(V(h_std.x * alpha, h_std.y * alpha, h_std.z));
 }
 

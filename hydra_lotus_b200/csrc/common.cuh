@@ -4,13 +4,13 @@
 //
 // The library is built with --fmad=false: every multiply and add in the
 // transport rounds separately, in the order written here, which is the
-// order of the reference's Slang source. Explicit __fmaf_rn is used only
-// where the rounding cannot change a result (the BVH's conservative slab
-// tests).
+// order of the reference's Slang source.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
+
+#include "lmath.cuh"
 
 namespace lotus {
 
@@ -98,7 +98,9 @@ __device__ __forceinline__ float power_heuristic(float chosen, float other) {
 __device__ __forceinline__ F3 sample_cosine_hemisphere(float ux, float uy) {
   const float radius = sqrtf(ux);
   const float phi = 2.0f * kPi * uy;
-  return V(radius * cosf(phi), radius * sinf(phi), sqrtf(fmaxf(0.0f, 1.0f - ux)));
+  float s, c;
+  lsincos(phi, s, c);
+  return V(radius * c, radius * s, sqrtf(fmaxf(0.0f, 1.0f - ux)));
 }
 
 // Waechter and Binder's self-intersection offset (Ray Tracing Gems 2019),

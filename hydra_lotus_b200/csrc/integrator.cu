@@ -198,9 +198,11 @@ __device__ __forceinline__ double4 add4(double4 a, float4 s) {
 // The reference integrator: one thread follows one camera path to its end
 // (path_trace.slang:279-287, 353-385), then adds it to the pixel's FP64
 // accumulation and writes the mean.
+template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
     const FrameConst* __restrict__ fcp, double4* __restrict__ accum, float4* __restrict__ color,
-    RayTotals* totals) {
+    RayTotals* totals, VisitCounters* visits) {
+  TraversalCounters vc[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
   const FrameConst& f = *fcp;
   const uint32_t rect[4] = {f.rect[0], f.rect[1], f.rect[2], f.rect[3]};
   uint32_t px, py;
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
       start_path(f, px, py, f.sample_index, o, d, tmax, rng);
       ++n_camera;
       Hit hit;
-      if (trace_closest(S, o, d, 0.0f, tmax, rng, hit)) {
+      if (trace_closest<kCount>(S, o, d, 0.0f, tmax, rng, hit, &vc[0])) {
         F3 T = V(1.0f), R = V(0.0f);
         float last_pdf = 0.0f;
         uint32_t flags = 0;
@@ -228,14 +230,14 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
               last_pdf, flags, rng, no, nd, req);
           if (req.pending) {
             ++n_shadow;
-            const float tr = trace_shadow(S, req.origin, req.direction, 0.0f, req.tmax);
+            const float tr = trace_shadow<kCount>(S, req.origin, req.direction, 0.0f, req.tmax, &vc[2]);
             if (tr > 0.0f) R = R + req.throughput * shadow_contribution(req.fl, req.weight, req.pdf, tr);
           }
           if (!cont) break;
           o = no;
           d = nd;
           ++n_extension;
-          if (!trace_closest(S, o, d, 0.0f, kFloatMax, rng, hit)) {
+          if (!trace_closest<kCount>(S, o, d, 0.0f, kFloatMax, rng, hit, &vc[1])) {
             R = R + T * miss_radiance(S, f, d, flags, last_pdf);
             break;
           }
@@ -249,6 +251,15 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
   warp_add64(&totals->camera, n_camera);
   warp_add64(&totals->extension, n_extension);
   warp_add64(&totals->shadow, n_shadow);
+  if (kCount) {
+    const uint32_t rays[3] = {n_camera, n_extension, n_shadow};
+    for (int k = 0; k < 3; ++k) {
+      warp_add64(&visits->rays[k], rays[k]);
+      warp_add64(&visits->nodes[k], vc[k].nodes);
+      warp_add64(&visits->triangles[k], vc[k].triangles);
+      warp_add64(&visits->instances[k], vc[k].instances);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -256,8 +267,10 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
 
 // Camera (wavefront.slang:206-225): starts each pixel's path and traces its
 // camera ray; a hit is queued for shading at bounce 0.
+template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
-    const FrameConst* __restrict__ fcp, PathState P, Queues Q) {
+    const FrameConst* __restrict__ fcp, PathState P, Queues Q, VisitCounters* visits) {
+  TraversalCounters vc = {0, 0, 0};
   const FrameConst& f = *fcp;
   if (!f.add_sample) return;
   const uint32_t rect[4] = {f.rect[0], f.rect[1], f.rect[2], f.rect[3]};
@@ -273,7 +286,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
     uint32_t rng;
     start_path(f, px, py, f.sample_index, o, d, tmax, rng);
     Hit hit;
-    found = trace_closest(S, o, d, 0.0f, tmax, rng, hit);
+    found = trace_closest<kCount>(S, o, d, 0.0f, tmax, rng, hit, &vc);
     if (found) {
       P.direction[slot] = F4(d, tmax);
       P.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng));
@@ -284,6 +297,12 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
   }
   const uint32_t at = warp_append(&Q.counts[1], found);
   if (found) Q.hit[at] = slot;
+  if (kCount) {
+    warp_add64(&visits->rays[0], valid ? 1u : 0u);
+    warp_add64(&visits->nodes[0], vc.nodes);
+    warp_add64(&visits->triangles[0], vc.triangles);
+    warp_add64(&visits->instances[0], vc.instances);
+  }
 }
 
 // Shade (wavefront.slang:264-285) with next event estimation's shadow ray
@@ -342,10 +361,24 @@ __global__ void __launch_bounds__(kBlock) k_wf_shade(SceneView S,
 
 // The shadow rays of bounce `bounce`: ShadowTransmittance and the rest of
 // ShadowedLight, added to the path's radiance.
+template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_wf_shadow(SceneView S, PathState P, Queues Q,
-    uint32_t bounce) {
+    uint32_t bounce, VisitCounters* visits) {
   const uint32_t n = Q.counts[3 * bounce + 2];
   const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blockIdx.x * blockDim.x >= n) return;
+  if (kCount) {
+    TraversalCounters vc = {0, 0, 0};
+    if (index < n) {
+      const float4 ro = Q.shadow.ray_o[index];
+      const float4 rd = Q.shadow.ray_d[index];
+      trace_shadow<true>(S, V(ro), V(rd), 0.0f, ro.w, &vc);
+    }
+    warp_add64(&visits->rays[2], index < n ? 1u : 0u);
+    warp_add64(&visits->nodes[2], vc.nodes);
+    warp_add64(&visits->triangles[2], vc.triangles);
+    warp_add64(&visits->instances[2], vc.instances);
+  }
   if (index >= n) return;
   const float4 ro = Q.shadow.ray_o[index];
   const float4 rd = Q.shadow.ray_d[index];
@@ -366,8 +399,11 @@ __global__ void __launch_bounds__(kBlock) k_wf_shadow(SceneView S, PathState P, 
 
 // Intersect (wavefront.slang:230-262): a hit is queued for shading; a miss
 // ends the path with the environment.
+template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_wf_extend(SceneView S,
-    const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce) {
+    const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce,
+    VisitCounters* visits) {
+  TraversalCounters vc = {0, 0, 0};
   const uint32_t n = Q.counts[3 * bounce];
   if (blockIdx.x * blockDim.x >= n) return;
   const FrameConst& f = *fcp;
@@ -382,7 +418,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_extend(SceneView S,
     float4 rad = P.radiance[slot];
     uint32_t rng = __float_as_uint(rad.w);
     Hit hit;
-    found = trace_closest(S, V(o), V(d), o.w, d.w, rng, hit);
+    found = trace_closest<kCount>(S, V(o), V(d), o.w, d.w, rng, hit, &vc);
     if (found) {
       P.hit[slot] = make_uint4(hit.instance, hit.tri, __float_as_uint(hit.b1), __float_as_uint(hit.b2));
       if (rng != __float_as_uint(rad.w)) {
@@ -398,6 +434,12 @@ __global__ void __launch_bounds__(kBlock) k_wf_extend(SceneView S,
   }
   const uint32_t at = warp_append(&Q.counts[3 * bounce + 1], found);
   if (found) Q.hit[at] = slot;
+  if (kCount) {
+    warp_add64(&visits->rays[1], valid ? 1u : 0u);
+    warp_add64(&visits->nodes[1], vc.nodes);
+    warp_add64(&visits->triangles[1], vc.triangles);
+    warp_add64(&visits->instances[1], vc.instances);
+  }
 }
 
 // Resolve (path_trace.slang:353-385): adds each ended path's sample to its
@@ -449,30 +491,78 @@ __global__ void k_fill(float4* color, uint32_t n, float4 v) {
 
 }  // namespace
 
+namespace {
+
+// Records an event pair around one launch when profiling.
+struct Timed {
+  SampleProfile* p;
+  cudaStream_t s;
+  int slot = -1;
+  Timed(SampleProfile* profile, cudaStream_t stream, int kind) : p(profile), s(stream) {
+    if (p && p->events && p->count < p->capacity) {
+      slot = p->count++;
+      p->kinds[slot] = kind;
+      cudaEventRecord(p->events[2 * slot], s);
+    }
+  }
+  ~Timed() {
+    if (slot >= 0) cudaEventRecord(p->events[2 * slot + 1], s);
+  }
+};
+
+}  // namespace
+
 void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
-    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream) {
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
+    SampleProfile* profile) {
   const uint32_t threads = tile_threads(rect);
   if (threads == 0) return;
-  k_reference_pt<<<(threads + kBlock - 1) / kBlock, kBlock, 0, stream>>>(S, fc, accum, color, totals);
+  const uint32_t grid = (threads + kBlock - 1) / kBlock;
+  Timed t(profile, stream, 0);
+  if (profile && profile->visits)
+    k_reference_pt<true><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
+  else
+    k_reference_pt<false><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, nullptr);
 }
 
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
-    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream) {
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
+    SampleProfile* profile) {
   (void)width;
   (void)height;
   const uint32_t threads = tile_threads(rect);
   if (threads == 0) return;
+  const bool count = profile && profile->visits;
+  VisitCounters* visits = profile ? profile->visits : nullptr;
   cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * 3 * (size_t)(max_bounces + 2), stream);
   const uint32_t grid_pixels = (threads + kBlock - 1) / kBlock;
   const uint32_t grid_queue = (Q.capacity + kBlock - 1) / kBlock;
-  k_wf_camera<<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q);
-  for (uint32_t b = 0; b <= max_bounces; ++b) {
-    if (b != 0) k_wf_extend<<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b);
-    k_wf_shade<<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b);
-    k_wf_shadow<<<grid_queue, kBlock, 0, stream>>>(S, P, Q, b);
+  {
+    Timed t(profile, stream, 0);
+    if (count) k_wf_camera<true><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, visits);
+    else k_wf_camera<false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, nullptr);
   }
-  k_wf_resolve<<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, accum, color);
+  for (uint32_t b = 0; b <= max_bounces; ++b) {
+    if (b != 0) {
+      Timed t(profile, stream, 1);
+      if (count) k_wf_extend<true><<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b, visits);
+      else k_wf_extend<false><<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b, nullptr);
+    }
+    {
+      Timed t(profile, stream, 2);
+      k_wf_shade<<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b);
+    }
+    {
+      Timed t(profile, stream, 3);
+      if (count) k_wf_shadow<true><<<grid_queue, kBlock, 0, stream>>>(S, P, Q, b, visits);
+      else k_wf_shadow<false><<<grid_queue, kBlock, 0, stream>>>(S, P, Q, b, nullptr);
+    }
+  }
+  {
+    Timed t(profile, stream, 4);
+    k_wf_resolve<<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, accum, color);
+  }
   k_wf_finish<<<1, 32, 0, stream>>>(const_cast<FrameConst*>(fc), Q.counts, max_bounces, totals);
 }
 

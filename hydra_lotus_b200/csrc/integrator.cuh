@@ -46,12 +46,34 @@ struct RayTotals {
   unsigned long long error;  // traversal or bookkeeping errors
 };
 
+// BVH visits by ray kind (camera, extension, shadow), for roofline
+// accounting.
+struct VisitCounters {
+  unsigned long long rays[3];
+  unsigned long long nodes[3];
+  unsigned long long triangles[3];
+  unsigned long long instances[3];
+};
+
+// Optional per-sample instrumentation: events around each kernel (its
+// class in `kinds`: 0 camera, 1 extend, 2 shade, 3 shadow, 4 resolve) and
+// visit counting variants of the tracing kernels.
+struct SampleProfile {
+  cudaEvent_t* events = nullptr;  // 2 per timed launch
+  int* kinds = nullptr;
+  int capacity = 0;               // timed launches that fit
+  int count = 0;
+  VisitCounters* visits = nullptr;  // non-null: count visits
+};
+
 void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
-    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream);
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
+    SampleProfile* profile = nullptr);
 
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
-    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream);
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
+    SampleProfile* profile = nullptr);
 
 void launch_advance(FrameConst* fc, cudaStream_t stream);
 

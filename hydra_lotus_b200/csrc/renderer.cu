@@ -380,6 +380,10 @@ struct Renderer {
   DeviceArray<float4> sq_o, sq_d, sq_fl, sq_thr;
   DeviceArray<FrameConst> frame_const;
   DeviceArray<RayTotals> totals;
+  DeviceArray<VisitCounters> visits;
+  // Profiling events, created on first use.
+  std::vector<cudaEvent_t> profile_events;
+  std::vector<int> profile_kinds;
 
   // Accumulation key (vulkan_backend.cpp:414-431).
   struct Key {
@@ -406,6 +410,7 @@ struct Renderer {
   } graph_key{};
 
   ~Renderer() {
+    for (cudaEvent_t e : profile_events) cudaEventDestroy(e);
     if (graph) cudaGraphExecDestroy(graph);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
@@ -840,9 +845,43 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   Q.shadow = ShadowQueue{R.sq_o.ptr, R.sq_d.ptr, R.sq_fl.ptr, R.sq_thr.ptr};
   Q.counts = R.counts.ptr;
   Q.capacity = t.width * t.height;
+  const bool want_timings = (d.flags & LOTUS_FRAME_TIMINGS) != 0;
+  const bool want_visits = (d.flags & LOTUS_FRAME_COUNT_VISITS) != 0;
+  SampleProfile profile;
+  if (want_timings || want_visits) {
+    const int capacity = 512;
+    if (want_timings && R.profile_events.size() < 2 * (size_t)capacity) {
+      while (R.profile_events.size() < 2 * (size_t)capacity) {
+        cudaEvent_t e;
+        if (!R.ok(cudaEventCreate(&e), "profiling event", detail)) return poison(detail);
+        R.profile_events.push_back(e);
+      }
+    }
+    R.profile_kinds.assign(capacity, 0);
+    if (want_timings) {
+      profile.events = R.profile_events.data();
+      profile.kinds = R.profile_kinds.data();
+      profile.capacity = capacity;
+    }
+    if (want_visits) {
+      if (!R.ok(R.visits.resize(1), "visit counters", detail) ||
+          !R.ok(cudaMemsetAsync(R.visits.ptr, 0, sizeof(VisitCounters), s), "visit counters", detail))
+        return poison(detail);
+      profile.visits = R.visits.ptr;
+    }
+  }
   cudaEventRecord(R.ev_start, s);
   for (uint32_t k = 0; k < submissions; ++k) {
-    if (wavefront) {
+    const bool profiled = (want_timings || want_visits) && k + 1 == submissions;
+    if (profiled) {
+      if (wavefront)
+        launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
+            R.accum.ptr, R.color.ptr, R.totals.ptr, s, &profile);
+      else
+        launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s,
+            &profile);
+      launch_advance(R.frame_const.ptr, s);
+    } else if (wavefront) {
       Renderer::GraphKey gk{};
       gk.scene_generation = R.scene_generation;
       gk.width = t.width;
@@ -880,6 +919,35 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   if (!R.ok(cudaStreamSynchronize(s), "render", detail)) return poison(detail);
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
+  if (want_timings) {
+    double by_kind[5] = {0, 0, 0, 0, 0};
+    uint32_t launches[5] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < profile.count; ++i) {
+      float kms = 0.0f;
+      cudaEventElapsedTime(&kms, R.profile_events[2 * i], R.profile_events[2 * i + 1]);
+      by_kind[R.profile_kinds[i]] += kms;
+      ++launches[R.profile_kinds[i]];
+    }
+    res.timings_available = 1;
+    res.camera_gpu_ms = by_kind[0];
+    res.extend_gpu_ms = by_kind[1];
+    res.shade_gpu_ms = by_kind[2];
+    res.shadow_gpu_ms = by_kind[3];
+    res.resolve_gpu_ms = by_kind[4];
+    res.extend_launches = launches[1];
+    res.shadow_launches = launches[3];
+  }
+  if (want_visits) {
+    VisitCounters v{};
+    if (!R.ok(cudaMemcpy(&v, R.visits.ptr, sizeof(v), cudaMemcpyDeviceToHost), "visit counters", detail))
+      return poison(detail);
+    for (int k = 0; k < 3; ++k) {
+      res.visit_rays[k] = v.rays[k];
+      res.node_visits[k] = v.nodes[k];
+      res.triangle_visits[k] = v.triangles[k];
+      res.instance_visits[k] = v.instances[k];
+    }
+  }
   R.accumulated += to_add;
   R.completion += submissions;
   if (t.read_back && color_out) {

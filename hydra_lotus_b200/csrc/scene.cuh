@@ -186,24 +186,25 @@ __device__ __forceinline__ bool intersect_triangle(const WatertightRay& r, F3 v0
   return true;
 }
 
-// Slab test of a node's two children against [tmin, tmax]. Uses fused
-// multiply-adds on (box - origin) * inverse; the margin on the far
-// distance keeps the test conservative for every hit the watertight
-// triangle test can report.
-__device__ __forceinline__ void test_children(const BvhNode& n, F3 oi, F3 inv, float tmin,
+// Slab test of a node's two children against [tmin, tmax]. The far
+// distance gets a relative margin of 2^-18 (the clamp to tmax included), so
+// a box is never culled where the triangle test, whose distances carry
+// their own rounding, could still accept a hit: hits are decided by
+// triangle tests alone, whatever the BVH's shape.
+__device__ __forceinline__ void test_children(const BvhNode& n, F3 o, F3 inv, float tmin,
     float tmax, bool& hit0, bool& hit1, float& near0, float& near1) {
-  const float x0 = __fmaf_rn(n.x.x, inv.x, -oi.x), x1 = __fmaf_rn(n.x.y, inv.x, -oi.x);
-  const float y0 = __fmaf_rn(n.y.x, inv.y, -oi.y), y1 = __fmaf_rn(n.y.y, inv.y, -oi.y);
-  const float z0 = __fmaf_rn(n.z.x, inv.z, -oi.z), z1 = __fmaf_rn(n.z.y, inv.z, -oi.z);
-  const float X0 = __fmaf_rn(n.x.z, inv.x, -oi.x), X1 = __fmaf_rn(n.x.w, inv.x, -oi.x);
-  const float Y0 = __fmaf_rn(n.y.z, inv.y, -oi.y), Y1 = __fmaf_rn(n.y.w, inv.y, -oi.y);
-  const float Z0 = __fmaf_rn(n.z.z, inv.z, -oi.z), Z1 = __fmaf_rn(n.z.w, inv.z, -oi.z);
+  const float x0 = (n.x.x - o.x) * inv.x, x1 = (n.x.y - o.x) * inv.x;
+  const float y0 = (n.y.x - o.y) * inv.y, y1 = (n.y.y - o.y) * inv.y;
+  const float z0 = (n.z.x - o.z) * inv.z, z1 = (n.z.y - o.z) * inv.z;
+  const float X0 = (n.x.z - o.x) * inv.x, X1 = (n.x.w - o.x) * inv.x;
+  const float Y0 = (n.y.z - o.y) * inv.y, Y1 = (n.y.w - o.y) * inv.y;
+  const float Z0 = (n.z.z - o.z) * inv.z, Z1 = (n.z.w - o.z) * inv.z;
   const float tn0 = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
   const float tf0 = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
   const float tn1 = fmaxf(fmaxf(fminf(X0, X1), fminf(Y0, Y1)), fmaxf(fminf(Z0, Z1), tmin));
   const float tf1 = fminf(fminf(fmaxf(X0, X1), fmaxf(Y0, Y1)), fminf(fmaxf(Z0, Z1), tmax));
-  hit0 = tn0 <= tf0 * 1.0000004f && n.c.x != kEmptyChild;
-  hit1 = tn1 <= tf1 * 1.0000004f && n.c.y != kEmptyChild;
+  hit0 = tn0 <= tf0 + fabsf(tf0) * 3.8146973e-6f && n.c.x != kEmptyChild;
+  hit1 = tn1 <= tf1 + fabsf(tf1) * 3.8146973e-6f && n.c.y != kEmptyChild;
   near0 = tn0;
   near1 = tn1;
 }
@@ -223,6 +224,7 @@ __device__ __forceinline__ F3 row_vector(const float4* r, F3 d) {
 struct TraversalCounters {
   uint32_t nodes;
   uint32_t triangles;
+  uint32_t instances;
 };
 
 // Walks the two-level BVH. kAnyHit: the shadow query of ShadowTransmittance
@@ -240,7 +242,6 @@ __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 dire
   int sp = 0;
   F3 o = origin, d = direction;
   F3 inv = safe_inverse(d);
-  F3 oi = o * inv;
   WatertightRay w;
   const BvhNode* __restrict__ pool = S.tlas;
   uint32_t instance = 0;
@@ -254,7 +255,7 @@ __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 dire
       if (kCount) ++counters->nodes;
       bool h0, h1;
       float t0, t1;
-      test_children(n, oi, inv, tmin, best, h0, h1, t0, t1);
+      test_children(n, o, inv, tmin, best, h0, h1, t0, t1);
       if (h0 && h1) {
         const bool first0 = t0 <= t1;
         const int32_t near_c = first0 ? n.c.x : n.c.y;
@@ -285,18 +286,17 @@ __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 dire
       o = origin;
       d = direction;
       inv = safe_inverse(d);
-      oi = o * inv;
     } else if (pool == S.tlas) {
       // A TLAS leaf: enter each instance in turn. The TLAS leaves hold one
       // instance, so `count` is 1.
       instance = (uint32_t)(~cur);
+      if (kCount) ++counters->instances;
       const InstanceTraversal rec = S.inst_trav[instance];
       if (rec.blas_root != (uint32_t)kEmptyChild && sp < kStackSize) {
         stack[sp++] = kExitInstance;
         o = row_point(rec.inv, origin);
         d = row_vector(rec.inv, direction);
         inv = safe_inverse(d);
-        oi = o * inv;
         w = prepare_ray(o, d);
         instance_opaque = (rec.flags & kInstanceOpaque) != 0;
         pool = S.blas;
@@ -351,19 +351,21 @@ __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 dire
   return kAnyHit ? transmittance : 0.0f;
 }
 
+template <bool kCount = false>
 __device__ __forceinline__ bool trace_closest(const SceneView& S, F3 o, F3 d, float tmin,
-    float tmax, uint32_t& rng, Hit& hit) {
+    float tmax, uint32_t& rng, Hit& hit, TraversalCounters* counters = nullptr) {
   bool found;
-  traverse<false, false>(S, o, d, tmin, tmax, rng, hit, found);
+  traverse<false, kCount>(S, o, d, tmin, tmax, rng, hit, found, counters);
   return found;
 }
 
+template <bool kCount = false>
 __device__ __forceinline__ float trace_shadow(const SceneView& S, F3 o, F3 d, float tmin,
-    float tmax) {
+    float tmax, TraversalCounters* counters = nullptr) {
   uint32_t rng = 0;
   Hit hit;
   bool found;
-  return traverse<true, false>(S, o, d, tmin, tmax, rng, hit, found);
+  return traverse<true, kCount>(S, o, d, tmin, tmax, rng, hit, found, counters);
 }
 
 }  // namespace lotus

@@ -156,16 +156,18 @@ __device__ __forceinline__ float sample_cumulative(const float* __restrict__ F, 
 }
 
 __device__ __forceinline__ void environment_uv(F3 local, float& u, float& v) {
-  const float uu = 0.5f - atan2f(local.x, local.z) * (0.5f / kPi);
-  v = acosf(fminf(fmaxf(local.y, -1.0f), 1.0f)) * (1.0f / kPi);
+  const float uu = 0.5f - latan2(local.x, local.z) * (0.5f / kPi);
+  v = lacos(fminf(fmaxf(local.y, -1.0f), 1.0f)) * (1.0f / kPi);
   u = uu - floorf(uu);
 }
 
 __device__ __forceinline__ F3 environment_direction(float u, float v) {
   const float theta = kPi * v;
   const float phi = kPi * (1.0f - 2.0f * u);
-  const float sin_theta = sinf(theta);
-  return V(sin_theta * sinf(phi), cosf(theta), sin_theta * cosf(phi));
+  float sin_theta, cos_theta, sin_phi, cos_phi;
+  lsincos(theta, sin_theta, cos_theta);
+  lsincos(phi, sin_phi, cos_phi);
+  return V(sin_theta * sin_phi, cos_theta, sin_theta * cos_phi);
 }
 
 // EnvironmentLookup (scene.slang:819-824): FP32 bilinear filtering,
@@ -196,7 +198,7 @@ __device__ __forceinline__ F3 environment_lookup(const SceneView& S, float u, fl
 __device__ __forceinline__ float environment_direction_pdf(const SceneView& S, float u, float v) {
   const uint32_t column = min((uint32_t)(u * float(S.env_columns)), S.env_columns - 1);
   const uint32_t row = min((uint32_t)(v * float(S.env_rows)), S.env_rows - 1);
-  const float sin_theta = sinf(kPi * v);
+  const float sin_theta = lsin(kPi * v);
   if (!(sin_theta > 0.0f)) return 0.0f;
   return S.env_floats[(uint64_t)row * S.env_columns + column] / (2.0f * kPi * kPi * sin_theta);
 }
@@ -209,7 +211,7 @@ __device__ __forceinline__ LightSample sample_environment(const SceneView& S, fl
   const float v = sample_cumulative(S.env_floats, cells, S.env_rows, ux, row);
   const float u = sample_cumulative(S.env_floats,
       cells + S.env_rows + 1 + (uint64_t)row * (S.env_columns + 1), S.env_columns, uy, column);
-  const float sin_theta = sinf(kPi * v);
+  const float sin_theta = lsin(kPi * v);
   const float density = S.env_floats[(uint64_t)row * S.env_columns + column];
   if (!(sin_theta > 0.0f) || !(density > 0.0f)) return no_light();
   const F3 local = environment_direction(u, v);

@@ -1,0 +1,46 @@
+"""Renders frames of a named workload through the C ABI, for profilers.
+
+    python -m hydra_lotus_b200.profile_frame --workload sphere-field \
+        --width 960 --height 540 --spp 1 --frames 2
+
+Prints the rays and device time of each frame. Used as the command under
+Nsight Compute: the workload's sizes are arguments so that a capture can
+run on a small case of the same kernels.
+"""
+
+import argparse
+import json
+
+from . import abi, renderer, scenes
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="sphere-field", choices=["sphere-field", "box-room"])
+    ap.add_argument("--width", type=int, default=960)
+    ap.add_argument("--height", type=int, default=540)
+    ap.add_argument("--spp", type=int, default=1)
+    ap.add_argument("--frames", type=int, default=2)
+    ap.add_argument("--depth", type=int, default=8)
+    ap.add_argument("--integrator", default="wavefront", choices=["wavefront", "reference"])
+    args = ap.parse_args()
+    if args.workload == "sphere-field":
+        scene = scenes.sphere_field(seed=0, width=args.width, height=args.height)
+    else:
+        scene = scenes.box_room(seed=0, size=args.width)
+        scene.height = args.height
+    integrator = abi.INTEGRATOR_WAVEFRONT if args.integrator == "wavefront" else abi.INTEGRATOR_REFERENCE
+    with renderer.CudaOffscreenRenderer(0) as r:
+        renderer.check(r.update_scene(scene), "update_scene")
+        for k in range(args.frames):
+            st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                                      max_bounces=args.depth, sample_index=k * args.spp)
+            res, _ = r.render_scene(scene.frame(st, frame_count=args.spp, read_back=False))
+            renderer.check(res, "render")
+            rays = res.camera_rays + res.extension_rays + res.shadow_rays
+            print(json.dumps({"frame": k, "rays": rays, "gpu_ms": round(res.gpu_ms, 3),
+                              "mrays_per_s": round(rays / res.gpu_ms / 1e3, 1)}))
+
+
+if __name__ == "__main__":
+    main()

@@ -157,6 +157,13 @@ typedef struct lotus_settings {
   uint32_t environment_background;
 } lotus_settings;
 
+/* lotus_frame_desc::flags. TIMINGS times the kernels of the call's last
+ * sample by class (the reference's WavefrontTimings, vulkan_backend.hpp:
+ * 52-68). COUNT_VISITS makes the last sample count BVH nodes, triangles and
+ * instances visited per ray kind (slower; for roofline accounting). */
+#define LOTUS_FRAME_TIMINGS 1u
+#define LOTUS_FRAME_COUNT_VISITS 2u
+
 /* One RenderScene call: DrawSummary::world_to_clip in the OpenGL clip
  * convention (extraction.hpp:23), the target and the settings. */
 typedef struct lotus_frame_desc {
@@ -164,7 +171,7 @@ typedef struct lotus_frame_desc {
   lotus_target target;
   lotus_settings settings;
   uint32_t frame_count;
-  uint32_t reserved;
+  uint32_t flags;   /* LOTUS_FRAME_* */
 } lotus_frame_desc;
 
 /* GpuFrameEvidence (vulkan_backend.hpp:202-249), in part. */
@@ -184,7 +191,22 @@ typedef struct lotus_frame_result {
    * ray queue; element 0 is the camera rays. */
   uint32_t wavefront_path_counts[LOTUS_MAX_REPORTED_BOUNCES];
   uint32_t wavefront_path_count_size;
-  uint32_t reserved;
+  /* With LOTUS_FRAME_TIMINGS: device time of the last sample's kernels, by
+   * class (wavefront integrator; the megakernel reports camera_gpu_ms). */
+  uint32_t timings_available;
+  double camera_gpu_ms;
+  double extend_gpu_ms;
+  double shade_gpu_ms;
+  double shadow_gpu_ms;
+  double resolve_gpu_ms;
+  uint32_t extend_launches;
+  uint32_t shadow_launches;
+  /* With LOTUS_FRAME_COUNT_VISITS: the last sample's visits, indexed
+   * camera, extension, shadow; rays[k] is the ray count they cover. */
+  uint64_t visit_rays[3];
+  uint64_t node_visits[3];
+  uint64_t triangle_visits[3];
+  uint64_t instance_visits[3];
   char detail[256];
 } lotus_frame_result;
 

@@ -84,6 +84,85 @@ inline uint32_t AsUint(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; 
 inline float AsFloat(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
 
 // ---------------------------------------------------------------------------
+// Elementary functions. The reference leaves sin, cos, atan2, acos and pow
+// to Slang, whose SPIR-V precision is implementation-defined; the CUDA
+// kernels use the project's own (Cody-Waite reduction and Taylor
+// polynomials, at most 4 ulp from the exact values), and the oracle
+// evaluates the same operations in the same order, so both agree bit for
+// bit.
+
+inline void lsincos(float x, float& s, float& c) {
+  const float k = std::rint(x * 0.636619772f);
+  const float r = ((x - k * 1.5703125f) - k * 4.837512969970703e-4f) - k * 7.549790126404332e-8f;
+  const float r2 = r * r;
+  const float sp = r + r * r2 * (-0.16666667f + r2 * (8.3333338e-3f + r2 * (-1.9841270e-4f +
+      r2 * 2.7557319e-6f)));
+  const float cp = 1.0f + r2 * (-0.5f + r2 * (4.1666668e-2f + r2 * (-1.3888889e-3f +
+      r2 * (2.4801588e-5f + r2 * -2.7557320e-7f))));
+  const int q = ((int)k) & 3;
+  if (q == 0) {
+    s = sp;
+    c = cp;
+  } else if (q == 1) {
+    s = cp;
+    c = -sp;
+  } else if (q == 2) {
+    s = -sp;
+    c = -cp;
+  } else {
+    s = -cp;
+    c = sp;
+  }
+}
+
+inline float lsin(float x) {
+  float s, c;
+  lsincos(x, s, c);
+  return s;
+}
+
+inline float lcos(float x) {
+  float s, c;
+  lsincos(x, s, c);
+  return c;
+}
+
+// atan(a) for a in [0, 1].
+inline float latan_unit(float a) {
+  float t = a, base = 0.0f;
+  if (a > 0.41421357f) {
+    t = (a - 1.0f) / (a + 1.0f);
+    base = 0.78539819f;
+  }
+  const float t2 = t * t;
+  const float p = 1.0f + t2 * (-0.33333334f + t2 * (0.2f + t2 * (-0.14285715f + t2 * (0.11111111f +
+      t2 * (-0.09090909f + t2 * (0.07692308f + t2 * (-0.06666667f + t2 * (0.05882353f +
+      t2 * (-0.05263158f + t2 * 0.04761905f)))))))));
+  return base + t * p;
+}
+
+inline float latan2(float y, float x) {
+  const float ax = std::fabs(x), ay = std::fabs(y);
+  const float mx = ax > ay ? ax : ay;
+  const float mn = ax > ay ? ay : ax;
+  if (mx == 0.0f) return x < 0.0f ? (y < 0.0f ? -3.14159274f : 3.14159274f) : 0.0f;
+  float r = latan_unit(mn / mx);
+  if (ay > ax) r = 1.57079637f - r;
+  if (x < 0.0f) r = 3.14159274f - r;
+  return y < 0.0f ? -r : r;
+}
+
+// For x in [-1, 1].
+inline float lacos(float x) { return latan2(std::sqrt((1.0f - x) * (1.0f + x)), x); }
+
+// pow(x, 5) as products.
+inline float lpow5(float x) {
+  const float x2 = x * x;
+  return x2 * x2 * x;
+}
+
+
+// ---------------------------------------------------------------------------
 // sampling.slang
 
 // PcgHash (sampling.slang:9-13).
@@ -135,8 +214,9 @@ inline float PowerHeuristic(float chosen, float other) {
 inline F3 SampleCosineHemisphere(float ux, float uy) {
   const float radius = std::sqrt(ux);
   const float phi = 2.0f * kPi * uy;
-  return V(radius * std::cos(phi), radius * std::sin(phi),
-      std::sqrt(std::fmax(0.0f, 1.0f - ux)));
+  float s, c;
+  lsincos(phi, s, c);
+  return V(radius * c, radius * s, std::sqrt(std::fmax(0.0f, 1.0f - ux)));
 }
 
 // ---------------------------------------------------------------------------
@@ -185,7 +265,7 @@ PreviewClosure MakePreviewClosure(F3 base_color, float roughness, float metallic
 
 // FresnelSchlick (preview.slang:92-95).
 inline F3 FresnelSchlick(F3 f0, float f90, float cos_theta) {
-  const float weight = std::pow(saturate(1.0f - cos_theta), 5.0f);
+  const float weight = lpow5(saturate(1.0f - cos_theta));
   return f0 * (1.0f - weight) + V(f90 * weight);
 }
 
@@ -240,7 +320,9 @@ inline F3 SampleGgxVisibleNormal(F3 wo, float alpha, float ux, float uy) {
   const float phi = 2.0f * kPi * ux;
   const float z = (1.0f - uy) * (1.0f + wo_std.z) - wo_std.z;
   const float sin_theta = std::sqrt(saturate(1.0f - z * z));
-  const F3 h_std = V(sin_theta * std::cos(phi), sin_theta * std::sin(phi), z) + wo_std;
+  float sp, cp;
+  lsincos(phi, sp, cp);
+  const F3 h_std = V(sin_theta * cp, sin_theta * sp, z) + wo_std;
   return normalize(V(h_std.x * alpha, h_std.y * alpha, h_std.z));
 }
 
@@ -932,22 +1014,22 @@ inline bool IntersectTriangle(const WatertightRay& r, F3 v0, F3 v1, F3 v2,
   return true;
 }
 
-// Whether the segment [tmin, tmax] meets the box; conservative by the
-// relative margin of Pharr et al. (PBR 3rd ed., section 3.9.2).
+// Whether the segment [tmin, tmax] meets the box. The far distance gets a
+// relative margin of 2^-18, so that a box is never culled where the
+// triangle test (whose distances carry their own rounding) could still
+// accept a hit: only triangle tests decide hits, whatever the BVH.
 inline bool OverlapsBox(const Box& b, F3 org, F3 inv, float tmin, float tmax) {
-  float t0 = tmin, t1 = tmax;
   const float o[3] = {org.x, org.y, org.z};
   const float d[3] = {inv.x, inv.y, inv.z};
+  float t0 = tmin, t1 = tmax;
   for (int a = 0; a < 3; ++a) {
     float tn = (b.lo[a] - o[a]) * d[a];
     float tf = (b.hi[a] - o[a]) * d[a];
     if (tn > tf) std::swap(tn, tf);
-    tf *= 1.0000004f;
     t0 = tn > t0 ? tn : t0;
     t1 = tf < t1 ? tf : t1;
-    if (t0 > t1) return false;
   }
-  return true;
+  return t0 <= t1 + std::fabs(t1) * 3.8146973e-6f;
 }
 
 inline F3 Inverse(F3 d) {
@@ -1247,8 +1329,8 @@ float SampleCumulative(const oracle_scene& s, uint64_t first, uint32_t count, fl
 
 // EnvironmentUv (scene.slang:805-809).
 inline void EnvironmentUv(F3 local, float& u, float& v) {
-  const float uu = 0.5f - std::atan2(local.x, local.z) * (0.5f / kPi);
-  v = std::acos(std::fmin(std::fmax(local.y, -1.0f), 1.0f)) * (1.0f / kPi);
+  const float uu = 0.5f - latan2(local.x, local.z) * (0.5f / kPi);
+  v = lacos(std::fmin(std::fmax(local.y, -1.0f), 1.0f)) * (1.0f / kPi);
   u = uu - std::floor(uu);
 }
 
@@ -1256,8 +1338,10 @@ inline void EnvironmentUv(F3 local, float& u, float& v) {
 inline F3 EnvironmentDirection(float u, float v) {
   const float theta = kPi * v;
   const float phi = kPi * (1.0f - 2.0f * u);
-  const float sin_theta = std::sin(theta);
-  return V(sin_theta * std::sin(phi), std::cos(theta), sin_theta * std::cos(phi));
+  float sin_theta, cos_theta, sin_phi, cos_phi;
+  lsincos(theta, sin_theta, cos_theta);
+  lsincos(phi, sin_phi, cos_phi);
+  return V(sin_theta * sin_phi, cos_theta, sin_theta * cos_phi);
 }
 
 // EnvironmentLookup (scene.slang:819-824): the bilinear texel, repeating
@@ -1293,7 +1377,7 @@ F3 EnvironmentLookup(const oracle_scene& s, float u, float v) {
 float EnvironmentDirectionPdf(const oracle_scene& s, float u, float v) {
   const uint32_t column = std::min(static_cast<uint32_t>(u * float(s.env.columns)), s.env.columns - 1);
   const uint32_t row = std::min(static_cast<uint32_t>(v * float(s.env.rows_count)), s.env.rows_count - 1);
-  const float sin_theta = std::sin(kPi * v);
+  const float sin_theta = lsin(kPi * v);
   if (!(sin_theta > 0.0f)) return 0.0f;
   return EnvFloat(s, uint64_t(row) * s.env.columns + column) / (2.0f * kPi * kPi * sin_theta);
 }
@@ -1306,7 +1390,7 @@ LightSample SampleEnvironment(const oracle_scene& s, float selection, float ux, 
   const float v = SampleCumulative(s, cells, e.rows_count, ux, row);
   const float u = SampleCumulative(s, cells + e.rows_count + 1 + uint64_t(row) * (e.columns + 1),
       e.columns, uy, column);
-  const float sin_theta = std::sin(kPi * v);
+  const float sin_theta = lsin(kPi * v);
   const float density = EnvFloat(s, uint64_t(row) * e.columns + column);
   if (!(sin_theta > 0.0f) || !(density > 0.0f)) return NoLight();
   const F3 local = EnvironmentDirection(u, v);
