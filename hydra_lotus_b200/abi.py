@@ -23,6 +23,8 @@ LIGHT_SAMPLING_RESTIR_INITIAL = 2
 MAX_BOUNCES = 1024
 MAX_REPORTED_BOUNCES = 64
 
+STATIC_MAX_PIXELS = 65536
+
 FRAME_TIMINGS = 1
 FRAME_COUNT_VISITS = 2
 

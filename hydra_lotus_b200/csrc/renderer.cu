@@ -17,6 +17,7 @@
 #include "../../include/lotus_cuda.h"
 #include "bvh_build.cuh"
 #include "integrator.cuh"
+#include "renderer_internal.cuh"
 
 namespace lotus {
 namespace {
@@ -1119,3 +1120,88 @@ int64_t lotus_cuda_read_light_table(lotus_cuda_renderer* r, uint32_t* records, u
 }
 
 }  // extern "C"
+
+namespace lotus {
+
+bool renderer_access(lotus_cuda_renderer* r, RendererAccess& out, std::string& detail) {
+  Renderer& R = r->r;
+  if (!R.failure.empty()) {
+    detail = "the renderer failed earlier: " + R.failure;
+    return false;
+  }
+  if (!R.scene_ready) {
+    detail = "no scene has been uploaded";
+    return false;
+  }
+  out.device = R.device;
+  out.stream = R.stream;
+  out.view = &R.view;
+  return true;
+}
+
+bool make_frame_constants(const lotus_frame_desc& d, FrameConst& fc, uint32_t rect[4],
+    std::string& detail) {
+  const lotus_settings& st = d.settings;
+  const lotus_target& t = d.target;
+  if (t.width == 0 || t.height == 0) {
+    detail = "the offscreen target is empty";
+    return false;
+  }
+  for (int k = 0; k < 4; ++k)
+    if (!std::isfinite(t.clear_color[k])) {
+      detail = "invalid offscreen clear values";
+      return false;
+    }
+  if (st.integrator > LOTUS_INTEGRATOR_WAVEFRONT || st.light_sampling > LOTUS_LIGHT_SAMPLING_MIS) {
+    detail = "unsupported integrator or light sampling";
+    return false;
+  }
+  if (st.max_bounces > LOTUS_MAX_BOUNCES) {
+    detail = "max_bounces exceeds " + std::to_string(LOTUS_MAX_BOUNCES);
+    return false;
+  }
+  float vulkan[16];
+  std::memcpy(vulkan, d.world_to_clip, sizeof(vulkan));
+  for (int c = 0; c < 4; ++c) {
+    const float z = d.world_to_clip[c * 4 + 2], w = d.world_to_clip[c * 4 + 3];
+    vulkan[c * 4 + 1] = -d.world_to_clip[c * 4 + 1];
+    vulkan[c * 4 + 2] = 0.5f * (z + w);
+  }
+  fc = FrameConst{};
+  if (!invert4(vulkan, fc.clip_to_world)) {
+    detail = "ray-query camera is singular or non-finite";
+    return false;
+  }
+  float vx = 0.0f, vy = 0.0f, vw = (float)t.width, vh = (float)t.height;
+  if (t.display_window[2] > 0.0f && t.display_window[3] > 0.0f) {
+    vx = t.display_window[0]; vy = t.display_window[1]; vw = t.display_window[2]; vh = t.display_window[3];
+  }
+  fc.ndc[0] = 2.0f / vw;
+  fc.ndc[1] = 2.0f / vh;
+  fc.ndc[2] = -2.0f * vx / vw - 1.0f;
+  fc.ndc[3] = -2.0f * vy / vh - 1.0f;
+  rect[0] = 0; rect[1] = 0; rect[2] = t.width; rect[3] = t.height;
+  if (t.data_window[2] > 0 && t.data_window[3] > 0) {
+    const int64_t x0 = std::max<int64_t>(t.data_window[0], 0), y0 = std::max<int64_t>(t.data_window[1], 0);
+    const int64_t x1 = std::min<int64_t>((int64_t)t.data_window[0] + t.data_window[2], t.width);
+    const int64_t y1 = std::min<int64_t>((int64_t)t.data_window[1] + t.data_window[3], t.height);
+    if (x1 <= x0 || y1 <= y0) {
+      rect[0] = rect[1] = rect[2] = rect[3] = 0;
+    } else {
+      rect[0] = (uint32_t)x0; rect[1] = (uint32_t)y0;
+      rect[2] = (uint32_t)(x1 - x0); rect[3] = (uint32_t)(y1 - y0);
+    }
+  }
+  for (int k = 0; k < 4; ++k) {
+    fc.rect[k] = rect[k];
+    fc.background[k] = t.clear_color[k];
+  }
+  fc.width = t.width;
+  fc.height = t.height;
+  fc.max_bounces = st.max_bounces;
+  fc.sample_lights = st.light_sampling != LOTUS_LIGHT_SAMPLING_BSDF ? 1u : 0u;
+  fc.environment_background = st.environment_background ? 1u : 0u;
+  return true;
+}
+
+}  // namespace lotus

@@ -1,0 +1,28 @@
+// SPDX-License-Identifier: Apache-2.0
+// Internal access to a renderer for the library's other entry points.
+#pragma once
+
+#include <string>
+
+#include "../../include/lotus_cuda.h"
+#include "integrator.cuh"
+
+namespace lotus {
+
+struct RendererAccess {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  const SceneView* view = nullptr;
+};
+
+// The renderer's device, stream and resident scene; false (with the
+// reason) when it has failed earlier or holds no scene.
+bool renderer_access(lotus_cuda_renderer* r, RendererAccess& out, std::string& detail);
+
+// Validates a frame's target, settings and camera as RenderScene does and
+// fills its constants and data window. sample_index, accumulated and
+// add_sample are left for the caller.
+bool make_frame_constants(const lotus_frame_desc& d, FrameConst& fc, uint32_t rect[4],
+    std::string& detail);
+
+}  // namespace lotus

@@ -51,6 +51,9 @@ def lib():
         L.lotus_cuda_read_color.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
         L.lotus_cuda_stream.restype = C.c_void_p
         L.lotus_cuda_stream.argtypes = [C.c_void_p]
+        L.lotus_cuda_render_static.restype = C.c_int32
+        L.lotus_cuda_render_static.argtypes = [C.c_void_p, C.POINTER(abi.FrameDesc), C.c_void_p,
+                                               C.POINTER(abi.FrameResult)]
         L.lotus_cuda_read_light_table.restype = C.c_int64
         L.lotus_cuda_read_light_table.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64,
                                                   C.c_void_p, C.c_uint64]
@@ -132,6 +135,15 @@ class CudaOffscreenRenderer:
             ptr = color.ctypes.data
         lib().lotus_cuda_render(self.handle, C.byref(frame), C.byref(res), ptr)
         return res, (color if frame.target.read_back else None)
+
+    def render_static(self, frame, color_device_ptr):
+        """lotus_cuda_render_static: renders `frame` into caller-owned device
+        memory (an integer device pointer to width*height*4 floats) without
+        allocating. Returns the lotus_frame_result."""
+        res = abi.FrameResult()
+        lib().lotus_cuda_render_static(self.handle, C.byref(frame), C.c_void_p(color_device_ptr),
+                                       C.byref(res))
+        return res
 
     def read_color(self, out):
         rc = lib().lotus_cuda_read_color(self.handle, out.ctypes.data, out.size)

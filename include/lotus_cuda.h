@@ -264,6 +264,34 @@ int64_t lotus_cuda_read_light_table(lotus_cuda_renderer* renderer,
     uint32_t* records, uint64_t record_capacity, uint32_t* offsets,
     uint64_t offset_capacity);
 
+/* The most pixels lotus_cuda_render_static renders. */
+#define LOTUS_STATIC_MAX_PIXELS 65536u
+
+/* Renders a frame without allocating device memory. No counterpart in the
+ * reference: its Vulkan renderer always allocates its own targets.
+ *
+ * For hosts that cannot call cudaMalloc when they want a frame: a delegate
+ * inside another framework's frame loop that owns every allocation, or a
+ * real-time caller that must not block in the allocator. The frame's
+ * scratch (path state, queues, accumulation, counters) lives in one
+ * file-scope device array of about 12 MB that every GPU which loads the
+ * library holds until the process exits. The caller passes the renderer
+ * (whose resident scene is the input), the frame, and `color_device`:
+ * device memory for width*height*4 floats, which receives the RGBA32F mean
+ * of frame_count samples from settings.sample_index (top-left rows; pixels
+ * outside the data window get the clear colour). Each call starts its own
+ * accumulation; none carries over.
+ *
+ * Limits: at most LOTUS_STATIC_MAX_PIXELS pixels (larger targets Fail with
+ * that reason); Radiance with BSDF or MIS light sampling. All calls share
+ * the one scratch array, which keeps the last call's contents, so calls
+ * whose GPU work overlaps (other threads or streams) race and corrupt each
+ * other. The first call on each device looks up the array's address with
+ * that device current; make it before any stream capture. Calls
+ * cudaMalloc, cudaFree and no allocating library routine. */
+int32_t lotus_cuda_render_static(lotus_cuda_renderer* renderer,
+    const lotus_frame_desc* frame, float* color_device, lotus_frame_result* result);
+
 #ifdef __cplusplus
 }
 #endif
