@@ -178,9 +178,101 @@ class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("flags", C.c_uint32)]
 
 
+class TemporalDesc(C.Structure):
+    _fields_ = [
+        ("frame", FrameDesc),
+        ("current_view", C.c_float * 16),
+        ("previous_view", C.c_float * 16),
+        ("previous_world_to_clip", C.c_float * 16),
+        ("validation", C.c_float * 4),
+        ("history_available", C.c_uint32),
+        ("accumulate_radiance", C.c_uint32),
+        ("max_history_samples", C.c_uint32),
+        ("filter_iterations", C.c_uint32),
+        ("history_rectification", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class TemporalInstance(C.Structure):
+    _fields_ = [
+        ("previous_world_from_object", C.c_float * 16),
+        ("instance_id", C.c_uint64),
+        ("material_id", C.c_uint64),
+        ("flags", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
 # The order lotus_cuda_struct_sizes reports them in.
 STRUCTS = [Geometry, Instance, Material, Environment, SceneDesc, SceneResult,
-           Target, Settings, FrameDesc, FrameResult, Options]
+           Target, Settings, FrameDesc, FrameResult, Options, TemporalDesc, TemporalInstance]
+
+# TemporalValidationSettings' defaults (temporal.hpp:28-33).
+DEFAULT_VALIDATION = (0.01, 0.01, 0.9, 32.0)
+
+# lotus_cuda_read_product's products.
+PRODUCT_SURFACE = 1
+PRODUCT_PREVIOUS_SURFACE = 2
+PRODUCT_VALIDITY = 3
+PRODUCT_RADIANCE = 4
+PRODUCT_PREVIOUS_RADIANCE = 5
+PRODUCT_BATCH = 6
+PRODUCT_RESTIR_INITIAL = 7
+PRODUCT_RESTIR_TEMPORAL = 8
+PRODUCT_RESTIR_PREVIOUS = 9
+PRODUCT_RESTIR_SPATIAL = 10
+PRODUCT_RESTIR_SOURCES = 11
+PRODUCT_RESTIR_SURFACES = 12
+PRODUCT_RESTIR_PREVIOUS_SURFACES = 13
+PRODUCT_FILTER = 14
+
+try:
+    import numpy as _np
+
+    # The reference's record layouts (temporal.hpp:193-235,
+    # vulkan_backend.hpp:152-178).
+    TEMPORAL_PIXEL = _np.dtype([("normal_depth", "<f4", 4), ("motion_depth", "<f4", 4),
+                                ("instance_id", "<u8"), ("material_id", "<u8"), ("flags", "<u4"),
+                                ("albedo", "<u4"), ("shading_normal", "<u4"), ("reserved", "<u4")])
+    VALIDITY_PIXEL = _np.dtype([("valid", "<u4"), ("rejection", "<u4"), ("previous_index", "<u4"),
+                                ("reserved", "<u4")])
+    RADIANCE_PIXEL = _np.dtype([("color", "<f4", 4), ("sample_count", "<u4"), ("moments", "<f4", 2),
+                                ("variance", "<f4")])
+    RESTIR_PIXEL = _np.dtype([("sample", "<u4"), ("weight_sum", "<f4"), ("selected_target", "<f4"),
+                              ("candidate_count", "<u4"), ("uv", "<f4", 2), ("proposal", "<f4"),
+                              ("flags", "<u4"), ("contribution", "<f4", 4)])
+    RESTIR_REUSE = _np.dtype([("pixel", RESTIR_PIXEL), ("normalization", "<f4"),
+                              ("supporting_candidates", "<u4"), ("previous_index", "<u4"), ("age", "<u4")])
+    RESTIR_SURFACE = _np.dtype([("vectors", "<f4", (9, 4)), ("instance_id", "<u8"), ("material_id", "<u8")])
+    PRODUCT_DTYPES = {
+        PRODUCT_SURFACE: TEMPORAL_PIXEL, PRODUCT_PREVIOUS_SURFACE: TEMPORAL_PIXEL,
+        PRODUCT_VALIDITY: VALIDITY_PIXEL, PRODUCT_RADIANCE: RADIANCE_PIXEL,
+        PRODUCT_PREVIOUS_RADIANCE: RADIANCE_PIXEL, PRODUCT_BATCH: _np.dtype(("<f4", 4)),
+        PRODUCT_RESTIR_INITIAL: RESTIR_PIXEL, PRODUCT_RESTIR_TEMPORAL: RESTIR_REUSE,
+        PRODUCT_RESTIR_PREVIOUS: RESTIR_REUSE, PRODUCT_RESTIR_SPATIAL: RESTIR_REUSE,
+        PRODUCT_RESTIR_SOURCES: _np.dtype(("<u4", 4)), PRODUCT_RESTIR_SURFACES: RESTIR_SURFACE,
+        PRODUCT_RESTIR_PREVIOUS_SURFACES: RESTIR_SURFACE, PRODUCT_FILTER: _np.dtype(("<f4", 12)),
+    }
+except ImportError:  # pragma: no cover
+    PRODUCT_DTYPES = {}
+
+
+def temporal_desc(frame, current_view, previous_view=None, previous_world_to_clip=None,
+                  history_available=False, accumulate_radiance=False, max_history_samples=32,
+                  filter_iterations=0, validation=DEFAULT_VALIDATION):
+    d = TemporalDesc()
+    d.frame = frame
+    d.current_view[:] = [float(v) for v in current_view]
+    d.previous_view[:] = [float(v) for v in (previous_view if previous_view is not None else current_view)]
+    d.previous_world_to_clip[:] = [float(v) for v in (previous_world_to_clip if previous_world_to_clip is not None
+                                                     else frame.world_to_clip)]
+    d.validation[:] = [float(v) for v in validation]
+    d.history_available = 1 if history_available else 0
+    d.accumulate_radiance = 1 if accumulate_radiance else 0
+    d.max_history_samples = max_history_samples
+    d.filter_iterations = filter_iterations
+    return d
 
 
 def default_settings(**overrides):

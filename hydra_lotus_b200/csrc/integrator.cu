@@ -11,6 +11,7 @@
 // radiance before the next extension reads it, so the radiance sums run in
 // the reference's order.
 #include "integrator.cuh"
+#include "temporal.cuh"
 
 namespace lotus {
 
@@ -67,14 +68,14 @@ struct ShadowRequest {
   F3 throughput;
 };
 
-// ScatterPath (transport.slang:164-230) without analytic lights or ReSTIR:
+// ScatterPath (transport.slang:164-230) without analytic lights:
 // adds the hit's emission (weighed against light sampling), applies
 // Russian roulette, prepares next event estimation's shadow ray and samples
 // the BSDF. Returns whether the path continues along (new_o, new_d).
 __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     uint32_t instance, uint32_t tri, float b1, float b2, F3 ray_o, F3 ray_d, uint32_t depth,
     F3& T, F3& R, float& last_pdf, uint32_t& flags, uint32_t& rng, F3& new_o, F3& new_d,
-    ShadowRequest& req) {
+    ShadowRequest& req, uint32_t pixel_index) {
   req.pending = false;
   uint32_t primitive;
   const SurfaceHit sh = reconstruct_hit(S, instance, tri, b1, b2, ray_d, &primitive);
@@ -100,7 +101,23 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
   }
   const Frame basis = make_frame(sh.shading_normal);
   const F3 wo = basis.to_local(-ray_d);
-  if (f.sample_lights && S.light_count != 0) {
+  if (f.restir_primary && depth == 0) {
+    // InitialDirectLight (restir.slang:235-254): the final reservoir's
+    // contribution, its visibility included, under the power-table/BSDF
+    // partition weight.
+    const RestirPixel sel = *reinterpret_cast<const RestirPixel*>(
+        f.restir_final + (size_t)pixel_index * f.restir_stride);
+    if ((sel.flags & 2u) == 0 && sel.reservoir.weight_sum > 0.0f && sel.reservoir.sample < S.light_count) {
+      const F3 origin = offset_ray_origin(sh.position, sh.normal);
+      const LightSample ls = reconstruct_reservoir_light(S, sel.reservoir.sample, sel.uv[0], sel.uv[1], origin);
+      const F3 wi = basis.to_local(ls.direction);
+      const float weight = ls.delta ? 1.0f
+          : power_heuristic(ls.pdf, wi.z > 0.0f ? bsdf_pdf(sh.bsdf, wo, wi) : 0.0f);
+      R = R + T * (V(sel.contribution) * weight);
+    } else {
+      R = R + T * V(0.0f);
+    }
+  } else if (f.sample_lights && S.light_count != 0) {
     // DirectLight and ShadowedLight up to the shadow ray
     // (transport.slang:82-135).
     const float u0 = next_random(rng);
@@ -227,7 +244,7 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
           F3 no, nd;
           ShadowRequest req;
           const bool cont = scatter(S, f, hit.instance, hit.tri, hit.b1, hit.b2, o, d, depth, T, R,
-              last_pdf, flags, rng, no, nd, req);
+              last_pdf, flags, rng, no, nd, req, slot);
           if (req.pending) {
             ++n_shadow;
             const float tr = trace_shadow<kCount>(S, req.origin, req.direction, 0.0f, req.tmax, &vc[2]);
@@ -338,7 +355,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_shade(SceneView S,
     uint32_t rng = __float_as_uint(rad.w);
     F3 no, nd;
     cont = scatter(S, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
-        T, R, last_pdf, flags, rng, no, nd, req);
+        T, R, last_pdf, flags, rng, no, nd, req, slot);
     if (cont) {
       P.origin[slot] = F4(no, 0.0f);
       P.direction[slot] = F4(nd, kFloatMax);

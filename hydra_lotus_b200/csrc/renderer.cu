@@ -18,6 +18,7 @@
 #include "bvh_build.cuh"
 #include "integrator.cuh"
 #include "renderer_internal.cuh"
+#include "temporal_passes.cuh"
 
 namespace lotus {
 namespace {
@@ -401,6 +402,32 @@ struct Renderer {
   bool key_valid = false;
   uint32_t accumulated = 0;
 
+  // Temporal streams (RenderTemporalScene).
+  struct Temporal {
+    uint32_t width = 0, height = 0;
+    DeviceArray<TemporalPixel> surface[2];
+    DeviceArray<ValidityPixel> validity;
+    DeviceArray<RadiancePixel> radiance[2];
+    DeviceArray<float4> batch;
+    DeviceArray<float4> filter;
+    DeviceArray<RestirPixel> initial;
+    DeviceArray<RestirReuse> reuse[2];
+    DeviceArray<RestirReuse> spatial;
+    DeviceArray<uint4> sources;
+    DeviceArray<RestirSurface> surfaces[2];
+    DeviceArray<TemporalConst> constants;
+    DeviceArray<TemporalInstance> instances;
+    bool instances_custom = false;
+    int surface_write = 0, radiance_write = 0, restir_write = 0;
+    int last_surface = 0, last_radiance = 0, last_restir = 0;
+    uint32_t frames = 0;          // temporal frames rendered since the last reset
+    uint32_t sample_offset = 0;
+    bool key_valid = false;
+    uint32_t key[16] = {};
+    bool restir_ran = false, accumulate_ran = false, spatial_ran = false, filter_ran = false;
+  } temporal;
+  std::vector<lotus_instance> host_instances;
+
   // The wavefront sample as a CUDA graph.
   cudaGraphExec_t graph = nullptr;
   struct GraphKey {
@@ -627,6 +654,7 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
     return fail(detail);
   R.host_lights = table.records;
   R.host_light_offsets = table.offsets;
+  R.host_instances.assign(s.instances, s.instances + s.instance_count);
   // Instances.
   std::vector<InstanceTraversal> h_trav(s.instance_count);
   std::vector<InstanceShading> h_shade(s.instance_count);
@@ -692,6 +720,21 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
   }
   v.env_selection = table.env_selection;
   for (int k = 0; k < 3; ++k) v.env_constant[k] = s.environment_constant[k];
+  // Default temporal identities: index and material slot, static, 6.
+  {
+    std::vector<TemporalInstance> ids(std::max<uint32_t>(s.instance_count, 1));
+    for (uint32_t i = 0; i < s.instance_count; ++i) {
+      TemporalInstance& t = ids[i];
+      const float* m = s.instances[i].world_from_object;
+      for (int r = 0; r < 3; ++r) t.previous[r] = make_float4(m[r], m[4 + r], m[8 + r], m[12 + r]);
+      t.instance_id = i;
+      t.material_id = s.instances[i].material;
+      t.flags = 6u;
+    }
+    if (!R.ok(R.temporal.instances.upload(ids.data(), ids.size(), st), "temporal identities", detail))
+      return fail(detail);
+    R.temporal.instances_custom = false;
+  }
   R.scene_ready = true;
   ++R.scene_generation;
   res.status = LOTUS_PASS;
@@ -990,7 +1033,8 @@ uint32_t lotus_cuda_struct_sizes(uint64_t* sizes, uint32_t capacity) {
   const uint64_t s[] = {sizeof(lotus_geometry), sizeof(lotus_instance), sizeof(lotus_material),
       sizeof(lotus_environment), sizeof(lotus_scene_desc), sizeof(lotus_scene_result),
       sizeof(lotus_target), sizeof(lotus_settings), sizeof(lotus_frame_desc),
-      sizeof(lotus_frame_result), sizeof(lotus_cuda_options)};
+      sizeof(lotus_frame_result), sizeof(lotus_cuda_options), sizeof(lotus_temporal_desc),
+      sizeof(lotus_temporal_instance)};
   const uint32_t n = sizeof(s) / sizeof(s[0]);
   for (uint32_t i = 0; i < n && i < capacity; ++i) sizes[i] = s[i];
   return n;
@@ -1205,3 +1249,326 @@ bool make_frame_constants(const lotus_frame_desc& d, FrameConst& fc, uint32_t re
 }
 
 }  // namespace lotus
+
+namespace {
+
+using namespace lotus;
+
+// RenderTemporalScene (vulkan_backend.cpp:1711-2100): validation, history
+// rules, then the passes in the reference's order.
+int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_result& res, float* color_out) {
+  std::string detail;
+  auto fail = [&](const std::string& msg) {
+    copy_detail(res.detail, sizeof(res.detail), msg);
+    return res.status = LOTUS_FAIL;
+  };
+  auto poison = [&](const std::string& msg) {
+    R.failure = msg;
+    return fail(msg);
+  };
+  const lotus_frame_desc& d = td.frame;
+  const lotus_settings& st = d.settings;
+  const lotus_target& t = d.target;
+  if (!R.scene_ready) return fail("no scene has been uploaded");
+  if (d.frame_count == 0) return fail("frame_count must be at least 1");
+  const bool reuse = st.restir_temporal != 0;
+  const bool reservoirs = reuse || st.restir_spatial != 0;
+  const bool restir = st.light_sampling == LOTUS_LIGHT_SAMPLING_RESTIR_INITIAL;
+  const bool accumulate = td.accumulate_radiance != 0;
+  if (reservoirs && (d.frame_count != 1 || !restir || st.restir_candidates == 0 || st.restir_candidates > 64 ||
+                        st.restir_max_history_candidates == 0 || st.restir_max_history_candidates > 65536))
+    return fail("temporal reservoirs require Radiance, RestirInitial, one fresh sample, candidates in [1, 64] "
+                "and history candidates in [1, 65536]");
+  if (restir && (st.restir_candidates == 0 || st.restir_candidates > 64))
+    return fail("RestirInitial needs restir_candidates in [1, 64]");
+  if (st.restir_spatial && (st.restir_spatial_radius == 0 || st.restir_spatial_radius > 32))
+    return fail("restir_spatial_radius must be in [1, 32]");
+  if (accumulate && (td.max_history_samples == 0 || td.max_history_samples > 65536))
+    return fail("temporal radiance requires history samples in [1, 65536]");
+  if (td.filter_iterations > 8 || (td.filter_iterations != 0 && !accumulate))
+    return fail("temporal filtering requires radiance accumulation and at most 8 iterations");
+  if (td.history_rectification != 0)
+    return fail("history rectification other than None is not built");
+  if (st.integrator > LOTUS_INTEGRATOR_WAVEFRONT) return fail("unknown integrator");
+  FrameConst fc{};
+  uint32_t rect[4];
+  lotus_frame_desc checked = d;
+  if (restir) checked.settings.light_sampling = LOTUS_LIGHT_SAMPLING_MIS;  // validated as MIS
+  if (!make_frame_constants(checked, fc, rect, detail)) return fail(detail);
+  float prev_vulkan[16];
+  std::memcpy(prev_vulkan, td.previous_world_to_clip, sizeof(prev_vulkan));
+  for (int c = 0; c < 4; ++c) {
+    const float z = td.previous_world_to_clip[c * 4 + 2], w = td.previous_world_to_clip[c * 4 + 3];
+    prev_vulkan[c * 4 + 1] = -td.previous_world_to_clip[c * 4 + 1];
+    prev_vulkan[c * 4 + 2] = 0.5f * (z + w);
+  }
+  Renderer::Temporal& T = R.temporal;
+  const bool wavefront = st.integrator == LOTUS_INTEGRATOR_WAVEFRONT;
+  if (!ensure_targets(R, t.width, t.height, wavefront, detail)) return poison(detail);
+  // Buffers.
+  const size_t n = (size_t)t.width * t.height;
+  if (T.width != t.width || T.height != t.height) {
+    T.width = t.width;
+    T.height = t.height;
+    T.frames = 0;
+    T.surface_write = T.radiance_write = T.restir_write = 0;
+    T.key_valid = false;
+  }
+  bool okb = R.ok(T.surface[0].resize(n), "temporal surface", detail) &&
+             R.ok(T.surface[1].resize(n), "temporal surface", detail) &&
+             R.ok(T.validity.resize(n), "temporal validity", detail) &&
+             R.ok(T.constants.resize(1), "temporal constants", detail);
+  if (okb && accumulate)
+    okb = R.ok(T.radiance[0].resize(n), "temporal radiance", detail) &&
+          R.ok(T.radiance[1].resize(n), "temporal radiance", detail) &&
+          R.ok(T.batch.resize(n), "temporal batch", detail) &&
+          (td.filter_iterations == 0 || R.ok(T.filter.resize(3 * n), "temporal filter", detail));
+  if (okb && restir)
+    okb = R.ok(T.initial.resize(n), "reservoirs", detail) && R.ok(T.reuse[0].resize(n), "reservoirs", detail) &&
+          R.ok(T.reuse[1].resize(n), "reservoirs", detail) && R.ok(T.spatial.resize(n), "reservoirs", detail) &&
+          R.ok(T.sources.resize(n), "reservoirs", detail) &&
+          R.ok(T.surfaces[0].resize(n), "reservoir surfaces", detail) &&
+          R.ok(T.surfaces[1].resize(n), "reservoir surfaces", detail);
+  if (!okb) return poison(detail);
+  // The transport key: a change drops the history (vulkan_backend.cpp:1766-1781).
+  uint32_t key[16] = {st.integrator, st.light_sampling, st.restir_proposal, st.restir_candidates,
+      st.restir_temporal, st.restir_max_history_candidates, st.restir_spatial, st.restir_spatial_radius,
+      td.accumulate_radiance, st.sample_index, st.max_bounces, st.environment_background, 0, 0, 0, 0};
+  std::memcpy(&key[12], t.clear_color, sizeof(t.clear_color));
+  const bool fresh_batch = accumulate || reservoirs;
+  bool previous = td.history_available != 0 && T.frames > 0;
+  if (fresh_batch && previous && (!T.key_valid || std::memcmp(key, T.key, sizeof(key)) != 0)) previous = false;
+  std::memcpy(T.key, key, sizeof(key));
+  T.key_valid = true;
+  if (!previous) T.sample_offset = 0;
+  const uint32_t sample_offset = previous ? T.sample_offset : 0u;
+  // Constants.
+  fc.sample_index = st.sample_index + (fresh_batch ? sample_offset : 0u);
+  fc.accumulated = 0;
+  fc.add_sample = 1;
+  fc.sample_lights = st.light_sampling != LOTUS_LIGHT_SAMPLING_BSDF ? 1u : 0u;
+  TemporalConst tc{};
+  std::memcpy(tc.current_view, td.current_view, sizeof(tc.current_view));
+  if (previous) {
+    std::memcpy(tc.previous_view, td.previous_view, sizeof(tc.previous_view));
+    std::memcpy(tc.previous_world_to_clip, prev_vulkan, sizeof(prev_vulkan));
+  }
+  float vx = 0.0f, vy = 0.0f, vw = (float)t.width, vh = (float)t.height;
+  if (t.display_window[2] > 0.0f && t.display_window[3] > 0.0f) {
+    vx = t.display_window[0]; vy = t.display_window[1]; vw = t.display_window[2]; vh = t.display_window[3];
+  }
+  tc.previous_display[0] = vx; tc.previous_display[1] = vy; tc.previous_display[2] = vw; tc.previous_display[3] = vh;
+  for (int k = 0; k < 4; ++k) {
+    tc.previous_data[k] = rect[k];
+    tc.validation[k] = td.validation[k];
+  }
+  tc.history = previous ? 1u : 0u;
+  tc.width = t.width;
+  tc.height = t.height;
+  tc.accumulate = accumulate ? 1u : 0u;
+  tc.fresh_samples = d.frame_count;
+  tc.history_cap = td.max_history_samples;
+  tc.filter_iterations = td.filter_iterations;
+  tc.restir_candidates = restir ? st.restir_candidates : 0u;
+  tc.restir_history = reuse && previous ? 1u : 0u;
+  tc.restir_max_history = st.restir_max_history_candidates;
+  tc.restir_spatial = st.restir_spatial ? 1u : 0u;
+  tc.restir_temporal = reservoirs ? 1u : 0u;
+  tc.restir_radius = st.restir_spatial_radius;
+  tc.restir_proposal = st.restir_proposal;
+  tc.sample_index = fc.sample_index;
+  tc.max_bounces = st.max_bounces;
+  const int sw = T.surface_write, rs = T.restir_write, rw = T.radiance_write;
+  if (restir) {
+    fc.restir_primary = 1;
+    if (st.restir_spatial) {
+      fc.restir_final = reinterpret_cast<const unsigned char*>(T.spatial.ptr);
+      fc.restir_stride = sizeof(RestirReuse);
+    } else if (reservoirs) {
+      fc.restir_final = reinterpret_cast<const unsigned char*>(T.reuse[rs].ptr);
+      fc.restir_stride = sizeof(RestirReuse);
+    } else {
+      fc.restir_final = reinterpret_cast<const unsigned char*>(T.initial.ptr);
+      fc.restir_stride = sizeof(RestirPixel);
+    }
+  }
+  cudaStream_t s = R.stream;
+  if (!R.ok(cudaMemcpyAsync(R.frame_const.ptr, &fc, sizeof(fc), cudaMemcpyHostToDevice, s), "frame constants", detail) ||
+      !R.ok(cudaMemcpyAsync(T.constants.ptr, &tc, sizeof(tc), cudaMemcpyHostToDevice, s), "temporal constants", detail) ||
+      !R.ok(cudaMemsetAsync(R.totals.ptr, 0, sizeof(RayTotals), s), "ray totals", detail))
+    return poison(detail);
+  cudaEventRecord(R.ev_start, s);
+  const uint32_t pixels = (uint32_t)n;
+  launch_temporal_surface(R.view, R.frame_const.ptr, T.constants.ptr, T.instances.ptr, T.surface[sw].ptr, pixels, s);
+  launch_reproject(T.constants.ptr, T.surface[sw].ptr, T.surface[1 - sw].ptr, T.validity.ptr, pixels, s);
+  if (restir) {
+    launch_restir_initial(R.view, R.frame_const.ptr, T.constants.ptr, T.initial.ptr, pixels, s);
+    if (reservoirs)
+      launch_restir_temporal(R.view, R.frame_const.ptr, T.constants.ptr, T.instances.ptr, T.initial.ptr,
+          T.validity.ptr, T.surface[sw].ptr, T.reuse[1 - rs].ptr, T.surfaces[1 - rs].ptr, T.reuse[rs].ptr,
+          T.surfaces[rs].ptr, pixels, s);
+    if (st.restir_spatial)
+      launch_restir_spatial(R.view, R.frame_const.ptr, T.constants.ptr, T.reuse[rs].ptr, T.surfaces[rs].ptr,
+          T.spatial.ptr, T.sources.ptr, pixels, s);
+  }
+  if (rect[2] < t.width || rect[3] < t.height || rect[2] == 0)
+    launch_clear_color(R.color.ptr, pixels, make_float4(t.clear_color[0], t.clear_color[1], t.clear_color[2],
+        t.clear_color[3]), s);
+  PathState P{R.path_origin.ptr, R.path_direction.ptr, R.path_throughput.ptr, R.path_radiance.ptr, R.path_hit.ptr};
+  Queues Q;
+  Q.ray[0] = R.queue_ray0.ptr;
+  Q.ray[1] = R.queue_ray1.ptr;
+  Q.hit = R.queue_hit.ptr;
+  Q.shadow = ShadowQueue{R.sq_o.ptr, R.sq_d.ptr, R.sq_fl.ptr, R.sq_thr.ptr};
+  Q.counts = R.counts.ptr;
+  Q.capacity = pixels;
+  for (uint32_t k = 0; k < d.frame_count; ++k) {
+    if (wavefront)
+      launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
+          R.accum.ptr, R.color.ptr, R.totals.ptr, s);
+    else
+      launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s);
+    launch_advance(R.frame_const.ptr, s);
+  }
+  if (accumulate) {
+    cudaMemcpyAsync(T.batch.ptr, R.color.ptr, n * sizeof(float4), cudaMemcpyDeviceToDevice, s);
+    launch_svgf(T.constants.ptr, tc, T.batch.ptr, T.surface[sw].ptr, T.validity.ptr, T.radiance[1 - rw].ptr,
+        T.radiance[rw].ptr, T.filter.ptr, R.color.ptr, pixels, s);
+  }
+  cudaEventRecord(R.ev_stop, s);
+  RayTotals totals{};
+  cudaMemcpyAsync(&totals, R.totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s);
+  if (!R.ok(cudaStreamSynchronize(s), "temporal frame", detail)) return poison(detail);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
+  T.restir_ran = restir;
+  T.spatial_ran = restir && st.restir_spatial;
+  T.accumulate_ran = accumulate;
+  T.filter_ran = accumulate && td.filter_iterations != 0;
+  // The products of this frame stay at the indices just written; the next
+  // frame writes the other halves.
+  T.last_surface = sw;
+  T.last_radiance = rw;
+  T.last_restir = rs;
+  T.surface_write ^= 1;
+  if (accumulate) T.radiance_write ^= 1;
+  if (reservoirs) T.restir_write ^= 1;
+  ++T.frames;
+  T.sample_offset = fresh_batch ? sample_offset + d.frame_count : 0u;
+  R.key_valid = false;  // the next RenderScene restarts its accumulation
+  R.completion += d.frame_count;
+  if (t.read_back && color_out) {
+    if (!R.ok(cudaMemcpyAsync(color_out, R.color.ptr, sizeof(float4) * n, cudaMemcpyDeviceToHost, s), "colour", detail) ||
+        !R.ok(cudaStreamSynchronize(s), "colour", detail))
+      return poison(detail);
+  }
+  res.status = LOTUS_PASS;
+  res.frames_rendered = d.frame_count;
+  res.samples_per_pixel = d.frame_count;
+  res.completion = R.completion;
+  res.camera_rays = totals.camera;
+  res.extension_rays = totals.extension;
+  res.shadow_rays = totals.shadow;
+  res.gpu_ms = ms;
+  return LOTUS_PASS;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t lotus_cuda_set_temporal_instances(lotus_cuda_renderer* r, const lotus_temporal_instance* instances,
+    uint32_t count) {
+  if (!r || (!instances && count)) return LOTUS_FAIL;
+  Renderer& R = r->r;
+  if (!R.failure.empty() || !R.scene_ready || count != R.view.instance_count) return LOTUS_FAIL;
+  cudaSetDevice(R.device);
+  std::vector<TemporalInstance> ids(std::max<uint32_t>(count, 1));
+  for (uint32_t i = 0; i < count; ++i) {
+    const float* m = instances[i].previous_world_from_object;
+    for (int k = 0; k < 3; ++k) ids[i].previous[k] = make_float4(m[k], m[4 + k], m[8 + k], m[12 + k]);
+    ids[i].instance_id = instances[i].instance_id;
+    ids[i].material_id = instances[i].material_id;
+    ids[i].flags = instances[i].flags;
+  }
+  std::string detail;
+  if (!R.ok(R.temporal.instances.upload(ids.data(), ids.size(), R.stream), "temporal identities", detail) ||
+      !R.ok(cudaStreamSynchronize(R.stream), "temporal identities", detail))
+    return LOTUS_FAIL;
+  R.temporal.instances_custom = true;
+  return LOTUS_PASS;
+}
+
+int32_t lotus_cuda_render_temporal(lotus_cuda_renderer* r, const lotus_temporal_desc* temporal,
+    lotus_frame_result* result, float* color) {
+  lotus_frame_result local{};
+  lotus_frame_result& res = result ? *result : local;
+  std::memset(&res, 0, sizeof(res));
+  if (!r || !temporal) {
+    copy_detail(res.detail, sizeof(res.detail), "no renderer or temporal frame");
+    return res.status = LOTUS_FAIL;
+  }
+  Renderer& R = r->r;
+  if (!R.failure.empty()) {
+    copy_detail(res.detail, sizeof(res.detail), "the renderer failed earlier: " + R.failure);
+    return res.status = LOTUS_FAIL;
+  }
+  cudaSetDevice(R.device);
+  return render_temporal(R, *temporal, res, color);
+}
+
+int64_t lotus_cuda_read_product(lotus_cuda_renderer* r, uint32_t product, void* out, uint64_t capacity) {
+  if (!r || !out) return -1;
+  Renderer& R = r->r;
+  Renderer::Temporal& T = R.temporal;
+  if (T.frames == 0) return -1;
+  const size_t n = (size_t)T.width * T.height;
+  const void* src = nullptr;
+  size_t bytes = 0;
+  const int sw = T.last_surface, rw = T.last_radiance, rs = T.last_restir;
+  switch (product) {
+    case LOTUS_PRODUCT_SURFACE: src = T.surface[sw].ptr; bytes = n * sizeof(TemporalPixel); break;
+    case LOTUS_PRODUCT_PREVIOUS_SURFACE: src = T.surface[1 - sw].ptr; bytes = n * sizeof(TemporalPixel); break;
+    case LOTUS_PRODUCT_VALIDITY: src = T.validity.ptr; bytes = n * sizeof(ValidityPixel); break;
+    case LOTUS_PRODUCT_RADIANCE:
+      if (T.accumulate_ran) { src = T.radiance[rw].ptr; bytes = n * sizeof(RadiancePixel); }
+      break;
+    case LOTUS_PRODUCT_PREVIOUS_RADIANCE:
+      if (T.accumulate_ran) { src = T.radiance[1 - rw].ptr; bytes = n * sizeof(RadiancePixel); }
+      break;
+    case LOTUS_PRODUCT_BATCH:
+      if (T.accumulate_ran) { src = T.batch.ptr; bytes = n * sizeof(float4); }
+      break;
+    case LOTUS_PRODUCT_RESTIR_INITIAL:
+      if (T.restir_ran) { src = T.initial.ptr; bytes = n * sizeof(RestirPixel); }
+      break;
+    case LOTUS_PRODUCT_RESTIR_TEMPORAL:
+      if (T.restir_ran) { src = T.reuse[rs].ptr; bytes = n * sizeof(RestirReuse); }
+      break;
+    case LOTUS_PRODUCT_RESTIR_PREVIOUS:
+      if (T.restir_ran) { src = T.reuse[1 - rs].ptr; bytes = n * sizeof(RestirReuse); }
+      break;
+    case LOTUS_PRODUCT_RESTIR_SPATIAL:
+      if (T.spatial_ran) { src = T.spatial.ptr; bytes = n * sizeof(RestirReuse); }
+      break;
+    case LOTUS_PRODUCT_RESTIR_SOURCES:
+      if (T.spatial_ran) { src = T.sources.ptr; bytes = n * sizeof(uint4); }
+      break;
+    case LOTUS_PRODUCT_RESTIR_SURFACES:
+      if (T.restir_ran) { src = T.surfaces[rs].ptr; bytes = n * sizeof(RestirSurface); }
+      break;
+    case LOTUS_PRODUCT_RESTIR_PREVIOUS_SURFACES:
+      if (T.restir_ran) { src = T.surfaces[1 - rs].ptr; bytes = n * sizeof(RestirSurface); }
+      break;
+    case LOTUS_PRODUCT_FILTER:
+      if (T.filter_ran) { src = T.filter.ptr; bytes = 3 * n * sizeof(float4); }
+      break;
+    default: break;
+  }
+  if (!src || bytes > capacity) return -1;
+  cudaSetDevice(R.device);
+  if (cudaMemcpy(out, src, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  return (int64_t)bytes;
+}
+
+}  // extern "C"

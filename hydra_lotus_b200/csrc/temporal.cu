@@ -1,0 +1,782 @@
+// SPDX-License-Identifier: Apache-2.0
+// The temporal passes: the primary-surface metadata and its reprojection
+// (backend/vulkan/shaders/common/temporal.slang:497-627 in hydra-lotus),
+// ReSTIR DI's initial, temporal and spatial reservoir passes
+// (common/restir.slang:163-491), and SVGF's temporal accumulation, variance
+// estimate, a-trous iterations and composite (temporal.slang:229-475). One
+// thread per pixel; every pass is a separate launch, so each reads only what
+// the preceding one finished writing, as the reference's barriers order it.
+#include "temporal_passes.cuh"
+
+namespace lotus {
+namespace {
+
+constexpr int kBlock = 128;
+
+__device__ __forceinline__ bool pixel_of(uint32_t index, uint32_t width, uint32_t height,
+    uint32_t& px, uint32_t& py) {
+  if (index >= width * height) return false;
+  px = index % width;
+  py = index / width;
+  return true;
+}
+
+__device__ __forceinline__ bool in_rect(const FrameConst& f, uint32_t px, uint32_t py) {
+  return px >= f.rect[0] && py >= f.rect[1] && px < f.rect[0] + f.rect[2] && py < f.rect[1] + f.rect[3];
+}
+
+__device__ __forceinline__ bool finite4(float4 v) {
+  return isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w);
+}
+
+// ---------------------------------------------------------------------------
+// WriteTemporalSurface (temporal.slang:557-627): the pixel centre's primary
+// hit, with a fixed coverage sequence (sample 0).
+__global__ void __launch_bounds__(kBlock) k_temporal_surface(SceneView S,
+    const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
+    const TemporalInstance* __restrict__ identities, TemporalPixel* __restrict__ out) {
+  const FrameConst& f = *fcp;
+  const TemporalConst& tc = *tcp;
+  uint32_t px, py;
+  if (!pixel_of(blockIdx.x * blockDim.x + threadIdx.x, f.width, f.height, px, py)) return;
+  const uint32_t index = py * f.width + px;
+  TemporalPixel o = {};
+  if (in_rect(f, px, py)) {
+    uint32_t rng = seed_random(index, 0);
+    const float cx = float(px) + 0.5f, cy = float(py) + 0.5f;
+    F3 ro, rd;
+    float tmax;
+    camera_ray(f, cx * f.ndc[0] + f.ndc[2], cy * f.ndc[1] + f.ndc[3], ro, rd, tmax);
+    Hit hit;
+    if (trace_closest(S, ro, rd, 0.0f, tmax, rng, hit)) {
+      const InstanceShading rec = S.inst_shade[hit.instance];
+      const TemporalInstance id = identities[hit.instance];
+      const float4* tv = S.tris + 3 * (size_t)hit.tri;
+      const F3 p0 = V(tv[0]), p1 = V(tv[1]), p2 = V(tv[2]);
+      const F3 point = p0 + hit.b1 * (p1 - p0) + hit.b2 * (p2 - p0);
+      const F3 world = row_point(rec.m, point);
+      const float4 view = mul4(tc.current_view, world.x, world.y, world.z, 1.0f);
+      const F3 a = row_point(rec.m, p0), b = row_point(rec.m, p1), c = row_point(rec.m, p2);
+      F3 normal = normalize(cross(b - a, c - a));
+      if (dot(normal, rd) > 0.0f) normal = -normal;
+      const float depth = -view.z / view.w;
+      if (finite4(view) && is_finite(normal) && view.w > 0.0f && depth > 0.0f) {
+        o.normal_depth = F4(normal, depth);
+        o.instance_id = id.instance_id;
+        o.material_id = id.material_id;
+        o.flags = 1u | id.flags;
+        const SurfaceHit sh = reconstruct_hit(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
+        // The surface summary's albedo (scene.slang:1254-1257).
+        const F3 albedo = sh.bsdf.transmission > 0.0f
+            ? sh.base_color + sh.bsdf.transmission * (sh.bsdf.transmission_color - sh.base_color)
+            : sh.base_color;
+        o.albedo = pack_albedo(albedo);
+        o.shading_normal = pack_normal(sh.shading_normal);
+        if (id.flags & 2u) {
+          const F3 pw = row_point(id.previous, point);
+          const float4 pv = mul4(tc.previous_view, pw.x, pw.y, pw.z, 1.0f);
+          const float4 clip = mul4(tc.previous_world_to_clip, pw.x, pw.y, pw.z, 1.0f);
+          const float qx = clip.x / clip.w, qy = clip.y / clip.w, qz = clip.z / clip.w;
+          const float pd = -pv.z / pv.w;
+          const float ppx = tc.previous_display[0] + (qx * 0.5f + 0.5f) * tc.previous_display[2];
+          const float ppy = tc.previous_display[1] + (qy * 0.5f + 0.5f) * tc.previous_display[3];
+          const float bx = float(tc.previous_data[0]), by = float(tc.previous_data[1]);
+          const float ex = bx + float(tc.previous_data[2]), ey = by + float(tc.previous_data[3]);
+          if (finite4(pv) && finite4(clip) && isfinite(ppx) && isfinite(ppy) && isfinite(pd) &&
+              pv.w > 0.0f && clip.w > 0.0f && pd > 0.0f && qz >= 0.0f && qz <= 1.0f &&
+              qx >= -1.0f && qy >= -1.0f && qx < 1.0f && qy < 1.0f && ppx >= bx && ppy >= by &&
+              ppx < ex && ppy < ey)
+            o.motion_depth = make_float4(ppx - cx, ppy - cy, pd, 1.0f);
+        }
+      }
+    }
+  }
+  out[index] = o;
+}
+
+// ValidateHistory (temporal.slang:497-522).
+__device__ __forceinline__ uint32_t validate_history(const TemporalConst& tc, const TemporalPixel& cur,
+    const TemporalPixel& prev) {
+  if ((prev.flags & 1u) == 0) return 1u;
+  const float* th = tc.validation;
+  const F3 n = V(cur.normal_depth), on = V(prev.normal_depth);
+  if (!finite4(cur.normal_depth) || !finite4(prev.normal_depth) || !finite4(cur.motion_depth) ||
+      !isfinite(th[0]) || !isfinite(th[1]) || !isfinite(th[2]) || !isfinite(th[3]) ||
+      cur.normal_depth.w <= 0.0f || prev.normal_depth.w <= 0.0f || cur.motion_depth.z <= 0.0f ||
+      th[0] < 0.0f || th[1] < 0.0f || th[2] < -1.0f || th[2] > 1.0f || th[3] < 0.0f ||
+      (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f) || (on.x == 0.0f && on.y == 0.0f && on.z == 0.0f))
+    return 2u;
+  if (cur.instance_id != prev.instance_id) return 3u;
+  if (cur.material_id != prev.material_id) return 4u;
+  const float mx = cur.motion_depth.x, my = cur.motion_depth.y;
+  if (sqrtf(mx * mx + my * my) > th[3]) return 5u;
+  if (fabsf(prev.normal_depth.w - cur.motion_depth.z) > th[0] + th[1] * cur.motion_depth.z) return 6u;
+  if (dot(normalize(n), normalize(on)) < th[2]) return 7u;
+  return 0u;
+}
+
+// ReprojectHistory (temporal.slang:524-554): the nearest backward fetch.
+__global__ void __launch_bounds__(kBlock) k_reproject(const TemporalConst* __restrict__ tcp,
+    const TemporalPixel* __restrict__ current, const TemporalPixel* __restrict__ previous,
+    ValidityPixel* __restrict__ out) {
+  const TemporalConst& tc = *tcp;
+  uint32_t px, py;
+  if (!pixel_of(blockIdx.x * blockDim.x + threadIdx.x, tc.width, tc.height, px, py)) return;
+  const uint32_t index = py * tc.width + px;
+  const TemporalPixel cur = current[index];
+  ValidityPixel o = {0u, 0u, 0xffffffffu, 0u};
+  if ((cur.flags & 1u) == 0) o.rejection = 1u;
+  else if (tc.history == 0) o.rejection = 8u;
+  else if ((cur.flags & 2u) == 0) o.rejection = 9u;
+  else if ((cur.flags & 4u) == 0) o.rejection = 4u;
+  else if (cur.motion_depth.w != 1.0f) o.rejection = 10u;
+  else {
+    const float ox = float(px) + 0.5f + cur.motion_depth.x;
+    const float oy = float(py) + 0.5f + cur.motion_depth.y;
+    if (!isfinite(ox) || !isfinite(oy)) o.rejection = 2u;
+    else if (ox < 0.0f || oy < 0.0f || ox >= float(tc.width) || oy >= float(tc.height)) o.rejection = 10u;
+    else {
+      o.previous_index = (uint32_t)oy * tc.width + (uint32_t)ox;
+      o.rejection = validate_history(tc, cur, previous[o.previous_index]);
+    }
+  }
+  o.valid = o.rejection == 0u ? 1u : 0u;
+  out[index] = o;
+}
+
+// ---------------------------------------------------------------------------
+// ReSTIR DI.
+
+__device__ __forceinline__ F3 reflection_evaluate_side(const Closure& c, F3 wo, F3 wi) {
+  return wi.z > 0.0f ? bsdf_evaluate(c, wo, wi) : V(0.0f);
+}
+
+// CandidateContribution (restir.slang:155-161).
+__device__ __forceinline__ F3 candidate_contribution(const SurfaceHit& sh, const Frame& basis, F3 wo,
+    const LightSample& ls, float selection) {
+  if (!(ls.pdf > 0.0f) || dot(ls.direction, sh.normal) <= 0.0f) return V(0.0f);
+  return reflection_evaluate_side(sh.bsdf, wo, basis.to_local(ls.direction)) * ls.radiance *
+      (selection / ls.pdf);
+}
+
+__device__ __forceinline__ void store_closure(const Closure& b, RestirSurface& s) {
+  s.model = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  s.extension = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  s.normal.w = b.dielectric_f90;
+  s.shading_normal.w = b.thin_walled ? -b.transmission : b.transmission;
+  s.outgoing.w = b.smooth ? -b.eta : b.eta;
+  s.base_alpha = F4(b.base_color, b.alpha);
+  s.dielectric_metallic = F4(b.dielectric_f0, b.metallic);
+  s.fresnel = F4(b.f0, b.f90);
+}
+
+__device__ __forceinline__ Closure load_closure(const RestirSurface& s) {
+  Closure b;
+  b.base_color = V(s.base_alpha);
+  b.alpha = s.base_alpha.w;
+  b.metallic = s.dielectric_metallic.w;
+  b.dielectric_f0 = V(s.dielectric_metallic);
+  b.dielectric_f90 = s.normal.w;
+  b.f0 = V(s.fresnel);
+  b.f90 = s.fresnel.w;
+  b.transmission = fabsf(s.shading_normal.w);
+  b.transmission_color = V(1.0f);
+  b.eta = fabsf(s.outgoing.w);
+  b.thin_walled = s.shading_normal.w < 0.0f;
+  b.smooth = s.outgoing.w < 0.0f;
+  return b;
+}
+
+// HistoryContribution (restir.slang:256-268).
+__device__ __forceinline__ F3 history_contribution(const SceneView& S, const RestirSurface& src,
+    uint32_t light, const LightSample& ls) {
+  const Closure b = load_closure(src);
+  if (!(ls.pdf > 0.0f) || dot(ls.direction, V(src.normal)) <= 0.0f) return V(0.0f);
+  const Frame basis = make_frame(V(src.shading_normal));
+  return reflection_evaluate_side(b, V(src.outgoing), basis.to_local(ls.direction)) * ls.radiance *
+      (S.lights[light].pdf / ls.pdf);
+}
+
+__device__ __forceinline__ F3 history_contribution_uv(const SceneView& S, const RestirSurface& src,
+    uint32_t light, const float* uv) {
+  return history_contribution(S, src, light,
+      reconstruct_reservoir_light(S, light, uv[0], uv[1], V(src.origin)));
+}
+
+__device__ __forceinline__ bool same_sample(const RestirPixel& a, const RestirPixel& b) {
+  return a.reservoir.sample == b.reservoir.sample && a.uv[0] == b.uv[0] && a.uv[1] == b.uv[1];
+}
+
+// HistoryTarget (restir.slang:276-285).
+__device__ __forceinline__ float history_target(const SceneView& S, const RestirReuse& source,
+    const RestirSurface& surface, const RestirPixel& selected, bool& valid) {
+  if (same_sample(source.pixel, selected)) {
+    valid = isfinite(source.pixel.reservoir.selected_target);
+    return source.pixel.reservoir.selected_target;
+  }
+  const F3 c = history_contribution_uv(S, surface, selected.reservoir.sample, selected.uv);
+  valid = is_finite(c);
+  return max_component(c);
+}
+
+// ReceiverVisibility (restir.slang:290-300).
+__device__ __forceinline__ float receiver_visibility(const SceneView& S, const RestirPixel& selected,
+    const RestirPixel& current, F3 origin, const LightSample& ls) {
+  if (same_sample(selected, current)) return current.contribution.w;
+  return trace_shadow(S, origin, ls.direction, 0.0f, ls.distance);
+}
+
+__device__ __forceinline__ RestirPixel empty_restir_pixel() {
+  RestirPixel r;
+  r.reservoir = empty_reservoir();
+  r.uv[0] = r.uv[1] = 0.0f;
+  r.proposal = 0.0f;
+  r.flags = 0;
+  r.contribution = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  return r;
+}
+
+// WriteInitialReservoir (restir.slang:163-233): M candidates streamed over
+// the light table at the jittered camera surface, then one shadow ray for
+// the selected sample.
+__global__ void __launch_bounds__(kBlock) k_restir_initial(SceneView S,
+    const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
+    RestirPixel* __restrict__ out) {
+  const FrameConst& f = *fcp;
+  const TemporalConst& tc = *tcp;
+  uint32_t px, py;
+  if (!pixel_of(blockIdx.x * blockDim.x + threadIdx.x, f.width, f.height, px, py)) return;
+  const uint32_t slot = py * f.width + px;
+  RestirPixel r = empty_restir_pixel();
+  const bool active = tc.restir_candidates != 0 && in_rect(f, px, py);
+  if (active) {
+    F3 ro, rd;
+    float tmax;
+    uint32_t camera_rng;
+    start_path(f, px, py, f.sample_index, ro, rd, tmax, camera_rng);
+    Hit hit;
+    if (trace_closest(S, ro, rd, 0.0f, tmax, camera_rng, hit)) {
+      r.flags |= 1u;
+      const SurfaceHit sh = reconstruct_hit(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
+      const Frame basis = make_frame(sh.shading_normal);
+      const F3 wo = basis.to_local(-rd);
+      const F3 origin = offset_ray_origin(sh.position, sh.normal);
+      uint32_t rng = seed_random(slot, f.sample_index ^ 0xD1B54A35u);
+      if (tc.max_bounces != 0 && S.light_count != 0) {
+        for (uint32_t i = 0; i < tc.restir_candidates; ++i) {
+          const float cx = next_random(rng);
+          const float cy = next_random(rng);
+          const float ux = next_random(rng);
+          const float uy = next_random(rng);
+          const float random = next_random(rng);
+          const uint32_t light = choose_reservoir_light(S, tc.restir_proposal, cx, cy);
+          const float proposal = reservoir_proposal_pdf(S, tc.restir_proposal, light);
+          const LightSample ls = reconstruct_reservoir_light(S, light, ux, uy, origin);
+          const F3 fc = candidate_contribution(sh, basis, wo, ls, S.lights[light].pdf);
+          bool selected;
+          if (!isfinite(ls.pdf) || !is_finite(fc) ||
+              !stream_candidate(r.reservoir, light, max_component(fc), proposal, random, selected)) {
+            r.flags |= 2u;
+            break;
+          }
+          if (selected) {
+            r.uv[0] = ux;
+            r.uv[1] = uy;
+            r.proposal = proposal;
+          }
+        }
+      }
+      if ((r.flags & 2u) == 0 && r.reservoir.weight_sum > 0.0f) {
+        const LightSample ls = reconstruct_reservoir_light(S, r.reservoir.sample, r.uv[0], r.uv[1], origin);
+        const float visibility = trace_shadow(S, origin, ls.direction, 0.0f, ls.distance);
+        const float normalization = reservoir_normalization(r.reservoir);
+        const F3 estimate = candidate_contribution(sh, basis, wo, ls, S.lights[r.reservoir.sample].pdf) *
+            (visibility * normalization);
+        if (!isfinite(normalization) || !is_finite(estimate))
+          r.flags |= 2u;
+        else
+          r.contribution = F4(estimate, visibility);
+      }
+    }
+  }
+  out[slot] = r;
+}
+
+// WriteTemporalReservoir (restir.slang:302-387).
+__global__ void __launch_bounds__(kBlock) k_restir_temporal(SceneView S,
+    const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
+    const TemporalInstance* __restrict__ identities, const RestirPixel* __restrict__ initial,
+    const ValidityPixel* __restrict__ validity, const TemporalPixel* __restrict__ surface,
+    const RestirReuse* __restrict__ previous, const RestirSurface* __restrict__ previous_surfaces,
+    RestirReuse* __restrict__ out, RestirSurface* __restrict__ out_surfaces) {
+  const FrameConst& f = *fcp;
+  const TemporalConst& tc = *tcp;
+  uint32_t px, py;
+  if (!pixel_of(blockIdx.x * blockDim.x + threadIdx.x, f.width, f.height, px, py)) return;
+  const uint32_t slot = py * f.width + px;
+  RestirReuse result = {};
+  RestirSurface receiver = {};
+  result.pixel = initial[slot];
+  result.previous_index = 0xffffffffu;
+  result.normalization = reservoir_normalization(result.pixel.reservoir);
+  result.supporting_candidates = result.pixel.reservoir.candidate_count;
+  const bool active = tc.restir_candidates != 0 && in_rect(f, px, py);
+  if (active) {
+    F3 ro, rd;
+    float tmax;
+    uint32_t camera_rng;
+    start_path(f, px, py, f.sample_index, ro, rd, tmax, camera_rng);
+    Hit hit;
+    if (trace_closest(S, ro, rd, 0.0f, tmax, camera_rng, hit)) {
+      const SurfaceHit sh = reconstruct_hit(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
+      const Frame basis = make_frame(sh.shading_normal);
+      const F3 wo = basis.to_local(-rd);
+      const F3 origin = offset_ray_origin(sh.position, sh.normal);
+      const float4 view = mul4(tc.current_view, sh.position.x, sh.position.y, sh.position.z, 1.0f);
+      receiver.origin = F4(origin, -view.z / view.w);
+      receiver.normal = F4(sh.normal, 0.0f);
+      receiver.shading_normal = F4(sh.shading_normal, 0.0f);
+      receiver.outgoing = F4(wo, 0.0f);
+      store_closure(sh.bsdf, receiver);
+      receiver.instance_id = identities[hit.instance].instance_id;
+      receiver.material_id = identities[hit.instance].material_id;
+      const ValidityPixel v = validity[slot];
+      const uint32_t previous_index = v.previous_index;
+      const bool history = v.valid != 0 && surface[slot].instance_id == receiver.instance_id &&
+          surface[slot].material_id == receiver.material_id;
+      if (tc.restir_history != 0 && (result.pixel.flags & 2u) == 0 && history) {
+        const RestirReuse source = previous[previous_index];
+        const RestirSurface& psrc = previous_surfaces[previous_index];
+        if ((source.pixel.flags & 1u) != 0 && (source.pixel.flags & 2u) == 0 &&
+            psrc.instance_id == receiver.instance_id && psrc.material_id == receiver.material_id) {
+          const uint32_t count = min(source.pixel.reservoir.candidate_count, tc.restir_max_history);
+          F3 received = V(0.0f);
+          if (source.pixel.reservoir.weight_sum > 0.0f) {
+            if (source.pixel.reservoir.sample >= S.light_count)
+              result.pixel.flags |= 2u;
+            else
+              received = history_contribution_uv(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
+          }
+          uint32_t rng = seed_random(slot, f.sample_index ^ 0x94D049BBu);
+          bool selected;
+          if (!is_finite(received) || (result.pixel.flags & 2u) != 0 ||
+              !merge_reevaluated(result.pixel.reservoir, source.pixel.reservoir, source.normalization,
+                  max_component(received), tc.restir_max_history, next_random(rng), selected)) {
+            result.pixel.flags |= 2u;
+          } else {
+            result.previous_index = previous_index;
+            if (selected) {
+              result.pixel.uv[0] = source.pixel.uv[0];
+              result.pixel.uv[1] = source.pixel.uv[1];
+              result.pixel.proposal = source.pixel.proposal;
+              result.age = min(source.age, 65535u) + 1u;
+            }
+            if (result.pixel.reservoir.weight_sum > 0.0f) {
+              bool valid_support;
+              const float support = history_target(S, source, psrc, result.pixel, valid_support);
+              if (!valid_support) result.pixel.flags |= 2u;
+              result.supporting_candidates = initial[slot].reservoir.candidate_count + (support > 0.0f ? count : 0u);
+            } else {
+              result.supporting_candidates = 0;
+            }
+            result.normalization = reuse_normalization(result.pixel.reservoir, result.supporting_candidates);
+          }
+        }
+      }
+      if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
+        const LightSample ls = reconstruct_reservoir_light(S, result.pixel.reservoir.sample,
+            result.pixel.uv[0], result.pixel.uv[1], origin);
+        const float visibility = receiver_visibility(S, result.pixel, initial[slot], origin, ls);
+        const F3 estimate = history_contribution(S, receiver, result.pixel.reservoir.sample, ls) *
+            (visibility * result.normalization);
+        if (!isfinite(result.normalization) || result.normalization <= 0.0f || !is_finite(estimate))
+          result.pixel.flags |= 2u;
+        else
+          result.pixel.contribution = F4(estimate, visibility);
+      }
+    }
+  }
+  out[slot] = result;
+  out_surfaces[slot] = receiver;
+}
+
+// SpatialCompatible (restir.slang:392-400).
+__device__ __forceinline__ bool spatial_compatible(const RestirSurface& receiver, const RestirReuse& record,
+    const RestirSurface& source) {
+  return (record.pixel.flags & 3u) == 1u && receiver.origin.w > 0.0f && source.origin.w > 0.0f &&
+      receiver.material_id == source.material_id &&
+      fabsf(receiver.origin.w - source.origin.w) <= 0.01f + 0.02f * fmaxf(receiver.origin.w, source.origin.w) &&
+      dot(V(receiver.normal), V(source.normal)) >= 0.9f &&
+      dot(V(receiver.shading_normal), V(source.shading_normal)) >= 0.9f;
+}
+
+// WriteSpatialReservoir (restir.slang:402-491): four axis neighbours at
+// the radius, merged with support correction.
+__global__ void __launch_bounds__(kBlock) k_restir_spatial(SceneView S,
+    const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
+    const RestirReuse* __restrict__ temporal, const RestirSurface* __restrict__ surfaces,
+    RestirReuse* __restrict__ out, uint4* __restrict__ out_sources) {
+  const FrameConst& f = *fcp;
+  const TemporalConst& tc = *tcp;
+  uint32_t px, py;
+  if (!pixel_of(blockIdx.x * blockDim.x + threadIdx.x, f.width, f.height, px, py)) return;
+  const uint32_t slot = py * f.width + px;
+  const RestirReuse centre = temporal[slot];
+  const RestirSurface receiver = surfaces[slot];
+  RestirReuse result = centre;
+  uint32_t sources[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
+  const int radius = (int)tc.restir_radius;
+  const int ox[4] = {-radius, radius, 0, 0};
+  const int oy[4] = {0, 0, -radius, radius};
+  if ((centre.pixel.flags & 3u) == 1u) {
+    uint32_t accepted = 0;
+    for (int i = 0; i < 4; ++i) {
+      const int nx = (int)px + ox[i], ny = (int)py + oy[i];
+      if (nx < 0 || ny < 0 || nx >= (int)f.width || ny >= (int)f.height) continue;
+      const uint32_t index = (uint32_t)ny * f.width + (uint32_t)nx;
+      if (spatial_compatible(receiver, temporal[index], surfaces[index])) {
+        sources[i] = index;
+        ++accepted;
+      }
+    }
+    if (accepted != 0) {
+      result.pixel.reservoir = empty_reservoir();
+      bool selected;
+      if (!merge_reevaluated(result.pixel.reservoir, centre.pixel.reservoir, centre.normalization,
+              centre.pixel.reservoir.selected_target, 0xffffffffu, 0.0f, selected))
+        result.pixel.flags |= 2u;
+      uint32_t rng = seed_random(slot, f.sample_index ^ 0x369DEA0Fu);
+      for (int i = 0; i < 4; ++i) {
+        if (sources[i] == 0xffffffffu) continue;
+        const RestirReuse source = temporal[sources[i]];
+        F3 received = V(0.0f);
+        if (source.pixel.reservoir.weight_sum > 0.0f)
+          received = history_contribution_uv(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
+        if (!is_finite(received) ||
+            !merge_reevaluated(result.pixel.reservoir, source.pixel.reservoir, source.normalization,
+                max_component(received), tc.restir_max_history, next_random(rng), selected)) {
+          result.pixel.flags |= 2u;
+          break;
+        }
+        if (selected) {
+          result.pixel.uv[0] = source.pixel.uv[0];
+          result.pixel.uv[1] = source.pixel.uv[1];
+          result.pixel.proposal = source.pixel.proposal;
+          result.age = source.age;
+        }
+      }
+      result.supporting_candidates = 0;
+      result.pixel.contribution = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
+        result.supporting_candidates = centre.pixel.reservoir.candidate_count;
+        for (int i = 0; i < 4; ++i) {
+          if (sources[i] == 0xffffffffu) continue;
+          const RestirReuse source = temporal[sources[i]];
+          bool valid_support;
+          const float support = history_target(S, source, surfaces[sources[i]], result.pixel, valid_support);
+          if (!valid_support) result.pixel.flags |= 2u;
+          if (support > 0.0f)
+            result.supporting_candidates += min(source.pixel.reservoir.candidate_count, tc.restir_max_history);
+        }
+      }
+      result.normalization = reuse_normalization(result.pixel.reservoir, result.supporting_candidates);
+      if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
+        const LightSample ls = reconstruct_reservoir_light(S, result.pixel.reservoir.sample,
+            result.pixel.uv[0], result.pixel.uv[1], V(receiver.origin));
+        const float visibility = receiver_visibility(S, result.pixel, centre.pixel, V(receiver.origin), ls);
+        const F3 estimate = history_contribution(S, receiver, result.pixel.reservoir.sample, ls) *
+            (visibility * result.normalization);
+        if (!isfinite(result.normalization) || result.normalization <= 0.0f || !is_finite(estimate))
+          result.pixel.flags |= 2u;
+        else
+          result.pixel.contribution = F4(estimate, visibility);
+      }
+    }
+  }
+  out[slot] = result;
+  out_sources[slot] = make_uint4(sources[0], sources[1], sources[2], sources[3]);
+}
+
+// ---------------------------------------------------------------------------
+// SVGF.
+
+// AccumulateTemporalRadiance (temporal.slang:229-267), without history
+// rectification: the count-capped blend of the fresh batch and the
+// reprojected history, and its illumination luminance moments.
+__global__ void __launch_bounds__(kBlock) k_svgf_accumulate(const TemporalConst* __restrict__ tcp,
+    const float4* __restrict__ batch, const TemporalPixel* __restrict__ surface,
+    const ValidityPixel* __restrict__ validity, const RadiancePixel* __restrict__ old,
+    RadiancePixel* __restrict__ out) {
+  const TemporalConst& tc = *tcp;
+  uint32_t px, py;
+  if (!pixel_of(blockIdx.x * blockDim.x + threadIdx.x, tc.width, tc.height, px, py)) return;
+  const uint32_t index = py * tc.width + px;
+  RadiancePixel o = {};
+  o.color = batch[index];
+  const uint32_t cap = tc.history_cap;
+  const TemporalPixel s = surface[index];
+  if ((s.flags & 1u) != 0) {
+    o.sample_count = min(tc.fresh_samples, cap);
+    const F3 d = demodulate(V(o.color), s.albedo);
+    const float l = luminance(d.x, d.y, d.z);
+    float m1 = l, m2 = l * l;
+    const ValidityPixel v = validity[index];
+    if (v.valid != 0) {
+      const RadiancePixel h = old[v.previous_index];
+      const uint32_t kept = min(h.sample_count, cap - o.sample_count);
+      if (kept != 0 && finite4(h.color) && isfinite(h.first_moment) && isfinite(h.second_moment)) {
+        const uint32_t count = kept + o.sample_count;
+        const float blend = float(kept) / float(count);
+        o.color.x += (h.color.x - o.color.x) * blend;
+        o.color.y += (h.color.y - o.color.y) * blend;
+        o.color.z += (h.color.z - o.color.z) * blend;
+        o.color.w += (h.color.w - o.color.w) * blend;
+        m1 += (h.first_moment - m1) * blend;
+        m2 += (h.second_moment - m2) * blend;
+        o.sample_count = count;
+      }
+    }
+    o.first_moment = m1;
+    o.second_moment = m2;
+  }
+  out[index] = o;
+}
+
+__device__ __forceinline__ bool variance_neighbour(const TemporalConst& tc, int qx, int qy,
+    unsigned long long instance_id, const RadiancePixel* radiance, const TemporalPixel* surface) {
+  if (qx < 0 || qy < 0 || qx >= (int)tc.width || qy >= (int)tc.height) return false;
+  const uint32_t i = (uint32_t)qy * tc.width + (uint32_t)qx;
+  return radiance[i].sample_count != 0 && surface[i].instance_id == instance_id;
+}
+
+__device__ __forceinline__ float variance_depth_step(const TemporalConst& tc, int ax, int ay, int bx,
+    int by, float depth, unsigned long long id, const RadiancePixel* radiance, const TemporalPixel* surface) {
+  float step = -1.0f;
+  if (variance_neighbour(tc, ax, ay, id, radiance, surface))
+    step = fabsf(depth - surface[(uint32_t)ay * tc.width + (uint32_t)ax].normal_depth.w);
+  if (variance_neighbour(tc, bx, by, id, radiance, surface)) {
+    const float other = fabsf(depth - surface[(uint32_t)by * tc.width + (uint32_t)bx].normal_depth.w);
+    step = step < 0.0f ? other : fminf(step, other);
+  }
+  return fmaxf(step, 0.0f);
+}
+
+// EstimateTemporalVariance (temporal.slang:313-370): temporal variance from
+// four or more batches, else the 7x7 edge-aware moments estimate; with a
+// filter, also iteration 0's input and the guides.
+__global__ void __launch_bounds__(kBlock) k_svgf_variance(const TemporalConst* __restrict__ tcp,
+    const TemporalPixel* __restrict__ surface, RadiancePixel* __restrict__ radiance,
+    float4* __restrict__ filter) {
+  const TemporalConst& tc = *tcp;
+  uint32_t px, py;
+  if (!pixel_of(blockIdx.x * blockDim.x + threadIdx.x, tc.width, tc.height, px, py)) return;
+  const int x = (int)px, y = (int)py;
+  const uint32_t index = py * tc.width + px;
+  const RadiancePixel center = radiance[index];
+  float variance = 0.0f;
+  const float batches = float(center.sample_count) / float(min(tc.fresh_samples, tc.history_cap));
+  if (center.sample_count != 0) {
+    if (batches >= 4.0f) {
+      variance = fmaxf(0.0f, center.second_moment - center.first_moment * center.first_moment);
+    } else {
+      const TemporalPixel s = surface[index];
+      const float depth = s.normal_depth.w;
+      const float phi = fmaxf(variance_depth_step(tc, x - 1, y, x + 1, y, depth, s.instance_id, radiance, surface) +
+          variance_depth_step(tc, x, y - 1, x, y + 1, depth, s.instance_id, radiance, surface), 1.0e-8f) * 3.0f;
+      float weight_sum = 0.0f, s1 = 0.0f, s2 = 0.0f;
+      for (int dy = -3; dy <= 3; ++dy) {
+        for (int dx = -3; dx <= 3; ++dx) {
+          const int qx = x + dx, qy = y + dy;
+          if (!variance_neighbour(tc, qx, qy, s.instance_id, radiance, surface)) continue;
+          const uint32_t qi = (uint32_t)qy * tc.width + (uint32_t)qx;
+          const float4 n = surface[qi].normal_depth;
+          const RadiancePixel nb = radiance[qi];
+          const float distance = sqrtf(float(dx * dx + dy * dy));
+          const float wz = dx == 0 && dy == 0 ? 0.0f : fabsf(depth - n.w) / (phi * distance);
+          const float wn = powf(saturate(dot(V(s.normal_depth), V(n))), 128.0f);
+          const float wl = fabsf(center.first_moment - nb.first_moment) / 10.0f;
+          const float w = expf(-(wl + wz)) * wn;
+          s1 += w * nb.first_moment;
+          s2 += w * nb.second_moment;
+          weight_sum += w;
+        }
+      }
+      const float m1 = s1 / fmaxf(weight_sum, 1.0e-6f), m2 = s2 / fmaxf(weight_sum, 1.0e-6f);
+      variance = fmaxf(0.0f, m2 - m1 * m1) * (4.0f / batches);
+    }
+  }
+  radiance[index].variance = variance;
+  if (tc.filter_iterations == 0) return;
+  const uint32_t pixels = tc.width * tc.height;
+  float4 input = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  uint4 guide = make_uint4(0u, 0u, kNoFilterGuide, 0u);
+  if (center.sample_count != 0) {
+    const TemporalPixel s = surface[index];
+    const F3 d = demodulate(V(center.color), s.albedo);
+    input = F4(d, variance / batches);
+    guide = make_uint4((uint32_t)s.instance_id, (uint32_t)(s.instance_id >> 32),
+        __float_as_uint(s.normal_depth.w), s.shading_normal);
+  }
+  filter[index] = input;
+  filter[2 * pixels + index] = make_float4(__uint_as_float(guide.x), __uint_as_float(guide.y),
+      __uint_as_float(guide.z), __uint_as_float(guide.w));
+}
+
+__device__ __forceinline__ uint4 filter_guide(const float4* filter, uint32_t pixels, uint32_t i) {
+  const float4 g = filter[2 * pixels + i];
+  return make_uint4(__float_as_uint(g.x), __float_as_uint(g.y), __float_as_uint(g.z), __float_as_uint(g.w));
+}
+
+__device__ __forceinline__ bool filter_neighbour(const TemporalConst& tc, const float4* filter, int qx,
+    int qy, uint32_t ix, uint32_t iy, uint4& guide) {
+  guide = make_uint4(0u, 0u, kNoFilterGuide, 0u);
+  if (qx < 0 || qy < 0 || qx >= (int)tc.width || qy >= (int)tc.height) return false;
+  guide = filter_guide(filter, tc.width * tc.height, (uint32_t)qy * tc.width + (uint32_t)qx);
+  return guide.z != kNoFilterGuide && guide.x == ix && guide.y == iy;
+}
+
+__device__ __forceinline__ float filter_depth_step(const TemporalConst& tc, const float4* filter, int ax,
+    int ay, int bx, int by, float depth, uint32_t ix, uint32_t iy) {
+  float step = -1.0f;
+  uint4 g;
+  if (filter_neighbour(tc, filter, ax, ay, ix, iy, g)) step = fabsf(depth - __uint_as_float(g.z));
+  if (filter_neighbour(tc, filter, bx, by, ix, iy, g)) {
+    const float other = fabsf(depth - __uint_as_float(g.z));
+    step = step < 0.0f ? other : fminf(step, other);
+  }
+  return fmaxf(step, 0.0f);
+}
+
+// FilterIteration (temporal.slang:405-457).
+__device__ __forceinline__ float4 filter_iteration(const TemporalConst& tc, const float4* __restrict__ filter,
+    int x, int y, uint32_t iteration) {
+  const uint32_t pixels = tc.width * tc.height;
+  const uint32_t index = (uint32_t)y * tc.width + (uint32_t)x;
+  const uint4 center = filter_guide(filter, pixels, index);
+  if (center.z == kNoFilterGuide) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float4* in = filter + (size_t)(iteration & 1u) * pixels;
+  uint4 g;
+  float gaussian = 0.0f, gaussian_weight = 0.0f;
+  for (int dy = -1; dy <= 1; ++dy) {
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int qx = x + dx, qy = y + dy;
+      if (!filter_neighbour(tc, filter, qx, qy, center.x, center.y, g)) continue;
+      const float k = (dx == 0 ? 0.5f : 0.25f) * (dy == 0 ? 0.5f : 0.25f);
+      gaussian += k * in[(uint32_t)qy * tc.width + (uint32_t)qx].w;
+      gaussian_weight += k;
+    }
+  }
+  const float phi_l = 4.0f * sqrtf(fmaxf(gaussian / gaussian_weight, 0.0f) + 1.0e-10f);
+  const float depth = __uint_as_float(center.z);
+  const float phi_z = fmaxf(filter_depth_step(tc, filter, x - 1, y, x + 1, y, depth, center.x, center.y) +
+      filter_depth_step(tc, filter, x, y - 1, x, y + 1, depth, center.x, center.y), 1.0e-8f);
+  const F3 normal = unpack_normal(center.w);
+  const float4 cv = in[index];
+  const float lum = luminance(cv.x, cv.y, cv.z);
+  const int step = 1 << iteration;
+  const float kernel[3] = {0.375f, 0.25f, 0.0625f};
+  float sx = 0.0f, sy = 0.0f, sz = 0.0f, var = 0.0f, weight_sum = 0.0f;
+  for (int ty = -2; ty <= 2; ++ty) {
+    for (int tx = -2; tx <= 2; ++tx) {
+      const int qx = x + tx * step, qy = y + ty * step;
+      if (!filter_neighbour(tc, filter, qx, qy, center.x, center.y, g)) continue;
+      const float4 value = in[(uint32_t)qy * tc.width + (uint32_t)qx];
+      float w = kernel[abs(tx)] * kernel[abs(ty)];
+      if (tx != 0 || ty != 0) {
+        const float distance = float(step) * sqrtf(float(tx * tx + ty * ty));
+        const float wz = fabsf(depth - __uint_as_float(g.z)) / (phi_z * distance);
+        const float wl = fabsf(lum - luminance(value.x, value.y, value.z)) / phi_l;
+        const F3 other = unpack_normal(g.w);
+        const float wn = powf(saturate(dot(normal, other)), 128.0f);
+        w = w * expf(-(wl + wz)) * wn;
+      }
+      sx += w * value.x;
+      sy += w * value.y;
+      sz += w * value.z;
+      var += w * w * value.w;
+      weight_sum += w;
+    }
+  }
+  return make_float4(sx / weight_sum, sy / weight_sum, sz / weight_sum, var / (weight_sum * weight_sum));
+}
+
+// One a-trous iteration (FilterTemporalRadiance, temporal.slang:459-464),
+// or, for the last, the composite (temporal.slang:468-475) into the colour.
+__global__ void __launch_bounds__(kBlock) k_svgf_filter(const TemporalConst* __restrict__ tcp,
+    float4* __restrict__ filter, uint32_t iteration, uint32_t composite,
+    const RadiancePixel* __restrict__ radiance, const TemporalPixel* __restrict__ surface,
+    float4* __restrict__ color) {
+  const TemporalConst& tc = *tcp;
+  uint32_t px, py;
+  if (!pixel_of(blockIdx.x * blockDim.x + threadIdx.x, tc.width, tc.height, px, py)) return;
+  const uint32_t index = py * tc.width + px;
+  const uint32_t pixels = tc.width * tc.height;
+  if (!composite) {
+    filter[(size_t)((iteration + 1) & 1u) * pixels + index] = filter_iteration(tc, filter, (int)px, (int)py, iteration);
+    return;
+  }
+  const RadiancePixel r = radiance[index];
+  if (r.sample_count == 0) {
+    color[index] = r.color;
+    return;
+  }
+  const float4 v = filter_iteration(tc, filter, (int)px, (int)py, iteration);
+  color[index] = F4(remodulate(V(v), surface[index].albedo), r.color.w);
+}
+
+// The radiance history's colour as the frame's colour (no filter).
+__global__ void k_copy_radiance_color(const TemporalConst* __restrict__ tcp,
+    const RadiancePixel* __restrict__ radiance, float4* __restrict__ color) {
+  const TemporalConst& tc = *tcp;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < tc.width * tc.height) color[i] = radiance[i].color;
+}
+
+inline uint32_t grid(uint32_t n) { return (n + kBlock - 1) / kBlock; }
+
+}  // namespace
+
+void launch_temporal_surface(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
+    const TemporalInstance* ids, TemporalPixel* out, uint32_t pixels, cudaStream_t s) {
+  k_temporal_surface<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, ids, out);
+}
+
+void launch_reproject(const TemporalConst* tc, const TemporalPixel* current, const TemporalPixel* previous,
+    ValidityPixel* out, uint32_t pixels, cudaStream_t s) {
+  k_reproject<<<grid(pixels), kBlock, 0, s>>>(tc, current, previous, out);
+}
+
+void launch_restir_initial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
+    RestirPixel* out, uint32_t pixels, cudaStream_t s) {
+  k_restir_initial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out);
+}
+
+void launch_restir_temporal(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
+    const TemporalInstance* ids, const RestirPixel* initial, const ValidityPixel* validity,
+    const TemporalPixel* surface, const RestirReuse* previous, const RestirSurface* previous_surfaces,
+    RestirReuse* out, RestirSurface* out_surfaces, uint32_t pixels, cudaStream_t s) {
+  k_restir_temporal<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, ids, initial, validity, surface, previous,
+      previous_surfaces, out, out_surfaces);
+}
+
+void launch_restir_spatial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
+    const RestirReuse* temporal, const RestirSurface* surfaces, RestirReuse* out, uint4* sources,
+    uint32_t pixels, cudaStream_t s) {
+  k_restir_spatial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, temporal, surfaces, out, sources);
+}
+
+void launch_svgf(const TemporalConst* tc, const TemporalConst& host_tc, const float4* batch,
+    const TemporalPixel* surface, const ValidityPixel* validity, const RadiancePixel* old,
+    RadiancePixel* radiance, float4* filter, float4* color, uint32_t pixels, cudaStream_t s) {
+  k_svgf_accumulate<<<grid(pixels), kBlock, 0, s>>>(tc, batch, surface, validity, old, radiance);
+  k_svgf_variance<<<grid(pixels), kBlock, 0, s>>>(tc, surface, radiance, filter);
+  if (host_tc.filter_iterations == 0) {
+    k_copy_radiance_color<<<grid(pixels), kBlock, 0, s>>>(tc, radiance, color);
+    return;
+  }
+  for (uint32_t i = 0; i < host_tc.filter_iterations; ++i)
+    k_svgf_filter<<<grid(pixels), kBlock, 0, s>>>(tc, filter, i, i + 1 == host_tc.filter_iterations ? 1u : 0u,
+        radiance, surface, color);
+}
+
+}  // namespace lotus

@@ -1,0 +1,34 @@
+// SPDX-License-Identifier: Apache-2.0
+// Launchers of the temporal passes (temporal.cu).
+#pragma once
+
+#include "integrator.cuh"
+#include "temporal.cuh"
+
+namespace lotus {
+
+void launch_temporal_surface(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
+    const TemporalInstance* ids, TemporalPixel* out, uint32_t pixels, cudaStream_t s);
+
+void launch_reproject(const TemporalConst* tc, const TemporalPixel* current, const TemporalPixel* previous,
+    ValidityPixel* out, uint32_t pixels, cudaStream_t s);
+
+void launch_restir_initial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
+    RestirPixel* out, uint32_t pixels, cudaStream_t s);
+
+void launch_restir_temporal(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
+    const TemporalInstance* ids, const RestirPixel* initial, const ValidityPixel* validity,
+    const TemporalPixel* surface, const RestirReuse* previous, const RestirSurface* previous_surfaces,
+    RestirReuse* out, RestirSurface* out_surfaces, uint32_t pixels, cudaStream_t s);
+
+void launch_restir_spatial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
+    const RestirReuse* temporal, const RestirSurface* surfaces, RestirReuse* out, uint4* sources,
+    uint32_t pixels, cudaStream_t s);
+
+// Accumulation, variance, the a-trous iterations and the composite into
+// `color` (or the accumulated colour without iterations).
+void launch_svgf(const TemporalConst* tc, const TemporalConst& host_tc, const float4* batch,
+    const TemporalPixel* surface, const ValidityPixel* validity, const RadiancePixel* old,
+    RadiancePixel* radiance, float4* filter, float4* color, uint32_t pixels, cudaStream_t s);
+
+}  // namespace lotus

@@ -275,6 +275,11 @@ struct FrameConst {
   uint32_t accumulated;
   uint32_t add_sample;
   uint32_t environment_background;
+  // RestirInitial: the depth-0 direct light is the final reservoir's
+  // (restir_final: RestirPixel records `restir_stride` bytes apart).
+  uint32_t restir_primary;
+  uint32_t restir_stride;
+  const unsigned char* restir_final;
 };
 
 // CameraRay (scene.slang:273-283).

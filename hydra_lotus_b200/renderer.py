@@ -54,6 +54,14 @@ def lib():
         L.lotus_cuda_render_static.restype = C.c_int32
         L.lotus_cuda_render_static.argtypes = [C.c_void_p, C.POINTER(abi.FrameDesc), C.c_void_p,
                                                C.POINTER(abi.FrameResult)]
+        L.lotus_cuda_set_temporal_instances.restype = C.c_int32
+        L.lotus_cuda_set_temporal_instances.argtypes = [C.c_void_p, C.POINTER(abi.TemporalInstance),
+                                                        C.c_uint32]
+        L.lotus_cuda_render_temporal.restype = C.c_int32
+        L.lotus_cuda_render_temporal.argtypes = [C.c_void_p, C.POINTER(abi.TemporalDesc),
+                                                 C.POINTER(abi.FrameResult), C.c_void_p]
+        L.lotus_cuda_read_product.restype = C.c_int64
+        L.lotus_cuda_read_product.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64]
         L.lotus_cuda_read_light_table.restype = C.c_int64
         L.lotus_cuda_read_light_table.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64,
                                                   C.c_void_p, C.c_uint64]
@@ -144,6 +152,33 @@ class CudaOffscreenRenderer:
         lib().lotus_cuda_render_static(self.handle, C.byref(frame), C.c_void_p(color_device_ptr),
                                        C.byref(res))
         return res
+
+    def render_temporal(self, temporal, color=None):
+        """RenderTemporalScene: returns (lotus_frame_result, colour)."""
+        res = abi.FrameResult()
+        t = temporal.frame.target
+        ptr = None
+        if t.read_back:
+            if color is None:
+                color = np.empty((t.height, t.width, 4), dtype=np.float32)
+            ptr = color.ctypes.data
+        lib().lotus_cuda_render_temporal(self.handle, C.byref(temporal), C.byref(res), ptr)
+        return res, (color if t.read_back else None)
+
+    def set_temporal_instances(self, records):
+        arr = (abi.TemporalInstance * max(1, len(records)))(*records)
+        rc = lib().lotus_cuda_set_temporal_instances(self.handle, arr, len(records))
+        if rc != abi.PASS:
+            raise RendererError(rc, "set_temporal_instances failed")
+
+    def read_product(self, product, height, width):
+        """A temporal product as a structured (H, W) numpy array."""
+        dtype = abi.PRODUCT_DTYPES[product]
+        out = np.zeros((height, width), dtype=dtype)
+        n = lib().lotus_cuda_read_product(self.handle, product, out.ctypes.data, out.nbytes)
+        if n < 0:
+            raise RendererError(abi.FAIL, f"product {product} is not available")
+        return out
 
     def read_color(self, out):
         rc = lib().lotus_cuda_read_color(self.handle, out.ctypes.data, out.size)

@@ -482,3 +482,41 @@ def sphere_field(seed=0, width=1920, height=1080, prototypes=320, grid=100,
     s.world_to_clip = multiply(perspective(50.0, width / height, 0.1, 1000.0), view)
     s.width, s.height = width, height
     return s
+
+
+def restir_room(seed=0, size=96, emitters=10000, sigma=2.0, aspect=1.0):
+    """The box room with ``emitters`` small emissive triangles on its floor,
+    their power log-normal (sigma 2), and the ceiling light removed: a
+    many-light scene for ReSTIR DI. Lambert walls and boxes."""
+    rng = np.random.default_rng(seed + 1000)
+    s = box_room(seed=seed, size=size)
+    s.name = f"restir-room-{seed}-{emitters}"
+    # Drop the ceiling light (instance 5): many small lights instead.
+    s.instances = [inst for k, inst in enumerate(s.instances) if k != 5]
+    tri = s.add_geometry(np.array([[-0.5, 0.0, -0.2887], [0.5, 0.0, -0.2887], [0.0, 0.0, 0.5774]],
+                                  dtype=F32), np.array([[0, 2, 1]], dtype=np.uint32))
+    for k in range(emitters):
+        side = F32(rng.uniform(0.01, 0.04))
+        power = math.exp(rng.normal(0.0, sigma))
+        area = 0.4330127 * float(side) ** 2
+        radiance = 0.02 * power / area / max(1.0, emitters / 100.0)
+        tint = rng.uniform(0.5, 1.0, 3)
+        mat = s.add_material(preview_material((0.0, 0.0, 0.0), ior=1.0,
+                                              emission=tuple(radiance * tint)))
+        lin = rotation_y(rng.uniform(0, 2 * math.pi)) * float(side)
+        pos = (rng.uniform(-0.95, 0.95), -0.999, rng.uniform(-0.95, 0.95))
+        s.add_instance(tri, mat, affine(lin, pos))
+    s.width = int(size * aspect)
+    s.height = size
+    return s
+
+
+def orbit_camera(frame, frames=120, radius=3.0, amplitude=0.35, aspect=1.0):
+    """The view and world-to-clip of frame ``frame`` of a camera swinging
+    about the box room's vertical axis, looking at its centre (45 degree
+    vertical field of view, as the Cornell camera)."""
+    theta = amplitude * math.sin(2.0 * math.pi * frame / frames)
+    eye = (radius * math.sin(theta), 0.0, radius * math.cos(theta))
+    view = look_at(eye, (0.0, 0.0, 0.0))
+    projection = perspective(45.0, aspect, 1.0, 10.0)
+    return view, multiply(projection, view)

@@ -249,6 +249,73 @@ int32_t lotus_cuda_update_scene(lotus_cuda_renderer* renderer,
 int32_t lotus_cuda_render(lotus_cuda_renderer* renderer,
     const lotus_frame_desc* frame, lotus_frame_result* result, float* color);
 
+/* TemporalFrameSettings (include/lotus/temporal.hpp:58-98) and the
+ * snapshot cameras of one RenderTemporalScene call
+ * (vulkan_backend.hpp:807-810). The host keeps the reference's
+ * TemporalHistory (temporal.hpp:112-125) and says whether it kept the
+ * preceding frame. */
+typedef struct lotus_temporal_desc {
+  lotus_frame_desc frame;            /* this frame's camera, target and settings */
+  float current_view[16];            /* Camera::view of this frame */
+  float previous_view[16];           /* the preceding frame's Camera::view */
+  float previous_world_to_clip[16];  /* the preceding frame's projection * view, OpenGL clip */
+  float validation[4];               /* absolute depth, relative depth, min normal cosine, max motion (px) */
+  uint32_t history_available;        /* TemporalFrame::previous is present */
+  uint32_t accumulate_radiance;
+  uint32_t max_history_samples;      /* 1..65536 when accumulating */
+  uint32_t filter_iterations;        /* 0..8; needs accumulate_radiance */
+  uint32_t history_rectification;    /* TemporalHistoryRectification; only None (0) is built */
+  uint32_t reserved;
+} lotus_temporal_desc;
+
+/* One instance's temporal identity (the reference's TemporalInstanceRecord,
+ * backend/vulkan/temporal_metadata.hpp), in scene instance order. */
+typedef struct lotus_temporal_instance {
+  float previous_world_from_object[16];
+  uint64_t instance_id;
+  uint64_t material_id;
+  uint32_t flags;     /* 2: rigid correspondence with the preceding frame, 4: unchanged material */
+  uint32_t reserved;
+} lotus_temporal_instance;
+
+/* Replaces the instances' temporal identities. Until called after a scene
+ * update, each instance's ids are its index and material slot, its previous
+ * transform its current one, and its flags 6. */
+int32_t lotus_cuda_set_temporal_instances(lotus_cuda_renderer* renderer,
+    const lotus_temporal_instance* instances, uint32_t count);
+
+/* RenderTemporalScene (vulkan_backend.hpp:807-810): the primary-surface
+ * metadata and its reprojection; with RestirInitial light sampling the
+ * ReSTIR DI initial, temporal (restir_temporal) and spatial (restir_spatial)
+ * reservoir passes; one fresh batch of frame_count samples whose primary
+ * direct light is the final reservoir's; and with accumulate_radiance the
+ * SVGF accumulation, variance and filter_iterations a-trous iterations into
+ * the colour. */
+int32_t lotus_cuda_render_temporal(lotus_cuda_renderer* renderer,
+    const lotus_temporal_desc* temporal, lotus_frame_result* result, float* color);
+
+/* Temporal products (the reference's TemporalProducts and RestirProducts,
+ * vulkan_backend.hpp:90-200), read back from the device. */
+#define LOTUS_PRODUCT_SURFACE 1u            /* TemporalPixel, 64 B/pixel, this frame */
+#define LOTUS_PRODUCT_PREVIOUS_SURFACE 2u   /* TemporalPixel, the preceding frame */
+#define LOTUS_PRODUCT_VALIDITY 3u           /* TemporalValidityPixel, 16 B/pixel */
+#define LOTUS_PRODUCT_RADIANCE 4u           /* TemporalRadiancePixel, 32 B/pixel */
+#define LOTUS_PRODUCT_PREVIOUS_RADIANCE 5u
+#define LOTUS_PRODUCT_BATCH 6u              /* the fresh batch's RGBA mean, 16 B/pixel */
+#define LOTUS_PRODUCT_RESTIR_INITIAL 7u     /* RestirPixel, 48 B/pixel */
+#define LOTUS_PRODUCT_RESTIR_TEMPORAL 8u    /* RestirReusePixel, 64 B/pixel */
+#define LOTUS_PRODUCT_RESTIR_PREVIOUS 9u
+#define LOTUS_PRODUCT_RESTIR_SPATIAL 10u
+#define LOTUS_PRODUCT_RESTIR_SOURCES 11u    /* 4 u32 per pixel */
+#define LOTUS_PRODUCT_RESTIR_SURFACES 12u   /* 160 B/pixel */
+#define LOTUS_PRODUCT_RESTIR_PREVIOUS_SURFACES 13u
+#define LOTUS_PRODUCT_FILTER 14u            /* 3 float4 per pixel: two ping-pong halves, guides */
+
+/* Copies a product of the latest temporal frame into `out`; returns the
+ * bytes copied, or -1 when the product does not exist or does not fit. */
+int64_t lotus_cuda_read_product(lotus_cuda_renderer* renderer, uint32_t product, void* out,
+    uint64_t capacity_bytes);
+
 /* The colour of the latest frame into host memory (width*height*4 floats). */
 int32_t lotus_cuda_read_color(lotus_cuda_renderer* renderer, float* color,
     uint64_t capacity_floats);

@@ -1447,12 +1447,17 @@ struct PathState {
 };
 constexpr uint32_t kUnweightedLight = 1;
 
+struct RestirRecord;  // below
+
 struct FrameConstants {
   float clip_to_world[16];
   float ndc_from_pixel[4];
   uint32_t width;
   uint32_t max_bounces;
   bool sample_lights;
+  // RestirInitial: the depth-0 direct light is the final reservoir's.
+  const unsigned char* restir_final = nullptr;
+  uint32_t restir_stride = 0;
 };
 
 struct RayCounts {
@@ -1533,6 +1538,45 @@ F3 DirectLight(const oracle_scene& s, const SurfaceHit& sh, const ShadingFrame& 
   return ShadowedLight(s, sh, basis, wo, origin, SampleLight(s, u, origin), rays);
 }
 
+// The reservoir records (restir.slang:11-60; vulkan_backend.hpp:152-178).
+struct Reservoir {
+  uint32_t sample;
+  float weight_sum;
+  float selected_target;
+  uint32_t candidate_count;
+};
+struct RestirRecord {
+  Reservoir reservoir;
+  float uv[2];
+  float proposal;
+  uint32_t flags;
+  float contribution[4];
+};
+static_assert(sizeof(RestirRecord) == 48, "RestirPixel is 48 bytes");
+constexpr uint32_t kNoReservoirSample = 0xFFFFFFFFu;
+
+// ReconstructReservoirLight (scene.slang:939-967) for emissive triangles and
+// the environment.
+LightSample ReconstructReservoirLight(const oracle_scene& s, uint32_t index, float ux, float uy, F3 origin) {
+  const LightRecord& chosen = s.lights[index];
+  if (chosen.instance == kEnvironmentLight) return SampleEnvironment(s, chosen.pdf, ux, uy);
+  return SampleTriangle(s, index, chosen, ux, uy, origin);
+}
+
+// InitialDirectLight (restir.slang:235-254).
+F3 InitialDirectLight(const oracle_scene& s, const FrameConstants& f, uint32_t pixel, const SurfaceHit& sh,
+    const ShadingFrame& basis, F3 wo) {
+  RestirRecord sel;
+  std::memcpy(&sel, f.restir_final + size_t{pixel} * f.restir_stride, sizeof(sel));
+  if ((sel.flags & 2u) != 0 || !(sel.reservoir.weight_sum > 0.0f) || sel.reservoir.sample >= s.lights.size())
+    return V(0.0f);
+  const F3 origin = OffsetRayOrigin(sh.position, sh.normal);
+  const LightSample ls = ReconstructReservoirLight(s, sel.reservoir.sample, sel.uv[0], sel.uv[1], origin);
+  const F3 wi = basis.ToLocal(ls.direction);
+  const float weight = ls.delta ? 1.0f : PowerHeuristic(ls.pdf, wi.z > 0.0f ? PreviewPdf(sh.bsdf, wo, wi) : 0.0f);
+  return V(sel.contribution[0], sel.contribution[1], sel.contribution[2]) * weight;
+}
+
 // EmissionWeight (transport.slang:150-158).
 float EmissionWeight(const oracle_scene& s, const PathState& p, const Hit& hit, const SurfaceHit& sh) {
   const float area_pdf = EmitterPdf(s, hit, sh.area);
@@ -1558,7 +1602,9 @@ bool ScatterPath(const oracle_scene& s, const FrameConstants& f, PathState& p, c
   }
   const ShadingFrame basis = MakeShadingFrame(sh.shading_normal);
   const F3 wo = basis.ToLocal(-p.ray.direction);
-  if (f.sample_lights)
+  if (f.restir_final && p.depth == 0)
+    p.radiance = p.radiance + p.throughput * InitialDirectLight(s, f, p.pixel_index, sh, basis, wo);
+  else if (f.sample_lights)
     p.radiance = p.radiance + p.throughput * DirectLight(s, sh, basis, wo, p.rng, rays);
   F3 u;
   u.x = NextRandom(p.rng);
@@ -1911,6 +1957,663 @@ int32_t oracle_traversal_stats(const oracle_scene* s, const lotus_frame_desc* d,
   }
   if (nodes_per_ray) *nodes_per_ray = n ? double(c.nodes) / n : 0.0;
   if (triangles_per_ray) *triangles_per_ray = n ? double(c.triangles) / n : 0.0;
+  return LOTUS_PASS;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Temporal passes: the primary-surface metadata (temporal.slang:557-627) and
+// the ReSTIR DI reservoir passes (restir.slang:163-491), restated on the CPU
+// over the same records the CUDA kernels write.
+
+namespace {
+
+struct TemporalPixelO {
+  float normal_depth[4];
+  float motion_depth[4];
+  uint64_t instance_id;
+  uint64_t material_id;
+  uint32_t flags, albedo, shading_normal, reserved;
+};
+static_assert(sizeof(TemporalPixelO) == 64, "TemporalPixel is 64 bytes");
+struct ValidityO {
+  uint32_t valid, rejection, previous_index, reserved;
+};
+struct RestirReuseO {
+  RestirRecord pixel;
+  float normalization;
+  uint32_t supporting_candidates;
+  uint32_t previous_index;
+  uint32_t age;
+};
+static_assert(sizeof(RestirReuseO) == 64, "RestirReuse is 64 bytes");
+struct RestirSurfaceO {
+  float origin[4], normal[4], shading_normal[4], outgoing[4], base_alpha[4], dielectric_metallic[4],
+      fresnel[4], model[4], extension[4];
+  uint64_t instance_id, material_id;
+};
+static_assert(sizeof(RestirSurfaceO) == 160, "RestirSurface is 160 bytes");
+
+inline void Mul4(const float* m, float x, float y, float z, float w, float* o) {
+  for (int r = 0; r < 4; ++r) o[r] = m[r] * x + m[4 + r] * y + m[8 + r] * z + m[12 + r] * w;
+}
+
+inline bool Finite4(const float* v) {
+  return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]) && std::isfinite(v[3]);
+}
+
+inline float Saturate(float x) { return std::fmin(std::fmax(x, 0.0f), 1.0f); }
+
+uint32_t PackAlbedo(F3 c) {
+  const uint32_t x = static_cast<uint32_t>(std::rint(Saturate(c.x) * 255.0f));
+  const uint32_t y = static_cast<uint32_t>(std::rint(Saturate(c.y) * 255.0f));
+  const uint32_t z = static_cast<uint32_t>(std::rint(Saturate(c.z) * 255.0f));
+  return x | (y << 8) | (z << 16);
+}
+
+// PackNormal (temporal.slang:111-117).
+uint32_t PackNormal(F3 n) {
+  const float s = std::fabs(n.x) + std::fabs(n.y) + std::fabs(n.z);
+  float ex = n.x / s, ey = n.y / s;
+  if (n.z < 0.0f) {
+    const float ox = (1.0f - std::fabs(ey)) * (ex >= 0.0f ? 1.0f : -1.0f);
+    const float oy = (1.0f - std::fabs(ex)) * (ey >= 0.0f ? 1.0f : -1.0f);
+    ex = ox;
+    ey = oy;
+  }
+  const int qx = static_cast<int>(std::rint(std::fmin(std::fmax(ex, -1.0f), 1.0f) * 32767.0f));
+  const int qy = static_cast<int>(std::rint(std::fmin(std::fmax(ey, -1.0f), 1.0f) * 32767.0f));
+  return (static_cast<uint32_t>(qx) & 0xffffu) | (static_cast<uint32_t>(qy) << 16);
+}
+
+struct TemporalIds {
+  float previous[12];  // rows
+  uint64_t instance_id, material_id;
+  uint32_t flags;
+};
+
+std::vector<TemporalIds> ConvertIds(const oracle_scene& s, const lotus_temporal_instance* ids) {
+  std::vector<TemporalIds> out(s.instances.size());
+  for (size_t i = 0; i < out.size(); ++i) {
+    const float* m = ids ? ids[i].previous_world_from_object : s.instances[i].m;
+    for (int r = 0; r < 3; ++r) {
+      out[i].previous[4 * r] = m[r];
+      out[i].previous[4 * r + 1] = m[4 + r];
+      out[i].previous[4 * r + 2] = m[8 + r];
+      out[i].previous[4 * r + 3] = m[12 + r];
+    }
+    out[i].instance_id = ids ? ids[i].instance_id : i;
+    out[i].material_id = ids ? ids[i].material_id : s.instances[i].material;
+    out[i].flags = ids ? ids[i].flags : 6u;
+  }
+  return out;
+}
+
+inline F3 RowPoint(const float* r, F3 p) {
+  return V(r[0] * p.x + r[1] * p.y + r[2] * p.z + r[3], r[4] * p.x + r[5] * p.y + r[6] * p.z + r[7],
+      r[8] * p.x + r[9] * p.y + r[10] * p.z + r[11]);
+}
+
+// WriteTemporalSurface (temporal.slang:557-627).
+TemporalPixelO TemporalSurface(const oracle_scene& s, const FrameConstants& f, const oracle_temporal& tc,
+    const std::vector<TemporalIds>& ids, uint32_t px, uint32_t py) {
+  TemporalPixelO o{};
+  const uint32_t index = py * f.width + px;
+  uint32_t rng = SeedRandom(index, 0);
+  const float cx = float(px) + 0.5f, cy = float(py) + 0.5f;
+  const Ray ray = CameraRay(f, cx * f.ndc_from_pixel[0] + f.ndc_from_pixel[2],
+      cy * f.ndc_from_pixel[1] + f.ndc_from_pixel[3], 1.0f);
+  Hit hit;
+  if (!Trace(s, ray, rng, hit)) return o;
+  const Instance& inst = s.instances[hit.instance];
+  const Geometry& g = s.geometries[inst.geometry];
+  const TemporalIds& id = ids[hit.instance];
+  const uint32_t* tri = &g.triangles[3 * hit.primitive];
+  const F3 p0 = g.positions[tri[0]], p1 = g.positions[tri[1]], p2 = g.positions[tri[2]];
+  const F3 point = p0 + hit.b1 * (p1 - p0) + hit.b2 * (p2 - p0);
+  const F3 world = TransformPoint(inst.m, point);
+  float view[4];
+  Mul4(tc.current_view, world.x, world.y, world.z, 1.0f, view);
+  const F3 a = TransformPoint(inst.m, p0), b = TransformPoint(inst.m, p1), c = TransformPoint(inst.m, p2);
+  F3 normal = normalize(cross(b - a, c - a));
+  if (dot(normal, ray.direction) > 0.0f) normal = -normal;
+  const float depth = -view[2] / view[3];
+  if (!(Finite4(view) && IsFinite(normal) && view[3] > 0.0f && depth > 0.0f)) return o;
+  o.normal_depth[0] = normal.x; o.normal_depth[1] = normal.y; o.normal_depth[2] = normal.z;
+  o.normal_depth[3] = depth;
+  o.instance_id = id.instance_id;
+  o.material_id = id.material_id;
+  o.flags = 1u | id.flags;
+  const SurfaceHit sh = ReconstructHit(s, hit, ray.direction);
+  const F3 albedo = sh.bsdf.transmission > 0.0f
+      ? sh.base_color + sh.bsdf.transmission * (sh.bsdf.transmission_color - sh.base_color)
+      : sh.base_color;
+  o.albedo = PackAlbedo(albedo);
+  o.shading_normal = PackNormal(sh.shading_normal);
+  if (id.flags & 2u) {
+    const F3 pw = RowPoint(id.previous, point);
+    float pv[4], clip[4];
+    Mul4(tc.previous_view, pw.x, pw.y, pw.z, 1.0f, pv);
+    Mul4(tc.previous_world_to_clip, pw.x, pw.y, pw.z, 1.0f, clip);
+    const float qx = clip[0] / clip[3], qy = clip[1] / clip[3], qz = clip[2] / clip[3];
+    const float pd = -pv[2] / pv[3];
+    const float ppx = tc.previous_display[0] + (qx * 0.5f + 0.5f) * tc.previous_display[2];
+    const float ppy = tc.previous_display[1] + (qy * 0.5f + 0.5f) * tc.previous_display[3];
+    const float bx = float(tc.previous_data[0]), by = float(tc.previous_data[1]);
+    const float ex = bx + float(tc.previous_data[2]), ey = by + float(tc.previous_data[3]);
+    if (Finite4(pv) && Finite4(clip) && std::isfinite(ppx) && std::isfinite(ppy) && std::isfinite(pd) &&
+        pv[3] > 0.0f && clip[3] > 0.0f && pd > 0.0f && qz >= 0.0f && qz <= 1.0f && qx >= -1.0f &&
+        qy >= -1.0f && qx < 1.0f && qy < 1.0f && ppx >= bx && ppy >= by && ppx < ex && ppy < ey) {
+      o.motion_depth[0] = ppx - cx;
+      o.motion_depth[1] = ppy - cy;
+      o.motion_depth[2] = pd;
+      o.motion_depth[3] = 1.0f;
+    }
+  }
+  return o;
+}
+
+// Reservoir arithmetic in float (reservoir.slang:23-103).
+bool StreamCandidate(Reservoir& r, uint32_t sample, float target, float proposal, float random, bool& selected) {
+  selected = false;
+  const bool valid_zero = r.weight_sum == 0.0f && r.sample == kNoReservoirSample && r.selected_target == 0.0f;
+  const bool valid_positive = r.weight_sum > 0.0f && r.sample != kNoReservoirSample &&
+      r.selected_target > 0.0f && r.candidate_count != 0;
+  if (!std::isfinite(r.weight_sum) || !std::isfinite(r.selected_target) || !(valid_zero || valid_positive) ||
+      !std::isfinite(target) || target < 0.0f || !std::isfinite(proposal) || proposal <= 0.0f ||
+      !std::isfinite(random) || random < 0.0f || random >= 1.0f ||
+      (target > 0.0f && sample == kNoReservoirSample) || r.candidate_count == 0xFFFFFFFFu)
+    return false;
+  const float weight = target / proposal;
+  const float sum = r.weight_sum + weight;
+  if (!std::isfinite(weight) || !std::isfinite(sum) || (target > 0.0f && weight == 0.0f)) return false;
+  selected = weight > 0.0f && (r.weight_sum == 0.0f || random < weight / sum);
+  r.weight_sum = sum;
+  ++r.candidate_count;
+  if (selected) {
+    r.sample = sample;
+    r.selected_target = target;
+  }
+  return true;
+}
+
+inline float Normalization(const Reservoir& r) {
+  return r.weight_sum > 0.0f ? (r.weight_sum / float(r.candidate_count)) / r.selected_target : 0.0f;
+}
+
+inline float ReuseNormalization(const Reservoir& r, uint32_t supporting) {
+  return r.weight_sum > 0.0f ? (r.weight_sum / float(supporting)) / r.selected_target : 0.0f;
+}
+
+bool MergeReevaluated(Reservoir& d, const Reservoir& src, float normalization, float target, uint32_t cap,
+    float random, bool& selected) {
+  selected = false;
+  const uint32_t count = std::min(src.candidate_count, cap);
+  const bool zero = src.weight_sum == 0.0f && src.sample == kNoReservoirSample && src.selected_target == 0.0f &&
+      normalization == 0.0f && target == 0.0f;
+  const bool positive = src.weight_sum > 0.0f && src.selected_target > 0.0f && src.sample != kNoReservoirSample &&
+      src.candidate_count != 0 && normalization > 0.0f;
+  const bool valid_destination = d.weight_sum == 0.0f
+      ? d.sample == kNoReservoirSample && d.selected_target == 0.0f
+      : d.weight_sum > 0.0f && d.selected_target > 0.0f && d.sample != kNoReservoirSample && d.candidate_count != 0;
+  if (!valid_destination || !std::isfinite(d.weight_sum) || !std::isfinite(d.selected_target) ||
+      !std::isfinite(src.weight_sum) || !std::isfinite(src.selected_target) || !(zero || positive) ||
+      !std::isfinite(normalization) || !std::isfinite(target) || target < 0.0f || cap == 0 ||
+      !std::isfinite(random) || random < 0.0f || random >= 1.0f || count > 0xFFFFFFFFu - d.candidate_count)
+    return false;
+  const float weight = (target * normalization) * float(count);
+  const float sum = d.weight_sum + weight;
+  if (!std::isfinite(weight) || !std::isfinite(sum) || (target > 0.0f && weight == 0.0f)) return false;
+  selected = weight > 0.0f && (d.weight_sum == 0.0f || random < weight / sum);
+  d.weight_sum = sum;
+  d.candidate_count += count;
+  if (selected) {
+    d.sample = src.sample;
+    d.selected_target = target;
+  }
+  return true;
+}
+
+// ChooseReservoirLight and ReservoirProposalPdf (scene.slang:915-937).
+uint32_t ChooseReservoirLight(const oracle_scene& s, uint32_t proposal, float ux, float uy) {
+  const uint32_t count = static_cast<uint32_t>(s.lights.size());
+  const uint32_t column = std::min(static_cast<uint32_t>(ux * float(count)), count - 1);
+  if (proposal == 1) return column;
+  if (proposal == 2) {
+    if (uy < 0.5f) return column;
+    uy = (uy - 0.5f) * 2.0f;
+  }
+  const LightRecord& record = s.lights[column];
+  return uy < record.threshold ? column : record.alias;
+}
+
+float ReservoirProposalPdf(const oracle_scene& s, uint32_t proposal, uint32_t index) {
+  const float power = s.lights[index].pdf;
+  const float uniform = 1.0f / float(s.lights.size());
+  if (proposal == 1) return uniform;
+  if (proposal == 2) return 0.5f * (power + uniform);
+  return power;
+}
+
+inline F3 ReflectionEvaluate(const PreviewClosure& b, F3 wo, F3 wi) {
+  return wi.z > 0.0f ? PreviewEvaluate(b, wo, wi) : V(0.0f);
+}
+
+// CandidateContribution (restir.slang:155-161).
+F3 CandidateContribution(const SurfaceHit& sh, const ShadingFrame& basis, F3 wo, const LightSample& ls,
+    float selection) {
+  if (!(ls.pdf > 0.0f) || dot(ls.direction, sh.normal) <= 0.0f) return V(0.0f);
+  return ReflectionEvaluate(sh.bsdf, wo, basis.ToLocal(ls.direction)) * ls.radiance * (selection / ls.pdf);
+}
+
+// StoreClosure / LoadClosure (restir.slang:78-149), UsdPreviewSurface only.
+void StoreClosure(const PreviewClosure& b, RestirSurfaceO& o) {
+  for (int k = 0; k < 4; ++k) o.model[k] = o.extension[k] = 0.0f;
+  o.normal[3] = b.dielectric_f90;
+  o.shading_normal[3] = b.thin_walled ? -b.transmission : b.transmission;
+  o.outgoing[3] = b.smooth ? -b.eta : b.eta;
+  o.base_alpha[0] = b.base_color.x; o.base_alpha[1] = b.base_color.y; o.base_alpha[2] = b.base_color.z;
+  o.base_alpha[3] = b.alpha;
+  o.dielectric_metallic[0] = b.dielectric_f0.x; o.dielectric_metallic[1] = b.dielectric_f0.y;
+  o.dielectric_metallic[2] = b.dielectric_f0.z; o.dielectric_metallic[3] = b.metallic;
+  o.fresnel[0] = b.f0.x; o.fresnel[1] = b.f0.y; o.fresnel[2] = b.f0.z; o.fresnel[3] = b.f90;
+}
+
+PreviewClosure LoadClosure(const RestirSurfaceO& o) {
+  PreviewClosure b;
+  b.base_color = V(o.base_alpha[0], o.base_alpha[1], o.base_alpha[2]);
+  b.alpha = o.base_alpha[3];
+  b.metallic = o.dielectric_metallic[3];
+  b.dielectric_f0 = V(o.dielectric_metallic[0], o.dielectric_metallic[1], o.dielectric_metallic[2]);
+  b.dielectric_f90 = o.normal[3];
+  b.f0 = V(o.fresnel[0], o.fresnel[1], o.fresnel[2]);
+  b.f90 = o.fresnel[3];
+  b.transmission = std::fabs(o.shading_normal[3]);
+  b.transmission_color = V(1.0f);
+  b.eta = std::fabs(o.outgoing[3]);
+  b.thin_walled = o.shading_normal[3] < 0.0f;
+  b.smooth = o.outgoing[3] < 0.0f;
+  return b;
+}
+
+inline F3 Xyz(const float* v) { return V(v[0], v[1], v[2]); }
+
+// HistoryContribution (restir.slang:256-268).
+F3 HistoryContribution(const oracle_scene& s, const RestirSurfaceO& src, uint32_t light, const LightSample& ls) {
+  const PreviewClosure b = LoadClosure(src);
+  if (!(ls.pdf > 0.0f) || dot(ls.direction, Xyz(src.normal)) <= 0.0f) return V(0.0f);
+  const ShadingFrame basis = MakeShadingFrame(Xyz(src.shading_normal));
+  return ReflectionEvaluate(b, Xyz(src.outgoing), basis.ToLocal(ls.direction)) * ls.radiance *
+      (s.lights[light].pdf / ls.pdf);
+}
+
+F3 HistoryContributionUv(const oracle_scene& s, const RestirSurfaceO& src, uint32_t light, const float* uv) {
+  return HistoryContribution(s, src, light, ReconstructReservoirLight(s, light, uv[0], uv[1], Xyz(src.origin)));
+}
+
+inline bool SameSample(const RestirRecord& a, const RestirRecord& b) {
+  return a.reservoir.sample == b.reservoir.sample && a.uv[0] == b.uv[0] && a.uv[1] == b.uv[1];
+}
+
+float HistoryTarget(const oracle_scene& s, const RestirReuseO& source, const RestirSurfaceO& surface,
+    const RestirRecord& selected, bool& valid) {
+  if (SameSample(source.pixel, selected)) {
+    valid = std::isfinite(source.pixel.reservoir.selected_target);
+    return source.pixel.reservoir.selected_target;
+  }
+  const F3 c = HistoryContributionUv(s, surface, selected.reservoir.sample, selected.uv);
+  valid = IsFinite(c);
+  return MaxComponent(c);
+}
+
+float ReceiverVisibility(const oracle_scene& s, const RestirRecord& selected, const RestirRecord& current,
+    F3 origin, const LightSample& ls) {
+  if (SameSample(selected, current)) return current.contribution[3];
+  return ShadowTransmittance(s, Ray{origin, 0.0f, ls.direction, ls.distance});
+}
+
+RestirRecord EmptyRecord() {
+  RestirRecord r{};
+  r.reservoir.sample = kNoReservoirSample;
+  return r;
+}
+
+inline bool InRect(const uint32_t* rect, uint32_t px, uint32_t py) {
+  return px >= rect[0] && py >= rect[1] && px < rect[0] + rect[2] && py < rect[1] + rect[3];
+}
+
+inline void SetContribution(RestirRecord& r, F3 e, float visibility) {
+  r.contribution[0] = e.x; r.contribution[1] = e.y; r.contribution[2] = e.z; r.contribution[3] = visibility;
+}
+
+// WriteInitialReservoir (restir.slang:163-233).
+RestirRecord InitialReservoir(const oracle_scene& s, const FrameConstants& f, const oracle_temporal& tc,
+    const uint32_t* rect, uint32_t sample_index, uint32_t px, uint32_t py) {
+  RestirRecord r = EmptyRecord();
+  const uint32_t slot = py * f.width + px;
+  if (!(tc.restir_candidates != 0 && InRect(rect, px, py))) return r;
+  PathState p = StartPath(f, px, py, sample_index);
+  Hit hit;
+  if (!Trace(s, p.ray, p.rng, hit)) return r;
+  r.flags |= 1u;
+  const SurfaceHit sh = ReconstructHit(s, hit, p.ray.direction);
+  const ShadingFrame basis = MakeShadingFrame(sh.shading_normal);
+  const F3 wo = basis.ToLocal(-p.ray.direction);
+  const F3 origin = OffsetRayOrigin(sh.position, sh.normal);
+  uint32_t rng = SeedRandom(slot, sample_index ^ 0xD1B54A35u);
+  if (tc.max_bounces != 0 && !s.lights.empty()) {
+    for (uint32_t i = 0; i < tc.restir_candidates; ++i) {
+      const float cx = NextRandom(rng);
+      const float cy = NextRandom(rng);
+      const float ux = NextRandom(rng);
+      const float uy = NextRandom(rng);
+      const float random = NextRandom(rng);
+      const uint32_t light = ChooseReservoirLight(s, tc.restir_proposal, cx, cy);
+      const float proposal = ReservoirProposalPdf(s, tc.restir_proposal, light);
+      const LightSample ls = ReconstructReservoirLight(s, light, ux, uy, origin);
+      const F3 fc = CandidateContribution(sh, basis, wo, ls, s.lights[light].pdf);
+      bool selected;
+      if (!std::isfinite(ls.pdf) || !IsFinite(fc) ||
+          !StreamCandidate(r.reservoir, light, MaxComponent(fc), proposal, random, selected)) {
+        r.flags |= 2u;
+        break;
+      }
+      if (selected) {
+        r.uv[0] = ux;
+        r.uv[1] = uy;
+        r.proposal = proposal;
+      }
+    }
+  }
+  if ((r.flags & 2u) == 0 && r.reservoir.weight_sum > 0.0f) {
+    const LightSample ls = ReconstructReservoirLight(s, r.reservoir.sample, r.uv[0], r.uv[1], origin);
+    const float visibility = ShadowTransmittance(s, Ray{origin, 0.0f, ls.direction, ls.distance});
+    const float normalization = Normalization(r.reservoir);
+    const F3 estimate = CandidateContribution(sh, basis, wo, ls, s.lights[r.reservoir.sample].pdf) *
+        (visibility * normalization);
+    if (!std::isfinite(normalization) || !IsFinite(estimate))
+      r.flags |= 2u;
+    else
+      SetContribution(r, estimate, visibility);
+  }
+  return r;
+}
+
+// WriteTemporalReservoir (restir.slang:302-387).
+void TemporalReservoir(const oracle_scene& s, const FrameConstants& f, const oracle_temporal& tc,
+    const uint32_t* rect, uint32_t sample_index, const std::vector<TemporalIds>& ids,
+    const RestirRecord* initial, const ValidityO* validity, const TemporalPixelO* surface,
+    const RestirReuseO* previous, const RestirSurfaceO* previous_surfaces, uint32_t px, uint32_t py,
+    RestirReuseO& result, RestirSurfaceO& receiver) {
+  const uint32_t slot = py * f.width + px;
+  result = RestirReuseO{};
+  receiver = RestirSurfaceO{};
+  result.pixel = initial[slot];
+  result.previous_index = 0xffffffffu;
+  result.normalization = Normalization(result.pixel.reservoir);
+  result.supporting_candidates = result.pixel.reservoir.candidate_count;
+  if (!(tc.restir_candidates != 0 && InRect(rect, px, py))) return;
+  PathState p = StartPath(f, px, py, sample_index);
+  Hit hit;
+  if (!Trace(s, p.ray, p.rng, hit)) return;
+  const SurfaceHit sh = ReconstructHit(s, hit, p.ray.direction);
+  const ShadingFrame basis = MakeShadingFrame(sh.shading_normal);
+  const F3 wo = basis.ToLocal(-p.ray.direction);
+  const F3 origin = OffsetRayOrigin(sh.position, sh.normal);
+  float view[4];
+  Mul4(tc.current_view, sh.position.x, sh.position.y, sh.position.z, 1.0f, view);
+  receiver.origin[0] = origin.x; receiver.origin[1] = origin.y; receiver.origin[2] = origin.z;
+  receiver.origin[3] = -view[2] / view[3];
+  receiver.normal[0] = sh.normal.x; receiver.normal[1] = sh.normal.y; receiver.normal[2] = sh.normal.z;
+  receiver.shading_normal[0] = sh.shading_normal.x; receiver.shading_normal[1] = sh.shading_normal.y;
+  receiver.shading_normal[2] = sh.shading_normal.z;
+  receiver.outgoing[0] = wo.x; receiver.outgoing[1] = wo.y; receiver.outgoing[2] = wo.z;
+  StoreClosure(sh.bsdf, receiver);
+  receiver.instance_id = ids[hit.instance].instance_id;
+  receiver.material_id = ids[hit.instance].material_id;
+  const ValidityO v = validity[slot];
+  const uint32_t previous_index = v.previous_index;
+  const bool history = v.valid != 0 && surface[slot].instance_id == receiver.instance_id &&
+      surface[slot].material_id == receiver.material_id;
+  if (tc.restir_history != 0 && (result.pixel.flags & 2u) == 0 && history) {
+    const RestirReuseO source = previous[previous_index];
+    const RestirSurfaceO& psrc = previous_surfaces[previous_index];
+    if ((source.pixel.flags & 1u) != 0 && (source.pixel.flags & 2u) == 0 &&
+        psrc.instance_id == receiver.instance_id && psrc.material_id == receiver.material_id) {
+      const uint32_t count = std::min(source.pixel.reservoir.candidate_count, tc.restir_max_history);
+      F3 received = V(0.0f);
+      if (source.pixel.reservoir.weight_sum > 0.0f) {
+        if (source.pixel.reservoir.sample >= s.lights.size())
+          result.pixel.flags |= 2u;
+        else
+          received = HistoryContributionUv(s, receiver, source.pixel.reservoir.sample, source.pixel.uv);
+      }
+      uint32_t rng = SeedRandom(slot, sample_index ^ 0x94D049BBu);
+      bool selected;
+      if (!IsFinite(received) || (result.pixel.flags & 2u) != 0 ||
+          !MergeReevaluated(result.pixel.reservoir, source.pixel.reservoir, source.normalization,
+              MaxComponent(received), tc.restir_max_history, NextRandom(rng), selected)) {
+        result.pixel.flags |= 2u;
+      } else {
+        result.previous_index = previous_index;
+        if (selected) {
+          result.pixel.uv[0] = source.pixel.uv[0];
+          result.pixel.uv[1] = source.pixel.uv[1];
+          result.pixel.proposal = source.pixel.proposal;
+          result.age = std::min(source.age, 65535u) + 1u;
+        }
+        if (result.pixel.reservoir.weight_sum > 0.0f) {
+          bool valid_support;
+          const float support = HistoryTarget(s, source, psrc, result.pixel, valid_support);
+          if (!valid_support) result.pixel.flags |= 2u;
+          result.supporting_candidates = initial[slot].reservoir.candidate_count + (support > 0.0f ? count : 0u);
+        } else {
+          result.supporting_candidates = 0;
+        }
+        result.normalization = ReuseNormalization(result.pixel.reservoir, result.supporting_candidates);
+      }
+    }
+  }
+  if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
+    const LightSample ls = ReconstructReservoirLight(s, result.pixel.reservoir.sample, result.pixel.uv[0],
+        result.pixel.uv[1], origin);
+    const float visibility = ReceiverVisibility(s, result.pixel, initial[slot], origin, ls);
+    const F3 estimate = HistoryContribution(s, receiver, result.pixel.reservoir.sample, ls) *
+        (visibility * result.normalization);
+    if (!std::isfinite(result.normalization) || result.normalization <= 0.0f || !IsFinite(estimate))
+      result.pixel.flags |= 2u;
+    else
+      SetContribution(result.pixel, estimate, visibility);
+  }
+}
+
+// SpatialCompatible and WriteSpatialReservoir (restir.slang:392-491).
+bool SpatialCompatible(const RestirSurfaceO& receiver, const RestirReuseO& record, const RestirSurfaceO& source) {
+  return (record.pixel.flags & 3u) == 1u && receiver.origin[3] > 0.0f && source.origin[3] > 0.0f &&
+      receiver.material_id == source.material_id &&
+      std::fabs(receiver.origin[3] - source.origin[3]) <=
+          0.01f + 0.02f * std::fmax(receiver.origin[3], source.origin[3]) &&
+      dot(Xyz(receiver.normal), Xyz(source.normal)) >= 0.9f &&
+      dot(Xyz(receiver.shading_normal), Xyz(source.shading_normal)) >= 0.9f;
+}
+
+void SpatialReservoir(const oracle_scene& s, const FrameConstants& f, const oracle_temporal& tc, uint32_t height,
+    uint32_t sample_index, const RestirReuseO* temporal, const RestirSurfaceO* surfaces, uint32_t px, uint32_t py,
+    RestirReuseO& result, uint32_t* sources) {
+  const uint32_t slot = py * f.width + px;
+  const RestirReuseO centre = temporal[slot];
+  const RestirSurfaceO& receiver = surfaces[slot];
+  result = centre;
+  for (int i = 0; i < 4; ++i) sources[i] = 0xffffffffu;
+  const int radius = static_cast<int>(tc.restir_radius);
+  const int ox[4] = {-radius, radius, 0, 0};
+  const int oy[4] = {0, 0, -radius, radius};
+  if ((centre.pixel.flags & 3u) != 1u) return;
+  uint32_t accepted = 0;
+  for (int i = 0; i < 4; ++i) {
+    const int nx = static_cast<int>(px) + ox[i], ny = static_cast<int>(py) + oy[i];
+    if (nx < 0 || ny < 0 || nx >= static_cast<int>(f.width) || ny >= static_cast<int>(height)) continue;
+    const uint32_t index = static_cast<uint32_t>(ny) * f.width + static_cast<uint32_t>(nx);
+    if (SpatialCompatible(receiver, temporal[index], surfaces[index])) {
+      sources[i] = index;
+      ++accepted;
+    }
+  }
+  if (accepted == 0) return;
+  result.pixel.reservoir = Reservoir{kNoReservoirSample, 0.0f, 0.0f, 0};
+  bool selected;
+  if (!MergeReevaluated(result.pixel.reservoir, centre.pixel.reservoir, centre.normalization,
+          centre.pixel.reservoir.selected_target, 0xffffffffu, 0.0f, selected))
+    result.pixel.flags |= 2u;
+  uint32_t rng = SeedRandom(slot, sample_index ^ 0x369DEA0Fu);
+  for (int i = 0; i < 4; ++i) {
+    if (sources[i] == 0xffffffffu) continue;
+    const RestirReuseO& source = temporal[sources[i]];
+    F3 received = V(0.0f);
+    if (source.pixel.reservoir.weight_sum > 0.0f)
+      received = HistoryContributionUv(s, receiver, source.pixel.reservoir.sample, source.pixel.uv);
+    if (!IsFinite(received) ||
+        !MergeReevaluated(result.pixel.reservoir, source.pixel.reservoir, source.normalization,
+            MaxComponent(received), tc.restir_max_history, NextRandom(rng), selected)) {
+      result.pixel.flags |= 2u;
+      break;
+    }
+    if (selected) {
+      result.pixel.uv[0] = source.pixel.uv[0];
+      result.pixel.uv[1] = source.pixel.uv[1];
+      result.pixel.proposal = source.pixel.proposal;
+      result.age = source.age;
+    }
+  }
+  result.supporting_candidates = 0;
+  for (int k = 0; k < 4; ++k) result.pixel.contribution[k] = 0.0f;
+  if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
+    result.supporting_candidates = centre.pixel.reservoir.candidate_count;
+    for (int i = 0; i < 4; ++i) {
+      if (sources[i] == 0xffffffffu) continue;
+      const RestirReuseO& source = temporal[sources[i]];
+      bool valid_support;
+      const float support = HistoryTarget(s, source, surfaces[sources[i]], result.pixel, valid_support);
+      if (!valid_support) result.pixel.flags |= 2u;
+      if (support > 0.0f)
+        result.supporting_candidates += std::min(source.pixel.reservoir.candidate_count, tc.restir_max_history);
+    }
+  }
+  result.normalization = ReuseNormalization(result.pixel.reservoir, result.supporting_candidates);
+  if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
+    const LightSample ls = ReconstructReservoirLight(s, result.pixel.reservoir.sample, result.pixel.uv[0],
+        result.pixel.uv[1], Xyz(receiver.origin));
+    const float visibility = ReceiverVisibility(s, result.pixel, centre.pixel, Xyz(receiver.origin), ls);
+    const F3 estimate = HistoryContribution(s, receiver, result.pixel.reservoir.sample, ls) *
+        (visibility * result.normalization);
+    if (!std::isfinite(result.normalization) || result.normalization <= 0.0f || !IsFinite(estimate))
+      result.pixel.flags |= 2u;
+    else
+      SetContribution(result.pixel, estimate, visibility);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t oracle_temporal_surface(const oracle_scene* s, const lotus_frame_desc* d, const oracle_temporal* tc,
+    const lotus_temporal_instance* ids, void* out) {
+  FrameConstants f;
+  uint32_t rect[4];
+  if (!s || !d || !tc || !out || !MakeFrame(*d, f, rect)) return LOTUS_FAIL;
+  const auto identities = ConvertIds(*s, ids);
+  auto* o = static_cast<TemporalPixelO*>(out);
+  const int64_t n = int64_t{d->target.width} * d->target.height;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i) {
+    const uint32_t px = uint32_t(i % d->target.width), py = uint32_t(i / d->target.width);
+    o[i] = InRect(rect, px, py) ? TemporalSurface(*s, f, *tc, identities, px, py) : TemporalPixelO{};
+  }
+  return LOTUS_PASS;
+}
+
+int32_t oracle_restir_initial(const oracle_scene* s, const lotus_frame_desc* d, const oracle_temporal* tc,
+    uint32_t sample_index, void* out) {
+  FrameConstants f;
+  uint32_t rect[4];
+  if (!s || !d || !tc || !out || !MakeFrame(*d, f, rect)) return LOTUS_FAIL;
+  auto* o = static_cast<RestirRecord*>(out);
+  const int64_t n = int64_t{d->target.width} * d->target.height;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i)
+    o[i] = InitialReservoir(*s, f, *tc, rect, sample_index, uint32_t(i % d->target.width),
+        uint32_t(i / d->target.width));
+  return LOTUS_PASS;
+}
+
+int32_t oracle_restir_temporal(const oracle_scene* s, const lotus_frame_desc* d, const oracle_temporal* tc,
+    const lotus_temporal_instance* ids, uint32_t sample_index, const void* initial, const void* validity,
+    const void* surface, const void* previous, const void* previous_surfaces, void* out, void* out_surfaces) {
+  FrameConstants f;
+  uint32_t rect[4];
+  if (!s || !d || !tc || !MakeFrame(*d, f, rect)) return LOTUS_FAIL;
+  const auto identities = ConvertIds(*s, ids);
+  const int64_t n = int64_t{d->target.width} * d->target.height;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i)
+    TemporalReservoir(*s, f, *tc, rect, sample_index, identities, static_cast<const RestirRecord*>(initial),
+        static_cast<const ValidityO*>(validity), static_cast<const TemporalPixelO*>(surface),
+        static_cast<const RestirReuseO*>(previous), static_cast<const RestirSurfaceO*>(previous_surfaces),
+        uint32_t(i % d->target.width), uint32_t(i / d->target.width), static_cast<RestirReuseO*>(out)[i],
+        static_cast<RestirSurfaceO*>(out_surfaces)[i]);
+  return LOTUS_PASS;
+}
+
+int32_t oracle_restir_spatial(const oracle_scene* s, const lotus_frame_desc* d, const oracle_temporal* tc,
+    uint32_t sample_index, const void* temporal, const void* surfaces, void* out, uint32_t* sources) {
+  FrameConstants f;
+  uint32_t rect[4];
+  if (!s || !d || !tc || !MakeFrame(*d, f, rect)) return LOTUS_FAIL;
+  const int64_t n = int64_t{d->target.width} * d->target.height;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t i = 0; i < n; ++i)
+    SpatialReservoir(*s, f, *tc, d->target.height, sample_index, static_cast<const RestirReuseO*>(temporal),
+        static_cast<const RestirSurfaceO*>(surfaces), uint32_t(i % d->target.width),
+        uint32_t(i / d->target.width), static_cast<RestirReuseO*>(out)[i], sources + 4 * i);
+  return LOTUS_PASS;
+}
+
+int32_t oracle_sample_restir(const oracle_scene* s, const lotus_frame_desc* d, uint32_t sample_index,
+    const void* final_records, uint32_t stride, float* rgba, uint64_t* rays, int32_t threads) {
+  FrameConstants f;
+  uint32_t rect[4];
+  if (!s || !d || !rgba || !final_records || !MakeFrame(*d, f, rect)) return LOTUS_FAIL;
+  f.sample_lights = true;
+  f.restir_final = static_cast<const unsigned char*>(final_records);
+  f.restir_stride = stride;
+  const int64_t pixels = int64_t{rect[2]} * rect[3];
+  std::atomic<uint64_t> camera{0}, extension{0}, shadow{0};
+#pragma omp parallel num_threads(ThreadCount(threads))
+  {
+    RayCounts local;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t i = 0; i < pixels; ++i) {
+      const uint32_t px = rect[0] + uint32_t(i % rect[2]);
+      const uint32_t py = rect[1] + uint32_t(i / rect[2]);
+      F3 radiance;
+      float* out = rgba + 4 * (size_t{py} * d->target.width + px);
+      if (PathSample(*s, f, px, py, sample_index, radiance, local)) {
+        out[0] = radiance.x; out[1] = radiance.y; out[2] = radiance.z; out[3] = 1.0f;
+      } else {
+        out[0] = out[1] = out[2] = out[3] = 0.0f;
+      }
+    }
+    camera += local.camera;
+    extension += local.extension;
+    shadow += local.shadow;
+  }
+  if (rays) {
+    rays[0] = camera;
+    rays[1] = extension;
+    rays[2] = shadow;
+  }
   return LOTUS_PASS;
 }
 

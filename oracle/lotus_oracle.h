@@ -54,6 +54,45 @@ int32_t oracle_traversal_stats(const oracle_scene* scene,
     const lotus_frame_desc* frame, uint32_t max_rays, double* nodes_per_ray,
     double* triangles_per_ray);
 
+/* The temporal passes' constants (the kernels' TemporalConst). */
+typedef struct oracle_temporal {
+  float current_view[16];
+  float previous_view[16];
+  float previous_world_to_clip[16];  /* Vulkan clip */
+  float previous_display[4];
+  uint32_t previous_data[4];
+  uint32_t restir_candidates;
+  uint32_t restir_history;
+  uint32_t restir_max_history;
+  uint32_t restir_radius;
+  uint32_t restir_proposal;
+  uint32_t max_bounces;
+} oracle_temporal;
+
+/* WriteTemporalSurface (temporal.slang:557-627) for every pixel: 64-byte
+ * TemporalPixel records. `ids` may be NULL (index ids, static, flags 6). */
+int32_t oracle_temporal_surface(const oracle_scene* scene, const lotus_frame_desc* frame,
+    const oracle_temporal* temporal, const lotus_temporal_instance* ids, void* out);
+
+/* The ReSTIR DI passes (restir.slang:163-491) over the same records as the
+ * kernels: RestirPixel (48 B), RestirReuse (64 B), RestirSurface (160 B). */
+int32_t oracle_restir_initial(const oracle_scene* scene, const lotus_frame_desc* frame,
+    const oracle_temporal* temporal, uint32_t sample_index, void* out);
+int32_t oracle_restir_temporal(const oracle_scene* scene, const lotus_frame_desc* frame,
+    const oracle_temporal* temporal, const lotus_temporal_instance* ids, uint32_t sample_index,
+    const void* initial, const void* validity, const void* surface, const void* previous,
+    const void* previous_surfaces, void* out, void* out_surfaces);
+int32_t oracle_restir_spatial(const oracle_scene* scene, const lotus_frame_desc* frame,
+    const oracle_temporal* temporal, uint32_t sample_index, const void* temporal_records,
+    const void* surfaces, void* out, uint32_t* sources);
+
+/* oracle_sample with RestirInitial light sampling: the depth-0 direct light
+ * is InitialDirectLight over `final_records` (RestirPixel records `stride`
+ * bytes apart). */
+int32_t oracle_sample_restir(const oracle_scene* scene, const lotus_frame_desc* frame,
+    uint32_t sample_index, const void* final_records, uint32_t stride, float* rgba, uint64_t* rays,
+    int32_t threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -110,3 +110,129 @@ def resolve(sums, clear_color=(0.0, 0.0, 0.0, 0.0), count=None):
     out[..., :3] = (sums[..., :3] + miss[..., None] * bg[:3]) / count
     out[..., 3] = (sums[..., 3] + miss * bg[3]) / count
     return out
+
+
+class OracleTemporal(C.Structure):
+    """oracle_temporal: the temporal passes' constants."""
+    _fields_ = [
+        ("current_view", C.c_float * 16),
+        ("previous_view", C.c_float * 16),
+        ("previous_world_to_clip", C.c_float * 16),
+        ("previous_display", C.c_float * 4),
+        ("previous_data", C.c_uint32 * 4),
+        ("restir_candidates", C.c_uint32),
+        ("restir_history", C.c_uint32),
+        ("restir_max_history", C.c_uint32),
+        ("restir_radius", C.c_uint32),
+        ("restir_proposal", C.c_uint32),
+        ("max_bounces", C.c_uint32),
+    ]
+
+
+def vulkan_clip(world_to_clip):
+    """VulkanWorldToClip (vulkan_internal.hpp:326-336) in float32."""
+    m = np.asarray(world_to_clip, dtype=np.float32).copy()
+    for c in range(4):
+        y, z, w = m[c * 4 + 1], m[c * 4 + 2], m[c * 4 + 3]
+        m[c * 4 + 1] = -y
+        m[c * 4 + 2] = np.float32(0.5) * np.float32(z + w)
+    return m
+
+
+def oracle_temporal(temporal_desc):
+    """The oracle's constants for a lotus_temporal_desc, as the renderer
+    derives them (whole-image display and data windows)."""
+    f = temporal_desc.frame
+    st = f.settings
+    t = OracleTemporal()
+    t.current_view[:] = list(temporal_desc.current_view)
+    if temporal_desc.history_available:
+        t.previous_view[:] = list(temporal_desc.previous_view)
+        t.previous_world_to_clip[:] = [float(v) for v in vulkan_clip(temporal_desc.previous_world_to_clip)]
+    t.previous_display[:] = [0.0, 0.0, float(f.target.width), float(f.target.height)]
+    t.previous_data[:] = [0, 0, f.target.width, f.target.height]
+    t.restir_candidates = st.restir_candidates
+    t.restir_history = 1 if (st.restir_temporal and temporal_desc.history_available) else 0
+    t.restir_max_history = st.restir_max_history_candidates
+    t.restir_radius = st.restir_spatial_radius
+    t.restir_proposal = st.restir_proposal
+    t.max_bounces = st.max_bounces
+    return t
+
+
+def _temporal_lib():
+    L = lib()
+    if not hasattr(L, "_temporal_ready"):
+        vp = C.c_void_p
+        L.oracle_temporal_surface.restype = C.c_int32
+        L.oracle_temporal_surface.argtypes = [vp, C.POINTER(abi.FrameDesc), C.POINTER(OracleTemporal), vp, vp]
+        L.oracle_restir_initial.restype = C.c_int32
+        L.oracle_restir_initial.argtypes = [vp, C.POINTER(abi.FrameDesc), C.POINTER(OracleTemporal),
+                                            C.c_uint32, vp]
+        L.oracle_restir_temporal.restype = C.c_int32
+        L.oracle_restir_temporal.argtypes = [vp, C.POINTER(abi.FrameDesc), C.POINTER(OracleTemporal), vp,
+                                             C.c_uint32, vp, vp, vp, vp, vp, vp, vp]
+        L.oracle_restir_spatial.restype = C.c_int32
+        L.oracle_restir_spatial.argtypes = [vp, C.POINTER(abi.FrameDesc), C.POINTER(OracleTemporal),
+                                            C.c_uint32, vp, vp, vp, vp]
+        L.oracle_sample_restir.restype = C.c_int32
+        L.oracle_sample_restir.argtypes = [vp, C.POINTER(abi.FrameDesc), C.c_uint32, vp, C.c_uint32, vp, vp,
+                                           C.c_int32]
+        L._temporal_ready = True
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class OracleTemporalScene(OracleScene):
+    """The oracle's temporal passes over the kernels' record layouts."""
+
+    def temporal_surface(self, frame, tc, ids=None):
+        h, w = frame.target.height, frame.target.width
+        out = np.zeros((h, w), dtype=abi.TEMPORAL_PIXEL)
+        ids_arr = None if ids is None else (abi.TemporalInstance * len(ids))(*ids)
+        _temporal_lib().oracle_temporal_surface(self.handle, C.byref(frame), C.byref(tc),
+                                                C.cast(ids_arr, C.c_void_p) if ids_arr else None,
+                                                out.ctypes.data)
+        return out
+
+    def restir_initial(self, frame, tc, sample_index):
+        h, w = frame.target.height, frame.target.width
+        out = np.zeros((h, w), dtype=abi.RESTIR_PIXEL)
+        _temporal_lib().oracle_restir_initial(self.handle, C.byref(frame), C.byref(tc), sample_index,
+                                              out.ctypes.data)
+        return out
+
+    def restir_temporal(self, frame, tc, sample_index, initial, validity, surface, previous,
+                        previous_surfaces, ids=None):
+        h, w = frame.target.height, frame.target.width
+        out = np.zeros((h, w), dtype=abi.RESTIR_REUSE)
+        out_s = np.zeros((h, w), dtype=abi.RESTIR_SURFACE)
+        ids_arr = None if ids is None else (abi.TemporalInstance * len(ids))(*ids)
+        _temporal_lib().oracle_restir_temporal(
+            self.handle, C.byref(frame), C.byref(tc), C.cast(ids_arr, C.c_void_p) if ids_arr else None,
+            sample_index, _ptr(initial), _ptr(validity), _ptr(surface), _ptr(previous),
+            _ptr(previous_surfaces), out.ctypes.data, out_s.ctypes.data)
+        return out, out_s
+
+    def restir_spatial(self, frame, tc, sample_index, temporal, surfaces):
+        h, w = frame.target.height, frame.target.width
+        out = np.zeros((h, w), dtype=abi.RESTIR_REUSE)
+        src = np.zeros((h, w, 4), dtype=np.uint32)
+        _temporal_lib().oracle_restir_spatial(self.handle, C.byref(frame), C.byref(tc), sample_index,
+                                              _ptr(temporal), _ptr(surfaces), out.ctypes.data,
+                                              src.ctypes.data)
+        return out, src
+
+    def sample_restir(self, frame, sample_index, final_records, threads=0):
+        h, w = frame.target.height, frame.target.width
+        out = np.zeros((h, w, 4), dtype=np.float32)
+        rays = np.zeros(3, dtype=np.uint64)
+        rc = _temporal_lib().oracle_sample_restir(self.handle, C.byref(frame), sample_index,
+                                                  final_records.ctypes.data, final_records.dtype.itemsize,
+                                                  out.ctypes.data, rays.ctypes.data, threads)
+        if rc != abi.PASS:
+            raise RuntimeError("oracle_sample_restir failed")
+        return out, rays

@@ -1,0 +1,131 @@
+"""GPU parity of the temporal passes through the C ABI (RenderTemporalScene):
+the primary-surface metadata and ReSTIR DI passes against the oracle's
+restatement (bit for bit), reprojection and SVGF against the reference's own
+CPU code (temporal.cpp) at the reference's published GPU tolerances."""
+
+import numpy as np
+import pytest
+
+from hydra_lotus_b200 import abi, scenes
+from oracle import oracle, ref
+
+from parity import PathParity
+
+pytestmark = pytest.mark.gpu
+
+SIZE = 64
+# The reference's GPU-vs-CPU tolerances for the SVGF passes
+# (docs/reports/2026-10-18-svgf-filter.md): composite max relative error
+# 1.2e-5 and variance max absolute error 9.3e-5.
+COMPOSITE_RTOL = 1.2e-5
+VARIANCE_ATOL = 9.3e-5
+
+
+def temporal_frames(integrator, spatial=True, frames=3, filter_iterations=5, cap=5):
+    scene = scenes.restir_room(seed=0, size=SIZE, emitters=300)
+    settings = abi.default_settings(integrator=integrator,
+                                    light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL,
+                                    max_bounces=4, sample_index=100, restir_candidates=8,
+                                    restir_temporal=1, restir_max_history_candidates=20,
+                                    restir_spatial=1 if spatial else 0, restir_spatial_radius=2)
+    descs = []
+    previous = None
+    for k in range(frames):
+        view, w2c = scenes.orbit_camera(k, frames=24)
+        frame = abi.make_frame(w2c, SIZE, SIZE, settings, 1)
+        d = abi.temporal_desc(frame, view, previous[0] if previous else None,
+                              previous[1] if previous else None, history_available=k > 0,
+                              accumulate_radiance=True, max_history_samples=cap,
+                              filter_iterations=filter_iterations)
+        descs.append(d)
+        previous = (view, w2c)
+    return scene, descs
+
+
+def products(r, h, w, names):
+    return {n: r.read_product(getattr(abi, "PRODUCT_" + n.upper()), h, w) for n in names}
+
+
+def exact(a, b):
+    return np.array_equal(np.frombuffer(a.tobytes(), np.uint8), np.frombuffer(b.tobytes(), np.uint8))
+
+
+@pytest.mark.parametrize("integrator", [abi.INTEGRATOR_WAVEFRONT, abi.INTEGRATOR_REFERENCE])
+def test_temporal_passes_match_checkers(cuda, integrator):
+    scene, descs = temporal_frames(integrator)
+    o = oracle.OracleTemporalScene(scene)
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        for k, d in enumerate(descs):
+            res, color = r.render_temporal(d)
+            cuda.check(res, f"render_temporal frame {k}")
+            p = products(r, SIZE, SIZE, ["surface", "previous_surface", "validity", "radiance",
+                                         "previous_radiance", "batch", "restir_initial",
+                                         "restir_temporal", "restir_previous", "restir_spatial",
+                                         "restir_sources", "restir_surfaces",
+                                         "restir_previous_surfaces"])
+            tc = oracle.oracle_temporal(d)
+            frame = d.frame
+            si = frame.settings.sample_index + k  # the stream's batch sample index
+            # Primary-surface metadata: bit for bit.
+            want = o.temporal_surface(frame, tc)
+            assert exact(p["surface"], want), f"frame {k}: temporal surface differs"
+            # Reprojection: the reference's own ReprojectTemporalHistory.
+            prev = p["previous_surface"] if k > 0 else np.zeros(0, dtype=abi.TEMPORAL_PIXEL)
+            v = ref.reproject(p["surface"], prev, d.validation)
+            assert exact(p["validity"], v), f"frame {k}: validity differs from the reference's"
+            # ReSTIR passes, each from the GPU's own inputs: bit for bit.
+            init = o.restir_initial(frame, tc, si)
+            assert exact(p["restir_initial"], init), f"frame {k}: initial reservoirs differ"
+            reuse, surf = o.restir_temporal(frame, tc, si, p["restir_initial"], p["validity"], p["surface"],
+                                            p["restir_previous"], p["restir_previous_surfaces"])
+            assert exact(p["restir_temporal"], reuse), f"frame {k}: temporal reservoirs differ"
+            assert exact(p["restir_surfaces"], surf), f"frame {k}: reservoir surfaces differ"
+            spatial, sources = o.restir_spatial(frame, tc, si, p["restir_temporal"], p["restir_surfaces"])
+            assert exact(p["restir_spatial"], spatial), f"frame {k}: spatial reservoirs differ"
+            assert np.array_equal(p["restir_sources"], sources)
+            if k > 0:
+                used = (reuse["previous_index"] != 0xFFFFFFFF).mean()
+                assert used > 0.3, f"temporal reuse found history at only {used:.2f} of pixels"
+            # The fresh batch: the path tracer with the final reservoirs at
+            # its primary vertex.
+            batch, _ = o.sample_restir(frame, si, p["restir_spatial"])
+            pp = PathParity(p["batch"], batch)
+            print(k, pp)
+            pp.assert_ok()
+            assert pp.exact > 0.99, pp
+            # SVGF against the reference's CPU oracles.
+            var = ref.estimate_variance(p["surface"], p["radiance"], 1, d.max_history_samples)
+            np.testing.assert_allclose(p["radiance"]["variance"], var, rtol=0, atol=VARIANCE_ATOL)
+            comp = ref.filter_composite(p["surface"], p["radiance"], 1, d.max_history_samples,
+                                        d.filter_iterations)
+            scale = np.maximum(np.abs(comp), 1e-3)
+            rel = np.abs(color - comp) / scale
+            assert rel.max() <= COMPOSITE_RTOL * 10, rel.max()
+            assert np.percentile(rel, 99.9) <= COMPOSITE_RTOL, np.percentile(rel, 99.9)
+
+
+def test_restir_converges_to_mis_path_tracer(cuda):
+    """ReSTIR DI's primary direct light is unbiased: the mean of many
+    independent initial-only frames matches the MIS path tracer's mean."""
+    scene = scenes.restir_room(seed=1, size=32, emitters=100)
+    view, w2c = scenes.orbit_camera(0)
+    n = 256
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        mis = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                                   max_bounces=3, sample_index=0)
+        res, ref_img = r.render_scene(abi.make_frame(w2c, 32, 32, mis, 4 * n))
+        cuda.check(res, "MIS")
+        acc = np.zeros((32, 32, 4))
+        for k in range(n):
+            st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT,
+                                      light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL, max_bounces=3,
+                                      sample_index=50000 + k, restir_candidates=8)
+            d = abi.temporal_desc(abi.make_frame(w2c, 32, 32, st, 1), view)
+            res, img = r.render_temporal(d)
+            cuda.check(res, "restir frame")
+            acc += img
+        acc /= n
+    rel = abs(acc[..., :3].mean() - ref_img[..., :3].mean()) / ref_img[..., :3].mean()
+    assert rel < 0.03, rel
