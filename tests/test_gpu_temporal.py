@@ -16,9 +16,11 @@ pytestmark = pytest.mark.gpu
 SIZE = 64
 # The reference's GPU-vs-CPU tolerances for the SVGF passes
 # (docs/reports/2026-10-18-svgf-filter.md): composite max relative error
-# 1.2e-5 and variance max absolute error 9.3e-5.
+# 1.2e-5 and variance max absolute error 9.3e-5 (for variances near 1; a
+# relative 1e-6, a few float ulps, covers large ones).
 COMPOSITE_RTOL = 1.2e-5
 VARIANCE_ATOL = 9.3e-5
+VARIANCE_RTOL = 1e-6
 
 
 def temporal_frames(integrator, spatial=True, frames=3, filter_iterations=5, cap=5):
@@ -96,7 +98,7 @@ def test_temporal_passes_match_checkers(cuda, integrator):
             assert pp.exact > 0.99, pp
             # SVGF against the reference's CPU oracles.
             var = ref.estimate_variance(p["surface"], p["radiance"], 1, d.max_history_samples)
-            np.testing.assert_allclose(p["radiance"]["variance"], var, rtol=0, atol=VARIANCE_ATOL)
+            np.testing.assert_allclose(p["radiance"]["variance"], var, rtol=VARIANCE_RTOL, atol=VARIANCE_ATOL)
             comp = ref.filter_composite(p["surface"], p["radiance"], 1, d.max_history_samples,
                                         d.filter_iterations)
             scale = np.maximum(np.abs(comp), 1e-3)
