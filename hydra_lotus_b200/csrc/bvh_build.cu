@@ -1,12 +1,15 @@
 // SPDX-License-Identifier: Apache-2.0
-// On-device BVH construction: a linear BVH (Karras, "Maximizing Parallelism
-// in the Construction of BVHs, Octrees, and k-d Trees", HPG 2012) over
-// 63-bit Morton codes of the primitives' centroids, sorted by CUB's radix
-// sort, with bounds fitted bottom-up. It replaces the driver's BLAS/TLAS
-// builds (backend/vulkan/gpu_scene.cpp:1899-1950, 2240-2322 in
+// On-device BVH construction, replacing the driver's BLAS/TLAS builds. Two
+// builders: a binned-SAH builder that runs one BVH per CTA (all of a
+// scene's BLASes in one launch, and the TLAS), and, for meshes too large
+// for one CTA, a linear BVH (Karras, "Maximizing Parallelism in the
+// Construction of BVHs, Octrees, and k-d Trees", HPG 2012) over 63-bit
+// Morton codes of the primitives' centroids, sorted by CUB's radix sort,
+// with bounds fitted bottom-up. The reference's builds are (backend/vulkan/gpu_scene.cpp:1899-1950, 2240-2322 in
 // hydra-lotus).
 #include "bvh_build.cuh"
 
+#include <cub/block/block_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
 
 namespace lotus {
@@ -253,6 +256,328 @@ __global__ void k_write_triangles(const uint32_t* __restrict__ values,
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Binned-SAH builder: one CTA builds one BVH top-down (Wald, "On fast
+// Construction of SAH-based Bounding Volume Hierarchies", 2007), binning
+// centroids into 16 bins per axis in shared memory and partitioning the
+// primitive indices with a block-wide scan. Every BVH of a batch builds in
+// its own CTA, so a scene's BLASes build concurrently across the SMs.
+
+constexpr int kSahBlock = 256;
+constexpr int kSahBins = 16;
+constexpr int kSahStack = 128;
+
+struct SahJob {
+  uint32_t prim_offset;  // first primitive in the batch's arrays
+  uint32_t count;
+  uint32_t node_base;    // first node slot
+  uint32_t leaf_base;    // first triangle-pool slot (BLAS)
+  uint32_t leaf_size;    // most primitives per leaf
+  uint32_t leaves_are_values;  // TLAS: leaves hold the primitive index itself
+};
+
+struct SahShared {
+  uint32_t bin_count[3][kSahBins];
+  uint32_t bin_lo[3][kSahBins][3];
+  uint32_t bin_hi[3][kSahBins][3];
+  uint32_t cb[6];        // centroid bounds (ordered)
+  uint32_t nb[6];        // node bounds (ordered)
+  uint32_t stack_begin[kSahStack], stack_end[kSahStack], stack_node[kSahStack];
+  int sp;
+  uint32_t next_node;
+  uint32_t begin, end, node;
+  int best_axis, best_split;
+  float best_cost[3];
+  int split_at[3];
+  uint32_t left_total;
+  uint32_t error;
+};
+
+__global__ void __launch_bounds__(kSahBlock) k_sah_build(const SahJob* __restrict__ jobs,
+    const float4* __restrict__ plo, const float4* __restrict__ phi, uint32_t* __restrict__ idx,
+    uint32_t* __restrict__ scratch, BvhNode* __restrict__ nodes, uint32_t* __restrict__ errors) {
+  using BlockScan = cub::BlockScan<uint32_t, kSahBlock>;
+  __shared__ typename BlockScan::TempStorage scan_storage;
+  __shared__ SahShared sh;
+  const SahJob job = jobs[blockIdx.x];
+  const uint32_t tid = threadIdx.x;
+  uint32_t* index = idx + job.prim_offset;
+  uint32_t* tmp = scratch + job.prim_offset;
+  if (job.count == 0) return;
+  if (tid == 0) {
+    sh.sp = 0;
+    sh.next_node = 1;
+    sh.error = 0;
+    sh.stack_begin[0] = 0;
+    sh.stack_end[0] = job.count;
+    sh.stack_node[0] = 0;
+    sh.sp = 1;
+  }
+  __syncthreads();
+  // Small sets: one leaf under the root, its second child empty.
+  if (job.count <= job.leaf_size) {
+    if (tid < 6) sh.nb[tid] = tid < 3 ? 0xFFFFFFFFu : 0u;
+    __syncthreads();
+    for (uint32_t i = tid; i < job.count; i += blockDim.x) {
+      const float4 l = plo[job.prim_offset + index[i]], h = phi[job.prim_offset + index[i]];
+      atomicMin(&sh.nb[0], ordered(l.x)); atomicMin(&sh.nb[1], ordered(l.y)); atomicMin(&sh.nb[2], ordered(l.z));
+      atomicMax(&sh.nb[3], ordered(h.x)); atomicMax(&sh.nb[4], ordered(h.y)); atomicMax(&sh.nb[5], ordered(h.z));
+    }
+    __syncthreads();
+    if (tid == 0) {
+      BvhNode nd;
+      nd.x = make_float4(unordered(sh.nb[0]), unordered(sh.nb[3]), 0.0f, 0.0f);
+      nd.y = make_float4(unordered(sh.nb[1]), unordered(sh.nb[4]), 0.0f, 0.0f);
+      nd.z = make_float4(unordered(sh.nb[2]), unordered(sh.nb[5]), 0.0f, 0.0f);
+      const int32_t leaf = job.leaves_are_values ? ~(int32_t)index[0] : ~(int32_t)job.leaf_base;
+      nd.c = make_int4(leaf, kEmptyChild, (int32_t)job.count, 0);
+      nodes[job.node_base] = nd;
+    }
+    return;
+  }
+  for (int guard = 0; guard < (int)(2 * job.count + 8); ++guard) {
+    __syncthreads();
+    if (sh.sp == 0) break;
+    if (tid == 0) {
+      --sh.sp;
+      sh.begin = sh.stack_begin[sh.sp];
+      sh.end = sh.stack_end[sh.sp];
+      sh.node = sh.stack_node[sh.sp];
+    }
+    if (tid < 6) sh.cb[tid] = tid < 3 ? 0xFFFFFFFFu : 0u;
+    for (uint32_t k = tid; k < 3 * kSahBins; k += blockDim.x) {
+      const uint32_t a = k / kSahBins, b = k % kSahBins;
+      sh.bin_count[a][b] = 0;
+      for (int c = 0; c < 3; ++c) {
+        sh.bin_lo[a][b][c] = 0xFFFFFFFFu;
+        sh.bin_hi[a][b][c] = 0u;
+      }
+    }
+    __syncthreads();
+    const uint32_t begin = sh.begin, end = sh.end;
+    // Centroid bounds.
+    for (uint32_t i = begin + tid; i < end; i += blockDim.x) {
+      const uint32_t p = job.prim_offset + index[i];
+      const float4 l = plo[p], h = phi[p];
+      const float cx = 0.5f * (l.x + h.x), cy = 0.5f * (l.y + h.y), cz = 0.5f * (l.z + h.z);
+      atomicMin(&sh.cb[0], ordered(cx)); atomicMin(&sh.cb[1], ordered(cy)); atomicMin(&sh.cb[2], ordered(cz));
+      atomicMax(&sh.cb[3], ordered(cx)); atomicMax(&sh.cb[4], ordered(cy)); atomicMax(&sh.cb[5], ordered(cz));
+    }
+    __syncthreads();
+    float cmin[3], scale[3];
+    for (int a = 0; a < 3; ++a) {
+      cmin[a] = unordered(sh.cb[a]);
+      const float extent = unordered(sh.cb[3 + a]) - cmin[a];
+      scale[a] = extent > 0.0f ? float(kSahBins) / extent : 0.0f;
+    }
+    // Binning on all three axes.
+    for (uint32_t i = begin + tid; i < end; i += blockDim.x) {
+      const uint32_t p = job.prim_offset + index[i];
+      const float4 l = plo[p], h = phi[p];
+      const float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+      for (int a = 0; a < 3; ++a) {
+        const int b = min(kSahBins - 1, max(0, (int)((c[a] - cmin[a]) * scale[a])));
+        atomicAdd(&sh.bin_count[a][b], 1u);
+        atomicMin(&sh.bin_lo[a][b][0], ordered(l.x)); atomicMin(&sh.bin_lo[a][b][1], ordered(l.y));
+        atomicMin(&sh.bin_lo[a][b][2], ordered(l.z));
+        atomicMax(&sh.bin_hi[a][b][0], ordered(h.x)); atomicMax(&sh.bin_hi[a][b][1], ordered(h.y));
+        atomicMax(&sh.bin_hi[a][b][2], ordered(h.z));
+      }
+    }
+    __syncthreads();
+    // The SAH sweep, one axis per thread.
+    if (tid < 3) {
+      const int a = tid;
+      float best = INFINITY;
+      int split = -1;
+      if (scale[a] > 0.0f) {
+        float right_area[kSahBins];
+        uint32_t right_count[kSahBins];
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        uint32_t cnt = 0;
+        for (int b = kSahBins - 1; b > 0; --b) {
+          if (sh.bin_count[a][b]) {
+            for (int c = 0; c < 3; ++c) {
+              lo[c] = fminf(lo[c], unordered(sh.bin_lo[a][b][c]));
+              hi[c] = fmaxf(hi[c], unordered(sh.bin_hi[a][b][c]));
+            }
+          }
+          cnt += sh.bin_count[a][b];
+          const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+          right_area[b] = cnt ? 2.0f * (dx * dy + dy * dz + dz * dx) : 0.0f;
+          right_count[b] = cnt;
+        }
+        lo[0] = lo[1] = lo[2] = INFINITY;
+        hi[0] = hi[1] = hi[2] = -INFINITY;
+        cnt = 0;
+        for (int b = 0; b < kSahBins - 1; ++b) {
+          if (sh.bin_count[a][b]) {
+            for (int c = 0; c < 3; ++c) {
+              lo[c] = fminf(lo[c], unordered(sh.bin_lo[a][b][c]));
+              hi[c] = fmaxf(hi[c], unordered(sh.bin_hi[a][b][c]));
+            }
+          }
+          cnt += sh.bin_count[a][b];
+          if (cnt == 0 || right_count[b + 1] == 0) continue;
+          const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+          const float cost = 2.0f * (dx * dy + dy * dz + dz * dx) * cnt + right_area[b + 1] * right_count[b + 1];
+          if (cost < best) {
+            best = cost;
+            split = b;
+          }
+        }
+      }
+      sh.best_cost[a] = best;
+      sh.split_at[a] = split;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int axis = -1;
+      float best = INFINITY;
+      for (int a = 0; a < 3; ++a)
+        if (sh.split_at[a] >= 0 && sh.best_cost[a] < best) {
+          best = sh.best_cost[a];
+          axis = a;
+        }
+      sh.best_axis = axis;
+      sh.best_split = axis >= 0 ? sh.split_at[axis] : -1;
+    }
+    __syncthreads();
+    const int axis = sh.best_axis, split = sh.best_split;
+    const uint32_t count = end - begin;
+    uint32_t mid;
+    if (axis < 0) {
+      mid = begin + count / 2;  // coincident centroids: split the list
+    } else {
+      // Stable partition: lefts to the front of tmp's range, rights after.
+      uint32_t left_base = 0;
+      uint32_t left_total = 0;
+      for (uint32_t t0 = begin; t0 < end; t0 += blockDim.x) {
+        const uint32_t i = t0 + tid;
+        uint32_t goes_left = 0;
+        uint32_t v = 0;
+        if (i < end) {
+          v = index[i];
+          const float4 l = plo[job.prim_offset + v], h = phi[job.prim_offset + v];
+          const float c = 0.5f * ((&l.x)[axis] + (&h.x)[axis]);
+          const int b = min(kSahBins - 1, max(0, (int)((c - cmin[axis]) * scale[axis])));
+          goes_left = b <= split ? 1u : 0u;
+        }
+        uint32_t prefix, tile_total;
+        BlockScan(scan_storage).ExclusiveSum(goes_left, prefix, tile_total);
+        __syncthreads();
+        if (i < end) {
+          if (goes_left) tmp[begin + left_base + prefix] = v;
+          else tmp[begin + (count - 1) - ((i - begin) - (left_base + prefix))] = v;
+        }
+        left_base += tile_total;
+        left_total = left_base;
+      }
+      __syncthreads();
+      // Rights were written back to front; copy both halves in order.
+      for (uint32_t i = begin + tid; i < end; i += blockDim.x) {
+        const uint32_t k = i - begin;
+        index[i] = k < left_total ? tmp[i] : tmp[begin + (count - 1) - (k - left_total)];
+      }
+      mid = begin + left_total;
+      if (mid == begin || mid == end) mid = begin + count / 2;
+    }
+    __syncthreads();
+    // Children bounds: a reduction over each half.
+    if (tid < 6) sh.nb[tid] = tid < 3 ? 0xFFFFFFFFu : 0u;
+    if (tid < 6) sh.cb[tid] = tid < 3 ? 0xFFFFFFFFu : 0u;  // reused for the right child
+    __syncthreads();
+    for (uint32_t i = begin + tid; i < end; i += blockDim.x) {
+      const float4 l = plo[job.prim_offset + index[i]], h = phi[job.prim_offset + index[i]];
+      uint32_t* b = i < mid ? sh.nb : sh.cb;
+      atomicMin(&b[0], ordered(l.x)); atomicMin(&b[1], ordered(l.y)); atomicMin(&b[2], ordered(l.z));
+      atomicMax(&b[3], ordered(h.x)); atomicMax(&b[4], ordered(h.y)); atomicMax(&b[5], ordered(h.z));
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const uint32_t ranges[2][2] = {{begin, mid}, {mid, end}};
+      const uint32_t* bounds[2] = {sh.nb, sh.cb};
+      int32_t child[2], ccount[2];
+      for (int k = 0; k < 2; ++k) {
+        const uint32_t n = ranges[k][1] - ranges[k][0];
+        if (n <= job.leaf_size) {
+          child[k] = job.leaves_are_values ? ~(int32_t)index[ranges[k][0]]
+                                           : ~(int32_t)(job.leaf_base + ranges[k][0]);
+          ccount[k] = (int32_t)n;
+        } else {
+          const uint32_t slot = sh.next_node++;
+          if (sh.sp >= kSahStack || slot >= job.count) {
+            sh.error = 1;
+            child[k] = kEmptyChild;
+            ccount[k] = 0;
+            continue;
+          }
+          sh.stack_begin[sh.sp] = ranges[k][0];
+          sh.stack_end[sh.sp] = ranges[k][1];
+          sh.stack_node[sh.sp] = slot;
+          ++sh.sp;
+          child[k] = (int32_t)(job.node_base + slot);
+          ccount[k] = 0;
+        }
+      }
+      BvhNode nd;
+      nd.x = make_float4(unordered(bounds[0][0]), unordered(bounds[0][3]), unordered(bounds[1][0]), unordered(bounds[1][3]));
+      nd.y = make_float4(unordered(bounds[0][1]), unordered(bounds[0][4]), unordered(bounds[1][1]), unordered(bounds[1][4]));
+      nd.z = make_float4(unordered(bounds[0][2]), unordered(bounds[0][5]), unordered(bounds[1][2]), unordered(bounds[1][5]));
+      nd.c = make_int4(child[0], child[1], ccount[0], ccount[1]);
+      nodes[job.node_base + sh.node] = nd;
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && (sh.error || sh.sp != 0)) atomicAdd(errors, 1u);
+}
+
+// Triangle boxes of every geometry of a batch: primitive i of job j at
+// prim_offset + i, its positions and triangles at the job's offsets.
+__global__ void k_batch_triangle_boxes(const float* __restrict__ positions, const uint32_t* __restrict__ triangles,
+    const uint64_t* __restrict__ vbase, const uint32_t* __restrict__ prim_job, const SahJob* __restrict__ jobs,
+    uint32_t total, float4* __restrict__ lo, float4* __restrict__ hi, uint32_t* __restrict__ idx) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const uint32_t j = prim_job[g];
+  const uint32_t local = g - jobs[j].prim_offset;
+  const float* P = positions + 3 * vbase[j];
+  float l[3] = {kFloatMax, kFloatMax, kFloatMax}, h[3] = {-kFloatMax, -kFloatMax, -kFloatMax};
+  for (int k = 0; k < 3; ++k) {
+    const uint32_t v = triangles[3 * (size_t)g + k];
+    for (int a = 0; a < 3; ++a) {
+      const float p = P[3 * (size_t)v + a];
+      l[a] = fminf(l[a], p);
+      h[a] = fmaxf(h[a], p);
+    }
+  }
+  lo[g] = make_float4(l[0], l[1], l[2], 0.0f);
+  hi[g] = make_float4(h[0], h[1], h[2], 0.0f);
+  idx[g] = local;
+}
+
+// The leaf-ordered triangle pool of a batch: pool slot leaf_base + i holds
+// triangle idx[prim_offset + i] of job j.
+__global__ void k_batch_write_triangles(const float* __restrict__ positions, const uint32_t* __restrict__ triangles,
+    const uint64_t* __restrict__ vbase, const uint64_t* __restrict__ tbase, const uint32_t* __restrict__ prim_job,
+    const SahJob* __restrict__ jobs, const uint32_t* __restrict__ idx, uint32_t total, float4* __restrict__ pool) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const uint32_t j = prim_job[g];
+  const SahJob job = jobs[j];
+  const uint32_t local = g - job.prim_offset;
+  const uint32_t p = idx[g];
+  const float* P = positions + 3 * vbase[j];
+  const uint32_t* T = triangles + 3 * tbase[j];
+  float4* out = pool + 3 * (size_t)(job.leaf_base + local);
+  for (int k = 0; k < 3; ++k) {
+    const uint32_t v = T[3 * (size_t)p + k];
+    out[k] = make_float4(P[3 * (size_t)v], P[3 * (size_t)v + 1], P[3 * (size_t)v + 2],
+        k == 0 ? __uint_as_float(p) : 0.0f);
+  }
+}
+
 inline uint32_t blocks(uint64_t n) { return (uint32_t)((n + kBuildBlock - 1) / kBuildBlock); }
 
 }  // namespace
@@ -340,6 +665,98 @@ cudaError_t BvhBuilder::build_triangles(const float* positions, const uint32_t* 
   if ((e = build_common(n, nodes, node_base, tri_base, false, stream, &sorted)) != cudaSuccess) return e;
   k_write_triangles<<<blocks(n), kBuildBlock, 0, stream>>>(sorted, positions, triangles, n, tri_pool, tri_base);
   return cudaGetLastError();
+}
+
+cudaError_t BvhBuilder::build_triangle_batch(const float* positions, const uint32_t* triangles,
+    const std::vector<BatchGeometry>& geometries, BvhNode* nodes, float4* tri_pool, cudaStream_t stream) {
+  std::vector<SahJob> jobs;
+  std::vector<uint64_t> vbase, tbase;
+  uint32_t total = 0;
+  for (const BatchGeometry& g : geometries) {
+    if (g.count == 0) continue;
+    SahJob j;
+    j.prim_offset = total;
+    j.count = g.count;
+    j.node_base = g.node_base;
+    j.leaf_base = g.tri_base;
+    j.leaf_size = 4;
+    j.leaves_are_values = 0;
+    jobs.push_back(j);
+    vbase.push_back(g.vertex_offset);
+    tbase.push_back(g.tri_base);
+    total += g.count;
+  }
+  if (jobs.empty()) return cudaSuccess;
+  std::vector<uint32_t> prim_job(total);
+  for (uint32_t k = 0; k < jobs.size(); ++k)
+    for (uint32_t i = 0; i < jobs[k].count; ++i) prim_job[jobs[k].prim_offset + i] = k;
+  cudaError_t e = reserve(total, stream);
+  if (e != cudaSuccess) return e;
+  SahJob* d_jobs = nullptr;
+  uint64_t* d_vbase = nullptr;
+  uint64_t* d_tbase = nullptr;
+  uint32_t* d_prim_job = nullptr;
+  uint32_t* d_tris = nullptr;
+  if ((e = cudaMalloc(&d_jobs, jobs.size() * sizeof(SahJob))) != cudaSuccess ||
+      (e = cudaMalloc(&d_vbase, jobs.size() * 8)) != cudaSuccess ||
+      (e = cudaMalloc(&d_tbase, jobs.size() * 8)) != cudaSuccess ||
+      (e = cudaMalloc(&d_prim_job, (size_t)total * 4)) != cudaSuccess ||
+      (e = cudaMalloc(&d_tris, (size_t)total * 12)) != cudaSuccess)
+    return e;
+  cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(SahJob), cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_vbase, vbase.data(), jobs.size() * 8, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_tbase, tbase.data(), jobs.size() * 8, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_prim_job, prim_job.data(), (size_t)total * 4, cudaMemcpyHostToDevice, stream);
+  // Each job's triangles, gathered in batch order.
+  for (size_t k = 0; k < jobs.size(); ++k)
+    cudaMemcpyAsync(d_tris + 3 * (size_t)jobs[k].prim_offset, triangles + 3 * tbase[k], (size_t)jobs[k].count * 12,
+        cudaMemcpyDeviceToDevice, stream);
+  k_batch_triangle_boxes<<<blocks(total), kBuildBlock, 0, stream>>>(positions, d_tris, d_vbase, d_prim_job,
+      d_jobs, total, plo_, phi_, values_);
+  cudaMemsetAsync(flags_, 0, 4, stream);
+  k_sah_build<<<(uint32_t)jobs.size(), kSahBlock, 0, stream>>>(d_jobs, plo_, phi_, values_, values_alt_, nodes,
+      flags_);
+  // The pool: leaf_base is the geometry's tri_base, and the batch's
+  // triangles are addressed through the gathered copy.
+  std::vector<uint64_t> zero(jobs.size());
+  for (size_t k = 0; k < jobs.size(); ++k) zero[k] = jobs[k].prim_offset;
+  cudaMemcpyAsync(d_tbase, zero.data(), jobs.size() * 8, cudaMemcpyHostToDevice, stream);
+  k_batch_write_triangles<<<blocks(total), kBuildBlock, 0, stream>>>(positions, d_tris, d_vbase, d_tbase,
+      d_prim_job, d_jobs, values_, total, tri_pool);
+  uint32_t errors = 0;
+  cudaMemcpyAsync(&errors, flags_, 4, cudaMemcpyDeviceToHost, stream);
+  e = cudaStreamSynchronize(stream);
+  cudaFree(d_jobs);
+  cudaFree(d_vbase);
+  cudaFree(d_tbase);
+  cudaFree(d_prim_job);
+  cudaFree(d_tris);
+  if (e != cudaSuccess) return e;
+  return errors ? cudaErrorUnknown : cudaSuccess;
+}
+
+cudaError_t BvhBuilder::build_instances_sah(const InstanceShading* shade, const InstanceTraversal* trav,
+    const BvhNode* blas, uint32_t n, BvhNode* nodes, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  cudaError_t e = reserve(n, stream);
+  if (e != cudaSuccess) return e;
+  init_bounds(bounds_, stream);
+  k_instance_boxes<<<blocks(n), kBuildBlock, 0, stream>>>(shade, trav, blas, n, plo_, phi_, bounds_);
+  std::vector<uint32_t> iota(n);
+  for (uint32_t i = 0; i < n; ++i) iota[i] = i;
+  cudaMemcpyAsync(values_, iota.data(), (size_t)n * 4, cudaMemcpyHostToDevice, stream);
+  SahJob job{0, n, 0, 0, 1, 1};
+  SahJob* d_job = nullptr;
+  if ((e = cudaMalloc(&d_job, sizeof(SahJob))) != cudaSuccess) return e;
+  cudaMemcpyAsync(d_job, &job, sizeof(job), cudaMemcpyHostToDevice, stream);
+  cudaMemsetAsync(flags_, 0, 4, stream);
+  k_sah_build<<<1, kSahBlock, 0, stream>>>(d_job, plo_, phi_, values_, values_alt_, nodes, flags_);
+  uint32_t errors = 0;
+  cudaMemcpyAsync(&errors, flags_, 4, cudaMemcpyDeviceToHost, stream);
+  e = cudaStreamSynchronize(stream);
+  cudaFree(d_job);
+  if (e != cudaSuccess) return e;
+  return errors ? cudaErrorUnknown : cudaSuccess;
 }
 
 cudaError_t BvhBuilder::build_instances(const InstanceShading* shade,

@@ -1,15 +1,36 @@
 // SPDX-License-Identifier: Apache-2.0
-// On-device LBVH builder (see bvh_build.cu).
+// On-device BVH builders: per-CTA binned SAH and LBVH (see bvh_build.cu).
 #pragma once
+
+#include <vector>
 
 #include "scene.cuh"
 
 namespace lotus {
 
-// Scratch for building one BVH at a time, grown to the largest primitive
-// count seen. A BVH over n > 1 primitives has n - 1 nodes; over one, one.
+// One geometry of a batched build: its triangles in the concatenated
+// arrays and its slots in the node and triangle pools.
+struct BatchGeometry {
+  uint64_t vertex_offset;
+  uint32_t tri_base;
+  uint32_t count;
+  uint32_t node_base;
+};
+
+// Geometries up to this many triangles build with the per-CTA binned-SAH
+// builder; larger ones with the LBVH.
+constexpr uint32_t kSahMaxTriangles = 65536;
+
+// Scratch for building BVHs, grown to the largest primitive count seen. A
+// BVH over n > 1 primitives has at most n - 1 nodes; over one, one.
 class BvhBuilder {
  public:
+  // Binned-SAH BLASes of many geometries in one launch (one CTA each).
+  cudaError_t build_triangle_batch(const float* positions, const uint32_t* triangles,
+      const std::vector<BatchGeometry>& geometries, BvhNode* nodes, float4* tri_pool, cudaStream_t stream);
+  // The binned-SAH TLAS (one instance per leaf).
+  cudaError_t build_instances_sah(const InstanceShading* shade, const InstanceTraversal* trav,
+      const BvhNode* blas, uint32_t n, BvhNode* nodes, cudaStream_t stream);
   ~BvhBuilder() { release(); }
   // One BLAS: nodes at nodes[node_base ...], leaf-ordered triangles at
   // tri_pool[3 * tri_base ...]. Positions and triangles are device arrays.

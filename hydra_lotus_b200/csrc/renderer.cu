@@ -593,12 +593,24 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
   if (!R.ok(d_pos.upload(h_pos.data(), h_pos.size(), st), "positions", detail) ||
       !R.ok(d_tri.upload(h_tri.data(), h_tri.size(), st), "triangles", detail))
     return fail(detail);
-  for (uint32_t g = 0; g < s.geometry_count; ++g) {
-    const lotus_geometry& geo = s.geometries[g];
-    if (!geo.triangle_count) continue;
-    cudaError_t e = R.builder.build_triangles(d_pos.ptr + 3 * vbase[g], d_tri.ptr + 3 * (size_t)tri_base[g],
-        geo.triangle_count, R.blas.ptr, node_base[g], R.tris.ptr, tri_base[g], st);
-    if (!R.ok(e, "BLAS build", detail)) return fail(detail);
+  {
+    // Geometries up to kSahMaxTriangles: binned SAH, all in one launch;
+    // larger ones: LBVH, one at a time.
+    std::vector<BatchGeometry> batch;
+    for (uint32_t g = 0; g < s.geometry_count; ++g) {
+      const lotus_geometry& geo = s.geometries[g];
+      if (!geo.triangle_count) continue;
+      if (geo.triangle_count <= kSahMaxTriangles) {
+        batch.push_back({vbase[g], tri_base[g], geo.triangle_count, node_base[g]});
+        continue;
+      }
+      cudaError_t e = R.builder.build_triangles(d_pos.ptr + 3 * vbase[g], d_tri.ptr + 3 * (size_t)tri_base[g],
+          geo.triangle_count, R.blas.ptr, node_base[g], R.tris.ptr, tri_base[g], st);
+      if (!R.ok(e, "BLAS build", detail)) return fail(detail);
+    }
+    if (!R.ok(R.builder.build_triangle_batch(d_pos.ptr, d_tri.ptr, batch, R.blas.ptr, R.tris.ptr, st),
+            "BLAS build", detail))
+      return fail(detail);
   }
   // Corner normals.
   if (normal_total) {
@@ -683,8 +695,12 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
       !R.ok(R.inst_shade.upload(h_shade.data(), h_shade.size(), st), "instances", detail) ||
       !R.ok(R.tlas.resize(std::max<uint32_t>(BvhBuilder::node_count(s.instance_count), 1)), "TLAS", detail))
     return fail(detail);
-  if (!R.ok(R.builder.build_instances(R.inst_shade.ptr, R.inst_trav.ptr, R.blas.ptr, s.instance_count,
-                R.tlas.ptr, st), "TLAS build", detail))
+  if (!R.ok(s.instance_count <= kSahMaxTriangles
+                ? R.builder.build_instances_sah(R.inst_shade.ptr, R.inst_trav.ptr, R.blas.ptr, s.instance_count,
+                      R.tlas.ptr, st)
+                : R.builder.build_instances(R.inst_shade.ptr, R.inst_trav.ptr, R.blas.ptr, s.instance_count,
+                      R.tlas.ptr, st),
+            "TLAS build", detail))
     return fail(detail);
   cudaEventRecord(R.ev_stop, st);
   if (!R.ok(cudaStreamSynchronize(st), "scene update", detail)) return fail(detail);

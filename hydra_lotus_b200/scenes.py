@@ -520,3 +520,23 @@ def orbit_camera(frame, frames=120, radius=3.0, amplitude=0.35, aspect=1.0):
     view = look_at(eye, (0.0, 0.0, 0.0))
     projection = perspective(45.0, aspect, 1.0, 10.0)
     return view, multiply(projection, view)
+
+
+def big_mesh(seed=0, size=96, subdivisions=6):
+    """One displaced icosphere of 20 * 4^subdivisions triangles (81,920 at
+    6, above the per-CTA SAH builder's limit, so it builds as an LBVH) with
+    a GGX and a Lambert instance of it under the procedural sky."""
+    s = Scene(f"big-mesh-{seed}")
+    v, f = icosphere(subdivisions)
+    r = 1.0 + 0.2 * perlin3(v * 3.0, seed)
+    p = (v * r[:, None]).astype(F32)
+    g = s.add_geometry(p, f, corner_normals(p, f))
+    metal = s.add_material(preview_material((0.9, 0.7, 0.5), roughness=0.3, metallic=1.0))
+    clay = s.add_material(preview_material((0.6, 0.6, 0.6), roughness=0.7, ior=1.0))
+    s.add_instance(g, metal, affine(np.eye(3), (-1.2, 0.0, 0.0)))
+    s.add_instance(g, clay, affine(rotation_y(0.7) * 0.8, (1.2, 0.0, 0.0)))
+    s.add_instance(s.add_geometry(*quad([[-6, -1.2, 6], [6, -1.2, 6], [6, -1.2, -6], [-6, -1.2, -6]])), clay)
+    s.set_environment(procedural_sky(256, 128, seed))
+    s.world_to_clip = multiply(perspective(45.0, 1.0, 0.1, 100.0), look_at((0.0, 1.5, 6.0), (0.0, 0.0, 0.0)))
+    s.width = s.height = size
+    return s

@@ -58,6 +58,19 @@ def test_sphere_field_paths_match_oracle(cuda, renderer, oracle_lib, integrator)
     p.assert_ok()
 
 
+@pytest.mark.parametrize("integrator", INTEGRATORS)
+def test_large_mesh_paths_match_oracle(cuda, renderer, oracle_lib, integrator):
+    """A mesh above the per-CTA SAH builder's limit builds as an LBVH."""
+    scene = scenes.big_mesh()
+    st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=6, sample_index=5)
+    res, color = render(cuda, renderer, scene, st)
+    want, _ = oracle_lib.OracleScene(scene).sample(scene.frame(st), 5)
+    p = PathParity(color, want)
+    print(p)
+    p.assert_ok()
+
+
 def test_light_table_matches_oracle(cuda, renderer, oracle_lib):
     for scene in (scenes.box_room(), scenes.cornell_reference(), small_sphere_field()):
         cuda.check(renderer.update_scene(scene), "update_scene")
