@@ -43,7 +43,10 @@ WORKLOAD = ("sphere-field seed 0: 4096 instanced Perlin-displaced icospheres (su
 # entry (4), origin, direction and radiance sections (48), the hit section
 # (16) and the hit-queue entry (4).
 EXTEND_STATE_BYTES = 72
-NODE_BYTES, TRIANGLE_BYTES, INSTANCE_BYTES = 64, 48, 64
+# A 4-wide node visit reads its six box bounds and four child references
+# (112 of its 128 bytes); a triangle test its three corners (48 of 64); an
+# instance entry its 64-byte traversal record.
+NODE_BYTES, TRIANGLE_BYTES, INSTANCE_BYTES = 112, 48, 64
 
 
 def settings(sample_index):

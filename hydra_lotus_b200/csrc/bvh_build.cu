@@ -248,12 +248,13 @@ __global__ void k_write_triangles(const uint32_t* __restrict__ values,
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t p = values[i];
-  float4* out = pool + 3 * (size_t)(base + i);
+  float4* out = pool + kTriStride * (size_t)(base + i);
   for (int k = 0; k < 3; ++k) {
     const uint32_t v = triangles[3 * (size_t)p + k];
     out[k] = make_float4(positions[3 * (size_t)v], positions[3 * (size_t)v + 1],
         positions[3 * (size_t)v + 2], k == 0 ? __uint_as_float(p) : 0.0f);
   }
+  out[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
 
@@ -292,6 +293,7 @@ struct SahShared {
   int split_at[3];
   uint32_t left_total;
   uint32_t error;
+  uint32_t done;
 };
 
 __global__ void __launch_bounds__(kSahBlock) k_sah_build(const SahJob* __restrict__ jobs,
@@ -337,14 +339,19 @@ __global__ void __launch_bounds__(kSahBlock) k_sah_build(const SahJob* __restric
     return;
   }
   for (int guard = 0; guard < (int)(2 * job.count + 8); ++guard) {
-    __syncthreads();
-    if (sh.sp == 0) break;
+    // Thread 0 pops the next range; the barrier publishes it (and orders
+    // the pop after every thread's use of the previous node's state).
     if (tid == 0) {
-      --sh.sp;
-      sh.begin = sh.stack_begin[sh.sp];
-      sh.end = sh.stack_end[sh.sp];
-      sh.node = sh.stack_node[sh.sp];
+      sh.done = sh.sp == 0 ? 1u : 0u;
+      if (sh.sp > 0) {
+        --sh.sp;
+        sh.begin = sh.stack_begin[sh.sp];
+        sh.end = sh.stack_end[sh.sp];
+        sh.node = sh.stack_node[sh.sp];
+      }
     }
+    __syncthreads();
+    if (sh.done) break;
     if (tid < 6) sh.cb[tid] = tid < 3 ? 0xFFFFFFFFu : 0u;
     for (uint32_t k = tid; k < 3 * kSahBins; k += blockDim.x) {
       const uint32_t a = k / kSahBins, b = k % kSahBins;
@@ -570,12 +577,90 @@ __global__ void k_batch_write_triangles(const float* __restrict__ positions, con
   const uint32_t p = idx[g];
   const float* P = positions + 3 * vbase[j];
   const uint32_t* T = triangles + 3 * tbase[j];
-  float4* out = pool + 3 * (size_t)(job.leaf_base + local);
+  float4* out = pool + kTriStride * (size_t)(job.leaf_base + local);
   for (int k = 0; k < 3; ++k) {
     const uint32_t v = T[3 * (size_t)p + k];
     out[k] = make_float4(P[3 * (size_t)v], P[3 * (size_t)v + 1], P[3 * (size_t)v + 2],
         k == 0 ? __uint_as_float(p) : 0.0f);
   }
+  out[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// The 4-wide nodes: wide node i holds binary node i's subtree cut at four
+// children, opening the interior child with the largest surface area until
+// there are four (the greedy collapse of Wald et al., "Getting Rid of
+// Packets", 2008). Every binary node gets a wide node at its own index, so
+// the collapse is one independent thread per node; a wide node whose binary
+// node was opened by its parent is never referenced.
+__global__ void k_collapse4(const BvhNode* __restrict__ bin, uint32_t n, Bvh4Node* __restrict__ wide,
+    int leaves_are_instances) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float lo[4][3], hi[4][3];
+  int32_t ref[4], cnt[4];
+  int k = 0;
+  auto take = [&](const BvhNode& nd) {
+    const float bx[4] = {nd.x.x, nd.x.y, nd.x.z, nd.x.w}, by[4] = {nd.y.x, nd.y.y, nd.y.z, nd.y.w},
+                bz[4] = {nd.z.x, nd.z.y, nd.z.z, nd.z.w};
+    const int32_t c[2] = {nd.c.x, nd.c.y}, m[2] = {nd.c.z, nd.c.w};
+    for (int j = 0; j < 2; ++j) {
+      if (c[j] == kEmptyChild || k >= 4) continue;
+      lo[k][0] = bx[2 * j]; hi[k][0] = bx[2 * j + 1];
+      lo[k][1] = by[2 * j]; hi[k][1] = by[2 * j + 1];
+      lo[k][2] = bz[2 * j]; hi[k][2] = bz[2 * j + 1];
+      ref[k] = c[j];
+      cnt[k] = m[j];
+      ++k;
+    }
+  };
+  take(bin[i]);
+  for (int round = 0; round < 2 && k < 4; ++round) {
+    int open = -1;
+    float best = -1.0f;
+    for (int j = 0; j < k; ++j) {
+      if (ref[j] < 0 || (uint32_t)ref[j] >= n) continue;
+      const float dx = hi[j][0] - lo[j][0], dy = hi[j][1] - lo[j][1], dz = hi[j][2] - lo[j][2];
+      const float area = dx * dy + dy * dz + dz * dx;
+      if (area > best) {
+        best = area;
+        open = j;
+      }
+    }
+    if (open < 0) break;
+    const BvhNode child = bin[ref[open]];
+    // Replace the opened child by the last one, then append its children.
+    --k;
+    for (int a = 0; a < 3; ++a) {
+      lo[open][a] = lo[k][a];
+      hi[open][a] = hi[k][a];
+    }
+    ref[open] = ref[k];
+    cnt[open] = cnt[k];
+    take(child);
+  }
+  float ox[4], oX[4], oy[4], oY[4], oz[4], oZ[4];
+  int32_t oc[4], on[4];
+  for (int j = 0; j < 4; ++j) {
+    const bool used = j < k;
+    ox[j] = used ? lo[j][0] : 0.0f; oX[j] = used ? hi[j][0] : 0.0f;
+    oy[j] = used ? lo[j][1] : 0.0f; oY[j] = used ? hi[j][1] : 0.0f;
+    oz[j] = used ? lo[j][2] : 0.0f; oZ[j] = used ? hi[j][2] : 0.0f;
+    oc[j] = used ? ref[j] : kEmptyChild;
+    on[j] = used ? cnt[j] : 0;
+    if (used && ref[j] < 0 && !leaves_are_instances) {
+      // BLAS leaf: the count goes into the reference's low bits.
+      const uint32_t first = ~(uint32_t)ref[j];
+      const uint32_t count = (uint32_t)min(max(cnt[j], 1), 1 << kLeafCountBits);
+      oc[j] = (int32_t)~((first << kLeafCountBits) | (count - 1u));
+    }
+  }
+  Bvh4Node w;
+  w.lo_x = make_float4(ox[0], ox[1], ox[2], ox[3]); w.hi_x = make_float4(oX[0], oX[1], oX[2], oX[3]);
+  w.lo_y = make_float4(oy[0], oy[1], oy[2], oy[3]); w.hi_y = make_float4(oY[0], oY[1], oY[2], oY[3]);
+  w.lo_z = make_float4(oz[0], oz[1], oz[2], oz[3]); w.hi_z = make_float4(oZ[0], oZ[1], oZ[2], oZ[3]);
+  w.child = make_int4(oc[0], oc[1], oc[2], oc[3]);
+  w.count = make_int4(on[0], on[1], on[2], on[3]);
+  wide[i] = w;
 }
 
 inline uint32_t blocks(uint64_t n) { return (uint32_t)((n + kBuildBlock - 1) / kBuildBlock); }
@@ -668,7 +753,8 @@ cudaError_t BvhBuilder::build_triangles(const float* positions, const uint32_t* 
 }
 
 cudaError_t BvhBuilder::build_triangle_batch(const float* positions, const uint32_t* triangles,
-    const std::vector<BatchGeometry>& geometries, BvhNode* nodes, float4* tri_pool, cudaStream_t stream) {
+    const std::vector<BatchGeometry>& geometries, BvhNode* nodes, float4* tri_pool, cudaStream_t stream,
+    uint32_t leaf_size) {
   std::vector<SahJob> jobs;
   std::vector<uint64_t> vbase, tbase;
   uint32_t total = 0;
@@ -679,7 +765,7 @@ cudaError_t BvhBuilder::build_triangle_batch(const float* positions, const uint3
     j.count = g.count;
     j.node_base = g.node_base;
     j.leaf_base = g.tri_base;
-    j.leaf_size = 4;
+    j.leaf_size = leaf_size;
     j.leaves_are_values = 0;
     jobs.push_back(j);
     vbase.push_back(g.vertex_offset);
@@ -757,6 +843,13 @@ cudaError_t BvhBuilder::build_instances_sah(const InstanceShading* shade, const 
   cudaFree(d_job);
   if (e != cudaSuccess) return e;
   return errors ? cudaErrorUnknown : cudaSuccess;
+}
+
+cudaError_t BvhBuilder::collapse(const BvhNode* binary, uint32_t n, Bvh4Node* wide, bool leaves_are_instances,
+    cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  k_collapse4<<<blocks(n), kBuildBlock, 0, stream>>>(binary, n, wide, leaves_are_instances ? 1 : 0);
+  return cudaGetLastError();
 }
 
 cudaError_t BvhBuilder::build_instances(const InstanceShading* shade,

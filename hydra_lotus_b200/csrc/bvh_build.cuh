@@ -27,19 +27,25 @@ class BvhBuilder {
  public:
   // Binned-SAH BLASes of many geometries in one launch (one CTA each).
   cudaError_t build_triangle_batch(const float* positions, const uint32_t* triangles,
-      const std::vector<BatchGeometry>& geometries, BvhNode* nodes, float4* tri_pool, cudaStream_t stream);
+      const std::vector<BatchGeometry>& geometries, BvhNode* nodes, float4* tri_pool, cudaStream_t stream,
+      uint32_t leaf_size);
   // The binned-SAH TLAS (one instance per leaf).
   cudaError_t build_instances_sah(const InstanceShading* shade, const InstanceTraversal* trav,
       const BvhNode* blas, uint32_t n, BvhNode* nodes, cudaStream_t stream);
   ~BvhBuilder() { release(); }
   // One BLAS: nodes at nodes[node_base ...], leaf-ordered triangles at
-  // tri_pool[3 * tri_base ...]. Positions and triangles are device arrays.
+  // tri_pool[kTriStride * tri_base ...]. Positions and triangles are device arrays.
   cudaError_t build_triangles(const float* positions, const uint32_t* triangles, uint32_t n,
       BvhNode* nodes, uint32_t node_base, float4* tri_pool, uint32_t tri_base,
       cudaStream_t stream);
   // The TLAS over the instances' world boxes; leaves hold instance indices.
   cudaError_t build_instances(const InstanceShading* shade, const InstanceTraversal* trav,
       const BvhNode* blas, uint32_t n, BvhNode* nodes, cudaStream_t stream);
+  // The 4-wide pool the traversal reads: wide[i] for every binary node i
+  // (node references keep their meaning; BLAS leaves take their counts into
+  // their references). One launch over the whole pool.
+  static cudaError_t collapse(const BvhNode* binary, uint32_t n, Bvh4Node* wide, bool leaves_are_instances,
+      cudaStream_t stream);
   void release();
 
   static uint32_t node_count(uint32_t n) { return n > 1 ? n - 1 : n; }

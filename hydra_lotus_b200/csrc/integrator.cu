@@ -10,6 +10,8 @@
 // shadow ray to the shadow kernel, which adds the light to the path's
 // radiance before the next extension reads it, so the radiance sums run in
 // the reference's order.
+#include <algorithm>
+
 #include "integrator.cuh"
 #include "temporal.cuh"
 
@@ -378,81 +380,154 @@ __global__ void __launch_bounds__(kBlock) k_wf_shade(SceneView S,
 
 // The shadow rays of bounce `bounce`: ShadowTransmittance and the rest of
 // ShadowedLight, added to the path's radiance.
+constexpr unsigned kFullWarp = 0xFFFFFFFFu;
+constexpr uint32_t kDefaultRefillBelow = 24;
+
+// The persistent kernels' ray fetch: when fewer than `refill_below` lanes
+// of the warp hold a ray (and the queue is not exhausted), the idle lanes
+// take the next queue entries with one atomic per warp. Returns the lane's
+// queue index, or n when it got none.
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor, uint32_t n, bool active,
+    uint32_t refill_below, bool& exhausted) {
+  const unsigned act = __ballot_sync(kFullWarp, active);
+  if (exhausted || (uint32_t)__popc(act) >= refill_below) return n;
+  const unsigned need = ~act;
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(cursor, (uint32_t)__popc(need));
+  base = __shfl_sync(kFullWarp, base, 0);
+  exhausted = base + (uint32_t)__popc(need) >= n;
+  if (active) return n;
+  const uint32_t index = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+  return index < n ? index : n;
+}
+
+// ShadowedLight's visibility (transport.slang:82-115) for the shadow queue,
+// as a persistent kernel: each lane walks one shadow ray at a time and adds
+// the light to the path's radiance when the ray arrives.
 template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_wf_shadow(SceneView S, PathState P, Queues Q,
-    uint32_t bounce, VisitCounters* visits) {
+    uint32_t bounce, uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits) {
   const uint32_t n = Q.counts[3 * bounce + 2];
-  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
-  if (blockIdx.x * blockDim.x >= n) return;
-  if (kCount) {
-    TraversalCounters vc = {0, 0, 0};
-    if (index < n) {
+  TraversalCounters vc = {0, 0, 0};
+  uint32_t rays = 0;
+  Walk W;
+  WalkStack stack;
+  uint32_t rng = 0;
+  uint32_t index = 0;
+  bool active = false, exhausted = false;
+  for (;;) {
+    const uint32_t got = warp_fetch(fetch, n, active, refill_below, exhausted);
+    if (got < n) {
+      index = got;
       const float4 ro = Q.shadow.ray_o[index];
       const float4 rd = Q.shadow.ray_d[index];
-      trace_shadow<true>(S, V(ro), V(rd), 0.0f, ro.w, &vc);
+      walk_begin(S, W, V(ro), V(rd), 0.0f, ro.w);
+      active = true;
+      ++rays;
     }
-    warp_add64(&visits->rays[2], index < n ? 1u : 0u);
+    if (!__any_sync(kFullWarp, active)) break;
+    if (walk_round<true, kCount>(S, W, stack, rng, active, &vc)) {
+      active = false;
+      const float tr = W.transmittance;
+      if (tr > 0.0f) {
+        const float4 rd = Q.shadow.ray_d[index];
+        const float4 fl = Q.shadow.fl[index];
+        const float4 thr = Q.shadow.thr[index];
+        const uint32_t slot = __float_as_uint(thr.w);
+        const F3 c = shadow_contribution(V(fl), rd.w, fl.w, tr);
+        float4 rad = P.radiance[slot];
+        const F3 R = V(rad) + V(thr) * c;
+        rad.x = R.x;
+        rad.y = R.y;
+        rad.z = R.z;
+        P.radiance[slot] = rad;
+      }
+    }
+  }
+  if (kCount) {
+    warp_add64(&visits->rays[2], rays);
     warp_add64(&visits->nodes[2], vc.nodes);
     warp_add64(&visits->triangles[2], vc.triangles);
     warp_add64(&visits->instances[2], vc.instances);
   }
-  if (index >= n) return;
-  const float4 ro = Q.shadow.ray_o[index];
-  const float4 rd = Q.shadow.ray_d[index];
-  const float tr = trace_shadow(S, V(ro), V(rd), 0.0f, ro.w);
-  if (tr > 0.0f) {
-    const float4 fl = Q.shadow.fl[index];
-    const float4 thr = Q.shadow.thr[index];
-    const uint32_t slot = __float_as_uint(thr.w);
-    const F3 c = shadow_contribution(V(fl), rd.w, fl.w, tr);
-    float4 rad = P.radiance[slot];
-    const F3 R = V(rad) + V(thr) * c;
-    rad.x = R.x;
-    rad.y = R.y;
-    rad.z = R.z;
-    P.radiance[slot] = rad;
-  }
 }
 
-// Intersect (wavefront.slang:230-262): a hit is queued for shading; a miss
-// ends the path with the environment.
+// Intersect (wavefront.slang:230-262) as a persistent kernel: a hit is
+// queued for shading; a miss ends the path with the environment. Each warp
+// stages its hits in shared memory and appends them to the hit queue 32 at
+// a time.
 template <bool kCount>
 __global__ void __launch_bounds__(kBlock) k_wf_extend(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce,
-    VisitCounters* visits) {
-  TraversalCounters vc = {0, 0, 0};
+    uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits) {
+  __shared__ uint32_t staged[kBlock / 32][64];
   const uint32_t n = Q.counts[3 * bounce];
-  if (blockIdx.x * blockDim.x >= n) return;
   const FrameConst& f = *fcp;
-  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = index < n;
-  bool found = false;
-  uint32_t slot = 0;
-  if (valid) {
-    slot = Q.ray[bounce & 1][index];
-    const float4 o = P.origin[slot];
-    const float4 d = P.direction[slot];
-    float4 rad = P.radiance[slot];
-    uint32_t rng = __float_as_uint(rad.w);
-    Hit hit;
-    found = trace_closest<kCount>(S, V(o), V(d), o.w, d.w, rng, hit, &vc);
-    if (found) {
-      P.hit[slot] = make_uint4(hit.instance, hit.tri, __float_as_uint(hit.b1), __float_as_uint(hit.b2));
-      if (rng != __float_as_uint(rad.w)) {
-        rad.w = __uint_as_float(rng);
-        P.radiance[slot] = rad;
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t* stage = staged[threadIdx.x >> 5];
+  uint32_t* hits = &Q.counts[3 * bounce + 1];
+  uint32_t staged_count = 0;
+  TraversalCounters vc = {0, 0, 0};
+  uint32_t rays = 0;
+  Walk W;
+  WalkStack stack;
+  uint32_t rng = 0, rng0 = 0, slot = 0;
+  bool active = false, exhausted = false;
+  for (;;) {
+    const uint32_t got = warp_fetch(fetch, n, active, refill_below, exhausted);
+    if (got < n) {
+      slot = Q.ray[bounce & 1][got];
+      const float4 o = P.origin[slot];
+      const float4 d = P.direction[slot];
+      rng = rng0 = __float_as_uint(P.radiance[slot].w);
+      walk_begin(S, W, V(o), V(d), o.w, d.w);
+      active = true;
+      ++rays;
+    }
+    if (!__any_sync(kFullWarp, active)) break;
+    bool emit = false;
+    if (walk_round<false, kCount>(S, W, stack, rng, active, &vc)) {
+      active = false;
+      if (W.found) {
+        P.hit[slot] = make_uint4(W.best_instance, W.best_tri, __float_as_uint(W.b1), __float_as_uint(W.b2));
+        if (rng != rng0) P.radiance[slot].w = __uint_as_float(rng);
+        emit = true;
+      } else {
+        const float4 rad = P.radiance[slot];
+        const float4 thr = P.throughput[slot];
+        const uint32_t flags = thr.w < 0.0f ? kUnweightedLight : 0u;
+        const F3 R = V(rad) + V(thr) * miss_radiance(S, f, W.direction, flags, thr.w);
+        P.radiance[slot] = F4(R, 1.0f);
       }
-    } else {
-      const float4 thr = P.throughput[slot];
-      const uint32_t flags = thr.w < 0.0f ? kUnweightedLight : 0u;
-      const F3 R = V(rad) + V(thr) * miss_radiance(S, f, V(d), flags, thr.w);
-      P.radiance[slot] = F4(R, 1.0f);
+    }
+    const unsigned em = __ballot_sync(kFullWarp, emit);
+    if (em) {
+      if (emit) stage[staged_count + (uint32_t)__popc(em & ((1u << lane) - 1u))] = slot;
+      staged_count += (uint32_t)__popc(em);
+      if (staged_count >= 32) {
+        __syncwarp();
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(hits, 32u);
+        base = __shfl_sync(kFullWarp, base, 0);
+        Q.hit[base + lane] = stage[lane];
+        const uint32_t carry = stage[32 + lane];
+        __syncwarp();
+        stage[lane] = carry;
+        __syncwarp();
+        staged_count -= 32;
+      }
     }
   }
-  const uint32_t at = warp_append(&Q.counts[3 * bounce + 1], found);
-  if (found) Q.hit[at] = slot;
+  __syncwarp();
+  if (staged_count) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(hits, staged_count);
+    base = __shfl_sync(kFullWarp, base, 0);
+    if (lane < staged_count) Q.hit[base + lane] = stage[lane];
+  }
   if (kCount) {
-    warp_add64(&visits->rays[1], valid ? 1u : 0u);
+    warp_add64(&visits->rays[1], rays);
     warp_add64(&visits->nodes[1], vc.nodes);
     warp_add64(&visits->triangles[1], vc.triangles);
     warp_add64(&visits->instances[1], vc.instances);
@@ -542,19 +617,36 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
     k_reference_pt<false><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, nullptr);
 }
 
+// Blocks of a persistent tracing kernel: every resident block on every
+// SM (or `blocks_per_sm`), no more than the queue could fill.
+template <typename Kernel>
+uint32_t persistent_grid(Kernel kernel, uint32_t capacity, const TraceTuning& tuning) {
+  int device = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0);
+  if (tuning.blocks_per_sm) per_sm = std::min<int>(per_sm, (int)tuning.blocks_per_sm);
+  const uint32_t grid = (uint32_t)std::max(1, sms) * (uint32_t)std::max(1, per_sm);
+  return std::max(1u, std::min(grid, (capacity + kBlock - 1) / kBlock));
+}
+
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
-    SampleProfile* profile) {
+    SampleProfile* profile, const TraceTuning& tuning) {
   (void)width;
   (void)height;
   const uint32_t threads = tile_threads(rect);
   if (threads == 0) return;
   const bool count = profile && profile->visits;
   VisitCounters* visits = profile ? profile->visits : nullptr;
-  cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * 3 * (size_t)(max_bounces + 2), stream);
+  cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * kQueueCounterWords * (size_t)(max_bounces + 2), stream);
+  uint32_t* fetch = Q.counts + 3 * (size_t)(max_bounces + 2);
+  const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid_pixels = (threads + kBlock - 1) / kBlock;
   const uint32_t grid_queue = (Q.capacity + kBlock - 1) / kBlock;
+  const uint32_t grid_extend = persistent_grid(count ? k_wf_extend<true> : k_wf_extend<false>, Q.capacity, tuning);
+  const uint32_t grid_shadow = persistent_grid(count ? k_wf_shadow<true> : k_wf_shadow<false>, Q.capacity, tuning);
   {
     Timed t(profile, stream, 0);
     if (count) k_wf_camera<true><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, visits);
@@ -563,8 +655,10 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   for (uint32_t b = 0; b <= max_bounces; ++b) {
     if (b != 0) {
       Timed t(profile, stream, 1);
-      if (count) k_wf_extend<true><<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b, visits);
-      else k_wf_extend<false><<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b, nullptr);
+      if (count)
+        k_wf_extend<true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill, visits);
+      else
+        k_wf_extend<false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill, nullptr);
     }
     {
       Timed t(profile, stream, 2);
@@ -572,8 +666,10 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     }
     {
       Timed t(profile, stream, 3);
-      if (count) k_wf_shadow<true><<<grid_queue, kBlock, 0, stream>>>(S, P, Q, b, visits);
-      else k_wf_shadow<false><<<grid_queue, kBlock, 0, stream>>>(S, P, Q, b, nullptr);
+      if (count)
+        k_wf_shadow<true><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, visits);
+      else
+        k_wf_shadow<false><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, nullptr);
     }
   }
   {

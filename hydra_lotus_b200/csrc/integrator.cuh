@@ -29,13 +29,25 @@ struct ShadowQueue {
 
 // Per-bounce queue counters: [3 * b] rays entering bounce b's extension
 // (b = 0: camera rays), [3 * b + 1] hits shaded at bounce b, [3 * b + 2]
-// shadow rays from bounce b.
+// shadow rays from bounce b. After the 3 * (max_bounces + 2) counts come
+// the persistent kernels' fetch cursors, two per bounce (extension,
+// shadow): kQueueCounterWords words per bounce in all, cleared per sample.
+constexpr uint32_t kQueueCounterWords = 5;
+
 struct Queues {
   uint32_t* ray[2];
   uint32_t* hit;
   ShadowQueue shadow;
   uint32_t* counts;
   uint32_t capacity;
+};
+
+// Launch shape of the persistent tracing kernels: a lane takes a new ray
+// when fewer than `refill_below` lanes of its warp still hold one. Zero
+// picks the default.
+struct TraceTuning {
+  uint32_t refill_below = 0;
+  uint32_t blocks_per_sm = 0;  // 0: as many as fit
 };
 
 // Ray totals over a RenderScene call.
@@ -73,7 +85,7 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
-    SampleProfile* profile = nullptr);
+    SampleProfile* profile = nullptr, const TraceTuning& tuning = TraceTuning());
 
 void launch_advance(FrameConst* fc, cudaStream_t stream);
 

@@ -349,13 +349,16 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
 
 struct Renderer {
   int device = 0;
+  uint32_t bvh_leaf_size = 1;
+  TraceTuning tuning;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   std::string failure;
   uint64_t completion = 0;
 
   // Scene.
-  DeviceArray<BvhNode> blas, tlas;
+  DeviceArray<BvhNode> blas, tlas;      // binary builds (build scratch)
+  DeviceArray<Bvh4Node> blas4, tlas4;   // the 4-wide pools the traversal reads
   DeviceArray<float4> tris;
   DeviceArray<InstanceTraversal> inst_trav;
   DeviceArray<InstanceShading> inst_shade;
@@ -452,14 +455,14 @@ struct Renderer {
   }
 
   void release_scene() {
-    blas.release(); tlas.release(); tris.release(); inst_trav.release(); inst_shade.release();
+    blas.release(); tlas.release(); blas4.release(); tlas4.release(); tris.release(); inst_trav.release(); inst_shade.release();
     materials.release(); normals.release(); lights.release(); light_verts.release();
     light_radiance.release(); env_texels.release(); env_floats.release();
     scene_ready = false;
   }
 
   uint64_t scene_bytes() const {
-    return blas.bytes() + tlas.bytes() + tris.bytes() + inst_trav.bytes() + inst_shade.bytes() +
+    return blas.bytes() + tlas.bytes() + blas4.bytes() + tlas4.bytes() + tris.bytes() + inst_trav.bytes() + inst_shade.bytes() +
            materials.bytes() + normals.bytes() + lights.bytes() + light_verts.bytes() +
            light_radiance.bytes() + env_texels.bytes() + env_floats.bytes();
   }
@@ -568,10 +571,10 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
       normal_total += geo.triangle_count;
     }
   }
-  if (nodes >= 0x7FFFFFF0ull || tri_total >= 0x7FFFFFF0ull)
-    return fail("the scene exceeds 2^31 triangles");
+  if (nodes >= kMaxSceneTriangles || tri_total >= kMaxSceneTriangles)
+    return fail("the scene holds 2^28 triangles or more");
   if (!R.ok(R.blas.resize(std::max<uint64_t>(nodes, 1)), "BLAS pool", detail) ||
-      !R.ok(R.tris.resize(3 * std::max<uint64_t>(tri_total, 1)), "triangle pool", detail))
+      !R.ok(R.tris.resize(kTriStride * std::max<uint64_t>(tri_total, 1)), "triangle pool", detail))
     return fail(detail);
   // Staging: every geometry's positions and triangles in one upload.
   std::vector<float> h_pos(3 * vert_total);
@@ -608,7 +611,8 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
           geo.triangle_count, R.blas.ptr, node_base[g], R.tris.ptr, tri_base[g], st);
       if (!R.ok(e, "BLAS build", detail)) return fail(detail);
     }
-    if (!R.ok(R.builder.build_triangle_batch(d_pos.ptr, d_tri.ptr, batch, R.blas.ptr, R.tris.ptr, st),
+    if (!R.ok(R.builder.build_triangle_batch(d_pos.ptr, d_tri.ptr, batch, R.blas.ptr, R.tris.ptr, st,
+                  R.bvh_leaf_size),
             "BLAS build", detail))
       return fail(detail);
   }
@@ -702,6 +706,12 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
                       R.tlas.ptr, st),
             "TLAS build", detail))
     return fail(detail);
+  if (!R.ok(R.blas4.resize(R.blas.count), "BLAS pool", detail) ||
+      !R.ok(R.tlas4.resize(R.tlas.count), "TLAS", detail) ||
+      !R.ok(BvhBuilder::collapse(R.blas.ptr, (uint32_t)nodes, R.blas4.ptr, false, st), "BVH collapse", detail) ||
+      !R.ok(BvhBuilder::collapse(R.tlas.ptr, BvhBuilder::node_count(s.instance_count), R.tlas4.ptr, true, st),
+          "BVH collapse", detail))
+    return fail(detail);
   cudaEventRecord(R.ev_stop, st);
   if (!R.ok(cudaStreamSynchronize(st), "scene update", detail)) return fail(detail);
   float ms = 0.0f;
@@ -711,8 +721,8 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
 
   SceneView& v = R.view;
   v = SceneView{};
-  v.tlas = R.tlas.ptr;
-  v.blas = R.blas.ptr;
+  v.tlas = R.tlas4.ptr;
+  v.blas = R.blas4.ptr;
   v.tris = R.tris.ptr;
   v.inst_trav = R.inst_trav.ptr;
   v.inst_shade = R.inst_shade.ptr;
@@ -778,7 +788,7 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
     R.key_valid = false;
   }
   if (!R.ok(R.accum.resize(n), "accumulation", detail) || !R.ok(R.color.resize(n), "colour", detail) ||
-      !R.ok(R.counts.resize(3 * (LOTUS_MAX_BOUNCES + 2)), "queue counts", detail) ||
+      !R.ok(R.counts.resize(kQueueCounterWords * (LOTUS_MAX_BOUNCES + 2)), "queue counts", detail) ||
       !R.ok(R.frame_const.resize(1), "frame constants", detail) ||
       !R.ok(R.totals.resize(1), "ray totals", detail))
     return false;
@@ -936,7 +946,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     if (profiled) {
       if (wavefront)
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
-            R.accum.ptr, R.color.ptr, R.totals.ptr, s, &profile);
+            R.accum.ptr, R.color.ptr, R.totals.ptr, s, &profile, R.tuning);
       else
         launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s,
             &profile);
@@ -957,7 +967,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
         if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
           return poison(detail);
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
-            R.accum.ptr, R.color.ptr, R.totals.ptr, s);
+            R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, R.tuning);
         launch_advance(R.frame_const.ptr, s);
         if (!R.ok(cudaStreamEndCapture(s, &g), "graph capture", detail)) return poison(detail);
         cudaError_t e = cudaGraphInstantiate(&R.graph, g, 0);
@@ -1090,6 +1100,23 @@ int32_t lotus_cuda_create(const lotus_cuda_options* options, lotus_cuda_renderer
   }
   Renderer& R = h->r;
   R.device = device;
+  if (options && options->bvh_leaf_size) {
+    if (options->bvh_leaf_size > 8) {
+      copy_detail(error, error_size, "bvh_leaf_size must be in 1..8");
+      delete h;
+      return LOTUS_FAIL;
+    }
+    R.bvh_leaf_size = options->bvh_leaf_size;
+  }
+  if (options && (options->trace_refill_below > 32 || options->trace_blocks_per_sm > 64)) {
+    copy_detail(error, error_size, "trace_refill_below must be in 0..32 and trace_blocks_per_sm in 0..64");
+    delete h;
+    return LOTUS_FAIL;
+  }
+  if (options) {
+    R.tuning.refill_below = options->trace_refill_below;
+    R.tuning.blocks_per_sm = options->trace_blocks_per_sm;
+  }
   std::string detail;
   if (!R.ok(cudaSetDevice(device), "cudaSetDevice", detail) ||
       !R.ok(cudaStreamCreateWithFlags(&R.stream, cudaStreamNonBlocking), "stream", detail) ||
@@ -1196,6 +1223,7 @@ bool renderer_access(lotus_cuda_renderer* r, RendererAccess& out, std::string& d
   out.device = R.device;
   out.stream = R.stream;
   out.view = &R.view;
+  out.tuning = R.tuning;
   return true;
 }
 
@@ -1441,7 +1469,7 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   for (uint32_t k = 0; k < d.frame_count; ++k) {
     if (wavefront)
       launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
-          R.accum.ptr, R.color.ptr, R.totals.ptr, s);
+          R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, R.tuning);
     else
       launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s);
     launch_advance(R.frame_const.ptr, s);

@@ -13,6 +13,7 @@ struct RendererAccess {
   int device = 0;
   cudaStream_t stream = nullptr;
   const SceneView* view = nullptr;
+  TraceTuning tuning;
 };
 
 // The renderer's device, stream and resident scene; false (with the

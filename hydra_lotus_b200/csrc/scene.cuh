@@ -28,10 +28,30 @@ namespace lotus {
 // instance in the TLAS) with `count` primitives.
 constexpr int32_t kEmptyChild = 0x7FFFFFFF;
 constexpr int32_t kExitInstance = 0x7FFFFFFE;
-constexpr int kStackSize = 96;
+constexpr int kStackSize = 128;
 // A walk that visits more nodes than this ends early: only a corrupt BVH
 // could need it, and the bound keeps such a walk from spinning.
 constexpr uint32_t kMaxTraversalSteps = 1u << 18;
+
+// Triangle records are four float4 (64 bytes, cache-sector aligned): three
+// object-space corners, the primitive index in the first corner's w.
+constexpr int kTriStride = 4;
+// Bits of a BLAS leaf reference that hold its triangle count less one
+// (leaves hold 1..8 triangles); the rest hold the first triangle, so a
+// scene holds fewer than 2^28 triangles.
+constexpr uint32_t kLeafCountBits = 3;
+constexpr uint32_t kMaxSceneTriangles = 1u << 28;
+
+// The traversal's 4-wide node: four children's boxes by axis and bound
+// (component i is child i) and their references: a node index, or for a
+// BLAS leaf ~(first triangle << kLeafCountBits | count - 1), for a TLAS
+// leaf ~instance; `count` keeps the leaves' triangle counts. 128 bytes.
+struct alignas(16) Bvh4Node {
+  float4 lo_x, hi_x, lo_y, hi_y, lo_z, hi_z;
+  int4 child;
+  int4 count;
+};
+static_assert(sizeof(Bvh4Node) == 128, "4-wide node is 128 bytes");
 
 struct alignas(16) BvhNode {
   float4 x;   // child 0 low, child 0 high, child 1 low, child 1 high (x axis)
@@ -82,9 +102,9 @@ struct alignas(16) LightRecord {
 };
 
 struct SceneView {
-  const BvhNode* __restrict__ tlas;
-  const BvhNode* __restrict__ blas;
-  const float4* __restrict__ tris;          // 3 per leaf-ordered triangle
+  const Bvh4Node* __restrict__ tlas;
+  const Bvh4Node* __restrict__ blas;
+  const float4* __restrict__ tris;          // kTriStride per leaf-ordered triangle
   const InstanceTraversal* __restrict__ inst_trav;
   const InstanceShading* __restrict__ inst_shade;
   const MaterialRecord* __restrict__ materials;
@@ -186,27 +206,34 @@ __device__ __forceinline__ bool intersect_triangle(const WatertightRay& r, F3 v0
   return true;
 }
 
-// Slab test of a node's two children against [tmin, tmax]. The far
+// Slab tests of a 4-wide node's children against [tmin, tmax]. The far
 // distance gets a relative margin of 2^-18 (the clamp to tmax included), so
 // a box is never culled where the triangle test, whose distances carry
 // their own rounding, could still accept a hit: hits are decided by
 // triangle tests alone, whatever the BVH's shape.
-__device__ __forceinline__ void test_children(const BvhNode& n, F3 o, F3 inv, float tmin,
-    float tmax, bool& hit0, bool& hit1, float& near0, float& near1) {
-  const float x0 = (n.x.x - o.x) * inv.x, x1 = (n.x.y - o.x) * inv.x;
-  const float y0 = (n.y.x - o.y) * inv.y, y1 = (n.y.y - o.y) * inv.y;
-  const float z0 = (n.z.x - o.z) * inv.z, z1 = (n.z.y - o.z) * inv.z;
-  const float X0 = (n.x.z - o.x) * inv.x, X1 = (n.x.w - o.x) * inv.x;
-  const float Y0 = (n.y.z - o.y) * inv.y, Y1 = (n.y.w - o.y) * inv.y;
-  const float Z0 = (n.z.z - o.z) * inv.z, Z1 = (n.z.w - o.z) * inv.z;
-  const float tn0 = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
-  const float tf0 = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
-  const float tn1 = fmaxf(fmaxf(fminf(X0, X1), fminf(Y0, Y1)), fmaxf(fminf(Z0, Z1), tmin));
-  const float tf1 = fminf(fminf(fmaxf(X0, X1), fmaxf(Y0, Y1)), fminf(fmaxf(Z0, Z1), tmax));
-  hit0 = tn0 <= tf0 + fabsf(tf0) * 3.8146973e-6f && n.c.x != kEmptyChild;
-  hit1 = tn1 <= tf1 + fabsf(tf1) * 3.8146973e-6f && n.c.y != kEmptyChild;
-  near0 = tn0;
-  near1 = tn1;
+__device__ __forceinline__ float slab_near(float lo, float hi, float o, float inv, float& far) {
+  const float a = (lo - o) * inv, b = (hi - o) * inv;
+  far = fmaxf(a, b);
+  return fminf(a, b);
+}
+
+__device__ __forceinline__ void test_children4(const Bvh4Node& n, F3 o, F3 inv, float tmin, float tmax,
+    float tn[4], bool hit[4]) {
+  const float lx[4] = {n.lo_x.x, n.lo_x.y, n.lo_x.z, n.lo_x.w}, hx[4] = {n.hi_x.x, n.hi_x.y, n.hi_x.z, n.hi_x.w};
+  const float ly[4] = {n.lo_y.x, n.lo_y.y, n.lo_y.z, n.lo_y.w}, hy[4] = {n.hi_y.x, n.hi_y.y, n.hi_y.z, n.hi_y.w};
+  const float lz[4] = {n.lo_z.x, n.lo_z.y, n.lo_z.z, n.lo_z.w}, hz[4] = {n.hi_z.x, n.hi_z.y, n.hi_z.z, n.hi_z.w};
+  const int c[4] = {n.child.x, n.child.y, n.child.z, n.child.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    float fx, fy, fz;
+    const float nx = slab_near(lx[i], hx[i], o.x, inv.x, fx);
+    const float ny = slab_near(ly[i], hy[i], o.y, inv.y, fy);
+    const float nz = slab_near(lz[i], hz[i], o.z, inv.z, fz);
+    const float t0 = fmaxf(fmaxf(nx, ny), fmaxf(nz, tmin));
+    const float t1 = fminf(fminf(fx, fy), fminf(fz, tmax));
+    tn[i] = t0;
+    hit[i] = t0 <= t1 + fabsf(t1) * 3.8146973e-6f && c[i] != kEmptyChild;
+  }
 }
 
 __device__ __forceinline__ F3 row_point(const float4* r, F3 p) {
@@ -227,128 +254,237 @@ struct TraversalCounters {
   uint32_t instances;
 };
 
-// Walks the two-level BVH. kAnyHit: the shadow query of ShadowTransmittance
-// (scene.slang:445-460), returning the transmittance; otherwise the closest
-// accepted hit of Trace (scene.slang:424-439), whose coverage tests draw
-// from `rng`.
+// The traversal state of one ray over the two-level 4-wide BVH. Walks are
+// made of four kinds of work: an interior node's slab tests (its hit
+// children pushed nearest last, the nearest taken next), one BLAS leaf's
+// triangle tests, an instance's entry and the exit marker. kAnyHit walks
+// are the shadow query of ShadowTransmittance (scene.slang:445-460); the
+// others find the closest accepted hit of Trace (scene.slang:424-439), whose
+// coverage tests draw from the path's random state. TLAS leaves (one
+// instance each) go on the stack like nodes, and entering one pushes a
+// marker that restores the world-space ray when popped.
+struct Walk {
+  F3 origin, direction;  // the world-space ray
+  F3 inv;                // 1 / direction in the current space
+  WatertightRay w;       // the ray in the current space (w.org its origin)
+  float tmin, best, transmittance;
+  uint32_t instance, best_instance, best_prim, best_tri;
+  float b1, b2;
+  int32_t cur;           // the next reference to process, or kWalkDone
+  int32_t leaf;          // a postponed BLAS leaf, or 0
+  uint32_t steps;
+  int sp;
+  bool found, in_blas, opaque;
+};
+
+// The walk's stack lives beside it (a local array of kStackSize entries),
+// so that the walk's scalars stay in registers.
+typedef int32_t WalkStack[kStackSize];
+
+constexpr int32_t kWalkDone = 0x7FFFFFFD;
+
+__device__ __forceinline__ void walk_begin(const SceneView& S, Walk& W, F3 origin, F3 direction,
+    float tmin, float tmax) {
+  W.origin = origin;
+  W.direction = direction;
+  W.inv = safe_inverse(direction);
+  W.w.org = origin;
+  W.tmin = tmin;
+  W.best = tmax;
+  W.transmittance = 1.0f;
+  W.found = false;
+  W.in_blas = false;
+  W.opaque = true;
+  W.instance = 0;
+  W.sp = 0;
+  W.steps = 0;
+  W.leaf = 0;
+  W.cur = S.instance_count != 0 ? 0 : kWalkDone;
+}
+
+__device__ __forceinline__ Hit walk_hit(const Walk& W) {
+  Hit h;
+  h.instance = W.best_instance;
+  h.tri = W.best_tri;
+  h.primitive = W.best_prim;
+  h.b1 = W.b1;
+  h.b2 = W.b2;
+  h.t = W.best;
+  return h;
+}
+
+__device__ __forceinline__ bool walk_at_node(const Walk& W) { return W.cur >= 0 && W.cur < kWalkDone; }
+
+// The next reference from the stack, or kWalkDone (also once the walk has
+// used its 2^18 steps).
+__device__ __forceinline__ void walk_pop(Walk& W, const WalkStack& stack) {
+  W.cur = (W.sp > 0 && W.steps < kMaxTraversalSteps) ? stack[--W.sp] : kWalkDone;
+}
+
+// Slab tests of the node at W.cur. Its hit children go on the stack
+// (nearest last) and the nearest becomes W.cur; with none hit, W.cur is
+// popped.
+template <bool kCount>
+__device__ __forceinline__ void walk_visit_node(const SceneView& S, Walk& W, WalkStack& stack,
+    TraversalCounters* counters) {
+  const Bvh4Node n = W.in_blas ? S.blas[W.cur] : S.tlas[W.cur];
+  if (kCount) ++counters->nodes;
+  ++W.steps;
+  float tn[4];
+  bool h[4];
+  test_children4(n, W.w.org, W.inv, W.tmin, W.best, tn, h);
+  float key[4];
+  int32_t ref[4] = {n.child.x, n.child.y, n.child.z, n.child.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) key[i] = h[i] ? tn[i] : INFINITY;
+#define LOTUS_CSWAP(a, b)                                    \
+  if (key[b] < key[a]) {                                     \
+    const float tk = key[a]; key[a] = key[b]; key[b] = tk;   \
+    const int32_t tr = ref[a]; ref[a] = ref[b]; ref[b] = tr; \
+  }
+  LOTUS_CSWAP(0, 1) LOTUS_CSWAP(2, 3) LOTUS_CSWAP(0, 2) LOTUS_CSWAP(1, 3) LOTUS_CSWAP(1, 2)
+#undef LOTUS_CSWAP
+  if (key[0] == INFINITY) {
+    walk_pop(W, stack);
+    return;
+  }
+#pragma unroll
+  for (int i = 3; i >= 1; --i)
+    if (key[i] != INFINITY && W.sp < kStackSize) stack[W.sp++] = ref[i];
+  W.cur = W.steps < kMaxTraversalSteps ? ref[0] : kWalkDone;
+}
+
+// The triangle tests of BLAS leaf `leaf` (a negative reference). Returns
+// true when an any-hit walk has met an opaque surface.
+template <bool kAnyHit, bool kCount>
+__device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int32_t leaf, uint32_t& rng,
+    TraversalCounters* counters) {
+  const uint32_t code = ~(uint32_t)leaf;
+  const uint32_t first = code >> kLeafCountBits;
+  const uint32_t count = (code & ((1u << kLeafCountBits) - 1u)) + 1u;
+  ++W.steps;
+  for (uint32_t k = 0; k < count; ++k) {
+    const float4* tv = S.tris + kTriStride * (size_t)(first + k);
+    const float4 a = tv[0], b = tv[1], cc = tv[2];
+    if (kCount) ++counters->triangles;
+    float t, b1, b2;
+    if (!intersect_triangle(W.w, V(a), V(b), V(cc), t, b1, b2)) continue;
+    if (!(t >= W.tmin) || !(t <= W.best)) continue;
+    const uint32_t prim = __float_as_uint(a.w);
+    if (kAnyHit) {
+      const float coverage = W.opaque ? 1.0f : instance_coverage(S, W.instance);
+      if (coverage >= 1.0f) {
+        W.found = true;
+        W.transmittance = 0.0f;
+        return true;
+      }
+      if (coverage > 0.0f) W.transmittance *= 1.0f - coverage;
+    } else {
+      if (W.found && t == W.best &&
+          (W.instance > W.best_instance || (W.instance == W.best_instance && prim >= W.best_prim)))
+        continue;
+      if (!W.opaque) {
+        const float coverage = instance_coverage(S, W.instance);
+        if (coverage <= 0.0f) continue;
+        if (coverage < 1.0f && !(next_random(rng) < coverage)) continue;
+      }
+      W.found = true;
+      W.best = t;
+      W.best_instance = W.instance;
+      W.best_prim = prim;
+      W.best_tri = first + k;
+      W.b1 = b1;
+      W.b2 = b2;
+    }
+  }
+  return false;
+}
+
+// W.cur is not an interior node: the exit marker, a BLAS leaf (tested
+// here), or a TLAS leaf (entered). Leaves W.cur at the next reference.
+// Returns true when an any-hit walk has met an opaque surface.
+template <bool kAnyHit, bool kCount>
+__device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStack& stack, uint32_t& rng,
+    TraversalCounters* counters) {
+  const int32_t cur = W.cur;
+  if (cur == kExitInstance) {
+    W.in_blas = false;
+    W.w.org = W.origin;
+    W.inv = safe_inverse(W.direction);
+  } else if (W.in_blas) {
+    if (walk_test_leaf<kAnyHit, kCount>(S, W, cur, rng, counters)) return true;
+  } else {
+    const uint32_t instance = ~(uint32_t)cur;
+    if (kCount) ++counters->instances;
+    ++W.steps;
+    const InstanceTraversal rec = S.inst_trav[instance];
+    if (rec.blas_root != (uint32_t)kEmptyChild && W.sp < kStackSize) {
+      stack[W.sp++] = kExitInstance;
+      const F3 o = row_point(rec.inv, W.origin);
+      const F3 d = row_vector(rec.inv, W.direction);
+      W.inv = safe_inverse(d);
+      W.w = prepare_ray(o, d);
+      W.instance = instance;
+      W.opaque = (rec.flags & kInstanceOpaque) != 0;
+      W.in_blas = true;
+      W.cur = (int32_t)rec.blas_root;
+      return false;
+    }
+  }
+  walk_pop(W, stack);
+  return false;
+}
+
+// The whole walk in one call (for kernels with one ray per thread).
 template <bool kAnyHit, bool kCount>
 __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 direction, float tmin,
     float tmax, uint32_t& rng, Hit& hit, bool& found, TraversalCounters* counters = nullptr) {
-  found = false;
-  float best = tmax;
-  float transmittance = 1.0f;
-  uint32_t best_instance = 0, best_prim = 0;
-  int32_t stack[kStackSize];
-  int sp = 0;
-  F3 o = origin, d = direction;
-  F3 inv = safe_inverse(d);
-  WatertightRay w;
-  const BvhNode* __restrict__ pool = S.tlas;
-  uint32_t instance = 0;
-  bool instance_opaque = true;
-  int32_t cur = S.instance_count ? 0 : kEmptyChild;
-  int32_t count = 0;
-  if (cur == kEmptyChild) return kAnyHit ? 1.0f : 0.0f;
-  for (uint32_t steps = 0; steps < kMaxTraversalSteps; ++steps) {
-    if (cur >= 0 && cur != kExitInstance) {
-      const BvhNode n = pool[cur];
-      if (kCount) ++counters->nodes;
-      bool h0, h1;
-      float t0, t1;
-      test_children(n, o, inv, tmin, best, h0, h1, t0, t1);
-      if (h0 && h1) {
-        const bool first0 = t0 <= t1;
-        const int32_t near_c = first0 ? n.c.x : n.c.y;
-        const int32_t far_c = first0 ? n.c.y : n.c.x;
-        const int32_t near_n = first0 ? n.c.z : n.c.w;
-        const int32_t far_n = first0 ? n.c.w : n.c.z;
-        if (far_c < 0) {
-          // Leaves go on the stack with their count in the next slot.
-          if (sp + 2 <= kStackSize) {
-            stack[sp++] = far_n;
-            stack[sp++] = far_c;
-          }
-        } else if (sp < kStackSize) {
-          stack[sp++] = far_c;
-        }
-        cur = near_c;
-        count = near_n;
-        continue;
-      }
-      if (h0 || h1) {
-        cur = h0 ? n.c.x : n.c.y;
-        count = h0 ? n.c.z : n.c.w;
-        continue;
-      }
-    } else if (cur == kExitInstance) {
-      // Back in world space.
-      pool = S.tlas;
-      o = origin;
-      d = direction;
-      inv = safe_inverse(d);
-    } else if (pool == S.tlas) {
-      // A TLAS leaf: enter each instance in turn. The TLAS leaves hold one
-      // instance, so `count` is 1.
-      instance = (uint32_t)(~cur);
-      if (kCount) ++counters->instances;
-      const InstanceTraversal rec = S.inst_trav[instance];
-      if (rec.blas_root != (uint32_t)kEmptyChild && sp < kStackSize) {
-        stack[sp++] = kExitInstance;
-        o = row_point(rec.inv, origin);
-        d = row_vector(rec.inv, direction);
-        inv = safe_inverse(d);
-        w = prepare_ray(o, d);
-        instance_opaque = (rec.flags & kInstanceOpaque) != 0;
-        pool = S.blas;
-        cur = (int32_t)rec.blas_root;
-        count = 0;
-        continue;
-      }
-    } else {
-      // BLAS leaf: `count` triangles from ~cur.
-      const uint32_t first = (uint32_t)(~cur);
-      for (int32_t k = 0; k < count; ++k) {
-        const float4* tv = S.tris + 3 * (size_t)(first + k);
-        const float4 a = tv[0], b = tv[1], c = tv[2];
-        if (kCount) ++counters->triangles;
-        float t, b1, b2;
-        if (!intersect_triangle(w, V(a), V(b), V(c), t, b1, b2)) continue;
-        if (!(t >= tmin) || !(t <= best)) continue;
-        const uint32_t prim = __float_as_uint(a.w);
-        if (kAnyHit) {
-          const float coverage = instance_opaque ? 1.0f : instance_coverage(S, instance);
-          if (coverage >= 1.0f) {
-            found = true;
-            return 0.0f;
-          }
-          if (coverage > 0.0f) transmittance *= 1.0f - coverage;
-        } else {
-          if (found && t == best &&
-              (instance > best_instance || (instance == best_instance && prim >= best_prim)))
-            continue;
-          if (!instance_opaque) {
-            const float coverage = instance_coverage(S, instance);
-            if (coverage <= 0.0f) continue;
-            if (coverage < 1.0f && !(next_random(rng) < coverage)) continue;
-          }
-          found = true;
-          best = t;
-          best_instance = instance;
-          best_prim = prim;
-          hit.instance = instance;
-          hit.tri = first + k;
-          hit.primitive = prim;
-          hit.b1 = b1;
-          hit.b2 = b2;
-          hit.t = t;
-        }
+  Walk W;
+  WalkStack stack;
+  walk_begin(S, W, origin, direction, tmin, tmax);
+  while (W.cur != kWalkDone) {
+    if (walk_at_node(W)) {
+      walk_visit_node<kCount>(S, W, stack, counters);
+    } else if (walk_other<kAnyHit, kCount>(S, W, stack, rng, counters)) {
+      break;
+    }
+  }
+  found = W.found;
+  if (!kAnyHit && W.found) hit = walk_hit(W);
+  return kAnyHit ? W.transmittance : 0.0f;
+}
+
+// One round of a warp's walks (for persistent kernels; every lane of the
+// warp calls it, `active` lanes hold a walk). Interior nodes first, each
+// lane postponing the first BLAS leaf it meets and carrying on, until no
+// lane is left at an interior node; then every postponed leaf is tested,
+// and finally each lane's exit marker, further leaf or instance entry.
+// Each kind of work thus runs once per round over all the lanes that have
+// it. Returns true for a lane whose walk has ended.
+template <bool kAnyHit, bool kCount>
+__device__ __forceinline__ bool walk_round(const SceneView& S, Walk& W, WalkStack& stack, uint32_t& rng,
+    bool active, TraversalCounters* counters) {
+  constexpr unsigned kAll = 0xFFFFFFFFu;
+  for (;;) {
+    const bool node = active && walk_at_node(W);
+    if (!__any_sync(kAll, node)) break;
+    if (node) {
+      walk_visit_node<kCount>(S, W, stack, counters);
+      if (W.in_blas && W.cur < 0 && W.leaf == 0) {
+        W.leaf = W.cur;
+        walk_pop(W, stack);
       }
     }
-    if (sp == 0) break;
-    cur = stack[--sp];
-    if (cur < 0) count = stack[--sp];
   }
-  return kAnyHit ? transmittance : 0.0f;
+  bool ended = false;
+  const bool leaf = active && W.leaf != 0;
+  if (__any_sync(kAll, leaf) && leaf) {
+    ended = walk_test_leaf<kAnyHit, kCount>(S, W, W.leaf, rng, counters);
+    W.leaf = 0;
+  }
+  if (active && !ended && W.cur != kWalkDone)
+    ended = walk_other<kAnyHit, kCount>(S, W, stack, rng, counters);
+  return active && (ended || (W.cur == kWalkDone && W.leaf == 0));
 }
 
 template <bool kCount = false>

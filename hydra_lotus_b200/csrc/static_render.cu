@@ -43,7 +43,7 @@ constexpr size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign;
 constexpr size_t kFrameOffset = 0;
 constexpr size_t kTotalsOffset = kFrameOffset + align_up(sizeof(FrameConst));
 constexpr size_t kCountsOffset = kTotalsOffset + align_up(sizeof(RayTotals));
-constexpr size_t kCountsBytes = align_up(sizeof(uint32_t) * 3 * (LOTUS_MAX_BOUNCES + 2));
+constexpr size_t kCountsBytes = align_up(sizeof(uint32_t) * kQueueCounterWords * (LOTUS_MAX_BOUNCES + 2));
 constexpr size_t kAccumOffset = kCountsOffset + kCountsBytes;
 constexpr size_t kPathOffset = kAccumOffset + align_up(sizeof(double4) * kMaxPixels);
 constexpr size_t kPathSectionBytes = align_up(16 * kMaxPixels);
@@ -140,7 +140,7 @@ extern "C" int32_t lotus_cuda_render_static(lotus_cuda_renderer* renderer,
   for (uint32_t k = 0; k < frame->frame_count; ++k) {
     if (wavefront)
       launch_wavefront_sample(*access.view, d_frame, rect, t.width, t.height,
-          frame->settings.max_bounces, P, Q, accum, color, d_totals, s);
+          frame->settings.max_bounces, P, Q, accum, color, d_totals, s, nullptr, access.tuning);
     else
       launch_reference_pt(*access.view, d_frame, rect, accum, color, d_totals, s);
     launch_advance(d_frame, s);

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal_surface(SceneView S,
     if (trace_closest(S, ro, rd, 0.0f, tmax, rng, hit)) {
       const InstanceShading rec = S.inst_shade[hit.instance];
       const TemporalInstance id = identities[hit.instance];
-      const float4* tv = S.tris + 3 * (size_t)hit.tri;
+      const float4* tv = S.tris + kTriStride * (size_t)hit.tri;
       const F3 p0 = V(tv[0]), p1 = V(tv[1]), p2 = V(tv[2]);
       const F3 point = p0 + hit.b1 * (p1 - p0) + hit.b2 * (p2 - p0);
       const F3 world = row_point(rec.m, point);

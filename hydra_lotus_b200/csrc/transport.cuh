@@ -49,7 +49,7 @@ __device__ __forceinline__ F3 shading_normal(const float* n, float b1, float b2,
 __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32_t instance,
     uint32_t tri, float b1, float b2, F3 direction, uint32_t* primitive_out = nullptr) {
   const InstanceShading rec = S.inst_shade[instance];
-  const float4* tv = S.tris + 3 * (size_t)tri;
+  const float4* tv = S.tris + kTriStride * (size_t)tri;
   const float4 a = tv[0], b = tv[1], c = tv[2];
   const uint32_t primitive = __float_as_uint(a.w);
   if (primitive_out) *primitive_out = primitive;

@@ -211,8 +211,16 @@ typedef struct lotus_frame_result {
 } lotus_frame_result;
 
 typedef struct lotus_cuda_options {
-  int32_t device;     /* CUDA device ordinal */
-  uint32_t flags;     /* reserved, 0 */
+  int32_t device;          /* CUDA device ordinal */
+  uint32_t flags;          /* reserved, 0 */
+  uint32_t bvh_leaf_size;  /* most triangles per BLAS leaf, 1..8; 0: the default (1) */
+  /* Launch shape of the persistent extension and shadow kernels (0: the
+   * defaults): a warp's idle lanes take new rays when fewer than
+   * trace_refill_below (1..32) of its lanes still hold one, and at most
+   * trace_blocks_per_sm blocks run on each SM. */
+  uint32_t trace_refill_below;
+  uint32_t trace_blocks_per_sm;
+  uint32_t reserved;
 } lotus_cuda_options;
 
 typedef struct lotus_cuda_renderer lotus_cuda_renderer;
@@ -236,9 +244,11 @@ int32_t lotus_cuda_create(const lotus_cuda_options* options,
 void lotus_cuda_destroy(lotus_cuda_renderer* renderer);
 
 /* UpdateScene (vulkan_backend.hpp:816-817): replaces the resident scene.
- * Builds one LBVH per geometry and one over the instances on the device,
- * the light table and the environment distribution. Restarts the
- * accumulation. */
+ * Builds the BVHs on the device (binned SAH per geometry, all geometries in
+ * one launch, LBVH above 65,536 triangles; binned SAH or LBVH over the
+ * instances; each collapsed to a 4-wide BVH), the light table and the
+ * environment distribution. Restarts the accumulation. A scene holds fewer
+ * than 2^28 triangles. */
 int32_t lotus_cuda_update_scene(lotus_cuda_renderer* renderer,
     const lotus_scene_desc* scene, lotus_scene_result* result);
 
