@@ -381,6 +381,10 @@ __global__ void __launch_bounds__(kBlock) k_wf_shade(SceneView S,
 // The shadow rays of bounce `bounce`: ShadowTransmittance and the rest of
 // ShadowedLight, added to the path's radiance.
 constexpr unsigned kFullWarp = 0xFFFFFFFFu;
+// Resident blocks per SM the persistent tracing kernels are compiled for:
+// six blocks of 128 (80 registers a thread) hide more of the node loads'
+// latency than five at the registers the code would take unbounded.
+constexpr int kTraceBlocksPerSm = 6;
 constexpr uint32_t kDefaultRefillBelow = 24;
 
 // The persistent kernels' ray fetch: when fewer than `refill_below` lanes
@@ -406,7 +410,7 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor, uint32_t n, boo
 // as a persistent kernel: each lane walks one shadow ray at a time and adds
 // the light to the path's radiance when the ray arrives.
 template <bool kCount>
-__global__ void __launch_bounds__(kBlock) k_wf_shadow(SceneView S, PathState P, Queues Q,
+__global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_shadow(SceneView S, PathState P, Queues Q,
     uint32_t bounce, uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits) {
   const uint32_t n = Q.counts[3 * bounce + 2];
   TraversalCounters vc = {0, 0, 0};
@@ -458,7 +462,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_shadow(SceneView S, PathState P, 
 // stages its hits in shared memory and appends them to the hit queue 32 at
 // a time.
 template <bool kCount>
-__global__ void __launch_bounds__(kBlock) k_wf_extend(SceneView S,
+__global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce,
     uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits) {
   __shared__ uint32_t staged[kBlock / 32][64];
