@@ -207,8 +207,20 @@ class TemporalInstance(C.Structure):
 
 
 # The order lotus_cuda_struct_sizes reports them in.
+class CacheDesc(C.Structure):
+    """lotus_cache_desc: the learned radiance cache's settings."""
+    _fields_ = [("enable", C.c_uint32), ("levels", C.c_uint32), ("log2_table", C.c_uint32),
+                ("min_resolution", C.c_uint32), ("max_resolution", C.c_uint32),
+                ("training_stride", C.c_uint32), ("training_steps", C.c_uint32), ("seed", C.c_uint32),
+                ("learning_rate", C.c_float), ("reserved", C.c_uint32 * 3)]
+
+
+CACHE_INPUTS = 64
+CACHE_WEIGHTS = 21504
+
 STRUCTS = [Geometry, Instance, Material, Environment, SceneDesc, SceneResult,
-           Target, Settings, FrameDesc, FrameResult, Options, TemporalDesc, TemporalInstance]
+           Target, Settings, FrameDesc, FrameResult, Options, TemporalDesc, TemporalInstance,
+           CacheDesc]
 
 # TemporalValidationSettings' defaults (temporal.hpp:28-33).
 DEFAULT_VALIDATION = (0.01, 0.01, 0.9, 32.0)

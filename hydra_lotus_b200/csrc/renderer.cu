@@ -17,6 +17,7 @@
 #include "../../include/lotus_cuda.h"
 #include "bvh_build.cuh"
 #include "integrator.cuh"
+#include "radiance_cache.cuh"
 #include "renderer_internal.cuh"
 #include "temporal_passes.cuh"
 
@@ -430,6 +431,13 @@ struct Renderer {
     bool restir_ran = false, accumulate_ran = false, spatial_ran = false, filter_ran = false;
   } temporal;
   std::vector<lotus_instance> host_instances;
+  // World bounds of the resident scene (the radiance cache's grid box).
+  float scene_lo[3] = {0.0f, 0.0f, 0.0f}, scene_hi[3] = {1.0f, 1.0f, 1.0f};
+
+  // The learned radiance cache.
+  RadianceCache cache;
+  lotus_cache_desc cache_desc{};
+  bool cache_enabled = false;
 
   // The wavefront sample as a CUDA graph.
   cudaGraphExec_t graph = nullptr;
@@ -671,6 +679,38 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
   R.host_lights = table.records;
   R.host_light_offsets = table.offsets;
   R.host_instances.assign(s.instances, s.instances + s.instance_count);
+  // World bounds: each instance's geometry box through its transform.
+  {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    std::vector<std::array<float, 6>> boxes(s.geometry_count);
+    for (uint32_t g = 0; g < s.geometry_count; ++g) {
+      std::array<float, 6> b = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+      const lotus_geometry& geo = s.geometries[g];
+      for (uint32_t v = 0; v < geo.vertex_count; ++v)
+        for (int a = 0; a < 3; ++a) {
+          b[a] = std::min(b[a], geo.positions[3 * (size_t)v + a]);
+          b[3 + a] = std::max(b[3 + a], geo.positions[3 * (size_t)v + a]);
+        }
+      boxes[g] = b;
+    }
+    for (uint32_t i = 0; i < s.instance_count; ++i) {
+      const std::array<float, 6>& b = boxes[s.instances[i].geometry];
+      if (!(b[0] <= b[3])) continue;
+      const float* m = s.instances[i].world_from_object;
+      for (int c = 0; c < 8; ++c) {
+        const float p[3] = {(c & 1) ? b[3] : b[0], (c & 2) ? b[4] : b[1], (c & 4) ? b[5] : b[2]};
+        for (int a = 0; a < 3; ++a) {
+          const float w = m[a] * p[0] + m[4 + a] * p[1] + m[8 + a] * p[2] + m[12 + a];
+          lo[a] = std::min(lo[a], w);
+          hi[a] = std::max(hi[a], w);
+        }
+      }
+    }
+    for (int a = 0; a < 3; ++a) {
+      R.scene_lo[a] = std::isfinite(lo[a]) ? lo[a] : 0.0f;
+      R.scene_hi[a] = std::isfinite(hi[a]) ? hi[a] : 1.0f;
+    }
+  }
   // Instances.
   std::vector<InstanceTraversal> h_trav(s.instance_count);
   std::vector<InstanceShading> h_shade(s.instance_count);
@@ -1060,7 +1100,7 @@ uint32_t lotus_cuda_struct_sizes(uint64_t* sizes, uint32_t capacity) {
       sizeof(lotus_environment), sizeof(lotus_scene_desc), sizeof(lotus_scene_result),
       sizeof(lotus_target), sizeof(lotus_settings), sizeof(lotus_frame_desc),
       sizeof(lotus_frame_result), sizeof(lotus_cuda_options), sizeof(lotus_temporal_desc),
-      sizeof(lotus_temporal_instance)};
+      sizeof(lotus_temporal_instance), sizeof(lotus_cache_desc)};
   const uint32_t n = sizeof(s) / sizeof(s[0]);
   for (uint32_t i = 0; i < n && i < capacity; ++i) sizes[i] = s[i];
   return n;
@@ -1616,3 +1656,96 @@ int64_t lotus_cuda_read_product(lotus_cuda_renderer* r, uint32_t product, void* 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The learned radiance cache.
+
+namespace {
+
+Renderer* cache_renderer(lotus_cuda_renderer* h, bool need_cache) {
+  if (!h || !h->r.failure.empty()) return nullptr;
+  if (need_cache && !h->r.cache.ready()) return nullptr;
+  cudaSetDevice(h->r.device);
+  return &h->r;
+}
+
+}  // namespace
+
+extern "C" int32_t lotus_cuda_configure_cache(lotus_cuda_renderer* h, const lotus_cache_desc* d, char* detail,
+    size_t detail_size) {
+  Renderer* R = cache_renderer(h, false);
+  if (!R || !d) {
+    copy_detail(detail, detail_size, !d ? "no cache description" : "the renderer has failed");
+    return LOTUS_FAIL;
+  }
+  CacheConfig c;
+  c.levels = d->levels ? d->levels : 16u;
+  c.log2_size = d->log2_table ? d->log2_table : 19u;
+  c.min_resolution = d->min_resolution ? d->min_resolution : 16u;
+  c.max_resolution = d->max_resolution ? d->max_resolution : 2048u;
+  c.learning_rate = d->learning_rate > 0.0f ? d->learning_rate : 1e-2f;
+  c.seed = d->seed;
+  if (c.levels > (uint32_t)kCacheMaxLevels || c.log2_size < 10 || c.log2_size > 22 || c.min_resolution < 2 ||
+      c.max_resolution < c.min_resolution || !std::isfinite(c.learning_rate)) {
+    copy_detail(detail, detail_size, "cache settings out of range (levels 1..16, log2_table 10..22, "
+        "2 <= min_resolution <= max_resolution)");
+    return LOTUS_FAIL;
+  }
+  cudaError_t e = R->cache.configure(c, R->scene_lo, R->scene_hi, R->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(R->stream);
+  if (e != cudaSuccess) {
+    copy_detail(detail, detail_size, std::string("cache set-up: ") + cudaGetErrorString(e));
+    R->cache.release();
+    return LOTUS_FAIL;
+  }
+  R->cache_desc = *d;
+  R->cache_enabled = d->enable != 0;
+  R->key_valid = false;
+  R->graph_key = Renderer::GraphKey{};
+  return LOTUS_PASS;
+}
+
+extern "C" int32_t lotus_cuda_cache_weights(lotus_cuda_renderer* h, float* weights, uint64_t count, int32_t write) {
+  Renderer* R = cache_renderer(h, true);
+  if (!R || !weights || count != kCacheWeights) return LOTUS_FAIL;
+  const cudaError_t e = write ? R->cache.write_weights(weights, R->stream) : R->cache.read_weights(weights, R->stream);
+  if (write) R->key_valid = false;
+  return e == cudaSuccess ? LOTUS_PASS : LOTUS_FAIL;
+}
+
+extern "C" int32_t lotus_cuda_cache_infer(lotus_cuda_renderer* h, const float* inputs, uint32_t n, float* outputs) {
+  Renderer* R = cache_renderer(h, true);
+  if (!R || !inputs || !outputs) return LOTUS_FAIL;
+  if (n == 0) return LOTUS_PASS;
+  const cudaError_t e = R->cache.infer_encoded(inputs, n, outputs, R->stream);
+  return e == cudaSuccess && R->cache.error_flag(R->stream) == 0 ? LOTUS_PASS : LOTUS_FAIL;
+}
+
+extern "C" int32_t lotus_cuda_cache_gradient(lotus_cuda_renderer* h, const float* inputs, const float* targets,
+    uint32_t n, float* weight_grad, float* input_grad, float* loss) {
+  Renderer* R = cache_renderer(h, true);
+  if (!R || !inputs || !targets) return LOTUS_FAIL;
+  if (n == 0) return LOTUS_PASS;
+  const cudaError_t e = R->cache.gradient_encoded(inputs, targets, n, weight_grad, input_grad, loss, R->stream);
+  return e == cudaSuccess && R->cache.error_flag(R->stream) == 0 ? LOTUS_PASS : LOTUS_FAIL;
+}
+
+extern "C" int32_t lotus_cuda_cache_encode(lotus_cuda_renderer* h, const float* records, uint32_t n, float* inputs) {
+  Renderer* R = cache_renderer(h, true);
+  if (!R || !records || !inputs) return LOTUS_FAIL;
+  if (n == 0) return LOTUS_PASS;
+  const cudaError_t e =
+      R->cache.encode(reinterpret_cast<const CacheRecord*>(records), n, inputs, R->stream);
+  return e == cudaSuccess ? LOTUS_PASS : LOTUS_FAIL;
+}
+
+extern "C" int32_t lotus_cuda_cache_train(lotus_cuda_renderer* h, const float* records, const float* targets,
+    uint32_t n, uint32_t steps, float* losses) {
+  Renderer* R = cache_renderer(h, true);
+  if (!R || !records || !targets) return LOTUS_FAIL;
+  if (n == 0 || steps == 0) return LOTUS_PASS;
+  const cudaError_t e = R->cache.train_records(reinterpret_cast<const CacheRecord*>(records), targets, n, steps,
+      losses, R->stream);
+  R->key_valid = false;
+  return e == cudaSuccess && R->cache.error_flag(R->stream) == 0 ? LOTUS_PASS : LOTUS_FAIL;
+}

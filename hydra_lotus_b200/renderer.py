@@ -62,6 +62,21 @@ def lib():
                                                  C.POINTER(abi.FrameResult), C.c_void_p]
         L.lotus_cuda_read_product.restype = C.c_int64
         L.lotus_cuda_read_product.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64]
+        L.lotus_cuda_configure_cache.restype = C.c_int32
+        L.lotus_cuda_configure_cache.argtypes = [C.c_void_p, C.POINTER(abi.CacheDesc), C.c_char_p,
+                                                 C.c_size_t]
+        L.lotus_cuda_cache_weights.restype = C.c_int32
+        L.lotus_cuda_cache_weights.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32]
+        L.lotus_cuda_cache_infer.restype = C.c_int32
+        L.lotus_cuda_cache_infer.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        L.lotus_cuda_cache_gradient.restype = C.c_int32
+        L.lotus_cuda_cache_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                                C.c_void_p, C.c_void_p, C.c_void_p]
+        L.lotus_cuda_cache_encode.restype = C.c_int32
+        L.lotus_cuda_cache_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        L.lotus_cuda_cache_train.restype = C.c_int32
+        L.lotus_cuda_cache_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                             C.c_void_p]
         L.lotus_cuda_read_light_table.restype = C.c_int64
         L.lotus_cuda_read_light_table.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64,
                                                   C.c_void_p, C.c_uint64]
@@ -186,6 +201,69 @@ class CudaOffscreenRenderer:
         if rc != abi.PASS:
             raise RendererError(rc, "read_color failed")
         return out
+
+    # --- the learned radiance cache -------------------------------------
+
+    def configure_cache(self, enable=True, **fields):
+        """lotus_cuda_configure_cache: fresh weights over the resident
+        scene's bounds; `fields` are lotus_cache_desc members."""
+        d = abi.CacheDesc(enable=1 if enable else 0, **fields)
+        err = C.create_string_buffer(256)
+        rc = lib().lotus_cuda_configure_cache(self.handle, C.byref(d), err, 256)
+        if rc != abi.PASS:
+            raise RendererError(rc, err.value.decode(errors="replace"))
+
+    def cache_weights(self, weights=None):
+        """Reads the cache's FP32 weights, or writes `weights`."""
+        if weights is None:
+            w = np.zeros(abi.CACHE_WEIGHTS, dtype=np.float32)
+            rc = lib().lotus_cuda_cache_weights(self.handle, w.ctypes.data, w.size, 0)
+        else:
+            w = np.ascontiguousarray(weights, dtype=np.float32).ravel()
+            rc = lib().lotus_cuda_cache_weights(self.handle, w.ctypes.data, w.size, 1)
+        if rc != abi.PASS:
+            raise RendererError(rc, "cache weights")
+        return w
+
+    def cache_infer(self, inputs):
+        x = np.ascontiguousarray(inputs, dtype=np.float32)
+        out = np.zeros((x.shape[0], 3), dtype=np.float32)
+        rc = lib().lotus_cuda_cache_infer(self.handle, x.ctypes.data, x.shape[0], out.ctypes.data)
+        if rc != abi.PASS:
+            raise RendererError(rc, "cache inference")
+        return out
+
+    def cache_gradient(self, inputs, targets):
+        """(weight gradients, input gradients, loss) of the relative L2 loss."""
+        x = np.ascontiguousarray(inputs, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        gw = np.zeros(abi.CACHE_WEIGHTS, dtype=np.float32)
+        gx = np.zeros_like(x)
+        loss = np.zeros(1, dtype=np.float32)
+        rc = lib().lotus_cuda_cache_gradient(self.handle, x.ctypes.data, t.ctypes.data, x.shape[0],
+                                             gw.ctypes.data, gx.ctypes.data, loss.ctypes.data)
+        if rc != abi.PASS:
+            raise RendererError(rc, "cache gradient")
+        return gw, gx, float(loss[0])
+
+    def cache_encode(self, records):
+        r = np.ascontiguousarray(records, dtype=np.float32)
+        out = np.zeros((r.shape[0], abi.CACHE_INPUTS), dtype=np.float32)
+        rc = lib().lotus_cuda_cache_encode(self.handle, r.ctypes.data, r.shape[0], out.ctypes.data)
+        if rc != abi.PASS:
+            raise RendererError(rc, "cache encode")
+        return out
+
+    def cache_train(self, records, targets, steps):
+        """Trains on raw records; returns the loss before each step."""
+        r = np.ascontiguousarray(records, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        losses = np.zeros(steps, dtype=np.float32)
+        rc = lib().lotus_cuda_cache_train(self.handle, r.ctypes.data, t.ctypes.data, r.shape[0], steps,
+                                          losses.ctypes.data)
+        if rc != abi.PASS:
+            raise RendererError(rc, "cache training")
+        return losses
 
     def light_table(self):
         n = lib().lotus_cuda_read_light_table(self.handle, None, 0, None, 0)

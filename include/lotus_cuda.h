@@ -369,6 +369,69 @@ int64_t lotus_cuda_read_light_table(lotus_cuda_renderer* renderer,
 int32_t lotus_cuda_render_static(lotus_cuda_renderer* renderer,
     const lotus_frame_desc* frame, float* color_device, lotus_frame_result* result);
 
+/* ------------------------------------------------------------------------
+ * Learned radiance cache. No counterpart in the reference: a hash-grid
+ * encoded MLP (five 64-wide ReLU layers, RGB out; BF16 on the tensor cores,
+ * FP32 accumulation) trained online on the wavefront path tracer's own
+ * radiance. With the cache enabled, wavefront paths end into it at their
+ * second vertex, except one path in `training_stride`, which is traced in
+ * full and trains it. */
+
+#define LOTUS_CACHE_INPUTS 64u
+#define LOTUS_CACHE_WEIGHTS 21504u  /* 5 x 64 x 64 + 64 x 16 FP32 */
+
+typedef struct lotus_cache_desc {
+  uint32_t enable;           /* 1: paths end into the cache; 0: plain PT */
+  uint32_t levels;           /* hash-grid levels, 1..16 (0: 16) */
+  uint32_t log2_table;       /* entries per level, log2, 10..22 (0: 19) */
+  uint32_t min_resolution;   /* coarsest grid resolution (0: 16) */
+  uint32_t max_resolution;   /* finest grid resolution (0: 2048) */
+  uint32_t training_stride;  /* one path in this many trains the cache (0: 32) */
+  uint32_t training_steps;   /* Adam steps per sample (0: 1) */
+  uint32_t seed;             /* weight and grid initialisation */
+  float learning_rate;       /* Adam step size (0: 1e-2) */
+  uint32_t reserved[3];
+} lotus_cache_desc;
+
+/* (Re)creates the cache over the resident scene's bounds (a unit box
+ * without a scene) with fresh weights, and sets whether RenderScene's
+ * wavefront samples use it. Restarts the accumulation. */
+int32_t lotus_cuda_configure_cache(lotus_cuda_renderer* renderer,
+    const lotus_cache_desc* desc, char* detail, size_t detail_size);
+
+/* The network's FP32 weights (LOTUS_CACHE_WEIGHTS floats; layer l < 5 is
+ * W[in][out] 64 x 64, layer 5 is 64 x 16 with RGB in its first three
+ * columns): read (write == 0) or replaced (write != 0). */
+int32_t lotus_cuda_cache_weights(lotus_cuda_renderer* renderer, float* weights,
+    uint64_t count, int32_t write);
+
+/* Network outputs (n x 3, host memory) for encoded inputs (n x 64). */
+int32_t lotus_cuda_cache_infer(lotus_cuda_renderer* renderer,
+    const float* inputs, uint32_t n, float* outputs);
+
+/* Gradients of the relative L2 loss sum_s,c (y - t)^2 / (y^2 + 0.01), the
+ * denominator held constant, over encoded inputs (n x 64) and targets
+ * (n x 3): weight gradients (LOTUS_CACHE_WEIGHTS), input gradients
+ * (n x 64) and the loss. Any output may be NULL. Leaves the weights as
+ * they are. */
+int32_t lotus_cuda_cache_gradient(lotus_cuda_renderer* renderer,
+    const float* inputs, const float* targets, uint32_t n, float* weight_grad,
+    float* input_grad, float* loss);
+
+/* The network inputs (n x 64) of raw records (n x 16 floats: position,
+ * roughness; direction, 0; normal, 0; albedo, 0). */
+int32_t lotus_cuda_cache_encode(lotus_cuda_renderer* renderer,
+    const float* records, uint32_t n, float* inputs);
+
+/* `steps` training steps on raw records (n x 16 floats, as above) and RGB
+ * targets (n x 3): each runs the training pass over all n records (the
+ * gradients of the relative L2 loss reaching the weights and the hash
+ * grid) and one Adam step. losses[k] (if not NULL) is the summed loss
+ * before step k. */
+int32_t lotus_cuda_cache_train(lotus_cuda_renderer* renderer,
+    const float* records, const float* targets, uint32_t n, uint32_t steps,
+    float* losses);
+
 #ifdef __cplusplus
 }
 #endif

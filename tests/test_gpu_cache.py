@@ -1,0 +1,112 @@
+"""GPU checks of the learned radiance cache's network through the C ABI:
+the tensor-core forward and backward passes against the FP64 oracle
+(oracle/cache_oracle.py) on the same BF16-rounded operands, the query
+encoding, and training with Adam on a known function."""
+
+import numpy as np
+import pytest
+
+from hydra_lotus_b200 import scenes
+from oracle import cache_oracle
+
+pytestmark = pytest.mark.gpu
+
+# The kernels accumulate in FP32 where the oracle uses FP64; a sum that
+# lands near a BF16 rounding boundary can round to the neighbouring BF16
+# value (2^-8 relative) and carry that to the outputs. Outputs must agree to
+# 2% of the outputs' RMS per element, gradients to 3% in norm per layer.
+OUTPUT_TOL = 2e-2
+GRAD_TOL = 3e-2
+
+
+def random_weights(rng):
+    w = []
+    for l in range(6):
+        outs = 64 if l < 5 else 16
+        limit = np.sqrt(6.0 / (64 + outs))
+        w.append(rng.uniform(-limit, limit, size=(64, outs)))
+    return np.concatenate([m.ravel() for m in w]).astype(np.float32)
+
+
+@pytest.fixture(scope="module")
+def cache_renderer(cuda):
+    scene = scenes.box_room(seed=0, size=32)
+    r = cuda.CudaOffscreenRenderer(0)
+    cuda.check(r.update_scene(scene), "update_scene")
+    r.configure_cache(enable=False, seed=7)
+    yield r
+    r.close()
+
+
+def test_forward_matches_oracle(cache_renderer):
+    rng = np.random.default_rng(1)
+    w = random_weights(rng)
+    cache_renderer.cache_weights(w)
+    assert np.array_equal(cache_renderer.cache_weights(), w)
+    x = rng.uniform(-1.0, 1.0, size=(1000, 64)).astype(np.float32)  # a partial last tile
+    y = cache_renderer.cache_infer(x)
+    ref = cache_oracle.infer(w, x)
+    scale = np.sqrt(np.mean(ref ** 2))
+    assert scale > 1e-2
+    err = np.abs(y - ref).max() / scale
+    assert err < OUTPUT_TOL, f"max error {err:.3g} of the output RMS"
+
+
+def test_gradients_match_oracle(cache_renderer):
+    rng = np.random.default_rng(2)
+    w = random_weights(rng)
+    cache_renderer.cache_weights(w)
+    n = 777
+    x = rng.uniform(-1.0, 1.0, size=(n, 64)).astype(np.float32)
+    t = rng.uniform(0.0, 2.0, size=(n, 3)).astype(np.float32)
+    gw, gx, loss = cache_renderer.cache_gradient(x, t)
+    rw, rx, rloss = cache_oracle.gradients(w, x, t)
+    assert abs(loss - rloss) <= 1e-2 * rloss
+    offsets = [0, 4096, 8192, 12288, 16384, 20480, 21504]
+    for l in range(6):
+        a, b = gw[offsets[l]:offsets[l + 1]], rw[offsets[l]:offsets[l + 1]]
+        if l == 5:  # only the three RGB columns carry gradient
+            a, b = a.reshape(64, 16)[:, :3], b.reshape(64, 16)[:, :3]
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert rel < GRAD_TOL, f"layer {l}: weight-gradient error {rel:.3g}"
+    rel = np.linalg.norm(gx - rx) / np.linalg.norm(rx)
+    assert rel < GRAD_TOL, f"input-gradient error {rel:.3g}"
+    # The weights are left as they were.
+    assert np.array_equal(cache_renderer.cache_weights(), w)
+
+
+def records_in_box(rng, n, lo, hi):
+    r = np.zeros((n, 16), dtype=np.float32)
+    r[:, 0:3] = rng.uniform(lo, hi, size=(n, 3))
+    r[:, 3] = rng.uniform(0.0, 1.0, size=n)
+    d = rng.normal(size=(n, 3))
+    r[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    nrm = rng.normal(size=(n, 3))
+    r[:, 8:11] = nrm / np.linalg.norm(nrm, axis=1, keepdims=True)
+    r[:, 12:15] = rng.uniform(0.0, 1.0, size=(n, 3))
+    return r
+
+
+def test_encoding(cache_renderer):
+    rng = np.random.default_rng(3)
+    rec = records_in_box(rng, 500, -1.0, 1.0)
+    x = cache_renderer.cache_encode(rec)
+    assert np.allclose(x[:, 32:], cache_oracle.encode_direct(rec), rtol=1e-5, atol=1e-6)
+    # Fresh grid features are uniform in +-1e-4; interpolation keeps them so.
+    assert np.abs(x[:, :32]).max() <= 1e-4 * 1.001
+    assert np.abs(x[:, :32]).max() > 0.0
+
+
+def test_training_fits_a_function(cuda):
+    scene = scenes.box_room(seed=0, size=32)
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        r.configure_cache(enable=False, seed=3, log2_table=16)
+        rng = np.random.default_rng(4)
+        rec = records_in_box(rng, 8192, 0.0, 1.0)
+        p = rec[:, 0:3]
+        target = np.stack([1.0 + np.sin(4.0 * p[:, 0]), 1.0 + p[:, 1] * p[:, 2], 0.5 + 0.5 * np.cos(3.0 * p[:, 2])],
+                          axis=1).astype(np.float32)
+        losses = r.cache_train(rec, target, 200)
+        assert np.all(np.isfinite(losses))
+        assert losses[-1] < 0.05 * losses[0], f"loss {losses[0]:.4g} -> {losses[-1]:.4g}"
