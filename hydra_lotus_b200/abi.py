@@ -170,6 +170,9 @@ class FrameResult(C.Structure):
         ("node_visits", C.c_uint64 * 3),
         ("triangle_visits", C.c_uint64 * 3),
         ("instance_visits", C.c_uint64 * 3),
+        ("cache_gpu_ms", C.c_double),
+        ("cache_queries", C.c_uint32),
+        ("cache_training_records", C.c_uint32),
         ("detail", C.c_char * 256),
     ]
 

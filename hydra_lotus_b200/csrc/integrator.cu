@@ -11,6 +11,9 @@
 // radiance before the next extension reads it, so the radiance sums run in
 // the reference's order.
 #include <algorithm>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include "integrator.cuh"
 #include "temporal.cuh"
@@ -77,10 +80,20 @@ struct ShadowRequest {
 __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     uint32_t instance, uint32_t tri, float b1, float b2, F3 ray_o, F3 ray_d, uint32_t depth,
     F3& T, F3& R, float& last_pdf, uint32_t& flags, uint32_t& rng, F3& new_o, F3& new_d,
-    ShadowRequest& req, uint32_t pixel_index) {
+    ShadowRequest& req, uint32_t pixel_index, CacheRecord* features = nullptr, bool end_here = false) {
   req.pending = false;
   uint32_t primitive;
   const SurfaceHit sh = reconstruct_hit(S, instance, tri, b1, b2, ray_d, &primitive);
+  if (features) {
+    // The radiance cache's description of this vertex, seen from the ray.
+    const F3 albedo = sh.bsdf.transmission > 0.0f
+        ? sh.base_color + sh.bsdf.transmission * (sh.bsdf.transmission_color - sh.base_color)
+        : sh.base_color;
+    features->pos_rough = F4(sh.position, sh.roughness);
+    features->dir = F4(-ray_d, 0.0f);
+    features->normal = F4(sh.shading_normal, 0.0f);
+    features->albedo = F4(albedo, sh.metallic);
+  }
   const bool weigh = f.sample_lights && (flags & kUnweightedLight) == 0;
   F3 emission = sh.emission;
   if (weigh && depth != 0 && max_component(emission) > 0.0f) {
@@ -95,7 +108,9 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     emission = emission * w;
   }
   R = R + T * emission;
-  if (depth >= f.max_bounces) return false;
+  // A path that ends into the radiance cache stops after the emission: the
+  // cache stands for everything scattered from here on.
+  if (depth >= f.max_bounces || end_here) return false;
   if (depth >= kRouletteBounces) {
     const float survival = fminf(max_component(T), kMaxSurvival);
     if (next_random(rng) >= survival) return false;
@@ -325,61 +340,105 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
 }
 
 // Shade (wavefront.slang:264-285) with next event estimation's shadow ray
-// deferred to the shadow queue.
+// deferred to the shadow queue. With the radiance cache, the paths reaching
+// their second vertex (bounce 1) end into the cache there (a query of the
+// cache records the vertex and the path's throughput), except the training
+// paths, one in `stride` chosen per sample, which record the vertex, their
+// throughput and radiance so far and carry on.
 __global__ void __launch_bounds__(kBlock) k_wf_shade(SceneView S,
-    const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce) {
+    const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C) {
   const uint32_t n = Q.counts[3 * bounce + 1];
-  if (blockIdx.x * blockDim.x >= n) return;
   const FrameConst& f = *fcp;
-  const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = index < n;
-  bool cont = false;
-  ShadowRequest req;
-  req.pending = false;
-  uint32_t slot = 0;
-  if (valid) {
-    slot = Q.hit[index];
-    const float4 dir = P.direction[slot];
-    const float4 rad = P.radiance[slot];
-    const uint4 h = P.hit[slot];
-    F3 T = V(1.0f);
-    float last_pdf = 0.0f;
-    uint32_t flags = 0;
-    F3 ro = V(0.0f);
-    if (bounce != 0) {
-      const float4 thr = P.throughput[slot];
-      T = V(thr);
-      last_pdf = thr.w;
-      flags = last_pdf < 0.0f ? kUnweightedLight : 0u;
-      if (f.sample_lights) ro = V(P.origin[slot]);
+  const bool cache_vertex = C.enabled && bounce == 1 && bounce < f.max_bounces;
+  // Grid-stride over the hit queue (the grid is sized to the SMs, not to
+  // the largest queue, so that the short queues of late bounces cost
+  // little).
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t index = base + threadIdx.x;
+    const bool valid = index < n;
+    bool cont = false, query = false, training = false;
+    ShadowRequest req;
+    req.pending = false;
+    uint32_t slot = 0;
+    CacheRecord features;
+    F3 T = V(1.0f), T_in = V(1.0f), R = V(0.0f);
+    if (valid) {
+      slot = Q.hit[index];
+      const float4 dir = P.direction[slot];
+      const float4 rad = P.radiance[slot];
+      const uint4 h = P.hit[slot];
+      float last_pdf = 0.0f;
+      uint32_t flags = 0;
+      F3 ro = V(0.0f);
+      if (bounce != 0) {
+        const float4 thr = P.throughput[slot];
+        T = V(thr);
+        last_pdf = thr.w;
+        flags = last_pdf < 0.0f ? kUnweightedLight : 0u;
+        if (f.sample_lights) ro = V(P.origin[slot]);
+      }
+      T_in = T;
+      R = V(rad);
+      uint32_t rng = __float_as_uint(rad.w);
+      if (cache_vertex)
+        training = pcg_hash(slot ^ pcg_hash(f.sample_index ^ 0xC2B2AE35u)) % C.stride == 0u;
+      F3 no, nd;
+      cont = scatter(S, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
+          T, R, last_pdf, flags, rng, no, nd, req, slot, cache_vertex ? &features : nullptr,
+          cache_vertex && !training);
+      query = cache_vertex && !training;
+      if (cont) {
+        P.origin[slot] = F4(no, 0.0f);
+        P.direction[slot] = F4(nd, kFloatMax);
+        P.throughput[slot] = F4(T, (flags & kUnweightedLight) ? -1.0f : last_pdf);
+        P.radiance[slot] = F4(R, __uint_as_float(rng));
+      } else {
+        P.radiance[slot] = F4(R, 1.0f);
+      }
     }
-    F3 R = V(rad);
-    uint32_t rng = __float_as_uint(rad.w);
-    F3 no, nd;
-    cont = scatter(S, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
-        T, R, last_pdf, flags, rng, no, nd, req, slot);
-    if (cont) {
-      P.origin[slot] = F4(no, 0.0f);
-      P.direction[slot] = F4(nd, kFloatMax);
-      P.throughput[slot] = F4(T, (flags & kUnweightedLight) ? -1.0f : last_pdf);
-      P.radiance[slot] = F4(R, __uint_as_float(rng));
-    } else {
-      P.radiance[slot] = F4(R, 1.0f);
+    if (cache_vertex) {
+      const uint32_t q_at = warp_append(&C.counters[0], query);
+      if (query && q_at < C.query_capacity) {
+        C.queries[q_at] = features;
+        C.query_slots[q_at] = slot;
+        C.query_throughput[q_at] = F4(T_in, 0.0f);
+      }
+      const uint32_t t_at = warp_append(&C.counters[1], training);
+      if (training && t_at < C.train_capacity) {
+        C.train[t_at] = features;
+        C.train_slots[t_at] = slot;
+        C.train_base[t_at] = F4(R, 0.0f);
+        C.train_throughput[t_at] = F4(T_in, 0.0f);
+      }
     }
-  }
-  const uint32_t ray_at = warp_append(&Q.counts[3 * (bounce + 1)], cont);
-  if (cont) Q.ray[(bounce + 1) & 1][ray_at] = slot;
-  const uint32_t sh_at = warp_append(&Q.counts[3 * bounce + 2], req.pending);
-  if (req.pending) {
-    Q.shadow.ray_o[sh_at] = F4(req.origin, req.tmax);
-    Q.shadow.ray_d[sh_at] = F4(req.direction, req.weight);
-    Q.shadow.fl[sh_at] = F4(req.fl, req.pdf);
-    Q.shadow.thr[sh_at] = F4(req.throughput, __uint_as_float(slot));
+    const uint32_t ray_at = warp_append(&Q.counts[3 * (bounce + 1)], cont);
+    if (cont) Q.ray[(bounce + 1) & 1][ray_at] = slot;
+    const uint32_t sh_at = warp_append(&Q.counts[3 * bounce + 2], req.pending);
+    if (req.pending) {
+      Q.shadow.ray_o[sh_at] = F4(req.origin, req.tmax);
+      Q.shadow.ray_d[sh_at] = F4(req.direction, req.weight);
+      Q.shadow.fl[sh_at] = F4(req.fl, req.pdf);
+      Q.shadow.thr[sh_at] = F4(req.throughput, __uint_as_float(slot));
+    }
   }
 }
 
-// The shadow rays of bounce `bounce`: ShadowTransmittance and the rest of
-// ShadowedLight, added to the path's radiance.
+// The training targets once the sample's paths have ended: the radiance a
+// training path gathered after its second vertex's emission, divided by its
+// throughput on arrival there.
+__global__ void k_cache_targets(CacheQueues C, PathState P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t n = min(C.counters[1], C.train_capacity);
+  if (i >= n) return;
+  const float4 r = P.radiance[C.train_slots[i]];
+  const float4 base = C.train_base[i];
+  const float4 t = C.train_throughput[i];
+  auto ratio = [](float a, float b) { return b > 0.0f ? fmaxf(a, 0.0f) / b : 0.0f; };
+  float4 target = make_float4(ratio(r.x - base.x, t.x), ratio(r.y - base.y, t.y), ratio(r.z - base.z, t.z), 0.0f);
+  if (!isfinite(target.x) || !isfinite(target.y) || !isfinite(target.z)) target = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  C.train_targets[i] = target;
+}
+
 constexpr unsigned kFullWarp = 0xFFFFFFFFu;
 // Resident blocks per SM the persistent tracing kernels are compiled for:
 // six blocks of 128 (80 registers a thread) hide more of the node loads'
@@ -623,12 +682,33 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
 
 // Blocks of a persistent tracing kernel: every resident block on every
 // SM (or `blocks_per_sm`), no more than the queue could fill.
-template <typename Kernel>
-uint32_t persistent_grid(Kernel kernel, uint32_t capacity, const TraceTuning& tuning) {
-  int device = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&device);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+// Resident blocks per SM of a kernel at kBlock threads, and the SM count,
+// looked up once per process and kernel (every device this library drives
+// is an sm_100 part with the same SM count).
+int blocks_per_sm(const void* kernel, int& sms) {
+  static std::mutex mutex;
+  static std::vector<std::pair<const void*, int>> known;
+  static int sm_count = 0;
+  std::lock_guard<std::mutex> lock(mutex);
+  if (sm_count == 0) {
+    int device = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device);
+  }
+  sms = sm_count;
+  for (const auto& k : known)
+    if (k.first == kernel) return k.second;
+  int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0);
+  known.emplace_back(kernel, per_sm);
+  return per_sm;
+}
+
+// Blocks of a persistent kernel: every resident block on every SM (or
+// `blocks_per_sm`), no more than the queue could fill.
+uint32_t persistent_grid(const void* kernel, uint32_t capacity, const TraceTuning& tuning) {
+  int sms = 0;
+  int per_sm = blocks_per_sm(kernel, sms);
   if (tuning.blocks_per_sm) per_sm = std::min<int>(per_sm, (int)tuning.blocks_per_sm);
   const uint32_t grid = (uint32_t)std::max(1, sms) * (uint32_t)std::max(1, per_sm);
   return std::max(1u, std::min(grid, (capacity + kBlock - 1) / kBlock));
@@ -637,7 +717,10 @@ uint32_t persistent_grid(Kernel kernel, uint32_t capacity, const TraceTuning& tu
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
-    SampleProfile* profile, const TraceTuning& tuning) {
+    SampleProfile* profile, const TraceTuning& tuning, const CacheQueues* cache) {
+  CacheQueues C{};
+  if (cache && cache->enabled && cache->cache) C = *cache;
+  else C.enabled = false;
   (void)width;
   (void)height;
   const uint32_t threads = tile_threads(rect);
@@ -645,12 +728,15 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   const bool count = profile && profile->visits;
   VisitCounters* visits = profile ? profile->visits : nullptr;
   cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * kQueueCounterWords * (size_t)(max_bounces + 2), stream);
+  if (C.enabled) cudaMemsetAsync(C.counters, 0, 2 * sizeof(uint32_t), stream);
   uint32_t* fetch = Q.counts + 3 * (size_t)(max_bounces + 2);
   const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid_pixels = (threads + kBlock - 1) / kBlock;
-  const uint32_t grid_queue = (Q.capacity + kBlock - 1) / kBlock;
-  const uint32_t grid_extend = persistent_grid(count ? k_wf_extend<true> : k_wf_extend<false>, Q.capacity, tuning);
-  const uint32_t grid_shadow = persistent_grid(count ? k_wf_shadow<true> : k_wf_shadow<false>, Q.capacity, tuning);
+  const uint32_t grid_extend = persistent_grid(
+      count ? (const void*)k_wf_extend<true> : (const void*)k_wf_extend<false>, Q.capacity, tuning);
+  const uint32_t grid_shadow = persistent_grid(
+      count ? (const void*)k_wf_shadow<true> : (const void*)k_wf_shadow<false>, Q.capacity, tuning);
+  const uint32_t grid_shade = persistent_grid((const void*)k_wf_shade, Q.capacity, TraceTuning());
   {
     Timed t(profile, stream, 0);
     if (count) k_wf_camera<true><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, visits);
@@ -666,7 +752,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     }
     {
       Timed t(profile, stream, 2);
-      k_wf_shade<<<grid_queue, kBlock, 0, stream>>>(S, fc, P, Q, b);
+      k_wf_shade<<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C);
     }
     {
       Timed t(profile, stream, 3);
@@ -674,6 +760,19 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
         k_wf_shadow<true><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, visits);
       else
         k_wf_shadow<false><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, nullptr);
+    }
+  }
+  if (C.enabled) {
+    // The paths that ended into the cache receive its answer; then the
+    // training paths' targets train it.
+    Timed t(profile, stream, 5);
+    launch_cache_infer_records(C.cache->net(), C.cache->grid(), C.queries, C.query_slots, C.query_throughput,
+        P.radiance, &C.counters[0], C.query_capacity, stream);
+    k_cache_targets<<<(C.train_capacity + kBlock - 1) / kBlock, kBlock, 0, stream>>>(C, P);
+    for (uint32_t k = 0; k < C.steps; ++k) {
+      launch_cache_train_records(C.cache->net(), C.cache->grid(), C.train, C.train_targets, &C.counters[1],
+          C.train_capacity, stream);
+      C.cache->adam_step_device(&C.counters[1], C.train_capacity, stream);
     }
   }
   {

@@ -2,6 +2,7 @@
 // Path state, queues and kernel entry points of the two integrators.
 #pragma once
 
+#include "radiance_cache.cuh"
 #include "transport.cuh"
 
 namespace lotus {
@@ -42,6 +43,27 @@ struct Queues {
   uint32_t capacity;
 };
 
+// The radiance cache's per-sample queues: queries (paths that end into the
+// cache at their second vertex) and training records, with their counts in
+// counters[0] and counters[1].
+struct CacheQueues {
+  bool enabled = false;
+  uint32_t stride = 32;           // one path in `stride` trains
+  uint32_t steps = 1;             // training steps per sample
+  RadianceCache* cache = nullptr;
+  CacheRecord* queries = nullptr;
+  uint32_t* query_slots = nullptr;
+  float4* query_throughput = nullptr;
+  uint32_t query_capacity = 0;
+  CacheRecord* train = nullptr;
+  uint32_t* train_slots = nullptr;
+  float4* train_base = nullptr;        // radiance after the second vertex's emission
+  float4* train_throughput = nullptr;  // throughput on arrival at the second vertex
+  float4* train_targets = nullptr;
+  uint32_t train_capacity = 0;
+  uint32_t* counters = nullptr;
+};
+
 // Launch shape of the persistent tracing kernels: a lane takes a new ray
 // when fewer than `refill_below` lanes of its warp still hold one. Zero
 // picks the default.
@@ -68,7 +90,8 @@ struct VisitCounters {
 };
 
 // Optional per-sample instrumentation: events around each kernel (its
-// class in `kinds`: 0 camera, 1 extend, 2 shade, 3 shadow, 4 resolve) and
+// class in `kinds`: 0 camera, 1 extend, 2 shade, 3 shadow, 4 resolve,
+// 5 radiance cache) and
 // visit counting variants of the tracing kernels.
 struct SampleProfile {
   cudaEvent_t* events = nullptr;  // 2 per timed launch
@@ -85,7 +108,8 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
-    SampleProfile* profile = nullptr, const TraceTuning& tuning = TraceTuning());
+    SampleProfile* profile = nullptr, const TraceTuning& tuning = TraceTuning(),
+    const CacheQueues* cache = nullptr);
 
 void launch_advance(FrameConst* fc, cudaStream_t stream);
 

@@ -296,56 +296,167 @@ __device__ __forceinline__ void operands_ready() {
 }
 
 // ---------------------------------------------------------------------------
-// Inference: outputs of the network for `n` queries.
+// Inference: outputs of the network for `n` queries. A CTA holds one copy
+// of the weights and kInferGroups warpgroups, each working through its own
+// tiles with its own activation tile, tensor-memory columns and mbarrier,
+// so that several tiles' encodings, MMAs and epilogues overlap on an SM.
+
+constexpr int kInferGroups = 4;
+constexpr int kInferThreads = 128 * kInferGroups;
+
+// Barrier of one warpgroup (named barrier 1 + group).
+__device__ __forceinline__ void group_sync(uint32_t group) {
+  asm volatile("bar.sync %0, 128;" ::"r"(group + 1u) : "memory");
+}
+
+// AND of `pred` over one warpgroup.
+__device__ __forceinline__ bool group_and(uint32_t group, bool pred) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(out)
+      : "r"(pred ? 1u : 0u), "r"(group + 1u)
+      : "memory");
+  return out != 0;
+}
+
+__device__ __forceinline__ void store_pair(unsigned char* tile, uint32_t row, uint32_t col, float a, float b) {
+  *reinterpret_cast<uint32_t*>(tile + tc::tile_offset(row, col)) = pack_bf16(a, b);
+}
+
+// encode_record written straight into row `row` of an operand tile, a
+// level at a time, so that the 64 inputs never sit in registers together.
+__device__ __forceinline__ void encode_record_to_tile(const CacheGrid& g, const CacheRecord& r, unsigned char* tile,
+    uint32_t row) {
+  float u[3];
+  grid_position(g, r, u);
+  // All levels unrolled, so that their 128 gathers can be in flight
+  // together.
+#pragma unroll
+  for (uint32_t l = 0; l < (uint32_t)kCacheMaxLevels; ++l) {
+    float a = 0.0f, b = 0.0f;
+    if (l < g.levels) {
+      const GridCell c = grid_cell(g, l, u);
+      const __half2* t = g.table + ((size_t)l << g.log2_size);
+      __half2 v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = t[c.index[k]];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const float2 f = __half22float2(v[k]);
+        a += c.weight[k] * f.x;
+        b += c.weight[k] * f.y;
+      }
+    }
+    store_pair(tile, row, 2 * l, a, b);
+  }
+  float x[16];
+  sh_basis(r.dir.x, r.dir.y, r.dir.z, x);
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    uint4 q;
+    q.x = pack_bf16(x[8 * c + 0], x[8 * c + 1]);
+    q.y = pack_bf16(x[8 * c + 2], x[8 * c + 3]);
+    q.z = pack_bf16(x[8 * c + 4], x[8 * c + 5]);
+    q.w = pack_bf16(x[8 * c + 6], x[8 * c + 7]);
+    *reinterpret_cast<uint4*>(tile + tc::tile_offset(row, 32 + 8 * c)) = q;
+  }
+  uint4 q;
+  q.x = pack_bf16(r.normal.x, r.normal.y);
+  q.y = pack_bf16(r.normal.z, r.pos_rough.w);
+  q.z = pack_bf16(r.albedo.x, r.albedo.y);
+  q.w = pack_bf16(r.albedo.z, 1.0f);
+  *reinterpret_cast<uint4*>(tile + tc::tile_offset(row, 48)) = q;
+  *reinterpret_cast<uint4*>(tile + tc::tile_offset(row, 56)) = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// The ReLU of a 64-column accumulator lane into row `row` of a tile, 16
+// columns at a time.
+__device__ __forceinline__ void relu_lane_to_tile(uint32_t taddr, unsigned char* tile, uint32_t row) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    float v[16];
+    tc::tmem_ld16(taddr + 16 * c, v);
+    tc::tmem_wait_ld();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint4 q;
+      q.x = pack_bf16(fmaxf(v[8 * h + 0], 0.0f), fmaxf(v[8 * h + 1], 0.0f));
+      q.y = pack_bf16(fmaxf(v[8 * h + 2], 0.0f), fmaxf(v[8 * h + 3], 0.0f));
+      q.z = pack_bf16(fmaxf(v[8 * h + 4], 0.0f), fmaxf(v[8 * h + 5], 0.0f));
+      q.w = pack_bf16(fmaxf(v[8 * h + 6], 0.0f), fmaxf(v[8 * h + 7], 0.0f));
+      *reinterpret_cast<uint4*>(tile + tc::tile_offset(row, 16 * c + 8 * h)) = q;
+    }
+  }
+}
+
 template <int kIO>
-__global__ void __launch_bounds__(kNetThreads) k_cache_infer(CacheNet net, CacheGrid grid, NetIO io) {
+__global__ void __launch_bounds__(kInferThreads, 1) k_cache_infer(CacheNet net, CacheGrid grid, NetIO io) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = align1024(smem_raw);
   unsigned char* W = smem;
-  unsigned char* A = smem + kCacheOperandBytes;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(A + kTile);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
   const uint32_t tid = threadIdx.x, warp = tid >> 5;
-  for (uint32_t i = tid; i < kCacheOperandBytes / 16; i += kNetThreads)
+  const uint32_t group = tid >> 7, row = tid & 127u;
+  unsigned char* A = smem + kCacheOperandBytes + group * kTile;
+  uint64_t* mbars = reinterpret_cast<uint64_t*>(smem + kCacheOperandBytes + kInferGroups * kTile);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbars + kInferGroups);
+  for (uint32_t i = tid; i < kCacheOperandBytes / 16; i += kInferThreads)
     reinterpret_cast<uint4*>(W)[i] = net.forward[i];
-  if (warp == 0) tc::tmem_alloc(tc::smem_u32(tslot), 64);
-  if (tid == 0) tc::mbar_init(tc::smem_u32(mbar), 1);
-  operands_ready();
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(tslot), 64 * kInferGroups);
+  if (tid < (uint32_t)kInferGroups) tc::mbar_init(tc::smem_u32(mbars + tid), 1);
+  tc::fence_async_shared();
+  tc::fence_before_sync();
+  __syncthreads();
   tc::fence_after_sync();
-  const uint32_t tmem = *tslot;
-  const uint32_t lane_addr = tmem + ((warp * 32u) << 16);
-  Barrier bar{tc::smem_u32(mbar)};
+  const uint32_t tmem = *tslot + 64u * group;
+  const uint32_t lane_addr = tmem + (((warp & 3u) * 32u) << 16);
+  const uint32_t mbar = tc::smem_u32(mbars + group);
+  uint32_t phase = 0;
   const uint32_t n = io_count(io);
   const uint32_t tiles = (n + 127) / 128;
+  const uint32_t stride = gridDim.x * kInferGroups;
   bool ok = true;
-  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-    const uint32_t q = tile * 128 + tid;
-    float x[64];
-    CacheRecord rec;
-    load_input<kIO>(io, grid, q, n, x, rec);
-    store_row64(A, tid, x);
-    operands_ready();
+  for (uint32_t tile = blockIdx.x * kInferGroups + group; tile < tiles && ok; tile += stride) {
+    const uint32_t q = tile * 128 + row;
+    if (kIO == kEncodedIO) {
+      float x[64];
+      CacheRecord rec;
+      load_input<kIO>(io, grid, q, n, x, rec);
+      store_row64(A, row, x);
+    } else if (q < n) {
+      encode_record_to_tile(grid, io.records[q], A, row);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        *reinterpret_cast<uint4*>(A + tc::tile_offset(row, 8 * c)) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    tc::fence_async_shared();
+    tc::fence_before_sync();
+    group_sync(group);
     float y[16];
     for (int l = 0; l < kCacheLayers && ok; ++l) {
-      if (tid == 0) {
+      if (row == 0) {
         tc::fence_after_sync();
         issue_k_major(tmem, tc::smem_u32(A), 64, tc::smem_u32(W) + layer_offset(l), 64, layer_outputs(l), 4);
-        tc::commit(bar.mbar);
+        tc::commit(mbar);
       }
       __syncwarp();
-      ok = bar.wait();
+      const bool waited = tc::mbar_wait(mbar, phase, kWaitPolls);
+      phase ^= 1u;
+      tc::fence_after_sync();
+      ok = group_and(group, waited);
       if (l < kCacheLayers - 1) {
-        load_lane64(lane_addr, x);
-#pragma unroll
-        for (int i = 0; i < 64; ++i) x[i] = fmaxf(x[i], 0.0f);
-        store_row64(A, tid, x);
-        operands_ready();
+        relu_lane_to_tile(lane_addr, A, row);
+        tc::fence_async_shared();
       } else {
         tc::tmem_ld16(lane_addr, y);
         tc::tmem_wait_ld();
-        tc::fence_before_sync();
-        __syncthreads();
       }
+      tc::fence_before_sync();
+      group_sync(group);
     }
     if (!ok || q >= n) continue;
     if (kIO == kEncodedIO) {
@@ -364,11 +475,11 @@ __global__ void __launch_bounds__(kNetThreads) k_cache_infer(CacheNet net, Cache
       io.radiance[slot] = r;
     }
   }
-  if (!ok && tid == 0) atomicExch(net.error, 1u);
+  if (!ok && row == 0) atomicExch(net.error, 1u);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  if (warp == 0) tc::tmem_dealloc(tmem, 64);
+  if (warp == 0) tc::tmem_dealloc(*tslot, 64 * kInferGroups);
 }
 
 // ---------------------------------------------------------------------------
@@ -585,45 +696,68 @@ __global__ void k_pack_weights(const float* __restrict__ w, unsigned char* __res
   *reinterpret_cast<__nv_bfloat16*>(backward + layer_offset(l) + tc::tile_offset_n(i, o, outs)) = v;
 }
 
+// Adam's per-step constants, on the device: [0] the step count, [1] and
+// [2] the bias corrections 1 - beta^t, [3] the gradient scale 1 / (3 n)
+// for n samples, [4] whether the step runs (n > 0).
+constexpr float kBeta1 = 0.9f, kBeta2 = 0.99f, kAdamEps = 1e-15f;
+
+__global__ void k_adam_prepare(float* c, const uint32_t* count, uint32_t capacity, uint32_t samples) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint32_t n = count ? min(*count, capacity) : samples;
+  if (n == 0) {
+    c[4] = 0.0f;
+    return;
+  }
+  const float t = c[0] + 1.0f;
+  c[0] = t;
+  c[1] = 1.0f - powf(kBeta1, t);
+  c[2] = 1.0f - powf(kBeta2, t);
+  c[3] = 1.0f / (3.0f * (float)n);
+  c[4] = 1.0f;
+}
+
+__device__ __forceinline__ float adam_update(float p, float grad, float* m, float* v, float lr, const float* c) {
+  if (!isfinite(grad)) grad = 0.0f;
+  const float mi = kBeta1 * *m + (1.0f - kBeta1) * grad;
+  const float vi = kBeta2 * *v + (1.0f - kBeta2) * grad * grad;
+  *m = mi;
+  *v = vi;
+  return p - lr * (mi / c[1]) / (sqrtf(vi / c[2]) + kAdamEps);
+}
+
 // Adam (Kingma and Ba, 2015) with bias correction over the weights; zeroes
 // the gradient. The output layer's unused columns stay as they are.
 __global__ void k_adam(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
-    uint32_t n, float lr, float beta1, float beta2, float eps, float scale, float c1, float c2) {
+    uint32_t n, float lr, const float* __restrict__ c) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float grad = g[i] * scale;
+  const float grad = g[i] * c[3];
   g[i] = 0.0f;
+  if (c[4] == 0.0f) return;
   if (i >= weight_offset(kCacheLayers - 1) && (i - weight_offset(kCacheLayers - 1)) % 16u >= 3u) return;
-  if (!isfinite(grad)) grad = 0.0f;
-  const float mi = beta1 * m[i] + (1.0f - beta1) * grad;
-  const float vi = beta2 * v[i] + (1.0f - beta2) * grad * grad;
-  m[i] = mi;
-  v[i] = vi;
-  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  p[i] = adam_update(p[i], grad, m + i, v + i, lr, c);
 }
 
 // The same over the hash grid, one entry (two features) per thread, which
-// also refreshes the entry's FP16 copy.
-__global__ void k_adam_grid(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m,
-    float* __restrict__ v, size_t entries, float lr, float beta1, float beta2, float eps, float scale, float c1,
-    float c2, __half2* __restrict__ table) {
+// also refreshes the entry's FP16 copy. Lazy: an entry no sample touched
+// in this step (zero gradient) keeps its moments and value, so a step
+// costs one read of the gradients plus the touched entries' updates (the
+// sparse Adam of embedding tables).
+__global__ void k_adam_grid(float2* __restrict__ p, float2* __restrict__ g, float2* __restrict__ m,
+    float2* __restrict__ v, size_t entries, float lr, const float* __restrict__ c, __half2* __restrict__ table) {
   const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= entries) return;
-  float out[2];
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const size_t i = 2 * e + k;
-    float grad = g[i] * scale;
-    g[i] = 0.0f;
-    if (!isfinite(grad)) grad = 0.0f;
-    const float mi = beta1 * m[i] + (1.0f - beta1) * grad;
-    const float vi = beta2 * v[i] + (1.0f - beta2) * grad * grad;
-    m[i] = mi;
-    v[i] = vi;
-    out[k] = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
-    p[i] = out[k];
-  }
-  table[e] = __floats2half2_rn(out[0], out[1]);
+  const float2 gr = g[e];
+  if (gr.x == 0.0f && gr.y == 0.0f) return;
+  g[e] = make_float2(0.0f, 0.0f);
+  if (c[4] == 0.0f) return;
+  float2 pe = p[e], me = m[e], ve = v[e];
+  pe.x = adam_update(pe.x, gr.x * c[3], &me.x, &ve.x, lr, c);
+  pe.y = adam_update(pe.y, gr.y * c[3], &me.y, &ve.y, lr, c);
+  p[e] = pe;
+  m[e] = me;
+  v[e] = ve;
+  table[e] = __floats2half2_rn(pe.x, pe.y);
 }
 
 __global__ void k_encode(CacheGrid grid, const CacheRecord* __restrict__ records, uint32_t n, float* out) {
@@ -634,7 +768,7 @@ __global__ void k_encode(CacheGrid grid, const CacheRecord* __restrict__ records
   for (int i = 0; i < 64; ++i) out[(size_t)q * 64 + i] = x[i];
 }
 
-constexpr size_t kInferSmem = kCacheOperandBytes + kTile + 64 + 1024;
+constexpr size_t kInferSmem = kCacheOperandBytes + kInferGroups * kTile + 64 + 1024;
 constexpr size_t kTrainSmem = 2 * kCacheOperandBytes + (kCacheLayers + 2) * kTile + kNarrowTile + 64 + 1024;
 
 template <typename Kernel>
@@ -643,9 +777,12 @@ cudaError_t allow_smem(Kernel k, size_t bytes) {
 }
 
 uint32_t sm_count() {
-  int device = 0, sms = 0;
-  cudaGetDevice(&device);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  static int sms = 0;
+  if (sms == 0) {
+    int device = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  }
   return (uint32_t)std::max(sms, 1);
 }
 
@@ -670,8 +807,8 @@ cudaError_t launch_cache_infer_records(const CacheNet& net, const CacheGrid& gri
   io.radiance = radiance;
   io.count = count;
   io.capacity = capacity;
-  const uint32_t grid_size = std::min(3 * sm_count(), std::max(1u, (capacity + 127) / 128));
-  k_cache_infer<kRecordIO><<<grid_size, kNetThreads, kInferSmem, s>>>(net, grid, io);
+  const uint32_t grid_size = std::min(sm_count(), std::max(1u, (capacity + 127) / 128 / kInferGroups + 1));
+  k_cache_infer<kRecordIO><<<grid_size, kInferThreads, kInferSmem, s>>>(net, grid, io);
   return cudaGetLastError();
 }
 
@@ -708,15 +845,16 @@ CacheNet RadianceCache::net() const {
 }
 
 void RadianceCache::release() {
-  void* ptrs[] = {master_, adam_m_, adam_v_, grid_master_, operands_, grad_, loss_, error_, grid_.table, grid_.grad};
+  void* ptrs[] = {master_, adam_m_, adam_v_, grid_master_, operands_, grad_, loss_, error_, grid_.table, grid_.grad,
+      adam_consts_};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   master_ = adam_m_ = adam_v_ = grid_master_ = grad_ = loss_ = nullptr;
   operands_ = nullptr;
   error_ = nullptr;
+  adam_consts_ = nullptr;
   grid_.table = nullptr;
   grid_.grad = nullptr;
-  adam_t_ = 0;
   grid_entries_ = 0;
 }
 
@@ -751,7 +889,8 @@ cudaError_t RadianceCache::configure(const CacheConfig& config, const float lo[3
       (e = cudaMalloc(&grad_, kCacheWeights * 4)) != cudaSuccess ||
       (e = cudaMalloc(&loss_, 4)) != cudaSuccess || (e = cudaMalloc(&error_, 4)) != cudaSuccess ||
       (e = cudaMalloc(&grid_.table, grid_entries_ * sizeof(__half2))) != cudaSuccess ||
-      (e = cudaMalloc(&grid_.grad, grid_floats * 4)) != cudaSuccess) {
+      (e = cudaMalloc(&grid_.grad, grid_floats * 4)) != cudaSuccess ||
+      (e = cudaMalloc(&adam_consts_, 8 * 4)) != cudaSuccess) {
     release();
     return e;
   }
@@ -761,6 +900,7 @@ cudaError_t RadianceCache::configure(const CacheConfig& config, const float lo[3
   cudaMemsetAsync(grid_.grad, 0, grid_floats * 4, s);
   cudaMemsetAsync(loss_, 0, 4, s);
   cudaMemsetAsync(error_, 0, 4, s);
+  cudaMemsetAsync(adam_consts_, 0, 8 * 4, s);
   cudaMemsetAsync(operands_, 0, 2 * kCacheOperandBytes, s);
   k_init_weights<<<(kCacheWeights + 255) / 256, 256, 0, s>>>(master_, config.seed);
   k_init_grid<<<(uint32_t)((grid_entries_ + 255) / 256), 256, 0, s>>>(grid_master_, grid_.table, grid_entries_,
@@ -777,16 +917,23 @@ cudaError_t RadianceCache::pack(cudaStream_t s) {
 
 cudaError_t RadianceCache::adam_step(uint32_t samples, cudaStream_t s) {
   if (!ready() || samples == 0) return cudaSuccess;
-  ++adam_t_;
-  const float beta1 = 0.9f, beta2 = 0.99f, eps = 1e-15f;
-  const float c1 = 1.0f - (float)std::pow((double)beta1, (double)adam_t_);
-  const float c2 = 1.0f - (float)std::pow((double)beta2, (double)adam_t_);
-  const float scale = 1.0f / (3.0f * (float)samples);
+  k_adam_prepare<<<1, 32, 0, s>>>(adam_consts_, nullptr, 0, samples);
+  return adam_kernels(s);
+}
+
+cudaError_t RadianceCache::adam_step_device(const uint32_t* count, uint32_t capacity, cudaStream_t s) {
+  if (!ready()) return cudaSuccess;
+  k_adam_prepare<<<1, 32, 0, s>>>(adam_consts_, count, capacity, 0);
+  return adam_kernels(s);
+}
+
+cudaError_t RadianceCache::adam_kernels(cudaStream_t s) {
   k_adam<<<(kCacheWeights + 255) / 256, 256, 0, s>>>(master_, grad_, adam_m_, adam_v_, kCacheWeights,
-      config_.learning_rate, beta1, beta2, eps, scale, c1, c2);
-  k_adam_grid<<<(uint32_t)((grid_entries_ + 255) / 256), 256, 0, s>>>(grid_master_, grid_.grad,
-      adam_m_ + kCacheWeights, adam_v_ + kCacheWeights, grid_entries_, config_.learning_rate, beta1, beta2, eps,
-      scale, c1, c2, grid_.table);
+      config_.learning_rate, adam_consts_);
+  k_adam_grid<<<(uint32_t)((grid_entries_ + 255) / 256), 256, 0, s>>>(reinterpret_cast<float2*>(grid_master_),
+      reinterpret_cast<float2*>(grid_.grad), reinterpret_cast<float2*>(adam_m_ + kCacheWeights),
+      reinterpret_cast<float2*>(adam_v_ + kCacheWeights), grid_entries_, config_.learning_rate, adam_consts_,
+      grid_.table);
   return pack(s);
 }
 
@@ -836,8 +983,8 @@ cudaError_t RadianceCache::infer_encoded(const float* inputs, uint32_t n, float*
   io.outputs = dout.ptr;
   io.n = n;
   io.capacity = n;
-  const uint32_t grid_size = std::min(3 * sm_count(), std::max(1u, (n + 127) / 128));
-  k_cache_infer<kEncodedIO><<<grid_size, kNetThreads, kInferSmem, s>>>(net(), grid_, io);
+  const uint32_t grid_size = std::min(sm_count(), std::max(1u, (n + 127) / 128 / kInferGroups + 1));
+  k_cache_infer<kEncodedIO><<<grid_size, kInferThreads, kInferSmem, s>>>(net(), grid_, io);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   cudaMemcpyAsync(outputs, dout.ptr, (size_t)n * 3 * 4, cudaMemcpyDeviceToHost, s);
   return cudaStreamSynchronize(s);

@@ -69,6 +69,12 @@ struct CacheConfig {
   uint32_t seed = 1;
 };
 
+cudaError_t launch_cache_infer_records(const CacheNet& net, const CacheGrid& grid, const CacheRecord* records,
+    const uint32_t* slots, const float4* throughput, float4* radiance, const uint32_t* count, uint32_t capacity,
+    cudaStream_t s);
+cudaError_t launch_cache_train_records(const CacheNet& net, const CacheGrid& grid, const CacheRecord* records,
+    const float4* targets, const uint32_t* count, uint32_t capacity, cudaStream_t s);
+
 class RadianceCache {
  public:
   ~RadianceCache() { release(); }
@@ -90,6 +96,10 @@ class RadianceCache {
   // One Adam step over the gradients accumulated since the last one,
   // averaged over `samples` samples.
   cudaError_t adam_step(uint32_t samples, cudaStream_t s);
+  // The same with the sample count read on the device (min(*count,
+  // capacity)) and the step counter kept there, so that it can be captured
+  // in a CUDA graph.
+  cudaError_t adam_step_device(const uint32_t* count, uint32_t capacity, cudaStream_t s);
 
   cudaError_t read_weights(float* host, cudaStream_t s);
   cudaError_t write_weights(const float* host, cudaStream_t s);
@@ -101,6 +111,7 @@ class RadianceCache {
 
  private:
   cudaError_t pack(cudaStream_t s);
+  cudaError_t adam_kernels(cudaStream_t s);
 
   CacheConfig config_;
   CacheGrid grid_{};
@@ -112,7 +123,7 @@ class RadianceCache {
   float* grad_ = nullptr;
   float* loss_ = nullptr;
   uint32_t* error_ = nullptr;
-  uint32_t adam_t_ = 0;
+  float* adam_consts_ = nullptr;  // device: step count, bias corrections, scale
   size_t grid_entries_ = 0;
 };
 

@@ -434,10 +434,15 @@ struct Renderer {
   // World bounds of the resident scene (the radiance cache's grid box).
   float scene_lo[3] = {0.0f, 0.0f, 0.0f}, scene_hi[3] = {1.0f, 1.0f, 1.0f};
 
-  // The learned radiance cache.
+  // The learned radiance cache and its per-sample queues.
   RadianceCache cache;
   lotus_cache_desc cache_desc{};
   bool cache_enabled = false;
+  DeviceArray<CacheRecord> cache_queries, cache_train;
+  DeviceArray<uint32_t> cache_query_slots, cache_train_slots, cache_counters;
+  DeviceArray<float4> cache_query_throughput, cache_train_base, cache_train_throughput, cache_train_targets;
+  uint32_t cache_pixels = 0;
+  uint32_t cache_generation = 0;  // bumped by every configuration
 
   // The wavefront sample as a CUDA graph.
   cudaGraphExec_t graph = nullptr;
@@ -445,6 +450,7 @@ struct Renderer {
     uint64_t scene_generation;
     uint32_t width, height, max_bounces;
     uint32_t rect[4];
+    uint32_t cache;  // the radiance cache's configuration count (0: off)
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
   } graph_key{};
 
@@ -847,6 +853,49 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
   return true;
 }
 
+// The radiance cache's queues for targets of `pixels` pixels: a query per
+// pixel, and training records for one pixel in `stride` with a margin for
+// the per-sample random choice.
+bool ensure_cache_queues(Renderer& R, uint32_t pixels, std::string& detail) {
+  const uint32_t stride = R.cache_desc.training_stride ? R.cache_desc.training_stride : 32u;
+  const uint32_t train = pixels / stride + pixels / (4 * stride) + 1024;
+  if (R.cache_pixels == pixels && R.cache_train.count == train) return true;
+  R.cache_pixels = 0;
+  if (!R.ok(R.cache_queries.resize(pixels), "cache queries", detail) ||
+      !R.ok(R.cache_query_slots.resize(pixels), "cache queries", detail) ||
+      !R.ok(R.cache_query_throughput.resize(pixels), "cache queries", detail) ||
+      !R.ok(R.cache_train.resize(train), "cache training records", detail) ||
+      !R.ok(R.cache_train_slots.resize(train), "cache training records", detail) ||
+      !R.ok(R.cache_train_base.resize(train), "cache training records", detail) ||
+      !R.ok(R.cache_train_throughput.resize(train), "cache training records", detail) ||
+      !R.ok(R.cache_train_targets.resize(train), "cache training records", detail) ||
+      !R.ok(R.cache_counters.resize(2), "cache counters", detail))
+    return false;
+  R.cache_pixels = pixels;
+  return true;
+}
+
+CacheQueues cache_queues(Renderer& R) {
+  CacheQueues C;
+  C.enabled = R.cache_enabled && R.cache.ready() && R.cache_pixels != 0;
+  if (!C.enabled) return C;
+  C.stride = R.cache_desc.training_stride ? R.cache_desc.training_stride : 32u;
+  C.steps = R.cache_desc.training_steps ? R.cache_desc.training_steps : 1u;
+  C.cache = &R.cache;
+  C.queries = R.cache_queries.ptr;
+  C.query_slots = R.cache_query_slots.ptr;
+  C.query_throughput = R.cache_query_throughput.ptr;
+  C.query_capacity = (uint32_t)R.cache_queries.count;
+  C.train = R.cache_train.ptr;
+  C.train_slots = R.cache_train_slots.ptr;
+  C.train_base = R.cache_train_base.ptr;
+  C.train_throughput = R.cache_train_throughput.ptr;
+  C.train_targets = R.cache_train_targets.ptr;
+  C.train_capacity = (uint32_t)R.cache_train.count;
+  C.counters = R.cache_counters.ptr;
+  return C;
+}
+
 int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, float* color_out) {
   std::string detail;
   auto fail = [&](const std::string& msg) {
@@ -884,6 +933,10 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   if (!invert4(vulkan, fc.clip_to_world)) return fail("ray-query camera is singular or non-finite");
   const bool wavefront = st.integrator == LOTUS_INTEGRATOR_WAVEFRONT;
   if (!ensure_targets(R, t.width, t.height, wavefront, detail)) return poison(detail);
+  // The radiance cache serves the wavefront integrator's samples.
+  const bool use_cache = wavefront && R.cache_enabled && R.cache.ready();
+  if (use_cache && !ensure_cache_queues(R, t.width * t.height, detail)) return poison(detail);
+  const CacheQueues cq = use_cache ? cache_queues(R) : CacheQueues();
   // DisplayViewport and DataScissor (vulkan_backend.cpp:651-677).
   float vx = 0.0f, vy = 0.0f, vw = (float)t.width, vh = (float)t.height;
   if (t.display_window[2] > 0.0f && t.display_window[3] > 0.0f) {
@@ -986,7 +1039,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     if (profiled) {
       if (wavefront)
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
-            R.accum.ptr, R.color.ptr, R.totals.ptr, s, &profile, R.tuning);
+            R.accum.ptr, R.color.ptr, R.totals.ptr, s, &profile, R.tuning, &cq);
       else
         launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s,
             &profile);
@@ -998,6 +1051,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
       gk.height = t.height;
       gk.max_bounces = st.max_bounces;
       std::memcpy(gk.rect, rect, sizeof(rect));
+      gk.cache = use_cache ? R.cache_generation : 0u;
       if (!R.graph || !(R.graph_key == gk)) {
         if (R.graph) {
           cudaGraphExecDestroy(R.graph);
@@ -1007,7 +1061,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
         if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
           return poison(detail);
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
-            R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, R.tuning);
+            R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, R.tuning, &cq);
         launch_advance(R.frame_const.ptr, s);
         if (!R.ok(cudaStreamEndCapture(s, &g), "graph capture", detail)) return poison(detail);
         cudaError_t e = cudaGraphInstantiate(&R.graph, g, 0);
@@ -1029,9 +1083,17 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   if (!R.ok(cudaStreamSynchronize(s), "render", detail)) return poison(detail);
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
+  if (use_cache) {
+    uint32_t cc[2] = {0, 0};
+    if (R.ok(cudaMemcpy(cc, R.cache_counters.ptr, sizeof(cc), cudaMemcpyDeviceToHost), "cache counters", detail)) {
+      res.cache_queries = std::min<uint32_t>(cc[0], (uint32_t)R.cache_queries.count);
+      res.cache_training_records = std::min<uint32_t>(cc[1], (uint32_t)R.cache_train.count);
+    }
+    if (R.cache.error_flag(s) != 0) return poison("a radiance-cache kernel's tensor-core wait gave up");
+  }
   if (want_timings) {
-    double by_kind[5] = {0, 0, 0, 0, 0};
-    uint32_t launches[5] = {0, 0, 0, 0, 0};
+    double by_kind[6] = {0, 0, 0, 0, 0, 0};
+    uint32_t launches[6] = {0, 0, 0, 0, 0, 0};
     for (int i = 0; i < profile.count; ++i) {
       float kms = 0.0f;
       cudaEventElapsedTime(&kms, R.profile_events[2 * i], R.profile_events[2 * i + 1]);
@@ -1044,6 +1106,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     res.shade_gpu_ms = by_kind[2];
     res.shadow_gpu_ms = by_kind[3];
     res.resolve_gpu_ms = by_kind[4];
+    res.cache_gpu_ms = by_kind[5];
     res.extend_launches = launches[1];
     res.shadow_launches = launches[3];
   }
@@ -1506,10 +1569,14 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   Q.shadow = ShadowQueue{R.sq_o.ptr, R.sq_d.ptr, R.sq_fl.ptr, R.sq_thr.ptr};
   Q.counts = R.counts.ptr;
   Q.capacity = pixels;
+  // The radiance cache serves the temporal frames' wavefront samples too.
+  const bool use_cache = wavefront && R.cache_enabled && R.cache.ready();
+  if (use_cache && !ensure_cache_queues(R, pixels, detail)) return poison(detail);
+  const CacheQueues cq = use_cache ? cache_queues(R) : CacheQueues();
   for (uint32_t k = 0; k < d.frame_count; ++k) {
     if (wavefront)
       launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
-          R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, R.tuning);
+          R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, R.tuning, &cq);
     else
       launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s);
     launch_advance(R.frame_const.ptr, s);
@@ -1700,8 +1767,9 @@ extern "C" int32_t lotus_cuda_configure_cache(lotus_cuda_renderer* h, const lotu
   }
   R->cache_desc = *d;
   R->cache_enabled = d->enable != 0;
+  R->cache_pixels = 0;
+  ++R->cache_generation;
   R->key_valid = false;
-  R->graph_key = Renderer::GraphKey{};
   return LOTUS_PASS;
 }
 

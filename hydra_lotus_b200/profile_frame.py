@@ -23,15 +23,17 @@ def main():
     ap.add_argument("--frames", type=int, default=2)
     ap.add_argument("--depth", type=int, default=8)
     ap.add_argument("--integrator", default="wavefront", choices=["wavefront", "reference"])
+    ap.add_argument("--cache", action="store_true", help="paths end into the learned radiance cache")
     args = ap.parse_args()
     if args.workload == "sphere-field":
         scene = scenes.sphere_field(seed=0, width=args.width, height=args.height)
     else:
-        scene = scenes.box_room(seed=0, size=args.width)
-        scene.height = args.height
+        scene = scenes.box_room_wide(seed=0, width=args.width, height=args.height)
     integrator = abi.INTEGRATOR_WAVEFRONT if args.integrator == "wavefront" else abi.INTEGRATOR_REFERENCE
     with renderer.CudaOffscreenRenderer(0) as r:
         renderer.check(r.update_scene(scene), "update_scene")
+        if args.cache:
+            r.configure_cache(enable=True, seed=1)
         for k in range(args.frames):
             st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
                                       max_bounces=args.depth, sample_index=k * args.spp)

@@ -129,6 +129,7 @@ class Scene:
         self.environment = None
         self.environment_constant = (0.0, 0.0, 0.0)
         self.world_to_clip = identity()
+        self.view = None  # world to view space, when the temporal passes need it
         self.width = 0
         self.height = 0
         self._desc = None
@@ -520,6 +521,16 @@ def orbit_camera(frame, frames=120, radius=3.0, amplitude=0.35, aspect=1.0):
     view = look_at(eye, (0.0, 0.0, 0.0))
     projection = perspective(45.0, aspect, 1.0, 10.0)
     return view, multiply(projection, view)
+
+
+def box_room_wide(seed=0, width=1920, height=1080):
+    """The box room (config 1's scene) framed for a wide target: the orbit
+    camera's first frame (the Cornell camera's eye and field of view) with
+    the target's aspect, its view matrix kept for the temporal passes."""
+    s = box_room(seed=seed, size=width)
+    s.width, s.height = width, height
+    s.view, s.world_to_clip = orbit_camera(0, aspect=width / height)
+    return s
 
 
 def big_mesh(seed=0, size=96, subdivisions=6):

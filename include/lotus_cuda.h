@@ -207,6 +207,12 @@ typedef struct lotus_frame_result {
   uint64_t node_visits[3];
   uint64_t triangle_visits[3];
   uint64_t instance_visits[3];
+  /* With the radiance cache: the last sample's cache kernels (inference,
+   * training, Adam) with LOTUS_FRAME_TIMINGS, and the sample's queries and
+   * training records. */
+  double cache_gpu_ms;
+  uint32_t cache_queries;
+  uint32_t cache_training_records;
   char detail[256];
 } lotus_frame_result;
 

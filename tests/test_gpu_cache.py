@@ -110,3 +110,35 @@ def test_training_fits_a_function(cuda):
         losses = r.cache_train(rec, target, 200)
         assert np.all(np.isfinite(losses))
         assert losses[-1] < 0.05 * losses[0], f"loss {losses[0]:.4g} -> {losses[-1]:.4g}"
+
+
+def test_cache_gains_over_plain_pt(cuda):
+    """What the trained cache gains: at equal sample counts its image is
+    closer to a converged plain-PT reference than plain PT's, and at many
+    samples its bias (plain PT being the judge) stays small."""
+    from hydra_lotus_b200 import abi, metrics
+    scene = scenes.box_room(seed=0, size=64)
+
+    def settings(sample_index):
+        return abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                                    max_bounces=6, sample_index=sample_index)
+
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        res, ref = r.render_scene(scene.frame(settings(1 << 24), frame_count=8192, read_back=True))
+        cuda.check(res, "reference")
+        res, plain = r.render_scene(scene.frame(settings(1000), frame_count=16, read_back=True))
+        cuda.check(res, "plain")
+        r.configure_cache(enable=True, seed=1)
+        res, _ = r.render_scene(scene.frame(settings(5000), frame_count=128, read_back=True))
+        cuda.check(res, "cache warm-up")
+        assert res.cache_queries > 0 and res.cache_training_records > 0
+        res, cached = r.render_scene(scene.frame(settings(9000), frame_count=16, read_back=True))
+        cuda.check(res, "cache")
+        res, cached_long = r.render_scene(scene.frame(settings(20000), frame_count=512, read_back=True))
+        cuda.check(res, "cache, long")
+    e_plain = metrics.relmse(plain, ref)
+    e_cache = metrics.relmse(cached, ref)
+    e_bias = metrics.relmse(cached_long, ref)
+    assert e_cache < 0.6 * e_plain, f"cache {e_cache:.4g} vs plain {e_plain:.4g} at 16 spp"
+    assert e_bias < 5e-3, f"cache at 512 spp: relMSE {e_bias:.4g} against plain PT"
