@@ -14,6 +14,11 @@ on its own GPU and rank 0 prints the job's total: replicas, no collective
 on the data path (weak scaling). `--impl reference` times the CPU oracle
 (the scalar restatement of the reference's path tracer) on the host cores
 on a bounded band of the same frame.
+
+The line's `time_to_relmse` object is the metric's other half (rank 0,
+`--convergence 0` skips it): device seconds until the running image's
+relMSE falls to 1e-3 for plain PT, the learned radiance cache, ReSTIR DI
+and cache + ReSTIR on the many-light box room at 1080p.
 """
 
 import argparse
@@ -174,6 +179,43 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def time_to_relmse_report(renderer_module):
+    """The metric's first half: device seconds to relMSE 1e-3 (epsilon 1e-2)
+    at 1080p on the box room with 10,000 emissive floor triangles (power
+    log-normal, sigma 2), depth 6, static camera, for plain wavefront PT,
+    the learned radiance cache, ReSTIR DI (temporal + spatial reuse) and
+    cache + ReSTIR. The reference is plain PT at 8192 spp over the middle
+    96 rows, its own noise subtracted. A method that does not reach the
+    target within its budget reports null with an extrapolation from its
+    last checkpoint (relMSE falling as 1/time)."""
+    from hydra_lotus_b200 import convergence
+    scene = scenes.box_room_wide(seed=0, emitters=10000)
+    depth, rows, target = 6, 96, 1e-3
+    budgets = {"plain": 40.0, "cache": 20.0, "restir": 8.0, "cache+restir": 20.0}
+    out = {"scene": "box room + 10,000 emissive floor triangles (power log-normal sigma 2), 1920x1080, "
+                    "depth 6, static camera",
+           "target": target, "epsilon": 1e-2, "unit": "s (device time)"}
+    with renderer_module.CudaOffscreenRenderer(0) as r:
+        renderer_module.check(r.update_scene(scene), "update_scene")
+        ref, noise, ref_s = convergence.reference(r, scene, depth, 8192, rows)
+        out["reference"] = {"method": "plain wavefront PT, FP64 accumulation", "spp": 8192,
+                            "rows": rows, "relmse_noise": noise, "device_s": round(ref_s, 3)}
+        for method, budget in budgets.items():
+            t, pts = convergence.time_to_relmse(r, scene, method, ref, noise, depth, rows, target=target,
+                                                max_seconds=budget)
+            entry = {"seconds": None if t is None else round(t, 4),
+                     "checkpoints": [[round(a, 4), float(f"{b:.4g}")] for a, b in pts]}
+            if t is None and pts:
+                entry["extrapolated_seconds"] = round(pts[-1][0] * pts[-1][1] / target, 2)
+            out[method] = entry
+    plain = out["plain"]["seconds"] or out["plain"].get("extrapolated_seconds")
+    for m in ("cache", "cache+restir", "restir"):
+        v = out[m]["seconds"]
+        if plain and v:
+            out[f"speedup_{m}_vs_plain"] = round(plain / v, 2)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -181,6 +223,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--convergence", type=int, default=1,
+                    help="1: also measure time to relMSE 1e-3 (plain PT, cache, ReSTIR, cache+ReSTIR)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -332,6 +376,8 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clock,
         }
+        if args.convergence:
+            line["time_to_relmse"] = time_to_relmse_report(renderer)
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:

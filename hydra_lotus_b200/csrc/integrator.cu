@@ -345,14 +345,20 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
 // cache records the vertex and the path's throughput), except the training
 // paths, one in `stride` chosen per sample, which record the vertex, their
 // throughput and radiance so far and carry on.
-__global__ void __launch_bounds__(kBlock) k_wf_shade(SceneView S,
+// kCacheVertex: the cache's vertex (bounce 1 with the cache enabled); the
+// other instantiation carries none of the cache's code or registers.
+// Compiled for six resident blocks per SM (80 registers): shading is
+// latency-bound and gains more from occupancy than from registers.
+constexpr int kShadeBlocksPerSm = 6;
+template <bool kCacheVertex>
+__global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C) {
   const uint32_t n = Q.counts[3 * bounce + 1];
   const FrameConst& f = *fcp;
-  const bool cache_vertex = C.enabled && bounce == 1 && bounce < f.max_bounces;
-  // Grid-stride over the hit queue (the grid is sized to the SMs, not to
-  // the largest queue, so that the short queues of late bounces cost
-  // little).
+  const bool cache_vertex = kCacheVertex && bounce < f.max_bounces;
+  // Grid-stride over the hit queue (the grid is sized to a few waves of
+  // the SMs, not to the largest queue, so that the short queues of late
+  // bounces cost little).
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     const uint32_t index = base + threadIdx.x;
     const bool valid = index < n;
@@ -396,7 +402,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_shade(SceneView S,
         P.radiance[slot] = F4(R, 1.0f);
       }
     }
-    if (cache_vertex) {
+    if (kCacheVertex) {
       const uint32_t q_at = warp_append(&C.counters[0], query);
       if (query && q_at < C.query_capacity) {
         C.queries[q_at] = features;
@@ -736,7 +742,10 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
       count ? (const void*)k_wf_extend<true> : (const void*)k_wf_extend<false>, Q.capacity, tuning);
   const uint32_t grid_shadow = persistent_grid(
       count ? (const void*)k_wf_shadow<true> : (const void*)k_wf_shadow<false>, Q.capacity, tuning);
-  const uint32_t grid_shade = persistent_grid((const void*)k_wf_shade, Q.capacity, TraceTuning());
+  // Shading: up to eight waves of resident blocks, grid-striding over
+  // longer queues.
+  const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
+      8u * persistent_grid((const void*)k_wf_shade<false>, Q.capacity, TraceTuning()));
   {
     Timed t(profile, stream, 0);
     if (count) k_wf_camera<true><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, visits);
@@ -752,7 +761,8 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     }
     {
       Timed t(profile, stream, 2);
-      k_wf_shade<<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C);
+      if (C.enabled && b == 1) k_wf_shade<true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C);
+      else k_wf_shade<false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C);
     }
     {
       Timed t(profile, stream, 3);

@@ -523,11 +523,13 @@ def orbit_camera(frame, frames=120, radius=3.0, amplitude=0.35, aspect=1.0):
     return view, multiply(projection, view)
 
 
-def box_room_wide(seed=0, width=1920, height=1080):
+def box_room_wide(seed=0, width=1920, height=1080, emitters=0):
     """The box room (config 1's scene) framed for a wide target: the orbit
     camera's first frame (the Cornell camera's eye and field of view) with
-    the target's aspect, its view matrix kept for the temporal passes."""
-    s = box_room(seed=seed, size=width)
+    the target's aspect, its view matrix kept for the temporal passes. With
+    `emitters`, the many-light variant (restir_room: that many emissive
+    floor triangles in place of the ceiling light)."""
+    s = restir_room(seed=seed, size=width, emitters=emitters) if emitters else box_room(seed=seed, size=width)
     s.width, s.height = width, height
     s.view, s.world_to_clip = orbit_camera(0, aspect=width / height)
     return s
