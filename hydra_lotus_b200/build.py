@@ -61,5 +61,39 @@ def build(force=False, verbose=False, jobs=None):
     return LIB
 
 
+# The C++ adapter (host/cuda_offscreen_renderer.*) implements the
+# reference's Lotus::OffscreenRenderer over the C ABI; it compiles against
+# the reference's headers, so it builds only where they are present (set
+# LOTUS_REFERENCE to the reference's tree). Its test driver links it with
+# the library into _lib/adapter_harness.
+HOST = os.path.join(HERE, "host")
+HARNESS = os.path.join(LIB_DIR, "adapter_harness")
+REFERENCE = os.environ.get("LOTUS_REFERENCE", "/root/reference")
+
+
+def reference_headers():
+    return os.path.exists(os.path.join(REFERENCE, "include", "lotus", "vulkan_backend.hpp"))
+
+
+def build_host(force=False, verbose=False):
+    """Builds the adapter's test driver; returns its path, or None when the
+    reference's headers are absent (a prebuilt driver is kept)."""
+    if not reference_headers():
+        return HARNESS if os.path.exists(HARNESS) else None
+    sources = [os.path.join(HOST, "cuda_offscreen_renderer.cpp"),
+               os.path.join(HERE, "..", "tests", "adapter_harness.cpp")]
+    inputs = sources + [os.path.join(HOST, "cuda_offscreen_renderer.hpp"), LIB]
+    if (not force and os.path.exists(HARNESS) and
+            all(os.path.getmtime(p) <= os.path.getmtime(HARNESS) for p in inputs)):
+        return HARNESS
+    cmd = ["g++", "-std=c++20", "-O2", "-Wall", "-Wextra", f"-I{REFERENCE}/include"] + sources + \
+          ["-o", HARNESS, f"-L{LIB_DIR}", "-llotus_cuda", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return HARNESS
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
+    build_host(force="--force" in sys.argv, verbose=True)

@@ -1,0 +1,384 @@
+// SPDX-License-Identifier: Apache-2.0
+// CudaOffscreenRenderer over the C ABI; see the header for the mapping.
+#include "cuda_offscreen_renderer.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <variant>
+
+namespace lotus_cuda_host {
+
+namespace {
+
+Lotus::FrameStatus to_status(int32_t s) {
+  return s == LOTUS_PASS ? Lotus::FrameStatus::Pass
+                         : (s == LOTUS_SKIP ? Lotus::FrameStatus::Skip : Lotus::FrameStatus::Fail);
+}
+
+// Column-major 4x4 product a * b.
+Lotus::Matrix4 multiply(const Lotus::Matrix4& a, const Lotus::Matrix4& b) {
+  Lotus::Matrix4 m{};
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) {
+      float s = 0.0f;
+      for (int k = 0; k < 4; ++k) s += a[k * 4 + r] * b[c * 4 + k];
+      m[c * 4 + r] = s;
+    }
+  return m;
+}
+
+// The sRGB transfer function's inverse (IEC 61966-2-1).
+float srgb_to_linear(float c) {
+  return c <= 0.04045f ? c / 12.92f : std::pow((c + 0.055f) / 1.055f, 2.4f);
+}
+
+// A texture's texels as linear RGBA floats.
+std::vector<float> texels_rgba32f(const Lotus::Texture& t) {
+  const size_t n = (size_t)t.width * t.height;
+  std::vector<float> out(4 * n, 0.0f);
+  if (t.format == Lotus::TextureFormat::Rgba32Float) {
+    std::memcpy(out.data(), t.texels.data(), std::min(t.texels.size(), out.size() * sizeof(float)));
+    return out;
+  }
+  const bool srgb = t.format == Lotus::TextureFormat::Rgba8Srgb;
+  for (size_t i = 0; i < n && 4 * i + 3 < t.texels.size(); ++i)
+    for (int c = 0; c < 4; ++c) {
+      const float v = t.texels[4 * i + c] / 255.0f;
+      out[4 * i + c] = (srgb && c < 3) ? srgb_to_linear(v) : v;
+    }
+  return out;
+}
+
+}  // namespace
+
+std::unique_ptr<Lotus::OffscreenRenderer> CudaOffscreenRenderer::Create(int device, Lotus::FrameStatus& status,
+    std::string& error) {
+  lotus_cuda_options options{};
+  options.device = device;
+  lotus_cuda_renderer* handle = nullptr;
+  char detail[256] = {};
+  const int32_t s = lotus_cuda_create(&options, &handle, detail, sizeof(detail));
+  status = to_status(s);
+  if (s != LOTUS_PASS) {
+    error = detail;
+    return nullptr;
+  }
+  error.clear();
+  return std::unique_ptr<Lotus::OffscreenRenderer>(new CudaOffscreenRenderer(device, handle));
+}
+
+CudaOffscreenRenderer::~CudaOffscreenRenderer() {
+  if (handle_) lotus_cuda_destroy(handle_);
+}
+
+Lotus::GpuFrameEvidence CudaOffscreenRenderer::Render(const Lotus::DrawSummary&, const Lotus::OffscreenTarget&,
+    std::uint32_t) {
+  Lotus::GpuFrameEvidence e;
+  e.status = Lotus::FrameStatus::Skip;
+  e.detail = "the bootstrap raster draw is not part of the CUDA integrator backend";
+  return e;
+}
+
+Lotus::BackendCapability CudaOffscreenRenderer::RayQueryCapability() const {
+  char detail[256] = {};
+  Lotus::BackendCapability c;
+  c.available = lotus_cuda_capability(device_, detail, sizeof(detail)) == LOTUS_PASS;
+  c.detail = detail;
+  return c;
+}
+
+Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpdate& u) {
+  Lotus::GpuSceneEvidence ev;
+  auto fail = [&](const std::string& why) {
+    ev.status = Lotus::FrameStatus::Fail;
+    ev.detail = why;
+    failed_ = true;
+    failure_ = why;
+    return ev;
+  };
+  if (failed_) return fail("the renderer has failed: " + failure_);
+  // An empty plan records no GPU work (vulkan_backend.hpp:812-815).
+  if (u.geometry_releases.empty() && u.geometry_uploads.empty() && u.texture_releases.empty() &&
+      u.texture_uploads.empty() && !u.instances_changed && !u.materials_changed && !u.environment_changed &&
+      !u.lights_changed) {
+    ev.status = Lotus::FrameStatus::Pass;
+    return ev;
+  }
+  // Releases, then uploads (extraction.hpp:95-106).
+  auto drop = [](auto& list, const void* p) {
+    list.erase(std::remove_if(list.begin(), list.end(), [&](const auto& s) { return s.get() == p; }), list.end());
+  };
+  for (const Lotus::MeshGeometry* g : u.geometry_releases) drop(geometries_, g);
+  for (const Lotus::Texture* t : u.texture_releases) drop(textures_, t);
+  for (const auto& g : u.geometry_uploads) geometries_.push_back(g);
+  for (const auto& t : u.texture_uploads) textures_.push_back(t);
+  if (u.instances_changed) instances_ = u.instances;
+  if (u.materials_changed) materials_ = u.materials;
+  if (u.environment_changed) {
+    environment_ = u.environment;
+    environment_map_ = u.environment_map;
+  }
+  if (u.lights_changed && !u.lights.empty()) return fail("analytic lights are not built in the CUDA backend");
+
+  // The scene description, rebuilt whole.
+  std::unordered_map<const Lotus::MeshGeometry*, uint32_t> slot;
+  std::vector<lotus_geometry> geos(geometries_.size());
+  std::vector<std::vector<float>> positions(geometries_.size()), normals(geometries_.size());
+  std::vector<std::vector<uint32_t>> triangles(geometries_.size());
+  for (size_t g = 0; g < geometries_.size(); ++g) {
+    const Lotus::MeshGeometry& m = *geometries_[g];
+    slot[&m] = (uint32_t)g;
+    positions[g].reserve(3 * m.positions.size());
+    for (const auto& p : m.positions) positions[g].insert(positions[g].end(), p.begin(), p.end());
+    triangles[g].reserve(3 * m.triangles.size());
+    for (const auto& t : m.triangles) triangles[g].insert(triangles[g].end(), t.begin(), t.end());
+    if (!m.normals.empty()) {
+      if (m.normals.size() != 3 * m.triangles.size()) return fail("shading normals must be one per triangle corner");
+      for (const auto& n : m.normals) normals[g].insert(normals[g].end(), n.begin(), n.end());
+    }
+    geos[g].positions = positions[g].data();
+    geos[g].triangles = triangles[g].data();
+    geos[g].normals = normals[g].empty() ? nullptr : normals[g].data();
+    geos[g].vertex_count = (uint32_t)m.positions.size();
+    geos[g].triangle_count = (uint32_t)m.triangles.size();
+  }
+  std::vector<lotus_material> mats(std::max<size_t>(materials_.size(), 1));
+  for (size_t i = 0; i < materials_.size(); ++i) {
+    const Lotus::SceneMaterial& sm = materials_[i];
+    for (const Lotus::Texture* t : sm.textures)
+      if (t) return fail("material " + std::to_string(i) + " has texture inputs, which are not built");
+    if (!std::holds_alternative<Lotus::PreviewSurface>(sm.material.surface))
+      return fail("material " + std::to_string(i) + ": only UsdPreviewSurface is built");
+    const Lotus::PreviewSurface& p = Lotus::Preview(sm.material);
+    lotus_material& m = mats[i];
+    std::memcpy(m.base_color, p.base_color.data(), 12);
+    m.roughness = p.roughness;
+    std::memcpy(m.emission, p.emission.data(), 12);
+    m.metallic = p.metallic;
+    std::memcpy(m.specular_color, p.specular_color.data(), 12);
+    m.ior = p.ior;
+    std::memcpy(m.transmission_color, p.transmission_color.data(), 12);
+    m.transmission = p.transmission;
+    m.opacity = sm.material.geometry.opacity;
+    m.opacity_threshold = sm.material.geometry.opacity_threshold;
+    m.flags = (p.use_specular_workflow ? LOTUS_MATERIAL_SPECULAR_WORKFLOW : 0u) |
+              (p.thin_walled ? LOTUS_MATERIAL_THIN_WALLED : 0u);
+  }
+  if (materials_.empty()) {
+    // A GPU scene starts with the default material alone (extraction.hpp).
+    const Lotus::PreviewSurface p;
+    std::memcpy(mats[0].base_color, p.base_color.data(), 12);
+    mats[0].roughness = p.roughness;
+    mats[0].ior = p.ior;
+    mats[0].transmission_color[0] = mats[0].transmission_color[1] = mats[0].transmission_color[2] = 1.0f;
+    mats[0].opacity = 1.0f;
+  }
+  std::vector<lotus_instance> insts(instances_.size());
+  for (size_t i = 0; i < instances_.size(); ++i) {
+    const Lotus::SceneInstance& si = instances_[i];
+    const auto it = slot.find(si.geometry);
+    if (it == slot.end()) return fail("instance " + std::to_string(i) + " names a geometry that is not resident");
+    std::memcpy(insts[i].world_from_object, si.world_from_object.data(), 64);
+    insts[i].geometry = it->second;
+    insts[i].material = si.material;
+  }
+  lotus_environment env{};
+  std::vector<float> env_texels;
+  if (environment_map_ && environment_map_->texture) {
+    const Lotus::Texture& t = *environment_map_->texture;
+    env_texels = texels_rgba32f(t);
+    env.texels = env_texels.data();
+    env.width = t.width;
+    env.height = t.height;
+    std::memcpy(env.scale, environment_map_->scale.data(), 12);
+    // Rows: the image frame's unit axes in world space, the columns of
+    // world_from_environment's linear part.
+    const Lotus::Matrix4& w = environment_map_->world_from_environment;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) env.environment_from_world[3 * r + c] = w[4 * r + c];
+  }
+  lotus_scene_desc desc{};
+  desc.geometries = geos.data();
+  desc.instances = insts.data();
+  desc.materials = mats.data();
+  desc.environment = env.texels ? &env : nullptr;
+  desc.geometry_count = (uint32_t)geos.size();
+  desc.instance_count = (uint32_t)insts.size();
+  desc.material_count = (uint32_t)mats.size();
+  std::memcpy(desc.environment_constant, environment_.data(), 12);
+  lotus_scene_result res{};
+  const int32_t s = lotus_cuda_update_scene(handle_, &desc, &res);
+  ev.status = to_status(s);
+  ev.detail = res.detail;
+  if (s != LOTUS_PASS) {
+    failed_ = true;
+    failure_ = ev.detail;
+    return ev;
+  }
+  device_bytes_ = res.device_bytes;
+  ev.stats.source_revision = u.source_revision;
+  ev.stats.resident_geometries = (uint32_t)geometries_.size();
+  ev.stats.instance_count = res.instance_count;
+  ev.stats.material_count = (uint32_t)mats.size();
+  ev.stats.environment_map = env.texels != nullptr;
+  ev.stats.resident_textures = (uint32_t)textures_.size();
+  ev.stats.acceleration_available = true;
+  ev.stats.blas_count = (uint32_t)geometries_.size();
+  ev.stats.tlas_instance_count = res.instance_count;
+  ev.timings.available = true;
+  ev.timings.blas_build_gpu_ms = res.build_gpu_ms;
+  return ev;
+}
+
+bool CudaOffscreenRenderer::FillFrame(const Lotus::Matrix4& world_to_clip, const Lotus::OffscreenTarget& t,
+    std::uint32_t frame_count, const Lotus::PathTracingSettings& s, lotus_frame_desc& f, std::string& error) const {
+  if (s.output != Lotus::SceneOutput::Radiance) {
+    error = "only the Radiance output is built in the CUDA backend";
+    return false;
+  }
+  f = lotus_frame_desc{};
+  std::memcpy(f.world_to_clip, world_to_clip.data(), 64);
+  f.target.width = t.width;
+  f.target.height = t.height;
+  std::memcpy(f.target.display_window, t.display_window.data(), 16);
+  std::memcpy(f.target.data_window, t.data_window.data(), 16);
+  std::memcpy(f.target.clear_color, t.clear_color.data(), 16);
+  f.target.read_back = t.read_back ? 1u : 0u;
+  f.settings.integrator =
+      s.integrator == Lotus::Integrator::Wavefront ? LOTUS_INTEGRATOR_WAVEFRONT : LOTUS_INTEGRATOR_REFERENCE;
+  f.settings.light_sampling = s.light_sampling == Lotus::LightSampling::Bsdf ? LOTUS_LIGHT_SAMPLING_BSDF
+                              : s.light_sampling == Lotus::LightSampling::Mis ? LOTUS_LIGHT_SAMPLING_MIS
+                                                                              : LOTUS_LIGHT_SAMPLING_RESTIR_INITIAL;
+  f.settings.sample_index = s.sample_index;
+  f.settings.max_bounces = s.max_bounces;
+  f.settings.max_samples = s.max_samples;
+  f.settings.restir_candidates = s.restir_candidates;
+  f.settings.restir_temporal = s.restir_temporal ? 1u : 0u;
+  f.settings.restir_max_history_candidates = s.restir_max_history_candidates;
+  f.settings.restir_spatial = s.restir_spatial ? 1u : 0u;
+  f.settings.restir_spatial_radius = s.restir_spatial_radius;
+  f.settings.restir_proposal = (uint32_t)s.restir_proposal;
+  f.settings.environment_background = s.environment_background ? 1u : 0u;
+  f.frame_count = frame_count;
+  f.flags = LOTUS_FRAME_TIMINGS;
+  return true;
+}
+
+void CudaOffscreenRenderer::FillEvidence(const lotus_frame_desc& f, const lotus_frame_result& r,
+    std::vector<float>& color, Lotus::GpuFrameEvidence& e) {
+  e.status = to_status(r.status);
+  e.detail = r.detail;
+  e.completion = r.completion;
+  e.frames_rendered = r.frames_rendered;
+  e.samples_per_pixel = r.samples_per_pixel;
+  e.primary_ray_timestamp_available = true;
+  e.primary_ray_gpu_ms = r.gpu_ms;
+  e.wavefront_rounds = r.wavefront_rounds;
+  e.wavefront_path_counts.assign(r.wavefront_path_counts,
+      r.wavefront_path_counts + std::min<uint32_t>(r.wavefront_path_count_size, LOTUS_MAX_REPORTED_BOUNCES));
+  e.wavefront_timings.available = r.timings_available != 0;
+  e.wavefront_timings.camera_gpu_ms = r.camera_gpu_ms;
+  e.wavefront_timings.intersect_gpu_ms = r.extend_gpu_ms;
+  e.wavefront_timings.shade_gpu_ms = r.shade_gpu_ms + r.shadow_gpu_ms;
+  if (r.status == LOTUS_PASS && f.target.read_back) {
+    // RGBA32F, top-left rows, linear (vulkan_backend.hpp:30-38).
+    Lotus::ColorProduct& c = e.color;
+    c.width = f.target.width;
+    c.height = f.target.height;
+    c.row_pitch = f.target.width * 16;
+    c.pixel_format = "rgba32-sfloat";
+    c.origin = "top-left";
+    c.color_space = "linear";
+    c.payload.resize(color.size() * sizeof(float));
+    std::memcpy(c.payload.data(), color.data(), c.payload.size());
+  }
+}
+
+Lotus::GpuFrameEvidence CudaOffscreenRenderer::RenderScene(const Lotus::DrawSummary& draw,
+    const Lotus::OffscreenTarget& target, std::uint32_t frame_count, const Lotus::PathTracingSettings& settings) {
+  Lotus::GpuFrameEvidence e;
+  lotus_frame_desc f;
+  std::string error;
+  if (!FillFrame(draw.world_to_clip, target, frame_count, settings, f, error)) {
+    e.status = Lotus::FrameStatus::Fail;
+    e.detail = error;
+    return e;
+  }
+  std::vector<float> color(target.read_back ? (size_t)target.width * target.height * 4 : 0);
+  lotus_frame_result r{};
+  lotus_cuda_render(handle_, &f, &r, color.empty() ? nullptr : color.data());
+  FillEvidence(f, r, color, e);
+  return e;
+}
+
+Lotus::GpuFrameEvidence CudaOffscreenRenderer::RenderTemporalScene(const Lotus::FrameSnapshot& snapshot,
+    const Lotus::OffscreenTarget& target, std::uint32_t frame_count, const Lotus::TemporalFrameSettings& temporal,
+    const Lotus::PathTracingSettings& settings) {
+  Lotus::GpuFrameEvidence e;
+  lotus_temporal_desc d{};
+  std::string error;
+  const Lotus::Matrix4 world_to_clip = multiply(snapshot.camera.projection, snapshot.camera.view);
+  if (!FillFrame(world_to_clip, target, frame_count, settings, d.frame, error)) {
+    e.status = Lotus::FrameStatus::Fail;
+    e.detail = error;
+    return e;
+  }
+  // The stream's history: the preceding frame's camera unless this frame is
+  // a cut.
+  const bool history = have_previous_camera_ && !temporal.camera_cut;
+  const Lotus::Camera& prev = history ? previous_camera_ : snapshot.camera;
+  std::memcpy(d.current_view, snapshot.camera.view.data(), 64);
+  std::memcpy(d.previous_view, prev.view.data(), 64);
+  const Lotus::Matrix4 prev_clip = multiply(prev.projection, prev.view);
+  std::memcpy(d.previous_world_to_clip, prev_clip.data(), 64);
+  d.validation[0] = temporal.validation.absolute_depth_tolerance;
+  d.validation[1] = temporal.validation.relative_depth_tolerance;
+  d.validation[2] = temporal.validation.minimum_normal_cosine;
+  d.validation[3] = temporal.validation.max_motion_pixels;
+  d.history_available = history ? 1u : 0u;
+  d.accumulate_radiance = temporal.accumulate_radiance ? 1u : 0u;
+  d.max_history_samples = temporal.max_history_samples;
+  d.filter_iterations = temporal.filter_iterations;
+  d.history_rectification = (uint32_t)temporal.history_rectification;
+  std::vector<float> color(target.read_back ? (size_t)target.width * target.height * 4 : 0);
+  lotus_frame_result r{};
+  lotus_cuda_render_temporal(handle_, &d, &r, color.empty() ? nullptr : color.data());
+  FillEvidence(d.frame, r, color, e);
+  if (r.status == LOTUS_PASS) {
+    // Only success advances history (vulkan_backend.hpp:793-806).
+    previous_camera_ = snapshot.camera;
+    have_previous_camera_ = true;
+  }
+  return e;
+}
+
+Lotus::GpuSceneContents CudaOffscreenRenderer::ReadBackScene() {
+  Lotus::GpuSceneContents c;
+  c.status = Lotus::FrameStatus::Skip;
+  c.detail = "scene readback is not built in the CUDA backend";
+  return c;
+}
+
+Lotus::PresentEvidence CudaOffscreenRenderer::Present(std::uint32_t, std::uint32_t, const Lotus::PresentView&) {
+  Lotus::PresentEvidence p;
+  p.status = Lotus::FrameStatus::Skip;
+  p.detail = "presentation is a graphics-side part of the reference; the CUDA backend has none";
+  return p;
+}
+
+Lotus::GpuResidency CudaOffscreenRenderer::Residency() const {
+  Lotus::GpuResidency r;
+  Lotus::GpuAllocationGroup g;
+  g.owner = "scene";
+  g.device_local = true;
+  g.allocations = 1;
+  g.bytes = device_bytes_;
+  r.groups.push_back(g);
+  r.device_local_bytes = device_bytes_;
+  r.budget_available = false;
+  r.budget_detail = "the CUDA backend reports the resident scene only";
+  return r;
+}
+
+}  // namespace lotus_cuda_host

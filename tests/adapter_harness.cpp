@@ -1,0 +1,182 @@
+// SPDX-License-Identifier: Apache-2.0
+// Test driver of CudaOffscreenRenderer (hydra_lotus_b200/host): reads a
+// scene and a frame from a small binary file, turns them into the
+// reference's own types (MeshGeometry, SceneInstance, SceneMaterial with a
+// PreviewSurface, SceneEnvironmentMap, SceneUpdate, DrawSummary,
+// OffscreenTarget, PathTracingSettings), drives the adapter through
+// Lotus::OffscreenRenderer's interface as a reference host would, and
+// writes the colour product's floats to the output file. Prints one JSON
+// line with the evidence. tests/test_gpu_adapter.py writes the input and
+// compares the output with the C ABI's own render of the same frame.
+//
+// Input (little-endian): "LTSC", u32 version 1; u32 geometry, instance and
+// material counts; f32 environment constant[3]; u32 has_environment (then
+// u32 width, height; f32 scale[3], rows[9]; f32 texels[4 w h]); per
+// geometry u32 vertices, triangles, has_normals, f32 positions[3 v], u32
+// indices[3 t], f32 normals[9 t] when present; per instance f32 m[16], u32
+// geometry, material; per material the 80-byte lotus_material; the frame:
+// f32 world_to_clip[16], u32 width, height, integrator, light_sampling,
+// max_bounces, sample_index, frame_count.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <memory>
+#include <vector>
+
+#include "../hydra_lotus_b200/host/cuda_offscreen_renderer.hpp"
+
+namespace {
+
+struct Reader {
+  std::vector<char> data;
+  size_t at = 0;
+  template <typename T>
+  T get() {
+    T v{};
+    if (at + sizeof(T) <= data.size()) std::memcpy(&v, data.data() + at, sizeof(T));
+    at += sizeof(T);
+    return v;
+  }
+  template <typename T>
+  void get(T* out, size_t n) {
+    for (size_t i = 0; i < n; ++i) out[i] = get<T>();
+  }
+  bool ok() const { return at <= data.size(); }
+};
+
+const char* status_name(Lotus::FrameStatus s) {
+  return s == Lotus::FrameStatus::Pass ? "pass" : (s == Lotus::FrameStatus::Skip ? "skip" : "fail");
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc != 3) {
+    std::fprintf(stderr, "usage: adapter_harness <scene file> <output floats>\n");
+    return 2;
+  }
+  Reader in;
+  {
+    std::ifstream f(argv[1], std::ios::binary);
+    in.data.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+  }
+  char magic[4];
+  in.get(magic, 4);
+  if (std::memcmp(magic, "LTSC", 4) != 0 || in.get<uint32_t>() != 1) {
+    std::fprintf(stderr, "not a scene file\n");
+    return 2;
+  }
+  const uint32_t ng = in.get<uint32_t>(), ni = in.get<uint32_t>(), nm = in.get<uint32_t>();
+  Lotus::SceneUpdate update;
+  update.source_revision = 1;
+  update.environment_changed = true;
+  in.get(update.environment.data(), 3);
+  std::shared_ptr<Lotus::Texture> env_texture;
+  if (in.get<uint32_t>()) {
+    env_texture = std::make_shared<Lotus::Texture>();
+    env_texture->width = in.get<uint32_t>();
+    env_texture->height = in.get<uint32_t>();
+    env_texture->format = Lotus::TextureFormat::Rgba32Float;
+    Lotus::SceneEnvironmentMap map;
+    in.get(map.scale.data(), 3);
+    float rows[9];
+    in.get(rows, 9);
+    // world_from_environment's columns are the image frame's axes.
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) map.world_from_environment[4 * r + c] = rows[3 * r + c];
+    std::vector<float> texels(4 * (size_t)env_texture->width * env_texture->height);
+    in.get(texels.data(), texels.size());
+    env_texture->texels.resize(texels.size() * sizeof(float));
+    std::memcpy(env_texture->texels.data(), texels.data(), env_texture->texels.size());
+    map.texture = env_texture.get();
+    update.texture_uploads.push_back(env_texture);
+    update.environment_map = map;
+  }
+  std::vector<std::shared_ptr<Lotus::MeshGeometry>> meshes;
+  for (uint32_t g = 0; g < ng; ++g) {
+    auto m = std::make_shared<Lotus::MeshGeometry>();
+    const uint32_t nv = in.get<uint32_t>(), nt = in.get<uint32_t>(), has_normals = in.get<uint32_t>();
+    m->positions.resize(nv);
+    for (auto& p : m->positions) in.get(p.data(), 3);
+    m->triangles.resize(nt);
+    for (auto& t : m->triangles) in.get(t.data(), 3);
+    if (has_normals) {
+      m->normals.resize(3 * (size_t)nt);
+      for (auto& n : m->normals) in.get(n.data(), 3);
+    }
+    meshes.push_back(m);
+    update.geometry_uploads.push_back(m);
+  }
+  update.instances_changed = true;
+  for (uint32_t i = 0; i < ni; ++i) {
+    Lotus::SceneInstance s;
+    in.get(s.world_from_object.data(), 16);
+    const uint32_t g = in.get<uint32_t>();
+    s.material = in.get<uint32_t>();
+    s.geometry = g < meshes.size() ? meshes[g].get() : nullptr;
+    update.instances.push_back(s);
+  }
+  update.materials_changed = true;
+  for (uint32_t i = 0; i < nm; ++i) {
+    const lotus_material lm = in.get<lotus_material>();
+    Lotus::SceneMaterial sm;
+    Lotus::PreviewSurface p;
+    std::memcpy(p.base_color.data(), lm.base_color, 12);
+    p.roughness = lm.roughness;
+    std::memcpy(p.emission.data(), lm.emission, 12);
+    p.metallic = lm.metallic;
+    std::memcpy(p.specular_color.data(), lm.specular_color, 12);
+    p.ior = lm.ior;
+    std::memcpy(p.transmission_color.data(), lm.transmission_color, 12);
+    p.transmission = lm.transmission;
+    p.use_specular_workflow = (lm.flags & LOTUS_MATERIAL_SPECULAR_WORKFLOW) != 0;
+    p.thin_walled = (lm.flags & LOTUS_MATERIAL_THIN_WALLED) != 0;
+    sm.material.surface = p;
+    sm.material.geometry.opacity = lm.opacity;
+    sm.material.geometry.opacity_threshold = lm.opacity_threshold;
+    update.materials.push_back(sm);
+  }
+  Lotus::DrawSummary draw;
+  in.get(draw.world_to_clip.data(), 16);
+  Lotus::OffscreenTarget target;
+  target.width = in.get<uint32_t>();
+  target.height = in.get<uint32_t>();
+  Lotus::PathTracingSettings settings;
+  settings.integrator = in.get<uint32_t>() == LOTUS_INTEGRATOR_WAVEFRONT ? Lotus::Integrator::Wavefront
+                                                                         : Lotus::Integrator::Reference;
+  const uint32_t ls = in.get<uint32_t>();
+  settings.light_sampling = ls == LOTUS_LIGHT_SAMPLING_BSDF ? Lotus::LightSampling::Bsdf : Lotus::LightSampling::Mis;
+  settings.max_bounces = in.get<uint32_t>();
+  settings.sample_index = in.get<uint32_t>();
+  const uint32_t frame_count = in.get<uint32_t>();
+  if (!in.ok()) {
+    std::fprintf(stderr, "truncated scene file\n");
+    return 2;
+  }
+
+  Lotus::FrameStatus status;
+  std::string error;
+  std::unique_ptr<Lotus::OffscreenRenderer> renderer =
+      lotus_cuda_host::CudaOffscreenRenderer::Create(0, status, error);
+  if (!renderer) {
+    std::printf("{\"create\": \"%s\", \"detail\": \"%s\"}\n", status_name(status), error.c_str());
+    return status == Lotus::FrameStatus::Skip ? 77 : 1;
+  }
+  const Lotus::BackendCapability cap = renderer->RayQueryCapability();
+  const Lotus::GpuSceneEvidence scene = renderer->UpdateScene(update);
+  const Lotus::GpuFrameEvidence frame = renderer->RenderScene(draw, target, frame_count, settings);
+  const Lotus::GpuFrameEvidence bootstrap = renderer->Render(draw, target, 1);
+  const Lotus::PresentEvidence present = renderer->Present(target.width, target.height);
+  std::printf(
+      "{\"capability\": %s, \"update\": \"%s\", \"update_detail\": \"%s\", \"instances\": %u, "
+      "\"render\": \"%s\", \"render_detail\": \"%s\", \"spp\": %u, \"rounds\": %u, \"paths\": %zu, "
+      "\"pixel_format\": \"%s\", \"row_pitch\": %u, \"bytes\": %zu, \"bootstrap\": \"%s\", \"present\": \"%s\"}\n",
+      cap.available ? "true" : "false", status_name(scene.status), scene.detail.c_str(), scene.stats.instance_count,
+      status_name(frame.status), frame.detail.c_str(), frame.samples_per_pixel, frame.wavefront_rounds,
+      frame.wavefront_path_counts.size(), frame.color.pixel_format.c_str(), frame.color.row_pitch,
+      frame.color.payload.size(), status_name(bootstrap.status), status_name(present.status));
+  std::ofstream out(argv[2], std::ios::binary);
+  out.write(reinterpret_cast<const char*>(frame.color.payload.data()), (std::streamsize)frame.color.payload.size());
+  return frame.status == Lotus::FrameStatus::Pass ? 0 : 1;
+}
