@@ -15,7 +15,7 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "liblotus_cuda.so")
 INCLUDE = os.path.join(HERE, "..", "include")
 SOURCES = ["integrator.cu", "bvh_build.cu", "renderer.cu", "static_render.cu", "temporal.cu",
-           "radiance_cache.cu"]
+           "radiance_cache.cu", "batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-Wall"]

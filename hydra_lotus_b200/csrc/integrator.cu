@@ -61,6 +61,22 @@ __device__ __forceinline__ void warp_add64(unsigned long long* counter, uint32_t
   if ((threadIdx.x & 31u) == 0 && v) atomicAdd(counter, v);
 }
 
+// The scene of a batch that owns path slot `slot` (binary search over the
+// scenes' slot ranges).
+__device__ __forceinline__ uint32_t table_scene(const SceneTable& B, uint32_t slot) {
+  uint32_t lo = 0, hi = B.count;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (B.slot_base[mid] <= slot) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ bool frame_rect_contains(const FrameConst& f, uint32_t px, uint32_t py) {
+  return px >= f.rect[0] && py >= f.rect[1] && px < f.rect[0] + f.rect[2] && py < f.rect[1] + f.rect[3];
+}
+
 // Next event estimation's pending shadow ray.
 struct ShadowRequest {
   bool pending;
@@ -301,26 +317,42 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
 
 // Camera (wavefront.slang:206-225): starts each pixel's path and traces its
 // camera ray; a hit is queued for shading at bounce 0.
-template <bool kCount>
+// In a batch (kBatch) one thread per path slot of every scene, in each
+// image's row order; otherwise 8x4 pixel tiles per warp.
+template <bool kCount, bool kBatch>
 __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
-    const FrameConst* __restrict__ fcp, PathState P, Queues Q, VisitCounters* visits) {
+    const FrameConst* __restrict__ fcp, PathState P, Queues Q, VisitCounters* visits, SceneTable B) {
   TraversalCounters vc = {0, 0, 0};
-  const FrameConst& f = *fcp;
-  if (!f.add_sample) return;
-  const uint32_t rect[4] = {f.rect[0], f.rect[1], f.rect[2], f.rect[3]};
-  uint32_t px, py;
   const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = tile_pixel(index, rect, px, py);
+  uint32_t px = 0, py = 0, slot = 0, scene = 0;
+  bool valid;
+  if (kBatch) {
+    slot = index;
+    valid = index < B.total_slots;
+    if (valid) {
+      scene = table_scene(B, slot);
+      const FrameConst& fb = B.frames[scene];
+      const uint32_t local = slot - B.slot_base[scene];
+      px = local % fb.width;
+      py = local / fb.width;
+      valid = fb.add_sample && frame_rect_contains(fb, px, py);
+    }
+  } else {
+    if (!fcp->add_sample) return;
+    const uint32_t rect[4] = {fcp->rect[0], fcp->rect[1], fcp->rect[2], fcp->rect[3]};
+    valid = tile_pixel(index, rect, px, py);
+    slot = py * fcp->width + px;
+  }
+  const FrameConst& f = kBatch ? B.frames[scene] : *fcp;
+  const SceneView& SS = kBatch ? B.views[scene] : S;
   bool found = false;
-  uint32_t slot = 0;
   if (valid) {
-    slot = py * f.width + px;
     F3 o, d;
     float tmax;
     uint32_t rng;
     start_path(f, px, py, f.sample_index, o, d, tmax, rng);
     Hit hit;
-    found = trace_closest<kCount>(S, o, d, 0.0f, tmax, rng, hit, &vc);
+    found = trace_closest<kCount>(SS, o, d, 0.0f, tmax, rng, hit, &vc);
     if (found) {
       P.direction[slot] = F4(d, tmax);
       P.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng));
@@ -350,12 +382,11 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
 // Compiled for six resident blocks per SM (80 registers): shading is
 // latency-bound and gains more from occupancy than from registers.
 constexpr int kShadeBlocksPerSm = 6;
-template <bool kCacheVertex>
+template <bool kCacheVertex, bool kBatch>
 __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneView S,
-    const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C) {
+    const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 1];
-  const FrameConst& f = *fcp;
-  const bool cache_vertex = kCacheVertex && bounce < f.max_bounces;
+  const bool cache_vertex = kCacheVertex && bounce < fcp->max_bounces;
   // Grid-stride over the hit queue (the grid is sized to a few waves of
   // the SMs, not to the largest queue, so that the short queues of late
   // bounces cost little).
@@ -370,6 +401,9 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
     F3 T = V(1.0f), T_in = V(1.0f), R = V(0.0f);
     if (valid) {
       slot = Q.hit[index];
+      const uint32_t scene = kBatch ? table_scene(B, slot) : 0u;
+      const FrameConst& f = kBatch ? B.frames[scene] : *fcp;
+      const SceneView& SS = kBatch ? B.views[scene] : S;
       const float4 dir = P.direction[slot];
       const float4 rad = P.radiance[slot];
       const uint4 h = P.hit[slot];
@@ -389,7 +423,7 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
       if (cache_vertex)
         training = pcg_hash(slot ^ pcg_hash(f.sample_index ^ 0xC2B2AE35u)) % C.stride == 0u;
       F3 no, nd;
-      cont = scatter(S, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
+      cont = scatter(SS, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
           T, R, last_pdf, flags, rng, no, nd, req, slot, cache_vertex ? &features : nullptr,
           cache_vertex && !training);
       query = cache_vertex && !training;
@@ -474,29 +508,30 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor, uint32_t n, boo
 // ShadowedLight's visibility (transport.slang:82-115) for the shadow queue,
 // as a persistent kernel: each lane walks one shadow ray at a time and adds
 // the light to the path's radiance when the ray arrives.
-template <bool kCount>
+template <bool kCount, bool kBatch>
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_shadow(SceneView S, PathState P, Queues Q,
-    uint32_t bounce, uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits) {
+    uint32_t bounce, uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 2];
   TraversalCounters vc = {0, 0, 0};
   uint32_t rays = 0;
   Walk W;
   WalkStack stack;
   uint32_t rng = 0;
-  uint32_t index = 0;
+  uint32_t index = 0, scene = 0;
   bool active = false, exhausted = false;
   for (;;) {
     const uint32_t got = warp_fetch(fetch, n, active, refill_below, exhausted);
     if (got < n) {
       index = got;
+      if (kBatch) scene = table_scene(B, __float_as_uint(Q.shadow.thr[index].w));
       const float4 ro = Q.shadow.ray_o[index];
       const float4 rd = Q.shadow.ray_d[index];
-      walk_begin(S, W, V(ro), V(rd), 0.0f, ro.w);
+      walk_begin(kBatch ? B.views[scene] : S, W, V(ro), V(rd), 0.0f, ro.w);
       active = true;
       ++rays;
     }
     if (!__any_sync(kFullWarp, active)) break;
-    if (walk_round<true, kCount>(S, W, stack, rng, active, &vc)) {
+    if (walk_round<true, kCount>(kBatch ? B.views[scene] : S, W, stack, rng, active, &vc)) {
       active = false;
       const float tr = W.transmittance;
       if (tr > 0.0f) {
@@ -526,13 +561,12 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_shadow(SceneVi
 // queued for shading; a miss ends the path with the environment. Each warp
 // stages its hits in shared memory and appends them to the hit queue 32 at
 // a time.
-template <bool kCount>
+template <bool kCount, bool kBatch>
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce,
-    uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits) {
+    uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits, SceneTable B) {
   __shared__ uint32_t staged[kBlock / 32][64];
   const uint32_t n = Q.counts[3 * bounce];
-  const FrameConst& f = *fcp;
   const unsigned lane = threadIdx.x & 31u;
   uint32_t* stage = staged[threadIdx.x >> 5];
   uint32_t* hits = &Q.counts[3 * bounce + 1];
@@ -541,22 +575,24 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneVi
   uint32_t rays = 0;
   Walk W;
   WalkStack stack;
-  uint32_t rng = 0, rng0 = 0, slot = 0;
+  uint32_t rng = 0, rng0 = 0, slot = 0, scene = 0;
   bool active = false, exhausted = false;
   for (;;) {
     const uint32_t got = warp_fetch(fetch, n, active, refill_below, exhausted);
     if (got < n) {
       slot = Q.ray[bounce & 1][got];
+      if (kBatch) scene = table_scene(B, slot);
       const float4 o = P.origin[slot];
       const float4 d = P.direction[slot];
       rng = rng0 = __float_as_uint(P.radiance[slot].w);
-      walk_begin(S, W, V(o), V(d), o.w, d.w);
+      walk_begin(kBatch ? B.views[scene] : S, W, V(o), V(d), o.w, d.w);
       active = true;
       ++rays;
     }
     if (!__any_sync(kFullWarp, active)) break;
     bool emit = false;
-    if (walk_round<false, kCount>(S, W, stack, rng, active, &vc)) {
+    const SceneView& SS = kBatch ? B.views[scene] : S;
+    if (walk_round<false, kCount>(SS, W, stack, rng, active, &vc)) {
       active = false;
       if (W.found) {
         P.hit[slot] = make_uint4(W.best_instance, W.best_tri, __float_as_uint(W.b1), __float_as_uint(W.b2));
@@ -566,7 +602,8 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneVi
         const float4 rad = P.radiance[slot];
         const float4 thr = P.throughput[slot];
         const uint32_t flags = thr.w < 0.0f ? kUnweightedLight : 0u;
-        const F3 R = V(rad) + V(thr) * miss_radiance(S, f, W.direction, flags, thr.w);
+        const FrameConst& f = kBatch ? B.frames[scene] : *fcp;
+        const F3 R = V(rad) + V(thr) * miss_radiance(SS, f, W.direction, flags, thr.w);
         P.radiance[slot] = F4(R, 1.0f);
       }
     }
@@ -606,21 +643,33 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneVi
 // Resolve (path_trace.slang:353-385): adds each ended path's sample to its
 // pixel and writes the mean; pixels outside the data window keep the clear
 // colour.
+template <bool kBatch>
 __global__ void __launch_bounds__(kBlock) k_wf_resolve(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, double4* __restrict__ accum,
-    float4* __restrict__ color) {
-  const FrameConst& f = *fcp;
-  const uint32_t rect[4] = {f.rect[0], f.rect[1], f.rect[2], f.rect[3]};
-  uint32_t px, py;
+    float4* __restrict__ color, SceneTable B) {
   const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!tile_pixel(index, rect, px, py)) return;
-  const uint32_t slot = py * f.width + px;
+  uint32_t px, py, slot, scene = 0;
+  if (kBatch) {
+    if (index >= B.total_slots) return;
+    slot = index;
+    scene = table_scene(B, slot);
+    const FrameConst& fb = B.frames[scene];
+    const uint32_t local = slot - B.slot_base[scene];
+    px = local % fb.width;
+    py = local / fb.width;
+    if (!frame_rect_contains(fb, px, py)) return;
+  } else {
+    const uint32_t rect[4] = {fcp->rect[0], fcp->rect[1], fcp->rect[2], fcp->rect[3]};
+    if (!tile_pixel(index, rect, px, py)) return;
+    slot = py * fcp->width + px;
+  }
+  const FrameConst& f = kBatch ? B.frames[scene] : *fcp;
   double4 sum = f.accumulated != 0 ? accum[slot] : make_double4(0.0, 0.0, 0.0, 0.0);
   if (f.add_sample) {
     sum = add4(sum, P.radiance[slot]);
     accum[slot] = sum;
   }
-  color[slot] = resolve_pixel(S, f, px, py, sum);
+  color[slot] = resolve_pixel(kBatch ? B.views[scene] : S, f, px, py, sum);
 }
 
 // Ends a sample: totals the queues' rays and advances the sample index.
@@ -642,6 +691,31 @@ __global__ void k_advance(FrameConst* fc) {
   if (threadIdx.x == 0 && blockIdx.x == 0 && fc->add_sample) {
     fc->sample_index += 1;
     fc->accumulated += 1;
+  }
+}
+
+// A batch's k_wf_finish and k_advance: every scene's camera rays, then every
+// scene's sample index.
+__global__ void k_wf_finish_batch(SceneTable B, const uint32_t* __restrict__ counts, uint32_t max_bounces,
+    RayTotals* totals) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long ext = 0, sh = 0, cam = 0;
+  for (uint32_t b = 0; b <= max_bounces; ++b) {
+    if (b != 0) ext += counts[3 * b];
+    sh += counts[3 * b + 2];
+  }
+  for (uint32_t k = 0; k < B.count; ++k)
+    if (B.frames[k].add_sample) cam += (unsigned long long)B.frames[k].rect[2] * B.frames[k].rect[3];
+  totals->camera += cam;
+  totals->extension += ext;
+  totals->shadow += sh;
+}
+
+__global__ void k_advance_batch(SceneTable B) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < B.count && B.frames[k].add_sample) {
+    B.frames[k].sample_index += 1;
+    B.frames[k].accumulated += 1;
   }
 }
 
@@ -738,38 +812,43 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   uint32_t* fetch = Q.counts + 3 * (size_t)(max_bounces + 2);
   const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid_pixels = (threads + kBlock - 1) / kBlock;
+  const SceneTable none;
   const uint32_t grid_extend = persistent_grid(
-      count ? (const void*)k_wf_extend<true> : (const void*)k_wf_extend<false>, Q.capacity, tuning);
+      count ? (const void*)k_wf_extend<true, false> : (const void*)k_wf_extend<false, false>, Q.capacity, tuning);
   const uint32_t grid_shadow = persistent_grid(
-      count ? (const void*)k_wf_shadow<true> : (const void*)k_wf_shadow<false>, Q.capacity, tuning);
+      count ? (const void*)k_wf_shadow<true, false> : (const void*)k_wf_shadow<false, false>, Q.capacity, tuning);
   // Shading: up to eight waves of resident blocks, grid-striding over
   // longer queues.
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
-      8u * persistent_grid((const void*)k_wf_shade<false>, Q.capacity, TraceTuning()));
+      8u * persistent_grid((const void*)k_wf_shade<false, false>, Q.capacity, TraceTuning()));
   {
     Timed t(profile, stream, 0);
-    if (count) k_wf_camera<true><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, visits);
-    else k_wf_camera<false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, nullptr);
+    if (count) k_wf_camera<true, false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, visits, none);
+    else k_wf_camera<false, false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
   }
   for (uint32_t b = 0; b <= max_bounces; ++b) {
     if (b != 0) {
       Timed t(profile, stream, 1);
       if (count)
-        k_wf_extend<true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill, visits);
+        k_wf_extend<true, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill, visits,
+            none);
       else
-        k_wf_extend<false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill, nullptr);
+        k_wf_extend<false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
+            nullptr, none);
     }
     {
       Timed t(profile, stream, 2);
-      if (C.enabled && b == 1) k_wf_shade<true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C);
-      else k_wf_shade<false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C);
+      if (C.enabled && b == 1) k_wf_shade<true, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
+      else k_wf_shade<false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
     }
     {
       Timed t(profile, stream, 3);
       if (count)
-        k_wf_shadow<true><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, visits);
+        k_wf_shadow<true, false><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, visits,
+            none);
       else
-        k_wf_shadow<false><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, nullptr);
+        k_wf_shadow<false, false><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill,
+            nullptr, none);
     }
   }
   if (C.enabled) {
@@ -787,9 +866,37 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   }
   {
     Timed t(profile, stream, 4);
-    k_wf_resolve<<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, accum, color);
+    k_wf_resolve<false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, accum, color, none);
   }
   k_wf_finish<<<1, 32, 0, stream>>>(const_cast<FrameConst*>(fc), Q.counts, max_bounces, totals);
+}
+
+void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const PathState& P, const Queues& Q,
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream, const TraceTuning& tuning) {
+  if (B.count == 0 || B.total_slots == 0) return;
+  const SceneView none_view{};
+  const FrameConst* no_frame = nullptr;
+  const CacheQueues no_cache;
+  cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * kQueueCounterWords * (size_t)(max_bounces + 2), stream);
+  uint32_t* fetch = Q.counts + 3 * (size_t)(max_bounces + 2);
+  const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
+  const uint32_t grid_slots = (B.total_slots + kBlock - 1) / kBlock;
+  const uint32_t grid_extend = persistent_grid((const void*)k_wf_extend<false, true>, Q.capacity, tuning);
+  const uint32_t grid_shadow = persistent_grid((const void*)k_wf_shadow<false, true>, Q.capacity, tuning);
+  const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
+      8u * persistent_grid((const void*)k_wf_shade<false, true>, Q.capacity, TraceTuning()));
+  k_wf_camera<false, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
+  for (uint32_t b = 0; b <= max_bounces; ++b) {
+    if (b != 0)
+      k_wf_extend<false, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, b, fetch + 2 * b,
+          refill, nullptr, B);
+    k_wf_shade<false, true><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, Q, b, no_cache, B);
+    k_wf_shadow<false, true><<<grid_shadow, kBlock, 0, stream>>>(none_view, P, Q, b, fetch + 2 * b + 1, refill,
+        nullptr, B);
+  }
+  k_wf_resolve<true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, accum, color, B);
+  k_wf_finish_batch<<<1, 32, 0, stream>>>(B, Q.counts, max_bounces, totals);
+  k_advance_batch<<<(B.count + 31) / 32, 32, 0, stream>>>(B);
 }
 
 void launch_advance(FrameConst* fc, cudaStream_t stream) { k_advance<<<1, 32, 0, stream>>>(fc); }

@@ -64,6 +64,17 @@ struct CacheQueues {
   uint32_t* counters = nullptr;
 };
 
+// Several scenes rendered as one wavefront: scene k owns the path slots
+// [slot_base[k], slot_base[k + 1]), in its image's row order, with its own
+// scene view and frame constants (device arrays of `count` entries).
+struct SceneTable {
+  const SceneView* views = nullptr;
+  FrameConst* frames = nullptr;
+  const uint32_t* slot_base = nullptr;  // count + 1 entries
+  uint32_t count = 0;
+  uint32_t total_slots = 0;
+};
+
 // Launch shape of the persistent tracing kernels: a lane takes a new ray
 // when fewer than `refill_below` lanes of its warp still hold one. Zero
 // picks the default.
@@ -110,6 +121,11 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
     SampleProfile* profile = nullptr, const TraceTuning& tuning = TraceTuning(),
     const CacheQueues* cache = nullptr);
+
+// One sample of every scene of a batch, as one set of wavefront launches
+// over all scenes' paths (the wavefront integrator, no radiance cache).
+void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const PathState& P, const Queues& Q,
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream, const TraceTuning& tuning);
 
 void launch_advance(FrameConst* fc, cudaStream_t stream);
 

@@ -77,6 +77,18 @@ def lib():
         L.lotus_cuda_cache_train.restype = C.c_int32
         L.lotus_cuda_cache_train.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                              C.c_void_p]
+        L.lotus_cuda_batch_create.restype = C.c_int32
+        L.lotus_cuda_batch_create.argtypes = [C.POINTER(abi.Options), C.POINTER(C.c_void_p), C.c_char_p,
+                                              C.c_size_t]
+        L.lotus_cuda_batch_destroy.restype = None
+        L.lotus_cuda_batch_destroy.argtypes = [C.c_void_p]
+        L.lotus_cuda_batch_set_scenes.restype = C.c_int32
+        L.lotus_cuda_batch_set_scenes.argtypes = [C.c_void_p, C.POINTER(abi.SceneDesc), C.c_uint32,
+                                                  C.POINTER(abi.SceneResult)]
+        L.lotus_cuda_batch_render.restype = C.c_int32
+        L.lotus_cuda_batch_render.argtypes = [C.c_void_p, C.POINTER(abi.FrameDesc), C.c_uint32,
+                                              C.POINTER(abi.FrameResult), C.POINTER(C.c_void_p),
+                                              C.POINTER(abi.FrameResult)]
         L.lotus_cuda_read_light_table.restype = C.c_int64
         L.lotus_cuda_read_light_table.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64,
                                                   C.c_void_p, C.c_uint64]
@@ -274,6 +286,59 @@ class CudaOffscreenRenderer:
         off = np.zeros(max(ninst, 1), dtype=np.uint32)
         lib().lotus_cuda_read_light_table(self.handle, rec.ctypes.data, n, off.ctypes.data, ninst)
         return rec[:n], off[:ninst]
+
+
+class CudaBatch:
+    """Several scenes rendered as one wavefront (lotus_cuda_batch_*)."""
+
+    def __init__(self, device=0, trace_refill_below=0, trace_blocks_per_sm=0):
+        self.handle = None
+        opts = abi.Options(device=device, flags=0, trace_refill_below=trace_refill_below,
+                           trace_blocks_per_sm=trace_blocks_per_sm)
+        h = C.c_void_p()
+        err = C.create_string_buffer(256)
+        status = lib().lotus_cuda_batch_create(C.byref(opts), C.byref(h), err, 256)
+        if status != abi.PASS:
+            raise RendererError(status, err.value.decode(errors="replace"))
+        self.handle = h
+        self.scenes = []
+
+    def close(self):
+        if self.handle:
+            lib().lotus_cuda_batch_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_scenes(self, scenes):
+        """Builds every scene; returns their lotus_scene_result."""
+        self.scenes = list(scenes)
+        descs = (abi.SceneDesc * len(self.scenes))(*[s.desc() for s in self.scenes])
+        results = (abi.SceneResult * len(self.scenes))()
+        lib().lotus_cuda_batch_set_scenes(self.handle, descs, len(self.scenes), results)
+        return list(results)
+
+    def render(self, frames):
+        """frames[k] renders scene k: (per-scene results, per-scene colours
+        (H, W, 4) or None, the call's total)."""
+        n = len(frames)
+        fa = (abi.FrameDesc * n)(*frames)
+        results = (abi.FrameResult * n)()
+        colors, ptrs = [], (C.c_void_p * n)()
+        for k, f in enumerate(frames):
+            if f.target.read_back:
+                c = np.empty((f.target.height, f.target.width, 4), dtype=np.float32)
+                colors.append(c)
+                ptrs[k] = c.ctypes.data
+            else:
+                colors.append(None)
+        total = abi.FrameResult()
+        lib().lotus_cuda_batch_render(self.handle, fa, n, results, ptrs, C.byref(total))
+        return list(results), colors, total
 
 
 def check(result, what="call"):

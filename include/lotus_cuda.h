@@ -376,6 +376,39 @@ int32_t lotus_cuda_render_static(lotus_cuda_renderer* renderer,
     const lotus_frame_desc* frame, float* color_device, lotus_frame_result* result);
 
 /* ------------------------------------------------------------------------
+ * Batched rendering. No counterpart in the reference: up to
+ * LOTUS_BATCH_MAX_SCENES independent scenes, each with its own target,
+ * rendered as one wavefront (one camera launch over all their pixels, then
+ * per bounce one extension, shading and shadow launch over all their
+ * queued paths), a sample captured as one CUDA graph. Each scene is built
+ * as lotus_cuda_update_scene builds one; each frame renders as
+ * lotus_cuda_render would render it (the same images, bit for bit), with
+ * the wavefront integrator, Bsdf or Mis light sampling and no max_samples. */
+
+#define LOTUS_BATCH_MAX_SCENES 64u
+
+typedef struct lotus_cuda_batch lotus_cuda_batch;
+
+/* options: the device and the persistent kernels' launch shape. */
+int32_t lotus_cuda_batch_create(const lotus_cuda_options* options,
+    lotus_cuda_batch** batch, char* error, size_t error_size);
+
+void lotus_cuda_batch_destroy(lotus_cuda_batch* batch);
+
+/* Replaces the batch's scenes; results[k] (if not NULL) for scene k. */
+int32_t lotus_cuda_batch_set_scenes(lotus_cuda_batch* batch,
+    const lotus_scene_desc* scenes, uint32_t count, lotus_scene_result* results);
+
+/* frames[k] renders scene k (count = the batch's scene count, every
+ * frame_count equal). A scene's accumulation continues while its frame
+ * description is unchanged. results[k] and colors[k] (host memory, W x H x 4
+ * floats, or NULL) are per scene; `total` (if not NULL) holds the rays and
+ * device time of the whole call. */
+int32_t lotus_cuda_batch_render(lotus_cuda_batch* batch,
+    const lotus_frame_desc* frames, uint32_t count, lotus_frame_result* results,
+    float* const* colors, lotus_frame_result* total);
+
+/* ------------------------------------------------------------------------
  * Learned radiance cache. No counterpart in the reference: a hash-grid
  * encoded MLP (five 64-wide ReLU layers, RGB out; BF16 on the tensor cores,
  * FP32 accumulation) trained online on the wavefront path tracer's own
