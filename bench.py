@@ -18,7 +18,9 @@ on a bounded band of the same frame.
 The line's `time_to_relmse` object is the metric's other half (rank 0,
 `--convergence 0` skips it): device seconds until the running image's
 relMSE falls to 1e-3 for plain PT, the learned radiance cache, ReSTIR DI
-and cache + ReSTIR on the many-light box room at 1080p.
+and cache + ReSTIR on the many-light box room at 1080p. Its `batch` object
+(`--batch 0` skips it) times the 64-scene batch workload rendered as one
+wavefront against the same scenes one at a time.
 """
 
 import argparse
@@ -216,6 +218,49 @@ def time_to_relmse_report(renderer_module):
     return out
 
 
+def batch_report(renderer_module, spp=8, depth=8):
+    """Config 4: the 64-scene batch workload (scenes.batch_workload: traced
+    triangles log-uniform in [1e4, 2e6], 256^2 .. 1024^2 targets), 8 spp,
+    depth 8, rendered as one wavefront per sample under a CUDA graph with
+    the tuner's launch shape, against the same scenes rendered one after
+    another by one renderer. Device time only (CUDA events)."""
+    from hydra_lotus_b200 import autotune
+    work = scenes.batch_workload(64, seed=0)
+
+    def st(k, first=0):
+        return abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                                    max_bounces=depth, sample_index=first + 1000 * k)
+
+    out = {"scenes": len(work), "pixels": sum(s.width * s.height for s in work),
+           "traced_triangles": sum(s.traced_triangle_count for s in work), "spp": spp, "depth": depth}
+    with renderer_module.CudaBatch(0) as batch:
+        res = batch.set_scenes(work)
+        if any(r.status != abi.PASS for r in res):
+            return {"error": [r.detail.decode() for r in res if r.status != abi.PASS][0]}
+        frames = [s.frame(st(k), frame_count=spp, read_back=False) for k, s in enumerate(work)]
+        best, times = autotune.tune_batch(batch, frames)
+        out["tuned"] = {"refill_below": best[0], "blocks_per_sm": best[1],
+                        "candidates_ms_per_sample": {f"{r}/{b}": round(t, 3) for (r, b), t in times.items()}}
+        frames = [s.frame(st(k, 7), frame_count=spp, read_back=False) for k, s in enumerate(work)]
+        _, _, total = batch.render(frames)
+        renderer_module.check(total, "batch")
+        rays = total.camera_rays + total.extension_rays + total.shadow_rays
+        out["batched"] = {"ms": round(total.gpu_ms, 2), "mrays_per_s": round(rays / total.gpu_ms / 1e3, 1),
+                          "scene_samples_per_s": round(len(work) * spp / (total.gpu_ms * 1e-3), 1)}
+    seq_ms, seq_rays = 0.0, 0
+    with renderer_module.CudaOffscreenRenderer(0, trace_refill_below=best[0], trace_blocks_per_sm=best[1]) as r:
+        for k, s in enumerate(work):
+            renderer_module.check(r.update_scene(s), "update_scene")
+            f = s.frame(st(k, 7), frame_count=spp, read_back=False)
+            res, _ = r.render_scene(f)
+            renderer_module.check(res, "sequential")
+            seq_ms += res.gpu_ms
+            seq_rays += res.camera_rays + res.extension_rays + res.shadow_rays
+    out["sequential"] = {"ms": round(seq_ms, 2), "mrays_per_s": round(seq_rays / seq_ms / 1e3, 1)}
+    out["speedup_batched_vs_sequential"] = round(seq_ms / out["batched"]["ms"], 3)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -223,6 +268,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--batch", type=int, default=1,
+                    help="1: also measure the 64-scene batch (config 4), batched vs one scene at a time")
     ap.add_argument("--convergence", type=int, default=1,
                     help="1: also measure time to relMSE 1e-3 (plain PT, cache, ReSTIR, cache+ReSTIR)")
     args = ap.parse_args()
@@ -378,6 +425,8 @@ def main():
         }
         if args.convergence:
             line["time_to_relmse"] = time_to_relmse_report(renderer)
+        if args.batch:
+            line["batch"] = batch_report(renderer)
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:

@@ -158,6 +158,18 @@ extern "C" void lotus_cuda_batch_destroy(lotus_cuda_batch* b) {
   delete b;
 }
 
+extern "C" int32_t lotus_cuda_batch_set_tuning(lotus_cuda_batch* b, uint32_t refill_below, uint32_t blocks_per_sm) {
+  if (!b || refill_below > 32 || blocks_per_sm > 64) return LOTUS_FAIL;
+  b->tuning.refill_below = refill_below;
+  b->tuning.blocks_per_sm = blocks_per_sm;
+  if (b->graph) {
+    cudaSetDevice(b->device);
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return LOTUS_PASS;
+}
+
 extern "C" int32_t lotus_cuda_batch_set_scenes(lotus_cuda_batch* b, const lotus_scene_desc* scenes, uint32_t count,
     lotus_scene_result* results) {
   if (!b || (!scenes && count)) return LOTUS_FAIL;

@@ -535,6 +535,52 @@ def box_room_wide(seed=0, width=1920, height=1080, emitters=0):
     return s
 
 
+def batch_room(seed=0, triangles=100_000, size=256):
+    """A config-1-style scene of about ``triangles`` traced triangles: the
+    seeded box room (walls, two boxes, ceiling light) filled with small
+    instanced, Perlin-displaced icospheres (four prototypes of subdivision
+    4, 5120 triangles each) in equal thirds Lambert, GGX conductor and
+    smooth dielectric; the Cornell camera on a size x size target."""
+    rng = np.random.default_rng(seed + 7000)
+    s = box_room(seed=seed, size=size)
+    s.name = f"batch-room-{seed}-{triangles}"
+    protos = []
+    for k in range(4):
+        v, f = icosphere(4)
+        r = 1.0 + 0.25 * perlin3(v * rng.uniform(1.5, 3.0) + rng.uniform(-100, 100, 3), seed * 131 + k)
+        p = (v * r[:, None]).astype(F32)
+        protos.append(s.add_geometry(p, f, corner_normals(p, f)))
+    count = max(1, int(round((triangles - 36) / 5120.0)))
+    radius = min(0.15, 0.6 / max(1.0, count ** (1.0 / 3.0)))
+    for n in range(count):
+        kind = n % 3
+        if kind == 0:
+            mat = preview_material(tuple(rng.uniform(0.1, 0.8, 3)), roughness=0.6, ior=1.0)
+        elif kind == 1:
+            mat = preview_material(tuple(rng.uniform(0.5, 1.0, 3)), roughness=rng.uniform(0.02, 0.8),
+                                   metallic=1.0)
+        else:
+            mat = preview_material((1.0, 1.0, 1.0), roughness=0.0, ior=1.5, transmission=1.0)
+        rad = radius * rng.uniform(0.5, 1.0)
+        pos = tuple(rng.uniform(-0.95 + rad, 0.95 - rad, 3))
+        s.add_instance(protos[n % 4], s.add_material(mat),
+                       affine(rotation_y(rng.uniform(0, 2 * math.pi)) * rad, pos))
+    return s
+
+
+def batch_workload(count=64, seed=0):
+    """Config 4: ``count`` independent batch rooms, traced triangles
+    log-uniform in [1e4, 2e6], resolutions uniform over 256^2, 512^2, 768^2
+    and 1024^2 (seeded)."""
+    rng = np.random.default_rng(seed + 4000)
+    out = []
+    for k in range(count):
+        tris = int(math.exp(rng.uniform(math.log(1e4), math.log(2e6))))
+        size = int(rng.choice([256, 512, 768, 1024]))
+        out.append(batch_room(seed=seed * 1000 + k, triangles=tris, size=size))
+    return out
+
+
 def big_mesh(seed=0, size=96, subdivisions=6):
     """One displaced icosphere of 20 * 4^subdivisions triangles (81,920 at
     6, above the per-CTA SAH builder's limit, so it builds as an LBVH) with

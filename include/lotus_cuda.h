@@ -399,6 +399,11 @@ void lotus_cuda_batch_destroy(lotus_cuda_batch* batch);
 int32_t lotus_cuda_batch_set_scenes(lotus_cuda_batch* batch,
     const lotus_scene_desc* scenes, uint32_t count, lotus_scene_result* results);
 
+/* The persistent kernels' launch shape (as lotus_cuda_options' trace_*
+ * fields; 0 picks the default), for a tuner. */
+int32_t lotus_cuda_batch_set_tuning(lotus_cuda_batch* batch,
+    uint32_t trace_refill_below, uint32_t trace_blocks_per_sm);
+
 /* frames[k] renders scene k (count = the batch's scene count, every
  * frame_count equal). A scene's accumulation continues while its frame
  * description is unchanged. results[k] and colors[k] (host memory, W x H x 4
