@@ -24,7 +24,25 @@ def main():
     ap.add_argument("--depth", type=int, default=8)
     ap.add_argument("--integrator", default="wavefront", choices=["wavefront", "reference"])
     ap.add_argument("--cache", action="store_true", help="paths end into the learned radiance cache")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="render the first N scenes of the 64-scene batch workload as one wavefront")
     args = ap.parse_args()
+    if args.batch:
+        work = scenes.batch_workload(64, seed=0)[:args.batch]
+        with renderer.CudaBatch(0) as b:
+            for r in b.set_scenes(work):
+                renderer.check(r, "batch scene")
+            for k in range(args.frames):
+                frames = [s.frame(abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT,
+                                                       light_sampling=abi.LIGHT_SAMPLING_MIS, max_bounces=args.depth,
+                                                       sample_index=1000 * i + k * args.spp),
+                                  frame_count=args.spp, read_back=False) for i, s in enumerate(work)]
+                _, _, total = b.render(frames)
+                renderer.check(total, "batch render")
+                rays = total.camera_rays + total.extension_rays + total.shadow_rays
+                print(json.dumps({"frame": k, "rays": rays, "gpu_ms": round(total.gpu_ms, 3),
+                                  "mrays_per_s": round(rays / total.gpu_ms / 1e3, 1)}))
+        return
     if args.workload == "sphere-field":
         scene = scenes.sphere_field(seed=0, width=args.width, height=args.height)
     else:
