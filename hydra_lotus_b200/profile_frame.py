@@ -24,9 +24,32 @@ def main():
     ap.add_argument("--depth", type=int, default=8)
     ap.add_argument("--integrator", default="wavefront", choices=["wavefront", "reference"])
     ap.add_argument("--cache", action="store_true", help="paths end into the learned radiance cache")
+    ap.add_argument("--temporal", action="store_true",
+                    help="temporal frames of the many-light room: ReSTIR DI (temporal + spatial) and SVGF")
     ap.add_argument("--batch", type=int, default=0,
                     help="render the first N scenes of the 64-scene batch workload as one wavefront")
     args = ap.parse_args()
+    if args.temporal:
+        scene = scenes.restir_room(seed=0, size=args.height, emitters=10000, aspect=args.width / args.height)
+        st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT,
+                                  light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL, max_bounces=args.depth,
+                                  sample_index=0, restir_candidates=8, restir_temporal=1,
+                                  restir_max_history_candidates=20, restir_spatial=1, restir_spatial_radius=30)
+        previous = None
+        with renderer.CudaOffscreenRenderer(0) as r:
+            renderer.check(r.update_scene(scene), "update_scene")
+            for k in range(args.frames):
+                view, w2c = scenes.orbit_camera(k, frames=120, aspect=args.width / args.height)
+                frame = abi.make_frame(w2c, args.width, args.height, st, 1, read_back=False)
+                d = abi.temporal_desc(frame, view, previous[0] if previous else None,
+                                      previous[1] if previous else None, history_available=k > 0,
+                                      accumulate_radiance=True, max_history_samples=5, filter_iterations=5)
+                res, _ = r.render_temporal(d)
+                renderer.check(res, "render_temporal")
+                previous = (view, w2c)
+                rays = res.camera_rays + res.extension_rays + res.shadow_rays
+                print(json.dumps({"frame": k, "rays": rays, "gpu_ms": round(res.gpu_ms, 3)}))
+        return
     if args.batch:
         work = scenes.batch_workload(64, seed=0)[:args.batch]
         with renderer.CudaBatch(0) as b:
