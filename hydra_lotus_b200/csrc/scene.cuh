@@ -6,10 +6,10 @@
 // 424-460 in hydra-lotus) become a two-level BVH walk:
 //   - one BLAS per geometry in object space, one TLAS over the instances'
 //     world boxes; all BLAS nodes share one pool and all triangles another;
-//   - 64-byte nodes holding both children's boxes by axis, so one node is
-//     four 16-byte loads and tests both children;
-//   - triangles stored in leaf order as three float4 corners (48 bytes),
-//     the original primitive index in the first corner's w;
+//   - 128-byte 4-wide nodes holding the children's boxes by axis and
+//     bound, so one node is seven 16-byte loads and tests four children;
+//   - triangles stored in leaf order as three float4 corners in a 64-byte
+//     record, the original primitive index in the first corner's w;
 //   - instance records split by use: a traversal record (object-from-world
 //     rows, BLAS root, flags) and a shading record (world-from-object rows,
 //     material, light-table offset, normals).
@@ -127,7 +127,6 @@ struct SceneView {
 struct Hit {
   uint32_t instance;
   uint32_t tri;        // leaf-ordered triangle-pool index
-  uint32_t primitive;  // the geometry's own triangle index
   float b1, b2;
   float t;
 };
@@ -153,7 +152,7 @@ __device__ __forceinline__ F3 safe_inverse(F3 d) {
 
 struct WatertightRay {
   F3 org;
-  int kx, ky, kz;
+  uint32_t axes;  // kx | ky << 2 | kz << 4
   float sx, sy, sz;
 };
 
@@ -161,31 +160,33 @@ __device__ __forceinline__ WatertightRay prepare_ray(F3 org, F3 dir) {
   WatertightRay w;
   w.org = org;
   const float ax = fabsf(dir.x), ay = fabsf(dir.y), az = fabsf(dir.z);
-  w.kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
-  w.kx = w.kz == 2 ? 0 : w.kz + 1;
-  w.ky = w.kx == 2 ? 0 : w.kx + 1;
-  if (component(dir, w.kz) < 0.0f) {
-    const int s = w.kx;
-    w.kx = w.ky;
-    w.ky = s;
+  const int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  int kx = kz == 2 ? 0 : kz + 1;
+  int ky = kx == 2 ? 0 : kx + 1;
+  if (component(dir, kz) < 0.0f) {
+    const int s = kx;
+    kx = ky;
+    ky = s;
   }
-  const float dz = component(dir, w.kz);
-  w.sx = component(dir, w.kx) / dz;
-  w.sy = component(dir, w.ky) / dz;
+  const float dz = component(dir, kz);
+  w.axes = (uint32_t)kx | (uint32_t)ky << 2 | (uint32_t)kz << 4;
+  w.sx = component(dir, kx) / dz;
+  w.sy = component(dir, ky) / dz;
   w.sz = 1.0f / dz;
   return w;
 }
 
 __device__ __forceinline__ bool intersect_triangle(const WatertightRay& r, F3 v0, F3 v1, F3 v2,
     float& t, float& b1, float& b2) {
+  const int kx = r.axes & 3u, ky = (r.axes >> 2) & 3u, kz = r.axes >> 4;
   const F3 A = v0 - r.org, B = v1 - r.org, C = v2 - r.org;
-  const float Akz = component(A, r.kz), Bkz = component(B, r.kz), Ckz = component(C, r.kz);
-  const float Ax = component(A, r.kx) - r.sx * Akz;
-  const float Ay = component(A, r.ky) - r.sy * Akz;
-  const float Bx = component(B, r.kx) - r.sx * Bkz;
-  const float By = component(B, r.ky) - r.sy * Bkz;
-  const float Cx = component(C, r.kx) - r.sx * Ckz;
-  const float Cy = component(C, r.ky) - r.sy * Ckz;
+  const float Akz = component(A, kz), Bkz = component(B, kz), Ckz = component(C, kz);
+  const float Ax = component(A, kx) - r.sx * Akz;
+  const float Ay = component(A, ky) - r.sy * Akz;
+  const float Bx = component(B, kx) - r.sx * Bkz;
+  const float By = component(B, ky) - r.sy * Bkz;
+  const float Cx = component(C, kx) - r.sx * Ckz;
+  const float Cy = component(C, ky) - r.sy * Ckz;
   float U = Cx * By - Cy * Bx;
   float W1 = Ax * Cy - Ay * Cx;
   float W2 = Bx * Ay - By * Ax;
@@ -268,7 +269,7 @@ struct Walk {
   F3 inv;                // 1 / direction in the current space
   WatertightRay w;       // the ray in the current space (w.org its origin)
   float tmin, best, transmittance;
-  uint32_t instance, best_instance, best_prim, best_tri;
+  uint32_t instance, best_instance, best_tri;
   float b1, b2;
   int32_t cur;           // the next reference to process, or kWalkDone
   int32_t leaf;          // a postponed BLAS leaf, or 0
@@ -306,7 +307,6 @@ __device__ __forceinline__ Hit walk_hit(const Walk& W) {
   Hit h;
   h.instance = W.best_instance;
   h.tri = W.best_tri;
-  h.primitive = W.best_prim;
   h.b1 = W.b1;
   h.b2 = W.b2;
   h.t = W.best;
@@ -381,7 +381,8 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
       if (coverage > 0.0f) W.transmittance *= 1.0f - coverage;
     } else {
       if (W.found && t == W.best &&
-          (W.instance > W.best_instance || (W.instance == W.best_instance && prim >= W.best_prim)))
+          (W.instance > W.best_instance ||
+           (W.instance == W.best_instance && prim >= __float_as_uint(S.tris[kTriStride * (size_t)W.best_tri].w))))
         continue;
       if (!W.opaque) {
         const float coverage = instance_coverage(S, W.instance);
@@ -391,7 +392,6 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
       W.found = true;
       W.best = t;
       W.best_instance = W.instance;
-      W.best_prim = prim;
       W.best_tri = first + k;
       W.b1 = b1;
       W.b2 = b2;
@@ -454,20 +454,29 @@ __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 dire
   return kAnyHit ? W.transmittance : 0.0f;
 }
 
+// Interior-node steps of a round stop once fewer lanes than this are at an
+// interior node while others wait with other work: the remaining lanes
+// carry their nodes into the next round instead of running the step
+// nearly alone.
+constexpr int kRoundNodeLanes = 8;
+
 // One round of a warp's walks (for persistent kernels; every lane of the
 // warp calls it, `active` lanes hold a walk). Interior nodes first, each
 // lane postponing the first BLAS leaf it meets and carrying on, until no
-// lane is left at an interior node; then every postponed leaf is tested,
-// and finally each lane's exit marker, further leaf or instance entry.
-// Each kind of work thus runs once per round over all the lanes that have
-// it. Returns true for a lane whose walk has ended.
+// lane is left at an interior node, or fewer than kRoundNodeLanes are and
+// another lane has other work; then every postponed leaf is tested, and
+// finally each lane not at an interior node takes its exit marker, further
+// leaf or instance entry. Each kind of work thus runs once per round over
+// all the lanes that have it. Returns true for a lane whose walk has ended.
 template <bool kAnyHit, bool kCount>
 __device__ __forceinline__ bool walk_round(const SceneView& S, Walk& W, WalkStack& stack, uint32_t& rng,
     bool active, TraversalCounters* counters) {
   constexpr unsigned kAll = 0xFFFFFFFFu;
   for (;;) {
     const bool node = active && walk_at_node(W);
-    if (!__any_sync(kAll, node)) break;
+    const unsigned at_node = __ballot_sync(kAll, node);
+    if (at_node == 0) break;
+    if (__popc(at_node) < kRoundNodeLanes && __any_sync(kAll, active && !node)) break;
     if (node) {
       walk_visit_node<kCount>(S, W, stack, counters);
       if (W.in_blas && W.cur < 0 && W.leaf == 0) {
@@ -482,7 +491,7 @@ __device__ __forceinline__ bool walk_round(const SceneView& S, Walk& W, WalkStac
     ended = walk_test_leaf<kAnyHit, kCount>(S, W, W.leaf, rng, counters);
     W.leaf = 0;
   }
-  if (active && !ended && W.cur != kWalkDone)
+  if (active && !ended && W.cur != kWalkDone && !walk_at_node(W))
     ended = walk_other<kAnyHit, kCount>(S, W, stack, rng, counters);
   return active && (ended || (W.cur == kWalkDone && W.leaf == 0));
 }
