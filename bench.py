@@ -82,7 +82,8 @@ class ClockSampler:
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+              "clocks.mem,clocks.max.mem,utilization.gpu")
 
     def __init__(self, device):
         self.device = device
@@ -112,7 +113,7 @@ class ClockSampler:
         self.file.seek(0)
         rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
         os.unlink(self.file.name)
-        sm, mx, reasons = [], None, set()
+        sm, mem, util, mx, mem_mx, reasons = [], [], [], None, None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             try:
@@ -121,12 +122,19 @@ class ClockSampler:
                 for name, v in zip(names, r[5:9]):
                     if v.strip() == "Active":
                         reasons.add(name)
+                mem.append(float(r[9]))
+                mem_mx = float(r[10])
+                util.append(float(r[11]))
             except (ValueError, IndexError):
                 continue
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+               "samples": len(sm)}
+        if mem:
+            out.update({"mem_mhz": statistics.median(mem), "mem_max_mhz": mem_mx,
+                        "gpu_util_pct": statistics.median(util) if util else None})
+        return out
 
 
 def cpu_baseline(scene, seconds, rows=64):
@@ -320,10 +328,12 @@ def main():
         start = torch.cuda.Event(enable_timing=True)
         stop = torch.cuda.Event(enable_timing=True)
         start.record(stream)
+        step_ms = []
         for _ in range(args.steps):
             res, _ = r.render_scene(frame())
             renderer.check(res, "render")
             rays += res.camera_rays + res.extension_rays + res.shadow_rays
+            step_ms.append(res.gpu_ms)
         stop.record(stream)
         torch.cuda.synchronize()
     barrier()
@@ -422,6 +432,11 @@ def main():
             },
             "cpu_baseline": cpu,
             "clocks": clock,
+            # The renderer's own per-step device times (its events around each
+            # frame's samples): a spread far above the median means the GPU
+            # was shared or throttled during the timed region.
+            "step_gpu_ms": {"min": round(min(step_ms), 2), "median": round(statistics.median(step_ms), 2),
+                            "max": round(max(step_ms), 2)},
         }
         if args.convergence:
             line["time_to_relmse"] = time_to_relmse_report(renderer)

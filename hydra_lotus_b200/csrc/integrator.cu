@@ -352,7 +352,18 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
     uint32_t rng;
     start_path(f, px, py, f.sample_index, o, d, tmax, rng);
     Hit hit;
-    found = trace_closest<kCount>(SS, o, d, 0.0f, tmax, rng, hit, &vc);
+    if (!kBatch && f.primary_hit != nullptr && f.sample_index == f.primary_sample) {
+      // The same camera ray's hit, traced by a pass earlier in the frame.
+      const uint4 ph = f.primary_hit[slot];
+      found = ph.x != kNoPrimaryHit;
+      hit.instance = ph.x;
+      hit.tri = ph.y;
+      hit.b1 = __uint_as_float(ph.z);
+      hit.b2 = __uint_as_float(ph.w);
+      rng = f.primary_rng[slot];
+    } else {
+      found = trace_closest<kCount>(SS, o, d, 0.0f, tmax, rng, hit, &vc);
+    }
     if (found) {
       P.direction[slot] = F4(d, tmax);
       P.radiance[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(rng));

@@ -419,6 +419,8 @@ struct Renderer {
     DeviceArray<RestirReuse> spatial;
     DeviceArray<uint4> sources;
     DeviceArray<RestirSurface> surfaces[2];
+    DeviceArray<uint4> primary_hit;     // the camera rays' hits, traced once per frame
+    DeviceArray<uint32_t> primary_rng;
     DeviceArray<TemporalConst> constants;
     DeviceArray<TemporalInstance> instances;
     bool instances_custom = false;
@@ -1475,7 +1477,8 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
           R.ok(T.reuse[1].resize(n), "reservoirs", detail) && R.ok(T.spatial.resize(n), "reservoirs", detail) &&
           R.ok(T.sources.resize(n), "reservoirs", detail) &&
           R.ok(T.surfaces[0].resize(n), "reservoir surfaces", detail) &&
-          R.ok(T.surfaces[1].resize(n), "reservoir surfaces", detail);
+          R.ok(T.surfaces[1].resize(n), "reservoir surfaces", detail) &&
+          R.ok(T.primary_hit.resize(n), "primary hits", detail) && R.ok(T.primary_rng.resize(n), "primary hits", detail);
   if (!okb) return poison(detail);
   // The transport key: a change drops the history (vulkan_backend.cpp:1766-1781).
   uint32_t key[16] = {st.integrator, st.light_sampling, st.restir_proposal, st.restir_candidates,
@@ -1528,6 +1531,13 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   const int sw = T.surface_write, rs = T.restir_write, rw = T.radiance_write;
   if (restir) {
     fc.restir_primary = 1;
+    if (st.restir_candidates != 0) {
+      // The initial pass traces the first sample's camera rays; the
+      // temporal pass and the path tracer's camera step reuse its hits.
+      fc.primary_hit = T.primary_hit.ptr;
+      fc.primary_rng = T.primary_rng.ptr;
+      fc.primary_sample = fc.sample_index;
+    }
     if (st.restir_spatial) {
       fc.restir_final = reinterpret_cast<const unsigned char*>(T.spatial.ptr);
       fc.restir_stride = sizeof(RestirReuse);
@@ -1549,11 +1559,12 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   launch_temporal_surface(R.view, R.frame_const.ptr, T.constants.ptr, T.instances.ptr, T.surface[sw].ptr, pixels, s);
   launch_reproject(T.constants.ptr, T.surface[sw].ptr, T.surface[1 - sw].ptr, T.validity.ptr, pixels, s);
   if (restir) {
-    launch_restir_initial(R.view, R.frame_const.ptr, T.constants.ptr, T.initial.ptr, pixels, s);
+    launch_restir_initial(R.view, R.frame_const.ptr, T.constants.ptr, T.initial.ptr, T.primary_hit.ptr,
+        T.primary_rng.ptr, pixels, s);
     if (reservoirs)
-      launch_restir_temporal(R.view, R.frame_const.ptr, T.constants.ptr, T.instances.ptr, T.initial.ptr,
-          T.validity.ptr, T.surface[sw].ptr, T.reuse[1 - rs].ptr, T.surfaces[1 - rs].ptr, T.reuse[rs].ptr,
-          T.surfaces[rs].ptr, pixels, s);
+      launch_restir_temporal(R.view, R.frame_const.ptr, T.constants.ptr, T.primary_hit.ptr, T.instances.ptr,
+          T.initial.ptr, T.validity.ptr, T.surface[sw].ptr, T.reuse[1 - rs].ptr, T.surfaces[1 - rs].ptr,
+          T.reuse[rs].ptr, T.surfaces[rs].ptr, pixels, s);
     if (st.restir_spatial)
       launch_restir_spatial(R.view, R.frame_const.ptr, T.constants.ptr, T.reuse[rs].ptr, T.surfaces[rs].ptr,
           T.spatial.ptr, T.sources.ptr, pixels, s);

@@ -29,6 +29,10 @@ __device__ __forceinline__ bool finite4(float4 v) {
   return isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w);
 }
 
+// The ReSTIR passes are latency-bound (light and triangle loads, shadow
+// rays): six resident blocks per SM hide more of it than registers save.
+constexpr int kRestirBlocksPerSm = 6;
+
 // ---------------------------------------------------------------------------
 // WriteTemporalSurface (temporal.slang:557-627): the pixel centre's primary
 // hit, with a fixed coverage sequence (sample 0).
@@ -239,9 +243,9 @@ __device__ __forceinline__ RestirPixel empty_restir_pixel() {
 // WriteInitialReservoir (restir.slang:163-233): M candidates streamed over
 // the light table at the jittered camera surface, then one shadow ray for
 // the selected sample.
-__global__ void __launch_bounds__(kBlock) k_restir_initial(SceneView S,
+__global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
-    RestirPixel* __restrict__ out) {
+    RestirPixel* __restrict__ out, uint4* __restrict__ primary_hit, uint32_t* __restrict__ primary_rng) {
   const FrameConst& f = *fcp;
   const TemporalConst& tc = *tcp;
   uint32_t px, py;
@@ -255,7 +259,11 @@ __global__ void __launch_bounds__(kBlock) k_restir_initial(SceneView S,
     uint32_t camera_rng;
     start_path(f, px, py, f.sample_index, ro, rd, tmax, camera_rng);
     Hit hit;
-    if (trace_closest(S, ro, rd, 0.0f, tmax, camera_rng, hit)) {
+    const bool found = trace_closest(S, ro, rd, 0.0f, tmax, camera_rng, hit);
+    primary_hit[slot] = found ? make_uint4(hit.instance, hit.tri, __float_as_uint(hit.b1), __float_as_uint(hit.b2))
+                              : make_uint4(kNoPrimaryHit, 0u, 0u, 0u);
+    primary_rng[slot] = camera_rng;
+    if (found) {
       r.flags |= 1u;
       const SurfaceHit sh = reconstruct_hit(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
       const Frame basis = make_frame(sh.shading_normal);
@@ -303,9 +311,9 @@ __global__ void __launch_bounds__(kBlock) k_restir_initial(SceneView S,
 }
 
 // WriteTemporalReservoir (restir.slang:302-387).
-__global__ void __launch_bounds__(kBlock) k_restir_temporal(SceneView S,
+__global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
-    const TemporalInstance* __restrict__ identities, const RestirPixel* __restrict__ initial,
+    const uint4* __restrict__ primary_hit, const TemporalInstance* __restrict__ identities, const RestirPixel* __restrict__ initial,
     const ValidityPixel* __restrict__ validity, const TemporalPixel* __restrict__ surface,
     const RestirReuse* __restrict__ previous, const RestirSurface* __restrict__ previous_surfaces,
     RestirReuse* __restrict__ out, RestirSurface* __restrict__ out_surfaces) {
@@ -326,9 +334,10 @@ __global__ void __launch_bounds__(kBlock) k_restir_temporal(SceneView S,
     float tmax;
     uint32_t camera_rng;
     start_path(f, px, py, f.sample_index, ro, rd, tmax, camera_rng);
-    Hit hit;
-    if (trace_closest(S, ro, rd, 0.0f, tmax, camera_rng, hit)) {
-      const SurfaceHit sh = reconstruct_hit(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
+    // The camera ray's hit as the initial pass traced it.
+    const uint4 ph = primary_hit[slot];
+    if (ph.x != kNoPrimaryHit) {
+      const SurfaceHit sh = reconstruct_hit(S, ph.x, ph.y, __uint_as_float(ph.z), __uint_as_float(ph.w), rd);
       const Frame basis = make_frame(sh.shading_normal);
       const F3 wo = basis.to_local(-rd);
       const F3 origin = offset_ray_origin(sh.position, sh.normal);
@@ -338,8 +347,8 @@ __global__ void __launch_bounds__(kBlock) k_restir_temporal(SceneView S,
       receiver.shading_normal = F4(sh.shading_normal, 0.0f);
       receiver.outgoing = F4(wo, 0.0f);
       store_closure(sh.bsdf, receiver);
-      receiver.instance_id = identities[hit.instance].instance_id;
-      receiver.material_id = identities[hit.instance].material_id;
+      receiver.instance_id = identities[ph.x].instance_id;
+      receiver.material_id = identities[ph.x].material_id;
       const ValidityPixel v = validity[slot];
       const uint32_t previous_index = v.previous_index;
       const bool history = v.valid != 0 && surface[slot].instance_id == receiver.instance_id &&
@@ -412,7 +421,7 @@ __device__ __forceinline__ bool spatial_compatible(const RestirSurface& receiver
 
 // WriteSpatialReservoir (restir.slang:402-491): four axis neighbours at
 // the radius, merged with support correction.
-__global__ void __launch_bounds__(kBlock) k_restir_spatial(SceneView S,
+__global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     const RestirReuse* __restrict__ temporal, const RestirSurface* __restrict__ surfaces,
     RestirReuse* __restrict__ out, uint4* __restrict__ out_sources) {
@@ -747,15 +756,16 @@ void launch_reproject(const TemporalConst* tc, const TemporalPixel* current, con
 }
 
 void launch_restir_initial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
-    RestirPixel* out, uint32_t pixels, cudaStream_t s) {
-  k_restir_initial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out);
+    RestirPixel* out, uint4* primary_hit, uint32_t* primary_rng, uint32_t pixels, cudaStream_t s) {
+  k_restir_initial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out, primary_hit, primary_rng);
 }
 
 void launch_restir_temporal(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
-    const TemporalInstance* ids, const RestirPixel* initial, const ValidityPixel* validity,
+    const uint4* primary_hit, const TemporalInstance* ids, const RestirPixel* initial,
+    const ValidityPixel* validity,
     const TemporalPixel* surface, const RestirReuse* previous, const RestirSurface* previous_surfaces,
     RestirReuse* out, RestirSurface* out_surfaces, uint32_t pixels, cudaStream_t s) {
-  k_restir_temporal<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, ids, initial, validity, surface, previous,
+  k_restir_temporal<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, primary_hit, ids, initial, validity, surface, previous,
       previous_surfaces, out, out_surfaces);
 }
 

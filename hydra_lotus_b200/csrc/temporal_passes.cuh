@@ -13,11 +13,14 @@ void launch_temporal_surface(const SceneView& S, const FrameConst* fc, const Tem
 void launch_reproject(const TemporalConst* tc, const TemporalPixel* current, const TemporalPixel* previous,
     ValidityPixel* out, uint32_t pixels, cudaStream_t s);
 
+// The initial reservoirs; each pixel's camera-ray hit and random state go
+// to primary_hit / primary_rng for the passes after it.
 void launch_restir_initial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
-    RestirPixel* out, uint32_t pixels, cudaStream_t s);
+    RestirPixel* out, uint4* primary_hit, uint32_t* primary_rng, uint32_t pixels, cudaStream_t s);
 
 void launch_restir_temporal(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
-    const TemporalInstance* ids, const RestirPixel* initial, const ValidityPixel* validity,
+    const uint4* primary_hit, const TemporalInstance* ids, const RestirPixel* initial,
+    const ValidityPixel* validity,
     const TemporalPixel* surface, const RestirReuse* previous, const RestirSurface* previous_surfaces,
     RestirReuse* out, RestirSurface* out_surfaces, uint32_t pixels, cudaStream_t s);
 

@@ -261,6 +261,9 @@ __device__ __forceinline__ float emitter_pdf(const SceneView& S, uint32_t instan
   return S.lights[first + primitive].pdf / area;
 }
 
+// A primary-hit record's instance for a camera ray that hit nothing.
+constexpr uint32_t kNoPrimaryHit = 0xFFFFFFFFu;
+
 // The frame's camera and target, set per RenderScene call; sample_index
 // and accumulated advance on the device between samples.
 struct FrameConst {
@@ -280,6 +283,13 @@ struct FrameConst {
   uint32_t restir_primary;
   uint32_t restir_stride;
   const unsigned char* restir_final;
+  // The primary hits of sample `primary_sample`, when a pass before it
+  // (ReSTIR's initial reservoirs) traced the same camera rays: per pixel
+  // (instance, triangle, b1, b2), instance ~0 for a miss, and the path's
+  // random state after the trace. Null otherwise.
+  const uint4* primary_hit;
+  const uint32_t* primary_rng;
+  uint32_t primary_sample;
 };
 
 // CameraRay (scene.slang:273-283).

@@ -3,7 +3,8 @@
     python -m hydra_lotus_b200.profile_frame --workload sphere-field \
         --width 960 --height 540 --spp 1 --frames 2
 
-Prints the rays and device time of each frame. Used as the command under
+Prints the rays, device time and paths per bounce (the extension
+kernel's rays at bounces 1 and up) of each frame. Used as the command under
 Nsight Compute: the workload's sizes are arguments so that a capture can
 run on a small case of the same kernels.
 """
@@ -26,6 +27,7 @@ def main():
     ap.add_argument("--cache", action="store_true", help="paths end into the learned radiance cache")
     ap.add_argument("--temporal", action="store_true",
                     help="temporal frames of the many-light room: ReSTIR DI (temporal + spatial) and SVGF")
+    ap.add_argument("--filter", type=int, default=5, help="a-trous iterations of the temporal frames")
     ap.add_argument("--batch", type=int, default=0,
                     help="render the first N scenes of the 64-scene batch workload as one wavefront")
     args = ap.parse_args()
@@ -38,12 +40,15 @@ def main():
         previous = None
         with renderer.CudaOffscreenRenderer(0) as r:
             renderer.check(r.update_scene(scene), "update_scene")
+            if args.cache:
+                r.configure_cache(enable=True, seed=1)
             for k in range(args.frames):
                 view, w2c = scenes.orbit_camera(k, frames=120, aspect=args.width / args.height)
                 frame = abi.make_frame(w2c, args.width, args.height, st, 1, read_back=False)
                 d = abi.temporal_desc(frame, view, previous[0] if previous else None,
                                       previous[1] if previous else None, history_available=k > 0,
-                                      accumulate_radiance=True, max_history_samples=5, filter_iterations=5)
+                                      accumulate_radiance=True, max_history_samples=5,
+                                      filter_iterations=args.filter)
                 res, _ = r.render_temporal(d)
                 renderer.check(res, "render_temporal")
                 previous = (view, w2c)
@@ -81,8 +86,10 @@ def main():
             res, _ = r.render_scene(scene.frame(st, frame_count=args.spp, read_back=False))
             renderer.check(res, "render")
             rays = res.camera_rays + res.extension_rays + res.shadow_rays
+            counts = [res.wavefront_path_counts[b] for b in range(res.wavefront_path_count_size)]
             print(json.dumps({"frame": k, "rays": rays, "gpu_ms": round(res.gpu_ms, 3),
-                              "mrays_per_s": round(rays / res.gpu_ms / 1e3, 1)}))
+                              "mrays_per_s": round(rays / res.gpu_ms / 1e3, 1),
+                              "paths_per_bounce": counts}))
 
 
 if __name__ == "__main__":
