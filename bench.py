@@ -54,6 +54,13 @@ EXTEND_STATE_BYTES = 72
 # (112 of its 128 bytes); a triangle test its three corners (48 of 64); an
 # instance entry its 64-byte traversal record.
 NODE_BYTES, TRIANGLE_BYTES, INSTANCE_BYTES = 112, 48, 64
+# DRAM bytes (read + write) per extension ray of k_wf_extend, from an Nsight
+# Compute capture of one launch (the sphere field at 960x540, bounce 1 of
+# the second frame: 354,127 rays, 115.2 MB read + 14.7 MB written, caches
+# flushed before the launch). Scaled by rays to the bench's launches.
+EXTEND_DRAM_BYTES_PER_RAY = 367.0
+# B200's nominal HBM3e bandwidth (GB/s), for the fraction against it.
+NOMINAL_HBM_GBS = 8000.0
 
 
 def settings(sample_index):
@@ -418,7 +425,10 @@ def main():
                 "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
                 "peak_kind": peak_kind,
-                "traffic": None,
+                "frac_of_nominal": round(achieved / NOMINAL_HBM_GBS, 4),
+                "traffic": round(EXTEND_DRAM_BYTES_PER_RAY * ext_rays_timed / launches),
+                "traffic_basis": "ncu dram__bytes_read.sum + dram__bytes_write.sum per extension ray "
+                                 "(one 960x540 launch), times this sample's rays per extend launch",
                 "bytes_per_ray": round(per_ray, 1),
                 "nodes_per_ray": round(counted.node_visits[1] / n_ext, 2),
                 "triangles_per_ray": round(counted.triangle_visits[1] / n_ext, 2),
