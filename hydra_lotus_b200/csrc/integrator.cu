@@ -568,6 +568,40 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_shadow(SceneVi
   }
 }
 
+// The ReSTIR passes' queued visibility rays (VisibilityQueue), as a
+// persistent any-hit kernel that completes each ray's pixel record.
+__global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_visibility(SceneView S, VisibilityQueue VQ,
+    uint32_t pass, unsigned char* __restrict__ records, uint32_t stride, uint32_t positive,
+    uint32_t refill_below) {
+  const uint32_t n = VQ.counters[2 * pass];
+  Walk W;
+  WalkStack stack;
+  uint32_t rng = 0, index = 0;
+  bool active = false, exhausted = false;
+  for (;;) {
+    const uint32_t got = warp_fetch(&VQ.counters[2 * pass + 1], n, active, refill_below, exhausted);
+    if (got < n) {
+      index = got;
+      const float4 o = VQ.origin[index];
+      walk_begin(S, W, V(o), V(VQ.direction[index]), 0.0f, o.w);
+      active = true;
+    }
+    if (!__any_sync(kFullWarp, active)) break;
+    if (walk_round<true, false>(S, W, stack, rng, active, nullptr)) {
+      active = false;
+      const float visibility = W.transmittance;
+      const uint32_t slot = VQ.slot[index];
+      const float4 c = VQ.pending[slot];
+      RestirPixel* p = reinterpret_cast<RestirPixel*>(records + (size_t)slot * stride);
+      const F3 estimate = V(c) * (visibility * c.w);
+      if (!isfinite(c.w) || (positive && c.w <= 0.0f) || !is_finite(estimate))
+        p->flags |= 2u;
+      else
+        p->contribution = F4(estimate, visibility);
+    }
+  }
+}
+
 // Intersect (wavefront.slang:230-262) as a persistent kernel: a hit is
 // queued for shading; a miss ends the path with the environment. Each warp
 // stages its hits in shared memory and appends them to the hit queue 32 at
@@ -908,6 +942,13 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   k_wf_resolve<true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, accum, color, B);
   k_wf_finish_batch<<<1, 32, 0, stream>>>(B, Q.counts, max_bounces, totals);
   k_advance_batch<<<(B.count + 31) / 32, 32, 0, stream>>>(B);
+}
+
+void launch_visibility(const SceneView& S, const VisibilityQueue& queue, uint32_t pass, unsigned char* records,
+    uint32_t stride, bool positive, cudaStream_t stream, const TraceTuning& tuning) {
+  const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
+  const uint32_t grid = persistent_grid((const void*)k_visibility, queue.capacity, tuning);
+  k_visibility<<<grid, kBlock, 0, stream>>>(S, queue, pass, records, stride, positive ? 1u : 0u, refill);
 }
 
 void launch_advance(FrameConst* fc, cudaStream_t stream) { k_advance<<<1, 32, 0, stream>>>(fc); }

@@ -127,6 +127,30 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
 void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream, const TraceTuning& tuning);
 
+// Deferred visibility of the ReSTIR passes. Each pass queues the shadow
+// ray of every pixel whose selected sample needs one (origin and distance,
+// direction, pixel) and keeps the pixel's unshadowed contribution and
+// normalization in `pending`; one persistent any-hit launch per pass then
+// traces the queue and completes the pixels' records. counters[2 p] and
+// counters[2 p + 1] are pass p's queued rays and fetch cursor.
+struct VisibilityQueue {
+  float4* origin;     // origin, distance
+  float4* direction;
+  uint32_t* slot;
+  float4* pending;    // per pixel
+  uint32_t* counters;
+  uint32_t capacity;
+};
+constexpr uint32_t kVisibilityPasses = 3;
+
+// Traces pass `pass`'s queue and completes the RestirPixel at `records +
+// slot * stride` of each ray: contribution = (unshadowed * (visibility *
+// normalization), visibility), or flag 2 when the normalization is not
+// finite (or, with `positive`, not above zero) or the estimate is not
+// finite (restir.slang:225-232, 380-386, 484-490).
+void launch_visibility(const SceneView& S, const VisibilityQueue& queue, uint32_t pass, unsigned char* records,
+    uint32_t stride, bool positive, cudaStream_t stream, const TraceTuning& tuning = TraceTuning());
+
 void launch_advance(FrameConst* fc, cudaStream_t stream);
 
 void launch_clear_color(float4* color, uint32_t pixels, float4 value, cudaStream_t stream);

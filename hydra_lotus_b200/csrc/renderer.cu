@@ -421,6 +421,9 @@ struct Renderer {
     DeviceArray<RestirSurface> surfaces[2];
     DeviceArray<uint4> primary_hit;     // the camera rays' hits, traced once per frame
     DeviceArray<uint32_t> primary_rng;
+    // The ReSTIR passes' deferred visibility (VisibilityQueue).
+    DeviceArray<float4> vis_origin, vis_direction, vis_pending;
+    DeviceArray<uint32_t> vis_slot, vis_counters;
     DeviceArray<TemporalConst> constants;
     DeviceArray<TemporalInstance> instances;
     bool instances_custom = false;
@@ -1478,7 +1481,12 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
           R.ok(T.sources.resize(n), "reservoirs", detail) &&
           R.ok(T.surfaces[0].resize(n), "reservoir surfaces", detail) &&
           R.ok(T.surfaces[1].resize(n), "reservoir surfaces", detail) &&
-          R.ok(T.primary_hit.resize(n), "primary hits", detail) && R.ok(T.primary_rng.resize(n), "primary hits", detail);
+          R.ok(T.primary_hit.resize(n), "primary hits", detail) && R.ok(T.primary_rng.resize(n), "primary hits", detail) &&
+          R.ok(T.vis_origin.resize(n), "visibility queue", detail) &&
+          R.ok(T.vis_direction.resize(n), "visibility queue", detail) &&
+          R.ok(T.vis_pending.resize(n), "visibility queue", detail) &&
+          R.ok(T.vis_slot.resize(n), "visibility queue", detail) &&
+          R.ok(T.vis_counters.resize(2 * kVisibilityPasses), "visibility queue", detail);
   if (!okb) return poison(detail);
   // The transport key: a change drops the history (vulkan_backend.cpp:1766-1781).
   uint32_t key[16] = {st.integrator, st.light_sampling, st.restir_proposal, st.restir_candidates,
@@ -1559,15 +1567,28 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   launch_temporal_surface(R.view, R.frame_const.ptr, T.constants.ptr, T.instances.ptr, T.surface[sw].ptr, pixels, s);
   launch_reproject(T.constants.ptr, T.surface[sw].ptr, T.surface[1 - sw].ptr, T.validity.ptr, pixels, s);
   if (restir) {
+    const VisibilityQueue vq{T.vis_origin.ptr, T.vis_direction.ptr, T.vis_slot.ptr, T.vis_pending.ptr,
+        T.vis_counters.ptr, pixels};
+    if (!R.ok(cudaMemsetAsync(T.vis_counters.ptr, 0, 2 * kVisibilityPasses * sizeof(uint32_t), s),
+            "visibility queue", detail))
+      return poison(detail);
     launch_restir_initial(R.view, R.frame_const.ptr, T.constants.ptr, T.initial.ptr, T.primary_hit.ptr,
-        T.primary_rng.ptr, pixels, s);
-    if (reservoirs)
+        T.primary_rng.ptr, vq, pixels, s);
+    launch_visibility(R.view, vq, 0, reinterpret_cast<unsigned char*>(T.initial.ptr), sizeof(RestirPixel), false,
+        s, R.tuning);
+    if (reservoirs) {
       launch_restir_temporal(R.view, R.frame_const.ptr, T.constants.ptr, T.primary_hit.ptr, T.instances.ptr,
           T.initial.ptr, T.validity.ptr, T.surface[sw].ptr, T.reuse[1 - rs].ptr, T.surfaces[1 - rs].ptr,
-          T.reuse[rs].ptr, T.surfaces[rs].ptr, pixels, s);
-    if (st.restir_spatial)
+          T.reuse[rs].ptr, T.surfaces[rs].ptr, vq, pixels, s);
+      launch_visibility(R.view, vq, 1, reinterpret_cast<unsigned char*>(T.reuse[rs].ptr), sizeof(RestirReuse),
+          true, s, R.tuning);
+    }
+    if (st.restir_spatial) {
       launch_restir_spatial(R.view, R.frame_const.ptr, T.constants.ptr, T.reuse[rs].ptr, T.surfaces[rs].ptr,
-          T.spatial.ptr, T.sources.ptr, pixels, s);
+          T.spatial.ptr, T.sources.ptr, vq, pixels, s);
+      launch_visibility(R.view, vq, 2, reinterpret_cast<unsigned char*>(T.spatial.ptr), sizeof(RestirReuse), true,
+          s, R.tuning);
+    }
   }
   if (rect[2] < t.width || rect[3] < t.height || rect[2] == 0)
     launch_clear_color(R.color.ptr, pixels, make_float4(t.clear_color[0], t.clear_color[1], t.clear_color[2],

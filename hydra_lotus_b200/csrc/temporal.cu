@@ -6,6 +6,8 @@
 // estimate, a-trous iterations and composite (temporal.slang:229-475). One
 // thread per pixel; every pass is a separate launch, so each reads only what
 // the preceding one finished writing, as the reference's barriers order it.
+#include <cooperative_groups.h>
+
 #include "temporal_passes.cuh"
 
 namespace lotus {
@@ -223,11 +225,41 @@ __device__ __forceinline__ float history_target(const SceneView& S, const Restir
   return max_component(c);
 }
 
-// ReceiverVisibility (restir.slang:290-300).
-__device__ __forceinline__ float receiver_visibility(const SceneView& S, const RestirPixel& selected,
-    const RestirPixel& current, F3 origin, const LightSample& ls) {
-  if (same_sample(selected, current)) return current.contribution.w;
-  return trace_shadow(S, origin, ls.direction, 0.0f, ls.distance);
+// Queues pixel `slot`'s shadow ray for pass `pass` of the deferred
+// visibility (VisibilityQueue), with its unshadowed contribution and
+// normalization; the visibility launch completes the record. One atomic
+// per group of lanes that queue together.
+__device__ __forceinline__ void queue_visibility(const VisibilityQueue& q, uint32_t pass, uint32_t slot,
+    F3 origin, const LightSample& ls, F3 unshadowed, float normalization) {
+  namespace cg = cooperative_groups;
+  cg::coalesced_group g = cg::coalesced_threads();
+  uint32_t base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(&q.counters[2 * pass], g.size());
+  base = g.shfl(base, 0);
+  const uint32_t i = base + g.thread_rank();
+  if (i >= q.capacity) return;  // one ray per pixel at most: never taken
+  q.origin[i] = F4(origin, ls.distance);
+  q.direction[i] = F4(ls.direction, 0.0f);
+  q.slot[i] = slot;
+  q.pending[slot] = F4(unshadowed, normalization);
+}
+
+// ReceiverVisibility (restir.slang:290-300) and the estimate after it: the
+// current sample's visibility when the selected sample is the current one,
+// else a queued shadow ray.
+__device__ __forceinline__ void receiver_estimate(const VisibilityQueue& q, uint32_t pass, uint32_t slot,
+    const RestirPixel& current, F3 origin, const LightSample& ls, F3 unshadowed, float normalization,
+    RestirPixel& selected) {
+  if (!same_sample(selected, current)) {
+    queue_visibility(q, pass, slot, origin, ls, unshadowed, normalization);
+    return;
+  }
+  const float visibility = current.contribution.w;
+  const F3 estimate = unshadowed * (visibility * normalization);
+  if (!isfinite(normalization) || normalization <= 0.0f || !is_finite(estimate))
+    selected.flags |= 2u;
+  else
+    selected.contribution = F4(estimate, visibility);
 }
 
 __device__ __forceinline__ RestirPixel empty_restir_pixel() {
@@ -242,10 +274,11 @@ __device__ __forceinline__ RestirPixel empty_restir_pixel() {
 
 // WriteInitialReservoir (restir.slang:163-233): M candidates streamed over
 // the light table at the jittered camera surface, then one shadow ray for
-// the selected sample.
+// the selected sample (queued for the deferred visibility, pass 0).
 __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
-    RestirPixel* __restrict__ out, uint4* __restrict__ primary_hit, uint32_t* __restrict__ primary_rng) {
+    RestirPixel* __restrict__ out, uint4* __restrict__ primary_hit, uint32_t* __restrict__ primary_rng,
+    VisibilityQueue VQ) {
   const FrameConst& f = *fcp;
   const TemporalConst& tc = *tcp;
   uint32_t px, py;
@@ -296,14 +329,9 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
       }
       if ((r.flags & 2u) == 0 && r.reservoir.weight_sum > 0.0f) {
         const LightSample ls = reconstruct_reservoir_light(S, r.reservoir.sample, r.uv[0], r.uv[1], origin);
-        const float visibility = trace_shadow(S, origin, ls.direction, 0.0f, ls.distance);
-        const float normalization = reservoir_normalization(r.reservoir);
-        const F3 estimate = candidate_contribution(sh, basis, wo, ls, S.lights[r.reservoir.sample].pdf) *
-            (visibility * normalization);
-        if (!isfinite(normalization) || !is_finite(estimate))
-          r.flags |= 2u;
-        else
-          r.contribution = F4(estimate, visibility);
+        queue_visibility(VQ, 0, slot, origin, ls,
+            candidate_contribution(sh, basis, wo, ls, S.lights[r.reservoir.sample].pdf),
+            reservoir_normalization(r.reservoir));
       }
     }
   }
@@ -316,7 +344,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
     const uint4* __restrict__ primary_hit, const TemporalInstance* __restrict__ identities, const RestirPixel* __restrict__ initial,
     const ValidityPixel* __restrict__ validity, const TemporalPixel* __restrict__ surface,
     const RestirReuse* __restrict__ previous, const RestirSurface* __restrict__ previous_surfaces,
-    RestirReuse* __restrict__ out, RestirSurface* __restrict__ out_surfaces) {
+    RestirReuse* __restrict__ out, RestirSurface* __restrict__ out_surfaces, VisibilityQueue VQ) {
   const FrameConst& f = *fcp;
   const TemporalConst& tc = *tcp;
   uint32_t px, py;
@@ -395,13 +423,9 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
       if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
         const LightSample ls = reconstruct_reservoir_light(S, result.pixel.reservoir.sample,
             result.pixel.uv[0], result.pixel.uv[1], origin);
-        const float visibility = receiver_visibility(S, result.pixel, initial[slot], origin, ls);
-        const F3 estimate = history_contribution(S, receiver, result.pixel.reservoir.sample, ls) *
-            (visibility * result.normalization);
-        if (!isfinite(result.normalization) || result.normalization <= 0.0f || !is_finite(estimate))
-          result.pixel.flags |= 2u;
-        else
-          result.pixel.contribution = F4(estimate, visibility);
+        receiver_estimate(VQ, 1, slot, initial[slot], origin, ls,
+            history_contribution(S, receiver, result.pixel.reservoir.sample, ls), result.normalization,
+            result.pixel);
       }
     }
   }
@@ -424,7 +448,7 @@ __device__ __forceinline__ bool spatial_compatible(const RestirSurface& receiver
 __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     const RestirReuse* __restrict__ temporal, const RestirSurface* __restrict__ surfaces,
-    RestirReuse* __restrict__ out, uint4* __restrict__ out_sources) {
+    RestirReuse* __restrict__ out, uint4* __restrict__ out_sources, VisibilityQueue VQ) {
   const FrameConst& f = *fcp;
   const TemporalConst& tc = *tcp;
   uint32_t px, py;
@@ -492,13 +516,9 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
       if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
         const LightSample ls = reconstruct_reservoir_light(S, result.pixel.reservoir.sample,
             result.pixel.uv[0], result.pixel.uv[1], V(receiver.origin));
-        const float visibility = receiver_visibility(S, result.pixel, centre.pixel, V(receiver.origin), ls);
-        const F3 estimate = history_contribution(S, receiver, result.pixel.reservoir.sample, ls) *
-            (visibility * result.normalization);
-        if (!isfinite(result.normalization) || result.normalization <= 0.0f || !is_finite(estimate))
-          result.pixel.flags |= 2u;
-        else
-          result.pixel.contribution = F4(estimate, visibility);
+        receiver_estimate(VQ, 2, slot, centre.pixel, V(receiver.origin), ls,
+            history_contribution(S, receiver, result.pixel.reservoir.sample, ls), result.normalization,
+            result.pixel);
       }
     }
   }
@@ -756,23 +776,24 @@ void launch_reproject(const TemporalConst* tc, const TemporalPixel* current, con
 }
 
 void launch_restir_initial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
-    RestirPixel* out, uint4* primary_hit, uint32_t* primary_rng, uint32_t pixels, cudaStream_t s) {
-  k_restir_initial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out, primary_hit, primary_rng);
+    RestirPixel* out, uint4* primary_hit, uint32_t* primary_rng, const VisibilityQueue& vq, uint32_t pixels,
+    cudaStream_t s) {
+  k_restir_initial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out, primary_hit, primary_rng, vq);
 }
 
 void launch_restir_temporal(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
     const uint4* primary_hit, const TemporalInstance* ids, const RestirPixel* initial,
-    const ValidityPixel* validity,
-    const TemporalPixel* surface, const RestirReuse* previous, const RestirSurface* previous_surfaces,
-    RestirReuse* out, RestirSurface* out_surfaces, uint32_t pixels, cudaStream_t s) {
+    const ValidityPixel* validity, const TemporalPixel* surface, const RestirReuse* previous,
+    const RestirSurface* previous_surfaces, RestirReuse* out, RestirSurface* out_surfaces,
+    const VisibilityQueue& vq, uint32_t pixels, cudaStream_t s) {
   k_restir_temporal<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, primary_hit, ids, initial, validity, surface, previous,
-      previous_surfaces, out, out_surfaces);
+      previous_surfaces, out, out_surfaces, vq);
 }
 
 void launch_restir_spatial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
     const RestirReuse* temporal, const RestirSurface* surfaces, RestirReuse* out, uint4* sources,
-    uint32_t pixels, cudaStream_t s) {
-  k_restir_spatial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, temporal, surfaces, out, sources);
+    const VisibilityQueue& vq, uint32_t pixels, cudaStream_t s) {
+  k_restir_spatial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, temporal, surfaces, out, sources, vq);
 }
 
 void launch_svgf(const TemporalConst* tc, const TemporalConst& host_tc, const float4* batch,
