@@ -167,6 +167,27 @@ def cpu_baseline(scene, seconds, rows=64):
                       f"({rays} rays in {dt:.1f} s), OpenMP over {threads} threads"}
 
 
+def rank_sample_base(rank):
+    """First sample index of a rank's frames: ranks render independent
+    samples of the same workload (replicas, no data-path collective)."""
+    return 1000003 * rank
+
+
+def reduce_over_ranks(rays, e2e_rays, ms, e2e_ms, world, device):
+    """The job's totals: rays summed over ranks, device times as the
+    slowest rank's (the rank that finishes last bounds the job)."""
+    import torch
+    stats = torch.tensor([rays, e2e_rays, ms, e2e_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        sums = stats[:2].clone()
+        dist.all_reduce(sums)
+        maxes = stats[2:].clone()
+        dist.all_reduce(maxes, op=dist.ReduceOp.MAX)
+        stats = torch.cat([sums, maxes])
+    return stats.tolist()
+
+
 def run_reference(args, rank):
     """--impl reference: the CPU oracle on the host cores."""
     if rank != 0:
@@ -314,7 +335,7 @@ def main():
     sres = renderer.check(r.update_scene(scene), "update_scene")
     stream = torch.cuda.ExternalStream(r.stream)
 
-    base = 1000003 * rank  # independent samples per rank
+    base = rank_sample_base(rank)
     step_index = [0]
 
     def frame(read_back=False, flags=0):
@@ -373,14 +394,7 @@ def main():
     counted, _ = r.render_scene(frame(flags=abi.FRAME_COUNT_VISITS))
     renderer.check(counted, "counted frame")
 
-    stats = torch.tensor([rays, e2e_rays, ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        sums = stats[:2].clone()
-        dist.all_reduce(sums)
-        maxes = stats[2:].clone()
-        dist.all_reduce(maxes, op=dist.ReduceOp.MAX)
-        stats = torch.cat([sums, maxes])
-    total_rays, total_e2e_rays, max_ms, max_e2e_ms = stats.tolist()
+    total_rays, total_e2e_rays, max_ms, max_e2e_ms = reduce_over_ranks(rays, e2e_rays, ms, e2e_ms, world, "cuda")
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
