@@ -254,6 +254,60 @@ def time_to_relmse_report(renderer_module):
     return out
 
 
+def scene_update_report(renderer_module, repeats=3):
+    """Scene uploads and edits on the shape of the reference's `geometry-v1`
+    workload (one indexed 512 x 512-quad grid: 524,288 triangles, 263,169
+    vertices), as the reference's performance baseline times them: the
+    initial upload and build, a compatible point edit of every position
+    (y += 0.01 x, lotus_cuda_update_geometry) and a transform edit (x +=
+    0.01, lotus_cuda_update_instances). Per kind, the median over `repeats`
+    of the device time of the update's uploads and builds (build_gpu_ms;
+    the initial one also spans its host staging) and of the call's host
+    wall time."""
+    grid = scenes.grid_mesh(quads=512)
+    out = {"workload": "one indexed 512x512-quad grid, 524,288 triangles, 263,169 vertices (geometry-v1's shape)",
+           "unit": "ms"}
+
+    def med(v):
+        return round(statistics.median(v), 4)
+
+    with renderer_module.CudaOffscreenRenderer(0) as r:
+        full, full_wall = [], []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            res = renderer_module.check(r.update_scene(grid), "update_scene")
+            full_wall.append((time.perf_counter() - t0) * 1e3)
+            full.append(res.build_gpu_ms)
+        p0 = grid.geometries[0][0].copy()
+        edit, edit_wall, move, move_wall = [], [], [], []
+        for k in range(repeats):
+            q = p0.copy()
+            q[:, 1] += 0.01 * (k + 1) * p0[:, 0]
+            grid.set_positions(0, q)
+            t0 = time.perf_counter()
+            res = renderer_module.check(r.update_geometry(grid, 0), "update_geometry")
+            edit_wall.append((time.perf_counter() - t0) * 1e3)
+            edit.append(res.build_gpu_ms)
+            m = np.array(grid.instances[0][0], dtype=np.float32)
+            m[12] += 0.01
+            grid.set_instance(0, m)
+            t0 = time.perf_counter()
+            res = renderer_module.check(r.update_instances(grid), "update_instances")
+            move_wall.append((time.perf_counter() - t0) * 1e3)
+            move.append(res.build_gpu_ms)
+    out["initial_build"] = {"gpu_ms": med(full), "wall_ms": med(full_wall)}
+    out["point_edit"] = {"gpu_ms": med(edit), "wall_ms": med(edit_wall)}
+    out["transform_edit"] = {"gpu_ms": med(move), "wall_ms": med(move_wall)}
+    out["reference_published"] = {
+        "hardware": "RTX A5000 (Vulkan, driver-built acceleration structures)",
+        "initial_build": {"gpu_upload_ms": 0.36, "gpu_blas_build_ms": 1.628, "gpu_tlas_build_ms": 0.033,
+                          "wall_ms": 8.241},
+        "point_edit": {"gpu_upload_ms": 0.359, "gpu_blas_refit_ms": 0.455, "gpu_tlas_refit_ms": 0.010,
+                       "wall_ms": 2.645},
+        "transform_edit": {"gpu_upload_ms": 0.001, "gpu_tlas_refit_ms": 0.010, "wall_ms": 0.183}}
+    return out
+
+
 def batch_report(renderer_module, spp=8, depth=8):
     """Config 4: the 64-scene batch workload (scenes.batch_workload: traced
     triangles log-uniform in [1e4, 2e6], 256^2 .. 1024^2 targets), 8 spp,
@@ -306,6 +360,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--batch", type=int, default=1,
                     help="1: also measure the 64-scene batch (config 4), batched vs one scene at a time")
+    ap.add_argument("--updates", type=int, default=1,
+                    help="1: also time scene uploads and edits on the geometry-v1-shaped grid")
     ap.add_argument("--convergence", type=int, default=1,
                     help="1: also measure time to relMSE 1e-3 (plain PT, cache, ReSTIR, cache+ReSTIR)")
     args = ap.parse_args()
@@ -466,6 +522,8 @@ def main():
             line["time_to_relmse"] = time_to_relmse_report(renderer)
         if args.batch:
             line["batch"] = batch_report(renderer)
+        if args.updates:
+            line["scene_updates"] = scene_update_report(renderer)
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:

@@ -592,9 +592,11 @@ __global__ void k_batch_write_triangles(const float* __restrict__ positions, con
 // Packets", 2008). Every binary node gets a wide node at its own index, so
 // the collapse is one independent thread per node; a wide node whose binary
 // node was opened by its parent is never referenced.
-__global__ void k_collapse4(const BvhNode* __restrict__ bin, uint32_t n, Bvh4Node* __restrict__ wide,
-    int leaves_are_instances) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_collapse4(const BvhNode* __restrict__ bin, uint32_t first, uint32_t count, uint32_t n,
+    Bvh4Node* __restrict__ wide, int leaves_are_instances) {
+  const uint32_t offset = blockIdx.x * blockDim.x + threadIdx.x;
+  if (offset >= count) return;
+  const uint32_t i = first + offset;
   if (i >= n) return;
   float lo[4][3], hi[4][3];
   int32_t ref[4], cnt[4];
@@ -847,8 +849,14 @@ cudaError_t BvhBuilder::build_instances_sah(const InstanceShading* shade, const 
 
 cudaError_t BvhBuilder::collapse(const BvhNode* binary, uint32_t n, Bvh4Node* wide, bool leaves_are_instances,
     cudaStream_t stream) {
-  if (n == 0) return cudaSuccess;
-  k_collapse4<<<blocks(n), kBuildBlock, 0, stream>>>(binary, n, wide, leaves_are_instances ? 1 : 0);
+  return collapse_range(binary, 0, n, n, wide, leaves_are_instances, stream);
+}
+
+cudaError_t BvhBuilder::collapse_range(const BvhNode* binary, uint32_t first, uint32_t count, uint32_t n,
+    Bvh4Node* wide, bool leaves_are_instances, cudaStream_t stream) {
+  if (count == 0) return cudaSuccess;
+  k_collapse4<<<blocks(count), kBuildBlock, 0, stream>>>(binary, first, count, n, wide,
+      leaves_are_instances ? 1 : 0);
   return cudaGetLastError();
 }
 

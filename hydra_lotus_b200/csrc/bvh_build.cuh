@@ -46,6 +46,10 @@ class BvhBuilder {
   // their references). One launch over the whole pool.
   static cudaError_t collapse(const BvhNode* binary, uint32_t n, Bvh4Node* wide, bool leaves_are_instances,
       cudaStream_t stream);
+  // The same over binary nodes [first, first + count) of a pool of n (one
+  // geometry's BLAS after it was rebuilt in place).
+  static cudaError_t collapse_range(const BvhNode* binary, uint32_t first, uint32_t count, uint32_t n,
+      Bvh4Node* wide, bool leaves_are_instances, cudaStream_t stream);
   void release();
 
   static uint32_t node_count(uint32_t n) { return n > 1 ? n - 1 : n; }

@@ -348,6 +348,27 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
 
 }  // namespace
 
+// The resident scene as the incremental updates need it: each geometry's
+// arrays (owned copies; `geometries` points into them), its box and its
+// places in the device arrays and pools, the materials and the
+// environment's summary.
+struct HostScene {
+  std::vector<std::vector<float>> positions, normals;
+  std::vector<std::vector<uint32_t>> triangles;
+  std::vector<lotus_geometry> geometries;
+  std::vector<std::array<float, 6>> boxes;
+  std::vector<uint64_t> vertex_base;
+  std::vector<uint32_t> node_base, tri_base, normal_base;
+  uint64_t nodes = 0;
+  std::vector<lotus_material> materials;
+  float environment_constant[3] = {0.0f, 0.0f, 0.0f};
+  bool env_bound = false;
+  double env_mean = 0.0;
+  uint32_t env_width = 0, env_height = 0, env_columns = 0, env_rows = 0;
+  float env_scale[3] = {0.0f, 0.0f, 0.0f};
+  float env_frame[9] = {};
+};
+
 struct Renderer {
   int device = 0;
   uint32_t bvh_leaf_size = 1;
@@ -372,6 +393,9 @@ struct Renderer {
   std::vector<LightRecord> host_lights;
   std::vector<uint32_t> host_light_offsets;
   SceneView view{};
+  HostScene host;                       // the resident scene's host copy
+  DeviceArray<float> scene_pos;         // every geometry's positions, kept for rebuilds
+  DeviceArray<uint32_t> scene_tri;      // every geometry's triangles
   bool scene_ready = false;
   uint64_t scene_generation = 0;
   BvhBuilder builder;
@@ -474,6 +498,7 @@ struct Renderer {
   }
 
   void release_scene() {
+    scene_pos.release(); scene_tri.release(); host = HostScene{};
     blas.release(); tlas.release(); blas4.release(); tlas4.release(); tris.release(); inst_trav.release(); inst_shade.release();
     materials.release(); normals.release(); lights.release(); light_verts.release();
     light_radiance.release(); env_texels.release(); env_floats.release();
@@ -481,7 +506,7 @@ struct Renderer {
   }
 
   uint64_t scene_bytes() const {
-    return blas.bytes() + tlas.bytes() + blas4.bytes() + tlas4.bytes() + tris.bytes() + inst_trav.bytes() + inst_shade.bytes() +
+    return scene_pos.bytes() + scene_tri.bytes() + blas.bytes() + tlas.bytes() + blas4.bytes() + tlas4.bytes() + tris.bytes() + inst_trav.bytes() + inst_shade.bytes() +
            materials.bytes() + normals.bytes() + lights.bytes() + light_verts.bytes() +
            light_radiance.bytes() + env_texels.bytes() + env_floats.bytes();
   }
@@ -558,6 +583,212 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Scene updates. A full update (UpdateScene) uploads every geometry, builds
+// every BLAS, the materials, the environment and the instance state; the
+// incremental ones rebuild only what an edit invalidates, from the resident
+// scene's host copy and its device position and triangle arrays:
+//   - lotus_cuda_update_instances (transform / material-slot edits): the
+//     light table, the instance records and the TLAS;
+//   - lotus_cuda_update_geometry (point edits of one geometry, topology
+//     kept): that geometry's BLAS, rebuilt in place in its own node and
+//     triangle ranges, its corner normals, then the instance state.
+// The reference refits in both cases (gpu_scene.cpp:2303-2322); a rebuild
+// decides the same hits, since hits are decided by triangle tests alone.
+
+// Host-side instance state, prepared before any of it goes to the device.
+struct InstanceState {
+  LightTable table;
+  std::vector<InstanceTraversal> trav;
+  std::vector<InstanceShading> shade;
+};
+
+lotus_scene_desc host_desc(const Renderer& R) {
+  const HostScene& h = R.host;
+  lotus_scene_desc d{};
+  d.geometries = h.geometries.data();
+  d.instances = R.host_instances.data();
+  d.materials = h.materials.data();
+  d.environment = nullptr;
+  d.geometry_count = (uint32_t)h.geometries.size();
+  d.instance_count = (uint32_t)R.host_instances.size();
+  d.material_count = (uint32_t)h.materials.size();
+  for (int k = 0; k < 3; ++k) d.environment_constant[k] = h.environment_constant[k];
+  return d;
+}
+
+std::array<float, 6> geometry_box(const lotus_geometry& geo) {
+  std::array<float, 6> b = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t v = 0; v < geo.vertex_count; ++v)
+    for (int a = 0; a < 3; ++a) {
+      b[a] = std::min(b[a], geo.positions[3 * (size_t)v + a]);
+      b[3 + a] = std::max(b[3 + a], geo.positions[3 * (size_t)v + a]);
+    }
+  return b;
+}
+
+// The light table, world bounds and instance records of the host copy.
+bool prepare_instances(Renderer& R, InstanceState& out, std::string& detail) {
+  const HostScene& h = R.host;
+  const lotus_scene_desc s = host_desc(R);
+  out.table = build_light_table(s, h.env_bound ? h.env_mean : 0.0);
+  // World bounds: each instance's geometry box through its transform.
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = 0; i < s.instance_count; ++i) {
+    const std::array<float, 6>& b = h.boxes[s.instances[i].geometry];
+    if (!(b[0] <= b[3])) continue;
+    const float* m = s.instances[i].world_from_object;
+    for (int c = 0; c < 8; ++c) {
+      const float p[3] = {(c & 1) ? b[3] : b[0], (c & 2) ? b[4] : b[1], (c & 4) ? b[5] : b[2]};
+      for (int a = 0; a < 3; ++a) {
+        const float w = m[a] * p[0] + m[4 + a] * p[1] + m[8 + a] * p[2] + m[12 + a];
+        lo[a] = std::min(lo[a], w);
+        hi[a] = std::max(hi[a], w);
+      }
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    R.scene_lo[a] = std::isfinite(lo[a]) ? lo[a] : 0.0f;
+    R.scene_hi[a] = std::isfinite(hi[a]) ? hi[a] : 1.0f;
+  }
+  out.trav.resize(s.instance_count);
+  out.shade.resize(s.instance_count);
+  for (uint32_t i = 0; i < s.instance_count; ++i) {
+    const lotus_instance& inst = s.instances[i];
+    const float* m = inst.world_from_object;
+    InstanceTraversal& t = out.trav[i];
+    InstanceShading& sh = out.shade[i];
+    if (!invert_affine(m, t.inv)) {
+      detail = "instance " + std::to_string(i) + " has a singular transform";
+      return false;
+    }
+    const lotus_geometry& geo = s.geometries[inst.geometry];
+    t.blas_root = geo.triangle_count ? h.node_base[inst.geometry] : (uint32_t)kEmptyChild;
+    t.flags = host_coverage(s.materials[inst.material]) >= 1.0f ? kInstanceOpaque : 0u;
+    t.material = inst.material;
+    t.light_offset = out.table.offsets[i];
+    for (int r = 0; r < 3; ++r) sh.m[r] = make_float4(m[r], m[4 + r], m[8 + r], m[12 + r]);
+    sh.material = inst.material;
+    sh.light_offset = out.table.offsets[i];
+    sh.normals = h.normal_base[inst.geometry];
+    // dot(c0, cross(c1, c2)) < 0 (scene.slang:1237-1240).
+    const float c0[3] = {m[0], m[1], m[2]}, c1[3] = {m[4], m[5], m[6]}, c2[3] = {m[8], m[9], m[10]};
+    const float x = c1[1] * c2[2] - c1[2] * c2[1], y = c1[2] * c2[0] - c1[0] * c2[2],
+                z = c1[0] * c2[1] - c1[1] * c2[0];
+    sh.mirror = (c0[0] * x + c0[1] * y + c0[2] * z) < 0.0f ? 1u : 0u;
+  }
+  return true;
+}
+
+// Uploads the prepared instance state, builds the TLAS and its 4-wide pool
+// and assembles the SceneView.
+bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
+  cudaStream_t st = R.stream;
+  const HostScene& h = R.host;
+  const uint32_t n = (uint32_t)R.host_instances.size();
+  if (!R.ok(R.lights.upload(in.table.records.data(), in.table.records.size(), st), "light table", detail) ||
+      !R.ok(R.light_verts.upload(in.table.verts.data(), in.table.verts.size(), st), "light corners", detail) ||
+      !R.ok(R.light_radiance.upload(in.table.radiance.data(), in.table.radiance.size(), st), "light radiance",
+          detail) ||
+      !R.ok(R.inst_trav.upload(in.trav.data(), in.trav.size(), st), "instances", detail) ||
+      !R.ok(R.inst_shade.upload(in.shade.data(), in.shade.size(), st), "instances", detail) ||
+      !R.ok(R.tlas.resize(std::max<uint32_t>(BvhBuilder::node_count(n), 1)), "TLAS", detail))
+    return false;
+  if (!R.ok(n <= kSahMaxTriangles
+                ? R.builder.build_instances_sah(R.inst_shade.ptr, R.inst_trav.ptr, R.blas.ptr, n, R.tlas.ptr, st)
+                : R.builder.build_instances(R.inst_shade.ptr, R.inst_trav.ptr, R.blas.ptr, n, R.tlas.ptr, st),
+          "TLAS build", detail) ||
+      !R.ok(R.tlas4.resize(R.tlas.count), "TLAS", detail) ||
+      !R.ok(BvhBuilder::collapse(R.tlas.ptr, BvhBuilder::node_count(n), R.tlas4.ptr, true, st), "BVH collapse",
+          detail))
+    return false;
+  R.host_lights = in.table.records;
+  R.host_light_offsets = in.table.offsets;
+  SceneView& v = R.view;
+  v = SceneView{};
+  v.tlas = R.tlas4.ptr;
+  v.blas = R.blas4.ptr;
+  v.tris = R.tris.ptr;
+  v.inst_trav = R.inst_trav.ptr;
+  v.inst_shade = R.inst_shade.ptr;
+  v.materials = R.materials.ptr;
+  v.normals = R.normals.ptr;
+  v.lights = R.lights.ptr;
+  v.light_verts = R.light_verts.ptr;
+  v.light_radiance = R.light_radiance.ptr;
+  v.env_texels = R.env_texels.ptr;
+  v.env_floats = R.env_floats.ptr;
+  v.instance_count = n;
+  v.light_count = (uint32_t)in.table.records.size();
+  v.env_bound = h.env_bound ? 1u : 0u;
+  if (h.env_bound) {
+    v.env_width = h.env_width;
+    v.env_height = h.env_height;
+    v.env_columns = h.env_columns;
+    v.env_rows = h.env_rows;
+    for (int k = 0; k < 3; ++k) v.env_scale[k] = h.env_scale[k];
+    for (int k = 0; k < 9; ++k) v.env_frame[k] = h.env_frame[k];
+  }
+  v.env_selection = in.table.env_selection;
+  for (int k = 0; k < 3; ++k) v.env_constant[k] = h.environment_constant[k];
+  return true;
+}
+
+// Builds the BLASes of the geometries in `which` from the device position
+// and triangle arrays: binned SAH for those up to kSahMaxTriangles (one
+// launch), LBVH for larger ones; then collapses their node ranges (or, with
+// `whole_pool`, the whole pool at once) into the 4-wide pool.
+bool build_blases(Renderer& R, const std::vector<uint32_t>& which, bool whole_pool, std::string& detail) {
+  cudaStream_t st = R.stream;
+  const HostScene& h = R.host;
+  std::vector<BatchGeometry> batch;
+  for (uint32_t g : which) {
+    const lotus_geometry& geo = h.geometries[g];
+    if (!geo.triangle_count) continue;
+    if (geo.triangle_count <= kSahMaxTriangles) {
+      batch.push_back({h.vertex_base[g], h.tri_base[g], geo.triangle_count, h.node_base[g]});
+      continue;
+    }
+    cudaError_t e = R.builder.build_triangles(R.scene_pos.ptr + 3 * h.vertex_base[g],
+        R.scene_tri.ptr + 3 * (size_t)h.tri_base[g], geo.triangle_count, R.blas.ptr, h.node_base[g], R.tris.ptr,
+        h.tri_base[g], st);
+    if (!R.ok(e, "BLAS build", detail)) return false;
+  }
+  if (!R.ok(R.builder.build_triangle_batch(R.scene_pos.ptr, R.scene_tri.ptr, batch, R.blas.ptr, R.tris.ptr, st,
+                R.bvh_leaf_size),
+          "BLAS build", detail))
+    return false;
+  const uint32_t pool = (uint32_t)h.nodes;
+  if (whole_pool) return R.ok(BvhBuilder::collapse(R.blas.ptr, pool, R.blas4.ptr, false, st), "BVH collapse", detail);
+  for (uint32_t g : which)
+    if (!R.ok(BvhBuilder::collapse_range(R.blas.ptr, h.node_base[g],
+                  BvhBuilder::node_count(h.geometries[g].triangle_count), pool, R.blas4.ptr, false, st),
+            "BVH collapse", detail))
+      return false;
+  return true;
+}
+
+int32_t finish_update(Renderer& R, lotus_scene_result& res, std::string& detail) {
+  cudaEventRecord(R.ev_stop, R.stream);
+  if (!R.ok(cudaStreamSynchronize(R.stream), "scene update", detail)) return -1;
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
+  R.scene_ready = true;
+  ++R.scene_generation;
+  const HostScene& h = R.host;
+  res.status = LOTUS_PASS;
+  uint64_t tris = 0;
+  for (const lotus_geometry& g : h.geometries) tris += g.triangle_count;
+  res.triangle_count = (uint32_t)tris;
+  res.instance_count = (uint32_t)R.host_instances.size();
+  res.light_count = (uint32_t)R.host_lights.size();
+  res.bvh_node_count = (uint32_t)h.nodes;
+  res.tlas_node_count = BvhBuilder::node_count(res.instance_count);
+  res.build_gpu_ms = ms;
+  res.device_bytes = R.scene_bytes();
+  return LOTUS_PASS;
+}
+
 int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result& res) {
   std::string detail;
   if (!validate_scene(s, detail)) {
@@ -572,76 +803,76 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
     return res.status = LOTUS_FAIL;
   };
   cudaEventRecord(R.ev_start, st);
-  // Geometry pools.
-  std::vector<uint32_t> node_base(s.geometry_count), tri_base(s.geometry_count),
-      normal_base(s.geometry_count, kNoLights);
+  // The host copy: every geometry's arrays, the materials, the instances.
+  HostScene& h = R.host;
+  h = HostScene{};
+  const uint32_t ng = s.geometry_count;
+  h.positions.resize(ng);
+  h.triangles.resize(ng);
+  h.normals.resize(ng);
+  h.geometries.resize(ng);
+  h.boxes.resize(ng);
+  h.vertex_base.resize(ng);
+  h.node_base.resize(ng);
+  h.tri_base.resize(ng);
+  h.normal_base.assign(ng, kNoLights);
   uint64_t nodes = 0, tri_total = 0, normal_total = 0, vert_total = 0;
-  uint32_t max_tris = 0;
-  for (uint32_t g = 0; g < s.geometry_count; ++g) {
+  for (uint32_t g = 0; g < ng; ++g) {
     const lotus_geometry& geo = s.geometries[g];
-    node_base[g] = (uint32_t)nodes;
-    tri_base[g] = (uint32_t)tri_total;
+    h.positions[g].assign(geo.positions, geo.positions + 3ull * geo.vertex_count);
+    h.triangles[g].assign(geo.triangles, geo.triangles + 3ull * geo.triangle_count);
+    if (geo.normals && geo.triangle_count) h.normals[g].assign(geo.normals, geo.normals + 9ull * geo.triangle_count);
+    lotus_geometry& copy = h.geometries[g];
+    copy = geo;
+    copy.positions = h.positions[g].data();
+    copy.triangles = h.triangles[g].data();
+    copy.normals = h.normals[g].empty() ? nullptr : h.normals[g].data();
+    h.boxes[g] = geometry_box(copy);
+    h.vertex_base[g] = vert_total;
+    h.node_base[g] = (uint32_t)nodes;
+    h.tri_base[g] = (uint32_t)tri_total;
     nodes += BvhBuilder::node_count(geo.triangle_count);
     tri_total += geo.triangle_count;
     vert_total += geo.vertex_count;
-    max_tris = std::max(max_tris, geo.triangle_count);
-    if (geo.normals && geo.triangle_count) {
-      normal_base[g] = (uint32_t)normal_total;
+    if (copy.normals) {
+      h.normal_base[g] = (uint32_t)normal_total;
       normal_total += geo.triangle_count;
     }
   }
+  h.nodes = nodes;
+  h.materials.assign(s.materials, s.materials + s.material_count);
+  for (int k = 0; k < 3; ++k) h.environment_constant[k] = s.environment_constant[k];
+  R.host_instances.assign(s.instances, s.instances + s.instance_count);
   if (nodes >= kMaxSceneTriangles || tri_total >= kMaxSceneTriangles)
     return fail("the scene holds 2^28 triangles or more");
   if (!R.ok(R.blas.resize(std::max<uint64_t>(nodes, 1)), "BLAS pool", detail) ||
+      !R.ok(R.blas4.resize(R.blas.count), "BLAS pool", detail) ||
       !R.ok(R.tris.resize(kTriStride * std::max<uint64_t>(tri_total, 1)), "triangle pool", detail))
     return fail(detail);
-  // Staging: every geometry's positions and triangles in one upload.
-  std::vector<float> h_pos(3 * vert_total);
-  std::vector<uint32_t> h_tri(3 * tri_total);
-  std::vector<uint64_t> vbase(s.geometry_count);
+  // Every geometry's positions and triangles in one upload each; they stay
+  // resident for the incremental updates' rebuilds.
   {
-    uint64_t v = 0, t = 0;
-    for (uint32_t g = 0; g < s.geometry_count; ++g) {
-      const lotus_geometry& geo = s.geometries[g];
-      vbase[g] = v;
-      if (geo.vertex_count) std::memcpy(&h_pos[3 * v], geo.positions, 12ull * geo.vertex_count);
-      if (geo.triangle_count) std::memcpy(&h_tri[3 * t], geo.triangles, 12ull * geo.triangle_count);
-      v += geo.vertex_count;
-      t += geo.triangle_count;
+    std::vector<float> h_pos(3 * vert_total);
+    std::vector<uint32_t> h_tri(3 * tri_total);
+    for (uint32_t g = 0; g < ng; ++g) {
+      if (!h.positions[g].empty())
+        std::memcpy(&h_pos[3 * h.vertex_base[g]], h.positions[g].data(), 4 * h.positions[g].size());
+      if (!h.triangles[g].empty())
+        std::memcpy(&h_tri[3 * (size_t)h.tri_base[g]], h.triangles[g].data(), 4 * h.triangles[g].size());
     }
-  }
-  DeviceArray<float> d_pos;
-  DeviceArray<uint32_t> d_tri;
-  if (!R.ok(d_pos.upload(h_pos.data(), h_pos.size(), st), "positions", detail) ||
-      !R.ok(d_tri.upload(h_tri.data(), h_tri.size(), st), "triangles", detail))
-    return fail(detail);
-  {
-    // Geometries up to kSahMaxTriangles: binned SAH, all in one launch;
-    // larger ones: LBVH, one at a time.
-    std::vector<BatchGeometry> batch;
-    for (uint32_t g = 0; g < s.geometry_count; ++g) {
-      const lotus_geometry& geo = s.geometries[g];
-      if (!geo.triangle_count) continue;
-      if (geo.triangle_count <= kSahMaxTriangles) {
-        batch.push_back({vbase[g], tri_base[g], geo.triangle_count, node_base[g]});
-        continue;
-      }
-      cudaError_t e = R.builder.build_triangles(d_pos.ptr + 3 * vbase[g], d_tri.ptr + 3 * (size_t)tri_base[g],
-          geo.triangle_count, R.blas.ptr, node_base[g], R.tris.ptr, tri_base[g], st);
-      if (!R.ok(e, "BLAS build", detail)) return fail(detail);
-    }
-    if (!R.ok(R.builder.build_triangle_batch(d_pos.ptr, d_tri.ptr, batch, R.blas.ptr, R.tris.ptr, st,
-                  R.bvh_leaf_size),
-            "BLAS build", detail))
+    if (!R.ok(R.scene_pos.upload(h_pos.data(), h_pos.size(), st), "positions", detail) ||
+        !R.ok(R.scene_tri.upload(h_tri.data(), h_tri.size(), st), "triangles", detail))
       return fail(detail);
   }
+  std::vector<uint32_t> all(ng);
+  for (uint32_t g = 0; g < ng; ++g) all[g] = g;
+  if (!build_blases(R, all, true, detail)) return fail(detail);
   // Corner normals.
   if (normal_total) {
     std::vector<float> h_n(9 * normal_total);
-    for (uint32_t g = 0; g < s.geometry_count; ++g)
-      if (normal_base[g] != kNoLights)
-        std::memcpy(&h_n[9 * (size_t)normal_base[g]], s.geometries[g].normals,
-            36ull * s.geometries[g].triangle_count);
+    for (uint32_t g = 0; g < ng; ++g)
+      if (h.normal_base[g] != kNoLights)
+        std::memcpy(&h_n[9 * (size_t)h.normal_base[g]], h.normals[g].data(), 4 * h.normals[g].size());
     if (!R.ok(R.normals.upload(h_n.data(), h_n.size(), st), "normals", detail)) return fail(detail);
   } else {
     R.normals.release();
@@ -664,139 +895,30 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
   if (!R.ok(R.materials.upload(h_mat.data(), h_mat.size(), st), "materials", detail)) return fail(detail);
   // Environment.
   EnvDistribution env;
-  bool env_bound = false;
   if (s.environment && s.environment->texels && s.environment->width && s.environment->height) {
     env = build_env_distribution(*s.environment);
-    env_bound = env.mean > 0.0;
+    h.env_bound = env.mean > 0.0;
   }
-  if (env_bound) {
+  if (h.env_bound) {
     const size_t texels = (size_t)s.environment->width * s.environment->height;
     if (!R.ok(R.env_texels.upload(reinterpret_cast<const float4*>(s.environment->texels), texels, st),
             "environment texels", detail) ||
         !R.ok(R.env_floats.upload(env.floats.data(), env.floats.size(), st), "environment distribution",
             detail))
       return fail(detail);
+    h.env_mean = env.mean;
+    h.env_width = s.environment->width;
+    h.env_height = s.environment->height;
+    h.env_columns = env.columns;
+    h.env_rows = env.rows;
+    for (int k = 0; k < 3; ++k) h.env_scale[k] = s.environment->scale[k];
+    for (int k = 0; k < 9; ++k) h.env_frame[k] = s.environment->environment_from_world[k];
   } else {
     R.env_texels.release();
     R.env_floats.release();
   }
-  // Light table.
-  LightTable table = build_light_table(s, env_bound ? env.mean : 0.0);
-  if (!R.ok(R.lights.upload(table.records.data(), table.records.size(), st), "light table", detail) ||
-      !R.ok(R.light_verts.upload(table.verts.data(), table.verts.size(), st), "light corners", detail) ||
-      !R.ok(R.light_radiance.upload(table.radiance.data(), table.radiance.size(), st), "light radiance",
-          detail))
-    return fail(detail);
-  R.host_lights = table.records;
-  R.host_light_offsets = table.offsets;
-  R.host_instances.assign(s.instances, s.instances + s.instance_count);
-  // World bounds: each instance's geometry box through its transform.
-  {
-    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    std::vector<std::array<float, 6>> boxes(s.geometry_count);
-    for (uint32_t g = 0; g < s.geometry_count; ++g) {
-      std::array<float, 6> b = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-      const lotus_geometry& geo = s.geometries[g];
-      for (uint32_t v = 0; v < geo.vertex_count; ++v)
-        for (int a = 0; a < 3; ++a) {
-          b[a] = std::min(b[a], geo.positions[3 * (size_t)v + a]);
-          b[3 + a] = std::max(b[3 + a], geo.positions[3 * (size_t)v + a]);
-        }
-      boxes[g] = b;
-    }
-    for (uint32_t i = 0; i < s.instance_count; ++i) {
-      const std::array<float, 6>& b = boxes[s.instances[i].geometry];
-      if (!(b[0] <= b[3])) continue;
-      const float* m = s.instances[i].world_from_object;
-      for (int c = 0; c < 8; ++c) {
-        const float p[3] = {(c & 1) ? b[3] : b[0], (c & 2) ? b[4] : b[1], (c & 4) ? b[5] : b[2]};
-        for (int a = 0; a < 3; ++a) {
-          const float w = m[a] * p[0] + m[4 + a] * p[1] + m[8 + a] * p[2] + m[12 + a];
-          lo[a] = std::min(lo[a], w);
-          hi[a] = std::max(hi[a], w);
-        }
-      }
-    }
-    for (int a = 0; a < 3; ++a) {
-      R.scene_lo[a] = std::isfinite(lo[a]) ? lo[a] : 0.0f;
-      R.scene_hi[a] = std::isfinite(hi[a]) ? hi[a] : 1.0f;
-    }
-  }
-  // Instances.
-  std::vector<InstanceTraversal> h_trav(s.instance_count);
-  std::vector<InstanceShading> h_shade(s.instance_count);
-  for (uint32_t i = 0; i < s.instance_count; ++i) {
-    const lotus_instance& inst = s.instances[i];
-    const float* m = inst.world_from_object;
-    InstanceTraversal& t = h_trav[i];
-    InstanceShading& sh = h_shade[i];
-    if (!invert_affine(m, t.inv)) return fail("instance " + std::to_string(i) + " has a singular transform");
-    const lotus_geometry& geo = s.geometries[inst.geometry];
-    t.blas_root = geo.triangle_count ? node_base[inst.geometry] : (uint32_t)kEmptyChild;
-    t.flags = host_coverage(s.materials[inst.material]) >= 1.0f ? kInstanceOpaque : 0u;
-    t.material = inst.material;
-    t.light_offset = table.offsets[i];
-    for (int r = 0; r < 3; ++r) sh.m[r] = make_float4(m[r], m[4 + r], m[8 + r], m[12 + r]);
-    sh.material = inst.material;
-    sh.light_offset = table.offsets[i];
-    sh.normals = normal_base[inst.geometry];
-    // dot(c0, cross(c1, c2)) < 0 (scene.slang:1237-1240).
-    const float c0[3] = {m[0], m[1], m[2]}, c1[3] = {m[4], m[5], m[6]}, c2[3] = {m[8], m[9], m[10]};
-    const float x = c1[1] * c2[2] - c1[2] * c2[1], y = c1[2] * c2[0] - c1[0] * c2[2],
-                z = c1[0] * c2[1] - c1[1] * c2[0];
-    sh.mirror = (c0[0] * x + c0[1] * y + c0[2] * z) < 0.0f ? 1u : 0u;
-  }
-  if (!R.ok(R.inst_trav.upload(h_trav.data(), h_trav.size(), st), "instances", detail) ||
-      !R.ok(R.inst_shade.upload(h_shade.data(), h_shade.size(), st), "instances", detail) ||
-      !R.ok(R.tlas.resize(std::max<uint32_t>(BvhBuilder::node_count(s.instance_count), 1)), "TLAS", detail))
-    return fail(detail);
-  if (!R.ok(s.instance_count <= kSahMaxTriangles
-                ? R.builder.build_instances_sah(R.inst_shade.ptr, R.inst_trav.ptr, R.blas.ptr, s.instance_count,
-                      R.tlas.ptr, st)
-                : R.builder.build_instances(R.inst_shade.ptr, R.inst_trav.ptr, R.blas.ptr, s.instance_count,
-                      R.tlas.ptr, st),
-            "TLAS build", detail))
-    return fail(detail);
-  if (!R.ok(R.blas4.resize(R.blas.count), "BLAS pool", detail) ||
-      !R.ok(R.tlas4.resize(R.tlas.count), "TLAS", detail) ||
-      !R.ok(BvhBuilder::collapse(R.blas.ptr, (uint32_t)nodes, R.blas4.ptr, false, st), "BVH collapse", detail) ||
-      !R.ok(BvhBuilder::collapse(R.tlas.ptr, BvhBuilder::node_count(s.instance_count), R.tlas4.ptr, true, st),
-          "BVH collapse", detail))
-    return fail(detail);
-  cudaEventRecord(R.ev_stop, st);
-  if (!R.ok(cudaStreamSynchronize(st), "scene update", detail)) return fail(detail);
-  float ms = 0.0f;
-  cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
-  d_pos.release();
-  d_tri.release();
-
-  SceneView& v = R.view;
-  v = SceneView{};
-  v.tlas = R.tlas4.ptr;
-  v.blas = R.blas4.ptr;
-  v.tris = R.tris.ptr;
-  v.inst_trav = R.inst_trav.ptr;
-  v.inst_shade = R.inst_shade.ptr;
-  v.materials = R.materials.ptr;
-  v.normals = R.normals.ptr;
-  v.lights = R.lights.ptr;
-  v.light_verts = R.light_verts.ptr;
-  v.light_radiance = R.light_radiance.ptr;
-  v.env_texels = R.env_texels.ptr;
-  v.env_floats = R.env_floats.ptr;
-  v.instance_count = s.instance_count;
-  v.light_count = (uint32_t)table.records.size();
-  v.env_bound = env_bound ? 1u : 0u;
-  if (env_bound) {
-    v.env_width = s.environment->width;
-    v.env_height = s.environment->height;
-    v.env_columns = env.columns;
-    v.env_rows = env.rows;
-    for (int k = 0; k < 3; ++k) v.env_scale[k] = s.environment->scale[k];
-    for (int k = 0; k < 9; ++k) v.env_frame[k] = s.environment->environment_from_world[k];
-  }
-  v.env_selection = table.env_selection;
-  for (int k = 0; k < 3; ++k) v.env_constant[k] = s.environment_constant[k];
+  InstanceState inst;
+  if (!prepare_instances(R, inst, detail) || !submit_instances(R, inst, detail)) return fail(detail);
   // Default temporal identities: index and material slot, static, 6.
   {
     std::vector<TemporalInstance> ids(std::max<uint32_t>(s.instance_count, 1));
@@ -812,16 +934,104 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
       return fail(detail);
     R.temporal.instances_custom = false;
   }
-  R.scene_ready = true;
-  ++R.scene_generation;
-  res.status = LOTUS_PASS;
-  res.triangle_count = (uint32_t)tri_total;
-  res.instance_count = s.instance_count;
-  res.light_count = (uint32_t)table.records.size();
-  res.bvh_node_count = (uint32_t)nodes;
-  res.tlas_node_count = BvhBuilder::node_count(s.instance_count);
-  res.build_gpu_ms = ms;
-  res.device_bytes = R.scene_bytes();
+  if (finish_update(R, res, detail) != LOTUS_PASS) return fail(detail);
+  return LOTUS_PASS;
+}
+
+// Transform and material-slot edits of the resident scene's instances
+// (any count; the geometries, materials and environment stay).
+int32_t update_instances(Renderer& R, const lotus_instance* instances, uint32_t count, lotus_scene_result& res) {
+  std::string detail;
+  auto reject = [&](const std::string& d) {
+    copy_detail(res.detail, sizeof(res.detail), d);
+    return res.status = LOTUS_FAIL;
+  };
+  if (!R.scene_ready) return reject("no resident scene to update");
+  if (count && !instances) return reject("the instance array is missing");
+  for (uint32_t i = 0; i < count; ++i) {
+    const lotus_instance& inst = instances[i];
+    if (inst.geometry >= R.host.geometries.size() || inst.material >= R.host.materials.size())
+      return reject("instance " + std::to_string(i) + " names a missing geometry or material");
+    const float* m = inst.world_from_object;
+    if (m[3] != 0.0f || m[7] != 0.0f || m[11] != 0.0f || m[15] != 1.0f)
+      return reject("instance " + std::to_string(i) + " has a projective transform");
+    float4 rows[3];
+    if (!invert_affine(m, rows)) return reject("instance " + std::to_string(i) + " has a singular transform");
+  }
+  auto fail = [&](const std::string& d) {
+    R.failure = d;
+    R.release_scene();
+    return reject(d);
+  };
+  const bool same_count = count == R.host_instances.size();
+  R.host_instances.assign(instances, instances + count);
+  InstanceState inst;
+  if (!prepare_instances(R, inst, detail)) return fail(detail);
+  cudaEventRecord(R.ev_start, R.stream);
+  if (!submit_instances(R, inst, detail)) return fail(detail);
+  if (!R.temporal.instances_custom || !same_count) {
+    // Default temporal identities follow the new placements (identities a
+    // host set for another instance count no longer apply).
+    R.temporal.instances_custom = false;
+    std::vector<TemporalInstance> ids(std::max<uint32_t>(count, 1));
+    for (uint32_t i = 0; i < count; ++i) {
+      TemporalInstance& t = ids[i];
+      const float* m = instances[i].world_from_object;
+      for (int r = 0; r < 3; ++r) t.previous[r] = make_float4(m[r], m[4 + r], m[8 + r], m[12 + r]);
+      t.instance_id = i;
+      t.material_id = instances[i].material;
+      t.flags = 6u;
+    }
+    if (!R.ok(R.temporal.instances.upload(ids.data(), ids.size(), R.stream), "temporal identities", detail))
+      return fail(detail);
+  }
+  if (finish_update(R, res, detail) != LOTUS_PASS) return fail(detail);
+  return LOTUS_PASS;
+}
+
+// New positions (and corner normals) of one resident geometry with its
+// vertex and triangle counts and its triangles kept.
+int32_t update_geometry(Renderer& R, uint32_t geometry, const float* positions, uint32_t vertex_count,
+    const float* normals, lotus_scene_result& res) {
+  std::string detail;
+  auto reject = [&](const std::string& d) {
+    copy_detail(res.detail, sizeof(res.detail), d);
+    return res.status = LOTUS_FAIL;
+  };
+  if (!R.scene_ready) return reject("no resident scene to update");
+  HostScene& h = R.host;
+  if (geometry >= h.geometries.size()) return reject("no geometry " + std::to_string(geometry));
+  lotus_geometry& geo = h.geometries[geometry];
+  if (vertex_count != geo.vertex_count) return reject("a point edit keeps the geometry's vertex count");
+  if (vertex_count && !positions) return reject("the position array is missing");
+  if ((normals != nullptr) != (geo.normals != nullptr))
+    return reject("a point edit of a geometry with corner normals gives new ones, and none otherwise");
+  for (uint64_t i = 0; i < 3ull * vertex_count; ++i)
+    if (!std::isfinite(positions[i])) return reject("the geometry has a non-finite position");
+  auto fail = [&](const std::string& d) {
+    R.failure = d;
+    R.release_scene();
+    return reject(d);
+  };
+  cudaStream_t st = R.stream;
+  std::copy(positions, positions + 3ull * vertex_count, h.positions[geometry].begin());
+  if (normals) std::copy(normals, normals + 9ull * geo.triangle_count, h.normals[geometry].begin());
+  h.boxes[geometry] = geometry_box(geo);
+  InstanceState inst;
+  if (!prepare_instances(R, inst, detail)) return fail(detail);
+  cudaEventRecord(R.ev_start, st);
+  if (vertex_count &&
+      !R.ok(cudaMemcpyAsync(R.scene_pos.ptr + 3 * h.vertex_base[geometry], h.positions[geometry].data(),
+                12ull * vertex_count, cudaMemcpyHostToDevice, st),
+          "positions", detail))
+    return fail(detail);
+  if (normals && geo.triangle_count &&
+      !R.ok(cudaMemcpyAsync(R.normals.ptr + 9 * (size_t)h.normal_base[geometry], h.normals[geometry].data(),
+                36ull * geo.triangle_count, cudaMemcpyHostToDevice, st),
+          "normals", detail))
+    return fail(detail);
+  if (!build_blases(R, {geometry}, false, detail) || !submit_instances(R, inst, detail)) return fail(detail);
+  if (finish_update(R, res, detail) != LOTUS_PASS) return fail(detail);
   return LOTUS_PASS;
 }
 
@@ -1260,6 +1470,42 @@ int32_t lotus_cuda_update_scene(lotus_cuda_renderer* r, const lotus_scene_desc* 
   }
   cudaSetDevice(R.device);
   return update_scene(R, *scene, res);
+}
+
+int32_t lotus_cuda_update_instances(lotus_cuda_renderer* r, const lotus_instance* instances, uint32_t count,
+    lotus_scene_result* result) {
+  lotus_scene_result local{};
+  lotus_scene_result& res = result ? *result : local;
+  std::memset(&res, 0, sizeof(res));
+  if (!r) {
+    copy_detail(res.detail, sizeof(res.detail), "no renderer");
+    return res.status = LOTUS_FAIL;
+  }
+  Renderer& R = r->r;
+  if (!R.failure.empty()) {
+    copy_detail(res.detail, sizeof(res.detail), "the renderer failed earlier: " + R.failure);
+    return res.status = LOTUS_FAIL;
+  }
+  cudaSetDevice(R.device);
+  return update_instances(R, instances, count, res);
+}
+
+int32_t lotus_cuda_update_geometry(lotus_cuda_renderer* r, uint32_t geometry, const float* positions,
+    uint32_t vertex_count, const float* normals, lotus_scene_result* result) {
+  lotus_scene_result local{};
+  lotus_scene_result& res = result ? *result : local;
+  std::memset(&res, 0, sizeof(res));
+  if (!r) {
+    copy_detail(res.detail, sizeof(res.detail), "no renderer");
+    return res.status = LOTUS_FAIL;
+  }
+  Renderer& R = r->r;
+  if (!R.failure.empty()) {
+    copy_detail(res.detail, sizeof(res.detail), "the renderer failed earlier: " + R.failure);
+    return res.status = LOTUS_FAIL;
+  }
+  cudaSetDevice(R.device);
+  return update_geometry(R, geometry, positions, vertex_count, normals, res);
 }
 
 int32_t lotus_cuda_render(lotus_cuda_renderer* r, const lotus_frame_desc* frame, lotus_frame_result* result,

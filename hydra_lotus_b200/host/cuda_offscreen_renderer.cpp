@@ -105,6 +105,7 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
     ev.status = Lotus::FrameStatus::Pass;
     return ev;
   }
+  if (UpdateIncrementally(u, ev)) return ev;
   // Releases, then uploads (extraction.hpp:95-106).
   auto drop = [](auto& list, const void* p) {
     list.erase(std::remove_if(list.begin(), list.end(), [&](const auto& s) { return s.get() == p; }), list.end());
@@ -122,13 +123,11 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
   if (u.lights_changed && !u.lights.empty()) return fail("analytic lights are not built in the CUDA backend");
 
   // The scene description, rebuilt whole.
-  std::unordered_map<const Lotus::MeshGeometry*, uint32_t> slot;
   std::vector<lotus_geometry> geos(geometries_.size());
   std::vector<std::vector<float>> positions(geometries_.size()), normals(geometries_.size());
   std::vector<std::vector<uint32_t>> triangles(geometries_.size());
   for (size_t g = 0; g < geometries_.size(); ++g) {
     const Lotus::MeshGeometry& m = *geometries_[g];
-    slot[&m] = (uint32_t)g;
     positions[g].reserve(3 * m.positions.size());
     for (const auto& p : m.positions) positions[g].insert(positions[g].end(), p.begin(), p.end());
     triangles[g].reserve(3 * m.triangles.size());
@@ -174,14 +173,10 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
     mats[0].transmission_color[0] = mats[0].transmission_color[1] = mats[0].transmission_color[2] = 1.0f;
     mats[0].opacity = 1.0f;
   }
-  std::vector<lotus_instance> insts(instances_.size());
-  for (size_t i = 0; i < instances_.size(); ++i) {
-    const Lotus::SceneInstance& si = instances_[i];
-    const auto it = slot.find(si.geometry);
-    if (it == slot.end()) return fail("instance " + std::to_string(i) + " names a geometry that is not resident");
-    std::memcpy(insts[i].world_from_object, si.world_from_object.data(), 64);
-    insts[i].geometry = it->second;
-    insts[i].material = si.material;
+  std::vector<lotus_instance> insts;
+  {
+    std::string error;
+    if (!InstanceArray(insts, error)) return fail(error);
   }
   lotus_environment env{};
   std::vector<float> env_texels;
@@ -216,19 +211,111 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
     failure_ = ev.detail;
     return ev;
   }
+  resident_ = true;
   device_bytes_ = res.device_bytes;
+  material_slots_ = (uint32_t)mats.size();
+  environment_map_bound_ = env.texels != nullptr;
+  SceneStats(u, res, ev);
+  return ev;
+}
+
+void CudaOffscreenRenderer::SceneStats(const Lotus::SceneUpdate& u, const lotus_scene_result& res,
+    Lotus::GpuSceneEvidence& ev) const {
   ev.stats.source_revision = u.source_revision;
   ev.stats.resident_geometries = (uint32_t)geometries_.size();
   ev.stats.instance_count = res.instance_count;
-  ev.stats.material_count = (uint32_t)mats.size();
-  ev.stats.environment_map = env.texels != nullptr;
+  ev.stats.material_count = material_slots_;
+  ev.stats.environment_map = environment_map_bound_;
   ev.stats.resident_textures = (uint32_t)textures_.size();
   ev.stats.acceleration_available = true;
   ev.stats.blas_count = (uint32_t)geometries_.size();
   ev.stats.tlas_instance_count = res.instance_count;
   ev.timings.available = true;
   ev.timings.blas_build_gpu_ms = res.build_gpu_ms;
-  return ev;
+}
+
+// The resident instances in the C ABI's form: geometry slots are the
+// positions in geometries_.
+bool CudaOffscreenRenderer::InstanceArray(std::vector<lotus_instance>& insts, std::string& error) const {
+  std::unordered_map<const Lotus::MeshGeometry*, uint32_t> slot;
+  for (size_t g = 0; g < geometries_.size(); ++g) slot[geometries_[g].get()] = (uint32_t)g;
+  insts.assign(instances_.size(), lotus_instance{});
+  for (size_t i = 0; i < instances_.size(); ++i) {
+    const Lotus::SceneInstance& si = instances_[i];
+    const auto it = slot.find(si.geometry);
+    if (it == slot.end()) {
+      error = "instance " + std::to_string(i) + " names a geometry that is not resident";
+      return false;
+    }
+    std::memcpy(insts[i].world_from_object, si.world_from_object.data(), 64);
+    insts[i].geometry = it->second;
+    insts[i].material = si.material;
+  }
+  return true;
+}
+
+bool CudaOffscreenRenderer::UpdateIncrementally(const Lotus::SceneUpdate& u, Lotus::GpuSceneEvidence& ev) {
+  if (!resident_ || !u.texture_releases.empty() || !u.texture_uploads.empty() || u.materials_changed ||
+      u.environment_changed || (u.lights_changed && !u.lights.empty()))
+    return false;
+  // Every release and upload must be one side of a replacement whose
+  // topology (vertex count, triangles, presence of corner normals) is kept.
+  if (u.geometry_releases.size() != u.geometry_replacements.size() ||
+      u.geometry_uploads.size() != u.geometry_replacements.size())
+    return false;
+  std::vector<std::pair<size_t, std::shared_ptr<const Lotus::MeshGeometry>>> edits;
+  for (const Lotus::SceneGeometryReplacement& r : u.geometry_replacements) {
+    size_t at = geometries_.size();
+    for (size_t g = 0; g < geometries_.size(); ++g)
+      if (geometries_[g].get() == r.previous) at = g;
+    std::shared_ptr<const Lotus::MeshGeometry> next;
+    for (const auto& up : u.geometry_uploads)
+      if (up.get() == r.replacement) next = up;
+    if (at == geometries_.size() || !next || !r.previous) return false;
+    const Lotus::MeshGeometry& a = *r.previous;
+    const Lotus::MeshGeometry& b = *next;
+    if (a.positions.size() != b.positions.size() || a.triangles != b.triangles ||
+        a.normals.empty() != b.normals.empty() || (!b.normals.empty() && b.normals.size() != 3 * b.triangles.size()))
+      return false;
+    edits.emplace_back(at, next);
+  }
+  if (edits.empty() && !u.instances_changed) return false;
+  auto fail = [&](const lotus_scene_result& res, int32_t s) {
+    ev.status = to_status(s);
+    ev.detail = res.detail;
+    failed_ = true;
+    failure_ = ev.detail;
+    return true;
+  };
+  lotus_scene_result res{};
+  for (const auto& [at, next] : edits) {
+    std::vector<float> positions, normals;
+    positions.reserve(3 * next->positions.size());
+    for (const auto& p : next->positions) positions.insert(positions.end(), p.begin(), p.end());
+    for (const auto& n : next->normals) normals.insert(normals.end(), n.begin(), n.end());
+    const int32_t s = lotus_cuda_update_geometry(handle_, (uint32_t)at, positions.data(),
+        (uint32_t)next->positions.size(), normals.empty() ? nullptr : normals.data(), &res);
+    if (s != LOTUS_PASS) return fail(res, s);
+    geometries_[at] = next;
+  }
+  if (u.instances_changed) {
+    instances_ = u.instances;
+    std::vector<lotus_instance> insts;
+    std::string error;
+    if (!InstanceArray(insts, error)) {
+      ev.status = Lotus::FrameStatus::Fail;
+      ev.detail = error;
+      failed_ = true;
+      failure_ = error;
+      return true;
+    }
+    const int32_t s = lotus_cuda_update_instances(handle_, insts.data(), (uint32_t)insts.size(), &res);
+    if (s != LOTUS_PASS) return fail(res, s);
+  }
+  ev.status = Lotus::FrameStatus::Pass;
+  device_bytes_ = res.device_bytes;
+  SceneStats(u, res, ev);
+  return true;
 }
 
 bool CudaOffscreenRenderer::FillFrame(const Lotus::Matrix4& world_to_clip, const Lotus::OffscreenTarget& t,

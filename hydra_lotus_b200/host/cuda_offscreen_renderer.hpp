@@ -67,6 +67,13 @@ class CudaOffscreenRenderer final : public Lotus::OffscreenRenderer {
       std::string& error) const;
   void FillEvidence(const lotus_frame_desc& frame, const lotus_frame_result& result, std::vector<float>& color,
       Lotus::GpuFrameEvidence& evidence);
+  // Plans that change instances only, or replace geometries with ones of
+  // the same topology (SceneGeometryReplacement), go to the incremental
+  // entry points; returns false when the plan needs a full update.
+  bool UpdateIncrementally(const Lotus::SceneUpdate& update, Lotus::GpuSceneEvidence& evidence);
+  bool InstanceArray(std::vector<lotus_instance>& out, std::string& error) const;
+  void SceneStats(const Lotus::SceneUpdate& update, const lotus_scene_result& result,
+      Lotus::GpuSceneEvidence& evidence) const;
 
   int device_;
   lotus_cuda_renderer* handle_;
@@ -80,6 +87,9 @@ class CudaOffscreenRenderer final : public Lotus::OffscreenRenderer {
   std::array<float, 3> environment_{};
   std::optional<Lotus::SceneEnvironmentMap> environment_map_;
   std::uint64_t device_bytes_ = 0;
+  bool resident_ = false;  // a full update has made the scene resident
+  std::uint32_t material_slots_ = 0;
+  bool environment_map_bound_ = false;
   // The preceding temporal frame's camera.
   bool have_previous_camera_ = false;
   Lotus::Camera previous_camera_;

@@ -44,6 +44,12 @@ def lib():
         L.lotus_cuda_update_scene.restype = C.c_int32
         L.lotus_cuda_update_scene.argtypes = [C.c_void_p, C.POINTER(abi.SceneDesc),
                                               C.POINTER(abi.SceneResult)]
+        L.lotus_cuda_update_instances.restype = C.c_int32
+        L.lotus_cuda_update_instances.argtypes = [C.c_void_p, C.POINTER(abi.Instance), C.c_uint32,
+                                                  C.POINTER(abi.SceneResult)]
+        L.lotus_cuda_update_geometry.restype = C.c_int32
+        L.lotus_cuda_update_geometry.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.c_uint32,
+                                                 C.POINTER(C.c_float), C.POINTER(abi.SceneResult)]
         L.lotus_cuda_render.restype = C.c_int32
         L.lotus_cuda_render.argtypes = [C.c_void_p, C.POINTER(abi.FrameDesc),
                                         C.POINTER(abi.FrameResult), C.c_void_p]
@@ -158,6 +164,29 @@ class CudaOffscreenRenderer:
         lotus_scene_result."""
         res = abi.SceneResult()
         lib().lotus_cuda_update_scene(self.handle, C.byref(scene.desc()), C.byref(res))
+        self.scene = scene
+        return res
+
+    def update_instances(self, scene):
+        """UpdateScene for an instance-only change (lotus_cuda_update_instances):
+        the resident scene takes `scene`'s instances; its geometries,
+        materials and environment stay as uploaded. Returns the
+        lotus_scene_result."""
+        d = scene.desc()
+        res = abi.SceneResult()
+        lib().lotus_cuda_update_instances(self.handle, d.instances, d.instance_count, C.byref(res))
+        self.scene = scene
+        return res
+
+    def update_geometry(self, scene, geometry):
+        """UpdateScene for a point edit (lotus_cuda_update_geometry): the
+        resident geometry `geometry` takes `scene`'s positions (and corner
+        normals) for it. Returns the lotus_scene_result."""
+        p, _, n = scene.geometries[geometry]
+        res = abi.SceneResult()
+        lib().lotus_cuda_update_geometry(
+            self.handle, geometry, p.ctypes.data_as(C.POINTER(C.c_float)), p.shape[0],
+            n.ctypes.data_as(C.POINTER(C.c_float)) if n is not None else C.POINTER(C.c_float)(), C.byref(res))
         self.scene = scene
         return res
 

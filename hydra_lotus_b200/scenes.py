@@ -154,6 +154,25 @@ class Scene:
         self._desc = None
         return len(self.instances) - 1
 
+    def set_instance(self, index, world_from_object=None, material=None):
+        """Edits instance `index`: its transform and/or material slot."""
+        m, g, mat = self.instances[index]
+        if world_from_object is not None:
+            m = np.asarray(world_from_object, dtype=F32).copy()
+        self.instances[index] = (m, g, mat if material is None else material)
+        self._desc = None
+
+    def set_positions(self, geometry, positions, normals=None):
+        """A point edit of `geometry`: new positions (same vertex count) and,
+        when it has corner normals, new ones."""
+        p, t, n = self.geometries[geometry]
+        positions = np.ascontiguousarray(positions, dtype=F32).reshape(-1, 3)
+        assert positions.shape == p.shape
+        if normals is not None:
+            normals = np.ascontiguousarray(normals, dtype=F32).reshape(-1, 3, 3)
+        self.geometries[geometry] = (positions, t, normals if n is not None else None)
+        self._desc = None
+
     def set_environment(self, texels, scale=(1.0, 1.0, 1.0), rows=None):
         texels = np.ascontiguousarray(texels, dtype=F32)
         assert texels.ndim == 3 and texels.shape[2] == 4
@@ -579,6 +598,30 @@ def batch_workload(count=64, seed=0):
         size = int(rng.choice([256, 512, 768, 1024]))
         out.append(batch_room(seed=seed * 1000 + k, triangles=tris, size=size))
     return out
+
+
+def grid_mesh(quads=512, size=96):
+    """One indexed grid of quads x quads quads in the xz-plane (512: 524,288
+    triangles and 263,169 vertices, the shape of the reference's
+    `geometry-v1` workload), gently displaced, under a constant sky, with
+    the camera above it."""
+    s = Scene(f"grid-{quads}")
+    k = np.arange(quads + 1, dtype=np.float64) / quads * 2.0 - 1.0
+    x, z = np.meshgrid(k, k, indexing="xy")
+    y = 0.05 * np.sin(6.0 * x) * np.cos(5.0 * z)
+    p = np.stack([x, y, z], axis=-1).reshape(-1, 3).astype(F32)
+    i = np.arange(quads, dtype=np.uint32)
+    a = (i[None, :] + (quads + 1) * i[:, None]).reshape(-1)
+    b, c, d = a + 1, a + quads + 1, a + quads + 2
+    f = np.stack([np.stack([a, c, b], -1), np.stack([b, c, d], -1)], axis=1).reshape(-1, 3)
+    g = s.add_geometry(p, f)
+    s.add_instance(g, s.add_material(preview_material((0.6, 0.6, 0.6), roughness=0.5, ior=1.0)))
+    s.add_instance(s.add_geometry(*quad([[-0.3, 1.5, -0.3], [0.3, 1.5, -0.3], [0.3, 1.5, 0.3], [-0.3, 1.5, 0.3]])),
+                   s.add_material(preview_material((0.0, 0.0, 0.0), ior=1.0, emission=(20.0, 20.0, 20.0))))
+    s.environment_constant = (0.3, 0.35, 0.4)
+    s.world_to_clip = multiply(perspective(50.0, 1.0, 0.1, 100.0), look_at((0.0, 2.2, 2.2), (0.0, 0.0, 0.0)))
+    s.width = s.height = size
+    return s
 
 
 def big_mesh(seed=0, size=96, subdivisions=6):

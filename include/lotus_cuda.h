@@ -9,6 +9,8 @@
  *
  *   CreateOffscreenRenderer  (vulkan_backend.hpp:879-883)  -> lotus_cuda_create
  *   UpdateScene(SceneUpdate) (vulkan_backend.hpp:816-817)  -> lotus_cuda_update_scene
+ *     (instance-only and point-edit updates: lotus_cuda_update_instances,
+ *      lotus_cuda_update_geometry)
  *   RenderScene(...)         (vulkan_backend.hpp:789-791)  -> lotus_cuda_render
  *   RayQueryCapability()     (vulkan_backend.hpp:767)      -> lotus_cuda_capability
  *   ~OffscreenRenderer       (vulkan_backend.hpp:757)      -> lotus_cuda_destroy
@@ -257,6 +259,26 @@ void lotus_cuda_destroy(lotus_cuda_renderer* renderer);
  * than 2^28 triangles. */
 int32_t lotus_cuda_update_scene(lotus_cuda_renderer* renderer,
     const lotus_scene_desc* scene, lotus_scene_result* result);
+
+/* UpdateScene with a SceneUpdate that changes instances only (transform
+ * edits, material slots; vulkan_backend.cpp's TLAS-only update path): the
+ * resident scene's instances become `instances` (any count, naming its
+ * geometries and materials). Rebuilds the light table, the instance records
+ * and the TLAS; the BLASes, materials and environment stay. Restarts the
+ * accumulation. Invalid instances Fail without poisoning; the scene is
+ * unchanged then. build_gpu_ms counts the uploads and builds. */
+int32_t lotus_cuda_update_instances(lotus_cuda_renderer* renderer,
+    const lotus_instance* instances, uint32_t count, lotus_scene_result* result);
+
+/* UpdateScene with a compatible point edit of one geometry (its triangles
+ * and vertex count kept; the reference refits, gpu_scene.cpp:2303-2322):
+ * the resident geometry `geometry` takes new positions (and new corner
+ * normals, which a geometry with corner normals must be given and one
+ * without must not). Rebuilds that geometry's BLAS in place, then the
+ * light table, instance records and TLAS. Restarts the accumulation. The
+ * images equal those of lotus_cuda_update_scene with the edited scene. */
+int32_t lotus_cuda_update_geometry(lotus_cuda_renderer* renderer, uint32_t geometry,
+    const float* positions, uint32_t vertex_count, const float* normals, lotus_scene_result* result);
 
 /* RenderScene (vulkan_backend.hpp:789-791), Radiance output: adds
  * frame_count samples per pixel (up to max_samples) to the accumulation and

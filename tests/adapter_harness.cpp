@@ -18,6 +18,7 @@
 // f32 world_to_clip[16], u32 width, height, integrator, light_sampling,
 // max_bounces, sample_index, frame_count.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iostream>
@@ -52,8 +53,10 @@ const char* status_name(Lotus::FrameStatus s) {
 }  // namespace
 
 int main(int argc, char** argv) {
-  if (argc != 3) {
-    std::fprintf(stderr, "usage: adapter_harness <scene file> <output floats>\n");
+  if (argc != 3 && argc != 6) {
+    std::fprintf(stderr,
+        "usage: adapter_harness <scene file> <output floats> "
+        "[<dx> <after instance edit floats> <after point edit floats>]\n");
     return 2;
   }
   Reader in;
@@ -176,7 +179,51 @@ int main(int argc, char** argv) {
       status_name(frame.status), frame.detail.c_str(), frame.samples_per_pixel, frame.wavefront_rounds,
       frame.wavefront_path_counts.size(), frame.color.pixel_format.c_str(), frame.color.row_pitch,
       frame.color.payload.size(), status_name(bootstrap.status), status_name(present.status));
-  std::ofstream out(argv[2], std::ios::binary);
-  out.write(reinterpret_cast<const char*>(frame.color.payload.data()), (std::streamsize)frame.color.payload.size());
-  return frame.status == Lotus::FrameStatus::Pass ? 0 : 1;
+  {
+    std::ofstream out(argv[2], std::ios::binary);
+    out.write(reinterpret_cast<const char*>(frame.color.payload.data()), (std::streamsize)frame.color.payload.size());
+  }
+  if (frame.status != Lotus::FrameStatus::Pass) return 1;
+  if (argc == 3) return 0;
+  // Edits, as a host's SceneExtraction plans them: an instance-only plan
+  // (instance 0 moves by dx), then a geometry replacement with the same
+  // topology (geometry 0's positions y += 0.01 x) whose instances name the
+  // replacement.
+  const float dx = std::strtof(argv[3], nullptr);
+  Lotus::SceneUpdate moved;
+  moved.source_revision = 2;
+  moved.instances_changed = true;
+  moved.instances = update.instances;
+  moved.instances[0].world_from_object[12] += dx;
+  const Lotus::GpuSceneEvidence s2 = renderer->UpdateScene(moved);
+  const Lotus::GpuFrameEvidence f2 = renderer->RenderScene(draw, target, frame_count, settings);
+  auto replacement = std::make_shared<Lotus::MeshGeometry>(*meshes[0]);
+  for (auto& p : replacement->positions) p[1] += 0.01f * p[0];
+  Lotus::SceneUpdate edited;
+  edited.source_revision = 3;
+  edited.geometry_releases.push_back(meshes[0].get());
+  edited.geometry_uploads.push_back(replacement);
+  edited.geometry_replacements.push_back({meshes[0].get(), replacement.get()});
+  edited.instances_changed = true;
+  edited.instances = moved.instances;
+  for (auto& inst : edited.instances)
+    if (inst.geometry == meshes[0].get()) inst.geometry = replacement.get();
+  const Lotus::GpuSceneEvidence s3 = renderer->UpdateScene(edited);
+  const Lotus::GpuFrameEvidence f3 = renderer->RenderScene(draw, target, frame_count, settings);
+  std::printf("{\"instance_edit\": \"%s\", \"instance_edit_render\": \"%s\", \"point_edit\": \"%s\", "
+              "\"point_edit_render\": \"%s\", \"detail\": \"%s%s\"}\n",
+      status_name(s2.status), status_name(f2.status), status_name(s3.status), status_name(f3.status),
+      s2.detail.c_str(), s3.detail.c_str());
+  {
+    std::ofstream out(argv[4], std::ios::binary);
+    out.write(reinterpret_cast<const char*>(f2.color.payload.data()), (std::streamsize)f2.color.payload.size());
+  }
+  {
+    std::ofstream out(argv[5], std::ios::binary);
+    out.write(reinterpret_cast<const char*>(f3.color.payload.data()), (std::streamsize)f3.color.payload.size());
+  }
+  return s2.status == Lotus::FrameStatus::Pass && f2.status == Lotus::FrameStatus::Pass &&
+                 s3.status == Lotus::FrameStatus::Pass && f3.status == Lotus::FrameStatus::Pass
+             ? 0
+             : 1;
 }

@@ -42,14 +42,25 @@ def write(path, scene, settings, frame_count):
         f.write(b"".join(out))
 
 
-def run(tmpdir, scene, settings, frame_count):
-    """(exit code, evidence dict, colour (H, W, 4) or None)."""
+def _image(path, scene):
+    if os.path.exists(path) and os.path.getsize(path) == scene.width * scene.height * 16:
+        return np.fromfile(path, dtype=np.float32).reshape(scene.height, scene.width, 4)
+    return None
+
+
+def run(tmpdir, scene, settings, frame_count, edit_dx=None):
+    """(exit code, evidence dict, colour (H, W, 4) or None). With edit_dx,
+    the driver then moves instance 0 by edit_dx in x (an instance-only
+    plan) and edits geometry 0 (y += 0.01 x, a same-topology replacement),
+    rendering after each: returns (code, [evidence dicts], [3 colours])."""
     inp = os.path.join(tmpdir, "scene.bin")
-    outp = os.path.join(tmpdir, "color.bin")
+    outs = [os.path.join(tmpdir, f"color{k}.bin") for k in range(3)]
     write(inp, scene, settings, frame_count)
-    p = subprocess.run([HARNESS, inp, outp], capture_output=True, text=True, timeout=600)
-    evidence = json.loads(p.stdout.strip().splitlines()[-1]) if p.stdout.strip() else {}
-    color = None
-    if os.path.exists(outp) and os.path.getsize(outp) == scene.width * scene.height * 16:
-        color = np.fromfile(outp, dtype=np.float32).reshape(scene.height, scene.width, 4)
-    return p.returncode, evidence, color
+    args = [HARNESS, inp, outs[0]]
+    if edit_dx is not None:
+        args += [repr(float(edit_dx)), outs[1], outs[2]]
+    p = subprocess.run(args, capture_output=True, text=True, timeout=600)
+    lines = [json.loads(line) for line in p.stdout.strip().splitlines() if line.startswith("{")]
+    if edit_dx is None:
+        return p.returncode, (lines[-1] if lines else {}), _image(outs[0], scene)
+    return p.returncode, lines, [_image(o, scene) for o in outs]

@@ -49,3 +49,32 @@ def test_adapter_renders_what_the_c_abi_renders(cuda, harness, tmp_path, integra
         cuda.check(res, "render_scene")
     assert color is not None
     assert np.array_equal(color, want), f"{np.count_nonzero(color != want)} values differ"
+
+
+def test_adapter_incremental_updates_render_what_full_updates_render(cuda, harness, tmp_path):
+    """An instance-only SceneUpdate and a same-topology geometry replacement
+    go through lotus_cuda_update_instances / lotus_cuda_update_geometry and
+    give the images a full update of the edited scene gives."""
+    scene = scenes.box_room(seed=0, size=48)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=5, sample_index=3)
+    code, evidence, colors = adapter_scene.run(str(tmp_path), scene, st, 4, edit_dx=0.05)
+    assert code == 0, evidence
+    assert evidence[-1]["instance_edit"] == "pass" and evidence[-1]["point_edit"] == "pass", evidence
+    moved = scenes.box_room(seed=0, size=48)
+    m = np.array(moved.instances[0][0], dtype=np.float32)
+    m[12] += np.float32(0.05)
+    moved.set_instance(0, m)
+    edited = scenes.box_room(seed=0, size=48)
+    edited.set_instance(0, m)
+    p, t, n = edited.geometries[0]
+    q = p.copy()
+    q[:, 1] += np.float32(0.01) * p[:, 0]
+    edited.set_positions(0, q)
+    for want_scene, got in ((moved, colors[1]), (edited, colors[2])):
+        with cuda.CudaOffscreenRenderer(0) as r:
+            cuda.check(r.update_scene(want_scene), "update_scene")
+            res, want = r.render_scene(want_scene.frame(st, frame_count=4))
+            cuda.check(res, "render_scene")
+        assert got is not None
+        assert np.array_equal(got, want), f"{np.count_nonzero(got != want)} values differ"
