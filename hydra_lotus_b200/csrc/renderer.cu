@@ -208,6 +208,26 @@ EnvDistribution build_env_distribution(const lotus_environment& e) {
   return d;
 }
 
+// Guide tables of the environment's cumulative distributions (the
+// marginal's, then each row's conditional's): entry k of a table with K
+// buckets counts the CDF entries <= k / K, so the device's FindInterval
+// searches only the entries between two consecutive guide values.
+std::vector<uint32_t> build_env_guides(const EnvDistribution& d) {
+  std::vector<uint32_t> g((kEnvGuideMarginal + 1) + (size_t)d.rows * (kEnvGuideConditional + 1));
+  const size_t cells = (size_t)d.columns * d.rows;
+  auto fill = [](const float* F, uint32_t entries, uint32_t buckets, uint32_t* out) {
+    for (uint32_t k = 0; k <= buckets; ++k) {
+      const float x = (float)k / (float)buckets;
+      out[k] = (uint32_t)(std::upper_bound(F, F + entries, x) - F);
+    }
+  };
+  fill(d.floats.data() + cells, d.rows + 1, kEnvGuideMarginal, g.data());
+  for (uint32_t row = 0; row < d.rows; ++row)
+    fill(d.floats.data() + cells + d.rows + 1 + (size_t)row * (d.columns + 1), d.columns + 1,
+        kEnvGuideConditional, g.data() + (kEnvGuideMarginal + 1) + (size_t)row * (kEnvGuideConditional + 1));
+  return g;
+}
+
 // The light table (BuildLightTable, gpu_scene.cpp:515-610): every emissive
 // triangle weighted by its mean emission times its world area, then the
 // environment image weighted as a distant light over the scene's bounding
@@ -390,6 +410,7 @@ struct Renderer {
   DeviceArray<float4> light_verts, light_radiance;
   DeviceArray<float4> env_texels;
   DeviceArray<float> env_floats;
+  DeviceArray<uint32_t> env_guide;
   std::vector<LightRecord> host_lights;
   std::vector<uint32_t> host_light_offsets;
   SceneView view{};
@@ -501,14 +522,14 @@ struct Renderer {
     scene_pos.release(); scene_tri.release(); host = HostScene{};
     blas.release(); tlas.release(); blas4.release(); tlas4.release(); tris.release(); inst_trav.release(); inst_shade.release();
     materials.release(); normals.release(); lights.release(); light_verts.release();
-    light_radiance.release(); env_texels.release(); env_floats.release();
+    light_radiance.release(); env_texels.release(); env_floats.release(); env_guide.release();
     scene_ready = false;
   }
 
   uint64_t scene_bytes() const {
     return scene_pos.bytes() + scene_tri.bytes() + blas.bytes() + tlas.bytes() + blas4.bytes() + tlas4.bytes() + tris.bytes() + inst_trav.bytes() + inst_shade.bytes() +
            materials.bytes() + normals.bytes() + lights.bytes() + light_verts.bytes() +
-           light_radiance.bytes() + env_texels.bytes() + env_floats.bytes();
+           light_radiance.bytes() + env_texels.bytes() + env_floats.bytes() + env_guide.bytes();
   }
 };
 
@@ -718,6 +739,7 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
   v.light_radiance = R.light_radiance.ptr;
   v.env_texels = R.env_texels.ptr;
   v.env_floats = R.env_floats.ptr;
+  v.env_guide = R.env_guide.ptr;
   v.instance_count = n;
   v.light_count = (uint32_t)in.table.records.size();
   v.env_bound = h.env_bound ? 1u : 0u;
@@ -906,6 +928,9 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
         !R.ok(R.env_floats.upload(env.floats.data(), env.floats.size(), st), "environment distribution",
             detail))
       return fail(detail);
+    const std::vector<uint32_t> guides = build_env_guides(env);
+    if (!R.ok(R.env_guide.upload(guides.data(), guides.size(), st), "environment guide tables", detail))
+      return fail(detail);
     h.env_mean = env.mean;
     h.env_width = s.environment->width;
     h.env_height = s.environment->height;
@@ -916,6 +941,7 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
   } else {
     R.env_texels.release();
     R.env_floats.release();
+    R.env_guide.release();
   }
   InstanceState inst;
   if (!prepare_instances(R, inst, detail) || !submit_instances(R, inst, detail)) return fail(detail);

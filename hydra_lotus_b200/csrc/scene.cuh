@@ -114,6 +114,7 @@ struct SceneView {
   const float4* __restrict__ light_radiance;// emission * coverage per light entry
   const float4* __restrict__ env_texels;
   const float* __restrict__ env_floats;     // density, marginal, conditional
+  const uint32_t* __restrict__ env_guide;   // guide tables of the marginal and each conditional
   uint32_t instance_count;
   uint32_t light_count;
   uint32_t env_bound;
@@ -123,6 +124,11 @@ struct SceneView {
   float env_frame[9];       // rows of environment_from_world
   float env_constant[3];
 };
+
+// Buckets of the environment distribution's guide tables (powers of two):
+// the marginal's, then each row's conditional's, kEnv* + 1 entries each.
+constexpr uint32_t kEnvGuideMarginal = 1024;
+constexpr uint32_t kEnvGuideConditional = 512;
 
 struct Hit {
   uint32_t instance;

@@ -128,10 +128,15 @@ __device__ __forceinline__ LightSample sample_triangle(const SceneView& S, uint3
   return s;
 }
 
-// FindInterval (scene.slang:775-789).
+// FindInterval (scene.slang:775-789): the largest i in [0, count) with
+// F[i] <= u. The binary search counts the entries <= u; a guide table
+// (entry k: the entries <= k / K, K a power of two so k / K and u * K are
+// exact) narrows it to [guide[k], guide[k + 1]] for the u of bucket k, the
+// same answer as a search over all count + 1 entries.
 __device__ __forceinline__ uint32_t find_interval(const float* __restrict__ F, uint64_t first,
-    uint32_t count, float u) {
-  uint32_t low = 0, len = count + 1;
+    uint32_t count, float u, const uint32_t* __restrict__ guide, uint32_t buckets) {
+  const uint32_t k = min((uint32_t)(u * float(buckets)), buckets - 1u);
+  uint32_t low = guide[k], len = guide[k + 1] - guide[k];
   while (len > 0) {
     const uint32_t half = len >> 1;
     const uint32_t middle = low + half;
@@ -147,8 +152,8 @@ __device__ __forceinline__ uint32_t find_interval(const float* __restrict__ F, u
 
 // SampleCumulative (scene.slang:794-800).
 __device__ __forceinline__ float sample_cumulative(const float* __restrict__ F, uint64_t first,
-    uint32_t count, float u, uint32_t& cell) {
-  cell = find_interval(F, first, count, u);
+    uint32_t count, float u, uint32_t& cell, const uint32_t* __restrict__ guide, uint32_t buckets) {
+  cell = find_interval(F, first, count, u, guide, buckets);
   const float low = F[first + cell];
   const float width = F[first + cell + 1] - low;
   const float offset = width > 0.0f ? (u - low) / width : 0.5f;
@@ -208,9 +213,10 @@ __device__ __forceinline__ LightSample sample_environment(const SceneView& S, fl
     float ux, float uy) {
   const uint64_t cells = (uint64_t)S.env_columns * S.env_rows;
   uint32_t row, column;
-  const float v = sample_cumulative(S.env_floats, cells, S.env_rows, ux, row);
+  const float v = sample_cumulative(S.env_floats, cells, S.env_rows, ux, row, S.env_guide, kEnvGuideMarginal);
   const float u = sample_cumulative(S.env_floats,
-      cells + S.env_rows + 1 + (uint64_t)row * (S.env_columns + 1), S.env_columns, uy, column);
+      cells + S.env_rows + 1 + (uint64_t)row * (S.env_columns + 1), S.env_columns, uy, column,
+      S.env_guide + (kEnvGuideMarginal + 1) + (size_t)row * (kEnvGuideConditional + 1), kEnvGuideConditional);
   const float sin_theta = lsin(kPi * v);
   const float density = S.env_floats[(uint64_t)row * S.env_columns + column];
   if (!(sin_theta > 0.0f) || !(density > 0.0f)) return no_light();
