@@ -28,6 +28,9 @@ def main():
     ap.add_argument("--temporal", action="store_true",
                     help="temporal frames of the many-light room: ReSTIR DI (temporal + spatial) and SVGF")
     ap.add_argument("--filter", type=int, default=5, help="a-trous iterations of the temporal frames")
+    ap.add_argument("--updates", action="store_true",
+                    help="scene upload and edits on the 512x512-quad grid (the geometry-v1 shape): one full "
+                         "update, one point edit, one transform edit")
     ap.add_argument("--batch", type=int, default=0,
                     help="render the first N scenes of the 64-scene batch workload as one wavefront")
     args = ap.parse_args()
@@ -54,6 +57,23 @@ def main():
                 previous = (view, w2c)
                 rays = res.camera_rays + res.extension_rays + res.shadow_rays
                 print(json.dumps({"frame": k, "rays": rays, "gpu_ms": round(res.gpu_ms, 3)}))
+        return
+    if args.updates:
+        grid = scenes.grid_mesh(quads=512)
+        with renderer.CudaOffscreenRenderer(0) as r:
+            res = renderer.check(r.update_scene(grid), "update_scene")
+            print(json.dumps({"update": "initial", "gpu_ms": round(res.build_gpu_ms, 3)}))
+            p = grid.geometries[0][0]
+            q = p.copy()
+            q[:, 1] += 0.01 * p[:, 0]
+            grid.set_positions(0, q)
+            res = renderer.check(r.update_geometry(grid, 0), "update_geometry")
+            print(json.dumps({"update": "point edit", "gpu_ms": round(res.build_gpu_ms, 3)}))
+            m = grid.instances[0][0].copy()
+            m[12] += 0.01
+            grid.set_instance(0, m)
+            res = renderer.check(r.update_instances(grid), "update_instances")
+            print(json.dumps({"update": "transform edit", "gpu_ms": round(res.build_gpu_ms, 3)}))
         return
     if args.batch:
         work = scenes.batch_workload(64, seed=0)[:args.batch]
