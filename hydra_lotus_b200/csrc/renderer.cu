@@ -1746,7 +1746,7 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
     okb = R.ok(T.radiance[0].resize(n), "temporal radiance", detail) &&
           R.ok(T.radiance[1].resize(n), "temporal radiance", detail) &&
           R.ok(T.batch.resize(n), "temporal batch", detail) &&
-          (td.filter_iterations == 0 || R.ok(T.filter.resize(3 * n), "temporal filter", detail));
+          (td.filter_iterations == 0 || R.ok(T.filter.resize(4 * n), "temporal filter", detail));
   if (okb && restir)
     okb = R.ok(T.initial.resize(n), "reservoirs", detail) && R.ok(T.reuse[0].resize(n), "reservoirs", detail) &&
           R.ok(T.reuse[1].resize(n), "reservoirs", detail) && R.ok(T.spatial.resize(n), "reservoirs", detail) &&

@@ -649,6 +649,10 @@ __global__ void __launch_bounds__(kBlock) k_svgf_variance(const TemporalConst* _
   filter[index] = input;
   filter[2 * pixels + index] = make_float4(__uint_as_float(guide.x), __uint_as_float(guide.y),
       __uint_as_float(guide.z), __uint_as_float(guide.w));
+  // The guide's shading normal unpacked once per frame (the a-trous taps
+  // read it instead of unpacking it 25 times per iteration).
+  filter[3 * pixels + index] =
+      center.sample_count != 0 ? F4(unpack_normal(guide.w), 0.0f) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
 __device__ __forceinline__ uint4 filter_guide(const float4* filter, uint32_t pixels, uint32_t i) {
@@ -686,7 +690,9 @@ __device__ __forceinline__ float4 filter_iteration(const TemporalConst& tc, cons
   const float4* in = filter + (size_t)(iteration & 1u) * pixels;
   uint4 g;
   float gaussian = 0.0f, gaussian_weight = 0.0f;
+#pragma unroll
   for (int dy = -1; dy <= 1; ++dy) {
+#pragma unroll
     for (int dx = -1; dx <= 1; ++dx) {
       const int qx = x + dx, qy = y + dy;
       if (!filter_neighbour(tc, filter, qx, qy, center.x, center.y, g)) continue;
@@ -699,24 +705,29 @@ __device__ __forceinline__ float4 filter_iteration(const TemporalConst& tc, cons
   const float depth = __uint_as_float(center.z);
   const float phi_z = fmaxf(filter_depth_step(tc, filter, x - 1, y, x + 1, y, depth, center.x, center.y) +
       filter_depth_step(tc, filter, x, y - 1, x, y + 1, depth, center.x, center.y), 1.0e-8f);
-  const F3 normal = unpack_normal(center.w);
+  const F3 normal = V(filter[3 * (size_t)pixels + index]);
   const float4 cv = in[index];
   const float lum = luminance(cv.x, cv.y, cv.z);
   const int step = 1 << iteration;
   const float kernel[3] = {0.375f, 0.25f, 0.0625f};
   float sx = 0.0f, sy = 0.0f, sz = 0.0f, var = 0.0f, weight_sum = 0.0f;
+#pragma unroll
   for (int ty = -2; ty <= 2; ++ty) {
+#pragma unroll
     for (int tx = -2; tx <= 2; ++tx) {
       const int qx = x + tx * step, qy = y + ty * step;
       if (!filter_neighbour(tc, filter, qx, qy, center.x, center.y, g)) continue;
       const float4 value = in[(uint32_t)qy * tc.width + (uint32_t)qx];
       float w = kernel[abs(tx)] * kernel[abs(ty)];
       if (tx != 0 || ty != 0) {
+        const F3 other = V(filter[3 * (size_t)pixels + (uint32_t)qy * tc.width + (uint32_t)qx]);
+        const float facing = saturate(dot(normal, other));
+        // A neighbour facing away weighs 0 (pow(0, 128)): its tap adds nothing.
+        if (facing == 0.0f) continue;
         const float distance = float(step) * sqrtf(float(tx * tx + ty * ty));
         const float wz = fabsf(depth - __uint_as_float(g.z)) / (phi_z * distance);
         const float wl = fabsf(lum - luminance(value.x, value.y, value.z)) / phi_l;
-        const F3 other = unpack_normal(g.w);
-        const float wn = powf(saturate(dot(normal, other)), 128.0f);
+        const float wn = powf(facing, 128.0f);
         w = w * expf(-(wl + wz)) * wn;
       }
       sx += w * value.x;
