@@ -710,6 +710,12 @@ __device__ __forceinline__ float4 filter_iteration(const TemporalConst& tc, cons
   const float lum = luminance(cv.x, cv.y, cv.z);
   const int step = 1 << iteration;
   const float kernel[3] = {0.375f, 0.25f, 0.0625f};
+  // The edge-stopping divisions as products: 1 / phi_l, and 1 / (phi_z *
+  // distance) for the five tap distances (squared 1, 2, 4, 5, 8 steps).
+  const float inv_phi_l = 1.0f / phi_l;
+  float inv_depth[9];
+#pragma unroll
+  for (int d2 = 1; d2 <= 8; ++d2) inv_depth[d2] = 1.0f / (phi_z * (float(step) * sqrtf(float(d2))));
   float sx = 0.0f, sy = 0.0f, sz = 0.0f, var = 0.0f, weight_sum = 0.0f;
 #pragma unroll
   for (int ty = -2; ty <= 2; ++ty) {
@@ -724,9 +730,8 @@ __device__ __forceinline__ float4 filter_iteration(const TemporalConst& tc, cons
         const float facing = saturate(dot(normal, other));
         // A neighbour facing away weighs 0 (pow(0, 128)): its tap adds nothing.
         if (facing == 0.0f) continue;
-        const float distance = float(step) * sqrtf(float(tx * tx + ty * ty));
-        const float wz = fabsf(depth - __uint_as_float(g.z)) / (phi_z * distance);
-        const float wl = fabsf(lum - luminance(value.x, value.y, value.z)) / phi_l;
+        const float wz = fabsf(depth - __uint_as_float(g.z)) * inv_depth[tx * tx + ty * ty];
+        const float wl = fabsf(lum - luminance(value.x, value.y, value.z)) * inv_phi_l;
         const float wn = powf(facing, 128.0f);
         w = w * expf(-(wl + wz)) * wn;
       }
