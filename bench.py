@@ -308,6 +308,43 @@ def scene_update_report(renderer_module, repeats=3):
     return out
 
 
+def temporal_report(renderer_module, frames=24):
+    """Frames per second of the temporal configurations at 1920x1080, 1 spp
+    per frame, over an orbiting camera (the median device time of frames
+    8.., once the histories are full): config 3 (ReSTIR DI with temporal
+    reuse, M cap 20, one spatial pass within 30 px; SVGF with 5 a-trous
+    iterations; the box room with 10,000 emissive floor triangles) and
+    config 5 (the learned radiance cache plus the same ReSTIR DI, no
+    a-trous iterations), depth 6."""
+    width, height = 1920, 1080
+    scene = scenes.restir_room(seed=0, size=height, emitters=10000, aspect=width / height)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT,
+                              light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL, max_bounces=6, sample_index=0,
+                              restir_candidates=8, restir_temporal=1, restir_max_history_candidates=20,
+                              restir_spatial=1, restir_spatial_radius=30)
+    out = {"resolution": [width, height], "depth": 6, "spp_per_frame": 1}
+    for name, cache, filt in (("restir+svgf", False, 5), ("cache+restir", True, 0)):
+        ms = []
+        previous = None
+        with renderer_module.CudaOffscreenRenderer(0) as r:
+            renderer_module.check(r.update_scene(scene), "update_scene")
+            if cache:
+                r.configure_cache(enable=True, seed=1)
+            for k in range(frames):
+                view, w2c = scenes.orbit_camera(k, frames=120, aspect=width / height)
+                frame = abi.make_frame(w2c, width, height, st, 1, read_back=False)
+                d = abi.temporal_desc(frame, view, previous[0] if previous else None,
+                                      previous[1] if previous else None, history_available=k > 0,
+                                      accumulate_radiance=True, max_history_samples=5, filter_iterations=filt)
+                res, _ = r.render_temporal(d)
+                renderer_module.check(res, name)
+                previous = (view, w2c)
+                ms.append(res.gpu_ms)
+        med = statistics.median(ms[8:])
+        out[name] = {"ms_per_frame": round(med, 3), "frames_per_s": round(1e3 / med, 1)}
+    return out
+
+
 def batch_report(renderer_module, spp=8, depth=8):
     """Config 4: the 64-scene batch workload (scenes.batch_workload: traced
     triangles log-uniform in [1e4, 2e6], 256^2 .. 1024^2 targets), 8 spp,
@@ -360,6 +397,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--batch", type=int, default=1,
                     help="1: also measure the 64-scene batch (config 4), batched vs one scene at a time")
+    ap.add_argument("--temporal", type=int, default=1,
+                    help="1: also measure frames/s of ReSTIR+SVGF (config 3) and cache+ReSTIR (config 5) at 1080p")
     ap.add_argument("--updates", type=int, default=1,
                     help="1: also time scene uploads and edits on the geometry-v1-shaped grid")
     ap.add_argument("--convergence", type=int, default=1,
@@ -524,6 +563,8 @@ def main():
             line["batch"] = batch_report(renderer)
         if args.updates:
             line["scene_updates"] = scene_update_report(renderer)
+        if args.temporal:
+            line["temporal"] = temporal_report(renderer)
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:
