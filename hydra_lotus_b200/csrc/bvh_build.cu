@@ -28,27 +28,42 @@ __device__ __forceinline__ float unordered(uint32_t u) {
 }
 
 // Triangle boxes in object space from the geometry's positions.
+// Folds a warp's primitive centroids into the centroid bounds with one
+// atomic per bound (lanes without a primitive add the identities); every
+// lane of the warp takes part.
+__device__ __forceinline__ void warp_centroid_bounds(uint32_t* bounds, bool valid, const float* l,
+    const float* h) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const uint32_t o = ordered(0.5f * (l[a] + h[a]));
+    const uint32_t lo = __reduce_min_sync(0xFFFFFFFFu, valid ? o : 0xFFFFFFFFu);
+    const uint32_t hi = __reduce_max_sync(0xFFFFFFFFu, valid ? o : 0u);
+    if ((threadIdx.x & 31u) == 0) {
+      atomicMin(&bounds[a], lo);
+      atomicMax(&bounds[3 + a], hi);
+    }
+  }
+}
+
 __global__ void k_triangle_boxes(const float* __restrict__ positions,
     const uint32_t* __restrict__ triangles, uint32_t n, float4* __restrict__ lo,
     float4* __restrict__ hi, uint32_t* __restrict__ centroid_bounds) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const bool valid = i < n;
   float l[3] = {kFloatMax, kFloatMax, kFloatMax}, h[3] = {-kFloatMax, -kFloatMax, -kFloatMax};
-  for (int k = 0; k < 3; ++k) {
-    const uint32_t v = triangles[3 * i + k];
-    for (int a = 0; a < 3; ++a) {
-      const float p = positions[3 * (size_t)v + a];
-      l[a] = fminf(l[a], p);
-      h[a] = fmaxf(h[a], p);
+  if (valid) {
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t v = triangles[3 * i + k];
+      for (int a = 0; a < 3; ++a) {
+        const float p = positions[3 * (size_t)v + a];
+        l[a] = fminf(l[a], p);
+        h[a] = fmaxf(h[a], p);
+      }
     }
+    lo[i] = make_float4(l[0], l[1], l[2], 0.0f);
+    hi[i] = make_float4(h[0], h[1], h[2], 0.0f);
   }
-  lo[i] = make_float4(l[0], l[1], l[2], 0.0f);
-  hi[i] = make_float4(h[0], h[1], h[2], 0.0f);
-  for (int a = 0; a < 3; ++a) {
-    const float c = 0.5f * (l[a] + h[a]);
-    atomicMin(&centroid_bounds[a], ordered(c));
-    atomicMax(&centroid_bounds[3 + a], ordered(c));
-  }
+  warp_centroid_bounds(centroid_bounds, valid, l, h);
 }
 
 // Instance world boxes: the BLAS root box's corners through
