@@ -217,22 +217,9 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def time_to_relmse_report(renderer_module):
-    """The metric's first half: device seconds to relMSE 1e-3 (epsilon 1e-2)
-    at 1080p on the box room with 10,000 emissive floor triangles (power
-    log-normal, sigma 2), depth 6, static camera, for plain wavefront PT,
-    the learned radiance cache, ReSTIR DI (temporal + spatial reuse) and
-    cache + ReSTIR. The reference is plain PT at 8192 spp over the middle
-    96 rows, its own noise subtracted. A method that does not reach the
-    target within its budget reports null with an extrapolation from its
-    last checkpoint (relMSE falling as 1/time)."""
+def _time_to_relmse(renderer_module, scene, label, budgets, depth=6, rows=96, target=1e-3):
     from hydra_lotus_b200 import convergence
-    scene = scenes.box_room_wide(seed=0, emitters=10000)
-    depth, rows, target = 6, 96, 1e-3
-    budgets = {"plain": 40.0, "cache": 20.0, "restir": 8.0, "cache+restir": 20.0}
-    out = {"scene": "box room + 10,000 emissive floor triangles (power log-normal sigma 2), 1920x1080, "
-                    "depth 6, static camera",
-           "target": target, "epsilon": 1e-2, "unit": "s (device time)"}
+    out = {"scene": label, "target": target, "epsilon": 1e-2, "unit": "s (device time)"}
     with renderer_module.CudaOffscreenRenderer(0) as r:
         renderer_module.check(r.update_scene(scene), "update_scene")
         ref, noise, ref_s = convergence.reference(r, scene, depth, 8192, rows)
@@ -251,6 +238,27 @@ def time_to_relmse_report(renderer_module):
         v = out[m]["seconds"]
         if plain and v:
             out[f"speedup_{m}_vs_plain"] = round(plain / v, 2)
+    return out
+
+
+def time_to_relmse_report(renderer_module):
+    """The metric's first half: device seconds to relMSE 1e-3 (epsilon 1e-2)
+    at 1080p, depth 6, static camera, for plain wavefront PT, the learned
+    radiance cache, ReSTIR DI (temporal + spatial reuse) and cache + ReSTIR:
+    on the box room with 10,000 emissive floor triangles (power log-normal,
+    sigma 2; the top-level entries) and on the config-1 box room with its
+    one ceiling light (`single_light`). The reference is plain PT at 8192
+    spp over the middle 96 rows, its own noise subtracted. A method that
+    does not reach the target within its budget reports null with an
+    extrapolation from its last checkpoint (relMSE falling as 1/time)."""
+    out = _time_to_relmse(
+        renderer_module, scenes.box_room_wide(seed=0, emitters=10000),
+        "box room + 10,000 emissive floor triangles (power log-normal sigma 2), 1920x1080, depth 6, static camera",
+        {"plain": 40.0, "cache": 20.0, "restir": 8.0, "cache+restir": 20.0})
+    out["single_light"] = _time_to_relmse(
+        renderer_module, scenes.box_room_wide(seed=0),
+        "config-1 box room (one ceiling quad light), 1920x1080, depth 6, static camera",
+        {"plain": 10.0, "cache": 10.0, "restir": 5.0, "cache+restir": 10.0})
     return out
 
 
