@@ -433,11 +433,78 @@ Lotus::GpuFrameEvidence CudaOffscreenRenderer::RenderTemporalScene(const Lotus::
   lotus_cuda_render_temporal(handle_, &d, &r, color.empty() ? nullptr : color.data());
   FillEvidence(d.frame, r, color, e);
   if (r.status == LOTUS_PASS) {
+    FillTemporalProducts(d, history, have_previous_camera_ && temporal.camera_cut, e);
     // Only success advances history (vulkan_backend.hpp:793-806).
     previous_camera_ = snapshot.camera;
     have_previous_camera_ = true;
   }
   return e;
+}
+
+namespace {
+
+static_assert(sizeof(Lotus::TemporalPixel) == 64, "the surface product is 64 bytes per pixel");
+static_assert(sizeof(Lotus::TemporalValidityPixel) == 16, "the validity product is 16 bytes per pixel");
+static_assert(sizeof(Lotus::TemporalRadiancePixel) == 32, "the radiance product is 32 bytes per pixel");
+static_assert(sizeof(Lotus::RestirPixel) == 48, "the initial reservoirs are 48 bytes per pixel");
+static_assert(sizeof(Lotus::RestirReusePixel) == 64, "the reuse records are 64 bytes per pixel");
+
+// One product into `out` (the C ABI's byte layout is the reference's type's);
+// empty when the frame has no such product.
+template <typename T>
+void read_product(lotus_cuda_renderer* handle, uint32_t product, size_t pixels, std::vector<T>& out) {
+  out.resize(pixels);
+  const int64_t got = lotus_cuda_read_product(handle, product, out.data(), pixels * sizeof(T));
+  out.resize(got > 0 ? (size_t)got / sizeof(T) : 0);
+}
+
+}  // namespace
+
+void CudaOffscreenRenderer::FillTemporalProducts(const lotus_temporal_desc& d, bool history, bool camera_cut,
+    Lotus::GpuFrameEvidence& e) {
+  const uint32_t w = d.frame.target.width, h = d.frame.target.height;
+  const size_t n = (size_t)w * h;
+  Lotus::TemporalProducts& t = e.temporal;
+  t.available = true;
+  t.history_available = history;
+  t.reset_reason = history ? Lotus::TemporalResetReason::None
+                           : (camera_cut ? Lotus::TemporalResetReason::CameraCut
+                                         : Lotus::TemporalResetReason::FirstFrame);
+  t.width = w;
+  t.height = h;
+  t.row_pitch = w * (uint32_t)sizeof(Lotus::TemporalPixel);
+  read_product(handle_, LOTUS_PRODUCT_SURFACE, n, t.current);
+  if (history) read_product(handle_, LOTUS_PRODUCT_PREVIOUS_SURFACE, n, t.previous);
+  read_product(handle_, LOTUS_PRODUCT_VALIDITY, n, t.validity);
+  t.validity_row_pitch = w * (uint32_t)sizeof(Lotus::TemporalValidityPixel);
+  if (d.accumulate_radiance) {
+    t.radiance_available = true;
+    read_product(handle_, LOTUS_PRODUCT_RADIANCE, n, t.radiance);
+    if (history) read_product(handle_, LOTUS_PRODUCT_PREVIOUS_RADIANCE, n, t.previous_radiance);
+    t.radiance_row_pitch = w * (uint32_t)sizeof(Lotus::TemporalRadiancePixel);
+    read_product(handle_, LOTUS_PRODUCT_BATCH, n, t.batch);
+    t.batch_sample_index = d.frame.settings.sample_index;
+    t.batch_samples = d.frame.frame_count;
+    t.filter_iterations = d.filter_iterations;
+  }
+  if (d.frame.settings.light_sampling != LOTUS_LIGHT_SAMPLING_RESTIR_INITIAL) return;
+  Lotus::RestirProducts& r = e.restir;
+  r.available = true;
+  r.width = w;
+  r.height = h;
+  r.row_pitch = w * (uint32_t)sizeof(Lotus::RestirPixel);
+  read_product(handle_, LOTUS_PRODUCT_RESTIR_INITIAL, n, r.initial);
+  if (d.frame.settings.restir_temporal) {
+    r.temporal_row_pitch = w * (uint32_t)sizeof(Lotus::RestirReusePixel);
+    read_product(handle_, LOTUS_PRODUCT_RESTIR_TEMPORAL, n, r.temporal);
+    read_product(handle_, LOTUS_PRODUCT_RESTIR_PREVIOUS, n, r.previous);
+    r.history_available = history && !r.previous.empty();
+  }
+  if (d.frame.settings.restir_spatial) {
+    r.spatial_row_pitch = w * (uint32_t)sizeof(Lotus::RestirReusePixel);
+    read_product(handle_, LOTUS_PRODUCT_RESTIR_SPATIAL, n, r.spatial);
+    read_product(handle_, LOTUS_PRODUCT_RESTIR_SOURCES, n, r.spatial_sources);
+  }
 }
 
 Lotus::GpuSceneContents CudaOffscreenRenderer::ReadBackScene() {

@@ -71,6 +71,10 @@ class CudaOffscreenRenderer final : public Lotus::OffscreenRenderer {
   // the same topology (SceneGeometryReplacement), go to the incremental
   // entry points; returns false when the plan needs a full update.
   bool UpdateIncrementally(const Lotus::SceneUpdate& update, Lotus::GpuSceneEvidence& evidence);
+  // The temporal and ReSTIR products of the frame just rendered
+  // (TemporalProducts, RestirProducts), read back through the C ABI.
+  void FillTemporalProducts(const lotus_temporal_desc& desc, bool history, bool camera_cut,
+      Lotus::GpuFrameEvidence& evidence);
   bool InstanceArray(std::vector<lotus_instance>& out, std::string& error) const;
   void SceneStats(const Lotus::SceneUpdate& update, const lotus_scene_result& result,
       Lotus::GpuSceneEvidence& evidence) const;

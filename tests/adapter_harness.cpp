@@ -23,6 +23,7 @@
 #include <fstream>
 #include <iostream>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "../hydra_lotus_b200/host/cuda_offscreen_renderer.hpp"
@@ -52,8 +53,60 @@ const char* status_name(Lotus::FrameStatus s) {
 
 }  // namespace
 
+template <typename T>
+void dump(const std::string& path, const std::vector<T>& v) {
+  std::ofstream out(path, std::ios::binary);
+  out.write(reinterpret_cast<const char*>(v.data()), (std::streamsize)(v.size() * sizeof(T)));
+}
+
+// Two temporal frames through RenderTemporalScene with a still camera
+// (view identity, projection the file's world_to_clip): ReSTIR DI with
+// temporal reuse and a spatial pass of radius 2, radiance accumulation
+// capped at 5 samples and 2 a-trous iterations. Writes each frame's colour
+// and its temporal and ReSTIR products to <prefix><frame>_<name>.bin.
+int temporal_frames(Lotus::OffscreenRenderer& renderer, const Lotus::DrawSummary& draw,
+    const Lotus::OffscreenTarget& target, Lotus::PathTracingSettings settings, const std::string& prefix) {
+  settings.light_sampling = Lotus::LightSampling::RestirInitial;
+  settings.restir_temporal = true;
+  settings.restir_spatial = true;
+  settings.restir_spatial_radius = 2;
+  Lotus::FrameSnapshot snapshot;
+  snapshot.camera.projection = draw.world_to_clip;
+  Lotus::TemporalFrameSettings temporal;
+  temporal.width = target.width;
+  temporal.height = target.height;
+  temporal.accumulate_radiance = true;
+  temporal.max_history_samples = 5;
+  temporal.filter_iterations = 2;
+  int code = 0;
+  for (int k = 0; k < 2; ++k) {
+    temporal.frame_index = (uint64_t)k;
+    const Lotus::GpuFrameEvidence e = renderer.RenderTemporalScene(snapshot, target, 1, temporal, settings);
+    const std::string base = prefix + std::to_string(k) + "_";
+    dump(base + "color.bin", e.color.payload);
+    dump(base + "surface.bin", e.temporal.current);
+    dump(base + "validity.bin", e.temporal.validity);
+    dump(base + "radiance.bin", e.temporal.radiance);
+    dump(base + "batch.bin", e.temporal.batch);
+    dump(base + "restir_initial.bin", e.restir.initial);
+    dump(base + "restir_temporal.bin", e.restir.temporal);
+    dump(base + "restir_spatial.bin", e.restir.spatial);
+    dump(base + "restir_sources.bin", e.restir.spatial_sources);
+    std::printf("{\"frame\": %d, \"render\": \"%s\", \"detail\": \"%s\", \"temporal\": %s, "
+                "\"history\": %s, \"restir\": %s, \"restir_history\": %s, \"surface_pixels\": %zu, "
+                "\"previous_pixels\": %zu, \"restir_previous_pixels\": %zu, \"filter_iterations\": %u}\n",
+        k, status_name(e.status), e.detail.c_str(), e.temporal.available ? "true" : "false",
+        e.temporal.history_available ? "true" : "false", e.restir.available ? "true" : "false",
+        e.restir.history_available ? "true" : "false", e.temporal.current.size(), e.temporal.previous.size(),
+        e.restir.previous.size(), e.temporal.filter_iterations);
+    if (e.status != Lotus::FrameStatus::Pass) code = 1;
+  }
+  return code;
+}
+
 int main(int argc, char** argv) {
-  if (argc != 3 && argc != 6) {
+  const bool temporal_mode = argc == 5 && std::string(argv[3]) == "--temporal";
+  if (argc != 3 && argc != 6 && !temporal_mode) {
     std::fprintf(stderr,
         "usage: adapter_harness <scene file> <output floats> "
         "[<dx> <after instance edit floats> <after point edit floats>]\n");
@@ -168,6 +221,13 @@ int main(int argc, char** argv) {
   }
   const Lotus::BackendCapability cap = renderer->RayQueryCapability();
   const Lotus::GpuSceneEvidence scene = renderer->UpdateScene(update);
+  if (temporal_mode) {
+    if (scene.status != Lotus::FrameStatus::Pass) {
+      std::printf("{\"update\": \"%s\", \"detail\": \"%s\"}\n", status_name(scene.status), scene.detail.c_str());
+      return 1;
+    }
+    return temporal_frames(*renderer, draw, target, settings, argv[4]);
+  }
   const Lotus::GpuFrameEvidence frame = renderer->RenderScene(draw, target, frame_count, settings);
   const Lotus::GpuFrameEvidence bootstrap = renderer->Render(draw, target, 1);
   const Lotus::PresentEvidence present = renderer->Present(target.width, target.height);

@@ -64,3 +64,24 @@ def run(tmpdir, scene, settings, frame_count, edit_dx=None):
     if edit_dx is None:
         return p.returncode, (lines[-1] if lines else {}), _image(outs[0], scene)
     return p.returncode, lines, [_image(o, scene) for o in outs]
+
+
+TEMPORAL_PRODUCTS = ["color", "surface", "validity", "radiance", "batch", "restir_initial", "restir_temporal",
+                     "restir_spatial", "restir_sources"]
+
+
+def run_temporal(tmpdir, scene, settings):
+    """The driver's temporal mode: two still-camera temporal frames through
+    RenderTemporalScene. Returns (exit code, [evidence per frame],
+    [{product name: raw bytes} per frame])."""
+    inp = os.path.join(tmpdir, "scene.bin")
+    prefix = os.path.join(tmpdir, "t")
+    write(inp, scene, settings, 1)
+    p = subprocess.run([HARNESS, inp, os.path.join(tmpdir, "unused.bin"), "--temporal", prefix],
+                       capture_output=True, text=True, timeout=600)
+    lines = [json.loads(line) for line in p.stdout.strip().splitlines() if line.startswith("{")]
+    frames = []
+    for k in range(2):
+        frames.append({name: open(f"{prefix}{k}_{name}.bin", "rb").read()
+                       for name in TEMPORAL_PRODUCTS if os.path.exists(f"{prefix}{k}_{name}.bin")})
+    return p.returncode, lines, frames

@@ -78,3 +78,39 @@ def test_adapter_incremental_updates_render_what_full_updates_render(cuda, harne
             cuda.check(res, "render_scene")
         assert got is not None
         assert np.array_equal(got, want), f"{np.count_nonzero(got != want)} values differ"
+
+
+def test_adapter_temporal_products_equal_the_c_abi(cuda, harness, tmp_path):
+    """RenderTemporalScene through the adapter returns the reference's
+    TemporalProducts and RestirProducts (surface, validity, radiance, batch,
+    initial / temporal / spatial reservoirs, spatial sources) and colour,
+    byte for byte what the C ABI's products are for the same two frames."""
+    scene = scenes.restir_room(seed=0, size=48, emitters=200)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=4, sample_index=5)
+    code, evidence, frames = adapter_scene.run_temporal(str(tmp_path), scene, st)
+    assert code == 0, evidence
+    assert [e["history"] for e in evidence] == [False, True], evidence
+    assert all(e["temporal"] and e["restir"] for e in evidence), evidence
+    assert evidence[1]["previous_pixels"] == scene.width * scene.height
+    rst = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT,
+                               light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL, max_bounces=4, sample_index=5,
+                               restir_temporal=1, restir_spatial=1, restir_spatial_radius=2)
+    identity = [1.0, 0, 0, 0, 0, 1.0, 0, 0, 0, 0, 1.0, 0, 0, 0, 0, 1.0]
+    names = {"surface": abi.PRODUCT_SURFACE, "validity": abi.PRODUCT_VALIDITY, "radiance": abi.PRODUCT_RADIANCE,
+             "batch": abi.PRODUCT_BATCH, "restir_initial": abi.PRODUCT_RESTIR_INITIAL,
+             "restir_temporal": abi.PRODUCT_RESTIR_TEMPORAL, "restir_spatial": abi.PRODUCT_RESTIR_SPATIAL,
+             "restir_sources": abi.PRODUCT_RESTIR_SOURCES}
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        for k in range(2):
+            frame = abi.make_frame(scene.world_to_clip, scene.width, scene.height, rst, 1)
+            d = abi.temporal_desc(frame, identity, identity, scene.world_to_clip, history_available=k > 0,
+                                  accumulate_radiance=True, max_history_samples=5, filter_iterations=2)
+            res, color = r.render_temporal(d)
+            cuda.check(res, f"render_temporal {k}")
+            got = frames[k]
+            assert got["color"] == color.tobytes(), f"frame {k}: colour differs"
+            for name, product in names.items():
+                want = r.read_product(product, scene.height, scene.width).tobytes()
+                assert got[name] == want, f"frame {k}: {name} differs"
