@@ -31,7 +31,14 @@ FRAME_COUNT_VISITS = 2
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
-ABI_VERSION = 1
+ABI_VERSION = 2
+
+# lotus_settings::output (SceneOutput).
+OUTPUT_RADIANCE = 0
+OUTPUT_BARYCENTRICS = 1
+OUTPUT_SHADING_NORMAL = 2
+OUTPUT_ALBEDO = 3
+OUTPUT_ROUGHNESS_METALLIC = 4
 
 
 class Geometry(C.Structure):
@@ -132,6 +139,7 @@ class Settings(C.Structure):
         ("restir_spatial_radius", C.c_uint32),
         ("restir_proposal", C.c_uint32),
         ("environment_background", C.c_uint32),
+        ("output", C.c_uint32),
     ]
 
 
@@ -300,7 +308,7 @@ def default_settings(**overrides):
                  restir_candidates=8, restir_temporal=0,
                  restir_max_history_candidates=32, restir_spatial=0,
                  restir_spatial_radius=1, restir_proposal=0,
-                 environment_background=0)
+                 environment_background=0, output=OUTPUT_RADIANCE)
     for k, v in overrides.items():
         setattr(s, k, v)
     return s

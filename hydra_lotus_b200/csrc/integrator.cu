@@ -568,6 +568,36 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_shadow(SceneVi
   }
 }
 
+// The diagnostic outputs (CameraPass's surface pass, path_trace.slang:
+// 67-98): the pixel centre's closest hit, traced with a fixed coverage
+// sequence (sample 0), as its barycentric weights or a diagnostic of its
+// surface; a miss leaves the pixel as it is (the clear colour).
+__global__ void __launch_bounds__(kBlock) k_diagnostic(SceneView S, const FrameConst* __restrict__ fcp,
+    uint32_t output, float4* __restrict__ color) {
+  const FrameConst& f = *fcp;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= f.rect[2] * f.rect[3]) return;
+  const uint32_t px = f.rect[0] + i % f.rect[2], py = f.rect[1] + i / f.rect[2];
+  const uint32_t slot = py * f.width + px;
+  uint32_t rng = seed_random(slot, 0);
+  F3 o, d;
+  float tmax;
+  camera_ray(f, (float(px) + 0.5f) * f.ndc[0] + f.ndc[2], (float(py) + 0.5f) * f.ndc[1] + f.ndc[3], o, d, tmax);
+  Hit hit;
+  if (!trace_closest(S, o, d, 0.0f, tmax, rng, hit)) return;
+  if (output == kOutputBarycentrics) {
+    color[slot] = make_float4(1.0f - hit.b1 - hit.b2, hit.b1, hit.b2, 1.0f);
+    return;
+  }
+  const SurfaceHit sh = reconstruct_hit(S, hit.instance, hit.tri, hit.b1, hit.b2, d);
+  if (output == kOutputAlbedo)
+    color[slot] = F4(sh.base_color, 1.0f);
+  else if (output == kOutputRoughnessMetallic)
+    color[slot] = make_float4(sh.roughness, sh.metallic, 0.0f, 1.0f);
+  else
+    color[slot] = F4(sh.shading_normal, 1.0f);
+}
+
 // The ReSTIR passes' queued visibility rays (VisibilityQueue), as a
 // persistent any-hit kernel that completes each ray's pixel record.
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_visibility(SceneView S, VisibilityQueue VQ,
@@ -949,6 +979,12 @@ void launch_visibility(const SceneView& S, const VisibilityQueue& queue, uint32_
   const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid = persistent_grid((const void*)k_visibility, queue.capacity, tuning);
   k_visibility<<<grid, kBlock, 0, stream>>>(S, queue, pass, records, stride, positive ? 1u : 0u, refill);
+}
+
+void launch_diagnostic(const SceneView& S, const FrameConst* fc, const uint32_t rect[4], uint32_t output,
+    float4* color, cudaStream_t stream) {
+  const uint32_t n = rect[2] * rect[3];
+  if (n) k_diagnostic<<<(n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(S, fc, output, color);
 }
 
 void launch_advance(FrameConst* fc, cudaStream_t stream) { k_advance<<<1, 32, 0, stream>>>(fc); }

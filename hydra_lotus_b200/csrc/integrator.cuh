@@ -151,6 +151,15 @@ constexpr uint32_t kVisibilityPasses = 3;
 void launch_visibility(const SceneView& S, const VisibilityQueue& queue, uint32_t pass, unsigned char* records,
     uint32_t stride, bool positive, cudaStream_t stream, const TraceTuning& tuning = TraceTuning());
 
+// The diagnostic outputs, numbered as lotus_settings::output.
+constexpr uint32_t kOutputBarycentrics = 1, kOutputShadingNormal = 2, kOutputAlbedo = 3,
+                   kOutputRoughnessMetallic = 4;
+
+// A diagnostic output (kOutputBarycentrics .. kOutputRoughnessMetallic) of
+// the pixels in `rect` into `color`; misses leave their pixels as they are.
+void launch_diagnostic(const SceneView& S, const FrameConst* fc, const uint32_t rect[4], uint32_t output,
+    float4* color, cudaStream_t stream);
+
 void launch_advance(FrameConst* fc, cudaStream_t stream);
 
 void launch_clear_color(float4* color, uint32_t pixels, float4 value, cudaStream_t stream);

@@ -389,6 +389,10 @@ struct HostScene {
   float env_frame[9] = {};
 };
 
+static_assert(LOTUS_OUTPUT_BARYCENTRICS == kOutputBarycentrics && LOTUS_OUTPUT_SHADING_NORMAL == kOutputShadingNormal &&
+                  LOTUS_OUTPUT_ALBEDO == kOutputAlbedo && LOTUS_OUTPUT_ROUGHNESS_METALLIC == kOutputRoughnessMetallic,
+    "diagnostic outputs are numbered as lotus_settings::output");
+
 struct Renderer {
   int device = 0;
   uint32_t bvh_leaf_size = 1;
@@ -1208,6 +1212,38 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   fc.max_bounces = st.max_bounces;
   fc.sample_lights = st.light_sampling != LOTUS_LIGHT_SAMPLING_BSDF ? 1u : 0u;
   fc.environment_background = st.environment_background ? 1u : 0u;
+  if (st.output > LOTUS_OUTPUT_ROUGHNESS_METALLIC) return fail("unknown scene output");
+  if (st.output != LOTUS_OUTPUT_RADIANCE) {
+    // A diagnostic of the pixel centres' closest hits: not accumulated, the
+    // radiance accumulation untouched.
+    cudaStream_t s = R.stream;
+    if (!R.ok(cudaMemcpyAsync(R.frame_const.ptr, &fc, sizeof(fc), cudaMemcpyHostToDevice, s), "frame constants",
+            detail))
+      return poison(detail);
+    launch_clear_color(R.color.ptr, t.width * t.height,
+        make_float4(t.clear_color[0], t.clear_color[1], t.clear_color[2], t.clear_color[3]), s);
+    cudaEventRecord(R.ev_start, s);
+    launch_diagnostic(R.view, R.frame_const.ptr, rect, st.output, R.color.ptr, s);
+    cudaEventRecord(R.ev_stop, s);
+    if (!R.ok(cudaGetLastError(), "diagnostic output", detail) ||
+        !R.ok(cudaStreamSynchronize(s), "diagnostic output", detail))
+      return poison(detail);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
+    if (t.read_back && color_out) {
+      if (!R.ok(cudaMemcpy(color_out, R.color.ptr, sizeof(float4) * (size_t)t.width * t.height,
+                    cudaMemcpyDeviceToHost), "colour readback", detail))
+        return poison(detail);
+    }
+    R.completion += 1;
+    res.status = LOTUS_PASS;
+    res.frames_rendered = 1;
+    res.samples_per_pixel = 0;
+    res.completion = R.completion;
+    res.camera_rays = (uint64_t)rect[2] * rect[3];
+    res.gpu_ms = ms;
+    return LOTUS_PASS;
+  }
   // The accumulation key (vulkan_backend.cpp:1188-1205).
   Renderer::Key key{};
   std::memcpy(key.world_to_clip, vulkan, sizeof(vulkan));
@@ -1620,6 +1656,10 @@ bool make_frame_constants(const lotus_frame_desc& d, FrameConst& fc, uint32_t re
       detail = "invalid offscreen clear values";
       return false;
     }
+  if (st.output != LOTUS_OUTPUT_RADIANCE) {
+    detail = "only lotus_cuda_render renders the diagnostic outputs";
+    return false;
+  }
   if (st.integrator > LOTUS_INTEGRATOR_WAVEFRONT || st.light_sampling > LOTUS_LIGHT_SAMPLING_MIS) {
     detail = "unsupported integrator or light sampling";
     return false;

@@ -320,11 +320,17 @@ bool CudaOffscreenRenderer::UpdateIncrementally(const Lotus::SceneUpdate& u, Lot
 
 bool CudaOffscreenRenderer::FillFrame(const Lotus::Matrix4& world_to_clip, const Lotus::OffscreenTarget& t,
     std::uint32_t frame_count, const Lotus::PathTracingSettings& s, lotus_frame_desc& f, std::string& error) const {
-  if (s.output != Lotus::SceneOutput::Radiance) {
-    error = "only the Radiance output is built in the CUDA backend";
-    return false;
-  }
   f = lotus_frame_desc{};
+  switch (s.output) {
+    case Lotus::SceneOutput::Radiance: f.settings.output = LOTUS_OUTPUT_RADIANCE; break;
+    case Lotus::SceneOutput::Barycentrics: f.settings.output = LOTUS_OUTPUT_BARYCENTRICS; break;
+    case Lotus::SceneOutput::ShadingNormal: f.settings.output = LOTUS_OUTPUT_SHADING_NORMAL; break;
+    case Lotus::SceneOutput::Albedo: f.settings.output = LOTUS_OUTPUT_ALBEDO; break;
+    case Lotus::SceneOutput::RoughnessMetallic: f.settings.output = LOTUS_OUTPUT_ROUGHNESS_METALLIC; break;
+    default:
+      error = "unknown scene output";
+      return false;
+  }
   std::memcpy(f.world_to_clip, world_to_clip.data(), 64);
   f.target.width = t.width;
   f.target.height = t.height;

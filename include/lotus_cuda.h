@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LOTUS_CUDA_ABI_VERSION 1u
+#define LOTUS_CUDA_ABI_VERSION 2u
 
 /* FrameStatus (vulkan_backend.hpp:23-27). */
 #define LOTUS_PASS 0
@@ -157,7 +157,19 @@ typedef struct lotus_settings {
   uint32_t restir_spatial_radius;
   uint32_t restir_proposal;
   uint32_t environment_background;
+  uint32_t output;            /* LOTUS_OUTPUT_* (SceneOutput) */
 } lotus_settings;
+
+/* lotus_settings::output (SceneOutput, vulkan_backend.hpp:617-634): the
+ * accumulated path-traced radiance, or a diagnostic of the pixel centre's
+ * closest hit (not accumulated; misses keep the clear colour): its
+ * barycentric weights (1 - b1 - b2, b1, b2, 1), the world-space shading
+ * normal, the base colour with alpha 1, or (roughness, metallic, 0, 1). */
+#define LOTUS_OUTPUT_RADIANCE 0u
+#define LOTUS_OUTPUT_BARYCENTRICS 1u
+#define LOTUS_OUTPUT_SHADING_NORMAL 2u
+#define LOTUS_OUTPUT_ALBEDO 3u
+#define LOTUS_OUTPUT_ROUGHNESS_METALLIC 4u
 
 /* lotus_frame_desc::flags. TIMINGS times the kernels of the call's last
  * sample by class (the reference's WavefrontTimings, vulkan_backend.hpp:
