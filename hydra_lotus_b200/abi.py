@@ -31,7 +31,7 @@ FRAME_COUNT_VISITS = 2
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # lotus_settings::output (SceneOutput).
 OUTPUT_RADIANCE = 0
@@ -86,6 +86,27 @@ class Environment(C.Structure):
     ]
 
 
+# lotus_light::shape (LightShape).
+LIGHT_SPHERE = 0
+LIGHT_RECT = 1
+LIGHT_DISK = 2
+LIGHT_DISTANT = 3
+
+
+class Light(C.Structure):
+    _fields_ = [
+        ("shape", C.c_uint32),
+        ("normalize", C.c_uint32),
+        ("world_from_light", C.c_float * 16),
+        ("radiance", C.c_float * 3),
+        ("radius", C.c_float),
+        ("width", C.c_float),
+        ("height", C.c_float),
+        ("angle", C.c_float),
+        ("reserved", C.c_uint32),
+    ]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("geometries", C.POINTER(Geometry)),
@@ -96,6 +117,8 @@ class SceneDesc(C.Structure):
         ("instance_count", C.c_uint32),
         ("material_count", C.c_uint32),
         ("environment_constant", C.c_float * 3),
+        ("lights", C.POINTER(Light)),
+        ("light_count", C.c_uint32),
     ]
 
 
@@ -229,7 +252,7 @@ class CacheDesc(C.Structure):
 CACHE_INPUTS = 64
 CACHE_WEIGHTS = 21504
 
-STRUCTS = [Geometry, Instance, Material, Environment, SceneDesc, SceneResult,
+STRUCTS = [Geometry, Instance, Material, Environment, Light, SceneDesc, SceneResult,
            Target, Settings, FrameDesc, FrameResult, Options, TemporalDesc, TemporalInstance,
            CacheDesc]
 

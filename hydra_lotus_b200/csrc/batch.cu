@@ -272,10 +272,12 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
   cudaError_t e = ensure_buffers(*b, base[count], count);
   if (e != cudaSuccess) return fail(std::string("batch buffers: ") + cudaGetErrorString(e), true);
   std::vector<SceneView> views(count);
+  bool analytic = false;
   for (uint32_t k = 0; k < count; ++k) {
     RendererAccess a;
     if (!renderer_access(b->scenes[k], a, detail)) return fail("scene " + std::to_string(k) + ": " + detail);
     views[k] = *a.view;
+    analytic = analytic || a.view->analytic_count != 0;
   }
   SceneTable B;
   B.views = b->views;
@@ -283,6 +285,7 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
   B.slot_base = b->slot_base;
   B.count = count;
   B.total_slots = base[count];
+  B.analytic = analytic;
   Queues Q = b->Q;
   Q.capacity = base[count];
   // Clear colours first: pixels outside a data window keep them.

@@ -18,6 +18,17 @@ constexpr float kPi = 3.14159265358979323846f;
 constexpr float kFloatMax = 3.402823466e+38f;
 constexpr uint32_t kNoLights = 0xFFFFFFFFu;
 constexpr uint32_t kEnvironmentLight = 0xFFFFFFFFu;
+// An analytic light's table entry has this bit in `instance`; the other
+// bits index the analytic records (gpu_scene.hpp:128-131). The shapes
+// (gpu_scene.hpp:136-142; a distant light of angle 0 is a parallel light),
+// and the crossing hierarchy's child encoding (gpu_scene.hpp:168-172).
+constexpr uint32_t kAnalyticLight = 0x80000000u;
+constexpr uint32_t kSphereLight = 0, kRectLight = 1, kDiskLight = 2, kDistantLight = 3, kParallelLight = 4;
+constexpr uint32_t kLightLeaf = 0x80000000u;
+constexpr uint32_t kNoLightChild = 0xFFFFFFFFu;
+// The crossing hierarchy's depth is at most ceil(log2(lights)); the host
+// refuses more lights than this stack holds levels for.
+constexpr uint32_t kLightStackSize = 32;
 
 struct F3 {
   float x, y, z;

@@ -77,8 +77,43 @@ __device__ __forceinline__ bool frame_rect_contains(const FrameConst& f, uint32_
   return px >= f.rect[0] && py >= f.rect[1] && px < f.rect[0] + f.rect[2] && py < f.rect[1] + f.rect[3];
 }
 
+// The light a pending shadow ray carries once its transmittance is known.
+__device__ __forceinline__ F3 shadow_contribution(F3 fl, float weight, float pdf,
+    float transmittance) {
+  const F3 c = fl * (transmittance * weight / pdf);
+  return is_finite(c) ? c : V(0.0f);
+}
+
+// ParallelLights (transport.slang:139-146): under BSDF sampling, the
+// parallel lights, which no sampled direction finds, each through its own
+// shadow ray traced here, as ShadowedLight carries a delta light. Not
+// inlined: the shading kernels hold none of the walk's registers for it.
+__device__ __noinline__ F3 parallel_lights(const SceneView& S, F3 position, F3 normal, const Closure& bsdf,
+    const Frame& basis, F3 wo, uint32_t& shadow_rays) {
+  const F3 origin = offset_ray_origin(position, normal);
+  F3 sum = V(0.0f);
+  for (uint32_t index = 0; index < S.analytic_count; ++index) {
+    const LightSample ls = parallel_light(S, index);
+    F3 c = V(0.0f);
+    if (ls.pdf > 0.0f && max_component(ls.radiance) > 0.0f && dot(ls.direction, normal) > 0.0f) {
+      const F3 wi = basis.to_local(ls.direction);
+      if (wi.z > 0.0f) {
+        const F3 fv = bsdf_evaluate(bsdf, wo, wi);
+        if (max_component(fv) > 0.0f) {
+          ++shadow_rays;
+          const float tr = trace_shadow(S, origin, ls.direction, 0.0f, ls.distance);
+          if (tr > 0.0f) c = shadow_contribution(fv * ls.radiance, 1.0f, ls.pdf, tr);
+        }
+      }
+    }
+    sum = sum + c;
+  }
+  return sum;
+}
+
 // Next event estimation's pending shadow ray.
 struct ShadowRequest {
+  uint32_t inline_shadow;  // shadow rays traced inside scatter (parallel lights)
   bool pending;
   F3 origin;
   F3 direction;
@@ -89,15 +124,20 @@ struct ShadowRequest {
   F3 throughput;
 };
 
-// ScatterPath (transport.slang:164-230) without analytic lights:
-// adds the hit's emission (weighed against light sampling), applies
-// Russian roulette, prepares next event estimation's shadow ray and samples
-// the BSDF. Returns whether the path continues along (new_o, new_d).
+// ScatterPath (transport.slang:164-230): adds the hit's emission (weighed
+// against light sampling) and that of the analytic lights the incoming ray
+// crossed, applies Russian roulette, prepares next event estimation's
+// shadow ray (under BSDF sampling, traces the parallel lights' own) and
+// samples the BSDF. Returns whether the path continues along (new_o, new_d).
+// kAnalytic: the scene may have analytic lights; the instantiation without
+// carries none of their code or registers.
+template <bool kAnalytic>
 __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     uint32_t instance, uint32_t tri, float b1, float b2, F3 ray_o, F3 ray_d, uint32_t depth,
     F3& T, F3& R, float& last_pdf, uint32_t& flags, uint32_t& rng, F3& new_o, F3& new_d,
     ShadowRequest& req, uint32_t pixel_index, CacheRecord* features = nullptr, bool end_here = false) {
   req.pending = false;
+  req.inline_shadow = 0;
   uint32_t primitive;
   const SurfaceHit sh = reconstruct_hit(S, instance, tri, b1, b2, ray_d, &primitive);
   if (features) {
@@ -124,6 +164,10 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     emission = emission * w;
   }
   R = R + T * emission;
+  // The analytic lights the ray crossed before the hit; camera rays do not
+  // see them.
+  if (kAnalytic && depth != 0 && S.analytic_count != 0)
+    R = R + T * crossed_lights(S, ray_o, ray_d, dot(sh.position - ray_o, ray_d), false, weigh, last_pdf);
   // A path that ends into the radiance cache stops after the emission: the
   // cache stands for everything scattered from here on.
   if (depth >= f.max_bounces || end_here) return false;
@@ -142,10 +186,11 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
         f.restir_final + (size_t)pixel_index * f.restir_stride);
     if ((sel.flags & 2u) == 0 && sel.reservoir.weight_sum > 0.0f && sel.reservoir.sample < S.light_count) {
       const F3 origin = offset_ray_origin(sh.position, sh.normal);
-      const LightSample ls = reconstruct_reservoir_light(S, sel.reservoir.sample, sel.uv[0], sel.uv[1], origin);
+      const LightSample ls = reconstruct_reservoir_light<kAnalytic>(S, sel.reservoir.sample, sel.uv[0], sel.uv[1], origin);
       const F3 wi = basis.to_local(ls.direction);
       const float weight = ls.delta ? 1.0f
-          : power_heuristic(ls.pdf, wi.z > 0.0f ? bsdf_pdf(sh.bsdf, wo, wi) : 0.0f);
+          : power_heuristic(kAnalytic ? reservoir_partition_pdf(S, sel.reservoir.sample, ls, origin) : ls.pdf,
+                wi.z > 0.0f ? bsdf_pdf(sh.bsdf, wo, wi) : 0.0f);
       R = R + T * (V(sel.contribution) * weight);
     } else {
       R = R + T * V(0.0f);
@@ -158,7 +203,7 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     const float u2 = next_random(rng);
     const float u3 = next_random(rng);
     const F3 origin = offset_ray_origin(sh.position, sh.normal);
-    const LightSample ls = sample_light(S, u0, u1, u2, u3, origin);
+    const LightSample ls = sample_light<kAnalytic>(S, u0, u1, u2, u3, origin);
     if (ls.pdf > 0.0f && max_component(ls.radiance) > 0.0f && dot(ls.direction, sh.normal) > 0.0f) {
       const F3 wi = basis.to_local(ls.direction);
       if (wi.z > 0.0f) {
@@ -175,6 +220,8 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
         }
       }
     }
+  } else if (kAnalytic && !f.sample_lights && S.analytic_count != 0) {
+    R = R + T * parallel_lights(S, sh.position, sh.normal, sh.bsdf, basis, wo, req.inline_shadow);
   }
   F3 u;
   u.x = next_random(rng);
@@ -196,22 +243,18 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
   return true;
 }
 
-// The light a pending shadow ray carries once its transmittance is known.
-__device__ __forceinline__ F3 shadow_contribution(F3 fl, float weight, float pdf,
-    float transmittance) {
-  const F3 c = fl * (transmittance * weight / pdf);
-  return is_finite(c) ? c : V(0.0f);
-}
-
-// MissPath (transport.slang:235-247) without analytic lights.
-__device__ __forceinline__ F3 miss_radiance(const SceneView& S, const FrameConst& f, F3 d,
-    uint32_t flags, float last_pdf) {
+// MissPath (transport.slang:235-247): an escaping continuation ray adds the
+// environment's radiance, the image's weighed against light sampling, then
+// that of the analytic lights it crossed.
+template <bool kAnalytic>
+__device__ __forceinline__ F3 miss_path(const SceneView& S, const FrameConst& f, F3 o, F3 d,
+    uint32_t flags, float last_pdf, F3 T, F3 R) {
+  const bool weigh = f.sample_lights && (flags & kUnweightedLight) == 0;
   F3 env = V(S.env_constant[0], S.env_constant[1], S.env_constant[2]);
-  if (S.env_bound) {
-    const bool weigh = f.sample_lights && (flags & kUnweightedLight) == 0;
-    env = env + environment_radiance(S, d, weigh, last_pdf);
-  }
-  return env;
+  if (S.env_bound) env = env + environment_radiance(S, d, weigh, last_pdf);
+  R = R + T * env;
+  if (kAnalytic && S.analytic_count != 0) R = R + T * crossed_lights(S, o, d, kFloatMax, true, weigh, last_pdf);
+  return R;
 }
 
 // The radiance pass's output (path_trace.slang:369-385) from the FP64
@@ -248,7 +291,7 @@ __device__ __forceinline__ double4 add4(double4 a, float4 s) {
 // The reference integrator: one thread follows one camera path to its end
 // (path_trace.slang:279-287, 353-385), then adds it to the pixel's FP64
 // accumulation and writes the mean.
-template <bool kCount>
+template <bool kCount, bool kAnalytic>
 __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
     const FrameConst* __restrict__ fcp, double4* __restrict__ accum, float4* __restrict__ color,
     RayTotals* totals, VisitCounters* visits) {
@@ -276,8 +319,9 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
         for (uint32_t depth = 0;; ++depth) {
           F3 no, nd;
           ShadowRequest req;
-          const bool cont = scatter(S, f, hit.instance, hit.tri, hit.b1, hit.b2, o, d, depth, T, R,
+          const bool cont = scatter<kAnalytic>(S, f, hit.instance, hit.tri, hit.b1, hit.b2, o, d, depth, T, R,
               last_pdf, flags, rng, no, nd, req, slot);
+          n_shadow += req.inline_shadow;
           if (req.pending) {
             ++n_shadow;
             const float tr = trace_shadow<kCount>(S, req.origin, req.direction, 0.0f, req.tmax, &vc[2]);
@@ -288,7 +332,7 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
           d = nd;
           ++n_extension;
           if (!trace_closest<kCount>(S, o, d, 0.0f, kFloatMax, rng, hit, &vc[1])) {
-            R = R + T * miss_radiance(S, f, d, flags, last_pdf);
+            R = miss_path<kAnalytic>(S, f, o, d, flags, last_pdf, T, R);
             break;
           }
         }
@@ -393,7 +437,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
 // Compiled for six resident blocks per SM (80 registers): shading is
 // latency-bound and gains more from occupancy than from registers.
 constexpr int kShadeBlocksPerSm = 6;
-template <bool kCacheVertex, bool kBatch>
+template <bool kCacheVertex, bool kBatch, bool kAnalytic>
 __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 1];
@@ -426,7 +470,7 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
         T = V(thr);
         last_pdf = thr.w;
         flags = last_pdf < 0.0f ? kUnweightedLight : 0u;
-        if (f.sample_lights) ro = V(P.origin[slot]);
+        if (f.sample_lights || (kAnalytic && SS.analytic_count != 0)) ro = V(P.origin[slot]);
       }
       T_in = T;
       R = V(rad);
@@ -434,7 +478,7 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
       if (cache_vertex)
         training = pcg_hash(slot ^ pcg_hash(f.sample_index ^ 0xC2B2AE35u)) % C.stride == 0u;
       F3 no, nd;
-      cont = scatter(SS, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
+      cont = scatter<kAnalytic>(SS, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
           T, R, last_pdf, flags, rng, no, nd, req, slot, cache_vertex ? &features : nullptr,
           cache_vertex && !training);
       query = cache_vertex && !training;
@@ -636,7 +680,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_visibility(SceneV
 // queued for shading; a miss ends the path with the environment. Each warp
 // stages its hits in shared memory and appends them to the hit queue 32 at
 // a time.
-template <bool kCount, bool kBatch>
+template <bool kCount, bool kBatch, bool kAnalytic>
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce,
     uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits, SceneTable B) {
@@ -678,7 +722,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneVi
         const float4 thr = P.throughput[slot];
         const uint32_t flags = thr.w < 0.0f ? kUnweightedLight : 0u;
         const FrameConst& f = kBatch ? B.frames[scene] : *fcp;
-        const F3 R = V(rad) + V(thr) * miss_radiance(SS, f, W.direction, flags, thr.w);
+        const F3 R = miss_path<kAnalytic>(SS, f, W.origin, W.direction, flags, thr.w, V(thr), V(rad));
         P.radiance[slot] = F4(R, 1.0f);
       }
     }
@@ -829,10 +873,14 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
   if (threads == 0) return;
   const uint32_t grid = (threads + kBlock - 1) / kBlock;
   Timed t(profile, stream, 0);
-  if (profile && profile->visits)
-    k_reference_pt<true><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
-  else
-    k_reference_pt<false><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, nullptr);
+  const bool analytic = S.analytic_count != 0;
+  if (profile && profile->visits) {
+    if (analytic) k_reference_pt<true, true><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
+    else k_reference_pt<true, false><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
+  } else {
+    if (analytic) k_reference_pt<false, true><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, nullptr);
+    else k_reference_pt<false, false><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, nullptr);
+  }
 }
 
 // Blocks of a persistent tracing kernel: every resident block on every
@@ -888,14 +936,16 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid_pixels = (threads + kBlock - 1) / kBlock;
   const SceneTable none;
+  const bool analytic = S.analytic_count != 0;
   const uint32_t grid_extend = persistent_grid(
-      count ? (const void*)k_wf_extend<true, false> : (const void*)k_wf_extend<false, false>, Q.capacity, tuning);
+      count ? (const void*)k_wf_extend<true, false, false> : (const void*)k_wf_extend<false, false, false>,
+      Q.capacity, tuning);
   const uint32_t grid_shadow = persistent_grid(
       count ? (const void*)k_wf_shadow<true, false> : (const void*)k_wf_shadow<false, false>, Q.capacity, tuning);
   // Shading: up to eight waves of resident blocks, grid-striding over
   // longer queues.
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
-      8u * persistent_grid((const void*)k_wf_shade<false, false>, Q.capacity, TraceTuning()));
+      8u * persistent_grid((const void*)k_wf_shade<false, false, false>, Q.capacity, TraceTuning()));
   {
     Timed t(profile, stream, 0);
     if (count) k_wf_camera<true, false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, visits, none);
@@ -904,17 +954,30 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   for (uint32_t b = 0; b <= max_bounces; ++b) {
     if (b != 0) {
       Timed t(profile, stream, 1);
-      if (count)
-        k_wf_extend<true, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill, visits,
-            none);
+      if (count && analytic)
+        k_wf_extend<true, false, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
+            visits, none);
+      else if (count)
+        k_wf_extend<true, false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
+            visits, none);
+      else if (analytic)
+        k_wf_extend<false, false, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
+            nullptr, none);
       else
-        k_wf_extend<false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
+        k_wf_extend<false, false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
             nullptr, none);
     }
     {
       Timed t(profile, stream, 2);
-      if (C.enabled && b == 1) k_wf_shade<true, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
-      else k_wf_shade<false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
+      const bool cache_vertex = C.enabled && b == 1;
+      if (cache_vertex && analytic)
+        k_wf_shade<true, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
+      else if (cache_vertex)
+        k_wf_shade<true, false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
+      else if (analytic)
+        k_wf_shade<false, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
+      else
+        k_wf_shade<false, false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
     }
     {
       Timed t(profile, stream, 3);
@@ -956,16 +1019,22 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   uint32_t* fetch = Q.counts + 3 * (size_t)(max_bounces + 2);
   const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid_slots = (B.total_slots + kBlock - 1) / kBlock;
-  const uint32_t grid_extend = persistent_grid((const void*)k_wf_extend<false, true>, Q.capacity, tuning);
+  const uint32_t grid_extend = persistent_grid((const void*)k_wf_extend<false, true, false>, Q.capacity, tuning);
   const uint32_t grid_shadow = persistent_grid((const void*)k_wf_shadow<false, true>, Q.capacity, tuning);
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
-      8u * persistent_grid((const void*)k_wf_shade<false, true>, Q.capacity, TraceTuning()));
+      8u * persistent_grid((const void*)k_wf_shade<false, true, false>, Q.capacity, TraceTuning()));
   k_wf_camera<false, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
   for (uint32_t b = 0; b <= max_bounces; ++b) {
-    if (b != 0)
-      k_wf_extend<false, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, b, fetch + 2 * b,
-          refill, nullptr, B);
-    k_wf_shade<false, true><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, Q, b, no_cache, B);
+    if (b != 0 && B.analytic)
+      k_wf_extend<false, true, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, b,
+          fetch + 2 * b, refill, nullptr, B);
+    else if (b != 0)
+      k_wf_extend<false, true, false><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, b,
+          fetch + 2 * b, refill, nullptr, B);
+    if (B.analytic)
+      k_wf_shade<false, true, true><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, Q, b, no_cache, B);
+    else
+      k_wf_shade<false, true, false><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, Q, b, no_cache, B);
     k_wf_shadow<false, true><<<grid_shadow, kBlock, 0, stream>>>(none_view, P, Q, b, fetch + 2 * b + 1, refill,
         nullptr, B);
   }

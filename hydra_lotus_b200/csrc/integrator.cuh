@@ -73,6 +73,7 @@ struct SceneTable {
   const uint32_t* slot_base = nullptr;  // count + 1 entries
   uint32_t count = 0;
   uint32_t total_slots = 0;
+  bool analytic = false;  // some scene has analytic lights
 };
 
 // Launch shape of the persistent tracing kernels: a lane takes a new ray

@@ -229,16 +229,197 @@ std::vector<uint32_t> build_env_guides(const EnvDistribution& d) {
 }
 
 // The light table (BuildLightTable, gpu_scene.cpp:515-610): every emissive
-// triangle weighted by its mean emission times its world area, then the
-// environment image weighted as a distant light over the scene's bounding
-// sphere, chosen by Vose's alias method.
+// triangle weighted by its mean emission times its world area, every
+// analytic light by its estimated power, then the environment image
+// weighted as a distant light over the scene's bounding sphere, chosen by
+// Vose's alias method; with the analytic records, the crossing hierarchy
+// over the bounded ones and the distant lights' indices.
 struct LightTable {
   std::vector<LightRecord> records;
   std::vector<uint32_t> offsets;  // per instance
   std::vector<float4> verts;      // 3 per entry
   std::vector<float4> radiance;   // 1 per entry
+  std::vector<AnalyticLight> analytic;
+  std::vector<LightNode> nodes;
+  std::vector<uint32_t> distant;
   float env_selection = 0.0f;
 };
+
+struct HostD3 {
+  double x, y, z;
+};
+HostD3 column3(const float* m, int c) { return HostD3{m[4 * c], m[4 * c + 1], m[4 * c + 2]}; }
+double dot3(HostD3 a, HostD3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+HostD3 cross3(HostD3 a, HostD3 b) { return HostD3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+HostD3 scale3(HostD3 a, double s) { return HostD3{a.x * s, a.y * s, a.z * s}; }
+float4 store4(HostD3 v, double w) { return make_float4((float)v.x, (float)v.y, (float)v.z, (float)w); }
+
+// MakeAnalyticLight (gpu_scene.cpp:272-369): a light's record and its table
+// weight, its estimated power over 2 pi, the scale of an emissive
+// triangle's (a distant light's through a disk of the scene's radius).
+// False for a light that emits nothing: black, of zero size, or whose
+// radiance after normalization is not a finite float.
+bool make_analytic_light(const lotus_light& light, double radius_of_scene, double& weight, AnalyticLight& rec) {
+  constexpr double kPiD = 3.14159265358979323846;
+  const float* m = light.world_from_light;
+  const HostD3 x = column3(m, 0), y = column3(m, 1), z = column3(m, 2), origin = column3(m, 3);
+  const double determinant = dot3(x, cross3(y, z));
+  rec = AnalyticLight{};
+  double extent = 0.0, scale = 1.0;
+  if (light.shape == LOTUS_LIGHT_SPHERE) {
+    const double radius = light.radius * std::cbrt(std::fabs(determinant));
+    extent = 4.0 * kPiD * radius * radius;
+    rec.shape = kSphereLight;
+    rec.position = store4(origin, radius);
+    rec.normal = store4(HostD3{0, 0, 0}, extent);
+  } else if (light.shape == LOTUS_LIGHT_RECT || light.shape == LOTUS_LIGHT_DISK) {
+    const bool rect = light.shape == LOTUS_LIGHT_RECT;
+    const HostD3 u = scale3(x, rect ? 0.5 * light.width : light.radius);
+    const HostD3 v = scale3(y, rect ? 0.5 * light.height : light.radius);
+    const HostD3 normal = cross3(u, v);
+    const double length = std::sqrt(dot3(normal, normal));
+    extent = (rect ? 4.0 : kPiD) * length;
+    rec.shape = rect ? kRectLight : kDiskLight;
+    rec.position = store4(origin, 0.0);
+    rec.axis_u = store4(u, 0.0);
+    rec.axis_v = store4(v, 0.0);
+    // The -Z side, where the frame's inverse transpose takes the normal.
+    if (length > 0.0) rec.normal = store4(scale3(normal, (determinant < 0.0 ? 1.0 : -1.0) / length), extent);
+  } else {
+    const double length = std::sqrt(dot3(z, z));
+    if (!(length > 0.0)) return false;
+    const double theta = std::min(static_cast<double>(light.angle) * kPiD / 360.0, kPiD);
+    const double half = std::sin(0.5 * theta);
+    const double one_minus_cos = 2.0 * half * half;
+    const double sin2 = std::sin(theta) * std::sin(theta);
+    rec.axis_u = store4(scale3(z, 1.0 / length), one_minus_cos);
+    rec.shape = kParallelLight;
+    extent = 1.0;
+    if (theta > 0.0) {
+      extent = theta <= 0.5 * kPiD ? kPiD * sin2 : kPiD;
+      if (light.normalize) scale = 1.0 / (theta <= 0.5 * kPiD ? kPiD * sin2 : (2.0 - sin2) * kPiD);
+      if (static_cast<float>(one_minus_cos) >= std::numeric_limits<float>::min()) {
+        rec.shape = kDistantLight;
+      } else {
+        // Too narrow a cone for float densities: its irradiance, from one
+        // direction.
+        scale *= extent;
+        extent = 1.0;
+      }
+    }
+  }
+  if (light.normalize && light.shape != LOTUS_LIGHT_DISTANT) scale = 1.0 / extent;
+  double radiance[3];
+  for (int c = 0; c < 3; ++c) radiance[c] = light.radiance[c] * scale;
+  const double mean = (radiance[0] + radiance[1] + radiance[2]) / 3.0;
+  constexpr double kFloatMaxD = std::numeric_limits<float>::max();
+  if (!(extent > 0.0) || !std::isfinite(extent) || !(mean > 0.0) ||
+      !(radiance[0] <= kFloatMaxD && radiance[1] <= kFloatMaxD && radiance[2] <= kFloatMaxD))
+    return false;
+  rec.radiance = store4(HostD3{radiance[0], radiance[1], radiance[2]}, 0.0);
+  weight = mean * extent / 2.0;
+  if (light.shape == LOTUS_LIGHT_DISTANT) weight *= radius_of_scene * radius_of_scene;
+  if (!std::isfinite(weight)) weight = std::numeric_limits<double>::max();
+  return true;
+}
+
+// A bounded light's box (BoundLight, gpu_scene.cpp:398-428), widened by
+// 1e-4 of its extent plus 1e-5 of its coordinates' magnitude and rounded
+// outwards, so that the crossing test's rounding of a grazing ray cannot
+// leave the light outside it; and the centre the hierarchy splits by.
+struct LightBox {
+  float low[3], high[3];
+  double centre[3];
+  uint32_t index;
+};
+
+LightBox bound_light(const AnalyticLight& light, uint32_t index) {
+  LightBox b;
+  b.index = index;
+  const float pos[3] = {light.position.x, light.position.y, light.position.z};
+  const float au[3] = {light.axis_u.x, light.axis_u.y, light.axis_u.z};
+  const float av[3] = {light.axis_v.x, light.axis_v.y, light.axis_v.z};
+  for (int a = 0; a < 3; ++a) {
+    const double centre = pos[a], u = au[a], v = av[a];
+    const double extent = light.shape == kSphereLight ? (double)light.position.w
+        : light.shape == kRectLight                   ? std::fabs(u) + std::fabs(v)
+                                                      : std::sqrt(u * u + v * v);
+    const double margin = 1e-4 * extent + 1e-5 * (std::fabs(centre) + extent);
+    b.centre[a] = centre;
+    b.low[a] = std::nextafter((float)(centre - extent - margin), -std::numeric_limits<float>::infinity());
+    b.high[a] = std::nextafter((float)(centre + extent + margin), std::numeric_limits<float>::infinity());
+  }
+  return b;
+}
+
+void store_bounds(float4& low, float4& high, const LightBox* first, const LightBox* last, uint32_t child) {
+  float lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = std::numeric_limits<float>::max();
+    hi[a] = -std::numeric_limits<float>::max();
+    for (const LightBox* it = first; it != last; ++it) {
+      lo[a] = std::min(lo[a], it->low[a]);
+      hi[a] = std::max(hi[a], it->high[a]);
+    }
+  }
+  float w;
+  std::memcpy(&w, &child, 4);
+  low = make_float4(lo[0], lo[1], lo[2], w);
+  high = make_float4(hi[0], hi[1], hi[2], 0.0f);
+}
+
+// BuildLightNode (gpu_scene.cpp:438-476): a leaf for one light, otherwise a
+// node whose children split the lights at the median centre along the axis
+// of widest centre spread (ties by index, so the hierarchy depends only on
+// the lights; depth at most ceil(log2(count))). Nodes in preorder.
+uint32_t build_light_node(LightBox* first, LightBox* last, std::vector<LightNode>& nodes) {
+  if (last - first == 1) return kLightLeaf | first->index;
+  const uint32_t node = (uint32_t)nodes.size();
+  nodes.emplace_back();
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) lo[a] = hi[a] = first->centre[a];
+  for (const LightBox* it = first; it != last; ++it)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], it->centre[a]);
+      hi[a] = std::max(hi[a], it->centre[a]);
+    }
+  int axis = 0;
+  for (int c = 1; c < 3; ++c)
+    if (hi[c] - lo[c] > hi[axis] - lo[axis]) axis = c;
+  LightBox* middle = first + (last - first) / 2;
+  std::nth_element(first, middle, last, [axis](const LightBox& a, const LightBox& b) {
+    return a.centre[axis] != b.centre[axis] ? a.centre[axis] < b.centre[axis] : a.index < b.index;
+  });
+  const uint32_t left = build_light_node(first, middle, nodes);
+  const uint32_t right = build_light_node(middle, last, nodes);
+  LightNode& stored = nodes[node];
+  store_bounds(stored.low0, stored.high0, first, middle, left);
+  store_bounds(stored.low1, stored.high1, middle, last, right);
+  return node;
+}
+
+// BuildLightHierarchy (gpu_scene.cpp:478-499): the crossing hierarchy over
+// the sphere, rect and disk lights and the distant lights' indices;
+// parallel lights, which no ray crosses, are in neither. One bounded light
+// gets a root whose second child is empty.
+void build_light_hierarchy(LightTable& table) {
+  std::vector<LightBox> bounded;
+  for (size_t i = 0; i < table.analytic.size(); ++i) {
+    const uint32_t shape = table.analytic[i].shape;
+    if (shape == kDistantLight)
+      table.distant.push_back((uint32_t)i);
+    else if (shape != kParallelLight)
+      bounded.push_back(bound_light(table.analytic[i], (uint32_t)i));
+  }
+  if (bounded.size() == 1) {
+    LightNode root;
+    store_bounds(root.low0, root.high0, bounded.data(), bounded.data() + 1, kLightLeaf | bounded[0].index);
+    store_bounds(root.low1, root.high1, nullptr, nullptr, kNoLightChild);
+    table.nodes.push_back(root);
+  } else if (bounded.size() > 1) {
+    build_light_node(bounded.data(), bounded.data() + bounded.size(), table.nodes);
+  }
+}
 
 double world_triangle_area(const lotus_geometry& g, uint32_t t, const float* m) {
   double corners[3][3];
@@ -318,10 +499,27 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
           mat.emission[2] * coverage, 0.0f));
     }
   }
+  bool distant = env_mean > 0.0;
+  for (uint32_t i = 0; i < s.light_count; ++i) distant = distant || s.lights[i].shape == LOTUS_LIGHT_DISTANT;
+  const double r = distant ? scene_radius(s) : 0.0;
+  std::vector<uint32_t> analytic_entries;
+  for (uint32_t i = 0; i < s.light_count; ++i) {
+    double weight = 0.0;
+    AnalyticLight rec;
+    if (!make_analytic_light(s.lights[i], r, weight, rec)) continue;
+    if (weight > 0.0) {
+      analytic_entries.push_back((uint32_t)table.records.size());
+      weights.push_back(weight);
+      table.records.push_back({0.0f, 1.0f, 0u, kAnalyticLight | (uint32_t)table.analytic.size()});
+      for (int k = 0; k < 3; ++k) table.verts.push_back(make_float4(0, 0, 0, 0));
+      table.radiance.push_back(make_float4(0, 0, 0, 0));
+    }
+    table.analytic.push_back(rec);
+  }
+  build_light_hierarchy(table);
   double env_weight = 0.0;
   if (env_mean > 0.0) {
     constexpr double kPiD = 3.14159265358979323846;
-    const double r = scene_radius(s);
     env_weight = kPiD * kPiD * r * r * env_mean;
     if (!std::isfinite(env_weight)) env_weight = std::numeric_limits<double>::max();
   }
@@ -362,6 +560,10 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
   }
   for (uint32_t i : small) { table.records[i].threshold = 1.0f; table.records[i].alias = i; }
   for (uint32_t i : large) { table.records[i].threshold = 1.0f; table.records[i].alias = i; }
+  // Each analytic record keeps its entry's probability, which weighs the
+  // emission BSDF sampling finds on it.
+  for (uint32_t entry : analytic_entries)
+    table.analytic[table.records[entry].instance & ~kAnalyticLight].radiance.w = table.records[entry].pdf;
   if (env_weight > 0.0) table.env_selection = table.records.back().pdf;
   return table;
 }
@@ -387,6 +589,7 @@ struct HostScene {
   uint32_t env_width = 0, env_height = 0, env_columns = 0, env_rows = 0;
   float env_scale[3] = {0.0f, 0.0f, 0.0f};
   float env_frame[9] = {};
+  std::vector<lotus_light> lights;      // the analytic lights
 };
 
 static_assert(LOTUS_OUTPUT_BARYCENTRICS == kOutputBarycentrics && LOTUS_OUTPUT_SHADING_NORMAL == kOutputShadingNormal &&
@@ -415,6 +618,9 @@ struct Renderer {
   DeviceArray<float4> env_texels;
   DeviceArray<float> env_floats;
   DeviceArray<uint32_t> env_guide;
+  DeviceArray<AnalyticLight> analytic;
+  DeviceArray<LightNode> light_nodes;
+  DeviceArray<uint32_t> distant;
   std::vector<LightRecord> host_lights;
   std::vector<uint32_t> host_light_offsets;
   SceneView view{};
@@ -527,13 +733,15 @@ struct Renderer {
     blas.release(); tlas.release(); blas4.release(); tlas4.release(); tris.release(); inst_trav.release(); inst_shade.release();
     materials.release(); normals.release(); lights.release(); light_verts.release();
     light_radiance.release(); env_texels.release(); env_floats.release(); env_guide.release();
+    analytic.release(); light_nodes.release(); distant.release();
     scene_ready = false;
   }
 
   uint64_t scene_bytes() const {
     return scene_pos.bytes() + scene_tri.bytes() + blas.bytes() + tlas.bytes() + blas4.bytes() + tlas4.bytes() + tris.bytes() + inst_trav.bytes() + inst_shade.bytes() +
            materials.bytes() + normals.bytes() + lights.bytes() + light_verts.bytes() +
-           light_radiance.bytes() + env_texels.bytes() + env_floats.bytes() + env_guide.bytes();
+           light_radiance.bytes() + env_texels.bytes() + env_floats.bytes() + env_guide.bytes() +
+           analytic.bytes() + light_nodes.bytes() + distant.bytes();
   }
 };
 
@@ -605,6 +813,27 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
     detail = "the environment image has no texels";
     return false;
   }
+  if (s.light_count && !s.lights) {
+    detail = "light_count without lights";
+    return false;
+  }
+  // The crossing hierarchy's depth, ceil(log2(lights)), must fit the
+  // traversal's stack.
+  if (s.light_count >= (1u << 30)) {
+    detail = "too many analytic lights";
+    return false;
+  }
+  for (uint32_t i = 0; i < s.light_count; ++i) {
+    const lotus_light& l = s.lights[i];
+    bool finite = std::isfinite(l.radius) && std::isfinite(l.width) && std::isfinite(l.height) &&
+        std::isfinite(l.angle);
+    for (float v : l.world_from_light) finite = finite && std::isfinite(v);
+    for (float v : l.radiance) finite = finite && std::isfinite(v);
+    if (l.shape > LOTUS_LIGHT_DISTANT || !finite) {
+      detail = "analytic light " + std::to_string(i) + " has an unknown shape or a non-finite value";
+      return false;
+    }
+  }
   return true;
 }
 
@@ -639,6 +868,8 @@ lotus_scene_desc host_desc(const Renderer& R) {
   d.instance_count = (uint32_t)R.host_instances.size();
   d.material_count = (uint32_t)h.materials.size();
   for (int k = 0; k < 3; ++k) d.environment_constant[k] = h.environment_constant[k];
+  d.lights = h.lights.data();
+  d.light_count = (uint32_t)h.lights.size();
   return d;
 }
 
@@ -715,6 +946,9 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
       !R.ok(R.light_verts.upload(in.table.verts.data(), in.table.verts.size(), st), "light corners", detail) ||
       !R.ok(R.light_radiance.upload(in.table.radiance.data(), in.table.radiance.size(), st), "light radiance",
           detail) ||
+      !R.ok(R.analytic.upload(in.table.analytic.data(), in.table.analytic.size(), st), "analytic lights", detail) ||
+      !R.ok(R.light_nodes.upload(in.table.nodes.data(), in.table.nodes.size(), st), "light hierarchy", detail) ||
+      !R.ok(R.distant.upload(in.table.distant.data(), in.table.distant.size(), st), "distant lights", detail) ||
       !R.ok(R.inst_trav.upload(in.trav.data(), in.trav.size(), st), "instances", detail) ||
       !R.ok(R.inst_shade.upload(in.shade.data(), in.shade.size(), st), "instances", detail) ||
       !R.ok(R.tlas.resize(std::max<uint32_t>(BvhBuilder::node_count(n), 1)), "TLAS", detail))
@@ -757,6 +991,12 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
   }
   v.env_selection = in.table.env_selection;
   for (int k = 0; k < 3; ++k) v.env_constant[k] = h.environment_constant[k];
+  v.analytic = R.analytic.ptr;
+  v.light_nodes = R.light_nodes.ptr;
+  v.distant = R.distant.ptr;
+  v.analytic_count = (uint32_t)in.table.analytic.size();
+  v.light_node_count = (uint32_t)in.table.nodes.size();
+  v.distant_count = (uint32_t)in.table.distant.size();
   return true;
 }
 
@@ -868,6 +1108,7 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
   h.nodes = nodes;
   h.materials.assign(s.materials, s.materials + s.material_count);
   for (int k = 0; k < 3; ++k) h.environment_constant[k] = s.environment_constant[k];
+  h.lights.assign(s.lights, s.lights + s.light_count);
   R.host_instances.assign(s.instances, s.instances + s.instance_count);
   if (nodes >= kMaxSceneTriangles || tri_total >= kMaxSceneTriangles)
     return fail("the scene holds 2^28 triangles or more");
@@ -1437,7 +1678,7 @@ uint32_t lotus_cuda_abi_version(void) { return LOTUS_CUDA_ABI_VERSION; }
 
 uint32_t lotus_cuda_struct_sizes(uint64_t* sizes, uint32_t capacity) {
   const uint64_t s[] = {sizeof(lotus_geometry), sizeof(lotus_instance), sizeof(lotus_material),
-      sizeof(lotus_environment), sizeof(lotus_scene_desc), sizeof(lotus_scene_result),
+      sizeof(lotus_environment), sizeof(lotus_light), sizeof(lotus_scene_desc), sizeof(lotus_scene_result),
       sizeof(lotus_target), sizeof(lotus_settings), sizeof(lotus_frame_desc),
       sizeof(lotus_frame_result), sizeof(lotus_cuda_options), sizeof(lotus_temporal_desc),
       sizeof(lotus_temporal_instance), sizeof(lotus_cache_desc)};

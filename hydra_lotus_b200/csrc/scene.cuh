@@ -101,6 +101,30 @@ struct alignas(16) LightRecord {
   uint32_t instance;
 };
 
+// One analytic light in world space (GpuAnalyticLightRecord,
+// gpu_scene.hpp:144-166): a sphere's centre and radius; a rect's or disk's
+// centre, half axes and emitting-side unit normal with its area in w; a
+// distant light's unit direction towards it in axis_u with 1 - cos of its
+// cone in w; the radiance with the light's table probability in w.
+struct alignas(16) AnalyticLight {
+  float4 position;
+  float4 axis_u;
+  float4 axis_v;
+  float4 normal;
+  float4 radiance;
+  uint32_t shape;
+  uint32_t reserved[3];
+};
+static_assert(sizeof(AnalyticLight) == 96, "AnalyticLight is 96 bytes");
+
+// One interior node of the binary crossing hierarchy over the sphere, rect
+// and disk lights (GpuLightNode, gpu_scene.hpp:174-186): each child's box,
+// the child's bits in low.w.
+struct alignas(16) LightNode {
+  float4 low0, high0, low1, high1;
+};
+static_assert(sizeof(LightNode) == 64, "LightNode is 64 bytes");
+
 struct SceneView {
   const Bvh4Node* __restrict__ tlas;
   const Bvh4Node* __restrict__ blas;
@@ -123,6 +147,12 @@ struct SceneView {
   float env_scale[3];
   float env_frame[9];       // rows of environment_from_world
   float env_constant[3];
+  const AnalyticLight* __restrict__ analytic;  // every analytic record, table entry or not
+  const LightNode* __restrict__ light_nodes;   // the crossing hierarchy (node 0: root)
+  const uint32_t* __restrict__ distant;        // indices of the distant lights
+  uint32_t analytic_count;
+  uint32_t light_node_count;
+  uint32_t distant_count;
 };
 
 // Buckets of the environment distribution's guide tables (powers of two):

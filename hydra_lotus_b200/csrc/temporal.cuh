@@ -278,12 +278,53 @@ __device__ __forceinline__ float reservoir_proposal_pdf(const SceneView& S, uint
   return power;
 }
 
-// ReconstructReservoirLight for emissive triangles and the environment.
+// ReconstructReservoirLight: the candidate (ux, uy) of light-table slot
+// `index`. Emissive triangles, rects and disks by area, the environment and
+// distant lights by their receiver-independent maps; a sphere light's
+// candidates are points uniform over its whole area, back-facing ones
+// carrying nothing. kAnalytic = false leaves out the analytic lights' code,
+// for scenes without them.
+template <bool kAnalytic = true>
 __device__ __forceinline__ LightSample reconstruct_reservoir_light(const SceneView& S,
     uint32_t index, float ux, float uy, F3 origin) {
   const LightRecord chosen = S.lights[index];
   if (chosen.instance == kEnvironmentLight) return sample_environment(S, chosen.pdf, ux, uy);
-  return sample_triangle(S, index, chosen.pdf, ux, uy, origin);
+  if (!kAnalytic || (chosen.instance & kAnalyticLight) == 0)
+    return sample_triangle(S, index, chosen.pdf, ux, uy, origin);
+  const AnalyticLight& light = S.analytic[chosen.instance & ~kAnalyticLight];
+  if (light.shape != kSphereLight) return sample_analytic(light, chosen.pdf, ux, uy, origin);
+  const float z = 1.0f - 2.0f * ux;
+  const float radius_xy = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+  const float phi = 2.0f * kPi * uy;
+  float sn, cs;
+  lsincos(phi, sn, cs);
+  const F3 normal = V(radius_xy * cs, radius_xy * sn, z);
+  const F3 toward = V(light.position) + light.position.w * normal - origin;
+  const float distance2 = dot(toward, toward);
+  if (!(distance2 > 0.0f)) return no_light();
+  LightSample s = no_light();
+  s.distance = sqrtf(distance2);
+  s.direction = toward / s.distance;
+  const float cosine = -dot(normal, s.direction);
+  if (!(cosine > 0.0f)) return no_light();
+  s.radiance = V(light.radiance);
+  s.pdf = chosen.pdf * distance2 / (cosine * 4.0f * kPi * light.position.w * light.position.w);
+  return s;
+}
+
+// ReservoirPartitionPdf (scene.slang:973-983): SampleLight's density for
+// the reservoir sample's direction, which for a sphere light is its cone's.
+__device__ __forceinline__ float reservoir_partition_pdf(const SceneView& S, uint32_t index,
+    const LightSample& ls, F3 origin) {
+  const LightRecord chosen = S.lights[index];
+  if ((chosen.instance & kAnalyticLight) != 0 && chosen.instance != kEnvironmentLight) {
+    const AnalyticLight& light = S.analytic[chosen.instance & ~kAnalyticLight];
+    if (light.shape == kSphereLight) {
+      const F3 offset = V(light.position) - origin;
+      return chosen.pdf * sphere_cone_pdf(light.position.w * light.position.w / dot(offset, offset));
+    }
+  }
+  return ls.pdf;
 }
 
 }  // namespace lotus

@@ -247,7 +247,239 @@ __device__ __forceinline__ F3 environment_radiance(const SceneView& S, F3 direct
   return radiance * power_heuristic(pdf, S.env_selection * environment_direction_pdf(S, u, v));
 }
 
+// SampleConcentricDisk (sampling.slang:89-104): Shirley and Chiu's map of
+// the square onto the unit disk.
+__device__ __forceinline__ void sample_concentric_disk(float ux, float uy, float& a, float& b) {
+  const float ox = 2.0f * ux - 1.0f, oy = 2.0f * uy - 1.0f;
+  if (ox == 0.0f && oy == 0.0f) {
+    a = b = 0.0f;
+    return;
+  }
+  float radius, theta;
+  if (fabsf(ox) > fabsf(oy)) {
+    radius = ox;
+    theta = 0.25f * kPi * (oy / ox);
+  } else {
+    radius = oy;
+    theta = 0.5f * kPi - 0.25f * kPi * (ox / oy);
+  }
+  float sn, cs;
+  lsincos(theta, sn, cs);
+  a = radius * cs;
+  b = radius * sn;
+}
+
+// SampleUniformCone (sampling.slang:109-116), about +z.
+__device__ __forceinline__ F3 sample_uniform_cone(float ux, float uy, float one_minus_cos_max) {
+  const float one_minus_cos = ux * one_minus_cos_max;
+  const float sin_theta = sqrtf(fmaxf(0.0f, one_minus_cos * (2.0f - one_minus_cos)));
+  const float phi = 2.0f * kPi * uy;
+  float sn, cs;
+  lsincos(phi, sn, cs);
+  return V(sin_theta * cs, sin_theta * sn, 1.0f - one_minus_cos);
+}
+
+// SphereConePdf (scene.slang:683-690): the solid-angle density of a
+// sphere's cone, 1 - cos(theta_max) without cancellation for small spheres.
+__device__ __forceinline__ float sphere_cone_pdf(float sin2_max) {
+  const float one_minus_cos = sin2_max < 0.00068523f ? 0.5f * sin2_max
+                                                     : 1.0f - sqrtf(fmaxf(0.0f, 1.0f - sin2_max));
+  return 1.0f / (2.0f * kPi * one_minus_cos);
+}
+
+// SampleAnalytic (scene.slang:695-768): a sphere by solid angle over its
+// cone (PBRT 4th ed. 6.2.4), a rect or disk by area, a distant light over
+// its cone, a parallel light along its direction (a delta light).
+__device__ __forceinline__ LightSample sample_analytic(const AnalyticLight& light, float selection,
+    float ux, float uy, F3 origin) {
+  LightSample s = no_light();
+  s.radiance = V(light.radiance);
+  if (light.shape == kSphereLight) {
+    const F3 centre = V(light.position);
+    const float radius = light.position.w;
+    const F3 to_centre = centre - origin;
+    const float distance2 = dot(to_centre, to_centre);
+    if (!(distance2 > radius * radius)) return no_light();
+    const float sin2_max = radius * radius / distance2;
+    const float sin_max = sqrtf(sin2_max);
+    const float cos_max = sqrtf(fmaxf(0.0f, 1.0f - sin2_max));
+    float cos_theta = (cos_max - 1.0f) * ux + 1.0f;
+    float sin2_theta = 1.0f - cos_theta * cos_theta;
+    if (sin2_max < 0.00068523f) {
+      sin2_theta = sin2_max * ux;
+      cos_theta = sqrtf(1.0f - sin2_theta);
+    }
+    const float cos_alpha = sin2_theta / sin_max + cos_theta * sqrtf(fmaxf(0.0f, 1.0f - sin2_theta / sin2_max));
+    const float sin_alpha = sqrtf(fmaxf(0.0f, 1.0f - cos_alpha * cos_alpha));
+    const float phi = 2.0f * kPi * uy;
+    float sn, cs;
+    lsincos(phi, sn, cs);
+    const Frame frame = make_frame(normalize(to_centre));
+    const F3 outward = frame.to_world(-V(sin_alpha * cs, sin_alpha * sn, cos_alpha));
+    const F3 toward = centre + radius * outward - origin;
+    s.distance = length(toward);
+    s.direction = toward / s.distance;
+    s.pdf = selection * sphere_cone_pdf(sin2_max);
+  } else if (light.shape == kRectLight || light.shape == kDiskLight) {
+    float a, b;
+    if (light.shape == kRectLight) {
+      a = 2.0f * ux - 1.0f;
+      b = 2.0f * uy - 1.0f;
+    } else {
+      sample_concentric_disk(ux, uy, a, b);
+    }
+    const F3 toward = V(light.position) + a * V(light.axis_u) + b * V(light.axis_v) - origin;
+    const float distance2 = dot(toward, toward);
+    if (!(distance2 > 0.0f)) return no_light();
+    s.distance = sqrtf(distance2);
+    s.direction = toward / s.distance;
+    const float cosine = -dot(V(light.normal), s.direction);
+    if (!(cosine > 0.0f)) return no_light();
+    s.pdf = selection * distance2 / (cosine * light.normal.w);
+  } else if (light.shape == kDistantLight) {
+    const Frame frame = make_frame(V(light.axis_u));
+    s.direction = normalize(frame.to_world(sample_uniform_cone(ux, uy, light.axis_u.w)));
+    s.distance = kFloatMax;
+    s.pdf = selection / (2.0f * kPi * light.axis_u.w);
+  } else {
+    s.direction = V(light.axis_u);
+    s.distance = kFloatMax;
+    s.pdf = selection;
+    s.delta = true;
+  }
+  return s;
+}
+
+// ParallelLight (scene.slang:986-1000): a parallel light's direction and
+// irradiance as a delta light of density 1; no light for other shapes.
+__device__ __forceinline__ LightSample parallel_light(const SceneView& S, uint32_t index) {
+  const AnalyticLight& light = S.analytic[index];
+  if (light.shape != kParallelLight) return no_light();
+  LightSample s;
+  s.direction = V(light.axis_u);
+  s.distance = kFloatMax;
+  s.radiance = V(light.radiance);
+  s.pdf = 1.0f;
+  s.delta = true;
+  return s;
+}
+
+// CrossedLight (scene.slang:1019-1091): the emission of analytic light
+// `index` if the ray crosses it before `distance` (a sphere's near side
+// from outside it, by the nearer root without cancellation; a rect's or
+// disk's emitting side; a distant light's cone for an escaping ray),
+// weighed against light sampling's density when `weigh`.
+__device__ __forceinline__ F3 crossed_light(const SceneView& S, uint32_t index, F3 origin, F3 direction,
+    float distance, bool escaped, bool weigh, float pdf) {
+  const AnalyticLight& light = S.analytic[index];
+  const uint32_t shape = light.shape;
+  float light_pdf = 0.0f;
+  if (shape == kSphereLight) {
+    const float radius = light.position.w;
+    const F3 offset = origin - V(light.position);
+    const float c = dot(offset, offset) - radius * radius;
+    const float b = -dot(offset, direction);
+    const F3 perpendicular = offset + b * direction;
+    const float discriminant = radius * radius - dot(perpendicular, perpendicular);
+    if (!(c > 0.0f) || !(b > 0.0f) || discriminant < 0.0f) return V(0.0f);
+    const float t = c / (b + sqrtf(discriminant));
+    if (!(t < distance)) return V(0.0f);
+    light_pdf = sphere_cone_pdf(radius * radius / dot(offset, offset));
+  } else if (shape == kRectLight || shape == kDiskLight) {
+    const F3 n = V(light.normal);
+    const float facing = dot(direction, n);
+    if (!(facing < 0.0f)) return V(0.0f);
+    const float t = dot(V(light.position) - origin, n) / facing;
+    if (!(t > 0.0f) || !(t < distance)) return V(0.0f);
+    const F3 q = origin + t * direction - V(light.position);
+    const F3 u = V(light.axis_u), v = V(light.axis_v);
+    const float uu = dot(u, u), uv = dot(u, v), vv = dot(v, v);
+    const float qu = dot(q, u), qv = dot(q, v);
+    const float determinant = uu * vv - uv * uv;
+    const float a = (qu * vv - qv * uv) / determinant;
+    const float b = (qv * uu - qu * uv) / determinant;
+    if (shape == kRectLight ? !(fabsf(a) <= 1.0f && fabsf(b) <= 1.0f) : !(a * a + b * b <= 1.0f)) return V(0.0f);
+    light_pdf = t * t / (-facing * light.normal.w);
+  } else if (shape == kDistantLight && escaped) {
+    const F3 toward = V(light.axis_u);
+    const float one_minus_cos = light.axis_u.w;
+    const float cosine = dot(direction, toward);
+    if (one_minus_cos <= 1.0f) {
+      const F3 across = cross(direction, toward);
+      if (!(cosine > 0.0f) || !(dot(across, across) <= one_minus_cos * (2.0f - one_minus_cos))) return V(0.0f);
+    } else if (!(cosine >= 1.0f - one_minus_cos)) {
+      return V(0.0f);
+    }
+    light_pdf = 1.0f / (2.0f * kPi * one_minus_cos);
+  } else {
+    return V(0.0f);
+  }
+  const float weight = weigh ? power_heuristic(pdf, light.radiance.w * light_pdf) : 1.0f;
+  return V(light.radiance) * weight;
+}
+
+// OverlapsBox (scene.slang:1095-1103).
+__device__ __forceinline__ bool overlaps_box(float4 low, float4 high, F3 origin, F3 inverse, float distance) {
+  const float t0x = (low.x - origin.x) * inverse.x, t1x = (high.x - origin.x) * inverse.x;
+  const float t0y = (low.y - origin.y) * inverse.y, t1y = (high.y - origin.y) * inverse.y;
+  const float t0z = (low.z - origin.z) * inverse.z, t1z = (high.z - origin.z) * inverse.z;
+  const float nx = fminf(t0x, t1x), ny = fminf(t0y, t1y), nz = fminf(t0z, t1z);
+  const float fx = fmaxf(t0x, t1x), fy = fmaxf(t0y, t1y), fz = fmaxf(t0z, t1z);
+  return fmaxf(fmaxf(nx, ny), fmaxf(nz, 0.0f)) <= fminf(fminf(fx, fy), fminf(fz, distance));
+}
+
+// CrossedLights (scene.slang:1110-1178): the analytic lights the ray
+// crosses before `distance`, summed in the crossing hierarchy's traversal
+// order (child 0 before child 1, the second of two interior children
+// stacked), then, for an escaping ray, the distant lights. Lights neither
+// block rays nor each other.
+static __device__ __noinline__ F3 crossed_lights(const SceneView& S, F3 origin, F3 direction, float distance,
+    bool escaped, bool weigh, float pdf) {
+  F3 sum = V(0.0f);
+  if (S.light_node_count != 0) {
+    const F3 inverse = safe_inverse(direction);
+    uint32_t stack[kLightStackSize];
+    uint32_t depth = 0, node = 0;
+    // A hierarchy of n nodes is walked in at most n steps.
+    for (uint32_t step = 0; step < S.light_node_count; ++step) {
+      const LightNode current = S.light_nodes[node];
+      const uint32_t child0 = __float_as_uint(current.low0.w);
+      const uint32_t child1 = __float_as_uint(current.low1.w);
+      const bool enter0 = overlaps_box(current.low0, current.high0, origin, inverse, distance);
+      const bool enter1 =
+          child1 != kNoLightChild && overlaps_box(current.low1, current.high1, origin, inverse, distance);
+      uint32_t next = 0xFFFFFFFFu;
+      if (enter0) {
+        if ((child0 & kLightLeaf) != 0)
+          sum = sum + crossed_light(S, child0 & ~kLightLeaf, origin, direction, distance, escaped, weigh, pdf);
+        else
+          next = child0;
+      }
+      if (enter1) {
+        if ((child1 & kLightLeaf) != 0)
+          sum = sum + crossed_light(S, child1 & ~kLightLeaf, origin, direction, distance, escaped, weigh, pdf);
+        else if (next == 0xFFFFFFFFu)
+          next = child1;
+        else if (depth < kLightStackSize)
+          stack[depth++] = child1;
+      }
+      if (next == 0xFFFFFFFFu) {
+        if (depth == 0) break;
+        next = stack[--depth];
+      }
+      node = next;
+    }
+  }
+  if (escaped)
+    for (uint32_t i = 0; i < S.distant_count; ++i)
+      sum = sum + crossed_light(S, S.distant[i], origin, direction, distance, escaped, weigh, pdf);
+  return sum;
+}
+
 // SampleLight (scene.slang:894-909): Vose's alias table, then a point.
+// kAnalytic = false leaves out the analytic lights' code, for scenes
+// without them.
+template <bool kAnalytic = true>
 __device__ __forceinline__ LightSample sample_light(const SceneView& S, float u0, float u1,
     float u2, float u3, F3 origin) {
   const uint32_t count = S.light_count;
@@ -256,6 +488,8 @@ __device__ __forceinline__ LightSample sample_light(const SceneView& S, float u0
   const uint32_t light = u1 < record.threshold ? column : record.alias;
   const LightRecord chosen = S.lights[light];
   if (chosen.instance == kEnvironmentLight) return sample_environment(S, chosen.pdf, u2, u3);
+  if (kAnalytic && (chosen.instance & kAnalyticLight) != 0)
+    return sample_analytic(S.analytic[chosen.instance & ~kAnalyticLight], chosen.pdf, u2, u3, origin);
   return sample_triangle(S, light, chosen.pdf, u2, u3, origin);
 }
 

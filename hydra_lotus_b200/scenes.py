@@ -128,6 +128,7 @@ class Scene:
         self.materials = [preview_material()]  # slot 0: the default material
         self.environment = None
         self.environment_constant = (0.0, 0.0, 0.0)
+        self.lights = []  # analytic lights (abi.Light)
         self.world_to_clip = identity()
         self.view = None  # world to view space, when the temporal passes need it
         self.width = 0
@@ -172,6 +173,21 @@ class Scene:
             normals = np.ascontiguousarray(normals, dtype=F32).reshape(-1, 3, 3)
         self.geometries[geometry] = (positions, t, normals if n is not None else None)
         self._desc = None
+
+    def add_light(self, shape, world_from_light=None, radiance=(1.0, 1.0, 1.0), normalize=False,
+                  radius=0.5, width=1.0, height=1.0, angle=0.53):
+        """An analytic light (Lotus::Light): abi.LIGHT_SPHERE, _RECT, _DISK or
+        _DISTANT, in the frame `world_from_light` (column-major)."""
+        light = abi.Light()
+        light.shape = shape
+        light.normalize = 1 if normalize else 0
+        m = identity() if world_from_light is None else np.asarray(world_from_light, dtype=F32)
+        light.world_from_light[:] = [float(v) for v in m.reshape(-1)]
+        light.radiance[:] = [float(v) for v in radiance]
+        light.radius, light.width, light.height, light.angle = radius, width, height, angle
+        self.lights.append(light)
+        self._desc = None
+        return len(self.lights) - 1
 
     def set_environment(self, texels, scale=(1.0, 1.0, 1.0), rows=None):
         texels = np.ascontiguousarray(texels, dtype=F32)
@@ -223,7 +239,12 @@ class Scene:
             env.scale[:] = [float(v) for v in scale]
             env.environment_from_world[:] = [float(v) for v in rows.reshape(-1)]
             d.environment = C.pointer(env)
-        self._keep = (geos, insts, mats, env)
+        lights = None
+        if self.lights:
+            lights = (abi.Light * len(self.lights))(*self.lights)
+            d.lights = lights
+            d.light_count = len(self.lights)
+        self._keep = (geos, insts, mats, env, lights)
         self._desc = d
         return d
 
@@ -640,5 +661,107 @@ def big_mesh(seed=0, size=96, subdivisions=6):
     s.add_instance(s.add_geometry(*quad([[-6, -1.2, 6], [6, -1.2, 6], [6, -1.2, -6], [-6, -1.2, -6]])), clay)
     s.set_environment(procedural_sky(256, 128, seed))
     s.world_to_clip = multiply(perspective(45.0, 1.0, 0.1, 100.0), look_at((0.0, 1.5, 6.0), (0.0, 0.0, 0.0)))
+    s.width = s.height = size
+    return s
+
+
+# ---------------------------------------------------------------------------
+# Analytic lights (Lotus::Light, render_world.hpp:79-114)
+
+# Frames whose -Z side faces down (-Y) and towards +X: a rect or disk in the
+# light's XY plane emits from its -Z side.
+FACING_DOWN = np.array([[1.0, 0.0, 0.0], [0.0, 0.0, 1.0], [0.0, -1.0, 0.0]])
+FACING_PLUS_X = np.array([[0.0, 0.0, -1.0], [0.0, 1.0, 0.0], [1.0, 0.0, 0.0]])
+
+
+def towards(direction):
+    """A frame whose +Z axis is `direction`: a distant light shining from
+    there along its -Z axis."""
+    z = np.asarray(direction, dtype=np.float64)
+    z = z / np.linalg.norm(z)
+    helper = np.array([0.0, 1.0, 0.0]) if abs(z[1]) < 0.9 else np.array([1.0, 0.0, 0.0])
+    x = np.cross(helper, z)
+    x /= np.linalg.norm(x)
+    y = np.cross(z, x)
+    return np.stack([x, y, z], axis=1)
+
+
+def lit_room(seed=0, size=128, parallel=True, environment=False):
+    """The box room with one light of every analytic shape besides its
+    ceiling emitter: two spheres (one small enough for the cone sampler's
+    small-angle branch from most of the room), a rect under the ceiling
+    facing down, a disk on the left wall facing +X, a distant light of 5
+    degrees and, with `parallel`, a parallel light, both reaching in through
+    the open front; optionally the procedural sky."""
+    s = box_room(seed=seed, size=size)
+    s.name = f"lit-room-{seed}"
+    s.add_light(abi.LIGHT_SPHERE, affine(translation=(-0.45, 0.35, -0.35)), radiance=(6.0, 4.5, 2.0),
+                radius=0.12)
+    s.add_light(abi.LIGHT_SPHERE, affine(linear=np.eye(3) * 0.5, translation=(0.55, -0.2, -0.6)),
+                radiance=(400.0, 300.0, 500.0), radius=0.02)
+    s.add_light(abi.LIGHT_RECT, affine(linear=FACING_DOWN, translation=(0.3, 0.9, 0.2)),
+                radiance=(2.0, 3.0, 4.0), width=0.5, height=0.3)
+    s.add_light(abi.LIGHT_DISK, affine(linear=FACING_PLUS_X, translation=(-0.97, -0.3, 0.1)),
+                radiance=(5.0, 1.0, 1.0), radius=0.2, normalize=True)
+    s.add_light(abi.LIGHT_DISTANT, affine(linear=towards((0.3, 0.4, 1.0))), radiance=(3.0, 3.0, 2.5),
+                angle=5.0)
+    if parallel:
+        s.add_light(abi.LIGHT_DISTANT, affine(linear=towards((-0.2, 0.3, 1.0))), radiance=(1.5, 1.2, 1.0),
+                    angle=0.0)
+    if environment:
+        s.set_environment(procedural_sky(256, 128, seed=seed))
+    return s
+
+
+def many_lights(seed=0, size=128, count=48):
+    """A ground plane with a few boxes under `count` seeded analytic lights
+    (spheres, rects and disks in equal shares, log-normal radiance) hovering
+    above it: the crossing hierarchy holds every one, and rays cross several
+    on their way."""
+    rng = np.random.default_rng(seed)
+    s = Scene(f"many-lights-{seed}")
+    ground = s.add_material(preview_material((0.5, 0.5, 0.5), roughness=0.6, ior=1.0))
+    s.add_instance(s.add_geometry(*quad([[-4, 0, 4], [4, 0, 4], [4, 0, -4], [-4, 0, -4]])), ground)
+    cube = s.add_geometry(*unit_cube())
+    for k in range(6):
+        extent = rng.uniform(0.3, 0.9, 3)
+        centre = (rng.uniform(-2.5, 2.5), extent[1] / 2 + 1e-3, rng.uniform(-2.5, 2.5))
+        mat = s.add_material(preview_material(tuple(rng.uniform(0.2, 0.8, 3)), roughness=rng.uniform(0.1, 0.9),
+                                              metallic=float(k % 2), ior=1.5))
+        s.add_instance(cube, mat, block(extent, rng.uniform(0.0, 180.0), centre))
+    for k in range(count):
+        centre = (rng.uniform(-3.5, 3.5), rng.uniform(0.6, 2.5), rng.uniform(-3.5, 3.5))
+        radiance = tuple(float(v) for v in np.exp(rng.normal(0.5, 1.0, 3)))
+        shape = (abi.LIGHT_SPHERE, abi.LIGHT_RECT, abi.LIGHT_DISK)[k % 3]
+        if shape == abi.LIGHT_SPHERE:
+            s.add_light(shape, affine(translation=centre), radiance=radiance, radius=rng.uniform(0.03, 0.25))
+        elif shape == abi.LIGHT_RECT:
+            s.add_light(shape, affine(linear=FACING_DOWN @ rotation_y(0.0), translation=centre), radiance=radiance,
+                        width=rng.uniform(0.1, 0.6), height=rng.uniform(0.1, 0.6))
+        else:
+            s.add_light(shape, affine(linear=FACING_DOWN, translation=centre), radiance=radiance,
+                        radius=rng.uniform(0.05, 0.3))
+    s.world_to_clip = multiply(perspective(55.0, 1.0, 0.1, 100.0), look_at((0.0, 4.0, 6.5), (0.0, 0.6, 0.0)))
+    s.width = s.height = size
+    return s
+
+
+def lit_plane(shape, size=33, height=1.0, radius=0.25, radiance=(2.0, 2.0, 2.0), albedo=0.5):
+    """A Lambert plane (y = 0, albedo `albedo`, uncoated) under one analytic
+    light centred `height` above the origin, seen from above: at the
+    plane's centre the light's irradiance has a closed form (a sphere:
+    pi L r^2 / h^2; a downward disk: pi L r^2 / (r^2 + h^2)), so the centre
+    pixel's direct radiance is albedo * L * r^2 / h^2 or
+    albedo * L * r^2 / (r^2 + h^2)."""
+    s = Scene(f"lit-plane-{shape}")
+    mat = s.add_material(preview_material((albedo, albedo, albedo), roughness=1.0, ior=1.0))
+    s.add_instance(s.add_geometry(*quad([[-50, 0, 50], [50, 0, 50], [50, 0, -50], [-50, 0, -50]])), mat)
+    if shape == abi.LIGHT_SPHERE:
+        s.add_light(shape, affine(translation=(0.0, height, 0.0)), radiance=radiance, radius=radius)
+    else:
+        s.add_light(shape, affine(linear=FACING_DOWN, translation=(0.0, height, 0.0)), radiance=radiance,
+                    radius=radius)
+    s.world_to_clip = multiply(perspective(20.0, 1.0, 0.1, 100.0),
+                               look_at((0.0, 3.0, 1e-3), (0.0, 0.0, 0.0), up=(0.0, 0.0, -1.0)))
     s.width = s.height = size
     return s

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LOTUS_CUDA_ABI_VERSION 2u
+#define LOTUS_CUDA_ABI_VERSION 3u
 
 /* FrameStatus (vulkan_backend.hpp:23-27). */
 #define LOTUS_PASS 0
@@ -107,6 +107,30 @@ typedef struct lotus_environment {
   float environment_from_world[9];  /* rows: the image frame's unit axes in world space */
 } lotus_environment;
 
+/* LightShape (render_world.hpp:79-84). */
+#define LOTUS_LIGHT_SPHERE 0u
+#define LOTUS_LIGHT_RECT 1u
+#define LOTUS_LIGHT_DISK 2u
+#define LOTUS_LIGHT_DISTANT 3u
+
+/* An analytic light: Lotus::Light (render_world.hpp:86-114). It only emits:
+ * it neither reflects nor blocks light, and camera rays do not see it. A
+ * sphere is centred on its frame's origin, its radius scaled by the cube
+ * root of the frame's absolute determinant; a rect or disk lies in its
+ * frame's XY plane and emits from its -Z side; a distant light shines along
+ * its frame's -Z axis, a parallel light when its angle is 0. */
+typedef struct lotus_light {
+  uint32_t shape;               /* LOTUS_LIGHT_* */
+  uint32_t normalize;           /* UsdLux normalize: radiance over area / size factor */
+  float world_from_light[16];   /* column-major */
+  float radiance[3];            /* linear RGB; a parallel light's irradiance */
+  float radius;                 /* sphere, disk */
+  float width;                  /* rect extent along X */
+  float height;                 /* rect extent along Y */
+  float angle;                  /* distant: angular diameter in degrees */
+  uint32_t reserved;
+} lotus_light;
+
 /* The whole scene. Slot 0 of materials is the default material. */
 typedef struct lotus_scene_desc {
   const lotus_geometry* geometries;
@@ -117,6 +141,8 @@ typedef struct lotus_scene_desc {
   uint32_t instance_count;
   uint32_t material_count;
   float environment_constant[3];  /* the constant environment radiance */
+  const lotus_light* lights;      /* analytic lights (the snapshot's Light list); NULL if none */
+  uint32_t light_count;
 } lotus_scene_desc;
 
 /* GpuSceneEvidence, in part. */

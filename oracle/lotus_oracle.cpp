@@ -21,8 +21,10 @@
 //   sampler hardware uses fixed-point weights.
 // - Accumulation. Samples are summed in FP64 (the precision policy), where
 //   the reference's image is RGBA32F.
-// Analytic lights, textured inputs and the glTF closure are not in the
-// restated path (no workload uses them).
+// Analytic lights (sphere, rect, disk, distant and parallel; their table
+// entries, crossing hierarchy, sampling and crossing tests) are restated from
+// gpu_scene.cpp:272-610 and scene.slang:680-1178. Textured inputs and the
+// glTF closure are not in the restated path (no workload uses them).
 
 #include "lotus_oracle.h"
 
@@ -48,6 +50,14 @@ constexpr float kPi = 3.14159265358979323846f;
 constexpr float kFloatMax = 3.402823466e+38f;
 constexpr uint32_t kNoLights = 0xFFFFFFFFu;
 constexpr uint32_t kEnvironmentLight = 0xFFFFFFFFu;
+// gpu_scene.hpp:128-172: an analytic light's table entry, its shapes, and
+// the crossing hierarchy's child encoding.
+constexpr uint32_t kAnalyticLight = 0x80000000u;
+constexpr uint32_t kSphereLight = 0, kRectLight = 1, kDiskLight = 2, kDistantLight = 3,
+                   kParallelLight = 4;
+constexpr uint32_t kLightLeaf = 0x80000000u;
+constexpr uint32_t kNoLightChild = 0xFFFFFFFFu;
+constexpr uint32_t kLightStackSize = 32;
 constexpr uint32_t kRouletteBounces = 3;  // transport.slang:21
 constexpr float kMaxSurvival = 0.95f;     // transport.slang:22
 constexpr float kMinAlpha = 1.0e-3f;      // preview.slang:17
@@ -670,6 +680,22 @@ struct LightRecord {
   uint32_t instance;
 };
 
+// GpuAnalyticLightRecord (gpu_scene.hpp:144-166).
+struct AnalyticLight {
+  float position[4];
+  float axis_u[4];
+  float axis_v[4];
+  float normal[4];
+  float radiance[4];
+  uint32_t shape;
+};
+
+// GpuLightNode (gpu_scene.hpp:174-186): per child its bounds, the child's
+// bits in low.w.
+struct LightNode {
+  float low0[4], high0[4], low1[4], high1[4];
+};
+
 struct Environment {
   bool bound = false;
   uint32_t width = 0, height = 0;
@@ -690,6 +716,10 @@ struct oracle_scene {
   Bvh tlas;
   std::vector<LightRecord> lights;
   std::vector<uint32_t> light_offsets;
+  std::vector<lotus_light> light_inputs;
+  std::vector<AnalyticLight> analytic;
+  std::vector<LightNode> light_nodes;
+  std::vector<uint32_t> distant;
   float environment_selection = 0.0f;
   F3 environment_constant{0, 0, 0};
   Environment env;
@@ -873,8 +903,177 @@ void BuildEnvironmentDistribution(Environment& env) {
   env.bound = env.mean > 0.0;
 }
 
-// BuildLightTable (gpu_scene.cpp:515-610), emissive triangles and the
-// environment image; no analytic lights.
+struct D3 {
+  double x, y, z;
+};
+inline D3 Column(const float* m, int c) { return D3{m[4 * c], m[4 * c + 1], m[4 * c + 2]}; }
+inline double Dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline D3 Cross(D3 a, D3 b) {
+  return D3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline D3 Scale(D3 a, double s) { return D3{a.x * s, a.y * s, a.z * s}; }
+inline void Store(float* out, D3 v, double w) {
+  out[0] = static_cast<float>(v.x);
+  out[1] = static_cast<float>(v.y);
+  out[2] = static_cast<float>(v.z);
+  out[3] = static_cast<float>(w);
+}
+
+// MakeAnalyticLight (gpu_scene.cpp:272-369): the record and its table
+// weight, the estimated power over 2 pi (a distant light's through a disk
+// of the scene's radius). False for a light that emits nothing.
+bool MakeAnalyticLight(const lotus_light& light, double scene_radius, double& weight, AnalyticLight& record) {
+  constexpr double kPiD = 3.14159265358979323846;
+  const float* m = light.world_from_light;
+  const D3 x = Column(m, 0), y = Column(m, 1), z = Column(m, 2), origin = Column(m, 3);
+  const double determinant = Dot(x, Cross(y, z));
+  record = AnalyticLight{};
+  double extent = 0.0, scale = 1.0;
+  if (light.shape == LOTUS_LIGHT_SPHERE) {
+    const double radius = light.radius * std::cbrt(std::fabs(determinant));
+    extent = 4.0 * kPiD * radius * radius;
+    record.shape = kSphereLight;
+    Store(record.position, origin, radius);
+    Store(record.normal, D3{0, 0, 0}, extent);
+  } else if (light.shape == LOTUS_LIGHT_RECT || light.shape == LOTUS_LIGHT_DISK) {
+    const bool rect = light.shape == LOTUS_LIGHT_RECT;
+    const D3 u = Scale(x, rect ? 0.5 * light.width : light.radius);
+    const D3 v = Scale(y, rect ? 0.5 * light.height : light.radius);
+    const D3 normal = Cross(u, v);
+    const double length = std::sqrt(Dot(normal, normal));
+    extent = (rect ? 4.0 : kPiD) * length;
+    record.shape = rect ? kRectLight : kDiskLight;
+    Store(record.position, origin, 0.0);
+    Store(record.axis_u, u, 0.0);
+    Store(record.axis_v, v, 0.0);
+    if (length > 0.0) Store(record.normal, Scale(normal, (determinant < 0.0 ? 1.0 : -1.0) / length), extent);
+  } else {
+    const double length = std::sqrt(Dot(z, z));
+    if (!(length > 0.0)) return false;
+    const double theta = std::min(static_cast<double>(light.angle) * kPiD / 360.0, kPiD);
+    const double half = std::sin(0.5 * theta);
+    const double one_minus_cos = 2.0 * half * half;
+    const double sin2 = std::sin(theta) * std::sin(theta);
+    Store(record.axis_u, Scale(z, 1.0 / length), one_minus_cos);
+    record.shape = kParallelLight;
+    extent = 1.0;
+    if (theta > 0.0) {
+      extent = theta <= 0.5 * kPiD ? kPiD * sin2 : kPiD;
+      if (light.normalize) scale = 1.0 / (theta <= 0.5 * kPiD ? kPiD * sin2 : (2.0 - sin2) * kPiD);
+      if (static_cast<float>(one_minus_cos) >= std::numeric_limits<float>::min()) {
+        record.shape = kDistantLight;
+      } else {
+        scale *= extent;
+        extent = 1.0;
+      }
+    }
+  }
+  if (light.normalize && light.shape != LOTUS_LIGHT_DISTANT) scale = 1.0 / extent;
+  double radiance[3];
+  for (int c = 0; c < 3; ++c) radiance[c] = light.radiance[c] * scale;
+  const double mean = (radiance[0] + radiance[1] + radiance[2]) / 3.0;
+  if (!(extent > 0.0) || !std::isfinite(extent) || !(mean > 0.0) ||
+      !(radiance[0] <= std::numeric_limits<float>::max() && radiance[1] <= std::numeric_limits<float>::max() &&
+          radiance[2] <= std::numeric_limits<float>::max()))
+    return false;
+  Store(record.radiance, D3{radiance[0], radiance[1], radiance[2]}, 0.0);
+  weight = mean * extent / 2.0;
+  if (light.shape == LOTUS_LIGHT_DISTANT) weight *= scene_radius * scene_radius;
+  if (!std::isfinite(weight)) weight = std::numeric_limits<double>::max();
+  return true;
+}
+
+// A bounded light's box (BoundLight, gpu_scene.cpp:398-428): its extent
+// widened by 1e-4 of itself plus 1e-5 of the coordinates' magnitude, then
+// rounded outwards.
+struct LightBounds {
+  float low[3], high[3];
+  double centre[3];
+  uint32_t index;
+};
+
+LightBounds BoundLight(const AnalyticLight& light, uint32_t index) {
+  LightBounds b;
+  b.index = index;
+  for (int a = 0; a < 3; ++a) {
+    const double centre = light.position[a];
+    const double u = light.axis_u[a], v = light.axis_v[a];
+    const double extent = light.shape == kSphereLight ? light.position[3]
+        : light.shape == kRectLight                   ? std::fabs(u) + std::fabs(v)
+                                                      : std::sqrt(u * u + v * v);
+    const double margin = 1e-4 * extent + 1e-5 * (std::fabs(centre) + extent);
+    b.centre[a] = centre;
+    b.low[a] = std::nextafter(static_cast<float>(centre - extent - margin), -std::numeric_limits<float>::infinity());
+    b.high[a] = std::nextafter(static_cast<float>(centre + extent + margin), std::numeric_limits<float>::infinity());
+  }
+  return b;
+}
+
+void StoreBounds(float* low, float* high, const LightBounds* first, const LightBounds* last, uint32_t child) {
+  for (int a = 0; a < 3; ++a) {
+    low[a] = std::numeric_limits<float>::max();
+    high[a] = -std::numeric_limits<float>::max();
+    for (const LightBounds* it = first; it != last; ++it) {
+      low[a] = std::min(low[a], it->low[a]);
+      high[a] = std::max(high[a], it->high[a]);
+    }
+  }
+  std::memcpy(&low[3], &child, 4);
+}
+
+// BuildLightNode (gpu_scene.cpp:438-476): a leaf for one light, else a node
+// split at the median centre (ties by index) along the axis of widest
+// centre spread; nodes numbered in preorder.
+uint32_t BuildLightNode(LightBounds* first, LightBounds* last, std::vector<LightNode>& nodes) {
+  if (last - first == 1) return kLightLeaf | first->index;
+  const uint32_t node = static_cast<uint32_t>(nodes.size());
+  nodes.emplace_back();
+  double low[3], high[3];
+  for (int a = 0; a < 3; ++a) low[a] = high[a] = first->centre[a];
+  for (const LightBounds* it = first; it != last; ++it)
+    for (int a = 0; a < 3; ++a) {
+      low[a] = std::min(low[a], it->centre[a]);
+      high[a] = std::max(high[a], it->centre[a]);
+    }
+  int axis = 0;
+  for (int c = 1; c < 3; ++c)
+    if (high[c] - low[c] > high[axis] - low[axis]) axis = c;
+  LightBounds* middle = first + (last - first) / 2;
+  std::nth_element(first, middle, last, [axis](const LightBounds& a, const LightBounds& b) {
+    return a.centre[axis] != b.centre[axis] ? a.centre[axis] < b.centre[axis] : a.index < b.index;
+  });
+  const uint32_t left = BuildLightNode(first, middle, nodes);
+  const uint32_t right = BuildLightNode(middle, last, nodes);
+  LightNode& stored = nodes[node];
+  StoreBounds(stored.low0, stored.high0, first, middle, left);
+  StoreBounds(stored.low1, stored.high1, middle, last, right);
+  return node;
+}
+
+// BuildLightHierarchy (gpu_scene.cpp:478-499).
+void BuildLightHierarchy(oracle_scene& s) {
+  s.light_nodes.clear();
+  s.distant.clear();
+  std::vector<LightBounds> bounded;
+  for (size_t i = 0; i < s.analytic.size(); ++i) {
+    const uint32_t shape = s.analytic[i].shape;
+    if (shape == kDistantLight)
+      s.distant.push_back(static_cast<uint32_t>(i));
+    else if (shape != kParallelLight)
+      bounded.push_back(BoundLight(s.analytic[i], static_cast<uint32_t>(i)));
+  }
+  if (bounded.size() == 1) {
+    LightNode root;
+    StoreBounds(root.low0, root.high0, bounded.data(), bounded.data() + 1, kLightLeaf | bounded[0].index);
+    StoreBounds(root.low1, root.high1, nullptr, nullptr, kNoLightChild);
+    s.light_nodes.push_back(root);
+  } else if (bounded.size() > 1) {
+    BuildLightNode(bounded.data(), bounded.data() + bounded.size(), s.light_nodes);
+  }
+}
+
+// BuildLightTable (gpu_scene.cpp:515-610): emissive triangles, analytic
+// lights, then the environment image.
 void BuildLightTable(oracle_scene& s) {
   s.light_offsets.assign(s.instances.size(), kNoLights);
   s.lights.clear();
@@ -892,8 +1091,23 @@ void BuildLightTable(oracle_scene& s) {
     }
   }
   const double environment_mean = s.env.mean;
-  const bool distant = environment_mean > 0.0;
+  bool distant = environment_mean > 0.0;
+  for (const lotus_light& l : s.light_inputs) distant = distant || l.shape == LOTUS_LIGHT_DISTANT;
   const double scene_radius = distant ? SceneRadius(s) : 0.0;
+  s.analytic.clear();
+  std::vector<uint32_t> analytic_entries;
+  for (const lotus_light& l : s.light_inputs) {
+    double weight = 0.0;
+    AnalyticLight record;
+    if (!MakeAnalyticLight(l, scene_radius, weight, record)) continue;
+    if (weight > 0.0) {
+      analytic_entries.push_back(static_cast<uint32_t>(s.lights.size()));
+      weights.push_back(weight);
+      s.lights.push_back({0.0f, 1.0f, 0, kAnalyticLight | static_cast<uint32_t>(s.analytic.size())});
+    }
+    s.analytic.push_back(record);
+  }
+  BuildLightHierarchy(s);
   double environment_weight = 0.0;
   if (environment_mean > 0.0) {
     constexpr double kPiD = 3.14159265358979323846;
@@ -935,6 +1149,8 @@ void BuildLightTable(oracle_scene& s) {
   }
   for (uint32_t i : small) { s.lights[i].threshold = 1.0f; s.lights[i].alias = i; }
   for (uint32_t i : large) { s.lights[i].threshold = 1.0f; s.lights[i].alias = i; }
+  for (uint32_t entry : analytic_entries)
+    s.analytic[s.lights[entry].instance & ~kAnalyticLight].radiance[3] = s.lights[entry].pdf;
   if (environment_weight > 0.0) s.environment_selection = s.lights.back().pdf;
 }
 
@@ -1414,6 +1630,228 @@ F3 EnvironmentRadiance(const oracle_scene& s, F3 direction, bool weigh, float pd
   return radiance * PowerHeuristic(pdf, s.environment_selection * EnvironmentDirectionPdf(s, u, v));
 }
 
+// SampleConcentricDisk (sampling.slang:89-104).
+inline void SampleConcentricDisk(float ux, float uy, float& a, float& b) {
+  const float ox = 2.0f * ux - 1.0f, oy = 2.0f * uy - 1.0f;
+  if (ox == 0.0f && oy == 0.0f) {
+    a = b = 0.0f;
+    return;
+  }
+  float radius, theta;
+  if (std::fabs(ox) > std::fabs(oy)) {
+    radius = ox;
+    theta = 0.25f * kPi * (oy / ox);
+  } else {
+    radius = oy;
+    theta = 0.5f * kPi - 0.25f * kPi * (ox / oy);
+  }
+  float sn, cs;
+  lsincos(theta, sn, cs);
+  a = radius * cs;
+  b = radius * sn;
+}
+
+// SampleUniformCone (sampling.slang:109-116).
+inline F3 SampleUniformCone(float ux, float uy, float one_minus_cos_max) {
+  const float one_minus_cos = ux * one_minus_cos_max;
+  const float sin_theta = std::sqrt(std::fmax(0.0f, one_minus_cos * (2.0f - one_minus_cos)));
+  const float phi = 2.0f * kPi * uy;
+  float sn, cs;
+  lsincos(phi, sn, cs);
+  return V(sin_theta * cs, sin_theta * sn, 1.0f - one_minus_cos);
+}
+
+inline F3 Xyz4(const float* v) { return V(v[0], v[1], v[2]); }
+
+// SphereConePdf (scene.slang:683-690).
+inline float SphereConePdf(float sin2_max) {
+  const float one_minus_cos = sin2_max < 0.00068523f ? 0.5f * sin2_max
+                                                     : 1.0f - std::sqrt(std::fmax(0.0f, 1.0f - sin2_max));
+  return 1.0f / (2.0f * kPi * one_minus_cos);
+}
+
+// SampleAnalytic (scene.slang:695-768).
+LightSample SampleAnalytic(const AnalyticLight& light, float selection, float ux, float uy, F3 origin) {
+  LightSample ls = NoLight();
+  ls.radiance = Xyz4(light.radiance);
+  if (light.shape == kSphereLight) {
+    const F3 centre = Xyz4(light.position);
+    const float radius = light.position[3];
+    const F3 to_centre = centre - origin;
+    const float distance2 = dot(to_centre, to_centre);
+    if (!(distance2 > radius * radius)) return NoLight();
+    const float sin2_max = radius * radius / distance2;
+    const float sin_max = std::sqrt(sin2_max);
+    const float cos_max = std::sqrt(std::fmax(0.0f, 1.0f - sin2_max));
+    float cos_theta = (cos_max - 1.0f) * ux + 1.0f;
+    float sin2_theta = 1.0f - cos_theta * cos_theta;
+    if (sin2_max < 0.00068523f) {
+      sin2_theta = sin2_max * ux;
+      cos_theta = std::sqrt(1.0f - sin2_theta);
+    }
+    const float cos_alpha = sin2_theta / sin_max +
+        cos_theta * std::sqrt(std::fmax(0.0f, 1.0f - sin2_theta / sin2_max));
+    const float sin_alpha = std::sqrt(std::fmax(0.0f, 1.0f - cos_alpha * cos_alpha));
+    const float phi = 2.0f * kPi * uy;
+    float sn, cs;
+    lsincos(phi, sn, cs);
+    const ShadingFrame frame = MakeShadingFrame(normalize(to_centre));
+    const F3 outward = frame.ToWorld(-V(sin_alpha * cs, sin_alpha * sn, cos_alpha));
+    const F3 toward = centre + radius * outward - origin;
+    ls.distance = length(toward);
+    ls.direction = toward / ls.distance;
+    ls.pdf = selection * SphereConePdf(sin2_max);
+  } else if (light.shape == kRectLight || light.shape == kDiskLight) {
+    float a, b;
+    if (light.shape == kRectLight) {
+      a = 2.0f * ux - 1.0f;
+      b = 2.0f * uy - 1.0f;
+    } else {
+      SampleConcentricDisk(ux, uy, a, b);
+    }
+    const F3 toward = Xyz4(light.position) + a * Xyz4(light.axis_u) + b * Xyz4(light.axis_v) - origin;
+    const float distance2 = dot(toward, toward);
+    if (!(distance2 > 0.0f)) return NoLight();
+    ls.distance = std::sqrt(distance2);
+    ls.direction = toward / ls.distance;
+    const float cosine = -dot(Xyz4(light.normal), ls.direction);
+    if (!(cosine > 0.0f)) return NoLight();
+    ls.pdf = selection * distance2 / (cosine * light.normal[3]);
+  } else if (light.shape == kDistantLight) {
+    const ShadingFrame frame = MakeShadingFrame(Xyz4(light.axis_u));
+    ls.direction = normalize(frame.ToWorld(SampleUniformCone(ux, uy, light.axis_u[3])));
+    ls.distance = kFloatMax;
+    ls.pdf = selection / (2.0f * kPi * light.axis_u[3]);
+  } else {
+    ls.direction = Xyz4(light.axis_u);
+    ls.distance = kFloatMax;
+    ls.pdf = selection;
+    ls.delta = true;
+  }
+  return ls;
+}
+
+// ParallelLight (scene.slang:986-1000).
+LightSample ParallelLight(const oracle_scene& s, uint32_t index) {
+  const AnalyticLight& light = s.analytic[index];
+  if (light.shape != kParallelLight) return NoLight();
+  LightSample ls;
+  ls.direction = Xyz4(light.axis_u);
+  ls.distance = kFloatMax;
+  ls.radiance = Xyz4(light.radiance);
+  ls.pdf = 1.0f;
+  ls.delta = true;
+  return ls;
+}
+
+// CrossedLight (scene.slang:1019-1091).
+F3 CrossedLight(const oracle_scene& s, uint32_t index, F3 origin, F3 direction, float distance, bool escaped,
+    bool weigh, float pdf) {
+  const AnalyticLight& light = s.analytic[index];
+  float light_pdf = 0.0f;
+  if (light.shape == kSphereLight) {
+    const float radius = light.position[3];
+    const F3 offset = origin - Xyz4(light.position);
+    const float c = dot(offset, offset) - radius * radius;
+    const float b = -dot(offset, direction);
+    const F3 perpendicular = offset + b * direction;
+    const float discriminant = radius * radius - dot(perpendicular, perpendicular);
+    if (!(c > 0.0f) || !(b > 0.0f) || discriminant < 0.0f) return V(0.0f);
+    const float t = c / (b + std::sqrt(discriminant));
+    if (!(t < distance)) return V(0.0f);
+    light_pdf = SphereConePdf(radius * radius / dot(offset, offset));
+  } else if (light.shape == kRectLight || light.shape == kDiskLight) {
+    const F3 n = Xyz4(light.normal);
+    const float facing = dot(direction, n);
+    if (!(facing < 0.0f)) return V(0.0f);
+    const float t = dot(Xyz4(light.position) - origin, n) / facing;
+    if (!(t > 0.0f) || !(t < distance)) return V(0.0f);
+    const F3 q = origin + t * direction - Xyz4(light.position);
+    const F3 u = Xyz4(light.axis_u), v = Xyz4(light.axis_v);
+    const float uu = dot(u, u), uv = dot(u, v), vv = dot(v, v);
+    const float qu = dot(q, u), qv = dot(q, v);
+    const float determinant = uu * vv - uv * uv;
+    const float a = (qu * vv - qv * uv) / determinant;
+    const float b = (qv * uu - qu * uv) / determinant;
+    if (light.shape == kRectLight ? !(std::fabs(a) <= 1.0f && std::fabs(b) <= 1.0f) : !(a * a + b * b <= 1.0f))
+      return V(0.0f);
+    light_pdf = t * t / (-facing * light.normal[3]);
+  } else if (light.shape == kDistantLight && escaped) {
+    const F3 toward = Xyz4(light.axis_u);
+    const float one_minus_cos = light.axis_u[3];
+    const float cosine = dot(direction, toward);
+    if (one_minus_cos <= 1.0f) {
+      const F3 across = cross(direction, toward);
+      if (!(cosine > 0.0f) || !(dot(across, across) <= one_minus_cos * (2.0f - one_minus_cos))) return V(0.0f);
+    } else if (!(cosine >= 1.0f - one_minus_cos)) {
+      return V(0.0f);
+    }
+    light_pdf = 1.0f / (2.0f * kPi * one_minus_cos);
+  } else {
+    return V(0.0f);
+  }
+  const float weight = weigh ? PowerHeuristic(pdf, light.radiance[3] * light_pdf) : 1.0f;
+  return Xyz4(light.radiance) * weight;
+}
+
+// OverlapsBox (scene.slang:1095-1103).
+inline bool OverlapsBox(const float* low, const float* high, F3 origin, F3 inverse, float distance) {
+  const float t0x = (low[0] - origin.x) * inverse.x, t1x = (high[0] - origin.x) * inverse.x;
+  const float t0y = (low[1] - origin.y) * inverse.y, t1y = (high[1] - origin.y) * inverse.y;
+  const float t0z = (low[2] - origin.z) * inverse.z, t1z = (high[2] - origin.z) * inverse.z;
+  const float nx = std::fmin(t0x, t1x), ny = std::fmin(t0y, t1y), nz = std::fmin(t0z, t1z);
+  const float fx = std::fmax(t0x, t1x), fy = std::fmax(t0y, t1y), fz = std::fmax(t0z, t1z);
+  return std::fmax(std::fmax(nx, ny), std::fmax(nz, 0.0f)) <= std::fmin(std::fmin(fx, fy), std::fmin(fz, distance));
+}
+
+inline float SafeInverse(float d) {
+  return 1.0f / (std::fabs(d) > 1e-30f ? d : (d < 0.0f ? -1e-30f : 1e-30f));
+}
+
+// CrossedLights (scene.slang:1110-1178): the crossing hierarchy's leaves in
+// its traversal order, then, for an escaping ray, the distant lights.
+F3 CrossedLights(const oracle_scene& s, F3 origin, F3 direction, float distance, bool escaped, bool weigh,
+    float pdf) {
+  F3 sum = V(0.0f);
+  if (!s.light_nodes.empty()) {
+    const F3 inverse = V(SafeInverse(direction.x), SafeInverse(direction.y), SafeInverse(direction.z));
+    uint32_t stack[kLightStackSize];
+    uint32_t depth = 0, node = 0;
+    while (true) {
+      const LightNode& current = s.light_nodes[node];
+      const uint32_t child0 = AsUint(current.low0[3]);
+      const uint32_t child1 = AsUint(current.low1[3]);
+      const bool enter0 = OverlapsBox(current.low0, current.high0, origin, inverse, distance);
+      const bool enter1 =
+          child1 != kNoLightChild && OverlapsBox(current.low1, current.high1, origin, inverse, distance);
+      uint32_t next = 0xFFFFFFFFu;
+      if (enter0) {
+        if ((child0 & kLightLeaf) != 0)
+          sum = sum + CrossedLight(s, child0 & ~kLightLeaf, origin, direction, distance, escaped, weigh, pdf);
+        else
+          next = child0;
+      }
+      if (enter1) {
+        if ((child1 & kLightLeaf) != 0)
+          sum = sum + CrossedLight(s, child1 & ~kLightLeaf, origin, direction, distance, escaped, weigh, pdf);
+        else if (next == 0xFFFFFFFFu)
+          next = child1;
+        else
+          stack[depth++] = child1;
+      }
+      if (next == 0xFFFFFFFFu) {
+        if (depth == 0) break;
+        next = stack[--depth];
+      }
+      node = next;
+    }
+  }
+  if (escaped)
+    for (uint32_t index : s.distant)
+      sum = sum + CrossedLight(s, index, origin, direction, distance, escaped, weigh, pdf);
+  return sum;
+}
+
 // SampleLight (scene.slang:894-909).
 LightSample SampleLight(const oracle_scene& s, const float* u, F3 origin) {
   const uint32_t count = static_cast<uint32_t>(s.lights.size());
@@ -1422,6 +1860,8 @@ LightSample SampleLight(const oracle_scene& s, const float* u, F3 origin) {
   const uint32_t light = u[1] < record.threshold ? column : record.alias;
   const LightRecord& chosen = s.lights[light];
   if (chosen.instance == kEnvironmentLight) return SampleEnvironment(s, chosen.pdf, u[2], u[3]);
+  if ((chosen.instance & kAnalyticLight) != 0)
+    return SampleAnalytic(s.analytic[chosen.instance & ~kAnalyticLight], chosen.pdf, u[2], u[3], origin);
   return SampleTriangle(s, light, chosen, u[2], u[3], origin);
 }
 
@@ -1555,12 +1995,45 @@ struct RestirRecord {
 static_assert(sizeof(RestirRecord) == 48, "RestirPixel is 48 bytes");
 constexpr uint32_t kNoReservoirSample = 0xFFFFFFFFu;
 
-// ReconstructReservoirLight (scene.slang:939-967) for emissive triangles and
-// the environment.
+// ReconstructReservoirLight (scene.slang:939-967): a sphere light's
+// candidates are points uniform over its whole area.
 LightSample ReconstructReservoirLight(const oracle_scene& s, uint32_t index, float ux, float uy, F3 origin) {
   const LightRecord& chosen = s.lights[index];
   if (chosen.instance == kEnvironmentLight) return SampleEnvironment(s, chosen.pdf, ux, uy);
-  return SampleTriangle(s, index, chosen, ux, uy, origin);
+  if ((chosen.instance & kAnalyticLight) == 0) return SampleTriangle(s, index, chosen, ux, uy, origin);
+  const AnalyticLight& light = s.analytic[chosen.instance & ~kAnalyticLight];
+  if (light.shape != kSphereLight) return SampleAnalytic(light, chosen.pdf, ux, uy, origin);
+  const float z = 1.0f - 2.0f * ux;
+  const float radius_xy = std::sqrt(std::fmax(0.0f, 1.0f - z * z));
+  const float phi = 2.0f * kPi * uy;
+  float sn, cs;
+  lsincos(phi, sn, cs);
+  const F3 normal = V(radius_xy * cs, radius_xy * sn, z);
+  const F3 toward = Xyz4(light.position) + light.position[3] * normal - origin;
+  const float distance2 = dot(toward, toward);
+  if (!(distance2 > 0.0f)) return NoLight();
+  LightSample ls = NoLight();
+  ls.distance = std::sqrt(distance2);
+  ls.direction = toward / ls.distance;
+  const float cosine = -dot(normal, ls.direction);
+  if (!(cosine > 0.0f)) return NoLight();
+  ls.radiance = Xyz4(light.radiance);
+  ls.pdf = chosen.pdf * distance2 / (cosine * 4.0f * kPi * light.position[3] * light.position[3]);
+  return ls;
+}
+
+// ReservoirPartitionPdf (scene.slang:973-983): a sphere light's reservoir
+// sample weighed at the cone density SampleLight would have used.
+float ReservoirPartitionPdf(const oracle_scene& s, uint32_t index, const LightSample& ls, F3 origin) {
+  const LightRecord& chosen = s.lights[index];
+  if ((chosen.instance & kAnalyticLight) != 0 && chosen.instance != kEnvironmentLight) {
+    const AnalyticLight& light = s.analytic[chosen.instance & ~kAnalyticLight];
+    if (light.shape == kSphereLight) {
+      const F3 offset = Xyz4(light.position) - origin;
+      return chosen.pdf * SphereConePdf(light.position[3] * light.position[3] / dot(offset, offset));
+    }
+  }
+  return ls.pdf;
 }
 
 // InitialDirectLight (restir.slang:235-254).
@@ -1573,7 +2046,9 @@ F3 InitialDirectLight(const oracle_scene& s, const FrameConstants& f, uint32_t p
   const F3 origin = OffsetRayOrigin(sh.position, sh.normal);
   const LightSample ls = ReconstructReservoirLight(s, sel.reservoir.sample, sel.uv[0], sel.uv[1], origin);
   const F3 wi = basis.ToLocal(ls.direction);
-  const float weight = ls.delta ? 1.0f : PowerHeuristic(ls.pdf, wi.z > 0.0f ? PreviewPdf(sh.bsdf, wo, wi) : 0.0f);
+  const float weight = ls.delta ? 1.0f
+      : PowerHeuristic(ReservoirPartitionPdf(s, sel.reservoir.sample, ls, origin),
+            wi.z > 0.0f ? PreviewPdf(sh.bsdf, wo, wi) : 0.0f);
   return V(sel.contribution[0], sel.contribution[1], sel.contribution[2]) * weight;
 }
 
@@ -1586,7 +2061,18 @@ float EmissionWeight(const oracle_scene& s, const PathState& p, const Hit& hit, 
   return PowerHeuristic(p.last_pdf, area_pdf * dot(toward, toward) / cosine);
 }
 
-// ScatterPath (transport.slang:164-230), without ReSTIR or analytic lights.
+// ParallelLights (transport.slang:139-146): under BSDF sampling, each
+// parallel light through its own shadow ray.
+F3 ParallelLights(const oracle_scene& s, const SurfaceHit& sh, const ShadingFrame& basis, F3 wo,
+    RayCounts& rays) {
+  const F3 origin = OffsetRayOrigin(sh.position, sh.normal);
+  F3 sum = V(0.0f);
+  for (uint32_t index = 0; index < s.analytic.size(); ++index)
+    sum = sum + ShadowedLight(s, sh, basis, wo, origin, ParallelLight(s, index), rays);
+  return sum;
+}
+
+// ScatterPath (transport.slang:164-230).
 bool ScatterPath(const oracle_scene& s, const FrameConstants& f, PathState& p, const Hit& hit,
     RayCounts& rays) {
   const SurfaceHit sh = ReconstructHit(s, hit, p.ray.direction);
@@ -1594,6 +2080,9 @@ bool ScatterPath(const oracle_scene& s, const FrameConstants& f, PathState& p, c
   if (WeighFoundLight(f, p) && p.depth != 0 && MaxComponent(emission) > 0.0f)
     emission = emission * EmissionWeight(s, p, hit, sh);
   p.radiance = p.radiance + p.throughput * emission;
+  if (p.depth != 0 && !s.analytic.empty())
+    p.radiance = p.radiance + p.throughput * CrossedLights(s, p.ray.origin, p.ray.direction,
+        dot(sh.position - p.ray.origin, p.ray.direction), false, WeighFoundLight(f, p), p.last_pdf);
   if (p.depth >= f.max_bounces) return false;
   if (p.depth >= kRouletteBounces) {
     const float survival = std::fmin(MaxComponent(p.throughput), kMaxSurvival);
@@ -1606,6 +2095,8 @@ bool ScatterPath(const oracle_scene& s, const FrameConstants& f, PathState& p, c
     p.radiance = p.radiance + p.throughput * InitialDirectLight(s, f, p.pixel_index, sh, basis, wo);
   else if (f.sample_lights)
     p.radiance = p.radiance + p.throughput * DirectLight(s, sh, basis, wo, p.rng, rays);
+  else if (!s.analytic.empty())
+    p.radiance = p.radiance + p.throughput * ParallelLights(s, sh, basis, wo, rays);
   F3 u;
   u.x = NextRandom(p.rng);
   u.y = NextRandom(p.rng);
@@ -1629,12 +2120,15 @@ bool ScatterPath(const oracle_scene& s, const FrameConstants& f, PathState& p, c
   return true;
 }
 
-// MissPath (transport.slang:235-247), without analytic lights.
+// MissPath (transport.slang:235-247).
 void MissPath(const oracle_scene& s, const FrameConstants& f, PathState& p) {
   F3 environment = s.environment_constant;
   if (s.env.bound)
     environment = environment + EnvironmentRadiance(s, p.ray.direction, WeighFoundLight(f, p), p.last_pdf);
   p.radiance = p.radiance + p.throughput * environment;
+  if (!s.analytic.empty())
+    p.radiance = p.radiance + p.throughput * CrossedLights(s, p.ray.origin, p.ray.direction, kFloatMax, true,
+        WeighFoundLight(f, p), p.last_pdf);
 }
 
 // TracePath and the radiance pass's sample (path_trace.slang:279-287,
@@ -1844,6 +2338,24 @@ oracle_scene* oracle_scene_create(const lotus_scene_desc* d, char* error, size_t
       s->env.rows[r] = V(e.environment_from_world[3 * r], e.environment_from_world[3 * r + 1],
           e.environment_from_world[3 * r + 2]);
     BuildEnvironmentDistribution(s->env);
+  }
+  if (d->light_count) {
+    if (!d->lights) {
+      SetError(error, error_size, "light_count without lights");
+      return nullptr;
+    }
+    s->light_inputs.assign(d->lights, d->lights + d->light_count);
+    for (const lotus_light& l : s->light_inputs) {
+      bool finite = true;
+      for (float v : l.world_from_light) finite = finite && std::isfinite(v);
+      for (float v : l.radiance) finite = finite && std::isfinite(v);
+      finite = finite && std::isfinite(l.radius) && std::isfinite(l.width) && std::isfinite(l.height) &&
+          std::isfinite(l.angle);
+      if (l.shape > LOTUS_LIGHT_DISTANT || !finite) {
+        SetError(error, error_size, "an analytic light has an unknown shape or non-finite values");
+        return nullptr;
+      }
+    }
   }
   BuildLightTable(*s);
   return s.release();

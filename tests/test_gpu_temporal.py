@@ -23,8 +23,18 @@ VARIANCE_ATOL = 9.3e-5
 VARIANCE_RTOL = 1e-6
 
 
-def temporal_frames(integrator, spatial=True, frames=3, filter_iterations=5, cap=5):
-    scene = scenes.restir_room(seed=0, size=SIZE, emitters=300)
+def restir_room_lit():
+    """The ReSTIR room with analytic lights besides its emissive triangles:
+    a sphere, a small sphere, a rect, a disk, a distant and a parallel light
+    (each a reservoir candidate; spheres by their whole area)."""
+    s = scenes.restir_room(seed=0, size=SIZE, emitters=120)
+    for light in scenes.lit_room(seed=0, size=SIZE).lights:
+        s.lights.append(light)
+    return s
+
+
+def temporal_frames(integrator, spatial=True, frames=3, filter_iterations=5, cap=5, lit=False):
+    scene = restir_room_lit() if lit else scenes.restir_room(seed=0, size=SIZE, emitters=300)
     settings = abi.default_settings(integrator=integrator,
                                     light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL,
                                     max_bounces=4, sample_index=100, restir_candidates=8,
@@ -52,9 +62,10 @@ def exact(a, b):
     return np.array_equal(np.frombuffer(a.tobytes(), np.uint8), np.frombuffer(b.tobytes(), np.uint8))
 
 
-@pytest.mark.parametrize("integrator", [abi.INTEGRATOR_WAVEFRONT, abi.INTEGRATOR_REFERENCE])
-def test_temporal_passes_match_checkers(cuda, integrator):
-    scene, descs = temporal_frames(integrator)
+@pytest.mark.parametrize("integrator,lit", [(abi.INTEGRATOR_WAVEFRONT, False), (abi.INTEGRATOR_REFERENCE, False),
+                                             (abi.INTEGRATOR_WAVEFRONT, True)])
+def test_temporal_passes_match_checkers(cuda, integrator, lit):
+    scene, descs = temporal_frames(integrator, lit=lit)
     o = oracle.OracleTemporalScene(scene)
     with cuda.CudaOffscreenRenderer(0) as r:
         cuda.check(r.update_scene(scene), "update_scene")
