@@ -120,7 +120,7 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
     environment_ = u.environment;
     environment_map_ = u.environment_map;
   }
-  if (u.lights_changed && !u.lights.empty()) return fail("analytic lights are not built in the CUDA backend");
+  if (u.lights_changed) lights_ = u.lights;
 
   // The scene description, rebuilt whole.
   std::vector<lotus_geometry> geos(geometries_.size());
@@ -193,7 +193,26 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
     for (int r = 0; r < 3; ++r)
       for (int c = 0; c < 3; ++c) env.environment_from_world[3 * r + c] = w[4 * r + c];
   }
+  // The analytic lights (render_world.hpp:79-114), field for field.
+  std::vector<lotus_light> lights(lights_.size());
+  for (size_t i = 0; i < lights_.size(); ++i) {
+    const Lotus::Light& l = lights_[i];
+    lotus_light& d = lights[i];
+    d.shape = l.shape == Lotus::LightShape::Sphere ? LOTUS_LIGHT_SPHERE
+              : l.shape == Lotus::LightShape::Rect ? LOTUS_LIGHT_RECT
+              : l.shape == Lotus::LightShape::Disk ? LOTUS_LIGHT_DISK
+                                                   : LOTUS_LIGHT_DISTANT;
+    d.normalize = l.normalize ? 1u : 0u;
+    std::memcpy(d.world_from_light, l.world_from_light.data(), 64);
+    std::memcpy(d.radiance, l.radiance.data(), 12);
+    d.radius = l.radius;
+    d.width = l.width;
+    d.height = l.height;
+    d.angle = l.angle;
+  }
   lotus_scene_desc desc{};
+  desc.lights = lights.empty() ? nullptr : lights.data();
+  desc.light_count = (uint32_t)lights.size();
   desc.geometries = geos.data();
   desc.instances = insts.data();
   desc.materials = mats.data();
@@ -256,7 +275,7 @@ bool CudaOffscreenRenderer::InstanceArray(std::vector<lotus_instance>& insts, st
 
 bool CudaOffscreenRenderer::UpdateIncrementally(const Lotus::SceneUpdate& u, Lotus::GpuSceneEvidence& ev) {
   if (!resident_ || !u.texture_releases.empty() || !u.texture_uploads.empty() || u.materials_changed ||
-      u.environment_changed || (u.lights_changed && !u.lights.empty()))
+      u.environment_changed || u.lights_changed)
     return false;
   // Every release and upload must be one side of a replacement whose
   // topology (vertex count, triangles, presence of corner normals) is kept.

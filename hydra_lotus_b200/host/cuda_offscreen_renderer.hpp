@@ -22,9 +22,10 @@
 //   Present                   presentation are graphics-side parts of the
 //                             reference that this backend does not build
 //   Residency()               the resident scene's device bytes
-// Scene content the backend does not build (texture inputs, analytic
-// lights, material models other than UsdPreviewSurface) makes UpdateScene
-// Fail with the reason, as the reference Fails on unsupported content.
+// Analytic lights (Lotus::Light) map field for field to lotus_light. Scene
+// content the backend does not build (texture inputs, material models other
+// than UsdPreviewSurface) makes UpdateScene Fail with the reason, as the
+// reference Fails on unsupported content.
 #pragma once
 
 #include <lotus/vulkan_backend.hpp>
@@ -90,6 +91,7 @@ class CudaOffscreenRenderer final : public Lotus::OffscreenRenderer {
   std::vector<Lotus::SceneMaterial> materials_;
   std::array<float, 3> environment_{};
   std::optional<Lotus::SceneEnvironmentMap> environment_map_;
+  std::vector<Lotus::Light> lights_;  // the analytic lights, in key order
   std::uint64_t device_bytes_ = 0;
   bool resident_ = false;  // a full update has made the scene resident
   std::uint32_t material_slots_ = 0;

@@ -119,7 +119,7 @@ int main(int argc, char** argv) {
   }
   char magic[4];
   in.get(magic, 4);
-  if (std::memcmp(magic, "LTSC", 4) != 0 || in.get<uint32_t>() != 1) {
+  if (std::memcmp(magic, "LTSC", 4) != 0 || in.get<uint32_t>() != 2) {
     std::fprintf(stderr, "not a scene file\n");
     return 2;
   }
@@ -192,6 +192,25 @@ int main(int argc, char** argv) {
     sm.material.geometry.opacity = lm.opacity;
     sm.material.geometry.opacity_threshold = lm.opacity_threshold;
     update.materials.push_back(sm);
+  }
+  // The analytic lights, as the reference's Light (render_world.hpp:86-114).
+  const uint32_t nl = in.get<uint32_t>();
+  if (nl) update.lights_changed = true;
+  for (uint32_t i = 0; i < nl; ++i) {
+    const lotus_light ll = in.get<lotus_light>();
+    Lotus::Light l;
+    l.shape = ll.shape == LOTUS_LIGHT_SPHERE ? Lotus::LightShape::Sphere
+              : ll.shape == LOTUS_LIGHT_RECT ? Lotus::LightShape::Rect
+              : ll.shape == LOTUS_LIGHT_DISK ? Lotus::LightShape::Disk
+                                             : Lotus::LightShape::Distant;
+    l.normalize = ll.normalize != 0;
+    std::memcpy(l.world_from_light.data(), ll.world_from_light, 64);
+    std::memcpy(l.radiance.data(), ll.radiance, 12);
+    l.radius = ll.radius;
+    l.width = ll.width;
+    l.height = ll.height;
+    l.angle = ll.angle;
+    update.lights.push_back(l);
   }
   Lotus::DrawSummary draw;
   in.get(draw.world_to_clip.data(), 16);

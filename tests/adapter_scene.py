@@ -13,7 +13,7 @@ HARNESS = os.path.join(ROOT, "hydra_lotus_b200", "_lib", "adapter_harness")
 
 
 def write(path, scene, settings, frame_count):
-    out = [b"LTSC", struct.pack("<I", 1)]
+    out = [b"LTSC", struct.pack("<I", 2)]
     out.append(struct.pack("<3I", len(scene.geometries), len(scene.instances), len(scene.materials)))
     out.append(struct.pack("<3f", *scene.environment_constant))
     if scene.environment is not None:
@@ -35,6 +35,9 @@ def write(path, scene, settings, frame_count):
         out.append(struct.pack("<2I", g, mat))
     for mat in scene.materials:
         out.append(bytes(mat))
+    out.append(struct.pack("<I", len(scene.lights)))
+    for light in scene.lights:
+        out.append(bytes(light))
     out.append(np.asarray(scene.world_to_clip, dtype=np.float32).reshape(16).tobytes())
     out.append(struct.pack("<7I", scene.width, scene.height, settings.integrator, settings.light_sampling,
                            settings.max_bounces, settings.sample_index, frame_count))

@@ -29,10 +29,18 @@ def small_sphere_field():
                                spheres=40, emitters=6, sky_size=(128, 64))
 
 
+ADAPTER_SCENES = {
+    "box_room": lambda: scenes.box_room(seed=0, size=64),
+    "sphere_field": small_sphere_field,
+    # Lotus::Light of every shape, mapped by the adapter to lotus_light.
+    "lit_room": lambda: scenes.lit_room(seed=2, size=64, environment=True),
+}
+
+
 @pytest.mark.parametrize("integrator", [abi.INTEGRATOR_REFERENCE, abi.INTEGRATOR_WAVEFRONT])
-@pytest.mark.parametrize("scene_name", ["box_room", "sphere_field"])
+@pytest.mark.parametrize("scene_name", list(ADAPTER_SCENES))
 def test_adapter_renders_what_the_c_abi_renders(cuda, harness, tmp_path, integrator, scene_name):
-    scene = scenes.box_room(seed=0, size=64) if scene_name == "box_room" else small_sphere_field()
+    scene = ADAPTER_SCENES[scene_name]()
     st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS, max_bounces=6,
                               sample_index=11)
     code, evidence, color = adapter_scene.run(str(tmp_path), scene, st, 4)
