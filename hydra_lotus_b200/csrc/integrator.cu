@@ -668,9 +668,10 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_visibility(SceneV
       const float4 c = VQ.pending[slot];
       RestirPixel* p = reinterpret_cast<RestirPixel*>(records + (size_t)slot * stride);
       const F3 estimate = V(c) * (visibility * c.w);
-      if (!isfinite(c.w) || (positive && c.w <= 0.0f) || !is_finite(estimate))
+      if (!isfinite(c.w) || (positive && c.w <= 0.0f) || !is_finite(estimate)) {
         p->flags |= 2u;
-      else
+        atomicMin(&VQ.failed[pass], slot);
+      } else
         p->contribution = F4(estimate, visibility);
     }
   }

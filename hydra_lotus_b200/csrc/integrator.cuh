@@ -141,6 +141,10 @@ struct VisibilityQueue {
   float4* pending;    // per pixel
   uint32_t* counters;
   uint32_t capacity;
+  // Per pass, the smallest pixel whose record's arithmetic failed (flag 2),
+  // or ~0: the frame then Fails as the reference's record readback does
+  // (vulkan_backend.cpp:1650-1705).
+  uint32_t* failed;
 };
 constexpr uint32_t kVisibilityPasses = 3;
 

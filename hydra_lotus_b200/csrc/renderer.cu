@@ -2039,7 +2039,7 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
           R.ok(T.vis_direction.resize(n), "visibility queue", detail) &&
           R.ok(T.vis_pending.resize(n), "visibility queue", detail) &&
           R.ok(T.vis_slot.resize(n), "visibility queue", detail) &&
-          R.ok(T.vis_counters.resize(2 * kVisibilityPasses), "visibility queue", detail);
+          R.ok(T.vis_counters.resize(3 * kVisibilityPasses), "visibility queue", detail);
   if (!okb) return poison(detail);
   // The transport key: a change drops the history (vulkan_backend.cpp:1766-1781).
   uint32_t key[16] = {st.integrator, st.light_sampling, st.restir_proposal, st.restir_candidates,
@@ -2121,9 +2121,10 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   launch_reproject(T.constants.ptr, T.surface[sw].ptr, T.surface[1 - sw].ptr, T.validity.ptr, pixels, s);
   if (restir) {
     const VisibilityQueue vq{T.vis_origin.ptr, T.vis_direction.ptr, T.vis_slot.ptr, T.vis_pending.ptr,
-        T.vis_counters.ptr, pixels};
+        T.vis_counters.ptr, pixels, T.vis_counters.ptr + 2 * kVisibilityPasses};
     if (!R.ok(cudaMemsetAsync(T.vis_counters.ptr, 0, 2 * kVisibilityPasses * sizeof(uint32_t), s),
-            "visibility queue", detail))
+            "visibility queue", detail) ||
+        !R.ok(cudaMemsetAsync(vq.failed, 0xFF, kVisibilityPasses * sizeof(uint32_t), s), "visibility queue", detail))
       return poison(detail);
     launch_restir_initial(R.view, R.frame_const.ptr, T.constants.ptr, T.initial.ptr, T.primary_hit.ptr,
         T.primary_rng.ptr, vq, pixels, s);
@@ -2174,7 +2175,28 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   cudaEventRecord(R.ev_stop, s);
   RayTotals totals{};
   cudaMemcpyAsync(&totals, R.totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s);
+  uint32_t failed[kVisibilityPasses] = {~0u, ~0u, ~0u};
+  if (restir)
+    cudaMemcpyAsync(failed, T.vis_counters.ptr + 2 * kVisibilityPasses, sizeof(failed), cudaMemcpyDeviceToHost, s);
   if (!R.ok(cudaStreamSynchronize(s), "temporal frame", detail)) return poison(detail);
+  // A reservoir whose arithmetic failed (flag 2) fails the frame and the
+  // renderer, as the reference's record readback does
+  // (vulkan_backend.cpp:1650-1705): the first failed initial record, else
+  // the first pixel whose temporal or spatial record failed.
+  if (failed[0] != ~0u) {
+    RestirPixel p{};
+    cudaMemcpy(&p, T.initial.ptr + failed[0], sizeof(p), cudaMemcpyDeviceToHost);
+    char where[320];
+    std::snprintf(where, sizeof(where),
+        "initial reservoir arithmetic is invalid or exceeds GPU float storage at pixel (%u, %u): light %u, "
+        "weight sum %g, target %g, candidates %u, proposal %g",
+        failed[0] % t.width, failed[0] / t.width, p.reservoir.sample, (double)p.reservoir.weight_sum,
+        (double)p.reservoir.selected_target, p.reservoir.candidate_count, (double)p.proposal);
+    return poison(where);
+  }
+  if (failed[1] != ~0u && failed[1] <= failed[2])
+    return poison("temporal reservoir arithmetic is invalid or exceeds GPU float storage");
+  if (failed[2] != ~0u) return poison("spatial reservoir arithmetic is invalid or exceeds GPU float storage");
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
   T.restir_ran = restir;

@@ -335,6 +335,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
       }
     }
   }
+  if (r.flags & 2u) atomicMin(&VQ.failed[0], slot);
   out[slot] = r;
 }
 
@@ -429,6 +430,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
       }
     }
   }
+  if (result.pixel.flags & 2u) atomicMin(&VQ.failed[1], slot);
   out[slot] = result;
   out_surfaces[slot] = receiver;
 }
@@ -522,6 +524,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
       }
     }
   }
+  if (result.pixel.flags & 2u) atomicMin(&VQ.failed[2], slot);
   out[slot] = result;
   out_sources[slot] = make_uint4(sources[0], sources[1], sources[2], sources[3]);
 }

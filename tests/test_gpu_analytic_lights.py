@@ -127,3 +127,36 @@ def test_invalid_lights_fail_without_poisoning(cuda, renderer):
     scene._desc = None
     assert renderer.update_scene(scene).status == abi.FAIL
     cuda.check(renderer.update_scene(scenes.lit_plane(abi.LIGHT_DISK, size=16)), "update after rejects")
+
+
+def test_spatial_overflow_fails_the_frame_and_latches(cuda):
+    """The reference's SpatialOverflow case (validation/restir-gpu-test.cpp,
+    SpatialOverflow): a white Lambert plane under a parallel light of
+    radiance 2.4e38, one candidate, spatial reuse. Every initial reservoir is
+    finite; merging neighbours overflows float, so the frame Fails with the
+    spatial pass's detail, and the failure latches."""
+    s = scenes.Scene("spatial-overflow")
+    white = s.add_material(scenes.preview_material((1.0, 1.0, 1.0), roughness=1.0, ior=1.0))
+    s.add_instance(s.add_geometry(*scenes.quad([[-9, 0, 9], [9, 0, 9], [9, 0, -9], [-9, 0, -9]])), white)
+    s.add_light(abi.LIGHT_DISTANT, scenes.affine(linear=scenes.towards((0.2, 1.0, 0.1))),
+                radiance=(2.4e38, 2.4e38, 2.4e38), angle=0.0)
+    view = scenes.look_at((0.0, 3.0, 1e-3), (0.0, 0.0, 0.0), up=(0.0, 0.0, -1.0))
+    w2c = scenes.multiply(scenes.perspective(40.0, 1.0, 0.1, 100.0), view)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL,
+                              max_bounces=1, sample_index=0, restir_candidates=1, restir_temporal=1,
+                              restir_spatial=1, restir_spatial_radius=2)
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(s), "update_scene")
+        d = abi.temporal_desc(abi.make_frame(w2c, 8, 8, st, 1), view)
+        res, _ = r.render_temporal(d)
+        assert res.status == abi.FAIL and b"spatial reservoir arithmetic" in res.detail, res.detail
+        res, _ = r.render_temporal(d)
+        assert res.status == abi.FAIL
+        st.restir_spatial = 0
+        res, _ = r.render_temporal(abi.temporal_desc(abi.make_frame(w2c, 8, 8, st, 1), view))
+        assert res.status == abi.FAIL
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(s), "update_scene")
+        st.restir_spatial = 0
+        res, _ = r.render_temporal(abi.temporal_desc(abi.make_frame(w2c, 8, 8, st, 1), view))
+        cuda.check(res, "the same frame without spatial reuse")
