@@ -353,6 +353,36 @@ def temporal_report(renderer_module, frames=24):
     return out
 
 
+def analytic_lights_report(renderer_module, frames=64, warmup=8):
+    """Analytic lights on the shape of the reference's many-lights-v1
+    workload (scenes.light_grid: the box room under a grid of sphere
+    lights), wavefront PT with NEE + MIS, 64 bounces, one sample per frame:
+    the median device milliseconds per frame at 128^2 and 512^2 pixels for
+    1 and 256 lights, beside the reference's published figures for its
+    light-crossing hierarchy (RTX A5000)."""
+    out = {"workload": "box room + side x side sphere lights (r 0.025) at y 0.85 (many-lights-v1's grid), "
+                       "wavefront, NEE+MIS, 64 bounces, 1 spp per frame", "unit": "ms per frame (device)"}
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=64, sample_index=0)
+    with renderer_module.CudaOffscreenRenderer(0) as r:
+        for side in (1, 16):
+            for size in (128, 512):
+                scene = scenes.light_grid(side=side, size=size)
+                renderer_module.check(r.update_scene(scene), "update_scene")
+                ms = []
+                for k in range(warmup + frames):
+                    st.sample_index = k
+                    res, _ = r.render_scene(scene.frame(st, 1, read_back=False))
+                    renderer_module.check(res, "light grid frame")
+                    if k >= warmup:
+                        ms.append(res.gpu_ms)
+                out[f"{side * side}_lights_{size}px"] = round(statistics.median(ms), 4)
+    out["reference_published"] = {
+        "hardware": "RTX A5000 (Vulkan ray query), light-crossing hierarchy, wavefront",
+        "1_lights_128px": 0.227, "256_lights_128px": 0.384, "1_lights_512px": 0.829, "256_lights_512px": 1.077}
+    return out
+
+
 def batch_report(renderer_module, spp=8, depth=8):
     """Config 4: the 64-scene batch workload (scenes.batch_workload: traced
     triangles log-uniform in [1e4, 2e6], 256^2 .. 1024^2 targets), 8 spp,
@@ -409,6 +439,8 @@ def main():
                     help="1: also measure frames/s of ReSTIR+SVGF (config 3) and cache+ReSTIR (config 5) at 1080p")
     ap.add_argument("--updates", type=int, default=1,
                     help="1: also time scene uploads and edits on the geometry-v1-shaped grid")
+    ap.add_argument("--lights", type=int, default=1,
+                    help="1: also time the many-lights-v1-shaped analytic light grid (1 and 256 sphere lights)")
     ap.add_argument("--convergence", type=int, default=1,
                     help="1: also measure time to relMSE 1e-3 (plain PT, cache, ReSTIR, cache+ReSTIR)")
     args = ap.parse_args()
@@ -573,6 +605,8 @@ def main():
             line["scene_updates"] = scene_update_report(renderer)
         if args.temporal:
             line["temporal"] = temporal_report(renderer)
+        if args.lights:
+            line["analytic_lights"] = analytic_lights_report(renderer)
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:

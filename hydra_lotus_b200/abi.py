@@ -22,6 +22,7 @@ LIGHT_SAMPLING_RESTIR_INITIAL = 2
 
 MAX_BOUNCES = 1024
 MAX_REPORTED_BOUNCES = 64
+WAVEFRONT_ROUNDS = 9
 
 STATIC_MAX_PIXELS = 65536
 
@@ -204,6 +205,7 @@ class FrameResult(C.Structure):
         ("cache_gpu_ms", C.c_double),
         ("cache_queries", C.c_uint32),
         ("cache_training_records", C.c_uint32),
+        ("tail_gpu_ms", C.c_double),
         ("detail", C.c_char * 256),
     ]
 

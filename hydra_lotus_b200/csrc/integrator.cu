@@ -15,6 +15,7 @@
 #include <utility>
 #include <vector>
 
+#include "../../include/lotus_cuda.h"
 #include "integrator.cuh"
 #include "temporal.cuh"
 
@@ -793,6 +794,64 @@ __global__ void __launch_bounds__(kBlock) k_wf_resolve(SceneView S,
 }
 
 // Ends a sample: totals the queues' rays and advances the sample index.
+// The tail (the reference's round scheduler ends its rounds with a tail
+// megakernel, vulkan_backend.cpp:3745-3845): the paths still queued for
+// bounce `first`, each followed to its end by one thread with the same
+// extension trace, scattering and shadow ray, in the same order, as the
+// wavefront's rounds, so every path ends with the radiance the rounds would
+// give it; the per-bounce queue counts are kept as the rounds keep them.
+// Threads take paths from `cursor` one at a time. Long paths then cost one
+// launch instead of three per bounce.
+template <bool kBatch, bool kAnalytic>
+__global__ void __launch_bounds__(kBlock) k_wf_tail(SceneView S, const FrameConst* __restrict__ fcp, PathState P,
+    Queues Q, uint32_t first, uint32_t* __restrict__ cursor, SceneTable B) {
+  const uint32_t n = Q.counts[3 * first];
+  for (;;) {
+    const uint32_t index = atomicAdd(cursor, 1u);
+    if (index >= n) return;
+    const uint32_t slot = Q.ray[first & 1][index];
+    const uint32_t scene = kBatch ? table_scene(B, slot) : 0u;
+    const FrameConst& f = kBatch ? B.frames[scene] : *fcp;
+    const SceneView& SS = kBatch ? B.views[scene] : S;
+    const float4 o = P.origin[slot];
+    const float4 d = P.direction[slot];
+    const float4 thr = P.throughput[slot];
+    const float4 rad = P.radiance[slot];
+    F3 ro = V(o), rd = V(d);
+    float tmin = o.w, tmax = d.w;
+    F3 T = V(thr), R = V(rad);
+    float last_pdf = thr.w;
+    uint32_t flags = last_pdf < 0.0f ? kUnweightedLight : 0u;
+    uint32_t rng = __float_as_uint(rad.w);
+    // A path's bounces are bounded by max_bounces (scatter ends it there).
+    for (uint32_t bounce = first; bounce <= f.max_bounces; ++bounce) {
+      Hit hit;
+      if (!trace_closest(SS, ro, rd, tmin, tmax, rng, hit)) {
+        R = miss_path<kAnalytic>(SS, f, ro, rd, flags, last_pdf, T, R);
+        break;
+      }
+      atomicAdd(&Q.counts[3 * bounce + 1], 1u);
+      F3 no, nd;
+      ShadowRequest req;
+      const bool cont = scatter<kAnalytic>(SS, f, hit.instance, hit.tri, hit.b1, hit.b2, ro, rd, bounce, T, R,
+          last_pdf, flags, rng, no, nd, req, slot);
+      if (req.pending) {
+        atomicAdd(&Q.counts[3 * bounce + 2], 1u);
+        const float tr = trace_shadow(SS, req.origin, req.direction, 0.0f, req.tmax);
+        if (tr > 0.0f) R = R + req.throughput * shadow_contribution(req.fl, req.weight, req.pdf, tr);
+      }
+      if (!cont) break;
+      atomicAdd(&Q.counts[3 * (bounce + 1)], 1u);
+      if (flags & kUnweightedLight) last_pdf = -1.0f;
+      ro = no;
+      rd = nd;
+      tmin = 0.0f;
+      tmax = kFloatMax;
+    }
+    P.radiance[slot] = F4(R, 1.0f);
+  }
+}
+
 __global__ void k_wf_finish(FrameConst* fc, const uint32_t* __restrict__ counts,
     uint32_t max_bounces, RayTotals* totals) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -918,6 +977,10 @@ uint32_t persistent_grid(const void* kernel, uint32_t capacity, const TraceTunin
   return std::max(1u, std::min(grid, (capacity + kBlock - 1) / kBlock));
 }
 
+uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits) {
+  return count_visits || max_bounces < LOTUS_WAVEFRONT_ROUNDS ? max_bounces + 1 : LOTUS_WAVEFRONT_ROUNDS;
+}
+
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
@@ -952,7 +1015,11 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     if (count) k_wf_camera<true, false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, visits, none);
     else k_wf_camera<false, false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
   }
-  for (uint32_t b = 0; b <= max_bounces; ++b) {
+  // Bounces 0 .. rounds - 1 as wavefront rounds; the paths queued for bounce
+  // `rounds` (if any can be) go to the tail kernel. Counting visits keeps
+  // every bounce in rounds, as the counted kernels are the rounds' own.
+  const uint32_t rounds = wavefront_rounds(max_bounces, count);
+  for (uint32_t b = 0; b < rounds; ++b) {
     if (b != 0) {
       Timed t(profile, stream, 1);
       if (count && analytic)
@@ -990,6 +1057,14 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
             nullptr, none);
     }
   }
+  if (rounds <= max_bounces) {
+    Timed t(profile, stream, 6);
+    uint32_t* cursor = fetch + 2 * (max_bounces + 1);
+    const uint32_t grid_tail = persistent_grid(
+        analytic ? (const void*)k_wf_tail<false, true> : (const void*)k_wf_tail<false, false>, Q.capacity, tuning);
+    if (analytic) k_wf_tail<false, true><<<grid_tail, kBlock, 0, stream>>>(S, fc, P, Q, rounds, cursor, none);
+    else k_wf_tail<false, false><<<grid_tail, kBlock, 0, stream>>>(S, fc, P, Q, rounds, cursor, none);
+  }
   if (C.enabled) {
     // The paths that ended into the cache receive its answer; then the
     // training paths' targets train it.
@@ -1025,7 +1100,8 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
       8u * persistent_grid((const void*)k_wf_shade<false, true, false>, Q.capacity, TraceTuning()));
   k_wf_camera<false, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
-  for (uint32_t b = 0; b <= max_bounces; ++b) {
+  const uint32_t rounds = wavefront_rounds(max_bounces, false);
+  for (uint32_t b = 0; b < rounds; ++b) {
     if (b != 0 && B.analytic)
       k_wf_extend<false, true, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, b,
           fetch + 2 * b, refill, nullptr, B);
@@ -1038,6 +1114,15 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
       k_wf_shade<false, true, false><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, Q, b, no_cache, B);
     k_wf_shadow<false, true><<<grid_shadow, kBlock, 0, stream>>>(none_view, P, Q, b, fetch + 2 * b + 1, refill,
         nullptr, B);
+  }
+  if (rounds <= max_bounces) {
+    uint32_t* cursor = fetch + 2 * (max_bounces + 1);
+    const uint32_t grid_tail = persistent_grid(
+        B.analytic ? (const void*)k_wf_tail<true, true> : (const void*)k_wf_tail<true, false>, Q.capacity, tuning);
+    if (B.analytic)
+      k_wf_tail<true, true><<<grid_tail, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rounds, cursor, B);
+    else
+      k_wf_tail<true, false><<<grid_tail, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rounds, cursor, B);
   }
   k_wf_resolve<true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, accum, color, B);
   k_wf_finish_batch<<<1, 32, 0, stream>>>(B, Q.counts, max_bounces, totals);

@@ -117,6 +117,11 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
     SampleProfile* profile = nullptr);
 
+// The bounces the wavefront integrator runs as rounds: all of them up to
+// LOTUS_WAVEFRONT_ROUNDS - 1 bounces (and whenever visits are counted),
+// else LOTUS_WAVEFRONT_ROUNDS, the tail kernel taking the rest.
+uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits);
+
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,

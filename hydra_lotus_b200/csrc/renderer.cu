@@ -1610,8 +1610,8 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     if (R.cache.error_flag(s) != 0) return poison("a radiance-cache kernel's tensor-core wait gave up");
   }
   if (want_timings) {
-    double by_kind[6] = {0, 0, 0, 0, 0, 0};
-    uint32_t launches[6] = {0, 0, 0, 0, 0, 0};
+    double by_kind[7] = {0, 0, 0, 0, 0, 0, 0};
+    uint32_t launches[7] = {0, 0, 0, 0, 0, 0, 0};
     for (int i = 0; i < profile.count; ++i) {
       float kms = 0.0f;
       cudaEventElapsedTime(&kms, R.profile_events[2 * i], R.profile_events[2 * i + 1]);
@@ -1625,6 +1625,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     res.shadow_gpu_ms = by_kind[3];
     res.resolve_gpu_ms = by_kind[4];
     res.cache_gpu_ms = by_kind[5];
+    res.tail_gpu_ms = by_kind[6];
     res.extend_launches = launches[1];
     res.shadow_launches = launches[3];
   }
@@ -1665,7 +1666,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
       if (c) last = b + 1;
     }
     res.wavefront_path_count_size = last;
-    res.wavefront_rounds = st.max_bounces + 1;
+    res.wavefront_rounds = wavefront_rounds(st.max_bounces, want_visits);
   }
   return LOTUS_PASS;
 }

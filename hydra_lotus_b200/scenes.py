@@ -765,3 +765,23 @@ def lit_plane(shape, size=33, height=1.0, radius=0.25, radiance=(2.0, 2.0, 2.0),
                                look_at((0.0, 3.0, 1e-3), (0.0, 0.0, 0.0), up=(0.0, 0.0, -1.0)))
     s.width = s.height = size
     return s
+
+
+def light_grid(side=16, size=512, seed=0):
+    """The box room without its ceiling emitter, lit by a side x side grid
+    of sphere lights (radius 0.025) 0.85 above its centre, spaced 0.12 x
+    15 / (side - 1) over [-0.9, 0.9] in x and z, with radiance (12, 10, 8)
+    scaled by 256 / side^2 so that the grid's power does not change with
+    its side: the shape of the reference's many-lights-v1 light grid
+    (SCENE.md's workloads), on the seeded box room."""
+    s = box_room(seed=seed, size=size)
+    s.name = f"light-grid-{side}x{side}"
+    s.instances = [inst for k, inst in enumerate(s.instances) if k != 5]
+    spacing = 0.0 if side == 1 else 0.12 * (15.0 / float(side - 1))
+    first = 0.0 if side == 1 else -0.9
+    scale = 256.0 / float(side * side)
+    for y in range(side):
+        for x in range(side):
+            s.add_light(abi.LIGHT_SPHERE, affine(translation=(first + spacing * x, 0.85, first + spacing * y)),
+                        radiance=(12.0 * scale, 10.0 * scale, 8.0 * scale), radius=0.025)
+    return s

@@ -56,6 +56,9 @@ extern "C" {
 
 /* kMaxWavefrontBounces (vulkan_backend.hpp:694): a larger max_bounces Fails. */
 #define LOTUS_MAX_BOUNCES 1024u
+/* Bounces the wavefront integrator runs as rounds of extension, shading and
+ * shadow kernels before its tail kernel takes the paths still queued. */
+#define LOTUS_WAVEFRONT_ROUNDS 9u
 /* How many per-bounce queue counts a frame result reports. */
 #define LOTUS_MAX_REPORTED_BOUNCES 64u
 
@@ -228,7 +231,10 @@ typedef struct lotus_frame_result {
   /* Device time of the call's samples (CUDA events), readback excluded. */
   double gpu_ms;
   /* Queue occupancy of the last sample: per bounce, paths that entered the
-   * ray queue; element 0 is the camera rays. */
+   * ray queue; element 0 is the camera rays. wavefront_rounds: the bounces
+   * run as extension and shading rounds; with max_bounces above
+   * LOTUS_WAVEFRONT_ROUNDS the tail kernel follows the paths still queued
+   * after them (their rays count at the bounce they leave from). */
   uint32_t wavefront_path_counts[LOTUS_MAX_REPORTED_BOUNCES];
   uint32_t wavefront_path_count_size;
   /* With LOTUS_FRAME_TIMINGS: device time of the last sample's kernels, by
@@ -253,6 +259,9 @@ typedef struct lotus_frame_result {
   double cache_gpu_ms;
   uint32_t cache_queries;
   uint32_t cache_training_records;
+  /* With LOTUS_FRAME_TIMINGS: the tail kernel's device time (the paths still
+   * queued after the wavefront_rounds rounds, each followed to its end). */
+  double tail_gpu_ms;
   char detail[256];
 } lotus_frame_result;
 

@@ -116,3 +116,29 @@ def test_cornell_negative_control_rejected(cuda, renderer, golden):
     _, color = render(cuda, renderer, scene, st, frame_count=1024)
     c = metrics.compare(color, 1024, golden["mean"], golden["variance"], golden["samples"])
     assert not c.ok, c
+
+
+@pytest.mark.parametrize("name", ["box_room", "lit_room"])
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+def test_tail_kernel_paths_match_oracle(cuda, renderer, oracle_lib, name, light_sampling):
+    """Above LOTUS_WAVEFRONT_ROUNDS - 1 bounces the wavefront integrator's
+    tail kernel follows the paths still queued after its rounds: each path
+    is the oracle's, and the per-bounce queue counts equal those of a
+    sample run in rounds throughout (counting visits keeps every bounce in
+    rounds)."""
+    scene = scenes.box_room(seed=2, size=96) if name == "box_room" else scenes.lit_room(seed=2, size=96)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=light_sampling, max_bounces=64,
+                              sample_index=21)
+    res, color = render(cuda, renderer, scene, st)
+    assert res.wavefront_rounds == abi.WAVEFRONT_ROUNDS
+    want, rays = oracle_lib.OracleScene(scene).sample(scene.frame(st), 21)
+    p = PathParity(color, want)
+    print(name, p, res.wavefront_path_count_size, rays, res.extension_rays, res.shadow_rays)
+    p.assert_ok()
+    assert p.exact > 0.9, p
+    assert res.wavefront_path_count_size > abi.WAVEFRONT_ROUNDS
+    counted, color2 = render(cuda, renderer, scene, st, flags=abi.FRAME_COUNT_VISITS)
+    assert counted.wavefront_rounds == 65
+    assert np.array_equal(color, color2)
+    assert list(res.wavefront_path_counts[:64]) == list(counted.wavefront_path_counts[:64])
+    assert (res.extension_rays, res.shadow_rays) == (counted.extension_rays, counted.shadow_rays)
