@@ -69,10 +69,11 @@ def settings(sample_index):
                                 max_bounces=DEPTH, sample_index=sample_index)
 
 
-def launches_per_sample(max_bounces):
-    # camera, shade and shadow per bounce, extend per bounce after the
-    # first, resolve, finish, advance
-    return 1 + 2 * (max_bounces + 1) + max_bounces + 3
+def launches_per_sample(max_bounces, rounds):
+    # camera; shade and shadow per round, extend per round after the first;
+    # the tail kernel when the rounds stop short of max_bounces + 1;
+    # resolve, finish, advance
+    return 1 + 2 * rounds + (rounds - 1) + (1 if rounds <= max_bounces else 0) + 3
 
 
 def measured_peaks():
@@ -539,8 +540,10 @@ def main():
         per_ray = (EXTEND_STATE_BYTES + NODE_BYTES * counted.node_visits[1] / n_ext +
                    TRIANGLE_BYTES * counted.triangle_visits[1] / n_ext +
                    INSTANCE_BYTES * counted.instance_visits[1] / n_ext)
+        # The rays the extension kernel traced: those of the rounds' bounces
+        # (the tail kernel traces the rest).
         ext_rays_timed = sum(timed.wavefront_path_counts[b]
-                             for b in range(1, timed.wavefront_path_count_size))
+                             for b in range(1, min(timed.wavefront_rounds, timed.wavefront_path_count_size)))
         ext_bytes = ext_rays_timed * per_ray
         achieved = ext_bytes / (timed.extend_gpu_ms * 1e-3) / 1e9 if timed.extend_gpu_ms else 0.0
         launches = timed.extend_launches or DEPTH
@@ -565,7 +568,7 @@ def main():
             "e2e": {"value": round(total_e2e_rays / (max_e2e_ms * 1e-3) / 1e6, 2),
                     "unit": "Mrays/s", "h2d_bytes_per_step": 160,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 16 + 64},
-            "gpu_launches": launches_per_sample(DEPTH) * SPP * args.steps,
+            "gpu_launches": launches_per_sample(DEPTH, timed.wavefront_rounds) * SPP * args.steps,
             "roofline": {
                 "kernel": "k_wf_extend",
                 "bound": "hbm",
@@ -587,7 +590,8 @@ def main():
                 "kernel_ms_per_sample": {
                     "camera": round(timed.camera_gpu_ms, 4), "extend": round(timed.extend_gpu_ms, 4),
                     "shade": round(timed.shade_gpu_ms, 4), "shadow": round(timed.shadow_gpu_ms, 4),
-                    "resolve": round(timed.resolve_gpu_ms, 4)},
+                    "tail": round(timed.tail_gpu_ms, 4), "resolve": round(timed.resolve_gpu_ms, 4)},
+                "wavefront_rounds": timed.wavefront_rounds,
             },
             "cpu_baseline": cpu,
             "clocks": clock,

@@ -213,7 +213,7 @@ class FrameResult(C.Structure):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("flags", C.c_uint32), ("bvh_leaf_size", C.c_uint32),
                 ("trace_refill_below", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("wavefront_rounds", C.c_uint32)]
 
 
 class TemporalDesc(C.Structure):

@@ -134,6 +134,7 @@ extern "C" int32_t lotus_cuda_batch_create(const lotus_cuda_options* options, lo
   if (options) {
     b->tuning.refill_below = options->trace_refill_below;
     b->tuning.blocks_per_sm = options->trace_blocks_per_sm;
+    b->tuning.rounds = options->wavefront_rounds;
   }
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&b->ev_start) != cudaSuccess || cudaEventCreate(&b->ev_stop) != cudaSuccess) {
@@ -195,6 +196,7 @@ extern "C" int32_t lotus_cuda_batch_set_scenes(lotus_cuda_batch* b, const lotus_
     o.device = b->device;
     o.trace_refill_below = b->tuning.refill_below;
     o.trace_blocks_per_sm = b->tuning.blocks_per_sm;
+    o.wavefront_rounds = b->tuning.rounds;
     lotus_cuda_renderer* r = nullptr;
     char err[256] = {};
     int32_t s = lotus_cuda_create(&o, &r, err, sizeof(err));

@@ -977,8 +977,10 @@ uint32_t persistent_grid(const void* kernel, uint32_t capacity, const TraceTunin
   return std::max(1u, std::min(grid, (capacity + kBlock - 1) / kBlock));
 }
 
-uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits) {
-  return count_visits || max_bounces < LOTUS_WAVEFRONT_ROUNDS ? max_bounces + 1 : LOTUS_WAVEFRONT_ROUNDS;
+uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, bool cache) {
+  uint32_t rounds = requested ? requested : LOTUS_WAVEFRONT_ROUNDS;
+  if (cache) rounds = std::max(rounds, 2u);
+  return count_visits || max_bounces < rounds ? max_bounces + 1 : rounds;
 }
 
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
@@ -1018,7 +1020,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   // Bounces 0 .. rounds - 1 as wavefront rounds; the paths queued for bounce
   // `rounds` (if any can be) go to the tail kernel. Counting visits keeps
   // every bounce in rounds, as the counted kernels are the rounds' own.
-  const uint32_t rounds = wavefront_rounds(max_bounces, count);
+  const uint32_t rounds = wavefront_rounds(max_bounces, count, tuning.rounds, C.enabled);
   for (uint32_t b = 0; b < rounds; ++b) {
     if (b != 0) {
       Timed t(profile, stream, 1);
@@ -1100,7 +1102,7 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
       8u * persistent_grid((const void*)k_wf_shade<false, true, false>, Q.capacity, TraceTuning()));
   k_wf_camera<false, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
-  const uint32_t rounds = wavefront_rounds(max_bounces, false);
+  const uint32_t rounds = wavefront_rounds(max_bounces, false, tuning.rounds);
   for (uint32_t b = 0; b < rounds; ++b) {
     if (b != 0 && B.analytic)
       k_wf_extend<false, true, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, b,

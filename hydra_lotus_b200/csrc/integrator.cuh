@@ -82,6 +82,7 @@ struct SceneTable {
 struct TraceTuning {
   uint32_t refill_below = 0;
   uint32_t blocks_per_sm = 0;  // 0: as many as fit
+  uint32_t rounds = 0;         // wavefront rounds before the tail; 0: the default
 };
 
 // Ray totals over a RenderScene call.
@@ -117,10 +118,11 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
     SampleProfile* profile = nullptr);
 
-// The bounces the wavefront integrator runs as rounds: all of them up to
-// LOTUS_WAVEFRONT_ROUNDS - 1 bounces (and whenever visits are counted),
-// else LOTUS_WAVEFRONT_ROUNDS, the tail kernel taking the rest.
-uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits);
+// The bounces the wavefront integrator runs as rounds (`requested`, or by
+// default LOTUS_WAVEFRONT_ROUNDS), the tail kernel taking the rest; all of
+// them when visits are counted, and with the radiance cache at least
+// bounces 0 and 1 (its vertex is shaded in round 1).
+uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, bool cache = false);
 
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,

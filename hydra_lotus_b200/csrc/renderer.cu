@@ -711,8 +711,20 @@ struct Renderer {
     uint32_t width, height, max_bounces;
     uint32_t rect[4];
     uint32_t cache;  // the radiance cache's configuration count (0: off)
+    uint32_t rounds; // wavefront rounds before the tail kernel
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
   } graph_key{};
+  static constexpr uint32_t kTailQueue = 65536;
+  // Rounds before the tail, chosen from the queue occupancy of the first
+  // sample rendered with `rounds_key` (its rounds field 0): the first bounce
+  // whose queue holds fewer than max(camera rays / 32, kTailQueue) paths
+  // (the reference's round scheduler stops at camera rays / 16; a floor of
+  // about the paths the tail kernel keeps resident at once, since its
+  // threads then run side by side; both measured best on B200 for a
+  // 36-triangle room at 128^2 and 512^2 and a 13.7M-triangle field at
+  // 1080p). Results do not depend on it.
+  GraphKey rounds_key{};
+  uint32_t auto_rounds = 0;
 
   ~Renderer() {
     for (cudaEvent_t e : profile_events) cudaEventDestroy(e);
@@ -1551,25 +1563,30 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
       profile.visits = R.visits.ptr;
     }
   }
+  // The graph's key without its rounds, and the rounds this call runs.
+  Renderer::GraphKey gk{};
+  gk.scene_generation = R.scene_generation;
+  gk.width = t.width;
+  gk.height = t.height;
+  gk.max_bounces = st.max_bounces;
+  std::memcpy(gk.rect, rect, sizeof(rect));
+  gk.cache = use_cache ? R.cache_generation : 0u;
+  TraceTuning tuning = R.tuning;
+  if (tuning.rounds == 0 && R.auto_rounds != 0 && R.rounds_key == gk) tuning.rounds = R.auto_rounds;
+  const bool choose_rounds = wavefront && R.tuning.rounds == 0 && !(R.rounds_key == gk);
   cudaEventRecord(R.ev_start, s);
   for (uint32_t k = 0; k < submissions; ++k) {
     const bool profiled = (want_timings || want_visits) && k + 1 == submissions;
     if (profiled) {
       if (wavefront)
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
-            R.accum.ptr, R.color.ptr, R.totals.ptr, s, &profile, R.tuning, &cq);
+            R.accum.ptr, R.color.ptr, R.totals.ptr, s, &profile, tuning, &cq);
       else
         launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s,
             &profile);
       launch_advance(R.frame_const.ptr, s);
     } else if (wavefront) {
-      Renderer::GraphKey gk{};
-      gk.scene_generation = R.scene_generation;
-      gk.width = t.width;
-      gk.height = t.height;
-      gk.max_bounces = st.max_bounces;
-      std::memcpy(gk.rect, rect, sizeof(rect));
-      gk.cache = use_cache ? R.cache_generation : 0u;
+      gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, use_cache);
       if (!R.graph || !(R.graph_key == gk)) {
         if (R.graph) {
           cudaGraphExecDestroy(R.graph);
@@ -1579,7 +1596,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
         if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
           return poison(detail);
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
-            R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, R.tuning, &cq);
+            R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, tuning, &cq);
         launch_advance(R.frame_const.ptr, s);
         if (!R.ok(cudaStreamEndCapture(s, &g), "graph capture", detail)) return poison(detail);
         cudaError_t e = cudaGraphInstantiate(&R.graph, g, 0);
@@ -1666,7 +1683,20 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
       if (c) last = b + 1;
     }
     res.wavefront_path_count_size = last;
-    res.wavefront_rounds = wavefront_rounds(st.max_bounces, want_visits);
+    res.wavefront_rounds = wavefront_rounds(st.max_bounces, want_visits, tuning.rounds, use_cache);
+    if (choose_rounds) {
+      const uint32_t camera = rect[2] * rect[3];
+      const uint32_t below = std::max(camera / 32u, Renderer::kTailQueue);
+      uint32_t rounds = st.max_bounces + 1;
+      for (uint32_t b = 1; b <= st.max_bounces; ++b)
+        if (counts[3 * b] < below) {
+          rounds = b;
+          break;
+        }
+      gk.rounds = 0;
+      R.rounds_key = gk;
+      R.auto_rounds = rounds;
+    }
   }
   return LOTUS_PASS;
 }
@@ -1730,14 +1760,17 @@ int32_t lotus_cuda_create(const lotus_cuda_options* options, lotus_cuda_renderer
     }
     R.bvh_leaf_size = options->bvh_leaf_size;
   }
-  if (options && (options->trace_refill_below > 32 || options->trace_blocks_per_sm > 64)) {
-    copy_detail(error, error_size, "trace_refill_below must be in 0..32 and trace_blocks_per_sm in 0..64");
+  if (options && (options->trace_refill_below > 32 || options->trace_blocks_per_sm > 64 ||
+                     options->wavefront_rounds > LOTUS_MAX_BOUNCES + 1)) {
+    copy_detail(error, error_size,
+        "trace_refill_below must be in 0..32, trace_blocks_per_sm in 0..64 and wavefront_rounds in 0..1025");
     delete h;
     return LOTUS_FAIL;
   }
   if (options) {
     R.tuning.refill_below = options->trace_refill_below;
     R.tuning.blocks_per_sm = options->trace_blocks_per_sm;
+    R.tuning.rounds = options->wavefront_rounds;
   }
   std::string detail;
   if (!R.ok(cudaSetDevice(device), "cudaSetDevice", detail) ||

@@ -275,7 +275,13 @@ typedef struct lotus_cuda_options {
    * trace_blocks_per_sm blocks run on each SM. */
   uint32_t trace_refill_below;
   uint32_t trace_blocks_per_sm;
-  uint32_t reserved;
+  /* Bounces the wavefront integrator runs as rounds before its tail kernel
+   * takes the paths still queued (1..LOTUS_MAX_BOUNCES + 1). 0: RenderScene
+   * chooses them from its first sample of each scene and frame shape (run
+   * with LOTUS_WAVEFRONT_ROUNDS): the first bounce whose queue held fewer
+   * than max(camera rays / 32, 65536) paths; other calls use
+   * LOTUS_WAVEFRONT_ROUNDS. Results do not depend on it. */
+  uint32_t wavefront_rounds;
 } lotus_cuda_options;
 
 typedef struct lotus_cuda_renderer lotus_cuda_renderer;
