@@ -44,6 +44,12 @@ struct lotus_cuda_batch {
   cudaGraphExec_t graph = nullptr;
   std::vector<uint32_t> graph_layout;
   uint32_t graph_bounces = 0;
+  uint32_t graph_rounds = 0;
+  // The wavefront rounds before the tail, chosen from the first sample of a
+  // layout (choose_wavefront_rounds over every scene's pixels).
+  std::vector<uint32_t> rounds_layout;
+  uint32_t rounds_bounces = 0;
+  uint32_t auto_rounds = 0;
 };
 
 namespace lotus {
@@ -304,8 +310,13 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
           cudaSuccess ||
       (e = cudaMemsetAsync(b->totals, 0, sizeof(RayTotals), s)) != cudaSuccess)
     return fail(std::string("batch upload: ") + cudaGetErrorString(e), true);
-  // One graph per layout: the sample over every scene.
-  if (!b->graph || b->graph_layout != layout || b->graph_bounces != max_bounces) {
+  // One graph per layout and round count: the sample over every scene.
+  TraceTuning tuning = b->tuning;
+  const bool rounds_known = b->rounds_layout == layout && b->rounds_bounces == max_bounces;
+  if (tuning.rounds == 0 && rounds_known) tuning.rounds = b->auto_rounds;
+  const bool choose_rounds = b->tuning.rounds == 0 && !rounds_known && frame_count != 0;
+  const uint32_t rounds = wavefront_rounds(max_bounces, false, tuning.rounds);
+  if (!b->graph || b->graph_layout != layout || b->graph_bounces != max_bounces || b->graph_rounds != rounds) {
     if (b->graph) {
       cudaGraphExecDestroy(b->graph);
       b->graph = nullptr;
@@ -313,7 +324,7 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
     cudaGraph_t g;
     if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
       return fail(std::string("graph capture: ") + cudaGetErrorString(e), true);
-    launch_wavefront_batch(B, max_bounces, b->P, Q, b->accum, b->color, b->totals, s, b->tuning);
+    launch_wavefront_batch(B, max_bounces, b->P, Q, b->accum, b->color, b->totals, s, tuning);
     if ((e = cudaStreamEndCapture(s, &g)) != cudaSuccess)
       return fail(std::string("graph capture: ") + cudaGetErrorString(e), true);
     e = cudaGraphInstantiate(&b->graph, g, 0);
@@ -321,6 +332,7 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
     if (e != cudaSuccess) return fail(std::string("graph instantiate: ") + cudaGetErrorString(e), true);
     b->graph_layout = layout;
     b->graph_bounces = max_bounces;
+    b->graph_rounds = rounds;
   }
   cudaEventRecord(b->ev_start, s);
   for (uint32_t i = 0; i < frame_count; ++i)
@@ -329,6 +341,11 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
   cudaEventRecord(b->ev_stop, s);
   RayTotals totals{};
   cudaMemcpyAsync(&totals, b->totals, sizeof(totals), cudaMemcpyDeviceToHost, s);
+  std::vector<uint32_t> counts;
+  if (choose_rounds) {
+    counts.assign(3 * (size_t)(max_bounces + 2), 0u);
+    cudaMemcpyAsync(counts.data(), Q.counts, counts.size() * 4, cudaMemcpyDeviceToHost, s);
+  }
   for (uint32_t k = 0; colors && k < count; ++k)
     if (colors[k] && frames[k].target.read_back)
       cudaMemcpyAsync(colors[k], b->color + base[k], sizeof(float4) * (base[k + 1] - base[k]),
@@ -337,6 +354,11 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
     return fail(std::string("batch render: ") + cudaGetErrorString(e), true);
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
+  if (choose_rounds) {
+    b->rounds_layout = layout;
+    b->rounds_bounces = max_bounces;
+    b->auto_rounds = choose_wavefront_rounds(counts.data(), base[count], max_bounces);
+  }
   for (uint32_t k = 0; k < count; ++k) {
     b->accumulated[k] += frame_count;
     b->completion[k] += frame_count;

@@ -977,6 +977,14 @@ uint32_t persistent_grid(const void* kernel, uint32_t capacity, const TraceTunin
   return std::max(1u, std::min(grid, (capacity + kBlock - 1) / kBlock));
 }
 
+uint32_t choose_wavefront_rounds(const uint32_t* counts, uint32_t camera, uint32_t max_bounces) {
+  constexpr uint32_t kTailQueue = 65536;
+  const uint32_t below = std::max(camera / 32u, kTailQueue);
+  for (uint32_t b = 1; b <= max_bounces; ++b)
+    if (counts[3 * b] < below) return b;
+  return max_bounces + 1;
+}
+
 uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, bool cache) {
   uint32_t rounds = requested ? requested : LOTUS_WAVEFRONT_ROUNDS;
   if (cache) rounds = std::max(rounds, 2u);

@@ -124,6 +124,14 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
 // bounces 0 and 1 (its vertex is shaded in round 1).
 uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, bool cache = false);
 
+// The rounds a sample should run, from a sample's queue counts (the
+// wavefront kernels' per-bounce words, 3 per bounce) and its camera rays:
+// the first bounce whose queue held fewer than max(camera / 32, 65,536)
+// paths (the reference's round scheduler stops at camera / 16; the floor is
+// about the paths the tail kernel keeps resident at once), else every
+// bounce. Results do not depend on it; only the launch count does.
+uint32_t choose_wavefront_rounds(const uint32_t* counts, uint32_t camera, uint32_t max_bounces);
+
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,

@@ -714,17 +714,11 @@ struct Renderer {
     uint32_t rounds; // wavefront rounds before the tail kernel
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
   } graph_key{};
-  static constexpr uint32_t kTailQueue = 65536;
-  // Rounds before the tail, chosen from the queue occupancy of the first
-  // sample rendered with `rounds_key` (its rounds field 0): the first bounce
-  // whose queue holds fewer than max(camera rays / 32, kTailQueue) paths
-  // (the reference's round scheduler stops at camera rays / 16; a floor of
-  // about the paths the tail kernel keeps resident at once, since its
-  // threads then run side by side; both measured best on B200 for a
-  // 36-triangle room at 128^2 and 512^2 and a 13.7M-triangle field at
-  // 1080p). Results do not depend on it.
-  GraphKey rounds_key{};
-  uint32_t auto_rounds = 0;
+  // Rounds before the tail, chosen (choose_wavefront_rounds) from the queue
+  // counts of the first sample rendered with `rounds_key` (its rounds field
+  // 0), for RenderScene and for the temporal frames.
+  GraphKey rounds_key{}, temporal_rounds_key{};
+  uint32_t auto_rounds = 0, temporal_auto_rounds = 0;
 
   ~Renderer() {
     for (cudaEvent_t e : profile_events) cudaEventDestroy(e);
@@ -1685,17 +1679,9 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     res.wavefront_path_count_size = last;
     res.wavefront_rounds = wavefront_rounds(st.max_bounces, want_visits, tuning.rounds, use_cache);
     if (choose_rounds) {
-      const uint32_t camera = rect[2] * rect[3];
-      const uint32_t below = std::max(camera / 32u, Renderer::kTailQueue);
-      uint32_t rounds = st.max_bounces + 1;
-      for (uint32_t b = 1; b <= st.max_bounces; ++b)
-        if (counts[3 * b] < below) {
-          rounds = b;
-          break;
-        }
       gk.rounds = 0;
       R.rounds_key = gk;
-      R.auto_rounds = rounds;
+      R.auto_rounds = choose_wavefront_rounds(counts.data(), rect[2] * rect[3], st.max_bounces);
     }
   }
   return LOTUS_PASS;
@@ -2193,10 +2179,22 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   const bool use_cache = wavefront && R.cache_enabled && R.cache.ready();
   if (use_cache && !ensure_cache_queues(R, pixels, detail)) return poison(detail);
   const CacheQueues cq = use_cache ? cache_queues(R) : CacheQueues();
+  // The wavefront rounds before the tail, as RenderScene chooses them.
+  Renderer::GraphKey rk{};
+  rk.scene_generation = R.scene_generation;
+  rk.width = t.width;
+  rk.height = t.height;
+  rk.max_bounces = st.max_bounces;
+  std::memcpy(rk.rect, rect, sizeof(rect));
+  rk.cache = use_cache ? R.cache_generation : 0u;
+  TraceTuning tuning = R.tuning;
+  if (tuning.rounds == 0 && R.temporal_auto_rounds != 0 && R.temporal_rounds_key == rk)
+    tuning.rounds = R.temporal_auto_rounds;
+  const bool choose_rounds = wavefront && d.frame_count != 0 && R.tuning.rounds == 0 && !(R.temporal_rounds_key == rk);
   for (uint32_t k = 0; k < d.frame_count; ++k) {
     if (wavefront)
       launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
-          R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, R.tuning, &cq);
+          R.accum.ptr, R.color.ptr, R.totals.ptr, s, nullptr, tuning, &cq);
     else
       launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s);
     launch_advance(R.frame_const.ptr, s);
@@ -2212,7 +2210,16 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   uint32_t failed[kVisibilityPasses] = {~0u, ~0u, ~0u};
   if (restir)
     cudaMemcpyAsync(failed, T.vis_counters.ptr + 2 * kVisibilityPasses, sizeof(failed), cudaMemcpyDeviceToHost, s);
+  std::vector<uint32_t> counts;
+  if (choose_rounds) {
+    counts.assign(3 * (size_t)(st.max_bounces + 2), 0u);
+    cudaMemcpyAsync(counts.data(), R.counts.ptr, counts.size() * 4, cudaMemcpyDeviceToHost, s);
+  }
   if (!R.ok(cudaStreamSynchronize(s), "temporal frame", detail)) return poison(detail);
+  if (choose_rounds) {
+    R.temporal_rounds_key = rk;
+    R.temporal_auto_rounds = choose_wavefront_rounds(counts.data(), rect[2] * rect[3], st.max_bounces);
+  }
   // A reservoir whose arithmetic failed (flag 2) fails the frame and the
   // renderer, as the reference's record readback does
   // (vulkan_backend.cpp:1650-1705): the first failed initial record, else
