@@ -24,6 +24,8 @@ def main():
     ap.add_argument("--frames", type=int, default=2)
     ap.add_argument("--depth", type=int, default=8)
     ap.add_argument("--integrator", default="wavefront", choices=["wavefront", "reference"])
+    ap.add_argument("--rounds", type=int, default=0,
+                    help="wavefront rounds before the tail kernel (0: chosen from the first sample)")
     ap.add_argument("--cache", action="store_true", help="paths end into the learned radiance cache")
     ap.add_argument("--temporal", action="store_true",
                     help="temporal frames of the many-light room: ReSTIR DI (temporal + spatial) and SVGF")
@@ -96,7 +98,7 @@ def main():
     else:
         scene = scenes.box_room_wide(seed=0, width=args.width, height=args.height)
     integrator = abi.INTEGRATOR_WAVEFRONT if args.integrator == "wavefront" else abi.INTEGRATOR_REFERENCE
-    with renderer.CudaOffscreenRenderer(0) as r:
+    with renderer.CudaOffscreenRenderer(0, wavefront_rounds=args.rounds) as r:
         renderer.check(r.update_scene(scene), "update_scene")
         if args.cache:
             r.configure_cache(enable=True, seed=1)
@@ -108,6 +110,7 @@ def main():
             rays = res.camera_rays + res.extension_rays + res.shadow_rays
             counts = [res.wavefront_path_counts[b] for b in range(res.wavefront_path_count_size)]
             print(json.dumps({"frame": k, "rays": rays, "gpu_ms": round(res.gpu_ms, 3),
+                              "wavefront_rounds": res.wavefront_rounds,
                               "mrays_per_s": round(rays / res.gpu_ms / 1e3, 1),
                               "paths_per_bounce": counts}))
 
