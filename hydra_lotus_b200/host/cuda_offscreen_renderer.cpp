@@ -393,6 +393,7 @@ void CudaOffscreenRenderer::FillEvidence(const lotus_frame_desc& f, const lotus_
   e.wavefront_timings.camera_gpu_ms = r.camera_gpu_ms;
   e.wavefront_timings.intersect_gpu_ms = r.extend_gpu_ms;
   e.wavefront_timings.shade_gpu_ms = r.shade_gpu_ms + r.shadow_gpu_ms;
+  e.wavefront_timings.tail_gpu_ms = r.tail_gpu_ms;
   if (r.status == LOTUS_PASS && f.target.read_back) {
     // RGBA32F, top-left rows, linear (vulkan_backend.hpp:30-38).
     Lotus::ColorProduct& c = e.color;
