@@ -994,7 +994,7 @@ uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requ
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
-    SampleProfile* profile, const TraceTuning& tuning, const CacheQueues* cache) {
+    SampleProfile* profile, const TraceTuning& tuning, const CacheQueues* cache, cudaEvent_t before_resolve) {
   CacheQueues C{};
   if (cache && cache->enabled && cache->cache) C = *cache;
   else C.enabled = false;
@@ -1089,10 +1089,27 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     }
   }
   {
+    // The accumulation adds samples in order: a sample in flight beside the
+    // one before it resolves after that one (and its ray totals).
+    if (before_resolve) cudaStreamWaitEvent(stream, before_resolve, 0);
     Timed t(profile, stream, 4);
     k_wf_resolve<false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, accum, color, none);
   }
   k_wf_finish<<<1, 32, 0, stream>>>(const_cast<FrameConst*>(fc), Q.counts, max_bounces, totals);
+}
+
+__global__ void k_next_frame(const FrameConst* __restrict__ fc, FrameConst* __restrict__ next) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  FrameConst f = *fc;
+  if (f.add_sample) {
+    f.sample_index += 1;
+    f.accumulated += 1;
+  }
+  *next = f;
+}
+
+void launch_next_frame(const FrameConst* fc, FrameConst* next, cudaStream_t stream) {
+  k_next_frame<<<1, 32, 0, stream>>>(fc, next);
 }
 
 void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const PathState& P, const Queues& Q,

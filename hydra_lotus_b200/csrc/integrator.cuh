@@ -136,7 +136,11 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
     SampleProfile* profile = nullptr, const TraceTuning& tuning = TraceTuning(),
-    const CacheQueues* cache = nullptr);
+    const CacheQueues* cache = nullptr, cudaEvent_t before_resolve = nullptr);
+
+// The frame constants of the sample after fc's: a copy of *fc advanced by
+// one sample (for two samples in flight at once, each with its own).
+void launch_next_frame(const FrameConst* fc, FrameConst* next, cudaStream_t stream);
 
 // One sample of every scene of a batch, as one set of wavefront launches
 // over all scenes' paths (the wavefront integrator, no radiance cache).

@@ -639,6 +639,15 @@ struct Renderer {
   DeviceArray<uint4> path_hit;
   DeviceArray<uint32_t> queue_ray0, queue_ray1, queue_hit, counts;
   DeviceArray<float4> sq_o, sq_d, sq_fl, sq_thr;
+  // A second path state and queue set, for the second of two samples in
+  // flight at once (RenderScene with two or more samples to add): its
+  // rounds overlap the first one's tail, on a second stream.
+  DeviceArray<float4> path_origin2, path_direction2, path_throughput2, path_radiance2;
+  DeviceArray<uint4> path_hit2;
+  DeviceArray<uint32_t> queue_ray02, queue_ray12, queue_hit2, counts2;
+  DeviceArray<float4> sq_o2, sq_d2, sq_fl2, sq_thr2;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_first_done = nullptr, ev_join = nullptr;
   DeviceArray<FrameConst> frame_const;
   DeviceArray<RayTotals> totals;
   DeviceArray<VisitCounters> visits;
@@ -704,8 +713,8 @@ struct Renderer {
   uint32_t cache_pixels = 0;
   uint32_t cache_generation = 0;  // bumped by every configuration
 
-  // The wavefront sample as a CUDA graph.
-  cudaGraphExec_t graph = nullptr;
+  // The wavefront sample as a CUDA graph, and two samples in flight.
+  cudaGraphExec_t graph = nullptr, graph_pair = nullptr;
   struct GraphKey {
     uint64_t scene_generation;
     uint32_t width, height, max_bounces;
@@ -713,7 +722,7 @@ struct Renderer {
     uint32_t cache;  // the radiance cache's configuration count (0: off)
     uint32_t rounds; // wavefront rounds before the tail kernel
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
-  } graph_key{};
+  } graph_key{}, graph_pair_key{};
   // Rounds before the tail, chosen (choose_wavefront_rounds) from the queue
   // counts of the first sample rendered with `rounds_key` (its rounds field
   // 0), for RenderScene and for the temporal frames.
@@ -723,6 +732,10 @@ struct Renderer {
   ~Renderer() {
     for (cudaEvent_t e : profile_events) cudaEventDestroy(e);
     if (graph) cudaGraphExecDestroy(graph);
+    if (graph_pair) cudaGraphExecDestroy(graph_pair);
+    for (cudaEvent_t e : {ev_fork, ev_first_done, ev_join})
+      if (e) cudaEventDestroy(e);
+    if (stream2) cudaStreamDestroy(stream2);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
     if (stream) cudaStreamDestroy(stream);
@@ -1321,13 +1334,17 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
     R.path_radiance.release(); R.path_hit.release();
     R.queue_ray0.release(); R.queue_ray1.release(); R.queue_hit.release();
     R.sq_o.release(); R.sq_d.release(); R.sq_fl.release(); R.sq_thr.release();
+    R.path_origin2.release(); R.path_direction2.release(); R.path_throughput2.release();
+    R.path_radiance2.release(); R.path_hit2.release();
+    R.queue_ray02.release(); R.queue_ray12.release(); R.queue_hit2.release();
+    R.sq_o2.release(); R.sq_d2.release(); R.sq_fl2.release(); R.sq_thr2.release();
     R.width = w;
     R.height = h;
     R.key_valid = false;
   }
   if (!R.ok(R.accum.resize(n), "accumulation", detail) || !R.ok(R.color.resize(n), "colour", detail) ||
       !R.ok(R.counts.resize(kQueueCounterWords * (LOTUS_MAX_BOUNCES + 2)), "queue counts", detail) ||
-      !R.ok(R.frame_const.resize(1), "frame constants", detail) ||
+      !R.ok(R.frame_const.resize(2), "frame constants", detail) ||
       !R.ok(R.totals.resize(1), "ray totals", detail))
     return false;
   if (wavefront) {
@@ -1343,6 +1360,18 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
       return false;
   }
   return true;
+}
+
+// The second path state and queue set (two samples in flight).
+bool ensure_pair_buffers(Renderer& R, size_t n, std::string& detail) {
+  return R.ok(R.path_origin2.resize(n), "path state", detail) && R.ok(R.path_direction2.resize(n), "path state", detail) &&
+         R.ok(R.path_throughput2.resize(n), "path state", detail) &&
+         R.ok(R.path_radiance2.resize(n), "path state", detail) && R.ok(R.path_hit2.resize(n), "path state", detail) &&
+         R.ok(R.queue_ray02.resize(n), "queues", detail) && R.ok(R.queue_ray12.resize(n), "queues", detail) &&
+         R.ok(R.queue_hit2.resize(n), "queues", detail) && R.ok(R.sq_o2.resize(n), "shadow queue", detail) &&
+         R.ok(R.sq_d2.resize(n), "shadow queue", detail) && R.ok(R.sq_fl2.resize(n), "shadow queue", detail) &&
+         R.ok(R.sq_thr2.resize(n), "shadow queue", detail) &&
+         R.ok(R.counts2.resize(kQueueCounterWords * (LOTUS_MAX_BOUNCES + 2)), "queue counts", detail);
 }
 
 // The radiance cache's queues for targets of `pixels` pixels: a query per
@@ -1568,9 +1597,61 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   TraceTuning tuning = R.tuning;
   if (tuning.rounds == 0 && R.auto_rounds != 0 && R.rounds_key == gk) tuning.rounds = R.auto_rounds;
   const bool choose_rounds = wavefront && R.tuning.rounds == 0 && !(R.rounds_key == gk);
+  // Two samples at a time where two or more are added without the radiance
+  // cache (which trains between samples) and outside the profiled last one:
+  // the second runs on its own path state and stream, beside the first,
+  // and resolves after it.
+  const uint32_t pairable = (wavefront && !use_cache && to_add >= 2)
+      ? submissions - ((want_timings || want_visits) ? 1u : 0u) : 0u;
+  if (pairable >= 2 && !ensure_pair_buffers(R, (size_t)t.width * t.height, detail)) return poison(detail);
+  PathState P2{R.path_origin2.ptr, R.path_direction2.ptr, R.path_throughput2.ptr, R.path_radiance2.ptr,
+      R.path_hit2.ptr};
+  Queues Q2 = Q;
+  Q2.ray[0] = R.queue_ray02.ptr;
+  Q2.ray[1] = R.queue_ray12.ptr;
+  Q2.hit = R.queue_hit2.ptr;
+  Q2.shadow = ShadowQueue{R.sq_o2.ptr, R.sq_d2.ptr, R.sq_fl2.ptr, R.sq_thr2.ptr};
+  Q2.counts = R.counts2.ptr;
+  bool last_in_pair = false;
   cudaEventRecord(R.ev_start, s);
   for (uint32_t k = 0; k < submissions; ++k) {
     const bool profiled = (want_timings || want_visits) && k + 1 == submissions;
+    if (!profiled && k + 2 <= pairable) {
+      gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, false);
+      if (!R.graph_pair || !(R.graph_pair_key == gk)) {
+        if (R.graph_pair) {
+          cudaGraphExecDestroy(R.graph_pair);
+          R.graph_pair = nullptr;
+        }
+        cudaGraph_t g;
+        FrameConst* fc0 = R.frame_const.ptr;
+        FrameConst* fc1 = R.frame_const.ptr + 1;
+        if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
+          return poison(detail);
+        launch_next_frame(fc0, fc1, s);
+        cudaEventRecord(R.ev_fork, s);
+        cudaStreamWaitEvent(R.stream2, R.ev_fork, 0);
+        launch_wavefront_sample(R.view, fc0, rect, t.width, t.height, st.max_bounces, P, Q, R.accum.ptr,
+            R.color.ptr, R.totals.ptr, s, nullptr, tuning, nullptr);
+        cudaEventRecord(R.ev_first_done, s);
+        launch_wavefront_sample(R.view, fc1, rect, t.width, t.height, st.max_bounces, P2, Q2, R.accum.ptr,
+            R.color.ptr, R.totals.ptr, R.stream2, nullptr, tuning, nullptr, R.ev_first_done);
+        cudaEventRecord(R.ev_join, R.stream2);
+        cudaStreamWaitEvent(s, R.ev_join, 0);
+        launch_advance(fc0, s);
+        launch_advance(fc0, s);
+        if (!R.ok(cudaStreamEndCapture(s, &g), "graph capture", detail)) return poison(detail);
+        cudaError_t e = cudaGraphInstantiate(&R.graph_pair, g, 0);
+        cudaGraphDestroy(g);
+        if (!R.ok(e, "graph instantiate", detail)) return poison(detail);
+        R.graph_pair_key = gk;
+      }
+      if (!R.ok(cudaGraphLaunch(R.graph_pair, s), "graph launch", detail)) return poison(detail);
+      ++k;
+      last_in_pair = true;
+      continue;
+    }
+    last_in_pair = false;
     if (profiled) {
       if (wavefront)
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
@@ -1608,7 +1689,9 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   RayTotals totals{};
   std::vector<uint32_t> counts(3 * (size_t)(st.max_bounces + 2), 0);
   cudaMemcpyAsync(&totals, R.totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s);
-  if (wavefront) cudaMemcpyAsync(counts.data(), R.counts.ptr, counts.size() * 4, cudaMemcpyDeviceToHost, s);
+  if (wavefront)
+    cudaMemcpyAsync(counts.data(), last_in_pair ? R.counts2.ptr : R.counts.ptr, counts.size() * 4,
+        cudaMemcpyDeviceToHost, s);
   if (!R.ok(cudaStreamSynchronize(s), "render", detail)) return poison(detail);
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
@@ -1761,6 +1844,10 @@ int32_t lotus_cuda_create(const lotus_cuda_options* options, lotus_cuda_renderer
   std::string detail;
   if (!R.ok(cudaSetDevice(device), "cudaSetDevice", detail) ||
       !R.ok(cudaStreamCreateWithFlags(&R.stream, cudaStreamNonBlocking), "stream", detail) ||
+      !R.ok(cudaStreamCreateWithFlags(&R.stream2, cudaStreamNonBlocking), "stream", detail) ||
+      !R.ok(cudaEventCreateWithFlags(&R.ev_fork, cudaEventDisableTiming), "event", detail) ||
+      !R.ok(cudaEventCreateWithFlags(&R.ev_first_done, cudaEventDisableTiming), "event", detail) ||
+      !R.ok(cudaEventCreateWithFlags(&R.ev_join, cudaEventDisableTiming), "event", detail) ||
       !R.ok(cudaEventCreate(&R.ev_start), "event", detail) || !R.ok(cudaEventCreate(&R.ev_stop), "event", detail)) {
     copy_detail(error, error_size, detail);
     delete h;
