@@ -40,6 +40,19 @@ struct lotus_cuda_batch {
   std::vector<lotus_frame_desc> last;
   std::vector<uint32_t> accumulated;
   std::vector<uint64_t> completion;
+  // A second path state and queue set and per-scene frame constants, for
+  // the second of two samples in flight (its rounds beside the first's
+  // tail, on a second stream; it resolves after the first).
+  void* buffers2[13] = {};
+  uint32_t capacity2 = 0;
+  lotus::PathState P2{};
+  lotus::Queues Q2{};
+  lotus::FrameConst* frames2 = nullptr;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_first = nullptr, ev_join = nullptr;
+  cudaGraphExec_t graph_pair = nullptr;
+  std::vector<uint32_t> pair_layout;
+  uint32_t pair_bounces = 0, pair_rounds = 0;
   // The captured sample.
   cudaGraphExec_t graph = nullptr;
   std::vector<uint32_t> graph_layout;
@@ -66,7 +79,45 @@ void release_buffers(lotus_cuda_batch& b) {
     if (p) cudaFree(p);
     p = nullptr;
   }
+  for (void*& p : b.buffers2) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
   b.capacity = 0;
+  b.capacity2 = 0;
+  if (b.graph_pair) {
+    cudaGraphExecDestroy(b.graph_pair);
+    b.graph_pair = nullptr;
+  }
+}
+
+// The second sample's path state, queues and frame constants.
+cudaError_t ensure_pair_buffers(lotus_cuda_batch& b) {
+  if (b.capacity2 >= b.capacity && b.buffers2[0]) return cudaSuccess;
+  const size_t n = std::max<uint32_t>(b.capacity, 1);
+  const size_t sizes[13] = {16 * n, 16 * n, 16 * n, 16 * n, 16 * n, 4 * n, 4 * n, 4 * n, 16 * n, 16 * n, 16 * n,
+      16 * n + sizeof(uint32_t) * kQueueCounterWords * (LOTUS_MAX_BOUNCES + 2), sizeof(FrameConst) * kMaxScenes};
+  for (int i = 0; i < 13; ++i) {
+    if (b.buffers2[i]) cudaFree(b.buffers2[i]);
+    b.buffers2[i] = nullptr;
+    const cudaError_t e = cudaMalloc(&b.buffers2[i], sizes[i]);
+    if (e != cudaSuccess) return e;
+  }
+  auto f4 = [&](int i) { return static_cast<float4*>(b.buffers2[i]); };
+  b.P2 = PathState{f4(0), f4(1), f4(2), f4(3), static_cast<uint4*>(b.buffers2[4])};
+  b.Q2 = b.Q;
+  b.Q2.ray[0] = static_cast<uint32_t*>(b.buffers2[5]);
+  b.Q2.ray[1] = static_cast<uint32_t*>(b.buffers2[6]);
+  b.Q2.hit = static_cast<uint32_t*>(b.buffers2[7]);
+  b.Q2.shadow = ShadowQueue{f4(8), f4(9), f4(10), f4(11)};
+  b.Q2.counts = reinterpret_cast<uint32_t*>(static_cast<char*>(b.buffers2[11]) + 16 * n);
+  b.frames2 = static_cast<FrameConst*>(b.buffers2[12]);
+  b.capacity2 = (uint32_t)n;
+  if (b.graph_pair) {
+    cudaGraphExecDestroy(b.graph_pair);
+    b.graph_pair = nullptr;
+  }
+  return cudaSuccess;
 }
 
 // The combined state for `pixels` path slots and `scenes` scenes.
@@ -143,6 +194,10 @@ extern "C" int32_t lotus_cuda_batch_create(const lotus_cuda_options* options, lo
     b->tuning.rounds = options->wavefront_rounds;
   }
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev_first, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&b->ev_start) != cudaSuccess || cudaEventCreate(&b->ev_stop) != cudaSuccess) {
     set_detail(error, error_size, "stream or event creation failed");
     lotus_cuda_batch_destroy(b);
@@ -161,6 +216,9 @@ extern "C" void lotus_cuda_batch_destroy(lotus_cuda_batch* b) {
   destroy_scenes(*b);
   if (b->ev_start) cudaEventDestroy(b->ev_start);
   if (b->ev_stop) cudaEventDestroy(b->ev_stop);
+  for (cudaEvent_t e : {b->ev_fork, b->ev_first, b->ev_join})
+    if (e) cudaEventDestroy(e);
+  if (b->stream2) cudaStreamDestroy(b->stream2);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -169,10 +227,14 @@ extern "C" int32_t lotus_cuda_batch_set_tuning(lotus_cuda_batch* b, uint32_t ref
   if (!b || refill_below > 32 || blocks_per_sm > 64) return LOTUS_FAIL;
   b->tuning.refill_below = refill_below;
   b->tuning.blocks_per_sm = blocks_per_sm;
+  cudaSetDevice(b->device);
   if (b->graph) {
-    cudaSetDevice(b->device);
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
+  }
+  if (b->graph_pair) {
+    cudaGraphExecDestroy(b->graph_pair);
+    b->graph_pair = nullptr;
   }
   return LOTUS_PASS;
 }
@@ -195,6 +257,10 @@ extern "C" int32_t lotus_cuda_batch_set_scenes(lotus_cuda_batch* b, const lotus_
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
+  }
+  if (b->graph_pair) {
+    cudaGraphExecDestroy(b->graph_pair);
+    b->graph_pair = nullptr;
   }
   int32_t status = LOTUS_PASS;
   for (uint32_t k = 0; k < count; ++k) {
@@ -334,17 +400,59 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
     b->graph_bounces = max_bounces;
     b->graph_rounds = rounds;
   }
+  // Two samples in flight (as lotus_cuda_render keeps them): the second on
+  // its own path state, queues, frame constants and stream, resolving after
+  // the first.
+  const bool pairs = frame_count >= 2;
+  if (pairs && (e = ensure_pair_buffers(*b)) != cudaSuccess)
+    return fail(std::string("batch buffers: ") + cudaGetErrorString(e), true);
+  Queues Q2 = b->Q2;
+  Q2.capacity = base[count];
+  if (pairs && (!b->graph_pair || b->pair_layout != layout || b->pair_bounces != max_bounces ||
+                   b->pair_rounds != rounds)) {
+    if (b->graph_pair) {
+      cudaGraphExecDestroy(b->graph_pair);
+      b->graph_pair = nullptr;
+    }
+    SceneTable B2 = B;
+    B2.frames = b->frames2;
+    cudaGraph_t g;
+    if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return fail(std::string("graph capture: ") + cudaGetErrorString(e), true);
+    launch_next_frames(b->frames, b->frames2, count, s);
+    cudaEventRecord(b->ev_fork, s);
+    cudaStreamWaitEvent(b->stream2, b->ev_fork, 0);
+    launch_wavefront_batch(B, max_bounces, b->P, Q, b->accum, b->color, b->totals, s, tuning);
+    cudaEventRecord(b->ev_first, s);
+    launch_wavefront_batch(B2, max_bounces, b->P2, Q2, b->accum, b->color, b->totals, b->stream2, tuning,
+        b->ev_first);
+    cudaEventRecord(b->ev_join, b->stream2);
+    cudaStreamWaitEvent(s, b->ev_join, 0);
+    launch_advance_batch(B, s);
+    if ((e = cudaStreamEndCapture(s, &g)) != cudaSuccess)
+      return fail(std::string("graph capture: ") + cudaGetErrorString(e), true);
+    e = cudaGraphInstantiate(&b->graph_pair, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(std::string("graph instantiate: ") + cudaGetErrorString(e), true);
+    b->pair_layout = layout;
+    b->pair_bounces = max_bounces;
+    b->pair_rounds = rounds;
+  }
+  bool last_pair = false;
   cudaEventRecord(b->ev_start, s);
-  for (uint32_t i = 0; i < frame_count; ++i)
-    if ((e = cudaGraphLaunch(b->graph, s)) != cudaSuccess)
+  for (uint32_t i = 0; i < frame_count;) {
+    last_pair = i + 2 <= frame_count;
+    if ((e = cudaGraphLaunch(last_pair ? b->graph_pair : b->graph, s)) != cudaSuccess)
       return fail(std::string("graph launch: ") + cudaGetErrorString(e), true);
+    i += last_pair ? 2 : 1;
+  }
   cudaEventRecord(b->ev_stop, s);
   RayTotals totals{};
   cudaMemcpyAsync(&totals, b->totals, sizeof(totals), cudaMemcpyDeviceToHost, s);
   std::vector<uint32_t> counts;
   if (choose_rounds) {
     counts.assign(3 * (size_t)(max_bounces + 2), 0u);
-    cudaMemcpyAsync(counts.data(), Q.counts, counts.size() * 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(counts.data(), last_pair ? Q2.counts : Q.counts, counts.size() * 4, cudaMemcpyDeviceToHost, s);
   }
   for (uint32_t k = 0; colors && k < count; ++k)
     if (colors[k] && frames[k].target.read_back)

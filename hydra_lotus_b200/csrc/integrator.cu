@@ -1112,8 +1112,28 @@ void launch_next_frame(const FrameConst* fc, FrameConst* next, cudaStream_t stre
   k_next_frame<<<1, 32, 0, stream>>>(fc, next);
 }
 
+__global__ void k_next_frames(const FrameConst* __restrict__ frames, FrameConst* __restrict__ next, uint32_t count) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  FrameConst f = frames[k];
+  if (f.add_sample) {
+    f.sample_index += 1;
+    f.accumulated += 1;
+  }
+  next[k] = f;
+}
+
+void launch_next_frames(const FrameConst* frames, FrameConst* next, uint32_t count, cudaStream_t stream) {
+  k_next_frames<<<(count + 31) / 32, 32, 0, stream>>>(frames, next, count);
+}
+
+void launch_advance_batch(const SceneTable& B, cudaStream_t stream) {
+  k_advance_batch<<<(B.count + 31) / 32, 32, 0, stream>>>(B);
+}
+
 void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const PathState& P, const Queues& Q,
-    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream, const TraceTuning& tuning) {
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream, const TraceTuning& tuning,
+    cudaEvent_t before_resolve) {
   if (B.count == 0 || B.total_slots == 0) return;
   const SceneView none_view{};
   const FrameConst* no_frame = nullptr;
@@ -1151,6 +1171,7 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
     else
       k_wf_tail<true, false><<<grid_tail, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rounds, cursor, B);
   }
+  if (before_resolve) cudaStreamWaitEvent(stream, before_resolve, 0);
   k_wf_resolve<true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, accum, color, B);
   k_wf_finish_batch<<<1, 32, 0, stream>>>(B, Q.counts, max_bounces, totals);
   k_advance_batch<<<(B.count + 31) / 32, 32, 0, stream>>>(B);

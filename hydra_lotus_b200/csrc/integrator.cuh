@@ -145,7 +145,13 @@ void launch_next_frame(const FrameConst* fc, FrameConst* next, cudaStream_t stre
 // One sample of every scene of a batch, as one set of wavefront launches
 // over all scenes' paths (the wavefront integrator, no radiance cache).
 void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const PathState& P, const Queues& Q,
-    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream, const TraceTuning& tuning);
+    double4* accum, float4* color, RayTotals* totals, cudaStream_t stream, const TraceTuning& tuning,
+    cudaEvent_t before_resolve = nullptr);
+
+// Every scene's frame constants advanced by one sample into `next` (the
+// batch's second sample in flight), and every scene's sample advanced.
+void launch_next_frames(const FrameConst* frames, FrameConst* next, uint32_t count, cudaStream_t stream);
+void launch_advance_batch(const SceneTable& B, cudaStream_t stream);
 
 // Deferred visibility of the ReSTIR passes. Each pass queues the shadow
 // ray of every pixel whose selected sample needs one (origin and distance,
