@@ -570,6 +570,10 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
 
 }  // namespace
 
+// The longest chain of samples one RenderScene graph holds (two in flight
+// at a time): each sample has its own frame constants.
+constexpr uint32_t kMaxChain = 16;
+
 // The resident scene as the incremental updates need it: each geometry's
 // arrays (owned copies; `geometries` points into them), its box and its
 // places in the device arrays and pools, the materials and the
@@ -648,6 +652,8 @@ struct Renderer {
   DeviceArray<float4> sq_o2, sq_d2, sq_fl2, sq_thr2;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_first_done = nullptr, ev_join = nullptr;
+  std::vector<cudaEvent_t> ev_sample_done;  // per sample of a chain: resolved and counted
+  uint32_t chain_length = 0;                // samples in graph_pair
   DeviceArray<FrameConst> frame_const;
   DeviceArray<RayTotals> totals;
   DeviceArray<VisitCounters> visits;
@@ -735,6 +741,7 @@ struct Renderer {
     if (graph_pair) cudaGraphExecDestroy(graph_pair);
     for (cudaEvent_t e : {ev_fork, ev_first_done, ev_join})
       if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_sample_done) cudaEventDestroy(e);
     if (stream2) cudaStreamDestroy(stream2);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
@@ -1344,7 +1351,7 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
   }
   if (!R.ok(R.accum.resize(n), "accumulation", detail) || !R.ok(R.color.resize(n), "colour", detail) ||
       !R.ok(R.counts.resize(kQueueCounterWords * (LOTUS_MAX_BOUNCES + 2)), "queue counts", detail) ||
-      !R.ok(R.frame_const.resize(2), "frame constants", detail) ||
+      !R.ok(R.frame_const.resize(kMaxChain), "frame constants", detail) ||
       !R.ok(R.totals.resize(1), "ray totals", detail))
     return false;
   if (wavefront) {
@@ -1603,6 +1610,11 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   // and resolves after it.
   const uint32_t pairable = (wavefront && !use_cache && to_add >= 2)
       ? submissions - ((want_timings || want_visits) ? 1u : 0u) : 0u;
+  while (R.ev_sample_done.size() < kMaxChain) {
+    cudaEvent_t e;
+    if (!R.ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event", detail)) return poison(detail);
+    R.ev_sample_done.push_back(e);
+  }
   if (pairable >= 2 && !ensure_pair_buffers(R, (size_t)t.width * t.height, detail)) return poison(detail);
   PathState P2{R.path_origin2.ptr, R.path_direction2.ptr, R.path_throughput2.ptr, R.path_radiance2.ptr,
       R.path_hit2.ptr};
@@ -1617,37 +1629,43 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   for (uint32_t k = 0; k < submissions; ++k) {
     const bool profiled = (want_timings || want_visits) && k + 1 == submissions;
     if (!profiled && k + 2 <= pairable) {
+      // A chain of `length` samples (even, at most kMaxChain): sample j on
+      // path state j % 2 and stream j % 2 with frame constants fc0 advanced
+      // by j; each resolves after sample j - 1, so only the chain's last
+      // tail is not overlapped by another sample's rounds.
+      const uint32_t length = std::min(kMaxChain, (pairable - k) & ~1u);
       gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, false);
-      if (!R.graph_pair || !(R.graph_pair_key == gk)) {
+      if (!R.graph_pair || !(R.graph_pair_key == gk) || R.chain_length != length) {
         if (R.graph_pair) {
           cudaGraphExecDestroy(R.graph_pair);
           R.graph_pair = nullptr;
         }
         cudaGraph_t g;
-        FrameConst* fc0 = R.frame_const.ptr;
-        FrameConst* fc1 = R.frame_const.ptr + 1;
+        FrameConst* fc = R.frame_const.ptr;
         if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
           return poison(detail);
-        launch_next_frame(fc0, fc1, s);
+        for (uint32_t j = 1; j < length; ++j) launch_next_frame(fc + j - 1, fc + j, s);
         cudaEventRecord(R.ev_fork, s);
         cudaStreamWaitEvent(R.stream2, R.ev_fork, 0);
-        launch_wavefront_sample(R.view, fc0, rect, t.width, t.height, st.max_bounces, P, Q, R.accum.ptr,
-            R.color.ptr, R.totals.ptr, s, nullptr, tuning, nullptr);
-        cudaEventRecord(R.ev_first_done, s);
-        launch_wavefront_sample(R.view, fc1, rect, t.width, t.height, st.max_bounces, P2, Q2, R.accum.ptr,
-            R.color.ptr, R.totals.ptr, R.stream2, nullptr, tuning, nullptr, R.ev_first_done);
+        for (uint32_t j = 0; j < length; ++j) {
+          const bool second = (j & 1u) != 0;
+          launch_wavefront_sample(R.view, fc + j, rect, t.width, t.height, st.max_bounces, second ? P2 : P,
+              second ? Q2 : Q, R.accum.ptr, R.color.ptr, R.totals.ptr, second ? R.stream2 : s, nullptr, tuning,
+              nullptr, j ? R.ev_sample_done[j - 1] : nullptr);
+          cudaEventRecord(R.ev_sample_done[j], second ? R.stream2 : s);
+        }
         cudaEventRecord(R.ev_join, R.stream2);
         cudaStreamWaitEvent(s, R.ev_join, 0);
-        launch_advance(fc0, s);
-        launch_advance(fc0, s);
+        for (uint32_t j = 0; j < length; ++j) launch_advance(fc, s);
         if (!R.ok(cudaStreamEndCapture(s, &g), "graph capture", detail)) return poison(detail);
         cudaError_t e = cudaGraphInstantiate(&R.graph_pair, g, 0);
         cudaGraphDestroy(g);
         if (!R.ok(e, "graph instantiate", detail)) return poison(detail);
         R.graph_pair_key = gk;
+        R.chain_length = length;
       }
       if (!R.ok(cudaGraphLaunch(R.graph_pair, s), "graph launch", detail)) return poison(detail);
-      ++k;
+      k += length - 1;
       last_in_pair = true;
       continue;
     }
