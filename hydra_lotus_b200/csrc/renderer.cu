@@ -651,9 +651,9 @@ struct Renderer {
   DeviceArray<uint32_t> queue_ray02, queue_ray12, queue_hit2, counts2;
   DeviceArray<float4> sq_o2, sq_d2, sq_fl2, sq_thr2;
   cudaStream_t stream2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_first_done = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<cudaEvent_t> ev_sample_done;  // per sample of a chain: resolved and counted
-  uint32_t chain_length = 0;                // samples in graph_pair
+  uint32_t chain_length = 0;                // samples in graph_chain
   DeviceArray<FrameConst> frame_const;
   DeviceArray<RayTotals> totals;
   DeviceArray<VisitCounters> visits;
@@ -720,7 +720,7 @@ struct Renderer {
   uint32_t cache_generation = 0;  // bumped by every configuration
 
   // The wavefront sample as a CUDA graph, and two samples in flight.
-  cudaGraphExec_t graph = nullptr, graph_pair = nullptr;
+  cudaGraphExec_t graph = nullptr, graph_chain = nullptr;
   struct GraphKey {
     uint64_t scene_generation;
     uint32_t width, height, max_bounces;
@@ -728,7 +728,7 @@ struct Renderer {
     uint32_t cache;  // the radiance cache's configuration count (0: off)
     uint32_t rounds; // wavefront rounds before the tail kernel
     bool operator==(const GraphKey& o) const { return std::memcmp(this, &o, sizeof(GraphKey)) == 0; }
-  } graph_key{}, graph_pair_key{};
+  } graph_key{}, graph_chain_key{};
   // Rounds before the tail, chosen (choose_wavefront_rounds) from the queue
   // counts of the first sample rendered with `rounds_key` (its rounds field
   // 0), for RenderScene and for the temporal frames.
@@ -738,8 +738,8 @@ struct Renderer {
   ~Renderer() {
     for (cudaEvent_t e : profile_events) cudaEventDestroy(e);
     if (graph) cudaGraphExecDestroy(graph);
-    if (graph_pair) cudaGraphExecDestroy(graph_pair);
-    for (cudaEvent_t e : {ev_fork, ev_first_done, ev_join})
+    if (graph_chain) cudaGraphExecDestroy(graph_chain);
+    for (cudaEvent_t e : {ev_fork, ev_join})
       if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ev_sample_done) cudaEventDestroy(e);
     if (stream2) cudaStreamDestroy(stream2);
@@ -1608,14 +1608,14 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   // cache (which trains between samples) and outside the profiled last one:
   // the second runs on its own path state and stream, beside the first,
   // and resolves after it.
-  const uint32_t pairable = (wavefront && !use_cache && to_add >= 2)
+  const uint32_t chainable = (wavefront && !use_cache && to_add >= 2)
       ? submissions - ((want_timings || want_visits) ? 1u : 0u) : 0u;
   while (R.ev_sample_done.size() < kMaxChain) {
     cudaEvent_t e;
     if (!R.ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event", detail)) return poison(detail);
     R.ev_sample_done.push_back(e);
   }
-  if (pairable >= 2 && !ensure_pair_buffers(R, (size_t)t.width * t.height, detail)) return poison(detail);
+  if (chainable >= 2 && !ensure_pair_buffers(R, (size_t)t.width * t.height, detail)) return poison(detail);
   PathState P2{R.path_origin2.ptr, R.path_direction2.ptr, R.path_throughput2.ptr, R.path_radiance2.ptr,
       R.path_hit2.ptr};
   Queues Q2 = Q;
@@ -1624,21 +1624,21 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   Q2.hit = R.queue_hit2.ptr;
   Q2.shadow = ShadowQueue{R.sq_o2.ptr, R.sq_d2.ptr, R.sq_fl2.ptr, R.sq_thr2.ptr};
   Q2.counts = R.counts2.ptr;
-  bool last_in_pair = false;
+  bool last_in_chain = false;
   cudaEventRecord(R.ev_start, s);
   for (uint32_t k = 0; k < submissions; ++k) {
     const bool profiled = (want_timings || want_visits) && k + 1 == submissions;
-    if (!profiled && k + 2 <= pairable) {
+    if (!profiled && k + 2 <= chainable) {
       // A chain of `length` samples (even, at most kMaxChain): sample j on
       // path state j % 2 and stream j % 2 with frame constants fc0 advanced
       // by j; each resolves after sample j - 1, so only the chain's last
       // tail is not overlapped by another sample's rounds.
-      const uint32_t length = std::min(kMaxChain, (pairable - k) & ~1u);
+      const uint32_t length = std::min(kMaxChain, (chainable - k) & ~1u);
       gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, false);
-      if (!R.graph_pair || !(R.graph_pair_key == gk) || R.chain_length != length) {
-        if (R.graph_pair) {
-          cudaGraphExecDestroy(R.graph_pair);
-          R.graph_pair = nullptr;
+      if (!R.graph_chain || !(R.graph_chain_key == gk) || R.chain_length != length) {
+        if (R.graph_chain) {
+          cudaGraphExecDestroy(R.graph_chain);
+          R.graph_chain = nullptr;
         }
         cudaGraph_t g;
         FrameConst* fc = R.frame_const.ptr;
@@ -1658,18 +1658,18 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
         cudaStreamWaitEvent(s, R.ev_join, 0);
         for (uint32_t j = 0; j < length; ++j) launch_advance(fc, s);
         if (!R.ok(cudaStreamEndCapture(s, &g), "graph capture", detail)) return poison(detail);
-        cudaError_t e = cudaGraphInstantiate(&R.graph_pair, g, 0);
+        cudaError_t e = cudaGraphInstantiate(&R.graph_chain, g, 0);
         cudaGraphDestroy(g);
         if (!R.ok(e, "graph instantiate", detail)) return poison(detail);
-        R.graph_pair_key = gk;
+        R.graph_chain_key = gk;
         R.chain_length = length;
       }
-      if (!R.ok(cudaGraphLaunch(R.graph_pair, s), "graph launch", detail)) return poison(detail);
+      if (!R.ok(cudaGraphLaunch(R.graph_chain, s), "graph launch", detail)) return poison(detail);
       k += length - 1;
-      last_in_pair = true;
+      last_in_chain = true;
       continue;
     }
-    last_in_pair = false;
+    last_in_chain = false;
     if (profiled) {
       if (wavefront)
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
@@ -1708,7 +1708,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   std::vector<uint32_t> counts(3 * (size_t)(st.max_bounces + 2), 0);
   cudaMemcpyAsync(&totals, R.totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s);
   if (wavefront)
-    cudaMemcpyAsync(counts.data(), last_in_pair ? R.counts2.ptr : R.counts.ptr, counts.size() * 4,
+    cudaMemcpyAsync(counts.data(), last_in_chain ? R.counts2.ptr : R.counts.ptr, counts.size() * 4,
         cudaMemcpyDeviceToHost, s);
   if (!R.ok(cudaStreamSynchronize(s), "render", detail)) return poison(detail);
   float ms = 0.0f;
@@ -1864,7 +1864,6 @@ int32_t lotus_cuda_create(const lotus_cuda_options* options, lotus_cuda_renderer
       !R.ok(cudaStreamCreateWithFlags(&R.stream, cudaStreamNonBlocking), "stream", detail) ||
       !R.ok(cudaStreamCreateWithFlags(&R.stream2, cudaStreamNonBlocking), "stream", detail) ||
       !R.ok(cudaEventCreateWithFlags(&R.ev_fork, cudaEventDisableTiming), "event", detail) ||
-      !R.ok(cudaEventCreateWithFlags(&R.ev_first_done, cudaEventDisableTiming), "event", detail) ||
       !R.ok(cudaEventCreateWithFlags(&R.ev_join, cudaEventDisableTiming), "event", detail) ||
       !R.ok(cudaEventCreate(&R.ev_start), "event", detail) || !R.ok(cudaEventCreate(&R.ev_stop), "event", detail)) {
     copy_detail(error, error_size, detail);
