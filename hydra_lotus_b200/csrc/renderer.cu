@@ -1603,6 +1603,8 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   gk.cache = use_cache ? R.cache_generation : 0u;
   TraceTuning tuning = R.tuning;
   if (tuning.rounds == 0 && R.auto_rounds != 0 && R.rounds_key == gk) tuning.rounds = R.auto_rounds;
+  // The rounds the call's last sample ran (the frame result reports them).
+  uint32_t last_rounds = wavefront_rounds(st.max_bounces, want_visits, tuning.rounds, use_cache);
   const bool choose_rounds = wavefront && R.tuning.rounds == 0 && !(R.rounds_key == gk);
   // Two samples at a time where two or more are added without the radiance
   // cache (which trains between samples) and outside the profiled last one:
@@ -1670,6 +1672,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
       continue;
     }
     last_in_chain = false;
+    last_rounds = wavefront_rounds(st.max_bounces, profiled && want_visits, tuning.rounds, use_cache);
     if (profiled) {
       if (wavefront)
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
@@ -1778,7 +1781,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
       if (c) last = b + 1;
     }
     res.wavefront_path_count_size = last;
-    res.wavefront_rounds = wavefront_rounds(st.max_bounces, want_visits, tuning.rounds, use_cache);
+    res.wavefront_rounds = last_rounds;
     if (choose_rounds) {
       gk.rounds = 0;
       R.rounds_key = gk;
