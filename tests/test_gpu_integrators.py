@@ -142,3 +142,22 @@ def test_tail_kernel_paths_match_oracle(cuda, renderer, oracle_lib, name, light_
     assert np.array_equal(color, color2)
     assert list(res.wavefront_path_counts[:64]) == list(counted.wavefront_path_counts[:64])
     assert (res.extension_rays, res.shadow_rays) == (counted.extension_rays, counted.shadow_rays)
+
+
+@pytest.mark.parametrize("frames", [2, 7, 16, 35])
+def test_sample_chains_equal_one_sample_at_a_time(cuda, renderer, frames):
+    """A call that adds several samples runs them two in flight, in chains of
+    up to 16 (each resolving after the one before): its image is bit for bit
+    the one `frames` calls of one sample give, the FP64 accumulation adding
+    the samples in the same order."""
+    scene = scenes.lit_room(seed=5, size=64)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=12, sample_index=300)
+    res, chained = render(cuda, renderer, scene, st, frame_count=frames)
+    assert res.samples_per_pixel == frames
+    cuda.check(renderer.update_scene(scene), "update_scene")
+    for k in range(frames):
+        res, single = renderer.render_scene(scene.frame(st, 1))
+        cuda.check(res, "one sample")
+    assert res.samples_per_pixel == frames
+    assert np.array_equal(chained, single), f"{np.count_nonzero(chained != single)} values differ"
