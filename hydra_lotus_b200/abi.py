@@ -32,7 +32,7 @@ FRAME_COUNT_VISITS = 2
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 # lotus_settings::output (SceneOutput).
 OUTPUT_RADIANCE = 0
@@ -213,7 +213,7 @@ class FrameResult(C.Structure):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("flags", C.c_uint32), ("bvh_leaf_size", C.c_uint32),
                 ("trace_refill_below", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32),
-                ("wavefront_rounds", C.c_uint32)]
+                ("wavefront_rounds", C.c_uint32), ("traversal_step_limit", C.c_uint32)]
 
 
 class TemporalDesc(C.Structure):

@@ -347,10 +347,18 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
   if (e != cudaSuccess) return fail(std::string("batch buffers: ") + cudaGetErrorString(e), true);
   std::vector<SceneView> views(count);
   bool analytic = false;
+  // Every scene's walks report to the first scene's walk-failure words.
+  uint32_t* walk_failure = nullptr;
+  uint32_t step_limit = 0;
   for (uint32_t k = 0; k < count; ++k) {
     RendererAccess a;
     if (!renderer_access(b->scenes[k], a, detail)) return fail("scene " + std::to_string(k) + ": " + detail);
     views[k] = *a.view;
+    if (!walk_failure) {
+      walk_failure = a.view->walk_failure;
+      step_limit = a.step_limit;
+    }
+    views[k].walk_failure = walk_failure;
     analytic = analytic || a.view->analytic_count != 0;
   }
   SceneTable B;
@@ -374,7 +382,8 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
           cudaSuccess ||
       (e = cudaMemcpyAsync(b->slot_base, base.data(), sizeof(uint32_t) * (count + 1), cudaMemcpyHostToDevice, s)) !=
           cudaSuccess ||
-      (e = cudaMemsetAsync(b->totals, 0, sizeof(RayTotals), s)) != cudaSuccess)
+      (e = cudaMemsetAsync(b->totals, 0, sizeof(RayTotals), s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(walk_failure, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess)
     return fail(std::string("batch upload: ") + cudaGetErrorString(e), true);
   // One graph per layout and round count: the sample over every scene.
   TraceTuning tuning = b->tuning;
@@ -449,6 +458,8 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
   cudaEventRecord(b->ev_stop, s);
   RayTotals totals{};
   cudaMemcpyAsync(&totals, b->totals, sizeof(totals), cudaMemcpyDeviceToHost, s);
+  uint32_t walks[2] = {0, 0};
+  cudaMemcpyAsync(walks, walk_failure, sizeof(walks), cudaMemcpyDeviceToHost, s);
   std::vector<uint32_t> counts;
   if (choose_rounds) {
     counts.assign(3 * (size_t)(max_bounces + 2), 0u);
@@ -460,6 +471,7 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
           cudaMemcpyDeviceToHost, s);
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
     return fail(std::string("batch render: ") + cudaGetErrorString(e), true);
+  if (walks[0]) return fail(walk_failure_detail(walks, step_limit), true);
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
   if (choose_rounds) {

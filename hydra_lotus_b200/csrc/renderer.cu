@@ -657,6 +657,10 @@ struct Renderer {
   DeviceArray<FrameConst> frame_const;
   DeviceArray<RayTotals> totals;
   DeviceArray<VisitCounters> visits;
+  // SceneView::walk_failure: failed BVH walks and their causes, cleared
+  // before and read after each frame.
+  DeviceArray<uint32_t> walk_failure;
+  uint32_t step_limit = kMaxTraversalSteps;
   // Profiling events, created on first use.
   std::vector<cudaEvent_t> profile_events;
   std::vector<int> profile_kinds;
@@ -1023,6 +1027,8 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
   v.analytic_count = (uint32_t)in.table.analytic.size();
   v.light_node_count = (uint32_t)in.table.nodes.size();
   v.distant_count = (uint32_t)in.table.distant.size();
+  v.step_limit = R.step_limit;
+  v.walk_failure = R.walk_failure.ptr;
   return true;
 }
 
@@ -1424,6 +1430,30 @@ CacheQueues cache_queues(Renderer& R) {
   return C;
 }
 
+}  // namespace
+
+namespace lotus {
+
+// The detail for a frame whose BVH walks failed (the two words of
+// SceneView::walk_failure), or "" when none did.
+std::string walk_failure_detail(const uint32_t words[2], uint32_t step_limit) {
+  if (words[0] == 0) return std::string();
+  std::string causes;
+  if (words[1] & kWalkFailedStack)
+    causes += "a traversal stack overflowed (" + std::to_string(kStackSize) + " entries)";
+  if (words[1] & kWalkFailedSteps) {
+    if (!causes.empty()) causes += " and ";
+    causes += "a walk ran out of its " + std::to_string(step_limit) + " steps";
+  }
+  return std::to_string(words[0]) + " BVH walk(s) ended early, so the frame's hits are incomplete: " + causes;
+}
+
+}  // namespace lotus
+
+namespace {
+
+using namespace lotus;
+
 int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, float* color_out) {
   std::string detail;
   auto fail = [&](const std::string& msg) {
@@ -1503,14 +1533,19 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     if (!R.ok(cudaMemcpyAsync(R.frame_const.ptr, &fc, sizeof(fc), cudaMemcpyHostToDevice, s), "frame constants",
             detail))
       return poison(detail);
+    if (!R.ok(cudaMemsetAsync(R.walk_failure.ptr, 0, 2 * sizeof(uint32_t), s), "walk failure words", detail))
+      return poison(detail);
     launch_clear_color(R.color.ptr, t.width * t.height,
         make_float4(t.clear_color[0], t.clear_color[1], t.clear_color[2], t.clear_color[3]), s);
     cudaEventRecord(R.ev_start, s);
     launch_diagnostic(R.view, R.frame_const.ptr, rect, st.output, R.color.ptr, s);
     cudaEventRecord(R.ev_stop, s);
+    uint32_t walks[2] = {0, 0};
+    cudaMemcpyAsync(walks, R.walk_failure.ptr, sizeof(walks), cudaMemcpyDeviceToHost, s);
     if (!R.ok(cudaGetLastError(), "diagnostic output", detail) ||
         !R.ok(cudaStreamSynchronize(s), "diagnostic output", detail))
       return poison(detail);
+    if (walks[0]) return poison(walk_failure_detail(walks, R.step_limit));
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
     if (t.read_back && color_out) {
@@ -1555,7 +1590,8 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   fc.add_sample = to_add > 0 ? 1u : 0u;
   cudaStream_t s = R.stream;
   if (!R.ok(cudaMemcpyAsync(R.frame_const.ptr, &fc, sizeof(fc), cudaMemcpyHostToDevice, s), "frame constants", detail) ||
-      !R.ok(cudaMemsetAsync(R.totals.ptr, 0, sizeof(RayTotals), s), "ray totals", detail))
+      !R.ok(cudaMemsetAsync(R.totals.ptr, 0, sizeof(RayTotals), s), "ray totals", detail) ||
+      !R.ok(cudaMemsetAsync(R.walk_failure.ptr, 0, 2 * sizeof(uint32_t), s), "walk failure words", detail))
     return poison(detail);
   if (rect[2] < t.width || rect[3] < t.height || rect[2] == 0)
     launch_clear_color(R.color.ptr, t.width * t.height,
@@ -1708,12 +1744,15 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   }
   cudaEventRecord(R.ev_stop, s);
   RayTotals totals{};
+  uint32_t walks[2] = {0, 0};
   std::vector<uint32_t> counts(3 * (size_t)(st.max_bounces + 2), 0);
   cudaMemcpyAsync(&totals, R.totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(walks, R.walk_failure.ptr, sizeof(walks), cudaMemcpyDeviceToHost, s);
   if (wavefront)
     cudaMemcpyAsync(counts.data(), last_in_chain ? R.counts2.ptr : R.counts.ptr, counts.size() * 4,
         cudaMemcpyDeviceToHost, s);
   if (!R.ok(cudaStreamSynchronize(s), "render", detail)) return poison(detail);
+  if (walks[0]) return poison(walk_failure_detail(walks, R.step_limit));
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, R.ev_start, R.ev_stop);
   if (use_cache) {
@@ -1861,9 +1900,12 @@ int32_t lotus_cuda_create(const lotus_cuda_options* options, lotus_cuda_renderer
     R.tuning.refill_below = options->trace_refill_below;
     R.tuning.blocks_per_sm = options->trace_blocks_per_sm;
     R.tuning.rounds = options->wavefront_rounds;
+    if (options->traversal_step_limit) R.step_limit = options->traversal_step_limit;
   }
   std::string detail;
   if (!R.ok(cudaSetDevice(device), "cudaSetDevice", detail) ||
+      !R.ok(R.walk_failure.resize(2), "walk failure words", detail) ||
+      !R.ok(cudaMemset(R.walk_failure.ptr, 0, 2 * sizeof(uint32_t)), "walk failure words", detail) ||
       !R.ok(cudaStreamCreateWithFlags(&R.stream, cudaStreamNonBlocking), "stream", detail) ||
       !R.ok(cudaStreamCreateWithFlags(&R.stream2, cudaStreamNonBlocking), "stream", detail) ||
       !R.ok(cudaEventCreateWithFlags(&R.ev_fork, cudaEventDisableTiming), "event", detail) ||
@@ -2008,7 +2050,13 @@ bool renderer_access(lotus_cuda_renderer* r, RendererAccess& out, std::string& d
   out.stream = R.stream;
   out.view = &R.view;
   out.tuning = R.tuning;
+  out.step_limit = R.step_limit;
+  out.cache_enabled = R.cache_enabled;
   return true;
+}
+
+void renderer_poison(lotus_cuda_renderer* r, const std::string& detail) {
+  if (r && r->r.failure.empty()) r->r.failure = detail;
 }
 
 bool make_frame_constants(const lotus_frame_desc& d, FrameConst& fc, uint32_t rect[4],
@@ -2240,7 +2288,8 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   cudaStream_t s = R.stream;
   if (!R.ok(cudaMemcpyAsync(R.frame_const.ptr, &fc, sizeof(fc), cudaMemcpyHostToDevice, s), "frame constants", detail) ||
       !R.ok(cudaMemcpyAsync(T.constants.ptr, &tc, sizeof(tc), cudaMemcpyHostToDevice, s), "temporal constants", detail) ||
-      !R.ok(cudaMemsetAsync(R.totals.ptr, 0, sizeof(RayTotals), s), "ray totals", detail))
+      !R.ok(cudaMemsetAsync(R.totals.ptr, 0, sizeof(RayTotals), s), "ray totals", detail) ||
+      !R.ok(cudaMemsetAsync(R.walk_failure.ptr, 0, 2 * sizeof(uint32_t), s), "walk failure words", detail))
     return poison(detail);
   cudaEventRecord(R.ev_start, s);
   const uint32_t pixels = (uint32_t)n;
@@ -2314,6 +2363,8 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   cudaEventRecord(R.ev_stop, s);
   RayTotals totals{};
   cudaMemcpyAsync(&totals, R.totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s);
+  uint32_t walks[2] = {0, 0};
+  cudaMemcpyAsync(walks, R.walk_failure.ptr, sizeof(walks), cudaMemcpyDeviceToHost, s);
   uint32_t failed[kVisibilityPasses] = {~0u, ~0u, ~0u};
   if (restir)
     cudaMemcpyAsync(failed, T.vis_counters.ptr + 2 * kVisibilityPasses, sizeof(failed), cudaMemcpyDeviceToHost, s);
@@ -2323,6 +2374,7 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
     cudaMemcpyAsync(counts.data(), R.counts.ptr, counts.size() * 4, cudaMemcpyDeviceToHost, s);
   }
   if (!R.ok(cudaStreamSynchronize(s), "temporal frame", detail)) return poison(detail);
+  if (walks[0]) return poison(walk_failure_detail(walks, R.step_limit));
   if (choose_rounds) {
     R.temporal_rounds_key = rk;
     R.temporal_auto_rounds = choose_wavefront_rounds(counts.data(), rect[2] * rect[3], st.max_bounces);

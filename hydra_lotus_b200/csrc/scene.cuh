@@ -29,9 +29,19 @@ namespace lotus {
 constexpr int32_t kEmptyChild = 0x7FFFFFFF;
 constexpr int32_t kExitInstance = 0x7FFFFFFE;
 constexpr int kStackSize = 128;
-// A walk that visits more nodes than this ends early: only a corrupt BVH
-// could need it, and the bound keeps such a walk from spinning.
+// A walk that takes more steps than this (SceneView::step_limit, unless a
+// test lowers it) ends early: only a corrupt BVH could need it, and the
+// bound keeps such a walk from spinning. A walk that ends on its step
+// limit, or that had to drop a child because its stack was full, reports
+// itself through SceneView::walk_failure, and the frame Fails.
 constexpr uint32_t kMaxTraversalSteps = 1u << 18;
+// Set in Walk::steps when a child did not fit on the stack: the walk then
+// counts as out of steps, ends at its next pop and reports the overflow.
+constexpr uint32_t kWalkOverflow = 1u << 31;
+// SceneView::walk_failure[1] bits: a walk ran out of steps; a walk's stack
+// overflowed.
+constexpr uint32_t kWalkFailedSteps = 1u;
+constexpr uint32_t kWalkFailedStack = 2u;
 
 // Triangle records are four float4 (64 bytes, cache-sector aligned): three
 // object-space corners, the primitive index in the first corner's w.
@@ -153,6 +163,10 @@ struct SceneView {
   uint32_t analytic_count;
   uint32_t light_node_count;
   uint32_t distant_count;
+  uint32_t step_limit;       // a walk's step budget (kMaxTraversalSteps)
+  // Two words the renderer clears before and reads after each frame: the
+  // number of walks that failed and the kWalkFailed* bits of their causes.
+  uint32_t* walk_failure;
 };
 
 // Buckets of the environment distribution's guide tables (powers of two):
@@ -352,9 +366,18 @@ __device__ __forceinline__ Hit walk_hit(const Walk& W) {
 __device__ __forceinline__ bool walk_at_node(const Walk& W) { return W.cur >= 0 && W.cur < kWalkDone; }
 
 // The next reference from the stack, or kWalkDone (also once the walk has
-// used its 2^18 steps).
-__device__ __forceinline__ void walk_pop(Walk& W, const WalkStack& stack) {
-  W.cur = (W.sp > 0 && W.steps < kMaxTraversalSteps) ? stack[--W.sp] : kWalkDone;
+// used its step budget, or overflowed its stack).
+__device__ __forceinline__ void walk_pop(const SceneView& S, Walk& W, const WalkStack& stack) {
+  W.cur = (W.sp > 0 && W.steps < S.step_limit) ? stack[--W.sp] : kWalkDone;
+}
+
+// A walk that has ended: if it ended on its step budget or a stack
+// overflow, its hits may be incomplete; count it and record the cause.
+__device__ __forceinline__ void walk_check_end(const SceneView& S, const Walk& W) {
+  if (W.steps >= S.step_limit) {
+    atomicAdd(&S.walk_failure[0], 1u);
+    atomicOr(&S.walk_failure[1], (W.steps & kWalkOverflow) ? kWalkFailedStack : kWalkFailedSteps);
+  }
 }
 
 // Slab tests of the node at W.cur. Its hit children go on the stack
@@ -381,13 +404,16 @@ __device__ __forceinline__ void walk_visit_node(const SceneView& S, Walk& W, Wal
   LOTUS_CSWAP(0, 1) LOTUS_CSWAP(2, 3) LOTUS_CSWAP(0, 2) LOTUS_CSWAP(1, 3) LOTUS_CSWAP(1, 2)
 #undef LOTUS_CSWAP
   if (key[0] == INFINITY) {
-    walk_pop(W, stack);
+    walk_pop(S, W, stack);
     return;
   }
 #pragma unroll
   for (int i = 3; i >= 1; --i)
-    if (key[i] != INFINITY && W.sp < kStackSize) stack[W.sp++] = ref[i];
-  W.cur = W.steps < kMaxTraversalSteps ? ref[0] : kWalkDone;
+    if (key[i] != INFINITY) {
+      if (W.sp < kStackSize) stack[W.sp++] = ref[i];
+      else W.steps |= kWalkOverflow;
+    }
+  W.cur = W.steps < S.step_limit ? ref[0] : kWalkDone;
 }
 
 // The triangle tests of BLAS leaf `leaf` (a negative reference). Returns
@@ -454,6 +480,7 @@ __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStac
     if (kCount) ++counters->instances;
     ++W.steps;
     const InstanceTraversal rec = S.inst_trav[instance];
+    if (rec.blas_root != (uint32_t)kEmptyChild && W.sp >= kStackSize) W.steps |= kWalkOverflow;
     if (rec.blas_root != (uint32_t)kEmptyChild && W.sp < kStackSize) {
       stack[W.sp++] = kExitInstance;
       const F3 o = row_point(rec.inv, W.origin);
@@ -467,7 +494,7 @@ __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStac
       return false;
     }
   }
-  walk_pop(W, stack);
+  walk_pop(S, W, stack);
   return false;
 }
 
@@ -485,6 +512,7 @@ __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 dire
       break;
     }
   }
+  walk_check_end(S, W);
   found = W.found;
   if (!kAnyHit && W.found) hit = walk_hit(W);
   return kAnyHit ? W.transmittance : 0.0f;
@@ -517,7 +545,7 @@ __device__ __forceinline__ bool walk_round(const SceneView& S, Walk& W, WalkStac
       walk_visit_node<kCount>(S, W, stack, counters);
       if (W.in_blas && W.cur < 0 && W.leaf == 0) {
         W.leaf = W.cur;
-        walk_pop(W, stack);
+        walk_pop(S, W, stack);
       }
     }
   }
@@ -529,7 +557,9 @@ __device__ __forceinline__ bool walk_round(const SceneView& S, Walk& W, WalkStac
   }
   if (active && !ended && W.cur != kWalkDone && !walk_at_node(W))
     ended = walk_other<kAnyHit, kCount>(S, W, stack, rng, counters);
-  return active && (ended || (W.cur == kWalkDone && W.leaf == 0));
+  const bool done = active && (ended || (W.cur == kWalkDone && W.leaf == 0));
+  if (done) walk_check_end(S, W);
+  return done;
 }
 
 template <bool kCount = false>

@@ -21,7 +21,14 @@
 //     other threads) race on the scratch and corrupt each other;
 //   - the scratch's device address is looked up (cudaGetSymbolAddress) on
 //     the first call on each device, with that device current; make that
-//     first call before any stream capture.
+//     first call before any stream capture. A cudaDeviceReset invalidates
+//     it together with every renderer on that device;
+//   - a renderer whose radiance cache is configured on Fails: this entry
+//     point never uses the cache, so its image would not be RenderScene's;
+//   - a launch or device error Fails the call and poisons the renderer, as
+//     lotus_cuda_render does; so does a BVH walk that ran out of steps or
+//     stack.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -91,6 +98,10 @@ extern "C" int32_t lotus_cuda_render_static(lotus_cuda_renderer* renderer,
     return res.status = LOTUS_FAIL;
   };
   if (!renderer || !frame || !color_device) return fail("no renderer, frame or output");
+  auto poison = [&](const std::string& d) {
+    renderer_poison(renderer, d);
+    return fail(d);
+  };
   RendererAccess access;
   std::string detail;
   if (!renderer_access(renderer, access, detail)) return fail(detail);
@@ -99,6 +110,10 @@ extern "C" int32_t lotus_cuda_render_static(lotus_cuda_renderer* renderer,
     return fail("the allocation-free entry point renders at most " + std::to_string(kMaxPixels) +
                 " pixels; the target has " + std::to_string((uint64_t)t.width * t.height));
   if (frame->frame_count == 0) return fail("frame_count must be at least 1");
+  if (access.cache_enabled)
+    return fail("the allocation-free entry point does not use the radiance cache; configure it off first");
+  const uint32_t max_samples = frame->settings.max_samples;
+  const uint32_t samples = max_samples ? std::min(frame->frame_count, max_samples) : frame->frame_count;
   FrameConst fc{};
   uint32_t rect[4];
   if (!make_frame_constants(*frame, fc, rect, detail)) return fail(detail);
@@ -131,13 +146,14 @@ extern "C" int32_t lotus_cuda_render_static(lotus_cuda_renderer* renderer,
   cudaStream_t s = access.stream;
   const float4 clear = make_float4(t.clear_color[0], t.clear_color[1], t.clear_color[2], t.clear_color[3]);
   if ((e = cudaMemcpyAsync(d_frame, &fc, sizeof(fc), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-      (e = cudaMemsetAsync(d_totals, 0, sizeof(RayTotals), s)) != cudaSuccess)
-    return fail(std::string("scratch set-up: ") + cudaGetErrorString(e));
+      (e = cudaMemsetAsync(d_totals, 0, sizeof(RayTotals), s)) != cudaSuccess ||
+      (e = cudaMemsetAsync(access.view->walk_failure, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess)
+    return poison(std::string("scratch set-up: ") + cudaGetErrorString(e));
   float4* color = reinterpret_cast<float4*>(color_device);
   if (rect[2] < t.width || rect[3] < t.height || rect[2] == 0)
     launch_clear_color(color, t.width * t.height, clear, s);
   const bool wavefront = frame->settings.integrator == LOTUS_INTEGRATOR_WAVEFRONT;
-  for (uint32_t k = 0; k < frame->frame_count; ++k) {
+  for (uint32_t k = 0; k < samples; ++k) {
     if (wavefront)
       launch_wavefront_sample(*access.view, d_frame, rect, t.width, t.height,
           frame->settings.max_bounces, P, Q, accum, color, d_totals, s, nullptr, access.tuning);
@@ -145,13 +161,18 @@ extern "C" int32_t lotus_cuda_render_static(lotus_cuda_renderer* renderer,
       launch_reference_pt(*access.view, d_frame, rect, accum, color, d_totals, s);
     launch_advance(d_frame, s);
   }
+  if ((e = cudaGetLastError()) != cudaSuccess) return poison(std::string("launch: ") + cudaGetErrorString(e));
   RayTotals totals{};
+  uint32_t walks[2] = {0, 0};
   if ((e = cudaMemcpyAsync(&totals, d_totals, sizeof(totals), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(walks, access.view->walk_failure, sizeof(walks), cudaMemcpyDeviceToHost, s)) !=
+          cudaSuccess ||
       (e = cudaStreamSynchronize(s)) != cudaSuccess)
-    return fail(std::string("render: ") + cudaGetErrorString(e));
+    return poison(std::string("render: ") + cudaGetErrorString(e));
+  if (walks[0]) return poison(walk_failure_detail(walks, access.step_limit));
   res.status = LOTUS_PASS;
-  res.frames_rendered = frame->frame_count;
-  res.samples_per_pixel = frame->frame_count;
+  res.frames_rendered = samples;
+  res.samples_per_pixel = samples;
   res.camera_rays = totals.camera;
   res.extension_rays = totals.extension;
   res.shadow_rays = totals.shadow;

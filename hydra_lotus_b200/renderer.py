@@ -126,11 +126,11 @@ class CudaOffscreenRenderer:
     accumulation targets."""
 
     def __init__(self, device=0, bvh_leaf_size=0, trace_refill_below=0, trace_blocks_per_sm=0,
-                 wavefront_rounds=0):
+                 wavefront_rounds=0, traversal_step_limit=0):
         self.handle = None
         opts = abi.Options(device=device, flags=0, bvh_leaf_size=bvh_leaf_size,
                            trace_refill_below=trace_refill_below, trace_blocks_per_sm=trace_blocks_per_sm,
-                           wavefront_rounds=wavefront_rounds)
+                           wavefront_rounds=wavefront_rounds, traversal_step_limit=traversal_step_limit)
         h = C.c_void_p()
         err = C.create_string_buffer(256)
         status = lib().lotus_cuda_create(C.byref(opts), C.byref(h), err, 256)

@@ -785,3 +785,127 @@ def light_grid(side=16, size=512, seed=0):
             s.add_light(abi.LIGHT_SPHERE, affine(translation=(first + spacing * x, 0.85, first + spacing * y)),
                         radiance=(12.0 * scale, 10.0 * scale, 8.0 * scale), radius=0.025)
     return s
+
+
+# ---------------------------------------------------------------------------
+# The reference's material-basics-v1 fixture
+
+def _fixed(value):
+    """A coordinate rounded to a multiple of 1e-6 (halves away from zero), as
+    the fixture's USD file spells it; -0 becomes +0."""
+    scaled = value * 1e6
+    rounded = math.floor(abs(scaled) + 0.5)
+    return float(F32(math.copysign(rounded, scaled) / 1e6 + 0.0))
+
+
+def uv_sphere(segments=32, rings=16):
+    """The unit UV sphere of the material fixtures (material_fixtures.cpp:29-64
+    in hydra-lotus): a pole vertex, rings-1 rings of `segments` vertices and
+    the other pole; the caps are triangle fans, the bands quads split as
+    fans from their first vertex. Its points double as its corner normals.
+    Returns (positions, triangles, corner normals)."""
+    points = [(0.0, 1.0, 0.0)]
+    for i in range(1, rings):
+        theta = math.pi * i / rings
+        for j in range(segments):
+            phi = 2.0 * math.pi * j / segments
+            points.append((_fixed(math.sin(theta) * math.cos(phi)), _fixed(math.cos(theta)),
+                           _fixed(-math.sin(theta) * math.sin(phi))))
+    points.append((0.0, -1.0, 0.0))
+    bottom = len(points) - 1
+
+    def ring(i, j):
+        return 1 + (i - 1) * segments + j % segments
+
+    faces = [[0, ring(1, j), ring(1, j + 1)] for j in range(segments)]
+    for i in range(1, rings - 1):
+        for j in range(segments):
+            faces.append([ring(i, j), ring(i + 1, j), ring(i + 1, j + 1), ring(i, j + 1)])
+    faces += [[ring(rings - 1, j), bottom, ring(rings - 1, j + 1)] for j in range(segments)]
+    triangles = []
+    for v in faces:
+        for k in range(1, len(v) - 1):
+            triangles.append((v[0], v[k], v[k + 1]))
+    positions = np.asarray(points, dtype=F32)
+    triangles = np.asarray(triangles, dtype=np.uint32)
+    return positions, triangles, positions[triangles]
+
+
+def _rotation_x_deg(degrees):
+    c, s = math.cos(math.radians(degrees)), math.sin(math.radians(degrees))
+    return np.array([[1, 0, 0, 0], [0, c, -s, 0], [0, s, c, 0], [0, 0, 0, 1]], dtype=np.float64)
+
+
+def _rotation_y_deg(degrees):
+    c, s = math.cos(math.radians(degrees)), math.sin(math.radians(degrees))
+    return np.array([[c, 0, s, 0], [0, 1, 0, 0], [-s, 0, c, 0], [0, 0, 0, 1]], dtype=np.float64)
+
+
+def material_studio(name, size):
+    """The camera, lights and backdrop every material fixture shares
+    (SetStudio, material_fixtures.cpp:119-157 in hydra-lotus): a camera at
+    z = 6.5 looking down -Z (focal 3.125, clip 1..100), a constant dome of
+    0.5, a 3x3 rect light of radiance 4 at (1.5, 2.5, 4) turned 20 degrees
+    about Y and -30 about X, and a 6x6 backdrop quad at z = -1 with a 0.5
+    grey coated-diffuse material."""
+    s = Scene(name)
+    focal, near, far = F32(3.125), F32(1.0), F32(100.0)
+    view = identity()
+    view[14] = -6.5
+    projection = np.array([focal, 0, 0, 0, 0, focal, 0, 0,
+                           0, 0, (far + near) / (near - far), -1,
+                           0, 0, F32(2.0) * far * near / (near - far), 0], dtype=F32)
+    s.world_to_clip = multiply(projection, view)
+    s.width = s.height = size
+    s.environment_constant = (0.5, 0.5, 0.5)
+    key = np.eye(4)
+    key[:3, 3] = (1.5, 2.5, 4.0)
+    key = key @ _rotation_y_deg(20.0) @ _rotation_x_deg(-30.0)
+    s.add_light(abi.LIGHT_RECT, key.astype(F32).reshape(-1, order="F"),
+                radiance=(4.0, 4.0, 4.0), width=3.0, height=3.0)
+    backdrop = s.add_geometry(*quad([[-3, -3, -1], [3, -3, -1], [3, 3, -1], [-3, 3, -1]]))
+    s.add_instance(backdrop, s.add_material(preview_material((0.5, 0.5, 0.5))))
+    return s
+
+
+def material_basics(metal50_scale=1.0, size=128):
+    """The reference's material-basics-v1 fixture (SetMaterialBasics,
+    material_fixtures.cpp:161-211 in hydra-lotus), which its golden images
+    validation/reference/material-basics-v1-{mean,variance}.pfm were
+    rendered from: a 4x4 grid of UV spheres of radius 0.4, centres 0.9
+    apart, in the material studio. Rows from the top: coated diffuse base
+    colours (white, red, dark, clamped), coated diffuse roughness 0, 0.25,
+    0.5, 1, a copper GGX conductor at roughness 0, 0.25, 0.5, 1, and gold
+    at metallic 0.25 and 0.75, ior 2.5, and the specular workflow.
+    ``metal50_scale`` scales the half-rough copper's base colour (the
+    fixture's negative control, DarkerMetal, scales it by 0.9)."""
+    s = material_studio("material-basics-v1", size)
+    grey, copper, gold = (0.5, 0.5, 0.5), (0.95, 0.64, 0.54), (0.9, 0.6, 0.2)
+    balls = [
+        preview_material((0.8, 0.8, 0.8)),
+        preview_material((0.8, 0.1, 0.05)),
+        preview_material((0.04, 0.04, 0.04)),
+        preview_material((1.0, 0.5, 0.0), roughness=1.0),
+        preview_material(grey, roughness=0.0),
+        preview_material(grey, roughness=0.25),
+        preview_material(grey, roughness=0.5),
+        preview_material(grey, roughness=1.0),
+        preview_material(copper, roughness=0.0, metallic=1.0),
+        preview_material(copper, roughness=0.25, metallic=1.0),
+        preview_material(tuple(F32(c) * F32(metal50_scale) for c in copper), roughness=0.5,
+                         metallic=1.0),
+        preview_material(copper, roughness=1.0, metallic=1.0),
+        preview_material(gold, roughness=0.3, metallic=0.25),
+        preview_material(gold, roughness=0.3, metallic=0.75),
+        preview_material((0.1, 0.2, 0.6), roughness=0.1, ior=2.5),
+        preview_material((0.05, 0.05, 0.05), roughness=0.2, specular_color=(0.9, 0.6, 0.3),
+                         flags=abi.MATERIAL_SPECULAR_WORKFLOW),
+    ]
+    ball = s.add_geometry(*uv_sphere())
+    columns, rows = (-1.35, -0.45, 0.45, 1.35), (1.35, 0.45, -0.45, -1.35)
+    for i, material in enumerate(balls):
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = placed[5] = placed[10] = 0.4
+        placed[12], placed[13] = columns[i % 4], rows[i // 4]
+        s.add_instance(ball, s.add_material(material), placed)
+    return s

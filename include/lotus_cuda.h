@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LOTUS_CUDA_ABI_VERSION 3u
+#define LOTUS_CUDA_ABI_VERSION 4u
 
 /* FrameStatus (vulkan_backend.hpp:23-27). */
 #define LOTUS_PASS 0
@@ -282,6 +282,12 @@ typedef struct lotus_cuda_options {
    * than max(camera rays / 32, 65536) paths; other calls use
    * LOTUS_WAVEFRONT_ROUNDS. Results do not depend on it. */
   uint32_t wavefront_rounds;
+  /* A BVH walk's step budget (node visits, leaf tests and instance entries);
+   * 0: 2^18, which only a corrupt BVH could need. A walk that runs out of it,
+   * or whose traversal stack overflows, makes its frame Fail with a detail
+   * naming the cause and poisons the renderer. Tests lower it to make the
+   * bound run out. */
+  uint32_t traversal_step_limit;
 } lotus_cuda_options;
 
 typedef struct lotus_cuda_renderer lotus_cuda_renderer;
@@ -438,15 +444,21 @@ int64_t lotus_cuda_read_light_table(lotus_cuda_renderer* renderer,
  * device memory for width*height*4 floats, which receives the RGBA32F mean
  * of frame_count samples from settings.sample_index (top-left rows; pixels
  * outside the data window get the clear colour). Each call starts its own
- * accumulation; none carries over.
+ * accumulation; none carries over. settings.max_samples, when nonzero,
+ * caps the samples added as RenderScene's does for a fresh accumulation.
  *
  * Limits: at most LOTUS_STATIC_MAX_PIXELS pixels (larger targets Fail with
- * that reason); Radiance with BSDF or MIS light sampling. All calls share
- * the one scratch array, which keeps the last call's contents, so calls
- * whose GPU work overlaps (other threads or streams) race and corrupt each
- * other. The first call on each device looks up the array's address with
- * that device current; make it before any stream capture. Calls
- * cudaMalloc, cudaFree and no allocating library routine. */
+ * that reason); Radiance with BSDF or MIS light sampling; a renderer whose
+ * radiance cache is configured on Fails (this entry point never uses the
+ * cache, so its image would not be RenderScene's). All calls share the one
+ * scratch array, which keeps the last call's contents, so calls whose GPU
+ * work overlaps (other threads or streams) race and corrupt each other.
+ * The first call on each device looks up the array's address with that
+ * device current; make it before any stream capture (a cudaDeviceReset
+ * invalidates that address together with every renderer on the device).
+ * A launch or device error Fails the call and poisons the renderer, as
+ * lotus_cuda_render does. Calls no cudaMalloc, cudaFree or allocating
+ * library routine. */
 int32_t lotus_cuda_render_static(lotus_cuda_renderer* renderer,
     const lotus_frame_desc* frame, float* color_device, lotus_frame_result* result);
 

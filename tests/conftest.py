@@ -29,8 +29,19 @@ def cuda():
     return renderer
 
 
+def load_golden(name):
+    import numpy as np
+    g = np.load(os.path.join(ROOT, "tests", "golden", name))
+    return {"mean": g["mean"], "variance": g["variance"], "samples": int(g["samples"])}
+
+
 @pytest.fixture(scope="session")
 def golden():
-    import numpy as np
-    g = np.load(os.path.join(ROOT, "tests", "golden", "cornell_box.npz"))
-    return {"mean": g["mean"], "variance": g["variance"], "samples": int(g["samples"])}
+    """The reference's Cornell box golden images (1024 spp)."""
+    return load_golden("cornell_box.npz")
+
+
+@pytest.fixture(scope="session")
+def golden_materials():
+    """The reference's material-basics-v1 golden images (4096 spp)."""
+    return load_golden("material_basics_v1.npz")

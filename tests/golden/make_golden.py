@@ -1,16 +1,21 @@
 """Writes the golden fixtures under tests/golden/ from the reference tree.
 
-Run in a checkout that has the reference at REFERENCE (default
-/root/reference); the fixtures it writes are committed, so tests never
-read the reference at run time.
+The reference tree is found at $LOTUS_REFERENCE, else at ../reference beside
+this checkout. The fixtures it writes are committed, so tests never read the
+reference at run time. Each is the reference's own golden image pair
+(validation/reference/<stem>-{mean,variance}.pfm of hydra-lotus v0.9.0),
+written by its GPU renderer with BSDF sampling, 64 bounces, from sample
+index 0 (docs/reference/SCENE.md, "Deterministic mode"), stored as float32
+arrays with rows from the top (the PFMs hold rows from the bottom,
+little-endian; ReadPfm, adapters/common/reference.cpp:100-131):
 
-- cornell_box.npz: validation/reference/cornell-box-mean.pfm and
-  cornell-box-variance.pfm of hydra-lotus v0.9.0: the Cornell box fixture
-  (adapters/common/reference.cpp:221-279) at 128x128, 1024 samples per
-  pixel from sample index 0, BSDF sampling, 64 bounces, as the reference's
-  GPU renderer wrote them (docs/reference/SCENE.md, "Deterministic mode").
-  Stored as float32 arrays with rows from the top (the PFMs hold rows from
-  the bottom, little-endian; ReadPfm, reference.cpp:100-131).
+- cornell_box.npz: the Cornell box fixture (adapters/common/reference.cpp:
+  221-279) at 128x128, 1024 samples per pixel.
+- material_basics_v1.npz: the material-basics-v1 fixture
+  (adapters/common/material_fixtures.cpp:161-211: a 4x4 grid of
+  UsdPreviewSurface balls under a constant dome and a rect light) at
+  128x128, 4096 samples per pixel (kMaterialReferenceSamples,
+  adapters/headless/main.cpp).
 """
 
 import os
@@ -18,8 +23,12 @@ import sys
 
 import numpy as np
 
-REFERENCE = os.environ.get("LOTUS_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+REFERENCE = os.environ.get("LOTUS_REFERENCE",
+                           os.path.join(HERE, "..", "..", "..", "reference"))
+
+FIXTURES = [("cornell-box", "cornell_box.npz", 1024),
+            ("material-basics-v1", "material_basics_v1.npz", 4096)]
 
 
 def read_pfm(path):
@@ -36,11 +45,16 @@ def read_pfm(path):
 
 def main():
     ref = os.path.join(REFERENCE, "validation", "reference")
-    mean = read_pfm(os.path.join(ref, "cornell-box-mean.pfm"))
-    variance = read_pfm(os.path.join(ref, "cornell-box-variance.pfm"))
-    out = os.path.join(HERE, "cornell_box.npz")
-    np.savez_compressed(out, mean=mean, variance=variance, samples=np.uint32(1024))
-    print("wrote", out, mean.shape)
+    if not os.path.isdir(ref):
+        print(f"no reference tree at {REFERENCE}; set LOTUS_REFERENCE", file=sys.stderr)
+        return 1
+    for stem, name, samples in FIXTURES:
+        mean = read_pfm(os.path.join(ref, f"{stem}-mean.pfm"))
+        variance = read_pfm(os.path.join(ref, f"{stem}-variance.pfm"))
+        out = os.path.join(HERE, name)
+        np.savez_compressed(out, mean=mean, variance=variance, samples=np.uint32(samples))
+        print("wrote", out, mean.shape)
+    return 0
 
 
 if __name__ == "__main__":

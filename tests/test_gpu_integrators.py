@@ -161,3 +161,89 @@ def test_sample_chains_equal_one_sample_at_a_time(cuda, renderer, frames):
         cuda.check(res, "one sample")
     assert res.samples_per_pixel == frames
     assert np.array_equal(chained, single), f"{np.count_nonzero(chained != single)} values differ"
+
+
+MATERIAL_MODES = [(abi.INTEGRATOR_REFERENCE, abi.LIGHT_SAMPLING_BSDF),
+                  (abi.INTEGRATOR_REFERENCE, abi.LIGHT_SAMPLING_MIS),
+                  (abi.INTEGRATOR_WAVEFRONT, abi.LIGHT_SAMPLING_MIS),
+                  (abi.INTEGRATOR_WAVEFRONT, abi.LIGHT_SAMPLING_BSDF)]
+
+
+@pytest.mark.parametrize("integrator,light_sampling", MATERIAL_MODES)
+def test_material_basics_matches_reference_golden(cuda, renderer, golden_materials, integrator,
+                                                  light_sampling):
+    """DES-Q5 against the reference's committed 4096-spp material-basics-v1
+    images (GGX conductors, rough and smooth coats, metallic mixes, ior
+    2.5, the specular workflow, a constant dome and a rect light), at the
+    reference's levels 16 and 256 spp in one accumulation (kMaterialLevels,
+    adapters/headless/main.cpp) and then at 1024 spp."""
+    scene = scenes.material_basics()
+    st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,
+                              max_bounces=64, sample_index=1 << 20)
+    g = golden_materials
+    cuda.check(renderer.update_scene(scene), "update_scene")
+    rendered = 0
+    for level in (16, 256, 1024):
+        res, color = renderer.render_scene(scene.frame(st, level - rendered))
+        cuda.check(res, "render_scene")
+        rendered = level
+        assert res.samples_per_pixel == level
+        c = metrics.compare(color, level, g["mean"], g["variance"], g["samples"])
+        print(level, c)
+        assert c.ok, c
+
+
+def test_material_basics_negative_control_rejected(cuda, renderer, golden_materials):
+    """The half-rough copper 10% darker (DarkerMetal) must not match."""
+    scene = scenes.material_basics(metal50_scale=0.9)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=64, sample_index=1 << 20)
+    _, color = render(cuda, renderer, scene, st, frame_count=256)
+    g = golden_materials
+    c = metrics.compare(color, 256, g["mean"], g["variance"], g["samples"])
+    assert not c.ok, c
+
+
+@pytest.mark.parametrize("integrator", INTEGRATORS)
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+def test_material_basics_paths_match_oracle(cuda, renderer, oracle_lib, integrator, light_sampling):
+    """Every path of the material fixture (corner normals, every
+    UsdPreviewSurface lobe, the dome and the rect light) against the
+    oracle's, whose image the previous tests pin to the reference's."""
+    scene = scenes.material_basics()
+    st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,
+                              max_bounces=64, sample_index=9)
+    res, color = render(cuda, renderer, scene, st)
+    want, rays = oracle_lib.OracleScene(scene).sample(scene.frame(st), 9)
+    p = PathParity(color, want)
+    print(p)
+    p.assert_ok()
+    assert p.exact > 0.9, p
+    assert res.camera_rays == rays[0]
+
+
+@pytest.fixture(scope="module")
+def bench_frame_scene():
+    return scenes.sphere_field(seed=0)
+
+
+@pytest.mark.parametrize("integrator", INTEGRATORS)
+@pytest.mark.parametrize("band", [300, 536, 1064])
+def test_bench_frame_band_paths_match_oracle(cuda, renderer, oracle_lib, bench_frame_scene,
+                                             integrator, band):
+    """The benchmarked frame itself (the seeded 1080p sphere field: 13.7M
+    instanced triangles, the 2048x1024 sky), 16 rows at the horizon (the
+    rows above it see only sky), the middle and the bottom, one sample at
+    depth 8: each path against the oracle's."""
+    scene = bench_frame_scene
+    st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=8, sample_index=40)
+    window = (0, band, scene.width, 16)
+    cuda.check(renderer.update_scene(scene), "update_scene")
+    res, color = renderer.render_scene(scene.frame(st, 1, data_window=window))
+    cuda.check(res, "render_scene")
+    want, rays = oracle_lib.OracleScene(scene).sample(scene.frame(st, data_window=window), 40)
+    p = PathParity(color[band:band + 16], want[band:band + 16])
+    print(p, res.camera_rays, res.extension_rays, res.shadow_rays, rays)
+    p.assert_ok()
+    assert res.camera_rays == rays[0] == scene.width * 16

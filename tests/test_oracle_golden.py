@@ -1,7 +1,17 @@
-"""CPU: the oracle against the reference's own golden Cornell images
-(validation/reference/cornell-box-{mean,variance}.pfm, 1024 spp, written by
-the reference's GPU renderer; fixtures in tests/golden) with the
-reference's DES-Q5 comparison, and the red-wall negative control."""
+"""CPU: the oracle against the reference's own golden images with the
+reference's DES-Q5 comparison, and each fixture's negative control.
+
+- validation/reference/cornell-box-{mean,variance}.pfm (1024 spp): coated
+  Lambert walls, a GGX metal block, an emissive quad; the red wall x1.1
+  must be rejected.
+- validation/reference/material-basics-v1-{mean,variance}.pfm (4096 spp):
+  coated diffuse, rough and smooth coats, GGX conductors from roughness 0
+  to 1, metallic mixes, ior 2.5 and the specular workflow, under a
+  constant dome and a rect light; the half-rough copper 10% darker must be
+  rejected (DarkerMetal, adapters/common/material_fixtures.cpp).
+
+Both were written by the reference's GPU renderer; fixtures in tests/golden.
+"""
 
 import numpy as np
 import pytest
@@ -11,12 +21,12 @@ from hydra_lotus_b200 import abi, metrics, scenes
 SPP = 256
 
 
-def oracle_image(oracle_lib, scene, light_sampling):
+def oracle_image(oracle_lib, scene, light_sampling, spp=SPP):
     st = abi.default_settings(integrator=abi.INTEGRATOR_REFERENCE, light_sampling=light_sampling,
                               max_bounces=64, sample_index=1 << 20)
-    frame = scene.frame(st, SPP)
-    sums, _ = oracle_lib.OracleScene(scene).accumulate(frame, 1 << 20, SPP)
-    return (sums / SPP).astype(np.float32)
+    frame = scene.frame(st, spp)
+    sums, _ = oracle_lib.OracleScene(scene).accumulate(frame, 1 << 20, spp)
+    return (sums / spp).astype(np.float32)
 
 
 @pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
@@ -29,4 +39,21 @@ def test_oracle_matches_reference_golden(oracle_lib, golden, light_sampling):
 def test_oracle_negative_control_rejected(oracle_lib, golden):
     img = oracle_image(oracle_lib, scenes.cornell_reference(red_scale=1.1), abi.LIGHT_SAMPLING_BSDF)
     c = metrics.compare(img, SPP, golden["mean"], golden["variance"], golden["samples"])
+    assert not c.ok, c
+
+
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+@pytest.mark.parametrize("spp", [16, 256])
+def test_oracle_matches_material_basics_golden(oracle_lib, golden_materials, light_sampling, spp):
+    img = oracle_image(oracle_lib, scenes.material_basics(), light_sampling, spp)
+    g = golden_materials
+    c = metrics.compare(img, spp, g["mean"], g["variance"], g["samples"])
+    assert c.ok, c
+
+
+def test_oracle_material_basics_negative_control_rejected(oracle_lib, golden_materials):
+    img = oracle_image(oracle_lib, scenes.material_basics(metal50_scale=0.9),
+                       abi.LIGHT_SAMPLING_MIS)
+    g = golden_materials
+    c = metrics.compare(img, SPP, g["mean"], g["variance"], g["samples"])
     assert not c.ok, c
