@@ -32,7 +32,7 @@ FRAME_COUNT_VISITS = 2
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 # lotus_settings::output (SceneOutput).
 OUTPUT_RADIANCE = 0
@@ -164,6 +164,7 @@ class Settings(C.Structure):
         ("restir_proposal", C.c_uint32),
         ("environment_background", C.c_uint32),
         ("output", C.c_uint32),
+        ("restir_spatial_neighbours", C.c_uint32),
     ]
 
 
@@ -333,7 +334,8 @@ def default_settings(**overrides):
                  restir_candidates=8, restir_temporal=0,
                  restir_max_history_candidates=32, restir_spatial=0,
                  restir_spatial_radius=1, restir_proposal=0,
-                 environment_background=0, output=OUTPUT_RADIANCE)
+                 environment_background=0, output=OUTPUT_RADIANCE,
+                 restir_spatial_neighbours=0)
     for k, v in overrides.items():
         setattr(s, k, v)
     return s

@@ -63,12 +63,13 @@ def build(force=False, verbose=False, jobs=None):
 
 # The C++ adapter (host/cuda_offscreen_renderer.*) implements the
 # reference's Lotus::OffscreenRenderer over the C ABI; it compiles against
-# the reference's headers, so it builds only where they are present (set
-# LOTUS_REFERENCE to the reference's tree). Its test driver links it with
+# the reference's headers, so it builds only where they are present
+# ($LOTUS_REFERENCE, else ../reference beside this checkout). Its test
+# driver links it with
 # the library into _lib/adapter_harness.
 HOST = os.path.join(HERE, "host")
 HARNESS = os.path.join(LIB_DIR, "adapter_harness")
-REFERENCE = os.environ.get("LOTUS_REFERENCE", "/root/reference")
+REFERENCE = os.environ.get("LOTUS_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 
 def reference_headers():

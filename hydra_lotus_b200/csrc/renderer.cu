@@ -560,8 +560,8 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
   }
   for (uint32_t i : small) { table.records[i].threshold = 1.0f; table.records[i].alias = i; }
   for (uint32_t i : large) { table.records[i].threshold = 1.0f; table.records[i].alias = i; }
-  // Each analytic record keeps its entry's probability, which weighs the
-  // emission BSDF sampling finds on it.
+  // An analytic light's record carries the probability of its table entry:
+  // a BSDF-sampled ray that crosses the light needs it for its MIS weight.
   for (uint32_t entry : analytic_entries)
     table.analytic[table.records[entry].instance & ~kAnalyticLight].radiance.w = table.records[entry].pdf;
   if (env_weight > 0.0) table.env_selection = table.records.back().pdf;
@@ -653,7 +653,6 @@ struct Renderer {
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<cudaEvent_t> ev_sample_done;  // per sample of a chain: resolved and counted
-  uint32_t chain_length = 0;                // samples in graph_chain
   DeviceArray<FrameConst> frame_const;
   DeviceArray<RayTotals> totals;
   DeviceArray<VisitCounters> visits;
@@ -706,7 +705,7 @@ struct Renderer {
     uint32_t frames = 0;          // temporal frames rendered since the last reset
     uint32_t sample_offset = 0;
     bool key_valid = false;
-    uint32_t key[16] = {};
+    uint32_t key[17] = {};
     bool restir_ran = false, accumulate_ran = false, spatial_ran = false, filter_ran = false;
   } temporal;
   std::vector<lotus_instance> host_instances;
@@ -723,8 +722,12 @@ struct Renderer {
   uint32_t cache_pixels = 0;
   uint32_t cache_generation = 0;  // bumped by every configuration
 
-  // The wavefront sample as a CUDA graph, and two samples in flight.
-  cudaGraphExec_t graph = nullptr, graph_chain = nullptr;
+  // The wavefront sample as a CUDA graph, and chains of two samples in
+  // flight: one instantiated graph per chain length (2, 4, .. kMaxChain,
+  // at index length / 2), all of one key, so that a call whose remainder
+  // makes a short chain does not re-instantiate the long one.
+  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph_chains[kMaxChain / 2 + 1] = {};
   struct GraphKey {
     uint64_t scene_generation;
     uint32_t width, height, max_bounces;
@@ -742,7 +745,8 @@ struct Renderer {
   ~Renderer() {
     for (cudaEvent_t e : profile_events) cudaEventDestroy(e);
     if (graph) cudaGraphExecDestroy(graph);
-    if (graph_chain) cudaGraphExecDestroy(graph_chain);
+    for (cudaGraphExec_t g : graph_chains)
+      if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t e : {ev_fork, ev_join})
       if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ev_sample_done) cudaEventDestroy(e);
@@ -1673,11 +1677,16 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
       // tail is not overlapped by another sample's rounds.
       const uint32_t length = std::min(kMaxChain, (chainable - k) & ~1u);
       gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, false);
-      if (!R.graph_chain || !(R.graph_chain_key == gk) || R.chain_length != length) {
-        if (R.graph_chain) {
-          cudaGraphExecDestroy(R.graph_chain);
-          R.graph_chain = nullptr;
-        }
+      if (!(R.graph_chain_key == gk)) {
+        for (cudaGraphExec_t& old : R.graph_chains)
+          if (old) {
+            cudaGraphExecDestroy(old);
+            old = nullptr;
+          }
+        R.graph_chain_key = gk;
+      }
+      cudaGraphExec_t& chain = R.graph_chains[length / 2];
+      if (!chain) {
         cudaGraph_t g;
         FrameConst* fc = R.frame_const.ptr;
         if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
@@ -1696,13 +1705,11 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
         cudaStreamWaitEvent(s, R.ev_join, 0);
         for (uint32_t j = 0; j < length; ++j) launch_advance(fc, s);
         if (!R.ok(cudaStreamEndCapture(s, &g), "graph capture", detail)) return poison(detail);
-        cudaError_t e = cudaGraphInstantiate(&R.graph_chain, g, 0);
+        cudaError_t e = cudaGraphInstantiate(&chain, g, 0);
         cudaGraphDestroy(g);
         if (!R.ok(e, "graph instantiate", detail)) return poison(detail);
-        R.graph_chain_key = gk;
-        R.chain_length = length;
       }
-      if (!R.ok(cudaGraphLaunch(R.graph_chain, s), "graph launch", detail)) return poison(detail);
+      if (!R.ok(cudaGraphLaunch(chain, s), "graph launch", detail)) return poison(detail);
       k += length - 1;
       last_in_chain = true;
       continue;
@@ -2163,6 +2170,8 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
     return fail("RestirInitial needs restir_candidates in [1, 64]");
   if (st.restir_spatial && (st.restir_spatial_radius == 0 || st.restir_spatial_radius > 32))
     return fail("restir_spatial_radius must be in [1, 32]");
+  if (st.restir_spatial_neighbours > LOTUS_MAX_SPATIAL_NEIGHBOURS)
+    return fail("restir_spatial_neighbours must be in [0, " + std::to_string(LOTUS_MAX_SPATIAL_NEIGHBOURS) + "]");
   if (accumulate && (td.max_history_samples == 0 || td.max_history_samples > 65536))
     return fail("temporal radiance requires history samples in [1, 65536]");
   if (td.filter_iterations > 8 || (td.filter_iterations != 0 && !accumulate))
@@ -2217,9 +2226,10 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
           R.ok(T.vis_counters.resize(3 * kVisibilityPasses), "visibility queue", detail);
   if (!okb) return poison(detail);
   // The transport key: a change drops the history (vulkan_backend.cpp:1766-1781).
-  uint32_t key[16] = {st.integrator, st.light_sampling, st.restir_proposal, st.restir_candidates,
+  uint32_t key[17] = {st.integrator, st.light_sampling, st.restir_proposal, st.restir_candidates,
       st.restir_temporal, st.restir_max_history_candidates, st.restir_spatial, st.restir_spatial_radius,
-      td.accumulate_radiance, st.sample_index, st.max_bounces, st.environment_background, 0, 0, 0, 0};
+      td.accumulate_radiance, st.sample_index, st.max_bounces, st.environment_background, 0, 0, 0, 0,
+      st.restir_spatial_neighbours};
   std::memcpy(&key[12], t.clear_color, sizeof(t.clear_color));
   const bool fresh_batch = accumulate || reservoirs;
   bool previous = td.history_available != 0 && T.frames > 0;
@@ -2261,6 +2271,7 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   tc.restir_spatial = st.restir_spatial ? 1u : 0u;
   tc.restir_temporal = reservoirs ? 1u : 0u;
   tc.restir_radius = st.restir_spatial_radius;
+  tc.restir_neighbours = st.restir_spatial_neighbours;
   tc.restir_proposal = st.restir_proposal;
   tc.sample_index = fc.sample_index;
   tc.max_bounces = st.max_bounces;

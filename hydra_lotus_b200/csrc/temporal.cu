@@ -8,6 +8,7 @@
 // the preceding one finished writing, as the reference's barriers order it.
 #include <cooperative_groups.h>
 
+#include "../../include/lotus_cuda.h"
 #include "temporal_passes.cuh"
 
 namespace lotus {
@@ -445,8 +446,47 @@ __device__ __forceinline__ bool spatial_compatible(const RestirSurface& receiver
       dot(V(receiver.shading_normal), V(source.shading_normal)) >= 0.9f;
 }
 
-// WriteSpatialReservoir (restir.slang:402-491): four axis neighbours at
-// the radius, merged with support correction.
+// The spatial pass's neighbour offsets: the reference's four axis
+// neighbours at the radius (restir.slang:408-410), or `count` distinct
+// offsets drawn uniformly from the disk of the radius, the centre excluded
+// (no counterpart in the reference): each the first of up to kDiskTries
+// draws of an offset in the enclosing square that falls inside the disk
+// and was not drawn before, from the pixel's own stream for this purpose.
+// Returns how many offsets there are.
+constexpr int kMaxNeighbours = LOTUS_MAX_SPATIAL_NEIGHBOURS;
+constexpr int kDiskTries = 16;
+
+__device__ __forceinline__ int spatial_offsets(uint32_t slot, uint32_t sample_index, int radius, uint32_t count,
+    int ox[kMaxNeighbours], int oy[kMaxNeighbours]) {
+  if (count == 0) {
+    ox[0] = -radius, oy[0] = 0;
+    ox[1] = radius, oy[1] = 0;
+    ox[2] = 0, oy[2] = -radius;
+    ox[3] = 0, oy[3] = radius;
+    return 4;
+  }
+  uint32_t rng = seed_random(slot, sample_index ^ 0x5BD1E995u);
+  const float side = float(2 * radius + 1);
+  int n = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    for (int t = 0; t < kDiskTries; ++t) {
+      const int dx = min((int)(next_random(rng) * side), 2 * radius) - radius;
+      const int dy = min((int)(next_random(rng) * side), 2 * radius) - radius;
+      if ((dx == 0 && dy == 0) || dx * dx + dy * dy > radius * radius) continue;
+      bool seen = false;
+      for (int k = 0; k < n; ++k) seen = seen || (ox[k] == dx && oy[k] == dy);
+      if (seen) continue;
+      ox[n] = dx;
+      oy[n] = dy;
+      ++n;
+      break;
+    }
+  }
+  return n;
+}
+
+// WriteSpatialReservoir (restir.slang:402-491): the neighbours above,
+// merged with support correction.
 __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     const RestirReuse* __restrict__ temporal, const RestirSurface* __restrict__ surfaces,
@@ -459,13 +499,14 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
   const RestirReuse centre = temporal[slot];
   const RestirSurface receiver = surfaces[slot];
   RestirReuse result = centre;
-  uint32_t sources[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
-  const int radius = (int)tc.restir_radius;
-  const int ox[4] = {-radius, radius, 0, 0};
-  const int oy[4] = {0, 0, -radius, radius};
+  uint32_t sources[kMaxNeighbours];
+  for (int i = 0; i < kMaxNeighbours; ++i) sources[i] = 0xffffffffu;
+  int ox[kMaxNeighbours], oy[kMaxNeighbours];
+  const int neighbours = (centre.pixel.flags & 3u) == 1u
+      ? spatial_offsets(slot, f.sample_index, (int)tc.restir_radius, tc.restir_neighbours, ox, oy) : 0;
   if ((centre.pixel.flags & 3u) == 1u) {
     uint32_t accepted = 0;
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < neighbours; ++i) {
       const int nx = (int)px + ox[i], ny = (int)py + oy[i];
       if (nx < 0 || ny < 0 || nx >= (int)f.width || ny >= (int)f.height) continue;
       const uint32_t index = (uint32_t)ny * f.width + (uint32_t)nx;
@@ -481,7 +522,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
               centre.pixel.reservoir.selected_target, 0xffffffffu, 0.0f, selected))
         result.pixel.flags |= 2u;
       uint32_t rng = seed_random(slot, f.sample_index ^ 0x369DEA0Fu);
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < neighbours; ++i) {
         if (sources[i] == 0xffffffffu) continue;
         const RestirReuse source = temporal[sources[i]];
         F3 received = V(0.0f);
@@ -504,7 +545,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
       result.pixel.contribution = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
         result.supporting_candidates = centre.pixel.reservoir.candidate_count;
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < neighbours; ++i) {
           if (sources[i] == 0xffffffffu) continue;
           const RestirReuse source = temporal[sources[i]];
           bool valid_support;

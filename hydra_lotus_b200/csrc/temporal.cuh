@@ -114,6 +114,7 @@ struct TemporalConst {
   uint32_t restir_spatial;
   uint32_t restir_temporal;
   uint32_t restir_radius;
+  uint32_t restir_neighbours;  // 0: four axis neighbours; else disk neighbours
   uint32_t restir_proposal;
   uint32_t sample_index;
   uint32_t max_bounces;

@@ -41,7 +41,8 @@ def main():
         st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT,
                                   light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL, max_bounces=args.depth,
                                   sample_index=0, restir_candidates=8, restir_temporal=1,
-                                  restir_max_history_candidates=20, restir_spatial=1, restir_spatial_radius=30)
+                                  restir_max_history_candidates=20, restir_spatial=1, restir_spatial_radius=30,
+                                  restir_spatial_neighbours=5)
         previous = None
         with renderer.CudaOffscreenRenderer(0) as r:
             renderer.check(r.update_scene(scene), "update_scene")

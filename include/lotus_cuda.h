@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LOTUS_CUDA_ABI_VERSION 4u
+#define LOTUS_CUDA_ABI_VERSION 5u
 
 /* FrameStatus (vulkan_backend.hpp:23-27). */
 #define LOTUS_PASS 0
@@ -187,7 +187,16 @@ typedef struct lotus_settings {
   uint32_t restir_proposal;
   uint32_t environment_background;
   uint32_t output;            /* LOTUS_OUTPUT_* (SceneOutput) */
+  /* The spatial pass's neighbours. 0: the reference's four axis neighbours
+   * at restir_spatial_radius (restir.slang:402-410). 1..8: that many
+   * distinct pixels drawn uniformly from the disk of that radius around the
+   * pixel (the pixel itself excluded), from their own random stream. No
+   * counterpart in the reference. */
+  uint32_t restir_spatial_neighbours;
 } lotus_settings;
+
+/* The most neighbours a disk-mode spatial pass draws. */
+#define LOTUS_MAX_SPATIAL_NEIGHBOURS 8u
 
 /* lotus_settings::output (SceneOutput, vulkan_backend.hpp:617-634): the
  * accumulated path-traced radiance, or a diagnostic of the pixel centre's

@@ -2,7 +2,8 @@
 (TEST INFRASTRUCTURE ONLY).
 
 Compiles, with g++ directly from the sources where they lie under the
-reference tree (default /root/reference, or $LOTUS_REFERENCE), into
+reference tree ($LOTUS_REFERENCE, else ../reference beside this
+checkout), into
 oracle/_ref/:
   - libref.so: backend/vulkan/temporal.cpp, temporal_metadata.cpp,
     reservoir.cpp and core/render-world/render_world.cpp, with this
@@ -19,7 +20,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("LOTUS_REFERENCE", "/root/reference")
+REF = os.environ.get("LOTUS_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 OUT = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT, "libref.so")
 TESTS = ["reservoir-test", "temporal-test", "restir-statistics-test"]

@@ -2950,20 +2950,56 @@ bool SpatialCompatible(const RestirSurfaceO& receiver, const RestirReuseO& recor
       dot(Xyz(receiver.shading_normal), Xyz(source.shading_normal)) >= 0.9f;
 }
 
-void SpatialReservoir(const oracle_scene& s, const FrameConstants& f, const oracle_temporal& tc, uint32_t height,
+// The spatial pass's neighbour offsets (the CUDA kernel's spatial_offsets):
+// the reference's four axis neighbours at the radius (restir.slang:408-410),
+// or, an extension of the reference, `count` distinct offsets drawn
+// uniformly from the disk of the radius without its centre, each the first
+// of up to 16 draws in the enclosing square that falls inside the disk and
+// was not drawn before, from the stream seeded with sample_index ^
+// 0x5BD1E995.
+constexpr int kMaxNeighbours = 8;
+
+int SpatialOffsets(uint32_t slot, uint32_t sample_index, int radius, uint32_t count, int* ox, int* oy) {
+  if (count == 0) {
+    const int ax[4] = {-radius, radius, 0, 0};
+    const int ay[4] = {0, 0, -radius, radius};
+    for (int i = 0; i < 4; ++i) ox[i] = ax[i], oy[i] = ay[i];
+    return 4;
+  }
+  uint32_t rng = SeedRandom(slot, sample_index ^ 0x5BD1E995u);
+  const float side = static_cast<float>(2 * radius + 1);
+  int n = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    for (int t = 0; t < 16; ++t) {
+      const int dx = std::min(static_cast<int>(NextRandom(rng) * side), 2 * radius) - radius;
+      const int dy = std::min(static_cast<int>(NextRandom(rng) * side), 2 * radius) - radius;
+      if ((dx == 0 && dy == 0) || dx * dx + dy * dy > radius * radius) continue;
+      bool seen = false;
+      for (int k = 0; k < n; ++k) seen = seen || (ox[k] == dx && oy[k] == dy);
+      if (seen) continue;
+      ox[n] = dx;
+      oy[n] = dy;
+      ++n;
+      break;
+    }
+  }
+  return n;
+}
+
+void SpatialReservoirAll(const oracle_scene& s, const FrameConstants& f, const oracle_temporal& tc, uint32_t height,
     uint32_t sample_index, const RestirReuseO* temporal, const RestirSurfaceO* surfaces, uint32_t px, uint32_t py,
     RestirReuseO& result, uint32_t* sources) {
   const uint32_t slot = py * f.width + px;
   const RestirReuseO centre = temporal[slot];
   const RestirSurfaceO& receiver = surfaces[slot];
   result = centre;
-  for (int i = 0; i < 4; ++i) sources[i] = 0xffffffffu;
-  const int radius = static_cast<int>(tc.restir_radius);
-  const int ox[4] = {-radius, radius, 0, 0};
-  const int oy[4] = {0, 0, -radius, radius};
+  for (int i = 0; i < kMaxNeighbours; ++i) sources[i] = 0xffffffffu;
   if ((centre.pixel.flags & 3u) != 1u) return;
+  int ox[kMaxNeighbours], oy[kMaxNeighbours];
+  const int neighbours =
+      SpatialOffsets(slot, sample_index, static_cast<int>(tc.restir_radius), tc.restir_neighbours, ox, oy);
   uint32_t accepted = 0;
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < neighbours; ++i) {
     const int nx = static_cast<int>(px) + ox[i], ny = static_cast<int>(py) + oy[i];
     if (nx < 0 || ny < 0 || nx >= static_cast<int>(f.width) || ny >= static_cast<int>(height)) continue;
     const uint32_t index = static_cast<uint32_t>(ny) * f.width + static_cast<uint32_t>(nx);
@@ -2979,7 +3015,7 @@ void SpatialReservoir(const oracle_scene& s, const FrameConstants& f, const orac
           centre.pixel.reservoir.selected_target, 0xffffffffu, 0.0f, selected))
     result.pixel.flags |= 2u;
   uint32_t rng = SeedRandom(slot, sample_index ^ 0x369DEA0Fu);
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < neighbours; ++i) {
     if (sources[i] == 0xffffffffu) continue;
     const RestirReuseO& source = temporal[sources[i]];
     F3 received = V(0.0f);
@@ -3002,7 +3038,7 @@ void SpatialReservoir(const oracle_scene& s, const FrameConstants& f, const orac
   for (int k = 0; k < 4; ++k) result.pixel.contribution[k] = 0.0f;
   if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
     result.supporting_candidates = centre.pixel.reservoir.candidate_count;
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < neighbours; ++i) {
       if (sources[i] == 0xffffffffu) continue;
       const RestirReuseO& source = temporal[sources[i]];
       bool valid_support;
@@ -3024,6 +3060,16 @@ void SpatialReservoir(const oracle_scene& s, const FrameConstants& f, const orac
     else
       SetContribution(result.pixel, estimate, visibility);
   }
+}
+
+// SpatialReservoirAll with the first four sources kept (the product's
+// layout: the reference's four axis neighbours).
+void SpatialReservoir(const oracle_scene& s, const FrameConstants& f, const oracle_temporal& tc, uint32_t height,
+    uint32_t sample_index, const RestirReuseO* temporal, const RestirSurfaceO* surfaces, uint32_t px, uint32_t py,
+    RestirReuseO& result, uint32_t* sources) {
+  uint32_t all[kMaxNeighbours];
+  SpatialReservoirAll(s, f, tc, height, sample_index, temporal, surfaces, px, py, result, all);
+  for (int i = 0; i < 4; ++i) sources[i] = all[i];
 }
 
 }  // namespace

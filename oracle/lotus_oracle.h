@@ -65,6 +65,7 @@ typedef struct oracle_temporal {
   uint32_t restir_history;
   uint32_t restir_max_history;
   uint32_t restir_radius;
+  uint32_t restir_neighbours;  /* 0: four axis neighbours; 1..8: disk neighbours */
   uint32_t restir_proposal;
   uint32_t max_bounces;
 } oracle_temporal;

@@ -124,6 +124,7 @@ class OracleTemporal(C.Structure):
         ("restir_history", C.c_uint32),
         ("restir_max_history", C.c_uint32),
         ("restir_radius", C.c_uint32),
+        ("restir_neighbours", C.c_uint32),
         ("restir_proposal", C.c_uint32),
         ("max_bounces", C.c_uint32),
     ]
@@ -155,6 +156,7 @@ def oracle_temporal(temporal_desc):
     t.restir_history = 1 if (st.restir_temporal and temporal_desc.history_available) else 0
     t.restir_max_history = st.restir_max_history_candidates
     t.restir_radius = st.restir_spatial_radius
+    t.restir_neighbours = st.restir_spatial_neighbours
     t.restir_proposal = st.restir_proposal
     t.max_bounces = st.max_bounces
     return t

@@ -33,13 +33,15 @@ def restir_room_lit():
     return s
 
 
-def temporal_frames(integrator, spatial=True, frames=3, filter_iterations=5, cap=5, lit=False):
+def temporal_frames(integrator, spatial=True, frames=3, filter_iterations=5, cap=5, lit=False, neighbours=0,
+                    radius=2):
     scene = restir_room_lit() if lit else scenes.restir_room(seed=0, size=SIZE, emitters=300)
     settings = abi.default_settings(integrator=integrator,
                                     light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL,
                                     max_bounces=4, sample_index=100, restir_candidates=8,
                                     restir_temporal=1, restir_max_history_candidates=20,
-                                    restir_spatial=1 if spatial else 0, restir_spatial_radius=2)
+                                    restir_spatial=1 if spatial else 0, restir_spatial_radius=radius,
+                                    restir_spatial_neighbours=neighbours)
     descs = []
     previous = None
     for k in range(frames):
@@ -62,10 +64,13 @@ def exact(a, b):
     return np.array_equal(np.frombuffer(a.tobytes(), np.uint8), np.frombuffer(b.tobytes(), np.uint8))
 
 
-@pytest.mark.parametrize("integrator,lit", [(abi.INTEGRATOR_WAVEFRONT, False), (abi.INTEGRATOR_REFERENCE, False),
-                                             (abi.INTEGRATOR_WAVEFRONT, True)])
-def test_temporal_passes_match_checkers(cuda, integrator, lit):
-    scene, descs = temporal_frames(integrator, lit=lit)
+@pytest.mark.parametrize("integrator,lit,neighbours,radius", [
+    (abi.INTEGRATOR_WAVEFRONT, False, 0, 2), (abi.INTEGRATOR_REFERENCE, False, 0, 2),
+    (abi.INTEGRATOR_WAVEFRONT, True, 0, 2),
+    # The disk mode: five neighbours drawn from a 30-pixel disk.
+    (abi.INTEGRATOR_WAVEFRONT, False, 5, 30)])
+def test_temporal_passes_match_checkers(cuda, integrator, lit, neighbours, radius):
+    scene, descs = temporal_frames(integrator, lit=lit, neighbours=neighbours, radius=radius)
     o = oracle.OracleTemporalScene(scene)
     with cuda.CudaOffscreenRenderer(0) as r:
         cuda.check(r.update_scene(scene), "update_scene")
