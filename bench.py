@@ -400,23 +400,30 @@ def scene_update_report(renderer_module, repeats=3):
     return out
 
 
-def temporal_report(renderer_module, frames=24):
-    """Frames per second of the temporal configurations at 1920x1080, 1 spp
-    per frame, over an orbiting camera (the median device time of frames
-    8.., once the histories are full): config 3 (ReSTIR DI with temporal
-    reuse, M cap 20, one spatial pass of 5 neighbours drawn from a 30 px disk; SVGF with 5 a-trous
-    iterations; the box room with 10,000 emissive floor triangles) and
-    config 5 (the learned radiance cache plus the same ReSTIR DI, no
-    a-trous iterations), depth 6."""
+def temporal_report(renderer_module, frames=120, checked=(0, 30, 60, 90, 119), ref_spp=4096, rows=64):
+    """The temporal configurations at 1920x1080, 1 spp per frame, over the
+    120-frame orbit of the box room with 10,000 emissive floor triangles,
+    depth 6: config 3 (ReSTIR DI with temporal reuse, M cap 20, one spatial
+    pass of 5 neighbours drawn from a 30 px disk; SVGF with FP16 moments
+    and 5 a-trous iterations) and config 5 (the learned radiance cache plus
+    the same ReSTIR DI, no a-trous iterations). Frames per second from the
+    median device time of frames 8.. (the histories full). Frames 0, 30,
+    60, 90 and 119 of config 3 are each checked against an FP64 plain-PT
+    reference of that frame's camera at 4,096 spp over three 64-row bands
+    (top, middle, bottom): the relMSE (epsilon 1e-2) of the filtered
+    composite and of the frame's own 1-spp batch."""
+    from hydra_lotus_b200 import convergence, metrics
     width, height = 1920, 1080
     scene = scenes.restir_room(seed=0, size=height, emitters=10000, aspect=width / height)
     st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT,
                               light_sampling=abi.LIGHT_SAMPLING_RESTIR_INITIAL, max_bounces=6, sample_index=0,
                               restir_candidates=8, restir_temporal=1, restir_max_history_candidates=20,
                               restir_spatial=1, restir_spatial_radius=30, restir_spatial_neighbours=5)
-    out = {"resolution": [width, height], "depth": 6, "spp_per_frame": 1}
+    band_list = convergence.bands(height, rows)
+    out = {"resolution": [width, height], "depth": 6, "spp_per_frame": 1, "orbit_frames": frames}
     for name, cache, filt in (("restir+svgf", False, 5), ("cache+restir", True, 0)):
         ms = []
+        checks = []
         previous = None
         with renderer_module.CudaOffscreenRenderer(0) as r:
             renderer_module.check(r.update_scene(scene), "update_scene")
@@ -424,14 +431,34 @@ def temporal_report(renderer_module, frames=24):
                 r.configure_cache(enable=True, seed=1)
             for k in range(frames):
                 view, w2c = scenes.orbit_camera(k, frames=120, aspect=width / height)
-                frame = abi.make_frame(w2c, width, height, st, 1, read_back=False)
+                check = not cache and k in checked
+                frame = abi.make_frame(w2c, width, height, st, 1, read_back=check)
                 d = abi.temporal_desc(frame, view, previous[0] if previous else None,
                                       previous[1] if previous else None, history_available=k > 0,
-                                      accumulate_radiance=True, max_history_samples=5, filter_iterations=filt)
-                res, _ = r.render_temporal(d)
+                                      accumulate_radiance=True, max_history_samples=5, filter_iterations=filt,
+                                      moment_precision=abi.MOMENTS_FP16)
+                res, img = r.render_temporal(d)
                 renderer_module.check(res, name)
                 previous = (view, w2c)
                 ms.append(res.gpu_ms)
+                if check:
+                    batch = r.read_product(abi.PRODUCT_BATCH, height, width)
+                    checks.append((k, img.copy(), batch.copy(), w2c))
+        if checks:
+            entries = []
+            with renderer_module.CudaOffscreenRenderer(0) as ref_r:
+                renderer_module.check(ref_r.update_scene(scene), "update_scene")
+                camera = scene.world_to_clip
+                for k, img, batch, w2c in checks:
+                    scene.world_to_clip = w2c
+                    ref, noise, _ = convergence.reference(ref_r, scene, 6, ref_spp, band_list)
+                    entries.append({"frame": k,
+                                    "relmse_composite": float(f"{metrics.relmse(convergence.band_pixels(img, band_list), ref):.4g}"),
+                                    "relmse_batch_1spp": float(f"{metrics.relmse(convergence.band_pixels(batch, band_list), ref):.4g}"),
+                                    "reference_noise": float(f"{noise:.3g}")})
+                scene.world_to_clip = camera
+            out[name + "_checked_frames"] = {"reference": f"plain PT, {ref_spp} spp, FP64, three {rows}-row bands",
+                                            "frames": entries}
         med = statistics.median(ms[8:])
         out[name] = {"ms_per_frame": round(med, 3), "frames_per_s": round(1e3 / med, 1)}
     return out

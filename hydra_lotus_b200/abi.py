@@ -29,6 +29,9 @@ STATIC_MAX_PIXELS = 65536
 FRAME_TIMINGS = 1
 FRAME_COUNT_VISITS = 2
 
+MOMENTS_FP32 = 0
+MOMENTS_FP16 = 1
+
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
@@ -229,7 +232,7 @@ class TemporalDesc(C.Structure):
         ("max_history_samples", C.c_uint32),
         ("filter_iterations", C.c_uint32),
         ("history_rectification", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("moment_precision", C.c_uint32),
     ]
 
 
@@ -311,7 +314,7 @@ except ImportError:  # pragma: no cover
 
 def temporal_desc(frame, current_view, previous_view=None, previous_world_to_clip=None,
                   history_available=False, accumulate_radiance=False, max_history_samples=32,
-                  filter_iterations=0, validation=DEFAULT_VALIDATION):
+                  filter_iterations=0, validation=DEFAULT_VALIDATION, moment_precision=0):
     d = TemporalDesc()
     d.frame = frame
     d.current_view[:] = [float(v) for v in current_view]
@@ -323,6 +326,7 @@ def temporal_desc(frame, current_view, previous_view=None, previous_world_to_cli
     d.accumulate_radiance = 1 if accumulate_radiance else 0
     d.max_history_samples = max_history_samples
     d.filter_iterations = filter_iterations
+    d.moment_precision = moment_precision
     return d
 
 

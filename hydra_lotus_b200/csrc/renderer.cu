@@ -705,7 +705,7 @@ struct Renderer {
     uint32_t frames = 0;          // temporal frames rendered since the last reset
     uint32_t sample_offset = 0;
     bool key_valid = false;
-    uint32_t key[17] = {};
+    uint32_t key[18] = {};
     bool restir_ran = false, accumulate_ran = false, spatial_ran = false, filter_ran = false;
   } temporal;
   std::vector<lotus_instance> host_instances;
@@ -2176,6 +2176,7 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
     return fail("temporal radiance requires history samples in [1, 65536]");
   if (td.filter_iterations > 8 || (td.filter_iterations != 0 && !accumulate))
     return fail("temporal filtering requires radiance accumulation and at most 8 iterations");
+  if (td.moment_precision > LOTUS_MOMENTS_FP16) return fail("unknown moment precision");
   if (td.history_rectification != 0)
     return fail("history rectification other than None is not built");
   if (st.integrator > LOTUS_INTEGRATOR_WAVEFRONT) return fail("unknown integrator");
@@ -2226,10 +2227,10 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
           R.ok(T.vis_counters.resize(3 * kVisibilityPasses), "visibility queue", detail);
   if (!okb) return poison(detail);
   // The transport key: a change drops the history (vulkan_backend.cpp:1766-1781).
-  uint32_t key[17] = {st.integrator, st.light_sampling, st.restir_proposal, st.restir_candidates,
+  uint32_t key[18] = {st.integrator, st.light_sampling, st.restir_proposal, st.restir_candidates,
       st.restir_temporal, st.restir_max_history_candidates, st.restir_spatial, st.restir_spatial_radius,
       td.accumulate_radiance, st.sample_index, st.max_bounces, st.environment_background, 0, 0, 0, 0,
-      st.restir_spatial_neighbours};
+      st.restir_spatial_neighbours, td.moment_precision};
   std::memcpy(&key[12], t.clear_color, sizeof(t.clear_color));
   const bool fresh_batch = accumulate || reservoirs;
   bool previous = td.history_available != 0 && T.frames > 0;
@@ -2265,6 +2266,7 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   tc.fresh_samples = d.frame_count;
   tc.history_cap = td.max_history_samples;
   tc.filter_iterations = td.filter_iterations;
+  tc.moments_half = td.moment_precision == LOTUS_MOMENTS_FP16 ? 1u : 0u;
   tc.restir_candidates = restir ? st.restir_candidates : 0u;
   tc.restir_history = reuse && previous ? 1u : 0u;
   tc.restir_max_history = st.restir_max_history_candidates;

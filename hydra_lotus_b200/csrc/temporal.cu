@@ -7,6 +7,7 @@
 // thread per pixel; every pass is a separate launch, so each reads only what
 // the preceding one finished writing, as the reference's barriers order it.
 #include <cooperative_groups.h>
+#include <cuda_fp16.h>
 
 #include "../../include/lotus_cuda.h"
 #include "temporal_passes.cuh"
@@ -573,6 +574,14 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
 // ---------------------------------------------------------------------------
 // SVGF.
 
+// A luminance moment rounded to half precision (round to nearest even),
+// saturating at the largest finite half, 65504 (a NaN stays a NaN, so the
+// next frame drops the history as the FP32 mode does): the moments stored
+// by the FP16 moment mode.
+__device__ __forceinline__ float half_moment(float m) {
+  return __half2float(__float2half_rn(m > 65504.0f ? 65504.0f : m));
+}
+
 // AccumulateTemporalRadiance (temporal.slang:229-267), without history
 // rectification: the count-capped blend of the fresh batch and the
 // reprojected history, and its illumination luminance moments.
@@ -608,6 +617,10 @@ __global__ void __launch_bounds__(kBlock) k_svgf_accumulate(const TemporalConst*
         m2 += (h.second_moment - m2) * blend;
         o.sample_count = count;
       }
+    }
+    if (tc.moments_half) {
+      m1 = half_moment(m1);
+      m2 = half_moment(m2);
     }
     o.first_moment = m1;
     o.second_moment = m2;

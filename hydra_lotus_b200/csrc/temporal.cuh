@@ -108,6 +108,7 @@ struct TemporalConst {
   uint32_t fresh_samples;
   uint32_t history_cap;
   uint32_t filter_iterations;
+  uint32_t moments_half;  // the accumulation stores its moments at half precision
   uint32_t restir_candidates;
   uint32_t restir_history;     // temporal reuse reads the preceding reservoirs
   uint32_t restir_max_history;

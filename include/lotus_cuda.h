@@ -371,8 +371,17 @@ typedef struct lotus_temporal_desc {
   uint32_t max_history_samples;      /* 1..65536 when accumulating */
   uint32_t filter_iterations;        /* 0..8; needs accumulate_radiance */
   uint32_t history_rectification;    /* TemporalHistoryRectification; only None (0) is built */
-  uint32_t reserved;
+  /* Precision of the luminance moments the temporal accumulation keeps
+   * between frames. LOTUS_MOMENTS_FP32: as the reference. LOTUS_MOMENTS_FP16:
+   * each blended moment is rounded to half precision (saturating at 65504)
+   * where the reference stores it, the blend itself staying FP32; the
+   * record keeps the reference's 32-byte layout. No counterpart in the
+   * reference. */
+  uint32_t moment_precision;
 } lotus_temporal_desc;
+
+#define LOTUS_MOMENTS_FP32 0u
+#define LOTUS_MOMENTS_FP16 1u
 
 /* One instance's temporal identity (the reference's TemporalInstanceRecord,
  * backend/vulkan/temporal_metadata.hpp), in scene instance order. */

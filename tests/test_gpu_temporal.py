@@ -17,10 +17,11 @@ SIZE = 64
 # The reference's GPU-vs-CPU tolerances for the SVGF passes
 # (docs/reports/2026-10-18-svgf-filter.md): composite max relative error
 # 1.2e-5 and variance max absolute error 9.3e-5 (for variances near 1; a
-# relative 1e-6, a few float ulps, covers large ones).
+# relative 4e-6, 32 float ulps, covers large ones, such as the variance of
+# 1000 a pixel of the disk-neighbour case reaches).
 COMPOSITE_RTOL = 1.2e-5
 VARIANCE_ATOL = 9.3e-5
-VARIANCE_RTOL = 1e-6
+VARIANCE_RTOL = 4e-6
 
 
 def restir_room_lit():
@@ -150,3 +151,41 @@ def test_restir_converges_to_mis_path_tracer(cuda):
     z = (a.mean() - b.mean()) / np.sqrt(a.var() / n + b.var() / n)
     print("MIS", a.mean(), "ReSTIR", b.mean(), "z", z, "variance ratio", b.var() / a.var())
     assert abs(z) < 4.0, z
+
+
+def test_fp16_moments(cuda):
+    """The FP16 moment mode (LOTUS_MOMENTS_FP16): the fresh frame's moments
+    are the FP32 mode's rounded to half precision; over later frames each
+    stored moment stays within a few half-precision rounding steps of the
+    FP32 mode's (relative 4e-3, the blend reading rounded history); the
+    variance the GPU derives from the stored moments matches the
+    reference's CPU EstimateTemporalVariance on the same moments at its
+    published tolerances, and the composite stays within 1e-3 relMSE of
+    the FP32 mode's."""
+    scene, descs32 = temporal_frames(abi.INTEGRATOR_WAVEFRONT)
+    _, descs16 = temporal_frames(abi.INTEGRATOR_WAVEFRONT)
+    for d in descs16:
+        d.moment_precision = abi.MOMENTS_FP16
+    from hydra_lotus_b200 import metrics
+    with cuda.CudaOffscreenRenderer(0) as r32, cuda.CudaOffscreenRenderer(0) as r16:
+        cuda.check(r32.update_scene(scene), "update_scene")
+        cuda.check(r16.update_scene(scene), "update_scene")
+        for k, (d32, d16) in enumerate(zip(descs32, descs16)):
+            res32, c32 = r32.render_temporal(d32)
+            cuda.check(res32, "FP32 frame")
+            res16, c16 = r16.render_temporal(d16)
+            cuda.check(res16, "FP16 frame")
+            p32 = products(r32, SIZE, SIZE, ["surface", "radiance"])
+            p16 = products(r16, SIZE, SIZE, ["surface", "radiance"])
+            for m in (0, 1):
+                a, b = p32["radiance"]["moments"][..., m], p16["radiance"]["moments"][..., m]
+                assert np.array_equal(b, b.astype(np.float16).astype(np.float32)), f"{m} is not half-valued"
+                if k == 0:
+                    assert np.array_equal(b, a.astype(np.float16).astype(np.float32)), m
+                else:
+                    assert np.all(np.abs(a - b) <= 4e-3 * np.abs(a) + 1e-7), (m, np.abs(a - b).max())
+            var = ref.estimate_variance(p16["surface"], p16["radiance"], 1, d16.max_history_samples)
+            np.testing.assert_allclose(p16["radiance"]["variance"], var, rtol=VARIANCE_RTOL, atol=VARIANCE_ATOL)
+            err = metrics.relmse(c16, c32)
+            print(k, "composite relMSE FP16 vs FP32", err)
+            assert err <= 1e-3, err
