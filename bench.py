@@ -249,9 +249,10 @@ def _seconds(entry):
 def time_to_relmse_report(renderer_module):
     """The metric's first half: device seconds to relMSE 1e-3 (epsilon 1e-2)
     at 1080p, depth 6, static camera, for plain wavefront PT, the learned
-    radiance cache, ReSTIR DI in three modes (temporal + spatial reuse,
-    initial candidates only, spatial reuse only; the spatial pass draws 5
-    neighbours from a 30-pixel disk) and the cache with each: on the box
+    radiance cache (paths ending into it at their second vertex, and at
+    their third: `cache_v3`), ReSTIR DI in three modes (temporal + spatial
+    reuse, initial candidates only, spatial reuse only; the spatial pass
+    draws 5 neighbours from a 30-pixel disk) and the cache with ReSTIR: on the box
     room with 10,000 emissive floor triangles (power log-normal, sigma 2;
     `many_lights`) and on the config-1 box room with its one ceiling light
     (`single_light`). The reference is plain PT at 16,384 spp with FP64
@@ -262,13 +263,15 @@ def time_to_relmse_report(renderer_module):
     many = _time_to_relmse(
         renderer_module, scenes.box_room_wide(seed=0, emitters=10000),
         "box room + 10,000 emissive floor triangles (power log-normal sigma 2), 1920x1080, depth 6, static camera",
-        {"plain": 40.0, "cache": 20.0, "restir": 4.0, "restir_initial": 4.0, "restir_spatial": 4.0,
-         "cache+restir": 20.0, "cache+restir_initial": 20.0, "cache+restir_spatial": 20.0})
+        {"plain": 40.0, "cache": 12.0, "cache_v3": 12.0, "restir": 4.0, "restir_initial": 4.0,
+         "restir_spatial": 4.0, "cache+restir": 12.0, "cache+restir_initial": 12.0,
+         "cache_v3+restir_initial": 12.0})
     single = _time_to_relmse(
         renderer_module, scenes.box_room_wide(seed=0),
         "config-1 box room (one ceiling quad light), 1920x1080, depth 6, static camera",
-        {"plain": 10.0, "cache": 10.0, "restir": 4.0, "restir_initial": 4.0, "restir_spatial": 4.0,
-         "cache+restir": 10.0, "cache+restir_initial": 10.0, "cache+restir_spatial": 10.0})
+        {"plain": 10.0, "cache": 6.0, "cache_v3": 6.0, "restir": 3.0, "restir_initial": 3.0,
+         "restir_spatial": 3.0, "cache+restir": 6.0, "cache+restir_initial": 6.0,
+         "cache_v3+restir_initial": 6.0})
     return {"many_lights": many, "single_light": single}
 
 
@@ -281,7 +284,7 @@ def time_to_relmse_summary(report):
         methods = [m for m in rep if isinstance(rep[m], dict) and "checkpoints" in rep[m]]
         secs = {m: _seconds(rep[m]) for m in methods}
         plain = secs.get("plain")
-        modes = [m for m in methods if m.startswith("cache+restir")]
+        modes = [m for m in methods if m.startswith("cache") and "restir" in m]
         best = min(modes, key=lambda m: secs[m] if secs[m] else float("inf"))
         entry = {"noise": rep["reference"]["relmse_noise_subtracted"],
                  "seconds": {m: (round(v, 3) if v else None) for m, v in secs.items()},

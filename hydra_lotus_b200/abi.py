@@ -252,7 +252,7 @@ class CacheDesc(C.Structure):
     _fields_ = [("enable", C.c_uint32), ("levels", C.c_uint32), ("log2_table", C.c_uint32),
                 ("min_resolution", C.c_uint32), ("max_resolution", C.c_uint32),
                 ("training_stride", C.c_uint32), ("training_steps", C.c_uint32), ("seed", C.c_uint32),
-                ("learning_rate", C.c_float), ("reserved", C.c_uint32 * 3)]
+                ("learning_rate", C.c_float), ("terminate_bounce", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
 
 CACHE_INPUTS = 64

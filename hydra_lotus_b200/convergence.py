@@ -29,6 +29,9 @@ Methods:
   restir_spatial   the initial candidates and one spatial pass, no temporal
                    reuse.
   cache+<restir*>  the cache with one of the ReSTIR modes.
+  cache_v3...      the same with the paths ending into the cache at their
+                   third vertex (lotus_cache_desc::terminate_bounce 2)
+                   instead of the second.
 """
 
 import numpy as np
@@ -123,7 +126,7 @@ def time_to_relmse(r, scene, method, ref, noise, depth, band_list, target=1e-3, 
     cache = method.startswith("cache")
     restir = method.split("+")[-1] if "restir" in method else None
     if cache:
-        r.configure_cache(enable=True, seed=1)
+        r.configure_cache(enable=True, seed=1, terminate_bounce=2 if method.startswith("cache_v3") else 1)
     seconds = 0.0
     points = []
 

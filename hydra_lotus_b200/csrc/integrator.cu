@@ -429,7 +429,8 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
 
 // Shade (wavefront.slang:264-285) with next event estimation's shadow ray
 // deferred to the shadow queue. With the radiance cache, the paths reaching
-// their second vertex (bounce 1) end into the cache there (a query of the
+// the cache's vertex (bounce 1, the second vertex, unless configured
+// otherwise) end into the cache there (a query of the
 // cache records the vertex and the path's throughput), except the training
 // paths, one in `stride` chosen per sample, which record the vertex, their
 // throughput and radiance so far and carry on.
@@ -520,7 +521,7 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
 }
 
 // The training targets once the sample's paths have ended: the radiance a
-// training path gathered after its second vertex's emission, divided by its
+// training path gathered after its cache vertex's emission, divided by its
 // throughput on arrival there.
 __global__ void k_cache_targets(CacheQueues C, PathState P) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -537,9 +538,12 @@ __global__ void k_cache_targets(CacheQueues C, PathState P) {
 
 constexpr unsigned kFullWarp = 0xFFFFFFFFu;
 // Resident blocks per SM the persistent tracing kernels are compiled for:
-// six blocks of 128 (80 registers a thread) hide more of the node loads'
-// latency than five at the registers the code would take unbounded.
-constexpr int kTraceBlocksPerSm = 6;
+// seven blocks of 128 (72 registers a thread; the extension walk spills a
+// few words to L1) hide more of the node loads' latency than six at 80
+// registers (sphere field, 1080p: extension kernels 2.30 -> 2.16 ms per
+// sample together with the approximate slab reciprocal and the evict_last
+// node loads).
+constexpr int kTraceBlocksPerSm = 7;
 constexpr uint32_t kDefaultRefillBelow = 24;
 
 // The persistent kernels' ray fetch: when fewer than `refill_below` lanes
@@ -985,9 +989,10 @@ uint32_t choose_wavefront_rounds(const uint32_t* counts, uint32_t camera, uint32
   return max_bounces + 1;
 }
 
-uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, bool cache) {
+uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, uint32_t cache_bounce) {
   uint32_t rounds = requested ? requested : LOTUS_WAVEFRONT_ROUNDS;
-  if (cache) rounds = std::max(rounds, 2u);
+  // The radiance cache's vertex is shaded in the rounds.
+  if (cache_bounce) rounds = std::max(rounds, cache_bounce + 1);
   return count_visits || max_bounces < rounds ? max_bounces + 1 : rounds;
 }
 
@@ -1028,7 +1033,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   // Bounces 0 .. rounds - 1 as wavefront rounds; the paths queued for bounce
   // `rounds` (if any can be) go to the tail kernel. Counting visits keeps
   // every bounce in rounds, as the counted kernels are the rounds' own.
-  const uint32_t rounds = wavefront_rounds(max_bounces, count, tuning.rounds, C.enabled);
+  const uint32_t rounds = wavefront_rounds(max_bounces, count, tuning.rounds, C.enabled ? C.bounce : 0u);
   for (uint32_t b = 0; b < rounds; ++b) {
     if (b != 0) {
       Timed t(profile, stream, 1);
@@ -1047,7 +1052,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     }
     {
       Timed t(profile, stream, 2);
-      const bool cache_vertex = C.enabled && b == 1;
+      const bool cache_vertex = C.enabled && b == C.bounce;
       if (cache_vertex && analytic)
         k_wf_shade<true, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
       else if (cache_vertex)

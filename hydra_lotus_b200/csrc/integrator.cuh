@@ -50,6 +50,7 @@ struct CacheQueues {
   bool enabled = false;
   uint32_t stride = 32;           // one path in `stride` trains
   uint32_t steps = 1;             // training steps per sample
+  uint32_t bounce = 1;            // paths end into the cache at this bounce's vertex
   RadianceCache* cache = nullptr;
   CacheRecord* queries = nullptr;
   uint32_t* query_slots = nullptr;
@@ -122,7 +123,7 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
 // default LOTUS_WAVEFRONT_ROUNDS), the tail kernel taking the rest; all of
 // them when visits are counted, and with the radiance cache at least
 // bounces 0 and 1 (its vertex is shaded in round 1).
-uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, bool cache = false);
+uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, uint32_t cache_bounce = 0);
 
 // The rounds a sample should run, from a sample's queue counts (the
 // wavefront kernels' per-bounce words, 3 per bounce) and its camera rays:

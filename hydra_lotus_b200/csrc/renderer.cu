@@ -1419,6 +1419,7 @@ CacheQueues cache_queues(Renderer& R) {
   if (!C.enabled) return C;
   C.stride = R.cache_desc.training_stride ? R.cache_desc.training_stride : 32u;
   C.steps = R.cache_desc.training_steps ? R.cache_desc.training_steps : 1u;
+  C.bounce = R.cache_desc.terminate_bounce ? R.cache_desc.terminate_bounce : 1u;
   C.cache = &R.cache;
   C.queries = R.cache_queries.ptr;
   C.query_slots = R.cache_query_slots.ptr;
@@ -1644,7 +1645,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   TraceTuning tuning = R.tuning;
   if (tuning.rounds == 0 && R.auto_rounds != 0 && R.rounds_key == gk) tuning.rounds = R.auto_rounds;
   // The rounds the call's last sample ran (the frame result reports them).
-  uint32_t last_rounds = wavefront_rounds(st.max_bounces, want_visits, tuning.rounds, use_cache);
+  uint32_t last_rounds = wavefront_rounds(st.max_bounces, want_visits, tuning.rounds, use_cache ? cq.bounce : 0u);
   const bool choose_rounds = wavefront && R.tuning.rounds == 0 && !(R.rounds_key == gk);
   // Two samples at a time where two or more are added without the radiance
   // cache (which trains between samples) and outside the profiled last one:
@@ -1715,7 +1716,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
       continue;
     }
     last_in_chain = false;
-    last_rounds = wavefront_rounds(st.max_bounces, profiled && want_visits, tuning.rounds, use_cache);
+    last_rounds = wavefront_rounds(st.max_bounces, profiled && want_visits, tuning.rounds, use_cache ? cq.bounce : 0u);
     if (profiled) {
       if (wavefront)
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
@@ -1725,7 +1726,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
             &profile);
       launch_advance(R.frame_const.ptr, s);
     } else if (wavefront) {
-      gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, use_cache);
+      gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, use_cache ? cq.bounce : 0u);
       if (!R.graph || !(R.graph_key == gk)) {
         if (R.graph) {
           cudaGraphExecDestroy(R.graph);
@@ -2573,9 +2574,9 @@ extern "C" int32_t lotus_cuda_configure_cache(lotus_cuda_renderer* h, const lotu
   c.learning_rate = d->learning_rate > 0.0f ? d->learning_rate : 1e-2f;
   c.seed = d->seed;
   if (c.levels > (uint32_t)kCacheMaxLevels || c.log2_size < 10 || c.log2_size > 22 || c.min_resolution < 2 ||
-      c.max_resolution < c.min_resolution || !std::isfinite(c.learning_rate)) {
+      c.max_resolution < c.min_resolution || !std::isfinite(c.learning_rate) || d->terminate_bounce > 16) {
     copy_detail(detail, detail_size, "cache settings out of range (levels 1..16, log2_table 10..22, "
-        "2 <= min_resolution <= max_resolution)");
+        "2 <= min_resolution <= max_resolution, terminate_bounce 0..16)");
     return LOTUS_FAIL;
   }
   cudaError_t e = R->cache.configure(c, R->scene_lo, R->scene_hi, R->stream);

@@ -200,6 +200,44 @@ __device__ __forceinline__ F3 safe_inverse(F3 d) {
   return V(inv(d.x), inv(d.y), inv(d.z));
 }
 
+// The reciprocal direction of the walks' slab tests, with the hardware's
+// approximate reciprocal (a few ulps): a slab test's far distance carries a
+// relative margin of 2^-18, far above that error, so boxes are still never
+// culled where a triangle test could accept a hit. The exact safe_inverse
+// stays where a box test decides a result (the light hierarchy's crossings).
+__device__ __forceinline__ F3 slab_inverse(F3 d) {
+  auto inv = [](float x) {
+    const float y = fabsf(x) > 1e-30f ? x : (x < 0.0f ? -1e-30f : 1e-30f);
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
+    return r;
+  };
+  return V(inv(d.x), inv(d.y), inv(d.z));
+}
+
+// Read-only loads of the BVH and triangle pools that ask L1 to keep their
+// lines over the path state's streaming accesses (evict_last).
+__device__ __forceinline__ float4 ld_keep(const float4* p) {
+  float4 v;
+  asm("ld.global.nc.L1::evict_last.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ int4 ld_keep_i(const int4* p) {
+  int4 v;
+  asm("ld.global.nc.L1::evict_last.v4.s32 {%0,%1,%2,%3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  return v;
+}
+// A node's boxes and child references; interior visits never read `count`.
+__device__ __forceinline__ Bvh4Node load_node(const Bvh4Node* p) {
+  Bvh4Node n;
+  n.lo_x = ld_keep(&p->lo_x); n.hi_x = ld_keep(&p->hi_x);
+  n.lo_y = ld_keep(&p->lo_y); n.hi_y = ld_keep(&p->hi_y);
+  n.lo_z = ld_keep(&p->lo_z); n.hi_z = ld_keep(&p->hi_z);
+  n.child = ld_keep_i(&p->child);
+  n.count = make_int4(0, 0, 0, 0);
+  return n;
+}
+
 struct WatertightRay {
   F3 org;
   uint32_t axes;  // kx | ky << 2 | kz << 4
@@ -338,7 +376,7 @@ __device__ __forceinline__ void walk_begin(const SceneView& S, Walk& W, F3 origi
     float tmin, float tmax) {
   W.origin = origin;
   W.direction = direction;
-  W.inv = safe_inverse(direction);
+  W.inv = slab_inverse(direction);
   W.w.org = origin;
   W.tmin = tmin;
   W.best = tmax;
@@ -386,7 +424,7 @@ __device__ __forceinline__ void walk_check_end(const SceneView& S, const Walk& W
 template <bool kCount>
 __device__ __forceinline__ void walk_visit_node(const SceneView& S, Walk& W, WalkStack& stack,
     TraversalCounters* counters) {
-  const Bvh4Node n = W.in_blas ? S.blas[W.cur] : S.tlas[W.cur];
+  const Bvh4Node n = load_node(W.in_blas ? S.blas + W.cur : S.tlas + W.cur);
   if (kCount) ++counters->nodes;
   ++W.steps;
   float tn[4];
@@ -427,7 +465,7 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
   ++W.steps;
   for (uint32_t k = 0; k < count; ++k) {
     const float4* tv = S.tris + kTriStride * (size_t)(first + k);
-    const float4 a = tv[0], b = tv[1], cc = tv[2];
+    const float4 a = ld_keep(tv), b = ld_keep(tv + 1), cc = ld_keep(tv + 2);
     if (kCount) ++counters->triangles;
     float t, b1, b2;
     if (!intersect_triangle(W.w, V(a), V(b), V(cc), t, b1, b2)) continue;
@@ -472,7 +510,7 @@ __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStac
   if (cur == kExitInstance) {
     W.in_blas = false;
     W.w.org = W.origin;
-    W.inv = safe_inverse(W.direction);
+    W.inv = slab_inverse(W.direction);
   } else if (W.in_blas) {
     if (walk_test_leaf<kAnyHit, kCount>(S, W, cur, rng, counters)) return true;
   } else {
@@ -485,7 +523,7 @@ __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStac
       stack[W.sp++] = kExitInstance;
       const F3 o = row_point(rec.inv, W.origin);
       const F3 d = row_vector(rec.inv, W.direction);
-      W.inv = safe_inverse(d);
+      W.inv = slab_inverse(d);
       W.w = prepare_ray(o, d);
       W.instance = instance;
       W.opaque = (rec.flags & kInstanceOpaque) != 0;

@@ -539,7 +539,12 @@ typedef struct lotus_cache_desc {
   uint32_t training_steps;   /* Adam steps per sample (0: 1) */
   uint32_t seed;             /* weight and grid initialisation */
   float learning_rate;       /* Adam step size (0: 1e-2) */
-  uint32_t reserved[3];
+  /* The bounce whose vertex the paths end into the cache at, 1..16 (0: 1,
+   * the second vertex). A later vertex shrinks the cache's bias in the
+   * image by the throughput of the bounces before it, at the cost of
+   * tracing them. */
+  uint32_t terminate_bounce;
+  uint32_t reserved[2];
 } lotus_cache_desc;
 
 /* (Re)creates the cache over the resident scene's bounds (a unit box

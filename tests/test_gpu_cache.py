@@ -142,3 +142,33 @@ def test_cache_gains_over_plain_pt(cuda):
     e_bias = metrics.relmse(cached_long, ref)
     assert e_cache < 0.6 * e_plain, f"cache {e_cache:.4g} vs plain {e_plain:.4g} at 16 spp"
     assert e_bias < 5e-3, f"cache at 512 spp: relMSE {e_bias:.4g} against plain PT"
+
+
+def test_later_cache_vertex_shrinks_bias(cuda):
+    """Paths ending into the cache at their third vertex
+    (lotus_cache_desc::terminate_bounce 2) query it less often than at the
+    second, and the trained cache's bias against plain PT is smaller."""
+    from hydra_lotus_b200 import abi, metrics
+    scene = scenes.box_room(seed=0, size=64)
+
+    def settings(sample_index):
+        return abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                                    max_bounces=6, sample_index=sample_index)
+
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        res, ref = r.render_scene(scene.frame(settings(1 << 24), frame_count=8192, read_back=True))
+        cuda.check(res, "reference")
+        out = {}
+        for bounce in (1, 2):
+            r.configure_cache(enable=True, seed=1, terminate_bounce=bounce)
+            res, _ = r.render_scene(scene.frame(settings(5000), frame_count=128, read_back=True))
+            cuda.check(res, "cache warm-up")
+            queries = res.cache_queries
+            res, img = r.render_scene(scene.frame(settings(20000), frame_count=512, read_back=True))
+            cuda.check(res, "cache, long")
+            out[bounce] = (queries, metrics.relmse(img, ref))
+        r.configure_cache(enable=False, seed=1)
+    print(out)
+    assert 0 < out[2][0] < out[1][0]
+    assert out[2][1] < out[1][1]
