@@ -28,6 +28,8 @@ STATIC_MAX_PIXELS = 65536
 
 FRAME_TIMINGS = 1
 FRAME_COUNT_VISITS = 2
+FRAME_DEPTH = 4
+FRAME_DEPTH_KEEP = 8
 
 MOMENTS_FP32 = 0
 MOMENTS_FP16 = 1
@@ -35,7 +37,7 @@ MOMENTS_FP16 = 1
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 # lotus_settings::output (SceneOutput).
 OUTPUT_RADIANCE = 0
@@ -148,7 +150,7 @@ class Target(C.Structure):
         ("data_window", C.c_int32 * 4),
         ("clear_color", C.c_float * 4),
         ("read_back", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("clear_depth", C.c_float),
     ]
 
 
@@ -347,7 +349,7 @@ def default_settings(**overrides):
 
 def make_frame(world_to_clip, width, height, settings=None, frame_count=1,
                clear_color=(0.0, 0.0, 0.0, 0.0), data_window=(0, 0, 0, 0),
-               display_window=(0.0, 0.0, 0.0, 0.0), read_back=True, flags=0):
+               display_window=(0.0, 0.0, 0.0, 0.0), read_back=True, flags=0, clear_depth=1.0):
     f = FrameDesc()
     for i, v in enumerate(world_to_clip):
         f.world_to_clip[i] = float(v)
@@ -358,6 +360,7 @@ def make_frame(world_to_clip, width, height, settings=None, frame_count=1,
         f.target.data_window[i] = data_window[i]
         f.target.clear_color[i] = clear_color[i]
     f.target.read_back = 1 if read_back else 0
+    f.target.clear_depth = clear_depth
     f.settings = settings if settings is not None else default_settings()
     f.frame_count = frame_count
     f.flags = flags

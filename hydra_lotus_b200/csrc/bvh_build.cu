@@ -680,9 +680,116 @@ __global__ void k_collapse4(const BvhNode* __restrict__ bin, uint32_t first, uin
   wide[i] = w;
 }
 
+// Refit after a point edit (the reference refits its BLAS there,
+// backend/vulkan/gpu_scene.cpp:1899-1950 in hydra-lotus): the topology is
+// kept and the boxes follow the new positions. First the leaf-ordered
+// triangle pool takes the new corners (the primitive index each record
+// keeps in its first corner's w names its triangle).
+__global__ void k_refit_triangles(const float* __restrict__ positions, const uint32_t* __restrict__ triangles,
+    float4* __restrict__ pool, uint32_t tri_base, uint32_t count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  float4* rec = pool + kTriStride * (size_t)(tri_base + i);
+  const uint32_t p = __float_as_uint(rec[0].w);
+  for (int k = 0; k < 3; ++k) {
+    const uint32_t v = triangles[3 * (size_t)p + k];
+    rec[k] = make_float4(positions[3 * (size_t)v], positions[3 * (size_t)v + 1], positions[3 * (size_t)v + 2],
+        k == 0 ? __uint_as_float(p) : 0.0f);
+  }
+}
+
+// Each binary node's parent (the root, node_base, has none) and a cleared
+// arrival count.
+__global__ void k_refit_parents(const BvhNode* __restrict__ nodes, uint32_t node_base, uint32_t count,
+    uint32_t* __restrict__ parent, uint32_t* __restrict__ arrivals) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int4 c = nodes[node_base + i].c;
+  if (c.x >= 0 && c.x != kEmptyChild) parent[(uint32_t)c.x - node_base] = node_base + i;
+  if (c.y >= 0 && c.y != kEmptyChild) parent[(uint32_t)c.y - node_base] = node_base + i;
+  arrivals[i] = 0;
+}
+
+__device__ __forceinline__ void store_child_box(BvhNode* node, int slot, float4 lo, float4 hi) {
+  float* x = reinterpret_cast<float*>(&node->x);
+  float* y = reinterpret_cast<float*>(&node->y);
+  float* z = reinterpret_cast<float*>(&node->z);
+  x[2 * slot] = lo.x; x[2 * slot + 1] = hi.x;
+  y[2 * slot] = lo.y; y[2 * slot + 1] = hi.y;
+  z[2 * slot] = lo.z; z[2 * slot + 1] = hi.z;
+}
+
+// Bottom-up boxes: each node's thread boxes its leaf children's triangles
+// into the node; a node is complete once all its non-empty children have
+// arrived (its leaves, then each interior child as it completes), and the
+// last arrival writes its box into its parent's slot and carries on there.
+__global__ void k_refit_up(BvhNode* nodes, const float4* __restrict__ pool, uint32_t node_base, uint32_t count,
+    const uint32_t* __restrict__ parent, uint32_t* arrivals) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint32_t node = node_base + i;
+  int4 c = nodes[node].c;
+  const int32_t ref[2] = {c.x, c.y};
+  const int32_t cnt[2] = {c.z, c.w};
+  uint32_t leaves = 0;
+  for (int k = 0; k < 2; ++k) {
+    if (ref[k] >= 0) continue;  // interior or empty
+    const uint32_t first = ~(uint32_t)ref[k];
+    float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.0f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+    for (int t = 0; t < max(cnt[k], 1); ++t)
+      for (int v = 0; v < 3; ++v) {
+        const float4 p = pool[kTriStride * (size_t)(first + t) + v];
+        lo = make_float4(fminf(lo.x, p.x), fminf(lo.y, p.y), fminf(lo.z, p.z), 0.0f);
+        hi = make_float4(fmaxf(hi.x, p.x), fmaxf(hi.y, p.y), fmaxf(hi.z, p.z), 0.0f);
+      }
+    store_child_box(&nodes[node], k, lo, hi);
+    ++leaves;
+  }
+  if (leaves == 0) return;
+  uint32_t arrived = leaves;
+  // A tree over the scene's triangles is far shallower than 256 levels; the
+  // bound only guards against corrupt input.
+  for (int level = 0; level < 256; ++level) {
+    __threadfence();
+    const uint32_t before = atomicAdd(&arrivals[node - node_base], arrived);
+    c = __ldcg(&nodes[node].c);
+    const uint32_t needed = (c.x != kEmptyChild ? 1u : 0u) + (c.y != kEmptyChild ? 1u : 0u);
+    if (before + arrived < needed) return;
+    __threadfence();
+    if (node == node_base) return;
+    const float4 bx = __ldcg(&nodes[node].x), by = __ldcg(&nodes[node].y), bz = __ldcg(&nodes[node].z);
+    float4 lo, hi;
+    if (c.y == kEmptyChild) {
+      lo = make_float4(bx.x, by.x, bz.x, 0.0f);
+      hi = make_float4(bx.y, by.y, bz.y, 0.0f);
+    } else {
+      lo = make_float4(fminf(bx.x, bx.z), fminf(by.x, by.z), fminf(bz.x, bz.z), 0.0f);
+      hi = make_float4(fmaxf(bx.y, bx.w), fmaxf(by.y, by.w), fmaxf(bz.y, bz.w), 0.0f);
+    }
+    const uint32_t up = parent[node - node_base];
+    const int4 pc = __ldcg(&nodes[up].c);
+    store_child_box(&nodes[up], pc.x == (int32_t)node ? 0 : 1, lo, hi);
+    node = up;
+    arrived = 1;
+  }
+}
+
 inline uint32_t blocks(uint64_t n) { return (uint32_t)((n + kBuildBlock - 1) / kBuildBlock); }
 
 }  // namespace
+
+cudaError_t BvhBuilder::refit_triangles(const float* positions, const uint32_t* triangles, uint32_t n,
+    BvhNode* nodes, uint32_t node_base, float4* tri_pool, uint32_t tri_base, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  cudaError_t e = reserve(n, stream);
+  if (e != cudaSuccess) return e;
+  const uint32_t count = node_count(n);
+  k_refit_triangles<<<blocks(n), kBuildBlock, 0, stream>>>(positions, triangles, tri_pool, tri_base, n);
+  k_refit_parents<<<blocks(count), kBuildBlock, 0, stream>>>(nodes, node_base, count, parent_internal_, flags_);
+  k_refit_up<<<blocks(count), kBuildBlock, 0, stream>>>(nodes, tri_pool, node_base, count, parent_internal_,
+      flags_);
+  return cudaGetLastError();
+}
 
 cudaError_t BvhBuilder::reserve(uint32_t n, cudaStream_t stream) {
   if (n <= capacity_) return cudaSuccess;

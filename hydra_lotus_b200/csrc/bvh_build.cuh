@@ -38,6 +38,11 @@ class BvhBuilder {
   cudaError_t build_triangles(const float* positions, const uint32_t* triangles, uint32_t n,
       BvhNode* nodes, uint32_t node_base, float4* tri_pool, uint32_t tri_base,
       cudaStream_t stream);
+  // Refits one BLAS built over the same triangles (a point edit): its
+  // leaf-ordered triangle records take the new positions and its binary
+  // nodes' boxes are recomputed bottom-up; the topology is kept.
+  cudaError_t refit_triangles(const float* positions, const uint32_t* triangles, uint32_t n,
+      BvhNode* nodes, uint32_t node_base, float4* tri_pool, uint32_t tri_base, cudaStream_t stream);
   // The TLAS over the instances' world boxes; leaves hold instance indices.
   cudaError_t build_instances(const InstanceShading* shade, const InstanceTraversal* trav,
       const BvhNode* blas, uint32_t n, BvhNode* nodes, cudaStream_t stream);

@@ -647,6 +647,36 @@ __global__ void __launch_bounds__(kBlock) k_diagnostic(SceneView S, const FrameC
     color[slot] = F4(sh.shading_normal, 1.0f);
 }
 
+// The camera pass's depth (CameraPass, path_trace.slang:69-97): the pixel
+// centre's closest hit, traced with the fixed coverage sequence of sample 0
+// as the diagnostics are, as Vulkan window depth: the hit position through
+// the frame's world-to-clip, z over w. A miss leaves the pixel's depth as
+// it is (the clear depth, or the preceding frame's).
+__global__ void __launch_bounds__(kBlock) k_depth(SceneView S, const FrameConst* __restrict__ fcp,
+    float* __restrict__ depth) {
+  const FrameConst& f = *fcp;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= f.rect[2] * f.rect[3]) return;
+  const uint32_t px = f.rect[0] + i % f.rect[2], py = f.rect[1] + i / f.rect[2];
+  const uint32_t slot = py * f.width + px;
+  uint32_t rng = seed_random(slot, 0);
+  F3 o, d;
+  float tmax;
+  camera_ray(f, (float(px) + 0.5f) * f.ndc[0] + f.ndc[2], (float(py) + 0.5f) * f.ndc[1] + f.ndc[3], o, d, tmax);
+  Hit hit;
+  if (!trace_closest(S, o, d, 0.0f, tmax, rng, hit)) return;
+  const F3 p = o + d * hit.t;
+  const float* m = f.world_to_clip;
+  const float z = m[2] * p.x + m[6] * p.y + m[10] * p.z + m[14];
+  const float w = m[3] * p.x + m[7] * p.y + m[11] * p.z + m[15];
+  depth[slot] = z / w;
+}
+
+__global__ void k_fill_float(float* __restrict__ out, uint32_t n, float value) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = value;
+}
+
 // The ReSTIR passes' queued visibility rays (VisibilityQueue), as a
 // persistent any-hit kernel that completes each ray's pixel record.
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_visibility(SceneView S, VisibilityQueue VQ,
@@ -1193,6 +1223,13 @@ void launch_diagnostic(const SceneView& S, const FrameConst* fc, const uint32_t 
     float4* color, cudaStream_t stream) {
   const uint32_t n = rect[2] * rect[3];
   if (n) k_diagnostic<<<(n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(S, fc, output, color);
+}
+
+void launch_depth(const SceneView& S, const FrameConst* fc, const uint32_t rect[4], float* depth, uint32_t pixels,
+    bool clear, float clear_depth, cudaStream_t stream) {
+  if (clear && pixels) k_fill_float<<<(pixels + 255) / 256, 256, 0, stream>>>(depth, pixels, clear_depth);
+  const uint32_t n = rect[2] * rect[3];
+  if (n) k_depth<<<(n + kBlock - 1) / kBlock, kBlock, 0, stream>>>(S, fc, depth);
 }
 
 void launch_advance(FrameConst* fc, cudaStream_t stream) { k_advance<<<1, 32, 0, stream>>>(fc); }

@@ -194,5 +194,9 @@ void launch_diagnostic(const SceneView& S, const FrameConst* fc, const uint32_t 
 void launch_advance(FrameConst* fc, cudaStream_t stream);
 
 void launch_clear_color(float4* color, uint32_t pixels, float4 value, cudaStream_t stream);
+// The depth product of the pixel centres' closest hits in `rect`; with
+// `clear`, every pixel first takes `clear_depth`.
+void launch_depth(const SceneView& S, const FrameConst* fc, const uint32_t rect[4], float* depth, uint32_t pixels,
+    bool clear, float clear_depth, cudaStream_t stream);
 
 }  // namespace lotus

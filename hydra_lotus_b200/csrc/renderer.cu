@@ -639,6 +639,9 @@ struct Renderer {
   uint32_t width = 0, height = 0;
   DeviceArray<double4> accum;
   DeviceArray<float4> color;
+  DeviceArray<float> depth;   // the D32 depth product (LOTUS_FRAME_DEPTH)
+  bool depth_valid = false;   // the latest RenderScene frame wrote it
+  bool depth_fresh = true;    // allocated since its last clear: DEPTH_KEEP clears it too
   DeviceArray<float4> path_origin, path_direction, path_throughput, path_radiance;
   DeviceArray<uint4> path_hit;
   DeviceArray<uint32_t> queue_ray0, queue_ray1, queue_hit, counts;
@@ -879,10 +882,11 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
 //   - lotus_cuda_update_instances (transform / material-slot edits): the
 //     light table, the instance records and the TLAS;
 //   - lotus_cuda_update_geometry (point edits of one geometry, topology
-//     kept): that geometry's BLAS, rebuilt in place in its own node and
+//     kept): that geometry's BLAS refitted in place in its own node and
 //     triangle ranges, its corner normals, then the instance state.
-// The reference refits in both cases (gpu_scene.cpp:2303-2322); a rebuild
-// decides the same hits, since hits are decided by triangle tests alone.
+// The reference refits in both cases (gpu_scene.cpp:2303-2322); the TLAS is
+// rebuilt here, which decides the same hits, since hits are decided by
+// triangle tests alone.
 
 // Host-side instance state, prepared before any of it goes to the device.
 struct InstanceState {
@@ -1337,7 +1341,20 @@ int32_t update_geometry(Renderer& R, uint32_t geometry, const float* positions, 
                 36ull * geo.triangle_count, cudaMemcpyHostToDevice, st),
           "normals", detail))
     return fail(detail);
-  if (!build_blases(R, {geometry}, false, detail) || !submit_instances(R, inst, detail)) return fail(detail);
+  // The BLAS is refitted in place (the reference refits on point edits,
+  // gpu_scene.cpp:1899-1950): its topology kept, its triangle records and
+  // boxes following the new positions; then its 4-wide nodes again.
+  const uint32_t count = geo.triangle_count;
+  if (count &&
+      (!R.ok(R.builder.refit_triangles(R.scene_pos.ptr + 3 * h.vertex_base[geometry],
+                 R.scene_tri.ptr + 3 * (size_t)h.tri_base[geometry], count, R.blas.ptr, h.node_base[geometry],
+                 R.tris.ptr, h.tri_base[geometry], st),
+           "BLAS refit", detail) ||
+          !R.ok(BvhBuilder::collapse_range(R.blas.ptr, h.node_base[geometry], BvhBuilder::node_count(count),
+                    (uint32_t)h.nodes, R.blas4.ptr, false, st),
+              "BVH collapse", detail)))
+    return fail(detail);
+  if (!submit_instances(R, inst, detail)) return fail(detail);
   if (finish_update(R, res, detail) != LOTUS_PASS) return fail(detail);
   return LOTUS_PASS;
 }
@@ -1347,6 +1364,9 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
   if (R.width != w || R.height != h) {
     R.accum.release();
     R.color.release();
+    R.depth.release();
+    R.depth_valid = false;
+    R.depth_fresh = true;
     R.path_origin.release(); R.path_direction.release(); R.path_throughput.release();
     R.path_radiance.release(); R.path_hit.release();
     R.queue_ray0.release(); R.queue_ray1.release(); R.queue_hit.release();
@@ -1360,6 +1380,7 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
     R.key_valid = false;
   }
   if (!R.ok(R.accum.resize(n), "accumulation", detail) || !R.ok(R.color.resize(n), "colour", detail) ||
+      !R.ok(R.depth.resize(n), "depth", detail) ||
       !R.ok(R.counts.resize(kQueueCounterWords * (LOTUS_MAX_BOUNCES + 2)), "queue counts", detail) ||
       !R.ok(R.frame_const.resize(kMaxChain), "frame constants", detail) ||
       !R.ok(R.totals.resize(1), "ray totals", detail))
@@ -1494,6 +1515,10 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   }
   FrameConst fc{};
   if (!invert4(vulkan, fc.clip_to_world)) return fail("ray-query camera is singular or non-finite");
+  std::memcpy(fc.world_to_clip, vulkan, sizeof(vulkan));
+  const bool want_depth = (d.flags & LOTUS_FRAME_DEPTH) != 0;
+  if (want_depth && !(t.clear_depth >= 0.0f && t.clear_depth <= 1.0f))
+    return fail("invalid offscreen clear values");
   const bool wavefront = st.integrator == LOTUS_INTEGRATOR_WAVEFRONT;
   if (!ensure_targets(R, t.width, t.height, wavefront, detail)) return poison(detail);
   // The radiance cache serves the wavefront integrator's samples.
@@ -1544,6 +1569,11 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
         make_float4(t.clear_color[0], t.clear_color[1], t.clear_color[2], t.clear_color[3]), s);
     cudaEventRecord(R.ev_start, s);
     launch_diagnostic(R.view, R.frame_const.ptr, rect, st.output, R.color.ptr, s);
+    if (want_depth)
+      launch_depth(R.view, R.frame_const.ptr, rect, R.depth.ptr, t.width * t.height,
+          (d.flags & LOTUS_FRAME_DEPTH_KEEP) == 0 || R.depth_fresh, t.clear_depth, s);
+    R.depth_valid = want_depth;
+  if (want_depth) R.depth_fresh = false;
     cudaEventRecord(R.ev_stop, s);
     uint32_t walks[2] = {0, 0};
     cudaMemcpyAsync(walks, R.walk_failure.ptr, sizeof(walks), cudaMemcpyDeviceToHost, s);
@@ -1601,6 +1631,13 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   if (rect[2] < t.width || rect[3] < t.height || rect[2] == 0)
     launch_clear_color(R.color.ptr, t.width * t.height,
         make_float4(t.clear_color[0], t.clear_color[1], t.clear_color[2], t.clear_color[3]), s);
+  // The camera pass's depth, once per call (the frame constants' camera and
+  // window, sample 0's coverage sequence).
+  if (want_depth)
+    launch_depth(R.view, R.frame_const.ptr, rect, R.depth.ptr, t.width * t.height,
+        (d.flags & LOTUS_FRAME_DEPTH_KEEP) == 0 || R.depth_fresh, t.clear_depth, s);
+  R.depth_valid = want_depth;
+  if (want_depth) R.depth_fresh = false;
   PathState P{R.path_origin.ptr, R.path_direction.ptr, R.path_throughput.ptr, R.path_radiance.ptr, R.path_hit.ptr};
   Queues Q;
   Q.ray[0] = R.queue_ray0.ptr;
@@ -2018,6 +2055,18 @@ int32_t lotus_cuda_read_color(lotus_cuda_renderer* r, float* color, uint64_t cap
   return LOTUS_PASS;
 }
 
+int32_t lotus_cuda_read_depth(lotus_cuda_renderer* r, float* depth, uint64_t capacity_floats) {
+  if (!r || !depth) return LOTUS_FAIL;
+  Renderer& R = r->r;
+  const uint64_t n = (uint64_t)R.width * R.height;
+  if (n == 0 || capacity_floats < n || !R.depth.ptr || !R.depth_valid) return LOTUS_FAIL;
+  cudaSetDevice(R.device);
+  if (cudaMemcpyAsync(depth, R.depth.ptr, n * 4, cudaMemcpyDeviceToHost, R.stream) != cudaSuccess ||
+      cudaStreamSynchronize(R.stream) != cudaSuccess)
+    return LOTUS_FAIL;
+  return LOTUS_PASS;
+}
+
 void* lotus_cuda_stream(lotus_cuda_renderer* r) { return r ? (void*)r->r.stream : nullptr; }
 
 int64_t lotus_cuda_read_light_table(lotus_cuda_renderer* r, uint32_t* records, uint64_t record_capacity,
@@ -2100,6 +2149,7 @@ bool make_frame_constants(const lotus_frame_desc& d, FrameConst& fc, uint32_t re
     vulkan[c * 4 + 2] = 0.5f * (z + w);
   }
   fc = FrameConst{};
+  std::memcpy(fc.world_to_clip, vulkan, sizeof(vulkan));
   if (!invert4(vulkan, fc.clip_to_world)) {
     detail = "ray-query camera is singular or non-finite";
     return false;

@@ -508,6 +508,7 @@ constexpr uint32_t kNoPrimaryHit = 0xFFFFFFFFu;
 // and accumulated advance on the device between samples.
 struct FrameConst {
   float clip_to_world[16];
+  float world_to_clip[16];  // Vulkan clip (the depth product's projection)
   float ndc[4];
   float background[4];
   uint32_t width, height;

@@ -357,6 +357,7 @@ bool CudaOffscreenRenderer::FillFrame(const Lotus::Matrix4& world_to_clip, const
   std::memcpy(f.target.data_window, t.data_window.data(), 16);
   std::memcpy(f.target.clear_color, t.clear_color.data(), 16);
   f.target.read_back = t.read_back ? 1u : 0u;
+  f.target.clear_depth = t.clear_depth;
   f.settings.integrator =
       s.integrator == Lotus::Integrator::Wavefront ? LOTUS_INTEGRATOR_WAVEFRONT : LOTUS_INTEGRATOR_REFERENCE;
   f.settings.light_sampling = s.light_sampling == Lotus::LightSampling::Bsdf ? LOTUS_LIGHT_SAMPLING_BSDF
@@ -373,7 +374,9 @@ bool CudaOffscreenRenderer::FillFrame(const Lotus::Matrix4& world_to_clip, const
   f.settings.restir_proposal = (uint32_t)s.restir_proposal;
   f.settings.environment_background = s.environment_background ? 1u : 0u;
   f.frame_count = frame_count;
-  f.flags = LOTUS_FRAME_TIMINGS;
+  // Every scene frame writes the camera pass's D32 depth, as the
+  // reference's does (vulkan_backend.hpp:769-773).
+  f.flags = LOTUS_FRAME_TIMINGS | LOTUS_FRAME_DEPTH | (t.clear_depth_enabled ? 0u : LOTUS_FRAME_DEPTH_KEEP);
   return true;
 }
 
@@ -405,6 +408,20 @@ void CudaOffscreenRenderer::FillEvidence(const lotus_frame_desc& f, const lotus_
     c.color_space = "linear";
     c.payload.resize(color.size() * sizeof(float));
     std::memcpy(c.payload.data(), color.data(), c.payload.size());
+    // D32 window depth, top-left rows (vulkan_backend.hpp:40-47, 1318-1324).
+    if (f.flags & LOTUS_FRAME_DEPTH) {
+      Lotus::DepthProduct& d = e.depth;
+      d.payload.resize((size_t)f.target.width * f.target.height);
+      if (lotus_cuda_read_depth(handle_, d.payload.data(), d.payload.size()) == LOTUS_PASS) {
+        d.width = f.target.width;
+        d.height = f.target.height;
+        d.row_pitch = f.target.width * sizeof(float);
+        d.pixel_format = "d32-sfloat";
+        d.origin = "top-left";
+      } else {
+        d.payload.clear();
+      }
+    }
   }
 }
 

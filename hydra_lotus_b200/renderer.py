@@ -55,6 +55,8 @@ def lib():
                                         C.POINTER(abi.FrameResult), C.c_void_p]
         L.lotus_cuda_read_color.restype = C.c_int32
         L.lotus_cuda_read_color.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
+        L.lotus_cuda_read_depth.restype = C.c_int32
+        L.lotus_cuda_read_depth.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
         L.lotus_cuda_stream.restype = C.c_void_p
         L.lotus_cuda_stream.argtypes = [C.c_void_p]
         L.lotus_cuda_render_static.restype = C.c_int32
@@ -239,6 +241,15 @@ class CudaOffscreenRenderer:
         n = lib().lotus_cuda_read_product(self.handle, product, out.ctypes.data, out.nbytes)
         if n < 0:
             raise RendererError(abi.FAIL, f"product {product} is not available")
+        return out
+
+    def read_depth(self, height, width):
+        """The latest frame's depth product (LOTUS_FRAME_DEPTH): (H, W)
+        float32 Vulkan window depth, top-left rows."""
+        out = np.empty((height, width), dtype=np.float32)
+        rc = lib().lotus_cuda_read_depth(self.handle, out.ctypes.data, out.size)
+        if rc != abi.PASS:
+            raise RendererError(rc, "read_depth failed: no depth product")
         return out
 
     def read_color(self, out):

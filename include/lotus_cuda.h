@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LOTUS_CUDA_ABI_VERSION 5u
+#define LOTUS_CUDA_ABI_VERSION 6u
 
 /* FrameStatus (vulkan_backend.hpp:23-27). */
 #define LOTUS_PASS 0
@@ -169,7 +169,7 @@ typedef struct lotus_target {
   int32_t data_window[4];    /* {x, y, w, h}; w or h <= 0 means the whole image */
   float clear_color[4];
   uint32_t read_back;        /* 0 keeps the frame on the device */
-  uint32_t reserved;
+  float clear_depth;         /* Vulkan window depth in [0, 1] of the depth product's clears (OffscreenTarget's 1) */
 } lotus_target;
 
 /* PathTracingSettings (vulkan_backend.hpp:697-738). */
@@ -215,6 +215,15 @@ typedef struct lotus_settings {
  * instances visited per ray kind (slower; for roofline accounting). */
 #define LOTUS_FRAME_TIMINGS 1u
 #define LOTUS_FRAME_COUNT_VISITS 2u
+/* DEPTH writes the D32 depth product (vulkan_backend.hpp:230, 769-773; the
+ * camera pass, path_trace.slang:69-97): the pixel centre's closest hit,
+ * traced with the fixed coverage sequence of sample 0, as Vulkan window
+ * depth (clip z / clip w through the frame's camera); pixels without a hit
+ * and outside the data window keep target.clear_depth, or with DEPTH_KEEP
+ * (OffscreenTarget::clear_depth_enabled false) the preceding frame's depth.
+ * lotus_cuda_read_depth copies it. */
+#define LOTUS_FRAME_DEPTH 4u
+#define LOTUS_FRAME_DEPTH_KEEP 8u
 
 /* One RenderScene call: DrawSummary::world_to_clip in the OpenGL clip
  * convention (extraction.hpp:23), the target and the settings. */
@@ -342,9 +351,11 @@ int32_t lotus_cuda_update_instances(lotus_cuda_renderer* renderer,
  * and vertex count kept; the reference refits, gpu_scene.cpp:2303-2322):
  * the resident geometry `geometry` takes new positions (and new corner
  * normals, which a geometry with corner normals must be given and one
- * without must not). Rebuilds that geometry's BLAS in place, then the
- * light table, instance records and TLAS. Restarts the accumulation. The
- * images equal those of lotus_cuda_update_scene with the edited scene. */
+ * without must not). Refits that geometry's BLAS in place (its topology
+ * kept, its boxes recomputed bottom-up from the new positions), then
+ * rebuilds the light table, instance records and TLAS. Restarts the
+ * accumulation. The images equal those of lotus_cuda_update_scene with the
+ * edited scene (hits are decided by triangle tests alone). */
 int32_t lotus_cuda_update_geometry(lotus_cuda_renderer* renderer, uint32_t geometry,
     const float* positions, uint32_t vertex_count, const float* normals, lotus_scene_result* result);
 
@@ -434,6 +445,11 @@ int64_t lotus_cuda_read_product(lotus_cuda_renderer* renderer, uint32_t product,
 /* The colour of the latest frame into host memory (width*height*4 floats). */
 int32_t lotus_cuda_read_color(lotus_cuda_renderer* renderer, float* color,
     uint64_t capacity_floats);
+
+/* The depth product of the latest RenderScene frame that asked for it
+ * (LOTUS_FRAME_DEPTH) into host memory: width*height floats, top-left rows.
+ * Fail when the latest frame wrote none. */
+int32_t lotus_cuda_read_depth(lotus_cuda_renderer* renderer, float* depth, uint64_t capacity_floats);
 
 /* The renderer's CUDA stream (a cudaStream_t), for callers that time its
  * work with their own events. */

@@ -113,3 +113,69 @@ def test_diagnostics_outside_render_scene_fail(cuda):
         st.output = 7
         assert r.render_scene(scene.frame(st, frame_count=1))[0].status == abi.FAIL
         cuda.check(r.render_scene(scene.frame(abi.default_settings(), frame_count=1))[0], "render after rejects")
+
+
+def depth_plane_scene(size=48, half=10.0):
+    """One quad at z = -2 facing the camera at z = +3 (the Cornell camera's
+    view): every pixel centre hits it at view depth 5 when it spans the
+    view (`half` large), a central square of pixels when it is small."""
+    s = scenes.Scene("depth-plane")
+    q = s.add_geometry(*scenes.quad([[-half, -half, -2.0], [half, -half, -2.0], [half, half, -2.0],
+                                     [-half, half, -2.0]]))
+    s.add_instance(q, s.add_material(scenes.preview_material((0.5, 0.5, 0.5))))
+    s.world_to_clip = scenes.cornell_camera()
+    s.width = s.height = size
+    return s
+
+
+def plane_depth(world_to_clip):
+    """The Vulkan window depth of a point at view depth 5 on the axis: the
+    OpenGL clip z and w of the Cornell projection, z mapped to (z + w) / 2."""
+    m = np.asarray(world_to_clip, dtype=np.float64)
+    p = np.array([0.0, 0.0, -2.0, 1.0])
+    clip = np.array([sum(m[c * 4 + r] * p[c] for c in range(4)) for r in range(4)])
+    return 0.5 * (clip[2] + clip[3]) / clip[3]
+
+
+def test_depth_product_of_a_plane(cuda):
+    scene = depth_plane_scene()
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, max_bounces=2)
+    want = plane_depth(scene.world_to_clip)
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        res, _ = r.render_scene(scene.frame(st, 2, flags=abi.FRAME_DEPTH))
+        cuda.check(res, "render_scene")
+        depth = r.read_depth(scene.height, scene.width)
+    print(want, depth.min(), depth.max())
+    assert 0.0 < want < 1.0
+    np.testing.assert_allclose(depth, want, rtol=1e-5)
+
+
+def test_depth_product_clears_and_keeps(cuda):
+    """Pixels whose centre misses keep the clear depth; with DEPTH_KEEP they
+    keep the preceding frame's; a frame without DEPTH has no depth product;
+    the hit pixels are the diagnostic pass's."""
+    scene = depth_plane_scene(half=0.5)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, max_bounces=2)
+    want = plane_depth(scene.world_to_clip)
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        cuda.check(r.render_scene(scene.frame(st, 1, flags=abi.FRAME_DEPTH, clear_depth=0.75))[0], "first")
+        first = r.read_depth(scene.height, scene.width)
+        hit = first != np.float32(0.75)
+        assert 0 < hit.sum() < hit.size
+        np.testing.assert_allclose(first[hit], want, rtol=1e-5)
+        cuda.check(r.render_scene(scene.frame(st, 1, flags=abi.FRAME_DEPTH | abi.FRAME_DEPTH_KEEP,
+                                              clear_depth=0.25))[0], "keep")
+        kept = r.read_depth(scene.height, scene.width)
+        assert np.array_equal(kept, first)
+        cuda.check(r.render_scene(scene.frame(st, 1, flags=abi.FRAME_DEPTH, clear_depth=0.25))[0], "clear")
+        cleared = r.read_depth(scene.height, scene.width)
+        assert np.array_equal(cleared[~hit], np.full((~hit).sum(), 0.25, np.float32))
+        dst = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, output=abi.OUTPUT_BARYCENTRICS)
+        res, bary = r.render_scene(scene.frame(dst, 1, clear_color=CLEAR))
+        cuda.check(res, "barycentrics")
+        assert np.array_equal(bary[..., 3] == 1.0, hit)
+        cuda.check(r.render_scene(scene.frame(st, 1))[0], "no depth")
+        with pytest.raises(cuda.RendererError):
+            r.read_depth(scene.height, scene.width)
