@@ -681,11 +681,13 @@ def main():
             "e2e": {"value": round(total_e2e_rays / (max_e2e_ms * 1e-3) / 1e6, 2),
                     "unit": "Mrays/s", "h2d_bytes_per_step": 160,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 16 + 64},
-            # Per step: SPP samples, chained 16 at a time two in flight, each
-            # chain computing its samples' frame constants (one launch each
-            # after the first).
-            "gpu_launches": (launches_per_sample(DEPTH, timed.wavefront_rounds) * SPP +
-                             sum(min(16, SPP - c) - 1 for c in range(0, SPP - SPP % 2, 16))) * args.steps,
+            # Per step: SPP samples in waves of two (each wave's launches as
+            # one sample's, its frame constants in place of the advance),
+            # chained 16 samples at a time, each chain advancing the frame
+            # constants once.
+            "gpu_launches": (launches_per_sample(DEPTH, timed.wavefront_rounds) * (SPP // 2) +
+                             launches_per_sample(DEPTH, timed.wavefront_rounds) * (SPP % 2) +
+                             (SPP + 15) // 16) * args.steps,
             "roofline": {
                 "kernel": "k_wf_extend",
                 "bound": "hbm",

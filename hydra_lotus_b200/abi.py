@@ -37,7 +37,7 @@ MOMENTS_FP16 = 1
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
-ABI_VERSION = 6
+ABI_VERSION = 7
 
 # lotus_settings::output (SceneOutput).
 OUTPUT_RADIANCE = 0
@@ -212,6 +212,8 @@ class FrameResult(C.Structure):
         ("cache_queries", C.c_uint32),
         ("cache_training_records", C.c_uint32),
         ("tail_gpu_ms", C.c_double),
+        ("last_wave_samples", C.c_uint32),
+        ("reserved", C.c_uint32),
         ("detail", C.c_char * 256),
     ]
 

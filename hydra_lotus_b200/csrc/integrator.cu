@@ -37,7 +37,7 @@ __device__ __forceinline__ bool tile_pixel(uint32_t index, const uint32_t* rect,
   return x < rect[2] && y < rect[3];
 }
 
-__host__ __forceinline__ uint32_t tile_threads(const uint32_t* rect) {
+__host__ __device__ __forceinline__ uint32_t tile_threads(const uint32_t* rect) {
   return ((rect[2] + 7) / 8) * ((rect[3] + 3) / 4) * 32;
 }
 
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, VisitCounters* visits, SceneTable B) {
   TraversalCounters vc = {0, 0, 0};
   const uint32_t index = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t px = 0, py = 0, slot = 0, scene = 0;
+  uint32_t px = 0, py = 0, slot = 0, scene = 0, wave_sample = 0;
   bool valid;
   if (kBatch) {
     slot = index;
@@ -384,9 +384,12 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
     }
   } else {
     if (!fcp->add_sample) return;
+    // The wave's samples one after another, each over the rect's tiles.
     const uint32_t rect[4] = {fcp->rect[0], fcp->rect[1], fcp->rect[2], fcp->rect[3]};
-    valid = tile_pixel(index, rect, px, py);
-    slot = py * fcp->width + px;
+    const uint32_t per_sample = tile_threads(rect);
+    wave_sample = index / per_sample;
+    valid = wave_sample < max(fcp->wave, 1u) && tile_pixel(index - wave_sample * per_sample, rect, px, py);
+    slot = wave_sample * fcp->wave_stride + py * fcp->width + px;
   }
   const FrameConst& f = kBatch ? B.frames[scene] : *fcp;
   const SceneView& SS = kBatch ? B.views[scene] : S;
@@ -395,9 +398,9 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
     F3 o, d;
     float tmax;
     uint32_t rng;
-    start_path(f, px, py, f.sample_index, o, d, tmax, rng);
+    start_path(f, px, py, f.sample_index + wave_sample, o, d, tmax, rng);
     Hit hit;
-    if (!kBatch && f.primary_hit != nullptr && f.sample_index == f.primary_sample) {
+    if (!kBatch && f.primary_hit != nullptr && wave_sample == 0 && f.sample_index == f.primary_sample) {
       // The same camera ray's hit, traced by a pass earlier in the frame.
       const uint4 ph = f.primary_hit[slot];
       found = ph.x != kNoPrimaryHit;
@@ -821,7 +824,9 @@ __global__ void __launch_bounds__(kBlock) k_wf_resolve(SceneView S,
   const FrameConst& f = kBatch ? B.frames[scene] : *fcp;
   double4 sum = f.accumulated != 0 ? accum[slot] : make_double4(0.0, 0.0, 0.0, 0.0);
   if (f.add_sample) {
-    sum = add4(sum, P.radiance[slot]);
+    // The wave's samples in order, as one at a time would add them.
+    const uint32_t wave = kBatch ? 1u : max(f.wave, 1u);
+    for (uint32_t k = 0; k < wave; ++k) sum = add4(sum, P.radiance[k * f.wave_stride + slot]);
     accum[slot] = sum;
   }
   color[slot] = resolve_pixel(kBatch ? B.views[scene] : S, f, px, py, sum);
@@ -895,15 +900,37 @@ __global__ void k_wf_finish(FrameConst* fc, const uint32_t* __restrict__ counts,
     if (b != 0) ext += counts[3 * b];
     sh += counts[3 * b + 2];
   }
-  totals->camera += (unsigned long long)fc->rect[2] * fc->rect[3];
+  totals->camera += (unsigned long long)fc->rect[2] * fc->rect[3] * max(fc->wave, 1u);
   totals->extension += ext;
   totals->shadow += sh;
 }
 
 __global__ void k_advance(FrameConst* fc) {
   if (threadIdx.x == 0 && blockIdx.x == 0 && fc->add_sample) {
-    fc->sample_index += 1;
-    fc->accumulated += 1;
+    fc->sample_index += max(fc->wave, 1u);
+    fc->accumulated += max(fc->wave, 1u);
+  }
+}
+
+// A wave's frame constants: `frame`'s advanced by `offset` samples, covering
+// `wave` samples whose slots lie `stride` apart.
+__global__ void k_wave_frame(const FrameConst* __restrict__ frame, FrameConst* __restrict__ out, uint32_t offset,
+    uint32_t wave, uint32_t stride) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  FrameConst f = *frame;
+  if (f.add_sample) {
+    f.sample_index += offset;
+    f.accumulated += offset;
+  }
+  f.wave = wave;
+  f.wave_stride = stride;
+  *out = f;
+}
+
+__global__ void k_advance_by(FrameConst* fc, uint32_t samples) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && fc->add_sample) {
+    fc->sample_index += samples;
+    fc->accumulated += samples;
   }
 }
 
@@ -1029,7 +1056,8 @@ uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requ
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
-    SampleProfile* profile, const TraceTuning& tuning, const CacheQueues* cache, cudaEvent_t before_resolve) {
+    SampleProfile* profile, const TraceTuning& tuning, const CacheQueues* cache, cudaEvent_t before_resolve,
+    uint32_t wave) {
   CacheQueues C{};
   if (cache && cache->enabled && cache->cache) C = *cache;
   else C.enabled = false;
@@ -1056,9 +1084,11 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
       8u * persistent_grid((const void*)k_wf_shade<false, false, false>, Q.capacity, TraceTuning()));
   {
+    // One camera thread per pixel of each of the wave's samples.
     Timed t(profile, stream, 0);
-    if (count) k_wf_camera<true, false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, visits, none);
-    else k_wf_camera<false, false><<<grid_pixels, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
+    const uint32_t grid_camera = (threads * std::max(wave, 1u) + kBlock - 1) / kBlock;
+    if (count) k_wf_camera<true, false><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, visits, none);
+    else k_wf_camera<false, false><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
   }
   // Bounces 0 .. rounds - 1 as wavefront rounds; the paths queued for bounce
   // `rounds` (if any can be) go to the tail kernel. Counting visits keeps
@@ -1137,14 +1167,23 @@ __global__ void k_next_frame(const FrameConst* __restrict__ fc, FrameConst* __re
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   FrameConst f = *fc;
   if (f.add_sample) {
-    f.sample_index += 1;
-    f.accumulated += 1;
+    f.sample_index += max(f.wave, 1u);
+    f.accumulated += max(f.wave, 1u);
   }
   *next = f;
 }
 
 void launch_next_frame(const FrameConst* fc, FrameConst* next, cudaStream_t stream) {
   k_next_frame<<<1, 32, 0, stream>>>(fc, next);
+}
+
+void launch_wave_frame(const FrameConst* frame, FrameConst* out, uint32_t offset, uint32_t wave, uint32_t stride,
+    cudaStream_t stream) {
+  k_wave_frame<<<1, 32, 0, stream>>>(frame, out, offset, wave, stride);
+}
+
+void launch_advance_by(FrameConst* fc, uint32_t samples, cudaStream_t stream) {
+  k_advance_by<<<1, 32, 0, stream>>>(fc, samples);
 }
 
 __global__ void k_next_frames(const FrameConst* __restrict__ frames, FrameConst* __restrict__ next, uint32_t count) {

@@ -137,7 +137,13 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
     SampleProfile* profile = nullptr, const TraceTuning& tuning = TraceTuning(),
-    const CacheQueues* cache = nullptr, cudaEvent_t before_resolve = nullptr);
+    const CacheQueues* cache = nullptr, cudaEvent_t before_resolve = nullptr, uint32_t wave = 1);
+// Frame constants for a wave: `frame`'s advanced by `offset` samples,
+// covering `wave` samples whose path slots lie `stride` apart.
+void launch_wave_frame(const FrameConst* frame, FrameConst* out, uint32_t offset, uint32_t wave, uint32_t stride,
+    cudaStream_t stream);
+// Advances the frame constants by `samples` samples.
+void launch_advance_by(FrameConst* fc, uint32_t samples, cudaStream_t stream);
 
 // The frame constants of the sample after fc's: a copy of *fc advanced by
 // one sample (for two samples in flight at once, each with its own).

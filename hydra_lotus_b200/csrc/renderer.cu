@@ -1386,15 +1386,17 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
       !R.ok(R.totals.resize(1), "ray totals", detail))
     return false;
   if (wavefront) {
-    if (!R.ok(R.path_origin.resize(n), "path state", detail) ||
-        !R.ok(R.path_direction.resize(n), "path state", detail) ||
-        !R.ok(R.path_throughput.resize(n), "path state", detail) ||
-        !R.ok(R.path_radiance.resize(n), "path state", detail) ||
-        !R.ok(R.path_hit.resize(n), "path state", detail) ||
-        !R.ok(R.queue_ray0.resize(n), "queues", detail) || !R.ok(R.queue_ray1.resize(n), "queues", detail) ||
-        !R.ok(R.queue_hit.resize(n), "queues", detail) || !R.ok(R.sq_o.resize(n), "shadow queue", detail) ||
-        !R.ok(R.sq_d.resize(n), "shadow queue", detail) || !R.ok(R.sq_fl.resize(n), "shadow queue", detail) ||
-        !R.ok(R.sq_thr.resize(n), "shadow queue", detail))
+    // Room for a wave of two samples.
+    const size_t w = 2 * n;
+    if (!R.ok(R.path_origin.resize(w), "path state", detail) ||
+        !R.ok(R.path_direction.resize(w), "path state", detail) ||
+        !R.ok(R.path_throughput.resize(w), "path state", detail) ||
+        !R.ok(R.path_radiance.resize(w), "path state", detail) ||
+        !R.ok(R.path_hit.resize(w), "path state", detail) ||
+        !R.ok(R.queue_ray0.resize(w), "queues", detail) || !R.ok(R.queue_ray1.resize(w), "queues", detail) ||
+        !R.ok(R.queue_hit.resize(w), "queues", detail) || !R.ok(R.sq_o.resize(w), "shadow queue", detail) ||
+        !R.ok(R.sq_d.resize(w), "shadow queue", detail) || !R.ok(R.sq_fl.resize(w), "shadow queue", detail) ||
+        !R.ok(R.sq_thr.resize(w), "shadow queue", detail))
       return false;
   }
   return true;
@@ -1684,18 +1686,25 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   // The rounds the call's last sample ran (the frame result reports them).
   uint32_t last_rounds = wavefront_rounds(st.max_bounces, want_visits, tuning.rounds, use_cache ? cq.bounce : 0u);
   const bool choose_rounds = wavefront && R.tuning.rounds == 0 && !(R.rounds_key == gk);
-  // Two samples at a time where two or more are added without the radiance
-  // cache (which trains between samples) and outside the profiled last one:
-  // the second runs on its own path state and stream, beside the first,
-  // and resolves after it.
-  const uint32_t chainable = (wavefront && !use_cache && to_add >= 2)
-      ? submissions - ((want_timings || want_visits) ? 1u : 0u) : 0u;
+  // Samples in waves: where two or more are added without the radiance
+  // cache (which trains between samples), the wavefront runs two samples as
+  // one wave, their paths in slots k * pixels + pixel of a path state twice
+  // the target's size, so that every launch holds both samples' paths and
+  // pays its ramp-up and drain once for them. Chains of up to kMaxChain / 2
+  // waves run two in flight: wave j on path state j % 2 and stream j % 2,
+  // each resolving (its samples in order) after wave j - 1, so that only
+  // the chain's last tail runs alone. A call's profiled part (timings or
+  // visit counts) is its last wave (or sample), run alone.
+  const uint32_t pixels = t.width * t.height;
+  const bool waves = wavefront && !use_cache && to_add >= 2;
+  const uint32_t profiled_samples = (want_timings || want_visits) ? (waves ? 2u : 1u) : 0u;
+  const uint32_t chainable = waves ? submissions - profiled_samples : 0u;
   while (R.ev_sample_done.size() < kMaxChain) {
     cudaEvent_t e;
     if (!R.ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event", detail)) return poison(detail);
     R.ev_sample_done.push_back(e);
   }
-  if (chainable >= 2 && !ensure_pair_buffers(R, (size_t)t.width * t.height, detail)) return poison(detail);
+  if (chainable >= 4 && !ensure_pair_buffers(R, 2 * (size_t)pixels, detail)) return poison(detail);
   PathState P2{R.path_origin2.ptr, R.path_direction2.ptr, R.path_throughput2.ptr, R.path_radiance2.ptr,
       R.path_hit2.ptr};
   Queues Q2 = Q;
@@ -1704,17 +1713,20 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   Q2.hit = R.queue_hit2.ptr;
   Q2.shadow = ShadowQueue{R.sq_o2.ptr, R.sq_d2.ptr, R.sq_fl2.ptr, R.sq_thr2.ptr};
   Q2.counts = R.counts2.ptr;
-  bool last_in_chain = false;
+  // A wave's queues hold both samples' paths.
+  Queues QW = Q, QW2 = Q2;
+  QW.capacity = QW2.capacity = 2 * pixels;
+  const uint32_t* last_counts = R.counts.ptr;  // the call's last launch's queue counts
+  uint32_t last_wave = 1;                      // and the samples it held
+  FrameConst* fc0 = R.frame_const.ptr;
   cudaEventRecord(R.ev_start, s);
-  for (uint32_t k = 0; k < submissions; ++k) {
-    const bool profiled = (want_timings || want_visits) && k + 1 == submissions;
-    if (!profiled && k + 2 <= chainable) {
-      // A chain of `length` samples (even, at most kMaxChain): sample j on
-      // path state j % 2 and stream j % 2 with frame constants fc0 advanced
-      // by j; each resolves after sample j - 1, so only the chain's last
-      // tail is not overlapped by another sample's rounds.
+  for (uint32_t k = 0; k < submissions;) {
+    if (k + 2 <= chainable) {
+      // A chain of `length` samples (even, at most kMaxChain) in length / 2
+      // waves; wave j's frame constants are fc0's advanced by 2j.
       const uint32_t length = std::min(kMaxChain, (chainable - k) & ~1u);
-      gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, false);
+      const uint32_t count = length / 2;
+      gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, 0u);
       if (!(R.graph_chain_key == gk)) {
         for (cudaGraphExec_t& old : R.graph_chains)
           if (old) {
@@ -1723,37 +1735,51 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
           }
         R.graph_chain_key = gk;
       }
-      cudaGraphExec_t& chain = R.graph_chains[length / 2];
+      cudaGraphExec_t& chain = R.graph_chains[count];
       if (!chain) {
         cudaGraph_t g;
-        FrameConst* fc = R.frame_const.ptr;
         if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
           return poison(detail);
-        for (uint32_t j = 1; j < length; ++j) launch_next_frame(fc + j - 1, fc + j, s);
+        for (uint32_t j = 0; j < count; ++j) launch_wave_frame(fc0, fc0 + 1 + j, 2 * j, 2, pixels, s);
         cudaEventRecord(R.ev_fork, s);
         cudaStreamWaitEvent(R.stream2, R.ev_fork, 0);
-        for (uint32_t j = 0; j < length; ++j) {
+        for (uint32_t j = 0; j < count; ++j) {
           const bool second = (j & 1u) != 0;
-          launch_wavefront_sample(R.view, fc + j, rect, t.width, t.height, st.max_bounces, second ? P2 : P,
-              second ? Q2 : Q, R.accum.ptr, R.color.ptr, R.totals.ptr, second ? R.stream2 : s, nullptr, tuning,
-              nullptr, j ? R.ev_sample_done[j - 1] : nullptr);
+          launch_wavefront_sample(R.view, fc0 + 1 + j, rect, t.width, t.height, st.max_bounces, second ? P2 : P,
+              second ? QW2 : QW, R.accum.ptr, R.color.ptr, R.totals.ptr, second ? R.stream2 : s, nullptr, tuning,
+              nullptr, j ? R.ev_sample_done[j - 1] : nullptr, 2);
           cudaEventRecord(R.ev_sample_done[j], second ? R.stream2 : s);
         }
         cudaEventRecord(R.ev_join, R.stream2);
         cudaStreamWaitEvent(s, R.ev_join, 0);
-        for (uint32_t j = 0; j < length; ++j) launch_advance(fc, s);
+        launch_advance_by(fc0, length, s);
         if (!R.ok(cudaStreamEndCapture(s, &g), "graph capture", detail)) return poison(detail);
         cudaError_t e = cudaGraphInstantiate(&chain, g, 0);
         cudaGraphDestroy(g);
         if (!R.ok(e, "graph instantiate", detail)) return poison(detail);
       }
       if (!R.ok(cudaGraphLaunch(chain, s), "graph launch", detail)) return poison(detail);
-      k += length - 1;
-      last_in_chain = true;
+      k += length;
+      last_counts = ((count - 1) & 1u) ? R.counts2.ptr : R.counts.ptr;
+      last_wave = 2;
+      last_rounds = gk.rounds;
       continue;
     }
-    last_in_chain = false;
+    const bool profiled = profiled_samples != 0 && k + profiled_samples == submissions;
     last_rounds = wavefront_rounds(st.max_bounces, profiled && want_visits, tuning.rounds, use_cache ? cq.bounce : 0u);
+    last_counts = R.counts.ptr;
+    if (profiled && profiled_samples == 2) {
+      // The profiled last wave: two samples in one wavefront, run alone.
+      launch_wave_frame(fc0, fc0 + 1, 0, 2, pixels, s);
+      launch_wavefront_sample(R.view, fc0 + 1, rect, t.width, t.height, st.max_bounces, P, QW, R.accum.ptr,
+          R.color.ptr, R.totals.ptr, s, &profile, tuning, &cq, nullptr, 2);
+      launch_advance_by(fc0, 2, s);
+      k += 2;
+      last_wave = 2;
+      continue;
+    }
+    last_wave = 1;
+    ++k;
     if (profiled) {
       if (wavefront)
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
@@ -1794,7 +1820,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   cudaMemcpyAsync(&totals, R.totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(walks, R.walk_failure.ptr, sizeof(walks), cudaMemcpyDeviceToHost, s);
   if (wavefront)
-    cudaMemcpyAsync(counts.data(), last_in_chain ? R.counts2.ptr : R.counts.ptr, counts.size() * 4,
+    cudaMemcpyAsync(counts.data(), last_counts, counts.size() * 4,
         cudaMemcpyDeviceToHost, s);
   if (!R.ok(cudaStreamSynchronize(s), "render", detail)) return poison(detail);
   if (walks[0]) return poison(walk_failure_detail(walks, R.step_limit));
@@ -1860,16 +1886,17 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   if (wavefront && to_add > 0) {
     uint32_t last = 0;
     for (uint32_t b = 0; b <= st.max_bounces && b < LOTUS_MAX_REPORTED_BOUNCES; ++b) {
-      const uint32_t c = b == 0 ? rect[2] * rect[3] : counts[3 * b];
+      const uint32_t c = b == 0 ? rect[2] * rect[3] * last_wave : counts[3 * b];
       res.wavefront_path_counts[b] = c;
       if (c) last = b + 1;
     }
     res.wavefront_path_count_size = last;
     res.wavefront_rounds = last_rounds;
+    res.last_wave_samples = last_wave;
     if (choose_rounds) {
       gk.rounds = 0;
       R.rounds_key = gk;
-      R.auto_rounds = choose_wavefront_rounds(counts.data(), rect[2] * rect[3], st.max_bounces);
+      R.auto_rounds = choose_wavefront_rounds(counts.data(), rect[2] * rect[3] * last_wave, st.max_bounces);
     }
   }
   return LOTUS_PASS;

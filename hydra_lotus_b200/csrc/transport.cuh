@@ -531,6 +531,10 @@ struct FrameConst {
   const uint4* primary_hit;
   const uint32_t* primary_rng;
   uint32_t primary_sample;
+  // The wavefront's samples: `wave` consecutive samples from sample_index
+  // (0 counts as 1), sample k's paths in the slots k * wave_stride + pixel.
+  uint32_t wave;
+  uint32_t wave_stride;
 };
 
 // CameraRay (scene.slang:273-283).

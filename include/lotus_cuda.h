@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LOTUS_CUDA_ABI_VERSION 6u
+#define LOTUS_CUDA_ABI_VERSION 7u
 
 /* FrameStatus (vulkan_backend.hpp:23-27). */
 #define LOTUS_PASS 0
@@ -280,6 +280,12 @@ typedef struct lotus_frame_result {
   /* With LOTUS_FRAME_TIMINGS: the tail kernel's device time (the paths still
    * queued after the wavefront_rounds rounds, each followed to its end). */
   double tail_gpu_ms;
+  /* The samples the call's last wavefront held: a call that adds two or
+   * more samples (without the radiance cache) runs them two to a wavefront,
+   * and then the queue counts, the timings and the visit counts above are
+   * those of its last wave, both samples together. */
+  uint32_t last_wave_samples;
+  uint32_t reserved;
   char detail[256];
 } lotus_frame_result;
 

@@ -179,11 +179,15 @@ def test_fp16_moments(cuda):
             p16 = products(r16, SIZE, SIZE, ["surface", "radiance"])
             for m in (0, 1):
                 a, b = p32["radiance"]["moments"][..., m], p16["radiance"]["moments"][..., m]
-                assert np.array_equal(b, b.astype(np.float16).astype(np.float32)), f"{m} is not half-valued"
+                assert np.array_equal(b, b.astype(np.float16).astype(np.float32), equal_nan=True), \
+                    f"moment {m} is not half-valued"
+                # Half rounding, saturating at the largest finite half.
+                half = np.where(a > 65504.0, np.float32(65504.0), a).astype(np.float16).astype(np.float32)
                 if k == 0:
-                    assert np.array_equal(b, a.astype(np.float16).astype(np.float32)), m
+                    differ = ~((b == half) | (np.isnan(a) & np.isnan(b)))
+                    assert not differ.any(), (m, a[differ][:8], b[differ][:8])
                 else:
-                    assert np.all(np.abs(a - b) <= 4e-3 * np.abs(a) + 1e-7), (m, np.abs(a - b).max())
+                    assert np.all(np.abs(half - b) <= 4e-3 * np.abs(half) + 1e-7), (m, np.abs(half - b).max())
             var = ref.estimate_variance(p16["surface"], p16["radiance"], 1, d16.max_history_samples)
             np.testing.assert_allclose(p16["radiance"]["variance"], var, rtol=VARIANCE_RTOL, atol=VARIANCE_ATOL)
             err = metrics.relmse(c16, c32)
