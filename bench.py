@@ -681,12 +681,11 @@ def main():
             "e2e": {"value": round(total_e2e_rays / (max_e2e_ms * 1e-3) / 1e6, 2),
                     "unit": "Mrays/s", "h2d_bytes_per_step": 160,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 16 + 64},
-            # Per step: SPP samples in waves of two (each wave's launches as
+            # Per step: SPP samples in waves of four (each wave's launches as
             # one sample's, its frame constants in place of the advance),
             # chained 16 samples at a time, each chain advancing the frame
             # constants once.
-            "gpu_launches": (launches_per_sample(DEPTH, timed.wavefront_rounds) * (SPP // 2) +
-                             launches_per_sample(DEPTH, timed.wavefront_rounds) * (SPP % 2) +
+            "gpu_launches": (launches_per_sample(DEPTH, timed.wavefront_rounds) * (SPP // 4 + SPP % 4) +
                              (SPP + 15) // 16) * args.steps,
             "roofline": {
                 "kernel": "k_wf_extend",

@@ -263,7 +263,8 @@ __device__ __forceinline__ F3 miss_path(const SceneView& S, const FrameConst& f,
 // environment image shows behind it.
 __device__ __forceinline__ float4 resolve_pixel(const SceneView& S, const FrameConst& f,
     uint32_t px, uint32_t py, double4 sum) {
-  const double count = (double)(f.accumulated + f.add_sample);
+  // The samples in the accumulation once this wave's are added.
+  const double count = (double)(f.accumulated + f.add_sample * max(f.wave, 1u));
   const bool env_shows = f.environment_background != 0 && S.env_bound != 0;
   if (sum.w == 0.0 && (!env_shows || count == 0.0))
     return make_float4(f.background[0], f.background[1], f.background[2], f.background[3]);

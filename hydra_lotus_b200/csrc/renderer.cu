@@ -146,86 +146,123 @@ float host_coverage(const lotus_material& m) {
 
 // The environment image's sampling distribution (BuildEnvironmentDistribution,
 // gpu_scene.cpp:638-711): cells of at most 2048 x 1024, each the mean
-// scaled radiance of its texels times sin(theta) at the row's centre.
-struct EnvDistribution {
-  uint32_t columns = 0, rows = 0;
-  std::vector<float> floats;  // density, marginal (rows + 1), conditional (rows x (columns + 1))
-  double mean = 0.0;
-};
-
-EnvDistribution build_env_distribution(const lotus_environment& e) {
-  constexpr double kPiD = 3.14159265358979323846;
-  EnvDistribution d;
-  d.columns = std::min(e.width, 2048u);
-  d.rows = std::min(e.height, 1024u);
-  const size_t cells = (size_t)d.columns * d.rows;
-  std::vector<double> sums(cells, 0.0);
-  std::vector<uint32_t> counts(cells, 0);
-  for (uint32_t y = 0; y < e.height; ++y) {
-    const size_t row = (uint64_t)y * d.rows / e.height;
-    for (uint32_t x = 0; x < e.width; ++x) {
-      const size_t column = (uint64_t)x * d.columns / e.width;
-      const float* t = e.texels + 4 * ((size_t)y * e.width + x);
+// scaled radiance of its texels times sin(theta) at the row's centre; the
+// floats are the density per cell, the marginal CDF (rows + 1) and each
+// row's conditional CDF (columns + 1), then guide tables of the CDFs.
+// The same distribution and guide tables built on the device from the
+// resident texels, in the host build's arithmetic and order (each cell's
+// texels rows first, each row's cells and the rows' sums one after
+// another, in double), so that it gives the host build's floats bit for bit:
+// one thread per cell for the cell means, per row for its sum and CDF, one
+// for the marginal. Only the rows' sin(theta) comes from the host, whose
+// libm the host build uses.
+__global__ void k_env_cells(const float4* __restrict__ texels, uint32_t width, uint32_t height,
+    uint32_t columns, uint32_t rows, float sx, float sy, float sz, const double* __restrict__ sin_theta,
+    double* __restrict__ values) {
+  const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= columns * rows) return;
+  const uint32_t row = cell / columns, column = cell % columns;
+  // The texels whose row (column) maps to this cell's: y * rows / height == row.
+  const uint32_t y0 = (uint32_t)(((uint64_t)row * height + rows - 1) / rows);
+  const uint32_t y1 = (uint32_t)(((uint64_t)(row + 1) * height + rows - 1) / rows);
+  const uint32_t x0 = (uint32_t)(((uint64_t)column * width + columns - 1) / columns);
+  const uint32_t x1 = (uint32_t)(((uint64_t)(column + 1) * width + columns - 1) / columns);
+  double sum = 0.0;
+  uint32_t count = 0;
+  const double scale[3] = {(double)sx, (double)sy, (double)sz};
+  for (uint32_t y = y0; y < y1; ++y)
+    for (uint32_t x = x0; x < x1; ++x) {
+      const float4 t = texels[(size_t)y * width + x];
+      const double c[3] = {(double)t.x, (double)t.y, (double)t.z};
       double radiance = 0.0;
-      for (int c = 0; c < 3; ++c) radiance += std::max((double)t[c], 0.0) * (double)e.scale[c];
-      sums[row * d.columns + column] += radiance / 3.0;
-      ++counts[row * d.columns + column];
+      for (int k = 0; k < 3; ++k) radiance += (c[k] < 0.0 ? 0.0 : c[k]) * scale[k];
+      sum += radiance / 3.0;
+      ++count;
     }
-  }
-  std::vector<double> values(cells), row_sums(d.rows, 0.0);
-  double total = 0.0;
-  for (uint32_t row = 0; row < d.rows; ++row) {
-    const double sin_theta = std::sin(kPiD * (row + 0.5) / d.rows);
-    for (uint32_t column = 0; column < d.columns; ++column) {
-      const size_t cell = (size_t)row * d.columns + column;
-      values[cell] = sums[cell] / counts[cell] * sin_theta;
-      row_sums[row] += values[cell];
-    }
-    total += row_sums[row];
-  }
-  const double mean = total / (double)cells;
-  d.floats.assign(cells + d.rows + 1 + (size_t)d.rows * (d.columns + 1), 0.0f);
-  if (!(mean > 0.0) || !std::isfinite(mean)) return d;
-  d.mean = mean;
-  float* density = d.floats.data();
-  float* marginal = density + cells;
-  float* conditional = marginal + d.rows + 1;
-  for (size_t cell = 0; cell < cells; ++cell) density[cell] = (float)(values[cell] / mean);
-  double cumulative = 0.0;
-  for (uint32_t row = 0; row < d.rows; ++row) {
-    cumulative += row_sums[row];
-    marginal[row + 1] = (float)(cumulative / total);
-    float* cdf = conditional + (size_t)row * (d.columns + 1);
-    double along = 0.0;
-    for (uint32_t column = 0; column < d.columns; ++column) {
-      along += values[(size_t)row * d.columns + column];
-      cdf[column + 1] = row_sums[row] > 0.0 ? (float)(along / row_sums[row])
-                                            : (float)(column + 1) / d.columns;
-    }
-    cdf[d.columns] = 1.0f;
-  }
-  marginal[d.rows] = 1.0f;
-  return d;
+  values[cell] = sum / count * sin_theta[row];
 }
 
-// Guide tables of the environment's cumulative distributions (the
-// marginal's, then each row's conditional's): entry k of a table with K
-// buckets counts the CDF entries <= k / K, so the device's FindInterval
-// searches only the entries between two consecutive guide values.
-std::vector<uint32_t> build_env_guides(const EnvDistribution& d) {
-  std::vector<uint32_t> g((kEnvGuideMarginal + 1) + (size_t)d.rows * (kEnvGuideConditional + 1));
-  const size_t cells = (size_t)d.columns * d.rows;
-  auto fill = [](const float* F, uint32_t entries, uint32_t buckets, uint32_t* out) {
-    for (uint32_t k = 0; k <= buckets; ++k) {
-      const float x = (float)k / (float)buckets;
-      out[k] = (uint32_t)(std::upper_bound(F, F + entries, x) - F);
-    }
-  };
-  fill(d.floats.data() + cells, d.rows + 1, kEnvGuideMarginal, g.data());
-  for (uint32_t row = 0; row < d.rows; ++row)
-    fill(d.floats.data() + cells + d.rows + 1 + (size_t)row * (d.columns + 1), d.columns + 1,
-        kEnvGuideConditional, g.data() + (kEnvGuideMarginal + 1) + (size_t)row * (kEnvGuideConditional + 1));
-  return g;
+__global__ void k_env_row_sums(const double* __restrict__ values, uint32_t columns, uint32_t rows,
+    double* __restrict__ row_sums) {
+  const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= rows) return;
+  double sum = 0.0;
+  for (uint32_t column = 0; column < columns; ++column) sum += values[(size_t)row * columns + column];
+  row_sums[row] = sum;
+}
+
+// totals[0]: the rows' sum; totals[1]: the mean over the cells.
+__global__ void k_env_total(const double* __restrict__ row_sums, uint32_t columns, uint32_t rows,
+    double* __restrict__ totals, float* __restrict__ marginal) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double total = 0.0;
+  for (uint32_t row = 0; row < rows; ++row) total += row_sums[row];
+  const double mean = total / (double)((size_t)columns * rows);
+  totals[0] = total;
+  totals[1] = mean;
+  if (!(mean > 0.0) || !isfinite(mean)) return;
+  double cumulative = 0.0;
+  marginal[0] = 0.0f;
+  for (uint32_t row = 0; row < rows; ++row) {
+    cumulative += row_sums[row];
+    marginal[row + 1] = (float)(cumulative / total);
+  }
+  marginal[rows] = 1.0f;
+}
+
+__global__ void k_env_density(const double* __restrict__ values, uint32_t cells, const double* __restrict__ totals,
+    float* __restrict__ density) {
+  const uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= cells) return;
+  const double mean = totals[1];
+  density[cell] = (mean > 0.0 && isfinite(mean)) ? (float)(values[cell] / mean) : 0.0f;
+}
+
+__global__ void k_env_conditional(const double* __restrict__ values, const double* __restrict__ row_sums,
+    uint32_t columns, uint32_t rows, float* __restrict__ conditional) {
+  const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= rows) return;
+  float* cdf = conditional + (size_t)row * (columns + 1);
+  const double sum = row_sums[row];
+  double along = 0.0;
+  cdf[0] = 0.0f;
+  for (uint32_t column = 0; column < columns; ++column) {
+    along += values[(size_t)row * columns + column];
+    cdf[column + 1] = sum > 0.0 ? (float)(along / sum) : (float)(column + 1) / columns;
+  }
+  cdf[columns] = 1.0f;
+}
+
+// Guide entry k of table `table` (0: the marginal; 1 + r: row r's
+// conditional): the CDF entries <= k / K (std::upper_bound's count).
+__global__ void k_env_guides(const float* __restrict__ marginal, const float* __restrict__ conditional,
+    uint32_t columns, uint32_t rows, uint32_t* __restrict__ guides) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t marginal_entries = kEnvGuideMarginal + 1;
+  const uint32_t total = marginal_entries + rows * (kEnvGuideConditional + 1);
+  if (i >= total) return;
+  const float* F;
+  uint32_t entries, buckets, k;
+  if (i < marginal_entries) {
+    F = marginal;
+    entries = rows + 1;
+    buckets = kEnvGuideMarginal;
+    k = i;
+  } else {
+    const uint32_t j = i - marginal_entries, row = j / (kEnvGuideConditional + 1);
+    F = conditional + (size_t)row * (columns + 1);
+    entries = columns + 1;
+    buckets = kEnvGuideConditional;
+    k = j % (kEnvGuideConditional + 1);
+  }
+  const float x = (float)k / (float)buckets;
+  uint32_t lo = 0, hi = entries;  // the first entry above x
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (x < F[mid]) hi = mid;
+    else lo = mid + 1;
+  }
+  guides[i] = lo;
 }
 
 // The light table (BuildLightTable, gpu_scene.cpp:515-610): every emissive
@@ -573,6 +610,9 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
 // The longest chain of samples one RenderScene graph holds (two in flight
 // at a time): each sample has its own frame constants.
 constexpr uint32_t kMaxChain = 16;
+// The most samples one wavefront holds (a wave): the path state and queues
+// have room for this many times the target's pixels.
+constexpr uint32_t kMaxWave = 4;
 
 // The resident scene as the incremental updates need it: each geometry's
 // arrays (owned copies; `geometries` points into them), its box and its
@@ -730,7 +770,7 @@ struct Renderer {
   // at index length / 2), all of one key, so that a call whose remainder
   // makes a short chain does not re-instantiate the long one.
   cudaGraphExec_t graph = nullptr;
-  cudaGraphExec_t graph_chains[kMaxChain / 2 + 1] = {};
+  cudaGraphExec_t graph_chains[2 * (kMaxChain / 2 + 1)] = {};
   struct GraphKey {
     uint64_t scene_generation;
     uint32_t width, height, max_bounces;
@@ -1095,6 +1135,49 @@ int32_t finish_update(Renderer& R, lotus_scene_result& res, std::string& detail)
   return LOTUS_PASS;
 }
 
+// The environment's sampling distribution and guide tables, built on the
+// device from the resident texels (the k_env_* kernels); `mean` is the mean
+// cell value, positive and finite for an image that can be sampled.
+bool build_env_distribution(Renderer& R, const lotus_environment& e, double& mean, std::string& detail) {
+  constexpr double kPiD = 3.14159265358979323846;
+  cudaStream_t st = R.stream;
+  const uint32_t columns = std::min(e.width, 2048u), rows = std::min(e.height, 1024u);
+  const uint32_t cells = columns * rows;
+  std::vector<double> sin_theta(rows);
+  for (uint32_t row = 0; row < rows; ++row) sin_theta[row] = std::sin(kPiD * (row + 0.5) / rows);
+  DeviceArray<double> values, row_sums, totals, sines;
+  const size_t floats = (size_t)cells + rows + 1 + (size_t)rows * (columns + 1);
+  const size_t guides = (kEnvGuideMarginal + 1) + (size_t)rows * (kEnvGuideConditional + 1);
+  if (!R.ok(values.resize(cells), "environment distribution", detail) ||
+      !R.ok(row_sums.resize(rows), "environment distribution", detail) ||
+      !R.ok(totals.resize(2), "environment distribution", detail) ||
+      !R.ok(sines.upload(sin_theta.data(), rows, st), "environment distribution", detail) ||
+      !R.ok(R.env_floats.resize(floats), "environment distribution", detail) ||
+      !R.ok(R.env_guide.resize(guides), "environment guide tables", detail) ||
+      !R.ok(cudaMemsetAsync(R.env_floats.ptr, 0, floats * sizeof(float), st), "environment distribution", detail))
+    return false;
+  float* density = R.env_floats.ptr;
+  float* marginal = density + cells;
+  float* conditional = marginal + rows + 1;
+  const uint32_t b = 256;
+  k_env_cells<<<(cells + b - 1) / b, b, 0, st>>>(R.env_texels.ptr, e.width, e.height, columns, rows, e.scale[0],
+      e.scale[1], e.scale[2], sines.ptr, values.ptr);
+  k_env_row_sums<<<(rows + b - 1) / b, b, 0, st>>>(values.ptr, columns, rows, row_sums.ptr);
+  k_env_total<<<1, 32, 0, st>>>(row_sums.ptr, columns, rows, totals.ptr, marginal);
+  k_env_density<<<(cells + b - 1) / b, b, 0, st>>>(values.ptr, cells, totals.ptr, density);
+  k_env_conditional<<<(rows + b - 1) / b, b, 0, st>>>(values.ptr, row_sums.ptr, columns, rows, conditional);
+  k_env_guides<<<(uint32_t)((guides + b - 1) / b), b, 0, st>>>(marginal, conditional, columns, rows,
+      R.env_guide.ptr);
+  double t[2] = {0.0, 0.0};
+  if (!R.ok(cudaGetLastError(), "environment distribution", detail) ||
+      !R.ok(cudaMemcpyAsync(t, totals.ptr, sizeof(t), cudaMemcpyDeviceToHost, st), "environment distribution",
+          detail) ||
+      !R.ok(cudaStreamSynchronize(st), "environment distribution", detail))
+    return false;
+  mean = t[1];
+  return true;
+}
+
 int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result& res) {
   std::string detail;
   if (!validate_scene(s, detail)) {
@@ -1200,27 +1283,24 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
     r.coverage = make_float4(m.opacity, m.opacity_threshold, fbits, 0.0f);
   }
   if (!R.ok(R.materials.upload(h_mat.data(), h_mat.size(), st), "materials", detail)) return fail(detail);
-  // Environment.
-  EnvDistribution env;
+  // Environment: the texels go to the device, where its sampling
+  // distribution is built (build_env_distribution).
+  h.env_bound = false;
+  double env_mean = 0.0;
   if (s.environment && s.environment->texels && s.environment->width && s.environment->height) {
-    env = build_env_distribution(*s.environment);
-    h.env_bound = env.mean > 0.0;
-  }
-  if (h.env_bound) {
     const size_t texels = (size_t)s.environment->width * s.environment->height;
     if (!R.ok(R.env_texels.upload(reinterpret_cast<const float4*>(s.environment->texels), texels, st),
             "environment texels", detail) ||
-        !R.ok(R.env_floats.upload(env.floats.data(), env.floats.size(), st), "environment distribution",
-            detail))
+        !build_env_distribution(R, *s.environment, env_mean, detail))
       return fail(detail);
-    const std::vector<uint32_t> guides = build_env_guides(env);
-    if (!R.ok(R.env_guide.upload(guides.data(), guides.size(), st), "environment guide tables", detail))
-      return fail(detail);
-    h.env_mean = env.mean;
+    h.env_bound = env_mean > 0.0 && std::isfinite(env_mean);
+  }
+  if (h.env_bound) {
+    h.env_mean = env_mean;
     h.env_width = s.environment->width;
     h.env_height = s.environment->height;
-    h.env_columns = env.columns;
-    h.env_rows = env.rows;
+    h.env_columns = std::min(s.environment->width, 2048u);
+    h.env_rows = std::min(s.environment->height, 1024u);
     for (int k = 0; k < 3; ++k) h.env_scale[k] = s.environment->scale[k];
     for (int k = 0; k < 9; ++k) h.env_frame[k] = s.environment->environment_from_world[k];
   } else {
@@ -1386,8 +1466,8 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
       !R.ok(R.totals.resize(1), "ray totals", detail))
     return false;
   if (wavefront) {
-    // Room for a wave of two samples.
-    const size_t w = 2 * n;
+    // Room for a wave of kMaxWave samples.
+    const size_t w = kMaxWave * n;
     if (!R.ok(R.path_origin.resize(w), "path state", detail) ||
         !R.ok(R.path_direction.resize(w), "path state", detail) ||
         !R.ok(R.path_throughput.resize(w), "path state", detail) ||
@@ -1687,24 +1767,26 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   uint32_t last_rounds = wavefront_rounds(st.max_bounces, want_visits, tuning.rounds, use_cache ? cq.bounce : 0u);
   const bool choose_rounds = wavefront && R.tuning.rounds == 0 && !(R.rounds_key == gk);
   // Samples in waves: where two or more are added without the radiance
-  // cache (which trains between samples), the wavefront runs two samples as
-  // one wave, their paths in slots k * pixels + pixel of a path state twice
-  // the target's size, so that every launch holds both samples' paths and
-  // pays its ramp-up and drain once for them. Chains of up to kMaxChain / 2
-  // waves run two in flight: wave j on path state j % 2 and stream j % 2,
-  // each resolving (its samples in order) after wave j - 1, so that only
-  // the chain's last tail runs alone. A call's profiled part (timings or
-  // visit counts) is its last wave (or sample), run alone.
+  // cache (which trains between samples), the wavefront runs `wave` samples
+  // (four, or two for a call of two or three) as one wave, their paths in
+  // slots k * pixels + pixel of a path state kMaxWave times the target's
+  // size, so that every launch holds the wave's paths and pays its ramp-up
+  // and drain once for them. Chains of up to kMaxChain samples run two
+  // waves in flight: wave j on path state j % 2 and stream j % 2, each
+  // resolving (its samples in order) after wave j - 1, so that only the
+  // chain's last tail runs alone. A call's profiled part (timings or visit
+  // counts) is its last wave (or sample), run alone.
   const uint32_t pixels = t.width * t.height;
   const bool waves = wavefront && !use_cache && to_add >= 2;
-  const uint32_t profiled_samples = (want_timings || want_visits) ? (waves ? 2u : 1u) : 0u;
+  const uint32_t wave = to_add >= kMaxWave ? kMaxWave : 2u;
+  const uint32_t profiled_samples = (want_timings || want_visits) ? (waves ? wave : 1u) : 0u;
   const uint32_t chainable = waves ? submissions - profiled_samples : 0u;
   while (R.ev_sample_done.size() < kMaxChain) {
     cudaEvent_t e;
     if (!R.ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event", detail)) return poison(detail);
     R.ev_sample_done.push_back(e);
   }
-  if (chainable >= 4 && !ensure_pair_buffers(R, 2 * (size_t)pixels, detail)) return poison(detail);
+  if (chainable >= 2 * wave && !ensure_pair_buffers(R, kMaxWave * (size_t)pixels, detail)) return poison(detail);
   PathState P2{R.path_origin2.ptr, R.path_direction2.ptr, R.path_throughput2.ptr, R.path_radiance2.ptr,
       R.path_hit2.ptr};
   Queues Q2 = Q;
@@ -1715,17 +1797,18 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   Q2.counts = R.counts2.ptr;
   // A wave's queues hold both samples' paths.
   Queues QW = Q, QW2 = Q2;
-  QW.capacity = QW2.capacity = 2 * pixels;
+  QW.capacity = QW2.capacity = wave * pixels;
   const uint32_t* last_counts = R.counts.ptr;  // the call's last launch's queue counts
   uint32_t last_wave = 1;                      // and the samples it held
   FrameConst* fc0 = R.frame_const.ptr;
   cudaEventRecord(R.ev_start, s);
   for (uint32_t k = 0; k < submissions;) {
-    if (k + 2 <= chainable) {
-      // A chain of `length` samples (even, at most kMaxChain) in length / 2
-      // waves; wave j's frame constants are fc0's advanced by 2j.
-      const uint32_t length = std::min(kMaxChain, (chainable - k) & ~1u);
-      const uint32_t count = length / 2;
+    if (k + wave <= chainable) {
+      // A chain of `length` samples (a multiple of the wave, at most
+      // kMaxChain) in length / wave waves; wave j's frame constants are
+      // fc0's advanced by j waves.
+      const uint32_t length = std::min(kMaxChain, (chainable - k) / wave * wave);
+      const uint32_t count = length / wave;
       gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, 0u);
       if (!(R.graph_chain_key == gk)) {
         for (cudaGraphExec_t& old : R.graph_chains)
@@ -1735,19 +1818,19 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
           }
         R.graph_chain_key = gk;
       }
-      cudaGraphExec_t& chain = R.graph_chains[count];
+      cudaGraphExec_t& chain = R.graph_chains[(wave == kMaxWave ? kMaxChain / 2 + 1 : 0) + count];
       if (!chain) {
         cudaGraph_t g;
         if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
           return poison(detail);
-        for (uint32_t j = 0; j < count; ++j) launch_wave_frame(fc0, fc0 + 1 + j, 2 * j, 2, pixels, s);
+        for (uint32_t j = 0; j < count; ++j) launch_wave_frame(fc0, fc0 + 1 + j, wave * j, wave, pixels, s);
         cudaEventRecord(R.ev_fork, s);
         cudaStreamWaitEvent(R.stream2, R.ev_fork, 0);
         for (uint32_t j = 0; j < count; ++j) {
           const bool second = (j & 1u) != 0;
           launch_wavefront_sample(R.view, fc0 + 1 + j, rect, t.width, t.height, st.max_bounces, second ? P2 : P,
               second ? QW2 : QW, R.accum.ptr, R.color.ptr, R.totals.ptr, second ? R.stream2 : s, nullptr, tuning,
-              nullptr, j ? R.ev_sample_done[j - 1] : nullptr, 2);
+              nullptr, j ? R.ev_sample_done[j - 1] : nullptr, wave);
           cudaEventRecord(R.ev_sample_done[j], second ? R.stream2 : s);
         }
         cudaEventRecord(R.ev_join, R.stream2);
@@ -1761,21 +1844,21 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
       if (!R.ok(cudaGraphLaunch(chain, s), "graph launch", detail)) return poison(detail);
       k += length;
       last_counts = ((count - 1) & 1u) ? R.counts2.ptr : R.counts.ptr;
-      last_wave = 2;
+      last_wave = wave;
       last_rounds = gk.rounds;
       continue;
     }
     const bool profiled = profiled_samples != 0 && k + profiled_samples == submissions;
     last_rounds = wavefront_rounds(st.max_bounces, profiled && want_visits, tuning.rounds, use_cache ? cq.bounce : 0u);
     last_counts = R.counts.ptr;
-    if (profiled && profiled_samples == 2) {
-      // The profiled last wave: two samples in one wavefront, run alone.
-      launch_wave_frame(fc0, fc0 + 1, 0, 2, pixels, s);
+    if (profiled && profiled_samples > 1) {
+      // The profiled last wave, run alone.
+      launch_wave_frame(fc0, fc0 + 1, 0, wave, pixels, s);
       launch_wavefront_sample(R.view, fc0 + 1, rect, t.width, t.height, st.max_bounces, P, QW, R.accum.ptr,
-          R.color.ptr, R.totals.ptr, s, &profile, tuning, &cq, nullptr, 2);
-      launch_advance_by(fc0, 2, s);
-      k += 2;
-      last_wave = 2;
+          R.color.ptr, R.totals.ptr, s, &profile, tuning, &cq, nullptr, wave);
+      launch_advance_by(fc0, wave, s);
+      k += wave;
+      last_wave = wave;
       continue;
     }
     last_wave = 1;
