@@ -281,9 +281,10 @@ typedef struct lotus_frame_result {
    * queued after the wavefront_rounds rounds, each followed to its end). */
   double tail_gpu_ms;
   /* The samples the call's last wavefront held: a call that adds two or
-   * more samples (without the radiance cache) runs them two to a wavefront,
-   * and then the queue counts, the timings and the visit counts above are
-   * those of its last wave, both samples together. */
+   * more samples (without the radiance cache) runs them in waves of four
+   * (two for a call of two or three) to a wavefront, and then the queue
+   * counts, the timings and the visit counts above are those of its last
+   * wave, its samples together. */
   uint32_t last_wave_samples;
   uint32_t reserved;
   char detail[256];
