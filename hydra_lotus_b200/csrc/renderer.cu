@@ -750,6 +750,7 @@ struct Renderer {
     bool key_valid = false;
     uint32_t key[18] = {};
     bool restir_ran = false, accumulate_ran = false, spatial_ran = false, filter_ran = false;
+    bool moments_half = false;  // the latest frame's radiance records keep FP16 central moments
   } temporal;
   std::vector<lotus_instance> host_instances;
   // World bounds of the resident scene (the radiance cache's grid box).
@@ -2428,6 +2429,7 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   tc.history_cap = td.max_history_samples;
   tc.filter_iterations = td.filter_iterations;
   tc.moments_half = td.moment_precision == LOTUS_MOMENTS_FP16 ? 1u : 0u;
+  T.moments_half = tc.moments_half != 0;
   tc.restir_candidates = restir ? st.restir_candidates : 0u;
   tc.restir_history = reuse && previous ? 1u : 0u;
   tc.restir_max_history = st.restir_max_history_candidates;
@@ -2700,6 +2702,12 @@ int64_t lotus_cuda_read_product(lotus_cuda_renderer* r, uint32_t product, void* 
   if (!src || bytes > capacity) return -1;
   cudaSetDevice(R.device);
   if (cudaMemcpy(out, src, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  if (T.moments_half && (product == LOTUS_PRODUCT_RADIANCE || product == LOTUS_PRODUCT_PREVIOUS_RADIANCE)) {
+    // The FP16 moment mode stores the central second moment; the product
+    // carries the raw one, as the passes reconstruct it.
+    RadiancePixel* p = static_cast<RadiancePixel*>(out);
+    for (size_t i = 0; i < n; ++i) p[i].second_moment = p[i].second_moment + p[i].first_moment * p[i].first_moment;
+  }
   return (int64_t)bytes;
 }
 

@@ -576,10 +576,19 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
 
 // A luminance moment rounded to half precision (round to nearest even),
 // saturating at the largest finite half, 65504 (a NaN stays a NaN, so the
-// next frame drops the history as the FP32 mode does): the moments stored
-// by the FP16 moment mode.
+// next frame drops the history as the FP32 mode does).
 __device__ __forceinline__ float half_moment(float m) {
   return __half2float(__float2half_rn(m > 65504.0f ? 65504.0f : m));
+}
+
+// The FP16 moment mode keeps the first moment and the central second
+// moment, m2 - m1^2, each at half precision: the raw second moment in half
+// precision would lose the variance to cancellation wherever it is small
+// beside m1^2 (a half's relative step of 2^-11 of m2 exceeds it), and the
+// variance is what SVGF's edge-stopping weighs. The second moment a pass
+// reads is then the central one plus the stored first moment squared.
+__device__ __forceinline__ float second_moment(const TemporalConst& tc, const RadiancePixel& r) {
+  return tc.moments_half ? r.second_moment + r.first_moment * r.first_moment : r.second_moment;
 }
 
 // AccumulateTemporalRadiance (temporal.slang:229-267), without history
@@ -614,13 +623,13 @@ __global__ void __launch_bounds__(kBlock) k_svgf_accumulate(const TemporalConst*
         o.color.z += (h.color.z - o.color.z) * blend;
         o.color.w += (h.color.w - o.color.w) * blend;
         m1 += (h.first_moment - m1) * blend;
-        m2 += (h.second_moment - m2) * blend;
+        m2 += (second_moment(tc, h) - m2) * blend;
         o.sample_count = count;
       }
     }
     if (tc.moments_half) {
       m1 = half_moment(m1);
-      m2 = half_moment(m2);
+      m2 = half_moment(fmaxf(m2 - m1 * m1, 0.0f));
     }
     o.first_moment = m1;
     o.second_moment = m2;
@@ -663,7 +672,7 @@ __global__ void __launch_bounds__(kBlock) k_svgf_variance(const TemporalConst* _
   const float batches = float(center.sample_count) / float(min(tc.fresh_samples, tc.history_cap));
   if (center.sample_count != 0) {
     if (batches >= 4.0f) {
-      variance = fmaxf(0.0f, center.second_moment - center.first_moment * center.first_moment);
+      variance = fmaxf(0.0f, second_moment(tc, center) - center.first_moment * center.first_moment);
     } else {
       const TemporalPixel s = surface[index];
       const float depth = s.normal_depth.w;
@@ -683,7 +692,7 @@ __global__ void __launch_bounds__(kBlock) k_svgf_variance(const TemporalConst* _
           const float wl = fabsf(center.first_moment - nb.first_moment) / 10.0f;
           const float w = expf(-(wl + wz)) * wn;
           s1 += w * nb.first_moment;
-          s2 += w * nb.second_moment;
+          s2 += w * second_moment(tc, nb);
           weight_sum += w;
         }
       }

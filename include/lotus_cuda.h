@@ -391,10 +391,12 @@ typedef struct lotus_temporal_desc {
   uint32_t history_rectification;    /* TemporalHistoryRectification; only None (0) is built */
   /* Precision of the luminance moments the temporal accumulation keeps
    * between frames. LOTUS_MOMENTS_FP32: as the reference. LOTUS_MOMENTS_FP16:
-   * each blended moment is rounded to half precision (saturating at 65504)
-   * where the reference stores it, the blend itself staying FP32; the
-   * record keeps the reference's 32-byte layout. No counterpart in the
-   * reference. */
+   * the first moment and the central second moment (m2 - m1^2, which keeps
+   * the variance from cancelling away) are rounded to half precision
+   * (saturating at 65504) where the reference stores the moments, the blend
+   * itself staying FP32; the record keeps the reference's 32-byte layout,
+   * and the radiance products give the raw second moment back. No
+   * counterpart in the reference. */
   uint32_t moment_precision;
 } lotus_temporal_desc;
 

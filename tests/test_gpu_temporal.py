@@ -154,14 +154,15 @@ def test_restir_converges_to_mis_path_tracer(cuda):
 
 
 def test_fp16_moments(cuda):
-    """The FP16 moment mode (LOTUS_MOMENTS_FP16): the fresh frame's moments
-    are the FP32 mode's rounded to half precision; over later frames each
-    stored moment stays within a few half-precision rounding steps of the
-    FP32 mode's (relative 4e-3, the blend reading rounded history); the
-    variance the GPU derives from the stored moments matches the
-    reference's CPU EstimateTemporalVariance on the same moments at its
-    published tolerances, and the composite stays within 1e-3 relMSE of
-    the FP32 mode's."""
+    """The FP16 moment mode (LOTUS_MOMENTS_FP16): the stored first moment is
+    half-valued (on the fresh frame, the FP32 mode's rounded to half
+    precision, saturating at 65504); the central second moment is kept at
+    half precision, so the second moment the passes use stays within a few
+    half rounding steps of the FP32 mode's (relative 4e-3, away from the
+    saturation); the variance the GPU derives from the stored moments
+    matches the reference's CPU EstimateTemporalVariance on the same moments
+    at its published tolerances, and the composite stays within 1e-3 relMSE
+    of the FP32 mode's."""
     scene, descs32 = temporal_frames(abi.INTEGRATOR_WAVEFRONT)
     _, descs16 = temporal_frames(abi.INTEGRATOR_WAVEFRONT)
     for d in descs16:
@@ -177,20 +178,15 @@ def test_fp16_moments(cuda):
             cuda.check(res16, "FP16 frame")
             p32 = products(r32, SIZE, SIZE, ["surface", "radiance"])
             p16 = products(r16, SIZE, SIZE, ["surface", "radiance"])
-            for m in (0, 1):
-                a, b = p32["radiance"]["moments"][..., m], p16["radiance"]["moments"][..., m]
-                assert np.array_equal(b, b.astype(np.float16).astype(np.float32), equal_nan=True), \
-                    f"moment {m} is not half-valued"
-                # Half rounding, saturating at the largest finite half.
-                half = np.where(a > 65504.0, np.float32(65504.0), a).astype(np.float16).astype(np.float32)
-                if k == 0:
-                    differ = ~((b == half) | (np.isnan(a) & np.isnan(b)))
-                    assert not differ.any(), (m, a[differ][:8], b[differ][:8])
-                else:
-                    # Away from the saturation (whose clamp a blend carries
-                    # forward), within a few half rounding steps.
-                    bad = (np.abs(half - b) > 4e-3 * np.abs(half) + 1e-7) & (a < 1.0e4)
-                    assert not bad.any(), (m, bad.sum(), a[bad][:5], b[bad][:5])
+            a1, b1 = p32["radiance"]["moments"][..., 0], p16["radiance"]["moments"][..., 0]
+            a2, b2 = p32["radiance"]["moments"][..., 1], p16["radiance"]["moments"][..., 1]
+            assert np.array_equal(b1, b1.astype(np.float16).astype(np.float32), equal_nan=True)
+            half1 = np.where(a1 > 65504.0, np.float32(65504.0), a1).astype(np.float16).astype(np.float32)
+            if k == 0:
+                assert np.array_equal(b1, half1, equal_nan=True)
+            calm = (a2 < 1.0e4) & (a1 < 1.0e2)
+            bad = calm & (np.abs(a2 - b2) > 4e-3 * np.abs(a2) + 1e-6)
+            assert not bad.any(), (k, bad.sum(), a2[bad][:5], b2[bad][:5])
             var = ref.estimate_variance(p16["surface"], p16["radiance"], 1, d16.max_history_samples)
             np.testing.assert_allclose(p16["radiance"]["variance"], var, rtol=VARIANCE_RTOL, atol=VARIANCE_ATOL)
             err = metrics.relmse(c16, c32)
