@@ -29,6 +29,13 @@ STATIC_MAX_PIXELS = 65536
 FRAME_TIMINGS = 1
 FRAME_COUNT_VISITS = 2
 FRAME_DEPTH = 4
+
+SCENE_POSITIONS = 1
+SCENE_TRIANGLES = 2
+SCENE_NORMALS = 3
+SCENE_INSTANCES = 4
+SCENE_MATERIALS = 5
+SCENE_ENVIRONMENT = 6
 FRAME_DEPTH_KEEP = 8
 
 MOMENTS_FP32 = 0
@@ -37,7 +44,7 @@ MOMENTS_FP16 = 1
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
-ABI_VERSION = 7
+ABI_VERSION = 8
 
 # lotus_settings::output (SceneOutput).
 OUTPUT_RADIANCE = 0
@@ -221,7 +228,8 @@ class FrameResult(C.Structure):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("flags", C.c_uint32), ("bvh_leaf_size", C.c_uint32),
                 ("trace_refill_below", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32),
-                ("wavefront_rounds", C.c_uint32), ("traversal_step_limit", C.c_uint32)]
+                ("wavefront_rounds", C.c_uint32), ("traversal_step_limit", C.c_uint32),
+                ("samples_per_wave", C.c_uint32)]
 
 
 class TemporalDesc(C.Structure):

@@ -610,9 +610,11 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
 // The longest chain of samples one RenderScene graph holds (two in flight
 // at a time): each sample has its own frame constants.
 constexpr uint32_t kMaxChain = 16;
-// The most samples one wavefront holds (a wave): the path state and queues
-// have room for this many times the target's pixels.
-constexpr uint32_t kMaxWave = 4;
+// Samples one wavefront holds (a wave) unless lotus_cuda_options says
+// otherwise, and the most it may: the path state and queues have room for
+// the renderer's wave size times the target's pixels.
+constexpr uint32_t kDefaultWave = 4;
+constexpr uint32_t kMaxWave = 8;
 
 // The resident scene as the incremental updates need it: each geometry's
 // arrays (owned copies; `geometries` points into them), its box and its
@@ -703,6 +705,7 @@ struct Renderer {
   // before and read after each frame.
   DeviceArray<uint32_t> walk_failure;
   uint32_t step_limit = kMaxTraversalSteps;
+  uint32_t wave = kDefaultWave;  // samples per wavefront (lotus_cuda_options::samples_per_wave)
   // Profiling events, created on first use.
   std::vector<cudaEvent_t> profile_events;
   std::vector<int> profile_kinds;
@@ -771,7 +774,7 @@ struct Renderer {
   // at index length / 2), all of one key, so that a call whose remainder
   // makes a short chain does not re-instantiate the long one.
   cudaGraphExec_t graph = nullptr;
-  cudaGraphExec_t graph_chains[2 * (kMaxChain / 2 + 1)] = {};
+  cudaGraphExec_t graph_chains[3 * (kMaxChain / 2 + 1)] = {};
   struct GraphKey {
     uint64_t scene_generation;
     uint32_t width, height, max_bounces;
@@ -1467,8 +1470,8 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
       !R.ok(R.totals.resize(1), "ray totals", detail))
     return false;
   if (wavefront) {
-    // Room for a wave of kMaxWave samples.
-    const size_t w = kMaxWave * n;
+    // Room for a wave of the renderer's wave size.
+    const size_t w = (size_t)R.wave * n;
     if (!R.ok(R.path_origin.resize(w), "path state", detail) ||
         !R.ok(R.path_direction.resize(w), "path state", detail) ||
         !R.ok(R.path_throughput.resize(w), "path state", detail) ||
@@ -1769,17 +1772,18 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   const bool choose_rounds = wavefront && R.tuning.rounds == 0 && !(R.rounds_key == gk);
   // Samples in waves: where two or more are added without the radiance
   // cache (which trains between samples), the wavefront runs `wave` samples
-  // (four, or two for a call of two or three) as one wave, their paths in
-  // slots k * pixels + pixel of a path state kMaxWave times the target's
-  // size, so that every launch holds the wave's paths and pays its ramp-up
-  // and drain once for them. Chains of up to kMaxChain samples run two
+  // (the renderer's wave size, halved while the call adds fewer) as one
+  // wave, their paths in slots k * pixels + pixel of a path state R.wave
+  // times the target's size, so that every launch holds the wave's paths
+  // and pays its ramp-up and drain once for them. Chains of up to kMaxChain samples run two
   // waves in flight: wave j on path state j % 2 and stream j % 2, each
   // resolving (its samples in order) after wave j - 1, so that only the
   // chain's last tail runs alone. A call's profiled part (timings or visit
   // counts) is its last wave (or sample), run alone.
   const uint32_t pixels = t.width * t.height;
-  const bool waves = wavefront && !use_cache && to_add >= 2;
-  const uint32_t wave = to_add >= kMaxWave ? kMaxWave : 2u;
+  uint32_t wave = std::max(R.wave, 1u);
+  while (wave > 1 && wave > to_add) wave /= 2;
+  const bool waves = wavefront && !use_cache && to_add >= 2 && wave >= 2;
   const uint32_t profiled_samples = (want_timings || want_visits) ? (waves ? wave : 1u) : 0u;
   const uint32_t chainable = waves ? submissions - profiled_samples : 0u;
   while (R.ev_sample_done.size() < kMaxChain) {
@@ -1787,7 +1791,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     if (!R.ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event", detail)) return poison(detail);
     R.ev_sample_done.push_back(e);
   }
-  if (chainable >= 2 * wave && !ensure_pair_buffers(R, kMaxWave * (size_t)pixels, detail)) return poison(detail);
+  if (chainable >= 2 * wave && !ensure_pair_buffers(R, (size_t)R.wave * pixels, detail)) return poison(detail);
   PathState P2{R.path_origin2.ptr, R.path_direction2.ptr, R.path_throughput2.ptr, R.path_radiance2.ptr,
       R.path_hit2.ptr};
   Queues Q2 = Q;
@@ -1819,7 +1823,9 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
           }
         R.graph_chain_key = gk;
       }
-      cudaGraphExec_t& chain = R.graph_chains[(wave == kMaxWave ? kMaxChain / 2 + 1 : 0) + count];
+      // One graph per chain length and wave size (2, 4, 8).
+      const uint32_t shape = wave >= 8 ? 2u : wave >= 4 ? 1u : 0u;
+      cudaGraphExec_t& chain = R.graph_chains[shape * (kMaxChain / 2 + 1) + count];
       if (!chain) {
         cudaGraph_t g;
         if (!R.ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture", detail))
@@ -2046,9 +2052,13 @@ int32_t lotus_cuda_create(const lotus_cuda_options* options, lotus_cuda_renderer
     R.bvh_leaf_size = options->bvh_leaf_size;
   }
   if (options && (options->trace_refill_below > 32 || options->trace_blocks_per_sm > 64 ||
-                     options->wavefront_rounds > LOTUS_MAX_BOUNCES + 1)) {
+                     options->wavefront_rounds > LOTUS_MAX_BOUNCES + 1 ||
+                     (options->samples_per_wave != 0 && options->samples_per_wave != 1 &&
+                      options->samples_per_wave != 2 && options->samples_per_wave != 4 &&
+                      options->samples_per_wave != kMaxWave))) {
     copy_detail(error, error_size,
-        "trace_refill_below must be in 0..32, trace_blocks_per_sm in 0..64 and wavefront_rounds in 0..1025");
+        "trace_refill_below must be in 0..32, trace_blocks_per_sm in 0..64, wavefront_rounds in 0..1025 "
+        "and samples_per_wave 0, 1, 2, 4 or 8");
     delete h;
     return LOTUS_FAIL;
   }
@@ -2057,6 +2067,7 @@ int32_t lotus_cuda_create(const lotus_cuda_options* options, lotus_cuda_renderer
     R.tuning.blocks_per_sm = options->trace_blocks_per_sm;
     R.tuning.rounds = options->wavefront_rounds;
     if (options->traversal_step_limit) R.step_limit = options->traversal_step_limit;
+    if (options->samples_per_wave) R.wave = options->samples_per_wave;
   }
   std::string detail;
   if (!R.ok(cudaSetDevice(device), "cudaSetDevice", detail) ||
@@ -2164,6 +2175,105 @@ int32_t lotus_cuda_read_color(lotus_cuda_renderer* r, float* color, uint64_t cap
       cudaStreamSynchronize(R.stream) != cudaSuccess)
     return LOTUS_FAIL;
   return LOTUS_PASS;
+}
+
+int64_t lotus_cuda_read_scene(lotus_cuda_renderer* r, uint32_t what, uint32_t index, void* out,
+    uint64_t capacity) {
+  if (!r) return -1;
+  Renderer& R = r->r;
+  if (!R.scene_ready || !R.failure.empty()) return -1;
+  const HostScene& h = R.host;
+  const bool per_geometry = what == LOTUS_SCENE_POSITIONS || what == LOTUS_SCENE_TRIANGLES ||
+      what == LOTUS_SCENE_NORMALS;
+  if (per_geometry && index >= h.geometries.size()) return -1;
+  const uint32_t n_inst = (uint32_t)R.host_instances.size();
+  uint64_t bytes = 0;
+  switch (what) {
+    case LOTUS_SCENE_POSITIONS: bytes = 12ull * h.geometries[index].vertex_count; break;
+    case LOTUS_SCENE_TRIANGLES: bytes = 12ull * h.geometries[index].triangle_count; break;
+    case LOTUS_SCENE_NORMALS:
+      bytes = h.normal_base[index] == kNoLights ? 0 : 36ull * h.geometries[index].triangle_count;
+      break;
+    case LOTUS_SCENE_INSTANCES: bytes = sizeof(lotus_instance) * (uint64_t)n_inst; break;
+    case LOTUS_SCENE_MATERIALS: bytes = sizeof(lotus_material) * (uint64_t)R.materials.count; break;
+    case LOTUS_SCENE_ENVIRONMENT: bytes = 12; break;
+    default: return -1;
+  }
+  if (!out) return (int64_t)bytes;
+  if (capacity < bytes) return -1;
+  if (bytes == 0) return 0;
+  cudaSetDevice(R.device);
+  auto copy = [&](const void* src) {
+    return cudaMemcpy(out, src, bytes, cudaMemcpyDeviceToHost) == cudaSuccess;
+  };
+  switch (what) {
+    case LOTUS_SCENE_POSITIONS:
+      return copy(R.scene_pos.ptr + 3 * h.vertex_base[index]) ? (int64_t)bytes : -1;
+    case LOTUS_SCENE_TRIANGLES:
+      return copy(R.scene_tri.ptr + 3 * (size_t)h.tri_base[index]) ? (int64_t)bytes : -1;
+    case LOTUS_SCENE_NORMALS:
+      return copy(R.normals.ptr + 9 * (size_t)h.normal_base[index]) ? (int64_t)bytes : -1;
+    case LOTUS_SCENE_INSTANCES: {
+      // The shading records hold world_from_object's rows and the material
+      // slot; the traversal records the BLAS root, which names the geometry.
+      std::vector<InstanceShading> shade(n_inst);
+      std::vector<InstanceTraversal> trav(n_inst);
+      if (n_inst &&
+          (cudaMemcpy(shade.data(), R.inst_shade.ptr, n_inst * sizeof(InstanceShading), cudaMemcpyDeviceToHost) !=
+               cudaSuccess ||
+           cudaMemcpy(trav.data(), R.inst_trav.ptr, n_inst * sizeof(InstanceTraversal), cudaMemcpyDeviceToHost) !=
+               cudaSuccess))
+        return -1;
+      lotus_instance* o = static_cast<lotus_instance*>(out);
+      for (uint32_t i = 0; i < n_inst; ++i) {
+        std::memset(&o[i], 0, sizeof(o[i]));
+        const float4* m = shade[i].m;
+        const float rows[3][4] = {{m[0].x, m[0].y, m[0].z, m[0].w}, {m[1].x, m[1].y, m[1].z, m[1].w},
+            {m[2].x, m[2].y, m[2].z, m[2].w}};
+        for (int c = 0; c < 4; ++c) {
+          for (int rr = 0; rr < 3; ++rr) o[i].world_from_object[c * 4 + rr] = rows[rr][c];
+          o[i].world_from_object[c * 4 + 3] = c == 3 ? 1.0f : 0.0f;
+        }
+        o[i].material = shade[i].material;
+        // The resident host copy keeps each instance's geometry; the device
+        // record's BLAS root must name the same one (or none, for a
+        // geometry without triangles).
+        const uint32_t g = R.host_instances[i].geometry;
+        const uint32_t want = h.geometries[g].triangle_count ? h.node_base[g] : (uint32_t)kEmptyChild;
+        if (trav[i].blas_root != want) return -1;
+        o[i].geometry = g;
+      }
+      return (int64_t)bytes;
+    }
+    case LOTUS_SCENE_MATERIALS: {
+      std::vector<MaterialRecord> rec(R.materials.count);
+      if (cudaMemcpy(rec.data(), R.materials.ptr, rec.size() * sizeof(MaterialRecord), cudaMemcpyDeviceToHost) !=
+          cudaSuccess)
+        return -1;
+      lotus_material* o = static_cast<lotus_material*>(out);
+      for (size_t i = 0; i < rec.size(); ++i) {
+        const MaterialRecord& m = rec[i];
+        std::memset(&o[i], 0, sizeof(o[i]));
+        o[i].base_color[0] = m.base_roughness.x; o[i].base_color[1] = m.base_roughness.y;
+        o[i].base_color[2] = m.base_roughness.z; o[i].roughness = m.base_roughness.w;
+        o[i].emission[0] = m.emission_metallic.x; o[i].emission[1] = m.emission_metallic.y;
+        o[i].emission[2] = m.emission_metallic.z; o[i].metallic = m.emission_metallic.w;
+        o[i].specular_color[0] = m.specular_ior.x; o[i].specular_color[1] = m.specular_ior.y;
+        o[i].specular_color[2] = m.specular_ior.z; o[i].ior = m.specular_ior.w;
+        o[i].transmission_color[0] = m.transmission.x; o[i].transmission_color[1] = m.transmission.y;
+        o[i].transmission_color[2] = m.transmission.z; o[i].transmission = m.transmission.w;
+        o[i].opacity = m.coverage.x;
+        o[i].opacity_threshold = m.coverage.y;
+        std::memcpy(&o[i].flags, &m.coverage.z, 4);
+      }
+      return (int64_t)bytes;
+    }
+    case LOTUS_SCENE_ENVIRONMENT:
+      std::memcpy(out, R.view.env_constant, 12);
+      return 12;
+    default:
+      return -1;
+  }
 }
 
 int32_t lotus_cuda_read_depth(lotus_cuda_renderer* r, float* depth, uint64_t capacity_floats) {

@@ -550,10 +550,81 @@ void CudaOffscreenRenderer::FillTemporalProducts(const lotus_temporal_desc& d, b
   }
 }
 
+// ReadBackScene (vulkan_backend.hpp:819-821): the resident scene as the
+// device holds it, through lotus_cuda_read_scene, decoded into the
+// reference's contents. The CUDA backend keeps no texture-coordinate or
+// colour sets and no textures, so those stay empty.
 Lotus::GpuSceneContents CudaOffscreenRenderer::ReadBackScene() {
   Lotus::GpuSceneContents c;
-  c.status = Lotus::FrameStatus::Skip;
-  c.detail = "scene readback is not built in the CUDA backend";
+  auto fail = [&](const std::string& d) {
+    c = Lotus::GpuSceneContents{};
+    c.status = Lotus::FrameStatus::Fail;
+    c.detail = d;
+    return c;
+  };
+  if (failed_) return fail("the renderer failed earlier: " + failure_);
+  c.status = Lotus::FrameStatus::Pass;
+  if (!resident_) return c;
+  auto read = [&](uint32_t what, uint32_t index, std::vector<unsigned char>& out) {
+    const int64_t n = lotus_cuda_read_scene(handle_, what, index, nullptr, 0);
+    if (n < 0) return false;
+    out.resize((size_t)n);
+    return n == 0 || lotus_cuda_read_scene(handle_, what, index, out.data(), out.size()) == n;
+  };
+  std::vector<unsigned char> bytes;
+  for (uint32_t g = 0; g < geometries_.size(); ++g) {
+    Lotus::GpuGeometryContents geo;
+    geo.slot = g;
+    if (!read(LOTUS_SCENE_POSITIONS, g, bytes)) return fail("scene readback: positions");
+    geo.positions.resize(bytes.size() / 12);
+    std::memcpy(geo.positions.data(), bytes.data(), bytes.size());
+    if (!read(LOTUS_SCENE_TRIANGLES, g, bytes)) return fail("scene readback: triangles");
+    geo.triangles.resize(bytes.size() / 12);
+    std::memcpy(geo.triangles.data(), bytes.data(), bytes.size());
+    if (!read(LOTUS_SCENE_NORMALS, g, bytes)) return fail("scene readback: normals");
+    geo.normals.resize(bytes.size() / 12);
+    std::memcpy(geo.normals.data(), bytes.data(), bytes.size());
+    c.geometries.push_back(std::move(geo));
+  }
+  if (!read(LOTUS_SCENE_INSTANCES, 0, bytes)) return fail("scene readback: instances");
+  const size_t n_inst = bytes.size() / sizeof(lotus_instance);
+  const auto* inst = reinterpret_cast<const lotus_instance*>(bytes.data());
+  for (size_t i = 0; i < n_inst; ++i) {
+    Lotus::GpuInstanceContents ic;
+    std::memcpy(ic.world_from_object.data(), inst[i].world_from_object, 64);
+    ic.geometry_slot = inst[i].geometry;
+    ic.material_slot = inst[i].material;
+    c.instances.push_back(ic);
+    // The TLAS input: the transform's first three rows, row-major.
+    Lotus::GpuTlasInstanceContents t;
+    for (int row = 0; row < 3; ++row)
+      for (int col = 0; col < 4; ++col) t.object_to_world[row * 4 + col] = inst[i].world_from_object[col * 4 + row];
+    t.geometry_slot = inst[i].geometry;
+    t.mask = 0xFFu;
+    c.tlas_instances.push_back(t);
+  }
+  std::vector<unsigned char> mat_bytes;
+  if (!read(LOTUS_SCENE_MATERIALS, 0, mat_bytes)) return fail("scene readback: materials");
+  const auto* mats = reinterpret_cast<const lotus_material*>(mat_bytes.data());
+  for (size_t i = 0; i < mat_bytes.size() / sizeof(lotus_material); ++i) {
+    Lotus::GpuMaterialContents mc;
+    Lotus::PreviewSurface& p = Lotus::Preview(mc.material);
+    std::memcpy(p.base_color.data(), mats[i].base_color, 12);
+    p.roughness = mats[i].roughness;
+    std::memcpy(p.emission.data(), mats[i].emission, 12);
+    p.metallic = mats[i].metallic;
+    std::memcpy(p.specular_color.data(), mats[i].specular_color, 12);
+    p.ior = mats[i].ior;
+    std::memcpy(p.transmission_color.data(), mats[i].transmission_color, 12);
+    p.transmission = mats[i].transmission;
+    p.use_specular_workflow = (mats[i].flags & LOTUS_MATERIAL_SPECULAR_WORKFLOW) != 0;
+    p.thin_walled = (mats[i].flags & LOTUS_MATERIAL_THIN_WALLED) != 0;
+    mc.material.geometry.opacity = mats[i].opacity;
+    mc.material.geometry.opacity_threshold = mats[i].opacity_threshold;
+    c.materials.push_back(mc);
+  }
+  if (!read(LOTUS_SCENE_ENVIRONMENT, 0, bytes) || bytes.size() != 12) return fail("scene readback: environment");
+  std::memcpy(c.environment.data(), bytes.data(), 12);
   return c;
 }
 

@@ -57,6 +57,8 @@ def lib():
         L.lotus_cuda_read_color.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
         L.lotus_cuda_read_depth.restype = C.c_int32
         L.lotus_cuda_read_depth.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
+        L.lotus_cuda_read_scene.restype = C.c_int64
+        L.lotus_cuda_read_scene.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint64]
         L.lotus_cuda_stream.restype = C.c_void_p
         L.lotus_cuda_stream.argtypes = [C.c_void_p]
         L.lotus_cuda_render_static.restype = C.c_int32
@@ -128,11 +130,12 @@ class CudaOffscreenRenderer:
     accumulation targets."""
 
     def __init__(self, device=0, bvh_leaf_size=0, trace_refill_below=0, trace_blocks_per_sm=0,
-                 wavefront_rounds=0, traversal_step_limit=0):
+                 wavefront_rounds=0, traversal_step_limit=0, samples_per_wave=0):
         self.handle = None
         opts = abi.Options(device=device, flags=0, bvh_leaf_size=bvh_leaf_size,
                            trace_refill_below=trace_refill_below, trace_blocks_per_sm=trace_blocks_per_sm,
-                           wavefront_rounds=wavefront_rounds, traversal_step_limit=traversal_step_limit)
+                           wavefront_rounds=wavefront_rounds, traversal_step_limit=traversal_step_limit,
+                           samples_per_wave=samples_per_wave)
         h = C.c_void_p()
         err = C.create_string_buffer(256)
         status = lib().lotus_cuda_create(C.byref(opts), C.byref(h), err, 256)
@@ -242,6 +245,30 @@ class CudaOffscreenRenderer:
         if n < 0:
             raise RendererError(abi.FAIL, f"product {product} is not available")
         return out
+
+    def read_scene(self, what, index=0):
+        """ReadBackScene: a copy of the resident scene as the device holds
+        it (abi.SCENE_*): positions (n, 3), triangles (n, 3), corner normals
+        (n, 3, 3) of geometry `index`; every instance or material as ctypes
+        records; the constant environment (3,)."""
+        n = lib().lotus_cuda_read_scene(self.handle, what, index, None, 0)
+        if n < 0:
+            raise RendererError(abi.FAIL, f"scene readback {what} failed")
+        buf = (C.c_uint8 * max(int(n), 1))()
+        if lib().lotus_cuda_read_scene(self.handle, what, index, C.addressof(buf), n) != n:
+            raise RendererError(abi.FAIL, f"scene readback {what} failed")
+        raw = bytes(buf)[:n]
+        if what == abi.SCENE_POSITIONS:
+            return np.frombuffer(raw, np.float32).reshape(-1, 3)
+        if what == abi.SCENE_TRIANGLES:
+            return np.frombuffer(raw, np.uint32).reshape(-1, 3)
+        if what == abi.SCENE_NORMALS:
+            return np.frombuffer(raw, np.float32).reshape(-1, 3, 3)
+        if what == abi.SCENE_ENVIRONMENT:
+            return np.frombuffer(raw, np.float32)
+        rec = abi.Instance if what == abi.SCENE_INSTANCES else abi.Material
+        count = n // C.sizeof(rec)
+        return list((rec * count).from_buffer_copy(raw)) if count else []
 
     def read_depth(self, height, width):
         """The latest frame's depth product (LOTUS_FRAME_DEPTH): (H, W)

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LOTUS_CUDA_ABI_VERSION 7u
+#define LOTUS_CUDA_ABI_VERSION 8u
 
 /* FrameStatus (vulkan_backend.hpp:23-27). */
 #define LOTUS_PASS 0
@@ -313,6 +313,12 @@ typedef struct lotus_cuda_options {
    * naming the cause and poisons the renderer. Tests lower it to make the
    * bound run out. */
   uint32_t traversal_step_limit;
+  /* Samples a RenderScene call that adds several runs in one wavefront
+   * (their paths side by side in one set of queues, so that each launch
+   * pays its ramp-up and drain once for all of them): 1, 2, 4 or 8; 0: 4.
+   * The path state and queues take this many times the target's pixels.
+   * Results do not depend on it. */
+  uint32_t samples_per_wave;
 } lotus_cuda_options;
 
 typedef struct lotus_cuda_renderer lotus_cuda_renderer;
@@ -454,6 +460,30 @@ int64_t lotus_cuda_read_product(lotus_cuda_renderer* renderer, uint32_t product,
 /* The colour of the latest frame into host memory (width*height*4 floats). */
 int32_t lotus_cuda_read_color(lotus_cuda_renderer* renderer, float* color,
     uint64_t capacity_floats);
+
+/* ReadBackScene (vulkan_backend.hpp:819-821), for validation: copies of the
+ * resident scene as the device holds it, decoded into this ABI's records.
+ * `what` selects the copy and `index` the geometry where one is meant:
+ *   LOTUS_SCENE_POSITIONS  geometry `index`'s positions, 3 floats per vertex
+ *   LOTUS_SCENE_TRIANGLES  its triangles, 3 vertex indices each
+ *   LOTUS_SCENE_NORMALS    its corner normals, 9 floats per triangle (none
+ *                          without them)
+ *   LOTUS_SCENE_INSTANCES  every instance: lotus_instance records from the
+ *                          device's instance records (world_from_object,
+ *                          geometry, material slot)
+ *   LOTUS_SCENE_MATERIALS  every material: lotus_material records from the
+ *                          device's material table
+ *   LOTUS_SCENE_ENVIRONMENT the constant environment radiance, 3 floats
+ * Returns the bytes the copy takes (with `out` NULL, without copying), or
+ * -1 without a scene or for an unknown selection or a short buffer. */
+#define LOTUS_SCENE_POSITIONS 1u
+#define LOTUS_SCENE_TRIANGLES 2u
+#define LOTUS_SCENE_NORMALS 3u
+#define LOTUS_SCENE_INSTANCES 4u
+#define LOTUS_SCENE_MATERIALS 5u
+#define LOTUS_SCENE_ENVIRONMENT 6u
+int64_t lotus_cuda_read_scene(lotus_cuda_renderer* renderer, uint32_t what, uint32_t index, void* out,
+    uint64_t capacity_bytes);
 
 /* The depth product of the latest RenderScene frame that asked for it
  * (LOTUS_FRAME_DEPTH) into host memory: width*height floats, top-left rows.

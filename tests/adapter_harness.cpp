@@ -289,10 +289,23 @@ int main(int argc, char** argv) {
     if (inst.geometry == meshes[0].get()) inst.geometry = replacement.get();
   const Lotus::GpuSceneEvidence s3 = renderer->UpdateScene(edited);
   const Lotus::GpuFrameEvidence f3 = renderer->RenderScene(draw, target, frame_count, settings);
+  // ReadBackScene after the edits: every instance as uploaded, and the
+  // geometry each instance names holding that geometry's points.
+  const Lotus::GpuSceneContents contents = renderer->ReadBackScene();
+  bool readback = contents.status == Lotus::FrameStatus::Pass && contents.instances.size() == edited.instances.size() &&
+                  contents.tlas_instances.size() == edited.instances.size();
+  for (size_t i = 0; readback && i < edited.instances.size(); ++i) {
+    const Lotus::GpuInstanceContents& got = contents.instances[i];
+    readback = got.world_from_object == edited.instances[i].world_from_object &&
+               got.material_slot == edited.instances[i].material && got.geometry_slot < contents.geometries.size() &&
+               contents.geometries[got.geometry_slot].positions == edited.instances[i].geometry->positions &&
+               contents.geometries[got.geometry_slot].triangles == edited.instances[i].geometry->triangles;
+  }
   std::printf("{\"instance_edit\": \"%s\", \"instance_edit_render\": \"%s\", \"point_edit\": \"%s\", "
-              "\"point_edit_render\": \"%s\", \"detail\": \"%s%s\"}\n",
+              "\"point_edit_render\": \"%s\", \"readback\": \"%s\", \"materials\": %zu, \"detail\": \"%s%s%s\"}\n",
       status_name(s2.status), status_name(f2.status), status_name(s3.status), status_name(f3.status),
-      s2.detail.c_str(), s3.detail.c_str());
+      readback ? "pass" : "fail", contents.materials.size(), s2.detail.c_str(), s3.detail.c_str(),
+      contents.detail.c_str());
   {
     std::ofstream out(argv[4], std::ios::binary);
     out.write(reinterpret_cast<const char*>(f2.color.payload.data()), (std::streamsize)f2.color.payload.size());
@@ -302,7 +315,7 @@ int main(int argc, char** argv) {
     out.write(reinterpret_cast<const char*>(f3.color.payload.data()), (std::streamsize)f3.color.payload.size());
   }
   return s2.status == Lotus::FrameStatus::Pass && f2.status == Lotus::FrameStatus::Pass &&
-                 s3.status == Lotus::FrameStatus::Pass && f3.status == Lotus::FrameStatus::Pass
+                 s3.status == Lotus::FrameStatus::Pass && f3.status == Lotus::FrameStatus::Pass && readback
              ? 0
              : 1;
 }

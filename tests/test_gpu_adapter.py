@@ -62,13 +62,15 @@ def test_adapter_renders_what_the_c_abi_renders(cuda, harness, tmp_path, integra
 def test_adapter_incremental_updates_render_what_full_updates_render(cuda, harness, tmp_path):
     """An instance-only SceneUpdate and a same-topology geometry replacement
     go through lotus_cuda_update_instances / lotus_cuda_update_geometry and
-    give the images a full update of the edited scene gives."""
+    give the images a full update of the edited scene gives; ReadBackScene
+    then returns the edited instances and the points each one names."""
     scene = scenes.box_room(seed=0, size=48)
     st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
                               max_bounces=5, sample_index=3)
     code, evidence, colors = adapter_scene.run(str(tmp_path), scene, st, 4, edit_dx=0.05)
     assert code == 0, evidence
     assert evidence[-1]["instance_edit"] == "pass" and evidence[-1]["point_edit"] == "pass", evidence
+    assert evidence[-1]["readback"] == "pass" and evidence[-1]["materials"] == len(scene.materials), evidence
     moved = scenes.box_room(seed=0, size=48)
     m = np.array(moved.instances[0][0], dtype=np.float32)
     m[12] += np.float32(0.05)

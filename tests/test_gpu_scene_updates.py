@@ -105,3 +105,36 @@ def test_invalid_edits_fail_without_poisoning(cuda):
         extra.add_geometry(*scenes.quad([[0, 0, 0], [1, 0, 0], [1, 0, 1], [0, 0, 1]]))
         assert r.update_geometry(extra, len(extra.geometries) - 1).status == abi.FAIL
         cuda.check(render(r, scene)[0], "render after rejected edits")
+
+
+def test_scene_readback_equals_the_scene(cuda):
+    """ReadBackScene (lotus_cuda_read_scene): the device's geometry arrays,
+    instance records and material table decode to the scene that was
+    uploaded, after an instance edit too."""
+    from hydra_lotus_b200 import abi
+    scene = scenes.material_basics(size=32)
+    scene.environment_constant = (0.5, 0.25, 0.125)
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        for g, (p, t, n) in enumerate(scene.geometries):
+            assert np.array_equal(r.read_scene(abi.SCENE_POSITIONS, g), p)
+            assert np.array_equal(r.read_scene(abi.SCENE_TRIANGLES, g), t)
+            normals = r.read_scene(abi.SCENE_NORMALS, g)
+            assert (n is None and normals.size == 0) or np.array_equal(normals, n)
+        insts = r.read_scene(abi.SCENE_INSTANCES)
+        assert len(insts) == len(scene.instances)
+        for got, (m, g, mat) in zip(insts, scene.instances):
+            assert np.array_equal(np.array(got.world_from_object[:], np.float32), m)
+            assert (got.geometry, got.material) == (g, mat)
+        mats = r.read_scene(abi.SCENE_MATERIALS)
+        assert len(mats) == len(scene.materials)
+        for got, want in zip(mats, scene.materials):
+            assert bytes(got) == bytes(want)
+        assert np.array_equal(r.read_scene(abi.SCENE_ENVIRONMENT), np.array([0.5, 0.25, 0.125], np.float32))
+        m = np.array(scene.instances[3][0], dtype=np.float32)
+        m[12] += 0.25
+        scene.set_instance(3, m, material=1)
+        cuda.check(r.update_instances(scene), "update_instances")
+        got = r.read_scene(abi.SCENE_INSTANCES)[3]
+        assert np.array_equal(np.array(got.world_from_object[:], np.float32), m)
+        assert got.material == 1
