@@ -73,10 +73,23 @@ def settings(sample_index):
 
 
 def launches_per_sample(max_bounces, rounds):
-    # camera; shade and shadow per round, extend per round after the first;
-    # the tail kernel when the rounds stop short of max_bounces + 1;
-    # resolve, finish, advance
-    return 1 + 2 * rounds + (rounds - 1) + (1 if rounds <= max_bounces else 0) + 3
+    # camera; shade and shadow per round, extend per round after the first
+    # with the queue reordering's scan and scatter before it; the tail
+    # kernel when the rounds stop short of max_bounces + 1; resolve, finish,
+    # advance
+    return 1 + 2 * rounds + 3 * (rounds - 1) + (1 if rounds <= max_bounces else 0) + 3
+
+
+def wave_count(spp, wave=8):
+    """Wavefronts a call adding `spp` samples runs: waves of `wave`, halved
+    while fewer samples remain."""
+    count = 0
+    while spp > 0:
+        while wave > spp:
+            wave //= 2
+        spp -= wave
+        count += 1
+    return count
 
 
 def measured_peaks():
@@ -681,11 +694,11 @@ def main():
             "e2e": {"value": round(total_e2e_rays / (max_e2e_ms * 1e-3) / 1e6, 2),
                     "unit": "Mrays/s", "h2d_bytes_per_step": 160,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 16 + 64},
-            # Per step: SPP samples in waves of four (each wave's launches as
-            # one sample's, its frame constants in place of the advance),
+            # Per step: SPP samples in waves of eight (each wave's launches
+            # as one sample's, its frame constants in place of the advance),
             # chained 16 samples at a time, each chain advancing the frame
             # constants once.
-            "gpu_launches": (launches_per_sample(DEPTH, timed.wavefront_rounds) * (SPP // 4 + SPP % 4) +
+            "gpu_launches": (launches_per_sample(DEPTH, timed.wavefront_rounds) * wave_count(SPP) +
                              (SPP + 15) // 16) * args.steps,
             "roofline": {
                 "kernel": "k_wf_extend",
@@ -694,6 +707,10 @@ def main():
                 "peak": peak,
                 "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
+                # The same bytes over the extension kernels' time plus the
+                # queue reordering that prepares their queues.
+                "frac_with_reordering": round(ext_bytes / ((timed.extend_gpu_ms + timed.sort_gpu_ms) * 1e-3) / 1e9
+                                              / peak, 4) if timed.extend_gpu_ms else 0.0,
                 "peak_kind": peak_kind,
                 "frac_of_nominal": round(achieved / NOMINAL_HBM_GBS, 4),
                 "traffic": round(EXTEND_DRAM_BYTES_PER_RAY * ext_rays_timed / launches),
@@ -703,12 +720,15 @@ def main():
                 "nodes_per_ray": round(counted.node_visits[1] / n_ext, 2),
                 "triangles_per_ray": round(counted.triangle_visits[1] / n_ext, 2),
                 "instances_per_ray": round(counted.instance_visits[1] / n_ext, 2),
-                "extend_ms_per_sample": round(timed.extend_gpu_ms, 4),
-                "extend_launches_per_sample": launches,
-                "kernel_ms_per_sample": {
+                # The instrumented frame's last wave (its samples together).
+                "last_wave_samples": timed.last_wave_samples,
+                "extend_ms_last_wave": round(timed.extend_gpu_ms, 4),
+                "extend_launches_last_wave": launches,
+                "kernel_ms_last_wave": {
                     "camera": round(timed.camera_gpu_ms, 4), "extend": round(timed.extend_gpu_ms, 4),
                     "shade": round(timed.shade_gpu_ms, 4), "shadow": round(timed.shadow_gpu_ms, 4),
-                    "tail": round(timed.tail_gpu_ms, 4), "resolve": round(timed.resolve_gpu_ms, 4)},
+                    "tail": round(timed.tail_gpu_ms, 4), "resolve": round(timed.resolve_gpu_ms, 4),
+                    "reorder": round(timed.sort_gpu_ms, 4)},
                 "wavefront_rounds": timed.wavefront_rounds,
             },
             "cpu_baseline": cpu,

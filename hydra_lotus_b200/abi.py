@@ -44,7 +44,7 @@ MOMENTS_FP16 = 1
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
-ABI_VERSION = 8
+ABI_VERSION = 9
 
 # lotus_settings::output (SceneOutput).
 OUTPUT_RADIANCE = 0
@@ -221,6 +221,7 @@ class FrameResult(C.Structure):
         ("tail_gpu_ms", C.c_double),
         ("last_wave_samples", C.c_uint32),
         ("reserved", C.c_uint32),
+        ("sort_gpu_ms", C.c_double),
         ("detail", C.c_char * 256),
     ]
 

@@ -477,7 +477,7 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
   if (choose_rounds) {
     b->rounds_layout = layout;
     b->rounds_bounces = max_bounces;
-    b->auto_rounds = choose_wavefront_rounds(counts.data(), base[count], max_bounces);
+    b->auto_rounds = choose_wavefront_rounds(counts.data(), extension_resident_threads(), max_bounces);
   }
   for (uint32_t k = 0; k < count; ++k) {
     b->accumulated[k] += frame_count;

@@ -55,6 +55,60 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
   return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
 }
 
+// The reordering key's grid: the box of the TLAS root's children (the
+// scene's box), kSortAxisBits cells per axis.
+struct SortGrid {
+  float lo[3];
+  float scale[3];
+};
+
+__device__ __forceinline__ SortGrid sort_grid(const SceneView& S) {
+  SortGrid g;
+  float hi[3];
+  for (int a = 0; a < 3; ++a) {
+    g.lo[a] = 3.0e38f;
+    hi[a] = -3.0e38f;
+    g.scale[a] = 0.0f;
+  }
+  if (S.tlas == nullptr || S.instance_count == 0) return g;
+  const Bvh4Node& r = S.tlas[0];
+  const int child[4] = {r.child.x, r.child.y, r.child.z, r.child.w};
+  const float lx[4] = {r.lo_x.x, r.lo_x.y, r.lo_x.z, r.lo_x.w}, hx[4] = {r.hi_x.x, r.hi_x.y, r.hi_x.z, r.hi_x.w};
+  const float ly[4] = {r.lo_y.x, r.lo_y.y, r.lo_y.z, r.lo_y.w}, hy[4] = {r.hi_y.x, r.hi_y.y, r.hi_y.z, r.hi_y.w};
+  const float lz[4] = {r.lo_z.x, r.lo_z.y, r.lo_z.z, r.lo_z.w}, hz[4] = {r.hi_z.x, r.hi_z.y, r.hi_z.z, r.hi_z.w};
+  for (int i = 0; i < 4; ++i) {
+    if (child[i] == kEmptyChild) continue;
+    g.lo[0] = fminf(g.lo[0], lx[i]); hi[0] = fmaxf(hi[0], hx[i]);
+    g.lo[1] = fminf(g.lo[1], ly[i]); hi[1] = fmaxf(hi[1], hy[i]);
+    g.lo[2] = fminf(g.lo[2], lz[i]); hi[2] = fmaxf(hi[2], hz[i]);
+  }
+  for (int a = 0; a < 3; ++a)
+    g.scale[a] = hi[a] > g.lo[a] ? (float)(1u << kSortAxisBits) / (hi[a] - g.lo[a]) : 0.0f;
+  return g;
+}
+
+// Every third bit from bit 0 for the low ten bits of v.
+__device__ __forceinline__ uint32_t spread_bits3(uint32_t v) {
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__device__ __forceinline__ uint32_t sort_key(const SortGrid& g, const F3& o, const F3& d) {
+  const float p[3] = {o.x, o.y, o.z};
+  constexpr uint32_t top = (1u << kSortAxisBits) - 1u;
+  uint32_t cell[3];
+  for (int a = 0; a < 3; ++a) {
+    const float v = (p[a] - g.lo[a]) * g.scale[a];
+    cell[a] = v > 0.0f ? (v < (float)top ? (uint32_t)v : top) : 0u;
+  }
+  const uint32_t morton = spread_bits3(cell[0]) | (spread_bits3(cell[1]) << 1) | (spread_bits3(cell[2]) << 2);
+  const uint32_t octant = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+  return (morton << 3) | octant;
+}
+
 __device__ __forceinline__ void warp_add64(unsigned long long* counter, uint32_t value) {
   unsigned long long v = value;
 #pragma unroll
@@ -448,6 +502,12 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 1];
   const bool cache_vertex = kCacheVertex && bounce < fcp->max_bounces;
+  const bool keyed = !kBatch && Q.keys != nullptr;
+  __shared__ SortGrid grid;
+  if (keyed) {
+    if (threadIdx.x == 0) grid = sort_grid(S);
+    __syncthreads();
+  }
   // Grid-stride over the hit queue (the grid is sized to a few waves of
   // the SMs, not to the largest queue, so that the short queues of late
   // bounces cost little).
@@ -457,7 +517,7 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
     bool cont = false, query = false, training = false;
     ShadowRequest req;
     req.pending = false;
-    uint32_t slot = 0;
+    uint32_t slot = 0, key = 0;
     CacheRecord features;
     F3 T = V(1.0f), T_in = V(1.0f), R = V(0.0f);
     if (valid) {
@@ -489,6 +549,7 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
           cache_vertex && !training);
       query = cache_vertex && !training;
       if (cont) {
+        if (keyed) key = sort_key(grid, no, nd);
         P.origin[slot] = F4(no, 0.0f);
         P.direction[slot] = F4(nd, kFloatMax);
         P.throughput[slot] = F4(T, (flags & kUnweightedLight) ? -1.0f : last_pdf);
@@ -514,6 +575,13 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
     }
     const uint32_t ray_at = warp_append(&Q.counts[3 * (bounce + 1)], cont);
     if (cont) Q.ray[(bounce + 1) & 1][ray_at] = slot;
+    if (keyed && cont) {
+      // The key beside the ray, and one histogram increment per key held
+      // by the warp's lanes.
+      Q.keys[ray_at] = key;
+      const unsigned peers = __match_any_sync(__activemask(), key);
+      if ((threadIdx.x & 31u) == (unsigned)(__ffs(peers) - 1)) atomicAdd(&Q.bins[key], (uint32_t)__popc(peers));
+    }
     const uint32_t sh_at = warp_append(&Q.counts[3 * bounce + 2], req.pending);
     if (req.pending) {
       Q.shadow.ray_o[sh_at] = F4(req.origin, req.tmax);
@@ -722,7 +790,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_visibility(SceneV
 // a time.
 template <bool kCount, bool kBatch, bool kAnalytic>
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneView S,
-    const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce,
+    const FrameConst* __restrict__ fcp, PathState P, Queues Q, const uint32_t* __restrict__ rays_in, uint32_t bounce,
     uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits, SceneTable B) {
   __shared__ uint32_t staged[kBlock / 32][64];
   const uint32_t n = Q.counts[3 * bounce];
@@ -739,7 +807,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneVi
   for (;;) {
     const uint32_t got = warp_fetch(fetch, n, active, refill_below, exhausted);
     if (got < n) {
-      slot = Q.ray[bounce & 1][got];
+      slot = rays_in[got];
       if (kBatch) scene = table_scene(B, slot);
       const float4 o = P.origin[slot];
       const float4 d = P.direction[slot];
@@ -892,6 +960,68 @@ __global__ void __launch_bounds__(kBlock) k_wf_tail(SceneView S, const FrameCons
   }
 }
 
+// The key histogram's exclusive prefix within each block of kSortScanBlock
+// bins, in place, and each block's total after the bins.
+__global__ void __launch_bounds__(kSortScanBlock) k_sort_scan(uint32_t* __restrict__ bins) {
+  __shared__ uint32_t warp_total[kSortScanBlock / 32];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t i = blockIdx.x * kSortScanBlock + threadIdx.x;
+  const uint32_t v = bins[i];
+  uint32_t x = v;
+  for (unsigned off = 1; off < 32; off <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFullWarp, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) warp_total[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t t = warp_total[lane];
+    for (unsigned off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFullWarp, t, off);
+      if (lane >= off) t += y;
+    }
+    warp_total[lane] = t;
+  }
+  __syncthreads();
+  const uint32_t before = warp == 0 ? 0u : warp_total[warp - 1];
+  bins[i] = before + x - v;
+  if (threadIdx.x == kSortScanBlock - 1) bins[kSortBins + blockIdx.x] = before + x;
+}
+
+// The queue in key order: each block first scans the block totals; a
+// warp's rays of one key take consecutive places from one atomic.
+constexpr int kSortScatterBlock = 256;
+static_assert(kSortBlocks == kSortScatterBlock, "one scatter thread per histogram block");
+__global__ void __launch_bounds__(kSortScatterBlock) k_sort_scatter(const uint32_t* __restrict__ rays,
+    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ count, uint32_t* __restrict__ bins,
+    uint32_t* __restrict__ sorted) {
+  __shared__ uint32_t block_base[kSortBlocks];
+  __shared__ uint32_t warp_total[kSortScatterBlock / 32];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t v = bins[kSortBins + threadIdx.x];
+  uint32_t x = v;
+  for (unsigned off = 1; off < 32; off <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFullWarp, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) warp_total[warp] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  for (unsigned w = 0; w < warp; ++w) before += warp_total[w];
+  block_base[threadIdx.x] = before + x - v;
+  __syncthreads();
+  const uint32_t n = *count;
+  for (uint32_t i = blockIdx.x * kSortScatterBlock + threadIdx.x; i < n; i += gridDim.x * kSortScatterBlock) {
+    const uint32_t key = keys[i];
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(&bins[key], (uint32_t)__popc(peers)) + block_base[key / kSortScanBlock];
+    base = __shfl_sync(peers, base, leader);
+    sorted[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = rays[i];
+  }
+}
+
 __global__ void k_wf_finish(FrameConst* fc, const uint32_t* __restrict__ counts,
     uint32_t max_bounces, RayTotals* totals) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -1039,12 +1169,16 @@ uint32_t persistent_grid(const void* kernel, uint32_t capacity, const TraceTunin
   return std::max(1u, std::min(grid, (capacity + kBlock - 1) / kBlock));
 }
 
-uint32_t choose_wavefront_rounds(const uint32_t* counts, uint32_t camera, uint32_t max_bounces) {
+uint32_t choose_wavefront_rounds(const uint32_t* counts, uint32_t resident, uint32_t max_bounces) {
   constexpr uint32_t kTailQueue = 65536;
-  const uint32_t below = std::max(camera / 32u, kTailQueue);
+  const uint32_t below = std::max(resident, kTailQueue);
   for (uint32_t b = 1; b <= max_bounces; ++b)
     if (counts[3 * b] < below) return b;
   return max_bounces + 1;
+}
+
+uint32_t extension_resident_threads() {
+  return persistent_grid((const void*)k_wf_extend<false, false, false>, 1u << 30, TraceTuning()) * kBlock;
 }
 
 uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, uint32_t cache_bounce) {
@@ -1095,33 +1229,49 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   // `rounds` (if any can be) go to the tail kernel. Counting visits keeps
   // every bounce in rounds, as the counted kernels are the rounds' own.
   const uint32_t rounds = wavefront_rounds(max_bounces, count, tuning.rounds, C.enabled ? C.bounce : 0u);
+  const bool keyed = Q.keys != nullptr && Q.sorted != nullptr && Q.bins != nullptr;
+  const uint32_t grid_scatter = persistent_grid((const void*)k_sort_scatter, Q.capacity, TraceTuning());
   for (uint32_t b = 0; b < rounds; ++b) {
+    // The queue this round's extension reads: bounce b's rays in key order
+    // where shade (b - 1) keyed them.
+    const uint32_t* rays = Q.ray[b & 1];
+    if (b != 0 && keyed) {
+      Timed t(profile, stream, 7);
+      k_sort_scan<<<kSortBlocks, kSortScanBlock, 0, stream>>>(Q.bins);
+      k_sort_scatter<<<grid_scatter, kSortScatterBlock, 0, stream>>>(Q.ray[b & 1], Q.keys, Q.counts + 3 * b, Q.bins,
+          Q.sorted);
+      rays = Q.sorted;
+    }
     if (b != 0) {
       Timed t(profile, stream, 1);
       if (count && analytic)
-        k_wf_extend<true, false, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
+        k_wf_extend<true, false, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b, refill,
             visits, none);
       else if (count)
-        k_wf_extend<true, false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
+        k_wf_extend<true, false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b, refill,
             visits, none);
       else if (analytic)
-        k_wf_extend<false, false, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
+        k_wf_extend<false, false, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b, refill,
             nullptr, none);
       else
-        k_wf_extend<false, false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, b, fetch + 2 * b, refill,
+        k_wf_extend<false, false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b, refill,
             nullptr, none);
     }
     {
+      // Shade keys the rays it queues when a round extends them.
+      Queues QS = Q;
+      if (keyed && b + 1 < rounds) cudaMemsetAsync(Q.bins, 0, sizeof(uint32_t) * kSortBins, stream);
+      else QS.keys = nullptr;
       Timed t(profile, stream, 2);
       const bool cache_vertex = C.enabled && b == C.bounce;
       if (cache_vertex && analytic)
-        k_wf_shade<true, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
+        k_wf_shade<true, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, QS, b, C, none);
       else if (cache_vertex)
-        k_wf_shade<true, false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
+        k_wf_shade<true, false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, QS, b, C, none);
       else if (analytic)
-        k_wf_shade<false, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
+        k_wf_shade<false, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, QS, b, C, none);
       else
-        k_wf_shade<false, false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, Q, b, C, none);
+        k_wf_shade<false, false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, QS, b, C, none);
     }
     {
       Timed t(profile, stream, 3);
@@ -1225,10 +1375,10 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   const uint32_t rounds = wavefront_rounds(max_bounces, false, tuning.rounds);
   for (uint32_t b = 0; b < rounds; ++b) {
     if (b != 0 && B.analytic)
-      k_wf_extend<false, true, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, b,
+      k_wf_extend<false, true, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, Q.ray[b & 1], b,
           fetch + 2 * b, refill, nullptr, B);
     else if (b != 0)
-      k_wf_extend<false, true, false><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, b,
+      k_wf_extend<false, true, false><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, Q.ray[b & 1], b,
           fetch + 2 * b, refill, nullptr, B);
     if (B.analytic)
       k_wf_shade<false, true, true><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, Q, b, no_cache, B);

@@ -41,7 +41,25 @@ struct Queues {
   ShadowQueue shadow;
   uint32_t* counts;
   uint32_t capacity;
+  // The extension queues of bounces 1 and on in key order (origin cell,
+  // then direction octant): the shading pass writes each queued ray's key
+  // beside it (`keys`) and counts the keys per bin (`bins`: kSortBins
+  // counters, then kSortBlocks block totals); a scan and a scatter write
+  // the queue in key order to `sorted`, which the extension pass reads.
+  // Null `keys`: the queues keep their append order.
+  uint32_t* keys = nullptr;
+  uint32_t* sorted = nullptr;
+  uint32_t* bins = nullptr;
 };
+
+// The reordering key: kSortAxisBits per axis of the origin's cell in a grid
+// over the scene's box, interleaved (a Morton code), above the direction's
+// octant. The histogram is scanned in blocks of kSortScanBlock bins.
+constexpr uint32_t kSortAxisBits = 5;
+constexpr uint32_t kSortBins = 1u << (3 * kSortAxisBits + 3);
+constexpr uint32_t kSortScanBlock = 1024;
+constexpr uint32_t kSortBlocks = kSortBins / kSortScanBlock;
+constexpr uint32_t kSortBinWords = kSortBins + kSortBlocks;
 
 // The radiance cache's per-sample queues: queries (paths that end into the
 // cache at their second vertex) and training records, with their counts in
@@ -105,7 +123,7 @@ struct VisitCounters {
 
 // Optional per-sample instrumentation: events around each kernel (its
 // class in `kinds`: 0 camera, 1 extend, 2 shade, 3 shadow, 4 resolve,
-// 5 radiance cache) and
+// 5 radiance cache, 6 tail, 7 queue reordering) and
 // visit counting variants of the tracing kernels.
 struct SampleProfile {
   cudaEvent_t* events = nullptr;  // 2 per timed launch
@@ -125,13 +143,18 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
 // bounces 0 and 1 (its vertex is shaded in round 1).
 uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, uint32_t cache_bounce = 0);
 
-// The rounds a sample should run, from a sample's queue counts (the
-// wavefront kernels' per-bounce words, 3 per bounce) and its camera rays:
-// the first bounce whose queue held fewer than max(camera / 32, 65,536)
-// paths (the reference's round scheduler stops at camera / 16; the floor is
-// about the paths the tail kernel keeps resident at once), else every
-// bounce. Results do not depend on it; only the launch count does.
-uint32_t choose_wavefront_rounds(const uint32_t* counts, uint32_t camera, uint32_t max_bounces);
+// The rounds a sample (or wave) should run, from its queue counts (the
+// wavefront kernels' per-bounce words, 3 per bounce): the first bounce whose
+// queue held fewer paths than the extension kernel keeps resident on the
+// device at once (`resident`, at least 65,536), else every bounce. A round
+// over a queue that cannot fill the device once costs more than the tail
+// kernel's share of it (the reference's round scheduler stops at a
+// sixteenth of the camera rays instead). Results do not depend on it; only
+// the launch count does.
+uint32_t choose_wavefront_rounds(const uint32_t* counts, uint32_t resident, uint32_t max_bounces);
+
+// Threads of the extension kernel resident on the device at once.
+uint32_t extension_resident_threads();
 
 void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     uint32_t width, uint32_t height, uint32_t max_bounces, const PathState& P, const Queues& Q,

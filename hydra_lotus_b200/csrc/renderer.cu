@@ -613,7 +613,7 @@ constexpr uint32_t kMaxChain = 16;
 // Samples one wavefront holds (a wave) unless lotus_cuda_options says
 // otherwise, and the most it may: the path state and queues have room for
 // the renderer's wave size times the target's pixels.
-constexpr uint32_t kDefaultWave = 4;
+constexpr uint32_t kDefaultWave = 8;
 constexpr uint32_t kMaxWave = 8;
 
 // The resident scene as the incremental updates need it: each geometry's
@@ -688,6 +688,7 @@ struct Renderer {
   DeviceArray<uint4> path_hit;
   DeviceArray<uint32_t> queue_ray0, queue_ray1, queue_hit, counts;
   DeviceArray<float4> sq_o, sq_d, sq_fl, sq_thr;
+  DeviceArray<uint32_t> sort_keys, sort_queue, sort_bins;  // Queues::keys, sorted, bins
   // A second path state and queue set, for the second of two samples in
   // flight at once (RenderScene with two or more samples to add): its
   // rounds overlap the first one's tail, on a second stream.
@@ -695,6 +696,7 @@ struct Renderer {
   DeviceArray<uint4> path_hit2;
   DeviceArray<uint32_t> queue_ray02, queue_ray12, queue_hit2, counts2;
   DeviceArray<float4> sq_o2, sq_d2, sq_fl2, sq_thr2;
+  DeviceArray<uint32_t> sort_keys2, sort_queue2, sort_bins2;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<cudaEvent_t> ev_sample_done;  // per sample of a chain: resolved and counted
@@ -1455,10 +1457,12 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
     R.path_radiance.release(); R.path_hit.release();
     R.queue_ray0.release(); R.queue_ray1.release(); R.queue_hit.release();
     R.sq_o.release(); R.sq_d.release(); R.sq_fl.release(); R.sq_thr.release();
+    R.sort_keys.release(); R.sort_queue.release(); R.sort_bins.release();
     R.path_origin2.release(); R.path_direction2.release(); R.path_throughput2.release();
     R.path_radiance2.release(); R.path_hit2.release();
     R.queue_ray02.release(); R.queue_ray12.release(); R.queue_hit2.release();
     R.sq_o2.release(); R.sq_d2.release(); R.sq_fl2.release(); R.sq_thr2.release();
+    R.sort_keys2.release(); R.sort_queue2.release(); R.sort_bins2.release();
     R.width = w;
     R.height = h;
     R.key_valid = false;
@@ -1480,7 +1484,9 @@ bool ensure_targets(Renderer& R, uint32_t w, uint32_t h, bool wavefront, std::st
         !R.ok(R.queue_ray0.resize(w), "queues", detail) || !R.ok(R.queue_ray1.resize(w), "queues", detail) ||
         !R.ok(R.queue_hit.resize(w), "queues", detail) || !R.ok(R.sq_o.resize(w), "shadow queue", detail) ||
         !R.ok(R.sq_d.resize(w), "shadow queue", detail) || !R.ok(R.sq_fl.resize(w), "shadow queue", detail) ||
-        !R.ok(R.sq_thr.resize(w), "shadow queue", detail))
+        !R.ok(R.sq_thr.resize(w), "shadow queue", detail) || !R.ok(R.sort_keys.resize(w), "queue keys", detail) ||
+        !R.ok(R.sort_queue.resize(w), "queue keys", detail) ||
+        !R.ok(R.sort_bins.resize(kSortBinWords), "queue keys", detail))
       return false;
   }
   return true;
@@ -1495,6 +1501,8 @@ bool ensure_pair_buffers(Renderer& R, size_t n, std::string& detail) {
          R.ok(R.queue_hit2.resize(n), "queues", detail) && R.ok(R.sq_o2.resize(n), "shadow queue", detail) &&
          R.ok(R.sq_d2.resize(n), "shadow queue", detail) && R.ok(R.sq_fl2.resize(n), "shadow queue", detail) &&
          R.ok(R.sq_thr2.resize(n), "shadow queue", detail) &&
+         R.ok(R.sort_keys2.resize(n), "queue keys", detail) && R.ok(R.sort_queue2.resize(n), "queue keys", detail) &&
+         R.ok(R.sort_bins2.resize(kSortBinWords), "queue keys", detail) &&
          R.ok(R.counts2.resize(kQueueCounterWords * (LOTUS_MAX_BOUNCES + 2)), "queue counts", detail);
 }
 
@@ -1732,6 +1740,9 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   Q.shadow = ShadowQueue{R.sq_o.ptr, R.sq_d.ptr, R.sq_fl.ptr, R.sq_thr.ptr};
   Q.counts = R.counts.ptr;
   Q.capacity = t.width * t.height;
+  Q.keys = R.sort_keys.ptr;
+  Q.sorted = R.sort_queue.ptr;
+  Q.bins = R.sort_bins.ptr;
   const bool want_timings = (d.flags & LOTUS_FRAME_TIMINGS) != 0;
   const bool want_visits = (d.flags & LOTUS_FRAME_COUNT_VISITS) != 0;
   SampleProfile profile;
@@ -1800,6 +1811,9 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   Q2.hit = R.queue_hit2.ptr;
   Q2.shadow = ShadowQueue{R.sq_o2.ptr, R.sq_d2.ptr, R.sq_fl2.ptr, R.sq_thr2.ptr};
   Q2.counts = R.counts2.ptr;
+  Q2.keys = R.sort_keys2.ptr;
+  Q2.sorted = R.sort_queue2.ptr;
+  Q2.bins = R.sort_bins2.ptr;
   // A wave's queues hold both samples' paths.
   Queues QW = Q, QW2 = Q2;
   QW.capacity = QW2.capacity = wave * pixels;
@@ -1925,8 +1939,8 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     if (R.cache.error_flag(s) != 0) return poison("a radiance-cache kernel's tensor-core wait gave up");
   }
   if (want_timings) {
-    double by_kind[7] = {0, 0, 0, 0, 0, 0, 0};
-    uint32_t launches[7] = {0, 0, 0, 0, 0, 0, 0};
+    double by_kind[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t launches[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = 0; i < profile.count; ++i) {
       float kms = 0.0f;
       cudaEventElapsedTime(&kms, R.profile_events[2 * i], R.profile_events[2 * i + 1]);
@@ -1941,6 +1955,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     res.resolve_gpu_ms = by_kind[4];
     res.cache_gpu_ms = by_kind[5];
     res.tail_gpu_ms = by_kind[6];
+    res.sort_gpu_ms = by_kind[7];
     res.extend_launches = launches[1];
     res.shadow_launches = launches[3];
   }
@@ -1986,7 +2001,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     if (choose_rounds) {
       gk.rounds = 0;
       R.rounds_key = gk;
-      R.auto_rounds = choose_wavefront_rounds(counts.data(), rect[2] * rect[3] * last_wave, st.max_bounces);
+      R.auto_rounds = choose_wavefront_rounds(counts.data(), extension_resident_threads(), st.max_bounces);
     }
   }
   return LOTUS_PASS;
@@ -2617,6 +2632,9 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   Q.shadow = ShadowQueue{R.sq_o.ptr, R.sq_d.ptr, R.sq_fl.ptr, R.sq_thr.ptr};
   Q.counts = R.counts.ptr;
   Q.capacity = pixels;
+  Q.keys = R.sort_keys.ptr;
+  Q.sorted = R.sort_queue.ptr;
+  Q.bins = R.sort_bins.ptr;
   // The radiance cache serves the temporal frames' wavefront samples too.
   const bool use_cache = wavefront && R.cache_enabled && R.cache.ready();
   if (use_cache && !ensure_cache_queues(R, pixels, detail)) return poison(detail);
@@ -2663,7 +2681,7 @@ int32_t render_temporal(Renderer& R, const lotus_temporal_desc& td, lotus_frame_
   if (walks[0]) return poison(walk_failure_detail(walks, R.step_limit));
   if (choose_rounds) {
     R.temporal_rounds_key = rk;
-    R.temporal_auto_rounds = choose_wavefront_rounds(counts.data(), rect[2] * rect[3], st.max_bounces);
+    R.temporal_auto_rounds = choose_wavefront_rounds(counts.data(), extension_resident_threads(), st.max_bounces);
   }
   // A reservoir whose arithmetic failed (flag 2) fails the frame and the
   // renderer, as the reference's record readback does

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LOTUS_CUDA_ABI_VERSION 8u
+#define LOTUS_CUDA_ABI_VERSION 9u
 
 /* FrameStatus (vulkan_backend.hpp:23-27). */
 #define LOTUS_PASS 0
@@ -281,12 +281,17 @@ typedef struct lotus_frame_result {
    * queued after the wavefront_rounds rounds, each followed to its end). */
   double tail_gpu_ms;
   /* The samples the call's last wavefront held: a call that adds two or
-   * more samples (without the radiance cache) runs them in waves of four
-   * (two for a call of two or three) to a wavefront, and then the queue
-   * counts, the timings and the visit counts above are those of its last
-   * wave, its samples together. */
+   * more samples (without the radiance cache) runs them in waves of eight
+   * (lotus_cuda_options::samples_per_wave; halved while the call adds fewer)
+   * to a wavefront, and then the queue counts, the timings and the visit
+   * counts above are those of its last wave, its samples together. */
   uint32_t last_wave_samples;
   uint32_t reserved;
+  /* With LOTUS_FRAME_TIMINGS: the device time spent putting the extension
+   * queues of bounces 1 and on in key order (origin cell, direction
+   * octant) before their rounds; the shading pass that queues the rays
+   * writes their keys. */
+  double sort_gpu_ms;
   char detail[256];
 } lotus_frame_result;
 
@@ -304,8 +309,9 @@ typedef struct lotus_cuda_options {
    * takes the paths still queued (1..LOTUS_MAX_BOUNCES + 1). 0: RenderScene
    * chooses them from its first sample of each scene and frame shape (run
    * with LOTUS_WAVEFRONT_ROUNDS): the first bounce whose queue held fewer
-   * than max(camera rays / 32, 65536) paths; other calls use
-   * LOTUS_WAVEFRONT_ROUNDS. Results do not depend on it. */
+   * paths than the extension kernel keeps resident on the device at once
+   * (at least 65536); other calls use LOTUS_WAVEFRONT_ROUNDS. Results do not
+   * depend on it. */
   uint32_t wavefront_rounds;
   /* A BVH walk's step budget (node visits, leaf tests and instance entries);
    * 0: 2^18, which only a corrupt BVH could need. A walk that runs out of it,
@@ -315,7 +321,7 @@ typedef struct lotus_cuda_options {
   uint32_t traversal_step_limit;
   /* Samples a RenderScene call that adds several runs in one wavefront
    * (their paths side by side in one set of queues, so that each launch
-   * pays its ramp-up and drain once for all of them): 1, 2, 4 or 8; 0: 4.
+   * pays its ramp-up and drain once for all of them): 1, 2, 4 or 8; 0: 8.
    * The path state and queues take this many times the target's pixels.
    * Results do not depend on it. */
   uint32_t samples_per_wave;
