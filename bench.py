@@ -515,7 +515,10 @@ def batch_report(renderer_module, spp=8, depth=8):
     triangles log-uniform in [1e4, 2e6], 256^2 .. 1024^2 targets), 8 spp,
     depth 8, rendered as one wavefront per sample under a CUDA graph with
     the tuner's launch shape, against the same scenes rendered one after
-    another by one renderer. Device time only (CUDA events)."""
+    another by one renderer: with its samples in waves of eight (the
+    renderer's default: each scene's samples share a wavefront) and with one
+    sample per wavefront (no batching of scenes or samples). Device time
+    only (CUDA events)."""
     from hydra_lotus_b200 import autotune
     work = scenes.batch_workload(64, seed=0)
 
@@ -531,25 +534,29 @@ def batch_report(renderer_module, spp=8, depth=8):
             return {"error": [r.detail.decode() for r in res if r.status != abi.PASS][0]}
         frames = [s.frame(st(k), frame_count=spp, read_back=False) for k, s in enumerate(work)]
         best, times = autotune.tune_batch(batch, frames)
-        out["tuned"] = {"refill_below": best[0], "blocks_per_sm": best[1],
-                        "candidates_ms_per_sample": {f"{r}/{b}": round(t, 3) for (r, b), t in times.items()}}
+        out["tuned"] = {"knobs": dict(zip(autotune.KNOBS, best)),
+                        "candidates_ms_per_sample": {autotune.shape_name(s): round(t, 3) for s, t in times.items()}}
         frames = [s.frame(st(k, 7), frame_count=spp, read_back=False) for k, s in enumerate(work)]
         _, _, total = batch.render(frames)
         renderer_module.check(total, "batch")
         rays = total.camera_rays + total.extension_rays + total.shadow_rays
         out["batched"] = {"ms": round(total.gpu_ms, 2), "mrays_per_s": round(rays / total.gpu_ms / 1e3, 1),
                           "scene_samples_per_s": round(len(work) * spp / (total.gpu_ms * 1e-3), 1)}
-    seq_ms, seq_rays = 0.0, 0
-    with renderer_module.CudaOffscreenRenderer(0, trace_refill_below=best[0], trace_blocks_per_sm=best[1]) as r:
-        for k, s in enumerate(work):
-            renderer_module.check(r.update_scene(s), "update_scene")
-            f = s.frame(st(k, 7), frame_count=spp, read_back=False)
-            res, _ = r.render_scene(f)
-            renderer_module.check(res, "sequential")
-            seq_ms += res.gpu_ms
-            seq_rays += res.camera_rays + res.extension_rays + res.shadow_rays
-    out["sequential"] = {"ms": round(seq_ms, 2), "mrays_per_s": round(seq_rays / seq_ms / 1e3, 1)}
-    out["speedup_batched_vs_sequential"] = round(seq_ms / out["batched"]["ms"], 3)
+    for name, wave in (("sequential", 0), ("sequential_one_sample_per_wavefront", 1)):
+        seq_ms, seq_rays = 0.0, 0
+        with renderer_module.CudaOffscreenRenderer(0, trace_refill_below=best[0], trace_blocks_per_sm=best[1],
+                                                   samples_per_wave=wave) as r:
+            for k, s in enumerate(work):
+                renderer_module.check(r.update_scene(s), "update_scene")
+                f = s.frame(st(k, 7), frame_count=spp, read_back=False)
+                res, _ = r.render_scene(f)
+                renderer_module.check(res, name)
+                seq_ms += res.gpu_ms
+                seq_rays += res.camera_rays + res.extension_rays + res.shadow_rays
+        out[name] = {"ms": round(seq_ms, 2), "mrays_per_s": round(seq_rays / seq_ms / 1e3, 1)}
+    out["speedup_batched_vs_sequential"] = round(out["sequential"]["ms"] / out["batched"]["ms"], 3)
+    out["speedup_batched_vs_one_sample_per_wavefront"] = round(
+        out["sequential_one_sample_per_wavefront"]["ms"] / out["batched"]["ms"], 3)
     return out
 
 

@@ -38,6 +38,12 @@ SCENE_MATERIALS = 5
 SCENE_ENVIRONMENT = 6
 FRAME_DEPTH_KEEP = 8
 
+# lotus_cuda_batch_set_tuning's camera order.
+CAMERA_TILE_ROWS = 1
+CAMERA_TILE_4X8 = 2
+CAMERA_TILE_8X4 = 3
+CAMERA_TILE_16X2 = 4
+
 MOMENTS_FP32 = 0
 MOMENTS_FP16 = 1
 

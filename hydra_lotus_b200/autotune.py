@@ -1,37 +1,70 @@
-"""Launch-shape tuner for the persistent tracing kernels.
+"""Launch-shape tuner for the batched wavefront.
 
-Times a workload once per candidate launch shape — the refill threshold
-(how empty a warp gets before its idle lanes take new rays from the queue)
-and the resident blocks per SM — and returns the fastest, with every
-candidate's device time. The workload is a callable that renders with the
+Knobs (each 0 picks the library's default):
+  refill_below   how empty a warp of the persistent tracing kernels gets
+                 before its idle lanes take new rays from the queue;
+  blocks_per_sm  resident blocks of those kernels per SM (0: as many as fit);
+  rounds         the bounces run as wavefront rounds before the tail kernel
+                 takes the paths still queued (the queue size at which one
+                 thread per path beats a round; 0: chosen from the first
+                 sample's queue counts);
+  camera_tile    the camera pass's order within each scene: the image's
+                 rows, or warp tiles of 4x8, 8x4 or 16x2 pixels.
+
+The search is coordinate descent: starting from the defaults, each knob in
+turn is swept over its candidates with the others at their best so far,
+for `passes` passes. The workload is a callable that renders with the
 current shape and returns its device milliseconds; each candidate runs it
 `repeats` times after one untimed run (the first run of a shape captures
-its CUDA graph) and keeps the median.
+its CUDA graph) and keeps the median. Returns the best shape and every
+measured candidate's time.
 """
 
 import statistics
 
-REFILL = (16, 20, 24, 28)
-BLOCKS = (0, 4)
+from . import abi
+
+KNOBS = ("refill_below", "blocks_per_sm", "rounds", "camera_tile")
+CANDIDATES = {
+    "refill_below": (0, 16, 24, 28),
+    "blocks_per_sm": (0, 4, 5),
+    "rounds": (0, 5, 9),
+    "camera_tile": (abi.CAMERA_TILE_ROWS, abi.CAMERA_TILE_4X8, abi.CAMERA_TILE_8X4, abi.CAMERA_TILE_16X2),
+}
 
 
-def tune(apply, workload, refill=REFILL, blocks=BLOCKS, repeats=2):
-    """apply(refill_below, blocks_per_sm) sets a shape; workload() -> ms.
-    Returns ((refill_below, blocks_per_sm), {shape: ms})."""
+def shape_name(shape):
+    return "/".join(f"{k}={v}" for k, v in zip(KNOBS, shape))
+
+
+def tune(apply, workload, candidates=None, repeats=2, passes=1):
+    """apply(*shape) sets a shape (one value per KNOBS entry); workload() ->
+    ms. Returns (best shape, {shape: ms})."""
+    candidates = candidates or CANDIDATES
     times = {}
-    for r in refill:
-        for b in blocks:
-            apply(r, b)
+
+    def measure(shape):
+        if shape not in times:
+            apply(*shape)
             workload()
-            times[(r, b)] = statistics.median(workload() for _ in range(repeats))
-    best = min(times, key=times.get)
+            times[shape] = statistics.median(workload() for _ in range(repeats))
+        return times[shape]
+
+    best = tuple(candidates[k][0] for k in KNOBS)
+    measure(best)
+    for _ in range(passes):
+        for i, knob in enumerate(KNOBS):
+            for value in candidates[knob]:
+                shape = best[:i] + (value,) + best[i + 1:]
+                if measure(shape) < times[best]:
+                    best = shape
     apply(*best)
     return best, times
 
 
 def tune_batch(batch, frames, **kw):
     """Tunes a CudaBatch on one sample of `frames` (their frame_count is
-    replaced by 1)."""
+    replaced by 1, and depth kept): returns tune()'s result."""
     from . import renderer
     one = []
     for f in frames:
@@ -45,4 +78,7 @@ def tune_batch(batch, frames, **kw):
         renderer.check(total, "batch tuning sample")
         return total.gpu_ms
 
-    return tune(batch.set_tuning, workload, **kw)
+    def apply(refill_below, blocks_per_sm, rounds, camera_tile):
+        batch.set_tuning(refill_below, blocks_per_sm, rounds, camera_tile)
+
+    return tune(apply, workload, **kw)

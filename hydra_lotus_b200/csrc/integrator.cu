@@ -96,12 +96,21 @@ __device__ __forceinline__ uint32_t spread_bits3(uint32_t v) {
   return v;
 }
 
+// A batch's keys lead with the scene, and its cells are coarser: six bits
+// of scene (LOTUS_BATCH_MAX_SCENES), three per axis, then the octant.
+constexpr uint32_t kBatchSortAxisBits = 3;
+static_assert(LOTUS_BATCH_MAX_SCENES <= (1u << (3 * (kSortAxisBits - kBatchSortAxisBits))),
+    "a batch's scene index fits above its cells");
+
+template <uint32_t kAxisBits>
 __device__ __forceinline__ uint32_t sort_key(const SortGrid& g, const F3& o, const F3& d) {
   const float p[3] = {o.x, o.y, o.z};
-  constexpr uint32_t top = (1u << kSortAxisBits) - 1u;
+  constexpr uint32_t top = (1u << kAxisBits) - 1u;
+  // The grid's scale is for kSortAxisBits cells per axis.
+  constexpr float coarse = 1.0f / (float)(1u << (kSortAxisBits - kAxisBits));
   uint32_t cell[3];
   for (int a = 0; a < 3; ++a) {
-    const float v = (p[a] - g.lo[a]) * g.scale[a];
+    const float v = (p[a] - g.lo[a]) * g.scale[a] * coarse;
     cell[a] = v > 0.0f ? (v < (float)top ? (uint32_t)v : top) : 0u;
   }
   const uint32_t morton = spread_bits3(cell[0]) | (spread_bits3(cell[1]) << 1) | (spread_bits3(cell[2]) << 2);
@@ -418,7 +427,8 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
 // Camera (wavefront.slang:206-225): starts each pixel's path and traces its
 // camera ray; a hit is queued for shading at bounce 0.
 // In a batch (kBatch) one thread per path slot of every scene, in each
-// image's row order; otherwise 8x4 pixel tiles per warp.
+// image's row order or in the table's warp tiles; otherwise 8x4 pixel
+// tiles per warp.
 template <bool kCount, bool kBatch>
 __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, VisitCounters* visits, SceneTable B) {
@@ -430,11 +440,19 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
     slot = index;
     valid = index < B.total_slots;
     if (valid) {
-      scene = table_scene(B, slot);
+      scene = table_scene(B, index);
       const FrameConst& fb = B.frames[scene];
-      const uint32_t local = slot - B.slot_base[scene];
-      px = local % fb.width;
-      py = local / fb.width;
+      const uint32_t local = index - B.slot_base[scene];
+      if (B.camera_tile) {
+        const uint32_t k = B.camera_tile;
+        const uint32_t tiles_x = fb.width >> k, tile = local >> 5, lane = local & 31u;
+        px = ((tile % tiles_x) << k) + (lane & ((1u << k) - 1u));
+        py = (tile / tiles_x) * (32u >> k) + (lane >> k);
+        slot = B.slot_base[scene] + py * fb.width + px;
+      } else {
+        px = local % fb.width;
+        py = local / fb.width;
+      }
       valid = fb.add_sample && frame_rect_contains(fb, px, py);
     }
   } else {
@@ -502,10 +520,14 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 1];
   const bool cache_vertex = kCacheVertex && bounce < fcp->max_bounces;
-  const bool keyed = !kBatch && Q.keys != nullptr;
-  __shared__ SortGrid grid;
+  const bool keyed = Q.keys != nullptr;
+  __shared__ SortGrid grids[kBatch ? LOTUS_BATCH_MAX_SCENES : 1];
   if (keyed) {
-    if (threadIdx.x == 0) grid = sort_grid(S);
+    if (kBatch) {
+      for (uint32_t k = threadIdx.x; k < B.count; k += blockDim.x) grids[k] = sort_grid(B.views[k]);
+    } else if (threadIdx.x == 0) {
+      grids[0] = sort_grid(S);
+    }
     __syncthreads();
   }
   // Grid-stride over the hit queue (the grid is sized to a few waves of
@@ -549,7 +571,10 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
           cache_vertex && !training);
       query = cache_vertex && !training;
       if (cont) {
-        if (keyed) key = sort_key(grid, no, nd);
+        if (keyed && kBatch)
+          key = (scene << (3 * kBatchSortAxisBits + 3)) | sort_key<kBatchSortAxisBits>(grids[scene], no, nd);
+        else if (keyed)
+          key = sort_key<kSortAxisBits>(grids[0], no, nd);
         P.origin[slot] = F4(no, 0.0f);
         P.direction[slot] = F4(nd, kFloatMax);
         P.throughput[slot] = F4(T, (flags & kUnweightedLight) ? -1.0f : last_pdf);
@@ -1373,17 +1398,29 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
       8u * persistent_grid((const void*)k_wf_shade<false, true, false>, Q.capacity, TraceTuning()));
   k_wf_camera<false, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
   const uint32_t rounds = wavefront_rounds(max_bounces, false, tuning.rounds);
+  const bool keyed = Q.keys != nullptr && Q.sorted != nullptr && Q.bins != nullptr;
+  const uint32_t grid_scatter = persistent_grid((const void*)k_sort_scatter, Q.capacity, TraceTuning());
   for (uint32_t b = 0; b < rounds; ++b) {
+    const uint32_t* rays = Q.ray[b & 1];
+    if (b != 0 && keyed) {
+      k_sort_scan<<<kSortBlocks, kSortScanBlock, 0, stream>>>(Q.bins);
+      k_sort_scatter<<<grid_scatter, kSortScatterBlock, 0, stream>>>(Q.ray[b & 1], Q.keys, Q.counts + 3 * b, Q.bins,
+          Q.sorted);
+      rays = Q.sorted;
+    }
     if (b != 0 && B.analytic)
-      k_wf_extend<false, true, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, Q.ray[b & 1], b,
+      k_wf_extend<false, true, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rays, b,
           fetch + 2 * b, refill, nullptr, B);
     else if (b != 0)
-      k_wf_extend<false, true, false><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, Q.ray[b & 1], b,
+      k_wf_extend<false, true, false><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rays, b,
           fetch + 2 * b, refill, nullptr, B);
+    Queues QS = Q;
+    if (keyed && b + 1 < rounds) cudaMemsetAsync(Q.bins, 0, sizeof(uint32_t) * kSortBins, stream);
+    else QS.keys = nullptr;
     if (B.analytic)
-      k_wf_shade<false, true, true><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, Q, b, no_cache, B);
+      k_wf_shade<false, true, true><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, QS, b, no_cache, B);
     else
-      k_wf_shade<false, true, false><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, Q, b, no_cache, B);
+      k_wf_shade<false, true, false><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, QS, b, no_cache, B);
     k_wf_shadow<false, true><<<grid_shadow, kBlock, 0, stream>>>(none_view, P, Q, b, fetch + 2 * b + 1, refill,
         nullptr, B);
   }

@@ -93,6 +93,10 @@ struct SceneTable {
   uint32_t count = 0;
   uint32_t total_slots = 0;
   bool analytic = false;  // some scene has analytic lights
+  // The camera pass's order within each scene: 0, each image's rows; k,
+  // warp tiles 2^k pixels wide and 32 / 2^k high (every scene's size a
+  // multiple of the tile).
+  uint32_t camera_tile = 0;
 };
 
 // Launch shape of the persistent tracing kernels: a lane takes a new ray
@@ -102,6 +106,7 @@ struct TraceTuning {
   uint32_t refill_below = 0;
   uint32_t blocks_per_sm = 0;  // 0: as many as fit
   uint32_t rounds = 0;         // wavefront rounds before the tail; 0: the default
+  uint32_t camera_tile = 0;    // a batch's camera order (LOTUS_CAMERA_TILE_*); 0: the default
 };
 
 // Ray totals over a RenderScene call.

@@ -96,7 +96,7 @@ def lib():
         L.lotus_cuda_batch_set_scenes.argtypes = [C.c_void_p, C.POINTER(abi.SceneDesc), C.c_uint32,
                                                   C.POINTER(abi.SceneResult)]
         L.lotus_cuda_batch_set_tuning.restype = C.c_int32
-        L.lotus_cuda_batch_set_tuning.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+        L.lotus_cuda_batch_set_tuning.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
         L.lotus_cuda_batch_render.restype = C.c_int32
         L.lotus_cuda_batch_render.argtypes = [C.c_void_p, C.POINTER(abi.FrameDesc), C.c_uint32,
                                               C.POINTER(abi.FrameResult), C.POINTER(C.c_void_p),
@@ -393,8 +393,11 @@ class CudaBatch:
         lib().lotus_cuda_batch_set_scenes(self.handle, descs, len(self.scenes), results)
         return list(results)
 
-    def set_tuning(self, refill_below=0, blocks_per_sm=0):
-        rc = lib().lotus_cuda_batch_set_tuning(self.handle, refill_below, blocks_per_sm)
+    def set_tuning(self, refill_below=0, blocks_per_sm=0, wavefront_rounds=0, camera_tile=0):
+        """The batch's launch shape (lotus_cuda_batch_set_tuning; 0: each
+        default); camera_tile is one of abi.CAMERA_TILE_*."""
+        rc = lib().lotus_cuda_batch_set_tuning(self.handle, refill_below, blocks_per_sm, wavefront_rounds,
+                                               camera_tile)
         if rc != abi.PASS:
             raise RendererError(rc, "batch tuning")
 

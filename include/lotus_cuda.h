@@ -565,10 +565,20 @@ void lotus_cuda_batch_destroy(lotus_cuda_batch* batch);
 int32_t lotus_cuda_batch_set_scenes(lotus_cuda_batch* batch,
     const lotus_scene_desc* scenes, uint32_t count, lotus_scene_result* results);
 
-/* The persistent kernels' launch shape (as lotus_cuda_options' trace_*
- * fields; 0 picks the default), for a tuner. */
+/* The batch's launch shape, for a tuner (0 picks each default): the
+ * persistent kernels' refill threshold and blocks per SM (as
+ * lotus_cuda_options' trace_* fields), the wavefront rounds before the tail
+ * kernel (as lotus_cuda_options::wavefront_rounds), and the camera pass's
+ * order within each scene: LOTUS_CAMERA_TILE_ROWS (the image's rows) or
+ * warp tiles of 4x8, 8x4 or 16x2 pixels (where every scene's size is a
+ * multiple of the tile; rows otherwise). Results do not depend on any of
+ * them. */
+#define LOTUS_CAMERA_TILE_ROWS 1u
+#define LOTUS_CAMERA_TILE_4X8 2u
+#define LOTUS_CAMERA_TILE_8X4 3u
+#define LOTUS_CAMERA_TILE_16X2 4u
 int32_t lotus_cuda_batch_set_tuning(lotus_cuda_batch* batch,
-    uint32_t trace_refill_below, uint32_t trace_blocks_per_sm);
+    uint32_t trace_refill_below, uint32_t trace_blocks_per_sm, uint32_t wavefront_rounds, uint32_t camera_tile);
 
 /* frames[k] renders scene k (count = the batch's scene count, every
  * frame_count equal). A scene's accumulation continues while its frame

@@ -1,6 +1,7 @@
 """GPU: a batch of scenes rendered as one wavefront gives every scene the
 image lotus_cuda_render gives it alone, bit for bit, over two calls that
-continue the accumulation."""
+continue the accumulation, whatever the tuner's launch shape (refill,
+blocks per SM, rounds before the tail, camera order)."""
 
 import numpy as np
 import pytest
@@ -25,9 +26,19 @@ def settings(k, sample_index):
                                 max_bounces=6 if k != 1 else 8, sample_index=sample_index)
 
 
-def test_batch_matches_single_renders(cuda):
+TUNINGS = [
+    (0, 0, 0, 0),
+    (24, 4, 5, abi.CAMERA_TILE_8X4),
+    (0, 0, 9, abi.CAMERA_TILE_4X8),
+    (16, 0, 3, abi.CAMERA_TILE_16X2),  # 16x2 does not divide 40: rows
+]
+
+
+@pytest.mark.parametrize("tuning", TUNINGS, ids=lambda t: "/".join(map(str, t)))
+def test_batch_matches_single_renders(cuda, tuning):
     scs = batch_scenes()
     with cuda.CudaBatch(0) as batch:
+        batch.set_tuning(*tuning)
         res = batch.set_scenes(scs)
         assert all(r.status == abi.PASS for r in res), [r.detail for r in res]
         frames = [s.frame(settings(k, 100 + k), frame_count=2) for k, s in enumerate(scs)]
