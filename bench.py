@@ -480,6 +480,55 @@ def temporal_report(renderer_module, frames=120, checked=(0, 30, 60, 90, 119), r
     return out
 
 
+# Tensor-core work the radiance cache's kernels issue per record: the
+# forward pass is five 64x64 layers and one 64x16 (three outputs padded to
+# 16) = 21,504 multiply-adds; training adds the input gradients and the
+# weight gradients of every layer, twice that again.
+CACHE_INFER_FLOPS = 2 * 21504
+CACHE_TRAIN_FLOPS = 3 * 2 * 21504
+
+
+def cache_kernels_report(renderer_module, samples=16, warmup=8):
+    """The radiance cache's kernels on the config-5 scene's 1080p frame
+    (scenes.box_room_wide, wavefront PT, depth 8, paths ending into the
+    cache at their second vertex, one path in 32 training): per sample, the
+    device time of inference (its spatial query sort included) and of
+    training (targets, the training pass, Adam), the records each handled,
+    and the tensor-core work they issued per second as a fraction of the
+    measured sustained BF16 GEMM rate."""
+    peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    peak, kind = 1400.0, "fallback"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peak, kind = float(json.load(f)["bf16_tflops_sustained"]), "measured sustained"
+    scene = scenes.box_room_wide(seed=0, width=WIDTH, height=HEIGHT)
+    infer, train, queries, records = [], [], [], []
+    with renderer_module.CudaOffscreenRenderer(0) as r:
+        renderer_module.check(r.update_scene(scene), "update_scene")
+        r.configure_cache(enable=True, seed=1)
+        for k in range(warmup + samples):
+            st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                                      max_bounces=DEPTH, sample_index=k)
+            res, _ = r.render_scene(scene.frame(st, 1, read_back=False, flags=abi.FRAME_TIMINGS))
+            renderer_module.check(res, "cache frame")
+            if k >= warmup:
+                infer.append(res.cache_infer_gpu_ms)
+                train.append(res.cache_train_gpu_ms)
+                queries.append(res.cache_queries)
+                records.append(res.cache_training_records)
+    i_ms, t_ms = statistics.median(infer), statistics.median(train)
+    q, n = statistics.median(queries), statistics.median(records)
+    i_tf = q * CACHE_INFER_FLOPS / (i_ms * 1e-3) / 1e12
+    t_tf = n * CACHE_TRAIN_FLOPS / (t_ms * 1e-3) / 1e12
+    return {"workload": f"box room, {WIDTH}x{HEIGHT}, 1 spp per sample, depth {DEPTH}, cache at the second vertex",
+            "infer_ms_per_sample": round(i_ms, 4), "queries_per_sample": int(q),
+            "train_ms_per_sample": round(t_ms, 4), "training_records_per_sample": int(n),
+            "infer_tflops": round(i_tf, 1), "infer_frac": round(i_tf / peak, 4),
+            "train_tflops": round(t_tf, 1), "train_frac": round(t_tf / peak, 4),
+            "peak_tflops": peak, "peak_kind": kind,
+            "flops_per_record": {"infer": CACHE_INFER_FLOPS, "train": CACHE_TRAIN_FLOPS}}
+
+
 def analytic_lights_report(renderer_module, frames=64, warmup=8):
     """Analytic lights on the shape of the reference's many-lights-v1
     workload (scenes.light_grid: the box room under a grid of sphere
@@ -756,6 +805,7 @@ def main():
             line["scene_updates"] = scene_update_report(renderer)
         if args.temporal:
             line["temporal"] = temporal_report(renderer)
+            line["cache_kernels"] = cache_kernels_report(renderer)
         if args.lights:
             line["analytic_lights"] = analytic_lights_report(renderer)
         # Last, so that a reader of the line's tail sees it.

@@ -228,6 +228,8 @@ class FrameResult(C.Structure):
         ("last_wave_samples", C.c_uint32),
         ("reserved", C.c_uint32),
         ("sort_gpu_ms", C.c_double),
+        ("cache_infer_gpu_ms", C.c_double),
+        ("cache_train_gpu_ms", C.c_double),
         ("detail", C.c_char * 256),
     ]
 

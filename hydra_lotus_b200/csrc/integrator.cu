@@ -589,6 +589,20 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
         C.queries[q_at] = features;
         C.query_slots[q_at] = slot;
         C.query_throughput[q_at] = F4(T_in, 0.0f);
+        if (C.query_keys != nullptr) {
+          const float p[3] = {features.pos_rough.x, features.pos_rough.y, features.pos_rough.z};
+          constexpr uint32_t top = (1u << kQuerySortAxisBits) - 1u;
+          uint32_t cell[3];
+          for (int a = 0; a < 3; ++a) {
+            const float v = (p[a] - C.grid_lo[a]) * C.grid_scale[a];
+            cell[a] = v > 0.0f ? (v < (float)top ? (uint32_t)v : top) : 0u;
+          }
+          const uint32_t key = spread_bits3(cell[0]) | (spread_bits3(cell[1]) << 1) | (spread_bits3(cell[2]) << 2);
+          C.query_keys[q_at] = key;
+          const unsigned peers = __match_any_sync(__activemask(), key);
+          if ((threadIdx.x & 31u) == (unsigned)(__ffs(peers) - 1))
+            atomicAdd(&C.query_bins[key], (uint32_t)__popc(peers));
+        }
       }
       const uint32_t t_at = warp_append(&C.counters[1], training);
       if (training && t_at < C.train_capacity) {
@@ -1014,11 +1028,13 @@ __global__ void __launch_bounds__(kSortScanBlock) k_sort_scan(uint32_t* __restri
 }
 
 // The queue in key order: each block first scans the block totals; a
-// warp's rays of one key take consecutive places from one atomic.
+// warp's entries of one key take consecutive places from one atomic. The
+// entries are `rays[i]`, or the indices i themselves where `rays` is null,
+// for i below min(*count, cap).
 constexpr int kSortScatterBlock = 256;
 static_assert(kSortBlocks == kSortScatterBlock, "one scatter thread per histogram block");
 __global__ void __launch_bounds__(kSortScatterBlock) k_sort_scatter(const uint32_t* __restrict__ rays,
-    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ count, uint32_t* __restrict__ bins,
+    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ count, uint32_t cap, uint32_t* __restrict__ bins,
     uint32_t* __restrict__ sorted) {
   __shared__ uint32_t block_base[kSortBlocks];
   __shared__ uint32_t warp_total[kSortScatterBlock / 32];
@@ -1035,7 +1051,7 @@ __global__ void __launch_bounds__(kSortScatterBlock) k_sort_scatter(const uint32
   for (unsigned w = 0; w < warp; ++w) before += warp_total[w];
   block_base[threadIdx.x] = before + x - v;
   __syncthreads();
-  const uint32_t n = *count;
+  const uint32_t n = min(*count, cap);
   for (uint32_t i = blockIdx.x * kSortScatterBlock + threadIdx.x; i < n; i += gridDim.x * kSortScatterBlock) {
     const uint32_t key = keys[i];
     const unsigned peers = __match_any_sync(__activemask(), key);
@@ -1043,7 +1059,7 @@ __global__ void __launch_bounds__(kSortScatterBlock) k_sort_scatter(const uint32
     uint32_t base = 0;
     if ((int)lane == leader) base = atomicAdd(&bins[key], (uint32_t)__popc(peers)) + block_base[key / kSortScanBlock];
     base = __shfl_sync(peers, base, leader);
-    sorted[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = rays[i];
+    sorted[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = rays != nullptr ? rays[i] : i;
   }
 }
 
@@ -1263,8 +1279,8 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     if (b != 0 && keyed) {
       Timed t(profile, stream, 7);
       k_sort_scan<<<kSortBlocks, kSortScanBlock, 0, stream>>>(Q.bins);
-      k_sort_scatter<<<grid_scatter, kSortScatterBlock, 0, stream>>>(Q.ray[b & 1], Q.keys, Q.counts + 3 * b, Q.bins,
-          Q.sorted);
+      k_sort_scatter<<<grid_scatter, kSortScatterBlock, 0, stream>>>(Q.ray[b & 1], Q.keys, Q.counts + 3 * b, Q.capacity,
+          Q.bins, Q.sorted);
       rays = Q.sorted;
     }
     if (b != 0) {
@@ -1287,8 +1303,10 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
       Queues QS = Q;
       if (keyed && b + 1 < rounds) cudaMemsetAsync(Q.bins, 0, sizeof(uint32_t) * kSortBins, stream);
       else QS.keys = nullptr;
-      Timed t(profile, stream, 2);
       const bool cache_vertex = C.enabled && b == C.bounce;
+      if (cache_vertex && C.query_keys != nullptr)
+        cudaMemsetAsync(C.query_bins, 0, sizeof(uint32_t) * kSortBins, stream);
+      Timed t(profile, stream, 2);
       if (cache_vertex && analytic)
         k_wf_shade<true, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, QS, b, C, none);
       else if (cache_vertex)
@@ -1319,9 +1337,20 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   if (C.enabled) {
     // The paths that ended into the cache receive its answer; then the
     // training paths' targets train it.
-    Timed t(profile, stream, 5);
-    launch_cache_infer_records(C.cache->net(), C.cache->grid(), C.queries, C.query_slots, C.query_throughput,
-        P.radiance, &C.counters[0], C.query_capacity, stream);
+    {
+      Timed t(profile, stream, 5);
+      const uint32_t* order = nullptr;
+      if (C.query_keys != nullptr) {
+        k_sort_scan<<<kSortBlocks, kSortScanBlock, 0, stream>>>(C.query_bins);
+        k_sort_scatter<<<persistent_grid((const void*)k_sort_scatter, C.query_capacity, TraceTuning()),
+            kSortScatterBlock, 0, stream>>>(nullptr, C.query_keys, &C.counters[0], C.query_capacity, C.query_bins,
+            C.query_order);
+        order = C.query_order;
+      }
+      launch_cache_infer_records(C.cache->net(), C.cache->grid(), C.queries, C.query_slots, C.query_throughput,
+          P.radiance, &C.counters[0], C.query_capacity, stream, order);
+    }
+    Timed t(profile, stream, 8);
     k_cache_targets<<<(C.train_capacity + kBlock - 1) / kBlock, kBlock, 0, stream>>>(C, P);
     for (uint32_t k = 0; k < C.steps; ++k) {
       launch_cache_train_records(C.cache->net(), C.cache->grid(), C.train, C.train_targets, &C.counters[1],
@@ -1404,8 +1433,8 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
     const uint32_t* rays = Q.ray[b & 1];
     if (b != 0 && keyed) {
       k_sort_scan<<<kSortBlocks, kSortScanBlock, 0, stream>>>(Q.bins);
-      k_sort_scatter<<<grid_scatter, kSortScatterBlock, 0, stream>>>(Q.ray[b & 1], Q.keys, Q.counts + 3 * b, Q.bins,
-          Q.sorted);
+      k_sort_scatter<<<grid_scatter, kSortScatterBlock, 0, stream>>>(Q.ray[b & 1], Q.keys, Q.counts + 3 * b, Q.capacity,
+          Q.bins, Q.sorted);
       rays = Q.sorted;
     }
     if (b != 0 && B.analytic)

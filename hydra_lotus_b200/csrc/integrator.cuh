@@ -81,7 +81,21 @@ struct CacheQueues {
   float4* train_targets = nullptr;
   uint32_t train_capacity = 0;
   uint32_t* counters = nullptr;
+  // The queries in spatial order: the shading pass writes each query's key
+  // (its position's cell, kQuerySortAxisBits per axis over the cache's
+  // grid box, interleaved) and counts the keys per bin; a scan and a
+  // scatter write the queries' indices in key order to `query_order`, and
+  // inference takes its queries in that order, so that neighbouring
+  // threads gather neighbouring hash-grid entries. Null keys: append order.
+  uint32_t* query_keys = nullptr;
+  uint32_t* query_order = nullptr;
+  uint32_t* query_bins = nullptr;  // kSortBinWords
+  float grid_lo[3] = {0.0f, 0.0f, 0.0f};
+  float grid_scale[3] = {0.0f, 0.0f, 0.0f};  // cells per unit length
 };
+
+constexpr uint32_t kQuerySortAxisBits = 6;
+static_assert((1u << (3 * kQuerySortAxisBits)) == kSortBins, "query keys fill the histogram");
 
 // Several scenes rendered as one wavefront: scene k owns the path slots
 // [slot_base[k], slot_base[k + 1]), in its image's row order, with its own
@@ -128,7 +142,8 @@ struct VisitCounters {
 
 // Optional per-sample instrumentation: events around each kernel (its
 // class in `kinds`: 0 camera, 1 extend, 2 shade, 3 shadow, 4 resolve,
-// 5 radiance cache, 6 tail, 7 queue reordering) and
+// 5 radiance-cache inference, 6 tail, 7 queue reordering, 8 radiance-cache
+// training) and
 // visit counting variants of the tracing kernels.
 struct SampleProfile {
   cudaEvent_t* events = nullptr;  // 2 per timed launch

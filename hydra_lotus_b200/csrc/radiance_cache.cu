@@ -232,6 +232,9 @@ struct NetIO {
   const uint32_t* slots;
   const float4* throughput;
   float4* radiance;
+  // Records: the order to take them in (record order[q] for query q), or
+  // null for their own order.
+  const uint32_t* order;
   // Count: *count when non-null, else n; clamped to capacity.
   const uint32_t* count;
   uint32_t n;
@@ -427,7 +430,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_cache_infer(CacheNet net, 
       load_input<kIO>(io, grid, q, n, x, rec);
       store_row64(A, row, x);
     } else if (q < n) {
-      encode_record_to_tile(grid, io.records[q], A, row);
+      encode_record_to_tile(grid, io.records[io.order ? io.order[q] : q], A, row);
     } else {
 #pragma unroll
       for (int c = 0; c < 8; ++c)
@@ -466,8 +469,9 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_cache_infer(CacheNet net, 
     } else {
       // The query's path ends here: its throughput times the cached
       // radiance (clamped at zero) joins the path's radiance.
-      const uint32_t slot = io.slots[q];
-      const float4 t = io.throughput[q];
+      const uint32_t record = io.order ? io.order[q] : q;
+      const uint32_t slot = io.slots[record];
+      const float4 t = io.throughput[record];
       float4 r = io.radiance[slot];
       r.x += t.x * fmaxf(y[0], 0.0f);
       r.y += t.y * fmaxf(y[1], 0.0f);
@@ -793,7 +797,7 @@ uint32_t sm_count() {
 
 cudaError_t launch_cache_infer_records(const CacheNet& net, const CacheGrid& grid, const CacheRecord* records,
     const uint32_t* slots, const float4* throughput, float4* radiance, const uint32_t* count, uint32_t capacity,
-    cudaStream_t s) {
+    cudaStream_t s, const uint32_t* order) {
   static bool configured = false;
   if (!configured) {
     cudaError_t e = allow_smem(k_cache_infer<kRecordIO>, kInferSmem);
@@ -805,6 +809,7 @@ cudaError_t launch_cache_infer_records(const CacheNet& net, const CacheGrid& gri
   io.slots = slots;
   io.throughput = throughput;
   io.radiance = radiance;
+  io.order = order;
   io.count = count;
   io.capacity = capacity;
   const uint32_t grid_size = std::min(sm_count(), std::max(1u, (capacity + 127) / 128 / kInferGroups + 1));

@@ -71,7 +71,7 @@ struct CacheConfig {
 
 cudaError_t launch_cache_infer_records(const CacheNet& net, const CacheGrid& grid, const CacheRecord* records,
     const uint32_t* slots, const float4* throughput, float4* radiance, const uint32_t* count, uint32_t capacity,
-    cudaStream_t s);
+    cudaStream_t s, const uint32_t* order = nullptr);
 cudaError_t launch_cache_train_records(const CacheNet& net, const CacheGrid& grid, const CacheRecord* records,
     const float4* targets, const uint32_t* count, uint32_t capacity, cudaStream_t s);
 

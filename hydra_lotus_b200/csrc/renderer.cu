@@ -689,6 +689,7 @@ struct Renderer {
   DeviceArray<uint32_t> queue_ray0, queue_ray1, queue_hit, counts;
   DeviceArray<float4> sq_o, sq_d, sq_fl, sq_thr;
   DeviceArray<uint32_t> sort_keys, sort_queue, sort_bins;  // Queues::keys, sorted, bins
+  DeviceArray<uint32_t> cache_query_keys, cache_query_order, cache_query_bins;  // CacheQueues::query_*
   // A second path state and queue set, for the second of two samples in
   // flight at once (RenderScene with two or more samples to add): its
   // rounds overlap the first one's tail, on a second stream.
@@ -1517,6 +1518,9 @@ bool ensure_cache_queues(Renderer& R, uint32_t pixels, std::string& detail) {
   if (!R.ok(R.cache_queries.resize(pixels), "cache queries", detail) ||
       !R.ok(R.cache_query_slots.resize(pixels), "cache queries", detail) ||
       !R.ok(R.cache_query_throughput.resize(pixels), "cache queries", detail) ||
+      !R.ok(R.cache_query_keys.resize(pixels), "cache queries", detail) ||
+      !R.ok(R.cache_query_order.resize(pixels), "cache queries", detail) ||
+      !R.ok(R.cache_query_bins.resize(kSortBinWords), "cache queries", detail) ||
       !R.ok(R.cache_train.resize(train), "cache training records", detail) ||
       !R.ok(R.cache_train_slots.resize(train), "cache training records", detail) ||
       !R.ok(R.cache_train_base.resize(train), "cache training records", detail) ||
@@ -1539,6 +1543,16 @@ CacheQueues cache_queues(Renderer& R) {
   C.queries = R.cache_queries.ptr;
   C.query_slots = R.cache_query_slots.ptr;
   C.query_throughput = R.cache_query_throughput.ptr;
+  C.query_keys = R.cache_query_keys.ptr;
+  C.query_order = R.cache_query_order.ptr;
+  C.query_bins = R.cache_query_bins.ptr;
+  {
+    const CacheGrid g = R.cache.grid();
+    for (int a = 0; a < 3; ++a) {
+      C.grid_lo[a] = g.lo[a];
+      C.grid_scale[a] = g.inv_extent[a] * (float)(1u << kQuerySortAxisBits);
+    }
+  }
   C.query_capacity = (uint32_t)R.cache_queries.count;
   C.train = R.cache_train.ptr;
   C.train_slots = R.cache_train_slots.ptr;
@@ -1939,8 +1953,8 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     if (R.cache.error_flag(s) != 0) return poison("a radiance-cache kernel's tensor-core wait gave up");
   }
   if (want_timings) {
-    double by_kind[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    uint32_t launches[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double by_kind[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t launches[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = 0; i < profile.count; ++i) {
       float kms = 0.0f;
       cudaEventElapsedTime(&kms, R.profile_events[2 * i], R.profile_events[2 * i + 1]);
@@ -1953,7 +1967,9 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     res.shade_gpu_ms = by_kind[2];
     res.shadow_gpu_ms = by_kind[3];
     res.resolve_gpu_ms = by_kind[4];
-    res.cache_gpu_ms = by_kind[5];
+    res.cache_gpu_ms = by_kind[5] + by_kind[8];
+    res.cache_infer_gpu_ms = by_kind[5];
+    res.cache_train_gpu_ms = by_kind[8];
     res.tail_gpu_ms = by_kind[6];
     res.sort_gpu_ms = by_kind[7];
     res.extend_launches = launches[1];

@@ -292,6 +292,11 @@ typedef struct lotus_frame_result {
    * octant) before their rounds; the shading pass that queues the rays
    * writes their keys. */
   double sort_gpu_ms;
+  /* With LOTUS_FRAME_TIMINGS and the radiance cache: cache_gpu_ms split
+   * into inference (the queries put in spatial order, then the network's
+   * forward pass) and training (targets, training passes, Adam). */
+  double cache_infer_gpu_ms;
+  double cache_train_gpu_ms;
   char detail[256];
 } lotus_frame_result;
 

@@ -172,3 +172,20 @@ def test_later_cache_vertex_shrinks_bias(cuda):
     print(out)
     assert 0 < out[2][0] < out[1][0]
     assert out[2][1] < out[1][1]
+
+
+def test_cache_timings_split(cuda):
+    """With LOTUS_FRAME_TIMINGS the cache's device time is reported split
+    into inference (its spatial query sort included) and training."""
+    from hydra_lotus_b200 import abi
+    scene = scenes.box_room(seed=0, size=64)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=6, sample_index=0)
+    with cuda.CudaOffscreenRenderer(0) as r:
+        cuda.check(r.update_scene(scene), "update_scene")
+        r.configure_cache(enable=True, seed=1)
+        res, _ = r.render_scene(scene.frame(st, frame_count=1, read_back=False, flags=abi.FRAME_TIMINGS))
+        cuda.check(res, "cache frame")
+    assert res.cache_queries > 0 and res.cache_training_records > 0
+    assert res.cache_infer_gpu_ms > 0.0 and res.cache_train_gpu_ms > 0.0
+    assert abs(res.cache_infer_gpu_ms + res.cache_train_gpu_ms - res.cache_gpu_ms) < 1e-9
