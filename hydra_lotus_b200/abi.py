@@ -47,6 +47,23 @@ CAMERA_TILE_16X2 = 4
 MOMENTS_FP32 = 0
 MOMENTS_FP16 = 1
 
+# Texture lookups (lotus_texture, lotus_texture_input, lotus_material::lookups).
+TEXTURE_RGBA8_UNORM = 0
+TEXTURE_RGBA8_SRGB = 1
+TEXTURE_RGBA32_FLOAT = 2
+WRAP_BLACK = 0
+WRAP_CLAMP = 1
+WRAP_REPEAT = 2
+WRAP_MIRROR = 3
+SLOT_OPACITY = 0
+SLOT_NORMAL = 1
+SLOT_BASE_COLOR = 2
+SLOT_ROUGHNESS = 3
+SLOT_METALLIC = 4
+SLOT_EMISSION = 5
+SLOT_SPECULAR_COLOR = 6
+TEXTURE_SLOTS = 7
+
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
 
@@ -67,6 +84,9 @@ class Geometry(C.Structure):
         ("normals", C.POINTER(C.c_float)),
         ("vertex_count", C.c_uint32),
         ("triangle_count", C.c_uint32),
+        ("texcoords", C.POINTER(C.c_float)),
+        ("texcoord_sets", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -75,6 +95,32 @@ class Instance(C.Structure):
         ("world_from_object", C.c_float * 16),
         ("geometry", C.c_uint32),
         ("material", C.c_uint32),
+        ("texcoord_set", C.c_uint32),  # k > 0: the geometry's set k - 1; 0: none
+        ("reserved", C.c_uint32),
+    ]
+
+
+class Texture(C.Structure):
+    _fields_ = [
+        ("texels", C.c_void_p),
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("format", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class TextureInput(C.Structure):
+    _fields_ = [
+        ("texture", C.c_uint32),  # k > 0: textures[k - 1]; 0: none (the fallback)
+        ("channel", C.c_uint32),
+        ("wrap_s", C.c_uint32),
+        ("wrap_t", C.c_uint32),
+        ("scale", C.c_float * 4),
+        ("bias", C.c_float * 4),
+        ("fallback", C.c_float * 4),
+        ("st_transform", C.c_float * 6),
+        ("reserved", C.c_uint32 * 2),
     ]
 
 
@@ -92,6 +138,9 @@ class Material(C.Structure):
         ("opacity_threshold", C.c_float),
         ("flags", C.c_uint32),
         ("reserved", C.c_uint32),
+        ("lookups", C.c_uint32 * 7),  # per SLOT_*: k > 0 for texture_inputs[k - 1]; 0: the constant
+        ("texcoord_fallback", C.c_float * 2),
+        ("reserved2", C.c_uint32),
     ]
 
 
@@ -138,6 +187,10 @@ class SceneDesc(C.Structure):
         ("environment_constant", C.c_float * 3),
         ("lights", C.POINTER(Light)),
         ("light_count", C.c_uint32),
+        ("textures", C.POINTER(Texture)),
+        ("texture_count", C.c_uint32),
+        ("texture_input_count", C.c_uint32),
+        ("texture_inputs", C.POINTER(TextureInput)),
     ]
 
 
@@ -279,7 +332,7 @@ class CacheDesc(C.Structure):
 CACHE_INPUTS = 64
 CACHE_WEIGHTS = 21504
 
-STRUCTS = [Geometry, Instance, Material, Environment, Light, SceneDesc, SceneResult,
+STRUCTS = [Geometry, Instance, Texture, TextureInput, Material, Environment, Light, SceneDesc, SceneResult,
            Target, Settings, FrameDesc, FrameResult, Options, TemporalDesc, TemporalInstance,
            CacheDesc]
 

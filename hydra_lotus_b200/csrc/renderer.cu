@@ -518,12 +518,25 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
     const lotus_instance& inst = s.instances[index];
     const lotus_geometry& g = s.geometries[inst.geometry];
     const lotus_material& mat = s.materials[inst.material];
-    // EmissionEstimate (gpu_scene.cpp:144-180) of a constant input.
+    // EmissionEstimate (gpu_scene.cpp:144-180): the mean of the constant's
+    // RGB, or of a lookup's bound for texels in [0, 1] (its fallback when
+    // it names no image).
     double e = ((double)mat.emission[0] + (double)mat.emission[1] + (double)mat.emission[2]) / 3.0;
+    const uint32_t emission_lookup = mat.lookups[LOTUS_SLOT_EMISSION];
+    if (emission_lookup != LOTUS_NO_LOOKUP) {
+      const lotus_texture_input& in = s.texture_inputs[emission_lookup - 1];
+      double c[3];
+      for (int k = 0; k < 3; ++k)
+        c[k] = in.texture == LOTUS_NO_TEXTURE ? std::max(0.0f, in.fallback[k])
+                                              : (double)std::max(0.0f, in.scale[k]) + std::max(0.0f, in.bias[k]);
+      e = (c[0] + c[1] + c[2]) / 3.0;
+    }
     if (!(std::isfinite(e) && e > 0.0)) e = 0.0;
     if (e <= 0.0 || g.triangle_count == 0) continue;
     table.offsets[index] = (uint32_t)table.records.size();
     const float coverage = host_coverage(mat);
+    // Textured emission or opacity: the sample looks it up (radiance w 1).
+    const bool looked_up = emission_lookup != LOTUS_NO_LOOKUP || mat.lookups[LOTUS_SLOT_OPACITY] != LOTUS_NO_LOOKUP;
     for (uint32_t t = 0; t < g.triangle_count; ++t) {
       weights.push_back(e * world_triangle_area(g, t, inst.world_from_object));
       table.records.push_back({0.0f, 1.0f, 0u, index});
@@ -533,7 +546,7 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
         table.verts.push_back(make_float4(w.x, w.y, w.z, 0.0f));
       }
       table.radiance.push_back(make_float4(mat.emission[0] * coverage, mat.emission[1] * coverage,
-          mat.emission[2] * coverage, 0.0f));
+          mat.emission[2] * coverage, looked_up ? 1.0f : 0.0f));
     }
   }
   bool distant = env_mean > 0.0;
@@ -636,6 +649,12 @@ struct HostScene {
   float env_scale[3] = {0.0f, 0.0f, 0.0f};
   float env_frame[9] = {};
   std::vector<lotus_light> lights;      // the analytic lights
+  // Texture lookups: the scene's texture inputs, its texture count, per
+  // geometry its texture-coordinate sets and the first (s, t) of its set 0
+  // in the device pool.
+  std::vector<lotus_texture_input> texture_inputs;
+  uint32_t texture_count = 0;
+  std::vector<uint64_t> texcoord_base;
 };
 
 static_assert(LOTUS_OUTPUT_BARYCENTRICS == kOutputBarycentrics && LOTUS_OUTPUT_SHADING_NORMAL == kOutputShadingNormal &&
@@ -667,6 +686,12 @@ struct Renderer {
   DeviceArray<AnalyticLight> analytic;
   DeviceArray<LightNode> light_nodes;
   DeviceArray<uint32_t> distant;
+  DeviceArray<float4> tex_texels;            // SceneView::tex_texels
+  DeviceArray<uint4> tex_info;
+  DeviceArray<TextureLookup> tex_lookups;
+  DeviceArray<MaterialLookups> mat_lookups;
+  DeviceArray<float2> texcoords;
+  DeviceArray<uint32_t> inst_texcoords;
   std::vector<LightRecord> host_lights;
   std::vector<uint32_t> host_light_offsets;
   SceneView view{};
@@ -818,6 +843,8 @@ struct Renderer {
     materials.release(); normals.release(); lights.release(); light_verts.release();
     light_radiance.release(); env_texels.release(); env_floats.release(); env_guide.release();
     analytic.release(); light_nodes.release(); distant.release();
+    tex_texels.release(); tex_info.release(); tex_lookups.release(); mat_lookups.release(); texcoords.release();
+    inst_texcoords.release();
     scene_ready = false;
   }
 
@@ -825,7 +852,8 @@ struct Renderer {
     return scene_pos.bytes() + scene_tri.bytes() + blas.bytes() + tlas.bytes() + blas4.bytes() + tlas4.bytes() + tris.bytes() + inst_trav.bytes() + inst_shade.bytes() +
            materials.bytes() + normals.bytes() + lights.bytes() + light_verts.bytes() +
            light_radiance.bytes() + env_texels.bytes() + env_floats.bytes() + env_guide.bytes() +
-           analytic.bytes() + light_nodes.bytes() + distant.bytes();
+           analytic.bytes() + light_nodes.bytes() + distant.bytes() + tex_texels.bytes() + tex_info.bytes() +
+           tex_lookups.bytes() + mat_lookups.bytes() + texcoords.bytes() + inst_texcoords.bytes();
   }
 };
 
@@ -850,10 +878,38 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
     detail = "the scene's geometry or instance array is missing";
     return false;
   }
+  if ((s.texture_count && !s.textures) || (s.texture_input_count && !s.texture_inputs)) {
+    detail = "the scene's texture or texture-input array is missing";
+    return false;
+  }
+  for (uint32_t i = 0; i < s.texture_count; ++i) {
+    const lotus_texture& t = s.textures[i];
+    if (t.width == 0 || t.height == 0 || !t.texels || t.format > LOTUS_TEXTURE_RGBA32_FLOAT ||
+        (uint64_t)t.width * t.height > (1ull << 28)) {
+      detail = "texture " + std::to_string(i) + " is empty, too large or of an unknown format";
+      return false;
+    }
+  }
+  for (uint32_t i = 0; i < s.texture_input_count; ++i) {
+    const lotus_texture_input& in = s.texture_inputs[i];
+    bool finite = true;
+    for (int k = 0; k < 4; ++k)
+      finite = finite && std::isfinite(in.scale[k]) && std::isfinite(in.bias[k]) && std::isfinite(in.fallback[k]);
+    for (int k = 0; k < 6; ++k) finite = finite && std::isfinite(in.st_transform[k]);
+    if ((in.texture != LOTUS_NO_TEXTURE && in.texture > s.texture_count) || in.channel > 3 ||
+        in.wrap_s > LOTUS_WRAP_MIRROR || in.wrap_t > LOTUS_WRAP_MIRROR || !finite) {
+      detail = "texture input " + std::to_string(i) + " names a missing texture or has an invalid field";
+      return false;
+    }
+  }
   for (uint32_t g = 0; g < s.geometry_count; ++g) {
     const lotus_geometry& geo = s.geometries[g];
     if (geo.triangle_count && (!geo.triangles || !geo.positions)) {
       detail = "geometry " + std::to_string(g) + " has triangles without data";
+      return false;
+    }
+    if (geo.texcoord_sets && !geo.texcoords) {
+      detail = "geometry " + std::to_string(g) + " has texture-coordinate sets without data";
       return false;
     }
     for (uint64_t i = 0; i < 3ull * geo.triangle_count; ++i)
@@ -873,6 +929,10 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
       detail = "instance " + std::to_string(i) + " names a missing geometry or material";
       return false;
     }
+    if (inst.texcoord_set != LOTUS_NO_TEXCOORDS && inst.texcoord_set > s.geometries[inst.geometry].texcoord_sets) {
+      detail = "instance " + std::to_string(i) + " names a missing texture-coordinate set";
+      return false;
+    }
     const float* m = inst.world_from_object;
     if (m[3] != 0.0f || m[7] != 0.0f || m[11] != 0.0f || m[15] != 1.0f) {
       detail = "instance " + std::to_string(i) + " has a projective transform";
@@ -889,6 +949,19 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
       }
     if (!(m.ior >= 1.0f)) {
       detail = "material " + std::to_string(i) + " has an ior below 1";
+      return false;
+    }
+    for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k)
+      if (m.lookups[k] != LOTUS_NO_LOOKUP && m.lookups[k] > s.texture_input_count) {
+        detail = "material " + std::to_string(i) + " names a missing texture input";
+        return false;
+      }
+    if (m.lookups[LOTUS_SLOT_NORMAL] != LOTUS_NO_LOOKUP) {
+      detail = "material " + std::to_string(i) + " has a normal-map lookup, which this backend does not support";
+      return false;
+    }
+    if (!std::isfinite(m.texcoord_fallback[0]) || !std::isfinite(m.texcoord_fallback[1])) {
+      detail = "material " + std::to_string(i) + " has a non-finite texture-coordinate fallback";
       return false;
     }
   }
@@ -940,6 +1013,7 @@ struct InstanceState {
   LightTable table;
   std::vector<InstanceTraversal> trav;
   std::vector<InstanceShading> shade;
+  std::vector<uint32_t> texcoords;  // SceneView::inst_texcoords
 };
 
 lotus_scene_desc host_desc(const Renderer& R) {
@@ -955,6 +1029,9 @@ lotus_scene_desc host_desc(const Renderer& R) {
   for (int k = 0; k < 3; ++k) d.environment_constant[k] = h.environment_constant[k];
   d.lights = h.lights.data();
   d.light_count = (uint32_t)h.lights.size();
+  d.texture_inputs = h.texture_inputs.data();
+  d.texture_input_count = (uint32_t)h.texture_inputs.size();
+  d.texture_count = h.texture_count;
   return d;
 }
 
@@ -994,6 +1071,7 @@ bool prepare_instances(Renderer& R, InstanceState& out, std::string& detail) {
   }
   out.trav.resize(s.instance_count);
   out.shade.resize(s.instance_count);
+  out.texcoords.resize(s.instance_count);
   for (uint32_t i = 0; i < s.instance_count; ++i) {
     const lotus_instance& inst = s.instances[i];
     const float* m = inst.world_from_object;
@@ -1005,7 +1083,12 @@ bool prepare_instances(Renderer& R, InstanceState& out, std::string& detail) {
     }
     const lotus_geometry& geo = s.geometries[inst.geometry];
     t.blas_root = geo.triangle_count ? h.node_base[inst.geometry] : (uint32_t)kEmptyChild;
-    t.flags = host_coverage(s.materials[inst.material]) >= 1.0f ? kInstanceOpaque : 0u;
+    const lotus_material& mat = s.materials[inst.material];
+    t.flags = host_coverage(mat) >= 1.0f && mat.lookups[LOTUS_SLOT_OPACITY] == LOTUS_NO_LOOKUP ? kInstanceOpaque : 0u;
+    out.texcoords[i] =
+        inst.texcoord_set == LOTUS_NO_TEXCOORDS || inst.texcoord_set > geo.texcoord_sets
+            ? kNoTexture
+            : (uint32_t)(h.texcoord_base[inst.geometry] + 3ull * geo.triangle_count * (inst.texcoord_set - 1));
     t.material = inst.material;
     t.light_offset = out.table.offsets[i];
     for (int r = 0; r < 3; ++r) sh.m[r] = make_float4(m[r], m[4 + r], m[8 + r], m[12 + r]);
@@ -1036,6 +1119,7 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
       !R.ok(R.distant.upload(in.table.distant.data(), in.table.distant.size(), st), "distant lights", detail) ||
       !R.ok(R.inst_trav.upload(in.trav.data(), in.trav.size(), st), "instances", detail) ||
       !R.ok(R.inst_shade.upload(in.shade.data(), in.shade.size(), st), "instances", detail) ||
+      !R.ok(R.inst_texcoords.upload(in.texcoords.data(), in.texcoords.size(), st), "instances", detail) ||
       !R.ok(R.tlas.resize(std::max<uint32_t>(BvhBuilder::node_count(n), 1)), "TLAS", detail))
     return false;
   if (!R.ok(n <= kSahMaxTriangles
@@ -1056,6 +1140,12 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
   v.inst_trav = R.inst_trav.ptr;
   v.inst_shade = R.inst_shade.ptr;
   v.materials = R.materials.ptr;
+  v.tex_texels = R.tex_texels.ptr;
+  v.tex_info = R.tex_info.ptr;
+  v.lookups = R.tex_lookups.ptr;
+  v.mat_lookups = R.mat_lookups.ptr;
+  v.texcoords = R.texcoords.ptr;
+  v.inst_texcoords = R.inst_texcoords.ptr;
   v.normals = R.normals.ptr;
   v.lights = R.lights.ptr;
   v.light_verts = R.light_verts.ptr;
@@ -1145,6 +1235,97 @@ int32_t finish_update(Renderer& R, lotus_scene_result& res, std::string& detail)
 // The environment's sampling distribution and guide tables, built on the
 // device from the resident texels (the k_env_* kernels); `mean` is the mean
 // cell value, positive and finite for an image that can be sampled.
+// The sRGB transfer function's inverse for each 8-bit code (IEC 61966-2-1:
+// linear below 0.04045, the 2.4 power above), in double, rounded to float.
+const float* srgb_to_linear_table() {
+  static const std::vector<float> table = [] {
+    std::vector<float> t(256);
+    for (int v = 0; v < 256; ++v) {
+      const double c = v / 255.0;
+      t[v] = (float)(c <= 0.04045 ? c / 12.92 : std::pow((c + 0.055) / 1.055, 2.4));
+    }
+    return t;
+  }();
+  return table.data();
+}
+
+// The scene's textures decoded to linear RGBA floats, one after another
+// (sRGB codes through srgb_to_linear_table, alpha and unorm codes / 255),
+// the texture inputs as TextureLookup records, each material's lookups and
+// every geometry's texture-coordinate sets in one pool.
+bool upload_textures(Renderer& R, const lotus_scene_desc& s, std::string& detail) {
+  cudaStream_t st = R.stream;
+  HostScene& h = R.host;
+  const float* srgb = srgb_to_linear_table();
+  std::vector<float4> texels;
+  std::vector<uint4> info(s.texture_count);
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < s.texture_count; ++i) total += (uint64_t)s.textures[i].width * s.textures[i].height;
+  if (total >= (1ull << 31)) {
+    detail = "the scene's textures hold 2^31 texels or more";
+    return false;
+  }
+  texels.reserve(total);
+  for (uint32_t i = 0; i < s.texture_count; ++i) {
+    const lotus_texture& t = s.textures[i];
+    info[i] = make_uint4((uint32_t)texels.size(), t.width, t.height, t.format);
+    const size_t n = (size_t)t.width * t.height;
+    if (t.format == LOTUS_TEXTURE_RGBA32_FLOAT) {
+      const float* f = static_cast<const float*>(t.texels);
+      for (size_t k = 0; k < n; ++k) texels.push_back(make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]));
+    } else {
+      const uint8_t* b = static_cast<const uint8_t*>(t.texels);
+      const bool encoded = t.format == LOTUS_TEXTURE_RGBA8_SRGB;
+      for (size_t k = 0; k < n; ++k) {
+        const uint8_t* c = b + 4 * k;
+        auto channel = [&](int j) { return encoded ? srgb[c[j]] : (float)(c[j] / 255.0); };
+        texels.push_back(make_float4(channel(0), channel(1), channel(2), (float)(c[3] / 255.0)));
+      }
+    }
+  }
+  std::vector<TextureLookup> lookups(s.texture_input_count);
+  for (uint32_t i = 0; i < s.texture_input_count; ++i) {
+    const lotus_texture_input& in = s.texture_inputs[i];
+    TextureLookup& L = lookups[i];
+    L.texture = in.texture == LOTUS_NO_TEXTURE ? kNoTexture : in.texture - 1;
+    L.channel = in.channel;
+    L.wrap_s = in.wrap_s;
+    L.wrap_t = in.wrap_t;
+    L.scale = make_float4(in.scale[0], in.scale[1], in.scale[2], in.scale[3]);
+    L.bias = make_float4(in.bias[0], in.bias[1], in.bias[2], in.bias[3]);
+    L.fallback = make_float4(in.fallback[0], in.fallback[1], in.fallback[2], in.fallback[3]);
+    L.st_s = make_float4(in.st_transform[0], in.st_transform[1], in.st_transform[2], 0.0f);
+    L.st_t = make_float4(in.st_transform[3], in.st_transform[4], in.st_transform[5], 0.0f);
+  }
+  std::vector<MaterialLookups> mats(s.material_count);
+  for (uint32_t i = 0; i < s.material_count; ++i) {
+    const lotus_material& m = s.materials[i];
+    MaterialLookups& ml = mats[i];
+    for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k)
+      ml.slot[k] = m.lookups[k] == LOTUS_NO_LOOKUP ? kNoTexture : m.lookups[k] - 1;
+    ml.fallback_s = m.texcoord_fallback[0];
+    ml.fallback_t = m.texcoord_fallback[1];
+    ml.reserved[0] = ml.reserved[1] = ml.reserved[2] = 0u;
+  }
+  std::vector<float2> coords;
+  h.texcoord_base.assign(s.geometry_count, 0);
+  for (uint32_t g = 0; g < s.geometry_count; ++g) {
+    const lotus_geometry& geo = s.geometries[g];
+    h.texcoord_base[g] = coords.size();
+    const size_t n = 3ull * geo.triangle_count * geo.texcoord_sets;
+    for (size_t k = 0; k < n; ++k) coords.push_back(make_float2(geo.texcoords[2 * k], geo.texcoords[2 * k + 1]));
+  }
+  if (coords.size() >= (size_t)kNoTexture) {
+    detail = "the scene's texture coordinates exceed 2^32 corners";
+    return false;
+  }
+  return R.ok(R.tex_texels.upload(texels.data(), texels.size(), st), "texels", detail) &&
+         R.ok(R.tex_info.upload(info.data(), info.size(), st), "textures", detail) &&
+         R.ok(R.tex_lookups.upload(lookups.data(), lookups.size(), st), "texture inputs", detail) &&
+         R.ok(R.mat_lookups.upload(mats.data(), mats.size(), st), "material lookups", detail) &&
+         R.ok(R.texcoords.upload(coords.data(), coords.size(), st), "texture coordinates", detail);
+}
+
 bool build_env_distribution(Renderer& R, const lotus_environment& e, double& mean, std::string& detail) {
   constexpr double kPiD = 3.14159265358979323846;
   cudaStream_t st = R.stream;
@@ -1223,6 +1404,7 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
     copy.positions = h.positions[g].data();
     copy.triangles = h.triangles[g].data();
     copy.normals = h.normals[g].empty() ? nullptr : h.normals[g].data();
+    copy.texcoords = nullptr;  // on the device only
     h.boxes[g] = geometry_box(copy);
     h.vertex_base[g] = vert_total;
     h.node_base[g] = (uint32_t)nodes;
@@ -1237,6 +1419,9 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
   }
   h.nodes = nodes;
   h.materials.assign(s.materials, s.materials + s.material_count);
+  h.texture_inputs.assign(s.texture_inputs, s.texture_inputs + s.texture_input_count);
+  h.texture_count = s.texture_count;
+  if (!upload_textures(R, s, detail)) return fail(detail);
   for (int k = 0; k < 3; ++k) h.environment_constant[k] = s.environment_constant[k];
   h.lights.assign(s.lights, s.lights + s.light_count);
   R.host_instances.assign(s.instances, s.instances + s.instance_count);
@@ -1284,7 +1469,10 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
     r.specular_ior = make_float4(m.specular_color[0], m.specular_color[1], m.specular_color[2], m.ior);
     r.transmission = make_float4(m.transmission_color[0], m.transmission_color[1],
         m.transmission_color[2], m.transmission);
-    uint32_t flags = m.flags;
+    uint32_t flags = m.flags & (LOTUS_MATERIAL_SPECULAR_WORKFLOW | LOTUS_MATERIAL_THIN_WALLED);
+    for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k)
+      if (m.lookups[k] != LOTUS_NO_LOOKUP) flags |= kMaterialTextured;
+    if (m.lookups[LOTUS_SLOT_OPACITY] != LOTUS_NO_LOOKUP) flags |= kMaterialOpacityTextured;
     float fbits;
     std::memcpy(&fbits, &flags, 4);
     r.coverage = make_float4(m.opacity, m.opacity_threshold, fbits, 0.0f);
@@ -1350,6 +1538,9 @@ int32_t update_instances(Renderer& R, const lotus_instance* instances, uint32_t 
     const lotus_instance& inst = instances[i];
     if (inst.geometry >= R.host.geometries.size() || inst.material >= R.host.materials.size())
       return reject("instance " + std::to_string(i) + " names a missing geometry or material");
+    if (inst.texcoord_set != LOTUS_NO_TEXCOORDS &&
+        inst.texcoord_set > R.host.geometries[inst.geometry].texcoord_sets)
+      return reject("instance " + std::to_string(i) + " names a missing texture-coordinate set");
     const float* m = inst.world_from_object;
     if (m[3] != 0.0f || m[7] != 0.0f || m[11] != 0.0f || m[15] != 1.0f)
       return reject("instance " + std::to_string(i) + " has a projective transform");
@@ -2030,7 +2221,8 @@ extern "C" {
 uint32_t lotus_cuda_abi_version(void) { return LOTUS_CUDA_ABI_VERSION; }
 
 uint32_t lotus_cuda_struct_sizes(uint64_t* sizes, uint32_t capacity) {
-  const uint64_t s[] = {sizeof(lotus_geometry), sizeof(lotus_instance), sizeof(lotus_material),
+  const uint64_t s[] = {sizeof(lotus_geometry), sizeof(lotus_instance), sizeof(lotus_texture),
+      sizeof(lotus_texture_input), sizeof(lotus_material),
       sizeof(lotus_environment), sizeof(lotus_light), sizeof(lotus_scene_desc), sizeof(lotus_scene_result),
       sizeof(lotus_target), sizeof(lotus_settings), sizeof(lotus_frame_desc),
       sizeof(lotus_frame_result), sizeof(lotus_cuda_options), sizeof(lotus_temporal_desc),

@@ -19,6 +19,7 @@
 // traversal order.
 #pragma once
 
+#include "../../include/lotus_cuda.h"
 #include "common.cuh"
 
 namespace lotus {
@@ -103,6 +104,40 @@ struct alignas(16) MaterialRecord {
 };
 static_assert(sizeof(MaterialRecord) == 80, "material record is 80 bytes");
 
+// MaterialRecord::coverage.z flag bits the renderer adds to the material's
+// own LOTUS_MATERIAL_* bits: some input has a texture lookup; the opacity
+// has one.
+constexpr uint32_t kMaterialTextured = 1u << 8;
+constexpr uint32_t kMaterialOpacityTextured = 1u << 9;
+
+// A texture input (TextureInputRecord, scene.slang:44-55): the texture's
+// index (kNoTexture: the fallback), channel and wrap modes, then scale,
+// bias and fallback, and the lookup's coordinate rows
+// (s' = st_s.x s + st_s.y t + st_s.z, t' likewise).
+struct alignas(16) TextureLookup {
+  uint32_t texture;
+  uint32_t channel;
+  uint32_t wrap_s;
+  uint32_t wrap_t;
+  float4 scale;
+  float4 bias;
+  float4 fallback;
+  float4 st_s;
+  float4 st_t;
+};
+static_assert(sizeof(TextureLookup) == 96, "TextureLookup is 96 bytes");
+constexpr uint32_t kNoTexture = 0xFFFFFFFFu;
+
+// A material's lookups per texture slot (kNoTexture: its constant) and its
+// texture-coordinate fallback.
+struct alignas(16) MaterialLookups {
+  uint32_t slot[LOTUS_TEXTURE_SLOTS];
+  float fallback_s;
+  float fallback_t;
+  uint32_t reserved[3];
+};
+static_assert(sizeof(MaterialLookups) == 48, "MaterialLookups is 48 bytes");
+
 // A light-table entry (GpuLightRecord, gpu_scene.hpp:120-126).
 struct alignas(16) LightRecord {
   float pdf;
@@ -164,6 +199,18 @@ struct SceneView {
   uint32_t light_node_count;
   uint32_t distant_count;
   uint32_t step_limit;       // a walk's step budget (kMaxTraversalSteps)
+  // Texture lookups: every texture's texels decoded to linear RGBA, one
+  // after another; per texture its first texel, width and height; the
+  // scene's texture inputs; per material its lookups (read only for
+  // kMaterialTextured materials); every geometry's texture-coordinate sets,
+  // three (s, t) per triangle; per instance the first coordinate of its
+  // set (kNoTexture: the material's fallback).
+  const float4* __restrict__ tex_texels;
+  const uint4* __restrict__ tex_info;
+  const TextureLookup* __restrict__ lookups;
+  const MaterialLookups* __restrict__ mat_lookups;
+  const float2* __restrict__ texcoords;
+  const uint32_t* __restrict__ inst_texcoords;
   // Two words the renderer clears before and reads after each frame: the
   // number of walks that failed and the kWalkFailed* bits of their causes.
   uint32_t* walk_failure;
@@ -181,16 +228,106 @@ struct Hit {
   float t;
 };
 
-// Coverage (scene.slang:393-406) of a material's constant opacity.
-__device__ __forceinline__ float material_coverage(const MaterialRecord& m) {
-  const float opacity = m.coverage.x;
+// One texel of a lookup's texture at integer coordinates (x, y), rows from
+// the top, after each axis's wrap (the Vulkan sampler address modes the
+// reference binds, vulkan_backend.cpp:3038-3053): transparent black outside
+// the image, the edge texel, the coordinate modulo the size, or mirrored
+// every size texels.
+__device__ __forceinline__ int32_t wrap_texel(int32_t i, int32_t n, uint32_t mode) {
+  if (mode == LOTUS_WRAP_CLAMP) return i < 0 ? 0 : (i >= n ? n - 1 : i);
+  if (mode == LOTUS_WRAP_REPEAT) {
+    const int32_t r = i % n;
+    return r < 0 ? r + n : r;
+  }
+  if (mode == LOTUS_WRAP_MIRROR) {
+    int32_t r = i % (2 * n);
+    if (r < 0) r += 2 * n;
+    return r < n ? r : 2 * n - 1 - r;
+  }
+  return (i < 0 || i >= n) ? -1 : i;
+}
+
+__device__ __forceinline__ float4 texel_at(const SceneView& S, const uint4& info, int32_t x, int32_t y,
+    uint32_t wrap_s, uint32_t wrap_t) {
+  const int32_t xi = wrap_texel(x, (int32_t)info.y, wrap_s);
+  const int32_t yi = wrap_texel(y, (int32_t)info.z, wrap_t);
+  if (xi < 0 || yi < 0) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  return S.tex_texels[info.x + (uint32_t)yi * info.y + (uint32_t)xi];
+}
+
+// Lookup (scene.slang:315-328): the bilinear texel at (s, t) (texel centres
+// at (i + 1/2) / size, rows from the image's top), times scale plus bias;
+// the unscaled fallback when the input names no image.
+__device__ __forceinline__ float4 texture_lookup(const SceneView& S, const TextureLookup& L, float s, float t) {
+  if (L.texture == kNoTexture) return L.fallback;
+  const float u = L.st_s.x * s + L.st_s.y * t + L.st_s.z;
+  const float v = 1.0f - (L.st_t.x * s + L.st_t.y * t + L.st_t.z);
+  const uint4 info = S.tex_info[L.texture];
+  // Far outside the image every wrap mode reads a defined texel; keep the
+  // integer conversion in range.
+  const float x = fminf(fmaxf(u * (float)info.y - 0.5f, -16777216.0f), 16777216.0f);
+  const float y = fminf(fmaxf(v * (float)info.z - 0.5f, -16777216.0f), 16777216.0f);
+  const float fx = floorf(x), fy = floorf(y);
+  const float ax = x - fx, ay = y - fy;
+  const int32_t ix = (int32_t)fx, iy = (int32_t)fy;
+  const float4 t00 = texel_at(S, info, ix, iy, L.wrap_s, L.wrap_t);
+  const float4 t10 = texel_at(S, info, ix + 1, iy, L.wrap_s, L.wrap_t);
+  const float4 t01 = texel_at(S, info, ix, iy + 1, L.wrap_s, L.wrap_t);
+  const float4 t11 = texel_at(S, info, ix + 1, iy + 1, L.wrap_s, L.wrap_t);
+  const float bx = 1.0f - ax, by = 1.0f - ay;
+  const float4 top = make_float4(t00.x * bx + t10.x * ax, t00.y * bx + t10.y * ax, t00.z * bx + t10.z * ax,
+      t00.w * bx + t10.w * ax);
+  const float4 bottom = make_float4(t01.x * bx + t11.x * ax, t01.y * bx + t11.y * ax, t01.z * bx + t11.z * ax,
+      t01.w * bx + t11.w * ax);
+  const float4 f = make_float4(top.x * by + bottom.x * ay, top.y * by + bottom.y * ay, top.z * by + bottom.z * ay,
+      top.w * by + bottom.w * ay);
+  return make_float4(f.x * L.scale.x + L.bias.x, f.y * L.scale.y + L.bias.y, f.z * L.scale.z + L.bias.z,
+      f.w * L.scale.w + L.bias.w);
+}
+
+__device__ __forceinline__ float lookup_channel(const float4& v, uint32_t channel) {
+  return channel == 0 ? v.x : channel == 1 ? v.y : channel == 2 ? v.z : v.w;
+}
+
+// HitTexcoords (scene.slang:362-374): the instance's set interpolated with
+// the barycentrics, or the material's fallback.
+__device__ __forceinline__ void hit_texcoords(const SceneView& S, uint32_t instance, const MaterialLookups& ml,
+    uint32_t primitive, float b1, float b2, float& s, float& t) {
+  const uint32_t base = S.inst_texcoords[instance];
+  if (base == kNoTexture) {
+    s = ml.fallback_s;
+    t = ml.fallback_t;
+    return;
+  }
+  const float2* c = S.texcoords + base + 3 * (size_t)primitive;
+  const float2 t0 = c[0], t1 = c[1], t2 = c[2];
+  s = t0.x + b1 * (t1.x - t0.x) + b2 * (t2.x - t0.x);
+  t = t0.y + b1 * (t1.y - t0.y) + b2 * (t2.y - t0.y);
+}
+
+// Coverage (scene.slang:393-406): the material's opacity, or its lookup's
+// channel at the hit, saturated (0 where the lookup overflows); 0 or 1
+// under a threshold.
+__device__ __forceinline__ float material_coverage(const SceneView& S, const MaterialRecord& m, uint32_t material,
+    uint32_t instance, uint32_t primitive, float b1, float b2) {
+  float opacity = m.coverage.x;
+  if (__float_as_uint(m.coverage.z) & kMaterialOpacityTextured) {
+    const MaterialLookups ml = S.mat_lookups[material];
+    float s, t;
+    hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
+    const TextureLookup& L = S.lookups[ml.slot[LOTUS_SLOT_OPACITY]];
+    opacity = lookup_channel(texture_lookup(S, L, s, t), L.channel);
+    opacity = isfinite(opacity) ? fminf(fmaxf(opacity, 0.0f), 1.0f) : 0.0f;
+  }
   const float threshold = m.coverage.y;
   if (threshold > 0.0f) return opacity >= threshold ? 1.0f : 0.0f;
   return opacity;
 }
 
-__device__ __forceinline__ float instance_coverage(const SceneView& S, uint32_t instance) {
-  return material_coverage(S.materials[S.inst_trav[instance].material]);
+__device__ __forceinline__ float instance_coverage(const SceneView& S, uint32_t instance, uint32_t primitive,
+    float b1, float b2) {
+  const uint32_t material = S.inst_trav[instance].material;
+  return material_coverage(S, S.materials[material], material, instance, primitive, b1, b2);
 }
 
 __device__ __forceinline__ F3 safe_inverse(F3 d) {
@@ -472,7 +609,7 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
     if (!(t >= W.tmin) || !(t <= W.best)) continue;
     const uint32_t prim = __float_as_uint(a.w);
     if (kAnyHit) {
-      const float coverage = W.opaque ? 1.0f : instance_coverage(S, W.instance);
+      const float coverage = W.opaque ? 1.0f : instance_coverage(S, W.instance, prim, b1, b2);
       if (coverage >= 1.0f) {
         W.found = true;
         W.transmittance = 0.0f;
@@ -485,7 +622,7 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
            (W.instance == W.best_instance && prim >= __float_as_uint(S.tris[kTriStride * (size_t)W.best_tri].w))))
         continue;
       if (!W.opaque) {
-        const float coverage = instance_coverage(S, W.instance);
+        const float coverage = instance_coverage(S, W.instance, prim, b1, b2);
         if (coverage <= 0.0f) continue;
         if (coverage < 1.0f && !(next_random(rng) < coverage)) continue;
       }

@@ -43,9 +43,22 @@ __device__ __forceinline__ F3 shading_normal(const float* n, float b1, float b2,
   return dot(s, direction) < 0.0f ? s : geometric;
 }
 
-// ReconstructHit and EvaluatePreview for constant material inputs
-// (scene.slang:1408-1449, 1184-1260). The corners come from the
-// leaf-ordered triangle pool, which holds the geometry's own positions.
+__device__ __forceinline__ float saturate1(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+
+// PreviewEmission (scene.slang:570-577): the constant, or the lookup's RGB
+// at (s, t), negative parts cut.
+__device__ __forceinline__ F3 preview_emission(const SceneView& S, const MaterialRecord& mat,
+    const MaterialLookups& ml, float s, float t) {
+  const uint32_t k = ml.slot[LOTUS_SLOT_EMISSION];
+  if (k == kNoTexture) return V(mat.emission_metallic);
+  const float4 v = texture_lookup(S, S.lookups[k], s, t);
+  return V(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f), fmaxf(v.z, 0.0f));
+}
+
+// ReconstructHit and EvaluatePreview (scene.slang:1408-1449, 1184-1260).
+// The corners come from the leaf-ordered triangle pool, which holds the
+// geometry's own positions. A texture lookup replaces its input's constant,
+// clamped into the input's range.
 __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32_t instance,
     uint32_t tri, float b1, float b2, F3 direction, uint32_t* primitive_out = nullptr) {
   const InstanceShading rec = S.inst_shade[instance];
@@ -70,6 +83,30 @@ __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32
   sh.roughness = mat.base_roughness.w;
   sh.metallic = mat.emission_metallic.w;
   const uint32_t flags = __float_as_uint(mat.coverage.z);
+  F3 emission = V(mat.emission_metallic);
+  F3 specular = V(mat.specular_ior);
+  if (flags & kMaterialTextured) {
+    const MaterialLookups ml = S.mat_lookups[rec.material];
+    float s, t;
+    hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
+    uint32_t k = ml.slot[LOTUS_SLOT_BASE_COLOR];
+    if (k != kNoTexture) {
+      const float4 v = texture_lookup(S, S.lookups[k], s, t);
+      sh.base_color = V(saturate1(v.x), saturate1(v.y), saturate1(v.z));
+    }
+    k = ml.slot[LOTUS_SLOT_ROUGHNESS];
+    if (k != kNoTexture)
+      sh.roughness = saturate1(lookup_channel(texture_lookup(S, S.lookups[k], s, t), S.lookups[k].channel));
+    k = ml.slot[LOTUS_SLOT_METALLIC];
+    if (k != kNoTexture)
+      sh.metallic = saturate1(lookup_channel(texture_lookup(S, S.lookups[k], s, t), S.lookups[k].channel));
+    emission = preview_emission(S, mat, ml, s, t);
+    k = ml.slot[LOTUS_SLOT_SPECULAR_COLOR];
+    if (k != kNoTexture) {
+      const float4 v = texture_lookup(S, S.lookups[k], s, t);
+      if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z)) specular = V(saturate1(v.x), saturate1(v.y), saturate1(v.z));
+    }
+  }
   const float transmission = mat.transmission.w;
   bool entering = true;
   if (transmission > 0.0f) {
@@ -77,9 +114,9 @@ __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32
     entering = dot(outward, direction) < 0.0f;
   }
   sh.bsdf = make_closure(sh.base_color, sh.roughness, sh.metallic, mat.specular_ior.w,
-      (flags & 1u) != 0, V(mat.specular_ior), transmission, V(mat.transmission),
+      (flags & 1u) != 0, specular, transmission, V(mat.transmission),
       (flags & 2u) != 0, entering);
-  sh.emission = V(mat.emission_metallic);
+  sh.emission = emission;
   return sh;
 }
 
@@ -112,7 +149,21 @@ __device__ __forceinline__ LightSample sample_triangle(const SceneView& S, uint3
   const F3 position = p0 + b1 * (p1 - p0) + b2 * (p2 - p0);
   const F3 normal = normalize(cross(p1 - p0, p2 - p0));
   const float area = triangle_area(p0, p1, p2);
-  const F3 radiance = V(S.light_radiance[light]);
+  const float4 stored = S.light_radiance[light];
+  F3 radiance = V(stored);
+  if (stored.w != 0.0f) {
+    // A textured emission or opacity: Emission(material, HitTexcoords) *
+    // Coverage(hit) at the sampled point (scene.slang:655-657).
+    const uint32_t instance = S.lights[light].instance;
+    const InstanceShading& rec = S.inst_shade[instance];
+    const uint32_t primitive = light - rec.light_offset;
+    const MaterialRecord& mat = S.materials[rec.material];
+    const MaterialLookups ml = S.mat_lookups[rec.material];
+    float s, t;
+    hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
+    radiance = preview_emission(S, mat, ml, s, t) *
+               material_coverage(S, mat, rec.material, instance, primitive, b1, b2);
+  }
   const F3 toward = position - origin;
   const float distance2 = dot(toward, toward);
   if (!(area > 0.0f) || !(distance2 > 0.0f) || max_component(radiance) <= 0.0f) return no_light();

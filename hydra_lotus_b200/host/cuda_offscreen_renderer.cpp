@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <unordered_map>
 #include <variant>
 
 namespace lotus_cuda_host {
@@ -124,7 +125,8 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
 
   // The scene description, rebuilt whole.
   std::vector<lotus_geometry> geos(geometries_.size());
-  std::vector<std::vector<float>> positions(geometries_.size()), normals(geometries_.size());
+  std::vector<std::vector<float>> positions(geometries_.size()), normals(geometries_.size()),
+      texcoords(geometries_.size());
   std::vector<std::vector<uint32_t>> triangles(geometries_.size());
   for (size_t g = 0; g < geometries_.size(); ++g) {
     const Lotus::MeshGeometry& m = *geometries_[g];
@@ -141,16 +143,62 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
     geos[g].normals = normals[g].empty() ? nullptr : normals[g].data();
     geos[g].vertex_count = (uint32_t)m.positions.size();
     geos[g].triangle_count = (uint32_t)m.triangles.size();
+    // Texture-coordinate sets in key order, one (s, t) per triangle corner.
+    for (const auto& [name, set] : m.texcoords) {
+      if (set.size() != 3 * m.triangles.size())
+        return fail("texture coordinates must be one per triangle corner (set " + name + ")");
+      for (const auto& st : set) texcoords[g].insert(texcoords[g].end(), st.begin(), st.end());
+    }
+    geos[g].texcoords = texcoords[g].empty() ? nullptr : texcoords[g].data();
+    geos[g].texcoord_sets = texcoords[g].empty() ? 0u : (uint32_t)m.texcoords.size();
   }
+  // Every resident texture (TextureFormat, material.hpp:15-23), counted
+  // from 1 by the lookups that name it.
+  std::vector<lotus_texture> texs(textures_.size());
+  std::unordered_map<const Lotus::Texture*, uint32_t> texture_ref;
+  for (size_t i = 0; i < textures_.size(); ++i) {
+    const Lotus::Texture& t = *textures_[i];
+    if (t.texels.size() != (size_t)t.width * t.height * Lotus::TexelBytes(t.format))
+      return fail("texture " + std::to_string(i) + " has the wrong number of texel bytes");
+    texs[i].texels = t.texels.data();
+    texs[i].width = t.width;
+    texs[i].height = t.height;
+    texs[i].format = t.format == Lotus::TextureFormat::Rgba8Srgb     ? LOTUS_TEXTURE_RGBA8_SRGB
+                     : t.format == Lotus::TextureFormat::Rgba32Float ? LOTUS_TEXTURE_RGBA32_FLOAT
+                                                                     : LOTUS_TEXTURE_RGBA8_UNORM;
+    texture_ref[&t] = (uint32_t)i + 1;
+  }
+  std::vector<lotus_texture_input> inputs;
   std::vector<lotus_material> mats(std::max<size_t>(materials_.size(), 1));
   for (size_t i = 0; i < materials_.size(); ++i) {
     const Lotus::SceneMaterial& sm = materials_[i];
-    for (const Lotus::Texture* t : sm.textures)
-      if (t) return fail("material " + std::to_string(i) + " has texture inputs, which are not built");
     if (!std::holds_alternative<Lotus::PreviewSurface>(sm.material.surface))
       return fail("material " + std::to_string(i) + ": only UsdPreviewSurface is built");
     const Lotus::PreviewSurface& p = Lotus::Preview(sm.material);
     lotus_material& m = mats[i];
+    // Each texture-input slot (material.hpp:266-273) with its resolved
+    // image (SceneMaterial::textures; none: the lookup's fallback).
+    const std::optional<Lotus::TextureInput>* slots[LOTUS_TEXTURE_SLOTS] = {&sm.material.geometry.opacity_texture,
+        &sm.material.geometry.normal_texture, &p.base_color_texture, &p.roughness_texture, &p.metallic_texture,
+        &p.emission_texture, &p.specular_color_texture};
+    for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k) {
+      if (!*slots[k]) continue;
+      const Lotus::TextureInput& in = **slots[k];
+      lotus_texture_input d{};
+      const Lotus::Texture* image = k < sm.textures.size() ? sm.textures[k] : nullptr;
+      const auto ref = image ? texture_ref.find(image) : texture_ref.end();
+      d.texture = ref == texture_ref.end() ? LOTUS_NO_TEXTURE : ref->second;
+      d.channel = in.channel;
+      d.wrap_s = (uint32_t)in.wrap_s;
+      d.wrap_t = (uint32_t)in.wrap_t;
+      std::memcpy(d.scale, in.scale.data(), 16);
+      std::memcpy(d.bias, in.bias.data(), 16);
+      std::memcpy(d.fallback, in.fallback.data(), 16);
+      std::memcpy(d.st_transform, in.st_transform.data(), 24);
+      inputs.push_back(d);
+      m.lookups[k] = (uint32_t)inputs.size();
+    }
+    std::memcpy(m.texcoord_fallback, sm.material.geometry.texcoord_fallback.data(), 8);
     std::memcpy(m.base_color, p.base_color.data(), 12);
     m.roughness = p.roughness;
     std::memcpy(m.emission, p.emission.data(), 12);
@@ -220,6 +268,10 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
   desc.geometry_count = (uint32_t)geos.size();
   desc.instance_count = (uint32_t)insts.size();
   desc.material_count = (uint32_t)mats.size();
+  desc.textures = texs.empty() ? nullptr : texs.data();
+  desc.texture_count = (uint32_t)texs.size();
+  desc.texture_inputs = inputs.empty() ? nullptr : inputs.data();
+  desc.texture_input_count = (uint32_t)inputs.size();
   std::memcpy(desc.environment_constant, environment_.data(), 12);
   lotus_scene_result res{};
   const int32_t s = lotus_cuda_update_scene(handle_, &desc, &res);
@@ -269,6 +321,8 @@ bool CudaOffscreenRenderer::InstanceArray(std::vector<lotus_instance>& insts, st
     std::memcpy(insts[i].world_from_object, si.world_from_object.data(), 64);
     insts[i].geometry = it->second;
     insts[i].material = si.material;
+    // The set its material's lookups read, counted from 1 (0: none).
+    insts[i].texcoord_set = si.texcoords == Lotus::kNoTexcoords ? LOTUS_NO_TEXCOORDS : si.texcoords + 1;
   }
   return true;
 }
@@ -294,7 +348,8 @@ bool CudaOffscreenRenderer::UpdateIncrementally(const Lotus::SceneUpdate& u, Lot
     const Lotus::MeshGeometry& a = *r.previous;
     const Lotus::MeshGeometry& b = *next;
     if (a.positions.size() != b.positions.size() || a.triangles != b.triangles ||
-        a.normals.empty() != b.normals.empty() || (!b.normals.empty() && b.normals.size() != 3 * b.triangles.size()))
+        a.normals.empty() != b.normals.empty() || (!b.normals.empty() && b.normals.size() != 3 * b.triangles.size()) ||
+        a.texcoords != b.texcoords)
       return false;
     edits.emplace_back(at, next);
   }

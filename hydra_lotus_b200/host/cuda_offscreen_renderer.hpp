@@ -18,14 +18,19 @@
 //                             through UpdateScene first, as it does for
 //                             RenderScene)
 //   RayQueryCapability()      lotus_cuda_capability
-//   Render, ReadBackScene,    Skip: the bootstrap raster, scene readback and
-//   Present                   presentation are graphics-side parts of the
-//                             reference that this backend does not build
+//   ReadBackScene()           lotus_cuda_read_scene
+//   Render, Present           Skip: the bootstrap raster and presentation are
+//                             graphics-side parts of the reference that this
+//                             backend does not build
 //   Residency()               the resident scene's device bytes
-// Analytic lights (Lotus::Light) map field for field to lotus_light. Scene
-// content the backend does not build (texture inputs, material models other
-// than UsdPreviewSurface) makes UpdateScene Fail with the reason, as the
-// reference Fails on unsupported content.
+// Analytic lights (Lotus::Light) map field for field to lotus_light; the
+// resident textures to lotus_texture, UsdPreviewSurface's texture inputs
+// (opacity, base colour, roughness, metallic, emission, specular colour)
+// to lotus_texture_input, each geometry's texture-coordinate sets in key
+// order and each instance's set. Scene content the backend does not build
+// (normal maps, material models other than UsdPreviewSurface) makes
+// UpdateScene Fail with the reason, as the reference Fails on unsupported
+// content.
 #pragma once
 
 #include <lotus/vulkan_backend.hpp>

@@ -133,6 +133,50 @@ class Scene:
         self.view = None  # world to view space, when the temporal passes need it
         self.width = 0
         self.height = 0
+        # Texture lookups: per geometry its texture-coordinate sets
+        # (sets, triangles, 3 corners, 2); per instance the set its material
+        # reads (k > 0: set k - 1; 0 or absent: the material's fallback); the
+        # images (rows from the top) with their LOTUS_TEXTURE_* formats; the
+        # texture inputs.
+        self.texcoords = {}
+        self.instance_texcoords = {}
+        self.textures = []
+        self.texture_inputs = []
+        self._desc = None
+
+    def add_texture(self, texels, fmt):
+        """An image (H, W, 4): uint8 for abi.TEXTURE_RGBA8_UNORM / _SRGB,
+        float32 for abi.TEXTURE_RGBA32_FLOAT. Returns the reference a
+        texture input names it by (its index + 1)."""
+        dtype = F32 if fmt == abi.TEXTURE_RGBA32_FLOAT else np.uint8
+        texels = np.ascontiguousarray(texels, dtype=dtype)
+        assert texels.ndim == 3 and texels.shape[2] == 4
+        self.textures.append((texels, fmt))
+        self._desc = None
+        return len(self.textures)
+
+    def add_texture_input(self, texture=0, channel=0, wrap_s=abi.WRAP_BLACK, wrap_t=abi.WRAP_BLACK,
+                          scale=(1.0, 1.0, 1.0, 1.0), bias=(0.0, 0.0, 0.0, 0.0), fallback=(0.0, 0.0, 0.0, 1.0),
+                          st_transform=(1.0, 0.0, 0.0, 0.0, 1.0, 0.0)):
+        """A texture input (TextureInput, material.hpp:52-74); `texture` is
+        add_texture's reference (0: none, the lookup returns `fallback`).
+        Returns the reference a material slot names it by (index + 1)."""
+        t = abi.TextureInput()
+        t.texture, t.channel, t.wrap_s, t.wrap_t = texture, channel, wrap_s, wrap_t
+        t.scale[:] = [float(v) for v in scale]
+        t.bias[:] = [float(v) for v in bias]
+        t.fallback[:] = [float(v) for v in fallback]
+        t.st_transform[:] = [float(v) for v in st_transform]
+        self.texture_inputs.append(t)
+        self._desc = None
+        return len(self.texture_inputs)
+
+    def set_texcoords(self, geometry, sets):
+        """Geometry `geometry`'s texture-coordinate sets: (sets, triangles,
+        3, 2) per-corner (s, t)."""
+        sets = np.ascontiguousarray(sets, dtype=F32)
+        assert sets.ndim == 4 and sets.shape[1:] == (self.geometries[geometry][1].shape[0], 3, 2)
+        self.texcoords[geometry] = sets
         self._desc = None
 
     def add_geometry(self, positions, triangles, normals=None):
@@ -149,9 +193,11 @@ class Scene:
         self._desc = None
         return len(self.materials) - 1
 
-    def add_instance(self, geometry, material, world_from_object=None):
+    def add_instance(self, geometry, material, world_from_object=None, texcoord_set=0):
         m = identity() if world_from_object is None else np.asarray(world_from_object, dtype=F32)
         self.instances.append((m.copy(), geometry, material))
+        if texcoord_set:
+            self.instance_texcoords[len(self.instances) - 1] = texcoord_set
         self._desc = None
         return len(self.instances) - 1
 
@@ -216,11 +262,15 @@ class Scene:
                                else C.POINTER(C.c_float)())
             geos[i].vertex_count = p.shape[0]
             geos[i].triangle_count = t.shape[0]
+            if i in self.texcoords:
+                geos[i].texcoords = self.texcoords[i].ctypes.data_as(C.POINTER(C.c_float))
+                geos[i].texcoord_sets = self.texcoords[i].shape[0]
         insts = (abi.Instance * max(1, len(self.instances)))()
         for i, (m, g, mat) in enumerate(self.instances):
             insts[i].world_from_object[:] = [float(v) for v in m]
             insts[i].geometry = g
             insts[i].material = mat
+            insts[i].texcoord_set = self.instance_texcoords.get(i, 0)
         mats = (abi.Material * len(self.materials))(*self.materials)
         d = abi.SceneDesc()
         d.geometries = geos
@@ -244,7 +294,20 @@ class Scene:
             lights = (abi.Light * len(self.lights))(*self.lights)
             d.lights = lights
             d.light_count = len(self.lights)
-        self._keep = (geos, insts, mats, env, lights)
+        textures = inputs = None
+        if self.textures:
+            textures = (abi.Texture * len(self.textures))()
+            for i, (texels, fmt) in enumerate(self.textures):
+                textures[i].texels = texels.ctypes.data
+                textures[i].height, textures[i].width = texels.shape[0], texels.shape[1]
+                textures[i].format = fmt
+            d.textures = textures
+            d.texture_count = len(self.textures)
+        if self.texture_inputs:
+            inputs = (abi.TextureInput * len(self.texture_inputs))(*self.texture_inputs)
+            d.texture_inputs = inputs
+            d.texture_input_count = len(self.texture_inputs)
+        self._keep = (geos, insts, mats, env, lights, textures, inputs)
         self._desc = d
         return d
 
@@ -908,4 +971,210 @@ def material_basics(metal50_scale=1.0, size=128):
         placed[0] = placed[5] = placed[10] = 0.4
         placed[12], placed[13] = columns[i % 4], rows[i // 4]
         s.add_instance(ball, s.add_material(material), placed)
+    return s
+
+
+def _texture_image(size, texel):
+    """An 8-bit image of size x size texels, rows from the top, texel(x, y)
+    giving its RGBA codes."""
+    return np.array([[texel(x, y) for x in range(size)] for y in range(size)], dtype=np.uint8)
+
+
+def _transform2d(scale_s, scale_t, degrees, translate_s, translate_t):
+    """A UsdTransform2d's st matrix as the reference's adapter composes it
+    (in double, then rounded): scale, then a counter-clockwise rotation,
+    then the translation; rows (m0 m1 m2), (m3 m4 m5)."""
+    c, s = math.cos(math.radians(degrees)), math.sin(math.radians(degrees))
+    return tuple(float(F32(v)) for v in (c * scale_s, -s * scale_t, translate_s,
+                                         s * scale_s, c * scale_t, translate_t))
+
+
+def material_textures(shifted_repeat=False, size=160):
+    """The reference's material-textures-v1 fixture (SetMaterialTextures,
+    material_fixtures.cpp:390-500 in hydra-lotus), which its golden images
+    validation/reference/material-textures-v1-{mean,variance}.pfm were
+    rendered from: 25 unit cards (scale 0.7, a 5 x 5 grid 0.8 apart) in the
+    material studio, each a UsdPreviewSurface whose base colour (and for
+    some roughness and metallic) is a texture lookup: the 4x4 palette under
+    each wrap mode over coordinates from -0.5 to 1.5, sRGB / raw / auto
+    decoding, a grey ramp, grey-alpha and RGBA channels on roughness and
+    metallic, scale and bias, missing images (fallbacks), a second
+    coordinate set, indexed and turned coordinates, the material's
+    coordinate fallback, an st transform, constants, and a 64x64 checker
+    minified. ``shifted_repeat`` moves the Repeat card's s by 1/8 (the
+    fixture's negative control, ShiftedRepeat: a texel-centre error)."""
+    s = material_studio("material-textures-v1", size)
+
+    def palette(x, y):
+        return (40 + 60 * x, 40 + 60 * y, 200 if (x + y) % 2 == 0 else 60, 255)
+
+    def ramp(x, y):
+        v = 15 + 15 * (x + 4 * y)
+        return (v, v, v, 255)
+
+    def grey_alpha(x, y):
+        v = 50 + 60 * x
+        return (v, v, v, 230 - 60 * y)
+
+    def rgba(x, y):
+        return (220 - 60 * x, 40 + 60 * y, 40 + 60 * ((x + y) % 4), 30 + 65 * x)
+
+    def checker(x, y):
+        v = 255 if (x + y) % 2 == 0 else 0
+        return (v, v, v, 255)
+
+    srgb, unorm = abi.TEXTURE_RGBA8_SRGB, abi.TEXTURE_RGBA8_UNORM
+    tex = {
+        "palette|sRGB": s.add_texture(_texture_image(4, palette), srgb),
+        "palette|raw": s.add_texture(_texture_image(4, palette), unorm),
+        "palette|auto": s.add_texture(_texture_image(4, palette), srgb),
+        "ramp|auto": s.add_texture(_texture_image(4, ramp), unorm),
+        "grey-alpha|auto": s.add_texture(_texture_image(4, grey_alpha), unorm),
+        "rgba|sRGB": s.add_texture(_texture_image(4, rgba), srgb),
+        "rgba|raw": s.add_texture(_texture_image(4, rgba), unorm),
+        "checker|raw": s.add_texture(_texture_image(64, checker), unorm),
+    }
+    clamp, black, rep, mirror = abi.WRAP_CLAMP, abi.WRAP_BLACK, abi.WRAP_REPEAT, abi.WRAP_MIRROR
+
+    def lookup(key, wrap_s=clamp, wrap_t=clamp, **kw):
+        return s.add_texture_input(tex.get(key, 0), wrap_s=wrap_s, wrap_t=wrap_t, **kw)
+
+    def textured(base, texcoords="st", **kw):
+        m = preview_material(**kw)
+        m.lookups[abi.SLOT_BASE_COLOR] = base
+        return m, texcoords
+
+    def constant(**kw):
+        return preview_material(**kw), "st"
+
+    unit = [(0, 0), (1, 0), (1, 1), (0, 1)]
+    wide = [(-0.5, -0.5), (1.5, -0.5), (1.5, 1.5), (-0.5, 1.5)]
+    turned = [(1, 0), (1, 1), (0, 1), (0, 0)]
+    one = {"st": unit}
+    spread = {"st": wide}
+    two = {"st": unit, "uv1": turned}
+
+    grey_alpha_m, _ = textured(lookup("grey-alpha|auto"))
+    grey_alpha_m.lookups[abi.SLOT_ROUGHNESS] = lookup("grey-alpha|auto", channel=3)
+    alpha_m, _ = textured(lookup("rgba|sRGB"))
+    alpha_m.lookups[abi.SLOT_ROUGHNESS] = lookup("rgba|sRGB", channel=3)
+    orm = preview_material(base_color=(0.95, 0.64, 0.54))
+    orm.lookups[abi.SLOT_METALLIC] = lookup("rgba|raw", channel=2)
+    orm.lookups[abi.SLOT_ROUGHNESS] = lookup("rgba|raw", channel=1)
+    missing = lookup("missing|sRGB", scale=(0.5, 0.5, 0.5, 1.0), fallback=(0.9, 0.2, 0.6, 1.0))
+    no_file = lookup("|auto", fallback=(0.2, 0.6, 0.9, 1.0))
+    constant_m, _ = textured(lookup("palette|sRGB"))
+    constant_m.texcoord_fallback[:] = [0.6, 0.3]
+    absent_m, _ = textured(lookup("palette|sRGB"))
+    absent_m.texcoord_fallback[:] = [0.1, 0.9]
+    cards = [
+        ("UseMetadata", textured(lookup("palette|sRGB", black, black)), spread),
+        ("Clamp", textured(lookup("palette|sRGB")), spread),
+        ("Repeat", textured(lookup("palette|sRGB", rep, rep)), spread),
+        ("Mirror", textured(lookup("palette|sRGB", mirror, mirror)), spread),
+        ("Mixed", textured(lookup("palette|sRGB", rep, black)), spread),
+        ("Srgb", textured(lookup("palette|sRGB")), one),
+        ("Raw", textured(lookup("palette|raw")), one),
+        ("Auto", textured(lookup("palette|auto")), one),
+        ("Grey", textured(lookup("ramp|auto")), one),
+        ("GreyAlpha", (grey_alpha_m, "st"), one),
+        ("Alpha", (alpha_m, "st"), one),
+        ("Orm", (orm, "st"), one),
+        ("ScaleBias", textured(lookup("palette|raw", scale=(2.0, 2.0, 2.0, 1.0), bias=(-0.5, -0.5, -0.5, 0.0))),
+         one),
+        ("Missing", textured(missing), one),
+        ("NoFile", textured(no_file), one),
+        ("Vertex", textured(lookup("palette|sRGB")), one),
+        ("Indexed", textured(lookup("palette|sRGB")), {"st": [(1, 0), (0, 0), (0, 1), (1, 1)]}),
+        ("Named", textured(lookup("palette|sRGB"), "uv1"), two),
+        ("Constant", (constant_m, ""), one),
+        ("Absent", (absent_m, "absent"), one),
+        ("Transform2d", textured(lookup("palette|sRGB", st_transform=_transform2d(2, 2, 30, 0.25, 0))), one),
+        ("SecondSource", textured(lookup("palette|sRGB")), two),
+        ("ColourOnScalar", constant(base_color=(0.3, 0.5, 0.7)), one),
+        ("ScalarOnColour", constant(), one),
+        ("Minified", textured(lookup("checker|raw", rep, rep)), one),
+    ]
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (1.6, 0.8, 0.0, -0.8, -1.6)
+    positions = [(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)]
+    for i, (name, (material, set_name), sets) in enumerate(cards):
+        card = s.add_geometry(np.array(positions, dtype=F32), np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+        names = sorted(sets)
+        corners = []
+        for key in names:
+            f = [list(c) for c in sets[key]]
+            if shifted_repeat and name == "Repeat" and key == "st":
+                for c in f:
+                    c[0] = float(F32(c[0]) + F32(0.125))
+            # The fan (0, 1, 2), (0, 2, 3) of the face's four corners.
+            corners.append([[f[0], f[1], f[2]], [f[0], f[2], f[3]]])
+        s.set_texcoords(card, np.array(corners, dtype=F32))
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = placed[5] = placed[10] = 0.7
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        texcoord_set = names.index(set_name) + 1 if set_name in names else 0
+        s.add_instance(card, s.add_material(material), placed, texcoord_set=texcoord_set)
+    return s
+
+
+def texture_cutouts(size=96):
+    """Texture lookups on coverage and emission, in the material studio:
+    cards masked by an 8x8 cutout's alpha at threshold 0.5 and
+    fractionally (threshold 0), a ramp's red as opacity at threshold 0.5,
+    an inverted mask (scale -1, bias 1), a card that glows through a mask,
+    a card whose emission is a texture (and so is each light sample's
+    radiance), and a masked card in front of a half-covered one. For
+    parity of every path with the oracle, not a reference golden."""
+    s = material_studio("texture-cutouts", size)
+
+    def cutout(x, y):
+        dx, dy = 2 * x - 7, 2 * y - 7
+        d = dx * dx + dy * dy
+        return (60 + 20 * x, 200 - 15 * y, 60, 255 if d <= 26 else 96 if d <= 50 else 0)
+
+    def ramp(x, y):
+        v = 15 + 15 * (x + 4 * y)
+        return (v, v, v, 255)
+
+    def palette(x, y):
+        return (40 + 60 * x, 40 + 60 * y, 200 if (x + y) % 2 == 0 else 60, 255)
+
+    cut = s.add_texture(_texture_image(8, cutout), abi.TEXTURE_RGBA8_SRGB)
+    rmp = s.add_texture(_texture_image(4, ramp), abi.TEXTURE_RGBA8_UNORM)
+    pal = s.add_texture(_texture_image(4, palette), abi.TEXTURE_RGBA8_SRGB)
+    clamp, rep = abi.WRAP_CLAMP, abi.WRAP_REPEAT
+
+    def masked(threshold, wrap=clamp):
+        m = preview_material(opacity_threshold=threshold)
+        m.lookups[abi.SLOT_BASE_COLOR] = s.add_texture_input(cut, wrap_s=wrap, wrap_t=wrap)
+        m.lookups[abi.SLOT_OPACITY] = s.add_texture_input(cut, channel=3, wrap_s=wrap, wrap_t=wrap)
+        return m
+
+    ramp_m = preview_material(base_color=(0.2, 0.6, 0.7), opacity_threshold=0.5)
+    ramp_m.lookups[abi.SLOT_OPACITY] = s.add_texture_input(rmp, channel=0, wrap_s=clamp, wrap_t=clamp)
+    inverted = preview_material(base_color=(0.2, 0.6, 0.7), opacity_threshold=0.5)
+    inverted.lookups[abi.SLOT_OPACITY] = s.add_texture_input(
+        cut, channel=3, wrap_s=clamp, wrap_t=clamp, scale=(1, 1, 1, -1), bias=(0, 0, 0, 1))
+    glowing = masked(0.5)
+    glowing.lookups[abi.SLOT_BASE_COLOR] = 0
+    glowing.emission[:] = [1.0, 0.6, 0.2]
+    lamp = preview_material(base_color=(0.1, 0.1, 0.1))
+    lamp.lookups[abi.SLOT_EMISSION] = s.add_texture_input(pal, wrap_s=clamp, wrap_t=clamp, scale=(3, 3, 3, 1))
+    half = preview_material(base_color=(0.7, 0.3, 0.2), opacity=0.5)
+    looks = [masked(0.5), masked(0.0), ramp_m, inverted, glowing, lamp, masked(0.5, rep), half]
+    positions = np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)], dtype=F32)
+    corners = np.array([[[[0, 0], [1, 0], [1, 1]], [[0, 0], [1, 1], [0, 1]]]], dtype=F32)
+    wide = np.array([[[[-0.5, -0.5], [1.5, -0.5], [1.5, 1.5]], [[-0.5, -0.5], [1.5, 1.5], [-0.5, 1.5]]]],
+                    dtype=F32)
+    columns, rows = (-1.2, 0.0, 1.2), (1.2, 0.0, -1.2)
+    for i, material in enumerate(looks):
+        card = s.add_geometry(positions, np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+        s.set_texcoords(card, wide if i == 6 else corners)
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = placed[5] = placed[10] = 1.0
+        placed[12], placed[13] = columns[i % 3], rows[i // 3]
+        if i == 7:
+            placed[14] = -0.3  # behind the masked card at the same place
+            placed[12], placed[13] = columns[0], rows[0]
+        s.add_instance(card, s.add_material(material), placed, texcoord_set=1)
     return s

@@ -73,6 +73,12 @@ typedef struct lotus_geometry {
   const float* normals;       /* NULL, or 9 floats per triangle: corner normals */
   uint32_t vertex_count;
   uint32_t triangle_count;
+  /* Texture-coordinate sets (MeshGeometry::texcoords, in key order): set k's
+   * (s, t) of triangle i's corner c at texcoords[6 * (k * triangle_count +
+   * i) + 2 * c]; NULL when texcoord_sets is 0. */
+  const float* texcoords;
+  uint32_t texcoord_sets;
+  uint32_t reserved;
 } lotus_geometry;
 
 /* One placed mesh: SceneUpdate's instance (extraction.hpp:313-354). */
@@ -80,7 +86,72 @@ typedef struct lotus_instance {
   float world_from_object[16]; /* column-major; the last row must be 0 0 0 1 */
   uint32_t geometry;           /* index into lotus_scene_desc::geometries */
   uint32_t material;           /* index into lotus_scene_desc::materials */
+  /* The texture-coordinate set its material's lookups read (SceneInstance::
+   * texcoords, extraction.hpp:44-48): k > 0 for its geometry's set k - 1,
+   * LOTUS_NO_TEXCOORDS (0) for the material's texcoord_fallback. */
+  uint32_t texcoord_set;
+  uint32_t reserved;
 } lotus_instance;
+
+/* Zero in every index field below means "none", so that a zeroed struct
+ * holds the defaults: no texture-coordinate set, no image, no lookup. */
+#define LOTUS_NO_TEXCOORDS 0u
+
+/* TextureFormat (material.hpp:15-23): texels of 4 bytes (8-bit channels,
+ * the sRGB format's red, green and blue sRGB-encoded, alpha linear) or of
+ * 16 (four floats). */
+#define LOTUS_TEXTURE_RGBA8_UNORM 0u
+#define LOTUS_TEXTURE_RGBA8_SRGB 1u
+#define LOTUS_TEXTURE_RGBA32_FLOAT 2u
+
+/* A decoded image (material.hpp:29-40): rows from the top of the image,
+ * texture coordinates (0, 0) its bottom-left corner. */
+typedef struct lotus_texture {
+  const void* texels;
+  uint32_t width;
+  uint32_t height;
+  uint32_t format;      /* LOTUS_TEXTURE_* */
+  uint32_t reserved;
+} lotus_texture;
+
+/* TextureWrap (material.hpp:42-50). */
+#define LOTUS_WRAP_BLACK 0u   /* transparent black */
+#define LOTUS_WRAP_CLAMP 1u   /* the nearest edge texel */
+#define LOTUS_WRAP_REPEAT 2u
+#define LOTUS_WRAP_MIRROR 3u
+
+#define LOTUS_NO_TEXTURE 0u
+
+/* A texture lookup that drives one material input (TextureInput,
+ * material.hpp:52-74): the texture filtered bilinearly at
+ * (m0 s + m1 t + m2, m3 s + m4 t + m5) of the material's texture
+ * coordinates, times scale plus bias; `fallback`, unscaled, when `texture`
+ * is LOTUS_NO_TEXTURE (a key naming no image). */
+typedef struct lotus_texture_input {
+  uint32_t texture;      /* k > 0: lotus_scene_desc::textures[k - 1]; LOTUS_NO_TEXTURE (0) */
+  uint32_t channel;      /* 0..3, a scalar input's channel */
+  uint32_t wrap_s;       /* LOTUS_WRAP_* */
+  uint32_t wrap_t;
+  float scale[4];
+  float bias[4];
+  float fallback[4];
+  float st_transform[6];
+  uint32_t reserved[2];
+} lotus_texture_input;
+
+/* A material's texture-input slots (material.hpp:266-273): a lookup
+ * replaces the input's constant, clamped into its range. The normal slot
+ * (tangent-space normal maps) is not supported: a material naming a lookup
+ * there fails the scene update. */
+#define LOTUS_SLOT_OPACITY 0u
+#define LOTUS_SLOT_NORMAL 1u
+#define LOTUS_SLOT_BASE_COLOR 2u
+#define LOTUS_SLOT_ROUGHNESS 3u
+#define LOTUS_SLOT_METALLIC 4u
+#define LOTUS_SLOT_EMISSION 5u
+#define LOTUS_SLOT_SPECULAR_COLOR 6u
+#define LOTUS_TEXTURE_SLOTS 7u
+#define LOTUS_NO_LOOKUP 0u
 
 /* UsdPreviewSurface's constants (material.hpp:137-173) plus the material's
  * coverage (material.hpp:103-116). */
@@ -97,6 +168,13 @@ typedef struct lotus_material {
   float opacity_threshold;  /* > 0: binary coverage */
   uint32_t flags;           /* LOTUS_MATERIAL_* */
   uint32_t reserved;
+  /* Per LOTUS_SLOT_*: k > 0 for lotus_scene_desc::texture_inputs[k - 1],
+   * LOTUS_NO_LOOKUP (0) for the constant. */
+  uint32_t lookups[LOTUS_TEXTURE_SLOTS];
+  /* The texture coordinates on an instance with no set
+   * (MaterialGeometry::texcoord_fallback). */
+  float texcoord_fallback[2];
+  uint32_t reserved2;
 } lotus_material;
 
 /* A latitude-longitude environment image (render_world.hpp:122-133): RGBA
@@ -146,6 +224,11 @@ typedef struct lotus_scene_desc {
   float environment_constant[3];  /* the constant environment radiance */
   const lotus_light* lights;      /* analytic lights (the snapshot's Light list); NULL if none */
   uint32_t light_count;
+  /* The images and lookups the materials' texture inputs name. */
+  const lotus_texture* textures;
+  uint32_t texture_count;
+  uint32_t texture_input_count;
+  const lotus_texture_input* texture_inputs;
 } lotus_scene_desc;
 
 /* GpuSceneEvidence, in part. */

@@ -662,6 +662,8 @@ struct Geometry {
   std::vector<F3> positions;
   std::vector<uint32_t> triangles;
   std::vector<F3> normals;  // 3 per triangle, or empty
+  std::vector<float> texcoords;  // set k, triangle i, corner c: 6 * (k * triangles + i) + 2 * c
+  uint32_t texcoord_sets = 0;
   Bvh bvh;
 };
 
@@ -670,7 +672,14 @@ struct Instance {
   float inv[12]; // object_from_world, rows of a 3x4 matrix
   uint32_t geometry;
   uint32_t material;
+  uint32_t texcoord_set;  // lotus_instance::texcoord_set (0: none)
   Box world;
+};
+
+// A texture decoded to linear RGBA floats, rows from the top.
+struct Texture {
+  uint32_t width = 0, height = 0;
+  std::vector<float> rgba;
 };
 
 struct LightRecord {
@@ -723,6 +732,8 @@ struct oracle_scene {
   float environment_selection = 0.0f;
   F3 environment_constant{0, 0, 0};
   Environment env;
+  std::vector<Texture> textures;
+  std::vector<lotus_texture_input> inputs;
 };
 
 namespace {
@@ -773,10 +784,21 @@ inline F3 TransformPoint(const float* m, F3 p) {
            m[2] * p.x + m[6] * p.y + m[10] * p.z + m[14]);
 }
 
-// EmissionEstimate for a constant UsdPreviewSurface (gpu_scene.cpp:144-180).
-double EmissionEstimate(const lotus_material& m) {
+// EmissionEstimate for a UsdPreviewSurface (gpu_scene.cpp:144-180): its
+// constant emission, or a lookup's bound for texels in [0, 1] (its
+// fallback when the lookup names no image).
+double EmissionEstimate(const oracle_scene& s, const lotus_material& m) {
   double e[3];
-  for (int c = 0; c < 3; ++c) e[c] = m.emission[c];
+  const uint32_t lookup = m.lookups[LOTUS_SLOT_EMISSION];
+  for (int c = 0; c < 3; ++c) {
+    if (lookup == LOTUS_NO_LOOKUP) {
+      e[c] = m.emission[c];
+    } else {
+      const lotus_texture_input& in = s.inputs[lookup - 1];
+      e[c] = in.texture == LOTUS_NO_TEXTURE ? std::max(0.0f, in.fallback[c])
+                                           : double{std::max(0.0f, in.scale[c])} + std::max(0.0f, in.bias[c]);
+    }
+  }
   const double factor = 1.0;
   const double mean = factor * (e[0] + e[1] + e[2]) / 3.0;
   return std::isfinite(mean) && mean > 0.0 ? mean : 0.0;
@@ -1081,7 +1103,7 @@ void BuildLightTable(oracle_scene& s) {
   for (size_t index = 0; index < s.instances.size(); ++index) {
     const Instance& inst = s.instances[index];
     const Geometry& g = s.geometries[inst.geometry];
-    const double emission = EmissionEstimate(s.materials[inst.material]);
+    const double emission = EmissionEstimate(s, s.materials[inst.material]);
     const uint32_t tris = static_cast<uint32_t>(g.triangles.size() / 3);
     if (emission <= 0.0 || tris == 0) continue;
     s.light_offsets[index] = static_cast<uint32_t>(s.lights.size());
@@ -1255,18 +1277,108 @@ inline F3 Inverse(F3 d) {
   return V(inv(d.x), inv(d.y), inv(d.z));
 }
 
-// Coverage (scene.slang:393-406): a material's constant opacity.
-inline float Coverage(const oracle_scene& s, uint32_t instance) {
+// A lookup's texel at integer (x, y) after each axis's wrap: transparent
+// black outside the image (LOTUS_WRAP_BLACK), the edge texel, the
+// coordinate modulo the size, or mirrored every size texels (the Vulkan
+// sampler address modes, vulkan_backend.cpp:3038-3053).
+int32_t WrapTexel(int32_t i, int32_t n, uint32_t mode) {
+  if (mode == LOTUS_WRAP_CLAMP) return i < 0 ? 0 : (i >= n ? n - 1 : i);
+  if (mode == LOTUS_WRAP_REPEAT) {
+    const int32_t r = i % n;
+    return r < 0 ? r + n : r;
+  }
+  if (mode == LOTUS_WRAP_MIRROR) {
+    int32_t r = i % (2 * n);
+    if (r < 0) r += 2 * n;
+    return r < n ? r : 2 * n - 1 - r;
+  }
+  return (i < 0 || i >= n) ? -1 : i;
+}
+
+struct Rgba {
+  float v[4];
+};
+
+Rgba TexelAt(const Texture& t, int32_t x, int32_t y, uint32_t wrap_s, uint32_t wrap_t) {
+  const int32_t xi = WrapTexel(x, static_cast<int32_t>(t.width), wrap_s);
+  const int32_t yi = WrapTexel(y, static_cast<int32_t>(t.height), wrap_t);
+  if (xi < 0 || yi < 0) return Rgba{{0.0f, 0.0f, 0.0f, 0.0f}};
+  const float* p = &t.rgba[4 * (size_t{static_cast<uint32_t>(yi)} * t.width + static_cast<uint32_t>(xi))];
+  return Rgba{{p[0], p[1], p[2], p[3]}};
+}
+
+// Lookup (scene.slang:315-328): the bilinear texel at (s, t), texel
+// centres at (i + 1/2) / size and rows from the image's top, times scale
+// plus bias; the unscaled fallback when the input names no image.
+Rgba Lookup(const oracle_scene& s, const lotus_texture_input& in, float st_s, float st_t) {
+  if (in.texture == LOTUS_NO_TEXTURE) return Rgba{{in.fallback[0], in.fallback[1], in.fallback[2], in.fallback[3]}};
+  const float* m = in.st_transform;
+  const float u = m[0] * st_s + m[1] * st_t + m[2];
+  const float v = 1.0f - (m[3] * st_s + m[4] * st_t + m[5]);
+  const Texture& t = s.textures[in.texture - 1];
+  const float x = std::fmin(std::fmax(u * static_cast<float>(t.width) - 0.5f, -16777216.0f), 16777216.0f);
+  const float y = std::fmin(std::fmax(v * static_cast<float>(t.height) - 0.5f, -16777216.0f), 16777216.0f);
+  const float fx = std::floor(x), fy = std::floor(y);
+  const float ax = x - fx, ay = y - fy;
+  const int32_t ix = static_cast<int32_t>(fx), iy = static_cast<int32_t>(fy);
+  const Rgba t00 = TexelAt(t, ix, iy, in.wrap_s, in.wrap_t);
+  const Rgba t10 = TexelAt(t, ix + 1, iy, in.wrap_s, in.wrap_t);
+  const Rgba t01 = TexelAt(t, ix, iy + 1, in.wrap_s, in.wrap_t);
+  const Rgba t11 = TexelAt(t, ix + 1, iy + 1, in.wrap_s, in.wrap_t);
+  const float bx = 1.0f - ax, by = 1.0f - ay;
+  Rgba r;
+  for (int c = 0; c < 4; ++c) {
+    const float top = t00.v[c] * bx + t10.v[c] * ax;
+    const float bottom = t01.v[c] * bx + t11.v[c] * ax;
+    const float f = top * by + bottom * ay;
+    r.v[c] = f * in.scale[c] + in.bias[c];
+  }
+  return r;
+}
+
+inline float Saturate(float x) { return std::fmin(std::fmax(x, 0.0f), 1.0f); }
+
+// HitTexcoords (scene.slang:362-374): the instance's set interpolated with
+// the barycentrics, or the material's fallback.
+void HitTexcoords(const oracle_scene& s, uint32_t instance, uint32_t primitive, float b1, float b2, float& st_s,
+    float& st_t) {
+  const Instance& inst = s.instances[instance];
+  const Geometry& g = s.geometries[inst.geometry];
+  const lotus_material& m = s.materials[inst.material];
+  if (inst.texcoord_set == LOTUS_NO_TEXCOORDS || inst.texcoord_set > g.texcoord_sets) {
+    st_s = m.texcoord_fallback[0];
+    st_t = m.texcoord_fallback[1];
+    return;
+  }
+  const size_t tris = g.triangles.size() / 3;
+  const float* c = &g.texcoords[6 * ((inst.texcoord_set - 1) * tris + primitive)];
+  st_s = c[0] + b1 * (c[2] - c[0]) + b2 * (c[4] - c[0]);
+  st_t = c[1] + b1 * (c[3] - c[1]) + b2 * (c[5] - c[1]);
+}
+
+// Coverage (scene.slang:393-406): the material's opacity, or its lookup's
+// channel at the hit (saturated, 0 where it overflows); binary under a
+// threshold.
+inline float Coverage(const oracle_scene& s, uint32_t instance, uint32_t primitive, float b1, float b2) {
   const lotus_material& m = s.materials[s.instances[instance].material];
-  const float opacity = m.opacity;
+  float opacity = m.opacity;
+  const uint32_t lookup = m.lookups[LOTUS_SLOT_OPACITY];
+  if (lookup != LOTUS_NO_LOOKUP) {
+    float st_s, st_t;
+    HitTexcoords(s, instance, primitive, b1, b2, st_s, st_t);
+    const lotus_texture_input& in = s.inputs[lookup - 1];
+    opacity = Lookup(s, in, st_s, st_t).v[in.channel];
+    opacity = std::isfinite(opacity) ? Saturate(opacity) : 0.0f;
+  }
   const float threshold = m.opacity_threshold;
   if (threshold > 0.0f) return opacity >= threshold ? 1.0f : 0.0f;
   return opacity;
 }
 
 // AcceptSurface (scene.slang:408-413).
-inline bool AcceptSurface(const oracle_scene& s, uint32_t instance, uint32_t& rng) {
-  const float coverage = Coverage(s, instance);
+inline bool AcceptSurface(const oracle_scene& s, uint32_t instance, uint32_t primitive, float b1, float b2,
+    uint32_t& rng) {
+  const float coverage = Coverage(s, instance, primitive, b1, b2);
   if (coverage <= 0.0f) return false;
   if (coverage >= 1.0f) return true;
   return NextRandom(rng) < coverage;
@@ -1351,7 +1463,7 @@ bool Trace(const oracle_scene& s, const Ray& ray, uint32_t& rng, Hit& hit,
         if (found && (t > best || (t == best &&
                 (ii > h.instance || (ii == h.instance && p >= h.primitive)))))
           return true;
-        if (!AcceptSurface(s, ii, rng)) return true;
+        if (!AcceptSurface(s, ii, p, b1, b2, rng)) return true;
         found = true;
         best = t;
         h.instance = ii;
@@ -1371,8 +1483,8 @@ float ShadowTransmittance(const oracle_scene& s, const Ray& ray) {
   float transmittance = 1.0f;
   bool blocked = false;
   Traverse(s, ray,
-      [&](uint32_t ii, uint32_t, float, float, float) {
-        const float coverage = Coverage(s, ii);
+      [&](uint32_t ii, uint32_t p, float, float b1, float b2) {
+        const float coverage = Coverage(s, ii, p, b1, b2);
         if (coverage >= 1.0f) {
           blocked = true;
           return false;
@@ -1432,8 +1544,23 @@ F3 ShadingNormal(const F3* n, float b1, float b2, const float* m, F3 geometric, 
 
 inline float TriangleArea(F3 p0, F3 p1, F3 p2) { return 0.5f * length(cross(p1 - p0, p2 - p0)); }
 
-// ReconstructHit + EvaluatePreview for constant inputs
-// (scene.slang:1408-1449, 1184-1260).
+// PreviewEmission (scene.slang:570-577): the constant, or the lookup's RGB
+// at (st_s, st_t) with negative parts cut.
+F3 PreviewEmission(const oracle_scene& s, const lotus_material& m, float st_s, float st_t) {
+  const uint32_t lookup = m.lookups[LOTUS_SLOT_EMISSION];
+  if (lookup == LOTUS_NO_LOOKUP) return V(m.emission[0], m.emission[1], m.emission[2]);
+  const Rgba v = Lookup(s, s.inputs[lookup - 1], st_s, st_t);
+  return V(std::fmax(v.v[0], 0.0f), std::fmax(v.v[1], 0.0f), std::fmax(v.v[2], 0.0f));
+}
+
+inline bool Textured(const lotus_material& m) {
+  for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k)
+    if (m.lookups[k] != LOTUS_NO_LOOKUP) return true;
+  return false;
+}
+
+// ReconstructHit + EvaluatePreview (scene.slang:1408-1449, 1184-1260): a
+// texture lookup replaces its input's constant, clamped into its range.
 SurfaceHit ReconstructHit(const oracle_scene& s, const Hit& hit, F3 direction) {
   const Instance& inst = s.instances[hit.instance];
   const Geometry& g = s.geometries[inst.geometry];
@@ -1454,8 +1581,30 @@ SurfaceHit ReconstructHit(const oracle_scene& s, const Hit& hit, F3 direction) {
   sh.base_color = V(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
   sh.roughness = mat.roughness;
   sh.metallic = mat.metallic;
-  const F3 emission = V(mat.emission[0], mat.emission[1], mat.emission[2]);
-  const F3 specular = V(mat.specular_color[0], mat.specular_color[1], mat.specular_color[2]);
+  F3 emission = V(mat.emission[0], mat.emission[1], mat.emission[2]);
+  F3 specular = V(mat.specular_color[0], mat.specular_color[1], mat.specular_color[2]);
+  if (Textured(mat)) {
+    float st_s, st_t;
+    HitTexcoords(s, hit.instance, hit.primitive, hit.b1, hit.b2, st_s, st_t);
+    uint32_t k = mat.lookups[LOTUS_SLOT_BASE_COLOR];
+    if (k != LOTUS_NO_LOOKUP) {
+      const Rgba v = Lookup(s, s.inputs[k - 1], st_s, st_t);
+      sh.base_color = V(Saturate(v.v[0]), Saturate(v.v[1]), Saturate(v.v[2]));
+    }
+    k = mat.lookups[LOTUS_SLOT_ROUGHNESS];
+    if (k != LOTUS_NO_LOOKUP)
+      sh.roughness = Saturate(Lookup(s, s.inputs[k - 1], st_s, st_t).v[s.inputs[k - 1].channel]);
+    k = mat.lookups[LOTUS_SLOT_METALLIC];
+    if (k != LOTUS_NO_LOOKUP)
+      sh.metallic = Saturate(Lookup(s, s.inputs[k - 1], st_s, st_t).v[s.inputs[k - 1].channel]);
+    emission = PreviewEmission(s, mat, st_s, st_t);
+    k = mat.lookups[LOTUS_SLOT_SPECULAR_COLOR];
+    if (k != LOTUS_NO_LOOKUP) {
+      const Rgba v = Lookup(s, s.inputs[k - 1], st_s, st_t);
+      if (std::isfinite(v.v[0]) && std::isfinite(v.v[1]) && std::isfinite(v.v[2]))
+        specular = V(Saturate(v.v[0]), Saturate(v.v[1]), Saturate(v.v[2]));
+    }
+  }
   bool entering = true;
   const float transmission = mat.transmission;
   if (transmission > 0.0f) {
@@ -1499,7 +1648,16 @@ LightSample SampleTriangle(const oracle_scene& s, uint32_t light, const LightRec
   const F3 position = p0 + b1 * (p1 - p0) + b2 * (p2 - p0);
   const F3 normal = normalize(cross(p1 - p0, p2 - p0));
   const float area = TriangleArea(p0, p1, p2);
-  const F3 radiance = V(mat.emission[0], mat.emission[1], mat.emission[2]) * Coverage(s, chosen.instance);
+  F3 radiance;
+  if (mat.lookups[LOTUS_SLOT_EMISSION] == LOTUS_NO_LOOKUP && mat.lookups[LOTUS_SLOT_OPACITY] == LOTUS_NO_LOOKUP) {
+    radiance = V(mat.emission[0], mat.emission[1], mat.emission[2]) * Coverage(s, chosen.instance, primitive, b1, b2);
+  } else {
+    // Emission(material, HitTexcoords) * Coverage(hit) at the sampled point
+    // (scene.slang:655-657).
+    float st_s, st_t;
+    HitTexcoords(s, chosen.instance, primitive, b1, b2, st_s, st_t);
+    radiance = PreviewEmission(s, mat, st_s, st_t) * Coverage(s, chosen.instance, primitive, b1, b2);
+  }
   const F3 toward = position - origin;
   const float distance2 = dot(toward, toward);
   if (!(area > 0.0f) || !(distance2 > 0.0f) || MaxComponent(radiance) <= 0.0f) return NoLight();
@@ -2279,6 +2437,10 @@ oracle_scene* oracle_scene_create(const lotus_scene_desc* d, char* error, size_t
       for (size_t k = 0; k < g.normals.size(); ++k)
         g.normals[k] = V(src.normals[3 * k], src.normals[3 * k + 1], src.normals[3 * k + 2]);
     }
+    if (src.texcoord_sets && src.texcoords) {
+      g.texcoord_sets = src.texcoord_sets;
+      g.texcoords.assign(src.texcoords, src.texcoords + 6 * size_t{src.texcoord_sets} * src.triangle_count);
+    }
     std::vector<Box> boxes(src.triangle_count);
     for (uint32_t t = 0; t < src.triangle_count; ++t)
       for (int k = 0; k < 3; ++k) {
@@ -2296,6 +2458,7 @@ oracle_scene* oracle_scene_create(const lotus_scene_desc* d, char* error, size_t
     std::memcpy(inst.m, src.world_from_object, sizeof(inst.m));
     inst.geometry = src.geometry;
     inst.material = src.material;
+    inst.texcoord_set = src.texcoord_set;
     if (src.geometry >= d->geometry_count || src.material >= d->material_count) {
       SetError(error, error_size, "an instance names a missing geometry or material");
       return nullptr;
@@ -2327,6 +2490,33 @@ oracle_scene* oracle_scene_create(const lotus_scene_desc* d, char* error, size_t
     instance_boxes[ii] = world;
   }
   s->tlas.Build(instance_boxes);
+  // Textures decoded to linear RGBA: sRGB codes through the inverse
+  // transfer function (linear below 0.04045, the 2.4 power above, in double),
+  // alpha and unorm codes / 255.
+  float srgb[256];
+  for (int v = 0; v < 256; ++v) {
+    const double c = v / 255.0;
+    srgb[v] = static_cast<float>(c <= 0.04045 ? c / 12.92 : std::pow((c + 0.055) / 1.055, 2.4));
+  }
+  s->textures.resize(d->texture_count);
+  for (uint32_t i = 0; i < d->texture_count; ++i) {
+    const lotus_texture& src = d->textures[i];
+    Texture& t = s->textures[i];
+    t.width = src.width;
+    t.height = src.height;
+    const size_t n = size_t{src.width} * src.height;
+    t.rgba.resize(4 * n);
+    if (src.format == LOTUS_TEXTURE_RGBA32_FLOAT) {
+      const float* f = static_cast<const float*>(src.texels);
+      std::copy(f, f + 4 * n, t.rgba.begin());
+    } else {
+      const uint8_t* b = static_cast<const uint8_t*>(src.texels);
+      for (size_t k = 0; k < 4 * n; ++k)
+        t.rgba[k] = (src.format == LOTUS_TEXTURE_RGBA8_SRGB && k % 4 != 3) ? srgb[b[k]]
+                                                                          : static_cast<float>(b[k] / 255.0);
+    }
+  }
+  s->inputs.assign(d->texture_inputs, d->texture_inputs + d->texture_input_count);
   s->environment_constant = V(d->environment_constant[0], d->environment_constant[1], d->environment_constant[2]);
   if (d->environment && d->environment->texels && d->environment->width && d->environment->height) {
     const lotus_environment& e = *d->environment;
@@ -2515,7 +2705,6 @@ inline bool Finite4(const float* v) {
   return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]) && std::isfinite(v[3]);
 }
 
-inline float Saturate(float x) { return std::fmin(std::fmax(x, 0.0f), 1.0f); }
 
 uint32_t PackAlbedo(F3 c) {
   const uint32_t x = static_cast<uint32_t>(std::rint(Saturate(c.x) * 255.0f));

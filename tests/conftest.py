@@ -45,3 +45,9 @@ def golden():
 def golden_materials():
     """The reference's material-basics-v1 golden images (4096 spp)."""
     return load_golden("material_basics_v1.npz")
+
+
+@pytest.fixture(scope="session")
+def golden_textures():
+    """The reference's material-textures-v1 golden images (4096 spp)."""
+    return load_golden("material_textures_v1.npz")

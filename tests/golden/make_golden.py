@@ -16,6 +16,9 @@ little-endian; ReadPfm, adapters/common/reference.cpp:100-131):
   UsdPreviewSurface balls under a constant dome and a rect light) at
   128x128, 4096 samples per pixel (kMaterialReferenceSamples,
   adapters/headless/main.cpp).
+- material_textures_v1.npz: the material-textures-v1 fixture
+  (adapters/common/material_fixtures.cpp:390-500: 25 texture-mapped cards
+  under the same studio) at 160x160, 4096 samples per pixel.
 """
 
 import os
@@ -28,7 +31,8 @@ REFERENCE = os.environ.get("LOTUS_REFERENCE",
                            os.path.join(HERE, "..", "..", "..", "reference"))
 
 FIXTURES = [("cornell-box", "cornell_box.npz", 1024),
-            ("material-basics-v1", "material_basics_v1.npz", 4096)]
+            ("material-basics-v1", "material_basics_v1.npz", 4096),
+            ("material-textures-v1", "material_textures_v1.npz", 4096)]
 
 
 def read_pfm(path):

@@ -9,6 +9,11 @@ reference's DES-Q5 comparison, and each fixture's negative control.
   to 1, metallic mixes, ior 2.5 and the specular workflow, under a
   constant dome and a rect light; the half-rough copper 10% darker must be
   rejected (DarkerMetal, adapters/common/material_fixtures.cpp).
+- validation/reference/material-textures-v1-{mean,variance}.pfm (4096
+  spp): 25 texture-mapped cards (wrap modes, sRGB / raw decoding, channels
+  on roughness and metallic, scale and bias, fallbacks, coordinate sets and
+  transforms, a minified checker); the Repeat card's coordinates moved by
+  1/8 must be rejected (ShiftedRepeat).
 
 Both were written by the reference's GPU renderer; fixtures in tests/golden.
 """
@@ -55,5 +60,21 @@ def test_oracle_material_basics_negative_control_rejected(oracle_lib, golden_mat
     img = oracle_image(oracle_lib, scenes.material_basics(metal50_scale=0.9),
                        abi.LIGHT_SAMPLING_MIS)
     g = golden_materials
+    c = metrics.compare(img, SPP, g["mean"], g["variance"], g["samples"])
+    assert not c.ok, c
+
+
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+@pytest.mark.parametrize("spp", [16, 256])
+def test_oracle_matches_material_textures_golden(oracle_lib, golden_textures, light_sampling, spp):
+    img = oracle_image(oracle_lib, scenes.material_textures(), light_sampling, spp)
+    g = golden_textures
+    c = metrics.compare(img, spp, g["mean"], g["variance"], g["samples"])
+    assert c.ok, c
+
+
+def test_oracle_material_textures_negative_control_rejected(oracle_lib, golden_textures):
+    img = oracle_image(oracle_lib, scenes.material_textures(shifted_repeat=True), abi.LIGHT_SAMPLING_MIS)
+    g = golden_textures
     c = metrics.compare(img, SPP, g["mean"], g["variance"], g["samples"])
     assert not c.ok, c
