@@ -58,10 +58,11 @@ EXTEND_STATE_BYTES = 72
 # instance entry its 64-byte traversal record.
 NODE_BYTES, TRIANGLE_BYTES, INSTANCE_BYTES = 112, 48, 64
 # DRAM bytes (read + write) per extension ray of k_wf_extend, from an Nsight
-# Compute capture of one launch (the sphere field at 960x540, bounce 1 of
-# the second frame: 354,127 rays, 115.2 MB read + 14.7 MB written, caches
-# flushed before the launch). Scaled by rays to the bench's launches.
-EXTEND_DRAM_BYTES_PER_RAY = 367.0
+# Compute capture of one launch (the sphere field at 960x540, one wave of
+# eight samples, bounce 1: 2,832,833 rays in key order, 499.4 MB read +
+# 63.3 MB written, caches flushed before the launch). Scaled by rays to the
+# bench's launches.
+EXTEND_DRAM_BYTES_PER_RAY = 198.6
 # B200's nominal HBM3e bandwidth (GB/s), for the fraction against it.
 NOMINAL_HBM_GBS = 8000.0
 
@@ -771,7 +772,8 @@ def main():
                 "frac_of_nominal": round(achieved / NOMINAL_HBM_GBS, 4),
                 "traffic": round(EXTEND_DRAM_BYTES_PER_RAY * ext_rays_timed / launches),
                 "traffic_basis": "ncu dram__bytes_read.sum + dram__bytes_write.sum per extension ray "
-                                 "(one 960x540 launch), times this sample's rays per extend launch",
+                                 "(one 960x540 launch of an 8-sample wave), times this wave's rays per extend "
+                                 "launch",
                 "bytes_per_ray": round(per_ray, 1),
                 "nodes_per_ray": round(counted.node_visits[1] / n_ext, 2),
                 "triangles_per_ray": round(counted.triangle_visits[1] / n_ext, 2),
