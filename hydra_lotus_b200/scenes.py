@@ -1178,3 +1178,208 @@ def texture_cutouts(size=96):
             placed[12], placed[13] = columns[0], rows[0]
         s.add_instance(card, s.add_material(material), placed, texcoord_set=1)
     return s
+
+
+# The coarse polygon sphere of the reference's material fixtures
+# (CoarseSphere, material_fixtures.cpp:594-628 in hydra-lotus): 16 segments,
+# 8 rings, faces counter-clockwise seen from outside, points rounded to six
+# decimals (Fixed) as its USD files store them.
+_COARSE_SEGMENTS, _COARSE_RINGS = 16, 8
+
+
+def _fixed(v):
+    return float(F32(round(v * 1e6) / 1e6 + 0.0))
+
+
+def coarse_sphere_polygons():
+    """(points in double, faces as vertex lists)."""
+    points = [(0.0, 1.0, 0.0)]
+    for i in range(1, _COARSE_RINGS):
+        theta = math.pi * i / _COARSE_RINGS
+        for j in range(_COARSE_SEGMENTS):
+            phi = 2 * math.pi * j / _COARSE_SEGMENTS
+            points.append((math.sin(theta) * math.cos(phi), math.cos(theta), -math.sin(theta) * math.sin(phi)))
+    points.append((0.0, -1.0, 0.0))
+    bottom = len(points) - 1
+
+    def ring(i, j):
+        return 1 + (i - 1) * _COARSE_SEGMENTS + j % _COARSE_SEGMENTS
+
+    faces = [[0, ring(1, j), ring(1, j + 1)] for j in range(_COARSE_SEGMENTS)]
+    for i in range(1, _COARSE_RINGS - 1):
+        for j in range(_COARSE_SEGMENTS):
+            faces.append([ring(i, j), ring(i + 1, j), ring(i + 1, j + 1), ring(i, j + 1)])
+    faces += [[ring(_COARSE_RINGS - 1, j), bottom, ring(_COARSE_RINGS - 1, j + 1)] for j in range(_COARSE_SEGMENTS)]
+    return points, faces
+
+
+def coarse_sphere_corners(faces):
+    """Each triangle corner as the adapter's fan triangulation makes them
+    (right-handed faces): (vertex, face, face-vertex index)."""
+    corners, first = [], 0
+    for f, vertices in enumerate(faces):
+        for k in range(1, len(vertices) - 1):
+            for i in (0, k, k + 1):
+                corners.append((vertices[i], f, first + i))
+        first += len(vertices)
+    return corners
+
+
+def coarse_sphere_latlong(scale=(4.0, 2.0)):
+    """The coarse sphere's (s, t) per face vertex in face order, times
+    `scale` (LatLong, material_fixtures.cpp:632-656)."""
+    seg, rings = float(_COARSE_SEGMENTS), float(_COARSE_RINGS)
+    out = []
+
+    def st(s, t):
+        out.append((float(F32(s * scale[0])), float(F32(t * scale[1]))))
+
+    for j in range(_COARSE_SEGMENTS):
+        st((j + 0.5) / seg, 1)
+        st(j / seg, 1 - 1 / rings)
+        st((j + 1) / seg, 1 - 1 / rings)
+    for i in range(1, _COARSE_RINGS - 1):
+        for j in range(_COARSE_SEGMENTS):
+            top, bot = 1 - i / rings, 1 - (i + 1) / rings
+            st(j / seg, top)
+            st(j / seg, bot)
+            st((j + 1) / seg, bot)
+            st((j + 1) / seg, top)
+    for j in range(_COARSE_SEGMENTS):
+        st(j / seg, 1 / rings)
+        st((j + 0.5) / seg, 0)
+        st((j + 1) / seg, 1 / rings)
+    return out
+
+
+def material_alpha(srgb_alpha=False, size=160):
+    """The reference's material-alpha-v1 fixture (SetMaterialAlpha,
+    material_fixtures.cpp:1056-1200 in hydra-lotus), which its golden images
+    validation/reference/material-alpha-v1-{mean,variance}.pfm were rendered
+    from: 24 cards and a coarse sphere (scale 0.7 / 0.35, a 5 x 5 grid 0.8
+    apart) in the material studio: constant coverage (half, quarter, zero,
+    thresholds below, at and above), texture coverage from RGBA and
+    grey-alpha images, a cutout (masked at 0.5 and fractional), a ramp's red,
+    an inverted mask, a black border, a missing image's fallback, a minified
+    checker, a masked card over a half-covered one, a masked sphere, and
+    emitters through a mask and at half coverage. ``srgb_alpha`` decodes the
+    sRGB images' alpha as colour (the fixture's negative control,
+    SrgbAlpha)."""
+    s = material_studio("material-alpha-v1", size)
+
+    def rgba(x, y):
+        return (220 - 60 * x, 40 + 60 * y, 40 + 60 * ((x + y) % 4), 30 + 65 * x)
+
+    def cutout(x, y):
+        dx, dy = 2 * x - 7, 2 * y - 7
+        d = dx * dx + dy * dy
+        return (60 + 20 * x, 200 - 15 * y, 60, 255 if d <= 26 else 96 if d <= 50 else 0)
+
+    def grey_alpha(x, y):
+        v = 50 + 60 * x
+        return (v, v, v, 230 - 60 * y)
+
+    def ramp(x, y):
+        v = 15 + 15 * (x + 4 * y)
+        return (v, v, v, 255)
+
+    def palette(x, y):
+        return (40 + 60 * x, 40 + 60 * y, 200 if (x + y) % 2 == 0 else 60, 255)
+
+    def checker(x, y):
+        v = 255 if (x + y) % 2 == 0 else 0
+        return (v, v, v, 255)
+
+    srgb, unorm = abi.TEXTURE_RGBA8_SRGB, abi.TEXTURE_RGBA8_UNORM
+
+    def image(size_, texel, fmt):
+        img = _texture_image(size_, texel)
+        if srgb_alpha and fmt == srgb:
+            a = img[..., 3].astype(np.float64) / 255.0
+            lin = np.where(a <= 0.04045, a / 12.92, ((a + 0.055) / 1.055) ** 2.4)
+            img[..., 3] = np.floor(lin * 255.0 + 0.5).astype(np.uint8)
+        return s.add_texture(img, fmt)
+
+    tex = {
+        "rgba|sRGB": image(4, rgba, srgb),
+        "cutout|sRGB": image(8, cutout, srgb),
+        "grey-alpha|auto": image(4, grey_alpha, unorm),
+        "ramp|raw": image(4, ramp, unorm),
+        "palette|sRGB": image(4, palette, srgb),
+        "checker|raw": image(64, checker, unorm),
+    }
+    clamp, rep, black = abi.WRAP_CLAMP, abi.WRAP_REPEAT, abi.WRAP_BLACK
+
+    def lookup(key, wrap=clamp, **kw):
+        return s.add_texture_input(tex.get(key, 0), wrap_s=wrap, wrap_t=wrap, **kw)
+
+    def covered(opacity, threshold=0.0):
+        return preview_material(base_color=(0.2, 0.6, 0.7), opacity=opacity, opacity_threshold=threshold)
+
+    def masked(key, threshold=0.5, wrap=clamp, **kw):
+        m = preview_material(opacity_threshold=threshold)
+        m.lookups[abi.SLOT_BASE_COLOR] = lookup(key, wrap, **kw)
+        m.lookups[abi.SLOT_OPACITY] = lookup(key, wrap, channel=3, **kw)
+        return m
+
+    ramp_m = covered(1.0, 0.5)
+    ramp_m.lookups[abi.SLOT_OPACITY] = lookup("ramp|raw", channel=0)
+    inverted = covered(1.0, 0.5)
+    inverted.lookups[abi.SLOT_OPACITY] = lookup("cutout|sRGB", channel=3, scale=(1, 1, 1, -1), bias=(0, 0, 0, 1))
+    minified = covered(1.0, 0.5)
+    minified.lookups[abi.SLOT_OPACITY] = lookup("checker|raw", rep, channel=0)
+    glowing_mask = masked("cutout|sRGB")
+    glowing_mask.lookups[abi.SLOT_BASE_COLOR] = 0
+    glowing_mask.emission[:] = [1.0, 0.6, 0.2]
+    glowing_half = preview_material(emission=(1.0, 0.6, 0.2), opacity=0.5)
+    looks = {
+        "Half": covered(0.5), "Quarter": covered(0.25), "Zero": covered(0.0), "Presence": covered(0.5),
+        "Clamped": covered(1.0, 1.0), "Below": covered(0.4, 0.5), "Equal": covered(0.5, 0.5),
+        "Above": covered(0.6, 0.5), "NonFinite": covered(1.0), "ThresholdMap": covered(0.5),
+        "Alpha": masked("rgba|sRGB"), "Cutout": masked("cutout|sRGB"), "GreyAlpha": masked("grey-alpha|auto"),
+        "Ramp": ramp_m, "NoAlpha": masked("palette|sRGB"), "Fractional": masked("cutout|sRGB", 0.0),
+        "Inverted": inverted, "BlackBorder": masked("palette|sRGB", wrap=black),
+        "Missing": masked("missing|sRGB", 0.0, fallback=(0.9, 0.2, 0.6, 0.3)),
+        "Minified": minified, "SphereCutout": masked("cutout|sRGB", wrap=rep),
+        "GlowingMask": glowing_mask, "GlowingHalf": glowing_half,
+    }
+    slot = {name: s.add_material(m) for name, m in looks.items()}
+    display = s.add_material(preview_material(base_color=(0.2, 0.6, 0.7), opacity=0.3))
+
+    card_p = np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)], dtype=F32)
+    card_t = np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32)
+    plain = s.add_geometry(card_p, card_t)
+    mapped = s.add_geometry(card_p, card_t)
+    s.set_texcoords(mapped, np.array([[[[0, 0], [1, 0], [1, 1]], [[0, 0], [1, 1], [0, 1]]]], dtype=F32))
+    wide = s.add_geometry(card_p, card_t)
+    w = [(-0.5, -0.5), (1.5, -0.5), (1.5, 1.5), (-0.5, 1.5)]
+    s.set_texcoords(wide, np.array([[[w[0], w[1], w[2]], [w[0], w[2], w[3]]]], dtype=F32))
+    stacked = s.add_geometry(
+        np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0),
+                  (-0.15, -0.15, 0.4), (0.45, -0.15, 0.4), (0.45, 0.45, 0.4), (-0.15, 0.45, 0.4)], dtype=F32),
+        np.array([[0, 1, 2], [0, 2, 3], [4, 5, 6], [4, 6, 7]], dtype=np.uint32))
+    points, faces = coarse_sphere_polygons()
+    corners = coarse_sphere_corners(faces)
+    fixed = np.array([[_fixed(c) for c in p] for p in points], dtype=F32)
+    tris = np.array([[corners[i][0], corners[i + 1][0], corners[i + 2][0]] for i in range(0, len(corners), 3)],
+                    dtype=np.uint32)
+    normals = np.array([fixed[v] for v, _, _ in corners], dtype=F32).reshape(-1, 3, 3)
+    sphere = s.add_geometry(fixed, tris, normals)
+    latlong = coarse_sphere_latlong()
+    s.set_texcoords(sphere, np.array([latlong[fv] for _, _, fv in corners], dtype=F32).reshape(1, -1, 3, 2))
+    objects = [
+        ("Half", plain), ("Quarter", plain), ("Zero", plain), ("Presence", plain), ("Clamped", plain),
+        ("Below", plain), ("Equal", plain), ("Above", plain), ("NonFinite", plain), ("ThresholdMap", mapped),
+        ("Alpha", mapped), ("Cutout", mapped), ("GreyAlpha", mapped), ("Ramp", mapped), ("NoAlpha", mapped),
+        ("Fractional", mapped), ("Inverted", mapped), ("BlackBorder", wide), ("Missing", mapped),
+        ("Minified", mapped), ("Half", stacked), ("SphereCutout", sphere), ("GlowingMask", mapped),
+        ("GlowingHalf", plain), (None, plain),
+    ]
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (1.6, 0.8, 0.0, -0.8, -1.6)
+    for i, (name, geo) in enumerate(objects):
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = placed[5] = placed[10] = 0.35 if geo == sphere else 0.7
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        has_st = geo in s.texcoords
+        s.add_instance(geo, display if name is None else slot[name], placed, texcoord_set=1 if has_st else 0)
+    return s

@@ -48,6 +48,12 @@ def golden_materials():
 
 
 @pytest.fixture(scope="session")
+def golden_alpha():
+    """The reference's material-alpha-v1 golden images (4096 spp)."""
+    return load_golden("material_alpha_v1.npz")
+
+
+@pytest.fixture(scope="session")
 def golden_textures():
     """The reference's material-textures-v1 golden images (4096 spp)."""
     return load_golden("material_textures_v1.npz")

@@ -5,7 +5,9 @@ EvaluatePreview and Coverage, scene.slang:315-413, 1184-1260).
   both integrators pass DES-Q5 at 16, 256 and 1024 spp, and the
   ShiftedRepeat negative control (the Repeat card's s moved by 1/8, a
   texel-centre error) is rejected.
-- Every path of that fixture, and of a scene of texture-masked coverage
+- The same for material-alpha-v1 (constant and texture coverage, a masked
+  sphere, emitters through a mask) and its SrgbAlpha negative control.
+- Every path of those fixtures, and of a scene of texture-masked coverage
   (threshold and fractional), textured emission (light samples included)
   and an inverted mask, equals the oracle's.
 - Invalid texture references fail the scene update with a detail.
@@ -64,8 +66,35 @@ def test_material_textures_negative_control_rejected(cuda, renderer, golden_text
 
 
 @pytest.mark.parametrize("integrator", INTEGRATORS)
+def test_material_alpha_matches_reference_golden(cuda, renderer, golden_alpha, integrator):
+    scene = scenes.material_alpha()
+    st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=64, sample_index=1 << 20)
+    g = golden_alpha
+    cuda.check(renderer.update_scene(scene), "update_scene")
+    rendered = 0
+    for level in (16, 256, 1024):
+        res, color = renderer.render_scene(scene.frame(st, level - rendered))
+        cuda.check(res, "render_scene")
+        rendered = level
+        c = metrics.compare(color, level, g["mean"], g["variance"], g["samples"])
+        print(level, c)
+        assert c.ok, c
+
+
+def test_material_alpha_negative_control_rejected(cuda, renderer, golden_alpha):
+    scene = scenes.material_alpha(srgb_alpha=True)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=64, sample_index=1 << 20)
+    _, color = render(cuda, renderer, scene, st, frame_count=256)
+    g = golden_alpha
+    c = metrics.compare(color, 256, g["mean"], g["variance"], g["samples"])
+    assert not c.ok, c
+
+
+@pytest.mark.parametrize("integrator", INTEGRATORS)
 @pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
-@pytest.mark.parametrize("scene_name", ["material_textures", "texture_cutouts"])
+@pytest.mark.parametrize("scene_name", ["material_textures", "texture_cutouts", "material_alpha"])
 def test_textured_paths_match_oracle(cuda, renderer, oracle_lib, integrator, light_sampling, scene_name):
     scene = getattr(scenes, scene_name)()
     st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,

@@ -14,6 +14,10 @@ reference's DES-Q5 comparison, and each fixture's negative control.
   on roughness and metallic, scale and bias, fallbacks, coordinate sets and
   transforms, a minified checker); the Repeat card's coordinates moved by
   1/8 must be rejected (ShiftedRepeat).
+- validation/reference/material-alpha-v1-{mean,variance}.pfm (4096 spp):
+  constant and texture coverage (thresholds, fractional, cutouts, a
+  masked sphere, emitters through a mask); the sRGB images' alpha decoded
+  as colour must be rejected (SrgbAlpha).
 
 Both were written by the reference's GPU renderer; fixtures in tests/golden.
 """
@@ -76,5 +80,21 @@ def test_oracle_matches_material_textures_golden(oracle_lib, golden_textures, li
 def test_oracle_material_textures_negative_control_rejected(oracle_lib, golden_textures):
     img = oracle_image(oracle_lib, scenes.material_textures(shifted_repeat=True), abi.LIGHT_SAMPLING_MIS)
     g = golden_textures
+    c = metrics.compare(img, SPP, g["mean"], g["variance"], g["samples"])
+    assert not c.ok, c
+
+
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+@pytest.mark.parametrize("spp", [16, 256])
+def test_oracle_matches_material_alpha_golden(oracle_lib, golden_alpha, light_sampling, spp):
+    img = oracle_image(oracle_lib, scenes.material_alpha(), light_sampling, spp)
+    g = golden_alpha
+    c = metrics.compare(img, spp, g["mean"], g["variance"], g["samples"])
+    assert c.ok, c
+
+
+def test_oracle_material_alpha_negative_control_rejected(oracle_lib, golden_alpha):
+    img = oracle_image(oracle_lib, scenes.material_alpha(srgb_alpha=True), abi.LIGHT_SAMPLING_MIS)
+    g = golden_alpha
     c = metrics.compare(img, SPP, g["mean"], g["variance"], g["samples"])
     assert not c.ok, c
