@@ -140,7 +140,7 @@ class Material(C.Structure):
         ("reserved", C.c_uint32),
         ("lookups", C.c_uint32 * 7),  # per SLOT_*: k > 0 for texture_inputs[k - 1]; 0: the constant
         ("texcoord_fallback", C.c_float * 2),
-        ("reserved2", C.c_uint32),
+        ("normal", C.c_float * 3),  # tangent-space shading normal; all zero: (0, 0, 1)
     ]
 
 

@@ -956,12 +956,9 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
         detail = "material " + std::to_string(i) + " names a missing texture input";
         return false;
       }
-    if (m.lookups[LOTUS_SLOT_NORMAL] != LOTUS_NO_LOOKUP) {
-      detail = "material " + std::to_string(i) + " has a normal-map lookup, which this backend does not support";
-      return false;
-    }
-    if (!std::isfinite(m.texcoord_fallback[0]) || !std::isfinite(m.texcoord_fallback[1])) {
-      detail = "material " + std::to_string(i) + " has a non-finite texture-coordinate fallback";
+    if (!std::isfinite(m.texcoord_fallback[0]) || !std::isfinite(m.texcoord_fallback[1]) ||
+        !std::isfinite(m.normal[0]) || !std::isfinite(m.normal[1]) || !std::isfinite(m.normal[2])) {
+      detail = "material " + std::to_string(i) + " has a non-finite texture-coordinate fallback or normal";
       return false;
     }
   }
@@ -1305,7 +1302,8 @@ bool upload_textures(Renderer& R, const lotus_scene_desc& s, std::string& detail
       ml.slot[k] = m.lookups[k] == LOTUS_NO_LOOKUP ? kNoTexture : m.lookups[k] - 1;
     ml.fallback_s = m.texcoord_fallback[0];
     ml.fallback_t = m.texcoord_fallback[1];
-    ml.reserved[0] = ml.reserved[1] = ml.reserved[2] = 0u;
+    const bool zero = m.normal[0] == 0.0f && m.normal[1] == 0.0f && m.normal[2] == 0.0f;
+    for (int k = 0; k < 3; ++k) ml.normal[k] = zero ? (k == 2 ? 1.0f : 0.0f) : m.normal[k];
   }
   std::vector<float2> coords;
   h.texcoord_base.assign(s.geometry_count, 0);
@@ -1472,6 +1470,10 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
     uint32_t flags = m.flags & (LOTUS_MATERIAL_SPECULAR_WORKFLOW | LOTUS_MATERIAL_THIN_WALLED);
     for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k)
       if (m.lookups[k] != LOTUS_NO_LOOKUP) flags |= kMaterialTextured;
+    // A constant tangent-space normal other than the identity (all zero
+    // stands for the identity).
+    if (!(m.normal[0] == 0.0f && m.normal[1] == 0.0f && (m.normal[2] == 0.0f || m.normal[2] == 1.0f)))
+      flags |= kMaterialTextured;
     if (m.lookups[LOTUS_SLOT_OPACITY] != LOTUS_NO_LOOKUP) flags |= kMaterialOpacityTextured;
     float fbits;
     std::memcpy(&fbits, &flags, 4);

@@ -109,6 +109,8 @@ static_assert(sizeof(MaterialRecord) == 80, "material record is 80 bytes");
 // has one.
 constexpr uint32_t kMaterialTextured = 1u << 8;
 constexpr uint32_t kMaterialOpacityTextured = 1u << 9;
+// kMaterialTextured is set too for a constant tangent-space normal other
+// than (0, 0, 1), which MaterialLookups::normal holds.
 
 // A texture input (TextureInputRecord, scene.slang:44-55): the texture's
 // index (kNoTexture: the fallback), channel and wrap modes, then scale,
@@ -134,7 +136,7 @@ struct alignas(16) MaterialLookups {
   uint32_t slot[LOTUS_TEXTURE_SLOTS];
   float fallback_s;
   float fallback_t;
-  uint32_t reserved[3];
+  float normal[3];  // the constant tangent-space normal
 };
 static_assert(sizeof(MaterialLookups) == 48, "MaterialLookups is 48 bytes");
 

@@ -45,6 +45,66 @@ __device__ __forceinline__ F3 shading_normal(const float* n, float b1, float b2,
 
 __device__ __forceinline__ float saturate1(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
 
+// TangentFrame (scene.slang:490-538): the texture coordinates'
+// differentials in world space, orthonormalized about the interpolated
+// shading normal, keeping the handedness of mirrored coordinates and
+// transforms; a frame about the normal alone where the instance has no
+// coordinates or they are degenerate or ill-conditioned. A normal-map
+// lookup (L non-null) transforms the differentials as its coordinates.
+__device__ __forceinline__ Frame tangent_frame(const SceneView& S, uint32_t instance, const TextureLookup* L,
+    uint32_t primitive, F3 edge1, F3 edge2, F3 normal) {
+  Frame basis = make_frame(normal);
+  const uint32_t base = S.inst_texcoords[instance];
+  if (base == kNoTexture) return basis;
+  const float2* c = S.texcoords + base + 3 * (size_t)primitive;
+  const float2 st0 = c[0], st1 = c[1], st2 = c[2];
+  float u1 = st1.x - st0.x, v1 = st1.y - st0.y, u2 = st2.x - st0.x, v2 = st2.y - st0.y;
+  if (L != nullptr) {
+    const float a1 = L->st_s.x * u1 + L->st_s.y * v1, b1 = L->st_t.x * u1 + L->st_t.y * v1;
+    const float a2 = L->st_s.x * u2 + L->st_s.y * v2, b2 = L->st_t.x * u2 + L->st_t.y * v2;
+    u1 = a1;
+    v1 = b1;
+    u2 = a2;
+    v2 = b2;
+  }
+  const float uv_scale = fmaxf(fmaxf(fabsf(u1), fabsf(v1)), fmaxf(fabsf(u2), fabsf(v2)));
+  const float edge_scale = fmaxf(fmaxf(fmaxf(fabsf(edge1.x), fabsf(edge1.y)), fabsf(edge1.z)),
+      fmaxf(fmaxf(fabsf(edge2.x), fabsf(edge2.y)), fabsf(edge2.z)));
+  if (!(uv_scale > 0.0f) || isinf(uv_scale) || !(edge_scale > 0.0f) || isinf(edge_scale)) return basis;
+  u1 = u1 / uv_scale;
+  v1 = v1 / uv_scale;
+  u2 = u2 / uv_scale;
+  v2 = v2 / uv_scale;
+  edge1 = V(edge1.x / edge_scale, edge1.y / edge_scale, edge1.z / edge_scale);
+  edge2 = V(edge2.x / edge_scale, edge2.y / edge_scale, edge2.z / edge_scale);
+  const float determinant = u1 * v2 - v1 * u2;
+  if (!(fabsf(determinant) > 1e-8f)) return basis;
+  const float orientation = determinant < 0.0f ? -1.0f : 1.0f;
+  F3 tangent = orientation * (edge1 * v2 - edge2 * v1);
+  const F3 bitangent = orientation * (edge2 * u1 - edge1 * u2);
+  tangent = tangent - normal * dot(normal, tangent);
+  const float length2 = dot(tangent, tangent);
+  if (!(length2 > 1e-16f) || isinf(length2)) return basis;
+  basis.t = tangent * rsqrt_rn(length2);
+  basis.b = cross(normal, basis.t);
+  if (dot(basis.b, bitangent) < 0.0f) basis.b = -basis.b;
+  return basis;
+}
+
+// MappedNormal (scene.slang:541-556): the tangent-space normal through the
+// frame, turned to the geometric side; the frame's normal where the input
+// is zero or non-finite or the mapped normal faces away from the ray.
+__device__ __forceinline__ F3 mapped_normal(F3 tangent_normal, const Frame& basis, F3 geometric, F3 direction) {
+  const float magnitude = fmaxf(fmaxf(fabsf(tangent_normal.x), fabsf(tangent_normal.y)), fabsf(tangent_normal.z));
+  if (!(magnitude > 0.0f) || !isfinite(tangent_normal.x) || !isfinite(tangent_normal.y) ||
+      !isfinite(tangent_normal.z))
+    return basis.n;
+  F3 shading = normalize(basis.to_world(V(tangent_normal.x / magnitude, tangent_normal.y / magnitude,
+      tangent_normal.z / magnitude)));
+  if (dot(shading, geometric) < 0.0f) shading = -shading;
+  return dot(shading, direction) < 0.0f ? shading : basis.n;
+}
+
 // PreviewEmission (scene.slang:570-577): the constant, or the lookup's RGB
 // at (s, t), negative parts cut.
 __device__ __forceinline__ F3 preview_emission(const SceneView& S, const MaterialRecord& mat,
@@ -101,11 +161,25 @@ __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32
     if (k != kNoTexture)
       sh.metallic = saturate1(lookup_channel(texture_lookup(S, S.lookups[k], s, t), S.lookups[k].channel));
     emission = preview_emission(S, mat, ml, s, t);
+    F3 tangent_normal = V(ml.normal[0], ml.normal[1], ml.normal[2]);
+    const uint32_t normal_lookup = ml.slot[LOTUS_SLOT_NORMAL];
+    if (normal_lookup != kNoTexture) {
+      const float4 v = texture_lookup(S, S.lookups[normal_lookup], s, t);
+      tangent_normal = V(fminf(fmaxf(v.x, -1.0f), 1.0f), fminf(fmaxf(v.y, -1.0f), 1.0f),
+          fminf(fmaxf(v.z, -1.0f), 1.0f));
+    }
     k = ml.slot[LOTUS_SLOT_SPECULAR_COLOR];
     if (k != kNoTexture) {
       const float4 v = texture_lookup(S, S.lookups[k], s, t);
       if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z)) specular = V(saturate1(v.x), saturate1(v.y), saturate1(v.z));
     }
+    // The constant-material path is kept exactly when the input is the
+    // identity.
+    if (tangent_normal.x != 0.0f || tangent_normal.y != 0.0f || tangent_normal.z != 1.0f)
+      sh.shading_normal = mapped_normal(tangent_normal,
+          tangent_frame(S, instance, normal_lookup != kNoTexture ? &S.lookups[normal_lookup] : nullptr, primitive,
+              p1 - p0, p2 - p0, sh.shading_normal),
+          sh.normal, direction);
   }
   const float transmission = mat.transmission.w;
   bool entering = true;

@@ -199,6 +199,7 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
       m.lookups[k] = (uint32_t)inputs.size();
     }
     std::memcpy(m.texcoord_fallback, sm.material.geometry.texcoord_fallback.data(), 8);
+    std::memcpy(m.normal, sm.material.geometry.normal.data(), 12);
     std::memcpy(m.base_color, p.base_color.data(), 12);
     m.roughness = p.roughness;
     std::memcpy(m.emission, p.emission.data(), 12);

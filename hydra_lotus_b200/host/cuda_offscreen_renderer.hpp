@@ -25,12 +25,12 @@
 //   Residency()               the resident scene's device bytes
 // Analytic lights (Lotus::Light) map field for field to lotus_light; the
 // resident textures to lotus_texture, UsdPreviewSurface's texture inputs
-// (opacity, base colour, roughness, metallic, emission, specular colour)
-// to lotus_texture_input, each geometry's texture-coordinate sets in key
-// order and each instance's set. Scene content the backend does not build
-// (normal maps, material models other than UsdPreviewSurface) makes
-// UpdateScene Fail with the reason, as the reference Fails on unsupported
-// content.
+// (opacity, normal, base colour, roughness, metallic, emission, specular
+// colour) to lotus_texture_input, each geometry's texture-coordinate sets
+// in key order and each instance's set. Scene content the backend does not
+// build (material models other than UsdPreviewSurface, vertex colours)
+// makes UpdateScene Fail with the reason, as the reference Fails on
+// unsupported content.
 #pragma once
 
 #include <lotus/vulkan_backend.hpp>

@@ -1383,3 +1383,189 @@ def material_alpha(srgb_alpha=False, size=160):
         has_st = geo in s.texcoords
         s.add_instance(geo, display if name is None else slot[name], placed, texcoord_set=1 if has_st else 0)
     return s
+
+
+def coarse_sphere_polygons_reversed():
+    """The coarse sphere with each face's vertices reversed, as a
+    left-handed mesh lists them (CoarseSphere(true))."""
+    points, faces = coarse_sphere_polygons()
+    return points, [list(reversed(f)) for f in faces]
+
+
+def coarse_sphere_corners_left(faces):
+    """Corners of a left-handed mesh as the adapter triangulates it: a
+    quad as (v2, v1, v0), (v2, v0, v3), other faces as (v0, v[k + 1], v[k])
+    (Polygons::Corners, material_fixtures.cpp:525-549)."""
+    corners, first = [], 0
+    for f, vertices in enumerate(faces):
+        if len(vertices) == 4:
+            tris = [(2, 1, 0), (2, 0, 3)]
+        else:
+            tris = [(0, k + 1, k) for k in range(1, len(vertices) - 1)]
+        for tri in tris:
+            for i in tri:
+                corners.append((vertices[i], f, first + i))
+        first += len(vertices)
+    return corners
+
+
+def coarse_smooth_normals(points, faces, left_handed=False):
+    """Storm's smooth vertex normals in float (SmoothNormals,
+    material_fixtures.cpp:565-589): per vertex the sum over its faces'
+    corners of cross(next - vertex, previous - vertex) (the two swapped on
+    a left-handed face), divided by the float length."""
+    pos = [[F32(_fixed(c)) for c in p] for p in points]
+    sums = [[F32(0.0)] * 3 for _ in points]
+    for vertices in faces:
+        n = len(vertices)
+        for i in range(n):
+            curr = pos[vertices[i]]
+            prev = pos[vertices[(i + n - 1) % n]]
+            nxt = pos[vertices[(i + 1) % n]]
+            if left_handed:
+                prev, nxt = nxt, prev
+            a = [nxt[k] - curr[k] for k in range(3)]
+            b = [prev[k] - curr[k] for k in range(3)]
+            s = sums[vertices[i]]
+            sums[vertices[i]] = [s[0] + (a[1] * b[2] - a[2] * b[1]), s[1] + (a[2] * b[0] - a[0] * b[2]),
+                                 s[2] + (a[0] * b[1] - a[1] * b[0])]
+    out = []
+    for s in sums:
+        length = np.sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2])
+        scale = 1.0 / float(max(length, F32(1e-10)))
+        out.append([float(F32(float(c) * scale)) for c in s])
+    return out
+
+
+def material_normals(flipped_green=False, size=160):
+    """The reference's material-normals-v1 fixture (SetMaterialNormals,
+    material_fixtures.cpp:692-828 in hydra-lotus), which its golden images
+    validation/reference/material-normals-v1-{mean,variance}.pfm were
+    rendered from: coarse spheres (scale 0.35) with faceted, per-vertex,
+    face-uniform, computed (Storm's smooth normals, right- and left-handed)
+    and inward corner normals, and cards (scale 0.7) and spheres with
+    tangent-space normal maps: raw, sRGB-decoded, unscaled and DirectX
+    images, a constant normal in the normal-only frame, an absent
+    coordinate set, mirrored and rotated coordinates, mirrored and
+    stretched transforms, and a glossy copper sphere. ``flipped_green``
+    reads the Mapped look's map with green negated (the fixture's negative
+    control, FlippedGreen)."""
+    s = material_studio("material-normals-v1", size)
+
+    def tilts(x, y):
+        return (32 + 64 * x, 224 - 64 * y, 200, 255)
+
+    def tilts_dx(x, y):
+        return (32 + 64 * x, 31 + 64 * y, 200, 255)
+
+    raw = s.add_texture(_texture_image(4, tilts), abi.TEXTURE_RGBA8_UNORM)
+    auto = s.add_texture(_texture_image(4, tilts), abi.TEXTURE_RGBA8_SRGB)
+    dx = s.add_texture(_texture_image(4, tilts_dx), abi.TEXTURE_RGBA8_UNORM)
+    clamp, rep = abi.WRAP_CLAMP, abi.WRAP_REPEAT
+
+    def normal_map(texture, wrap=clamp, green=(2.0, -1.0)):
+        return s.add_texture_input(texture, wrap_s=wrap, wrap_t=wrap, scale=(2.0, green[0], 2.0, 1.0),
+                                   bias=(-1.0, green[1], -1.0, 0.0))
+
+    def bumpy(lookup):
+        m = preview_material(base_color=(0.7, 0.7, 0.7), roughness=0.4)
+        if lookup:
+            m.lookups[abi.SLOT_NORMAL] = lookup
+        return m, "st" if lookup else ""
+
+    constant_m, _ = bumpy(0)
+    constant_m.normal[:] = [0.4, 0.3, 0.866]
+    absent_m, _ = bumpy(normal_map(raw))
+    absent_m.texcoord_fallback[:] = [0.25, 0.75]
+    glossy = preview_material(base_color=(0.95, 0.64, 0.54), roughness=0.25, metallic=1.0)
+    glossy.lookups[abi.SLOT_NORMAL] = normal_map(raw, rep)
+    looks = {
+        "Smooth": (preview_material(base_color=(0.6, 0.6, 0.6), roughness=0.3), ""),
+        "Mapped": bumpy(normal_map(raw, green=(-2.0, 1.0) if flipped_green else (2.0, -1.0))),
+        "Auto": bumpy(normal_map(auto)),
+        "Unscaled": bumpy(s.add_texture_input(raw, wrap_s=clamp, wrap_t=clamp)),
+        "DirectX": bumpy(normal_map(dx, green=(-2.0, 1.0))),
+        "Constant": (constant_m, ""),
+        "AbsentSet": (absent_m, "absent"),
+        "SphereMapped": bumpy(normal_map(raw, rep)),
+        "SphereGlossy": (glossy, "st"),
+    }
+    slot = {name: (s.add_material(m), set_name) for name, (m, set_name) in looks.items()}
+
+    points, faces = coarse_sphere_polygons()
+    corners = coarse_sphere_corners(faces)
+    fixed = np.array([[_fixed(c) for c in p] for p in points], dtype=F32)
+    tris = np.array([[corners[i][0], corners[i + 1][0], corners[i + 2][0]] for i in range(0, len(corners), 3)],
+                    dtype=np.uint32)
+    latlong = coarse_sphere_latlong()
+    mapped_st = np.array([latlong[fv] for _, _, fv in corners], dtype=F32).reshape(1, -1, 3, 2)
+
+    def per_vertex(values):
+        return np.array([values[v] for v, _, _ in corners], dtype=F32).reshape(-1, 3, 3)
+
+    point_normals = [[_fixed(c) for c in p] for p in points]
+    inward = [[_fixed(-c) for c in p] for p in points]
+    face_normals = []
+    for f in faces:
+        c = [sum(points[v][k] for v in f) for k in range(3)]
+        length = math.sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2])
+        face_normals.append([_fixed(c[k] / length) for k in range(3)])
+    uniform = np.array([face_normals[f] for _, f, _ in corners], dtype=F32).reshape(-1, 3, 3)
+    smooth = per_vertex(coarse_smooth_normals(points, faces))
+    rpoints, rfaces = coarse_sphere_polygons_reversed()
+    rcorners = coarse_sphere_corners_left(rfaces)
+    rtris = np.array([[rcorners[i][0], rcorners[i + 1][0], rcorners[i + 2][0]] for i in range(0, len(rcorners), 3)],
+                     dtype=np.uint32)
+    rsmooth = coarse_smooth_normals(rpoints, rfaces, left_handed=True)
+    left_normals = np.array([rsmooth[v] for v, _, _ in rcorners], dtype=F32).reshape(-1, 3, 3)
+
+    def sphere_mesh(normals, mapped):
+        g = s.add_geometry(fixed, tris, normals)
+        if mapped:
+            s.set_texcoords(g, mapped_st)
+        return g
+
+    def card(face):
+        g = s.add_geometry(np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)],
+                                    dtype=F32), np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+        s.set_texcoords(g, np.array([[[face[0], face[1], face[2]], [face[0], face[2], face[3]]]], dtype=F32))
+        return g
+
+    unit = [(0, 0), (1, 0), (1, 1), (0, 1)]
+    turned = [(1, 0), (1, 1), (0, 1), (0, 0)]
+    sphere, card_scale = (0.35, 0.35, 0.35), (0.7, 0.7, 0.7)
+    objects = [
+        ("Smooth", sphere_mesh(None, False), sphere),
+        ("Smooth", sphere_mesh(per_vertex(point_normals), False), sphere),
+        ("Smooth", sphere_mesh(per_vertex(point_normals), False), sphere),
+        ("Smooth", sphere_mesh(uniform, False), sphere),
+        ("Smooth", sphere_mesh(per_vertex(point_normals), False), sphere),
+        ("Smooth", sphere_mesh(smooth, False), sphere),
+        ("Smooth", s.add_geometry(fixed, rtris, left_normals), sphere),
+        ("Smooth", sphere_mesh(smooth, False), sphere),
+        ("Smooth", sphere_mesh(None, False), sphere),
+        ("Smooth", sphere_mesh(per_vertex(inward), False), sphere),
+        ("Mapped", card(unit), card_scale),
+        ("Auto", card(unit), card_scale),
+        ("Unscaled", card(unit), card_scale),
+        ("DirectX", card(unit), card_scale),
+        ("Constant", card(unit), card_scale),
+        ("Mapped", card([(1, 0), (0, 0), (0, 1), (1, 1)]), card_scale),
+        ("Mapped", card(turned), card_scale),
+        ("Mapped", card(unit), (-0.7, 0.7, 0.7)),
+        ("Mapped", card(unit), (0.7, 0.35, 0.7)),
+        ("AbsentSet", card(unit), card_scale),
+        ("SphereMapped", sphere_mesh(per_vertex(point_normals), True), sphere),
+        ("SphereMapped", sphere_mesh(None, True), sphere),
+        ("SphereMapped", sphere_mesh(smooth, True), sphere),
+        ("SphereGlossy", sphere_mesh(per_vertex(point_normals), True), sphere),
+        ("Constant", sphere_mesh(per_vertex(point_normals), True), sphere),
+    ]
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (1.6, 0.8, 0.0, -0.8, -1.6)
+    for i, (look, geo, scale) in enumerate(objects):
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0], placed[5], placed[10] = scale
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        material, set_name = slot[look]
+        s.add_instance(geo, material, placed, texcoord_set=1 if set_name == "st" and geo in s.texcoords else 0)
+    return s

@@ -140,9 +140,9 @@ typedef struct lotus_texture_input {
 } lotus_texture_input;
 
 /* A material's texture-input slots (material.hpp:266-273): a lookup
- * replaces the input's constant, clamped into its range. The normal slot
- * (tangent-space normal maps) is not supported: a material naming a lookup
- * there fails the scene update. */
+ * replaces the input's constant, clamped into its range (the normal slot's
+ * into [-1, 1]: a tangent-space normal, in the frame of the texture
+ * coordinates' differentials about the interpolated shading normal). */
 #define LOTUS_SLOT_OPACITY 0u
 #define LOTUS_SLOT_NORMAL 1u
 #define LOTUS_SLOT_BASE_COLOR 2u
@@ -174,7 +174,10 @@ typedef struct lotus_material {
   /* The texture coordinates on an instance with no set
    * (MaterialGeometry::texcoord_fallback). */
   float texcoord_fallback[2];
-  uint32_t reserved2;
+  /* The tangent-space shading normal (MaterialGeometry::normal, in
+   * [-1, 1]); all zero means the identity (0, 0, 1). A normal-map lookup
+   * (LOTUS_SLOT_NORMAL) replaces it. */
+  float normal[3];
 } lotus_material;
 
 /* A latitude-longitude environment image (render_world.hpp:122-133): RGBA

@@ -1556,7 +1556,67 @@ F3 PreviewEmission(const oracle_scene& s, const lotus_material& m, float st_s, f
 inline bool Textured(const lotus_material& m) {
   for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k)
     if (m.lookups[k] != LOTUS_NO_LOOKUP) return true;
-  return false;
+  return !(m.normal[0] == 0.0f && m.normal[1] == 0.0f && (m.normal[2] == 0.0f || m.normal[2] == 1.0f));
+}
+
+// TangentFrame (scene.slang:490-538): the texture coordinates'
+// differentials in world space, orthonormalized about the interpolated
+// shading normal, keeping mirrored coordinates' handedness; the
+// normal-only frame without usable coordinates. A normal-map lookup
+// transforms the differentials as its coordinates.
+ShadingFrame TangentFrame(const oracle_scene& s, uint32_t instance, const lotus_texture_input* input,
+    uint32_t primitive, F3 edge1, F3 edge2, F3 normal) {
+  ShadingFrame basis = MakeShadingFrame(normal);
+  const Instance& inst = s.instances[instance];
+  const Geometry& g = s.geometries[inst.geometry];
+  if (inst.texcoord_set == LOTUS_NO_TEXCOORDS || inst.texcoord_set > g.texcoord_sets) return basis;
+  const size_t tris = g.triangles.size() / 3;
+  const float* c = &g.texcoords[6 * ((inst.texcoord_set - 1) * tris + primitive)];
+  float u1 = c[2] - c[0], v1 = c[3] - c[1], u2 = c[4] - c[0], v2 = c[5] - c[1];
+  if (input) {
+    const float* m = input->st_transform;
+    const float a1 = m[0] * u1 + m[1] * v1, b1 = m[3] * u1 + m[4] * v1;
+    const float a2 = m[0] * u2 + m[1] * v2, b2 = m[3] * u2 + m[4] * v2;
+    u1 = a1;
+    v1 = b1;
+    u2 = a2;
+    v2 = b2;
+  }
+  const float uv_scale = std::fmax(std::fmax(std::fabs(u1), std::fabs(v1)), std::fmax(std::fabs(u2), std::fabs(v2)));
+  const float edge_scale = std::fmax(std::fmax(std::fmax(std::fabs(edge1.x), std::fabs(edge1.y)), std::fabs(edge1.z)),
+      std::fmax(std::fmax(std::fabs(edge2.x), std::fabs(edge2.y)), std::fabs(edge2.z)));
+  if (!(uv_scale > 0.0f) || std::isinf(uv_scale) || !(edge_scale > 0.0f) || std::isinf(edge_scale)) return basis;
+  u1 = u1 / uv_scale;
+  v1 = v1 / uv_scale;
+  u2 = u2 / uv_scale;
+  v2 = v2 / uv_scale;
+  edge1 = V(edge1.x / edge_scale, edge1.y / edge_scale, edge1.z / edge_scale);
+  edge2 = V(edge2.x / edge_scale, edge2.y / edge_scale, edge2.z / edge_scale);
+  const float determinant = u1 * v2 - v1 * u2;
+  if (!(std::fabs(determinant) > 1e-8f)) return basis;
+  const float orientation = determinant < 0.0f ? -1.0f : 1.0f;
+  F3 tangent = orientation * (edge1 * v2 - edge2 * v1);
+  const F3 bitangent = orientation * (edge2 * u1 - edge1 * u2);
+  tangent = tangent - normal * dot(normal, tangent);
+  const float length2 = dot(tangent, tangent);
+  if (!(length2 > 1e-16f) || std::isinf(length2)) return basis;
+  basis.tangent = tangent * rsqrt(length2);
+  basis.bitangent = cross(normal, basis.tangent);
+  if (dot(basis.bitangent, bitangent) < 0.0f) basis.bitangent = -basis.bitangent;
+  return basis;
+}
+
+// MappedNormal (scene.slang:541-556).
+F3 MappedNormal(F3 tangent_normal, const ShadingFrame& basis, F3 geometric, F3 direction) {
+  const float magnitude =
+      std::fmax(std::fmax(std::fabs(tangent_normal.x), std::fabs(tangent_normal.y)), std::fabs(tangent_normal.z));
+  if (!(magnitude > 0.0f) || !std::isfinite(tangent_normal.x) || !std::isfinite(tangent_normal.y) ||
+      !std::isfinite(tangent_normal.z))
+    return basis.normal;
+  F3 shading = normalize(basis.ToWorld(
+      V(tangent_normal.x / magnitude, tangent_normal.y / magnitude, tangent_normal.z / magnitude)));
+  if (dot(shading, geometric) < 0.0f) shading = -shading;
+  return dot(shading, direction) < 0.0f ? shading : basis.normal;
 }
 
 // ReconstructHit + EvaluatePreview (scene.slang:1408-1449, 1184-1260): a
@@ -1598,12 +1658,25 @@ SurfaceHit ReconstructHit(const oracle_scene& s, const Hit& hit, F3 direction) {
     if (k != LOTUS_NO_LOOKUP)
       sh.metallic = Saturate(Lookup(s, s.inputs[k - 1], st_s, st_t).v[s.inputs[k - 1].channel]);
     emission = PreviewEmission(s, mat, st_s, st_t);
+    const bool zero = mat.normal[0] == 0.0f && mat.normal[1] == 0.0f && mat.normal[2] == 0.0f;
+    F3 tangent_normal = zero ? V(0.0f, 0.0f, 1.0f) : V(mat.normal[0], mat.normal[1], mat.normal[2]);
+    const uint32_t normal_lookup = mat.lookups[LOTUS_SLOT_NORMAL];
+    if (normal_lookup != LOTUS_NO_LOOKUP) {
+      const Rgba v = Lookup(s, s.inputs[normal_lookup - 1], st_s, st_t);
+      tangent_normal = V(std::fmin(std::fmax(v.v[0], -1.0f), 1.0f), std::fmin(std::fmax(v.v[1], -1.0f), 1.0f),
+          std::fmin(std::fmax(v.v[2], -1.0f), 1.0f));
+    }
     k = mat.lookups[LOTUS_SLOT_SPECULAR_COLOR];
     if (k != LOTUS_NO_LOOKUP) {
       const Rgba v = Lookup(s, s.inputs[k - 1], st_s, st_t);
       if (std::isfinite(v.v[0]) && std::isfinite(v.v[1]) && std::isfinite(v.v[2]))
         specular = V(Saturate(v.v[0]), Saturate(v.v[1]), Saturate(v.v[2]));
     }
+    if (tangent_normal.x != 0.0f || tangent_normal.y != 0.0f || tangent_normal.z != 1.0f)
+      sh.shading_normal = MappedNormal(tangent_normal,
+          TangentFrame(s, hit.instance, normal_lookup != LOTUS_NO_LOOKUP ? &s.inputs[normal_lookup - 1] : nullptr,
+              hit.primitive, p1 - p0, p2 - p0, sh.shading_normal),
+          sh.normal, direction);
   }
   bool entering = true;
   const float transmission = mat.transmission;

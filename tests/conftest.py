@@ -54,6 +54,12 @@ def golden_alpha():
 
 
 @pytest.fixture(scope="session")
+def golden_normals():
+    """The reference's material-normals-v1 golden images (4096 spp)."""
+    return load_golden("material_normals_v1.npz")
+
+
+@pytest.fixture(scope="session")
 def golden_textures():
     """The reference's material-textures-v1 golden images (4096 spp)."""
     return load_golden("material_textures_v1.npz")

@@ -23,6 +23,10 @@ little-endian; ReadPfm, adapters/common/reference.cpp:100-131):
   (adapters/common/material_fixtures.cpp:1056-1200: constant and texture
   coverage on 24 cards and a coarse sphere) at 160x160, 4096 samples per
   pixel.
+- material_normals_v1.npz: the material-normals-v1 fixture
+  (adapters/common/material_fixtures.cpp:692-828: corner normals of every
+  kind and tangent-space normal maps on coarse spheres and cards) at
+  160x160, 4096 samples per pixel.
 """
 
 import os
@@ -37,7 +41,8 @@ REFERENCE = os.environ.get("LOTUS_REFERENCE",
 FIXTURES = [("cornell-box", "cornell_box.npz", 1024),
             ("material-basics-v1", "material_basics_v1.npz", 4096),
             ("material-textures-v1", "material_textures_v1.npz", 4096),
-            ("material-alpha-v1", "material_alpha_v1.npz", 4096)]
+            ("material-alpha-v1", "material_alpha_v1.npz", 4096),
+            ("material-normals-v1", "material_normals_v1.npz", 4096)]
 
 
 def read_pfm(path):

@@ -6,7 +6,9 @@ EvaluatePreview and Coverage, scene.slang:315-413, 1184-1260).
   ShiftedRepeat negative control (the Repeat card's s moved by 1/8, a
   texel-centre error) is rejected.
 - The same for material-alpha-v1 (constant and texture coverage, a masked
-  sphere, emitters through a mask) and its SrgbAlpha negative control.
+  sphere, emitters through a mask) and its SrgbAlpha negative control, and
+  for material-normals-v1 (corner normals and tangent-space normal maps)
+  and its FlippedGreen negative control.
 - Every path of those fixtures, and of a scene of texture-masked coverage
   (threshold and fractional), textured emission (light samples included)
   and an inverted mask, equals the oracle's.
@@ -66,11 +68,13 @@ def test_material_textures_negative_control_rejected(cuda, renderer, golden_text
 
 
 @pytest.mark.parametrize("integrator", INTEGRATORS)
-def test_material_alpha_matches_reference_golden(cuda, renderer, golden_alpha, integrator):
-    scene = scenes.material_alpha()
+@pytest.mark.parametrize("fixture", ["alpha", "normals"])
+def test_material_fixture_matches_reference_golden(cuda, renderer, golden_alpha, golden_normals, integrator,
+                                                   fixture):
+    scene = getattr(scenes, f"material_{fixture}")()
     st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
                               max_bounces=64, sample_index=1 << 20)
-    g = golden_alpha
+    g = golden_alpha if fixture == "alpha" else golden_normals
     cuda.check(renderer.update_scene(scene), "update_scene")
     rendered = 0
     for level in (16, 256, 1024):
@@ -82,19 +86,21 @@ def test_material_alpha_matches_reference_golden(cuda, renderer, golden_alpha, i
         assert c.ok, c
 
 
-def test_material_alpha_negative_control_rejected(cuda, renderer, golden_alpha):
-    scene = scenes.material_alpha(srgb_alpha=True)
+@pytest.mark.parametrize("fixture", ["alpha", "normals"])
+def test_material_fixture_negative_control_rejected(cuda, renderer, golden_alpha, golden_normals, fixture):
+    scene = scenes.material_alpha(srgb_alpha=True) if fixture == "alpha" else \
+        scenes.material_normals(flipped_green=True)
     st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
                               max_bounces=64, sample_index=1 << 20)
     _, color = render(cuda, renderer, scene, st, frame_count=256)
-    g = golden_alpha
+    g = golden_alpha if fixture == "alpha" else golden_normals
     c = metrics.compare(color, 256, g["mean"], g["variance"], g["samples"])
     assert not c.ok, c
 
 
 @pytest.mark.parametrize("integrator", INTEGRATORS)
 @pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
-@pytest.mark.parametrize("scene_name", ["material_textures", "texture_cutouts", "material_alpha"])
+@pytest.mark.parametrize("scene_name", ["material_textures", "texture_cutouts", "material_alpha", "material_normals"])
 def test_textured_paths_match_oracle(cuda, renderer, oracle_lib, integrator, light_sampling, scene_name):
     scene = getattr(scenes, scene_name)()
     st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,
@@ -127,12 +133,12 @@ def test_textured_scene_batched_equals_single(cuda):
             assert np.array_equal(colors[k], want), f"scene {k}"
 
 
-@pytest.mark.parametrize("case", ["normal_map", "missing_texture", "missing_input", "missing_set"])
+@pytest.mark.parametrize("case", ["bad_normal", "missing_texture", "missing_input", "missing_set"])
 def test_invalid_texture_references_fail(cuda, case):
     scene = scenes.texture_cutouts(size=16)
-    if case == "normal_map":
-        scene.materials[1].lookups[abi.SLOT_NORMAL] = 1
-        want = "normal-map"
+    if case == "bad_normal":
+        scene.materials[1].normal[:] = [float("nan"), 0.0, 1.0]
+        want = "non-finite"
     elif case == "missing_texture":
         scene.texture_inputs[0].texture = len(scene.textures) + 1
         want = "missing texture"

@@ -18,6 +18,12 @@ reference's DES-Q5 comparison, and each fixture's negative control.
   constant and texture coverage (thresholds, fractional, cutouts, a
   masked sphere, emitters through a mask); the sRGB images' alpha decoded
   as colour must be rejected (SrgbAlpha).
+- validation/reference/material-normals-v1-{mean,variance}.pfm (4096 spp):
+  faceted, per-vertex, uniform, computed (right- and left-handed) and
+  inward corner normals, and tangent-space normal maps (raw, sRGB,
+  unscaled, DirectX, constant, absent set, mirrored, rotated, stretched,
+  glossy); the Mapped look's green negated must be rejected
+  (FlippedGreen).
 
 Both were written by the reference's GPU renderer; fixtures in tests/golden.
 """
@@ -96,5 +102,21 @@ def test_oracle_matches_material_alpha_golden(oracle_lib, golden_alpha, light_sa
 def test_oracle_material_alpha_negative_control_rejected(oracle_lib, golden_alpha):
     img = oracle_image(oracle_lib, scenes.material_alpha(srgb_alpha=True), abi.LIGHT_SAMPLING_MIS)
     g = golden_alpha
+    c = metrics.compare(img, SPP, g["mean"], g["variance"], g["samples"])
+    assert not c.ok, c
+
+
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+@pytest.mark.parametrize("spp", [16, 256])
+def test_oracle_matches_material_normals_golden(oracle_lib, golden_normals, light_sampling, spp):
+    img = oracle_image(oracle_lib, scenes.material_normals(), light_sampling, spp)
+    g = golden_normals
+    c = metrics.compare(img, spp, g["mean"], g["variance"], g["samples"])
+    assert c.ok, c
+
+
+def test_oracle_material_normals_negative_control_rejected(oracle_lib, golden_normals):
+    img = oracle_image(oracle_lib, scenes.material_normals(flipped_green=True), abi.LIGHT_SAMPLING_MIS)
+    g = golden_normals
     c = metrics.compare(img, SPP, g["mean"], g["variance"], g["samples"])
     assert not c.ok, c
