@@ -375,7 +375,7 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
       step_limit = a.step_limit;
     }
     views[k].walk_failure = walk_failure;
-    analytic = analytic || a.view->analytic_count != 0;
+    analytic = analytic || a.view->analytic_count != 0 || a.view->textured != 0;
   }
   SceneTable B;
   B.views = b->views;

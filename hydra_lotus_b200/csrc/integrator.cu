@@ -193,8 +193,9 @@ struct ShadowRequest {
 // crossed, applies Russian roulette, prepares next event estimation's
 // shadow ray (under BSDF sampling, traces the parallel lights' own) and
 // samples the BSDF. Returns whether the path continues along (new_o, new_d).
-// kAnalytic: the scene may have analytic lights; the instantiation without
-// carries none of their code or registers.
+// kAnalytic: the scene may have analytic lights or texture lookups
+// (SceneView::textured); the instantiation without carries none of their
+// code or registers.
 template <bool kAnalytic>
 __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     uint32_t instance, uint32_t tri, float b1, float b2, F3 ray_o, F3 ray_d, uint32_t depth,
@@ -203,7 +204,7 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
   req.pending = false;
   req.inline_shadow = 0;
   uint32_t primitive;
-  const SurfaceHit sh = reconstruct_hit(S, instance, tri, b1, b2, ray_d, &primitive);
+  const SurfaceHit sh = reconstruct_hit<kAnalytic>(S, instance, tri, b1, b2, ray_d, &primitive);
   if (features) {
     // The radiance cache's description of this vertex, seen from the ray.
     const F3 albedo = sh.bsdf.transmission > 0.0f
@@ -377,7 +378,7 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
       start_path(f, px, py, f.sample_index, o, d, tmax, rng);
       ++n_camera;
       Hit hit;
-      if (trace_closest<kCount>(S, o, d, 0.0f, tmax, rng, hit, &vc[0])) {
+      if (trace_closest<kCount, kAnalytic>(S, o, d, 0.0f, tmax, rng, hit, &vc[0])) {
         F3 T = V(1.0f), R = V(0.0f);
         float last_pdf = 0.0f;
         uint32_t flags = 0;
@@ -389,14 +390,14 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
           n_shadow += req.inline_shadow;
           if (req.pending) {
             ++n_shadow;
-            const float tr = trace_shadow<kCount>(S, req.origin, req.direction, 0.0f, req.tmax, &vc[2]);
+            const float tr = trace_shadow<kCount, kAnalytic>(S, req.origin, req.direction, 0.0f, req.tmax, &vc[2]);
             if (tr > 0.0f) R = R + req.throughput * shadow_contribution(req.fl, req.weight, req.pdf, tr);
           }
           if (!cont) break;
           o = no;
           d = nd;
           ++n_extension;
-          if (!trace_closest<kCount>(S, o, d, 0.0f, kFloatMax, rng, hit, &vc[1])) {
+          if (!trace_closest<kCount, kAnalytic>(S, o, d, 0.0f, kFloatMax, rng, hit, &vc[1])) {
             R = miss_path<kAnalytic>(S, f, o, d, flags, last_pdf, T, R);
             break;
           }
@@ -429,7 +430,7 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
 // In a batch (kBatch) one thread per path slot of every scene, in each
 // image's row order or in the table's warp tiles; otherwise 8x4 pixel
 // tiles per warp.
-template <bool kCount, bool kBatch>
+template <bool kCount, bool kBatch, bool kTextured>
 __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, VisitCounters* visits, SceneTable B) {
   TraversalCounters vc = {0, 0, 0};
@@ -483,7 +484,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
       hit.b2 = __uint_as_float(ph.w);
       rng = f.primary_rng[slot];
     } else {
-      found = trace_closest<kCount>(SS, o, d, 0.0f, tmax, rng, hit, &vc);
+      found = trace_closest<kCount, kTextured>(SS, o, d, 0.0f, tmax, rng, hit, &vc);
     }
     if (found) {
       P.direction[slot] = F4(d, tmax);
@@ -679,7 +680,7 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor, uint32_t n, boo
 // ShadowedLight's visibility (transport.slang:82-115) for the shadow queue,
 // as a persistent kernel: each lane walks one shadow ray at a time and adds
 // the light to the path's radiance when the ray arrives.
-template <bool kCount, bool kBatch>
+template <bool kCount, bool kBatch, bool kTextured>
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_shadow(SceneView S, PathState P, Queues Q,
     uint32_t bounce, uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 2];
@@ -702,7 +703,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_shadow(SceneVi
       ++rays;
     }
     if (!__any_sync(kFullWarp, active)) break;
-    if (walk_round<true, kCount>(kBatch ? B.views[scene] : S, W, stack, rng, active, &vc)) {
+    if (walk_round<true, kCount, kTextured>(kBatch ? B.views[scene] : S, W, stack, rng, active, &vc)) {
       active = false;
       const float tr = W.transmittance;
       if (tr > 0.0f) {
@@ -858,7 +859,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneVi
     if (!__any_sync(kFullWarp, active)) break;
     bool emit = false;
     const SceneView& SS = kBatch ? B.views[scene] : S;
-    if (walk_round<false, kCount>(SS, W, stack, rng, active, &vc)) {
+    if (walk_round<false, kCount, kAnalytic>(SS, W, stack, rng, active, &vc)) {
       active = false;
       if (W.found) {
         P.hit[slot] = make_uint4(W.best_instance, W.best_tri, __float_as_uint(W.b1), __float_as_uint(W.b2));
@@ -973,7 +974,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_tail(SceneView S, const FrameCons
     // A path's bounces are bounded by max_bounces (scatter ends it there).
     for (uint32_t bounce = first; bounce <= f.max_bounces; ++bounce) {
       Hit hit;
-      if (!trace_closest(SS, ro, rd, tmin, tmax, rng, hit)) {
+      if (!trace_closest<false, kAnalytic>(SS, ro, rd, tmin, tmax, rng, hit)) {
         R = miss_path<kAnalytic>(SS, f, ro, rd, flags, last_pdf, T, R);
         break;
       }
@@ -984,7 +985,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_tail(SceneView S, const FrameCons
           last_pdf, flags, rng, no, nd, req, slot);
       if (req.pending) {
         atomicAdd(&Q.counts[3 * bounce + 2], 1u);
-        const float tr = trace_shadow(SS, req.origin, req.direction, 0.0f, req.tmax);
+        const float tr = trace_shadow<false, kAnalytic>(SS, req.origin, req.direction, 0.0f, req.tmax);
         if (tr > 0.0f) R = R + req.throughput * shadow_contribution(req.fl, req.weight, req.pdf, tr);
       }
       if (!cont) break;
@@ -1166,7 +1167,8 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
   if (threads == 0) return;
   const uint32_t grid = (threads + kBlock - 1) / kBlock;
   Timed t(profile, stream, 0);
-  const bool analytic = S.analytic_count != 0;
+  // The instantiations with analytic lights' and texture lookups' code.
+  const bool analytic = S.analytic_count != 0 || S.textured != 0;
   if (profile && profile->visits) {
     if (analytic) k_reference_pt<true, true><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
     else k_reference_pt<true, false><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
@@ -1249,12 +1251,14 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid_pixels = (threads + kBlock - 1) / kBlock;
   const SceneTable none;
-  const bool analytic = S.analytic_count != 0;
+  // The instantiations with analytic lights' and texture lookups' code.
+  const bool analytic = S.analytic_count != 0 || S.textured != 0;
   const uint32_t grid_extend = persistent_grid(
       count ? (const void*)k_wf_extend<true, false, false> : (const void*)k_wf_extend<false, false, false>,
       Q.capacity, tuning);
   const uint32_t grid_shadow = persistent_grid(
-      count ? (const void*)k_wf_shadow<true, false> : (const void*)k_wf_shadow<false, false>, Q.capacity, tuning);
+      count ? (const void*)k_wf_shadow<true, false, true> : (const void*)k_wf_shadow<false, false, false>, Q.capacity,
+      tuning);
   // Shading: up to eight waves of resident blocks, grid-striding over
   // longer queues.
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
@@ -1263,8 +1267,9 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     // One camera thread per pixel of each of the wave's samples.
     Timed t(profile, stream, 0);
     const uint32_t grid_camera = (threads * std::max(wave, 1u) + kBlock - 1) / kBlock;
-    if (count) k_wf_camera<true, false><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, visits, none);
-    else k_wf_camera<false, false><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
+    if (count) k_wf_camera<true, false, true><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, visits, none);
+    else if (analytic) k_wf_camera<false, false, true><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
+    else k_wf_camera<false, false, false><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
   }
   // Bounces 0 .. rounds - 1 as wavefront rounds; the paths queued for bounce
   // `rounds` (if any can be) go to the tail kernel. Counting visits keeps
@@ -1319,11 +1324,15 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     {
       Timed t(profile, stream, 3);
       if (count)
-        k_wf_shadow<true, false><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, visits,
+        k_wf_shadow<true, false, true><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, visits,
             none);
       else
-        k_wf_shadow<false, false><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill,
-            nullptr, none);
+        if (analytic)
+          k_wf_shadow<false, false, true><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill,
+              nullptr, none);
+        else
+          k_wf_shadow<false, false, false><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill,
+              nullptr, none);
     }
   }
   if (rounds <= max_bounces) {
@@ -1422,10 +1431,11 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid_slots = (B.total_slots + kBlock - 1) / kBlock;
   const uint32_t grid_extend = persistent_grid((const void*)k_wf_extend<false, true, false>, Q.capacity, tuning);
-  const uint32_t grid_shadow = persistent_grid((const void*)k_wf_shadow<false, true>, Q.capacity, tuning);
+  const uint32_t grid_shadow = persistent_grid((const void*)k_wf_shadow<false, true, true>, Q.capacity, tuning);
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
       8u * persistent_grid((const void*)k_wf_shade<false, true, false>, Q.capacity, TraceTuning()));
-  k_wf_camera<false, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
+  if (B.analytic) k_wf_camera<false, true, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
+  else k_wf_camera<false, true, false><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
   const uint32_t rounds = wavefront_rounds(max_bounces, false, tuning.rounds);
   const bool keyed = Q.keys != nullptr && Q.sorted != nullptr && Q.bins != nullptr;
   const uint32_t grid_scatter = persistent_grid((const void*)k_sort_scatter, Q.capacity, TraceTuning());
@@ -1450,8 +1460,12 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
       k_wf_shade<false, true, true><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, QS, b, no_cache, B);
     else
       k_wf_shade<false, true, false><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, QS, b, no_cache, B);
-    k_wf_shadow<false, true><<<grid_shadow, kBlock, 0, stream>>>(none_view, P, Q, b, fetch + 2 * b + 1, refill,
-        nullptr, B);
+    if (B.analytic)
+      k_wf_shadow<false, true, true><<<grid_shadow, kBlock, 0, stream>>>(none_view, P, Q, b, fetch + 2 * b + 1,
+          refill, nullptr, B);
+    else
+      k_wf_shadow<false, true, false><<<grid_shadow, kBlock, 0, stream>>>(none_view, P, Q, b, fetch + 2 * b + 1,
+          refill, nullptr, B);
   }
   if (rounds <= max_bounces) {
     uint32_t* cursor = fetch + 2 * (max_bounces + 1);

@@ -1137,6 +1137,12 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
   v.inst_trav = R.inst_trav.ptr;
   v.inst_shade = R.inst_shade.ptr;
   v.materials = R.materials.ptr;
+  v.textured = 0;
+  for (const lotus_material& m : h.materials) {
+    bool any = !(m.normal[0] == 0.0f && m.normal[1] == 0.0f && (m.normal[2] == 0.0f || m.normal[2] == 1.0f));
+    for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k) any = any || m.lookups[k] != LOTUS_NO_LOOKUP;
+    if (any) v.textured = 1;
+  }
   v.tex_texels = R.tex_texels.ptr;
   v.tex_info = R.tex_info.ptr;
   v.lookups = R.tex_lookups.ptr;

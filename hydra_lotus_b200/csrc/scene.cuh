@@ -201,6 +201,7 @@ struct SceneView {
   uint32_t light_node_count;
   uint32_t distant_count;
   uint32_t step_limit;       // a walk's step budget (kMaxTraversalSteps)
+  uint32_t textured;         // some material has a texture lookup or a mapped normal
   // Texture lookups: every texture's texels decoded to linear RGBA, one
   // after another; per texture its first texel, width and height; the
   // scene's texture inputs; per material its lookups (read only for
@@ -307,29 +308,43 @@ __device__ __forceinline__ void hit_texcoords(const SceneView& S, uint32_t insta
   t = t0.y + b1 * (t1.y - t0.y) + b2 * (t2.y - t0.y);
 }
 
+// The opacity lookup's channel at a hit, saturated (0 where the lookup
+// overflows). Not inlined: the walks that meet textured coverage are rare,
+// and its registers stay out of the traversal kernels.
+static __device__ __noinline__ float textured_opacity(const SceneView& S, uint32_t material, uint32_t instance,
+    uint32_t primitive, float b1, float b2) {
+  const MaterialLookups ml = S.mat_lookups[material];
+  float s, t;
+  hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
+  const TextureLookup& L = S.lookups[ml.slot[LOTUS_SLOT_OPACITY]];
+  const float opacity = lookup_channel(texture_lookup(S, L, s, t), L.channel);
+  return isfinite(opacity) ? fminf(fmaxf(opacity, 0.0f), 1.0f) : 0.0f;
+}
+
 // Coverage (scene.slang:393-406): the material's opacity, or its lookup's
-// channel at the hit, saturated (0 where the lookup overflows); 0 or 1
-// under a threshold.
+// channel at the hit; 0 or 1 under a threshold.
 __device__ __forceinline__ float material_coverage(const SceneView& S, const MaterialRecord& m, uint32_t material,
     uint32_t instance, uint32_t primitive, float b1, float b2) {
   float opacity = m.coverage.x;
-  if (__float_as_uint(m.coverage.z) & kMaterialOpacityTextured) {
-    const MaterialLookups ml = S.mat_lookups[material];
-    float s, t;
-    hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
-    const TextureLookup& L = S.lookups[ml.slot[LOTUS_SLOT_OPACITY]];
-    opacity = lookup_channel(texture_lookup(S, L, s, t), L.channel);
-    opacity = isfinite(opacity) ? fminf(fmaxf(opacity, 0.0f), 1.0f) : 0.0f;
-  }
+  if (__float_as_uint(m.coverage.z) & kMaterialOpacityTextured)
+    opacity = textured_opacity(S, material, instance, primitive, b1, b2);
   const float threshold = m.coverage.y;
   if (threshold > 0.0f) return opacity >= threshold ? 1.0f : 0.0f;
   return opacity;
 }
 
+// kTextured false: the scene has no textured coverage (SceneView::textured
+// clear), and the walk compiles without the lookup.
+template <bool kTextured = true>
 __device__ __forceinline__ float instance_coverage(const SceneView& S, uint32_t instance, uint32_t primitive,
     float b1, float b2) {
   const uint32_t material = S.inst_trav[instance].material;
-  return material_coverage(S, S.materials[material], material, instance, primitive, b1, b2);
+  const MaterialRecord& m = S.materials[material];
+  if (!kTextured) {
+    if (m.coverage.y > 0.0f) return m.coverage.x >= m.coverage.y ? 1.0f : 0.0f;
+    return m.coverage.x;
+  }
+  return material_coverage(S, m, material, instance, primitive, b1, b2);
 }
 
 __device__ __forceinline__ F3 safe_inverse(F3 d) {
@@ -595,7 +610,7 @@ __device__ __forceinline__ void walk_visit_node(const SceneView& S, Walk& W, Wal
 
 // The triangle tests of BLAS leaf `leaf` (a negative reference). Returns
 // true when an any-hit walk has met an opaque surface.
-template <bool kAnyHit, bool kCount>
+template <bool kAnyHit, bool kCount, bool kTextured = true>
 __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int32_t leaf, uint32_t& rng,
     TraversalCounters* counters) {
   const uint32_t code = ~(uint32_t)leaf;
@@ -611,7 +626,7 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
     if (!(t >= W.tmin) || !(t <= W.best)) continue;
     const uint32_t prim = __float_as_uint(a.w);
     if (kAnyHit) {
-      const float coverage = W.opaque ? 1.0f : instance_coverage(S, W.instance, prim, b1, b2);
+      const float coverage = W.opaque ? 1.0f : instance_coverage<kTextured>(S, W.instance, prim, b1, b2);
       if (coverage >= 1.0f) {
         W.found = true;
         W.transmittance = 0.0f;
@@ -624,7 +639,7 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
            (W.instance == W.best_instance && prim >= __float_as_uint(S.tris[kTriStride * (size_t)W.best_tri].w))))
         continue;
       if (!W.opaque) {
-        const float coverage = instance_coverage(S, W.instance, prim, b1, b2);
+        const float coverage = instance_coverage<kTextured>(S, W.instance, prim, b1, b2);
         if (coverage <= 0.0f) continue;
         if (coverage < 1.0f && !(next_random(rng) < coverage)) continue;
       }
@@ -642,7 +657,7 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
 // W.cur is not an interior node: the exit marker, a BLAS leaf (tested
 // here), or a TLAS leaf (entered). Leaves W.cur at the next reference.
 // Returns true when an any-hit walk has met an opaque surface.
-template <bool kAnyHit, bool kCount>
+template <bool kAnyHit, bool kCount, bool kTextured = true>
 __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStack& stack, uint32_t& rng,
     TraversalCounters* counters) {
   const int32_t cur = W.cur;
@@ -651,7 +666,7 @@ __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStac
     W.w.org = W.origin;
     W.inv = slab_inverse(W.direction);
   } else if (W.in_blas) {
-    if (walk_test_leaf<kAnyHit, kCount>(S, W, cur, rng, counters)) return true;
+    if (walk_test_leaf<kAnyHit, kCount, kTextured>(S, W, cur, rng, counters)) return true;
   } else {
     const uint32_t instance = ~(uint32_t)cur;
     if (kCount) ++counters->instances;
@@ -676,7 +691,7 @@ __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStac
 }
 
 // The whole walk in one call (for kernels with one ray per thread).
-template <bool kAnyHit, bool kCount>
+template <bool kAnyHit, bool kCount, bool kTextured = true>
 __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 direction, float tmin,
     float tmax, uint32_t& rng, Hit& hit, bool& found, TraversalCounters* counters = nullptr) {
   Walk W;
@@ -685,7 +700,7 @@ __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 dire
   while (W.cur != kWalkDone) {
     if (walk_at_node(W)) {
       walk_visit_node<kCount>(S, W, stack, counters);
-    } else if (walk_other<kAnyHit, kCount>(S, W, stack, rng, counters)) {
+    } else if (walk_other<kAnyHit, kCount, kTextured>(S, W, stack, rng, counters)) {
       break;
     }
   }
@@ -709,7 +724,7 @@ constexpr int kRoundNodeLanes = 8;
 // finally each lane not at an interior node takes its exit marker, further
 // leaf or instance entry. Each kind of work thus runs once per round over
 // all the lanes that have it. Returns true for a lane whose walk has ended.
-template <bool kAnyHit, bool kCount>
+template <bool kAnyHit, bool kCount, bool kTextured = true>
 __device__ __forceinline__ bool walk_round(const SceneView& S, Walk& W, WalkStack& stack, uint32_t& rng,
     bool active, TraversalCounters* counters) {
   constexpr unsigned kAll = 0xFFFFFFFFu;
@@ -729,31 +744,31 @@ __device__ __forceinline__ bool walk_round(const SceneView& S, Walk& W, WalkStac
   bool ended = false;
   const bool leaf = active && W.leaf != 0;
   if (__any_sync(kAll, leaf) && leaf) {
-    ended = walk_test_leaf<kAnyHit, kCount>(S, W, W.leaf, rng, counters);
+    ended = walk_test_leaf<kAnyHit, kCount, kTextured>(S, W, W.leaf, rng, counters);
     W.leaf = 0;
   }
   if (active && !ended && W.cur != kWalkDone && !walk_at_node(W))
-    ended = walk_other<kAnyHit, kCount>(S, W, stack, rng, counters);
+    ended = walk_other<kAnyHit, kCount, kTextured>(S, W, stack, rng, counters);
   const bool done = active && (ended || (W.cur == kWalkDone && W.leaf == 0));
   if (done) walk_check_end(S, W);
   return done;
 }
 
-template <bool kCount = false>
+template <bool kCount = false, bool kTextured = true>
 __device__ __forceinline__ bool trace_closest(const SceneView& S, F3 o, F3 d, float tmin,
     float tmax, uint32_t& rng, Hit& hit, TraversalCounters* counters = nullptr) {
   bool found;
-  traverse<false, kCount>(S, o, d, tmin, tmax, rng, hit, found, counters);
+  traverse<false, kCount, kTextured>(S, o, d, tmin, tmax, rng, hit, found, counters);
   return found;
 }
 
-template <bool kCount = false>
+template <bool kCount = false, bool kTextured = true>
 __device__ __forceinline__ float trace_shadow(const SceneView& S, F3 o, F3 d, float tmin,
     float tmax, TraversalCounters* counters = nullptr) {
   uint32_t rng = 0;
   Hit hit;
   bool found;
-  return traverse<true, kCount>(S, o, d, tmin, tmax, rng, hit, found, counters);
+  return traverse<true, kCount, kTextured>(S, o, d, tmin, tmax, rng, hit, found, counters);
 }
 
 }  // namespace lotus

@@ -115,10 +115,71 @@ __device__ __forceinline__ F3 preview_emission(const SceneView& S, const Materia
   return V(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f), fmaxf(v.z, 0.0f));
 }
 
+// EvaluatePreview's textured inputs (scene.slang:1184-1230): each lookup
+// replaces its input's constant, clamped into the input's range, and a
+// tangent-space normal other than the identity maps the shading normal.
+// Not inlined: shading of untextured materials keeps its registers.
+struct TexturedInputs {
+  F3 base_color;
+  float roughness;
+  float metallic;
+  F3 emission;
+  F3 specular;
+  F3 shading_normal;
+};
+
+static __device__ __noinline__ TexturedInputs textured_inputs(const SceneView& S, uint32_t instance, uint32_t material,
+    uint32_t primitive, float b1, float b2, F3 edge1, F3 edge2, F3 geometric, F3 shading, F3 direction) {
+  const MaterialRecord mat = S.materials[material];
+  const MaterialLookups ml = S.mat_lookups[material];
+  TexturedInputs out;
+  out.base_color = V(mat.base_roughness);
+  out.roughness = mat.base_roughness.w;
+  out.metallic = mat.emission_metallic.w;
+  out.specular = V(mat.specular_ior);
+  out.shading_normal = shading;
+  float s, t;
+  hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
+  uint32_t k = ml.slot[LOTUS_SLOT_BASE_COLOR];
+  if (k != kNoTexture) {
+    const float4 v = texture_lookup(S, S.lookups[k], s, t);
+    out.base_color = V(saturate1(v.x), saturate1(v.y), saturate1(v.z));
+  }
+  k = ml.slot[LOTUS_SLOT_ROUGHNESS];
+  if (k != kNoTexture)
+    out.roughness = saturate1(lookup_channel(texture_lookup(S, S.lookups[k], s, t), S.lookups[k].channel));
+  k = ml.slot[LOTUS_SLOT_METALLIC];
+  if (k != kNoTexture)
+    out.metallic = saturate1(lookup_channel(texture_lookup(S, S.lookups[k], s, t), S.lookups[k].channel));
+  out.emission = preview_emission(S, mat, ml, s, t);
+  F3 tangent_normal = V(ml.normal[0], ml.normal[1], ml.normal[2]);
+  const uint32_t normal_lookup = ml.slot[LOTUS_SLOT_NORMAL];
+  if (normal_lookup != kNoTexture) {
+    const float4 v = texture_lookup(S, S.lookups[normal_lookup], s, t);
+    tangent_normal = V(fminf(fmaxf(v.x, -1.0f), 1.0f), fminf(fmaxf(v.y, -1.0f), 1.0f), fminf(fmaxf(v.z, -1.0f), 1.0f));
+  }
+  k = ml.slot[LOTUS_SLOT_SPECULAR_COLOR];
+  if (k != kNoTexture) {
+    const float4 v = texture_lookup(S, S.lookups[k], s, t);
+    if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z)) out.specular = V(saturate1(v.x), saturate1(v.y), saturate1(v.z));
+  }
+  // The constant-material path is kept exactly when the input is the
+  // identity.
+  if (tangent_normal.x != 0.0f || tangent_normal.y != 0.0f || tangent_normal.z != 1.0f)
+    out.shading_normal = mapped_normal(tangent_normal,
+        tangent_frame(S, instance, normal_lookup != kNoTexture ? &S.lookups[normal_lookup] : nullptr, primitive,
+            edge1, edge2, shading),
+        geometric, direction);
+  return out;
+}
+
 // ReconstructHit and EvaluatePreview (scene.slang:1408-1449, 1184-1260).
 // The corners come from the leaf-ordered triangle pool, which holds the
 // geometry's own positions. A texture lookup replaces its input's constant,
 // clamped into the input's range.
+// kTextured false: the scene has no texture lookups (SceneView::textured
+// clear), and the hit compiles without them.
+template <bool kTextured = true>
 __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32_t instance,
     uint32_t tri, float b1, float b2, F3 direction, uint32_t* primitive_out = nullptr) {
   const InstanceShading rec = S.inst_shade[instance];
@@ -145,41 +206,15 @@ __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32
   const uint32_t flags = __float_as_uint(mat.coverage.z);
   F3 emission = V(mat.emission_metallic);
   F3 specular = V(mat.specular_ior);
-  if (flags & kMaterialTextured) {
-    const MaterialLookups ml = S.mat_lookups[rec.material];
-    float s, t;
-    hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
-    uint32_t k = ml.slot[LOTUS_SLOT_BASE_COLOR];
-    if (k != kNoTexture) {
-      const float4 v = texture_lookup(S, S.lookups[k], s, t);
-      sh.base_color = V(saturate1(v.x), saturate1(v.y), saturate1(v.z));
-    }
-    k = ml.slot[LOTUS_SLOT_ROUGHNESS];
-    if (k != kNoTexture)
-      sh.roughness = saturate1(lookup_channel(texture_lookup(S, S.lookups[k], s, t), S.lookups[k].channel));
-    k = ml.slot[LOTUS_SLOT_METALLIC];
-    if (k != kNoTexture)
-      sh.metallic = saturate1(lookup_channel(texture_lookup(S, S.lookups[k], s, t), S.lookups[k].channel));
-    emission = preview_emission(S, mat, ml, s, t);
-    F3 tangent_normal = V(ml.normal[0], ml.normal[1], ml.normal[2]);
-    const uint32_t normal_lookup = ml.slot[LOTUS_SLOT_NORMAL];
-    if (normal_lookup != kNoTexture) {
-      const float4 v = texture_lookup(S, S.lookups[normal_lookup], s, t);
-      tangent_normal = V(fminf(fmaxf(v.x, -1.0f), 1.0f), fminf(fmaxf(v.y, -1.0f), 1.0f),
-          fminf(fmaxf(v.z, -1.0f), 1.0f));
-    }
-    k = ml.slot[LOTUS_SLOT_SPECULAR_COLOR];
-    if (k != kNoTexture) {
-      const float4 v = texture_lookup(S, S.lookups[k], s, t);
-      if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z)) specular = V(saturate1(v.x), saturate1(v.y), saturate1(v.z));
-    }
-    // The constant-material path is kept exactly when the input is the
-    // identity.
-    if (tangent_normal.x != 0.0f || tangent_normal.y != 0.0f || tangent_normal.z != 1.0f)
-      sh.shading_normal = mapped_normal(tangent_normal,
-          tangent_frame(S, instance, normal_lookup != kNoTexture ? &S.lookups[normal_lookup] : nullptr, primitive,
-              p1 - p0, p2 - p0, sh.shading_normal),
-          sh.normal, direction);
+  if (kTextured && (flags & kMaterialTextured)) {
+    const TexturedInputs ti = textured_inputs(S, instance, rec.material, primitive, b1, b2, p1 - p0, p2 - p0,
+        sh.normal, sh.shading_normal, direction);
+    sh.base_color = ti.base_color;
+    sh.roughness = ti.roughness;
+    sh.metallic = ti.metallic;
+    emission = ti.emission;
+    specular = ti.specular;
+    sh.shading_normal = ti.shading_normal;
   }
   const float transmission = mat.transmission.w;
   bool entering = true;
@@ -212,8 +247,23 @@ __device__ __forceinline__ LightSample no_light() {
   return s;
 }
 
+// A textured emitter's radiance at barycentrics (b1, b2) of light-table
+// entry `light`: Emission(material, HitTexcoords) * Coverage(hit)
+// (scene.slang:655-657). Not inlined, as textured_inputs.
+static __device__ __noinline__ F3 textured_light_radiance(const SceneView& S, uint32_t light, float b1, float b2) {
+  const uint32_t instance = S.lights[light].instance;
+  const InstanceShading& rec = S.inst_shade[instance];
+  const uint32_t primitive = light - rec.light_offset;
+  const MaterialRecord& mat = S.materials[rec.material];
+  const MaterialLookups ml = S.mat_lookups[rec.material];
+  float s, t;
+  hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
+  return preview_emission(S, mat, ml, s, t) * material_coverage(S, mat, rec.material, instance, primitive, b1, b2);
+}
+
 // SampleTriangle (scene.slang:632-677), over the light table's
 // world-space corners.
+template <bool kTextured = true>
 __device__ __forceinline__ LightSample sample_triangle(const SceneView& S, uint32_t light,
     float pdf, float ux, float uy, F3 origin) {
   const float root = sqrtf(ux);
@@ -225,19 +275,7 @@ __device__ __forceinline__ LightSample sample_triangle(const SceneView& S, uint3
   const float area = triangle_area(p0, p1, p2);
   const float4 stored = S.light_radiance[light];
   F3 radiance = V(stored);
-  if (stored.w != 0.0f) {
-    // A textured emission or opacity: Emission(material, HitTexcoords) *
-    // Coverage(hit) at the sampled point (scene.slang:655-657).
-    const uint32_t instance = S.lights[light].instance;
-    const InstanceShading& rec = S.inst_shade[instance];
-    const uint32_t primitive = light - rec.light_offset;
-    const MaterialRecord& mat = S.materials[rec.material];
-    const MaterialLookups ml = S.mat_lookups[rec.material];
-    float s, t;
-    hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
-    radiance = preview_emission(S, mat, ml, s, t) *
-               material_coverage(S, mat, rec.material, instance, primitive, b1, b2);
-  }
+  if (kTextured && stored.w != 0.0f) radiance = textured_light_radiance(S, light, b1, b2);
   const F3 toward = position - origin;
   const float distance2 = dot(toward, toward);
   if (!(area > 0.0f) || !(distance2 > 0.0f) || max_component(radiance) <= 0.0f) return no_light();
@@ -615,7 +653,7 @@ __device__ __forceinline__ LightSample sample_light(const SceneView& S, float u0
   if (chosen.instance == kEnvironmentLight) return sample_environment(S, chosen.pdf, u2, u3);
   if (kAnalytic && (chosen.instance & kAnalyticLight) != 0)
     return sample_analytic(S.analytic[chosen.instance & ~kAnalyticLight], chosen.pdf, u2, u3, origin);
-  return sample_triangle(S, light, chosen.pdf, u2, u3, origin);
+  return sample_triangle<kAnalytic>(S, light, chosen.pdf, u2, u3, origin);
 }
 
 // EmitterPdf (scene.slang:1004-1010).
