@@ -980,13 +980,22 @@ def _texture_image(size, texel):
     return np.array([[texel(x, y) for x in range(size)] for y in range(size)], dtype=np.uint8)
 
 
-def _transform2d(scale_s, scale_t, degrees, translate_s, translate_t):
+def _transform2d_double(scale_s, scale_t, degrees, translate_s, translate_t, inner=(1, 0, 0, 0, 1, 0)):
+    c, s = math.cos(degrees * (math.pi / 180.0)), math.sin(degrees * (math.pi / 180.0))
+    local = (c * scale_s, -s * scale_t, translate_s, s * scale_s, c * scale_t, translate_t)
+    i = inner
+    return (local[0] * i[0] + local[1] * i[3], local[0] * i[1] + local[1] * i[4], local[0] * i[2] + local[1] * i[5] + local[2],
+            local[3] * i[0] + local[4] * i[3], local[3] * i[1] + local[4] * i[4], local[3] * i[2] + local[4] * i[5] + local[5])
+
+
+def _transform2d(scale_s, scale_t, degrees, translate_s, translate_t, inner=None):
     """A UsdTransform2d's st matrix as the reference's adapter composes it
     (in double, then rounded): scale, then a counter-clockwise rotation,
-    then the translation; rows (m0 m1 m2), (m3 m4 m5)."""
-    c, s = math.cos(math.radians(degrees)), math.sin(math.radians(degrees))
-    return tuple(float(F32(v)) for v in (c * scale_s, -s * scale_t, translate_s,
-                                         s * scale_s, c * scale_t, translate_t))
+    then the translation, applied after `inner` (a double matrix from
+    _transform2d_double); rows (m0 m1 m2), (m3 m4 m5)."""
+    m = _transform2d_double(scale_s, scale_t, degrees, translate_s, translate_t,
+                            inner if inner is not None else (1, 0, 0, 0, 1, 0))
+    return tuple(float(F32(v)) for v in m)
 
 
 def material_textures(shifted_repeat=False, size=160):
@@ -1568,4 +1577,155 @@ def material_normals(flipped_green=False, size=160):
         placed[12], placed[13] = columns[i % 5], rows[i // 5]
         material, set_name = slot[look]
         s.add_instance(geo, material, placed, texcoord_set=1 if set_name == "st" and geo in s.texcoords else 0)
+    return s
+
+
+def _coarse_smooth_sphere(s):
+    """The coarse polygon sphere with its points (rounded) as corner
+    normals, as a geometry of scene `s`; with the st set when `mapped`."""
+    points, faces = coarse_sphere_polygons()
+    corners = coarse_sphere_corners(faces)
+    fixed = np.array([[_fixed(c) for c in p] for p in points], dtype=F32)
+    tris = np.array([[corners[i][0], corners[i + 1][0], corners[i + 2][0]] for i in range(0, len(corners), 3)],
+                    dtype=np.uint32)
+    normals = np.array([fixed[v] for v, _, _ in corners], dtype=F32).reshape(-1, 3, 3)
+    return s.add_geometry(fixed, tris, normals)
+
+
+def material_transmission(untinted=False, size=160):
+    """The reference's material-transmission-v1 fixture
+    (SetMaterialTransmission, material_fixtures.cpp:1588-1671 in
+    hydra-lotus): 15 objects on the middle three rows in the material
+    studio: solid coarse spheres of smooth, rough, tinted, index-matched and
+    partial transmission, thin-walled cards (smooth, rough, tinted,
+    index-matched, ior 2.42), a mirrored sphere and the translator's no-ops.
+    ``untinted`` drops the tinted sphere's transmission colour (the
+    fixture's negative control, UntintedGlass)."""
+    s = material_studio("material-transmission-v1", size)
+    teal, amber = (0.2, 0.6, 0.7), (0.9, 0.45, 0.15)
+
+    def glass(roughness, tint=(1.0, 1.0, 1.0), thin=False, ior=1.5):
+        return preview_material(base_color=(0.8, 0.8, 0.8), roughness=roughness, transmission=1.0,
+                                transmission_color=tint, ior=ior,
+                                flags=abi.MATERIAL_THIN_WALLED if thin else 0)
+
+    looks = {
+        "Smooth": glass(0.0), "Rough": glass(0.35),
+        "Tinted": glass(0.0, (1.0, 1.0, 1.0) if untinted else amber),
+        "Matched": glass(0.4, (0.5, 0.8, 0.9), ior=1.0),
+        "Partial": preview_material(base_color=teal, roughness=0.15, transmission=0.5, metallic=0.25),
+        "ThinSmooth": glass(0.0, thin=True), "ThinRough": glass(0.4, thin=True),
+        "ThinTinted": glass(0.1, (0.3, 0.7, 0.9), thin=True),
+        "ThinMatched": glass(0.2, (0.9, 0.6, 0.3), thin=True, ior=1.0),
+        "ThinDense": glass(0.0, thin=True, ior=2.42),
+        "Depth": glass(0.0), "NoSpecular": glass(0.2), "Ignored": glass(0.1),
+        "Graph": preview_material(base_color=teal, roughness=0.3),
+    }
+    slot = {name: s.add_material(m) for name, m in looks.items()}
+    sphere = _coarse_smooth_sphere(s)
+    card = s.add_geometry(np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)], dtype=F32),
+                          np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+    objects = [("Smooth", sphere, False), ("Rough", sphere, False), ("Tinted", sphere, False),
+               ("Matched", sphere, False), ("Partial", sphere, False), ("ThinSmooth", card, False),
+               ("ThinRough", card, False), ("ThinTinted", card, False), ("ThinMatched", card, False),
+               ("ThinDense", card, False), ("Smooth", sphere, True), ("Depth", sphere, False),
+               ("NoSpecular", sphere, False), ("Ignored", sphere, False), ("Graph", sphere, False)]
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (0.8, 0.0, -0.8)
+    for i, (look, geo, mirrored) in enumerate(objects):
+        scale = 0.35 if geo == sphere else 0.7
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = -scale if mirrored else scale
+        placed[5] = placed[10] = scale
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        s.add_instance(geo, slot[look], placed)
+    return s
+
+
+def material_transforms(reversed_rotation=False, size=160):
+    """The reference's material-transforms-v1 fixture
+    (SetMaterialTransforms, material_fixtures.cpp:1749-1825 in hydra-lotus):
+    15 cards on the middle three rows in the material studio whose lookups
+    carry UsdTransform2d st transforms: scale, rotation, translation, both,
+    a flip, a normal map turned and tiled, a transform on one input only, a
+    chain of two, on emission, on a constant's coordinates (no set), on an
+    absent set's fallback, on coverage, the identity, and a connected
+    rotation left untranslated. ``reversed_rotation`` reverses the rotated
+    card's rotation (the fixture's negative control, ReversedRotation)."""
+    s = material_studio("material-transforms-v1", size)
+
+    def palette_img(x, y):
+        return (40 + 60 * x, 40 + 60 * y, 200 if (x + y) % 2 == 0 else 60, 255)
+
+    def tilts_img(x, y):
+        return (32 + 64 * x, 224 - 64 * y, 200, 255)
+
+    def ramp_img(x, y):
+        v = 15 + 15 * (x + 4 * y)
+        return (v, v, v, 255)
+
+    def cutout_img(x, y):
+        dx, dy = 2 * x - 7, 2 * y - 7
+        d = dx * dx + dy * dy
+        return (60 + 20 * x, 200 - 15 * y, 60, 255 if d <= 26 else 96 if d <= 50 else 0)
+
+    pal = s.add_texture(_texture_image(4, palette_img), abi.TEXTURE_RGBA8_SRGB)
+    tlt = s.add_texture(_texture_image(4, tilts_img), abi.TEXTURE_RGBA8_UNORM)
+    rmp = s.add_texture(_texture_image(4, ramp_img), abi.TEXTURE_RGBA8_UNORM)
+    cut = s.add_texture(_texture_image(8, cutout_img), abi.TEXTURE_RGBA8_SRGB)
+    rep, clamp = abi.WRAP_REPEAT, abi.WRAP_CLAMP
+
+    def placed(texture, transform, wrap=rep, **kw):
+        return s.add_texture_input(texture, wrap_s=wrap, wrap_t=wrap, st_transform=transform, **kw)
+
+    def palette(transform, wrap=rep, texcoords="st"):
+        m = preview_material()
+        m.lookups[abi.SLOT_BASE_COLOR] = placed(pal, transform, wrap)
+        return m, texcoords
+
+    def tilts(transform):
+        m = preview_material(base_color=(0.7, 0.7, 0.7), roughness=0.4)
+        m.lookups[abi.SLOT_NORMAL] = placed(tlt, transform, scale=(2, 2, 2, 1), bias=(-1, -1, -1, 0))
+        return m, "st"
+
+    t = _transform2d
+    per_input, _ = palette(t(1, 1, 0, 0, 0))
+    per_input.lookups[abi.SLOT_ROUGHNESS] = placed(rmp, t(4, 4, 0, 0, 0), channel=0)
+    emission = preview_material(base_color=(0.0, 0.0, 0.0))
+    emission.lookups[abi.SLOT_EMISSION] = placed(pal, t(1, 1, 60, 0, 0))
+    constant, _ = palette(t(1, 1, 0, 0.125, 0.5), clamp)
+    constant.texcoord_fallback[:] = [0.5, 0.25]
+    absent, _ = palette(t(2, 2, 0, 0, 0), clamp)
+    absent.texcoord_fallback[:] = [0.125, 0.25]
+    coverage = preview_material(base_color=(0.2, 0.6, 0.7), opacity_threshold=0.5)
+    coverage.lookups[abi.SLOT_OPACITY] = placed(cut, t(1, 1, 45, 0, 0), channel=3)
+    cards = [
+        ("Scale", palette(t(2, 2, 0, 0, 0))),
+        ("Rotate", palette(t(1, 1, -30 if reversed_rotation else 30, 0, 0))),
+        ("Translate", palette(t(1, 1, 0, 0.25, 0.5))),
+        ("Combined", palette(t(2, 1, 30, 0.25, 0))),
+        ("Flip", palette(t(-1, 1, 0, 0, 0))),
+        ("NormalTurned", tilts(t(1, 1, 90, 0, 0))),
+        ("NormalTiled", tilts(t(3, 3, 0, 0, 0))),
+        ("PerInput", (per_input, "st")),
+        ("Chain", palette(t(1, 1, 45, 0, 0, _transform2d_double(2, 2, 0, 0, 0)))),
+        ("Emission", (emission, "st")),
+        ("ConstantIn", (constant, "")),
+        ("Absent", (absent, "absent")),
+        ("Coverage", (coverage, "st")),
+        ("Identity", palette(t(1, 1, 0, 0, 0))),
+        ("Connected", (preview_material(), "st")),
+    ]
+    positions = np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)], dtype=F32)
+    corners = np.array([[[[0, 0], [1, 0], [1, 1]], [[0, 0], [1, 1], [0, 1]]]], dtype=F32)
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (0.8, 0.0, -0.8)
+    for i, (name, (material, set_name)) in enumerate(cards):
+        card = s.add_geometry(positions, np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+        has_st = name != "ConstantIn"
+        if has_st:
+            s.set_texcoords(card, corners)
+        placed_m = np.eye(4, dtype=F32).reshape(-1)
+        placed_m[0] = placed_m[5] = placed_m[10] = 0.7
+        placed_m[12], placed_m[13] = columns[i % 5], rows[i // 5]
+        s.add_instance(card, s.add_material(material), placed_m,
+                       texcoord_set=1 if has_st and set_name == "st" else 0)
     return s

@@ -60,6 +60,13 @@ def golden_normals():
 
 
 @pytest.fixture(scope="session")
+def golden_fixtures():
+    """The reference's material-transmission-v1 and material-transforms-v1
+    golden images (4096 spp), by fixture name."""
+    return {name: load_golden(f"material_{name}_v1.npz") for name in ("transmission", "transforms")}
+
+
+@pytest.fixture(scope="session")
 def golden_textures():
     """The reference's material-textures-v1 golden images (4096 spp)."""
     return load_golden("material_textures_v1.npz")

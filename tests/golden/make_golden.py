@@ -27,6 +27,11 @@ little-endian; ReadPfm, adapters/common/reference.cpp:100-131):
   (adapters/common/material_fixtures.cpp:692-828: corner normals of every
   kind and tangent-space normal maps on coarse spheres and cards) at
   160x160, 4096 samples per pixel.
+- material_transmission_v1.npz and material_transforms_v1.npz: the
+  material-transmission-v1 and material-transforms-v1 fixtures
+  (adapters/common/material_fixtures.cpp:1588-1671, 1749-1825: solid and
+  thin-walled transmission; st transforms on every textured input) at
+  160x160, 4096 samples per pixel.
 """
 
 import os
@@ -42,7 +47,9 @@ FIXTURES = [("cornell-box", "cornell_box.npz", 1024),
             ("material-basics-v1", "material_basics_v1.npz", 4096),
             ("material-textures-v1", "material_textures_v1.npz", 4096),
             ("material-alpha-v1", "material_alpha_v1.npz", 4096),
-            ("material-normals-v1", "material_normals_v1.npz", 4096)]
+            ("material-normals-v1", "material_normals_v1.npz", 4096),
+            ("material-transmission-v1", "material_transmission_v1.npz", 4096),
+            ("material-transforms-v1", "material_transforms_v1.npz", 4096)]
 
 
 def read_pfm(path):

@@ -6,9 +6,10 @@ EvaluatePreview and Coverage, scene.slang:315-413, 1184-1260).
   ShiftedRepeat negative control (the Repeat card's s moved by 1/8, a
   texel-centre error) is rejected.
 - The same for material-alpha-v1 (constant and texture coverage, a masked
-  sphere, emitters through a mask) and its SrgbAlpha negative control, and
-  for material-normals-v1 (corner normals and tangent-space normal maps)
-  and its FlippedGreen negative control.
+  sphere, emitters through a mask), material-normals-v1 (corner normals and
+  tangent-space normal maps), material-transmission-v1 (solid and
+  thin-walled transmission) and material-transforms-v1 (st transforms), each
+  with its negative control.
 - Every path of those fixtures, and of a scene of texture-masked coverage
   (threshold and fractional), textured emission (light samples included)
   and an inverted mask, equals the oracle's.
@@ -67,14 +68,23 @@ def test_material_textures_negative_control_rejected(cuda, renderer, golden_text
     assert not c.ok, c
 
 
+FIXTURES = ["alpha", "normals", "transmission", "transforms"]
+NEGATIVE = {"alpha": {"srgb_alpha": True}, "normals": {"flipped_green": True}, "transmission": {"untinted": True},
+            "transforms": {"reversed_rotation": True}}
+
+
+@pytest.fixture(scope="module")
+def goldens(golden_alpha, golden_normals, golden_fixtures):
+    return {"alpha": golden_alpha, "normals": golden_normals, **golden_fixtures}
+
+
 @pytest.mark.parametrize("integrator", INTEGRATORS)
-@pytest.mark.parametrize("fixture", ["alpha", "normals"])
-def test_material_fixture_matches_reference_golden(cuda, renderer, golden_alpha, golden_normals, integrator,
-                                                   fixture):
+@pytest.mark.parametrize("fixture", FIXTURES)
+def test_material_fixture_matches_reference_golden(cuda, renderer, goldens, integrator, fixture):
     scene = getattr(scenes, f"material_{fixture}")()
     st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
                               max_bounces=64, sample_index=1 << 20)
-    g = golden_alpha if fixture == "alpha" else golden_normals
+    g = goldens[fixture]
     cuda.check(renderer.update_scene(scene), "update_scene")
     rendered = 0
     for level in (16, 256, 1024):
@@ -86,21 +96,21 @@ def test_material_fixture_matches_reference_golden(cuda, renderer, golden_alpha,
         assert c.ok, c
 
 
-@pytest.mark.parametrize("fixture", ["alpha", "normals"])
-def test_material_fixture_negative_control_rejected(cuda, renderer, golden_alpha, golden_normals, fixture):
-    scene = scenes.material_alpha(srgb_alpha=True) if fixture == "alpha" else \
-        scenes.material_normals(flipped_green=True)
+@pytest.mark.parametrize("fixture", FIXTURES)
+def test_material_fixture_negative_control_rejected(cuda, renderer, goldens, fixture):
+    scene = getattr(scenes, f"material_{fixture}")(**NEGATIVE[fixture])
     st = abi.default_settings(integrator=abi.INTEGRATOR_WAVEFRONT, light_sampling=abi.LIGHT_SAMPLING_MIS,
                               max_bounces=64, sample_index=1 << 20)
     _, color = render(cuda, renderer, scene, st, frame_count=256)
-    g = golden_alpha if fixture == "alpha" else golden_normals
+    g = goldens[fixture]
     c = metrics.compare(color, 256, g["mean"], g["variance"], g["samples"])
     assert not c.ok, c
 
 
 @pytest.mark.parametrize("integrator", INTEGRATORS)
 @pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
-@pytest.mark.parametrize("scene_name", ["material_textures", "texture_cutouts", "material_alpha", "material_normals"])
+@pytest.mark.parametrize("scene_name", ["material_textures", "texture_cutouts", "material_alpha", "material_normals",
+                                        "material_transmission", "material_transforms"])
 def test_textured_paths_match_oracle(cuda, renderer, oracle_lib, integrator, light_sampling, scene_name):
     scene = getattr(scenes, scene_name)()
     st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,

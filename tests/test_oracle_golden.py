@@ -24,6 +24,11 @@ reference's DES-Q5 comparison, and each fixture's negative control.
   unscaled, DirectX, constant, absent set, mirrored, rotated, stretched,
   glossy); the Mapped look's green negated must be rejected
   (FlippedGreen).
+- validation/reference/material-transmission-v1 and material-transforms-v1
+  (4096 spp): solid and thin-walled transmission, and st transforms on
+  every textured input; the tinted sphere's colour dropped
+  (UntintedGlass) and the rotation reversed (ReversedRotation) must be
+  rejected.
 
 Both were written by the reference's GPU renderer; fixtures in tests/golden.
 """
@@ -118,5 +123,26 @@ def test_oracle_matches_material_normals_golden(oracle_lib, golden_normals, ligh
 def test_oracle_material_normals_negative_control_rejected(oracle_lib, golden_normals):
     img = oracle_image(oracle_lib, scenes.material_normals(flipped_green=True), abi.LIGHT_SAMPLING_MIS)
     g = golden_normals
+    c = metrics.compare(img, SPP, g["mean"], g["variance"], g["samples"])
+    assert not c.ok, c
+
+
+NEGATIVE = {"transmission": {"untinted": True}, "transforms": {"reversed_rotation": True}}
+
+
+@pytest.mark.parametrize("name", sorted(NEGATIVE))
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+@pytest.mark.parametrize("spp", [16, 256])
+def test_oracle_matches_material_fixture_golden(oracle_lib, golden_fixtures, name, light_sampling, spp):
+    img = oracle_image(oracle_lib, getattr(scenes, f"material_{name}")(), light_sampling, spp)
+    g = golden_fixtures[name]
+    c = metrics.compare(img, spp, g["mean"], g["variance"], g["samples"])
+    assert c.ok, c
+
+
+@pytest.mark.parametrize("name", sorted(NEGATIVE))
+def test_oracle_material_fixture_negative_control_rejected(oracle_lib, golden_fixtures, name):
+    img = oracle_image(oracle_lib, getattr(scenes, f"material_{name}")(**NEGATIVE[name]), abi.LIGHT_SAMPLING_MIS)
+    g = golden_fixtures[name]
     c = metrics.compare(img, SPP, g["mean"], g["variance"], g["samples"])
     assert not c.ok, c
