@@ -1729,3 +1729,135 @@ def material_transforms(reversed_rotation=False, size=160):
         s.add_instance(card, s.add_material(material), placed_m,
                        texcoord_set=1 if has_st and set_name == "st" else 0)
     return s
+
+
+def _glow_image(srgb):
+    """The 4x4 float image of the reference's material fixtures (Glow,
+    material_fixtures.cpp:827-848): RGBE-decoded values, the colour
+    channels decoded from sRGB in double where `srgb`."""
+    out = np.zeros((4, 4, 4), dtype=F32)
+    for y in range(4):
+        for x in range(4):
+            unit = float(F32(math.ldexp(1.0, 127 + y - 136)))
+            v = [(240 - 50 * x) * unit, (80 + 50 * x) * unit, 160 * unit, 1.0]
+            for c in range(4):
+                if srgb and c < 3:
+                    v[c] = v[c] / 12.92 if v[c] <= 0.04045 else ((v[c] + 0.055) / 1.055) ** 2.4
+                out[y, x, c] = F32(v[c])
+    return out
+
+
+def material_emission(raw_emission=False, size=160):
+    """The reference's material-emission-v1 fixture (SetMaterialEmission,
+    material_fixtures.cpp:875-1009 in hydra-lotus): 25 objects in the
+    material studio: constant emitters (warm, bright, dim, clamped, a
+    metal), a back-facing, mirrored, stretched and tilted card, a faceted
+    sphere, emission maps (sRGB, raw, auto, grey, scale and bias, a missing
+    image's fallback, inverted, float images raw / auto / sRGB-decoded), a
+    textured sphere, a map shared with the base colour, an unlit card and a
+    card whose second quad is a subset bound to an emitter. ``raw_emission``
+    reads the sRGB palette as raw (the fixture's negative control,
+    RawEmission)."""
+    s = material_studio("material-emission-v1", size)
+
+    def palette(x, y):
+        return (40 + 60 * x, 40 + 60 * y, 200 if (x + y) % 2 == 0 else 60, 255)
+
+    def ramp(x, y):
+        v = 15 + 15 * (x + 4 * y)
+        return (v, v, v, 255)
+
+    srgb, unorm, flt = abi.TEXTURE_RGBA8_SRGB, abi.TEXTURE_RGBA8_UNORM, abi.TEXTURE_RGBA32_FLOAT
+    tex = {
+        "palette|sRGB": s.add_texture(_texture_image(4, palette), unorm if raw_emission else srgb),
+        "palette|raw": s.add_texture(_texture_image(4, palette), unorm),
+        "palette|auto": s.add_texture(_texture_image(4, palette), srgb),
+        "ramp|auto": s.add_texture(_texture_image(4, ramp), unorm),
+        "glow|raw": s.add_texture(_glow_image(False), flt),
+        "glow|auto": s.add_texture(_glow_image(False), flt),
+        "glow|sRGB": s.add_texture(_glow_image(True), flt),
+    }
+    clamp, rep = abi.WRAP_CLAMP, abi.WRAP_REPEAT
+
+    def lookup(key, wrap=clamp, **kw):
+        return s.add_texture_input(tex.get(key, 0), wrap_s=wrap, wrap_t=wrap, **kw)
+
+    def glowing(ref, **kw):
+        m = preview_material(**kw)
+        m.lookups[abi.SLOT_EMISSION] = ref
+        return m
+
+    shared = glowing(lookup("palette|sRGB"))
+    shared.lookups[abi.SLOT_BASE_COLOR] = lookup("palette|sRGB")
+    looks = {
+        "Warm": preview_material(emission=(1.0, 0.6, 0.2)),
+        "Bright": preview_material(emission=(6.0, 6.0, 6.0)),
+        "Dim": preview_material(emission=(0.05, 0.1, 0.2)),
+        "Clamped": preview_material(emission=(2.0, 0.0, 0.5)),
+        "NonFinite": preview_material(),
+        "Metal": preview_material(base_color=(0.95, 0.64, 0.54), roughness=0.25, metallic=1.0,
+                                  emission=(0.6, 0.2, 0.1)),
+        "Cool": preview_material(emission=(0.4, 0.8, 1.0)),
+        "Srgb": glowing(lookup("palette|sRGB")),
+        "Raw": glowing(lookup("palette|raw")),
+        "Auto": glowing(lookup("palette|auto")),
+        "Grey": glowing(lookup("ramp|auto")),
+        "ScaleBias": glowing(lookup("palette|raw", scale=(3, 3, 3, 1), bias=(0.2, 0.1, 0.0, 0.0))),
+        "Missing": glowing(lookup("missing|sRGB", fallback=(2.0, 1.0, 0.5, 1.0))),
+        "Inverted": glowing(lookup("palette|raw", scale=(-1, -1, -1, 1), bias=(1, 1, 1, 0))),
+        "Hdr": glowing(lookup("glow|raw")),
+        "HdrAuto": glowing(lookup("glow|auto")),
+        "HdrSrgb": glowing(lookup("glow|sRGB")),
+        "SphereTextured": glowing(lookup("palette|sRGB", rep)),
+        "Shared": shared,
+        "Unlit": glowing(lookup("palette|sRGB"), base_color=(0.0, 0.0, 0.0), ior=1.0),
+        "Base": preview_material(base_color=(0.6, 0.6, 0.6), roughness=0.3),
+    }
+    slot = {name: s.add_material(m) for name, m in looks.items()}
+
+    points, faces = coarse_sphere_polygons()
+    corners = coarse_sphere_corners(faces)
+    fixed = np.array([[_fixed(c) for c in p] for p in points], dtype=F32)
+    tris = np.array([[corners[i][0], corners[i + 1][0], corners[i + 2][0]] for i in range(0, len(corners), 3)],
+                    dtype=np.uint32)
+    faceted = s.add_geometry(fixed, tris)
+    smooth = s.add_geometry(fixed, tris, np.array([fixed[v] for v, _, _ in corners], dtype=F32).reshape(-1, 3, 3))
+    textured = s.add_geometry(fixed, tris)
+    latlong = coarse_sphere_latlong()
+    s.set_texcoords(textured, np.array([latlong[fv] for _, _, fv in corners], dtype=F32).reshape(1, -1, 3, 2))
+    card_p = np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)], dtype=F32)
+    plain = s.add_geometry(card_p, np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+    mapped = s.add_geometry(card_p, np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+    s.set_texcoords(mapped, np.array([[[[0, 0], [1, 0], [1, 1]], [[0, 0], [1, 1], [0, 1]]]], dtype=F32))
+    back = s.add_geometry(card_p, np.array([[0, 3, 2], [0, 2, 1]], dtype=np.uint32))
+    # TwoQuads' faces as the subset split leaves them (FacesOf): the left
+    # quad's points 0, 1, 4, 5 and the right quad's 1, 2, 3, 4.
+    left = s.add_geometry(np.array([(-0.5, -0.5, 0.0), (0.0, -0.5, 0.0), (0.0, 0.5, 0.0), (-0.5, 0.5, 0.0)], dtype=F32),
+                          np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+    right = s.add_geometry(np.array([(0.0, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (0.0, 0.5, 0.0)], dtype=F32),
+                           np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+    sph, crd = (0.35, 0.35, 0.35), (0.7, 0.7, 0.7)
+    objects = [
+        ("Warm", plain, crd, 0), ("Bright", plain, crd, 0), ("Dim", plain, crd, 0), ("Clamped", plain, crd, 0),
+        ("NonFinite", plain, crd, 0), ("Metal", smooth, sph, 0), ("Warm", back, crd, 0),
+        ("Warm", plain, (-0.7, 0.7, 0.7), 0), ("Warm", plain, (0.7, 0.35, 0.7), 0), ("Cool", faceted, sph, 0),
+        ("Srgb", mapped, crd, 0), ("Raw", mapped, crd, 0), ("Auto", mapped, crd, 0), ("Grey", mapped, crd, 0),
+        ("ScaleBias", mapped, crd, 0), ("Missing", mapped, crd, 0), ("Inverted", mapped, crd, 0),
+        ("Hdr", mapped, crd, 0), ("HdrAuto", mapped, crd, 0), ("HdrSrgb", mapped, crd, 0),
+        ("Warm", plain, crd, 60), ("SphereTextured", textured, sph, 0), ("Shared", mapped, crd, 0),
+        ("Unlit", mapped, crd, 0), ("Base", None, crd, 0),
+    ]
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (1.6, 0.8, 0.0, -0.8, -1.6)
+    for i, (look, geo, scale, rotate_x) in enumerate(objects):
+        t = np.eye(4)
+        t[0, 3], t[1, 3] = columns[i % 5], rows[i // 5]
+        c, sn = math.cos(rotate_x * math.pi / 180), math.sin(rotate_x * math.pi / 180)
+        rx = np.array([[1, 0, 0, 0], [0, c, -sn, 0], [0, sn, c, 0], [0, 0, 0, 1]], dtype=np.float64)
+        sc = np.diag([scale[0], scale[1], scale[2], 1.0])
+        m = (t @ rx @ sc).astype(F32).reshape(-1, order="F")
+        if geo is None:
+            s.add_instance(left, slot["Base"], m)
+            s.add_instance(right, slot["Warm"], m)
+        else:
+            s.add_instance(geo, slot[look], m, texcoord_set=1 if geo in s.texcoords else 0)
+    return s

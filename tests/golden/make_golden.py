@@ -32,6 +32,10 @@ little-endian; ReadPfm, adapters/common/reference.cpp:100-131):
   (adapters/common/material_fixtures.cpp:1588-1671, 1749-1825: solid and
   thin-walled transmission; st transforms on every textured input) at
   160x160, 4096 samples per pixel.
+- material_emission_v1.npz: the material-emission-v1 fixture
+  (adapters/common/material_fixtures.cpp:875-1009: constant emitters and
+  emission maps, float images included) at 160x160, 4096 samples per
+  pixel.
 """
 
 import os
@@ -49,7 +53,8 @@ FIXTURES = [("cornell-box", "cornell_box.npz", 1024),
             ("material-alpha-v1", "material_alpha_v1.npz", 4096),
             ("material-normals-v1", "material_normals_v1.npz", 4096),
             ("material-transmission-v1", "material_transmission_v1.npz", 4096),
-            ("material-transforms-v1", "material_transforms_v1.npz", 4096)]
+            ("material-transforms-v1", "material_transforms_v1.npz", 4096),
+            ("material-emission-v1", "material_emission_v1.npz", 4096)]
 
 
 def read_pfm(path):
