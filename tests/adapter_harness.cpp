@@ -119,7 +119,7 @@ int main(int argc, char** argv) {
   }
   char magic[4];
   in.get(magic, 4);
-  if (std::memcmp(magic, "LTSC", 4) != 0 || in.get<uint32_t>() != 2) {
+  if (std::memcmp(magic, "LTSC", 4) != 0 || in.get<uint32_t>() != 3) {
     std::fprintf(stderr, "not a scene file\n");
     return 2;
   }
@@ -161,6 +161,13 @@ int main(int argc, char** argv) {
       m->normals.resize(3 * (size_t)nt);
       for (auto& n : m->normals) in.get(n.data(), 3);
     }
+    // Texture-coordinate sets, named so that key order is file order.
+    const uint32_t sets = in.get<uint32_t>();
+    for (uint32_t k = 0; k < sets; ++k) {
+      auto& set = m->texcoords["st" + std::to_string(100 + k)];
+      set.resize(3 * (size_t)nt);
+      for (auto& st : set) in.get(st.data(), 2);
+    }
     meshes.push_back(m);
     update.geometry_uploads.push_back(m);
   }
@@ -170,12 +177,32 @@ int main(int argc, char** argv) {
     in.get(s.world_from_object.data(), 16);
     const uint32_t g = in.get<uint32_t>();
     s.material = in.get<uint32_t>();
+    const uint32_t set = in.get<uint32_t>();
+    s.texcoords = set == 0 ? Lotus::kNoTexcoords : set - 1;
     s.geometry = g < meshes.size() ? meshes[g].get() : nullptr;
     update.instances.push_back(s);
   }
   update.materials_changed = true;
+  std::vector<lotus_material> materials(nm);
+  for (uint32_t i = 0; i < nm; ++i) materials[i] = in.get<lotus_material>();
+  // The images, then the texture inputs the materials' lookups name.
+  std::vector<std::shared_ptr<Lotus::Texture>> textures(in.get<uint32_t>());
+  for (auto& t : textures) {
+    t = std::make_shared<Lotus::Texture>();
+    t->width = in.get<uint32_t>();
+    t->height = in.get<uint32_t>();
+    const uint32_t format = in.get<uint32_t>();
+    t->format = format == LOTUS_TEXTURE_RGBA8_SRGB     ? Lotus::TextureFormat::Rgba8Srgb
+                : format == LOTUS_TEXTURE_RGBA32_FLOAT ? Lotus::TextureFormat::Rgba32Float
+                                                       : Lotus::TextureFormat::Rgba8Unorm;
+    t->texels.resize((size_t)t->width * t->height * Lotus::TexelBytes(t->format));
+    in.get(t->texels.data(), t->texels.size());
+    update.texture_uploads.push_back(t);
+  }
+  std::vector<lotus_texture_input> inputs(in.get<uint32_t>());
+  for (auto& input : inputs) input = in.get<lotus_texture_input>();
   for (uint32_t i = 0; i < nm; ++i) {
-    const lotus_material lm = in.get<lotus_material>();
+    const lotus_material& lm = materials[i];
     Lotus::SceneMaterial sm;
     Lotus::PreviewSurface p;
     std::memcpy(p.base_color.data(), lm.base_color, 12);
@@ -191,6 +218,32 @@ int main(int argc, char** argv) {
     sm.material.surface = p;
     sm.material.geometry.opacity = lm.opacity;
     sm.material.geometry.opacity_threshold = lm.opacity_threshold;
+    std::memcpy(sm.material.geometry.texcoord_fallback.data(), lm.texcoord_fallback, 8);
+    if (lm.normal[0] != 0.0f || lm.normal[1] != 0.0f || lm.normal[2] != 0.0f)
+      std::memcpy(sm.material.geometry.normal.data(), lm.normal, 12);
+    // Each slot's lookup, its image resolved as the host's extraction
+    // would (SceneMaterial::textures; none for a key without an image).
+    auto& preview = std::get<Lotus::PreviewSurface>(sm.material.surface);
+    std::optional<Lotus::TextureInput>* slots[LOTUS_TEXTURE_SLOTS] = {&sm.material.geometry.opacity_texture,
+        &sm.material.geometry.normal_texture, &preview.base_color_texture, &preview.roughness_texture,
+        &preview.metallic_texture, &preview.emission_texture, &preview.specular_color_texture};
+    for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k) {
+      if (lm.lookups[k] == LOTUS_NO_LOOKUP || lm.lookups[k] > inputs.size()) continue;
+      const lotus_texture_input& d = inputs[lm.lookups[k] - 1];
+      Lotus::TextureInput t;
+      t.texture = d.texture == LOTUS_NO_TEXTURE ? std::string("missing") : "tex" + std::to_string(d.texture);
+      t.channel = d.channel;
+      t.wrap_s = (Lotus::TextureWrap)d.wrap_s;
+      t.wrap_t = (Lotus::TextureWrap)d.wrap_t;
+      std::memcpy(t.scale.data(), d.scale, 16);
+      std::memcpy(t.bias.data(), d.bias, 16);
+      std::memcpy(t.fallback.data(), d.fallback, 16);
+      std::memcpy(t.st_transform.data(), d.st_transform, 24);
+      *slots[k] = t;
+      sm.textures[k] = d.texture != LOTUS_NO_TEXTURE && d.texture <= textures.size()
+                           ? textures[d.texture - 1].get()
+                           : nullptr;
+    }
     update.materials.push_back(sm);
   }
   // The analytic lights, as the reference's Light (render_world.hpp:86-114).

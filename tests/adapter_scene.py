@@ -13,7 +13,7 @@ HARNESS = os.path.join(ROOT, "hydra_lotus_b200", "_lib", "adapter_harness")
 
 
 def write(path, scene, settings, frame_count):
-    out = [b"LTSC", struct.pack("<I", 2)]
+    out = [b"LTSC", struct.pack("<I", 3)]
     out.append(struct.pack("<3I", len(scene.geometries), len(scene.instances), len(scene.materials)))
     out.append(struct.pack("<3f", *scene.environment_constant))
     if scene.environment is not None:
@@ -24,17 +24,28 @@ def write(path, scene, settings, frame_count):
         out.append(np.ascontiguousarray(texels, dtype=np.float32).tobytes())
     else:
         out.append(struct.pack("<I", 0))
-    for p, t, n in scene.geometries:
+    for g, (p, t, n) in enumerate(scene.geometries):
         out.append(struct.pack("<3I", p.shape[0], t.shape[0], 0 if n is None else 1))
         out.append(np.ascontiguousarray(p, dtype=np.float32).tobytes())
         out.append(np.ascontiguousarray(t, dtype=np.uint32).tobytes())
         if n is not None:
             out.append(np.ascontiguousarray(n, dtype=np.float32).tobytes())
-    for m, g, mat in scene.instances:
+        sets = scene.texcoords.get(g)
+        out.append(struct.pack("<I", 0 if sets is None else sets.shape[0]))
+        if sets is not None:
+            out.append(np.ascontiguousarray(sets, dtype=np.float32).tobytes())
+    for i, (m, g, mat) in enumerate(scene.instances):
         out.append(np.asarray(m, dtype=np.float32).reshape(16).tobytes())
-        out.append(struct.pack("<2I", g, mat))
+        out.append(struct.pack("<3I", g, mat, scene.instance_texcoords.get(i, 0)))
     for mat in scene.materials:
         out.append(bytes(mat))
+    out.append(struct.pack("<I", len(scene.textures)))
+    for texels, fmt in scene.textures:
+        out.append(struct.pack("<3I", texels.shape[1], texels.shape[0], fmt))
+        out.append(np.ascontiguousarray(texels).tobytes())
+    out.append(struct.pack("<I", len(scene.texture_inputs)))
+    for t in scene.texture_inputs:
+        out.append(bytes(t))
     out.append(struct.pack("<I", len(scene.lights)))
     for light in scene.lights:
         out.append(bytes(light))

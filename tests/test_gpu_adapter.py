@@ -34,6 +34,12 @@ ADAPTER_SCENES = {
     "sphere_field": small_sphere_field,
     # Lotus::Light of every shape, mapped by the adapter to lotus_light.
     "lit_room": lambda: scenes.lit_room(seed=2, size=64, environment=True),
+    # Textures, texture inputs on every PreviewSurface slot, coordinate sets
+    # and fallbacks, normal maps, mapped by the adapter from the
+    # reference's Texture / TextureInput / MeshGeometry::texcoords.
+    "material_textures": lambda: scenes.material_textures(size=64),
+    "material_normals": lambda: scenes.material_normals(size=64),
+    "texture_cutouts": lambda: scenes.texture_cutouts(size=64),
 }
 
 
