@@ -233,10 +233,8 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
   // see them.
   if (kAnalytic && depth != 0 && S.analytic_count != 0)
     R = R + T * crossed_lights(S, ray_o, ray_d, dot(sh.position - ray_o, ray_d), false, weigh, last_pdf);
-  // A path that ends into the radiance cache stops after the emission: the
-  // cache stands for everything scattered from here on.
-  if (depth >= f.max_bounces || end_here) return false;
-  if (depth >= kRouletteBounces) {
+  if (depth >= f.max_bounces) return false;
+  if (!end_here && depth >= kRouletteBounces) {
     const float survival = fminf(max_component(T), kMaxSurvival);
     if (next_random(rng) >= survival) return false;
     T = T / survival;
@@ -288,6 +286,10 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
   } else if (kAnalytic && !f.sample_lights && S.analytic_count != 0) {
     R = R + T * parallel_lights(S, sh.position, sh.normal, sh.bsdf, basis, wo, req.inline_shadow);
   }
+  // A path that ends into the radiance cache stops after next event
+  // estimation at its cache vertex: the cache stands for the light the
+  // vertex scatters but its direct light, which the shadow ray brings.
+  if (end_here) return false;
   F3 u;
   u.x = next_random(rng);
   u.y = next_random(rng);
@@ -609,7 +611,6 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
       if (training && t_at < C.train_capacity) {
         C.train[t_at] = features;
         C.train_slots[t_at] = slot;
-        C.train_base[t_at] = F4(R, 0.0f);
         C.train_throughput[t_at] = F4(T_in, 0.0f);
       }
     }
@@ -633,8 +634,8 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
 }
 
 // The training targets once the sample's paths have ended: the radiance a
-// training path gathered after its cache vertex's emission, divided by its
-// throughput on arrival there.
+// training path gathered after its cache vertex's emission and next event
+// estimation, divided by its throughput on arrival there.
 __global__ void k_cache_targets(CacheQueues C, PathState P) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t n = min(C.counters[1], C.train_capacity);
@@ -646,6 +647,15 @@ __global__ void k_cache_targets(CacheQueues C, PathState P) {
   float4 target = make_float4(ratio(r.x - base.x, t.x), ratio(r.y - base.y, t.y), ratio(r.z - base.z, t.z), 0.0f);
   if (!isfinite(target.x) || !isfinite(target.y) || !isfinite(target.z)) target = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   C.train_targets[i] = target;
+}
+
+// Each training path's radiance once its cache vertex's emission and shadow
+// ray are in (after that bounce's shadow launch): what the cache's target
+// leaves out.
+__global__ void k_cache_base(CacheQueues C, PathState P) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t n = min(C.counters[1], C.train_capacity);
+  if (i < n) C.train_base[i] = P.radiance[C.train_slots[i]];
 }
 
 constexpr unsigned kFullWarp = 0xFFFFFFFFu;
@@ -1334,6 +1344,9 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
           k_wf_shadow<false, false, false><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill,
               nullptr, none);
     }
+    // The training paths' radiance up to their cache vertex's shadow ray.
+    if (C.enabled && b == C.bounce)
+      k_cache_base<<<(C.train_capacity + kBlock - 1) / kBlock, kBlock, 0, stream>>>(C, P);
   }
   if (rounds <= max_bounces) {
     Timed t(profile, stream, 6);

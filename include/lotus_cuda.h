@@ -685,8 +685,10 @@ int32_t lotus_cuda_batch_render(lotus_cuda_batch* batch,
  * encoded MLP (five 64-wide ReLU layers, RGB out; BF16 on the tensor cores,
  * FP32 accumulation) trained online on the wavefront path tracer's own
  * radiance. With the cache enabled, wavefront paths end into it at their
- * second vertex, except one path in `training_stride`, which is traced in
- * full and trains it. */
+ * second vertex, after next event estimation there (the cache stands for
+ * the light the vertex scatters besides its direct light), except one path
+ * in `training_stride`, which is traced in full and trains it on what it
+ * gathered after that vertex's emission and shadow ray. */
 
 #define LOTUS_CACHE_INPUTS 64u
 #define LOTUS_CACHE_WEIGHTS 21504u  /* 5 x 64 x 64 + 64 x 16 FP32 */
