@@ -12,6 +12,7 @@
 // the reference's order.
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -193,10 +194,10 @@ struct ShadowRequest {
 // crossed, applies Russian roulette, prepares next event estimation's
 // shadow ray (under BSDF sampling, traces the parallel lights' own) and
 // samples the BSDF. Returns whether the path continues along (new_o, new_d).
-// kAnalytic: the scene may have analytic lights or texture lookups
-// (SceneView::textured); the instantiation without carries none of their
-// code or registers.
-template <bool kAnalytic>
+// kAnalytic: the scene may have analytic lights; kTextured: texture
+// lookups (SceneView::textured). The instantiations without carry none of
+// their code or registers.
+template <bool kAnalytic, bool kTextured>
 __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     uint32_t instance, uint32_t tri, float b1, float b2, F3 ray_o, F3 ray_d, uint32_t depth,
     F3& T, F3& R, float& last_pdf, uint32_t& flags, uint32_t& rng, F3& new_o, F3& new_d,
@@ -204,7 +205,7 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
   req.pending = false;
   req.inline_shadow = 0;
   uint32_t primitive;
-  const SurfaceHit sh = reconstruct_hit<kAnalytic>(S, instance, tri, b1, b2, ray_d, &primitive);
+  const SurfaceHit sh = reconstruct_hit<kTextured>(S, instance, tri, b1, b2, ray_d, &primitive);
   if (features) {
     // The radiance cache's description of this vertex, seen from the ray.
     const F3 albedo = sh.bsdf.transmission > 0.0f
@@ -249,7 +250,7 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
         f.restir_final + (size_t)pixel_index * f.restir_stride);
     if ((sel.flags & 2u) == 0 && sel.reservoir.weight_sum > 0.0f && sel.reservoir.sample < S.light_count) {
       const F3 origin = offset_ray_origin(sh.position, sh.normal);
-      const LightSample ls = reconstruct_reservoir_light<kAnalytic>(S, sel.reservoir.sample, sel.uv[0], sel.uv[1], origin);
+      const LightSample ls = reconstruct_reservoir_light<kAnalytic, kTextured>(S, sel.reservoir.sample, sel.uv[0], sel.uv[1], origin);
       const F3 wi = basis.to_local(ls.direction);
       const float weight = ls.delta ? 1.0f
           : power_heuristic(kAnalytic ? reservoir_partition_pdf(S, sel.reservoir.sample, ls, origin) : ls.pdf,
@@ -266,7 +267,7 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     const float u2 = next_random(rng);
     const float u3 = next_random(rng);
     const F3 origin = offset_ray_origin(sh.position, sh.normal);
-    const LightSample ls = sample_light<kAnalytic>(S, u0, u1, u2, u3, origin);
+    const LightSample ls = sample_light<kAnalytic, kTextured>(S, u0, u1, u2, u3, origin);
     if (ls.pdf > 0.0f && max_component(ls.radiance) > 0.0f && dot(ls.direction, sh.normal) > 0.0f) {
       const F3 wi = basis.to_local(ls.direction);
       if (wi.z > 0.0f) {
@@ -359,7 +360,7 @@ __device__ __forceinline__ double4 add4(double4 a, float4 s) {
 // The reference integrator: one thread follows one camera path to its end
 // (path_trace.slang:279-287, 353-385), then adds it to the pixel's FP64
 // accumulation and writes the mean.
-template <bool kCount, bool kAnalytic>
+template <bool kCount, bool kAnalytic, bool kTextured>
 __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
     const FrameConst* __restrict__ fcp, double4* __restrict__ accum, float4* __restrict__ color,
     RayTotals* totals, VisitCounters* visits) {
@@ -380,26 +381,26 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
       start_path(f, px, py, f.sample_index, o, d, tmax, rng);
       ++n_camera;
       Hit hit;
-      if (trace_closest<kCount, kAnalytic>(S, o, d, 0.0f, tmax, rng, hit, &vc[0])) {
+      if (trace_closest<kCount, kTextured>(S, o, d, 0.0f, tmax, rng, hit, &vc[0])) {
         F3 T = V(1.0f), R = V(0.0f);
         float last_pdf = 0.0f;
         uint32_t flags = 0;
         for (uint32_t depth = 0;; ++depth) {
           F3 no, nd;
           ShadowRequest req;
-          const bool cont = scatter<kAnalytic>(S, f, hit.instance, hit.tri, hit.b1, hit.b2, o, d, depth, T, R,
+          const bool cont = scatter<kAnalytic, kTextured>(S, f, hit.instance, hit.tri, hit.b1, hit.b2, o, d, depth, T, R,
               last_pdf, flags, rng, no, nd, req, slot);
           n_shadow += req.inline_shadow;
           if (req.pending) {
             ++n_shadow;
-            const float tr = trace_shadow<kCount, kAnalytic>(S, req.origin, req.direction, 0.0f, req.tmax, &vc[2]);
+            const float tr = trace_shadow<kCount, kTextured>(S, req.origin, req.direction, 0.0f, req.tmax, &vc[2]);
             if (tr > 0.0f) R = R + req.throughput * shadow_contribution(req.fl, req.weight, req.pdf, tr);
           }
           if (!cont) break;
           o = no;
           d = nd;
           ++n_extension;
-          if (!trace_closest<kCount, kAnalytic>(S, o, d, 0.0f, kFloatMax, rng, hit, &vc[1])) {
+          if (!trace_closest<kCount, kTextured>(S, o, d, 0.0f, kFloatMax, rng, hit, &vc[1])) {
             R = miss_path<kAnalytic>(S, f, o, d, flags, last_pdf, T, R);
             break;
           }
@@ -518,7 +519,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
 // Compiled for six resident blocks per SM (80 registers): shading is
 // latency-bound and gains more from occupancy than from registers.
 constexpr int kShadeBlocksPerSm = 6;
-template <bool kCacheVertex, bool kBatch, bool kAnalytic>
+template <bool kCacheVertex, bool kBatch, bool kAnalytic, bool kTextured>
 __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 1];
@@ -569,7 +570,7 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
       if (cache_vertex)
         training = pcg_hash(slot ^ pcg_hash(f.sample_index ^ 0xC2B2AE35u)) % C.stride == 0u;
       F3 no, nd;
-      cont = scatter<kAnalytic>(SS, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
+      cont = scatter<kAnalytic, kTextured>(SS, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
           T, R, last_pdf, flags, rng, no, nd, req, slot, cache_vertex ? &features : nullptr,
           cache_vertex && !training);
       query = cache_vertex && !training;
@@ -838,7 +839,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_visibility(SceneV
 // queued for shading; a miss ends the path with the environment. Each warp
 // stages its hits in shared memory and appends them to the hit queue 32 at
 // a time.
-template <bool kCount, bool kBatch, bool kAnalytic>
+template <bool kCount, bool kBatch, bool kAnalytic, bool kTextured>
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, const uint32_t* __restrict__ rays_in, uint32_t bounce,
     uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits, SceneTable B) {
@@ -869,7 +870,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneVi
     if (!__any_sync(kFullWarp, active)) break;
     bool emit = false;
     const SceneView& SS = kBatch ? B.views[scene] : S;
-    if (walk_round<false, kCount, kAnalytic>(SS, W, stack, rng, active, &vc)) {
+    if (walk_round<false, kCount, kTextured>(SS, W, stack, rng, active, &vc)) {
       active = false;
       if (W.found) {
         P.hit[slot] = make_uint4(W.best_instance, W.best_tri, __float_as_uint(W.b1), __float_as_uint(W.b2));
@@ -960,7 +961,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_resolve(SceneView S,
 // give it; the per-bounce queue counts are kept as the rounds keep them.
 // Threads take paths from `cursor` one at a time. Long paths then cost one
 // launch instead of three per bounce.
-template <bool kBatch, bool kAnalytic>
+template <bool kBatch, bool kAnalytic, bool kTextured>
 __global__ void __launch_bounds__(kBlock) k_wf_tail(SceneView S, const FrameConst* __restrict__ fcp, PathState P,
     Queues Q, uint32_t first, uint32_t* __restrict__ cursor, SceneTable B) {
   const uint32_t n = Q.counts[3 * first];
@@ -984,18 +985,18 @@ __global__ void __launch_bounds__(kBlock) k_wf_tail(SceneView S, const FrameCons
     // A path's bounces are bounded by max_bounces (scatter ends it there).
     for (uint32_t bounce = first; bounce <= f.max_bounces; ++bounce) {
       Hit hit;
-      if (!trace_closest<false, kAnalytic>(SS, ro, rd, tmin, tmax, rng, hit)) {
+      if (!trace_closest<false, kTextured>(SS, ro, rd, tmin, tmax, rng, hit)) {
         R = miss_path<kAnalytic>(SS, f, ro, rd, flags, last_pdf, T, R);
         break;
       }
       atomicAdd(&Q.counts[3 * bounce + 1], 1u);
       F3 no, nd;
       ShadowRequest req;
-      const bool cont = scatter<kAnalytic>(SS, f, hit.instance, hit.tri, hit.b1, hit.b2, ro, rd, bounce, T, R,
+      const bool cont = scatter<kAnalytic, kTextured>(SS, f, hit.instance, hit.tri, hit.b1, hit.b2, ro, rd, bounce, T, R,
           last_pdf, flags, rng, no, nd, req, slot);
       if (req.pending) {
         atomicAdd(&Q.counts[3 * bounce + 2], 1u);
-        const float tr = trace_shadow<false, kAnalytic>(SS, req.origin, req.direction, 0.0f, req.tmax);
+        const float tr = trace_shadow<false, kTextured>(SS, req.origin, req.direction, 0.0f, req.tmax);
         if (tr > 0.0f) R = R + req.throughput * shadow_contribution(req.fl, req.weight, req.pdf, tr);
       }
       if (!cont) break;
@@ -1170,6 +1171,18 @@ struct Timed {
 
 }  // namespace
 
+// Calls f(analytic, textured) with each as a compile-time constant
+// (std::true_type / std::false_type), so that a launch takes the
+// instantiation without the analytic lights' or texture lookups' code when
+// the scene has none.
+template <class F>
+void with_features(bool analytic, bool textured, F&& f) {
+  if (analytic && textured) f(std::true_type{}, std::true_type{});
+  else if (analytic) f(std::true_type{}, std::false_type{});
+  else if (textured) f(std::false_type{}, std::true_type{});
+  else f(std::false_type{}, std::false_type{});
+}
+
 void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_t rect[4],
     double4* accum, float4* color, RayTotals* totals, cudaStream_t stream,
     SampleProfile* profile) {
@@ -1177,15 +1190,15 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
   if (threads == 0) return;
   const uint32_t grid = (threads + kBlock - 1) / kBlock;
   Timed t(profile, stream, 0);
-  // The instantiations with analytic lights' and texture lookups' code.
-  const bool analytic = S.analytic_count != 0 || S.textured != 0;
+  // Counting visits takes the instantiation with every feature's code.
   if (profile && profile->visits) {
-    if (analytic) k_reference_pt<true, true><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
-    else k_reference_pt<true, false><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
-  } else {
-    if (analytic) k_reference_pt<false, true><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, nullptr);
-    else k_reference_pt<false, false><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, nullptr);
+    k_reference_pt<true, true, true><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
+    return;
   }
+  with_features(S.analytic_count != 0, S.textured != 0, [&](auto a, auto x) {
+    k_reference_pt<false, decltype(a)::value, decltype(x)::value><<<grid, kBlock, 0, stream>>>(S, fc, accum, color,
+        totals, nullptr);
+  });
 }
 
 // Blocks of a persistent tracing kernel: every resident block on every
@@ -1231,7 +1244,7 @@ uint32_t choose_wavefront_rounds(const uint32_t* counts, uint32_t resident, uint
 }
 
 uint32_t extension_resident_threads() {
-  return persistent_grid((const void*)k_wf_extend<false, false, false>, 1u << 30, TraceTuning()) * kBlock;
+  return persistent_grid((const void*)k_wf_extend<false, false, false, false>, 1u << 30, TraceTuning()) * kBlock;
 }
 
 uint32_t wavefront_rounds(uint32_t max_bounces, bool count_visits, uint32_t requested, uint32_t cache_bounce) {
@@ -1261,10 +1274,11 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid_pixels = (threads + kBlock - 1) / kBlock;
   const SceneTable none;
-  // The instantiations with analytic lights' and texture lookups' code.
-  const bool analytic = S.analytic_count != 0 || S.textured != 0;
+  // The scene's features select the instantiations (counting visits takes
+  // the one with every feature's code).
+  const bool analytic = S.analytic_count != 0, textured = S.textured != 0;
   const uint32_t grid_extend = persistent_grid(
-      count ? (const void*)k_wf_extend<true, false, false> : (const void*)k_wf_extend<false, false, false>,
+      count ? (const void*)k_wf_extend<true, false, true, true> : (const void*)k_wf_extend<false, false, false, false>,
       Q.capacity, tuning);
   const uint32_t grid_shadow = persistent_grid(
       count ? (const void*)k_wf_shadow<true, false, true> : (const void*)k_wf_shadow<false, false, false>, Q.capacity,
@@ -1272,13 +1286,13 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   // Shading: up to eight waves of resident blocks, grid-striding over
   // longer queues.
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
-      8u * persistent_grid((const void*)k_wf_shade<false, false, false>, Q.capacity, TraceTuning()));
+      8u * persistent_grid((const void*)k_wf_shade<false, false, false, false>, Q.capacity, TraceTuning()));
   {
     // One camera thread per pixel of each of the wave's samples.
     Timed t(profile, stream, 0);
     const uint32_t grid_camera = (threads * std::max(wave, 1u) + kBlock - 1) / kBlock;
     if (count) k_wf_camera<true, false, true><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, visits, none);
-    else if (analytic) k_wf_camera<false, false, true><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
+    else if (textured) k_wf_camera<false, false, true><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
     else k_wf_camera<false, false, false><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
   }
   // Bounces 0 .. rounds - 1 as wavefront rounds; the paths queued for bounce
@@ -1300,18 +1314,14 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     }
     if (b != 0) {
       Timed t(profile, stream, 1);
-      if (count && analytic)
-        k_wf_extend<true, false, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b, refill,
-            visits, none);
-      else if (count)
-        k_wf_extend<true, false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b, refill,
-            visits, none);
-      else if (analytic)
-        k_wf_extend<false, false, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b, refill,
-            nullptr, none);
+      if (count)
+        k_wf_extend<true, false, true, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b,
+            refill, visits, none);
       else
-        k_wf_extend<false, false, false><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b, refill,
-            nullptr, none);
+        with_features(analytic, textured, [&](auto a, auto x) {
+          k_wf_extend<false, false, decltype(a)::value, decltype(x)::value><<<grid_extend, kBlock, 0, stream>>>(S, fc,
+              P, Q, rays, b, fetch + 2 * b, refill, nullptr, none);
+        });
     }
     {
       // Shade keys the rays it queues when a round extends them.
@@ -1322,14 +1332,14 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
       if (cache_vertex && C.query_keys != nullptr)
         cudaMemsetAsync(C.query_bins, 0, sizeof(uint32_t) * kSortBins, stream);
       Timed t(profile, stream, 2);
-      if (cache_vertex && analytic)
-        k_wf_shade<true, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, QS, b, C, none);
-      else if (cache_vertex)
-        k_wf_shade<true, false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, QS, b, C, none);
-      else if (analytic)
-        k_wf_shade<false, false, true><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, QS, b, C, none);
-      else
-        k_wf_shade<false, false, false><<<grid_shade, kBlock, 0, stream>>>(S, fc, P, QS, b, C, none);
+      with_features(analytic, textured, [&](auto a, auto x) {
+        if (cache_vertex)
+          k_wf_shade<true, false, decltype(a)::value, decltype(x)::value><<<grid_shade, kBlock, 0, stream>>>(S, fc, P,
+              QS, b, C, none);
+        else
+          k_wf_shade<false, false, decltype(a)::value, decltype(x)::value><<<grid_shade, kBlock, 0, stream>>>(S, fc, P,
+              QS, b, C, none);
+      });
     }
     {
       Timed t(profile, stream, 3);
@@ -1337,7 +1347,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
         k_wf_shadow<true, false, true><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, visits,
             none);
       else
-        if (analytic)
+        if (textured)
           k_wf_shadow<false, false, true><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill,
               nullptr, none);
         else
@@ -1351,10 +1361,11 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   if (rounds <= max_bounces) {
     Timed t(profile, stream, 6);
     uint32_t* cursor = fetch + 2 * (max_bounces + 1);
-    const uint32_t grid_tail = persistent_grid(
-        analytic ? (const void*)k_wf_tail<false, true> : (const void*)k_wf_tail<false, false>, Q.capacity, tuning);
-    if (analytic) k_wf_tail<false, true><<<grid_tail, kBlock, 0, stream>>>(S, fc, P, Q, rounds, cursor, none);
-    else k_wf_tail<false, false><<<grid_tail, kBlock, 0, stream>>>(S, fc, P, Q, rounds, cursor, none);
+    with_features(analytic, textured, [&](auto a, auto x) {
+      const auto kernel = k_wf_tail<false, decltype(a)::value, decltype(x)::value>;
+      const uint32_t grid_tail = persistent_grid((const void*)kernel, Q.capacity, tuning);
+      kernel<<<grid_tail, kBlock, 0, stream>>>(S, fc, P, Q, rounds, cursor, none);
+    });
   }
   if (C.enabled) {
     // The paths that ended into the cache receive its answer; then the
@@ -1443,11 +1454,11 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   uint32_t* fetch = Q.counts + 3 * (size_t)(max_bounces + 2);
   const uint32_t refill = tuning.refill_below ? std::min(tuning.refill_below, 32u) : kDefaultRefillBelow;
   const uint32_t grid_slots = (B.total_slots + kBlock - 1) / kBlock;
-  const uint32_t grid_extend = persistent_grid((const void*)k_wf_extend<false, true, false>, Q.capacity, tuning);
+  const uint32_t grid_extend = persistent_grid((const void*)k_wf_extend<false, true, false, false>, Q.capacity, tuning);
   const uint32_t grid_shadow = persistent_grid((const void*)k_wf_shadow<false, true, true>, Q.capacity, tuning);
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
-      8u * persistent_grid((const void*)k_wf_shade<false, true, false>, Q.capacity, TraceTuning()));
-  if (B.analytic) k_wf_camera<false, true, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
+      8u * persistent_grid((const void*)k_wf_shade<false, true, false, false>, Q.capacity, TraceTuning()));
+  if (B.textured) k_wf_camera<false, true, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
   else k_wf_camera<false, true, false><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
   const uint32_t rounds = wavefront_rounds(max_bounces, false, tuning.rounds);
   const bool keyed = Q.keys != nullptr && Q.sorted != nullptr && Q.bins != nullptr;
@@ -1460,20 +1471,19 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
           Q.bins, Q.sorted);
       rays = Q.sorted;
     }
-    if (b != 0 && B.analytic)
-      k_wf_extend<false, true, true><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rays, b,
-          fetch + 2 * b, refill, nullptr, B);
-    else if (b != 0)
-      k_wf_extend<false, true, false><<<grid_extend, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rays, b,
-          fetch + 2 * b, refill, nullptr, B);
+    if (b != 0)
+      with_features(B.analytic, B.textured, [&](auto a, auto x) {
+        k_wf_extend<false, true, decltype(a)::value, decltype(x)::value><<<grid_extend, kBlock, 0, stream>>>(none_view,
+            no_frame, P, Q, rays, b, fetch + 2 * b, refill, nullptr, B);
+      });
     Queues QS = Q;
     if (keyed && b + 1 < rounds) cudaMemsetAsync(Q.bins, 0, sizeof(uint32_t) * kSortBins, stream);
     else QS.keys = nullptr;
-    if (B.analytic)
-      k_wf_shade<false, true, true><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, QS, b, no_cache, B);
-    else
-      k_wf_shade<false, true, false><<<grid_shade, kBlock, 0, stream>>>(none_view, B.frames, P, QS, b, no_cache, B);
-    if (B.analytic)
+    with_features(B.analytic, B.textured, [&](auto a, auto x) {
+      k_wf_shade<false, true, decltype(a)::value, decltype(x)::value><<<grid_shade, kBlock, 0, stream>>>(none_view,
+          B.frames, P, QS, b, no_cache, B);
+    });
+    if (B.textured)
       k_wf_shadow<false, true, true><<<grid_shadow, kBlock, 0, stream>>>(none_view, P, Q, b, fetch + 2 * b + 1,
           refill, nullptr, B);
     else
@@ -1482,12 +1492,11 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   }
   if (rounds <= max_bounces) {
     uint32_t* cursor = fetch + 2 * (max_bounces + 1);
-    const uint32_t grid_tail = persistent_grid(
-        B.analytic ? (const void*)k_wf_tail<true, true> : (const void*)k_wf_tail<true, false>, Q.capacity, tuning);
-    if (B.analytic)
-      k_wf_tail<true, true><<<grid_tail, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rounds, cursor, B);
-    else
-      k_wf_tail<true, false><<<grid_tail, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rounds, cursor, B);
+    with_features(B.analytic, B.textured, [&](auto a, auto x) {
+      const auto kernel = k_wf_tail<true, decltype(a)::value, decltype(x)::value>;
+      const uint32_t grid_tail = persistent_grid((const void*)kernel, Q.capacity, tuning);
+      kernel<<<grid_tail, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rounds, cursor, B);
+    });
   }
   if (before_resolve) cudaStreamWaitEvent(stream, before_resolve, 0);
   k_wf_resolve<true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, accum, color, B);

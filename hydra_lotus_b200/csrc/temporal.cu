@@ -40,6 +40,7 @@ constexpr int kRestirBlocksPerSm = 6;
 // ---------------------------------------------------------------------------
 // WriteTemporalSurface (temporal.slang:557-627): the pixel centre's primary
 // hit, with a fixed coverage sequence (sample 0).
+template <bool kTextured>
 __global__ void __launch_bounds__(kBlock) k_temporal_surface(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     const TemporalInstance* __restrict__ identities, TemporalPixel* __restrict__ out) {
@@ -56,7 +57,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal_surface(SceneView S,
     float tmax;
     camera_ray(f, cx * f.ndc[0] + f.ndc[2], cy * f.ndc[1] + f.ndc[3], ro, rd, tmax);
     Hit hit;
-    if (trace_closest(S, ro, rd, 0.0f, tmax, rng, hit)) {
+    if (trace_closest<false, kTextured>(S, ro, rd, 0.0f, tmax, rng, hit)) {
       const InstanceShading rec = S.inst_shade[hit.instance];
       const TemporalInstance id = identities[hit.instance];
       const float4* tv = S.tris + kTriStride * (size_t)hit.tri;
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal_surface(SceneView S,
         o.instance_id = id.instance_id;
         o.material_id = id.material_id;
         o.flags = 1u | id.flags;
-        const SurfaceHit sh = reconstruct_hit(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
+        const SurfaceHit sh = reconstruct_hit<kTextured>(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
         // The surface summary's albedo (scene.slang:1254-1257).
         const F3 albedo = sh.bsdf.transmission > 0.0f
             ? sh.base_color + sh.bsdf.transmission * (sh.bsdf.transmission_color - sh.base_color)
@@ -205,10 +206,11 @@ __device__ __forceinline__ F3 history_contribution(const SceneView& S, const Res
       (S.lights[light].pdf / ls.pdf);
 }
 
+template <bool kTextured>
 __device__ __forceinline__ F3 history_contribution_uv(const SceneView& S, const RestirSurface& src,
     uint32_t light, const float* uv) {
   return history_contribution(S, src, light,
-      reconstruct_reservoir_light(S, light, uv[0], uv[1], V(src.origin)));
+      reconstruct_reservoir_light<true, kTextured>(S, light, uv[0], uv[1], V(src.origin)));
 }
 
 __device__ __forceinline__ bool same_sample(const RestirPixel& a, const RestirPixel& b) {
@@ -216,13 +218,14 @@ __device__ __forceinline__ bool same_sample(const RestirPixel& a, const RestirPi
 }
 
 // HistoryTarget (restir.slang:276-285).
+template <bool kTextured>
 __device__ __forceinline__ float history_target(const SceneView& S, const RestirReuse& source,
     const RestirSurface& surface, const RestirPixel& selected, bool& valid) {
   if (same_sample(source.pixel, selected)) {
     valid = isfinite(source.pixel.reservoir.selected_target);
     return source.pixel.reservoir.selected_target;
   }
-  const F3 c = history_contribution_uv(S, surface, selected.reservoir.sample, selected.uv);
+  const F3 c = history_contribution_uv<kTextured>(S, surface, selected.reservoir.sample, selected.uv);
   valid = is_finite(c);
   return max_component(c);
 }
@@ -277,6 +280,7 @@ __device__ __forceinline__ RestirPixel empty_restir_pixel() {
 // WriteInitialReservoir (restir.slang:163-233): M candidates streamed over
 // the light table at the jittered camera surface, then one shadow ray for
 // the selected sample (queued for the deferred visibility, pass 0).
+template <bool kTextured>
 __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     RestirPixel* __restrict__ out, uint4* __restrict__ primary_hit, uint32_t* __restrict__ primary_rng,
@@ -294,13 +298,13 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
     uint32_t camera_rng;
     start_path(f, px, py, f.sample_index, ro, rd, tmax, camera_rng);
     Hit hit;
-    const bool found = trace_closest(S, ro, rd, 0.0f, tmax, camera_rng, hit);
+    const bool found = trace_closest<false, kTextured>(S, ro, rd, 0.0f, tmax, camera_rng, hit);
     primary_hit[slot] = found ? make_uint4(hit.instance, hit.tri, __float_as_uint(hit.b1), __float_as_uint(hit.b2))
                               : make_uint4(kNoPrimaryHit, 0u, 0u, 0u);
     primary_rng[slot] = camera_rng;
     if (found) {
       r.flags |= 1u;
-      const SurfaceHit sh = reconstruct_hit(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
+      const SurfaceHit sh = reconstruct_hit<kTextured>(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
       const Frame basis = make_frame(sh.shading_normal);
       const F3 wo = basis.to_local(-rd);
       const F3 origin = offset_ray_origin(sh.position, sh.normal);
@@ -314,7 +318,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
           const float random = next_random(rng);
           const uint32_t light = choose_reservoir_light(S, tc.restir_proposal, cx, cy);
           const float proposal = reservoir_proposal_pdf(S, tc.restir_proposal, light);
-          const LightSample ls = reconstruct_reservoir_light(S, light, ux, uy, origin);
+          const LightSample ls = reconstruct_reservoir_light<true, kTextured>(S, light, ux, uy, origin);
           const F3 fc = candidate_contribution(sh, basis, wo, ls, S.lights[light].pdf);
           bool selected;
           if (!isfinite(ls.pdf) || !is_finite(fc) ||
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
         }
       }
       if ((r.flags & 2u) == 0 && r.reservoir.weight_sum > 0.0f) {
-        const LightSample ls = reconstruct_reservoir_light(S, r.reservoir.sample, r.uv[0], r.uv[1], origin);
+        const LightSample ls = reconstruct_reservoir_light<true, kTextured>(S, r.reservoir.sample, r.uv[0], r.uv[1], origin);
         queue_visibility(VQ, 0, slot, origin, ls,
             candidate_contribution(sh, basis, wo, ls, S.lights[r.reservoir.sample].pdf),
             reservoir_normalization(r.reservoir));
@@ -342,6 +346,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
 }
 
 // WriteTemporalReservoir (restir.slang:302-387).
+template <bool kTextured>
 __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     const uint4* __restrict__ primary_hit, const TemporalInstance* __restrict__ identities, const RestirPixel* __restrict__ initial,
@@ -368,7 +373,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
     // The camera ray's hit as the initial pass traced it.
     const uint4 ph = primary_hit[slot];
     if (ph.x != kNoPrimaryHit) {
-      const SurfaceHit sh = reconstruct_hit(S, ph.x, ph.y, __uint_as_float(ph.z), __uint_as_float(ph.w), rd);
+      const SurfaceHit sh = reconstruct_hit<kTextured>(S, ph.x, ph.y, __uint_as_float(ph.z), __uint_as_float(ph.w), rd);
       const Frame basis = make_frame(sh.shading_normal);
       const F3 wo = basis.to_local(-rd);
       const F3 origin = offset_ray_origin(sh.position, sh.normal);
@@ -395,7 +400,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
             if (source.pixel.reservoir.sample >= S.light_count)
               result.pixel.flags |= 2u;
             else
-              received = history_contribution_uv(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
+              received = history_contribution_uv<kTextured>(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
           }
           uint32_t rng = seed_random(slot, f.sample_index ^ 0x94D049BBu);
           bool selected;
@@ -413,7 +418,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
             }
             if (result.pixel.reservoir.weight_sum > 0.0f) {
               bool valid_support;
-              const float support = history_target(S, source, psrc, result.pixel, valid_support);
+              const float support = history_target<kTextured>(S, source, psrc, result.pixel, valid_support);
               if (!valid_support) result.pixel.flags |= 2u;
               result.supporting_candidates = initial[slot].reservoir.candidate_count + (support > 0.0f ? count : 0u);
             } else {
@@ -424,7 +429,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
         }
       }
       if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
-        const LightSample ls = reconstruct_reservoir_light(S, result.pixel.reservoir.sample,
+        const LightSample ls = reconstruct_reservoir_light<true, kTextured>(S, result.pixel.reservoir.sample,
             result.pixel.uv[0], result.pixel.uv[1], origin);
         receiver_estimate(VQ, 1, slot, initial[slot], origin, ls,
             history_contribution(S, receiver, result.pixel.reservoir.sample, ls), result.normalization,
@@ -488,6 +493,7 @@ __device__ __forceinline__ int spatial_offsets(uint32_t slot, uint32_t sample_in
 
 // WriteSpatialReservoir (restir.slang:402-491): the neighbours above,
 // merged with support correction.
+template <bool kTextured>
 __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     const RestirReuse* __restrict__ temporal, const RestirSurface* __restrict__ surfaces,
@@ -528,7 +534,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
         const RestirReuse source = temporal[sources[i]];
         F3 received = V(0.0f);
         if (source.pixel.reservoir.weight_sum > 0.0f)
-          received = history_contribution_uv(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
+          received = history_contribution_uv<kTextured>(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
         if (!is_finite(received) ||
             !merge_reevaluated(result.pixel.reservoir, source.pixel.reservoir, source.normalization,
                 max_component(received), tc.restir_max_history, next_random(rng), selected)) {
@@ -550,7 +556,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
           if (sources[i] == 0xffffffffu) continue;
           const RestirReuse source = temporal[sources[i]];
           bool valid_support;
-          const float support = history_target(S, source, surfaces[sources[i]], result.pixel, valid_support);
+          const float support = history_target<kTextured>(S, source, surfaces[sources[i]], result.pixel, valid_support);
           if (!valid_support) result.pixel.flags |= 2u;
           if (support > 0.0f)
             result.supporting_candidates += min(source.pixel.reservoir.candidate_count, tc.restir_max_history);
@@ -558,7 +564,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
       }
       result.normalization = reuse_normalization(result.pixel.reservoir, result.supporting_candidates);
       if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
-        const LightSample ls = reconstruct_reservoir_light(S, result.pixel.reservoir.sample,
+        const LightSample ls = reconstruct_reservoir_light<true, kTextured>(S, result.pixel.reservoir.sample,
             result.pixel.uv[0], result.pixel.uv[1], V(receiver.origin));
         receiver_estimate(VQ, 2, slot, centre.pixel, V(receiver.origin), ls,
             history_contribution(S, receiver, result.pixel.reservoir.sample, ls), result.normalization,
@@ -849,7 +855,8 @@ inline uint32_t grid(uint32_t n) { return (n + kBlock - 1) / kBlock; }
 
 void launch_temporal_surface(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
     const TemporalInstance* ids, TemporalPixel* out, uint32_t pixels, cudaStream_t s) {
-  k_temporal_surface<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, ids, out);
+  if (S.textured) k_temporal_surface<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, ids, out);
+  else k_temporal_surface<false><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, ids, out);
 }
 
 void launch_reproject(const TemporalConst* tc, const TemporalPixel* current, const TemporalPixel* previous,
@@ -860,7 +867,8 @@ void launch_reproject(const TemporalConst* tc, const TemporalPixel* current, con
 void launch_restir_initial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
     RestirPixel* out, uint4* primary_hit, uint32_t* primary_rng, const VisibilityQueue& vq, uint32_t pixels,
     cudaStream_t s) {
-  k_restir_initial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out, primary_hit, primary_rng, vq);
+  if (S.textured) k_restir_initial<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out, primary_hit, primary_rng, vq);
+  else k_restir_initial<false><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out, primary_hit, primary_rng, vq);
 }
 
 void launch_restir_temporal(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
@@ -868,14 +876,19 @@ void launch_restir_temporal(const SceneView& S, const FrameConst* fc, const Temp
     const ValidityPixel* validity, const TemporalPixel* surface, const RestirReuse* previous,
     const RestirSurface* previous_surfaces, RestirReuse* out, RestirSurface* out_surfaces,
     const VisibilityQueue& vq, uint32_t pixels, cudaStream_t s) {
-  k_restir_temporal<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, primary_hit, ids, initial, validity, surface, previous,
-      previous_surfaces, out, out_surfaces, vq);
+  if (S.textured)
+    k_restir_temporal<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, primary_hit, ids, initial, validity, surface,
+        previous, previous_surfaces, out, out_surfaces, vq);
+  else
+    k_restir_temporal<false><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, primary_hit, ids, initial, validity, surface,
+        previous, previous_surfaces, out, out_surfaces, vq);
 }
 
 void launch_restir_spatial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
     const RestirReuse* temporal, const RestirSurface* surfaces, RestirReuse* out, uint4* sources,
     const VisibilityQueue& vq, uint32_t pixels, cudaStream_t s) {
-  k_restir_spatial<<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, temporal, surfaces, out, sources, vq);
+  if (S.textured) k_restir_spatial<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, temporal, surfaces, out, sources, vq);
+  else k_restir_spatial<false><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, temporal, surfaces, out, sources, vq);
 }
 
 void launch_svgf(const TemporalConst* tc, const TemporalConst& host_tc, const float4* batch,

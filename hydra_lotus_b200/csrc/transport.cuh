@@ -642,7 +642,7 @@ static __device__ __noinline__ F3 crossed_lights(const SceneView& S, F3 origin, 
 // SampleLight (scene.slang:894-909): Vose's alias table, then a point.
 // kAnalytic = false leaves out the analytic lights' code, for scenes
 // without them.
-template <bool kAnalytic = true>
+template <bool kAnalytic = true, bool kTextured = true>
 __device__ __forceinline__ LightSample sample_light(const SceneView& S, float u0, float u1,
     float u2, float u3, F3 origin) {
   const uint32_t count = S.light_count;
@@ -653,7 +653,7 @@ __device__ __forceinline__ LightSample sample_light(const SceneView& S, float u0
   if (chosen.instance == kEnvironmentLight) return sample_environment(S, chosen.pdf, u2, u3);
   if (kAnalytic && (chosen.instance & kAnalyticLight) != 0)
     return sample_analytic(S.analytic[chosen.instance & ~kAnalyticLight], chosen.pdf, u2, u3, origin);
-  return sample_triangle<kAnalytic>(S, light, chosen.pdf, u2, u3, origin);
+  return sample_triangle<kTextured>(S, light, chosen.pdf, u2, u3, origin);
 }
 
 // EmitterPdf (scene.slang:1004-1010).
