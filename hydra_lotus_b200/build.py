@@ -28,7 +28,7 @@ FUSED = {"radiance_cache.cu", "bvh_build.cu"}
 
 def _inputs():
     files = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
-             if f.endswith((".cu", ".cuh", ".h"))]
+             if f.endswith((".cu", ".cuh", ".h", ".inc"))]
     files += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
     return files
 
@@ -67,6 +67,26 @@ def build(force=False, verbose=False, jobs=None):
     return LIB
 
 
+# The albedo tables' generator (csrc/albedo_tables_gen.cpp), which wrote
+# csrc/albedo_tables.inc and checks it: a host program.
+TABLE_TOOL = os.path.join(LIB_DIR, "albedo_tables_gen")
+
+
+def build_table_tool(force=False, verbose=False):
+    """Builds the albedo tables' generator; returns its path."""
+    src = os.path.join(CSRC, "albedo_tables_gen.cpp")
+    inputs = [src, os.path.join(CSRC, "albedo.cuh"), os.path.join(CSRC, "lmath.cuh")]
+    if (not force and os.path.exists(TABLE_TOOL) and
+            all(os.path.getmtime(p) <= os.path.getmtime(TABLE_TOOL) for p in inputs)):
+        return TABLE_TOOL
+    os.makedirs(LIB_DIR, exist_ok=True)
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-ffp-contract=off", src, "-o", TABLE_TOOL, "-lpthread"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return TABLE_TOOL
+
+
 # The C++ adapter (host/cuda_offscreen_renderer.*) implements the
 # reference's Lotus::OffscreenRenderer over the C ABI; it compiles against
 # the reference's headers, so it builds only where they are present
@@ -103,4 +123,5 @@ def build_host(force=False, verbose=False):
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
+    build_table_tool(force="--force" in sys.argv, verbose=True)
     build_host(force="--force" in sys.argv, verbose=True)

@@ -16,7 +16,13 @@
 // 1e-10 for |t| <= tan(pi/8)). acos(x) = atan2(sqrt((1 - x)(1 + x)), x).
 #pragma once
 
+#if defined(__CUDACC__)
 #include <cuda_runtime.h>
+#endif
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
 
 namespace lotus {
 
@@ -94,6 +100,81 @@ LOTUS_HD float lacos(float x) { return latan2(sqrtf((1.0f - x) * (1.0f + x)), x)
 LOTUS_HD float lpow5(float x) {
   const float x2 = x * x;
   return x2 * x2 * x;
+}
+
+LOTUS_HD uint32_t lbits(float x) {
+#if defined(__CUDA_ARCH__)
+  return __float_as_uint(x);
+#else
+  uint32_t u;
+  memcpy(&u, &x, sizeof(u));
+  return u;
+#endif
+}
+
+LOTUS_HD float lfloat(uint32_t u) {
+#if defined(__CUDA_ARCH__)
+  return __uint_as_float(u);
+#else
+  float x;
+  memcpy(&x, &u, sizeof(x));
+  return x;
+#endif
+}
+
+// Natural logarithm for finite x > 0 (-infinity at 0, NaN below). The
+// argument is split as m * 2^e with m in [sqrt(1/2), sqrt(2)), and
+// log(m) = 2 atanh(s), s = (m - 1) / (m + 1), |s| <= 0.1716, by its
+// series to s^15 (remainder below 1e-13); e * log(2) is added in two
+// parts, the first exact for |e| < 2^9.
+LOTUS_HD float llog(float x) {
+  if (!(x > 0.0f)) return x == 0.0f ? -lfloat(0x7f800000u) : lfloat(0x7fc00000u);
+  int e = 0;
+  if (x < 1.17549435e-38f) {
+    x *= 8388608.0f;  // 2^23: a subnormal becomes normal
+    e = -23;
+  }
+  const uint32_t b = lbits(x);
+  e += (int)((b >> 23) & 0xffu) - 127;
+  float m = lfloat((b & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.41421354f) {
+    m *= 0.5f;
+    e += 1;
+  }
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float s2 = s * s;
+  const float p = s2 * (0.333333343f + s2 * (0.2f + s2 * (0.142857149f + s2 * (0.111111112f +
+      s2 * (0.0909090936f + s2 * (0.0769230798f + s2 * 0.0666666701f))))));
+  const float log_m = 2.0f * s + 2.0f * s * p;
+  const float fe = (float)e;
+  return fe * 0.693145751953125f + (fe * 1.42860677e-6f + log_m);
+}
+
+// e^x: x = k log(2) + r with |r| <= log(2)/2 (Cody and Waite's reduction,
+// log(2) in the same two parts as above), e^r by its Taylor series to r^8
+// (remainder below 4e-9 relative), times 2^k assembled from bits.
+LOTUS_HD float lexp(float x) {
+  if (!(x > -104.0f)) return x == x ? 0.0f : x;
+  if (x > 89.0f) return lfloat(0x7f800000u);
+  const float k = rintf(x * 1.44269502f);
+  const float r = (x - k * 0.693145751953125f) - k * 1.42860677e-6f;
+  const float p = 1.0f + r * (1.0f + r * (0.5f + r * (0.166666672f + r * (0.0416666679f +
+      r * (0.00833333377f + r * (0.00138888892f + r * (0.000198412701f + r * 2.48015876e-5f)))))));
+  int ki = (int)k;
+  float scale = 1.0f;
+  if (ki < -126) {
+    ki += 64;
+    scale = 5.42101086e-20f;  // 2^-64
+  } else if (ki > 127) {
+    ki -= 1;
+    scale = 2.0f;
+  }
+  return p * lfloat((uint32_t)(ki + 127) << 23) * scale;
+}
+
+// x^y for x >= 0 and y > 0.
+LOTUS_HD float lpow(float x, float y) {
+  return x > 0.0f ? lexp(y * llog(x)) : 0.0f;
 }
 
 }  // namespace lotus

@@ -36,6 +36,18 @@ little-endian; ReadPfm, adapters/common/reference.cpp:100-131):
   (adapters/common/material_fixtures.cpp:875-1009: constant emitters and
   emission maps, float images included) at 160x160, 4096 samples per
   pixel.
+- material_gltf_v1.npz and material_gltf_extensions_v1.npz: the
+  material-gltf-v1 and material-gltf-extensions-v1 fixtures
+  (adapters/common/material_fixtures.cpp:2035-2300: MaterialX's glTF PBR
+  surface, its core and its extensions) at 160x160, 4096 samples per
+  pixel.
+
+It also writes albedo_tables_reference.npz: every 7th value of the
+reference's directional albedo tables (backend/vulkan/
+bsdf-albedo-tables.inc, 76800 floats in albedo.slang's layout) with its
+index, which the library's own tables are compared with.
+
+Arguments name the fixtures to write (file names); none writes all.
 """
 
 import os
@@ -54,7 +66,21 @@ FIXTURES = [("cornell-box", "cornell_box.npz", 1024),
             ("material-normals-v1", "material_normals_v1.npz", 4096),
             ("material-transmission-v1", "material_transmission_v1.npz", 4096),
             ("material-transforms-v1", "material_transforms_v1.npz", 4096),
-            ("material-emission-v1", "material_emission_v1.npz", 4096)]
+            ("material-emission-v1", "material_emission_v1.npz", 4096),
+            ("material-gltf-v1", "material_gltf_v1.npz", 4096),
+            ("material-gltf-extensions-v1", "material_gltf_extensions_v1.npz", 4096)]
+TABLES = "albedo_tables_reference.npz"
+TABLE_STRIDE = 7
+
+
+def read_table_inc(path):
+    values = []
+    with open(path) as f:
+        for line in f:
+            if line.startswith("//"):
+                continue
+            values += [float(v) for v in line.strip().split(",") if v.strip()]
+    return np.array(values, dtype=np.float32)
 
 
 def read_pfm(path):
@@ -74,12 +100,21 @@ def main():
     if not os.path.isdir(ref):
         print(f"no reference tree at {REFERENCE}; set LOTUS_REFERENCE", file=sys.stderr)
         return 1
+    wanted = set(sys.argv[1:])
     for stem, name, samples in FIXTURES:
+        if wanted and name not in wanted:
+            continue
         mean = read_pfm(os.path.join(ref, f"{stem}-mean.pfm"))
         variance = read_pfm(os.path.join(ref, f"{stem}-variance.pfm"))
         out = os.path.join(HERE, name)
         np.savez_compressed(out, mean=mean, variance=variance, samples=np.uint32(samples))
         print("wrote", out, mean.shape)
+    if not wanted or TABLES in wanted:
+        table = read_table_inc(os.path.join(REFERENCE, "backend", "vulkan", "bsdf-albedo-tables.inc"))
+        index = np.arange(0, table.size, TABLE_STRIDE, dtype=np.uint32)
+        out = os.path.join(HERE, TABLES)
+        np.savez_compressed(out, index=index, value=table[index], size=np.uint32(table.size))
+        print("wrote", out, index.size)
     return 0
 
 
