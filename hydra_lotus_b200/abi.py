@@ -62,12 +62,28 @@ SLOT_ROUGHNESS = 3
 SLOT_METALLIC = 4
 SLOT_EMISSION = 5
 SLOT_SPECULAR_COLOR = 6
-TEXTURE_SLOTS = 7
+# glTF PBR's slots (0 and 1 are the geometry's, as above).
+GLTF_SLOT_BASE_COLOR = 2
+GLTF_SLOT_METALLIC = 3
+GLTF_SLOT_ROUGHNESS = 4
+GLTF_SLOT_EMISSIVE = 5
+GLTF_SLOT_SPECULAR = 6
+GLTF_SLOT_SPECULAR_COLOR = 7
+GLTF_SLOT_TRANSMISSION = 8
+GLTF_SLOT_CLEARCOAT = 9
+GLTF_SLOT_CLEARCOAT_ROUGHNESS = 10
+GLTF_SLOT_CLEARCOAT_NORMAL = 11
+GLTF_SLOT_SHEEN_COLOR = 12
+GLTF_SLOT_SHEEN_ROUGHNESS = 13
+TEXTURE_SLOTS = 14
 
 MATERIAL_SPECULAR_WORKFLOW = 1
 MATERIAL_THIN_WALLED = 2
+# lotus_material::model (ShadingModel).
+MODEL_PREVIEW_SURFACE = 0
+MODEL_GLTF_PBR = 1
 
-ABI_VERSION = 9
+ABI_VERSION = 10
 
 # lotus_settings::output (SceneOutput).
 OUTPUT_RADIANCE = 0
@@ -137,10 +153,17 @@ class Material(C.Structure):
         ("opacity", C.c_float),
         ("opacity_threshold", C.c_float),
         ("flags", C.c_uint32),
-        ("reserved", C.c_uint32),
-        ("lookups", C.c_uint32 * 7),  # per SLOT_*: k > 0 for texture_inputs[k - 1]; 0: the constant
+        ("model", C.c_uint32),  # MODEL_*
+        ("lookups", C.c_uint32 * 14),  # per slot: k > 0 for texture_inputs[k - 1]; 0: the constant
         ("texcoord_fallback", C.c_float * 2),
         ("normal", C.c_float * 3),  # tangent-space shading normal; all zero: (0, 0, 1)
+        # glTF PBR's inputs beyond the shared fields above.
+        ("emissive_strength", C.c_float),
+        ("specular", C.c_float),
+        ("clearcoat", C.c_float),
+        ("clearcoat_roughness", C.c_float),
+        ("sheen_color", C.c_float * 3),
+        ("sheen_roughness", C.c_float),
     ]
 
 

@@ -362,7 +362,7 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
   cudaError_t e = ensure_buffers(*b, base[count], count);
   if (e != cudaSuccess) return fail(std::string("batch buffers: ") + cudaGetErrorString(e), true);
   std::vector<SceneView> views(count);
-  bool analytic = false, textured = false;
+  bool analytic = false, full_shading = false;
   // Every scene's walks report to the first scene's walk-failure words.
   uint32_t* walk_failure = nullptr;
   uint32_t step_limit = 0;
@@ -376,7 +376,7 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
     }
     views[k].walk_failure = walk_failure;
     analytic = analytic || a.view->analytic_count != 0;
-    textured = textured || a.view->textured != 0;
+    full_shading = full_shading || a.view->full_shading != 0;
   }
   SceneTable B;
   B.views = b->views;
@@ -385,7 +385,7 @@ extern "C" int32_t lotus_cuda_batch_render(lotus_cuda_batch* b, const lotus_fram
   B.count = count;
   B.total_slots = base[count];
   B.analytic = analytic;
-  B.textured = textured;
+  B.full_shading = full_shading;
   {
     // Warp tiles where every scene's size is a multiple of the tile.
     const uint32_t tile = b->tuning.camera_tile ? b->tuning.camera_tile : kDefaultBatchCameraTile;

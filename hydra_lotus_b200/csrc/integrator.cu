@@ -153,7 +153,8 @@ __device__ __forceinline__ F3 shadow_contribution(F3 fl, float weight, float pdf
 // parallel lights, which no sampled direction finds, each through its own
 // shadow ray traced here, as ShadowedLight carries a delta light. Not
 // inlined: the shading kernels hold none of the walk's registers for it.
-__device__ __noinline__ F3 parallel_lights(const SceneView& S, F3 position, F3 normal, const Closure& bsdf,
+template <bool kFullShading>
+__device__ __noinline__ F3 parallel_lights(const SceneView& S, F3 position, F3 normal, const SurfaceHit& sh,
     const Frame& basis, F3 wo, uint32_t& shadow_rays) {
   const F3 origin = offset_ray_origin(position, normal);
   F3 sum = V(0.0f);
@@ -163,7 +164,7 @@ __device__ __noinline__ F3 parallel_lights(const SceneView& S, F3 position, F3 n
     if (ls.pdf > 0.0f && max_component(ls.radiance) > 0.0f && dot(ls.direction, normal) > 0.0f) {
       const F3 wi = basis.to_local(ls.direction);
       if (wi.z > 0.0f) {
-        const F3 fv = bsdf_evaluate(bsdf, wo, wi);
+        const F3 fv = surface_evaluate<kFullShading>(sh, wo, wi);
         if (max_component(fv) > 0.0f) {
           ++shadow_rays;
           const float tr = trace_shadow(S, origin, ls.direction, 0.0f, ls.distance);
@@ -194,10 +195,10 @@ struct ShadowRequest {
 // crossed, applies Russian roulette, prepares next event estimation's
 // shadow ray (under BSDF sampling, traces the parallel lights' own) and
 // samples the BSDF. Returns whether the path continues along (new_o, new_d).
-// kAnalytic: the scene may have analytic lights; kTextured: texture
-// lookups (SceneView::textured). The instantiations without carry none of
-// their code or registers.
-template <bool kAnalytic, bool kTextured>
+// kAnalytic: the scene may have analytic lights; kFullShading: texture
+// lookups or glTF PBR materials (SceneView::full_shading). The
+// instantiations without carry none of their code or registers.
+template <bool kAnalytic, bool kFullShading>
 __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     uint32_t instance, uint32_t tri, float b1, float b2, F3 ray_o, F3 ray_d, uint32_t depth,
     F3& T, F3& R, float& last_pdf, uint32_t& flags, uint32_t& rng, F3& new_o, F3& new_d,
@@ -205,7 +206,7 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
   req.pending = false;
   req.inline_shadow = 0;
   uint32_t primitive;
-  const SurfaceHit sh = reconstruct_hit<kTextured>(S, instance, tri, b1, b2, ray_d, &primitive);
+  const SurfaceHit sh = reconstruct_hit<kFullShading>(S, instance, tri, b1, b2, ray_d, &primitive);
   if (features) {
     // The radiance cache's description of this vertex, seen from the ray.
     const F3 albedo = sh.bsdf.transmission > 0.0f
@@ -250,11 +251,11 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
         f.restir_final + (size_t)pixel_index * f.restir_stride);
     if ((sel.flags & 2u) == 0 && sel.reservoir.weight_sum > 0.0f && sel.reservoir.sample < S.light_count) {
       const F3 origin = offset_ray_origin(sh.position, sh.normal);
-      const LightSample ls = reconstruct_reservoir_light<kAnalytic, kTextured>(S, sel.reservoir.sample, sel.uv[0], sel.uv[1], origin);
+      const LightSample ls = reconstruct_reservoir_light<kAnalytic, kFullShading>(S, sel.reservoir.sample, sel.uv[0], sel.uv[1], origin);
       const F3 wi = basis.to_local(ls.direction);
       const float weight = ls.delta ? 1.0f
           : power_heuristic(kAnalytic ? reservoir_partition_pdf(S, sel.reservoir.sample, ls, origin) : ls.pdf,
-                wi.z > 0.0f ? bsdf_pdf(sh.bsdf, wo, wi) : 0.0f);
+                wi.z > 0.0f ? surface_pdf<kFullShading>(sh, wo, wi) : 0.0f);
       R = R + T * (V(sel.contribution) * weight);
     } else {
       R = R + T * V(0.0f);
@@ -267,25 +268,25 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
     const float u2 = next_random(rng);
     const float u3 = next_random(rng);
     const F3 origin = offset_ray_origin(sh.position, sh.normal);
-    const LightSample ls = sample_light<kAnalytic, kTextured>(S, u0, u1, u2, u3, origin);
+    const LightSample ls = sample_light<kAnalytic, kFullShading>(S, u0, u1, u2, u3, origin);
     if (ls.pdf > 0.0f && max_component(ls.radiance) > 0.0f && dot(ls.direction, sh.normal) > 0.0f) {
       const F3 wi = basis.to_local(ls.direction);
       if (wi.z > 0.0f) {
-        const F3 fv = bsdf_evaluate(sh.bsdf, wo, wi);
+        const F3 fv = surface_evaluate<kFullShading>(sh, wo, wi);
         if (max_component(fv) > 0.0f) {
           req.pending = true;
           req.origin = origin;
           req.direction = ls.direction;
           req.tmax = ls.distance;
           req.fl = fv * ls.radiance;
-          req.weight = ls.delta ? 1.0f : power_heuristic(ls.pdf, bsdf_pdf(sh.bsdf, wo, wi));
+          req.weight = ls.delta ? 1.0f : power_heuristic(ls.pdf, surface_pdf<kFullShading>(sh, wo, wi));
           req.pdf = ls.pdf;
           req.throughput = T;
         }
       }
     }
   } else if (kAnalytic && !f.sample_lights && S.analytic_count != 0) {
-    R = R + T * parallel_lights(S, sh.position, sh.normal, sh.bsdf, basis, wo, req.inline_shadow);
+    R = R + T * parallel_lights<kFullShading>(S, sh.position, sh.normal, sh, basis, wo, req.inline_shadow);
   }
   // A path that ends into the radiance cache stops after next event
   // estimation at its cache vertex: the cache stands for the light the
@@ -296,7 +297,7 @@ __device__ __forceinline__ bool scatter(const SceneView& S, const FrameConst& f,
   u.y = next_random(rng);
   u.z = next_random(rng);
   BsdfSample s;
-  if (!bsdf_sample(sh.bsdf, wo, u, s)) return false;
+  if (!surface_sample<kFullShading>(sh, wo, u, s)) return false;
   const F3 wi = normalize(basis.to_world(s.wi));
   const float side = dot(wi, sh.normal);
   if (s.transmitted ? side >= 0.0f : side <= 0.0f) return false;
@@ -360,7 +361,7 @@ __device__ __forceinline__ double4 add4(double4 a, float4 s) {
 // The reference integrator: one thread follows one camera path to its end
 // (path_trace.slang:279-287, 353-385), then adds it to the pixel's FP64
 // accumulation and writes the mean.
-template <bool kCount, bool kAnalytic, bool kTextured>
+template <bool kCount, bool kAnalytic, bool kFullShading>
 __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
     const FrameConst* __restrict__ fcp, double4* __restrict__ accum, float4* __restrict__ color,
     RayTotals* totals, VisitCounters* visits) {
@@ -381,26 +382,26 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
       start_path(f, px, py, f.sample_index, o, d, tmax, rng);
       ++n_camera;
       Hit hit;
-      if (trace_closest<kCount, kTextured>(S, o, d, 0.0f, tmax, rng, hit, &vc[0])) {
+      if (trace_closest<kCount, kFullShading>(S, o, d, 0.0f, tmax, rng, hit, &vc[0])) {
         F3 T = V(1.0f), R = V(0.0f);
         float last_pdf = 0.0f;
         uint32_t flags = 0;
         for (uint32_t depth = 0;; ++depth) {
           F3 no, nd;
           ShadowRequest req;
-          const bool cont = scatter<kAnalytic, kTextured>(S, f, hit.instance, hit.tri, hit.b1, hit.b2, o, d, depth, T, R,
+          const bool cont = scatter<kAnalytic, kFullShading>(S, f, hit.instance, hit.tri, hit.b1, hit.b2, o, d, depth, T, R,
               last_pdf, flags, rng, no, nd, req, slot);
           n_shadow += req.inline_shadow;
           if (req.pending) {
             ++n_shadow;
-            const float tr = trace_shadow<kCount, kTextured>(S, req.origin, req.direction, 0.0f, req.tmax, &vc[2]);
+            const float tr = trace_shadow<kCount, kFullShading>(S, req.origin, req.direction, 0.0f, req.tmax, &vc[2]);
             if (tr > 0.0f) R = R + req.throughput * shadow_contribution(req.fl, req.weight, req.pdf, tr);
           }
           if (!cont) break;
           o = no;
           d = nd;
           ++n_extension;
-          if (!trace_closest<kCount, kTextured>(S, o, d, 0.0f, kFloatMax, rng, hit, &vc[1])) {
+          if (!trace_closest<kCount, kFullShading>(S, o, d, 0.0f, kFloatMax, rng, hit, &vc[1])) {
             R = miss_path<kAnalytic>(S, f, o, d, flags, last_pdf, T, R);
             break;
           }
@@ -433,7 +434,7 @@ __global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
 // In a batch (kBatch) one thread per path slot of every scene, in each
 // image's row order or in the table's warp tiles; otherwise 8x4 pixel
 // tiles per warp.
-template <bool kCount, bool kBatch, bool kTextured>
+template <bool kCount, bool kBatch, bool kFullShading>
 __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, VisitCounters* visits, SceneTable B) {
   TraversalCounters vc = {0, 0, 0};
@@ -487,7 +488,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
       hit.b2 = __uint_as_float(ph.w);
       rng = f.primary_rng[slot];
     } else {
-      found = trace_closest<kCount, kTextured>(SS, o, d, 0.0f, tmax, rng, hit, &vc);
+      found = trace_closest<kCount, kFullShading>(SS, o, d, 0.0f, tmax, rng, hit, &vc);
     }
     if (found) {
       P.direction[slot] = F4(d, tmax);
@@ -519,7 +520,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
 // Compiled for six resident blocks per SM (80 registers): shading is
 // latency-bound and gains more from occupancy than from registers.
 constexpr int kShadeBlocksPerSm = 6;
-template <bool kCacheVertex, bool kBatch, bool kAnalytic, bool kTextured>
+template <bool kCacheVertex, bool kBatch, bool kAnalytic, bool kFullShading>
 __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 1];
@@ -570,7 +571,7 @@ __global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneVie
       if (cache_vertex)
         training = pcg_hash(slot ^ pcg_hash(f.sample_index ^ 0xC2B2AE35u)) % C.stride == 0u;
       F3 no, nd;
-      cont = scatter<kAnalytic, kTextured>(SS, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
+      cont = scatter<kAnalytic, kFullShading>(SS, f, h.x, h.y, __uint_as_float(h.z), __uint_as_float(h.w), ro, V(dir), bounce,
           T, R, last_pdf, flags, rng, no, nd, req, slot, cache_vertex ? &features : nullptr,
           cache_vertex && !training);
       query = cache_vertex && !training;
@@ -691,7 +692,7 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor, uint32_t n, boo
 // ShadowedLight's visibility (transport.slang:82-115) for the shadow queue,
 // as a persistent kernel: each lane walks one shadow ray at a time and adds
 // the light to the path's radiance when the ray arrives.
-template <bool kCount, bool kBatch, bool kTextured>
+template <bool kCount, bool kBatch, bool kFullShading>
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_shadow(SceneView S, PathState P, Queues Q,
     uint32_t bounce, uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 2];
@@ -714,7 +715,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_shadow(SceneVi
       ++rays;
     }
     if (!__any_sync(kFullWarp, active)) break;
-    if (walk_round<true, kCount, kTextured>(kBatch ? B.views[scene] : S, W, stack, rng, active, &vc)) {
+    if (walk_round<true, kCount, kFullShading>(kBatch ? B.views[scene] : S, W, stack, rng, active, &vc)) {
       active = false;
       const float tr = W.transmittance;
       if (tr > 0.0f) {
@@ -839,7 +840,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_visibility(SceneV
 // queued for shading; a miss ends the path with the environment. Each warp
 // stages its hits in shared memory and appends them to the hit queue 32 at
 // a time.
-template <bool kCount, bool kBatch, bool kAnalytic, bool kTextured>
+template <bool kCount, bool kBatch, bool kAnalytic, bool kFullShading>
 __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, const uint32_t* __restrict__ rays_in, uint32_t bounce,
     uint32_t* __restrict__ fetch, uint32_t refill_below, VisitCounters* visits, SceneTable B) {
@@ -870,7 +871,7 @@ __global__ void __launch_bounds__(kBlock, kTraceBlocksPerSm) k_wf_extend(SceneVi
     if (!__any_sync(kFullWarp, active)) break;
     bool emit = false;
     const SceneView& SS = kBatch ? B.views[scene] : S;
-    if (walk_round<false, kCount, kTextured>(SS, W, stack, rng, active, &vc)) {
+    if (walk_round<false, kCount, kFullShading>(SS, W, stack, rng, active, &vc)) {
       active = false;
       if (W.found) {
         P.hit[slot] = make_uint4(W.best_instance, W.best_tri, __float_as_uint(W.b1), __float_as_uint(W.b2));
@@ -961,7 +962,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_resolve(SceneView S,
 // give it; the per-bounce queue counts are kept as the rounds keep them.
 // Threads take paths from `cursor` one at a time. Long paths then cost one
 // launch instead of three per bounce.
-template <bool kBatch, bool kAnalytic, bool kTextured>
+template <bool kBatch, bool kAnalytic, bool kFullShading>
 __global__ void __launch_bounds__(kBlock) k_wf_tail(SceneView S, const FrameConst* __restrict__ fcp, PathState P,
     Queues Q, uint32_t first, uint32_t* __restrict__ cursor, SceneTable B) {
   const uint32_t n = Q.counts[3 * first];
@@ -985,18 +986,18 @@ __global__ void __launch_bounds__(kBlock) k_wf_tail(SceneView S, const FrameCons
     // A path's bounces are bounded by max_bounces (scatter ends it there).
     for (uint32_t bounce = first; bounce <= f.max_bounces; ++bounce) {
       Hit hit;
-      if (!trace_closest<false, kTextured>(SS, ro, rd, tmin, tmax, rng, hit)) {
+      if (!trace_closest<false, kFullShading>(SS, ro, rd, tmin, tmax, rng, hit)) {
         R = miss_path<kAnalytic>(SS, f, ro, rd, flags, last_pdf, T, R);
         break;
       }
       atomicAdd(&Q.counts[3 * bounce + 1], 1u);
       F3 no, nd;
       ShadowRequest req;
-      const bool cont = scatter<kAnalytic, kTextured>(SS, f, hit.instance, hit.tri, hit.b1, hit.b2, ro, rd, bounce, T, R,
+      const bool cont = scatter<kAnalytic, kFullShading>(SS, f, hit.instance, hit.tri, hit.b1, hit.b2, ro, rd, bounce, T, R,
           last_pdf, flags, rng, no, nd, req, slot);
       if (req.pending) {
         atomicAdd(&Q.counts[3 * bounce + 2], 1u);
-        const float tr = trace_shadow<false, kTextured>(SS, req.origin, req.direction, 0.0f, req.tmax);
+        const float tr = trace_shadow<false, kFullShading>(SS, req.origin, req.direction, 0.0f, req.tmax);
         if (tr > 0.0f) R = R + req.throughput * shadow_contribution(req.fl, req.weight, req.pdf, tr);
       }
       if (!cont) break;
@@ -1176,10 +1177,10 @@ struct Timed {
 // instantiation without the analytic lights' or texture lookups' code when
 // the scene has none.
 template <class F>
-void with_features(bool analytic, bool textured, F&& f) {
-  if (analytic && textured) f(std::true_type{}, std::true_type{});
+void with_features(bool analytic, bool full_shading, F&& f) {
+  if (analytic && full_shading) f(std::true_type{}, std::true_type{});
   else if (analytic) f(std::true_type{}, std::false_type{});
-  else if (textured) f(std::false_type{}, std::true_type{});
+  else if (full_shading) f(std::false_type{}, std::true_type{});
   else f(std::false_type{}, std::false_type{});
 }
 
@@ -1195,7 +1196,7 @@ void launch_reference_pt(const SceneView& S, const FrameConst* fc, const uint32_
     k_reference_pt<true, true, true><<<grid, kBlock, 0, stream>>>(S, fc, accum, color, totals, profile->visits);
     return;
   }
-  with_features(S.analytic_count != 0, S.textured != 0, [&](auto a, auto x) {
+  with_features(S.analytic_count != 0, S.full_shading != 0, [&](auto a, auto x) {
     k_reference_pt<false, decltype(a)::value, decltype(x)::value><<<grid, kBlock, 0, stream>>>(S, fc, accum, color,
         totals, nullptr);
   });
@@ -1276,7 +1277,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   const SceneTable none;
   // The scene's features select the instantiations (counting visits takes
   // the one with every feature's code).
-  const bool analytic = S.analytic_count != 0, textured = S.textured != 0;
+  const bool analytic = S.analytic_count != 0, full_shading = S.full_shading != 0;
   const uint32_t grid_extend = persistent_grid(
       count ? (const void*)k_wf_extend<true, false, true, true> : (const void*)k_wf_extend<false, false, false, false>,
       Q.capacity, tuning);
@@ -1292,7 +1293,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
     Timed t(profile, stream, 0);
     const uint32_t grid_camera = (threads * std::max(wave, 1u) + kBlock - 1) / kBlock;
     if (count) k_wf_camera<true, false, true><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, visits, none);
-    else if (textured) k_wf_camera<false, false, true><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
+    else if (full_shading) k_wf_camera<false, false, true><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
     else k_wf_camera<false, false, false><<<grid_camera, kBlock, 0, stream>>>(S, fc, P, Q, nullptr, none);
   }
   // Bounces 0 .. rounds - 1 as wavefront rounds; the paths queued for bounce
@@ -1318,7 +1319,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
         k_wf_extend<true, false, true, true><<<grid_extend, kBlock, 0, stream>>>(S, fc, P, Q, rays, b, fetch + 2 * b,
             refill, visits, none);
       else
-        with_features(analytic, textured, [&](auto a, auto x) {
+        with_features(analytic, full_shading, [&](auto a, auto x) {
           k_wf_extend<false, false, decltype(a)::value, decltype(x)::value><<<grid_extend, kBlock, 0, stream>>>(S, fc,
               P, Q, rays, b, fetch + 2 * b, refill, nullptr, none);
         });
@@ -1332,7 +1333,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
       if (cache_vertex && C.query_keys != nullptr)
         cudaMemsetAsync(C.query_bins, 0, sizeof(uint32_t) * kSortBins, stream);
       Timed t(profile, stream, 2);
-      with_features(analytic, textured, [&](auto a, auto x) {
+      with_features(analytic, full_shading, [&](auto a, auto x) {
         if (cache_vertex)
           k_wf_shade<true, false, decltype(a)::value, decltype(x)::value><<<grid_shade, kBlock, 0, stream>>>(S, fc, P,
               QS, b, C, none);
@@ -1347,7 +1348,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
         k_wf_shadow<true, false, true><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill, visits,
             none);
       else
-        if (textured)
+        if (full_shading)
           k_wf_shadow<false, false, true><<<grid_shadow, kBlock, 0, stream>>>(S, P, Q, b, fetch + 2 * b + 1, refill,
               nullptr, none);
         else
@@ -1361,7 +1362,7 @@ void launch_wavefront_sample(const SceneView& S, const FrameConst* fc, const uin
   if (rounds <= max_bounces) {
     Timed t(profile, stream, 6);
     uint32_t* cursor = fetch + 2 * (max_bounces + 1);
-    with_features(analytic, textured, [&](auto a, auto x) {
+    with_features(analytic, full_shading, [&](auto a, auto x) {
       const auto kernel = k_wf_tail<false, decltype(a)::value, decltype(x)::value>;
       const uint32_t grid_tail = persistent_grid((const void*)kernel, Q.capacity, tuning);
       kernel<<<grid_tail, kBlock, 0, stream>>>(S, fc, P, Q, rounds, cursor, none);
@@ -1458,7 +1459,7 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   const uint32_t grid_shadow = persistent_grid((const void*)k_wf_shadow<false, true, true>, Q.capacity, tuning);
   const uint32_t grid_shade = std::min((Q.capacity + kBlock - 1) / kBlock,
       8u * persistent_grid((const void*)k_wf_shade<false, true, false, false>, Q.capacity, TraceTuning()));
-  if (B.textured) k_wf_camera<false, true, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
+  if (B.full_shading) k_wf_camera<false, true, true><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
   else k_wf_camera<false, true, false><<<grid_slots, kBlock, 0, stream>>>(none_view, no_frame, P, Q, nullptr, B);
   const uint32_t rounds = wavefront_rounds(max_bounces, false, tuning.rounds);
   const bool keyed = Q.keys != nullptr && Q.sorted != nullptr && Q.bins != nullptr;
@@ -1472,18 +1473,18 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
       rays = Q.sorted;
     }
     if (b != 0)
-      with_features(B.analytic, B.textured, [&](auto a, auto x) {
+      with_features(B.analytic, B.full_shading, [&](auto a, auto x) {
         k_wf_extend<false, true, decltype(a)::value, decltype(x)::value><<<grid_extend, kBlock, 0, stream>>>(none_view,
             no_frame, P, Q, rays, b, fetch + 2 * b, refill, nullptr, B);
       });
     Queues QS = Q;
     if (keyed && b + 1 < rounds) cudaMemsetAsync(Q.bins, 0, sizeof(uint32_t) * kSortBins, stream);
     else QS.keys = nullptr;
-    with_features(B.analytic, B.textured, [&](auto a, auto x) {
+    with_features(B.analytic, B.full_shading, [&](auto a, auto x) {
       k_wf_shade<false, true, decltype(a)::value, decltype(x)::value><<<grid_shade, kBlock, 0, stream>>>(none_view,
           B.frames, P, QS, b, no_cache, B);
     });
-    if (B.textured)
+    if (B.full_shading)
       k_wf_shadow<false, true, true><<<grid_shadow, kBlock, 0, stream>>>(none_view, P, Q, b, fetch + 2 * b + 1,
           refill, nullptr, B);
     else
@@ -1492,7 +1493,7 @@ void launch_wavefront_batch(const SceneTable& B, uint32_t max_bounces, const Pat
   }
   if (rounds <= max_bounces) {
     uint32_t* cursor = fetch + 2 * (max_bounces + 1);
-    with_features(B.analytic, B.textured, [&](auto a, auto x) {
+    with_features(B.analytic, B.full_shading, [&](auto a, auto x) {
       const auto kernel = k_wf_tail<true, decltype(a)::value, decltype(x)::value>;
       const uint32_t grid_tail = persistent_grid((const void*)kernel, Q.capacity, tuning);
       kernel<<<grid_tail, kBlock, 0, stream>>>(none_view, no_frame, P, Q, rounds, cursor, B);

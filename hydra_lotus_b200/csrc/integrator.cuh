@@ -107,7 +107,7 @@ struct SceneTable {
   uint32_t count = 0;
   uint32_t total_slots = 0;
   bool analytic = false;  // some scene has analytic lights
-  bool textured = false;  // some scene has texture lookups
+  bool full_shading = false;  // some scene has texture lookups or glTF PBR materials
   // The camera pass's order within each scene: 0, each image's rows; k,
   // warp tiles 2^k pixels wide and 32 / 2^k high (every scene's size a
   // multiple of the tile).

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/lotus_cuda.h"
+#include "albedo.cuh"
 #include "bvh_build.cuh"
 #include "integrator.cuh"
 #include "radiance_cache.cuh"
@@ -521,7 +522,11 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
     // EmissionEstimate (gpu_scene.cpp:144-180): the mean of the constant's
     // RGB, or of a lookup's bound for texels in [0, 1] (its fallback when
     // it names no image).
-    double e = ((double)mat.emission[0] + (double)mat.emission[1] + (double)mat.emission[2]) / 3.0;
+    // glTF PBR's emissive (the same slot as UsdPreviewSurface's emission)
+    // is scaled by its strength.
+    const bool gltf = mat.model == LOTUS_MODEL_GLTF_PBR;
+    const double factor = gltf ? (double)mat.emissive_strength : 1.0;
+    double e = factor * ((double)mat.emission[0] + (double)mat.emission[1] + (double)mat.emission[2]) / 3.0;
     const uint32_t emission_lookup = mat.lookups[LOTUS_SLOT_EMISSION];
     if (emission_lookup != LOTUS_NO_LOOKUP) {
       const lotus_texture_input& in = s.texture_inputs[emission_lookup - 1];
@@ -529,7 +534,7 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
       for (int k = 0; k < 3; ++k)
         c[k] = in.texture == LOTUS_NO_TEXTURE ? std::max(0.0f, in.fallback[k])
                                               : (double)std::max(0.0f, in.scale[k]) + std::max(0.0f, in.bias[k]);
-      e = (c[0] + c[1] + c[2]) / 3.0;
+      e = factor * (c[0] + c[1] + c[2]) / 3.0;
     }
     if (!(std::isfinite(e) && e > 0.0)) e = 0.0;
     if (e <= 0.0 || g.triangle_count == 0) continue;
@@ -545,8 +550,14 @@ LightTable build_light_table(const lotus_scene_desc& s, double env_mean) {
             g.positions + 3 * (size_t)g.triangles[3 * (size_t)t + k]);
         table.verts.push_back(make_float4(w.x, w.y, w.z, 0.0f));
       }
-      table.radiance.push_back(make_float4(mat.emission[0] * coverage, mat.emission[1] * coverage,
-          mat.emission[2] * coverage, looked_up ? 1.0f : 0.0f));
+      // Emission(material, st) * Coverage(hit) (scene.slang:655-657): glTF
+      // PBR's emissive times its strength.
+      const float strength = gltf ? mat.emissive_strength : 1.0f;
+      const float e3[3] = {gltf ? mat.emission[0] * strength : mat.emission[0],
+                           gltf ? mat.emission[1] * strength : mat.emission[1],
+                           gltf ? mat.emission[2] * strength : mat.emission[2]};
+      table.radiance.push_back(make_float4(e3[0] * coverage, e3[1] * coverage, e3[2] * coverage,
+          looked_up ? 1.0f : 0.0f));
     }
   }
   bool distant = env_mean > 0.0;
@@ -661,6 +672,13 @@ static_assert(LOTUS_OUTPUT_BARYCENTRICS == kOutputBarycentrics && LOTUS_OUTPUT_S
                   LOTUS_OUTPUT_ALBEDO == kOutputAlbedo && LOTUS_OUTPUT_ROUGHNESS_METALLIC == kOutputRoughnessMetallic,
     "diagnostic outputs are numbered as lotus_settings::output");
 
+// The directional albedo tables (albedo_tables_gen.cpp's output, in
+// albedo.cuh's layout).
+const float kAlbedoTableData[] = {
+#include "albedo_tables.inc"
+};
+static_assert(sizeof(kAlbedoTableData) == albedo::kSize * sizeof(float), "albedo tables");
+
 struct Renderer {
   int device = 0;
   uint32_t bvh_leaf_size = 1;
@@ -690,6 +708,7 @@ struct Renderer {
   DeviceArray<uint4> tex_info;
   DeviceArray<TextureLookup> tex_lookups;
   DeviceArray<MaterialLookups> mat_lookups;
+  DeviceArray<float> albedo_tables;  // the composed closure's (albedo.cuh), uploaded once
   DeviceArray<float2> texcoords;
   DeviceArray<uint32_t> inst_texcoords;
   std::vector<LightRecord> host_lights;
@@ -951,6 +970,28 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
       detail = "material " + std::to_string(i) + " has an ior below 1";
       return false;
     }
+    if (m.model != LOTUS_MODEL_PREVIEW_SURFACE && m.model != LOTUS_MODEL_GLTF_PBR) {
+      detail = "material " + std::to_string(i) + " has an unknown model";
+      return false;
+    }
+    if (m.model == LOTUS_MODEL_GLTF_PBR) {
+      // ValidGltfPbr (gpu_scene.cpp:853-881).
+      const auto unit = [](float v) { return v >= 0.0f && v <= 1.0f; };
+      const auto radiance = [](const float* c) {
+        return std::isfinite(c[0]) && std::isfinite(c[1]) && std::isfinite(c[2]) && c[0] >= 0.0f &&
+            c[1] >= 0.0f && c[2] >= 0.0f;
+      };
+      const bool valid = unit(m.base_color[0]) && unit(m.base_color[1]) && unit(m.base_color[2]) &&
+          unit(m.roughness) && unit(m.metallic) && radiance(m.emission) &&
+          std::isfinite(m.emissive_strength) && m.emissive_strength >= 0.0f && unit(m.specular) &&
+          radiance(m.specular_color) && unit(m.transmission) && unit(m.clearcoat) &&
+          unit(m.clearcoat_roughness) && unit(m.sheen_color[0]) && unit(m.sheen_color[1]) &&
+          unit(m.sheen_color[2]) && unit(m.sheen_roughness);
+      if (!valid) {
+        detail = "material " + std::to_string(i) + " has a glTF PBR input out of its range";
+        return false;
+      }
+    }
     for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k)
       if (m.lookups[k] != LOTUS_NO_LOOKUP && m.lookups[k] > s.texture_input_count) {
         detail = "material " + std::to_string(i) + " names a missing texture input";
@@ -1137,16 +1178,18 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
   v.inst_trav = R.inst_trav.ptr;
   v.inst_shade = R.inst_shade.ptr;
   v.materials = R.materials.ptr;
-  v.textured = 0;
+  v.full_shading = 0;
   for (const lotus_material& m : h.materials) {
-    bool any = !(m.normal[0] == 0.0f && m.normal[1] == 0.0f && (m.normal[2] == 0.0f || m.normal[2] == 1.0f));
+    bool any = !(m.normal[0] == 0.0f && m.normal[1] == 0.0f && (m.normal[2] == 0.0f || m.normal[2] == 1.0f)) ||
+        m.model == LOTUS_MODEL_GLTF_PBR;
     for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k) any = any || m.lookups[k] != LOTUS_NO_LOOKUP;
-    if (any) v.textured = 1;
+    if (any) v.full_shading = 1;
   }
   v.tex_texels = R.tex_texels.ptr;
   v.tex_info = R.tex_info.ptr;
   v.lookups = R.tex_lookups.ptr;
   v.mat_lookups = R.mat_lookups.ptr;
+  v.albedo_tables = R.albedo_tables.ptr;
   v.texcoords = R.texcoords.ptr;
   v.inst_texcoords = R.inst_texcoords.ptr;
   v.normals = R.normals.ptr;
@@ -1310,6 +1353,7 @@ bool upload_textures(Renderer& R, const lotus_scene_desc& s, std::string& detail
     ml.fallback_t = m.texcoord_fallback[1];
     const bool zero = m.normal[0] == 0.0f && m.normal[1] == 0.0f && m.normal[2] == 0.0f;
     for (int k = 0; k < 3; ++k) ml.normal[k] = zero ? (k == 2 ? 1.0f : 0.0f) : m.normal[k];
+    ml.reserved = 0;
   }
   std::vector<float2> coords;
   h.texcoord_base.assign(s.geometry_count, 0);
@@ -1473,7 +1517,17 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
     r.specular_ior = make_float4(m.specular_color[0], m.specular_color[1], m.specular_color[2], m.ior);
     r.transmission = make_float4(m.transmission_color[0], m.transmission_color[1],
         m.transmission_color[2], m.transmission);
-    uint32_t flags = m.flags & (LOTUS_MATERIAL_SPECULAR_WORKFLOW | LOTUS_MATERIAL_THIN_WALLED);
+    const bool gltf = m.model == LOTUS_MODEL_GLTF_PBR;
+    uint32_t flags = gltf ? kMaterialGltf : m.flags & (LOTUS_MATERIAL_SPECULAR_WORKFLOW | LOTUS_MATERIAL_THIN_WALLED);
+    // glTF PBR: the dielectric's reflectance at normal incidence from its
+    // index, in double so that the default index gives the float nearest
+    // 0.04 (gpu_scene.cpp:2059-2063).
+    const double root = (1.0 - (double)m.ior) / (1.0 + (double)m.ior);
+    const float dielectric_f0 = gltf ? (float)(root * root) : 0.0f;
+    r.gltf = gltf ? make_float4(m.specular, m.clearcoat, m.clearcoat_roughness, m.emissive_strength)
+                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    r.sheen = gltf ? make_float4(m.sheen_color[0], m.sheen_color[1], m.sheen_color[2], m.sheen_roughness)
+                   : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k)
       if (m.lookups[k] != LOTUS_NO_LOOKUP) flags |= kMaterialTextured;
     // A constant tangent-space normal other than the identity (all zero
@@ -1483,9 +1537,13 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
     if (m.lookups[LOTUS_SLOT_OPACITY] != LOTUS_NO_LOOKUP) flags |= kMaterialOpacityTextured;
     float fbits;
     std::memcpy(&fbits, &flags, 4);
-    r.coverage = make_float4(m.opacity, m.opacity_threshold, fbits, 0.0f);
+    r.coverage = make_float4(m.opacity, m.opacity_threshold, fbits, dielectric_f0);
   }
   if (!R.ok(R.materials.upload(h_mat.data(), h_mat.size(), st), "materials", detail)) return fail(detail);
+  // The composed closure's albedo tables, once per renderer.
+  if (R.albedo_tables.count != albedo::kSize &&
+      !R.ok(R.albedo_tables.upload(kAlbedoTableData, albedo::kSize, st), "albedo tables", detail))
+    return fail(detail);
   // Environment: the texels go to the device, where its sampling
   // distribution is built (build_env_distribution).
   h.env_bound = false;
@@ -2495,7 +2553,18 @@ int64_t lotus_cuda_read_scene(lotus_cuda_renderer* r, uint32_t what, uint32_t in
         o[i].transmission_color[2] = m.transmission.z; o[i].transmission = m.transmission.w;
         o[i].opacity = m.coverage.x;
         o[i].opacity_threshold = m.coverage.y;
-        std::memcpy(&o[i].flags, &m.coverage.z, 4);
+        uint32_t flags;
+        std::memcpy(&flags, &m.coverage.z, 4);
+        o[i].flags = flags & (LOTUS_MATERIAL_SPECULAR_WORKFLOW | LOTUS_MATERIAL_THIN_WALLED);
+        if (flags & kMaterialGltf) {
+          o[i].model = LOTUS_MODEL_GLTF_PBR;
+          o[i].specular = m.gltf.x;
+          o[i].clearcoat = m.gltf.y;
+          o[i].clearcoat_roughness = m.gltf.z;
+          o[i].emissive_strength = m.gltf.w;
+          o[i].sheen_color[0] = m.sheen.x; o[i].sheen_color[1] = m.sheen.y; o[i].sheen_color[2] = m.sheen.z;
+          o[i].sheen_roughness = m.sheen.w;
+        }
       }
       return (int64_t)bytes;
     }

@@ -94,21 +94,26 @@ static_assert(sizeof(InstanceShading) == 64, "shading record is 64 bytes");
 
 constexpr uint32_t kInstanceOpaque = 1u;
 
-// lotus_material as five float4.
+// lotus_material as seven float4. The fields marked glTF hold MaterialX's
+// glTF PBR inputs on a material of that model (kMaterialGltf).
 struct alignas(16) MaterialRecord {
   float4 base_roughness;       // base colour, roughness
-  float4 emission_metallic;    // emission, metallic
+  float4 emission_metallic;    // emission (glTF: emissive), metallic
   float4 specular_ior;         // specular colour, ior
-  float4 transmission;         // transmission colour, transmission
-  float4 coverage;             // opacity, threshold, flags (bits), reserved
+  float4 transmission;         // transmission colour (glTF: unused), transmission
+  float4 coverage;             // opacity, threshold, flags (bits), glTF: the dielectric's f0
+  float4 gltf;                 // glTF: specular, clearcoat, clearcoat roughness, emissive strength
+  float4 sheen;                // glTF: sheen colour, sheen roughness
 };
-static_assert(sizeof(MaterialRecord) == 80, "material record is 80 bytes");
+static_assert(sizeof(MaterialRecord) == 112, "material record is 112 bytes");
 
 // MaterialRecord::coverage.z flag bits the renderer adds to the material's
 // own LOTUS_MATERIAL_* bits: some input has a texture lookup; the opacity
 // has one.
 constexpr uint32_t kMaterialTextured = 1u << 8;
 constexpr uint32_t kMaterialOpacityTextured = 1u << 9;
+// The material is MaterialX's glTF PBR surface (LOTUS_MODEL_GLTF_PBR).
+constexpr uint32_t kMaterialGltf = 1u << 10;
 // kMaterialTextured is set too for a constant tangent-space normal other
 // than (0, 0, 1), which MaterialLookups::normal holds.
 
@@ -137,8 +142,9 @@ struct alignas(16) MaterialLookups {
   float fallback_s;
   float fallback_t;
   float normal[3];  // the constant tangent-space normal
+  uint32_t reserved;
 };
-static_assert(sizeof(MaterialLookups) == 48, "MaterialLookups is 48 bytes");
+static_assert(sizeof(MaterialLookups) == 80, "MaterialLookups is 80 bytes");
 
 // A light-table entry (GpuLightRecord, gpu_scene.hpp:120-126).
 struct alignas(16) LightRecord {
@@ -201,7 +207,8 @@ struct SceneView {
   uint32_t light_node_count;
   uint32_t distant_count;
   uint32_t step_limit;       // a walk's step budget (kMaxTraversalSteps)
-  uint32_t textured;         // some material has a texture lookup or a mapped normal
+  uint32_t full_shading;     // some material has a texture lookup, a mapped normal or the glTF PBR model
+  const float* __restrict__ albedo_tables;  // the composed closure's (albedo.cuh), 76800 floats
   // Texture lookups: every texture's texels decoded to linear RGBA, one
   // after another; per texture its first texel, width and height; the
   // scene's texture inputs; per material its lookups (read only for
@@ -333,14 +340,14 @@ __device__ __forceinline__ float material_coverage(const SceneView& S, const Mat
   return opacity;
 }
 
-// kTextured false: the scene has no textured coverage (SceneView::textured
+// kFullShading false: the scene has no textured coverage (SceneView::full_shading
 // clear), and the walk compiles without the lookup.
-template <bool kTextured = true>
+template <bool kFullShading = true>
 __device__ __forceinline__ float instance_coverage(const SceneView& S, uint32_t instance, uint32_t primitive,
     float b1, float b2) {
   const uint32_t material = S.inst_trav[instance].material;
   const MaterialRecord& m = S.materials[material];
-  if (!kTextured) {
+  if (!kFullShading) {
     if (m.coverage.y > 0.0f) return m.coverage.x >= m.coverage.y ? 1.0f : 0.0f;
     return m.coverage.x;
   }
@@ -610,7 +617,7 @@ __device__ __forceinline__ void walk_visit_node(const SceneView& S, Walk& W, Wal
 
 // The triangle tests of BLAS leaf `leaf` (a negative reference). Returns
 // true when an any-hit walk has met an opaque surface.
-template <bool kAnyHit, bool kCount, bool kTextured = true>
+template <bool kAnyHit, bool kCount, bool kFullShading = true>
 __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int32_t leaf, uint32_t& rng,
     TraversalCounters* counters) {
   const uint32_t code = ~(uint32_t)leaf;
@@ -626,7 +633,7 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
     if (!(t >= W.tmin) || !(t <= W.best)) continue;
     const uint32_t prim = __float_as_uint(a.w);
     if (kAnyHit) {
-      const float coverage = W.opaque ? 1.0f : instance_coverage<kTextured>(S, W.instance, prim, b1, b2);
+      const float coverage = W.opaque ? 1.0f : instance_coverage<kFullShading>(S, W.instance, prim, b1, b2);
       if (coverage >= 1.0f) {
         W.found = true;
         W.transmittance = 0.0f;
@@ -639,7 +646,7 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
            (W.instance == W.best_instance && prim >= __float_as_uint(S.tris[kTriStride * (size_t)W.best_tri].w))))
         continue;
       if (!W.opaque) {
-        const float coverage = instance_coverage<kTextured>(S, W.instance, prim, b1, b2);
+        const float coverage = instance_coverage<kFullShading>(S, W.instance, prim, b1, b2);
         if (coverage <= 0.0f) continue;
         if (coverage < 1.0f && !(next_random(rng) < coverage)) continue;
       }
@@ -657,7 +664,7 @@ __device__ __forceinline__ bool walk_test_leaf(const SceneView& S, Walk& W, int3
 // W.cur is not an interior node: the exit marker, a BLAS leaf (tested
 // here), or a TLAS leaf (entered). Leaves W.cur at the next reference.
 // Returns true when an any-hit walk has met an opaque surface.
-template <bool kAnyHit, bool kCount, bool kTextured = true>
+template <bool kAnyHit, bool kCount, bool kFullShading = true>
 __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStack& stack, uint32_t& rng,
     TraversalCounters* counters) {
   const int32_t cur = W.cur;
@@ -666,7 +673,7 @@ __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStac
     W.w.org = W.origin;
     W.inv = slab_inverse(W.direction);
   } else if (W.in_blas) {
-    if (walk_test_leaf<kAnyHit, kCount, kTextured>(S, W, cur, rng, counters)) return true;
+    if (walk_test_leaf<kAnyHit, kCount, kFullShading>(S, W, cur, rng, counters)) return true;
   } else {
     const uint32_t instance = ~(uint32_t)cur;
     if (kCount) ++counters->instances;
@@ -691,7 +698,7 @@ __device__ __forceinline__ bool walk_other(const SceneView& S, Walk& W, WalkStac
 }
 
 // The whole walk in one call (for kernels with one ray per thread).
-template <bool kAnyHit, bool kCount, bool kTextured = true>
+template <bool kAnyHit, bool kCount, bool kFullShading = true>
 __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 direction, float tmin,
     float tmax, uint32_t& rng, Hit& hit, bool& found, TraversalCounters* counters = nullptr) {
   Walk W;
@@ -700,7 +707,7 @@ __device__ __forceinline__ float traverse(const SceneView& S, F3 origin, F3 dire
   while (W.cur != kWalkDone) {
     if (walk_at_node(W)) {
       walk_visit_node<kCount>(S, W, stack, counters);
-    } else if (walk_other<kAnyHit, kCount, kTextured>(S, W, stack, rng, counters)) {
+    } else if (walk_other<kAnyHit, kCount, kFullShading>(S, W, stack, rng, counters)) {
       break;
     }
   }
@@ -724,7 +731,7 @@ constexpr int kRoundNodeLanes = 8;
 // finally each lane not at an interior node takes its exit marker, further
 // leaf or instance entry. Each kind of work thus runs once per round over
 // all the lanes that have it. Returns true for a lane whose walk has ended.
-template <bool kAnyHit, bool kCount, bool kTextured = true>
+template <bool kAnyHit, bool kCount, bool kFullShading = true>
 __device__ __forceinline__ bool walk_round(const SceneView& S, Walk& W, WalkStack& stack, uint32_t& rng,
     bool active, TraversalCounters* counters) {
   constexpr unsigned kAll = 0xFFFFFFFFu;
@@ -744,31 +751,31 @@ __device__ __forceinline__ bool walk_round(const SceneView& S, Walk& W, WalkStac
   bool ended = false;
   const bool leaf = active && W.leaf != 0;
   if (__any_sync(kAll, leaf) && leaf) {
-    ended = walk_test_leaf<kAnyHit, kCount, kTextured>(S, W, W.leaf, rng, counters);
+    ended = walk_test_leaf<kAnyHit, kCount, kFullShading>(S, W, W.leaf, rng, counters);
     W.leaf = 0;
   }
   if (active && !ended && W.cur != kWalkDone && !walk_at_node(W))
-    ended = walk_other<kAnyHit, kCount, kTextured>(S, W, stack, rng, counters);
+    ended = walk_other<kAnyHit, kCount, kFullShading>(S, W, stack, rng, counters);
   const bool done = active && (ended || (W.cur == kWalkDone && W.leaf == 0));
   if (done) walk_check_end(S, W);
   return done;
 }
 
-template <bool kCount = false, bool kTextured = true>
+template <bool kCount = false, bool kFullShading = true>
 __device__ __forceinline__ bool trace_closest(const SceneView& S, F3 o, F3 d, float tmin,
     float tmax, uint32_t& rng, Hit& hit, TraversalCounters* counters = nullptr) {
   bool found;
-  traverse<false, kCount, kTextured>(S, o, d, tmin, tmax, rng, hit, found, counters);
+  traverse<false, kCount, kFullShading>(S, o, d, tmin, tmax, rng, hit, found, counters);
   return found;
 }
 
-template <bool kCount = false, bool kTextured = true>
+template <bool kCount = false, bool kFullShading = true>
 __device__ __forceinline__ float trace_shadow(const SceneView& S, F3 o, F3 d, float tmin,
     float tmax, TraversalCounters* counters = nullptr) {
   uint32_t rng = 0;
   Hit hit;
   bool found;
-  return traverse<true, kCount, kTextured>(S, o, d, tmin, tmax, rng, hit, found, counters);
+  return traverse<true, kCount, kFullShading>(S, o, d, tmin, tmax, rng, hit, found, counters);
 }
 
 }  // namespace lotus

@@ -40,7 +40,7 @@ constexpr int kRestirBlocksPerSm = 6;
 // ---------------------------------------------------------------------------
 // WriteTemporalSurface (temporal.slang:557-627): the pixel centre's primary
 // hit, with a fixed coverage sequence (sample 0).
-template <bool kTextured>
+template <bool kFullShading>
 __global__ void __launch_bounds__(kBlock) k_temporal_surface(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     const TemporalInstance* __restrict__ identities, TemporalPixel* __restrict__ out) {
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal_surface(SceneView S,
     float tmax;
     camera_ray(f, cx * f.ndc[0] + f.ndc[2], cy * f.ndc[1] + f.ndc[3], ro, rd, tmax);
     Hit hit;
-    if (trace_closest<false, kTextured>(S, ro, rd, 0.0f, tmax, rng, hit)) {
+    if (trace_closest<false, kFullShading>(S, ro, rd, 0.0f, tmax, rng, hit)) {
       const InstanceShading rec = S.inst_shade[hit.instance];
       const TemporalInstance id = identities[hit.instance];
       const float4* tv = S.tris + kTriStride * (size_t)hit.tri;
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(kBlock) k_temporal_surface(SceneView S,
         o.instance_id = id.instance_id;
         o.material_id = id.material_id;
         o.flags = 1u | id.flags;
-        const SurfaceHit sh = reconstruct_hit<kTextured>(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
+        const SurfaceHit sh = reconstruct_hit<kFullShading>(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
         // The surface summary's albedo (scene.slang:1254-1257).
         const F3 albedo = sh.bsdf.transmission > 0.0f
             ? sh.base_color + sh.bsdf.transmission * (sh.bsdf.transmission_color - sh.base_color)
@@ -156,21 +156,52 @@ __global__ void __launch_bounds__(kBlock) k_reproject(const TemporalConst* __res
 // ---------------------------------------------------------------------------
 // ReSTIR DI.
 
-__device__ __forceinline__ F3 reflection_evaluate_side(const Closure& c, F3 wo, F3 wi) {
-  return wi.z > 0.0f ? bsdf_evaluate(c, wo, wi) : V(0.0f);
+// A stored surface's closure, by its model.
+struct StoredClosure {
+  bool gltf;
+  Closure preview;
+  GltfClosure composed;
+};
+
+// ReflectionEvaluate (restir.slang:66-72): ReSTIR's targets are the
+// reflection side's.
+template <bool kFullShading>
+__device__ __forceinline__ F3 reflection_evaluate_side(const StoredClosure& c, F3 wo, F3 wi) {
+  if (!(wi.z > 0.0f)) return V(0.0f);
+  if (kFullShading && c.gltf) return gltf_evaluate(c.composed, wo, wi);
+  return bsdf_evaluate(c.preview, wo, wi);
 }
 
 // CandidateContribution (restir.slang:155-161).
+template <bool kFullShading>
 __device__ __forceinline__ F3 candidate_contribution(const SurfaceHit& sh, const Frame& basis, F3 wo,
     const LightSample& ls, float selection) {
   if (!(ls.pdf > 0.0f) || dot(ls.direction, sh.normal) <= 0.0f) return V(0.0f);
-  return reflection_evaluate_side(sh.bsdf, wo, basis.to_local(ls.direction)) * ls.radiance *
-      (selection / ls.pdf);
+  const F3 wi = basis.to_local(ls.direction);
+  const F3 f = wi.z > 0.0f ? surface_evaluate<kFullShading>(sh, wo, wi) : V(0.0f);
+  return f * ls.radiance * (selection / ls.pdf);
 }
 
-__device__ __forceinline__ void store_closure(const Closure& b, RestirSurface& s) {
+// StoreClosure (restir.slang:78-103): the preview closure's fields, or
+// glTF PBR's 22 terms (PackGltfPbrTerms, gltf_pbr.slang:162-188) in the
+// same lanes and `extension`. `outgoing.xyz` is already set.
+template <bool kFullShading>
+__device__ __forceinline__ void store_closure(const SurfaceHit& sh, RestirSurface& s) {
   s.model = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   s.extension = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (kFullShading && sh.gltf) {
+    const GltfTerms& g = sh.gltf_terms;
+    s.model = make_float4(1.0f, g.e1, g.share, g.f90);
+    s.base_alpha = F4(g.base_color, g.alpha);
+    s.dielectric_metallic = F4(g.f0, g.metallic);
+    s.normal.w = g.transmission;
+    s.shading_normal.w = g.coat_scale;
+    s.outgoing.w = g.coat_dim;
+    s.fresnel = make_float4(g.coat_alpha, g.coat_normal.x, g.coat_normal.y, g.sheen_roughness);
+    s.extension = F4(g.sheen_color, g.sheen_dim);
+    return;
+  }
+  const Closure& b = sh.bsdf;
   s.normal.w = b.dielectric_f90;
   s.shading_normal.w = b.thin_walled ? -b.transmission : b.transmission;
   s.outgoing.w = b.smooth ? -b.eta : b.eta;
@@ -179,8 +210,35 @@ __device__ __forceinline__ void store_closure(const Closure& b, RestirSurface& s
   s.fresnel = F4(b.f0, b.f90);
 }
 
-__device__ __forceinline__ Closure load_closure(const RestirSurface& s) {
-  Closure b;
+// LoadClosure (restir.slang:106-150): the glTF closure is rebuilt from its
+// terms for the stored outgoing direction (UnpackGltfPbrTerms,
+// gltf_pbr.slang:190-214: the coat's normal from its tangent components).
+template <bool kFullShading>
+__device__ __forceinline__ StoredClosure load_closure(const RestirSurface& s) {
+  StoredClosure c;
+  c.gltf = kFullShading && (uint32_t)s.model.x == 1u;
+  if (kFullShading && c.gltf) {
+    GltfTerms g;
+    g.base_color = V(s.base_alpha);
+    g.alpha = s.base_alpha.w;
+    g.metallic = s.dielectric_metallic.w;
+    g.e1 = s.model.y;
+    g.share = s.model.z;
+    g.f0 = V(s.dielectric_metallic);
+    g.f90 = s.model.w;
+    g.transmission = s.normal.w;
+    g.coat_scale = s.shading_normal.w;
+    g.coat_dim = s.outgoing.w;
+    g.coat_alpha = s.fresnel.x;
+    const float tx = s.fresnel.y, ty = s.fresnel.z;
+    g.coat_normal = V(tx, ty, sqrtf(fmaxf(1.0f - (tx * tx + ty * ty), 0.0f)));
+    g.sheen_color = V(s.extension);
+    g.sheen_roughness = s.fresnel.w;
+    g.sheen_dim = s.extension.w;
+    c.composed = make_gltf_closure(g, V(s.outgoing));
+    return c;
+  }
+  Closure& b = c.preview;
   b.base_color = V(s.base_alpha);
   b.alpha = s.base_alpha.w;
   b.metallic = s.dielectric_metallic.w;
@@ -193,24 +251,25 @@ __device__ __forceinline__ Closure load_closure(const RestirSurface& s) {
   b.eta = fabsf(s.outgoing.w);
   b.thin_walled = s.shading_normal.w < 0.0f;
   b.smooth = s.outgoing.w < 0.0f;
-  return b;
+  return c;
 }
 
 // HistoryContribution (restir.slang:256-268).
+template <bool kFullShading>
 __device__ __forceinline__ F3 history_contribution(const SceneView& S, const RestirSurface& src,
     uint32_t light, const LightSample& ls) {
-  const Closure b = load_closure(src);
   if (!(ls.pdf > 0.0f) || dot(ls.direction, V(src.normal)) <= 0.0f) return V(0.0f);
+  const StoredClosure b = load_closure<kFullShading>(src);
   const Frame basis = make_frame(V(src.shading_normal));
-  return reflection_evaluate_side(b, V(src.outgoing), basis.to_local(ls.direction)) * ls.radiance *
+  return reflection_evaluate_side<kFullShading>(b, V(src.outgoing), basis.to_local(ls.direction)) * ls.radiance *
       (S.lights[light].pdf / ls.pdf);
 }
 
-template <bool kTextured>
+template <bool kFullShading>
 __device__ __forceinline__ F3 history_contribution_uv(const SceneView& S, const RestirSurface& src,
     uint32_t light, const float* uv) {
-  return history_contribution(S, src, light,
-      reconstruct_reservoir_light<true, kTextured>(S, light, uv[0], uv[1], V(src.origin)));
+  return history_contribution<kFullShading>(S, src, light,
+      reconstruct_reservoir_light<true, kFullShading>(S, light, uv[0], uv[1], V(src.origin)));
 }
 
 __device__ __forceinline__ bool same_sample(const RestirPixel& a, const RestirPixel& b) {
@@ -218,14 +277,14 @@ __device__ __forceinline__ bool same_sample(const RestirPixel& a, const RestirPi
 }
 
 // HistoryTarget (restir.slang:276-285).
-template <bool kTextured>
+template <bool kFullShading>
 __device__ __forceinline__ float history_target(const SceneView& S, const RestirReuse& source,
     const RestirSurface& surface, const RestirPixel& selected, bool& valid) {
   if (same_sample(source.pixel, selected)) {
     valid = isfinite(source.pixel.reservoir.selected_target);
     return source.pixel.reservoir.selected_target;
   }
-  const F3 c = history_contribution_uv<kTextured>(S, surface, selected.reservoir.sample, selected.uv);
+  const F3 c = history_contribution_uv<kFullShading>(S, surface, selected.reservoir.sample, selected.uv);
   valid = is_finite(c);
   return max_component(c);
 }
@@ -280,7 +339,7 @@ __device__ __forceinline__ RestirPixel empty_restir_pixel() {
 // WriteInitialReservoir (restir.slang:163-233): M candidates streamed over
 // the light table at the jittered camera surface, then one shadow ray for
 // the selected sample (queued for the deferred visibility, pass 0).
-template <bool kTextured>
+template <bool kFullShading>
 __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     RestirPixel* __restrict__ out, uint4* __restrict__ primary_hit, uint32_t* __restrict__ primary_rng,
@@ -298,13 +357,13 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
     uint32_t camera_rng;
     start_path(f, px, py, f.sample_index, ro, rd, tmax, camera_rng);
     Hit hit;
-    const bool found = trace_closest<false, kTextured>(S, ro, rd, 0.0f, tmax, camera_rng, hit);
+    const bool found = trace_closest<false, kFullShading>(S, ro, rd, 0.0f, tmax, camera_rng, hit);
     primary_hit[slot] = found ? make_uint4(hit.instance, hit.tri, __float_as_uint(hit.b1), __float_as_uint(hit.b2))
                               : make_uint4(kNoPrimaryHit, 0u, 0u, 0u);
     primary_rng[slot] = camera_rng;
     if (found) {
       r.flags |= 1u;
-      const SurfaceHit sh = reconstruct_hit<kTextured>(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
+      const SurfaceHit sh = reconstruct_hit<kFullShading>(S, hit.instance, hit.tri, hit.b1, hit.b2, rd);
       const Frame basis = make_frame(sh.shading_normal);
       const F3 wo = basis.to_local(-rd);
       const F3 origin = offset_ray_origin(sh.position, sh.normal);
@@ -318,8 +377,8 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
           const float random = next_random(rng);
           const uint32_t light = choose_reservoir_light(S, tc.restir_proposal, cx, cy);
           const float proposal = reservoir_proposal_pdf(S, tc.restir_proposal, light);
-          const LightSample ls = reconstruct_reservoir_light<true, kTextured>(S, light, ux, uy, origin);
-          const F3 fc = candidate_contribution(sh, basis, wo, ls, S.lights[light].pdf);
+          const LightSample ls = reconstruct_reservoir_light<true, kFullShading>(S, light, ux, uy, origin);
+          const F3 fc = candidate_contribution<kFullShading>(sh, basis, wo, ls, S.lights[light].pdf);
           bool selected;
           if (!isfinite(ls.pdf) || !is_finite(fc) ||
               !stream_candidate(r.reservoir, light, max_component(fc), proposal, random, selected)) {
@@ -334,9 +393,9 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
         }
       }
       if ((r.flags & 2u) == 0 && r.reservoir.weight_sum > 0.0f) {
-        const LightSample ls = reconstruct_reservoir_light<true, kTextured>(S, r.reservoir.sample, r.uv[0], r.uv[1], origin);
+        const LightSample ls = reconstruct_reservoir_light<true, kFullShading>(S, r.reservoir.sample, r.uv[0], r.uv[1], origin);
         queue_visibility(VQ, 0, slot, origin, ls,
-            candidate_contribution(sh, basis, wo, ls, S.lights[r.reservoir.sample].pdf),
+            candidate_contribution<kFullShading>(sh, basis, wo, ls, S.lights[r.reservoir.sample].pdf),
             reservoir_normalization(r.reservoir));
       }
     }
@@ -346,7 +405,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_initial(S
 }
 
 // WriteTemporalReservoir (restir.slang:302-387).
-template <bool kTextured>
+template <bool kFullShading>
 __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     const uint4* __restrict__ primary_hit, const TemporalInstance* __restrict__ identities, const RestirPixel* __restrict__ initial,
@@ -373,7 +432,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
     // The camera ray's hit as the initial pass traced it.
     const uint4 ph = primary_hit[slot];
     if (ph.x != kNoPrimaryHit) {
-      const SurfaceHit sh = reconstruct_hit<kTextured>(S, ph.x, ph.y, __uint_as_float(ph.z), __uint_as_float(ph.w), rd);
+      const SurfaceHit sh = reconstruct_hit<kFullShading>(S, ph.x, ph.y, __uint_as_float(ph.z), __uint_as_float(ph.w), rd);
       const Frame basis = make_frame(sh.shading_normal);
       const F3 wo = basis.to_local(-rd);
       const F3 origin = offset_ray_origin(sh.position, sh.normal);
@@ -382,7 +441,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
       receiver.normal = F4(sh.normal, 0.0f);
       receiver.shading_normal = F4(sh.shading_normal, 0.0f);
       receiver.outgoing = F4(wo, 0.0f);
-      store_closure(sh.bsdf, receiver);
+      store_closure<kFullShading>(sh, receiver);
       receiver.instance_id = identities[ph.x].instance_id;
       receiver.material_id = identities[ph.x].material_id;
       const ValidityPixel v = validity[slot];
@@ -400,7 +459,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
             if (source.pixel.reservoir.sample >= S.light_count)
               result.pixel.flags |= 2u;
             else
-              received = history_contribution_uv<kTextured>(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
+              received = history_contribution_uv<kFullShading>(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
           }
           uint32_t rng = seed_random(slot, f.sample_index ^ 0x94D049BBu);
           bool selected;
@@ -418,7 +477,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
             }
             if (result.pixel.reservoir.weight_sum > 0.0f) {
               bool valid_support;
-              const float support = history_target<kTextured>(S, source, psrc, result.pixel, valid_support);
+              const float support = history_target<kFullShading>(S, source, psrc, result.pixel, valid_support);
               if (!valid_support) result.pixel.flags |= 2u;
               result.supporting_candidates = initial[slot].reservoir.candidate_count + (support > 0.0f ? count : 0u);
             } else {
@@ -429,10 +488,10 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_temporal(
         }
       }
       if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
-        const LightSample ls = reconstruct_reservoir_light<true, kTextured>(S, result.pixel.reservoir.sample,
+        const LightSample ls = reconstruct_reservoir_light<true, kFullShading>(S, result.pixel.reservoir.sample,
             result.pixel.uv[0], result.pixel.uv[1], origin);
         receiver_estimate(VQ, 1, slot, initial[slot], origin, ls,
-            history_contribution(S, receiver, result.pixel.reservoir.sample, ls), result.normalization,
+            history_contribution<kFullShading>(S, receiver, result.pixel.reservoir.sample, ls), result.normalization,
             result.pixel);
       }
     }
@@ -493,7 +552,7 @@ __device__ __forceinline__ int spatial_offsets(uint32_t slot, uint32_t sample_in
 
 // WriteSpatialReservoir (restir.slang:402-491): the neighbours above,
 // merged with support correction.
-template <bool kTextured>
+template <bool kFullShading>
 __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(SceneView S,
     const FrameConst* __restrict__ fcp, const TemporalConst* __restrict__ tcp,
     const RestirReuse* __restrict__ temporal, const RestirSurface* __restrict__ surfaces,
@@ -534,7 +593,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
         const RestirReuse source = temporal[sources[i]];
         F3 received = V(0.0f);
         if (source.pixel.reservoir.weight_sum > 0.0f)
-          received = history_contribution_uv<kTextured>(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
+          received = history_contribution_uv<kFullShading>(S, receiver, source.pixel.reservoir.sample, source.pixel.uv);
         if (!is_finite(received) ||
             !merge_reevaluated(result.pixel.reservoir, source.pixel.reservoir, source.normalization,
                 max_component(received), tc.restir_max_history, next_random(rng), selected)) {
@@ -556,7 +615,7 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
           if (sources[i] == 0xffffffffu) continue;
           const RestirReuse source = temporal[sources[i]];
           bool valid_support;
-          const float support = history_target<kTextured>(S, source, surfaces[sources[i]], result.pixel, valid_support);
+          const float support = history_target<kFullShading>(S, source, surfaces[sources[i]], result.pixel, valid_support);
           if (!valid_support) result.pixel.flags |= 2u;
           if (support > 0.0f)
             result.supporting_candidates += min(source.pixel.reservoir.candidate_count, tc.restir_max_history);
@@ -564,10 +623,10 @@ __global__ void __launch_bounds__(kBlock, kRestirBlocksPerSm) k_restir_spatial(S
       }
       result.normalization = reuse_normalization(result.pixel.reservoir, result.supporting_candidates);
       if ((result.pixel.flags & 2u) == 0 && result.pixel.reservoir.weight_sum > 0.0f) {
-        const LightSample ls = reconstruct_reservoir_light<true, kTextured>(S, result.pixel.reservoir.sample,
+        const LightSample ls = reconstruct_reservoir_light<true, kFullShading>(S, result.pixel.reservoir.sample,
             result.pixel.uv[0], result.pixel.uv[1], V(receiver.origin));
         receiver_estimate(VQ, 2, slot, centre.pixel, V(receiver.origin), ls,
-            history_contribution(S, receiver, result.pixel.reservoir.sample, ls), result.normalization,
+            history_contribution<kFullShading>(S, receiver, result.pixel.reservoir.sample, ls), result.normalization,
             result.pixel);
       }
     }
@@ -855,7 +914,7 @@ inline uint32_t grid(uint32_t n) { return (n + kBlock - 1) / kBlock; }
 
 void launch_temporal_surface(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
     const TemporalInstance* ids, TemporalPixel* out, uint32_t pixels, cudaStream_t s) {
-  if (S.textured) k_temporal_surface<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, ids, out);
+  if (S.full_shading) k_temporal_surface<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, ids, out);
   else k_temporal_surface<false><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, ids, out);
 }
 
@@ -867,7 +926,7 @@ void launch_reproject(const TemporalConst* tc, const TemporalPixel* current, con
 void launch_restir_initial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
     RestirPixel* out, uint4* primary_hit, uint32_t* primary_rng, const VisibilityQueue& vq, uint32_t pixels,
     cudaStream_t s) {
-  if (S.textured) k_restir_initial<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out, primary_hit, primary_rng, vq);
+  if (S.full_shading) k_restir_initial<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out, primary_hit, primary_rng, vq);
   else k_restir_initial<false><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, out, primary_hit, primary_rng, vq);
 }
 
@@ -876,7 +935,7 @@ void launch_restir_temporal(const SceneView& S, const FrameConst* fc, const Temp
     const ValidityPixel* validity, const TemporalPixel* surface, const RestirReuse* previous,
     const RestirSurface* previous_surfaces, RestirReuse* out, RestirSurface* out_surfaces,
     const VisibilityQueue& vq, uint32_t pixels, cudaStream_t s) {
-  if (S.textured)
+  if (S.full_shading)
     k_restir_temporal<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, primary_hit, ids, initial, validity, surface,
         previous, previous_surfaces, out, out_surfaces, vq);
   else
@@ -887,7 +946,7 @@ void launch_restir_temporal(const SceneView& S, const FrameConst* fc, const Temp
 void launch_restir_spatial(const SceneView& S, const FrameConst* fc, const TemporalConst* tc,
     const RestirReuse* temporal, const RestirSurface* surfaces, RestirReuse* out, uint4* sources,
     const VisibilityQueue& vq, uint32_t pixels, cudaStream_t s) {
-  if (S.textured) k_restir_spatial<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, temporal, surfaces, out, sources, vq);
+  if (S.full_shading) k_restir_spatial<true><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, temporal, surfaces, out, sources, vq);
   else k_restir_spatial<false><<<grid(pixels), kBlock, 0, s>>>(S, fc, tc, temporal, surfaces, out, sources, vq);
 }
 

@@ -285,14 +285,14 @@ __device__ __forceinline__ float reservoir_proposal_pdf(const SceneView& S, uint
 // distant lights by their receiver-independent maps; a sphere light's
 // candidates are points uniform over its whole area, back-facing ones
 // carrying nothing. kAnalytic = false leaves out the analytic lights' code,
-// kTextured = false the texture lookups', for scenes without them.
-template <bool kAnalytic = true, bool kTextured = true>
+// kFullShading = false the texture lookups', for scenes without them.
+template <bool kAnalytic = true, bool kFullShading = true>
 __device__ __forceinline__ LightSample reconstruct_reservoir_light(const SceneView& S,
     uint32_t index, float ux, float uy, F3 origin) {
   const LightRecord chosen = S.lights[index];
   if (chosen.instance == kEnvironmentLight) return sample_environment(S, chosen.pdf, ux, uy);
   if (!kAnalytic || (chosen.instance & kAnalyticLight) == 0)
-    return sample_triangle<kTextured>(S, index, chosen.pdf, ux, uy, origin);
+    return sample_triangle<kFullShading>(S, index, chosen.pdf, ux, uy, origin);
   const AnalyticLight& light = S.analytic[chosen.instance & ~kAnalyticLight];
   if (light.shape != kSphereLight) return sample_analytic(light, chosen.pdf, ux, uy, origin);
   const float z = 1.0f - 2.0f * ux;

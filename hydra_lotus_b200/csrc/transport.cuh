@@ -5,6 +5,7 @@
 #pragma once
 
 #include "bsdf.cuh"
+#include "gltf.cuh"
 #include "scene.cuh"
 
 namespace lotus {
@@ -17,8 +18,11 @@ struct SurfaceHit {
   F3 base_color;
   float roughness;
   float metallic;
-  Closure bsdf;
+  Closure bsdf;       // UsdPreviewSurface's closure
   F3 emission;
+  bool gltf;          // the closure is glTF PBR's: `composed`, built from `gltf_terms`
+  GltfClosure composed;
+  GltfTerms gltf_terms;
 };
 
 __device__ __forceinline__ F3 transform_point(const float4* m, F3 p) { return row_point(m, p); }
@@ -115,6 +119,24 @@ __device__ __forceinline__ F3 preview_emission(const SceneView& S, const Materia
   return V(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f), fmaxf(v.z, 0.0f));
 }
 
+// GltfEmission (scene.slang:579-588): emissive, or its lookup's RGB with
+// negative parts cut, times the strength.
+__device__ __forceinline__ F3 gltf_emission(const SceneView& S, const MaterialRecord& mat,
+    const MaterialLookups& ml, float s, float t) {
+  const float strength = mat.gltf.w;
+  const uint32_t k = ml.slot[LOTUS_GLTF_SLOT_EMISSIVE];
+  if (k == kNoTexture) return V(mat.emission_metallic) * strength;
+  const float4 v = texture_lookup(S, S.lookups[k], s, t);
+  return V(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f), fmaxf(v.z, 0.0f)) * strength;
+}
+
+// Emission (scene.slang:590-600) by the material's model.
+__device__ __forceinline__ F3 material_emission(const SceneView& S, const MaterialRecord& mat,
+    const MaterialLookups& ml, float s, float t) {
+  return (__float_as_uint(mat.coverage.z) & kMaterialGltf) ? gltf_emission(S, mat, ml, s, t)
+                                                           : preview_emission(S, mat, ml, s, t);
+}
+
 // EvaluatePreview's textured inputs (scene.slang:1184-1230): each lookup
 // replaces its input's constant, clamped into the input's range, and a
 // tangent-space normal other than the identity maps the shading normal.
@@ -173,13 +195,135 @@ static __device__ __noinline__ TexturedInputs textured_inputs(const SceneView& S
   return out;
 }
 
+// What EvaluateGltfPbr gives the hit (scene.slang:1276-1406).
+struct GltfHit {
+  F3 base_color;
+  float roughness;
+  float metallic;
+  F3 emission;
+  F3 shading_normal;
+  GltfTerms terms;
+  GltfClosure closure;
+};
+
+__device__ __forceinline__ float gltf_scalar(const SceneView& S, const MaterialLookups& ml, uint32_t slot,
+    float s, float t, float constant) {
+  const uint32_t k = ml.slot[slot];
+  if (k == kNoTexture) return constant;
+  return saturate(lookup_channel(texture_lookup(S, S.lookups[k], s, t), S.lookups[k].channel));
+}
+
+__device__ __forceinline__ F3 clamp_unit_normal(float4 v) {
+  return V(fminf(fmaxf(v.x, -1.0f), 1.0f), fminf(fmaxf(v.y, -1.0f), 1.0f), fminf(fmaxf(v.z, -1.0f), 1.0f));
+}
+
+// EvaluateGltfPbr (scene.slang:1276-1406): the model's inputs at the hit,
+// each texture lookup replacing its constant, clamped into its range; the
+// mapped shading normal; the coat's normal in the shading frame; the terms
+// with their table values at wo; and the closure. Not inlined: the
+// shading kernels keep none of its registers for other materials.
+static __device__ __noinline__ GltfHit gltf_hit(const SceneView& S, uint32_t instance, uint32_t material,
+    uint32_t primitive, float b1, float b2, F3 edge1, F3 edge2, F3 geometric, F3 shading, F3 direction) {
+  const MaterialRecord mat = S.materials[material];
+  const MaterialLookups ml = S.mat_lookups[material];
+  GltfHit out;
+  out.base_color = V(mat.base_roughness);
+  out.roughness = mat.base_roughness.w;
+  out.metallic = mat.emission_metallic.w;
+  out.emission = V(mat.emission_metallic) * mat.gltf.w;
+  F3 tangent_normal = V(ml.normal[0], ml.normal[1], ml.normal[2]);
+  const float dielectric_f0 = mat.coverage.w;
+  float specular = mat.gltf.x;
+  float transmission = mat.transmission.w;
+  F3 specular_color = V(mat.specular_ior);
+  float clearcoat = mat.gltf.y;
+  F3 sheen_color = V(mat.sheen);
+  float sheen_roughness = mat.sheen.w;
+  float clearcoat_roughness = mat.gltf.z;
+  const F3 mesh_normal = shading;
+  F3 coat_tangent_normal = V(0.0f, 0.0f, 1.0f);
+  out.shading_normal = shading;
+  if (__float_as_uint(mat.coverage.z) & kMaterialTextured) {
+    float s, t;
+    hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
+    uint32_t k = ml.slot[LOTUS_GLTF_SLOT_BASE_COLOR];
+    if (k != kNoTexture) {
+      const float4 v = texture_lookup(S, S.lookups[k], s, t);
+      out.base_color = V(saturate(v.x), saturate(v.y), saturate(v.z));
+    }
+    out.roughness = gltf_scalar(S, ml, LOTUS_GLTF_SLOT_ROUGHNESS, s, t, out.roughness);
+    out.metallic = gltf_scalar(S, ml, LOTUS_GLTF_SLOT_METALLIC, s, t, out.metallic);
+    out.emission = gltf_emission(S, mat, ml, s, t);
+    k = ml.slot[LOTUS_SLOT_NORMAL];
+    if (k != kNoTexture) tangent_normal = clamp_unit_normal(texture_lookup(S, S.lookups[k], s, t));
+    specular = gltf_scalar(S, ml, LOTUS_GLTF_SLOT_SPECULAR, s, t, specular);
+    transmission = gltf_scalar(S, ml, LOTUS_GLTF_SLOT_TRANSMISSION, s, t, transmission);
+    clearcoat = gltf_scalar(S, ml, LOTUS_GLTF_SLOT_CLEARCOAT, s, t, clearcoat);
+    clearcoat_roughness = gltf_scalar(S, ml, LOTUS_GLTF_SLOT_CLEARCOAT_ROUGHNESS, s, t, clearcoat_roughness);
+    sheen_roughness = gltf_scalar(S, ml, LOTUS_GLTF_SLOT_SHEEN_ROUGHNESS, s, t, sheen_roughness);
+    k = ml.slot[LOTUS_GLTF_SLOT_SPECULAR_COLOR];
+    if (k != kNoTexture) {
+      const float4 v = texture_lookup(S, S.lookups[k], s, t);
+      specular_color = V(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f), fmaxf(v.z, 0.0f));
+    }
+    k = ml.slot[LOTUS_GLTF_SLOT_SHEEN_COLOR];
+    if (k != kNoTexture) {
+      const float4 v = texture_lookup(S, S.lookups[k], s, t);
+      sheen_color = V(saturate(v.x), saturate(v.y), saturate(v.z));
+    }
+    k = ml.slot[LOTUS_GLTF_SLOT_CLEARCOAT_NORMAL];
+    if (k != kNoTexture) coat_tangent_normal = clamp_unit_normal(texture_lookup(S, S.lookups[k], s, t));
+  }
+  if (tangent_normal.x != 0.0f || tangent_normal.y != 0.0f || tangent_normal.z != 1.0f) {
+    const uint32_t k = ml.slot[LOTUS_SLOT_NORMAL];
+    out.shading_normal = mapped_normal(tangent_normal,
+        tangent_frame(S, instance, k != kNoTexture ? &S.lookups[k] : nullptr, primitive, edge1, edge2, shading),
+        geometric, direction);
+  }
+  // The closure's outgoing direction in the shading frame: without a coat
+  // only its cosine counts.
+  const float cos_o = dot(out.shading_normal, -direction);
+  F3 wo = V(sqrtf(fmaxf(1.0f - cos_o * cos_o, 0.0f)), 0.0f, cos_o);
+  GltfInputs in;
+  in.base_color = out.base_color;
+  in.roughness = out.roughness;
+  in.metallic = out.metallic;
+  in.dielectric_f0 = dielectric_f0;
+  in.specular = specular;
+  in.specular_color = specular_color;
+  in.transmission = transmission;
+  in.clearcoat = clearcoat;
+  in.clearcoat_roughness = clearcoat_roughness;
+  in.clearcoat_normal = V(0.0f, 0.0f, 1.0f);
+  in.sheen_color = sheen_color;
+  in.sheen_roughness = sheen_roughness;
+  if (clearcoat > 0.0f) {
+    F3 coat_normal = mesh_normal;
+    if (coat_tangent_normal.x != 0.0f || coat_tangent_normal.y != 0.0f || coat_tangent_normal.z != 1.0f) {
+      const uint32_t k = ml.slot[LOTUS_GLTF_SLOT_CLEARCOAT_NORMAL];
+      coat_normal = mapped_normal(coat_tangent_normal,
+          tangent_frame(S, instance, k != kNoTexture ? &S.lookups[k] : nullptr, primitive, edge1, edge2,
+              mesh_normal),
+          geometric, direction);
+    }
+    const Frame basis = make_frame(out.shading_normal);
+    const F3 local = basis.to_local(-direction);
+    wo.x = local.x;
+    wo.y = local.y;
+    in.clearcoat_normal = normalize(basis.to_local(coat_normal));
+  }
+  out.terms = make_gltf_terms(in, wo, S.albedo_tables);
+  out.closure = make_gltf_closure(out.terms, wo);
+  return out;
+}
+
 // ReconstructHit and EvaluatePreview (scene.slang:1408-1449, 1184-1260).
 // The corners come from the leaf-ordered triangle pool, which holds the
 // geometry's own positions. A texture lookup replaces its input's constant,
 // clamped into the input's range.
-// kTextured false: the scene has no texture lookups (SceneView::textured
+// kFullShading false: the scene has no texture lookups (SceneView::full_shading
 // clear), and the hit compiles without them.
-template <bool kTextured = true>
+template <bool kFullShading = true>
 __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32_t instance,
     uint32_t tri, float b1, float b2, F3 direction, uint32_t* primitive_out = nullptr) {
   const InstanceShading rec = S.inst_shade[instance];
@@ -206,7 +350,24 @@ __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32
   const uint32_t flags = __float_as_uint(mat.coverage.z);
   F3 emission = V(mat.emission_metallic);
   F3 specular = V(mat.specular_ior);
-  if (kTextured && (flags & kMaterialTextured)) {
+  sh.gltf = false;
+  if (kFullShading && (flags & kMaterialGltf)) {
+    const GltfHit g = gltf_hit(S, instance, rec.material, primitive, b1, b2, p1 - p0, p2 - p0, sh.normal,
+        sh.shading_normal, direction);
+    sh.base_color = g.base_color;
+    sh.roughness = g.roughness;
+    sh.metallic = g.metallic;
+    sh.shading_normal = g.shading_normal;
+    sh.emission = g.emission;
+    sh.gltf = true;
+    sh.composed = g.closure;
+    sh.gltf_terms = g.terms;
+    // MakeBsdfClosure(model, composed) (bsdf.slang:42-50): the preview
+    // closure it carries beside the composed one.
+    sh.bsdf = make_closure(V(0.0f), 1.0f, 0.0f, 1.5f, false, V(0.0f), 0.0f, V(1.0f), false, true);
+    return sh;
+  }
+  if (kFullShading && (flags & kMaterialTextured)) {
     const TexturedInputs ti = textured_inputs(S, instance, rec.material, primitive, b1, b2, p1 - p0, p2 - p0,
         sh.normal, sh.shading_normal, direction);
     sh.base_color = ti.base_color;
@@ -227,6 +388,27 @@ __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32
       (flags & 2u) != 0, entering);
   sh.emission = emission;
   return sh;
+}
+
+// BsdfEvaluate, BsdfPdf and BsdfSample (bsdf.slang:52-90): the hit's
+// closure by its model. kFullShading false: no glTF PBR material is in the
+// scene, and only UsdPreviewSurface's closure is compiled.
+template <bool kFullShading>
+__device__ __forceinline__ F3 surface_evaluate(const SurfaceHit& sh, F3 wo, F3 wi) {
+  if (kFullShading && sh.gltf) return gltf_evaluate(sh.composed, wo, wi);
+  return bsdf_evaluate(sh.bsdf, wo, wi);
+}
+
+template <bool kFullShading>
+__device__ __forceinline__ float surface_pdf(const SurfaceHit& sh, F3 wo, F3 wi) {
+  if (kFullShading && sh.gltf) return gltf_pdf(sh.composed, wo, wi);
+  return bsdf_pdf(sh.bsdf, wo, wi);
+}
+
+template <bool kFullShading>
+__device__ __forceinline__ bool surface_sample(const SurfaceHit& sh, F3 wo, F3 u, BsdfSample& s) {
+  if (kFullShading && sh.gltf) return gltf_sample(sh.composed, wo, u, s);
+  return bsdf_sample(sh.bsdf, wo, u, s);
 }
 
 struct LightSample {
@@ -258,12 +440,12 @@ static __device__ __noinline__ F3 textured_light_radiance(const SceneView& S, ui
   const MaterialLookups ml = S.mat_lookups[rec.material];
   float s, t;
   hit_texcoords(S, instance, ml, primitive, b1, b2, s, t);
-  return preview_emission(S, mat, ml, s, t) * material_coverage(S, mat, rec.material, instance, primitive, b1, b2);
+  return material_emission(S, mat, ml, s, t) * material_coverage(S, mat, rec.material, instance, primitive, b1, b2);
 }
 
 // SampleTriangle (scene.slang:632-677), over the light table's
 // world-space corners.
-template <bool kTextured = true>
+template <bool kFullShading = true>
 __device__ __forceinline__ LightSample sample_triangle(const SceneView& S, uint32_t light,
     float pdf, float ux, float uy, F3 origin) {
   const float root = sqrtf(ux);
@@ -275,7 +457,7 @@ __device__ __forceinline__ LightSample sample_triangle(const SceneView& S, uint3
   const float area = triangle_area(p0, p1, p2);
   const float4 stored = S.light_radiance[light];
   F3 radiance = V(stored);
-  if (kTextured && stored.w != 0.0f) radiance = textured_light_radiance(S, light, b1, b2);
+  if (kFullShading && stored.w != 0.0f) radiance = textured_light_radiance(S, light, b1, b2);
   const F3 toward = position - origin;
   const float distance2 = dot(toward, toward);
   if (!(area > 0.0f) || !(distance2 > 0.0f) || max_component(radiance) <= 0.0f) return no_light();
@@ -642,7 +824,7 @@ static __device__ __noinline__ F3 crossed_lights(const SceneView& S, F3 origin, 
 // SampleLight (scene.slang:894-909): Vose's alias table, then a point.
 // kAnalytic = false leaves out the analytic lights' code, for scenes
 // without them.
-template <bool kAnalytic = true, bool kTextured = true>
+template <bool kAnalytic = true, bool kFullShading = true>
 __device__ __forceinline__ LightSample sample_light(const SceneView& S, float u0, float u1,
     float u2, float u3, F3 origin) {
   const uint32_t count = S.light_count;
@@ -653,7 +835,7 @@ __device__ __forceinline__ LightSample sample_light(const SceneView& S, float u0
   if (chosen.instance == kEnvironmentLight) return sample_environment(S, chosen.pdf, u2, u3);
   if (kAnalytic && (chosen.instance & kAnalyticLight) != 0)
     return sample_analytic(S.analytic[chosen.instance & ~kAnalyticLight], chosen.pdf, u2, u3, origin);
-  return sample_triangle<kTextured>(S, light, chosen.pdf, u2, u3, origin);
+  return sample_triangle<kFullShading>(S, light, chosen.pdf, u2, u3, origin);
 }
 
 // EmitterPdf (scene.slang:1004-1010).

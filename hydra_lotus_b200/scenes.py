@@ -118,6 +118,32 @@ def preview_material(base_color=(0.18, 0.18, 0.18), roughness=0.5, metallic=0.0,
     return m
 
 
+def gltf_material(base_color=(1.0, 1.0, 1.0), metallic=1.0, roughness=1.0, emissive=(0.0, 0.0, 0.0),
+                  emissive_strength=1.0, ior=1.5, specular=1.0, specular_color=(1.0, 1.0, 1.0),
+                  transmission=0.0, clearcoat=0.0, clearcoat_roughness=0.0, sheen_color=(0.0, 0.0, 0.0),
+                  sheen_roughness=0.0, opacity=1.0, opacity_threshold=0.0):
+    """MaterialX's glTF PBR surface with the definition's defaults, a rough
+    white metal (GltfPbr, material.hpp:180-217)."""
+    m = abi.Material()
+    m.model = abi.MODEL_GLTF_PBR
+    m.base_color[:] = [float(v) for v in base_color]
+    m.metallic = metallic
+    m.roughness = roughness
+    m.emission[:] = [float(v) for v in emissive]
+    m.emissive_strength = emissive_strength
+    m.ior = ior
+    m.specular = specular
+    m.specular_color[:] = [float(v) for v in specular_color]
+    m.transmission = transmission
+    m.clearcoat = clearcoat
+    m.clearcoat_roughness = clearcoat_roughness
+    m.sheen_color[:] = [float(v) for v in sheen_color]
+    m.sheen_roughness = sheen_roughness
+    m.opacity = opacity
+    m.opacity_threshold = opacity_threshold
+    return m
+
+
 class Scene:
     """A scene in the C ABI's layout, plus its camera and target size."""
 
@@ -1860,4 +1886,174 @@ def material_emission(raw_emission=False, size=160):
             s.add_instance(right, slot["Warm"], m)
         else:
             s.add_instance(geo, slot[look], m, texcoord_set=1 if geo in s.texcoords else 0)
+    return s
+
+
+def _place2d(pivot, scale, degrees, offset, order):
+    """ND_place2d's st matrix in double (Place2d, material_fixtures.cpp:
+    1394-1413 in hydra-lotus): it moves by the offset, rotates about the
+    pivot and divides by the scale, in operation order `order`."""
+    c, s = math.cos(degrees * (math.pi / 180.0)), math.sin(degrees * (math.pi / 180.0))
+    m = [0.0] * 6
+    if order == 0:
+        m[0], m[1] = c / scale[0], s / scale[1]
+        m[3], m[4] = -s / scale[0], c / scale[1]
+        m[2] = -(m[0] * pivot[0] + m[1] * pivot[1]) - offset[0] + pivot[0]
+        m[5] = -(m[3] * pivot[0] + m[4] * pivot[1]) - offset[1] + pivot[1]
+    else:
+        m[0], m[1] = c / scale[0], s / scale[0]
+        m[3], m[4] = -s / scale[1], c / scale[1]
+        x, y = -pivot[0] - offset[0], -pivot[1] - offset[1]
+        m[2] = (c * x + s * y) / scale[0] + pivot[0]
+        m[5] = (-s * x + c * y) / scale[1] + pivot[1]
+    return m
+
+
+def gltf_place(scale, degrees, offset):
+    """ND_gltf_image's placement as the reference's translator composes it
+    (GltfPlace, material_fixtures.cpp:1415-1421): ND_place2d about (0, 1)
+    in order 0, the scale inverted, the rotation negated and the offset
+    negated in s; rounded to float."""
+    m = _place2d((0.0, 1.0), (1.0 / scale[0], 1.0 / scale[1]), -degrees, (-offset[0], offset[1]), 0)
+    return tuple(float(F32(v)) for v in m)
+
+
+def _palette(x, y):
+    return (40 + 60 * x, 40 + 60 * y, 200 if (x + y) % 2 == 0 else 60, 255)
+
+
+def _rgba(x, y):
+    return (220 - 60 * x, 40 + 60 * y, 40 + 60 * ((x + y) % 4), 30 + 65 * x)
+
+
+def _tilts(x, y):
+    return (32 + 64 * x, 224 - 64 * y, 200, 255)
+
+
+def _cutout(x, y):
+    dx, dy = 2 * x - 7, 2 * y - 7
+    d = dx * dx + dy * dy
+    return (60 + 20 * x, 200 - 15 * y, 60, 255 if d <= 26 else (96 if d <= 50 else 0))
+
+
+def _unit_card(s):
+    """A unit card in the XY plane with the st set over the unit square
+    (Card({{"st", Corners(kUnit)}}), material_fixtures.cpp:315-330)."""
+    g = s.add_geometry(np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)],
+                                dtype=F32), np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+    s.set_texcoords(g, np.array([[[(0, 0), (1, 0), (1, 1)], [(0, 0), (1, 1), (0, 1)]]], dtype=F32))
+    return g
+
+
+def _wrapped_sphere(s):
+    """The coarse sphere with its points as corner normals and the st set
+    longitude by latitude times (4, 2)."""
+    g = _coarse_smooth_sphere(s)
+    points, faces = coarse_sphere_polygons()
+    corners = coarse_sphere_corners(faces)
+    latlong = coarse_sphere_latlong()
+    s.set_texcoords(g, np.array([latlong[fv] for _, _, fv in corners], dtype=F32).reshape(1, -1, 3, 2))
+    return g
+
+
+def material_gltf(exchanged_channels=False, size=160):
+    """The reference's material-gltf-v1 fixture (SetMaterialGltf,
+    material_fixtures.cpp:2274-2371 in hydra-lotus), which its golden
+    images validation/reference/material-gltf-v1-{mean,variance}.pfm were
+    rendered from: MaterialX's glTF PBR surface on a 5x5 grid in the
+    material studio, coarse spheres (scale 0.35) and st-mapped cards (scale
+    0.7). Rows from the top: constants (the definition's defaults, a red
+    dielectric, a glossy grey, copper, a half-metal); base-colour images
+    (plain, a factor, the same as ND_gltf_colorimage, copper with metallic
+    and roughness packed in one image, a placed image); normal maps and
+    emission; alpha modes; unrepresented inputs, which render as the rest
+    of the material. ``exchanged_channels`` reads Packed's metallic from
+    green and roughness from blue (the fixture's negative control,
+    ExchangedChannels)."""
+    s = material_studio("material-gltf-v1", size)
+    palette_tex = s.add_texture(_texture_image(4, _palette), abi.TEXTURE_RGBA8_SRGB)
+    rgba_tex = s.add_texture(_texture_image(4, _rgba), abi.TEXTURE_RGBA8_UNORM)
+    tilts_tex = s.add_texture(_texture_image(4, _tilts), abi.TEXTURE_RGBA8_UNORM)
+    cutout_tex = s.add_texture(_texture_image(8, _cutout), abi.TEXTURE_RGBA8_SRGB)
+    rep = abi.WRAP_REPEAT
+    copper, red, teal, grey = (0.95, 0.64, 0.54), (0.8, 0.2, 0.1), (0.2, 0.6, 0.7), (0.7, 0.7, 0.7)
+    transparent = (0.0, 0.0, 0.0, 0.0)
+
+    def periodic(texture, **kw):
+        return s.add_texture_input(texture, wrap_s=rep, wrap_t=rep, **kw)
+
+    palette = periodic(palette_tex, fallback=transparent)
+    tinted = periodic(palette_tex, fallback=transparent, scale=(1.0, 0.5, 0.25, 1.0))
+    rotated = periodic(palette_tex, fallback=transparent, st_transform=gltf_place((2.0, 1.0), 30.0,
+                                                                                   (float(F32(0.1)), float(F32(0.2)))))
+
+    def textured(lookup):
+        m = gltf_material((1.0, 1.0, 1.0), 0.0, 0.6)
+        m.lookups[abi.GLTF_SLOT_BASE_COLOR] = lookup
+        return m, True
+
+    packed = gltf_material(copper, 1.0, 1.0)
+    packed.lookups[abi.GLTF_SLOT_METALLIC] = periodic(rgba_tex, fallback=transparent,
+                                                      channel=1 if exchanged_channels else 2)
+    packed.lookups[abi.GLTF_SLOT_ROUGHNESS] = periodic(rgba_tex, fallback=transparent,
+                                                       channel=2 if exchanged_channels else 1)
+    bumps = periodic(tilts_tex, scale=(2.0, 2.0, 2.0, 1.0), bias=(-1.0, -1.0, -1.0, 0.0),
+                     fallback=(-1.0, -1.0, -1.0, 1.0))
+    gltf_bumps = periodic(tilts_tex, scale=(2.0, 2.0, 2.0, 1.0), bias=(-1.0, -1.0, -1.0, 0.0),
+                          fallback=(0.0, 0.0, 1.0, 1.0))
+
+    def bumpy(m, lookup):
+        m.lookups[abi.SLOT_NORMAL] = lookup
+        return m, True
+
+    emissive = gltf_material(grey, 0.0, 0.4, emissive=(1.0, 0.6, 0.2))
+    emissive_map = gltf_material(grey, 0.0, 0.4, emissive_strength=2.0)
+    emissive_map.lookups[abi.GLTF_SLOT_EMISSIVE] = periodic(palette_tex)
+    cutout = periodic(cutout_tex, fallback=transparent)
+    mask = gltf_material((1.0, 1.0, 1.0), 0.0, 0.6, opacity_threshold=0.5)
+    mask.lookups[abi.GLTF_SLOT_BASE_COLOR] = cutout
+    mask.lookups[abi.SLOT_OPACITY] = periodic(cutout_tex, fallback=transparent, channel=3)
+    blend = gltf_material((1.0, 1.0, 1.0), 0.0, 0.6, opacity_threshold=0.0)
+    blend.lookups[abi.GLTF_SLOT_BASE_COLOR] = cutout
+    blend.lookups[abi.SLOT_OPACITY] = periodic(cutout_tex, fallback=transparent, channel=3)
+    unlit = gltf_material((0.0, 0.0, 0.0), 0.0, 1.0, emissive=teal, specular=0.0)
+    looks = [
+        ("Defaults", (gltf_material((1.0, 1.0, 1.0), 1.0, 1.0), False)),
+        ("Dielectric", (gltf_material(red, 0.0, 0.5), False)),
+        ("Glossy", (gltf_material((0.5, 0.5, 0.5), 0.0, 0.1), False)),
+        ("Metal", (gltf_material(copper, 1.0, 0.3), False)),
+        ("Mixed", (gltf_material((0.9, 0.6, 0.2), 0.5, 0.3), False)),
+        ("Image", textured(palette)),
+        ("Factor", textured(tinted)),
+        ("ColorImage", textured(tinted)),
+        ("Packed", (packed, True)),
+        ("Rotated", textured(rotated)),
+        ("GltfNormal", bumpy(gltf_material(grey, 0.0, 0.4), gltf_bumps)),
+        ("NormalMap", bumpy(gltf_material(grey, 0.0, 0.4), bumps)),
+        ("NormalMetal", bumpy(gltf_material(copper, 1.0, 0.25), gltf_bumps)),
+        ("Emissive", (emissive, False)),
+        ("EmissiveMap", (emissive_map, True)),
+        ("Opaque", (gltf_material(teal, 0.0, 0.5), False)),
+        ("Mask", (mask, True)),
+        ("MaskZero", (gltf_material(teal, 0.0, 0.5), False)),
+        ("MaskAll", (gltf_material(teal, 0.0, 0.5, opacity=0.0), False)),
+        ("Blend", (blend, True)),
+        ("Iridescence", (gltf_material(red, 0.0, 0.5), False)),
+        ("Thickness", (gltf_material(red, 0.0, 0.5), False)),
+        ("Unlit", (unlit, False)),
+        ("Anisotropy", (gltf_material(red, 0.0, 0.5), False)),
+        ("VertexColor", (gltf_material((1.0, 1.0, 1.0), 0.0, 0.6), False)),
+    ]
+    smooth = _coarse_smooth_sphere(s)
+    wrapped = _wrapped_sphere(s)
+    card = _unit_card(s)
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (1.6, 0.8, 0.0, -0.8, -1.6)
+    for i, (name, (m, uses_st)) in enumerate(looks):
+        ball = i < 5 or name == "NormalMetal"
+        geo = wrapped if name == "NormalMetal" else (smooth if ball else card)
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = placed[5] = placed[10] = 0.35 if ball else 0.7
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        s.add_instance(geo, s.add_material(m), placed,
+                       texcoord_set=1 if uses_st and geo in s.texcoords else 0)
     return s

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define LOTUS_CUDA_ABI_VERSION 9u
+#define LOTUS_CUDA_ABI_VERSION 10u
 
 /* FrameStatus (vulkan_backend.hpp:23-27). */
 #define LOTUS_PASS 0
@@ -65,6 +65,10 @@ extern "C" {
 /* UsdPreviewSurface flags (gpu_scene.hpp:82-87). */
 #define LOTUS_MATERIAL_SPECULAR_WORKFLOW 1u
 #define LOTUS_MATERIAL_THIN_WALLED 2u
+
+/* ShadingModel (material.hpp:90-99): the material's surface model. */
+#define LOTUS_MODEL_PREVIEW_SURFACE 0u
+#define LOTUS_MODEL_GLTF_PBR 1u
 
 /* One mesh: Lotus::MeshGeometry (render_world.hpp:39-58), object space. */
 typedef struct lotus_geometry {
@@ -139,22 +143,44 @@ typedef struct lotus_texture_input {
   uint32_t reserved[2];
 } lotus_texture_input;
 
-/* A material's texture-input slots (material.hpp:266-273): a lookup
- * replaces the input's constant, clamped into its range (the normal slot's
+/* A material's texture-input slots (material.hpp:262-286): a lookup
+ * replaces the input's constant, clamped into its range (the normal slots'
  * into [-1, 1]: a tangent-space normal, in the frame of the texture
- * coordinates' differentials about the interpolated shading normal). */
+ * coordinates' differentials about the interpolated shading normal).
+ * Slots 0 and 1 are the geometry's in every model; the others are
+ * numbered per model. */
 #define LOTUS_SLOT_OPACITY 0u
 #define LOTUS_SLOT_NORMAL 1u
+/* UsdPreviewSurface's. */
 #define LOTUS_SLOT_BASE_COLOR 2u
 #define LOTUS_SLOT_ROUGHNESS 3u
 #define LOTUS_SLOT_METALLIC 4u
 #define LOTUS_SLOT_EMISSION 5u
 #define LOTUS_SLOT_SPECULAR_COLOR 6u
-#define LOTUS_TEXTURE_SLOTS 7u
+/* glTF PBR's. */
+#define LOTUS_GLTF_SLOT_BASE_COLOR 2u
+#define LOTUS_GLTF_SLOT_METALLIC 3u
+#define LOTUS_GLTF_SLOT_ROUGHNESS 4u
+#define LOTUS_GLTF_SLOT_EMISSIVE 5u
+#define LOTUS_GLTF_SLOT_SPECULAR 6u
+#define LOTUS_GLTF_SLOT_SPECULAR_COLOR 7u
+#define LOTUS_GLTF_SLOT_TRANSMISSION 8u
+#define LOTUS_GLTF_SLOT_CLEARCOAT 9u
+#define LOTUS_GLTF_SLOT_CLEARCOAT_ROUGHNESS 10u
+#define LOTUS_GLTF_SLOT_CLEARCOAT_NORMAL 11u
+#define LOTUS_GLTF_SLOT_SHEEN_COLOR 12u
+#define LOTUS_GLTF_SLOT_SHEEN_ROUGHNESS 13u
+#define LOTUS_TEXTURE_SLOTS 14u
 #define LOTUS_NO_LOOKUP 0u
 
-/* UsdPreviewSurface's constants (material.hpp:137-173) plus the material's
- * coverage (material.hpp:103-116). */
+/* A material (material.hpp:219-245): its surface model's constants,
+ * UsdPreviewSurface's (material.hpp:137-173) or MaterialX's glTF PBR
+ * surface's (material.hpp:180-217), plus its coverage (material.hpp:
+ * 103-116). The first fields serve both models: base_color, roughness,
+ * metallic, emission (glTF PBR's emissive), specular_color, ior and
+ * transmission carry the inputs of those names; transmission_color and
+ * flags are UsdPreviewSurface's only, and the fields after `normal` glTF
+ * PBR's only. */
 typedef struct lotus_material {
   float base_color[3];
   float roughness;
@@ -167,7 +193,7 @@ typedef struct lotus_material {
   float opacity;            /* surface coverage in [0, 1] */
   float opacity_threshold;  /* > 0: binary coverage */
   uint32_t flags;           /* LOTUS_MATERIAL_* */
-  uint32_t reserved;
+  uint32_t model;           /* LOTUS_MODEL_* */
   /* Per LOTUS_SLOT_*: k > 0 for lotus_scene_desc::texture_inputs[k - 1],
    * LOTUS_NO_LOOKUP (0) for the constant. */
   uint32_t lookups[LOTUS_TEXTURE_SLOTS];
@@ -178,6 +204,17 @@ typedef struct lotus_material {
    * [-1, 1]); all zero means the identity (0, 0, 1). A normal-map lookup
    * (LOTUS_SLOT_NORMAL) replaces it. */
   float normal[3];
+  /* glTF PBR: a finite, non-negative factor on emissive. */
+  float emissive_strength;
+  /* glTF PBR, each in [0, 1]: the dielectric reflection's weight, the
+   * clearcoat's weight and roughness. */
+  float specular;
+  float clearcoat;
+  float clearcoat_roughness;
+  /* glTF PBR: the sheen's colour (each in [0, 1]; the largest is its
+   * weight) and roughness in [0, 1]. */
+  float sheen_color[3];
+  float sheen_roughness;
 } lotus_material;
 
 /* A latitude-longitude environment image (render_world.hpp:122-133): RGBA

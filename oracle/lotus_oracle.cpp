@@ -529,6 +529,729 @@ bool PreviewSample(const PreviewClosure& b, F3 wo, F3 u, BsdfSampleResult& s) {
 }
 
 // ---------------------------------------------------------------------------
+// Composed closures and MaterialX's glTF PBR surface (bsdf/albedo.slang,
+// bsdf/lobes.slang, bsdf/composed.slang, bsdf/gltf_pbr.slang), with the
+// scene passes' configuration: no attenuating layer and no dielectric
+// refraction, thin-wall or delta paths (LOTUS_COMPOSED_FULL 0).
+
+// The elementary functions the albedo axes and the sheen need, written out
+// as the library does (natural log by 2 atanh((m - 1) / (m + 1)) after
+// splitting off the binary exponent; exp by Cody and Waite's reduction and
+// Taylor's series), so that host and device agree bit for bit where the
+// reference uses the shading language's log and pow.
+inline float LLog(float x) {
+  if (!(x > 0.0f)) return x == 0.0f ? -AsFloat(0x7f800000u) : AsFloat(0x7fc00000u);
+  int e = 0;
+  if (x < 1.17549435e-38f) {
+    x *= 8388608.0f;
+    e = -23;
+  }
+  const uint32_t b = AsUint(x);
+  e += (int)((b >> 23) & 0xffu) - 127;
+  float m = AsFloat((b & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.41421354f) {
+    m *= 0.5f;
+    e += 1;
+  }
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float s2 = s * s;
+  const float p = s2 * (0.333333343f + s2 * (0.2f + s2 * (0.142857149f + s2 * (0.111111112f +
+      s2 * (0.0909090936f + s2 * (0.0769230798f + s2 * 0.0666666701f))))));
+  const float log_m = 2.0f * s + 2.0f * s * p;
+  const float fe = (float)e;
+  return fe * 0.693145751953125f + (fe * 1.42860677e-6f + log_m);
+}
+
+inline float LExp(float x) {
+  if (!(x > -104.0f)) return x == x ? 0.0f : x;
+  if (x > 89.0f) return AsFloat(0x7f800000u);
+  const float k = std::rint(x * 1.44269502f);
+  const float r = (x - k * 0.693145751953125f) - k * 1.42860677e-6f;
+  const float p = 1.0f + r * (1.0f + r * (0.5f + r * (0.166666672f + r * (0.0416666679f +
+      r * (0.00833333377f + r * (0.00138888892f + r * (0.000198412701f + r * 2.48015876e-5f)))))));
+  int ki = (int)k;
+  float scale = 1.0f;
+  if (ki < -126) {
+    ki += 64;
+    scale = 5.42101086e-20f;
+  } else if (ki > 127) {
+    ki -= 1;
+    scale = 2.0f;
+  }
+  return p * AsFloat((uint32_t)(ki + 127) << 23) * scale;
+}
+
+inline float LPow(float x, float y) { return x > 0.0f ? LExp(y * LLog(x)) : 0.0f; }
+
+// The directional albedo tables' data: the library's own generated tables
+// (albedo.slang's layout, 76800 floats).
+const float kAlbedoTableData[] = {
+#include "../hydra_lotus_b200/csrc/albedo_tables.inc"
+};
+static_assert(sizeof(kAlbedoTableData) == 76800 * sizeof(float), "albedo tables");
+
+// albedo.slang:22-65.
+constexpr uint32_t kAlbedoGgx = 0, kAlbedoSchlickShare = 1, kAlbedoDielectric = 2, kAlbedoSheen = 3;
+constexpr uint32_t kDielectricEntering = 0, kDielectricLeaving = 1, kDielectricThin = 2,
+                   kDielectricSheets = 3;
+constexpr uint32_t kGgxCosines = 32, kDielectricCosines = 48, kAlbedoAlphas = 32, kAlbedoIndices = 16;
+constexpr float kAlbedoMinIndex = 1.01f, kAlbedoMaxIndex = 3.0f;
+constexpr float kMinCosine = 2.0e-4f, kCosineSlope = 4.0f, kAlphaSlope = 2.0f, kIndexSlope = 0.5f;
+constexpr float kMinSheenAxis = 0.005f;
+constexpr uint32_t kCriticalNode = kDielectricCosines / 2;
+constexpr float kCriticalCoordinate = float(kCriticalNode) / float(kDielectricCosines - 1);
+constexpr float kMinEvanescent = 2.0e-3f;
+
+uint32_t AlbedoTableOffset(uint32_t table) {
+  const uint32_t ggx = kGgxCosines * kAlbedoAlphas;
+  if (table <= kAlbedoDielectric) return table * ggx;
+  return (table - 1) * ggx + kDielectricSheets * kAlbedoIndices * kDielectricCosines * kAlbedoAlphas;
+}
+
+// albedo.slang:86-190.
+inline float LogLinearScale(float v, float slope) { return LLog(v) + slope * v; }
+
+inline float LogLinearCoordinate(float v, float low, float high, float slope) {
+  const float clamped = std::fmin(std::fmax(v, low), high);
+  return (LogLinearScale(clamped, slope) - LogLinearScale(low, slope)) /
+      (LogLinearScale(high, slope) - LogLinearScale(low, slope));
+}
+
+inline float CosineCoordinate(float c) { return LogLinearCoordinate(c, kMinCosine, 1.0f, kCosineSlope); }
+inline float AlphaCoordinate(float a) { return LogLinearCoordinate(a, kMinAlpha, 1.0f, kAlphaSlope); }
+inline float SheenCoordinate(float r) { return LogLinearCoordinate(r, kMinSheenAxis, 1.0f, kAlphaSlope); }
+inline float IndexCoordinate(float index) {
+  return LogLinearCoordinate(index - 1.0f, kAlbedoMinIndex - 1.0f, kAlbedoMaxIndex - 1.0f, kIndexSlope);
+}
+
+inline float CriticalCosine(float index) { return std::sqrt(std::fmax(1.0f - 1.0f / (index * index), 0.0f)); }
+
+inline float EvanescentScale(float mu, float index, float critical) {
+  const float tau = std::fmax(index * std::sqrt(std::fmax(critical * critical - mu * mu, 0.0f)),
+      kMinEvanescent);
+  return LLog(mu) - LLog(tau) + kCosineSlope * mu;
+}
+
+inline float LeavingCoordinate(float cos_theta, float index) {
+  const float critical = CriticalCosine(index);
+  if (cos_theta < critical) {
+    const float low = EvanescentScale(kMinCosine, index, critical);
+    const float high = EvanescentScale(critical, index, critical);
+    return kCriticalCoordinate *
+        saturate((EvanescentScale(std::fmax(cos_theta, kMinCosine), index, critical) - low) / (high - low));
+  }
+  const float refracted = std::sqrt(std::fmax(1.0f - index * index * (1.0f - cos_theta * cos_theta), 0.0f));
+  // lerp(kCriticalCoordinate, 1, x)
+  const float x = CosineCoordinate(refracted);
+  return kCriticalCoordinate + (1.0f - kCriticalCoordinate) * x;
+}
+
+// albedo.slang:246-312.
+inline void CubicWeights(float t, float w[4]) {
+  const float t2 = t * t;
+  const float t3 = t2 * t;
+  w[0] = -0.5f * t3 + t2 - 0.5f * t;
+  w[1] = 1.5f * t3 - 2.5f * t2 + 1.0f;
+  w[2] = -1.5f * t3 + 2.0f * t2 + 0.5f * t;
+  w[3] = 0.5f * t3 - 0.5f * t2;
+}
+
+float FetchNode(uint32_t base, uint32_t cosines, int cosine, int alpha, int first, int last) {
+  const int last_alpha = (int)kAlbedoAlphas - 1;
+  const int c = std::min(std::max(cosine, first), last);
+  const int a = std::min(std::max(alpha, 0), last_alpha);
+  const int dc = cosine < first ? 1 : (cosine > last ? -1 : 0);
+  const int da = alpha < 0 ? 1 : (alpha > last_alpha ? -1 : 0);
+  const float at = kAlbedoTableData[base + (uint32_t)(a * (int)cosines + c)];
+  if (dc == 0 && da == 0) return at;
+  const float inner = kAlbedoTableData[base + (uint32_t)((a + da) * (int)cosines + c + dc)];
+  return 2.0f * at - inner;
+}
+
+float FetchSlice(uint32_t base, uint32_t cosines, float x_cosine, float x_alpha, bool split) {
+  const float fc = saturate(x_cosine) * float(cosines - 1);
+  const float fa = saturate(x_alpha) * float(kAlbedoAlphas - 1);
+  const int c0 = (int)std::min((uint32_t)fc, cosines - 2);
+  const int a0 = (int)std::min((uint32_t)fa, kAlbedoAlphas - 2);
+  int first = 0;
+  int last = (int)cosines - 1;
+  if (split) {
+    if (c0 < (int)kCriticalNode) last = (int)kCriticalNode;
+    else first = (int)kCriticalNode;
+  }
+  float wc[4], wa[4];
+  CubicWeights(fc - float(c0), wc);
+  CubicWeights(fa - float(a0), wa);
+  float value = 0.0f;
+  for (int j = 0; j < 4; ++j) {
+    float row = 0.0f;
+    for (int i = 0; i < 4; ++i) row += wc[i] * FetchNode(base, cosines, c0 + i - 1, a0 + j - 1, first, last);
+    value += wa[j] * row;
+  }
+  return value;
+}
+
+// albedo.slang:314-373.
+float AlbedoGgx(float cos_theta, float alpha) {
+  return FetchSlice(AlbedoTableOffset(kAlbedoGgx), kGgxCosines, CosineCoordinate(cos_theta),
+      AlphaCoordinate(alpha), false);
+}
+
+float AlbedoSchlickShare(float cos_theta, float alpha) {
+  return FetchSlice(AlbedoTableOffset(kAlbedoSchlickShare), kGgxCosines, CosineCoordinate(cos_theta),
+      AlphaCoordinate(alpha), false);
+}
+
+float AlbedoSheen(float cos_theta, float roughness) {
+  return std::fmax(FetchSlice(AlbedoTableOffset(kAlbedoSheen), kGgxCosines, CosineCoordinate(cos_theta),
+      SheenCoordinate(roughness), false), 0.0f);
+}
+
+float AlbedoDielectric(float cos_theta, float alpha, float eta, bool thin_walled) {
+  uint32_t sheet = thin_walled ? kDielectricThin : kDielectricEntering;
+  float index = eta;
+  if (eta < 1.0f) {
+    index = 1.0f / eta;
+    sheet = thin_walled ? kDielectricThin : kDielectricLeaving;
+  }
+  index = std::fmin(std::fmax(index, kAlbedoMinIndex), kAlbedoMaxIndex);
+  const float fi = IndexCoordinate(index) * float(kAlbedoIndices - 1);
+  const int i0 = (int)std::min((uint32_t)fi, kAlbedoIndices - 2);
+  const bool split = sheet == kDielectricLeaving;
+  const float x_cosine = split ? LeavingCoordinate(cos_theta, index) : CosineCoordinate(cos_theta);
+  const float x_alpha = AlphaCoordinate(alpha);
+  const uint32_t slice_size = kDielectricCosines * kAlbedoAlphas;
+  const uint32_t base = AlbedoTableOffset(kAlbedoDielectric) + sheet * kAlbedoIndices * slice_size;
+  float slices[4];
+  for (int j = 0; j < 4; ++j) {
+    const int slice = std::min(std::max(i0 + j - 1, 0), (int)kAlbedoIndices - 1);
+    slices[j] = FetchSlice(base + (uint32_t)slice * slice_size, kDielectricCosines, x_cosine, x_alpha, split);
+  }
+  if (i0 == 0) slices[0] = 2.0f * slices[1] - slices[2];
+  if (i0 == (int)kAlbedoIndices - 2) slices[3] = 2.0f * slices[2] - slices[1];
+  float w[4];
+  CubicWeights(fi - float(i0), w);
+  return w[0] * slices[0] + w[1] * slices[1] + w[2] * slices[2] + w[3] * slices[3];
+}
+
+// --- Lobes (lobes.slang) ---------------------------------------------------
+
+constexpr uint32_t kLambertLobe = 0, kGgxSchlickLobe = 1, kGgxDielectricLobe = 2, kSheenLobe = 3;
+constexpr uint32_t kScatterReflect = 1, kScatterTransmit = 2, kScatterBoth = 3;
+constexpr float kMinSheenRoughness = 0.005f;
+
+struct Lobe {
+  uint32_t type;
+  F3 normal;
+  F3 color;
+  F3 f90;
+  float alpha;
+  float eta;
+  uint32_t scatter;
+  bool thin_walled;
+  bool transmit;
+  bool smooth;
+  bool compensate;
+  F3 compensation;
+};
+
+Lobe MakeLobe(uint32_t type, F3 normal) {
+  Lobe lobe;
+  lobe.type = type;
+  lobe.normal = normal;
+  lobe.color = V(1.0f);
+  lobe.f90 = V(1.0f);
+  lobe.alpha = 1.0f;
+  lobe.eta = 1.0f;
+  lobe.scatter = kScatterReflect;
+  lobe.thin_walled = false;
+  lobe.transmit = false;
+  lobe.smooth = false;
+  lobe.compensate = false;
+  lobe.compensation = V(1.0f);
+  return lobe;
+}
+
+Lobe MakeLambertLobe(F3 color, F3 normal) {
+  Lobe lobe = MakeLobe(kLambertLobe, normal);
+  lobe.color = color;
+  return lobe;
+}
+
+Lobe MakeGgxSchlickLobe(F3 f0, F3 f90, float alpha, F3 normal, bool compensate) {
+  Lobe lobe = MakeLobe(kGgxSchlickLobe, normal);
+  lobe.color = f0;
+  lobe.f90 = f90;
+  lobe.alpha = std::fmax(alpha, kMinAlpha);
+  lobe.compensate = compensate;
+  return lobe;
+}
+
+Lobe MakeSheenLobe(F3 color, float roughness, F3 normal) {
+  Lobe lobe = MakeLobe(kSheenLobe, normal);
+  lobe.color = color;
+  lobe.alpha = std::fmax(roughness, kMinSheenRoughness);
+  return lobe;
+}
+
+Lobe MakeGgxDielectricLobe(float eta, F3 tint, float alpha, uint32_t scatter, bool thin_walled, F3 normal,
+    bool compensate) {
+  Lobe lobe = MakeLobe(kGgxDielectricLobe, normal);
+  lobe.color = tint;
+  lobe.alpha = std::fmax(alpha, kMinAlpha);
+  lobe.eta = eta;
+  lobe.scatter = scatter;
+  lobe.thin_walled = thin_walled;
+  lobe.smooth = alpha < kMinAlpha || eta == 1.0f;
+  lobe.compensate = compensate;
+  return lobe;
+}
+
+inline bool LobeScattersToward(const Lobe& lobe, F3 wi) {
+  if (lobe.type == kGgxDielectricLobe)
+    return wi.z > 0.0f ? (lobe.scatter & kScatterReflect) != 0 : (lobe.scatter & kScatterTransmit) != 0;
+  return lobe.transmit ? wi.z < 0.0f : wi.z > 0.0f;
+}
+
+inline F3 SchlickFresnel(F3 f0, F3 f90, float cos_theta) {
+  const float weight = lpow5(saturate(1.0f - cos_theta));
+  return f0 * (1.0f - weight) + f90 * weight;
+}
+
+inline float DielectricReflectance(const Lobe& lobe, float cos_theta) {
+  const float r = FresnelDielectric(cos_theta, lobe.eta);
+  return lobe.thin_walled ? 2.0f * r / (1.0f + r) : r;
+}
+
+inline float GgxReflection(F3 wo, F3 wi, F3 h, float alpha) {
+  const float g2 = 1.0f / (1.0f + GgxLambda(wo, alpha) + GgxLambda(wi, alpha));
+  return GgxD(h, alpha) * g2 / (4.0f * wo.z);
+}
+
+inline float GgxReflectionPdf(F3 wo, F3 h, float alpha) {
+  const float g1 = 1.0f / (1.0f + GgxLambda(wo, alpha));
+  return GgxD(h, alpha) * g1 / (4.0f * wo.z);
+}
+
+// SheenValue (lobes.slang:260-271).
+F3 SheenValue(const Lobe& lobe, F3 wo, F3 wi) {
+  if (!(wi.z > 0.0f)) return V(0.0f);
+  const F3 h = normalize(wo + wi);
+  const float inverse = 1.0f / lobe.alpha;
+  const float sin2 = std::fmax(1.0f - h.z * h.z, 0.0f);
+  const float d = (2.0f + inverse) * LPow(sin2, 0.5f * inverse) / (2.0f * kPi);
+  return lobe.color * lobe.compensation * (d * wi.z / (4.0f * (wi.z + wo.z - wi.z * wo.z)));
+}
+
+// DielectricValue (lobes.slang:273-303), reflection only.
+F3 DielectricValue(const Lobe& lobe, F3 wo, F3 wi) {
+  if (lobe.smooth) return V(0.0f);
+  if (wi.z > 0.0f) {
+    if ((lobe.scatter & kScatterReflect) == 0) return V(0.0f);
+    const F3 h = normalize(wo + wi);
+    return lobe.color * lobe.compensation *
+        (DielectricReflectance(lobe, dot(wo, h)) * GgxReflection(wo, wi, h, lobe.alpha));
+  }
+  return V(0.0f);
+}
+
+// LobeValue (lobes.slang:306-325).
+F3 LobeValue(const Lobe& lobe, F3 wo, F3 wi) {
+  if (!(wo.z > 0.0f)) return V(0.0f);
+  switch (lobe.type) {
+    case kLambertLobe:
+      return wi.z > 0.0f ? lobe.color * (wi.z / kPi) : V(0.0f);
+    case kGgxSchlickLobe: {
+      const F3 wr = lobe.transmit ? V(wi.x, wi.y, -wi.z) : wi;
+      if (!(wr.z > 0.0f)) return V(0.0f);
+      const F3 h = normalize(wo + wr);
+      return SchlickFresnel(lobe.color, lobe.f90, dot(wo, h)) * lobe.compensation *
+          GgxReflection(wo, wr, h, lobe.alpha);
+    }
+    case kSheenLobe:
+      return SheenValue(lobe, wo, wi);
+    default:
+      return DielectricValue(lobe, wo, wi);
+  }
+}
+
+// DielectricPdf (lobes.slang:327-362), reflection only.
+float DielectricPdf(const Lobe& lobe, F3 wo, F3 wi) {
+  if (lobe.smooth) return 0.0f;
+  const bool both = lobe.scatter == kScatterBoth;
+  if (wi.z > 0.0f) {
+    if ((lobe.scatter & kScatterReflect) == 0) return 0.0f;
+    const F3 h = normalize(wo + wi);
+    const float choice = both ? DielectricReflectance(lobe, dot(wo, h)) : 1.0f;
+    return choice * GgxReflectionPdf(wo, h, lobe.alpha);
+  }
+  return 0.0f;
+}
+
+// LobePdf (lobes.slang:364-383).
+float LobePdf(const Lobe& lobe, F3 wo, F3 wi) {
+  if (!(wo.z > 0.0f)) return 0.0f;
+  switch (lobe.type) {
+    case kLambertLobe:
+      return wi.z > 0.0f ? wi.z / kPi : 0.0f;
+    case kGgxSchlickLobe: {
+      const F3 wr = lobe.transmit ? V(wi.x, wi.y, -wi.z) : wi;
+      return wr.z > 0.0f ? GgxReflectionPdf(wo, normalize(wo + wr), lobe.alpha) : 0.0f;
+    }
+    case kSheenLobe:
+      return wi.z > 0.0f ? 1.0f / (2.0f * kPi) : 0.0f;
+    default:
+      return DielectricPdf(lobe, wo, wi);
+  }
+}
+
+// LobeSample (lobes.slang:446-508), without the dielectric's refraction,
+// thin-wall and delta paths.
+bool LobeSample(const Lobe& lobe, F3 wo, F3 u, F3& wi) {
+  wi = V(0.0f, 0.0f, 1.0f);
+  if (!(wo.z > 0.0f)) return false;
+  switch (lobe.type) {
+    case kLambertLobe:
+      wi = SampleCosineHemisphere(u.x, u.y);
+      return wi.z > 0.0f;
+    case kGgxSchlickLobe: {
+      const F3 h = SampleGgxVisibleNormal(wo, lobe.alpha, u.x, u.y);
+      wi = 2.0f * dot(wo, h) * h - wo;
+      if (!(wi.z > 0.0f)) return false;
+      if (lobe.transmit) wi.z = -wi.z;
+      return true;
+    }
+    case kSheenLobe: {
+      const float sin_theta = std::sqrt(std::fmax(1.0f - u.x * u.x, 0.0f));
+      const float phi = 2.0f * kPi * u.y;
+      float s, c;
+      lsincos(phi, s, c);
+      wi = V(sin_theta * c, sin_theta * s, u.x);
+      return wi.z > 0.0f;
+    }
+    default: {
+      const F3 h = SampleGgxVisibleNormal(wo, lobe.alpha, u.x, u.y);
+      const float cos_oh = dot(wo, h);
+      if (!(cos_oh > 0.0f)) return false;
+      const F3 reflected = 2.0f * cos_oh * h - wo;
+      bool reflect = lobe.scatter == kScatterReflect;
+      if (lobe.scatter == kScatterBoth) reflect = u.z < DielectricReflectance(lobe, cos_oh);
+      if (reflect) {
+        wi = reflected;
+        return reflected.z > 0.0f;
+      }
+      return false;
+    }
+  }
+}
+
+// --- Composed closures (composed.slang) -------------------------------------
+
+constexpr uint32_t kMaxLobes = 6;
+constexpr float kSelectionFloor = 0.05f;
+
+struct ComposedClosure {
+  uint32_t count = 0;
+  Lobe lobes[kMaxLobes];
+  F3 weights[kMaxLobes];
+  float probabilities[kMaxLobes];
+};
+
+struct ComposedBuilder {
+  ComposedClosure closure;
+  F3 albedos[kMaxLobes];
+  F3 estimates[kMaxLobes];
+};
+
+// No layer of these closures attenuates (ComposedAttenuate is never
+// called): every attenuation factor is 1.
+inline F3 AttenuationFactor() { return V(1.0f); }
+
+ComposedBuilder ComposedBegin() {
+  ComposedBuilder builder;
+  builder.closure.count = 0;
+  for (uint32_t k = 0; k < kMaxLobes; ++k) {
+    builder.closure.lobes[k] = MakeLambertLobe(V(0.0f), V(0.0f, 0.0f, 1.0f));
+    builder.closure.weights[k] = V(0.0f);
+    builder.closure.probabilities[k] = 0.0f;
+    builder.albedos[k] = V(0.0f);
+    builder.estimates[k] = V(0.0f);
+  }
+  return builder;
+}
+
+uint32_t ComposedPush(ComposedBuilder& b, const Lobe& lobe, F3 albedo, F3 estimate) {
+  const uint32_t k = b.closure.count;
+  if (k >= kMaxLobes) return k;
+  b.closure.count = k + 1;
+  b.closure.weights[k] = V(1.0f);
+  b.closure.lobes[k] = lobe;
+  b.albedos[k] = albedo;
+  b.estimates[k] = estimate;
+  return k;
+}
+
+uint32_t ComposedAddLambert(ComposedBuilder& b, const Lobe& lobe, F3 wo) {
+  const F3 albedo = dot(wo, lobe.normal) > 0.0f ? lobe.color : V(0.0f);
+  return ComposedPush(b, lobe, albedo, albedo);
+}
+
+uint32_t ComposedAddSchlick(ComposedBuilder& b, const Lobe& added, F3 wo, float e1, float share) {
+  Lobe lobe = added;
+  F3 albedo = V(0.0f);
+  if (dot(wo, lobe.normal) > 0.0f) {
+    if (lobe.compensate && e1 > 0.0f) lobe.compensation = V(1.0f) + lobe.color * ((1.0f - e1) / e1);
+    albedo = (lobe.color * (e1 - share) + lobe.f90 * share) * lobe.compensation;
+  }
+  return ComposedPush(b, lobe, lobe.transmit ? V(0.0f) : albedo, albedo);
+}
+
+uint32_t ComposedAddWeighted(ComposedBuilder& b, const Lobe& lobe, F3 weight, F3 albedo) {
+  const uint32_t k = ComposedPush(b, lobe, albedo, albedo * lobe.color);
+  if (k < kMaxLobes) b.closure.weights[k] = weight;
+  return k;
+}
+
+void ComposedScale(ComposedBuilder& b, uint32_t begin, uint32_t end, F3 scale) {
+  for (uint32_t k = begin; k < std::min(end, b.closure.count); ++k)
+    b.closure.weights[k] = b.closure.weights[k] * scale;
+}
+
+void ComposedMix(ComposedBuilder& b, uint32_t begin, uint32_t split, uint32_t end, float mix) {
+  ComposedScale(b, begin, split, V(1.0f - mix));
+  ComposedScale(b, split, end, V(mix));
+}
+
+F3 ComposedAlbedo(const ComposedBuilder& b, uint32_t begin, uint32_t end) {
+  F3 albedo = V(0.0f);
+  for (uint32_t k = begin; k < std::min(end, b.closure.count); ++k)
+    albedo = albedo + b.closure.weights[k] * AttenuationFactor() * b.albedos[k];
+  return albedo;
+}
+
+inline F3 SaturateRgb(F3 v) { return V(saturate(v.x), saturate(v.y), saturate(v.z)); }
+
+void ComposedLayer(ComposedBuilder& b, uint32_t begin, uint32_t split, uint32_t end) {
+  const F3 top = ComposedAlbedo(b, begin, split);
+  ComposedScale(b, split, end, SaturateRgb(V(1.0f) - top));
+}
+
+void ComposedLayerScalar(ComposedBuilder& b, uint32_t begin, uint32_t split, uint32_t end) {
+  const F3 top = ComposedAlbedo(b, begin, split);
+  ComposedScale(b, split, end, SaturateRgb(V(1.0f - MaxComponent(top))));
+}
+
+ComposedClosure ComposedFinalize(const ComposedBuilder& b) {
+  ComposedClosure closure = b.closure;
+  float total = 0.0f;
+  for (uint32_t k = 0; k < closure.count; ++k) {
+    const float estimate = MaxComponent(closure.weights[k] * AttenuationFactor() * b.estimates[k]);
+    closure.probabilities[k] = estimate > 0.0f ? estimate : 0.0f;
+    total += closure.probabilities[k];
+  }
+  if (!(total > 0.0f)) return closure;
+  float floored = 0.0f;
+  for (uint32_t k = 0; k < closure.count; ++k)
+    if (closure.probabilities[k] > 0.0f) {
+      closure.probabilities[k] = std::fmax(closure.probabilities[k] / total, kSelectionFloor);
+      floored += closure.probabilities[k];
+    }
+  for (uint32_t k = 0; k < closure.count; ++k) closure.probabilities[k] /= floored;
+  return closure;
+}
+
+F3 ComposedEvaluate(const ComposedClosure& c, F3 wo, F3 wi) {
+  F3 value = V(0.0f);
+  for (uint32_t k = 0; k < c.count; ++k) {
+    const Lobe& lobe = c.lobes[k];
+    if (!LobeScattersToward(lobe, wi)) continue;
+    const ShadingFrame frame = MakeShadingFrame(lobe.normal);
+    value = value + c.weights[k] * AttenuationFactor() * LobeValue(lobe, frame.ToLocal(wo), frame.ToLocal(wi));
+  }
+  return value;
+}
+
+float ComposedPdf(const ComposedClosure& c, F3 wo, F3 wi) {
+  float pdf = 0.0f;
+  for (uint32_t k = 0; k < c.count; ++k) {
+    const Lobe& lobe = c.lobes[k];
+    if (!(c.probabilities[k] > 0.0f) || !LobeScattersToward(lobe, wi)) continue;
+    const ShadingFrame frame = MakeShadingFrame(lobe.normal);
+    pdf += c.probabilities[k] * LobePdf(lobe, frame.ToLocal(wo), frame.ToLocal(wi));
+  }
+  return pdf;
+}
+
+bool ComposedSample(const ComposedClosure& c, F3 wo, F3 u, BsdfSampleResult& s) {
+  s.wi = V(0.0f, 0.0f, 1.0f);
+  s.weight = V(0.0f);
+  s.pdf = 0.0f;
+  s.delta = false;
+  s.transmitted = false;
+  uint32_t chosen = kMaxLobes;
+  float start = 0.0f, end = 0.0f;
+  for (uint32_t k = 0; k < c.count; ++k) {
+    const float p = c.probabilities[k];
+    if (!(p > 0.0f)) continue;
+    chosen = k;
+    start = end;
+    end += p;
+    if (u.z < end) break;
+  }
+  if (chosen == kMaxLobes) return false;
+  const float probability = c.probabilities[chosen];
+  u.z = std::fmin(std::fmax((u.z - start) / probability, 0.0f), 0.99999994f);
+  const Lobe& lobe = c.lobes[chosen];
+  const ShadingFrame frame = MakeShadingFrame(lobe.normal);
+  F3 local;
+  if (!LobeSample(lobe, frame.ToLocal(wo), u, local)) return false;
+  s.wi = frame.ToWorld(local);
+  if (!LobeScattersToward(lobe, s.wi)) return false;
+  s.transmitted = s.wi.z < 0.0f;
+  s.pdf = ComposedPdf(c, wo, s.wi);
+  if (!(s.pdf > 0.0f)) return false;
+  s.weight = ComposedEvaluate(c, wo, s.wi) / s.pdf;
+  return IsFinite(s.weight);
+}
+
+// --- MaterialX's glTF PBR (gltf_pbr.slang) ------------------------------------
+
+constexpr float kGltfClearcoatIndex = 1.5f;
+
+struct GltfPbrInputs {
+  F3 base_color;
+  float roughness;
+  float metallic;
+  float dielectric_f0;
+  float specular;
+  F3 specular_color;
+  float transmission;
+  float clearcoat;
+  float clearcoat_roughness;
+  F3 clearcoat_normal;
+  F3 sheen_color;
+  float sheen_roughness;
+};
+
+// MakeGltfPbrInputs (gltf_pbr.slang:54-72).
+GltfPbrInputs MakeGltfPbrInputs(F3 base_color, float roughness, float metallic) {
+  GltfPbrInputs in;
+  in.base_color = base_color;
+  in.roughness = roughness;
+  in.metallic = metallic;
+  in.dielectric_f0 = 0.04f;
+  in.specular = 1.0f;
+  in.specular_color = V(1.0f);
+  in.transmission = 0.0f;
+  in.clearcoat = 0.0f;
+  in.clearcoat_roughness = 0.0f;
+  in.clearcoat_normal = V(0.0f, 0.0f, 1.0f);
+  in.sheen_color = V(0.0f);
+  in.sheen_roughness = 0.0f;
+  return in;
+}
+
+struct GltfPbrTerms {
+  F3 base_color;
+  float alpha;
+  float metallic;
+  float e1;
+  float share;
+  F3 f0;
+  float f90;
+  float transmission;
+  float coat_scale;
+  float coat_dim;
+  float coat_alpha;
+  F3 coat_normal;
+  F3 sheen_color;
+  float sheen_roughness;
+  float sheen_dim;
+};
+
+// MakeGltfPbrTerms (gltf_pbr.slang:106-157).
+GltfPbrTerms MakeGltfPbrTerms(const GltfPbrInputs& in, F3 wo) {
+  GltfPbrTerms t;
+  t.base_color = in.base_color;
+  t.alpha = std::fmax(in.roughness * in.roughness, kMinAlpha);
+  t.metallic = in.metallic;
+  t.e1 = 0.0f;
+  t.share = 0.0f;
+  if (wo.z > 0.0f) {
+    t.e1 = AlbedoGgx(wo.z, t.alpha);
+    t.share = AlbedoSchlickShare(wo.z, t.alpha);
+  }
+  t.f0 = SaturateRgb(in.specular_color * in.dielectric_f0) * in.specular;
+  t.f90 = in.specular;
+  t.transmission = in.transmission;
+  t.coat_scale = 0.0f;
+  t.coat_dim = 0.0f;
+  t.coat_alpha = std::fmax(in.clearcoat_roughness * in.clearcoat_roughness, kMinAlpha);
+  t.coat_normal = in.clearcoat_normal.z > 0.0f ? in.clearcoat_normal : V(0.0f, 0.0f, 1.0f);
+  const float coat_cos = dot(wo, t.coat_normal);
+  if (in.clearcoat > 0.0f && coat_cos > 0.0f) {
+    const float reflected = AlbedoDielectric(coat_cos, t.coat_alpha, kGltfClearcoatIndex, false);
+    const float coat_e1 = AlbedoGgx(coat_cos, t.coat_alpha);
+    const float coat_root = (1.0f - kGltfClearcoatIndex) / (1.0f + kGltfClearcoatIndex);
+    float compensation = 1.0f;
+    if (coat_e1 > 0.0f) compensation += coat_root * coat_root * (1.0f - coat_e1) / coat_e1;
+    t.coat_scale = in.clearcoat * compensation;
+    t.coat_dim = saturate(t.coat_scale * reflected);
+  }
+  t.sheen_color = in.sheen_color;
+  t.sheen_roughness = std::fmax(in.sheen_roughness * in.sheen_roughness, kMinSheenRoughness);
+  t.sheen_dim = 0.0f;
+  const float sheen = MaxComponent(in.sheen_color);
+  if (sheen > 0.0f && wo.z > 0.0f) {
+    const float e = AlbedoSheen(wo.z, t.sheen_roughness);
+    if (e > 1.0f) t.sheen_color = in.sheen_color * (1.0f / e);
+    t.sheen_dim = saturate(sheen * std::fmin(e, 1.0f));
+  }
+  return t;
+}
+
+// MakeGltfPbrClosure (gltf_pbr.slang:230-290).
+ComposedClosure MakeGltfPbrClosure(const GltfPbrTerms& t, F3 wo) {
+  const F3 normal = V(0.0f, 0.0f, 1.0f);
+  const F3 white = V(1.0f);
+  ComposedBuilder b = ComposedBegin();
+  const uint32_t coat = b.closure.count;
+  if (t.coat_scale > 0.0f)
+    ComposedAddWeighted(b,
+        MakeGgxDielectricLobe(kGltfClearcoatIndex, white, t.coat_alpha, kScatterReflect, false, t.coat_normal,
+            false),
+        V(t.coat_scale), V(t.coat_dim / t.coat_scale));
+  const uint32_t sheen = b.closure.count;
+  if (t.sheen_dim > 0.0f)
+    ComposedAddWeighted(b, MakeSheenLobe(white, t.sheen_roughness, normal), t.sheen_color,
+        V(t.sheen_dim / MaxComponent(t.sheen_color)));
+  const bool dielectric = t.metallic < 1.0f;
+  const uint32_t top = b.closure.count;
+  if (dielectric && t.f90 > 0.0f)
+    ComposedAddSchlick(b, MakeGgxSchlickLobe(t.f0, V(t.f90), t.alpha, normal, true), wo, t.e1, t.share);
+  const uint32_t diffuse = b.closure.count;
+  if (dielectric && t.transmission < 1.0f) ComposedAddLambert(b, MakeLambertLobe(t.base_color, normal), wo);
+  const uint32_t transmitted = b.closure.count;
+  if (dielectric && t.transmission > 0.0f) {
+    Lobe lobe = MakeGgxSchlickLobe(white, white, t.alpha, normal, true);
+    lobe.transmit = true;
+    const uint32_t k = ComposedAddSchlick(b, lobe, wo, t.e1, t.share);
+    ComposedScale(b, k, k + 1, t.base_color);
+  }
+  const uint32_t metal = b.closure.count;
+  if (t.transmission > 0.0f) ComposedMix(b, diffuse, transmitted, metal, t.transmission);
+  ComposedLayerScalar(b, top, diffuse, metal);
+  if (t.metallic > 0.0f)
+    ComposedAddSchlick(b, MakeGgxSchlickLobe(t.base_color, white, t.alpha, normal, true), wo, t.e1, t.share);
+  const uint32_t end = b.closure.count;
+  ComposedMix(b, top, metal, end, t.metallic);
+  ComposedLayerScalar(b, sheen, top, end);
+  ComposedLayer(b, coat, sheen, end);
+  return ComposedFinalize(b);
+}
+
+
+// ---------------------------------------------------------------------------
 // Scene
 
 struct Box {
@@ -784,7 +1507,7 @@ inline F3 TransformPoint(const float* m, F3 p) {
            m[2] * p.x + m[6] * p.y + m[10] * p.z + m[14]);
 }
 
-// EmissionEstimate for a UsdPreviewSurface (gpu_scene.cpp:144-180): its
+// EmissionEstimate (gpu_scene.cpp:144-180): its
 // constant emission, or a lookup's bound for texels in [0, 1] (its
 // fallback when the lookup names no image).
 double EmissionEstimate(const oracle_scene& s, const lotus_material& m) {
@@ -799,7 +1522,9 @@ double EmissionEstimate(const oracle_scene& s, const lotus_material& m) {
                                            : double{std::max(0.0f, in.scale[c])} + std::max(0.0f, in.bias[c]);
     }
   }
-  const double factor = 1.0;
+  // glTF PBR's emissive (slot 5, as UsdPreviewSurface's emission) is
+  // scaled by its strength.
+  const double factor = m.model == LOTUS_MODEL_GLTF_PBR ? double{m.emissive_strength} : 1.0;
   const double mean = factor * (e[0] + e[1] + e[2]) / 3.0;
   return std::isfinite(mean) && mean > 0.0 ? mean : 0.0;
 }
@@ -1509,7 +2234,25 @@ struct SurfaceHit {
   float metallic;
   PreviewClosure bsdf;
   F3 emission;
+  // A glTF PBR surface's closure, built from its terms (MakeBsdfClosure,
+  // bsdf.slang:42-50); `bsdf` then holds the placeholder preview closure.
+  bool gltf = false;
+  ComposedClosure composed;
+  GltfPbrTerms gltf_terms;
 };
+
+// BsdfEvaluate, BsdfPdf and BsdfSample (bsdf.slang:52-90).
+F3 BsdfEvaluate(const SurfaceHit& sh, F3 wo, F3 wi) {
+  return sh.gltf ? ComposedEvaluate(sh.composed, wo, wi) : PreviewEvaluate(sh.bsdf, wo, wi);
+}
+
+float BsdfPdf(const SurfaceHit& sh, F3 wo, F3 wi) {
+  return sh.gltf ? ComposedPdf(sh.composed, wo, wi) : PreviewPdf(sh.bsdf, wo, wi);
+}
+
+bool BsdfSample(const SurfaceHit& sh, F3 wo, F3 u, BsdfSampleResult& s) {
+  return sh.gltf ? ComposedSample(sh.composed, wo, u, s) : PreviewSample(sh.bsdf, wo, u, s);
+}
 
 // OffsetRayOrigin (scene.slang:1454-1469).
 F3 OffsetRayOrigin(F3 position, F3 normal) {
@@ -1551,6 +2294,21 @@ F3 PreviewEmission(const oracle_scene& s, const lotus_material& m, float st_s, f
   if (lookup == LOTUS_NO_LOOKUP) return V(m.emission[0], m.emission[1], m.emission[2]);
   const Rgba v = Lookup(s, s.inputs[lookup - 1], st_s, st_t);
   return V(std::fmax(v.v[0], 0.0f), std::fmax(v.v[1], 0.0f), std::fmax(v.v[2], 0.0f));
+}
+
+// GltfEmission (scene.slang:579-588): emissive or its lookup, times the
+// strength.
+F3 GltfEmission(const oracle_scene& s, const lotus_material& m, float st_s, float st_t) {
+  const float strength = m.emissive_strength;
+  const uint32_t lookup = m.lookups[LOTUS_GLTF_SLOT_EMISSIVE];
+  if (lookup == LOTUS_NO_LOOKUP) return V(m.emission[0], m.emission[1], m.emission[2]) * strength;
+  const Rgba v = Lookup(s, s.inputs[lookup - 1], st_s, st_t);
+  return V(std::fmax(v.v[0], 0.0f), std::fmax(v.v[1], 0.0f), std::fmax(v.v[2], 0.0f)) * strength;
+}
+
+// Emission (scene.slang:590-600).
+F3 Emission(const oracle_scene& s, const lotus_material& m, float st_s, float st_t) {
+  return m.model == LOTUS_MODEL_GLTF_PBR ? GltfEmission(s, m, st_s, st_t) : PreviewEmission(s, m, st_s, st_t);
 }
 
 inline bool Textured(const lotus_material& m) {
@@ -1621,6 +2379,114 @@ F3 MappedNormal(F3 tangent_normal, const ShadingFrame& basis, F3 geometric, F3 d
 
 // ReconstructHit + EvaluatePreview (scene.slang:1408-1449, 1184-1260): a
 // texture lookup replaces its input's constant, clamped into its range.
+// GltfScalar (scene.slang:1262-1274): a scalar input's lookup channel,
+// clamped to [0, 1], or its constant.
+float GltfScalar(const oracle_scene& s, const lotus_material& m, uint32_t slot, float st_s, float st_t,
+    float constant) {
+  const uint32_t k = m.lookups[slot];
+  if (k == LOTUS_NO_LOOKUP) return constant;
+  const lotus_texture_input& in = s.inputs[k - 1];
+  return saturate(Lookup(s, in, st_s, st_t).v[in.channel]);
+}
+
+inline F3 ClampNormal(const Rgba& v) {
+  return V(std::fmin(std::fmax(v.v[0], -1.0f), 1.0f), std::fmin(std::fmax(v.v[1], -1.0f), 1.0f),
+      std::fmin(std::fmax(v.v[2], -1.0f), 1.0f));
+}
+
+// EvaluateGltfPbr (scene.slang:1276-1406).
+void EvaluateGltfPbr(const oracle_scene& s, const Hit& hit, const lotus_material& mat, F3 edge1, F3 edge2,
+    F3 direction, SurfaceHit& sh) {
+  sh.base_color = V(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
+  sh.roughness = mat.roughness;
+  sh.metallic = mat.metallic;
+  F3 emission = V(mat.emission[0], mat.emission[1], mat.emission[2]) * mat.emissive_strength;
+  const bool zero = mat.normal[0] == 0.0f && mat.normal[1] == 0.0f && mat.normal[2] == 0.0f;
+  F3 tangent_normal = zero ? V(0.0f, 0.0f, 1.0f) : V(mat.normal[0], mat.normal[1], mat.normal[2]);
+  // The dielectric's reflectance at normal incidence, which the host
+  // computes in double (gpu_scene.cpp:2059-2063).
+  const double root = (1.0 - double{mat.ior}) / (1.0 + double{mat.ior});
+  const float dielectric_f0 = static_cast<float>(root * root);
+  float specular = mat.specular;
+  float transmission = mat.transmission;
+  F3 specular_color = V(mat.specular_color[0], mat.specular_color[1], mat.specular_color[2]);
+  float clearcoat = mat.clearcoat;
+  F3 sheen_color = V(mat.sheen_color[0], mat.sheen_color[1], mat.sheen_color[2]);
+  float sheen_roughness = mat.sheen_roughness;
+  float clearcoat_roughness = mat.clearcoat_roughness;
+  const F3 mesh_normal = sh.shading_normal;
+  F3 coat_tangent_normal = V(0.0f, 0.0f, 1.0f);
+  if (Textured(mat)) {
+    float st_s, st_t;
+    HitTexcoords(s, hit.instance, hit.primitive, hit.b1, hit.b2, st_s, st_t);
+    uint32_t k = mat.lookups[LOTUS_GLTF_SLOT_BASE_COLOR];
+    if (k != LOTUS_NO_LOOKUP) {
+      const Rgba v = Lookup(s, s.inputs[k - 1], st_s, st_t);
+      sh.base_color = V(saturate(v.v[0]), saturate(v.v[1]), saturate(v.v[2]));
+    }
+    sh.roughness = GltfScalar(s, mat, LOTUS_GLTF_SLOT_ROUGHNESS, st_s, st_t, sh.roughness);
+    sh.metallic = GltfScalar(s, mat, LOTUS_GLTF_SLOT_METALLIC, st_s, st_t, sh.metallic);
+    emission = GltfEmission(s, mat, st_s, st_t);
+    k = mat.lookups[LOTUS_SLOT_NORMAL];
+    if (k != LOTUS_NO_LOOKUP) tangent_normal = ClampNormal(Lookup(s, s.inputs[k - 1], st_s, st_t));
+    specular = GltfScalar(s, mat, LOTUS_GLTF_SLOT_SPECULAR, st_s, st_t, specular);
+    transmission = GltfScalar(s, mat, LOTUS_GLTF_SLOT_TRANSMISSION, st_s, st_t, transmission);
+    clearcoat = GltfScalar(s, mat, LOTUS_GLTF_SLOT_CLEARCOAT, st_s, st_t, clearcoat);
+    clearcoat_roughness = GltfScalar(s, mat, LOTUS_GLTF_SLOT_CLEARCOAT_ROUGHNESS, st_s, st_t, clearcoat_roughness);
+    sheen_roughness = GltfScalar(s, mat, LOTUS_GLTF_SLOT_SHEEN_ROUGHNESS, st_s, st_t, sheen_roughness);
+    k = mat.lookups[LOTUS_GLTF_SLOT_SPECULAR_COLOR];
+    if (k != LOTUS_NO_LOOKUP) {
+      const Rgba v = Lookup(s, s.inputs[k - 1], st_s, st_t);
+      specular_color = V(std::fmax(v.v[0], 0.0f), std::fmax(v.v[1], 0.0f), std::fmax(v.v[2], 0.0f));
+    }
+    k = mat.lookups[LOTUS_GLTF_SLOT_SHEEN_COLOR];
+    if (k != LOTUS_NO_LOOKUP) {
+      const Rgba v = Lookup(s, s.inputs[k - 1], st_s, st_t);
+      sheen_color = V(saturate(v.v[0]), saturate(v.v[1]), saturate(v.v[2]));
+    }
+    k = mat.lookups[LOTUS_GLTF_SLOT_CLEARCOAT_NORMAL];
+    if (k != LOTUS_NO_LOOKUP) coat_tangent_normal = ClampNormal(Lookup(s, s.inputs[k - 1], st_s, st_t));
+  }
+  if (tangent_normal.x != 0.0f || tangent_normal.y != 0.0f || tangent_normal.z != 1.0f) {
+    const uint32_t k = mat.lookups[LOTUS_SLOT_NORMAL];
+    sh.shading_normal = MappedNormal(tangent_normal,
+        TangentFrame(s, hit.instance, k != LOTUS_NO_LOOKUP ? &s.inputs[k - 1] : nullptr, hit.primitive, edge1,
+            edge2, sh.shading_normal),
+        sh.normal, direction);
+  }
+  const float cos_o = dot(sh.shading_normal, -direction);
+  F3 wo = V(std::sqrt(std::fmax(1.0f - cos_o * cos_o, 0.0f)), 0.0f, cos_o);
+  GltfPbrInputs inputs = MakeGltfPbrInputs(sh.base_color, sh.roughness, sh.metallic);
+  inputs.dielectric_f0 = dielectric_f0;
+  inputs.specular = specular;
+  inputs.specular_color = specular_color;
+  inputs.transmission = transmission;
+  inputs.clearcoat = clearcoat;
+  inputs.clearcoat_roughness = clearcoat_roughness;
+  inputs.sheen_color = sheen_color;
+  inputs.sheen_roughness = sheen_roughness;
+  if (clearcoat > 0.0f) {
+    F3 coat_normal = mesh_normal;
+    if (coat_tangent_normal.x != 0.0f || coat_tangent_normal.y != 0.0f || coat_tangent_normal.z != 1.0f) {
+      const uint32_t k = mat.lookups[LOTUS_GLTF_SLOT_CLEARCOAT_NORMAL];
+      coat_normal = MappedNormal(coat_tangent_normal,
+          TangentFrame(s, hit.instance, k != LOTUS_NO_LOOKUP ? &s.inputs[k - 1] : nullptr, hit.primitive,
+              edge1, edge2, mesh_normal),
+          sh.normal, direction);
+    }
+    const ShadingFrame basis = MakeShadingFrame(sh.shading_normal);
+    const F3 local = basis.ToLocal(-direction);
+    wo.x = local.x;
+    wo.y = local.y;
+    inputs.clearcoat_normal = normalize(basis.ToLocal(coat_normal));
+  }
+  sh.gltf_terms = MakeGltfPbrTerms(inputs, wo);
+  sh.composed = MakeGltfPbrClosure(sh.gltf_terms, wo);
+  sh.gltf = true;
+  sh.bsdf = MakePreviewClosure(V(0.0f), 1.0f, 0.0f, 1.5f, false, V(0.0f), 0.0f, V(1.0f), false, true);
+  sh.emission = emission;
+}
+
 SurfaceHit ReconstructHit(const oracle_scene& s, const Hit& hit, F3 direction) {
   const Instance& inst = s.instances[hit.instance];
   const Geometry& g = s.geometries[inst.geometry];
@@ -1638,6 +2504,10 @@ SurfaceHit ReconstructHit(const oracle_scene& s, const Hit& hit, F3 direction) {
     sh.shading_normal = ShadingNormal(&g.normals[3 * hit.primitive], hit.b1, hit.b2,
         inst.m, sh.normal, direction);
   const lotus_material& mat = s.materials[inst.material];
+  if (mat.model == LOTUS_MODEL_GLTF_PBR) {
+    EvaluateGltfPbr(s, hit, mat, p1 - p0, p2 - p0, direction, sh);
+    return sh;
+  }
   sh.base_color = V(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
   sh.roughness = mat.roughness;
   sh.metallic = mat.metallic;
@@ -1723,13 +2593,16 @@ LightSample SampleTriangle(const oracle_scene& s, uint32_t light, const LightRec
   const float area = TriangleArea(p0, p1, p2);
   F3 radiance;
   if (mat.lookups[LOTUS_SLOT_EMISSION] == LOTUS_NO_LOOKUP && mat.lookups[LOTUS_SLOT_OPACITY] == LOTUS_NO_LOOKUP) {
-    radiance = V(mat.emission[0], mat.emission[1], mat.emission[2]) * Coverage(s, chosen.instance, primitive, b1, b2);
+    const float strength = mat.model == LOTUS_MODEL_GLTF_PBR ? mat.emissive_strength : 1.0f;
+    const F3 e = mat.model == LOTUS_MODEL_GLTF_PBR ? V(mat.emission[0], mat.emission[1], mat.emission[2]) * strength
+                                                   : V(mat.emission[0], mat.emission[1], mat.emission[2]);
+    radiance = e * Coverage(s, chosen.instance, primitive, b1, b2);
   } else {
     // Emission(material, HitTexcoords) * Coverage(hit) at the sampled point
     // (scene.slang:655-657).
     float st_s, st_t;
     HitTexcoords(s, chosen.instance, primitive, b1, b2, st_s, st_t);
-    radiance = PreviewEmission(s, mat, st_s, st_t) * Coverage(s, chosen.instance, primitive, b1, b2);
+    radiance = Emission(s, mat, st_s, st_t) * Coverage(s, chosen.instance, primitive, b1, b2);
   }
   const F3 toward = position - origin;
   const float distance2 = dot(toward, toward);
@@ -2185,13 +3058,13 @@ F3 ShadowedLight(const oracle_scene& s, const SurfaceHit& sh, const ShadingFrame
     return V(0.0f);
   const F3 wi = basis.ToLocal(ls.direction);
   if (wi.z <= 0.0f) return V(0.0f);
-  const F3 f = PreviewEvaluate(sh.bsdf, wo, wi);
+  const F3 f = BsdfEvaluate(sh, wo, wi);
   if (MaxComponent(f) <= 0.0f) return V(0.0f);
   Ray shadow{origin, 0.0f, ls.direction, ls.distance};
   ++rays.shadow;
   const float transmittance = ShadowTransmittance(s, shadow);
   if (transmittance <= 0.0f) return V(0.0f);
-  const float weight = ls.delta ? 1.0f : PowerHeuristic(ls.pdf, PreviewPdf(sh.bsdf, wo, wi));
+  const float weight = ls.delta ? 1.0f : PowerHeuristic(ls.pdf, BsdfPdf(sh, wo, wi));
   const F3 contribution = f * ls.radiance * (transmittance * weight / ls.pdf);
   return IsFinite(contribution) ? contribution : V(0.0f);
 }
@@ -2279,7 +3152,7 @@ F3 InitialDirectLight(const oracle_scene& s, const FrameConstants& f, uint32_t p
   const F3 wi = basis.ToLocal(ls.direction);
   const float weight = ls.delta ? 1.0f
       : PowerHeuristic(ReservoirPartitionPdf(s, sel.reservoir.sample, ls, origin),
-            wi.z > 0.0f ? PreviewPdf(sh.bsdf, wo, wi) : 0.0f);
+            wi.z > 0.0f ? BsdfPdf(sh, wo, wi) : 0.0f);
   return V(sel.contribution[0], sel.contribution[1], sel.contribution[2]) * weight;
 }
 
@@ -2333,7 +3206,7 @@ bool ScatterPath(const oracle_scene& s, const FrameConstants& f, PathState& p, c
   u.y = NextRandom(p.rng);
   u.z = NextRandom(p.rng);
   BsdfSampleResult sample;
-  if (!PreviewSample(sh.bsdf, wo, u, sample)) return false;
+  if (!BsdfSample(sh, wo, u, sample)) return false;
   const F3 wi = normalize(basis.ToWorld(sample.wi));
   const float side = dot(wi, sh.normal);
   if (sample.transmitted ? side >= 0.0f : side <= 0.0f) return false;
@@ -2970,20 +3843,81 @@ float ReservoirProposalPdf(const oracle_scene& s, uint32_t proposal, uint32_t in
   return power;
 }
 
-inline F3 ReflectionEvaluate(const PreviewClosure& b, F3 wo, F3 wi) {
-  return wi.z > 0.0f ? PreviewEvaluate(b, wo, wi) : V(0.0f);
+// A stored surface's closure: its model's tag and representation
+// (BsdfClosure, bsdf.slang:26-30).
+struct StoredClosureO {
+  bool gltf = false;
+  PreviewClosure preview;
+  ComposedClosure composed;
+};
+
+// ReflectionEvaluate (restir.slang:66-72).
+inline F3 ReflectionEvaluate(const StoredClosureO& c, F3 wo, F3 wi) {
+  if (!(wi.z > 0.0f)) return V(0.0f);
+  return c.gltf ? ComposedEvaluate(c.composed, wo, wi) : PreviewEvaluate(c.preview, wo, wi);
 }
 
 // CandidateContribution (restir.slang:155-161).
 F3 CandidateContribution(const SurfaceHit& sh, const ShadingFrame& basis, F3 wo, const LightSample& ls,
     float selection) {
   if (!(ls.pdf > 0.0f) || dot(ls.direction, sh.normal) <= 0.0f) return V(0.0f);
-  return ReflectionEvaluate(sh.bsdf, wo, basis.ToLocal(ls.direction)) * ls.radiance * (selection / ls.pdf);
+  const F3 wi = basis.ToLocal(ls.direction);
+  const F3 f = wi.z > 0.0f ? BsdfEvaluate(sh, wo, wi) : V(0.0f);
+  return f * ls.radiance * (selection / ls.pdf);
 }
 
-// StoreClosure / LoadClosure (restir.slang:78-149), UsdPreviewSurface only.
-void StoreClosure(const PreviewClosure& b, RestirSurfaceO& o) {
+// PackGltfPbrTerms (gltf_pbr.slang:162-188).
+void PackGltfPbrTerms(const GltfPbrTerms& g, float lanes[22]) {
+  lanes[0] = g.base_color.x; lanes[1] = g.base_color.y; lanes[2] = g.base_color.z;
+  lanes[3] = g.alpha; lanes[4] = g.metallic; lanes[5] = g.e1; lanes[6] = g.share;
+  lanes[7] = g.f0.x; lanes[8] = g.f0.y; lanes[9] = g.f0.z; lanes[10] = g.f90;
+  lanes[11] = g.transmission; lanes[12] = g.coat_scale; lanes[13] = g.coat_dim; lanes[14] = g.coat_alpha;
+  lanes[15] = g.coat_normal.x; lanes[16] = g.coat_normal.y;
+  lanes[17] = g.sheen_color.x; lanes[18] = g.sheen_color.y; lanes[19] = g.sheen_color.z;
+  lanes[20] = g.sheen_roughness; lanes[21] = g.sheen_dim;
+}
+
+// UnpackGltfPbrTerms (gltf_pbr.slang:190-214).
+GltfPbrTerms UnpackGltfPbrTerms(const float lanes[22]) {
+  GltfPbrTerms g;
+  g.base_color = V(lanes[0], lanes[1], lanes[2]);
+  g.alpha = lanes[3];
+  g.metallic = lanes[4];
+  g.e1 = lanes[5];
+  g.share = lanes[6];
+  g.f0 = V(lanes[7], lanes[8], lanes[9]);
+  g.f90 = lanes[10];
+  g.transmission = lanes[11];
+  g.coat_scale = lanes[12];
+  g.coat_dim = lanes[13];
+  g.coat_alpha = lanes[14];
+  const float tx = lanes[15], ty = lanes[16];
+  g.coat_normal = V(tx, ty, std::sqrt(std::fmax(1.0f - (tx * tx + ty * ty), 0.0f)));
+  g.sheen_color = V(lanes[17], lanes[18], lanes[19]);
+  g.sheen_roughness = lanes[20];
+  g.sheen_dim = lanes[21];
+  return g;
+}
+
+// StoreClosure / LoadClosure (restir.slang:78-149).
+void StoreClosure(const SurfaceHit& sh, RestirSurfaceO& o) {
   for (int k = 0; k < 4; ++k) o.model[k] = o.extension[k] = 0.0f;
+  if (sh.gltf) {
+    float lanes[22];
+    PackGltfPbrTerms(sh.gltf_terms, lanes);
+    o.model[0] = 1.0f;
+    o.base_alpha[0] = lanes[0]; o.base_alpha[1] = lanes[1]; o.base_alpha[2] = lanes[2]; o.base_alpha[3] = lanes[3];
+    o.dielectric_metallic[0] = lanes[7]; o.dielectric_metallic[1] = lanes[8];
+    o.dielectric_metallic[2] = lanes[9]; o.dielectric_metallic[3] = lanes[4];
+    o.model[1] = lanes[5]; o.model[2] = lanes[6]; o.model[3] = lanes[10];
+    o.normal[3] = lanes[11];
+    o.shading_normal[3] = lanes[12];
+    o.outgoing[3] = lanes[13];
+    o.fresnel[0] = lanes[14]; o.fresnel[1] = lanes[15]; o.fresnel[2] = lanes[16]; o.fresnel[3] = lanes[20];
+    o.extension[0] = lanes[17]; o.extension[1] = lanes[18]; o.extension[2] = lanes[19]; o.extension[3] = lanes[21];
+    return;
+  }
+  const PreviewClosure& b = sh.bsdf;
   o.normal[3] = b.dielectric_f90;
   o.shading_normal[3] = b.thin_walled ? -b.transmission : b.transmission;
   o.outgoing[3] = b.smooth ? -b.eta : b.eta;
@@ -2994,8 +3928,27 @@ void StoreClosure(const PreviewClosure& b, RestirSurfaceO& o) {
   o.fresnel[0] = b.f0.x; o.fresnel[1] = b.f0.y; o.fresnel[2] = b.f0.z; o.fresnel[3] = b.f90;
 }
 
-PreviewClosure LoadClosure(const RestirSurfaceO& o) {
-  PreviewClosure b;
+StoredClosureO LoadClosure(const RestirSurfaceO& o) {
+  StoredClosureO c;
+  if ((uint32_t)o.model[0] == 1u) {
+    float lanes[22];
+    lanes[0] = o.base_alpha[0]; lanes[1] = o.base_alpha[1]; lanes[2] = o.base_alpha[2]; lanes[3] = o.base_alpha[3];
+    lanes[4] = o.dielectric_metallic[3];
+    lanes[5] = o.model[1]; lanes[6] = o.model[2];
+    lanes[7] = o.dielectric_metallic[0]; lanes[8] = o.dielectric_metallic[1]; lanes[9] = o.dielectric_metallic[2];
+    lanes[10] = o.model[3];
+    lanes[11] = o.normal[3];
+    lanes[12] = o.shading_normal[3];
+    lanes[13] = o.outgoing[3];
+    lanes[14] = o.fresnel[0]; lanes[15] = o.fresnel[1]; lanes[16] = o.fresnel[2];
+    lanes[17] = o.extension[0]; lanes[18] = o.extension[1]; lanes[19] = o.extension[2];
+    lanes[20] = o.fresnel[3];
+    lanes[21] = o.extension[3];
+    c.gltf = true;
+    c.composed = MakeGltfPbrClosure(UnpackGltfPbrTerms(lanes), V(o.outgoing[0], o.outgoing[1], o.outgoing[2]));
+    return c;
+  }
+  PreviewClosure& b = c.preview;
   b.base_color = V(o.base_alpha[0], o.base_alpha[1], o.base_alpha[2]);
   b.alpha = o.base_alpha[3];
   b.metallic = o.dielectric_metallic[3];
@@ -3008,15 +3961,15 @@ PreviewClosure LoadClosure(const RestirSurfaceO& o) {
   b.eta = std::fabs(o.outgoing[3]);
   b.thin_walled = o.shading_normal[3] < 0.0f;
   b.smooth = o.outgoing[3] < 0.0f;
-  return b;
+  return c;
 }
 
 inline F3 Xyz(const float* v) { return V(v[0], v[1], v[2]); }
 
 // HistoryContribution (restir.slang:256-268).
 F3 HistoryContribution(const oracle_scene& s, const RestirSurfaceO& src, uint32_t light, const LightSample& ls) {
-  const PreviewClosure b = LoadClosure(src);
   if (!(ls.pdf > 0.0f) || dot(ls.direction, Xyz(src.normal)) <= 0.0f) return V(0.0f);
+  const StoredClosureO b = LoadClosure(src);
   const ShadingFrame basis = MakeShadingFrame(Xyz(src.shading_normal));
   return ReflectionEvaluate(b, Xyz(src.outgoing), basis.ToLocal(ls.direction)) * ls.radiance *
       (s.lights[light].pdf / ls.pdf);
@@ -3143,7 +4096,7 @@ void TemporalReservoir(const oracle_scene& s, const FrameConstants& f, const ora
   receiver.shading_normal[0] = sh.shading_normal.x; receiver.shading_normal[1] = sh.shading_normal.y;
   receiver.shading_normal[2] = sh.shading_normal.z;
   receiver.outgoing[0] = wo.x; receiver.outgoing[1] = wo.y; receiver.outgoing[2] = wo.z;
-  StoreClosure(sh.bsdf, receiver);
+  StoreClosure(sh, receiver);
   receiver.instance_id = ids[hit.instance].instance_id;
   receiver.material_id = ids[hit.instance].material_id;
   const ValidityO v = validity[slot];
