@@ -172,17 +172,38 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
   std::vector<lotus_material> mats(std::max<size_t>(materials_.size(), 1));
   for (size_t i = 0; i < materials_.size(); ++i) {
     const Lotus::SceneMaterial& sm = materials_[i];
-    if (!std::holds_alternative<Lotus::PreviewSurface>(sm.material.surface))
-      return fail("material " + std::to_string(i) + ": only UsdPreviewSurface is built");
-    const Lotus::PreviewSurface& p = Lotus::Preview(sm.material);
+    const auto* preview = std::get_if<Lotus::PreviewSurface>(&sm.material.surface);
+    const auto* gltf = std::get_if<Lotus::GltfPbr>(&sm.material.surface);
+    if (!preview && !gltf)
+      return fail("material " + std::to_string(i) + ": only UsdPreviewSurface and glTF PBR are built");
     lotus_material& m = mats[i];
-    // Each texture-input slot (material.hpp:266-273) with its resolved
+    // Each texture-input slot (material.hpp:262-312) with its resolved
     // image (SceneMaterial::textures; none: the lookup's fallback).
-    const std::optional<Lotus::TextureInput>* slots[LOTUS_TEXTURE_SLOTS] = {&sm.material.geometry.opacity_texture,
-        &sm.material.geometry.normal_texture, &p.base_color_texture, &p.roughness_texture, &p.metallic_texture,
-        &p.emission_texture, &p.specular_color_texture};
+    const std::optional<Lotus::TextureInput>* slots[LOTUS_TEXTURE_SLOTS] = {};
+    slots[LOTUS_SLOT_OPACITY] = &sm.material.geometry.opacity_texture;
+    slots[LOTUS_SLOT_NORMAL] = &sm.material.geometry.normal_texture;
+    if (preview) {
+      slots[LOTUS_SLOT_BASE_COLOR] = &preview->base_color_texture;
+      slots[LOTUS_SLOT_ROUGHNESS] = &preview->roughness_texture;
+      slots[LOTUS_SLOT_METALLIC] = &preview->metallic_texture;
+      slots[LOTUS_SLOT_EMISSION] = &preview->emission_texture;
+      slots[LOTUS_SLOT_SPECULAR_COLOR] = &preview->specular_color_texture;
+    } else {
+      slots[LOTUS_GLTF_SLOT_BASE_COLOR] = &gltf->base_color.texture;
+      slots[LOTUS_GLTF_SLOT_METALLIC] = &gltf->metallic.texture;
+      slots[LOTUS_GLTF_SLOT_ROUGHNESS] = &gltf->roughness.texture;
+      slots[LOTUS_GLTF_SLOT_EMISSIVE] = &gltf->emissive.texture;
+      slots[LOTUS_GLTF_SLOT_SPECULAR] = &gltf->specular.texture;
+      slots[LOTUS_GLTF_SLOT_SPECULAR_COLOR] = &gltf->specular_color.texture;
+      slots[LOTUS_GLTF_SLOT_TRANSMISSION] = &gltf->transmission.texture;
+      slots[LOTUS_GLTF_SLOT_CLEARCOAT] = &gltf->clearcoat.texture;
+      slots[LOTUS_GLTF_SLOT_CLEARCOAT_ROUGHNESS] = &gltf->clearcoat_roughness.texture;
+      slots[LOTUS_GLTF_SLOT_CLEARCOAT_NORMAL] = &gltf->clearcoat_normal_texture;
+      slots[LOTUS_GLTF_SLOT_SHEEN_COLOR] = &gltf->sheen_color.texture;
+      slots[LOTUS_GLTF_SLOT_SHEEN_ROUGHNESS] = &gltf->sheen_roughness.texture;
+    }
     for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k) {
-      if (!*slots[k]) continue;
+      if (!slots[k] || !*slots[k]) continue;
       const Lotus::TextureInput& in = **slots[k];
       lotus_texture_input d{};
       const Lotus::Texture* image = k < sm.textures.size() ? sm.textures[k] : nullptr;
@@ -200,6 +221,26 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
     }
     std::memcpy(m.texcoord_fallback, sm.material.geometry.texcoord_fallback.data(), 8);
     std::memcpy(m.normal, sm.material.geometry.normal.data(), 12);
+    m.opacity = sm.material.geometry.opacity;
+    m.opacity_threshold = sm.material.geometry.opacity_threshold;
+    if (gltf) {
+      m.model = LOTUS_MODEL_GLTF_PBR;
+      std::memcpy(m.base_color, gltf->base_color.value.data(), 12);
+      m.metallic = gltf->metallic.value;
+      m.roughness = gltf->roughness.value;
+      std::memcpy(m.emission, gltf->emissive.value.data(), 12);
+      m.emissive_strength = gltf->emissive_strength;
+      m.ior = gltf->ior;
+      m.specular = gltf->specular.value;
+      std::memcpy(m.specular_color, gltf->specular_color.value.data(), 12);
+      m.transmission = gltf->transmission.value;
+      m.clearcoat = gltf->clearcoat.value;
+      m.clearcoat_roughness = gltf->clearcoat_roughness.value;
+      std::memcpy(m.sheen_color, gltf->sheen_color.value.data(), 12);
+      m.sheen_roughness = gltf->sheen_roughness.value;
+      continue;
+    }
+    const Lotus::PreviewSurface& p = *preview;
     std::memcpy(m.base_color, p.base_color.data(), 12);
     m.roughness = p.roughness;
     std::memcpy(m.emission, p.emission.data(), 12);
@@ -208,8 +249,6 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
     m.ior = p.ior;
     std::memcpy(m.transmission_color, p.transmission_color.data(), 12);
     m.transmission = p.transmission;
-    m.opacity = sm.material.geometry.opacity;
-    m.opacity_threshold = sm.material.geometry.opacity_threshold;
     m.flags = (p.use_specular_workflow ? LOTUS_MATERIAL_SPECULAR_WORKFLOW : 0u) |
               (p.thin_walled ? LOTUS_MATERIAL_THIN_WALLED : 0u);
   }
@@ -664,6 +703,26 @@ Lotus::GpuSceneContents CudaOffscreenRenderer::ReadBackScene() {
   const auto* mats = reinterpret_cast<const lotus_material*>(mat_bytes.data());
   for (size_t i = 0; i < mat_bytes.size() / sizeof(lotus_material); ++i) {
     Lotus::GpuMaterialContents mc;
+    mc.material.geometry.opacity = mats[i].opacity;
+    mc.material.geometry.opacity_threshold = mats[i].opacity_threshold;
+    if (mats[i].model == LOTUS_MODEL_GLTF_PBR) {
+      Lotus::GltfPbr& g = mc.material.surface.emplace<Lotus::GltfPbr>();
+      std::memcpy(g.base_color.value.data(), mats[i].base_color, 12);
+      g.metallic.value = mats[i].metallic;
+      g.roughness.value = mats[i].roughness;
+      std::memcpy(g.emissive.value.data(), mats[i].emission, 12);
+      g.emissive_strength = mats[i].emissive_strength;
+      g.ior = mats[i].ior;
+      g.specular.value = mats[i].specular;
+      std::memcpy(g.specular_color.value.data(), mats[i].specular_color, 12);
+      g.transmission.value = mats[i].transmission;
+      g.clearcoat.value = mats[i].clearcoat;
+      g.clearcoat_roughness.value = mats[i].clearcoat_roughness;
+      std::memcpy(g.sheen_color.value.data(), mats[i].sheen_color, 12);
+      g.sheen_roughness.value = mats[i].sheen_roughness;
+      c.materials.push_back(mc);
+      continue;
+    }
     Lotus::PreviewSurface& p = Lotus::Preview(mc.material);
     std::memcpy(p.base_color.data(), mats[i].base_color, 12);
     p.roughness = mats[i].roughness;
@@ -675,8 +734,6 @@ Lotus::GpuSceneContents CudaOffscreenRenderer::ReadBackScene() {
     p.transmission = mats[i].transmission;
     p.use_specular_workflow = (mats[i].flags & LOTUS_MATERIAL_SPECULAR_WORKFLOW) != 0;
     p.thin_walled = (mats[i].flags & LOTUS_MATERIAL_THIN_WALLED) != 0;
-    mc.material.geometry.opacity = mats[i].opacity;
-    mc.material.geometry.opacity_threshold = mats[i].opacity_threshold;
     c.materials.push_back(mc);
   }
   if (!read(LOTUS_SCENE_ENVIRONMENT, 0, bytes) || bytes.size() != 12) return fail("scene readback: environment");

@@ -9,7 +9,8 @@
 //
 // What maps where:
 //   UpdateScene(SceneUpdate)  resident geometry, instances, UsdPreviewSurface
-//                             materials and the environment, rebuilt into one
+//                             and glTF PBR materials and the environment,
+//                             rebuilt into one
 //                             lotus_scene_desc -> lotus_cuda_update_scene
 //   RenderScene(...)          lotus_cuda_render (Radiance output)
 //   RenderTemporalScene(...)  lotus_cuda_render_temporal with the snapshot's
@@ -24,13 +25,12 @@
 //                             backend does not build
 //   Residency()               the resident scene's device bytes
 // Analytic lights (Lotus::Light) map field for field to lotus_light; the
-// resident textures to lotus_texture, UsdPreviewSurface's texture inputs
-// (opacity, normal, base colour, roughness, metallic, emission, specular
-// colour) to lotus_texture_input, each geometry's texture-coordinate sets
-// in key order and each instance's set. Scene content the backend does not
-// build (material models other than UsdPreviewSurface, vertex colours)
-// makes UpdateScene Fail with the reason, as the reference Fails on
-// unsupported content.
+// resident textures to lotus_texture, each model's texture inputs in the
+// reference's slot numbering (material.hpp:262-312) to lotus_texture_input,
+// each geometry's texture-coordinate sets in key order and each instance's
+// set. Scene content the backend does not build (the reserved Standard
+// Surface and OpenPBR models, vertex colours) makes UpdateScene Fail with
+// the reason, as the reference Fails on unsupported content.
 #pragma once
 
 #include <lotus/vulkan_backend.hpp>

@@ -2057,3 +2057,96 @@ def material_gltf(exchanged_channels=False, size=160):
         s.add_instance(geo, s.add_material(m), placed,
                        texcoord_set=1 if uses_st and geo in s.texcoords else 0)
     return s
+
+
+def material_gltf_extensions(exchanged_coat=False, size=160):
+    """The reference's material-gltf-extensions-v1 fixture
+    (SetMaterialGltfExtensions, material_fixtures.cpp:2063-2272 in
+    hydra-lotus), which its golden images validation/reference/
+    material-gltf-extensions-v1-{mean,variance}.pfm were rendered from:
+    glTF PBR's extensions on the 5x5 grid in the material studio. Rows from
+    the top: the dielectric's reflection (ior 1 and 2.4, half specular, a
+    tinted and a mapped specular); thin transmission on cards; clearcoat
+    (over a rough red dielectric and copper, rough, over a normal-mapped
+    base, with its own normal map); sheen over a dark rough dielectric;
+    every extension together, mapped coat and specular colour, and inputs
+    the model does not represent. Spheres are wrapped in (s, t) where a
+    lookup reads. ``exchanged_coat`` swaps CoatRough's clearcoat weight and
+    roughness (the fixture's negative control, ExchangedCoat)."""
+    s = material_studio("material-gltf-extensions-v1", size)
+    palette_tex = s.add_texture(_texture_image(4, _palette), abi.TEXTURE_RGBA8_SRGB)
+    rgba_tex = s.add_texture(_texture_image(4, _rgba), abi.TEXTURE_RGBA8_UNORM)
+    tilts_tex = s.add_texture(_texture_image(4, _tilts), abi.TEXTURE_RGBA8_UNORM)
+    rep = abi.WRAP_REPEAT
+    transparent = (0.0, 0.0, 0.0, 0.0)
+    copper, red, teal = (0.95, 0.64, 0.54), (0.8, 0.2, 0.1), (0.2, 0.6, 0.7)
+    dark, white = (0.05, 0.05, 0.08), (1.0, 1.0, 1.0)
+
+    def periodic(texture, **kw):
+        return s.add_texture_input(texture, wrap_s=rep, wrap_t=rep, **kw)
+
+    palette = periodic(palette_tex, fallback=transparent)
+
+    def scalars(channel):
+        return periodic(rgba_tex, fallback=transparent, channel=channel)
+
+    bumps = periodic(tilts_tex, scale=(2.0, 2.0, 2.0, 1.0), bias=(-1.0, -1.0, -1.0, 0.0),
+                     fallback=(0.0, 0.0, 1.0, 1.0))
+    looks = []
+
+    def add(name, base, metallic, roughness, textured=False, **kw):
+        m = gltf_material(base, metallic, roughness, **kw)
+        looks.append((name, m, textured))
+        return m
+
+    # The dielectric's reflection.
+    add("IorOne", red, 0.0, 0.2, ior=1.0)
+    add("IorHigh", red, 0.0, 0.2, ior=2.4)
+    add("SpecularHalf", red, 0.0, 0.2, specular=0.5)
+    add("SpecularTint", (0.6, 0.6, 0.6), 0.0, 0.2, ior=2.4, specular_color=(1.0, 0.3, 0.1))
+    add("SpecularMap", red, 0.0, 0.2, True, ior=2.4).lookups[abi.GLTF_SLOT_SPECULAR] = scalars(0)
+    # Transmission.
+    add("Glass", white, 0.0, 0.0, transmission=1.0)
+    add("GlassRough", white, 0.0, 0.4, transmission=1.0)
+    add("GlassTinted", teal, 0.0, 0.0, transmission=1.0)
+    add("GlassHalf", (0.9, 0.6, 0.2), 0.0, 0.3, transmission=0.5)
+    add("GlassMap", white, 0.0, 0.1, True).lookups[abi.GLTF_SLOT_TRANSMISSION] = scalars(1)
+    # Clearcoat.
+    add("Coat", red, 0.0, 0.7, clearcoat=1.0)
+    add("CoatMetal", copper, 1.0, 0.4, clearcoat=0.5)
+    add("CoatRough", red, 0.0, 0.7, clearcoat=0.5 if exchanged_coat else 1.0,
+        clearcoat_roughness=1.0 if exchanged_coat else 0.5)
+    add("CoatOverBumps", red, 0.0, 0.7, True, clearcoat=1.0).lookups[abi.SLOT_NORMAL] = bumps
+    add("CoatNormal", red, 0.0, 0.7, True, clearcoat=1.0).lookups[abi.GLTF_SLOT_CLEARCOAT_NORMAL] = bumps
+    # Sheen.
+    add("Sheen", dark, 0.0, 0.8, sheen_color=white, sheen_roughness=0.7)
+    add("SheenColor", dark, 0.0, 0.8, sheen_color=(0.9, 0.4, 0.1), sheen_roughness=0.5)
+    add("SheenRough", dark, 0.0, 0.8, sheen_color=(0.5, 0.5, 0.5), sheen_roughness=1.0)
+    sheen_map = add("SheenMap", dark, 0.0, 0.8, True)
+    sheen_map.lookups[abi.GLTF_SLOT_SHEEN_COLOR] = palette
+    sheen_map.lookups[abi.GLTF_SLOT_SHEEN_ROUGHNESS] = scalars(1)
+    add("SheenCoat", dark, 0.0, 0.8, sheen_color=(0.9, 0.4, 0.1), sheen_roughness=0.5, clearcoat=1.0)
+    # Together, mapped weights, and unrepresented inputs.
+    add("All", (0.9, 0.6, 0.2), 0.3, 0.4, ior=1.8, specular=0.8, specular_color=(1.0, 0.8, 0.6),
+        transmission=0.4, clearcoat=0.7, clearcoat_roughness=0.2, sheen_color=(0.3, 0.5, 0.8),
+        sheen_roughness=0.6)
+    coat_map = add("CoatMap", red, 0.0, 0.7, True)
+    coat_map.lookups[abi.GLTF_SLOT_CLEARCOAT] = scalars(0)
+    coat_map.lookups[abi.GLTF_SLOT_CLEARCOAT_ROUGHNESS] = scalars(2)
+    add("SpecularColorMap", (0.6, 0.6, 0.6), 0.0, 0.2, True, ior=2.4).lookups[
+        abi.GLTF_SLOT_SPECULAR_COLOR] = palette
+    add("Thickness", teal, 0.0, 0.0, transmission=1.0)
+    add("Diagnosed", red, 0.0, 0.7, clearcoat=1.0)
+
+    smooth = _coarse_smooth_sphere(s)
+    wrapped = _wrapped_sphere(s)
+    card = _unit_card(s)
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (1.6, 0.8, 0.0, -0.8, -1.6)
+    for i, (name, m, textured) in enumerate(looks):
+        is_card = name.startswith("Glass") or name == "Thickness"
+        geo = card if is_card else (wrapped if textured else smooth)
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = placed[5] = placed[10] = 0.7 if is_card else 0.35
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        s.add_instance(geo, s.add_material(m), placed, texcoord_set=1 if textured else 0)
+    return s

@@ -61,9 +61,11 @@ def golden_normals():
 
 @pytest.fixture(scope="session")
 def golden_fixtures():
-    """The reference's material-transmission-v1, material-transforms-v1 and
-    material-emission-v1 golden images (4096 spp), by fixture name."""
-    return {name: load_golden(f"material_{name}_v1.npz") for name in ("transmission", "transforms", "emission")}
+    """The reference's material-transmission-v1, material-transforms-v1,
+    material-emission-v1, material-gltf-v1 and material-gltf-extensions-v1
+    golden images (4096 spp), by fixture name."""
+    return {name: load_golden(f"material_{name}_v1.npz")
+            for name in ("transmission", "transforms", "emission", "gltf", "gltf_extensions")}
 
 
 @pytest.fixture(scope="session")

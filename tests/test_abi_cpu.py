@@ -26,7 +26,7 @@ def test_library_exports_every_declared_function():
 
 def test_version_and_struct_sizes():
     lib = renderer.lib()
-    assert lib.lotus_cuda_abi_version() == abi.ABI_VERSION == 9
+    assert lib.lotus_cuda_abi_version() == abi.ABI_VERSION == 10
     sizes = abi.check_struct_sizes(lib)
     assert len(sizes) == len(abi.STRUCTS)
 

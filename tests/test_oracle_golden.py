@@ -29,6 +29,14 @@ reference's DES-Q5 comparison, and each fixture's negative control.
   every textured input; the tinted sphere's colour dropped
   (UntintedGlass) and the rotation reversed (ReversedRotation) must be
   rejected.
+- validation/reference/material-gltf-v1 and material-gltf-extensions-v1
+  (4096 spp): MaterialX's glTF PBR surface through the composed closure
+  and its albedo tables (constants, images, packed channels, placements,
+  normal maps, emission, alpha modes; ior, specular, thin transmission,
+  clearcoat with its own normal, sheen, everything together), at 16, 256
+  and 1024 spp; Packed's metallic and roughness read from exchanged
+  channels (ExchangedChannels) and CoatRough's weight and roughness
+  exchanged (ExchangedCoat) must be rejected.
 
 Both were written by the reference's GPU renderer; fixtures in tests/golden.
 """
@@ -128,12 +136,14 @@ def test_oracle_material_normals_negative_control_rejected(oracle_lib, golden_no
 
 
 NEGATIVE = {"transmission": {"untinted": True}, "transforms": {"reversed_rotation": True},
-            "emission": {"raw_emission": True}}
+            "emission": {"raw_emission": True}, "gltf": {"exchanged_channels": True},
+            "gltf_extensions": {"exchanged_coat": True}}
 # material-emission-v1 at 256 spp: one 8x8 tile of the unlit card (pure
 # emission from the sRGB palette, so the golden's variance is the pixel
 # jitter's alone) sits 0.25% above the reference's, 6.3 standard errors;
 # every other tile and the 16-spp level pass.
-LEVELS = {"transmission": (16, 256), "transforms": (16, 256), "emission": (16,)}
+LEVELS = {"transmission": (16, 256), "transforms": (16, 256), "emission": (16,), "gltf": (16, 256, 1024),
+          "gltf_extensions": (16, 256, 1024)}
 
 
 @pytest.mark.parametrize("name,spp", [(n, s) for n in sorted(NEGATIVE) for s in LEVELS[n]])
