@@ -560,6 +560,38 @@ def analytic_lights_report(renderer_module, frames=64, warmup=8):
     return out
 
 
+def gltf_cost_report(renderer_module, size=1024, frames=64, warmup=8):
+    """What the glTF PBR closure costs beside UsdPreviewSurface's on one
+    scene: the reference's cornell-v1 and cornell-gltf-v1 benchmark
+    workloads (the Cornell box, then with every material glTF PBR) at
+    size^2, one sample per frame, 64 bounces, BSDF sampling (the reference
+    benchmark's defaults): the median device milliseconds per frame under
+    each integrator, beside the reference's published figures."""
+    out = {"workload": f"cornell-v1 and cornell-gltf-v1, {size}x{size}, 1 spp per frame, 64 bounces, "
+                       "BSDF sampling", "unit": "ms per frame (device)"}
+    with renderer_module.CudaOffscreenRenderer(0) as r:
+        for name, integrator in (("reference", abi.INTEGRATOR_REFERENCE), ("wavefront", abi.INTEGRATOR_WAVEFRONT)):
+            st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_BSDF,
+                                      max_bounces=64, sample_index=0)
+            for workload, scene in (("cornell-v1", scenes.cornell_reference(size=size)),
+                                    ("cornell-gltf-v1", scenes.cornell_gltf(size=size))):
+                renderer_module.check(r.update_scene(scene), "update_scene")
+                ms = []
+                for k in range(warmup + frames):
+                    st.sample_index = k
+                    res, _ = r.render_scene(scene.frame(st, 1, read_back=False))
+                    renderer_module.check(res, workload)
+                    if k >= warmup:
+                        ms.append(res.gpu_ms)
+                out[f"{name}_{workload}"] = round(statistics.median(ms), 4)
+            out[f"{name}_ratio"] = round(out[f"{name}_cornell-gltf-v1"] / out[f"{name}_cornell-v1"], 3)
+    out["reference_published"] = {
+        "hardware": "the reference's development workstation (Vulkan ray query, unlocked clocks), 1024^2",
+        "reference_cornell-v1": 1.62, "reference_cornell-gltf-v1": 3.85,
+        "wavefront_cornell-v1": 2.21, "wavefront_cornell-gltf-v1": 3.63}
+    return out
+
+
 def batch_report(renderer_module, spp=8, depth=8):
     """Config 4: the 64-scene batch workload (scenes.batch_workload: traced
     triangles log-uniform in [1e4, 2e6], 256^2 .. 1024^2 targets), 8 spp,
@@ -810,6 +842,7 @@ def main():
             line["cache_kernels"] = cache_kernels_report(renderer)
         if args.lights:
             line["analytic_lights"] = analytic_lights_report(renderer)
+            line["gltf_cost"] = gltf_cost_report(renderer)
         # Last, so that a reader of the line's tail sees it.
         if convergence_report:
             line["time_to_relmse"] = time_to_relmse_summary(convergence_report)

@@ -487,6 +487,21 @@ def cornell_reference(red_scale=1.0, size=128):
     return s
 
 
+def cornell_gltf(size=128):
+    """The reference's cornell-gltf-v1 benchmark workload (MakeWorkload,
+    adapters/common/workloads.cpp:104-122 in hydra-lotus): the Cornell box
+    with every material MaterialX's glTF PBR of the same base colour,
+    roughness, metallic and emission, the rest at the definition's
+    defaults."""
+    s = cornell_reference(size=size)
+    s.name = "cornell-gltf"
+    for k, m in enumerate(s.materials):
+        s.materials[k] = gltf_material(tuple(m.base_color), metallic=m.metallic, roughness=m.roughness,
+                                       emissive=tuple(m.emission))
+    s._desc = None
+    return s
+
+
 def box_room(seed=0, size=256):
     """The seeded box room: 10 wall triangles (floor, ceiling, back, left,
     right; open front), two boxes of 12 triangles with a y-rotation in
