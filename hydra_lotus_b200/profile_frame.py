@@ -17,7 +17,11 @@ from . import abi, renderer, scenes
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="sphere-field", choices=["sphere-field", "box-room"])
+    ap.add_argument("--workload", default="sphere-field",
+                    choices=["sphere-field", "box-room", "cornell", "cornell-gltf"],
+                    help="cornell and cornell-gltf: the reference's cornell-v1 and cornell-gltf-v1 workloads "
+                         "(square, --height pixels a side)")
+    ap.add_argument("--light-sampling", default="mis", choices=["mis", "bsdf"])
     ap.add_argument("--width", type=int, default=960)
     ap.add_argument("--height", type=int, default=540)
     ap.add_argument("--spp", type=int, default=1)
@@ -96,15 +100,20 @@ def main():
         return
     if args.workload == "sphere-field":
         scene = scenes.sphere_field(seed=0, width=args.width, height=args.height)
+    elif args.workload == "cornell":
+        scene = scenes.cornell_reference(size=args.height)
+    elif args.workload == "cornell-gltf":
+        scene = scenes.cornell_gltf(size=args.height)
     else:
         scene = scenes.box_room_wide(seed=0, width=args.width, height=args.height)
+    light_sampling = abi.LIGHT_SAMPLING_MIS if args.light_sampling == "mis" else abi.LIGHT_SAMPLING_BSDF
     integrator = abi.INTEGRATOR_WAVEFRONT if args.integrator == "wavefront" else abi.INTEGRATOR_REFERENCE
     with renderer.CudaOffscreenRenderer(0, wavefront_rounds=args.rounds) as r:
         renderer.check(r.update_scene(scene), "update_scene")
         if args.cache:
             r.configure_cache(enable=True, seed=1)
         for k in range(args.frames):
-            st = abi.default_settings(integrator=integrator, light_sampling=abi.LIGHT_SAMPLING_MIS,
+            st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,
                                       max_bounces=args.depth, sample_index=k * args.spp)
             res, _ = r.render_scene(scene.frame(st, frame_count=args.spp, read_back=False))
             renderer.check(res, "render")
