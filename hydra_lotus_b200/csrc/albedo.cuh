@@ -179,6 +179,33 @@ LOTUS_HD float ggx(const float* __restrict__ t, float cos_theta, float alpha) {
       alpha_coordinate(alpha), false);
 }
 
+// E1 and Eschlick at one (cosine, alpha): the two tables share their grid,
+// so one pass computes the coordinates, weights and node indices once and
+// reads both. Each value equals the one-table lookup's bit for bit.
+LOTUS_HD void ggx_and_share(const float* __restrict__ t, float cos_theta, float alpha, float& e1,
+    float& share) {
+  constexpr uint32_t n_cos = kGgxCosines;
+  const float fc = unit_clamp(cosine_coordinate(cos_theta)) * (float)(n_cos - 1);
+  const float fa = unit_clamp(alpha_coordinate(alpha)) * (float)(kAlphas - 1);
+  const uint32_t ic = (uint32_t)fc, ia = (uint32_t)fa;
+  const int c0 = (int)(ic < n_cos - 2 ? ic : n_cos - 2);
+  const int a0 = (int)(ia < kAlphas - 2 ? ia : kAlphas - 2);
+  const Cubic wc = cubic_weights(fc - (float)c0);
+  const Cubic wa = cubic_weights(fa - (float)a0);
+  float v0 = 0.0f, v1 = 0.0f;
+  for (int j = 0; j < 4; ++j) {
+    float r0 = 0.0f, r1 = 0.0f;
+    for (int i = 0; i < 4; ++i) {
+      r0 += wc.w[i] * fetch_node(t, offset(kGgx), (int)n_cos, c0 + i - 1, a0 + j - 1, 0, (int)n_cos - 1);
+      r1 += wc.w[i] * fetch_node(t, offset(kSchlickShare), (int)n_cos, c0 + i - 1, a0 + j - 1, 0, (int)n_cos - 1);
+    }
+    v0 += wa.w[j] * r0;
+    v1 += wa.w[j] * r1;
+  }
+  e1 = v0;
+  share = v1;
+}
+
 // Eschlick: the albedo per unit (f90 - f0) of Schlick's Fresnel.
 LOTUS_HD float schlick_share(const float* __restrict__ t, float cos_theta, float alpha) {
   return fetch_slice(t, offset(kSchlickShare), kGgxCosines, cosine_coordinate(cos_theta),

@@ -77,10 +77,7 @@ __device__ __forceinline__ GltfTerms make_gltf_terms(const GltfInputs& in, F3 wo
   t.metallic = in.metallic;
   t.e1 = 0.0f;
   t.share = 0.0f;
-  if (wo.z > 0.0f) {
-    t.e1 = albedo::ggx(tables, wo.z, t.alpha);
-    t.share = albedo::schlick_share(tables, wo.z, t.alpha);
-  }
+  if (wo.z > 0.0f) albedo::ggx_and_share(tables, wo.z, t.alpha, t.e1, t.share);
   const F3 tinted = in.specular_color * in.dielectric_f0;
   t.f0 = V(saturate(tinted.x), saturate(tinted.y), saturate(tinted.z)) * in.specular;
   t.f90 = in.specular;

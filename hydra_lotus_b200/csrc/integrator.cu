@@ -357,12 +357,19 @@ __device__ __forceinline__ double4 add4(double4 a, float4 s) {
   return make_double4(a.x + (double)s.x, a.y + (double)s.y, a.z + (double)s.z, a.w + (double)s.w);
 }
 
+// Resident blocks a SM of the per-thread path loops (the reference
+// integrator, the tail kernel): four (at most 128 registers a thread)
+// without analytic lights or full shading, else three (at most 168). The
+// full-shading instantiations would otherwise take over 220 registers and
+// keep a third of the warps resident.
+constexpr int path_loop_blocks(bool analytic, bool full_shading) { return analytic || full_shading ? 3 : 4; }
+
 // ---------------------------------------------------------------------------
 // The reference integrator: one thread follows one camera path to its end
 // (path_trace.slang:279-287, 353-385), then adds it to the pixel's FP64
 // accumulation and writes the mean.
 template <bool kCount, bool kAnalytic, bool kFullShading>
-__global__ void __launch_bounds__(kBlock) k_reference_pt(SceneView S,
+__global__ void __launch_bounds__(kBlock, path_loop_blocks(kAnalytic, kFullShading)) k_reference_pt(SceneView S,
     const FrameConst* __restrict__ fcp, double4* __restrict__ accum, float4* __restrict__ color,
     RayTotals* totals, VisitCounters* visits) {
   TraversalCounters vc[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -963,7 +970,7 @@ __global__ void __launch_bounds__(kBlock) k_wf_resolve(SceneView S,
 // Threads take paths from `cursor` one at a time. Long paths then cost one
 // launch instead of three per bounce.
 template <bool kBatch, bool kAnalytic, bool kFullShading>
-__global__ void __launch_bounds__(kBlock) k_wf_tail(SceneView S, const FrameConst* __restrict__ fcp, PathState P,
+__global__ void __launch_bounds__(kBlock, path_loop_blocks(kAnalytic, kFullShading)) k_wf_tail(SceneView S, const FrameConst* __restrict__ fcp, PathState P,
     Queues Q, uint32_t first, uint32_t* __restrict__ cursor, SceneTable B) {
   const uint32_t n = Q.counts[3 * first];
   for (;;) {
