@@ -2165,3 +2165,46 @@ def material_gltf_extensions(exchanged_coat=False, size=160):
         placed[12], placed[13] = columns[i % 5], rows[i // 5]
         s.add_instance(geo, s.add_material(m), placed, texcoord_set=1 if textured else 0)
     return s
+
+
+# The reference's glTF furnace planes (GltfFurnaceFailure,
+# adapters/headless/main.cpp:1632-1700 in hydra-lotus): white glTF PBR
+# materials that return a white environment whatever their lobes.
+GLTF_FURNACE_PLANES = {
+    "dielectric": {"metallic": 0.0, "roughness": 0.2},
+    "rough dielectric": {"metallic": 0.0, "roughness": 1.0},
+    "metal": {"metallic": 1.0, "roughness": 0.2},
+    "rough metal": {"metallic": 1.0, "roughness": 1.0},
+    "clearcoat": {"metallic": 0.0, "roughness": 0.5, "clearcoat": 1.0},
+    "rough clearcoat": {"metallic": 0.0, "roughness": 0.5, "clearcoat": 0.5, "clearcoat_roughness": 0.4},
+    "sheen": {"metallic": 0.0, "roughness": 0.5, "sheen_color": (1.0, 1.0, 1.0), "sheen_roughness": 0.7},
+    "transmission": {"metallic": 0.0, "roughness": 0.2, "transmission": 1.0},
+    "half transmission": {"metallic": 0.0, "roughness": 0.5, "transmission": 0.5, "specular": 0.5},
+    "every extension": {"metallic": 0.3, "roughness": 0.5, "ior": 1.8, "transmission": 0.4, "clearcoat": 0.7,
+                        "clearcoat_roughness": 0.2, "sheen_color": (0.5, 0.5, 0.5), "sheen_roughness": 0.6},
+}
+
+
+def gltf_furnace(plane, cos_view, size=64):
+    """A 32x32 white glTF PBR plane tilted about X to view cosine
+    `cos_view` under a white constant environment, seen by the bootstrap
+    camera with an orthographic projection (GltfFurnaceFailure,
+    adapters/headless/main.cpp:1700-1720): no scattered ray meets the plane
+    again, so each pixel's mean is the closure's directional albedo, 1 for
+    an energy-conserving white closure."""
+    s = Scene(f"gltf-furnace-{plane}-{cos_view}")
+    view = identity()
+    view[14] = -3.0
+    projection = identity()
+    projection[10] = F32(-2.0) / F32(9.0)
+    projection[14] = F32(-11.0) / F32(9.0)
+    s.world_to_clip = multiply(projection, view)
+    s.width = s.height = size
+    s.environment_constant = (1.0, 1.0, 1.0)
+    g = s.add_geometry(np.array([(-16, -16, 0), (16, -16, 0), (16, 16, 0), (-16, 16, 0)], dtype=F32),
+                       np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+    tilted = identity()
+    sin_view = float(F32(math.sqrt(1.0 - float(F32(cos_view)) ** 2)))
+    tilted[5], tilted[6], tilted[9], tilted[10] = cos_view, sin_view, -sin_view, cos_view
+    s.add_instance(g, s.add_material(gltf_material(**GLTF_FURNACE_PLANES[plane])), tilted)
+    return s

@@ -13,6 +13,8 @@ gltf_pbr.slang, composed.slang, lobes.slang and albedo.slang).
   bit for bit, and so does the batch path tracer after them.
 - A batch of glTF scenes equals single renders; out-of-range inputs fail
   the scene update with a detail.
+- The reference's glTF white furnace: every white glTF plane returns the
+  environment within its tolerance, both integrators and samplings.
 """
 
 import numpy as np
@@ -188,3 +190,26 @@ def test_invalid_gltf_inputs_fail(cuda, case):
         assert res.status == abi.FAIL
         want = "unknown model" if case == "model" else "glTF PBR input"
         assert want in res.detail.decode(), res.detail
+
+
+@pytest.mark.parametrize("integrator", INTEGRATORS)
+@pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
+def test_gltf_white_furnace(cuda, renderer, integrator, light_sampling):
+    """The reference's renderer.path.gltf_furnace (GltfFurnaceFailure,
+    adapters/headless/main.cpp:1632-1770): every white glTF plane returns
+    the white environment, 1 within five standard errors and 8e-3, at view
+    cosines 1, 0.5 and 0.125, 32 spp."""
+    from test_oracle_gltf_cpu import SAMPLES, furnace_check
+    failures = []
+    for plane in sorted(scenes.GLTF_FURNACE_PLANES):
+        for cos_view in (1.0, 0.5, 0.125):
+            scene = scenes.gltf_furnace(plane, cos_view)
+            st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,
+                                      max_bounces=64, sample_index=0)
+            cuda.check(renderer.update_scene(scene), "update_scene")
+            res, image = renderer.render_scene(scene.frame(st, SAMPLES))
+            cuda.check(res, "render_scene")
+            mean, tol, ok = furnace_check(image)
+            if not ok:
+                failures.append((plane, cos_view, mean.tolist(), tol.tolist()))
+    assert not failures, failures
