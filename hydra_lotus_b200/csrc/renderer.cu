@@ -1885,7 +1885,19 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   if (want_depth && !(t.clear_depth >= 0.0f && t.clear_depth <= 1.0f))
     return fail("invalid offscreen clear values");
   const bool wavefront = st.integrator == LOTUS_INTEGRATOR_WAVEFRONT;
-  if (!ensure_targets(R, t.width, t.height, wavefront, detail)) return poison(detail);
+  // The reference integrator's paths run on the wavefront's compacted
+  // queues too when one launch holds at least as many as the extension
+  // kernel keeps resident (the target's pixels times the samples of a
+  // wave): each path is computed as in the per-thread loop, bit for bit,
+  // and the sorted queues keep software traversal coherent. Below that the
+  // frame is latency-bound and the per-thread loop (k_reference_pt) is
+  // faster. The frame's evidence stays the reference integrator's.
+  const uint64_t launch_paths = (uint64_t)t.width * t.height *
+      std::min(std::max(d.frame_count, 1u), std::max(R.wave, 1u));
+  const bool queued = wavefront ||
+      (st.integrator == LOTUS_INTEGRATOR_REFERENCE && st.light_sampling <= LOTUS_LIGHT_SAMPLING_MIS &&
+       st.output == LOTUS_OUTPUT_RADIANCE && launch_paths >= extension_resident_threads());
+  if (!ensure_targets(R, t.width, t.height, queued, detail)) return poison(detail);
   // The radiance cache serves the wavefront integrator's samples.
   const bool use_cache = wavefront && R.cache_enabled && R.cache.ready();
   if (use_cache && !ensure_cache_queues(R, t.width * t.height, detail)) return poison(detail);
@@ -2051,7 +2063,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   if (tuning.rounds == 0 && R.auto_rounds != 0 && R.rounds_key == gk) tuning.rounds = R.auto_rounds;
   // The rounds the call's last sample ran (the frame result reports them).
   uint32_t last_rounds = wavefront_rounds(st.max_bounces, want_visits, tuning.rounds, use_cache ? cq.bounce : 0u);
-  const bool choose_rounds = wavefront && R.tuning.rounds == 0 && !(R.rounds_key == gk);
+  const bool choose_rounds = queued && R.tuning.rounds == 0 && !(R.rounds_key == gk);
   // Samples in waves: where two or more are added without the radiance
   // cache (which trains between samples), the wavefront runs `wave` samples
   // (the renderer's wave size, halved while the call adds fewer) as one
@@ -2065,7 +2077,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   const uint32_t pixels = t.width * t.height;
   uint32_t wave = std::max(R.wave, 1u);
   while (wave > 1 && wave > to_add) wave /= 2;
-  const bool waves = wavefront && !use_cache && to_add >= 2 && wave >= 2;
+  const bool waves = queued && !use_cache && to_add >= 2 && wave >= 2;
   const uint32_t profiled_samples = (want_timings || want_visits) ? (waves ? wave : 1u) : 0u;
   const uint32_t chainable = waves ? submissions - profiled_samples : 0u;
   while (R.ev_sample_done.size() < kMaxChain) {
@@ -2156,14 +2168,14 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     last_wave = 1;
     ++k;
     if (profiled) {
-      if (wavefront)
+      if (queued)
         launch_wavefront_sample(R.view, R.frame_const.ptr, rect, t.width, t.height, st.max_bounces, P, Q,
             R.accum.ptr, R.color.ptr, R.totals.ptr, s, &profile, tuning, &cq);
       else
         launch_reference_pt(R.view, R.frame_const.ptr, rect, R.accum.ptr, R.color.ptr, R.totals.ptr, s,
             &profile);
       launch_advance(R.frame_const.ptr, s);
-    } else if (wavefront) {
+    } else if (queued) {
       gk.rounds = wavefront_rounds(st.max_bounces, false, tuning.rounds, use_cache ? cq.bounce : 0u);
       if (!R.graph || !(R.graph_key == gk)) {
         if (R.graph) {
@@ -2194,7 +2206,7 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
   std::vector<uint32_t> counts(3 * (size_t)(st.max_bounces + 2), 0);
   cudaMemcpyAsync(&totals, R.totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(walks, R.walk_failure.ptr, sizeof(walks), cudaMemcpyDeviceToHost, s);
-  if (wavefront)
+  if (queued)
     cudaMemcpyAsync(counts.data(), last_counts, counts.size() * 4,
         cudaMemcpyDeviceToHost, s);
   if (!R.ok(cudaStreamSynchronize(s), "render", detail)) return poison(detail);
@@ -2271,6 +2283,8 @@ int32_t render(Renderer& R, const lotus_frame_desc& d, lotus_frame_result& res, 
     res.wavefront_path_count_size = last;
     res.wavefront_rounds = last_rounds;
     res.last_wave_samples = last_wave;
+  }
+  if (queued && to_add > 0) {
     if (choose_rounds) {
       gk.rounds = 0;
       R.rounds_key = gk;

@@ -163,6 +163,42 @@ def test_sample_chains_equal_one_sample_at_a_time(cuda, renderer, frames):
     assert np.array_equal(chained, single), f"{np.count_nonzero(chained != single)} values differ"
 
 
+def test_reference_integrator_on_queues_matches_oracle(cuda, renderer, oracle_lib):
+    """A reference-integrator frame of at least the extension kernel's
+    resident threads (here 512^2 paths) runs on the wavefront's queues:
+    path for path the oracle's, with the reference integrator's evidence
+    (no wavefront path counts or rounds)."""
+    scene = scenes.box_room(seed=0, size=512)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_REFERENCE, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=12, sample_index=5)
+    res, color = render(cuda, renderer, scene, st)
+    assert res.wavefront_rounds == 0 and res.wavefront_path_count_size == 0
+    want, rays = oracle_lib.OracleScene(scene).sample(scene.frame(st), 5)
+    p = PathParity(color, want)
+    print(p)
+    p.assert_ok()
+    assert p.exact > 0.9, p
+    assert res.camera_rays == rays[0]
+
+
+def test_reference_integrator_queued_accumulation_equals_per_thread_loop(cuda, renderer):
+    """Eight samples in one call at 192^2 (a wave of eight holds 294,912
+    paths: the queues) equal eight one-sample calls (36,864 paths each: the
+    per-thread loop, k_reference_pt) bit for bit: the two schedules compute
+    each path and add the samples to the FP64 accumulation identically."""
+    scene = scenes.lit_room(seed=2, size=192)
+    st = abi.default_settings(integrator=abi.INTEGRATOR_REFERENCE, light_sampling=abi.LIGHT_SAMPLING_MIS,
+                              max_bounces=12, sample_index=40)
+    res, queued = render(cuda, renderer, scene, st, frame_count=8)
+    assert res.samples_per_pixel == 8
+    cuda.check(renderer.update_scene(scene), "update_scene")
+    for k in range(8):
+        res, single = renderer.render_scene(scene.frame(st, 1))
+        cuda.check(res, "one sample")
+    assert res.samples_per_pixel == 8
+    assert np.array_equal(queued, single), f"{np.count_nonzero(queued != single)} values differ"
+
+
 MATERIAL_MODES = [(abi.INTEGRATOR_REFERENCE, abi.LIGHT_SAMPLING_BSDF),
                   (abi.INTEGRATOR_REFERENCE, abi.LIGHT_SAMPLING_MIS),
                   (abi.INTEGRATOR_WAVEFRONT, abi.LIGHT_SAMPLING_MIS),
