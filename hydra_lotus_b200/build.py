@@ -4,9 +4,10 @@ nvcc for sm_100a.
 The sources whose arithmetic the oracle restates bit for bit (transport,
 traversal, ReSTIR, the scene tables) are compiled with --fmad=false, so
 that their multiply and add steps round separately in source order. The
-radiance cache (checked against its oracle within stated tolerances) and
-the BVH builders (whose trees never change a hit: hits are decided by
-triangle tests alone) are compiled with fused multiply-adds.
+radiance cache (checked against its oracle within stated tolerances), the
+SVGF passes (checked against the reference's CPU code within its published
+GPU tolerances) and the BVH builders (whose trees never change a hit: hits
+are decided by triangle tests alone) are compiled with fused multiply-adds.
 """
 
 import os
@@ -18,12 +19,12 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "liblotus_cuda.so")
 INCLUDE = os.path.join(HERE, "..", "include")
-SOURCES = ["integrator.cu", "bvh_build.cu", "renderer.cu", "static_render.cu", "temporal.cu",
+SOURCES = ["integrator.cu", "bvh_build.cu", "renderer.cu", "static_render.cu", "temporal.cu", "svgf.cu",
            "radiance_cache.cu", "batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
 # Sources compiled with fused multiply-adds; every other one with --fmad=false.
-FUSED = {"radiance_cache.cu", "bvh_build.cu"}
+FUSED = {"radiance_cache.cu", "bvh_build.cu", "svgf.cu"}
 
 
 def _inputs():

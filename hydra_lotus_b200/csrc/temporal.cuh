@@ -90,6 +90,19 @@ struct alignas(16) TemporalInstance {
 };
 static_assert(sizeof(TemporalInstance) == 80, "TemporalInstance is 80 bytes");
 
+// Pixel (px, py) of a one-thread-per-pixel launch's thread `index`.
+__device__ __forceinline__ bool pixel_of(uint32_t index, uint32_t width, uint32_t height,
+    uint32_t& px, uint32_t& py) {
+  if (index >= width * height) return false;
+  px = index % width;
+  py = index / width;
+  return true;
+}
+
+__device__ __forceinline__ bool finite4(float4 v) {
+  return isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w);
+}
+
 constexpr uint32_t kNoReservoirSample = 0xFFFFFFFFu;
 constexpr uint32_t kNoFilterGuide = 0xFFFFFFFFu;
 
