@@ -15,16 +15,24 @@
 //   which is what the CUDA kernels do too. Equal distances resolve to the
 //   smaller (instance, primitive), so the closest hit does not depend on the
 //   traversal order.
-// - Textures. Only the environment image is a texture here; it is filtered
-//   bilinearly in FP32 (repeat across longitude, clamp at the poles, as the
-//   reference's sampler, gpu_scene.cpp:2212-2214), where the reference's
-//   sampler hardware uses fixed-point weights.
+// - Textures. Images (material lookups and the environment) are filtered
+//   bilinearly in FP32 (the environment repeating across longitude and
+//   clamped at the poles, as the reference's sampler, gpu_scene.cpp:
+//   2212-2214), where the reference's sampler hardware uses fixed-point
+//   weights.
 // - Accumulation. Samples are summed in FP64 (the precision policy), where
 //   the reference's image is RGBA32F.
+// - The log and power of the glTF closure's albedo axes and sheen are the
+//   library's portable ones (restated below), where the reference uses the
+//   shading language's; its albedo tables are the library's own cubature
+//   of the same lobes (albedo_tables.inc), on the reference's grid.
 // Analytic lights (sphere, rect, disk, distant and parallel; their table
 // entries, crossing hierarchy, sampling and crossing tests) are restated from
-// gpu_scene.cpp:272-610 and scene.slang:680-1178. Textured inputs and the
-// glTF closure are not in the restated path (no workload uses them).
+// gpu_scene.cpp:272-610 and scene.slang:680-1178; texture lookups and the
+// textured inputs from scene.slang:315-413 and 1184-1260; MaterialX's glTF
+// PBR surface, with the general composed closure the reference builds it
+// from, from bsdf/albedo.slang, lobes.slang, composed.slang, gltf_pbr.slang
+// and scene.slang:1262-1406.
 
 #include "lotus_oracle.h"
 
