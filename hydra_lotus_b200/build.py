@@ -4,10 +4,11 @@ nvcc for sm_100a.
 The sources whose arithmetic the oracle restates bit for bit (transport,
 traversal, ReSTIR, the scene tables) are compiled with --fmad=false, so
 that their multiply and add steps round separately in source order. The
-radiance cache (checked against its oracle within stated tolerances), the
-SVGF passes (checked against the reference's CPU code within its published
-GPU tolerances) and the BVH builders (whose trees never change a hit: hits
-are decided by triangle tests alone) are compiled with fused multiply-adds.
+radiance cache (checked against its oracle within stated tolerances) and
+the BVH builders (whose trees never change a hit: hits are decided by
+triangle tests alone) are compiled with fused multiply-adds. The SVGF
+passes are not: fused, their edge-stopping and neighbour tests decide
+differently from the reference's CPU SVGF at a few pixels a frame.
 """
 
 import os
@@ -24,7 +25,7 @@ SOURCES = ["integrator.cu", "bvh_build.cu", "renderer.cu", "static_render.cu", "
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
 # Sources compiled with fused multiply-adds; every other one with --fmad=false.
-FUSED = {"radiance_cache.cu", "bvh_build.cu", "svgf.cu"}
+FUSED = {"radiance_cache.cu", "bvh_build.cu"}
 
 
 def _inputs():
