@@ -525,10 +525,12 @@ __global__ void __launch_bounds__(kBlock) k_wf_camera(SceneView S,
 // kCacheVertex: the cache's vertex (bounce 1 with the cache enabled); the
 // other instantiation carries none of the cache's code or registers.
 // Compiled for six resident blocks per SM (80 registers): shading is
-// latency-bound and gains more from occupancy than from registers.
+// latency-bound and gains more from occupancy than from registers. The
+// full-shading instantiation (texture lookups, glTF PBR) at four (128
+// registers): at 80 it spilled 350-550 bytes a thread.
 constexpr int kShadeBlocksPerSm = 6;
 template <bool kCacheVertex, bool kBatch, bool kAnalytic, bool kFullShading>
-__global__ void __launch_bounds__(kBlock, kShadeBlocksPerSm) k_wf_shade(SceneView S,
+__global__ void __launch_bounds__(kBlock, kFullShading ? 4 : kShadeBlocksPerSm) k_wf_shade(SceneView S,
     const FrameConst* __restrict__ fcp, PathState P, Queues Q, uint32_t bounce, CacheQueues C, SceneTable B) {
   const uint32_t n = Q.counts[3 * bounce + 1];
   const bool cache_vertex = kCacheVertex && bounce < fcp->max_bounces;
