@@ -102,7 +102,9 @@ class Geometry(C.Structure):
         ("triangle_count", C.c_uint32),
         ("texcoords", C.POINTER(C.c_float)),
         ("texcoord_sets", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("color_sets", C.c_uint32),
+        ("colors", C.POINTER(C.c_float)),
+        ("color_counts", C.POINTER(C.c_uint32)),
     ]
 
 
@@ -112,7 +114,7 @@ class Instance(C.Structure):
         ("geometry", C.c_uint32),
         ("material", C.c_uint32),
         ("texcoord_set", C.c_uint32),  # k > 0: the geometry's set k - 1; 0: none
-        ("reserved", C.c_uint32),
+        ("color_set", C.c_uint32),  # k > 0: the geometry's colour set k - 1; 0: none
     ]
 
 

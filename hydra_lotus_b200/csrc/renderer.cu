@@ -666,6 +666,9 @@ struct HostScene {
   std::vector<lotus_texture_input> texture_inputs;
   uint32_t texture_count = 0;
   std::vector<uint64_t> texcoord_base;
+  // Per geometry and colour set: its first value in the device's colour
+  // array (floats) and whether it is one value for the whole mesh.
+  std::vector<std::vector<uint2>> color_sets;
 };
 
 static_assert(LOTUS_OUTPUT_BARYCENTRICS == kOutputBarycentrics && LOTUS_OUTPUT_SHADING_NORMAL == kOutputShadingNormal &&
@@ -711,6 +714,8 @@ struct Renderer {
   DeviceArray<float> albedo_tables;  // the composed closure's (albedo.cuh), uploaded once
   DeviceArray<float2> texcoords;
   DeviceArray<uint32_t> inst_texcoords;
+  DeviceArray<float> colors;         // every geometry's colour sets, RGB
+  DeviceArray<uint2> inst_colors;    // per instance: (first float, whole-mesh flag) or kNoTexture
   std::vector<LightRecord> host_lights;
   std::vector<uint32_t> host_light_offsets;
   SceneView view{};
@@ -863,7 +868,7 @@ struct Renderer {
     light_radiance.release(); env_texels.release(); env_floats.release(); env_guide.release();
     analytic.release(); light_nodes.release(); distant.release();
     tex_texels.release(); tex_info.release(); tex_lookups.release(); mat_lookups.release(); texcoords.release();
-    inst_texcoords.release();
+    inst_texcoords.release(); colors.release(); inst_colors.release();
     scene_ready = false;
   }
 
@@ -872,7 +877,8 @@ struct Renderer {
            materials.bytes() + normals.bytes() + lights.bytes() + light_verts.bytes() +
            light_radiance.bytes() + env_texels.bytes() + env_floats.bytes() + env_guide.bytes() +
            analytic.bytes() + light_nodes.bytes() + distant.bytes() + tex_texels.bytes() + tex_info.bytes() +
-           tex_lookups.bytes() + mat_lookups.bytes() + texcoords.bytes() + inst_texcoords.bytes();
+           tex_lookups.bytes() + mat_lookups.bytes() + texcoords.bytes() + inst_texcoords.bytes() +
+           colors.bytes() + inst_colors.bytes();
   }
 };
 
@@ -931,6 +937,24 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
       detail = "geometry " + std::to_string(g) + " has texture-coordinate sets without data";
       return false;
     }
+    if (geo.color_sets && (!geo.colors || !geo.color_counts)) {
+      detail = "geometry " + std::to_string(g) + " has colour sets without data";
+      return false;
+    }
+    uint64_t color_values = 0;
+    for (uint32_t k = 0; k < geo.color_sets; ++k) {
+      if (geo.color_counts[k] != 1 && geo.color_counts[k] != 3ull * geo.triangle_count) {
+        detail = "geometry " + std::to_string(g) + "'s colour set " + std::to_string(k) +
+                 " has neither one value nor one per triangle corner";
+        return false;
+      }
+      color_values += geo.color_counts[k];
+    }
+    for (uint64_t i = 0; i < 3 * color_values; ++i)
+      if (!std::isfinite(geo.colors[i])) {
+        detail = "geometry " + std::to_string(g) + " has a non-finite colour";
+        return false;
+      }
     for (uint64_t i = 0; i < 3ull * geo.triangle_count; ++i)
       if (geo.triangles[i] >= geo.vertex_count) {
         detail = "geometry " + std::to_string(g) + " indexes past its vertices";
@@ -950,6 +974,10 @@ bool validate_scene(const lotus_scene_desc& s, std::string& detail) {
     }
     if (inst.texcoord_set != LOTUS_NO_TEXCOORDS && inst.texcoord_set > s.geometries[inst.geometry].texcoord_sets) {
       detail = "instance " + std::to_string(i) + " names a missing texture-coordinate set";
+      return false;
+    }
+    if (inst.color_set != LOTUS_NO_COLORS && inst.color_set > s.geometries[inst.geometry].color_sets) {
+      detail = "instance " + std::to_string(i) + " names a missing colour set";
       return false;
     }
     const float* m = inst.world_from_object;
@@ -1052,6 +1080,7 @@ struct InstanceState {
   std::vector<InstanceTraversal> trav;
   std::vector<InstanceShading> shade;
   std::vector<uint32_t> texcoords;  // SceneView::inst_texcoords
+  std::vector<uint2> colors;        // SceneView::inst_colors
 };
 
 lotus_scene_desc host_desc(const Renderer& R) {
@@ -1110,6 +1139,7 @@ bool prepare_instances(Renderer& R, InstanceState& out, std::string& detail) {
   out.trav.resize(s.instance_count);
   out.shade.resize(s.instance_count);
   out.texcoords.resize(s.instance_count);
+  out.colors.resize(s.instance_count);
   for (uint32_t i = 0; i < s.instance_count; ++i) {
     const lotus_instance& inst = s.instances[i];
     const float* m = inst.world_from_object;
@@ -1127,6 +1157,9 @@ bool prepare_instances(Renderer& R, InstanceState& out, std::string& detail) {
         inst.texcoord_set == LOTUS_NO_TEXCOORDS || inst.texcoord_set > geo.texcoord_sets
             ? kNoTexture
             : (uint32_t)(h.texcoord_base[inst.geometry] + 3ull * geo.triangle_count * (inst.texcoord_set - 1));
+    out.colors[i] = inst.color_set == LOTUS_NO_COLORS || inst.color_set > geo.color_sets
+                        ? make_uint2(kNoTexture, 0u)
+                        : h.color_sets[inst.geometry][inst.color_set - 1];
     t.material = inst.material;
     t.light_offset = out.table.offsets[i];
     for (int r = 0; r < 3; ++r) sh.m[r] = make_float4(m[r], m[4 + r], m[8 + r], m[12 + r]);
@@ -1158,6 +1191,7 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
       !R.ok(R.inst_trav.upload(in.trav.data(), in.trav.size(), st), "instances", detail) ||
       !R.ok(R.inst_shade.upload(in.shade.data(), in.shade.size(), st), "instances", detail) ||
       !R.ok(R.inst_texcoords.upload(in.texcoords.data(), in.texcoords.size(), st), "instances", detail) ||
+      !R.ok(R.inst_colors.upload(in.colors.data(), in.colors.size(), st), "instances", detail) ||
       !R.ok(R.tlas.resize(std::max<uint32_t>(BvhBuilder::node_count(n), 1)), "TLAS", detail))
     return false;
   if (!R.ok(n <= kSahMaxTriangles
@@ -1179,6 +1213,7 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
   v.inst_shade = R.inst_shade.ptr;
   v.materials = R.materials.ptr;
   v.full_shading = 0;
+  for (const uint2& c : in.colors) if (c.x != kNoTexture) v.full_shading = 1;
   for (const lotus_material& m : h.materials) {
     bool any = !(m.normal[0] == 0.0f && m.normal[1] == 0.0f && (m.normal[2] == 0.0f || m.normal[2] == 1.0f)) ||
         m.model == LOTUS_MODEL_GLTF_PBR;
@@ -1192,6 +1227,8 @@ bool submit_instances(Renderer& R, InstanceState& in, std::string& detail) {
   v.albedo_tables = R.albedo_tables.ptr;
   v.texcoords = R.texcoords.ptr;
   v.inst_texcoords = R.inst_texcoords.ptr;
+  v.colors = R.colors.ptr;
+  v.inst_colors = R.inst_colors.ptr;
   v.normals = R.normals.ptr;
   v.lights = R.lights.ptr;
   v.light_verts = R.light_verts.ptr;
@@ -1367,11 +1404,27 @@ bool upload_textures(Renderer& R, const lotus_scene_desc& s, std::string& detail
     detail = "the scene's texture coordinates exceed 2^32 corners";
     return false;
   }
+  std::vector<float> colors;
+  R.host.color_sets.assign(s.geometry_count, {});
+  for (uint32_t g = 0; g < s.geometry_count; ++g) {
+    const lotus_geometry& geo = s.geometries[g];
+    const float* values = geo.colors;
+    for (uint32_t k = 0; k < geo.color_sets; ++k) {
+      R.host.color_sets[g].push_back(make_uint2((uint32_t)colors.size(), geo.color_counts[k] == 1 ? 1u : 0u));
+      colors.insert(colors.end(), values, values + 3ull * geo.color_counts[k]);
+      values += 3ull * geo.color_counts[k];
+    }
+  }
+  if (colors.size() >= (size_t)kNoTexture) {
+    detail = "the scene's colour sets exceed 2^32 values";
+    return false;
+  }
   return R.ok(R.tex_texels.upload(texels.data(), texels.size(), st), "texels", detail) &&
          R.ok(R.tex_info.upload(info.data(), info.size(), st), "textures", detail) &&
          R.ok(R.tex_lookups.upload(lookups.data(), lookups.size(), st), "texture inputs", detail) &&
          R.ok(R.mat_lookups.upload(mats.data(), mats.size(), st), "material lookups", detail) &&
-         R.ok(R.texcoords.upload(coords.data(), coords.size(), st), "texture coordinates", detail);
+         R.ok(R.texcoords.upload(coords.data(), coords.size(), st), "texture coordinates", detail) &&
+         R.ok(R.colors.upload(colors.data(), colors.size(), st), "colour sets", detail);
 }
 
 bool build_env_distribution(Renderer& R, const lotus_environment& e, double& mean, std::string& detail) {
@@ -1453,6 +1506,8 @@ int32_t update_scene(Renderer& R, const lotus_scene_desc& s, lotus_scene_result&
     copy.triangles = h.triangles[g].data();
     copy.normals = h.normals[g].empty() ? nullptr : h.normals[g].data();
     copy.texcoords = nullptr;  // on the device only
+    copy.colors = nullptr;
+    copy.color_counts = nullptr;
     h.boxes[g] = geometry_box(copy);
     h.vertex_base[g] = vert_total;
     h.node_base[g] = (uint32_t)nodes;
@@ -1607,6 +1662,8 @@ int32_t update_instances(Renderer& R, const lotus_instance* instances, uint32_t 
     if (inst.texcoord_set != LOTUS_NO_TEXCOORDS &&
         inst.texcoord_set > R.host.geometries[inst.geometry].texcoord_sets)
       return reject("instance " + std::to_string(i) + " names a missing texture-coordinate set");
+    if (inst.color_set != LOTUS_NO_COLORS && inst.color_set > R.host.geometries[inst.geometry].color_sets)
+      return reject("instance " + std::to_string(i) + " names a missing colour set");
     const float* m = inst.world_from_object;
     if (m[3] != 0.0f || m[7] != 0.0f || m[11] != 0.0f || m[15] != 1.0f)
       return reject("instance " + std::to_string(i) + " has a projective transform");

@@ -221,6 +221,8 @@ struct SceneView {
   const MaterialLookups* __restrict__ mat_lookups;
   const float2* __restrict__ texcoords;
   const uint32_t* __restrict__ inst_texcoords;
+  const float* __restrict__ colors;        // colour sets, RGB
+  const uint2* __restrict__ inst_colors;   // per instance: (first float, whole-mesh flag) or kNoTexture
   // Two words the renderer clears before and reads after each frame: the
   // number of walks that failed and the kWalkFailed* bits of their causes.
   uint32_t* walk_failure;

@@ -151,11 +151,12 @@ struct TexturedInputs {
 };
 
 static __device__ __noinline__ TexturedInputs textured_inputs(const SceneView& S, uint32_t instance, uint32_t material,
-    uint32_t primitive, float b1, float b2, F3 edge1, F3 edge2, F3 geometric, F3 shading, F3 direction) {
+    uint32_t primitive, float b1, float b2, F3 edge1, F3 edge2, F3 geometric, F3 shading, F3 direction,
+    F3 base_color) {
   const MaterialRecord mat = S.materials[material];
   const MaterialLookups ml = S.mat_lookups[material];
   TexturedInputs out;
-  out.base_color = V(mat.base_roughness);
+  out.base_color = base_color;
   out.roughness = mat.base_roughness.w;
   out.metallic = mat.emission_metallic.w;
   out.specular = V(mat.specular_ior);
@@ -317,6 +318,16 @@ static __device__ __noinline__ GltfHit gltf_hit(const SceneView& S, uint32_t ins
   return out;
 }
 
+// HitColor (scene.slang:376-386): the instance's colour set at the hit,
+// one value for the whole mesh or the corners' interpolated.
+__device__ __forceinline__ F3 hit_color(const SceneView& S, uint2 set, uint32_t primitive, float b1, float b2) {
+  const float* c = S.colors + set.x;
+  if (set.y) return V(c[0], c[1], c[2]);
+  c += 9 * (size_t)primitive;
+  const F3 c0 = V(c[0], c[1], c[2]), c1 = V(c[3], c[4], c[5]), c2 = V(c[6], c[7], c[8]);
+  return c0 + b1 * (c1 - c0) + b2 * (c2 - c0);
+}
+
 // ReconstructHit and EvaluatePreview (scene.slang:1408-1449, 1184-1260).
 // The corners come from the leaf-ordered triangle pool, which holds the
 // geometry's own positions. A texture lookup replaces its input's constant,
@@ -367,9 +378,18 @@ __device__ __forceinline__ SurfaceHit reconstruct_hit(const SceneView& S, uint32
     sh.bsdf = make_closure(V(0.0f), 1.0f, 0.0f, 1.5f, false, V(0.0f), 0.0f, V(1.0f), false, true);
     return sh;
   }
+  if (kFullShading) {
+    // EvaluatePreview's base colour: the instance's colour set, clamped,
+    // where it reads one.
+    const uint2 set = S.inst_colors[instance];
+    if (set.x != kNoTexture) {
+      const F3 c = hit_color(S, set, primitive, b1, b2);
+      sh.base_color = V(saturate(c.x), saturate(c.y), saturate(c.z));
+    }
+  }
   if (kFullShading && (flags & kMaterialTextured)) {
     const TexturedInputs ti = textured_inputs(S, instance, rec.material, primitive, b1, b2, p1 - p0, p2 - p0,
-        sh.normal, sh.shading_normal, direction);
+        sh.normal, sh.shading_normal, direction, sh.base_color);
     sh.base_color = ti.base_color;
     sh.roughness = ti.roughness;
     sh.metallic = ti.metallic;

@@ -126,8 +126,8 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
   // The scene description, rebuilt whole.
   std::vector<lotus_geometry> geos(geometries_.size());
   std::vector<std::vector<float>> positions(geometries_.size()), normals(geometries_.size()),
-      texcoords(geometries_.size());
-  std::vector<std::vector<uint32_t>> triangles(geometries_.size());
+      texcoords(geometries_.size()), colors(geometries_.size());
+  std::vector<std::vector<uint32_t>> triangles(geometries_.size()), color_counts(geometries_.size());
   for (size_t g = 0; g < geometries_.size(); ++g) {
     const Lotus::MeshGeometry& m = *geometries_[g];
     positions[g].reserve(3 * m.positions.size());
@@ -151,6 +151,17 @@ Lotus::GpuSceneEvidence CudaOffscreenRenderer::UpdateScene(const Lotus::SceneUpd
     }
     geos[g].texcoords = texcoords[g].empty() ? nullptr : texcoords[g].data();
     geos[g].texcoord_sets = texcoords[g].empty() ? 0u : (uint32_t)m.texcoords.size();
+    // Colour sets in key order: one RGB per triangle corner, or one for the
+    // mesh (MeshGeometry::colors, render_world.hpp:52-55).
+    for (const auto& [name, set] : m.colors) {
+      if (set.size() != 1 && set.size() != 3 * m.triangles.size())
+        return fail("colours must be one per triangle corner or one per mesh (set " + name + ")");
+      for (const auto& c : set) colors[g].insert(colors[g].end(), c.begin(), c.end());
+      color_counts[g].push_back((uint32_t)set.size());
+    }
+    geos[g].color_sets = (uint32_t)color_counts[g].size();
+    geos[g].colors = colors[g].empty() ? nullptr : colors[g].data();
+    geos[g].color_counts = color_counts[g].empty() ? nullptr : color_counts[g].data();
   }
   // Every resident texture (TextureFormat, material.hpp:15-23), counted
   // from 1 by the lookups that name it.
@@ -363,6 +374,7 @@ bool CudaOffscreenRenderer::InstanceArray(std::vector<lotus_instance>& insts, st
     insts[i].material = si.material;
     // The set its material's lookups read, counted from 1 (0: none).
     insts[i].texcoord_set = si.texcoords == Lotus::kNoTexcoords ? LOTUS_NO_TEXCOORDS : si.texcoords + 1;
+    insts[i].color_set = si.colors == Lotus::kNoColors ? LOTUS_NO_COLORS : si.colors + 1;
   }
   return true;
 }
@@ -389,7 +401,7 @@ bool CudaOffscreenRenderer::UpdateIncrementally(const Lotus::SceneUpdate& u, Lot
     const Lotus::MeshGeometry& b = *next;
     if (a.positions.size() != b.positions.size() || a.triangles != b.triangles ||
         a.normals.empty() != b.normals.empty() || (!b.normals.empty() && b.normals.size() != 3 * b.triangles.size()) ||
-        a.texcoords != b.texcoords)
+        a.texcoords != b.texcoords || a.colors != b.colors)
       return false;
     edits.emplace_back(at, next);
   }

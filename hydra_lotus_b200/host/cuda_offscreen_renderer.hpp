@@ -28,9 +28,10 @@
 // resident textures to lotus_texture, each model's texture inputs in the
 // reference's slot numbering (material.hpp:262-312) to lotus_texture_input,
 // each geometry's texture-coordinate sets in key order and each instance's
-// set. Scene content the backend does not build (the reserved Standard
-// Surface and OpenPBR models, vertex colours) makes UpdateScene Fail with
-// the reason, as the reference Fails on unsupported content.
+// set, and each geometry's colour sets in key order and each instance's
+// colour set. Scene content the backend does not build (the reserved
+// Standard Surface and OpenPBR models) makes UpdateScene Fail with the
+// reason, as the reference Fails on unsupported content.
 #pragma once
 
 #include <lotus/vulkan_backend.hpp>

@@ -166,6 +166,8 @@ class Scene:
         # texture inputs.
         self.texcoords = {}
         self.instance_texcoords = {}
+        self.colors = {}            # geometry -> (flat RGB array, per-set value counts)
+        self.instance_colors = {}
         self.textures = []
         self.texture_inputs = []
         self._desc = None
@@ -197,6 +199,15 @@ class Scene:
         self._desc = None
         return len(self.texture_inputs)
 
+    def set_colors(self, geometry, sets):
+        """Geometry `geometry`'s colour sets (MeshGeometry::colors, in key
+        order): each an array of RGB, one per triangle corner (triangle by
+        triangle) or one for the whole mesh."""
+        arrays = [np.ascontiguousarray(c, dtype=F32).reshape(-1, 3) for c in sets]
+        counts = np.array([a.shape[0] for a in arrays], dtype=np.uint32)
+        self.colors[geometry] = (np.ascontiguousarray(np.concatenate(arrays).reshape(-1)), counts)
+        self._desc = None
+
     def set_texcoords(self, geometry, sets):
         """Geometry `geometry`'s texture-coordinate sets: (sets, triangles,
         3, 2) per-corner (s, t)."""
@@ -219,11 +230,13 @@ class Scene:
         self._desc = None
         return len(self.materials) - 1
 
-    def add_instance(self, geometry, material, world_from_object=None, texcoord_set=0):
+    def add_instance(self, geometry, material, world_from_object=None, texcoord_set=0, color_set=0):
         m = identity() if world_from_object is None else np.asarray(world_from_object, dtype=F32)
         self.instances.append((m.copy(), geometry, material))
         if texcoord_set:
             self.instance_texcoords[len(self.instances) - 1] = texcoord_set
+        if color_set:
+            self.instance_colors[len(self.instances) - 1] = color_set
         self._desc = None
         return len(self.instances) - 1
 
@@ -291,12 +304,18 @@ class Scene:
             if i in self.texcoords:
                 geos[i].texcoords = self.texcoords[i].ctypes.data_as(C.POINTER(C.c_float))
                 geos[i].texcoord_sets = self.texcoords[i].shape[0]
+            if i in self.colors:
+                values, counts = self.colors[i]
+                geos[i].colors = values.ctypes.data_as(C.POINTER(C.c_float))
+                geos[i].color_counts = counts.ctypes.data_as(C.POINTER(C.c_uint32))
+                geos[i].color_sets = counts.shape[0]
         insts = (abi.Instance * max(1, len(self.instances)))()
         for i, (m, g, mat) in enumerate(self.instances):
             insts[i].world_from_object[:] = [float(v) for v in m]
             insts[i].geometry = g
             insts[i].material = mat
             insts[i].texcoord_set = self.instance_texcoords.get(i, 0)
+            insts[i].color_set = self.instance_colors.get(i, 0)
         mats = (abi.Material * len(self.materials))(*self.materials)
         d = abi.SceneDesc()
         d.geometries = geos
@@ -2207,4 +2226,87 @@ def gltf_furnace(plane, cos_view, size=64):
     sin_view = float(F32(math.sqrt(1.0 - float(F32(cos_view)) ** 2)))
     tilted[5], tilted[6], tilted[9], tilted[10] = cos_view, sin_view, -sin_view, cos_view
     s.add_instance(g, s.add_material(gltf_material(**GLTF_FURNACE_PLANES[plane])), tilted)
+    return s
+
+
+def material_primvars(swapped_colors=False, size=160):
+    """The reference's material-primvars-v1 fixture (SetMaterialPrimvars,
+    material_fixtures.cpp:1941-2031 in hydra-lotus), which its golden images
+    validation/reference/material-primvars-v1-{mean,variance}.pfm were
+    rendered from, in the form its translator hands the renderer: cards and
+    two-quad meshes (scale 0.7, the middle three rows of the 5x5 grid) whose
+    colour sets a UsdPreviewSurface material's base colour reads by name —
+    per corner (vertex, varying, face-varying), per face, one value for the
+    mesh, displayColor, an absent set (the material's own colour), an
+    out-of-range colour the shader clamps, a set no material reads, unbound
+    meshes' displayColor, and displayOpacity as constant coverage.
+    ``swapped_colors`` swaps red and blue of the Vertex mesh's colours (the
+    fixture's negative control, SwappedColors)."""
+    s = material_studio("material-primvars-v1", size)
+    corners = [(1, 0, 0), (1, 1, 0), (0, 1, 1), (0, 0, 1)]
+    straight, reversed_ = (0, 1, 2, 3), (3, 2, 1, 0)
+
+    def card():
+        return s.add_geometry(np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)],
+                                       dtype=F32), np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+
+    def colored(at, swap=False):
+        g = card()
+        values = [corners[at[c]] for c in (0, 1, 2, 0, 2, 3)]
+        if swap:
+            values = [(b, gg, r) for r, gg, b in values]
+        s.set_colors(g, [values])
+        return g
+
+    def constant(color):
+        g = card()
+        s.set_colors(g, [[color]])
+        return g
+
+    def uniform():
+        g = s.add_geometry(np.array([(-0.5, -0.5, 0.0), (0.0, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0),
+                                     (0.0, 0.5, 0.0), (-0.5, 0.5, 0.0)], dtype=F32),
+                           np.array([[0, 1, 4], [0, 4, 5], [1, 2, 3], [1, 3, 4]], dtype=np.uint32))
+        faces = (0, 0, 1, 1)
+        s.set_colors(g, [[(1.0, 0.5, 0.0) if f == 0 else (0.0, 0.5, 1.0) for f in faces for _ in range(3)]])
+        return g
+
+    reader = lambda fallback=(0.0, 0.0, 0.0): preview_material(fallback, roughness=0.4)
+    teal = (0.2, 0.6, 0.7)
+    looks = {
+        "Tint": reader(),
+        "Display": reader(),
+        "Absent": reader((1.0, 0.25, 0.0)),
+        "Unnamed": reader((0.25, 0.5, 0.75)),
+        "Glowing": preview_material((0.5, 0.5, 0.5)),
+        "Varying": preview_material(),
+        "OpacityColor": preview_material(teal, opacity=0.25),
+        "OpacityOnly": preview_material(opacity=0.5),
+        "Teal": preview_material(teal),
+    }
+    slot = {name: s.add_material(m) for name, m in looks.items()}
+    # (geometry, material, whether the material reads the mesh's one set)
+    objects = [
+        (colored(straight, swapped_colors), "Tint", True),
+        (colored(straight), "Tint", True),
+        (colored(reversed_), "Tint", True),
+        (uniform(), "Tint", True),
+        (constant((0.25, 0.75, 0.5)), "Tint", True),
+        (constant((0.2, 0.6, 0.7)), "Display", True),
+        (card(), "Absent", False),
+        (constant((1.5, -0.5, 0.5)), "Unnamed", True),
+        (colored(straight), "Glowing", False),
+        (colored(straight), "Varying", True),
+        (uniform(), "Varying", True),
+        (colored(reversed_), "Varying", True),
+        (card(), "OpacityColor", False),
+        (card(), "OpacityOnly", False),
+        (card(), "Teal", False),
+    ]
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (0.8, 0.0, -0.8)
+    for i, (geo, look, reads) in enumerate(objects):
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = placed[5] = placed[10] = 0.7
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        s.add_instance(geo, slot[look], placed, color_set=1 if reads else 0)
     return s

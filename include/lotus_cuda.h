@@ -82,7 +82,13 @@ typedef struct lotus_geometry {
    * i) + 2 * c]; NULL when texcoord_sets is 0. */
   const float* texcoords;
   uint32_t texcoord_sets;
-  uint32_t reserved;
+  /* Colour sets (MeshGeometry::colors, in key order): linear RGB, finite,
+   * unclamped; set k holds color_counts[k] RGB values, 3 * triangle_count
+   * (one per triangle corner, triangle by triangle) or 1 (the whole mesh),
+   * the sets one after another in `colors`. NULL when color_sets is 0. */
+  uint32_t color_sets;
+  const float* colors;
+  const uint32_t* color_counts;
 } lotus_geometry;
 
 /* One placed mesh: SceneUpdate's instance (extraction.hpp:313-354). */
@@ -94,12 +100,18 @@ typedef struct lotus_instance {
    * texcoords, extraction.hpp:44-48): k > 0 for its geometry's set k - 1,
    * LOTUS_NO_TEXCOORDS (0) for the material's texcoord_fallback. */
   uint32_t texcoord_set;
-  uint32_t reserved;
+  /* The colour set its UsdPreviewSurface material's base colour reads
+   * (SceneInstance::colors, extraction.hpp:49-51): k > 0 for its geometry's
+   * set k - 1, clamped into [0, 1], LOTUS_NO_COLORS (0) for the material's
+   * own base colour. A base-colour texture lookup wins; glTF PBR reads no
+   * colour set. */
+  uint32_t color_set;
 } lotus_instance;
 
 /* Zero in every index field below means "none", so that a zeroed struct
  * holds the defaults: no texture-coordinate set, no image, no lookup. */
 #define LOTUS_NO_TEXCOORDS 0u
+#define LOTUS_NO_COLORS 0u
 
 /* TextureFormat (material.hpp:15-23): texels of 4 bytes (8-bit channels,
  * the sRGB format's red, green and blue sRGB-encoded, alpha linear) or of

@@ -1395,6 +1395,8 @@ struct Geometry {
   std::vector<F3> normals;  // 3 per triangle, or empty
   std::vector<float> texcoords;  // set k, triangle i, corner c: 6 * (k * triangles + i) + 2 * c
   uint32_t texcoord_sets = 0;
+  // Colour sets: each one RGB per triangle corner, or one for the mesh.
+  std::vector<std::vector<F3>> colors;
   Bvh bvh;
 };
 
@@ -1404,6 +1406,7 @@ struct Instance {
   uint32_t geometry;
   uint32_t material;
   uint32_t texcoord_set;  // lotus_instance::texcoord_set (0: none)
+  uint32_t color_set;     // lotus_instance::color_set (0: none)
   Box world;
 };
 
@@ -2495,6 +2498,13 @@ void EvaluateGltfPbr(const oracle_scene& s, const Hit& hit, const lotus_material
   sh.emission = emission;
 }
 
+// HitColor (scene.slang:376-386).
+F3 HitColor(const std::vector<F3>& set, uint32_t primitive, float b1, float b2) {
+  if (set.size() == 1) return set[0];
+  const F3 c0 = set[3 * primitive], c1 = set[3 * primitive + 1], c2 = set[3 * primitive + 2];
+  return c0 + b1 * (c1 - c0) + b2 * (c2 - c0);
+}
+
 SurfaceHit ReconstructHit(const oracle_scene& s, const Hit& hit, F3 direction) {
   const Instance& inst = s.instances[hit.instance];
   const Geometry& g = s.geometries[inst.geometry];
@@ -2517,6 +2527,12 @@ SurfaceHit ReconstructHit(const oracle_scene& s, const Hit& hit, F3 direction) {
     return sh;
   }
   sh.base_color = V(mat.base_color[0], mat.base_color[1], mat.base_color[2]);
+  // EvaluatePreview (scene.slang:1187-1189): the instance's colour set,
+  // clamped, where it reads one.
+  if (inst.color_set != LOTUS_NO_COLORS && inst.color_set <= g.colors.size()) {
+    const F3 c = HitColor(g.colors[inst.color_set - 1], hit.primitive, hit.b1, hit.b2);
+    sh.base_color = V(saturate(c.x), saturate(c.y), saturate(c.z));
+  }
   sh.roughness = mat.roughness;
   sh.metallic = mat.metallic;
   F3 emission = V(mat.emission[0], mat.emission[1], mat.emission[2]);
@@ -3391,6 +3407,17 @@ oracle_scene* oracle_scene_create(const lotus_scene_desc* d, char* error, size_t
       for (size_t k = 0; k < g.normals.size(); ++k)
         g.normals[k] = V(src.normals[3 * k], src.normals[3 * k + 1], src.normals[3 * k + 2]);
     }
+    if (src.color_sets && src.colors && src.color_counts) {
+      const float* c = src.colors;
+      for (uint32_t k = 0; k < src.color_sets; ++k) {
+        std::vector<F3> set(src.color_counts[k]);
+        for (F3& v : set) {
+          v = V(c[0], c[1], c[2]);
+          c += 3;
+        }
+        g.colors.push_back(std::move(set));
+      }
+    }
     if (src.texcoord_sets && src.texcoords) {
       g.texcoord_sets = src.texcoord_sets;
       g.texcoords.assign(src.texcoords, src.texcoords + 6 * size_t{src.texcoord_sets} * src.triangle_count);
@@ -3413,6 +3440,7 @@ oracle_scene* oracle_scene_create(const lotus_scene_desc* d, char* error, size_t
     inst.geometry = src.geometry;
     inst.material = src.material;
     inst.texcoord_set = src.texcoord_set;
+    inst.color_set = src.color_set;
     if (src.geometry >= d->geometry_count || src.material >= d->material_count) {
       SetError(error, error_size, "an instance names a missing geometry or material");
       return nullptr;
