@@ -2310,3 +2310,136 @@ def material_primvars(swapped_colors=False, size=160):
         placed[12], placed[13] = columns[i % 5], rows[i // 5]
         s.add_instance(geo, slot[look], placed, color_set=1 if reads else 0)
     return s
+
+
+def _faces_of(points, triangles, faces_of_triangle, faces, normals=None, texcoords=None, colors=None):
+    """The part of a mesh a GeomSubset binds, as extraction hands it over
+    (FacesOf, material_fixtures.cpp:342-375 in hydra-lotus): the triangles
+    whose source face is in `faces`, in order, the points they use in
+    point order, and their corners' normals, texture-coordinate sets and
+    colour sets (a whole-mesh colour kept whole). `texcoords` and `colors`
+    are lists of per-corner arrays in key order."""
+    kept = [t for t in range(len(triangles)) if faces_of_triangle[t] in faces]
+    used = sorted({int(v) for t in kept for v in triangles[t]})
+    index = {v: i for i, v in enumerate(used)}
+    part_points = np.array([points[v] for v in used], dtype=F32)
+    part_tris = np.array([[index[int(v)] for v in triangles[t]] for t in kept], dtype=np.uint32)
+    part_normals = None if normals is None else np.array([normals[t] for t in kept], dtype=F32)
+    part_st = [np.array([s[3 * t:3 * t + 3] for t in kept], dtype=F32).reshape(-1, 3, 2) for s in texcoords or []]
+    part_colors = [c if len(c) == 1 else [c[3 * t + k] for t in kept for k in range(3)] for c in colors or []]
+    return part_points, part_tris, part_normals, part_st, part_colors
+
+
+def material_subsets(ignored_subset=False, size=160):
+    """The reference's material-subsets-v1 fixture (SetMaterialSubsets,
+    material_fixtures.cpp:1840-1939 in hydra-lotus), which its golden images
+    validation/reference/material-subsets-v1-{mean,variance}.pfm were
+    rendered from, in the form extraction hands the renderer: each bound
+    GeomSubset a mesh of its own faces (and the rest of the mesh another),
+    each with its material — partial and full splits, an unbound rest lit by
+    displayColor, a subset without a binding, another family, coordinate
+    sets per part, an emitting part, a half-covered part, overlapping and
+    out-of-range subsets, a sphere's top, a hole, a material shared by two
+    parts, a colour set per part and a mirrored card. ``ignored_subset``
+    binds Partial's subset to the mesh's grey (the fixture's negative
+    control, IgnoredSubset)."""
+    s = material_studio("material-subsets-v1", size)
+    palette_tex = s.add_texture(_texture_image(4, _palette), abi.TEXTURE_RGBA8_SRGB)
+    clamp = abi.WRAP_CLAMP
+    red, blue, grey = (0.8, 0.1, 0.05), (0.1, 0.2, 0.8), (0.6, 0.6, 0.6)
+    teal = (0.2, 0.6, 0.7)
+
+    def textured():
+        m = preview_material()
+        m.lookups[abi.SLOT_BASE_COLOR] = s.add_texture_input(palette_tex, wrap_s=clamp, wrap_t=clamp)
+        return m
+
+    looks = {
+        "Grey": (preview_material(grey, roughness=0.3), None, None),
+        "Red": (preview_material(red, roughness=0.3), None, None),
+        "Blue": (preview_material(blue, roughness=0.3), None, None),
+        "Glow": (preview_material(emission=(2.0, 1.0, 0.5)), None, None),
+        "Half": (preview_material(red, opacity=0.5), None, None),
+        "Palette": (textured(), "st", None),
+        "Turned": (textured(), "uv1", None),
+        "Tint": (preview_material((0.0, 0.0, 0.0), roughness=0.4), None, "tint"),
+        "": (preview_material(teal), None, None),  # an unbound part's displayColor material
+    }
+    slot = {name: s.add_material(m) for name, (m, _, _) in looks.items()}
+    # TwoQuads: the left and right quads, faces 0 and 1.
+    quad_points = [(-0.5, -0.5, 0.0), (0.0, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (0.0, 0.5, 0.0),
+                   (-0.5, 0.5, 0.0)]
+    quad_tris = [(0, 1, 4), (0, 4, 5), (1, 2, 3), (1, 3, 4)]
+    quad_faces = (0, 0, 1, 1)
+
+    def corners(face):
+        return [face[0], face[1], face[2], face[0], face[2], face[3]]
+
+    left = [(0, 0), (0.5, 0), (0.5, 1), (0, 1)]
+    right = [(0.5, 0), (1, 0), (1, 1), (0.5, 1)]
+    swap = lambda face: [(t_, s_) for s_, t_ in face]
+    sets_st = {"st": corners(left) + corners(right), "uv1": corners(swap(left)) + corners(swap(right))}
+    tints = [(1, 0, 0), (1, 0.5, 0), (1, 1, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1)]
+    tinted = {"tint": [tints[v] for tri in quad_tris for v in tri]}
+    teal_colors = {"displayColor": [teal]}
+
+    def quads(faces, st=None, colors=None):
+        st_names = sorted(st) if st else []
+        color_names = sorted(colors) if colors else []
+        p, t, _, part_st, part_colors = _faces_of(
+            quad_points, quad_tris, quad_faces, faces, texcoords=[st[n] for n in st_names],
+            colors=[colors[n] for n in color_names])
+        return (p, t, None, dict(zip(st_names, part_st)), dict(zip(color_names, part_colors)))
+
+    points, polys = coarse_sphere_polygons()
+    sphere_corners = coarse_sphere_corners(polys)
+    fixed = [[_fixed(c) for c in p] for p in points]
+    sphere_tris = [(sphere_corners[i][0], sphere_corners[i + 1][0], sphere_corners[i + 2][0])
+                   for i in range(0, len(sphere_corners), 3)]
+    sphere_faces = [sphere_corners[i][1] for i in range(0, len(sphere_corners), 3)]
+    sphere_normals = np.array([fixed[v] for v, _, _ in sphere_corners], dtype=F32).reshape(-1, 3, 3)
+
+    def ball(faces):
+        p, t, n, _, _ = _faces_of(fixed, sphere_tris, sphere_faces, faces, normals=sphere_normals)
+        return (p, t, n, {}, {})
+
+    top, bottom = set(range(32)), set(range(32, len(polys)))
+    whole = quads({0, 1})
+
+    def partial(mesh_look, subset_look):
+        return [(quads({0}), mesh_look), (quads({1}), subset_look)]
+
+    objects = [
+        (partial("Grey", "Grey" if ignored_subset else "Red"), 0.7, 0.7),
+        ([(quads({0}), "Red"), (quads({1}), "Blue")], 0.7, 0.7),
+        ([(quads({0}, colors=teal_colors), ""), (quads({1}, colors=teal_colors), "Red")], 0.7, 0.7),
+        ([(whole, "Blue")], 0.7, 0.7),
+        (partial("Blue", "Red"), 0.7, 0.7),
+        ([(quads({0}, st=sets_st), "Turned"), (quads({1}, st=sets_st), "Palette")], 0.7, 0.7),
+        (partial("Grey", "Glow"), 0.7, 0.7),
+        (partial("Grey", "Half"), 0.7, 0.7),
+        ([(whole, "Red")], 0.7, 0.7),
+        (partial("Grey", "Red"), 0.7, 0.7),
+        ([(ball(bottom), "Grey"), (ball(top), "Red")], 0.35, 0.35),
+        ([(quads({1}), "Red")], 0.7, 0.7),
+        ([(quads({0}), "Red"), (quads({1}), "Red")], 0.7, 0.7),
+        ([(quads({0}, colors=tinted), "Grey"), (quads({1}, colors=tinted), "Tint")], 0.7, 0.7),
+        (partial("Grey", "Red"), -0.7, 0.7),
+    ]
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (0.8, 0.0, -0.8)
+    for i, (parts, scale_x, scale) in enumerate(objects):
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0], placed[5], placed[10] = scale_x, scale, scale
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        for (p, t, n, st, colors), look in parts:
+            g = s.add_geometry(p, t, n)
+            st_names, color_names = sorted(st), sorted(colors)
+            if st_names:
+                s.set_texcoords(g, np.stack([st[k] for k in st_names]))
+            if color_names:
+                s.set_colors(g, [colors[k] for k in color_names])
+            _, wants_st, wants_color = looks[look]
+            tex_set = st_names.index(wants_st) + 1 if wants_st in st_names else 0
+            color_set = color_names.index(wants_color) + 1 if wants_color in color_names else 0
+            s.add_instance(g, slot[look], placed, texcoord_set=tex_set, color_set=color_set)
+    return s

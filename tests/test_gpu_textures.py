@@ -12,7 +12,9 @@ EvaluatePreview and Coverage, scene.slang:315-413, 1184-1260).
   with its negative control.
 - The same for material-primvars-v1 (colour sets read as a base colour:
   per corner, per face, per mesh, displayColor, an absent set, clamped
-  colours, displayOpacity), with its negative control (SwappedColors).
+  colours, displayOpacity), with its negative control (SwappedColors), and
+  material-subsets-v1 (GeomSubset bindings as extraction splits them),
+  with its negative control (IgnoredSubset).
 - Every path of those fixtures, and of a scene of texture-masked coverage
   (threshold and fractional), textured emission (light samples included)
   and an inverted mask, equals the oracle's.
@@ -71,10 +73,10 @@ def test_material_textures_negative_control_rejected(cuda, renderer, golden_text
     assert not c.ok, c
 
 
-FIXTURES = ["alpha", "normals", "transmission", "transforms", "emission", "primvars"]
+FIXTURES = ["alpha", "normals", "transmission", "transforms", "emission", "primvars", "subsets"]
 NEGATIVE = {"alpha": {"srgb_alpha": True}, "normals": {"flipped_green": True}, "transmission": {"untinted": True},
             "transforms": {"reversed_rotation": True}, "emission": {"raw_emission": True},
-            "primvars": {"swapped_colors": True}}
+            "primvars": {"swapped_colors": True}, "subsets": {"ignored_subset": True}}
 # Levels of the DES-Q5 comparison. On cards that show only a texture's
 # emission (material-emission-v1's unlit card, material-transforms-v1's
 # emission card) the golden's variance is the pixel jitter's alone, and the
@@ -122,7 +124,7 @@ def test_material_fixture_negative_control_rejected(cuda, renderer, goldens, fix
 @pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
 @pytest.mark.parametrize("scene_name", ["material_textures", "texture_cutouts", "material_alpha", "material_normals",
                                         "material_transmission", "material_transforms", "material_emission",
-                                        "material_primvars"])
+                                        "material_primvars", "material_subsets"])
 def test_textured_paths_match_oracle(cuda, renderer, oracle_lib, integrator, light_sampling, scene_name):
     scene = getattr(scenes, scene_name)()
     st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,
