@@ -2443,3 +2443,116 @@ def material_subsets(ignored_subset=False, size=160):
             color_set = color_names.index(wants_color) + 1 if wants_color in color_names else 0
             s.add_instance(g, slot[look], placed, texcoord_set=tex_set, color_set=color_set)
     return s
+
+
+def _ramp(x, y):
+    v = 15 + 15 * (x + 4 * y)
+    return (v, v, v, 255)
+
+
+def material_mtlx(unweighted_image=False, size=160):
+    """The reference's material-mtlx-v1 fixture (SetMaterialMtlx,
+    material_fixtures.cpp:1247-1382 in hydra-lotus), which its golden
+    images validation/reference/material-mtlx-v1-{mean,variance}.pfm were
+    rendered from, in the form its MaterialX translator hands the renderer:
+    Standard Surface networks as UsdPreviewSurface materials (weighted base
+    colours, metal, ior 2.5 and 1, emission times its colour, opacity,
+    clamped inputs, unrepresented lobes, precedence over a preview
+    surface), image lookups (sRGB and raw, a weighted image, metalness and
+    roughness channels, an emission map, periodic / clamp / mirror /
+    constant addressing, a named coordinate set, normal maps at two scales,
+    tiling) and defaults of what is not translated, on coarse spheres
+    (scale 0.35) and cards (0.7) of the 5x5 grid. ``unweighted_image``
+    drops the weighted image's 0.5 base weight (the fixture's negative
+    control, UnweightedImage)."""
+    s = material_studio("material-mtlx-v1", size)
+    srgb = s.add_texture(_texture_image(4, _palette), abi.TEXTURE_RGBA8_SRGB)
+    raw = s.add_texture(_texture_image(4, _palette), abi.TEXTURE_RGBA8_UNORM)
+    rgba = s.add_texture(_texture_image(4, _rgba), abi.TEXTURE_RGBA8_UNORM)
+    ramp = s.add_texture(_texture_image(4, _ramp), abi.TEXTURE_RGBA8_UNORM)
+    tilts = s.add_texture(_texture_image(4, _tilts), abi.TEXTURE_RGBA8_UNORM)
+    rep, clamp, mirror, black = abi.WRAP_REPEAT, abi.WRAP_CLAMP, abi.WRAP_MIRROR, abi.WRAP_BLACK
+
+    def standard(base=(0.8, 0.8, 0.8), roughness=0.2, **kw):
+        return preview_material(base, roughness=roughness, **kw)
+
+    def textured(texture, wrap=rep, uv="st", **kw):
+        m = standard()
+        m.lookups[abi.SLOT_BASE_COLOR] = s.add_texture_input(texture, wrap_s=wrap, wrap_t=wrap, **kw)
+        return m, uv
+
+    def bumpy(scale):
+        m = standard((0.7, 0.7, 0.7), 0.4)
+        m.lookups[abi.SLOT_NORMAL] = s.add_texture_input(
+            tilts, wrap_s=rep, wrap_t=rep, scale=(2.0 * scale, 2.0 * scale, 2.0, 1.0),
+            bias=(-scale, -scale, -1.0, 0.0), fallback=(-scale, -scale, -1.0, 1.0))
+        return m, "st"
+
+    copper, teal, black_ = (0.95, 0.64, 0.54), (0.2, 0.6, 0.7), (0.0, 0.0, 0.0)
+    channels = standard(copper)
+    channels.lookups[abi.SLOT_METALLIC] = s.add_texture_input(rgba, channel=2, wrap_s=rep, wrap_t=rep)
+    channels.lookups[abi.SLOT_ROUGHNESS] = s.add_texture_input(ramp, wrap_s=rep, wrap_t=rep)
+    emission_map = standard(black_)
+    emission_map.lookups[abi.SLOT_EMISSION] = s.add_texture_input(raw, wrap_s=rep, wrap_t=rep)
+    weight = 1.0 if unweighted_image else 0.5
+    looks = {
+        "Defaults": (standard(), None),
+        "Weighted": (standard((float(F32(0.5) * F32(0.9)), float(F32(0.5) * F32(0.3)),
+                               float(F32(0.5) * F32(0.1)))), None),
+        "Metal": (standard(copper, 0.3, metallic=1.0), None),
+        "Ior": (standard((0.1, 0.2, 0.6), 0.1, ior=2.5), None),
+        "NoSpecular": (standard((0.6, 0.6, 0.6), 0.1, ior=1.0), None),
+        "Emissive": (standard(black_, emission=(2.0, float(F32(2.0) * F32(0.6)), float(F32(2.0) * F32(0.2)))),
+                     None),
+        "Opacity": (standard(teal, opacity=0.5), None),
+        "Clamped": (standard((1.0, float(F32(1.5) * F32(0.5)), 0.0), 1.0), None),
+        "Lobes": (standard(teal), None),
+        "Precedence": (standard((0.1, 0.2, 0.8)), None),
+        "Srgb": textured(srgb),
+        "Raw": textured(raw),
+        "WeightedImage": textured(srgb, scale=(weight, weight, weight, 1.0), fallback=(0.0, 0.0, 0.0, 1.0)),
+        "Channels": (channels, "st"),
+        "EmissionMap": (emission_map, "st"),
+        "Clamp": textured(srgb, wrap=clamp),
+        "Mirror": textured(srgb, wrap=mirror),
+        "Constant": textured(srgb, wrap=black),
+        "Named": textured(srgb, uv="uv1"),
+        "NormalMap": bumpy(1.0),
+        "NormalScale": bumpy(0.5),
+        "Tiled": textured(srgb),
+        "Fileless": (standard((0.2, 0.6, 0.9)), None),
+        "Untranslated": (standard(), None),
+    }
+    slot = {name: (s.add_material(m), uv) for name, (m, uv) in looks.items()}
+    smooth = _coarse_smooth_sphere(s)
+    bumpy_sphere = _wrapped_sphere(s)
+
+    def card(sets):
+        g = s.add_geometry(np.array([(-0.5, -0.5, 0.0), (0.5, -0.5, 0.0), (0.5, 0.5, 0.0), (-0.5, 0.5, 0.0)],
+                                    dtype=F32), np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32))
+        if sets:
+            s.set_texcoords(g, np.array([[[f[0], f[1], f[2]], [f[0], f[2], f[3]]] for f in sets], dtype=F32))
+        return g, ["st", "uv1"][:len(sets)]
+
+    unit = [(0, 0), (1, 0), (1, 1), (0, 1)]
+    wide_face = [(-0.5, -0.5), (1.5, -0.5), (1.5, 1.5), (-0.5, 1.5)]
+    turned = [(1, 0), (1, 1), (0, 1), (0, 0)]
+    plain, mapped, wide, named = card([]), card([unit]), card([wide_face]), card([unit, turned])
+    sphere = (smooth, [])
+    bumpy_geo = (bumpy_sphere, ["st"])
+    objects = [("Defaults", sphere), ("Weighted", sphere), ("Metal", sphere), ("Ior", sphere),
+               ("NoSpecular", sphere), ("Emissive", plain), ("Opacity", plain), ("Clamped", plain),
+               ("Lobes", plain), ("Precedence", plain), ("Srgb", mapped), ("Raw", mapped),
+               ("WeightedImage", mapped), ("Channels", mapped), ("EmissionMap", mapped), ("Srgb", wide),
+               ("Clamp", wide), ("Mirror", wide), ("Constant", wide), ("Named", named),
+               ("NormalMap", bumpy_geo), ("NormalScale", mapped), ("Tiled", mapped), ("Fileless", plain),
+               ("Untranslated", mapped)]
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (1.6, 0.8, 0.0, -0.8, -1.6)
+    for i, (look, (geo, sets)) in enumerate(objects):
+        material, uv = slot[look]
+        scale = 0.35 if geo in (smooth, bumpy_sphere) else 0.7
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = placed[5] = placed[10] = scale
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        s.add_instance(geo, material, placed, texcoord_set=sets.index(uv) + 1 if uv in sets else 0)
+    return s

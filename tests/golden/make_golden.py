@@ -43,6 +43,9 @@ little-endian; ReadPfm, adapters/common/reference.cpp:100-131):
 - material_subsets_v1.npz: the material-subsets-v1 fixture
   (adapters/common/material_fixtures.cpp:1840-1939: GeomSubset bindings as
   extraction splits them) at 160x160, 4096 samples per pixel.
+- material_mtlx_v1.npz: the material-mtlx-v1 fixture
+  (adapters/common/material_fixtures.cpp:1247-1382: Standard Surface
+  networks as translated) at 160x160, 4096 samples per pixel.
 - material_gltf_v1.npz and material_gltf_extensions_v1.npz: the
   material-gltf-v1 and material-gltf-extensions-v1 fixtures
   (adapters/common/material_fixtures.cpp:2035-2300: MaterialX's glTF PBR
@@ -77,7 +80,8 @@ FIXTURES = [("cornell-box", "cornell_box.npz", 1024),
             ("material-gltf-v1", "material_gltf_v1.npz", 4096),
             ("material-gltf-extensions-v1", "material_gltf_extensions_v1.npz", 4096),
             ("material-primvars-v1", "material_primvars_v1.npz", 4096),
-            ("material-subsets-v1", "material_subsets_v1.npz", 4096)]
+            ("material-subsets-v1", "material_subsets_v1.npz", 4096),
+            ("material-mtlx-v1", "material_mtlx_v1.npz", 4096)]
 TABLES = "albedo_tables_reference.npz"
 TABLE_STRIDE = 7
 
