@@ -2556,3 +2556,92 @@ def material_mtlx(unweighted_image=False, size=160):
         placed[12], placed[13] = columns[i % 5], rows[i // 5]
         s.add_instance(geo, material, placed, texcoord_set=sets.index(uv) + 1 if uv in sets else 0)
     return s
+
+
+def _srgb_to_linear(value):
+    """The sRGB transfer function's decode, in double (IEC 61966-2-1)."""
+    return value / 12.92 if value <= 0.04045 else ((value + 0.055) / 1.055) ** 2.4
+
+
+def material_graphs(reversed_gltf_rotation=False, size=160):
+    """The reference's material-graphs-v1 fixture (SetMaterialGraphs,
+    material_fixtures.cpp:1440-1564 in hydra-lotus), which its golden
+    images validation/reference/material-graphs-v1-{mean,variance}.pfm were
+    rendered from, in the form its MaterialX graph translator hands the
+    renderer: 25 st-mapped cards (scale 0.7) whose Standard Surface base
+    colours come from node graphs folded into constants or texture inputs —
+    sRGB and linear constants, sRGB and raw images, separated channels, a
+    colour image times its colour, multiply / mix / weight / add as scale
+    and bias, tiling, place2d in both operation orders, a glTF image's
+    placement, coordinate arithmetic, glTF and ND normal maps, invert,
+    combine, clamp, a mix's default, a file-less image's default, a folded
+    power, an image's alpha as roughness, and an untranslated graph's
+    default. ``reversed_gltf_rotation`` turns the glTF image's rotation the
+    other way (the fixture's negative control, ReversedGltfRotation)."""
+    s = material_studio("material-graphs-v1", size)
+    srgb = s.add_texture(_texture_image(4, _palette), abi.TEXTURE_RGBA8_SRGB)
+    raw = s.add_texture(_texture_image(4, _palette), abi.TEXTURE_RGBA8_UNORM)
+    rgba_tex = s.add_texture(_texture_image(4, _rgba), abi.TEXTURE_RGBA8_UNORM)
+    tilts = s.add_texture(_texture_image(4, _tilts), abi.TEXTURE_RGBA8_UNORM)
+    rep = abi.WRAP_REPEAT
+
+    def standard(base=(0.8, 0.8, 0.8), roughness=0.2):
+        return preview_material(base, roughness=roughness)
+
+    def lookup(texture=None, **kw):
+        return s.add_texture_input(srgb if texture is None else texture, wrap_s=rep, wrap_t=rep, **kw)
+
+    def textured(**kw):
+        m = standard()
+        m.lookups[abi.SLOT_BASE_COLOR] = lookup(**kw)
+        return m
+
+    def bumpy(fallback):
+        m = standard((0.7, 0.7, 0.7), 0.4)
+        m.lookups[abi.SLOT_NORMAL] = lookup(tilts, scale=(2.0, 2.0, 2.0, 1.0), bias=(-1.0, -1.0, -1.0, 0.0),
+                                            fallback=fallback)
+        return m
+
+    decoded = tuple(float(F32(_srgb_to_linear(float(F32(c))))) for c in (0.8, 0.4, 0.2))
+    separate = standard((0.95, 0.64, 0.54))
+    separate.lookups[abi.SLOT_ROUGHNESS] = lookup(rgba_tex, channel=1)
+    separate.lookups[abi.SLOT_METALLIC] = lookup(rgba_tex, channel=2)
+    placed_scale, placed_offset, degrees = (2.0, 1.0), (float(F32(0.1)), float(F32(0.2))), 30.0
+    half = dict(scale=(0.5, 0.5, 0.5, 1.0), fallback=(0.0, 0.0, 0.0, 1.0))
+    folded = tuple(float(F32((float(F32(c)) + float(F32(0.1))) ** 2.0)) for c in (0.2, 0.3, 0.4))
+    alpha = standard()
+    alpha.lookups[abi.SLOT_BASE_COLOR] = lookup(rgba_tex, fallback=(0.0, 0.0, 0.0, 0.0))
+    alpha.lookups[abi.SLOT_ROUGHNESS] = lookup(rgba_tex, fallback=(0.0, 0.0, 0.0, 0.0), channel=3)
+    rotation = -degrees if reversed_gltf_rotation else degrees
+    looks = [
+        standard(decoded), standard(decoded),
+        textured(), textured(texture=raw), separate,
+        textured(scale=(1.0, 0.5, 0.25, 1.0), fallback=(0.0, 0.0, 0.0, 0.0)),
+        textured(**half), textured(**half), textured(**half),
+        textured(scale=(0.5, 0.5, 0.5, 1.0), bias=(0.1, 0.1, 0.1, 0.0), fallback=(0.1, 0.1, 0.1, 1.0)),
+        textured(st_transform=(2.0, 0.0, -0.25, 0.0, 3.0, -0.5)),
+        textured(st_transform=tuple(float(F32(v)) for v in _place2d((0.5, 0.5), placed_scale, degrees,
+                                                                      placed_offset, 0))),
+        textured(st_transform=tuple(float(F32(v)) for v in _place2d((0.5, 0.5), placed_scale, degrees,
+                                                                      placed_offset, 1))),
+        textured(st_transform=gltf_place(placed_scale, rotation, placed_offset)),
+        textured(st_transform=(2.0, 0.0, 0.25, 0.0, 2.0, 0.0)),
+        bumpy((0.0, 0.0, 1.0, 1.0)), bumpy((-1.0, -1.0, -1.0, 1.0)),
+        textured(scale=(-1.0, -1.0, -1.0, 1.0), bias=(1.0, 1.0, 1.0, 0.0), fallback=(1.0, 1.0, 1.0, 1.0)),
+        textured(scale=(0.5, 1.0, 1.0, 1.0)),
+        textured(),
+        textured(scale=(0.0, 0.0, 0.0, 1.0), bias=(0.2, 0.6, 0.9, 0.0), fallback=(0.2, 0.6, 0.9, 1.0)),
+        standard((float(F32(0.5) * F32(0.4)), 0.5, float(F32(0.5) * F32(1.6)))),
+        standard(folded),
+        alpha,
+        standard(),
+    ]
+    card = _unit_card(s)
+    columns, rows = (-1.6, -0.8, 0.0, 0.8, 1.6), (1.6, 0.8, 0.0, -0.8, -1.6)
+    for i, m in enumerate(looks):
+        placed = np.eye(4, dtype=F32).reshape(-1)
+        placed[0] = placed[5] = placed[10] = 0.7
+        placed[12], placed[13] = columns[i % 5], rows[i // 5]
+        uses_st = any(k != 0 for k in m.lookups)
+        s.add_instance(card, s.add_material(m), placed, texcoord_set=1 if uses_st else 0)
+    return s

@@ -63,11 +63,11 @@ def golden_normals():
 def golden_fixtures():
     """The reference's material-transmission-v1, material-transforms-v1,
     material-emission-v1, material-gltf-v1, material-gltf-extensions-v1,
-    material-primvars-v1, material-subsets-v1 and material-mtlx-v1 golden
-    images (4096 spp), by fixture name."""
+    material-primvars-v1, material-subsets-v1, material-mtlx-v1 and
+    material-graphs-v1 golden images (4096 spp), by fixture name."""
     return {name: load_golden(f"material_{name}_v1.npz")
             for name in ("transmission", "transforms", "emission", "gltf", "gltf_extensions", "primvars",
-                         "subsets", "mtlx")}
+                         "subsets", "mtlx", "graphs")}
 
 
 @pytest.fixture(scope="session")

@@ -46,6 +46,9 @@ little-endian; ReadPfm, adapters/common/reference.cpp:100-131):
 - material_mtlx_v1.npz: the material-mtlx-v1 fixture
   (adapters/common/material_fixtures.cpp:1247-1382: Standard Surface
   networks as translated) at 160x160, 4096 samples per pixel.
+- material_graphs_v1.npz: the material-graphs-v1 fixture
+  (adapters/common/material_fixtures.cpp:1440-1564: MaterialX node graphs
+  as translated) at 160x160, 4096 samples per pixel.
 - material_gltf_v1.npz and material_gltf_extensions_v1.npz: the
   material-gltf-v1 and material-gltf-extensions-v1 fixtures
   (adapters/common/material_fixtures.cpp:2035-2300: MaterialX's glTF PBR
@@ -81,7 +84,8 @@ FIXTURES = [("cornell-box", "cornell_box.npz", 1024),
             ("material-gltf-extensions-v1", "material_gltf_extensions_v1.npz", 4096),
             ("material-primvars-v1", "material_primvars_v1.npz", 4096),
             ("material-subsets-v1", "material_subsets_v1.npz", 4096),
-            ("material-mtlx-v1", "material_mtlx_v1.npz", 4096)]
+            ("material-mtlx-v1", "material_mtlx_v1.npz", 4096),
+            ("material-graphs-v1", "material_graphs_v1.npz", 4096)]
 TABLES = "albedo_tables_reference.npz"
 TABLE_STRIDE = 7
 

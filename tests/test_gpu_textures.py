@@ -16,7 +16,8 @@ EvaluatePreview and Coverage, scene.slang:315-413, 1184-1260).
   material-subsets-v1 (GeomSubset bindings as extraction splits them),
   with its negative control (IgnoredSubset), and material-mtlx-v1
   (Standard Surface networks as translated), with its negative control
-  (UnweightedImage).
+  (UnweightedImage), and material-graphs-v1 (MaterialX node graphs as
+  translated), with its negative control (ReversedGltfRotation).
 - Every path of those fixtures, and of a scene of texture-masked coverage
   (threshold and fractional), textured emission (light samples included)
   and an inverted mask, equals the oracle's.
@@ -75,11 +76,11 @@ def test_material_textures_negative_control_rejected(cuda, renderer, golden_text
     assert not c.ok, c
 
 
-FIXTURES = ["alpha", "normals", "transmission", "transforms", "emission", "primvars", "subsets", "mtlx"]
+FIXTURES = ["alpha", "normals", "transmission", "transforms", "emission", "primvars", "subsets", "mtlx", "graphs"]
 NEGATIVE = {"alpha": {"srgb_alpha": True}, "normals": {"flipped_green": True}, "transmission": {"untinted": True},
             "transforms": {"reversed_rotation": True}, "emission": {"raw_emission": True},
             "primvars": {"swapped_colors": True}, "subsets": {"ignored_subset": True},
-            "mtlx": {"unweighted_image": True}}
+            "mtlx": {"unweighted_image": True}, "graphs": {"reversed_gltf_rotation": True}}
 # Levels of the DES-Q5 comparison. On cards that show only a texture's
 # emission (material-emission-v1's unlit card, material-transforms-v1's
 # emission card) the golden's variance is the pixel jitter's alone, and the
@@ -127,7 +128,8 @@ def test_material_fixture_negative_control_rejected(cuda, renderer, goldens, fix
 @pytest.mark.parametrize("light_sampling", [abi.LIGHT_SAMPLING_BSDF, abi.LIGHT_SAMPLING_MIS])
 @pytest.mark.parametrize("scene_name", ["material_textures", "texture_cutouts", "material_alpha", "material_normals",
                                         "material_transmission", "material_transforms", "material_emission",
-                                        "material_primvars", "material_subsets", "material_mtlx"])
+                                        "material_primvars", "material_subsets", "material_mtlx",
+                                        "material_graphs"])
 def test_textured_paths_match_oracle(cuda, renderer, oracle_lib, integrator, light_sampling, scene_name):
     scene = getattr(scenes, scene_name)()
     st = abi.default_settings(integrator=integrator, light_sampling=light_sampling,

@@ -41,6 +41,9 @@ reference's DES-Q5 comparison, and each fixture's negative control.
   Surface networks as the translator hands them over (UsdPreviewSurface
   materials with lookups); the weighted image's base weight dropped
   (UnweightedImage) must be rejected.
+- validation/reference/material-graphs-v1 (4096 spp): MaterialX node graphs
+  folded into constants and lookups by the translator; the glTF image's
+  rotation reversed (ReversedGltfRotation) must be rejected.
 - validation/reference/material-gltf-v1 and material-gltf-extensions-v1
   (4096 spp): MaterialX's glTF PBR surface through the composed closure
   and its albedo tables (constants, images, packed channels, placements,
@@ -150,14 +153,15 @@ def test_oracle_material_normals_negative_control_rejected(oracle_lib, golden_no
 NEGATIVE = {"transmission": {"untinted": True}, "transforms": {"reversed_rotation": True},
             "emission": {"raw_emission": True}, "gltf": {"exchanged_channels": True},
             "gltf_extensions": {"exchanged_coat": True}, "primvars": {"swapped_colors": True},
-            "subsets": {"ignored_subset": True}, "mtlx": {"unweighted_image": True}}
+            "subsets": {"ignored_subset": True}, "mtlx": {"unweighted_image": True},
+            "graphs": {"reversed_gltf_rotation": True}}
 # material-emission-v1 at 256 spp: one 8x8 tile of the unlit card (pure
 # emission from the sRGB palette, so the golden's variance is the pixel
 # jitter's alone) sits 0.25% above the reference's, 6.3 standard errors;
 # every other tile and the 16-spp level pass.
 LEVELS = {"transmission": (16, 256), "transforms": (16, 256), "emission": (16,), "gltf": (16, 256, 1024),
           "gltf_extensions": (16, 256, 1024), "primvars": (16, 256, 1024), "subsets": (16, 256, 1024),
-          "mtlx": (16, 256, 1024)}
+          "mtlx": (16, 256, 1024), "graphs": (16, 256, 1024)}
 
 
 @pytest.mark.parametrize("name,spp", [(n, s) for n in sorted(NEGATIVE) for s in LEVELS[n]])
