@@ -14,7 +14,7 @@
 // u32 width, height; f32 scale[3], rows[9]; f32 texels[4 w h]); per
 // geometry u32 vertices, triangles, has_normals, f32 positions[3 v], u32
 // indices[3 t], f32 normals[9 t] when present; per instance f32 m[16], u32
-// geometry, material; per material the 80-byte lotus_material; the frame:
+// geometry, material; per material the lotus_material; the frame:
 // f32 world_to_clip[16], u32 width, height, integrator, light_sampling,
 // max_bounces, sample_index, frame_count.
 #include <cstdio>
@@ -204,18 +204,55 @@ int main(int argc, char** argv) {
   for (uint32_t i = 0; i < nm; ++i) {
     const lotus_material& lm = materials[i];
     Lotus::SceneMaterial sm;
-    Lotus::PreviewSurface p;
-    std::memcpy(p.base_color.data(), lm.base_color, 12);
-    p.roughness = lm.roughness;
-    std::memcpy(p.emission.data(), lm.emission, 12);
-    p.metallic = lm.metallic;
-    std::memcpy(p.specular_color.data(), lm.specular_color, 12);
-    p.ior = lm.ior;
-    std::memcpy(p.transmission_color.data(), lm.transmission_color, 12);
-    p.transmission = lm.transmission;
-    p.use_specular_workflow = (lm.flags & LOTUS_MATERIAL_SPECULAR_WORKFLOW) != 0;
-    p.thin_walled = (lm.flags & LOTUS_MATERIAL_THIN_WALLED) != 0;
-    sm.material.surface = p;
+    std::optional<Lotus::TextureInput>* slots[LOTUS_TEXTURE_SLOTS] = {};
+    slots[LOTUS_SLOT_OPACITY] = &sm.material.geometry.opacity_texture;
+    slots[LOTUS_SLOT_NORMAL] = &sm.material.geometry.normal_texture;
+    if (lm.model == LOTUS_MODEL_GLTF_PBR) {
+      // MaterialX's glTF PBR surface (material.hpp:180-217).
+      Lotus::GltfPbr& g = sm.material.surface.emplace<Lotus::GltfPbr>();
+      std::memcpy(g.base_color.value.data(), lm.base_color, 12);
+      g.metallic.value = lm.metallic;
+      g.roughness.value = lm.roughness;
+      std::memcpy(g.emissive.value.data(), lm.emission, 12);
+      g.emissive_strength = lm.emissive_strength;
+      g.ior = lm.ior;
+      g.specular.value = lm.specular;
+      std::memcpy(g.specular_color.value.data(), lm.specular_color, 12);
+      g.transmission.value = lm.transmission;
+      g.clearcoat.value = lm.clearcoat;
+      g.clearcoat_roughness.value = lm.clearcoat_roughness;
+      std::memcpy(g.sheen_color.value.data(), lm.sheen_color, 12);
+      g.sheen_roughness.value = lm.sheen_roughness;
+      slots[LOTUS_GLTF_SLOT_BASE_COLOR] = &g.base_color.texture;
+      slots[LOTUS_GLTF_SLOT_METALLIC] = &g.metallic.texture;
+      slots[LOTUS_GLTF_SLOT_ROUGHNESS] = &g.roughness.texture;
+      slots[LOTUS_GLTF_SLOT_EMISSIVE] = &g.emissive.texture;
+      slots[LOTUS_GLTF_SLOT_SPECULAR] = &g.specular.texture;
+      slots[LOTUS_GLTF_SLOT_SPECULAR_COLOR] = &g.specular_color.texture;
+      slots[LOTUS_GLTF_SLOT_TRANSMISSION] = &g.transmission.texture;
+      slots[LOTUS_GLTF_SLOT_CLEARCOAT] = &g.clearcoat.texture;
+      slots[LOTUS_GLTF_SLOT_CLEARCOAT_ROUGHNESS] = &g.clearcoat_roughness.texture;
+      slots[LOTUS_GLTF_SLOT_CLEARCOAT_NORMAL] = &g.clearcoat_normal_texture;
+      slots[LOTUS_GLTF_SLOT_SHEEN_COLOR] = &g.sheen_color.texture;
+      slots[LOTUS_GLTF_SLOT_SHEEN_ROUGHNESS] = &g.sheen_roughness.texture;
+    } else {
+      Lotus::PreviewSurface& p = sm.material.surface.emplace<Lotus::PreviewSurface>();
+      std::memcpy(p.base_color.data(), lm.base_color, 12);
+      p.roughness = lm.roughness;
+      std::memcpy(p.emission.data(), lm.emission, 12);
+      p.metallic = lm.metallic;
+      std::memcpy(p.specular_color.data(), lm.specular_color, 12);
+      p.ior = lm.ior;
+      std::memcpy(p.transmission_color.data(), lm.transmission_color, 12);
+      p.transmission = lm.transmission;
+      p.use_specular_workflow = (lm.flags & LOTUS_MATERIAL_SPECULAR_WORKFLOW) != 0;
+      p.thin_walled = (lm.flags & LOTUS_MATERIAL_THIN_WALLED) != 0;
+      slots[LOTUS_SLOT_BASE_COLOR] = &p.base_color_texture;
+      slots[LOTUS_SLOT_ROUGHNESS] = &p.roughness_texture;
+      slots[LOTUS_SLOT_METALLIC] = &p.metallic_texture;
+      slots[LOTUS_SLOT_EMISSION] = &p.emission_texture;
+      slots[LOTUS_SLOT_SPECULAR_COLOR] = &p.specular_color_texture;
+    }
     sm.material.geometry.opacity = lm.opacity;
     sm.material.geometry.opacity_threshold = lm.opacity_threshold;
     std::memcpy(sm.material.geometry.texcoord_fallback.data(), lm.texcoord_fallback, 8);
@@ -223,12 +260,8 @@ int main(int argc, char** argv) {
       std::memcpy(sm.material.geometry.normal.data(), lm.normal, 12);
     // Each slot's lookup, its image resolved as the host's extraction
     // would (SceneMaterial::textures; none for a key without an image).
-    auto& preview = std::get<Lotus::PreviewSurface>(sm.material.surface);
-    std::optional<Lotus::TextureInput>* slots[LOTUS_TEXTURE_SLOTS] = {&sm.material.geometry.opacity_texture,
-        &sm.material.geometry.normal_texture, &preview.base_color_texture, &preview.roughness_texture,
-        &preview.metallic_texture, &preview.emission_texture, &preview.specular_color_texture};
     for (uint32_t k = 0; k < LOTUS_TEXTURE_SLOTS; ++k) {
-      if (lm.lookups[k] == LOTUS_NO_LOOKUP || lm.lookups[k] > inputs.size()) continue;
+      if (!slots[k] || lm.lookups[k] == LOTUS_NO_LOOKUP || lm.lookups[k] > inputs.size()) continue;
       const lotus_texture_input& d = inputs[lm.lookups[k] - 1];
       Lotus::TextureInput t;
       t.texture = d.texture == LOTUS_NO_TEXTURE ? std::string("missing") : "tex" + std::to_string(d.texture);

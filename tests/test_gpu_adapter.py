@@ -38,6 +38,9 @@ ADAPTER_SCENES = {
     # and fallbacks, normal maps, mapped by the adapter from the
     # reference's Texture / TextureInput / MeshGeometry::texcoords.
     "material_textures": lambda: scenes.material_textures(size=64),
+    # glTF PBR materials with every extension and their lookups.
+    "material_gltf": lambda: scenes.material_gltf(size=64),
+    "material_gltf_extensions": lambda: scenes.material_gltf_extensions(size=64),
     "material_normals": lambda: scenes.material_normals(size=64),
     "texture_cutouts": lambda: scenes.texture_cutouts(size=64),
 }
